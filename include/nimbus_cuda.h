@@ -1,0 +1,238 @@
+/*
+ * nimbus_cuda.h -- C-ABI of the B200 (sm_100a) CUDA backend for the Nimbus
+ * dynamical-core hot path: the Klemp-Wilhelmson split-explicit acoustic
+ * substep loop and the conservative WENO5 scalar transport on the flat
+ * Cartesian Arakawa C-grid.
+ *
+ * Plain pointers and sizes only.  Every field is row-major [nx][ny][nz] float
+ * (k fastest, index (i*ny + j)*nz + k): u on x-faces i+1/2, v on y-faces
+ * j+1/2, w on z-faces k+1/2, scalars at cell centres.  Base-state columns are
+ * FP64, as the reference CPU solver holds them.
+ *
+ * Memory: each argument block names where its field pointers live.
+ *   NIMBUS_MEMORY_HOST    host arrays; the call stages them through the
+ *                         context's device workspace and returns after the
+ *                         results are back in the host arrays (the reference's
+ *                         "fence-confirmed" dispatch contract).  A refused or
+ *                         failed call leaves every host array untouched.
+ *   NIMBUS_MEMORY_DEVICE  device pointers; the call enqueues on `stream` (a
+ *                         cudaStream_t, NULL = the context's stream) and returns
+ *                         without synchronising.
+ *
+ * Errors: every entry point returns a nimbus_status; nimbus_cuda_last_error()
+ * gives the message of the last failure on that context.  No exception or
+ * C++ type crosses this boundary.  A context is used by one host thread at a
+ * time.
+ */
+#ifndef NIMBUS_CUDA_H
+#define NIMBUS_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NIMBUS_CUDA_ABI_VERSION 1
+
+typedef enum nimbus_status
+{
+    NIMBUS_OK = 0,
+    NIMBUS_ERR_INVALID_ARGUMENT = 1, /* dispatch refused before any mutation */
+    NIMBUS_ERR_CUDA = 2,             /* a CUDA runtime call failed */
+    NIMBUS_ERR_OUT_OF_MEMORY = 3,    /* device allocation or admission failed */
+    NIMBUS_ERR_NONFINITE = 4,        /* a produced value was non-finite; outputs not published */
+    NIMBUS_ERR_UNSUPPORTED = 5,      /* valid request outside this backend's contract */
+    NIMBUS_ERR_NO_DEVICE = 6         /* no usable sm_100 device */
+} nimbus_status;
+
+typedef enum nimbus_memory
+{
+    NIMBUS_MEMORY_HOST = 0,
+    NIMBUS_MEMORY_DEVICE = 1
+} nimbus_memory;
+
+/* Lateral boundary codes: tmv::init::config::LateralBC (include/init/config/config_v1.hpp:40-48). */
+enum
+{
+    NIMBUS_BC_PERIODIC = 0,
+    NIMBUS_BC_RADIATIVE = 1,
+    NIMBUS_BC_RIGID = 2,
+    NIMBUS_BC_RIGID_SLIP = 3,
+    NIMBUS_BC_ZERO_GRADIENT = 4
+};
+/* Bottom: BottomBC {RigidNoSlip, RigidSlip}; top: TopBC {Rigid, RigidWithSponge, Open}. */
+enum
+{
+    NIMBUS_BOTTOM_NO_SLIP = 0,
+    NIMBUS_BOTTOM_SLIP = 1
+};
+enum
+{
+    NIMBUS_TOP_RIGID = 0,
+    NIMBUS_TOP_SPONGE = 1,
+    NIMBUS_TOP_OPEN = 2
+};
+
+typedef struct nimbus_cuda_context nimbus_cuda_context;
+
+/* Context lifecycle.  Replaces ComputeBackend::initialize / shutdown
+ * (include/compute/backend_interface.hpp:19-60) for the CUDA backend: binds a
+ * device, creates a stream, and owns the staging workspace.  Fails with
+ * NIMBUS_ERR_NO_DEVICE when no sm_100 device is present -- there is no CPU
+ * fallback. */
+nimbus_status nimbus_cuda_create(int device, nimbus_cuda_context** out);
+void nimbus_cuda_destroy(nimbus_cuda_context* ctx);
+const char* nimbus_cuda_last_error(const nimbus_cuda_context* ctx);
+int nimbus_cuda_abi_version(void);
+/* Kernels this context launched so far (all entry points); the analogue of
+ * ComputeBackend::successful_kernel_dispatch_count (backend_interface.hpp:55-60). */
+uint64_t nimbus_cuda_kernel_launches(const nimbus_cuda_context* ctx);
+/* The context's stream, as a cudaStream_t. */
+void* nimbus_cuda_stream(const nimbus_cuda_context* ctx);
+/* Waits for all work on the context's stream, then reads and clears the
+ * device status word that NIMBUS_MEMORY_DEVICE calls accumulate: returns
+ * NIMBUS_ERR_NONFINITE if any enqueued call produced a non-finite retained
+ * mass flux or transported scalar since the last check. */
+nimbus_status nimbus_cuda_synchronize(nimbus_cuda_context* ctx);
+
+/*
+ * One fused acoustic substep, in place on (u, v, w, rho, p).
+ * Replaces DynamicsComputeKernels::dispatch_acoustic_substep_fused_cartesian_cgrid
+ * (include/compute/dispatch/dynamics.hpp:220-277,686; CPU semantics
+ * src/compute/cpu/acoustic_cgrid_fast.cpp:12-219): flux-form continuity on
+ * 1<=i<=nx-2, 1<=j<=ny-2, all k; rho forward Euler with fallback and clamp;
+ * p = p00 (rho R_d theta / p00)^gamma with clamp; then u,v,w forward Euler
+ * from the new pressure gradient (k<=nz-2) with clamps.  Interior arithmetic
+ * is FP64 over FP32 storage, the reference's own sequence.
+ * drho_scratch is optional (NULL = not written); when given it receives the
+ * stored FP32 continuity tendency.  Requires nx>=3, ny>=3, nz>=2, base_len>=nz.
+ */
+typedef struct nimbus_acoustic_fused_args
+{
+    float* u;
+    float* v;
+    float* w;
+    float* rho;
+    float* p;
+    const float* theta;
+    const double* rho0_base; /* FP64 [base_len] */
+    const double* p0_base;   /* FP64 [base_len] */
+    int base_len;
+    int nx, ny, nz;
+    double dx, dy, dz;
+    double dt_small;
+    double gamma;            /* cp / (cp - R_d) */
+    float rho_min, rho_max;
+    float p_min, p_max;
+    float p_ref_fallback;
+    float wind_clamp_h, wind_clamp_v;
+    float* drho_scratch;
+    int memory;              /* nimbus_memory */
+    void* stream;            /* cudaStream_t for NIMBUS_MEMORY_DEVICE, NULL = context stream */
+} nimbus_acoustic_fused_args;
+
+nimbus_status nimbus_cuda_acoustic_fused(nimbus_cuda_context* ctx, const nimbus_acoustic_fused_args* a);
+
+/*
+ * All n_substeps acoustic substeps of one large step in one submission, with
+ * the boundary closure after every substep and the time-averaged face mass
+ * flux exported.  Replaces
+ * DynamicsComputeKernels::dispatch_acoustic_substeps_batched_cartesian_cgrid
+ * (include/compute/dispatch/dynamics.hpp:279-326,726; contract
+ * include/compute/acoustic_cgrid_dispatch_contract.hpp:114-156) and follows
+ * the CPU loop order of SplitExplicitScheme::step_split_acoustic
+ * (src/numerics/time_stepping/schemes/split_explicit/split_explicit.cpp:174-260):
+ *   per substep: mass_flux += weight * rho_face * (velocity - frame) from the
+ *   pre-substep state (advection_cartesian.cpp:610-870, unfused FP64 add);
+ *   fused substep; boundary closure W, E, S, N, vertical with the KW78
+ *   radiation integrated over dt_small
+ *   (boundary_conditions_cartesian_cgrid.cpp:884-1187).
+ * wave_history (in) / wave_history_output (out): KW78 face memory, layout
+ *   u_west[ny*nz], u_east[ny*nz], v_south[nx*nz], v_north[nx*nz]
+ *   (2*(nx+ny)*nz floats).  wave_history NULL seeds it from the current faces
+ *   (seed_acoustic_radiation, :798-822).  The two may be the same array.
+ * density_begin: optional; receives rho at loop start (the scalar-paired
+ *   density of CartesianCGridTransportContext::capture_density_begin).
+ * mass_flux_*: accumulated into (callers zero them at the start of a large
+ *   step, as CartesianCGridTransportContext::begin does).
+ * Requires nx>=4, ny>=4, nz>=2, 1<=n_substeps<=4096.
+ */
+typedef struct nimbus_acoustic_batched_args
+{
+    float* u;
+    float* v;
+    float* w;
+    float* rho;
+    float* p;
+    const float* theta;
+    const double* rho0_base;
+    const double* p0_base;
+    int base_len;
+    int nx, ny, nz;
+    double dx, dy, dz;
+    double dt_small;
+    int n_substeps;
+    double gamma;
+    float rho_min, rho_max;
+    float p_min, p_max;
+    float p_ref_fallback;
+    float wind_clamp_h, wind_clamp_v;
+    int bc_west, bc_east, bc_south, bc_north, bc_bottom, bc_top;
+    float* mass_flux_x;
+    float* mass_flux_y;
+    float* mass_flux_z;
+    int accumulate_mass_flux;
+    double mass_flux_weight;  /* dt_small / dt_large */
+    float frame_velocity_u_ms, frame_velocity_v_ms;
+    const float* wave_history;
+    float* wave_history_output;
+    float* density_begin;
+    int memory;
+    void* stream;
+} nimbus_acoustic_batched_args;
+
+nimbus_status nimbus_cuda_acoustic_batched(nimbus_cuda_context* ctx, const nimbus_acoustic_batched_args* a);
+
+/*
+ * Conservative flux-form transport of n_scalars scalars against the retained
+ * time-averaged face mass fluxes.  Replaces
+ * AdvectionComputeKernels::dispatch_advect_scalars_conservative_cartesian_cgrid
+ * (include/compute/dispatch/advection.hpp:154-230; CPU semantics
+ * advect_scalar_conservative_3d_cartesian_impl, advection_cartesian.cpp:1652-2640):
+ * face value by WENO5-JS where the 5-point stencil fits, else the MC-limited
+ * slope (weno5_face.hpp:43-86, advection_cartesian.cpp:1943-2172);
+ * positive-definite donor limiting for flagged scalars (:2174-2240);
+ * phi_new = (rho_begin phi - dt div SF) / max(rho_end, rho_floor) on
+ * 1<=i<=nx-2, 1<=j<=ny-2, all k (:2465-2640).  q_in[s] may equal q_out[s]
+ * (in place).  At most 16 scalars.
+ */
+typedef struct nimbus_scalar_transport_args
+{
+    const float* const* q_in;
+    float* const* q_out;
+    const int* positive_definite;
+    int n_scalars;
+    int nx, ny, nz;
+    double dx, dy, dz;
+    double dt;
+    const float* rho_end;
+    const float* rho_begin;
+    const float* mass_flux_x;
+    const float* mass_flux_y;
+    const float* mass_flux_z;
+    int weno;                 /* 1 = WENO5 (production), 0 = MC everywhere */
+    int top_open;             /* C-grid open top owns the k=nz-1 boundary face */
+    float rho_floor;          /* 0.05 (density_min_kgm3) */
+    int memory;
+    void* stream;
+} nimbus_scalar_transport_args;
+
+nimbus_status nimbus_cuda_scalar_transport(nimbus_cuda_context* ctx, const nimbus_scalar_transport_args* a);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NIMBUS_CUDA_H */

@@ -1,0 +1,52 @@
+"""Builds the in-tree CUDA backend library for sm_100a.
+
+    python -m nimbus_b200.build
+
+Produces nimbus_b200/lib/libnimbus_cuda.so from nimbus_b200/csrc with
+`nvcc -gencode arch=compute_100a,code=sm_100a`.  The reference-precision
+kernels are compiled with --fmad=false: the CPU solver they match performs
+every multiply and add separately, and a contracted FMA would change the
+rounding of stored values.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+CSRC = PKG / "csrc"
+LIB = PKG / "lib"
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def sources():
+    return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cuh")) + [PKG.parent / "include" / "nimbus_cuda.h"]
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    LIB.mkdir(exist_ok=True)
+    out = LIB / "libnimbus_cuda.so"
+    newest = max(p.stat().st_mtime for p in sources())
+    if out.exists() and not force and out.stat().st_mtime >= newest:
+        return out
+    cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
+           str(CSRC / "nimbus_cuda.cu"), "-o", str(out)]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return out
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))

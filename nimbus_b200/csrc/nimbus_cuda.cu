@@ -1,0 +1,599 @@
+// C-ABI of the B200 CUDA backend (include/nimbus_cuda.h).
+//
+// Host-memory calls stage through a per-context device workspace and return
+// fence-confirmed, leaving host arrays untouched on any refusal or failure
+// (include/compute/dispatch/dynamics.hpp:682-683).  Device-memory calls only
+// enqueue; nimbus_cuda_synchronize() reports their status word.
+#include "../../include/nimbus_cuda.h"
+
+#include "acoustic_kernels.cuh"
+#include "transport_kernels.cuh"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <utility>
+
+using namespace nimbus;
+
+namespace
+{
+
+constexpr int kThreads = 256;
+
+struct DeviceBuffer
+{
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+
+enum Slot
+{
+    kU, kV, kW, kRho, kP, kTheta, kRhoAlt, kDrho, kRho0, kP0, kMfx, kMfy, kMfz, kWave, kRhoBegin,
+    kRhoEnd, kSf, kRl, kQ0, kSlotCount = kQ0 + 2 * kMaxScalars
+};
+
+}  // namespace
+
+struct nimbus_cuda_context
+{
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    unsigned* status = nullptr;  // device status word
+    uint64_t launches = 0;
+    std::string error;
+    DeviceBuffer ws[kSlotCount];
+};
+
+namespace
+{
+
+nimbus_status fail(nimbus_cuda_context* ctx, nimbus_status s, const std::string& msg)
+{
+    if (ctx) ctx->error = msg;
+    return s;
+}
+
+nimbus_status cuda_fail(nimbus_cuda_context* ctx, cudaError_t e, const char* where)
+{
+    return fail(ctx, e == cudaErrorMemoryAllocation ? NIMBUS_ERR_OUT_OF_MEMORY : NIMBUS_ERR_CUDA,
+                std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define NB_CUDA(ctx, call)                                   \
+    do {                                                     \
+        cudaError_t e_ = (call);                             \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
+    } while (0)
+
+template <class T>
+nimbus_status ensure(nimbus_cuda_context* ctx, Slot slot, size_t count, T** out)
+{
+    DeviceBuffer& b = ctx->ws[slot];
+    const size_t bytes = count * sizeof(T);
+    if (b.bytes < bytes)
+    {
+        if (b.ptr) cudaFree(b.ptr);
+        b.ptr = nullptr;
+        b.bytes = 0;
+        void* p = nullptr;
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "workspace allocation");
+        b.ptr = p;
+        b.bytes = bytes;
+    }
+    *out = static_cast<T*>(b.ptr);
+    return NIMBUS_OK;
+}
+
+int grid_for(const nimbus_cuda_context* ctx, long long work)
+{
+    long long blocks = (work + kThreads - 1) / kThreads;
+    const long long cap = static_cast<long long>(ctx->sm_count) * 16;
+    if (blocks > cap) blocks = cap;
+    return blocks < 1 ? 1 : static_cast<int>(blocks);
+}
+
+bool finite_positive(double v) { return std::isfinite(v) && v > 0.0; }
+bool valid_bounds(float lo, float hi) { return std::isfinite(lo) && std::isfinite(hi) && lo > 0.0f && lo <= hi; }
+bool cells_fit(int nx, int ny, int nz)
+{
+    return static_cast<long long>(nx) * ny * nz < static_cast<long long>(std::numeric_limits<int>::max()) / 4;
+}
+
+// Mirrors valid_acoustic_cgrid_dispatch (src/compute/cpu/acoustic_cgrid.cpp:11-46).
+const char* check_acoustic_common(const float* u, const float* v, const float* w, const float* rho, const float* p,
+                                  const float* theta, const double* rho0, const double* p0, int base_len, int nx,
+                                  int ny, int nz, double dx, double dy, double dz, double dt, double gamma,
+                                  float rho_min, float rho_max, float p_min, float p_max, float p_ref,
+                                  float wind_h, float wind_v)
+{
+    if (!u || !v || !w || !rho || !p || !theta || !rho0 || !p0) return "a required field pointer is null";
+    if (nx < 3 || ny < 3 || nz < 2) return "grid must be at least 3x3x2";
+    if (!cells_fit(nx, ny, nz)) return "grid too large for one dispatch";
+    if (base_len < nz) return "base profiles shorter than nz";
+    if (!finite_positive(dx) || !finite_positive(dy) || !finite_positive(dz)) return "grid spacing must be finite and positive";
+    if (!finite_positive(dt)) return "dt_small must be finite and positive";
+    if (!finite_positive(gamma)) return "gamma must be finite and positive";
+    if (!valid_bounds(rho_min, rho_max) || !valid_bounds(p_min, p_max)) return "invalid clamp bounds";
+    if (!finite_positive(p_ref)) return "p_ref_fallback must be finite and positive";
+    if (!std::isfinite(wind_h) || wind_h < 0.0f || !std::isfinite(wind_v) || wind_v < 0.0f) return "invalid wind clamps";
+    const void* outs[] = {u, v, w, rho, p};
+    for (int a = 0; a < 5; ++a)
+    {
+        if (outs[a] == theta) return "theta aliases an output field";
+        for (int b = 0; b < a; ++b)
+            if (outs[a] == outs[b]) return "output fields alias";
+    }
+    return nullptr;
+}
+
+AcousticParams acoustic_params(int nx, int ny, int nz, double dx, double dy, double dz, double dt, double gamma,
+                               float rho_min, float rho_max, float p_min, float p_max, float p_ref, float wind_h,
+                               float wind_v)
+{
+    AcousticParams P{};
+    P.d = Dims{nx, ny, nz};
+    P.inv_dx = 1.0 / dx;
+    P.inv_dy = 1.0 / dy;
+    P.inv_dz = 1.0 / dz;
+    P.dt_small = dt;
+    P.gamma = gamma;
+    P.rho_min = rho_min;
+    P.rho_max = rho_max;
+    P.p_min = p_min;
+    P.p_max = p_max;
+    P.p_ref_fallback = p_ref;
+    P.wind_h = wind_h;
+    P.wind_v = wind_v;
+    return P;
+}
+
+nimbus_status upload(nimbus_cuda_context* ctx, void* dst, const void* src, size_t bytes)
+{
+    NB_CUDA(ctx, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    return NIMBUS_OK;
+}
+
+nimbus_status download(nimbus_cuda_context* ctx, void* dst, const void* src, size_t bytes)
+{
+    NB_CUDA(ctx, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    return NIMBUS_OK;
+}
+
+nimbus_status read_status(nimbus_cuda_context* ctx, cudaStream_t stream, unsigned* flags)
+{
+    unsigned h = 0;
+    NB_CUDA(ctx, cudaMemcpyAsync(&h, ctx->status, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+    NB_CUDA(ctx, cudaMemsetAsync(ctx->status, 0, sizeof(unsigned), stream));
+    NB_CUDA(ctx, cudaStreamSynchronize(stream));
+    *flags = h;
+    return NIMBUS_OK;
+}
+
+#define NB_TRY(expr)                         \
+    do {                                     \
+        nimbus_status s_ = (expr);           \
+        if (s_ != NIMBUS_OK) return s_;      \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// Device-side sequences (all pointers device memory).
+// ---------------------------------------------------------------------------
+
+struct AcousticDevice
+{
+    float *u, *v, *w, *rho, *p;
+    const float* theta;
+    const double *rho0, *p0;
+    float* rho_alt;   // ping-pong partner of rho
+    float* drho;      // optional
+    float *mfx, *mfy, *mfz;  // optional (all or none)
+};
+
+// One substep: continuity+EOS into rho_next, momentum in place.  Returns the
+// buffer now holding rho.
+float* launch_substep(nimbus_cuda_context* ctx, cudaStream_t st, const AcousticParams& P, float* rho_cur,
+                      float* rho_next, const AcousticDevice& D)
+{
+    const int blocks = grid_for(ctx, P.d.cells());
+    acoustic_continuity_eos_kernel<<<blocks, kThreads, 0, st>>>(P, rho_cur, D.u, D.v, D.w, D.theta, D.rho0, rho_next,
+                                                                D.p, D.drho, D.mfx, D.mfy, D.mfz, ctx->status);
+    acoustic_momentum_kernel<<<blocks, kThreads, 0, st>>>(P, rho_next, D.p, D.p0, D.u, D.v, D.w);
+    ctx->launches += 2;
+    return rho_next;
+}
+
+void launch_boundaries(nimbus_cuda_context* ctx, cudaStream_t st, const BoundaryParams& B, const AcousticDevice& D,
+                       float* rho, float* wave)
+{
+    const Dims d = B.d;
+    const int yz = d.ny * d.nz, xz = d.nx * d.nz;
+    acoustic_bc_we_kernel<<<grid_for(ctx, yz), kThreads, 0, st>>>(B, D.u, D.v, D.w, rho, D.p, wave, wave + yz);
+    acoustic_bc_sn_kernel<<<grid_for(ctx, xz), kThreads, 0, st>>>(B, D.u, D.v, D.w, rho, D.p, wave + 2 * yz,
+                                                                  wave + 2 * yz + xz);
+    acoustic_bc_vertical_kernel<<<grid_for(ctx, d.nx * d.ny), kThreads, 0, st>>>(B, D.u, D.v, D.w);
+    ctx->launches += 3;
+}
+
+nimbus_status run_batched_device(nimbus_cuda_context* ctx, cudaStream_t st, const nimbus_acoustic_batched_args* a,
+                                 const AcousticDevice& D, float* wave, const float* wave_in, float* density_begin)
+{
+    const Dims d{a->nx, a->ny, a->nz};
+    const size_t n = static_cast<size_t>(d.cells());
+    const int yz = d.ny * d.nz, xz = d.nx * d.nz;
+    if (wave_in == nullptr)
+    {
+        acoustic_seed_radiation_kernel<<<grid_for(ctx, yz + xz), kThreads, 0, st>>>(d, D.u, D.v, wave);
+        ctx->launches += 1;
+    }
+    else if (wave_in != wave)
+    {
+        NB_CUDA(ctx, cudaMemcpyAsync(wave, wave_in, sizeof(float) * 2 * (yz + xz), cudaMemcpyDeviceToDevice, st));
+    }
+    if (density_begin)
+        NB_CUDA(ctx, cudaMemcpyAsync(density_begin, D.rho, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+
+    AcousticParams P = acoustic_params(a->nx, a->ny, a->nz, a->dx, a->dy, a->dz, a->dt_small, a->gamma, a->rho_min,
+                                       a->rho_max, a->p_min, a->p_max, a->p_ref_fallback, a->wind_clamp_h,
+                                       a->wind_clamp_v);
+    P.weight = a->mass_flux_weight;
+    P.frame_u = a->frame_velocity_u_ms;
+    P.frame_v = a->frame_velocity_v_ms;
+    P.top_open = a->bc_top == kTopOpen;
+
+    BoundaryParams B{};
+    B.d = d;
+    B.west = a->bc_west; B.east = a->bc_east; B.south = a->bc_south; B.north = a->bc_north;
+    B.bottom = a->bc_bottom; B.top = a->bc_top;
+    B.dt_rad = static_cast<float>(a->dt_small);
+    B.inv_dx = 1.0f / static_cast<float>(a->dx);
+    B.inv_dy = 1.0f / static_cast<float>(a->dy);
+    B.frame_u = a->frame_velocity_u_ms;
+    B.frame_v = a->frame_velocity_v_ms;
+
+    float* cur = D.rho;
+    float* alt = D.rho_alt;
+    for (int s = 0; s < a->n_substeps; ++s)
+    {
+        float* now = launch_substep(ctx, st, P, cur, alt, D);
+        launch_boundaries(ctx, st, B, D, now, wave);
+        alt = cur;
+        cur = now;
+    }
+    if (cur != D.rho)
+        NB_CUDA(ctx, cudaMemcpyAsync(D.rho, cur, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+    NB_CUDA(ctx, cudaGetLastError());
+    return NIMBUS_OK;
+}
+
+const char* check_batched(const nimbus_acoustic_batched_args* a)
+{
+    const char* why = check_acoustic_common(a->u, a->v, a->w, a->rho, a->p, a->theta, a->rho0_base, a->p0_base,
+                                            a->base_len, a->nx, a->ny, a->nz, a->dx, a->dy, a->dz, a->dt_small,
+                                            a->gamma, a->rho_min, a->rho_max, a->p_min, a->p_max,
+                                            a->p_ref_fallback, a->wind_clamp_h, a->wind_clamp_v);
+    if (why) return why;
+    if (a->nx < 4 || a->ny < 4) return "batched acoustic loop needs nx>=4 and ny>=4";
+    if (a->n_substeps < 1 || a->n_substeps > 4096) return "n_substeps must be in [1, 4096]";
+    for (int bc : {a->bc_west, a->bc_east, a->bc_south, a->bc_north})
+        if (bc < 0 || bc > 4) return "lateral boundary code out of range";
+    if (a->bc_bottom < 0 || a->bc_bottom > 1 || a->bc_top < 0 || a->bc_top > 2) return "vertical boundary code out of range";
+    if (!a->wave_history_output) return "wave_history_output is required";
+    if (a->accumulate_mass_flux)
+    {
+        if (!a->mass_flux_x || !a->mass_flux_y || !a->mass_flux_z) return "mass flux outputs are required";
+        if (!finite_positive(a->mass_flux_weight)) return "mass_flux_weight must be finite and positive";
+    }
+    if (!std::isfinite(a->frame_velocity_u_ms) || !std::isfinite(a->frame_velocity_v_ms)) return "frame velocity must be finite";
+    return nullptr;
+}
+
+const char* check_transport(const nimbus_scalar_transport_args* a)
+{
+    if (a->n_scalars < 0 || a->n_scalars > kMaxScalars) return "n_scalars must be in [0, 16]";
+    if (a->n_scalars == 0) return nullptr;
+    if (!a->q_in || !a->q_out || !a->positive_definite) return "scalar pointer arrays are required";
+    if (!a->rho_end || !a->rho_begin || !a->mass_flux_x || !a->mass_flux_y || !a->mass_flux_z)
+        return "density and mass-flux pointers are required";
+    if (a->nx < 3 || a->ny < 3 || a->nz < 2) return "grid must be at least 3x3x2";
+    if (!cells_fit(a->nx, a->ny, a->nz)) return "grid too large for one dispatch";
+    if (!finite_positive(a->dx) || !finite_positive(a->dy) || !finite_positive(a->dz) || !finite_positive(a->dt))
+        return "spacing and dt must be finite and positive";
+    if (!(std::isfinite(a->rho_floor) && a->rho_floor > 0.0f)) return "rho_floor must be finite and positive";
+    for (int s = 0; s < a->n_scalars; ++s)
+    {
+        if (!a->q_in[s] || !a->q_out[s]) return "null scalar field";
+        for (int t = 0; t < s; ++t)
+            if (a->q_out[s] == a->q_out[t] || a->q_in[s] == a->q_in[t]) return "duplicate scalar field";
+    }
+    return nullptr;
+}
+
+TransportParams transport_params(const nimbus_scalar_transport_args* a)
+{
+    TransportParams T{};
+    T.d = Dims{a->nx, a->ny, a->nz};
+    T.inv_dx = 1.0 / a->dx;
+    T.inv_dy = 1.0 / a->dy;
+    T.inv_dz = 1.0 / a->dz;
+    T.dt = a->dt;
+    T.rho_floor = static_cast<double>(a->rho_floor);
+    T.weno = a->weno != 0;
+    T.top_open = a->top_open != 0;
+    T.n_scalars = a->n_scalars;
+    for (int s = 0; s < a->n_scalars; ++s) T.positive_definite[s] = a->positive_definite[s] != 0;
+    return T;
+}
+
+nimbus_status run_transport_device(nimbus_cuda_context* ctx, cudaStream_t st, const TransportParams& T,
+                                   const float* rho_end, const float* rho_begin, const float* mfx, const float* mfy,
+                                   const float* mfz)
+{
+    const size_t n = static_cast<size_t>(T.d.cells());
+    float* sf = nullptr;
+    float* rl = nullptr;
+    NB_TRY(ensure(ctx, kSf, 3 * n * T.n_scalars, &sf));
+    NB_TRY(ensure(ctx, kRl, n * T.n_scalars, &rl));
+    const dim3 grid(grid_for(ctx, T.d.cells()), T.n_scalars);
+    transport_faces_kernel<<<grid, kThreads, 0, st>>>(T, mfx, mfy, mfz, sf);
+    transport_limiter_kernel<<<grid, kThreads, 0, st>>>(T, rho_begin, sf, rl);
+    transport_update_kernel<<<grid, kThreads, 0, st>>>(T, rho_end, rho_begin, sf, rl, ctx->status);
+    ctx->launches += 3;
+    NB_CUDA(ctx, cudaGetLastError());
+    return NIMBUS_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Exported entry points.
+// ---------------------------------------------------------------------------
+
+extern "C" {
+
+int nimbus_cuda_abi_version(void) { return NIMBUS_CUDA_ABI_VERSION; }
+
+nimbus_status nimbus_cuda_create(int device, nimbus_cuda_context** out)
+{
+    if (!out) return NIMBUS_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0 || device < 0 || device >= count)
+        return NIMBUS_ERR_NO_DEVICE;
+    cudaDeviceProp prop{};
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return NIMBUS_ERR_NO_DEVICE;
+    if (prop.major != 10) return NIMBUS_ERR_NO_DEVICE;  // built for sm_100a only
+    auto* ctx = new (std::nothrow) nimbus_cuda_context();
+    if (!ctx) return NIMBUS_ERR_OUT_OF_MEMORY;
+    ctx->device = device;
+    ctx->sm_count = prop.multiProcessorCount;
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&ctx->status, sizeof(unsigned)) != cudaSuccess || cudaMemset(ctx->status, 0, sizeof(unsigned)) != cudaSuccess)
+    {
+        nimbus_cuda_destroy(ctx);
+        return NIMBUS_ERR_CUDA;
+    }
+    *out = ctx;
+    return NIMBUS_OK;
+}
+
+void nimbus_cuda_destroy(nimbus_cuda_context* ctx)
+{
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (auto& b : ctx->ws)
+        if (b.ptr) cudaFree(b.ptr);
+    if (ctx->status) cudaFree(ctx->status);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char* nimbus_cuda_last_error(const nimbus_cuda_context* ctx) { return ctx ? ctx->error.c_str() : "null context"; }
+uint64_t nimbus_cuda_kernel_launches(const nimbus_cuda_context* ctx) { return ctx ? ctx->launches : 0; }
+void* nimbus_cuda_stream(const nimbus_cuda_context* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
+
+nimbus_status nimbus_cuda_synchronize(nimbus_cuda_context* ctx)
+{
+    if (!ctx) return NIMBUS_ERR_INVALID_ARGUMENT;
+    unsigned flags = 0;
+    NB_TRY(read_status(ctx, ctx->stream, &flags));
+    if (flags & kStatusNonfiniteMassFlux) return fail(ctx, NIMBUS_ERR_NONFINITE, "non-finite retained face mass flux");
+    if (flags & kStatusNonfiniteTransport) return fail(ctx, NIMBUS_ERR_NONFINITE, "non-finite transported scalar");
+    return NIMBUS_OK;
+}
+
+nimbus_status nimbus_cuda_acoustic_fused(nimbus_cuda_context* ctx, const nimbus_acoustic_fused_args* a)
+{
+    if (!ctx || !a) return NIMBUS_ERR_INVALID_ARGUMENT;
+    if (const char* why = check_acoustic_common(a->u, a->v, a->w, a->rho, a->p, a->theta, a->rho0_base, a->p0_base,
+                                                a->base_len, a->nx, a->ny, a->nz, a->dx, a->dy, a->dz, a->dt_small,
+                                                a->gamma, a->rho_min, a->rho_max, a->p_min, a->p_max,
+                                                a->p_ref_fallback, a->wind_clamp_h, a->wind_clamp_v))
+        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, why);
+    if (a->memory != NIMBUS_MEMORY_HOST && a->memory != NIMBUS_MEMORY_DEVICE)
+        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "unknown memory kind");
+    NB_CUDA(ctx, cudaSetDevice(ctx->device));
+    const size_t n = static_cast<size_t>(a->nx) * a->ny * a->nz;
+    const size_t bytes = n * sizeof(float);
+    const AcousticParams P = acoustic_params(a->nx, a->ny, a->nz, a->dx, a->dy, a->dz, a->dt_small, a->gamma,
+                                             a->rho_min, a->rho_max, a->p_min, a->p_max, a->p_ref_fallback,
+                                             a->wind_clamp_h, a->wind_clamp_v);
+    AcousticDevice D{};
+    cudaStream_t st = ctx->stream;
+    if (a->memory == NIMBUS_MEMORY_DEVICE)
+    {
+        if (a->stream) st = static_cast<cudaStream_t>(a->stream);
+        D = {a->u, a->v, a->w, a->rho, a->p, a->theta, a->rho0_base, a->p0_base, nullptr, a->drho_scratch};
+        NB_TRY(ensure(ctx, kRhoAlt, n, &D.rho_alt));
+        float* now = launch_substep(ctx, st, P, D.rho, D.rho_alt, D);
+        NB_CUDA(ctx, cudaMemcpyAsync(D.rho, now, bytes, cudaMemcpyDeviceToDevice, st));
+        NB_CUDA(ctx, cudaGetLastError());
+        return NIMBUS_OK;
+    }
+    float *u, *v, *w, *rho, *p, *theta, *alt, *drho = nullptr;
+    double *rho0, *p0;
+    NB_TRY(ensure(ctx, kU, n, &u));
+    NB_TRY(ensure(ctx, kV, n, &v));
+    NB_TRY(ensure(ctx, kW, n, &w));
+    NB_TRY(ensure(ctx, kRho, n, &rho));
+    NB_TRY(ensure(ctx, kP, n, &p));
+    NB_TRY(ensure(ctx, kTheta, n, &theta));
+    NB_TRY(ensure(ctx, kRhoAlt, n, &alt));
+    NB_TRY(ensure(ctx, kRho0, static_cast<size_t>(a->nz), &rho0));
+    NB_TRY(ensure(ctx, kP0, static_cast<size_t>(a->nz), &p0));
+    if (a->drho_scratch) NB_TRY(ensure(ctx, kDrho, n, &drho));
+    NB_TRY(upload(ctx, u, a->u, bytes));
+    NB_TRY(upload(ctx, v, a->v, bytes));
+    NB_TRY(upload(ctx, w, a->w, bytes));
+    NB_TRY(upload(ctx, rho, a->rho, bytes));
+    NB_TRY(upload(ctx, p, a->p, bytes));
+    NB_TRY(upload(ctx, theta, a->theta, bytes));
+    NB_TRY(upload(ctx, rho0, a->rho0_base, sizeof(double) * a->nz));
+    NB_TRY(upload(ctx, p0, a->p0_base, sizeof(double) * a->nz));
+    D = {u, v, w, rho, p, theta, rho0, p0, alt, drho};
+    float* now = launch_substep(ctx, st, P, rho, alt, D);
+    NB_CUDA(ctx, cudaGetLastError());
+    NB_CUDA(ctx, cudaStreamSynchronize(st));
+    NB_TRY(download(ctx, a->u, u, bytes));
+    NB_TRY(download(ctx, a->v, v, bytes));
+    NB_TRY(download(ctx, a->w, w, bytes));
+    NB_TRY(download(ctx, a->rho, now, bytes));
+    NB_TRY(download(ctx, a->p, p, bytes));
+    if (drho) NB_TRY(download(ctx, a->drho_scratch, drho, bytes));
+    NB_CUDA(ctx, cudaStreamSynchronize(st));
+    return NIMBUS_OK;
+}
+
+nimbus_status nimbus_cuda_acoustic_batched(nimbus_cuda_context* ctx, const nimbus_acoustic_batched_args* a)
+{
+    if (!ctx || !a) return NIMBUS_ERR_INVALID_ARGUMENT;
+    if (const char* why = check_batched(a)) return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, why);
+    if (a->memory != NIMBUS_MEMORY_HOST && a->memory != NIMBUS_MEMORY_DEVICE)
+        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "unknown memory kind");
+    NB_CUDA(ctx, cudaSetDevice(ctx->device));
+    const size_t n = static_cast<size_t>(a->nx) * a->ny * a->nz;
+    const size_t bytes = n * sizeof(float);
+    const size_t waves = 2 * (static_cast<size_t>(a->nx) + a->ny) * a->nz;
+    const bool mf = a->accumulate_mass_flux != 0;
+    cudaStream_t st = ctx->stream;
+    if (a->memory == NIMBUS_MEMORY_DEVICE)
+    {
+        if (a->stream) st = static_cast<cudaStream_t>(a->stream);
+        AcousticDevice D{a->u, a->v, a->w, a->rho, a->p, a->theta, a->rho0_base, a->p0_base, nullptr, nullptr,
+                         mf ? a->mass_flux_x : nullptr, mf ? a->mass_flux_y : nullptr, mf ? a->mass_flux_z : nullptr};
+        NB_TRY(ensure(ctx, kRhoAlt, n, &D.rho_alt));
+        return run_batched_device(ctx, st, a, D, a->wave_history_output, a->wave_history, a->density_begin);
+    }
+    float *u, *v, *w, *rho, *p, *theta, *alt, *wave, *rb = nullptr, *mx = nullptr, *my = nullptr, *mz = nullptr;
+    double *rho0, *p0;
+    NB_TRY(ensure(ctx, kU, n, &u));
+    NB_TRY(ensure(ctx, kV, n, &v));
+    NB_TRY(ensure(ctx, kW, n, &w));
+    NB_TRY(ensure(ctx, kRho, n, &rho));
+    NB_TRY(ensure(ctx, kP, n, &p));
+    NB_TRY(ensure(ctx, kTheta, n, &theta));
+    NB_TRY(ensure(ctx, kRhoAlt, n, &alt));
+    NB_TRY(ensure(ctx, kWave, waves, &wave));
+    NB_TRY(ensure(ctx, kRho0, static_cast<size_t>(a->nz), &rho0));
+    NB_TRY(ensure(ctx, kP0, static_cast<size_t>(a->nz), &p0));
+    if (a->density_begin) NB_TRY(ensure(ctx, kRhoBegin, n, &rb));
+    if (mf)
+    {
+        NB_TRY(ensure(ctx, kMfx, n, &mx));
+        NB_TRY(ensure(ctx, kMfy, n, &my));
+        NB_TRY(ensure(ctx, kMfz, n, &mz));
+        NB_TRY(upload(ctx, mx, a->mass_flux_x, bytes));
+        NB_TRY(upload(ctx, my, a->mass_flux_y, bytes));
+        NB_TRY(upload(ctx, mz, a->mass_flux_z, bytes));
+    }
+    NB_TRY(upload(ctx, u, a->u, bytes));
+    NB_TRY(upload(ctx, v, a->v, bytes));
+    NB_TRY(upload(ctx, w, a->w, bytes));
+    NB_TRY(upload(ctx, rho, a->rho, bytes));
+    NB_TRY(upload(ctx, p, a->p, bytes));
+    NB_TRY(upload(ctx, theta, a->theta, bytes));
+    NB_TRY(upload(ctx, rho0, a->rho0_base, sizeof(double) * a->nz));
+    NB_TRY(upload(ctx, p0, a->p0_base, sizeof(double) * a->nz));
+    if (a->wave_history) NB_TRY(upload(ctx, wave, a->wave_history, sizeof(float) * waves));
+    AcousticDevice D{u, v, w, rho, p, theta, rho0, p0, alt, nullptr, mx, my, mz};
+    NB_TRY(run_batched_device(ctx, st, a, D, wave, a->wave_history ? wave : nullptr, rb));
+    unsigned flags = 0;
+    NB_TRY(read_status(ctx, st, &flags));
+    if (flags & kStatusNonfiniteMassFlux)
+        return fail(ctx, NIMBUS_ERR_NONFINITE, "non-finite retained face mass flux; host fields left untouched");
+    NB_TRY(download(ctx, a->u, u, bytes));
+    NB_TRY(download(ctx, a->v, v, bytes));
+    NB_TRY(download(ctx, a->w, w, bytes));
+    NB_TRY(download(ctx, a->rho, rho, bytes));
+    NB_TRY(download(ctx, a->p, p, bytes));
+    NB_TRY(download(ctx, a->wave_history_output, wave, sizeof(float) * waves));
+    if (rb) NB_TRY(download(ctx, a->density_begin, rb, bytes));
+    if (mf)
+    {
+        NB_TRY(download(ctx, a->mass_flux_x, mx, bytes));
+        NB_TRY(download(ctx, a->mass_flux_y, my, bytes));
+        NB_TRY(download(ctx, a->mass_flux_z, mz, bytes));
+    }
+    NB_CUDA(ctx, cudaStreamSynchronize(st));
+    return NIMBUS_OK;
+}
+
+nimbus_status nimbus_cuda_scalar_transport(nimbus_cuda_context* ctx, const nimbus_scalar_transport_args* a)
+{
+    if (!ctx || !a) return NIMBUS_ERR_INVALID_ARGUMENT;
+    if (const char* why = check_transport(a)) return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, why);
+    if (a->n_scalars == 0) return NIMBUS_OK;
+    if (a->memory != NIMBUS_MEMORY_HOST && a->memory != NIMBUS_MEMORY_DEVICE)
+        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "unknown memory kind");
+    NB_CUDA(ctx, cudaSetDevice(ctx->device));
+    TransportParams T = transport_params(a);
+    const size_t n = static_cast<size_t>(T.d.cells());
+    const size_t bytes = n * sizeof(float);
+    cudaStream_t st = ctx->stream;
+    if (a->memory == NIMBUS_MEMORY_DEVICE)
+    {
+        if (a->stream) st = static_cast<cudaStream_t>(a->stream);
+        for (int s = 0; s < a->n_scalars; ++s)
+        {
+            T.q_in[s] = a->q_in[s];
+            T.q_out[s] = a->q_out[s];
+        }
+        return run_transport_device(ctx, st, T, a->rho_end, a->rho_begin, a->mass_flux_x, a->mass_flux_y,
+                                    a->mass_flux_z);
+    }
+    float *re, *rb, *mx, *my, *mz;
+    NB_TRY(ensure(ctx, kRhoEnd, n, &re));
+    NB_TRY(ensure(ctx, kRhoBegin, n, &rb));
+    NB_TRY(ensure(ctx, kMfx, n, &mx));
+    NB_TRY(ensure(ctx, kMfy, n, &my));
+    NB_TRY(ensure(ctx, kMfz, n, &mz));
+    NB_TRY(upload(ctx, re, a->rho_end, bytes));
+    NB_TRY(upload(ctx, rb, a->rho_begin, bytes));
+    NB_TRY(upload(ctx, mx, a->mass_flux_x, bytes));
+    NB_TRY(upload(ctx, my, a->mass_flux_y, bytes));
+    NB_TRY(upload(ctx, mz, a->mass_flux_z, bytes));
+    for (int s = 0; s < a->n_scalars; ++s)
+    {
+        float *qi, *qo;
+        NB_TRY(ensure(ctx, static_cast<Slot>(kQ0 + 2 * s), n, &qi));
+        NB_TRY(ensure(ctx, static_cast<Slot>(kQ0 + 2 * s + 1), n, &qo));
+        NB_TRY(upload(ctx, qi, a->q_in[s], bytes));
+        T.q_in[s] = qi;
+        T.q_out[s] = qo;
+    }
+    NB_TRY(run_transport_device(ctx, st, T, re, rb, mx, my, mz));
+    unsigned flags = 0;
+    NB_TRY(read_status(ctx, st, &flags));
+    if (flags & kStatusNonfiniteTransport)
+        return fail(ctx, NIMBUS_ERR_NONFINITE, "non-finite transported scalar; host fields left untouched");
+    for (int s = 0; s < a->n_scalars; ++s) NB_TRY(download(ctx, a->q_out[s], T.q_out[s], bytes));
+    NB_CUDA(ctx, cudaStreamSynchronize(st));
+    return NIMBUS_OK;
+}
+
+}  // extern "C"

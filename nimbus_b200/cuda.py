@@ -1,0 +1,337 @@
+"""ctypes binding of the C-ABI in include/nimbus_cuda.h.
+
+This is the Python stub a maintainer would bind the backend with; the names
+and argument blocks mirror the reference's dispatch structs
+(include/compute/dispatch/dynamics.hpp, include/compute/dispatch/advection.hpp)
+and ``CudaComputeBackend`` mirrors ``ComputeBackend`` /
+``DynamicsComputeKernels`` / ``AdvectionComputeKernels``
+(include/compute/backend_interface.hpp).  Dispatches return ``bool`` as the
+reference's do; ``last_error`` holds the reason for a ``False``.
+
+There is no fallback: if the shared library is missing or no sm_100 device is
+present, construction raises.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from pathlib import Path
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import initial
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libnimbus_cuda.so"
+
+NIMBUS_OK = 0
+STATUS_NAMES = {
+    0: "NIMBUS_OK",
+    1: "NIMBUS_ERR_INVALID_ARGUMENT",
+    2: "NIMBUS_ERR_CUDA",
+    3: "NIMBUS_ERR_OUT_OF_MEMORY",
+    4: "NIMBUS_ERR_NONFINITE",
+    5: "NIMBUS_ERR_UNSUPPORTED",
+    6: "NIMBUS_ERR_NO_DEVICE",
+}
+MEMORY_HOST, MEMORY_DEVICE = 0, 1
+
+_fp = ctypes.POINTER(ctypes.c_float)
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+
+class AcousticFusedArgs(ctypes.Structure):
+    _fields_ = [
+        ("u", _fp), ("v", _fp), ("w", _fp), ("rho", _fp), ("p", _fp), ("theta", _fp),
+        ("rho0_base", _dp), ("p0_base", _dp), ("base_len", ctypes.c_int),
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("dz", ctypes.c_double),
+        ("dt_small", ctypes.c_double), ("gamma", ctypes.c_double),
+        ("rho_min", ctypes.c_float), ("rho_max", ctypes.c_float),
+        ("p_min", ctypes.c_float), ("p_max", ctypes.c_float), ("p_ref_fallback", ctypes.c_float),
+        ("wind_clamp_h", ctypes.c_float), ("wind_clamp_v", ctypes.c_float),
+        ("drho_scratch", _fp), ("memory", ctypes.c_int), ("stream", ctypes.c_void_p),
+    ]
+
+
+class AcousticBatchedArgs(ctypes.Structure):
+    _fields_ = [
+        ("u", _fp), ("v", _fp), ("w", _fp), ("rho", _fp), ("p", _fp), ("theta", _fp),
+        ("rho0_base", _dp), ("p0_base", _dp), ("base_len", ctypes.c_int),
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("dz", ctypes.c_double),
+        ("dt_small", ctypes.c_double), ("n_substeps", ctypes.c_int), ("gamma", ctypes.c_double),
+        ("rho_min", ctypes.c_float), ("rho_max", ctypes.c_float),
+        ("p_min", ctypes.c_float), ("p_max", ctypes.c_float), ("p_ref_fallback", ctypes.c_float),
+        ("wind_clamp_h", ctypes.c_float), ("wind_clamp_v", ctypes.c_float),
+        ("bc_west", ctypes.c_int), ("bc_east", ctypes.c_int), ("bc_south", ctypes.c_int),
+        ("bc_north", ctypes.c_int), ("bc_bottom", ctypes.c_int), ("bc_top", ctypes.c_int),
+        ("mass_flux_x", _fp), ("mass_flux_y", _fp), ("mass_flux_z", _fp),
+        ("accumulate_mass_flux", ctypes.c_int), ("mass_flux_weight", ctypes.c_double),
+        ("frame_velocity_u_ms", ctypes.c_float), ("frame_velocity_v_ms", ctypes.c_float),
+        ("wave_history", _fp), ("wave_history_output", _fp), ("density_begin", _fp),
+        ("memory", ctypes.c_int), ("stream", ctypes.c_void_p),
+    ]
+
+
+class ScalarTransportArgs(ctypes.Structure):
+    _fields_ = [
+        ("q_in", ctypes.POINTER(_fp)), ("q_out", ctypes.POINTER(_fp)), ("positive_definite", _ip),
+        ("n_scalars", ctypes.c_int), ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("dz", ctypes.c_double), ("dt", ctypes.c_double),
+        ("rho_end", _fp), ("rho_begin", _fp), ("mass_flux_x", _fp), ("mass_flux_y", _fp),
+        ("mass_flux_z", _fp), ("weno", ctypes.c_int), ("top_open", ctypes.c_int),
+        ("rho_floor", ctypes.c_float), ("memory", ctypes.c_int), ("stream", ctypes.c_void_p),
+    ]
+
+
+EXPORTED_SYMBOLS = (
+    "nimbus_cuda_abi_version", "nimbus_cuda_create", "nimbus_cuda_destroy", "nimbus_cuda_last_error",
+    "nimbus_cuda_kernel_launches", "nimbus_cuda_stream", "nimbus_cuda_synchronize",
+    "nimbus_cuda_acoustic_fused", "nimbus_cuda_acoustic_batched", "nimbus_cuda_scalar_transport",
+)
+
+
+def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
+    """Load the backend library; raise if it is missing (no fallback path)."""
+    if not path.exists():
+        raise RuntimeError(f"CUDA backend library {path} is missing; run __graft_entry__.build()")
+    lib = ctypes.CDLL(str(path))
+    lib.nimbus_cuda_create.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+    lib.nimbus_cuda_destroy.argtypes = [ctypes.c_void_p]
+    lib.nimbus_cuda_last_error.argtypes = [ctypes.c_void_p]
+    lib.nimbus_cuda_last_error.restype = ctypes.c_char_p
+    lib.nimbus_cuda_kernel_launches.argtypes = [ctypes.c_void_p]
+    lib.nimbus_cuda_kernel_launches.restype = ctypes.c_uint64
+    lib.nimbus_cuda_stream.argtypes = [ctypes.c_void_p]
+    lib.nimbus_cuda_stream.restype = ctypes.c_void_p
+    lib.nimbus_cuda_synchronize.argtypes = [ctypes.c_void_p]
+    lib.nimbus_cuda_acoustic_fused.argtypes = [ctypes.c_void_p, ctypes.POINTER(AcousticFusedArgs)]
+    lib.nimbus_cuda_acoustic_batched.argtypes = [ctypes.c_void_p, ctypes.POINTER(AcousticBatchedArgs)]
+    lib.nimbus_cuda_scalar_transport.argtypes = [ctypes.c_void_p, ctypes.POINTER(ScalarTransportArgs)]
+    return lib
+
+
+def _f(a) -> "ctypes._Pointer":
+    """float* of a host float32 array, or of a device tensor (int address)."""
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return ctypes.cast(ctypes.c_void_p(a), _fp)
+    if hasattr(a, "data_ptr"):
+        assert a.dtype.__str__() == "torch.float32" and a.is_contiguous()
+        return ctypes.cast(ctypes.c_void_p(a.data_ptr()), _fp)
+    assert a.dtype == np.float32 and a.flags["C_CONTIGUOUS"], (a.dtype, a.flags)
+    return a.ctypes.data_as(_fp)
+
+
+def _d(a):
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        assert a.dtype.__str__() == "torch.float64" and a.is_contiguous()
+        return ctypes.cast(ctypes.c_void_p(a.data_ptr()), _dp)
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"], "base profiles must be contiguous float64"
+    return a.ctypes.data_as(_dp)
+
+
+class NimbusCudaError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class Context:
+    """Owns one nimbus_cuda_context (device, stream, staging workspace)."""
+
+    def __init__(self, device: int = 0, lib: Optional[ctypes.CDLL] = None):
+        self.lib = lib or load_library()
+        handle = ctypes.c_void_p()
+        rc = self.lib.nimbus_cuda_create(int(device), ctypes.byref(handle))
+        if rc != NIMBUS_OK:
+            raise NimbusCudaError(rc, "could not create a CUDA context on an sm_100 device")
+        self.handle = handle
+        self.device = device
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.nimbus_cuda_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def last_error(self) -> str:
+        return self.lib.nimbus_cuda_last_error(self.handle).decode()
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(self.lib.nimbus_cuda_kernel_launches(self.handle))
+
+    @property
+    def stream(self) -> int:
+        return int(self.lib.nimbus_cuda_stream(self.handle) or 0)
+
+    def check(self, rc: int):
+        if rc != NIMBUS_OK:
+            raise NimbusCudaError(rc, self.last_error)
+
+    def synchronize(self):
+        self.check(self.lib.nimbus_cuda_synchronize(self.handle))
+
+    # -- raw entry points -------------------------------------------------
+    def acoustic_fused(self, args: AcousticFusedArgs) -> int:
+        return self.lib.nimbus_cuda_acoustic_fused(self.handle, ctypes.byref(args))
+
+    def acoustic_batched(self, args: AcousticBatchedArgs) -> int:
+        return self.lib.nimbus_cuda_acoustic_batched(self.handle, ctypes.byref(args))
+
+    def scalar_transport(self, args: ScalarTransportArgs) -> int:
+        return self.lib.nimbus_cuda_scalar_transport(self.handle, ctypes.byref(args))
+
+
+def clamp_defaults() -> dict:
+    """The reference's dispatch constants (dynamics.cpp:4560-4586, field_bounds.hpp)."""
+    return dict(gamma=initial.GAMMA, rho_min=initial.RHO_MIN, rho_max=initial.RHO_MAX, p_min=initial.P_MIN,
+                p_max=initial.P_MAX, p_ref_fallback=100000.0, wind_clamp_h=initial.WIND_H,
+                wind_clamp_v=initial.WIND_V)
+
+
+def fused_args(st, rho0, p0, dt_small, grid, drho=None, memory=MEMORY_HOST, stream=None) -> AcousticFusedArgs:
+    nx, ny, nz = (st["u"].shape if hasattr(st["u"], "shape") else st["shape"])
+    a = AcousticFusedArgs()
+    a.u, a.v, a.w, a.rho, a.p, a.theta = (_f(st[k]) for k in ("u", "v", "w", "rho", "p", "theta"))
+    a.rho0_base, a.p0_base = _d(rho0), _d(p0)
+    a._keep = (rho0, p0)
+    a.base_len = nz
+    a.nx, a.ny, a.nz = nx, ny, nz
+    a.dx, a.dy, a.dz = grid
+    a.dt_small = dt_small
+    for key, val in clamp_defaults().items():
+        setattr(a, key, val)
+    a.drho_scratch = _f(drho)
+    a.memory = memory
+    a.stream = stream
+    return a
+
+
+def batched_args(st, rho0, p0, dt_small, n_substeps, grid, bc, mfx, mfy, mfz, weight, wave_in, wave_out,
+                 density_begin=None, frame=(0.0, 0.0), memory=MEMORY_HOST, stream=None) -> AcousticBatchedArgs:
+    nx, ny, nz = st["u"].shape
+    a = AcousticBatchedArgs()
+    a.u, a.v, a.w, a.rho, a.p, a.theta = (_f(st[k]) for k in ("u", "v", "w", "rho", "p", "theta"))
+    a.rho0_base, a.p0_base = _d(rho0), _d(p0)
+    a.base_len = nz
+    a.nx, a.ny, a.nz = nx, ny, nz
+    a.dx, a.dy, a.dz = grid
+    a.dt_small = dt_small
+    a.n_substeps = n_substeps
+    for key, val in clamp_defaults().items():
+        setattr(a, key, val)
+    a.bc_west, a.bc_east, a.bc_south, a.bc_north, a.bc_bottom, a.bc_top = (int(x) for x in bc)
+    a.mass_flux_x, a.mass_flux_y, a.mass_flux_z = _f(mfx), _f(mfy), _f(mfz)
+    a.accumulate_mass_flux = 1 if mfx is not None else 0
+    a.mass_flux_weight = weight
+    a.frame_velocity_u_ms, a.frame_velocity_v_ms = frame
+    a.wave_history = _f(wave_in)
+    a.wave_history_output = _f(wave_out)
+    a.density_begin = _f(density_begin)
+    a.memory = memory
+    a.stream = stream
+    return a
+
+
+def transport_args(q_in: Sequence, q_out: Sequence, pd: Sequence[int], rho_end, rho_begin, mfx, mfy, mfz, dt,
+                   grid, weno=True, top_open=False, memory=MEMORY_HOST, stream=None) -> ScalarTransportArgs:
+    n = len(q_in)
+    nx, ny, nz = rho_end.shape
+    a = ScalarTransportArgs()
+    qi = (_fp * max(n, 1))(*[_f(q) for q in q_in])
+    qo = (_fp * max(n, 1))(*[_f(q) for q in q_out])
+    flags = (ctypes.c_int * max(n, 1))(*[int(x) for x in pd])
+    a._keep = (qi, qo, flags)
+    a.q_in, a.q_out, a.positive_definite = qi, qo, flags
+    a.n_scalars = n
+    a.nx, a.ny, a.nz = nx, ny, nz
+    a.dx, a.dy, a.dz = grid
+    a.dt = dt
+    a.rho_end, a.rho_begin = _f(rho_end), _f(rho_begin)
+    a.mass_flux_x, a.mass_flux_y, a.mass_flux_z = _f(mfx), _f(mfy), _f(mfz)
+    a.weno = int(weno)
+    a.top_open = int(top_open)
+    a.rho_floor = initial.RHO_MIN
+    a.memory = memory
+    a.stream = stream
+    return a
+
+
+class CudaComputeBackend:
+    """Mirror of the reference's ComputeBackend for the CUDA backend: name(),
+    initialize(), shutdown(), supports(), successful_kernel_dispatch_count()
+    and the three hot-path dispatches.  Dispatches take host numpy arrays and
+    return ``True`` on success, ``False`` when refused (``last_error`` says why),
+    leaving the arrays untouched on refusal -- the reference's contract."""
+
+    SUPPORTED = ("AcousticSubstepFusedCartesianCgrid", "AcousticSubstepsBatchedCartesianCgrid",
+                 "ConservativeCartesianCgridTransport")
+
+    def __init__(self, device: int = 0):
+        self.device = device
+        self.ctx: Optional[Context] = None
+        self.last_error = ""
+
+    def name(self) -> str:
+        return "cuda"
+
+    def initialize(self) -> bool:
+        try:
+            self.ctx = Context(self.device)
+            return True
+        except Exception as exc:  # the reference reports initialize failures as (false, error)
+            self.last_error = str(exc)
+            return False
+
+    def shutdown(self):
+        if self.ctx:
+            self.ctx.close()
+            self.ctx = None
+
+    def supports(self, op: str) -> bool:
+        return op in self.SUPPORTED
+
+    def supports_supplied_cartesian_cgrid_mass_flux(self) -> bool:
+        return True
+
+    def supports_batched_cartesian_cgrid_mass_flux_export(self) -> bool:
+        return True
+
+    def successful_kernel_dispatch_count(self) -> int:
+        return self.ctx.kernel_launches if self.ctx else 0
+
+    def _run(self, fn, args) -> bool:
+        rc = fn(args)
+        if rc != NIMBUS_OK:
+            self.last_error = f"{STATUS_NAMES.get(rc, rc)}: {self.ctx.last_error}"
+            return False
+        return True
+
+    def dispatch_acoustic_substep_fused_cartesian_cgrid(self, st, rho0, p0, dt_small, grid, drho=None) -> bool:
+        return self._run(self.ctx.acoustic_fused, fused_args(st, rho0, p0, dt_small, grid, drho))
+
+    def dispatch_acoustic_substeps_batched_cartesian_cgrid(self, st, rho0, p0, dt_small, n_substeps, grid, bc,
+                                                           mfx, mfy, mfz, weight, wave_in, wave_out,
+                                                           density_begin=None, frame=(0.0, 0.0)) -> bool:
+        return self._run(self.ctx.acoustic_batched,
+                         batched_args(st, rho0, p0, dt_small, n_substeps, grid, bc, mfx, mfy, mfz, weight,
+                                      wave_in, wave_out, density_begin, frame))
+
+    def dispatch_advect_scalars_conservative_cartesian_cgrid(self, q_in, q_out, pd, rho_end, rho_begin, mfx, mfy,
+                                                             mfz, dt, grid, weno=True, top_open=False) -> bool:
+        return self._run(self.ctx.scalar_transport,
+                         transport_args(q_in, q_out, pd, rho_end, rho_begin, mfx, mfy, mfz, dt, grid, weno,
+                                        top_open))

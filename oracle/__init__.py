@@ -1,0 +1,173 @@
+"""Test infrastructure: ctypes access to the two CPU oracles of the hot path.
+
+* ``Restatement("f32" | "f64")`` -- the C restatement in ``nimbus_oracle.c``
+  (FP32 storage mirroring the reference CPU solver, or FP64 storage for the
+  error statement).
+* ``ReferenceHarness`` -- the reference Nimbus CPU solver itself, built from
+  its own sources by ``oracle/ref.mk`` and driven through ``ref_harness.cpp``.
+
+Only tests, the smoke check and bench.py's CPU-baseline leg use this package,
+and only as the checker.  Nothing in ``nimbus_b200`` imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+BUILD = ROOT / "_build"
+REF = ROOT / "_ref"
+
+_F = ctypes.POINTER(ctypes.c_float)
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
+
+
+def _ptr(a, ctype):
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+def _fp(a):
+    assert a.flags["C_CONTIGUOUS"], "oracle arrays must be C-contiguous"
+    if a.dtype == np.float32:
+        return _ptr(a, ctypes.c_float)
+    if a.dtype == np.float64:
+        return _ptr(a, ctypes.c_double)
+    raise TypeError(a.dtype)
+
+
+def _bcs(bc):
+    arr = (ctypes.c_int * 6)(*[int(x) for x in bc])
+    return arr
+
+
+class Restatement:
+    """The C restatement, compiled with FP32 ("f32") or FP64 ("f64") storage."""
+
+    def __init__(self, precision: str = "f32"):
+        assert precision in ("f32", "f64")
+        self.precision = precision
+        self.dtype = np.float32 if precision == "f32" else np.float64
+        path = BUILD / f"liboracle_{precision}.so"
+        if not path.exists():
+            raise FileNotFoundError(f"{path} missing: run `make -f oracle/oracle.mk`")
+        self.lib = ctypes.CDLL(str(path))
+        self.lib.oracle_weno5_face.restype = ctypes.c_double
+        self.lib.oracle_weno5_face.argtypes = [ctypes.c_double] * 5
+        self.lib.oracle_mc_slope.restype = ctypes.c_double
+        self.lib.oracle_mc_slope.argtypes = [ctypes.c_double] * 3
+        self.lib.oracle_gamma.restype = ctypes.c_double
+        assert self.lib.oracle_real_bytes() == np.dtype(self.dtype).itemsize
+
+    def _chk(self, *arrs):
+        for a in arrs:
+            if a is not None:
+                assert a.dtype == self.dtype and a.flags["C_CONTIGUOUS"], (a.dtype, self.dtype)
+
+    def weno5_face(self, a, b, c, d, e):
+        return self.lib.oracle_weno5_face(a, b, c, d, e)
+
+    def mc_slope(self, qm, q0, qp):
+        return self.lib.oracle_mc_slope(qm, q0, qp)
+
+    def acoustic_fused(self, st, rho0, p0, dt_small, grid, drho=None):
+        u, v, w, rho, p, th = (st[k] for k in ("u", "v", "w", "rho", "p", "theta"))
+        self._chk(u, v, w, rho, p, th, drho)
+        nx, ny, nz = u.shape
+        self.lib.oracle_acoustic_fused(
+            nx, ny, nz, ctypes.c_double(grid[0]), ctypes.c_double(grid[1]), ctypes.c_double(grid[2]),
+            _fp(u), _fp(v), _fp(w), _fp(rho), _fp(p), _fp(th), _fp(rho0), _fp(p0),
+            ctypes.c_double(dt_small), _fp(drho) if drho is not None else None)
+
+    def acoustic_loop(self, st, rho0, p0, dt_large, n_substeps, grid, bc, frame=(0.0, 0.0)):
+        u, v, w, rho, p, th = (st[k] for k in ("u", "v", "w", "rho", "p", "theta"))
+        self._chk(u, v, w, rho, p, th)
+        nx, ny, nz = u.shape
+        out = {k: np.zeros_like(u) for k in ("mfx", "mfy", "mfz", "rho_begin")}
+        out["wave"] = np.zeros(2 * (nx + ny) * nz, self.dtype)
+        rc = self.lib.oracle_acoustic_loop(
+            nx, ny, nz, ctypes.c_double(grid[0]), ctypes.c_double(grid[1]), ctypes.c_double(grid[2]),
+            _fp(u), _fp(v), _fp(w), _fp(rho), _fp(p), _fp(th), _fp(rho0), _fp(p0),
+            ctypes.c_double(dt_large), int(n_substeps), _bcs(bc), ctypes.c_double(frame[0]),
+            ctypes.c_double(frame[1]), _fp(out["mfx"]), _fp(out["mfy"]), _fp(out["mfz"]),
+            _fp(out["rho_begin"]), _fp(out["wave"]))
+        if rc != 0:
+            raise FloatingPointError("oracle mass-flux accumulation produced a non-finite flux")
+        return out
+
+    def scalar_transport(self, qs, pd, rho_end, rho_begin, mfx, mfy, mfz, dt, grid, weno=True, top_open=False):
+        self._chk(rho_end, rho_begin, mfx, mfy, mfz, *qs)
+        nx, ny, nz = rho_end.shape
+        n = len(qs)
+        ctype = ctypes.c_float if self.dtype == np.float32 else ctypes.c_double
+        arr = (ctypes.POINTER(ctype) * max(n, 1))(*[_ptr(q, ctype) for q in qs])
+        flags = (ctypes.c_int * max(n, 1))(*[int(x) for x in pd])
+        rc = self.lib.oracle_scalar_transport(
+            nx, ny, nz, ctypes.c_double(grid[0]), ctypes.c_double(grid[1]), ctypes.c_double(grid[2]),
+            arr, flags, n, _fp(rho_end), _fp(rho_begin), _fp(mfx), _fp(mfy), _fp(mfz),
+            ctypes.c_double(dt), int(weno), int(top_open))
+        if rc != 0:
+            raise MemoryError("oracle transport scratch allocation failed")
+
+
+class ReferenceHarness:
+    """The reference CPU solver's own objects behind ``ref_harness.cpp``."""
+
+    def __init__(self, threads: int | None = None):
+        path = REF / "libnimbus_ref_harness.so"
+        if not path.exists():
+            raise FileNotFoundError(f"{path} missing: run `make -f oracle/ref.mk all harness`")
+        self.lib = ctypes.CDLL(str(path))
+        self.lib.ref_last_error.restype = ctypes.c_char_p
+        self.threads = self.lib.ref_set_threads(int(threads or 0))
+
+    def set_threads(self, n):
+        self.threads = self.lib.ref_set_threads(int(n))
+        return self.threads
+
+    def _rc(self, rc):
+        if rc != 0:
+            raise RuntimeError(self.lib.ref_last_error().decode())
+
+    def acoustic_fused(self, st, rho0, p0, dt_small, grid, drho=None):
+        u, v, w, rho, p, th = (st[k] for k in ("u", "v", "w", "rho", "p", "theta"))
+        nx, ny, nz = u.shape
+        scratch = drho if drho is not None else np.zeros_like(u)
+        self._rc(self.lib.ref_acoustic_fused(
+            _fp(u), _fp(v), _fp(w), _fp(rho), _fp(p), _fp(th), _fp(rho0), _fp(p0), nx, ny, nz,
+            ctypes.c_double(grid[0]), ctypes.c_double(grid[1]), ctypes.c_double(grid[2]),
+            ctypes.c_double(dt_small), _fp(scratch)))
+
+    def acoustic_loop(self, st, rho0, p0, dt_large, n_substeps, grid, bc):
+        u, v, w, rho, p, th = (st[k] for k in ("u", "v", "w", "rho", "p", "theta"))
+        nx, ny, nz = u.shape
+        out = {k: np.zeros_like(u) for k in ("mfx", "mfy", "mfz", "rho_begin")}
+        out["wave"] = np.zeros(2 * (nx + ny) * nz, np.float32)
+        self._rc(self.lib.ref_acoustic_loop(
+            _fp(u), _fp(v), _fp(w), _fp(rho), _fp(p), _fp(th), _fp(rho0), _fp(p0), nx, ny, nz,
+            ctypes.c_double(grid[0]), ctypes.c_double(grid[1]), ctypes.c_double(grid[2]),
+            ctypes.c_double(dt_large), int(n_substeps), *[int(x) for x in bc],
+            _fp(out["mfx"]), _fp(out["mfy"]), _fp(out["mfz"]), _fp(out["rho_begin"]), _fp(out["wave"])))
+        return out
+
+    def scalar_transport(self, qs, pd, u, v, w, rho_end, rho_begin, mfx, mfy, mfz, dt, grid,
+                         weno=True, top_open=False):
+        nx, ny, nz = rho_end.shape
+        n = len(qs)
+        arr = (_F * max(n, 1))(*[_ptr(q, ctypes.c_float) for q in qs])
+        flags = (ctypes.c_int * max(n, 1))(*[int(x) for x in pd])
+        self._rc(self.lib.ref_scalar_transport(
+            arr, flags, n, _fp(u), _fp(v), _fp(w), _fp(rho_end), _fp(rho_begin), _fp(mfx), _fp(mfy),
+            _fp(mfz), nx, ny, nz, ctypes.c_double(grid[0]), ctypes.c_double(grid[1]),
+            ctypes.c_double(grid[2]), ctypes.c_double(dt), int(weno), int(top_open)))
+
+
+def reference_available() -> bool:
+    return (REF / "libnimbus_ref_harness.so").exists()
+
+
+def restatement_available() -> bool:
+    return (BUILD / "liboracle_f32.so").exists() and (BUILD / "liboracle_f64.so").exists()

@@ -1,0 +1,310 @@
+// Test infrastructure, not product code.
+//
+// A thin extern "C" harness around the reference Nimbus CPU solver, linked
+// from the reference's own sources (oracle/ref.mk builds them, unmodified,
+// into oracle/_ref/libnimbus_ref.a).  It lets the Python tests and the CPU
+// baseline of bench.py drive the reference's real kernels on arrays that the
+// CUDA path also receives:
+//
+//   ref_acoustic_fused      CpuComputeBackend::dispatch_acoustic_substep_fused_cartesian_cgrid
+//                           (src/compute/cpu/acoustic_cgrid.cpp:50, fast path
+//                           src/compute/cpu/acoustic_cgrid_fast.cpp:12-219)
+//   ref_acoustic_loop       the production per-substep order of
+//                           SplitExplicitScheme::step_split_acoustic
+//                           (src/numerics/time_stepping/schemes/split_explicit/split_explicit.cpp:174-260):
+//                           seed KW78 radiation, then N x {retained mass-flux accumulate
+//                           (advection_cartesian.cpp:610-870, Host precision, as
+//                           dynamics.cpp:4545-4557 calls it), fused substep, apply_acoustic(dt_s)
+//                           (boundary_conditions_cartesian_cgrid.cpp:141,884-1187)}
+//   ref_scalar_transport    advect_scalars_conservative_3d_cartesian
+//                           (advection_cartesian.cpp:3532) on a retained context whose
+//                           face mass fluxes and beginning density are supplied
+//                           (CartesianCGridTransportContext::record_external_accumulation).
+//
+// Nothing here re-implements the physics; every number comes from the
+// reference objects.  Errors are reported as a negative return code and a
+// message retrievable with ref_last_error().
+#include "compute/backend_interface.hpp"
+#include "compute/compute_backend_factory.hpp"
+#include "compute/dispatch/dynamics.hpp"
+#include "boundary_conditions/factory.hpp"
+#include "boundary_conditions/boundary_conditions_base.hpp"
+#include "core/field/field3d.hpp"
+#include "core/field/field_bounds.hpp"
+#include "core/runtime/simulation_state.hpp"
+#include "core/runtime/runtime_config.hpp"
+#include "dynamics/dynamics_base.hpp"
+#include "numerics/advection/advection_cartesian.hpp"
+
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <string>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace
+{
+thread_local std::string g_error;
+
+int fail(const char* what)
+{
+    g_error = what;
+    return -1;
+}
+
+void to_field(Field3D& f, const float* src, int nx, int ny, int nz)
+{
+    f.resize(nx, ny, nz, 0.0f);
+    std::memcpy(f.data(), src, sizeof(float) * static_cast<std::size_t>(nx) * ny * nz);
+}
+
+void from_field(float* dst, const Field3D& f)
+{
+    std::memcpy(dst, const_cast<Field3D&>(f).data(), sizeof(float) * f.size());
+}
+
+using tmv::init::config::BottomBC;
+using tmv::init::config::LateralBC;
+using tmv::init::config::TopBC;
+
+// A self-contained level for one call: grid, fields, base profiles and the
+// boundary-condition configuration, viewed exactly as the solver views its own.
+struct Level
+{
+    SimulationStorageState storage;
+    SimulationStateView view;
+
+    static SimulationStorageState& configured(SimulationStorageState& s, int nx, int ny, int nz,
+                                              double dx, double dy, double dz)
+    {
+        s.configuration.stagger_type = StaggerType::CGrid;
+        s.grid.geometry.initialize(nx, ny, nz, dx, dz, dy, CoordinateSystem::Cartesian, StaggerType::CGrid);
+        return s;
+    }
+
+    Level(int nx, int ny, int nz, double dx, double dy, double dz, double dt)
+        : storage(GridStorageState(nx, ny, nz, dx, dz, dt, dy)),
+          view(make_simulation_state_view(configured(storage, nx, ny, nz, dx, dy, dz)))
+    {
+    }
+
+    void set_bcs(int west, int east, int south, int north, int bottom, int top)
+    {
+        auto& c = storage.configuration;
+        c.lateral_bc_west = static_cast<LateralBC>(west);
+        c.lateral_bc_east = static_cast<LateralBC>(east);
+        c.lateral_bc_south = static_cast<LateralBC>(south);
+        c.lateral_bc_north = static_cast<LateralBC>(north);
+        c.bottom_bc = static_cast<BottomBC>(bottom);
+        c.top_bc = static_cast<TopBC>(top);
+    }
+};
+
+AcousticSubstepFusedCartesianCgridDispatch make_fused(Level& L, const double* rho0, const double* p0b,
+                                                      double dt_small, float* drho_scratch)
+{
+    auto& f = L.storage.fields;
+    AcousticSubstepFusedCartesianCgridDispatch d;
+    d.u = f.u.data();
+    d.v = f.v.data();
+    d.w = f.w.data();
+    d.rho = f.rho.data();
+    d.p = f.p.data();
+    d.theta_data = f.theta.data();
+    d.base_len = L.storage.grid.nz;
+    d.nx = L.storage.grid.nr;
+    d.ny = L.storage.grid.nth;
+    d.nz = L.storage.grid.nz;
+    d.gamma_val = static_cast<float>(dynamics_constants::gamma);
+    d.rho_min = density_min_kgm3;
+    d.rho_max = density_max_kgm3;
+    d.p_min = pressure_min_pa;
+    d.p_max = pressure_max_pa;
+    d.p_ref_fallback = static_cast<float>(p0);
+    d.wind_clamp_h = wind_horizontal_abs_max_ms;
+    d.wind_clamp_v = wind_vertical_abs_max_ms;
+    d.rho0_base_host = rho0;
+    d.p0_base_host = p0b;
+    d.dx_host = L.storage.grid.dx;
+    d.dy_host = L.storage.grid.dy;
+    d.dz_host = L.storage.grid.dz;
+    d.dt_small_host = dt_small;
+    d.gamma_host = dynamics_constants::gamma;
+    d.drho_scratch = drho_scratch;
+    return d;
+}
+} // namespace
+
+extern "C" {
+
+const char* ref_last_error(void) { return g_error.c_str(); }
+
+int ref_set_threads(int n)
+{
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+    return omp_get_max_threads();
+#else
+    (void)n;
+    return 1;
+#endif
+}
+
+// One fused acoustic substep on host arrays, in place.
+int ref_acoustic_fused(float* u, float* v, float* w, float* rho, float* p, const float* theta,
+                       const double* rho0, const double* p0b, int nx, int ny, int nz,
+                       double dx, double dy, double dz, double dt_small, float* drho_scratch)
+{
+    try
+    {
+        auto backend = create_cpu_compute_backend();
+        std::string err;
+        if (!backend->initialize(err)) return fail(err.c_str());
+        AcousticSubstepFusedCartesianCgridDispatch d;
+        d.u = u; d.v = v; d.w = w; d.rho = rho; d.p = p; d.theta_data = theta;
+        d.base_len = nz; d.nx = nx; d.ny = ny; d.nz = nz;
+        d.gamma_val = static_cast<float>(dynamics_constants::gamma);
+        d.rho_min = density_min_kgm3; d.rho_max = density_max_kgm3;
+        d.p_min = pressure_min_pa; d.p_max = pressure_max_pa;
+        d.p_ref_fallback = static_cast<float>(p0);
+        d.wind_clamp_h = wind_horizontal_abs_max_ms; d.wind_clamp_v = wind_vertical_abs_max_ms;
+        d.rho0_base_host = rho0; d.p0_base_host = p0b;
+        d.dx_host = dx; d.dy_host = dy; d.dz_host = dz; d.dt_small_host = dt_small;
+        d.gamma_host = dynamics_constants::gamma;
+        d.drho_scratch = drho_scratch;
+        if (!backend->dynamics_kernels()->dispatch_acoustic_substep_fused_cartesian_cgrid(d))
+            return fail("reference CPU backend refused the fused acoustic dispatch");
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        return fail(e.what());
+    }
+}
+
+// The acoustic substep loop of one large step, in place, exporting the
+// time-averaged face mass fluxes, the beginning density and the KW78
+// radiation history (layout: u_west[ny*nz], u_east[ny*nz], v_south[nx*nz],
+// v_north[nx*nz]).  wave_in may be null: the loop then seeds from the
+// post-slow faces, which is what seed_acoustic_radiation does every step.
+int ref_acoustic_loop(float* u, float* v, float* w, float* rho, float* p, const float* theta,
+                      const double* rho0, const double* p0b, int nx, int ny, int nz,
+                      double dx, double dy, double dz, double dt_large, int n_substeps,
+                      int bc_west, int bc_east, int bc_south, int bc_north, int bc_bottom, int bc_top,
+                      float* mfx, float* mfy, float* mfz, float* rho_begin, float* wave_out)
+{
+    try
+    {
+        if (n_substeps < 1) return fail("n_substeps must be >= 1");
+        Level L(nx, ny, nz, dx, dy, dz, dt_large);
+        L.set_bcs(bc_west, bc_east, bc_south, bc_north, bc_bottom, bc_top);
+        auto& f = L.storage.fields;
+        to_field(f.u, u, nx, ny, nz);
+        to_field(f.v, v, nx, ny, nz);
+        to_field(f.w, w, nx, ny, nz);
+        to_field(f.rho, rho, nx, ny, nz);
+        to_field(f.p, p, nx, ny, nz);
+        to_field(f.theta, theta, nx, ny, nz);
+        Field3D scratch(nx, ny, nz, 0.0f);
+
+        auto backend = create_cpu_compute_backend();
+        std::string err;
+        if (!backend->initialize(err)) return fail(err.c_str());
+        auto bc = tmv::create_cartesian_cgrid_bc_scheme(L.view);
+        tmv::CartesianCGridTransportContext ctx;
+        ctx.begin(L.view, nx, ny, nz, dt_large);
+
+        const double dt_small = dt_large / n_substeps;
+        bc->seed_acoustic_radiation();
+        for (int n = 0; n < n_substeps; ++n)
+        {
+            ctx.accumulate(L.view, f.rho, f.u, f.v, f.w, dt_small);
+            auto d = make_fused(L, rho0, p0b, dt_small, scratch.data());
+            if (!backend->dynamics_kernels()->dispatch_acoustic_substep_fused_cartesian_cgrid(d))
+                return fail("reference CPU backend refused the fused acoustic dispatch");
+            bc->apply_acoustic(dt_small);
+        }
+        ctx.complete(L.view);
+
+        from_field(u, f.u);
+        from_field(v, f.v);
+        from_field(w, f.w);
+        from_field(rho, f.rho);
+        from_field(p, f.p);
+        if (mfx) from_field(mfx, ctx.mass_flux_x);
+        if (mfy) from_field(mfy, ctx.mass_flux_y);
+        if (mfz) from_field(mfz, ctx.mass_flux_z);
+        if (rho_begin) from_field(rho_begin, ctx.density_begin);
+        if (wave_out)
+        {
+            const auto& s = *L.view.boundary_condition_runtime;
+            const std::size_t yz = std::size_t(ny) * nz, xz = std::size_t(nx) * nz;
+            std::memcpy(wave_out, s.radiative_u_west.data(), yz * sizeof(float));
+            std::memcpy(wave_out + yz, s.radiative_u_east.data(), yz * sizeof(float));
+            std::memcpy(wave_out + 2 * yz, s.radiative_v_south.data(), xz * sizeof(float));
+            std::memcpy(wave_out + 2 * yz + xz, s.radiative_v_north.data(), xz * sizeof(float));
+        }
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        return fail(e.what());
+    }
+}
+
+// Conservative WENO5 (or MC) transport of n scalars, in place, against the
+// supplied retained face mass fluxes.  rho_end is the density the dynamics
+// retained; rho_begin the density paired with the scalars at step start.
+int ref_scalar_transport(float** q, const int* positive_definite, int n_scalars,
+                         const float* u, const float* v, const float* w, const float* rho_end,
+                         const float* rho_begin, const float* mfx, const float* mfy, const float* mfz,
+                         int nx, int ny, int nz, double dx, double dy, double dz, double dt,
+                         int weno, int top_open)
+{
+    try
+    {
+        if (n_scalars < 0 || n_scalars > 16) return fail("n_scalars out of range");
+        Level L(nx, ny, nz, dx, dy, dz, dt);
+        L.set_bcs(4, 4, 4, 4, 1, top_open ? 2 : 0);
+        auto& f = L.storage.fields;
+        to_field(f.u, u, nx, ny, nz);
+        to_field(f.v, v, nx, ny, nz);
+        to_field(f.w, w, nx, ny, nz);
+        to_field(f.rho, rho_end, nx, ny, nz);
+        tmv::CartesianCGridTransportContext ctx;
+        ctx.begin(L.view, nx, ny, nz, dt);
+        Field3D begin_density;
+        to_field(begin_density, rho_begin, nx, ny, nz);
+        ctx.capture_density_begin(begin_density);
+        std::memcpy(ctx.mass_flux_x.data(), mfx, sizeof(float) * f.u.size());
+        std::memcpy(ctx.mass_flux_y.data(), mfy, sizeof(float) * f.u.size());
+        std::memcpy(ctx.mass_flux_z.data(), mfz, sizeof(float) * f.u.size());
+        ctx.record_external_accumulation(dt, 1);
+        ctx.complete(L.view);
+
+        std::unique_ptr<Field3D[]> fields(new Field3D[n_scalars > 0 ? n_scalars : 1]);
+        tmv::CartesianScalarTransport scalars[16]{};
+        for (int s = 0; s < n_scalars; ++s)
+        {
+            to_field(fields[s], q[s], nx, ny, nz);
+            scalars[s].field = &fields[s];
+            scalars[s].kappa = 0.0;
+            scalars[s].positive_definite = positive_definite[s] != 0;
+        }
+        tmv::advect_scalars_conservative_3d_cartesian(
+            L.view, scalars, static_cast<std::size_t>(n_scalars), dt, &ctx,
+            weno ? tmv::CartesianFaceReconstruction::WENO5 : tmv::CartesianFaceReconstruction::MonotonicCentered);
+        for (int s = 0; s < n_scalars; ++s)
+            from_field(q[s], fields[s]);
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        return fail(e.what());
+    }
+}
+
+} // extern "C"

@@ -1,0 +1,90 @@
+"""Generates the golden fixtures in tests/golden/ from the reference Nimbus CPU
+solver itself (its own sources, built by oracle/ref.mk and driven through
+oracle/ref_harness.cpp).
+
+    make -f oracle/ref.mk -j8 all harness
+    python tests/golden/make_golden.py
+
+Each fixture is one .npz holding the seeded inputs and the reference's
+outputs for a small grid, so the parity tests can pin the oracle restatement
+and the CUDA path without the reference tree present.
+"""
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE.parents[1]))
+
+from nimbus_b200.initial import Case, perturbed_state  # noqa: E402
+from oracle import ReferenceHarness  # noqa: E402
+
+GRID = (1000.0, 1000.0, 500.0)
+
+# (name, lateral W,E,S,N, bottom, top)
+BC_SETS = {
+    "radiative_slip_rigidlid": (1, 1, 1, 1, 1, 0),
+    "periodic_noslip_open": (0, 0, 0, 0, 0, 2),
+    "mixed_walls_sponge": (2, 3, 4, 1, 1, 1),
+}
+
+
+def close_walls(st, bc):
+    """Zero-time wall closure so a rigid wall starts impermeable (the solver
+    applies its boundary conditions before the first step)."""
+    u, v = st["u"], st["v"]
+    if bc[0] in (2, 3):
+        u[0] = 0.0
+    if bc[1] in (2, 3):
+        u[-2] = 0.0
+        u[-1] = 0.0
+    if bc[2] in (2, 3):
+        v[:, 0] = 0.0
+    if bc[3] in (2, 3):
+        v[:, -2] = 0.0
+        v[:, -1] = 0.0
+
+
+def main():
+    ref = ReferenceHarness(threads=1)
+    case = Case(14, 12, 9, *GRID, 6.0, seed=5)
+    st, base = perturbed_state(case, seed=11)
+
+    # 1. One fused substep.
+    inp = {k: v.copy() for k, v in st.items()}
+    out = {k: v.copy() for k, v in st.items()}
+    drho = np.zeros(case.shape, np.float32)
+    ref.acoustic_fused(out, base["rho0"], base["p0"], 0.6, GRID, drho)
+    np.savez_compressed(HERE / "fused_substep.npz", grid=np.array(GRID), dt_small=0.6, rho0=base["rho0"],
+                        p0=base["p0"], **{f"in_{k}": v for k, v in inp.items()},
+                        **{f"out_{k}": out[k] for k in ("u", "v", "w", "rho", "p")}, out_drho=drho)
+
+    # 2. Acoustic loop + 3. transport, per boundary set.
+    for name, bc in BC_SETS.items():
+        st2 = {k: v.copy() for k, v in st.items()}
+        close_walls(st2, bc)
+        inp = {k: v.copy() for k, v in st2.items()}
+        n_sub, dt_large = 7, 6.0
+        loop = ref.acoustic_loop(st2, base["rho0"], base["p0"], dt_large, n_sub, GRID, bc)
+        top_open = bc[5] == 2
+        scalars = {}
+        for weno in (1, 0):
+            qs = [st2["theta"].copy(), st2["qv"].copy(), st2["qc"].copy(), st2["qr"].copy()]
+            ref.scalar_transport(qs, [0, 1, 1, 1], st2["u"], st2["v"], st2["w"], st2["rho"], loop["rho_begin"],
+                                 loop["mfx"], loop["mfy"], loop["mfz"], dt_large, GRID, weno=bool(weno),
+                                 top_open=top_open)
+            for key, q in zip(("theta", "qv", "qc", "qr"), qs):
+                scalars[f"tr{'weno' if weno else 'mc'}_{key}"] = q
+        np.savez_compressed(
+            HERE / f"loop_{name}.npz", grid=np.array(GRID), dt_large=dt_large, n_substeps=n_sub, bc=np.array(bc),
+            rho0=base["rho0"], p0=base["p0"], **{f"in_{k}": v for k, v in inp.items()},
+            **{f"out_{k}": st2[k] for k in ("u", "v", "w", "rho", "p")},
+            **{f"out_{k}": v for k, v in loop.items()}, **scalars)
+        print("wrote", name)
+
+
+if __name__ == "__main__":
+    main()
