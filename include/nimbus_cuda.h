@@ -97,6 +97,24 @@ void* nimbus_cuda_stream(const nimbus_cuda_context* ctx);
  * mass flux or transported scalar since the last check. */
 nimbus_status nimbus_cuda_synchronize(nimbus_cuda_context* ctx);
 
+/* Kernel families for per-launch device timing. */
+enum
+{
+    NIMBUS_KERNEL_ACOUSTIC_SUBSTEP = 0,   /* continuity + EOS (+ retained mass flux) */
+    NIMBUS_KERNEL_ACOUSTIC_MOMENTUM = 1,
+    NIMBUS_KERNEL_ACOUSTIC_BOUNDARY = 2,  /* the three face-closure kernels of one substep */
+    NIMBUS_KERNEL_TRANSPORT_FACES = 3,
+    NIMBUS_KERNEL_TRANSPORT_LIMITER = 4,
+    NIMBUS_KERNEL_TRANSPORT_UPDATE = 5,
+    NIMBUS_KERNEL_FAMILIES = 6
+};
+/* When enabled, every launch is bracketed by CUDA events on its own stream
+ * and nimbus_cuda_kernel_timing() returns, per family, the launch count and
+ * the summed device time since timing was enabled (it synchronises).  Timing
+ * adds two event records per launch; leave it off for throughput runs. */
+nimbus_status nimbus_cuda_set_kernel_timing(nimbus_cuda_context* ctx, int enable);
+nimbus_status nimbus_cuda_kernel_timing(nimbus_cuda_context* ctx, int family, uint64_t* launches, double* total_ms);
+
 /*
  * One fused acoustic substep, in place on (u, v, w, rho, p).
  * Replaces DynamicsComputeKernels::dispatch_acoustic_substep_fused_cartesian_cgrid

@@ -15,6 +15,7 @@
 #include <limits>
 #include <string>
 #include <utility>
+#include <vector>
 
 using namespace nimbus;
 
@@ -37,9 +38,20 @@ enum Slot
 
 }  // namespace
 
+struct TimedLaunch
+{
+    int family;
+    cudaEvent_t start, stop;
+};
+
 struct nimbus_cuda_context
 {
     int device = 0;
+    bool timing = false;
+    std::vector<TimedLaunch> pending;
+    std::vector<cudaEvent_t> event_pool;
+    uint64_t timed_launches[NIMBUS_KERNEL_FAMILIES] = {};
+    double timed_ms[NIMBUS_KERNEL_FAMILIES] = {};
     int sm_count = 148;
     cudaStream_t stream = nullptr;
     unsigned* status = nullptr;  // device status word
@@ -87,6 +99,61 @@ nimbus_status ensure(nimbus_cuda_context* ctx, Slot slot, size_t count, T** out)
     }
     *out = static_cast<T*>(b.ptr);
     return NIMBUS_OK;
+}
+
+cudaEvent_t take_event(nimbus_cuda_context* ctx)
+{
+    if (!ctx->event_pool.empty())
+    {
+        cudaEvent_t e = ctx->event_pool.back();
+        ctx->event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// Brackets the launches issued between begin() and end() with CUDA events on
+// their stream when kernel timing is enabled.
+struct LaunchTimer
+{
+    nimbus_cuda_context* ctx;
+    cudaStream_t stream;
+    int family;
+    cudaEvent_t start = nullptr;
+    LaunchTimer(nimbus_cuda_context* c, cudaStream_t s, int f) : ctx(c), stream(s), family(f)
+    {
+        if (ctx->timing)
+        {
+            start = take_event(ctx);
+            cudaEventRecord(start, stream);
+        }
+    }
+    ~LaunchTimer()
+    {
+        if (start)
+        {
+            cudaEvent_t stop = take_event(ctx);
+            cudaEventRecord(stop, stream);
+            ctx->pending.push_back({family, start, stop});
+        }
+    }
+};
+
+void drain_timing(nimbus_cuda_context* ctx)
+{
+    for (auto& t : ctx->pending)
+    {
+        float ms = 0.0f;
+        cudaEventSynchronize(t.stop);
+        cudaEventElapsedTime(&ms, t.start, t.stop);
+        ctx->timed_launches[t.family] += 1;
+        ctx->timed_ms[t.family] += ms;
+        ctx->event_pool.push_back(t.start);
+        ctx->event_pool.push_back(t.stop);
+    }
+    ctx->pending.clear();
 }
 
 int grid_for(const nimbus_cuda_context* ctx, long long work)
@@ -200,9 +267,16 @@ float* launch_substep(nimbus_cuda_context* ctx, cudaStream_t st, const AcousticP
                       float* rho_next, const AcousticDevice& D)
 {
     const int blocks = grid_for(ctx, P.d.cells());
-    acoustic_continuity_eos_kernel<<<blocks, kThreads, 0, st>>>(P, rho_cur, D.u, D.v, D.w, D.theta, D.rho0, rho_next,
-                                                                D.p, D.drho, D.mfx, D.mfy, D.mfz, ctx->status);
-    acoustic_momentum_kernel<<<blocks, kThreads, 0, st>>>(P, rho_next, D.p, D.p0, D.u, D.v, D.w);
+    {
+        LaunchTimer t(ctx, st, NIMBUS_KERNEL_ACOUSTIC_SUBSTEP);
+        acoustic_continuity_eos_kernel<<<blocks, kThreads, 0, st>>>(P, rho_cur, D.u, D.v, D.w, D.theta, D.rho0,
+                                                                    rho_next, D.p, D.drho, D.mfx, D.mfy, D.mfz,
+                                                                    ctx->status);
+    }
+    {
+        LaunchTimer t(ctx, st, NIMBUS_KERNEL_ACOUSTIC_MOMENTUM);
+        acoustic_momentum_kernel<<<blocks, kThreads, 0, st>>>(P, rho_next, D.p, D.p0, D.u, D.v, D.w);
+    }
     ctx->launches += 2;
     return rho_next;
 }
@@ -212,6 +286,7 @@ void launch_boundaries(nimbus_cuda_context* ctx, cudaStream_t st, const Boundary
 {
     const Dims d = B.d;
     const int yz = d.ny * d.nz, xz = d.nx * d.nz;
+    LaunchTimer t(ctx, st, NIMBUS_KERNEL_ACOUSTIC_BOUNDARY);
     acoustic_bc_we_kernel<<<grid_for(ctx, yz), kThreads, 0, st>>>(B, D.u, D.v, D.w, rho, D.p, wave, wave + yz);
     acoustic_bc_sn_kernel<<<grid_for(ctx, xz), kThreads, 0, st>>>(B, D.u, D.v, D.w, rho, D.p, wave + 2 * yz,
                                                                   wave + 2 * yz + xz);
@@ -339,9 +414,18 @@ nimbus_status run_transport_device(nimbus_cuda_context* ctx, cudaStream_t st, co
     NB_TRY(ensure(ctx, kSf, 3 * n * T.n_scalars, &sf));
     NB_TRY(ensure(ctx, kRl, n * T.n_scalars, &rl));
     const dim3 grid(grid_for(ctx, T.d.cells()), T.n_scalars);
-    transport_faces_kernel<<<grid, kThreads, 0, st>>>(T, mfx, mfy, mfz, sf);
-    transport_limiter_kernel<<<grid, kThreads, 0, st>>>(T, rho_begin, sf, rl);
-    transport_update_kernel<<<grid, kThreads, 0, st>>>(T, rho_end, rho_begin, sf, rl, ctx->status);
+    {
+        LaunchTimer t(ctx, st, NIMBUS_KERNEL_TRANSPORT_FACES);
+        transport_faces_kernel<<<grid, kThreads, 0, st>>>(T, mfx, mfy, mfz, sf);
+    }
+    {
+        LaunchTimer t(ctx, st, NIMBUS_KERNEL_TRANSPORT_LIMITER);
+        transport_limiter_kernel<<<grid, kThreads, 0, st>>>(T, rho_begin, sf, rl);
+    }
+    {
+        LaunchTimer t(ctx, st, NIMBUS_KERNEL_TRANSPORT_UPDATE);
+        transport_update_kernel<<<grid, kThreads, 0, st>>>(T, rho_end, rho_begin, sf, rl, ctx->status);
+    }
     ctx->launches += 3;
     NB_CUDA(ctx, cudaGetLastError());
     return NIMBUS_OK;
@@ -386,6 +470,8 @@ void nimbus_cuda_destroy(nimbus_cuda_context* ctx)
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    drain_timing(ctx);
+    for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
     for (auto& b : ctx->ws)
         if (b.ptr) cudaFree(b.ptr);
     if (ctx->status) cudaFree(ctx->status);
@@ -404,6 +490,29 @@ nimbus_status nimbus_cuda_synchronize(nimbus_cuda_context* ctx)
     NB_TRY(read_status(ctx, ctx->stream, &flags));
     if (flags & kStatusNonfiniteMassFlux) return fail(ctx, NIMBUS_ERR_NONFINITE, "non-finite retained face mass flux");
     if (flags & kStatusNonfiniteTransport) return fail(ctx, NIMBUS_ERR_NONFINITE, "non-finite transported scalar");
+    return NIMBUS_OK;
+}
+
+nimbus_status nimbus_cuda_set_kernel_timing(nimbus_cuda_context* ctx, int enable)
+{
+    if (!ctx) return NIMBUS_ERR_INVALID_ARGUMENT;
+    drain_timing(ctx);
+    ctx->timing = enable != 0;
+    for (int f = 0; f < NIMBUS_KERNEL_FAMILIES; ++f)
+    {
+        ctx->timed_launches[f] = 0;
+        ctx->timed_ms[f] = 0.0;
+    }
+    return NIMBUS_OK;
+}
+
+nimbus_status nimbus_cuda_kernel_timing(nimbus_cuda_context* ctx, int family, uint64_t* launches, double* total_ms)
+{
+    if (!ctx || family < 0 || family >= NIMBUS_KERNEL_FAMILIES || !launches || !total_ms)
+        return NIMBUS_ERR_INVALID_ARGUMENT;
+    drain_timing(ctx);
+    *launches = ctx->timed_launches[family];
+    *total_ms = ctx->timed_ms[family];
     return NIMBUS_OK;
 }
 

@@ -90,7 +90,10 @@ EXPORTED_SYMBOLS = (
     "nimbus_cuda_abi_version", "nimbus_cuda_create", "nimbus_cuda_destroy", "nimbus_cuda_last_error",
     "nimbus_cuda_kernel_launches", "nimbus_cuda_stream", "nimbus_cuda_synchronize",
     "nimbus_cuda_acoustic_fused", "nimbus_cuda_acoustic_batched", "nimbus_cuda_scalar_transport",
+    "nimbus_cuda_set_kernel_timing", "nimbus_cuda_kernel_timing",
 )
+KERNEL_FAMILIES = ("acoustic_substep", "acoustic_momentum", "acoustic_boundary", "transport_faces",
+                   "transport_limiter", "transport_update")
 
 
 def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
@@ -110,6 +113,9 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
     lib.nimbus_cuda_acoustic_fused.argtypes = [ctypes.c_void_p, ctypes.POINTER(AcousticFusedArgs)]
     lib.nimbus_cuda_acoustic_batched.argtypes = [ctypes.c_void_p, ctypes.POINTER(AcousticBatchedArgs)]
     lib.nimbus_cuda_scalar_transport.argtypes = [ctypes.c_void_p, ctypes.POINTER(ScalarTransportArgs)]
+    lib.nimbus_cuda_set_kernel_timing.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    lib.nimbus_cuda_kernel_timing.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64),
+                                              ctypes.POINTER(ctypes.c_double)]
     return lib
 
 
@@ -183,6 +189,19 @@ class Context:
 
     def synchronize(self):
         self.check(self.lib.nimbus_cuda_synchronize(self.handle))
+
+    def set_kernel_timing(self, enable: bool):
+        self.check(self.lib.nimbus_cuda_set_kernel_timing(self.handle, int(enable)))
+
+    def kernel_timing(self) -> dict:
+        """{family: (launches, total_ms)} since timing was enabled."""
+        out = {}
+        for f, name in enumerate(KERNEL_FAMILIES):
+            n = ctypes.c_uint64()
+            ms = ctypes.c_double()
+            self.check(self.lib.nimbus_cuda_kernel_timing(self.handle, f, ctypes.byref(n), ctypes.byref(ms)))
+            out[name] = (int(n.value), float(ms.value))
+        return out
 
     # -- raw entry points -------------------------------------------------
     def acoustic_fused(self, args: AcousticFusedArgs) -> int:

@@ -1,0 +1,176 @@
+"""CUDA path against the reference, bit for bit.
+
+The golden fixtures were produced by the reference CPU solver itself
+(tests/golden/make_golden.py); the CUDA kernels run in reference precision
+(FP64 interior arithmetic over FP32 storage, no contracted FMA), so every
+stored value must be identical -- the tolerance is zero ULP.  Larger seeded
+cases compare against the oracle restatement, itself pinned bit-exact to the
+reference (tests/test_oracle.py)."""
+import glob
+
+import numpy as np
+import pytest
+
+import oracle
+from nimbus_b200 import cuda
+from nimbus_b200.initial import Case, initial_state, perturbed_state
+from tests.golden.make_golden import BC_SETS, close_walls
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = sorted(glob.glob("tests/golden/loop_*.npz"))
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = cuda.Context(0)
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="module")
+def o32():
+    return oracle.Restatement("f32")
+
+
+def _state(g, prefix="in_"):
+    return {k[len(prefix):]: g[k].copy() for k in g.files if k.startswith(prefix)}
+
+
+def assert_bitwise(a, b, what):
+    a = np.ascontiguousarray(a)
+    b = np.ascontiguousarray(b)
+    bad = np.count_nonzero(a.view(np.uint32) != b.view(np.uint32))
+    assert bad == 0, f"{what}: {bad}/{a.size} values differ, max |diff| {np.abs(a - b).max():.3e}"
+
+
+def run_loop(ctx, st, rho0, p0, dt, n, grid, bc, wave_in=None):
+    shape = st["u"].shape
+    mf = [np.zeros(shape, np.float32) for _ in range(3)]
+    rb = np.zeros(shape, np.float32)
+    wave = np.zeros(2 * (shape[0] + shape[1]) * shape[2], np.float32)
+    ctx.check(ctx.acoustic_batched(cuda.batched_args(st, rho0, p0, dt / n, n, grid, bc, *mf, (dt / n) / dt, wave_in,
+                                                     wave, rb)))
+    return dict(mfx=mf[0], mfy=mf[1], mfz=mf[2], rho_begin=rb, wave=wave)
+
+
+def test_fused_substep_matches_reference(ctx):
+    g = np.load("tests/golden/fused_substep.npz")
+    st = _state(g)
+    drho = np.zeros_like(st["u"])
+    ctx.check(ctx.acoustic_fused(cuda.fused_args(st, g["rho0"], g["p0"], float(g["dt_small"]), tuple(g["grid"]),
+                                                 drho)))
+    for k in ("u", "v", "w", "rho", "p"):
+        assert_bitwise(st[k], g["out_" + k], k)
+    assert_bitwise(drho, g["out_drho"], "drho")
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=lambda p: p.split("/")[-1])
+def test_acoustic_loop_and_transport_match_reference(ctx, path):
+    g = np.load(path)
+    st = _state(g)
+    bc = tuple(int(x) for x in g["bc"])
+    dt, n = float(g["dt_large"]), int(g["n_substeps"])
+    out = run_loop(ctx, st, g["rho0"], g["p0"], dt, n, tuple(g["grid"]), bc)
+    for k in ("u", "v", "w", "rho", "p"):
+        assert_bitwise(st[k], g["out_" + k], k)
+    for k in ("mfx", "mfy", "mfz", "rho_begin", "wave"):
+        assert_bitwise(out[k], g["out_" + k], k)
+    src = _state(g)
+    for tag, weno in (("weno", 1), ("mc", 0)):
+        qi = [src[k].copy() for k in ("theta", "qv", "qc", "qr")]
+        qo = [np.zeros_like(q) for q in qi]
+        ctx.check(ctx.scalar_transport(cuda.transport_args(
+            qi, qo, [0, 1, 1, 1], g["out_rho"], g["out_rho_begin"], g["out_mfx"], g["out_mfy"], g["out_mfz"], dt,
+            tuple(g["grid"]), weno=weno, top_open=bc[5] == 2)))
+        for key, q in zip(("theta", "qv", "qc", "qr"), qo):
+            assert_bitwise(q, g[f"tr{tag}_{key}"], f"{tag} {key}")
+
+
+@pytest.mark.parametrize("bc_name", list(BC_SETS))
+def test_seeded_loop_vs_oracle_ragged_grid(ctx, o32, bc_name):
+    """Odd, non-power-of-two extents and a carried-in wave history."""
+    bc = BC_SETS[bc_name]
+    grid = (700.0, 650.0, 330.0)
+    case = Case(37, 29, 23, *grid, 5.0, seed=7)
+    st, base = perturbed_state(case, seed=8)
+    close_walls(st, bc)
+    gpu = {k: v.copy() for k, v in st.items()}
+    cpu = {k: v.copy() for k, v in st.items()}
+    out = run_loop(ctx, gpu, base["rho0"], base["p0"], 5.0, 11, grid, bc)
+    ref = o32.acoustic_loop(cpu, base["rho0"], base["p0"], 5.0, 11, grid, bc)
+    for k in ("u", "v", "w", "rho", "p"):
+        assert_bitwise(gpu[k], cpu[k], k)
+    for k in out:
+        assert_bitwise(out[k], ref[k], k)
+    # second large step continues from the carried KW78 history
+    wave_in = out["wave"].copy()
+    out2 = run_loop(ctx, gpu, base["rho0"], base["p0"], 5.0, 11, grid, bc, wave_in=wave_in)
+    assert out2["wave"].shape == wave_in.shape and np.isfinite(out2["wave"]).all()
+
+
+def test_minimum_grid_and_in_place_transport(ctx, o32):
+    """The reference's minimum extents (4x4x2 batched) and in-place scalars."""
+    grid = (500.0, 500.0, 250.0)
+    case = Case(4, 4, 2, *grid, 2.0)
+    st, base = perturbed_state(case, seed=3)
+    gpu = {k: v.copy() for k, v in st.items()}
+    cpu = {k: v.copy() for k, v in st.items()}
+    bc = (1, 1, 1, 1, 1, 0)
+    out = run_loop(ctx, gpu, base["rho0"], base["p0"], 2.0, 3, grid, bc)
+    ref = o32.acoustic_loop(cpu, base["rho0"], base["p0"], 2.0, 3, grid, bc)
+    for k in ("u", "v", "w", "rho", "p"):
+        assert_bitwise(gpu[k], cpu[k], k)
+    qs = [gpu["theta"].copy(), gpu["qv"].copy()]
+    ctx.check(ctx.scalar_transport(cuda.transport_args(qs, qs, [0, 1], gpu["rho"], out["rho_begin"], out["mfx"],
+                                                       out["mfy"], out["mfz"], 2.0, grid)))
+    qr = [cpu["theta"].copy(), cpu["qv"].copy()]
+    o32.scalar_transport(qr, [0, 1], cpu["rho"], ref["rho_begin"], ref["mfx"], ref["mfy"], ref["mfz"], 2.0, grid)
+    for a, b in zip(qs, qr):
+        assert_bitwise(a, b, "scalar")
+
+
+def test_hydrostatic_identity(ctx):
+    """A resting base state is a fixed point of the substep to within a few ULP
+    (the reference's hydrostatic-identity parity case)."""
+    case = Case(12, 10, 16, 1000.0, 1000.0, 500.0, 6.0, bubble_amp=0.0)
+    st, base = initial_state(case)
+    for k in ("u", "v", "w"):
+        st[k][:] = 0.0
+    before = {k: v.copy() for k, v in st.items()}
+    ctx.check(ctx.acoustic_fused(cuda.fused_args(st, base["rho0"], base["p0"], 0.6, (1000.0, 1000.0, 500.0))))
+    for k in ("rho", "p"):
+        rel = np.abs(st[k].astype(np.float64) - before[k]) / np.abs(before[k])
+        assert rel.max() <= 8 * np.finfo(np.float32).eps, (k, rel.max())
+    assert np.abs(st["w"]).max() < 1e-3
+
+
+def test_refused_dispatch_leaves_host_fields_untouched(ctx):
+    case = Case(8, 8, 4, 1000.0, 1000.0, 500.0, 6.0)
+    st, base = perturbed_state(case)
+    before = {k: v.copy() for k, v in st.items()}
+    args = cuda.fused_args(st, base["rho0"], base["p0"], -1.0, (1000.0, 1000.0, 500.0))  # dt < 0
+    rc = ctx.acoustic_fused(args)
+    assert rc == 1 and "dt_small" in ctx.last_error
+    args = cuda.fused_args(st, base["rho0"], base["p0"], 0.5, (1000.0, 1000.0, 500.0))
+    args.rho_min = 3.0  # rho_min > rho_max
+    assert ctx.acoustic_fused(args) == 1
+    for k in st:
+        assert_bitwise(st[k], before[k], k)
+
+
+def test_nonfinite_mass_flux_is_reported_not_published(ctx):
+    case = Case(8, 8, 4, 1000.0, 1000.0, 500.0, 6.0)
+    st, base = perturbed_state(case)
+    shape = case.shape
+    mf = [np.zeros(shape, np.float32) for _ in range(3)]
+    mf[0][3, 3, 1] = np.float32(3.4e38)  # the next weighted add overflows the FP32 store
+    st["u"][3, 3, 1] = 150.0
+    before = {k: v.copy() for k, v in st.items()}
+    wave = np.zeros(2 * (8 + 8) * 4, np.float32)
+    args = cuda.batched_args(st, base["rho0"], base["p0"], 0.5, 2, (1000.0, 1000.0, 500.0), (1, 1, 1, 1, 1, 0),
+                             *mf, 1e36, None, wave)
+    rc = ctx.acoustic_batched(args)
+    assert rc == 4, ctx.last_error   # NIMBUS_ERR_NONFINITE
+    for k in st:
+        assert_bitwise(st[k], before[k], k)
