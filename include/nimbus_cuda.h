@@ -44,7 +44,8 @@ typedef enum nimbus_status
     NIMBUS_ERR_OUT_OF_MEMORY = 3,    /* device allocation or admission failed */
     NIMBUS_ERR_NONFINITE = 4,        /* a produced value was non-finite; outputs not published */
     NIMBUS_ERR_UNSUPPORTED = 5,      /* valid request outside this backend's contract */
-    NIMBUS_ERR_NO_DEVICE = 6         /* no usable sm_100 device */
+    NIMBUS_ERR_NO_DEVICE = 6,        /* no usable sm_100 device */
+    NIMBUS_ERR_TOO_LARGE = 7         /* grid exceeds a fixed capacity (see NIMBUS_STATIC_SCRATCH_CELLS) */
 } nimbus_status;
 
 typedef enum nimbus_memory
@@ -152,6 +153,35 @@ typedef struct nimbus_acoustic_fused_args
 } nimbus_acoustic_fused_args;
 
 nimbus_status nimbus_cuda_acoustic_fused(nimbus_cuda_context* ctx, const nimbus_acoustic_fused_args* a);
+
+/*
+ * The fused acoustic substep for callers that cannot allocate device memory.
+ * This entry point has no counterpart in the reference.
+ *
+ * Who needs it: a host that has already committed its whole HBM budget (for
+ * example runs admitted by free device memory, whose state is sized up front
+ * and must not grow), or a latency-sensitive stepping loop that cannot afford
+ * the implicit device-wide synchronisation of cudaMalloc/cudaFree.  Every
+ * other entry point may grow the context workspace; this one allocates
+ * nothing and needs no context.
+ *
+ * Same arithmetic and results as nimbus_cuda_acoustic_fused.  Requirements:
+ *   - memory == NIMBUS_MEMORY_DEVICE: every field pointer is device memory on
+ *     the current device; the substep is enqueued on `stream` (NULL = the
+ *     default stream) and the call returns without synchronising;
+ *   - nx*ny*nz <= NIMBUS_STATIC_SCRATCH_CELLS, else NIMBUS_ERR_TOO_LARGE.
+ * Scratch: the new density is staged in one file-scope device array of
+ * NIMBUS_STATIC_SCRATCH_CELLS floats (16 MiB) that every GPU which loads the
+ * library holds until the process exits.  The first call on a device resolves
+ * that array's device address (with the device current), so make the first
+ * call on each device before any stream capture.  Every call shares the one
+ * array: calls that overlap on the GPU (different streams, or different host
+ * threads on the same device) race and must be serialised by the caller.
+ * Each call overwrites the whole scratch range it reads, so no clearing is
+ * needed between calls.
+ */
+#define NIMBUS_STATIC_SCRATCH_CELLS 4194304
+nimbus_status nimbus_cuda_acoustic_fused_static_scratch(const nimbus_acoustic_fused_args* a);
 
 /*
  * All n_substeps acoustic substeps of one large step in one submission, with

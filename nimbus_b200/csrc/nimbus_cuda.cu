@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <mutex>
 #include <string>
 #include <utility>
 #include <vector>
@@ -706,3 +707,75 @@ nimbus_status nimbus_cuda_scalar_transport(nimbus_cuda_context* ctx, const nimbu
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Fused acoustic substep with static scratch: no device allocation at all.
+// ---------------------------------------------------------------------------
+namespace
+{
+
+constexpr int kStaticScratchMaxDevices = 64;
+
+// The density ping-pong partner for nimbus_cuda_acoustic_fused_static_scratch.
+// Host code must not pass this symbol to a kernel: on the host it names a
+// stand-in, not the device address, which is resolved per device below.
+static __device__ __align__(256) float g_static_rho_scratch[NIMBUS_STATIC_SCRATCH_CELLS];
+
+std::mutex g_static_scratch_mutex;
+float* g_static_scratch_ptr[kStaticScratchMaxDevices] = {};
+int g_static_scratch_sms[kStaticScratchMaxDevices] = {};
+
+}  // namespace
+
+extern "C" nimbus_status nimbus_cuda_acoustic_fused_static_scratch(const nimbus_acoustic_fused_args* a)
+{
+    if (!a) return NIMBUS_ERR_INVALID_ARGUMENT;
+    if (a->memory != NIMBUS_MEMORY_DEVICE) return NIMBUS_ERR_INVALID_ARGUMENT;
+    if (check_acoustic_common(a->u, a->v, a->w, a->rho, a->p, a->theta, a->rho0_base, a->p0_base, a->base_len,
+                              a->nx, a->ny, a->nz, a->dx, a->dy, a->dz, a->dt_small, a->gamma, a->rho_min,
+                              a->rho_max, a->p_min, a->p_max, a->p_ref_fallback, a->wind_clamp_h,
+                              a->wind_clamp_v) != nullptr)
+        return NIMBUS_ERR_INVALID_ARGUMENT;
+    const long long cells = static_cast<long long>(a->nx) * a->ny * a->nz;
+    if (cells > NIMBUS_STATIC_SCRATCH_CELLS) return NIMBUS_ERR_TOO_LARGE;
+
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return NIMBUS_ERR_CUDA;
+    if (dev < 0 || dev >= kStaticScratchMaxDevices) return NIMBUS_ERR_UNSUPPORTED;
+    float* scratch = nullptr;
+    int sms = 0;
+    {
+        std::lock_guard<std::mutex> lock(g_static_scratch_mutex);
+        if (!g_static_scratch_ptr[dev])
+        {
+            // Set-up, once per device, with that device current.
+            void* ptr = nullptr;
+            if (cudaGetSymbolAddress(&ptr, g_static_rho_scratch) != cudaSuccess || ptr == nullptr)
+                return NIMBUS_ERR_CUDA;
+            int count = 0;
+            if (cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || count <= 0)
+                return NIMBUS_ERR_CUDA;
+            g_static_scratch_ptr[dev] = static_cast<float*>(ptr);
+            g_static_scratch_sms[dev] = count;
+        }
+        scratch = g_static_scratch_ptr[dev];
+        sms = g_static_scratch_sms[dev];
+    }
+
+    const AcousticParams P = acoustic_params(a->nx, a->ny, a->nz, a->dx, a->dy, a->dz, a->dt_small, a->gamma,
+                                             a->rho_min, a->rho_max, a->p_min, a->p_max, a->p_ref_fallback,
+                                             a->wind_clamp_h, a->wind_clamp_v);
+    cudaStream_t st = static_cast<cudaStream_t>(a->stream);
+    long long blocks = (cells + kThreads - 1) / kThreads;
+    if (blocks > static_cast<long long>(sms) * 16) blocks = static_cast<long long>(sms) * 16;
+    acoustic_continuity_eos_kernel<<<static_cast<int>(blocks), kThreads, 0, st>>>(
+        P, a->rho, a->u, a->v, a->w, a->theta, a->rho0_base, scratch, a->p, a->drho_scratch, nullptr, nullptr,
+        nullptr, nullptr);
+    acoustic_momentum_kernel<<<static_cast<int>(blocks), kThreads, 0, st>>>(P, scratch, a->p, a->p0_base, a->u,
+                                                                             a->v, a->w);
+    if (cudaMemcpyAsync(a->rho, scratch, sizeof(float) * static_cast<size_t>(cells), cudaMemcpyDeviceToDevice, st) !=
+        cudaSuccess)
+        return NIMBUS_ERR_CUDA;
+    if (cudaGetLastError() != cudaSuccess) return NIMBUS_ERR_CUDA;
+    return NIMBUS_OK;
+}

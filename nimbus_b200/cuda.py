@@ -33,6 +33,7 @@ STATUS_NAMES = {
     4: "NIMBUS_ERR_NONFINITE",
     5: "NIMBUS_ERR_UNSUPPORTED",
     6: "NIMBUS_ERR_NO_DEVICE",
+    7: "NIMBUS_ERR_TOO_LARGE",
 }
 MEMORY_HOST, MEMORY_DEVICE = 0, 1
 
@@ -91,7 +92,9 @@ EXPORTED_SYMBOLS = (
     "nimbus_cuda_kernel_launches", "nimbus_cuda_stream", "nimbus_cuda_synchronize",
     "nimbus_cuda_acoustic_fused", "nimbus_cuda_acoustic_batched", "nimbus_cuda_scalar_transport",
     "nimbus_cuda_set_kernel_timing", "nimbus_cuda_kernel_timing",
+    "nimbus_cuda_acoustic_fused_static_scratch",
 )
+STATIC_SCRATCH_CELLS = 4194304  # NIMBUS_STATIC_SCRATCH_CELLS
 KERNEL_FAMILIES = ("acoustic_substep", "acoustic_momentum", "acoustic_boundary", "transport_faces",
                    "transport_limiter", "transport_update")
 
@@ -113,6 +116,7 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
     lib.nimbus_cuda_acoustic_fused.argtypes = [ctypes.c_void_p, ctypes.POINTER(AcousticFusedArgs)]
     lib.nimbus_cuda_acoustic_batched.argtypes = [ctypes.c_void_p, ctypes.POINTER(AcousticBatchedArgs)]
     lib.nimbus_cuda_scalar_transport.argtypes = [ctypes.c_void_p, ctypes.POINTER(ScalarTransportArgs)]
+    lib.nimbus_cuda_acoustic_fused_static_scratch.argtypes = [ctypes.POINTER(AcousticFusedArgs)]
     lib.nimbus_cuda_set_kernel_timing.argtypes = [ctypes.c_void_p, ctypes.c_int]
     lib.nimbus_cuda_kernel_timing.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64),
                                               ctypes.POINTER(ctypes.c_double)]
