@@ -44,6 +44,12 @@ def parse():
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--substep-form", choices=("auto", "fused", "split"), default="auto",
+                    help="acoustic substep kernels: autotuned (default) or pinned (profiling runs pin the "
+                         "form the plain run chose, since a profiler distorts the autotuner's timings)")
+    ap.add_argument("--precision", choices=("fp32", "reference"), default="fp32",
+                    help="fp32: FP32 stencils on the FP64 base state (the timed form); "
+                         "reference: FP64 interior arithmetic, bit-exact to the CPU solver")
     return ap.parse_args()
 
 
@@ -231,7 +237,11 @@ def run_ours(args):
     case.member = rank  # each rank advances its own ensemble member
     case.seed = case.seed + 1000 * rank
     ctx = cuda.Context(device)
-    run = ResidentRun(ctx, case, device=f"cuda:{device}")
+    precision = cuda.PRECISION_FP32 if args.precision == "fp32" else cuda.PRECISION_REFERENCE
+    other = cuda.PRECISION_REFERENCE if precision == cuda.PRECISION_FP32 else cuda.PRECISION_FP32
+    form = {"auto": cuda.SUBSTEP_AUTO, "fused": cuda.SUBSTEP_FUSED, "split": cuda.SUBSTEP_SPLIT}[args.substep_form]
+    ctx.set_substep_form(form)
+    run = ResidentRun(ctx, case, device=f"cuda:{device}", precision=precision, autotune=form == cuda.SUBSTEP_AUTO)
     stream = run.torch_stream
 
     def barrier():
@@ -272,19 +282,35 @@ def run_ours(args):
     timing = ctx.kernel_timing()
     ctx.set_kernel_timing(False)
     n_sub = run.n_substeps
-    fam = ("acoustic_substep", "acoustic_momentum", "acoustic_boundary")
-    substeps = timing["acoustic_substep"][0]
-    substep_ms = sum(timing[f][1] for f in fam) / max(substeps, 1)
+    launches_sub, total_sub = timing["acoustic_substep"]
+    # One substep = the fused kernel, or the split form's two launches.
+    substep_ms = (total_sub + timing["acoustic_momentum"][1]) / max(launches_sub, 1)
     achieved = SUBSTEP_BYTES_PER_CELL * case.cells / (substep_ms / 1e3) / 1e9
     peak, peak_kind = load_peaks()
     traffic = load_traffic().get(args.workload, {}).get("acoustic_substep_bytes_per_substep")
     total_ms = sum(v[1] for v in timing.values())
     shares = {k: round(v[1] / total_ms, 4) for k, v in timing.items()} if total_ms else {}
 
+    # The other precision mode, same workload, device-timed (reported beside).
+    alt = ResidentRun(ctx, case, device=f"cuda:{device}", precision=other, autotune=form == cuda.SUBSTEP_AUTO)
+    for _ in range(3):
+        alt.step()
+    alt.torch_stream.synchronize()
+    a0 = torch.cuda.Event(enable_timing=True)
+    a1 = torch.cuda.Event(enable_timing=True)
+    a0.record(alt.torch_stream)
+    for _ in range(args.steps):
+        alt.step()
+    a1.record(alt.torch_stream)
+    a1.synchronize()
+    alt_ms = a0.elapsed_time(a1) / args.steps
+    del alt
+    ctx.set_precision(precision)
+
     # End-to-end through the reference-facing host API (pinned host arrays).
     e2e = None
     if args.e2e_steps > 0:
-        host = HostStepper(ctx, case)
+        host = HostStepper(ctx, case, precision=precision)
         host.step()
         torch.cuda.synchronize()
         barrier()
@@ -312,15 +338,26 @@ def run_ours(args):
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64 arithmetic, f32 storage",
+            "vs_baseline": None,
+            "dtype": "f32 (stencils), f64 (base state, EOS, mass-flux sums)" if precision == cuda.PRECISION_FP32
+            else "f64 arithmetic, f32 storage",
             "data": "synthetic (seeded WK82 supercell: analytic sounding, cos^2 bubble, theta noise)",
             "config": {"workload": args.workload, "grid": list(case.shape), "dx_m": case.dx, "dz_m": case.dz,
                        "dt_s": case.dt, "acoustic_substeps": n_sub, "scalars": 4,
                        "path": "acoustic loop (mass flux, fused substep, KW78 boundaries) + WENO5 transport",
-                       "precision": "reference: FP64 interior arithmetic over FP32 storage, bit-exact to the CPU solver",
+                       "precision": args.precision,
+                       "precision_modes": {
+                           args.precision: {"value": value, "ms_per_step": ms / args.steps},
+                           ("reference" if args.precision == "fp32" else "fp32"): {
+                               "value": cells_total * 1e3 / alt_ms if world == 1 else None, "ms_per_step": alt_ms}},
+                       "substep_form": {"chosen": args.substep_form if form != cuda.SUBSTEP_AUTO else
+                                        ("fused" if run.tuned and run.tuned[0] == 1 else "split"),
+                                        "autotune_ms_per_substep": run.tuned[1] if run.tuned else None},
                        "parallelism": f"{world} independent member(s), one per GPU",
                        "l2": "inputs larger than L2 (resident state ~%d MB per GPU)" % (case.cells * 4 * 17 // 2**20)},
-            "roofline": {"bound": "hbm", "kernel": "acoustic substep (continuity/EOS + momentum + boundary launches)",
+            "roofline": {"bound": "hbm",
+                         "kernel": "acoustic substep (%s form)" % (args.substep_form if form != cuda.SUBSTEP_AUTO else
+                                                                   ("fused" if run.tuned and run.tuned[0] == 1 else "split")),
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_kind": peak_kind, "traffic": traffic,
                          "algorithmic_bytes_per_cell": SUBSTEP_BYTES_PER_CELL,

@@ -98,6 +98,44 @@ void* nimbus_cuda_stream(const nimbus_cuda_context* ctx);
  * mass flux or transported scalar since the last check. */
 nimbus_status nimbus_cuda_synchronize(nimbus_cuda_context* ctx);
 
+/* Arithmetic of the hot-path kernels on this context.
+ *   NIMBUS_PRECISION_REFERENCE (default): FP64 interior arithmetic over FP32
+ *     storage in the reference CPU solver's operation order -- bit-identical
+ *     results to the reference.
+ *   NIMBUS_PRECISION_FP32: FP32 stencil arithmetic with the FP64 base state
+ *     (hydrostatic pressure differences carried as FP32 hi+lo pairs), FP64
+ *     EOS power law and FP64 retained mass-flux sums; errors against the FP64
+ *     oracle are stated, not zero. */
+enum
+{
+    NIMBUS_PRECISION_REFERENCE = 0,
+    NIMBUS_PRECISION_FP32 = 1
+};
+nimbus_status nimbus_cuda_set_precision(nimbus_cuda_context* ctx, int precision);
+
+/* Form of the acoustic substep kernels.
+ *   NIMBUS_SUBSTEP_AUTO  (default) the form the autotuner chose for the grid
+ *                        shape and precision, else SPLIT.
+ *   NIMBUS_SUBSTEP_FUSED one launch per substep: 2.5-D i-marching strips with
+ *                        cp.async-staged shared-memory planes (64 B/cell).
+ *   NIMBUS_SUBSTEP_SPLIT two launches per substep (continuity+EOS, momentum),
+ *                        one thread per cell (84 B/cell, fewer instructions).
+ * Every form gives identical results in reference precision. */
+enum
+{
+    NIMBUS_SUBSTEP_AUTO = 0,
+    NIMBUS_SUBSTEP_FUSED = 1,
+    NIMBUS_SUBSTEP_SPLIT = 2
+};
+nimbus_status nimbus_cuda_set_substep_form(nimbus_cuda_context* ctx, int form);
+/* Autotuner: times each substep form on an nx*ny*nz scratch state (a few
+ * substeps each, CUDA events, after a warm-up) in the context's current
+ * precision and records the fastest for NIMBUS_SUBSTEP_AUTO launches of that
+ * shape.  Synchronous; allocates scratch.  *chosen_form (may be NULL)
+ * receives the choice and *ms_per_substep (may be NULL) its time. */
+nimbus_status nimbus_cuda_autotune_substep(nimbus_cuda_context* ctx, int nx, int ny, int nz, int* chosen_form,
+                                           double* ms_per_substep);
+
 /* Kernel families for per-launch device timing. */
 enum
 {

@@ -6,11 +6,14 @@
 // enqueue; nimbus_cuda_synchronize() reports their status word.
 #include "../../include/nimbus_cuda.h"
 
+#include "acoustic_fused.cuh"
 #include "acoustic_kernels.cuh"
+#include "acoustic_split.cuh"
 #include "transport_kernels.cuh"
 
 #include <cmath>
 #include <cstdio>
+#include <cstdint>
 #include <cstring>
 #include <limits>
 #include <mutex>
@@ -34,7 +37,7 @@ struct DeviceBuffer
 enum Slot
 {
     kU, kV, kW, kRho, kP, kTheta, kRhoAlt, kDrho, kRho0, kP0, kMfx, kMfy, kMfz, kWave, kRhoBegin,
-    kRhoEnd, kSf, kRl, kQ0, kSlotCount = kQ0 + 2 * kMaxScalars
+    kRhoEnd, kSf, kRl, kUAlt, kVAlt, kWAlt, kDp0, kQ0, kSlotCount = kQ0 + 2 * kMaxScalars
 };
 
 }  // namespace
@@ -48,6 +51,13 @@ struct TimedLaunch
 struct nimbus_cuda_context
 {
     int device = 0;
+    int precision = NIMBUS_PRECISION_REFERENCE;
+    int substep_form = NIMBUS_SUBSTEP_AUTO;
+    struct TunedShape
+    {
+        int nx, ny, nz, precision, form;
+    };
+    std::vector<TunedShape> tuned;
     bool timing = false;
     std::vector<TimedLaunch> pending;
     std::vector<cudaEvent_t> event_pool;
@@ -204,7 +214,7 @@ AcousticParams acoustic_params(int nx, int ny, int nz, double dx, double dy, dou
                                float wind_v)
 {
     AcousticParams P{};
-    P.d = Dims{nx, ny, nz};
+    P.d = make_dims(nx, ny, nz);
     P.inv_dx = 1.0 / dx;
     P.inv_dy = 1.0 / dy;
     P.inv_dz = 1.0 / dz;
@@ -260,26 +270,170 @@ struct AcousticDevice
     float* rho_alt;   // ping-pong partner of rho
     float* drho;      // optional
     float *mfx, *mfy, *mfz;  // optional (all or none)
+    float *u_alt, *v_alt, *w_alt;  // ping-pong partners of u, v, w (fused substep)
 };
 
-// One substep: continuity+EOS into rho_next, momentum in place.  Returns the
-// buffer now holding rho.
-float* launch_substep(nimbus_cuda_context* ctx, cudaStream_t st, const AcousticParams& P, float* rho_cur,
-                      float* rho_next, const AcousticDevice& D)
+nimbus_status ensure_alts(nimbus_cuda_context* ctx, size_t n, AcousticDevice& D)
 {
-    const int blocks = grid_for(ctx, P.d.cells());
+    NB_TRY(ensure(ctx, kRhoAlt, n, &D.rho_alt));
+    NB_TRY(ensure(ctx, kUAlt, n, &D.u_alt));
+    NB_TRY(ensure(ctx, kVAlt, n, &D.v_alt));
+    NB_TRY(ensure(ctx, kWAlt, n, &D.w_alt));
+    return NIMBUS_OK;
+}
+
+// Fused one-launch substep: reads (u,v,w,rho)[cur], writes (u,v,w,rho)[alt],
+// p in place, mass fluxes in place.
+constexpr int kFusedTJ = 8;
+constexpr int kFusedBlock = 256;
+
+struct Prognostic
+{
+    float *u, *v, *w, *rho;
+};
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+template <class Policy>
+nimbus_status launch_fused_impl(nimbus_cuda_context* ctx, cudaStream_t st, FusedParams F, const Prognostic& in,
+                                const Prognostic& out, float* p, const float* theta, const double* rho0,
+                                const double* p0, const float2* dp0, float* drho, float* mfx, float* mfy, float* mfz)
+{
+    const size_t smem = FusedSmem<kFusedTJ>::floats(F.d.nz) * sizeof(float);
+    auto kernel = acoustic_substep_fused_kernel<kFusedTJ, kFusedBlock, Policy>;
+    if (smem > 220 * 1024) return fail(ctx, NIMBUS_ERR_UNSUPPORTED, "nz too large for the fused substep's shared window");
+    static int occupancy_cache[2][512] = {};
+    const int pol = Policy::exact_pow ? 0 : 1;
+    int& occ = occupancy_cache[pol][F.d.nz < 512 ? F.d.nz : 511];
+    if (occ == 0)
+    {
+        NB_CUDA(ctx, cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+        int blocks = 0;
+        NB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, kFusedBlock, smem));
+        occ = blocks > 0 ? blocks : 1;
+    }
+    // Chunk the i-march so the grid is about one full wave of resident CTAs
+    // (each chunk recomputes one plane, so longer chunks waste less).
+    const int strips = (F.d.ny + kFusedTJ - 1) / kFusedTJ;
+    const int resident = ctx->sm_count * occ;
+    int chunks = resident / strips;
+    if (chunks < 1) chunks = 1;
+    if (chunks > F.d.nx) chunks = F.d.nx;
+    F.chunk = (F.d.nx + chunks - 1) / chunks;
+    chunks = (F.d.nx + F.chunk - 1) / F.chunk;
+    F.nz_magic = fused_nz_magic(static_cast<unsigned>(F.d.nz));
+    F.vec4 = (F.d.nz % 4 == 0) && aligned16(in.rho) && aligned16(in.u) && aligned16(in.v) && aligned16(in.w) &&
+             aligned16(theta);
+    LaunchTimer t(ctx, st, NIMBUS_KERNEL_ACOUSTIC_SUBSTEP);
+    kernel<<<strips * chunks, kFusedBlock, smem, st>>>(F, in.rho, in.u, in.v, in.w, theta, rho0, p0, dp0, drho,
+                                                       out.rho, p, out.u, out.v, out.w, mfx, mfy, mfz, ctx->status);
+    ctx->launches += 1;
+    return NIMBUS_OK;
+}
+
+template <class Policy>
+nimbus_status launch_split_impl(nimbus_cuda_context* ctx, cudaStream_t st, FusedParams F, const Prognostic& in,
+                                const Prognostic& out, float* p, const float* theta, const double* rho0,
+                                const double* p0, const float2* dp0, float* drho, float* mfx, float* mfy, float* mfz)
+{
+    const long long n = F.d.cells();
+    long long blocks = (n + kThreads - 1) / kThreads;
+    const long long cap = static_cast<long long>(ctx->sm_count) * 32;
+    if (blocks > cap) blocks = cap;
     {
         LaunchTimer t(ctx, st, NIMBUS_KERNEL_ACOUSTIC_SUBSTEP);
-        acoustic_continuity_eos_kernel<<<blocks, kThreads, 0, st>>>(P, rho_cur, D.u, D.v, D.w, D.theta, D.rho0,
-                                                                    rho_next, D.p, D.drho, D.mfx, D.mfy, D.mfz,
-                                                                    ctx->status);
+        split_continuity_eos_kernel<Policy><<<static_cast<int>(blocks), kThreads, 0, st>>>(
+            F, in.rho, in.u, in.v, in.w, theta, rho0, out.rho, p, drho, mfx, mfy, mfz, ctx->status);
     }
     {
         LaunchTimer t(ctx, st, NIMBUS_KERNEL_ACOUSTIC_MOMENTUM);
-        acoustic_momentum_kernel<<<blocks, kThreads, 0, st>>>(P, rho_next, D.p, D.p0, D.u, D.v, D.w);
+        split_momentum_kernel<Policy><<<static_cast<int>(blocks), kThreads, 0, st>>>(F, out.rho, p, p0, dp0, in.u,
+                                                                                      in.v, in.w, out.u, out.v, out.w);
     }
     ctx->launches += 2;
-    return rho_next;
+    return NIMBUS_OK;
+}
+
+int resolve_form(const nimbus_cuda_context* ctx, const Dims& d)
+{
+    if (ctx->substep_form != NIMBUS_SUBSTEP_AUTO) return ctx->substep_form;
+    for (const auto& e : ctx->tuned)
+        if (e.nx == d.nx && e.ny == d.ny && e.nz == d.nz && e.precision == ctx->precision) return e.form;
+    return NIMBUS_SUBSTEP_SPLIT;
+}
+
+nimbus_status launch_fused(nimbus_cuda_context* ctx, cudaStream_t st, const FusedParams& F, const Prognostic& in,
+                           const Prognostic& out, float* p, const float* theta, const double* rho0, const double* p0,
+                           const float2* dp0, float* drho, float* mfx, float* mfy, float* mfz)
+{
+    const bool fp32 = ctx->precision == NIMBUS_PRECISION_FP32;
+    if (resolve_form(ctx, F.d) == NIMBUS_SUBSTEP_SPLIT)
+    {
+        if (fp32) return launch_split_impl<Fp32Policy>(ctx, st, F, in, out, p, theta, rho0, p0, dp0, drho, mfx, mfy, mfz);
+        return launch_split_impl<RefPolicy>(ctx, st, F, in, out, p, theta, rho0, p0, dp0, drho, mfx, mfy, mfz);
+    }
+    if (fp32) return launch_fused_impl<Fp32Policy>(ctx, st, F, in, out, p, theta, rho0, p0, dp0, drho, mfx, mfy, mfz);
+    return launch_fused_impl<RefPolicy>(ctx, st, F, in, out, p, theta, rho0, p0, dp0, drho, mfx, mfy, mfz);
+}
+
+// Resting state for the autotuner: rho=1.1, u=v=w=0, p=9e4, theta=300, zero
+// fluxes; profiles rho0=1.1, p0=9e4 and a zero hydrostatic difference.
+__global__ void fill_tuning_state(float* buf, size_t n, double* prof, int nz, float2* dp0)
+{
+    for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x)
+    {
+        buf[c] = 0.0f;            // u
+        buf[n + c] = 0.0f;        // v
+        buf[2 * n + c] = 0.0f;    // w
+        buf[3 * n + c] = 1.1f;    // rho
+        buf[4 * n + c] = 0.0f;
+        buf[5 * n + c] = 0.0f;
+        buf[6 * n + c] = 0.0f;
+        buf[7 * n + c] = 1.1f;
+        buf[8 * n + c] = 90000.0f;  // p
+        buf[9 * n + c] = 300.0f;    // theta
+        buf[10 * n + c] = 0.0f;
+        buf[11 * n + c] = 0.0f;
+        buf[12 * n + c] = 0.0f;
+    }
+    if (blockIdx.x == 0)
+        for (int k = threadIdx.x; k < nz; k += blockDim.x)
+        {
+            prof[k] = 1.1;
+            prof[nz + k] = 90000.0;
+            dp0[k] = make_float2(0.0f, 0.0f);
+        }
+}
+
+__global__ void dp0_split_kernel(const double* __restrict__ p0, int nz, float2* __restrict__ out)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nz) return;
+    const double dp = (k + 1 < nz) ? p0[k + 1] - p0[k] : 0.0;
+    const float hi = (float)dp;
+    out[k] = make_float2(hi, (float)(dp - (double)hi));
+}
+
+FusedParams fused_params(const nimbus_cuda_context* ctx, int nx, int ny, int nz, double dx, double dy, double dz,
+                         double dt, double gamma, float rho_min, float rho_max, float p_min, float p_max, float p_ref,
+                         float wind_h, float wind_v)
+{
+    FusedParams F{};
+    F.d = make_dims(nx, ny, nz);
+    F.inv_dx = 1.0 / dx;
+    F.inv_dy = 1.0 / dy;
+    F.inv_dz = 1.0 / dz;
+    F.dt_small = dt;
+    F.gamma = gamma;
+    F.rho_min = rho_min;
+    F.rho_max = rho_max;
+    F.p_min = p_min;
+    F.p_max = p_max;
+    F.p_ref_fallback = p_ref;
+    F.wind_h = wind_h;
+    F.wind_v = wind_v;
+    F.chunk = 1;  // set at launch from the kernel's occupancy
+    return F;
 }
 
 void launch_boundaries(nimbus_cuda_context* ctx, cudaStream_t st, const BoundaryParams& B, const AcousticDevice& D,
@@ -298,7 +452,7 @@ void launch_boundaries(nimbus_cuda_context* ctx, cudaStream_t st, const Boundary
 nimbus_status run_batched_device(nimbus_cuda_context* ctx, cudaStream_t st, const nimbus_acoustic_batched_args* a,
                                  const AcousticDevice& D, float* wave, const float* wave_in, float* density_begin)
 {
-    const Dims d{a->nx, a->ny, a->nz};
+    const Dims d = make_dims(a->nx, a->ny, a->nz);
     const size_t n = static_cast<size_t>(d.cells());
     const int yz = d.ny * d.nz, xz = d.nx * d.nz;
     if (wave_in == nullptr)
@@ -313,13 +467,12 @@ nimbus_status run_batched_device(nimbus_cuda_context* ctx, cudaStream_t st, cons
     if (density_begin)
         NB_CUDA(ctx, cudaMemcpyAsync(density_begin, D.rho, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
 
-    AcousticParams P = acoustic_params(a->nx, a->ny, a->nz, a->dx, a->dy, a->dz, a->dt_small, a->gamma, a->rho_min,
-                                       a->rho_max, a->p_min, a->p_max, a->p_ref_fallback, a->wind_clamp_h,
-                                       a->wind_clamp_v);
-    P.weight = a->mass_flux_weight;
-    P.frame_u = a->frame_velocity_u_ms;
-    P.frame_v = a->frame_velocity_v_ms;
-    P.top_open = a->bc_top == kTopOpen;
+    FusedParams F = fused_params(ctx, a->nx, a->ny, a->nz, a->dx, a->dy, a->dz, a->dt_small, a->gamma, a->rho_min,
+                                 a->rho_max, a->p_min, a->p_max, a->p_ref_fallback, a->wind_clamp_h, a->wind_clamp_v);
+    F.weight = a->mass_flux_weight;
+    F.frame_u = a->frame_velocity_u_ms;
+    F.frame_v = a->frame_velocity_v_ms;
+    F.top_open = a->bc_top == kTopOpen;
 
     BoundaryParams B{};
     B.d = d;
@@ -331,17 +484,50 @@ nimbus_status run_batched_device(nimbus_cuda_context* ctx, cudaStream_t st, cons
     B.frame_u = a->frame_velocity_u_ms;
     B.frame_v = a->frame_velocity_v_ms;
 
-    float* cur = D.rho;
-    float* alt = D.rho_alt;
+    float2* dp0 = nullptr;
+    NB_TRY(ensure(ctx, kDp0, static_cast<size_t>(d.nz), &dp0));
+    dp0_split_kernel<<<(d.nz + 127) / 128, 128, 0, st>>>(D.p0, d.nz, dp0);
+    ctx->launches += 1;
+    Prognostic user{D.u, D.v, D.w, D.rho};
+    Prognostic work{D.u_alt, D.v_alt, D.w_alt, D.rho_alt};
+    Prognostic cur = user, alt = work;
     for (int s = 0; s < a->n_substeps; ++s)
     {
-        float* now = launch_substep(ctx, st, P, cur, alt, D);
-        launch_boundaries(ctx, st, B, D, now, wave);
-        alt = cur;
-        cur = now;
+        NB_TRY(launch_fused(ctx, st, F, cur, alt, D.p, D.theta, D.rho0, D.p0, dp0, nullptr, D.mfx, D.mfy, D.mfz));
+        AcousticDevice E = D;
+        E.u = alt.u; E.v = alt.v; E.w = alt.w;
+        launch_boundaries(ctx, st, B, E, alt.rho, wave);
+        std::swap(cur, alt);
     }
-    if (cur != D.rho)
-        NB_CUDA(ctx, cudaMemcpyAsync(D.rho, cur, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+    if (cur.u != user.u)
+    {
+        NB_CUDA(ctx, cudaMemcpyAsync(user.u, cur.u, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+        NB_CUDA(ctx, cudaMemcpyAsync(user.v, cur.v, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+        NB_CUDA(ctx, cudaMemcpyAsync(user.w, cur.w, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+        NB_CUDA(ctx, cudaMemcpyAsync(user.rho, cur.rho, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+    }
+    NB_CUDA(ctx, cudaGetLastError());
+    return NIMBUS_OK;
+}
+
+// One fused substep on device memory, result back in the caller's arrays.
+nimbus_status run_fused_device(nimbus_cuda_context* ctx, cudaStream_t st, const nimbus_acoustic_fused_args* a,
+                               const AcousticDevice& D)
+{
+    const size_t n = static_cast<size_t>(a->nx) * a->ny * a->nz;
+    FusedParams F = fused_params(ctx, a->nx, a->ny, a->nz, a->dx, a->dy, a->dz, a->dt_small, a->gamma, a->rho_min,
+                                 a->rho_max, a->p_min, a->p_max, a->p_ref_fallback, a->wind_clamp_h, a->wind_clamp_v);
+    float2* dp0 = nullptr;
+    NB_TRY(ensure(ctx, kDp0, static_cast<size_t>(a->nz), &dp0));
+    dp0_split_kernel<<<(a->nz + 127) / 128, 128, 0, st>>>(D.p0, a->nz, dp0);
+    ctx->launches += 1;
+    Prognostic user{D.u, D.v, D.w, D.rho};
+    Prognostic work{D.u_alt, D.v_alt, D.w_alt, D.rho_alt};
+    NB_TRY(launch_fused(ctx, st, F, user, work, D.p, D.theta, D.rho0, D.p0, dp0, D.drho, nullptr, nullptr, nullptr));
+    NB_CUDA(ctx, cudaMemcpyAsync(user.u, work.u, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+    NB_CUDA(ctx, cudaMemcpyAsync(user.v, work.v, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+    NB_CUDA(ctx, cudaMemcpyAsync(user.w, work.w, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+    NB_CUDA(ctx, cudaMemcpyAsync(user.rho, work.rho, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
     NB_CUDA(ctx, cudaGetLastError());
     return NIMBUS_OK;
 }
@@ -392,7 +578,7 @@ const char* check_transport(const nimbus_scalar_transport_args* a)
 TransportParams transport_params(const nimbus_scalar_transport_args* a)
 {
     TransportParams T{};
-    T.d = Dims{a->nx, a->ny, a->nz};
+    T.d = make_dims(a->nx, a->ny, a->nz);
     T.inv_dx = 1.0 / a->dx;
     T.inv_dy = 1.0 / a->dy;
     T.inv_dz = 1.0 / a->dz;
@@ -417,7 +603,10 @@ nimbus_status run_transport_device(nimbus_cuda_context* ctx, cudaStream_t st, co
     const dim3 grid(grid_for(ctx, T.d.cells()), T.n_scalars);
     {
         LaunchTimer t(ctx, st, NIMBUS_KERNEL_TRANSPORT_FACES);
-        transport_faces_kernel<<<grid, kThreads, 0, st>>>(T, mfx, mfy, mfz, sf);
+        if (ctx->precision == NIMBUS_PRECISION_FP32)
+            transport_faces_f32_kernel<<<grid, kThreads, 0, st>>>(T, mfx, mfy, mfz, sf);
+        else
+            transport_faces_kernel<<<grid, kThreads, 0, st>>>(T, mfx, mfy, mfz, sf);
     }
     {
         LaunchTimer t(ctx, st, NIMBUS_KERNEL_TRANSPORT_LIMITER);
@@ -494,6 +683,107 @@ nimbus_status nimbus_cuda_synchronize(nimbus_cuda_context* ctx)
     return NIMBUS_OK;
 }
 
+nimbus_status nimbus_cuda_set_precision(nimbus_cuda_context* ctx, int precision)
+{
+    if (!ctx) return NIMBUS_ERR_INVALID_ARGUMENT;
+    if (precision != NIMBUS_PRECISION_REFERENCE && precision != NIMBUS_PRECISION_FP32)
+        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "unknown precision");
+    ctx->precision = precision;
+    return NIMBUS_OK;
+}
+
+nimbus_status nimbus_cuda_set_substep_form(nimbus_cuda_context* ctx, int form)
+{
+    if (!ctx) return NIMBUS_ERR_INVALID_ARGUMENT;
+    if (form != NIMBUS_SUBSTEP_AUTO && form != NIMBUS_SUBSTEP_FUSED && form != NIMBUS_SUBSTEP_SPLIT)
+        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "unknown substep form");
+    ctx->substep_form = form;
+    return NIMBUS_OK;
+}
+
+nimbus_status nimbus_cuda_autotune_substep(nimbus_cuda_context* ctx, int nx, int ny, int nz, int* chosen_form,
+                                           double* ms_per_substep)
+{
+    if (!ctx) return NIMBUS_ERR_INVALID_ARGUMENT;
+    if (nx < 3 || ny < 3 || nz < 2 || !cells_fit(nx, ny, nz)) return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "bad shape");
+    NB_CUDA(ctx, cudaSetDevice(ctx->device));
+    const size_t n = static_cast<size_t>(nx) * ny * nz;
+    // Scratch state: a resting isothermal column is enough to exercise every
+    // instruction path the timing depends on.
+    float* buf = nullptr;
+    double* prof = nullptr;
+    float2* dp0 = nullptr;
+    NB_CUDA(ctx, cudaMalloc(&buf, sizeof(float) * n * 13));
+    if (cudaMalloc(&prof, sizeof(double) * 2 * nz) != cudaSuccess || cudaMalloc(&dp0, sizeof(float2) * nz) != cudaSuccess)
+    {
+        cudaFree(buf);
+        if (prof) cudaFree(prof);
+        return fail(ctx, NIMBUS_ERR_OUT_OF_MEMORY, "autotune scratch");
+    }
+    cudaStream_t st = ctx->stream;
+    Prognostic a{buf, buf + n, buf + 2 * n, buf + 3 * n};
+    Prognostic b{buf + 4 * n, buf + 5 * n, buf + 6 * n, buf + 7 * n};
+    float* p = buf + 8 * n;
+    float* theta = buf + 9 * n;
+    float* mf = buf + 10 * n;
+    fill_tuning_state<<<grid_for(ctx, static_cast<long long>(n)), kThreads, 0, st>>>(buf, n, prof, nz, dp0);
+    FusedParams F = fused_params(ctx, nx, ny, nz, 250.0, 250.0, 250.0, 0.1, 1004.0 / 717.0, 0.05f, 2.0f, 1000.0f,
+                                 200000.0f, 100000.0f, 180.0f, 120.0f);
+    F.weight = 0.1;
+    const int saved_form = ctx->substep_form;
+    const bool saved_timing = ctx->timing;
+    ctx->timing = false;
+    int best = NIMBUS_SUBSTEP_SPLIT;
+    double best_ms = 1e30;
+    nimbus_status rc = NIMBUS_OK;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    for (int form : {NIMBUS_SUBSTEP_SPLIT, NIMBUS_SUBSTEP_FUSED})
+    {
+        ctx->substep_form = form;
+        const int reps = 6;
+        for (int w = 0; w < 2 + reps && rc == NIMBUS_OK; ++w)
+        {
+            if (w == 2) cudaEventRecord(e0, st);
+            rc = launch_fused(ctx, st, F, (w & 1) ? b : a, (w & 1) ? a : b, p, theta, prof, prof + nz, dp0, nullptr,
+                              mf, mf + n, mf + 2 * n);
+        }
+        cudaEventRecord(e1, st);
+        if (rc != NIMBUS_OK) break;
+        if (cudaEventSynchronize(e1) != cudaSuccess) { rc = cuda_fail(ctx, cudaGetLastError(), "autotune"); break; }
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        const double per = ms / reps;
+        if (per < best_ms)
+        {
+            best_ms = per;
+            best = form;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaMemsetAsync(ctx->status, 0, sizeof(unsigned), st);
+    cudaStreamSynchronize(st);
+    cudaFree(buf);
+    cudaFree(prof);
+    cudaFree(dp0);
+    ctx->substep_form = saved_form;
+    ctx->timing = saved_timing;
+    if (rc != NIMBUS_OK) return rc;
+    bool found = false;
+    for (auto& e : ctx->tuned)
+        if (e.nx == nx && e.ny == ny && e.nz == nz && e.precision == ctx->precision)
+        {
+            e.form = best;
+            found = true;
+        }
+    if (!found) ctx->tuned.push_back({nx, ny, nz, ctx->precision, best});
+    if (chosen_form) *chosen_form = best;
+    if (ms_per_substep) *ms_per_substep = best_ms;
+    return NIMBUS_OK;
+}
+
 nimbus_status nimbus_cuda_set_kernel_timing(nimbus_cuda_context* ctx, int enable)
 {
     if (!ctx) return NIMBUS_ERR_INVALID_ARGUMENT;
@@ -539,11 +829,8 @@ nimbus_status nimbus_cuda_acoustic_fused(nimbus_cuda_context* ctx, const nimbus_
     {
         if (a->stream) st = static_cast<cudaStream_t>(a->stream);
         D = {a->u, a->v, a->w, a->rho, a->p, a->theta, a->rho0_base, a->p0_base, nullptr, a->drho_scratch};
-        NB_TRY(ensure(ctx, kRhoAlt, n, &D.rho_alt));
-        float* now = launch_substep(ctx, st, P, D.rho, D.rho_alt, D);
-        NB_CUDA(ctx, cudaMemcpyAsync(D.rho, now, bytes, cudaMemcpyDeviceToDevice, st));
-        NB_CUDA(ctx, cudaGetLastError());
-        return NIMBUS_OK;
+        NB_TRY(ensure_alts(ctx, n, D));
+        return run_fused_device(ctx, st, a, D);
     }
     float *u, *v, *w, *rho, *p, *theta, *alt, *drho = nullptr;
     double *rho0, *p0;
@@ -566,13 +853,13 @@ nimbus_status nimbus_cuda_acoustic_fused(nimbus_cuda_context* ctx, const nimbus_
     NB_TRY(upload(ctx, rho0, a->rho0_base, sizeof(double) * a->nz));
     NB_TRY(upload(ctx, p0, a->p0_base, sizeof(double) * a->nz));
     D = {u, v, w, rho, p, theta, rho0, p0, alt, drho};
-    float* now = launch_substep(ctx, st, P, rho, alt, D);
-    NB_CUDA(ctx, cudaGetLastError());
+    NB_TRY(ensure_alts(ctx, n, D));
+    NB_TRY(run_fused_device(ctx, st, a, D));
     NB_CUDA(ctx, cudaStreamSynchronize(st));
     NB_TRY(download(ctx, a->u, u, bytes));
     NB_TRY(download(ctx, a->v, v, bytes));
     NB_TRY(download(ctx, a->w, w, bytes));
-    NB_TRY(download(ctx, a->rho, now, bytes));
+    NB_TRY(download(ctx, a->rho, rho, bytes));
     NB_TRY(download(ctx, a->p, p, bytes));
     if (drho) NB_TRY(download(ctx, a->drho_scratch, drho, bytes));
     NB_CUDA(ctx, cudaStreamSynchronize(st));
@@ -596,7 +883,7 @@ nimbus_status nimbus_cuda_acoustic_batched(nimbus_cuda_context* ctx, const nimbu
         if (a->stream) st = static_cast<cudaStream_t>(a->stream);
         AcousticDevice D{a->u, a->v, a->w, a->rho, a->p, a->theta, a->rho0_base, a->p0_base, nullptr, nullptr,
                          mf ? a->mass_flux_x : nullptr, mf ? a->mass_flux_y : nullptr, mf ? a->mass_flux_z : nullptr};
-        NB_TRY(ensure(ctx, kRhoAlt, n, &D.rho_alt));
+        NB_TRY(ensure_alts(ctx, n, D));
         return run_batched_device(ctx, st, a, D, a->wave_history_output, a->wave_history, a->density_begin);
     }
     float *u, *v, *w, *rho, *p, *theta, *alt, *wave, *rb = nullptr, *mx = nullptr, *my = nullptr, *mz = nullptr;
@@ -631,6 +918,7 @@ nimbus_status nimbus_cuda_acoustic_batched(nimbus_cuda_context* ctx, const nimbu
     NB_TRY(upload(ctx, p0, a->p0_base, sizeof(double) * a->nz));
     if (a->wave_history) NB_TRY(upload(ctx, wave, a->wave_history, sizeof(float) * waves));
     AcousticDevice D{u, v, w, rho, p, theta, rho0, p0, alt, nullptr, mx, my, mz};
+    NB_TRY(ensure_alts(ctx, n, D));
     NB_TRY(run_batched_device(ctx, st, a, D, wave, a->wave_history ? wave : nullptr, rb));
     unsigned flags = 0;
     NB_TRY(read_status(ctx, st, &flags));

@@ -49,14 +49,55 @@ enum : unsigned
 struct Dims
 {
     int nx, ny, nz;
+    // Division by nz and ny as (x * magic) >> 32 with magic = ceil(2^32 / d)
+    // = (2^32 + e) / d: floor(x*magic / 2^32) = floor(x / d) whenever
+    // x * e < 2^32, since the excess x*e/(d*2^32) then stays below 1/d.
+    // make_dims() checks that bound for the largest dividend and leaves the
+    // magic at 0 (plain division) when it does not hold.
+    unsigned nz_magic = 0, ny_magic = 0;
     __host__ __device__ __forceinline__ int cells() const { return nx * ny * nz; }
     __host__ __device__ __forceinline__ int at(int i, int j, int k) const { return (i * ny + j) * nz + k; }
     __host__ __device__ __forceinline__ int sx() const { return ny * nz; }  // stride of i
     __host__ __device__ __forceinline__ int sy() const { return nz; }       // stride of j
 };
 
+__host__ __device__ __forceinline__ unsigned div_magic(unsigned d)
+{
+    return (unsigned)((0x100000000ull + d - 1) / d);
+}
+
+// Magic for dividing every x <= x_max by d, or 0 if the bound fails.
+__host__ __device__ __forceinline__ unsigned checked_magic(unsigned d, unsigned long long x_max)
+{
+    if (d == 0) return 0;
+    const unsigned m = div_magic(d);
+    const unsigned long long e = (unsigned long long)m * d - 0x100000000ull;
+    return (x_max * e < 0x100000000ull) ? m : 0u;
+}
+
+__host__ __device__ __forceinline__ Dims make_dims(int nx, int ny, int nz)
+{
+    Dims d;
+    d.nx = nx;
+    d.ny = ny;
+    d.nz = nz;
+    const unsigned long long cells = (unsigned long long)nx * ny * nz;
+    d.nz_magic = checked_magic((unsigned)nz, cells);
+    d.ny_magic = checked_magic((unsigned)ny, (unsigned long long)nx * ny);
+    if (d.nz_magic == 0 || d.ny_magic == 0) d.nz_magic = d.ny_magic = 0;
+    return d;
+}
+
 __device__ __forceinline__ void decompose(const Dims& d, int c, int& i, int& j, int& k)
 {
+    if (d.nz_magic != 0)
+    {
+        const int t = (int)__umulhi((unsigned)c, d.nz_magic);
+        k = c - t * d.nz;
+        i = (int)__umulhi((unsigned)t, d.ny_magic);
+        j = t - i * d.ny;
+        return;
+    }
     k = c % d.nz;
     const int t = c / d.nz;
     j = t % d.ny;

@@ -90,6 +90,99 @@ __device__ __forceinline__ double face_value(const float* __restrict__ q, int ba
 #undef NQ
 }
 
+// FP32 face offset from the donor value: weno5_face_offset_fp32
+// (include/numerics/advection/weno5_face.hpp:88-120), the reference's own FP32
+// GPU reconstruction (scale-normalised, so moisture-scale fields keep their
+// nonlinear weights).
+__device__ __forceinline__ float weno5_offset_f32(float a, float b, float c, float d, float e)
+{
+    const float magnitude = fmaxf(fmaxf(fmaxf(fabsf(a), fabsf(b)), fmaxf(fabsf(c), fabsf(d))), fabsf(e));
+    const float scale = fmaxf(magnitude, 1e-20f);
+    if (!isfinite(scale)) return 0.0f;
+    const float inv = __frcp_rn(scale);
+    auto diff = [&](float value) {
+        const float delta = value - c;
+        return isfinite(delta) ? delta * inv : value * inv - c * inv;
+    };
+    const float ac = diff(a), bc = diff(b), dc = diff(d), ec = diff(e);
+    const float p0 = (1.0f / 3.0f) * ac - (7.0f / 6.0f) * bc;
+    const float p1 = -(1.0f / 6.0f) * bc + (1.0f / 3.0f) * dc;
+    const float p2 = (5.0f / 6.0f) * dc - (1.0f / 6.0f) * ec;
+    const float s0a = ac - 2.0f * bc, s0b = ac - 4.0f * bc;
+    const float s1a = bc + dc, s1b = bc - dc;
+    const float s2a = ec - 2.0f * dc, s2b = ec - 4.0f * dc;
+    const float b0 = (13.0f / 12.0f) * s0a * s0a + 0.25f * s0b * s0b;
+    const float b1 = (13.0f / 12.0f) * s1a * s1a + 0.25f * s1b * s1b;
+    const float b2 = (13.0f / 12.0f) * s2a * s2a + 0.25f * s2b * s2b;
+    const float relative = magnitude * inv;
+    const float flo = 1e-20f * inv;
+    const float epsilon = 1e-6f * relative * relative + flo * flo;
+    const float e0 = epsilon + b0, e1 = epsilon + b1, e2 = epsilon + b2;
+    const float minimum = fminf(fminf(e0, e1), e2);
+    const float r0 = __fdividef(minimum, e0), r1 = __fdividef(minimum, e1), r2 = __fdividef(minimum, e2);
+    const float a0 = 0.1f * r0 * r0, a1 = 0.6f * r1 * r1, a2 = 0.3f * r2 * r2;
+    const float sum = a0 + a1 + a2;
+    const float offset = scale * __fdividef(a0 * p0 + a1 * p1 + a2 * p2, sum);
+    return isfinite(offset) ? offset : 0.0f;
+}
+
+__device__ __forceinline__ float mc_slope_f32(float qm, float q0, float qp)
+{
+    const float right = qp - q0, left = q0 - qm;
+    const float a = 0.5f * (right + left), b = 2.0f * right, c = 2.0f * left;
+    if (a > 0.0f && b > 0.0f && c > 0.0f) return fminf(a, fminf(b, c));
+    if (a < 0.0f && b < 0.0f && c < 0.0f) return fmaxf(a, fmaxf(b, c));
+    return 0.0f;
+}
+
+// FP32 scalar face flux M*phi as M*base + M*offset (the reference's FP32 GPU form).
+__device__ __forceinline__ float face_flux_f32(const float* __restrict__ q, int base, int stride, int l, int n,
+                                               float mflux, int weno)
+{
+#define NQ(m) (q[base + (m) * stride])
+    float donor, offset;
+    if (mflux >= 0.0f)
+    {
+        donor = NQ(l);
+        if (weno && l >= 2 && l + 2 <= n - 1) offset = weno5_offset_f32(NQ(l - 2), NQ(l - 1), donor, NQ(l + 1), NQ(l + 2));
+        else offset = 0.5f * ((l >= 1) ? mc_slope_f32(NQ(l - 1), donor, NQ(l + 1)) : 0.0f);
+    }
+    else
+    {
+        donor = NQ(l + 1);
+        if (weno && l - 1 >= 0 && l + 3 <= n - 1) offset = weno5_offset_f32(NQ(l + 3), NQ(l + 2), donor, NQ(l), NQ(l - 1));
+        else offset = -0.5f * ((l + 1 <= n - 2) ? mc_slope_f32(NQ(l), donor, NQ(l + 2)) : 0.0f);
+    }
+    return __fmaf_rn(mflux, donor, mflux * offset);
+#undef NQ
+}
+
+__global__ void __launch_bounds__(256) transport_faces_f32_kernel(TransportParams T, const float* __restrict__ mfx,
+                                                                  const float* __restrict__ mfy,
+                                                                  const float* __restrict__ mfz, float* __restrict__ sf)
+{
+    const Dims d = T.d;
+    const int n = d.cells();
+    const int s = blockIdx.y;
+    const float* __restrict__ q = T.q_in[s];
+    float* __restrict__ sfx = sf + (size_t)s * 3 * n;
+    float* __restrict__ sfy = sfx + n;
+    float* __restrict__ sfz = sfy + n;
+    const int kz_end = T.top_open ? d.nz : d.nz - 1;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+    {
+        int i, j, k;
+        decompose(d, c, i, j, k);
+        if (i <= d.nx - 2) sfx[c] = face_flux_f32(q, c - i * d.sx(), d.sx(), i, d.nx, mfx[c], T.weno);
+        if (j <= d.ny - 2) sfy[c] = face_flux_f32(q, c - j * d.sy(), d.sy(), j, d.ny, mfy[c], T.weno);
+        if (k < kz_end)
+        {
+            const float mf = mfz[c];
+            sfz[c] = (k == d.nz - 1) ? mf * q[c] : face_flux_f32(q, c - k, 1, k, d.nz, mf, T.weno);
+        }
+    }
+}
+
 __global__ void __launch_bounds__(256) transport_faces_kernel(TransportParams T, const float* __restrict__ mfx,
                                                               const float* __restrict__ mfy,
                                                               const float* __restrict__ mfz, float* __restrict__ sf)

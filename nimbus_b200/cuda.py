@@ -92,8 +92,11 @@ EXPORTED_SYMBOLS = (
     "nimbus_cuda_kernel_launches", "nimbus_cuda_stream", "nimbus_cuda_synchronize",
     "nimbus_cuda_acoustic_fused", "nimbus_cuda_acoustic_batched", "nimbus_cuda_scalar_transport",
     "nimbus_cuda_set_kernel_timing", "nimbus_cuda_kernel_timing",
-    "nimbus_cuda_acoustic_fused_static_scratch",
+    "nimbus_cuda_acoustic_fused_static_scratch", "nimbus_cuda_set_precision",
+    "nimbus_cuda_set_substep_form", "nimbus_cuda_autotune_substep",
 )
+SUBSTEP_AUTO, SUBSTEP_FUSED, SUBSTEP_SPLIT = 0, 1, 2
+PRECISION_REFERENCE, PRECISION_FP32 = 0, 1
 STATIC_SCRATCH_CELLS = 4194304  # NIMBUS_STATIC_SCRATCH_CELLS
 KERNEL_FAMILIES = ("acoustic_substep", "acoustic_momentum", "acoustic_boundary", "transport_faces",
                    "transport_limiter", "transport_update")
@@ -116,6 +119,10 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
     lib.nimbus_cuda_acoustic_fused.argtypes = [ctypes.c_void_p, ctypes.POINTER(AcousticFusedArgs)]
     lib.nimbus_cuda_acoustic_batched.argtypes = [ctypes.c_void_p, ctypes.POINTER(AcousticBatchedArgs)]
     lib.nimbus_cuda_scalar_transport.argtypes = [ctypes.c_void_p, ctypes.POINTER(ScalarTransportArgs)]
+    lib.nimbus_cuda_set_precision.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    lib.nimbus_cuda_set_substep_form.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    lib.nimbus_cuda_autotune_substep.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                 ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
     lib.nimbus_cuda_acoustic_fused_static_scratch.argtypes = [ctypes.POINTER(AcousticFusedArgs)]
     lib.nimbus_cuda_set_kernel_timing.argtypes = [ctypes.c_void_p, ctypes.c_int]
     lib.nimbus_cuda_kernel_timing.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64),
@@ -194,6 +201,19 @@ class Context:
     def synchronize(self):
         self.check(self.lib.nimbus_cuda_synchronize(self.handle))
 
+    def set_precision(self, precision: int):
+        self.check(self.lib.nimbus_cuda_set_precision(self.handle, int(precision)))
+
+    def set_substep_form(self, form: int):
+        self.check(self.lib.nimbus_cuda_set_substep_form(self.handle, int(form)))
+
+    def autotune_substep(self, nx: int, ny: int, nz: int):
+        """(chosen form, ms per substep) for this shape in the current precision."""
+        form = ctypes.c_int()
+        ms = ctypes.c_double()
+        self.check(self.lib.nimbus_cuda_autotune_substep(self.handle, nx, ny, nz, ctypes.byref(form), ctypes.byref(ms)))
+        return int(form.value), float(ms.value)
+
     def set_kernel_timing(self, enable: bool):
         self.check(self.lib.nimbus_cuda_set_kernel_timing(self.handle, int(enable)))
 
@@ -230,7 +250,7 @@ def fused_args(st, rho0, p0, dt_small, grid, drho=None, memory=MEMORY_HOST, stre
     a = AcousticFusedArgs()
     a.u, a.v, a.w, a.rho, a.p, a.theta = (_f(st[k]) for k in ("u", "v", "w", "rho", "p", "theta"))
     a.rho0_base, a.p0_base = _d(rho0), _d(p0)
-    a._keep = (rho0, p0)
+    a._keep = (dict(st), rho0, p0, drho)  # the block holds raw pointers: keep every array alive
     a.base_len = nz
     a.nx, a.ny, a.nz = nx, ny, nz
     a.dx, a.dy, a.dz = grid
@@ -247,6 +267,7 @@ def batched_args(st, rho0, p0, dt_small, n_substeps, grid, bc, mfx, mfy, mfz, we
                  density_begin=None, frame=(0.0, 0.0), memory=MEMORY_HOST, stream=None) -> AcousticBatchedArgs:
     nx, ny, nz = st["u"].shape
     a = AcousticBatchedArgs()
+    a._keep = (dict(st), rho0, p0, mfx, mfy, mfz, wave_in, wave_out, density_begin)
     a.u, a.v, a.w, a.rho, a.p, a.theta = (_f(st[k]) for k in ("u", "v", "w", "rho", "p", "theta"))
     a.rho0_base, a.p0_base = _d(rho0), _d(p0)
     a.base_len = nz
@@ -277,7 +298,7 @@ def transport_args(q_in: Sequence, q_out: Sequence, pd: Sequence[int], rho_end, 
     qi = (_fp * max(n, 1))(*[_f(q) for q in q_in])
     qo = (_fp * max(n, 1))(*[_f(q) for q in q_out])
     flags = (ctypes.c_int * max(n, 1))(*[int(x) for x in pd])
-    a._keep = (qi, qo, flags)
+    a._keep = (qi, qo, flags, list(q_in), list(q_out), rho_end, rho_begin, mfx, mfy, mfz)
     a.q_in, a.q_out, a.positive_definite = qi, qo, flags
     a.n_scalars = n
     a.nx, a.ny, a.nz = nx, ny, nz

@@ -6,8 +6,9 @@ the hot path it owns):
   1. open the retained transport context: zero the face mass-flux sums
      (CartesianCGridTransportContext::begin);
   2. the acoustic loop: N substeps, each with mass-flux accumulation, the
-     fused substep and the boundary closure; the KW78 history carries over
-     between large steps (split_explicit.cpp:174-260);
+     fused substep and the boundary closure; the KW78 radiation memory is
+     re-seeded from the live faces at the start of every large step, as
+     seed_acoustic_radiation does (split_explicit.cpp:174-205);
   3. conservative WENO5 transport of theta, qv, qc, qr against the retained
      fluxes and densities (advection_batch.cpp:565-760).
 
@@ -29,8 +30,14 @@ PROGNOSTIC = ("u", "v", "w", "rho", "p") + SCALARS
 
 
 class ResidentRun:
-    def __init__(self, ctx: cuda.Context, case: Case, state=None, base=None, device="cuda"):
+    def __init__(self, ctx: cuda.Context, case: Case, state=None, base=None, device="cuda",
+                 precision: int = cuda.PRECISION_FP32, autotune: bool = True):
         self.ctx = ctx
+        self.precision = precision
+        self.tuned = None
+        if autotune:
+            ctx.set_precision(precision)
+            self.tuned = ctx.autotune_substep(case.nx, case.ny, case.nz)
         self.case = case
         if state is None:
             state, base = initial_state(case)
@@ -45,16 +52,12 @@ class ResidentRun:
         self.wave = torch.zeros(2 * (case.nx + case.ny) * case.nz, dtype=torch.float32, device=dev)
         self.rho0 = torch.from_numpy(base["rho0"]).to(dev)
         self.p0 = torch.from_numpy(base["p0"]).to(dev)
-        self.have_wave = False
         self.stream = ctx.stream
         grid = (case.dx, case.dy, case.dz)
         n = self.n_substeps
-        self._loop_seed = cuda.batched_args(self.fields, self.rho0, self.p0, case.dt / n, n, grid, case.bc, *self.mf,
-                                            (case.dt / n) / case.dt, None, self.wave, self.rho_begin,
-                                            memory=cuda.MEMORY_DEVICE)
-        self._loop_carry = cuda.batched_args(self.fields, self.rho0, self.p0, case.dt / n, n, grid, case.bc,
-                                             *self.mf, (case.dt / n) / case.dt, self.wave, self.wave, self.rho_begin,
-                                             memory=cuda.MEMORY_DEVICE)
+        self._loop = cuda.batched_args(self.fields, self.rho0, self.p0, case.dt / n, n, grid, case.bc, *self.mf,
+                                       (case.dt / n) / case.dt, None, self.wave, self.rho_begin,
+                                       memory=cuda.MEMORY_DEVICE)
         qs = [self.fields[k] for k in SCALARS]
         self._transport = cuda.transport_args(qs, qs, POSITIVE, self.fields["rho"], self.rho_begin, *self.mf, case.dt,
                                               grid, weno=True, top_open=case.bc[5] == 2, memory=cuda.MEMORY_DEVICE)
@@ -66,11 +69,11 @@ class ResidentRun:
 
     def step(self):
         """Enqueue one large step on the context stream (no host synchronisation)."""
+        self.ctx.set_precision(self.precision)
         with torch.cuda.stream(self.torch_stream):
             for m in self.mf:
                 m.zero_()
-        self.ctx.check(self.ctx.acoustic_batched(self._loop_carry if self.have_wave else self._loop_seed))
-        self.have_wave = True
+        self.ctx.check(self.ctx.acoustic_batched(self._loop))
         self.ctx.check(self.ctx.scalar_transport(self._transport))
 
     def download(self) -> dict:
@@ -84,8 +87,10 @@ class HostStepper:
     every call uploads its inputs from (pinned) host arrays and returns the
     results to them, as the reference's fence-confirmed dispatches do."""
 
-    def __init__(self, ctx: cuda.Context, case: Case, state=None, base=None, pin=True):
+    def __init__(self, ctx: cuda.Context, case: Case, state=None, base=None, pin=True,
+                 precision: int = cuda.PRECISION_FP32):
         self.ctx = ctx
+        self.precision = precision
         self.case = case
         if state is None:
             state, base = initial_state(case)
@@ -102,12 +107,10 @@ class HostStepper:
         self.mf = [host(np.zeros(shape, np.float32)) for _ in range(3)]
         self.rho_begin = host(np.zeros(shape, np.float32))
         self.wave = host(np.zeros(2 * (case.nx + case.ny) * case.nz, np.float32))
-        self.have_wave = False
         grid = (case.dx, case.dy, case.dz)
         n = self.n_substeps
-        self._loop = [cuda.batched_args(self.fields, base["rho0"], base["p0"], case.dt / n, n, grid, case.bc, *self.mf,
-                                        (case.dt / n) / case.dt, w, self.wave, self.rho_begin)
-                      for w in (None, self.wave)]
+        self._loop = cuda.batched_args(self.fields, base["rho0"], base["p0"], case.dt / n, n, grid, case.bc, *self.mf,
+                                       (case.dt / n) / case.dt, None, self.wave, self.rho_begin)
         qs = [self.fields[k] for k in SCALARS]
         self._transport = cuda.transport_args(qs, qs, POSITIVE, self.fields["rho"], self.rho_begin, *self.mf, case.dt,
                                               grid, weno=True, top_open=case.bc[5] == 2)
@@ -118,16 +121,17 @@ class HostStepper:
         n = self.case.cells * 4
         w = self.wave.nbytes
         prof = self.base["rho0"].nbytes + self.base["p0"].nbytes
-        # acoustic batch: in u,v,w,rho,p,theta + 3 mass fluxes + wave history + profiles;
-        #                 out u,v,w,rho,p + 3 mass fluxes + rho_begin + wave history
+        # acoustic batch: in u,v,w,rho,p,theta + 3 mass fluxes + profiles (the KW78
+        #                 memory is seeded on the device); out u,v,w,rho,p + 3 mass
+        #                 fluxes + rho_begin + wave history
         # transport:      in rho_end, rho_begin, 3 mass fluxes, 4 scalars; out 4 scalars
-        h2d = 9 * n + w + prof + 9 * n
+        h2d = 9 * n + prof + 9 * n
         d2h = 9 * n + w + 4 * n
         return h2d, d2h
 
     def step(self):
+        self.ctx.set_precision(self.precision)
         for m in self.mf:
             m[...] = 0.0
-        self.ctx.check(self.ctx.acoustic_batched(self._loop[1 if self.have_wave else 0]))
-        self.have_wave = True
+        self.ctx.check(self.ctx.acoustic_batched(self._loop))
         self.ctx.check(self.ctx.scalar_transport(self._transport))

@@ -66,3 +66,43 @@ def test_no_device_is_an_error_not_a_fallback():
     assert exc.value.status == 6  # NIMBUS_ERR_NO_DEVICE
     backend = cuda.CudaComputeBackend()
     assert backend.initialize() is False and "NO_DEVICE" in backend.last_error
+
+
+def test_argument_blocks_keep_their_arrays_alive():
+    """Argument blocks hold raw pointers; the binding must keep every array
+    they point at alive even when the caller passed temporaries."""
+    import gc
+
+    import numpy as np
+
+    shape = (6, 5, 4)
+
+    def tmp():
+        return np.random.default_rng(0).random(shape).astype(np.float32)
+
+    a = cuda.transport_args([tmp(), tmp()], [tmp(), tmp()], [0, 1], tmp(), tmp(), tmp(), tmp(), tmp(), 1.0,
+                            (1.0, 1.0, 1.0))
+    st = {k: tmp() for k in ("u", "v", "w", "rho", "p", "theta")}
+    b = cuda.batched_args(st, np.ones(4), np.ones(4), 0.1, 2, (1.0, 1.0, 1.0), (1, 1, 1, 1, 1, 0), tmp(), tmp(),
+                          tmp(), 0.5, None, np.zeros(2 * 11 * 4, np.float32), tmp())
+    del st
+    gc.collect()
+
+    def kept_addresses(block):
+        out = set()
+        for item in block._keep:
+            items = item.values() if isinstance(item, dict) else (item if isinstance(item, list) else [item])
+            for arr in items:
+                if isinstance(arr, np.ndarray):
+                    out.add(arr.ctypes.data)
+        return out
+
+    for block, names in ((a, ("rho_end", "rho_begin", "mass_flux_x", "mass_flux_y", "mass_flux_z")),
+                         (b, ("u", "rho", "theta", "rho0_base", "mass_flux_z", "wave_history_output",
+                              "density_begin"))):
+        kept = kept_addresses(block)
+        for name in names:
+            addr = ctypes.cast(getattr(block, name), ctypes.c_void_p).value
+            assert addr in kept, name
+    for i in range(2):
+        assert ctypes.cast(a.q_in[i], ctypes.c_void_p).value in kept_addresses(a)

@@ -21,9 +21,13 @@ pytestmark = pytest.mark.gpu
 GOLDEN = sorted(glob.glob("tests/golden/loop_*.npz"))
 
 
-@pytest.fixture(scope="module")
-def ctx():
+@pytest.fixture(scope="module", params=[cuda.SUBSTEP_FUSED, cuda.SUBSTEP_SPLIT], ids=["fused", "split"])
+def ctx(request):
+    """A reference-precision context, once per substep form: every form must
+    reproduce the reference bit for bit."""
     c = cuda.Context(0)
+    c.set_precision(cuda.PRECISION_REFERENCE)
+    c.set_substep_form(request.param)
     yield c
     c.close()
 
