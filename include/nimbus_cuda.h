@@ -145,7 +145,9 @@ enum
     NIMBUS_KERNEL_TRANSPORT_FACES = 3,
     NIMBUS_KERNEL_TRANSPORT_LIMITER = 4,
     NIMBUS_KERNEL_TRANSPORT_UPDATE = 5,
-    NIMBUS_KERNEL_FAMILIES = 6
+    NIMBUS_KERNEL_SLOW = 6,               /* slow tendencies (k1+predictor, k2+apply) */
+    NIMBUS_KERNEL_MICROPHYSICS = 7,       /* Kessler and the EOS re-projection */
+    NIMBUS_KERNEL_FAMILIES = 8
 };
 /* When enabled, every launch is bracketed by CUDA events on its own stream
  * and nimbus_cuda_kernel_timing() returns, per family, the launch count and
@@ -316,6 +318,123 @@ typedef struct nimbus_scalar_transport_args
 } nimbus_scalar_transport_args;
 
 nimbus_status nimbus_cuda_scalar_transport(nimbus_cuda_context* ctx, const nimbus_scalar_transport_args* a);
+
+/*
+ * Slow (advective) tendencies of the C-grid KW scheme and the Heun slow step.
+ *
+ * nimbus_cuda_slow_tendencies evaluates the operator once: it replaces
+ * DynamicsComputeKernels::dispatch_cartesian_cgrid_slow_tendencies
+ * (include/compute/dispatch/dynamics.hpp:374-420) with CPU semantics
+ * CartesianCGrid3DScheme::compute_slow_tendencies (cartesian_cgrid_3d.cpp:724-1416)
+ * on the stationary flat branch: du, dv, dw on 1<=i<=nx-2, 1<=j<=ny-2,
+ * 0<=k<=nz-2 (fd5/fd3/fd1 upwind-biased advection, f-plane Coriolis on the
+ * perturbation wind, buoyancy with vapour and hydrometeor loading on w) and
+ * dp = -u.grad p on 1<=k<=nz-2; zero elsewhere.  u, v, w, p are inputs and
+ * du_dt .. dp_dt are required outputs.
+ *
+ * nimbus_cuda_slow_step advances u, v, w, p in place by one Heun slow step
+ * with dt_large: k1 = L(x), x* = x + dt k1, k2 = L(x*), x += dt*0.5f(k2+k1)
+ * (prepare_slow_rk2_tendencies, dynamics.cpp:5123-5292, then
+ * apply_slow_tendencies, dynamics.cpp:1955-2092).  du_dt .. dp_dt are
+ * optional and receive the averaged tendency.
+ *
+ * qv/qc/qr may be NULL (dry, or no loading); qi, qs, qg, qh are taken as zero.
+ */
+typedef struct nimbus_slow_args
+{
+    float* u;
+    float* v;
+    float* w;
+    float* p;
+    const float* rho;
+    const float* qv;
+    const float* qc;
+    const float* qr;
+    const double* rho0_base;
+    const double* qv0_base;  /* may be NULL when qv is NULL */
+    const double* u0_base;   /* environment wind for the Coriolis terms; NULL = 0 */
+    const double* v0_base;
+    int base_len;
+    int nx, ny, nz;
+    double dx, dy, dz;
+    double dt_large;
+    double gravity;          /* 9.81 */
+    double coriolis_f;
+    float frame_velocity_u_ms, frame_velocity_v_ms;
+    float* du_dt;
+    float* dv_dt;
+    float* dw_dt;
+    float* dp_dt;
+    int memory;
+    void* stream;
+} nimbus_slow_args;
+
+nimbus_status nimbus_cuda_slow_tendencies(nimbus_cuda_context* ctx, const nimbus_slow_args* a);
+nimbus_status nimbus_cuda_slow_step(nimbus_cuda_context* ctx, const nimbus_slow_args* a);
+
+/*
+ * Kessler warm-rain microphysics.
+ * nimbus_cuda_kessler_tendencies replaces the Kessler MicrophysicsComputeKernels
+ * dispatches (include/compute/dispatch/microphysics.hpp) with CPU semantics
+ * KesslerScheme::compute_tendencies (src/microphysics/schemes/kessler/kessler.cpp:103-520):
+ * coupled saturation adjustment, autoconversion (qc0 1e-3, 1e-3 /s),
+ * accretion (2.2), rain evaporation and rain sedimentation over the cell
+ * domain [i0,i1)x[j0,j1)x[k0,k1); dtheta/dqv/dqc/dqr are required outputs
+ * (zero outside the domain).
+ * nimbus_cuda_kessler_step also applies them with dt over the domain: water
+ * species as clamp(q + dt dq, 0, 0.05) (bounded_water_value,
+ * microphysics_step.cpp:503-532), theta as theta + dt dtheta; the tendency
+ * outputs are optional there.
+ */
+typedef struct nimbus_kessler_args
+{
+    float* theta;
+    float* qv;
+    float* qc;
+    float* qr;
+    const float* p;
+    const float* rho;
+    int nx, ny, nz;
+    double dz;
+    double dt;
+    int domain[6];           /* i0, i1, j0, j1, k0, k1; the C-grid uses {1, nx-1, 1, ny-1, 0, nz} */
+    float* dtheta_dt;
+    float* dqv_dt;
+    float* dqc_dt;
+    float* dqr_dt;
+    int memory;
+    void* stream;
+} nimbus_kessler_args;
+
+nimbus_status nimbus_cuda_kessler_tendencies(nimbus_cuda_context* ctx, const nimbus_kessler_args* a);
+nimbus_status nimbus_cuda_kessler_step(nimbus_cuda_context* ctx, const nimbus_kessler_args* a);
+
+/*
+ * EOS pressure re-projection after transport and microphysics
+ * (tmv::dynamics_eos::apply_pressure_projection, eos_apply.cpp:50-200):
+ * p = clamp(float(p00 (rho R_d theta / p00)^gamma), 1000, 2e5) in FP64 for
+ * every cell.  qv/qc/qr are optional (all or none); given, the state counts as
+ * complete and the attributed cells (the one-cell lateral ring dropped where
+ * the extent is >= 3) are also checked as the reference's energy attribution
+ * checks them.  The energy report itself is not formed.  An invalid cell
+ * refuses the whole projection and p keeps its old values: host memory returns
+ * NIMBUS_ERR_NONFINITE; device memory reports it at nimbus_cuda_synchronize.
+ */
+typedef struct nimbus_eos_args
+{
+    float* p;
+    const float* rho;
+    const float* theta;
+    const float* qv;
+    const float* qc;
+    const float* qr;
+    int nx, ny, nz;
+    double gamma;
+    int memory;
+    void* stream;
+} nimbus_eos_args;
+
+nimbus_status nimbus_cuda_eos_projection(nimbus_cuda_context* ctx, const nimbus_eos_args* a);
 
 #ifdef __cplusplus
 }

@@ -9,6 +9,8 @@
 #include "acoustic_fused.cuh"
 #include "acoustic_kernels.cuh"
 #include "acoustic_split.cuh"
+#include "slow_kernels.cuh"
+#include "physics_kernels.cuh"
 #include "transport_kernels.cuh"
 
 #include <cmath>
@@ -37,7 +39,9 @@ struct DeviceBuffer
 enum Slot
 {
     kU, kV, kW, kRho, kP, kTheta, kRhoAlt, kDrho, kRho0, kP0, kMfx, kMfy, kMfz, kWave, kRhoBegin,
-    kRhoEnd, kSf, kRl, kUAlt, kVAlt, kWAlt, kDp0, kQ0, kSlotCount = kQ0 + 2 * kMaxScalars
+    kRhoEnd, kSf, kRl, kUAlt, kVAlt, kWAlt, kDp0, kSlowK1, kSlowStar, kSlowOut, kQv, kQc, kQr, kQv0, kU0, kV0,
+    kQrAlt, kKesslerOut, kEosCandidate,
+    kQ0, kSlotCount = kQ0 + 2 * kMaxScalars
 };
 
 }  // namespace
@@ -621,6 +625,292 @@ nimbus_status run_transport_device(nimbus_cuda_context* ctx, cudaStream_t st, co
     return NIMBUS_OK;
 }
 
+const char* check_slow(const nimbus_slow_args* a, bool step)
+{
+    if (!a->u || !a->v || !a->w || !a->p || !a->rho || !a->rho0_base) return "a required field pointer is null";
+    if (a->nx < 3 || a->ny < 3 || a->nz < 2) return "grid must be at least 3x3x2";
+    if (!cells_fit(a->nx, a->ny, a->nz)) return "grid too large for one dispatch";
+    if (a->base_len < a->nz) return "base profiles shorter than nz";
+    if (!finite_positive(a->dx) || !finite_positive(a->dy) || !finite_positive(a->dz)) return "invalid spacing";
+    if (step && !finite_positive(a->dt_large)) return "dt_large must be finite and positive";
+    if (!std::isfinite(a->gravity) || !std::isfinite(a->coriolis_f)) return "gravity and coriolis_f must be finite";
+    if (a->qv && !a->qv0_base) return "qv requires qv0_base";
+    if ((a->qc == nullptr) != (a->qr == nullptr)) return "qc and qr come together";
+    const bool outs = a->du_dt && a->dv_dt && a->dw_dt && a->dp_dt;
+    const bool none = !a->du_dt && !a->dv_dt && !a->dw_dt && !a->dp_dt;
+    if (!step && !outs) return "tendency outputs are required";
+    if (step && !outs && !none) return "tendency outputs come together";
+    return nullptr;
+}
+
+SlowParams slow_params(const nimbus_slow_args* a)
+{
+    SlowParams S{};
+    S.d = make_dims(a->nx, a->ny, a->nz);
+    S.inv_dx = 1.0 / a->dx;
+    S.inv_dy = 1.0 / a->dy;
+    S.inv_dz = 1.0 / a->dz;
+    S.dt = a->dt_large;
+    S.coriolis_f = a->coriolis_f;
+    S.frame_u = a->frame_velocity_u_ms;
+    S.frame_v = a->frame_velocity_v_ms;
+    S.gravity = a->gravity;
+    S.moist = a->qv != nullptr;
+    S.loading = a->qc != nullptr;
+    return S;
+}
+
+struct SlowDevice
+{
+    float *u, *v, *w, *p;
+    const float *rho, *qv, *qc, *qr;
+    const double *rho0, *qv0, *u0, *v0;
+    float *du, *dv, *dw, *dp;
+};
+
+template <class Policy>
+nimbus_status run_slow_device(nimbus_cuda_context* ctx, cudaStream_t st, const SlowParams& S, const SlowDevice& D,
+                              bool step)
+{
+    const size_t n = static_cast<size_t>(S.d.cells());
+    const int blocks = grid_for(ctx, static_cast<long long>(n));
+    LaunchTimer t(ctx, st, NIMBUS_KERNEL_SLOW);
+    if (!step)
+    {
+        slow_predict_kernel<Policy><<<blocks, kThreads, 0, st>>>(S, D.u, D.v, D.w, D.rho, D.p, D.qv, D.qc, D.qr, D.rho0,
+                                                                 D.qv0, D.u0, D.v0, D.du, D.dv, D.dw, D.dp, nullptr,
+                                                                 nullptr, nullptr, nullptr);
+        ctx->launches += 1;
+        NB_CUDA(ctx, cudaGetLastError());
+        return NIMBUS_OK;
+    }
+    float *k1 = nullptr, *xs = nullptr;
+    NB_TRY(ensure(ctx, kSlowK1, 4 * n, &k1));
+    NB_TRY(ensure(ctx, kSlowStar, 4 * n, &xs));
+    slow_predict_kernel<Policy><<<blocks, kThreads, 0, st>>>(S, D.u, D.v, D.w, D.rho, D.p, D.qv, D.qc, D.qr, D.rho0,
+                                                             D.qv0, D.u0, D.v0, k1, k1 + n, k1 + 2 * n, k1 + 3 * n, xs,
+                                                             xs + n, xs + 2 * n, xs + 3 * n);
+    slow_correct_kernel<Policy><<<blocks, kThreads, 0, st>>>(S, xs, xs + n, xs + 2 * n, D.rho, xs + 3 * n, D.qv, D.qc,
+                                                             D.qr, D.rho0, D.qv0, D.u0, D.v0, k1, k1 + n, k1 + 2 * n,
+                                                             k1 + 3 * n, D.u, D.v, D.w, D.p, D.du, D.dv, D.dw, D.dp);
+    ctx->launches += 2;
+    NB_CUDA(ctx, cudaGetLastError());
+    return NIMBUS_OK;
+}
+
+nimbus_status slow_entry(nimbus_cuda_context* ctx, const nimbus_slow_args* a, bool step)
+{
+    if (!ctx || !a) return NIMBUS_ERR_INVALID_ARGUMENT;
+    if (const char* why = check_slow(a, step)) return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, why);
+    if (a->memory != NIMBUS_MEMORY_HOST && a->memory != NIMBUS_MEMORY_DEVICE)
+        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "unknown memory kind");
+    NB_CUDA(ctx, cudaSetDevice(ctx->device));
+    const SlowParams S = slow_params(a);
+    const bool fp32 = ctx->precision == NIMBUS_PRECISION_FP32;
+    cudaStream_t st = ctx->stream;
+    if (a->memory == NIMBUS_MEMORY_DEVICE)
+    {
+        if (a->stream) st = static_cast<cudaStream_t>(a->stream);
+        SlowDevice D{a->u, a->v, a->w, a->p, a->rho, a->qv, a->qc, a->qr, a->rho0_base, a->qv0_base, a->u0_base,
+                     a->v0_base, a->du_dt, a->dv_dt, a->dw_dt, a->dp_dt};
+        return fp32 ? run_slow_device<Fp32Policy>(ctx, st, S, D, step) : run_slow_device<RefPolicy>(ctx, st, S, D, step);
+    }
+    const size_t n = static_cast<size_t>(a->nx) * a->ny * a->nz;
+    const size_t bytes = n * sizeof(float);
+    const size_t nzb = sizeof(double) * static_cast<size_t>(a->nz);
+    float *u, *v, *w, *p, *rho, *qv = nullptr, *qc = nullptr, *qr = nullptr, *out = nullptr;
+    double *rho0, *qv0 = nullptr, *u0 = nullptr, *v0 = nullptr;
+    NB_TRY(ensure(ctx, kU, n, &u));
+    NB_TRY(ensure(ctx, kV, n, &v));
+    NB_TRY(ensure(ctx, kW, n, &w));
+    NB_TRY(ensure(ctx, kP, n, &p));
+    NB_TRY(ensure(ctx, kRho, n, &rho));
+    NB_TRY(ensure(ctx, kRho0, static_cast<size_t>(a->nz), &rho0));
+    NB_TRY(upload(ctx, u, a->u, bytes));
+    NB_TRY(upload(ctx, v, a->v, bytes));
+    NB_TRY(upload(ctx, w, a->w, bytes));
+    NB_TRY(upload(ctx, p, a->p, bytes));
+    NB_TRY(upload(ctx, rho, a->rho, bytes));
+    NB_TRY(upload(ctx, rho0, a->rho0_base, nzb));
+    if (a->qv)
+    {
+        NB_TRY(ensure(ctx, kQv, n, &qv));
+        NB_TRY(ensure(ctx, kQv0, static_cast<size_t>(a->nz), &qv0));
+        NB_TRY(upload(ctx, qv, a->qv, bytes));
+        NB_TRY(upload(ctx, qv0, a->qv0_base, nzb));
+    }
+    if (a->qc)
+    {
+        NB_TRY(ensure(ctx, kQc, n, &qc));
+        NB_TRY(ensure(ctx, kQr, n, &qr));
+        NB_TRY(upload(ctx, qc, a->qc, bytes));
+        NB_TRY(upload(ctx, qr, a->qr, bytes));
+    }
+    if (a->u0_base)
+    {
+        NB_TRY(ensure(ctx, kU0, static_cast<size_t>(a->nz), &u0));
+        NB_TRY(upload(ctx, u0, a->u0_base, nzb));
+    }
+    if (a->v0_base)
+    {
+        NB_TRY(ensure(ctx, kV0, static_cast<size_t>(a->nz), &v0));
+        NB_TRY(upload(ctx, v0, a->v0_base, nzb));
+    }
+    const bool want_out = a->du_dt != nullptr;
+    if (want_out) NB_TRY(ensure(ctx, kSlowOut, 4 * n, &out));
+    SlowDevice D{u, v, w, p, rho, qv, qc, qr, rho0, qv0, u0, v0, out, out ? out + n : nullptr,
+                 out ? out + 2 * n : nullptr, out ? out + 3 * n : nullptr};
+    NB_TRY(fp32 ? run_slow_device<Fp32Policy>(ctx, st, S, D, step) : run_slow_device<RefPolicy>(ctx, st, S, D, step));
+    NB_CUDA(ctx, cudaStreamSynchronize(st));
+    if (step)
+    {
+        NB_TRY(download(ctx, a->u, u, bytes));
+        NB_TRY(download(ctx, a->v, v, bytes));
+        NB_TRY(download(ctx, a->w, w, bytes));
+        NB_TRY(download(ctx, a->p, p, bytes));
+    }
+    if (want_out)
+    {
+        NB_TRY(download(ctx, a->du_dt, out, bytes));
+        NB_TRY(download(ctx, a->dv_dt, out + n, bytes));
+        NB_TRY(download(ctx, a->dw_dt, out + 2 * n, bytes));
+        NB_TRY(download(ctx, a->dp_dt, out + 3 * n, bytes));
+    }
+    NB_CUDA(ctx, cudaStreamSynchronize(st));
+    return NIMBUS_OK;
+}
+
+const char* check_kessler(const nimbus_kessler_args* a, bool step)
+{
+    if (!a->theta || !a->qv || !a->qc || !a->qr || !a->p || !a->rho) return "a required field pointer is null";
+    if (a->nx < 1 || a->ny < 1 || a->nz < 1 || !cells_fit(a->nx, a->ny, a->nz)) return "invalid grid";
+    if (!finite_positive(a->dz)) return "dz must be finite and positive";
+    if (!std::isfinite(a->dt) || a->dt < 0.0) return "dt must be finite and non-negative";
+    const int* d = a->domain;
+    if (d[0] < 0 || d[1] > a->nx || d[0] >= d[1] || d[2] < 0 || d[3] > a->ny || d[2] >= d[3] || d[4] < 0 ||
+        d[5] > a->nz || d[4] >= d[5])
+        return "cell domain is empty or outside the grid";
+    const bool outs = a->dtheta_dt && a->dqv_dt && a->dqc_dt && a->dqr_dt;
+    const bool none = !a->dtheta_dt && !a->dqv_dt && !a->dqc_dt && !a->dqr_dt;
+    if (!step && !outs) return "tendency outputs are required";
+    if (step && !outs && !none) return "tendency outputs come together";
+    return nullptr;
+}
+
+KesslerParams kessler_params(const nimbus_kessler_args* a)
+{
+    KesslerParams K{};
+    K.d = make_dims(a->nx, a->ny, a->nz);
+    K.dz = a->dz;
+    K.dt = a->dt;
+    K.i0 = a->domain[0]; K.i1 = a->domain[1];
+    K.j0 = a->domain[2]; K.j1 = a->domain[3];
+    K.k0 = a->domain[4]; K.k1 = a->domain[5];
+    // KesslerScheme defaults (kessler.hpp:40-46, microphysics/config.hpp:11-18).
+    K.qc0 = 1.0e-3;
+    K.c_auto = 1.0e-3;
+    K.c_accr = 2.2;
+    K.evap_eff = 1.0;
+    K.vt_max = 20.0;
+    return K;
+}
+
+// Kessler on device memory; in the step form qr is rewritten through the
+// workspace ping-pong buffer.
+nimbus_status run_kessler_device(nimbus_cuda_context* ctx, cudaStream_t st, const KesslerParams& K, float* theta,
+                                 float* qv, float* qc, float* qr, const float* p, const float* rho, float* dth,
+                                 float* dqv, float* dqc, float* dqr, bool step)
+{
+    const size_t n = static_cast<size_t>(K.d.cells());
+    const int blocks = grid_for(ctx, static_cast<long long>(n));
+    LaunchTimer t(ctx, st, NIMBUS_KERNEL_MICROPHYSICS);
+    if (!step)
+    {
+        kessler_kernel<false><<<blocks, kThreads, 0, st>>>(K, theta, qv, qc, qr, p, rho, nullptr, dth, dqv, dqc, dqr);
+        ctx->launches += 1;
+    }
+    else
+    {
+        float* qr_new = nullptr;
+        NB_TRY(ensure(ctx, kQrAlt, n, &qr_new));
+        kessler_kernel<true><<<blocks, kThreads, 0, st>>>(K, theta, qv, qc, qr, p, rho, qr_new, dth, dqv, dqc, dqr);
+        NB_CUDA(ctx, cudaMemcpyAsync(qr, qr_new, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+        ctx->launches += 1;
+    }
+    NB_CUDA(ctx, cudaGetLastError());
+    return NIMBUS_OK;
+}
+
+nimbus_status kessler_entry(nimbus_cuda_context* ctx, const nimbus_kessler_args* a, bool step)
+{
+    if (!ctx || !a) return NIMBUS_ERR_INVALID_ARGUMENT;
+    if (const char* why = check_kessler(a, step)) return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, why);
+    if (a->memory != NIMBUS_MEMORY_HOST && a->memory != NIMBUS_MEMORY_DEVICE)
+        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "unknown memory kind");
+    NB_CUDA(ctx, cudaSetDevice(ctx->device));
+    const KesslerParams K = kessler_params(a);
+    cudaStream_t st = ctx->stream;
+    if (a->memory == NIMBUS_MEMORY_DEVICE)
+    {
+        if (a->stream) st = static_cast<cudaStream_t>(a->stream);
+        return run_kessler_device(ctx, st, K, a->theta, a->qv, a->qc, a->qr, a->p, a->rho, a->dtheta_dt, a->dqv_dt,
+                                  a->dqc_dt, a->dqr_dt, step);
+    }
+    const size_t n = static_cast<size_t>(K.d.cells());
+    const size_t bytes = n * sizeof(float);
+    float *th, *qv, *qc, *qr, *p, *rho, *out = nullptr;
+    NB_TRY(ensure(ctx, kTheta, n, &th));
+    NB_TRY(ensure(ctx, kQv, n, &qv));
+    NB_TRY(ensure(ctx, kQc, n, &qc));
+    NB_TRY(ensure(ctx, kQr, n, &qr));
+    NB_TRY(ensure(ctx, kP, n, &p));
+    NB_TRY(ensure(ctx, kRho, n, &rho));
+    NB_TRY(upload(ctx, th, a->theta, bytes));
+    NB_TRY(upload(ctx, qv, a->qv, bytes));
+    NB_TRY(upload(ctx, qc, a->qc, bytes));
+    NB_TRY(upload(ctx, qr, a->qr, bytes));
+    NB_TRY(upload(ctx, p, a->p, bytes));
+    NB_TRY(upload(ctx, rho, a->rho, bytes));
+    const bool want_out = a->dtheta_dt != nullptr;
+    if (want_out) NB_TRY(ensure(ctx, kKesslerOut, 4 * n, &out));
+    NB_TRY(run_kessler_device(ctx, st, K, th, qv, qc, qr, p, rho, out, out ? out + n : nullptr,
+                              out ? out + 2 * n : nullptr, out ? out + 3 * n : nullptr, step));
+    NB_CUDA(ctx, cudaStreamSynchronize(st));
+    if (step)
+    {
+        NB_TRY(download(ctx, a->theta, th, bytes));
+        NB_TRY(download(ctx, a->qv, qv, bytes));
+        NB_TRY(download(ctx, a->qc, qc, bytes));
+        NB_TRY(download(ctx, a->qr, qr, bytes));
+    }
+    if (want_out)
+    {
+        NB_TRY(download(ctx, a->dtheta_dt, out, bytes));
+        NB_TRY(download(ctx, a->dqv_dt, out + n, bytes));
+        NB_TRY(download(ctx, a->dqc_dt, out + 2 * n, bytes));
+        NB_TRY(download(ctx, a->dqr_dt, out + 3 * n, bytes));
+    }
+    NB_CUDA(ctx, cudaStreamSynchronize(st));
+    return NIMBUS_OK;
+}
+
+nimbus_status run_eos_device(nimbus_cuda_context* ctx, cudaStream_t st, const nimbus_eos_args* a, float* p,
+                             const float* rho, const float* theta, const float* qv, const float* qc,
+                             const float* qr)
+{
+    const Dims d = make_dims(a->nx, a->ny, a->nz);
+    const long long n = d.cells();
+    float* candidate = nullptr;
+    NB_TRY(ensure(ctx, kEosCandidate, static_cast<size_t>(n), &candidate));
+    LaunchTimer t(ctx, st, NIMBUS_KERNEL_MICROPHYSICS);
+    eos_candidate_kernel<<<grid_for(ctx, n), kThreads, 0, st>>>(d, rho, theta, p, qv, qc, qr, a->gamma, candidate,
+                                                                 ctx->status);
+    eos_publish_kernel<<<grid_for(ctx, (n + 3) / 4), kThreads, 0, st>>>(n, candidate, p, ctx->status);
+    ctx->launches += 2;
+    NB_CUDA(ctx, cudaGetLastError());
+    return NIMBUS_OK;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -680,6 +970,72 @@ nimbus_status nimbus_cuda_synchronize(nimbus_cuda_context* ctx)
     NB_TRY(read_status(ctx, ctx->stream, &flags));
     if (flags & kStatusNonfiniteMassFlux) return fail(ctx, NIMBUS_ERR_NONFINITE, "non-finite retained face mass flux");
     if (flags & kStatusNonfiniteTransport) return fail(ctx, NIMBUS_ERR_NONFINITE, "non-finite transported scalar");
+    if (flags & kStatusInvalidEos) return fail(ctx, NIMBUS_ERR_NONFINITE, "EOS projection met an invalid state");
+    return NIMBUS_OK;
+}
+
+nimbus_status nimbus_cuda_slow_tendencies(nimbus_cuda_context* ctx, const nimbus_slow_args* a)
+{
+    return slow_entry(ctx, a, false);
+}
+
+nimbus_status nimbus_cuda_slow_step(nimbus_cuda_context* ctx, const nimbus_slow_args* a)
+{
+    return slow_entry(ctx, a, true);
+}
+
+nimbus_status nimbus_cuda_kessler_tendencies(nimbus_cuda_context* ctx, const nimbus_kessler_args* a)
+{
+    return kessler_entry(ctx, a, false);
+}
+
+nimbus_status nimbus_cuda_kessler_step(nimbus_cuda_context* ctx, const nimbus_kessler_args* a)
+{
+    return kessler_entry(ctx, a, true);
+}
+
+nimbus_status nimbus_cuda_eos_projection(nimbus_cuda_context* ctx, const nimbus_eos_args* a)
+{
+    if (!ctx || !a) return NIMBUS_ERR_INVALID_ARGUMENT;
+    if (!a->p || !a->rho || !a->theta || a->nx < 1 || a->ny < 1 || a->nz < 1 ||
+        !cells_fit(a->nx, a->ny, a->nz) || !finite_positive(a->gamma))
+        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "invalid EOS projection arguments");
+    const bool moist = a->qv && a->qc && a->qr;
+    if (!moist && (a->qv || a->qc || a->qr)) return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "qv, qc, qr come together");
+    if (a->memory != NIMBUS_MEMORY_HOST && a->memory != NIMBUS_MEMORY_DEVICE)
+        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "unknown memory kind");
+    NB_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    if (a->memory == NIMBUS_MEMORY_DEVICE)
+    {
+        if (a->stream) st = static_cast<cudaStream_t>(a->stream);
+        return run_eos_device(ctx, st, a, a->p, a->rho, a->theta, a->qv, a->qc, a->qr);
+    }
+    const size_t n = static_cast<size_t>(a->nx) * a->ny * a->nz;
+    const size_t bytes = n * sizeof(float);
+    float *p, *rho, *th, *qv = nullptr, *qc = nullptr, *qr = nullptr;
+    NB_TRY(ensure(ctx, kP, n, &p));
+    NB_TRY(ensure(ctx, kRho, n, &rho));
+    NB_TRY(ensure(ctx, kTheta, n, &th));
+    NB_TRY(upload(ctx, p, a->p, bytes));
+    NB_TRY(upload(ctx, rho, a->rho, bytes));
+    NB_TRY(upload(ctx, th, a->theta, bytes));
+    if (moist)
+    {
+        NB_TRY(ensure(ctx, kQv, n, &qv));
+        NB_TRY(ensure(ctx, kQc, n, &qc));
+        NB_TRY(ensure(ctx, kQr, n, &qr));
+        NB_TRY(upload(ctx, qv, a->qv, bytes));
+        NB_TRY(upload(ctx, qc, a->qc, bytes));
+        NB_TRY(upload(ctx, qr, a->qr, bytes));
+    }
+    NB_TRY(run_eos_device(ctx, st, a, p, rho, th, qv, qc, qr));
+    unsigned flags = 0;
+    NB_TRY(read_status(ctx, st, &flags));
+    if (flags & kStatusInvalidEos)
+        return fail(ctx, NIMBUS_ERR_NONFINITE, "EOS pressure projection rejected an invalid physical state");
+    NB_TRY(download(ctx, a->p, p, bytes));
+    NB_CUDA(ctx, cudaStreamSynchronize(st));
     return NIMBUS_OK;
 }
 

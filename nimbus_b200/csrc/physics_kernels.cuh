@@ -1,0 +1,337 @@
+// Kessler warm-rain microphysics and the EOS pressure re-projection, sm_100a.
+//
+// Kessler (KesslerScheme::compute_tendencies, kessler.cpp:103-520) is one
+// thread per cell, k fastest.  The sedimentation's column coupling -- cell k
+// loses its own fall flux and gains its upper neighbour's, in that order
+// (kessler.cpp:479-518) -- is a per-cell formula, so each thread recomputes
+// the flux of cell k+1 from the original qr and densities instead of walking
+// the column: (pre_k - own_k) + recv_{k+1}, the reference's exact FP32 order.
+// The step form applies the tendencies in the same launch (theta, qv, qc in
+// place; qr to a separate buffer, because the thread below still reads the
+// original qr of this cell).
+#pragma once
+
+#include "stencil_common.cuh"
+
+namespace nimbus
+{
+
+struct KesslerParams
+{
+    Dims d;
+    double dz;
+    double dt;
+    int i0, i1, j0, j1, k0, k1;  // cell domain
+    double qc0, c_auto, c_accr, evap_eff, vt_max;
+};
+
+// Constants: microphysics_base.hpp:1073-1080, fall_speeds.hpp:60-68.
+constexpr double kKT0 = 273.15, kKLv = 2.5e6, kKCp = 1004.0, kKRv = 461.5, kKRd = 287.0, kKP0 = 100000.0;
+constexpr double kRainA = 36.34, kRainB = 0.1346, kRainMinQ = 1.0e-9, kFallRho = 1.2;
+
+__device__ __forceinline__ double kclamp(double v, double lo, double hi) { return v < lo ? lo : (hi < v ? hi : v); }
+__device__ __forceinline__ double kmax(double a, double b) { return a < b ? b : a; }
+__device__ __forceinline__ double kmin(double a, double b) { return b < a ? b : a; }
+
+__device__ __forceinline__ double k_theta_to_temperature(double theta, double p)
+{
+    if (!isfinite(theta) || !isfinite(p)) return kKT0;
+    const double th = kclamp(theta, 150.0, 700.0), ps = kclamp(p, 100.0, 200000.0);
+    const double T = th * pow(ps / kKP0, kKRd / kKCp);
+    return isfinite(T) ? T : kKT0;
+}
+
+__device__ __forceinline__ double k_qvs_water(double T, double p)
+{
+    double e = 0.0;
+    if (isfinite(T))
+    {
+        const double tc = kclamp(T, 150.0, 400.0) - kKT0;
+        const double value = 611.21 * exp((18.678 - tc / 234.5) * tc / (257.14 + tc));
+        e = isfinite(value) ? kmax(0.0, value) : 0.0;
+    }
+    if (!isfinite(e) || !isfinite(p)) return 0.0;
+    const double ps = kclamp(p, 100.0, 200000.0);
+    return kclamp(0.62198 * e / kmax(ps - e, 1.0), 0.0, 0.2);
+}
+
+__device__ __forceinline__ double k_sat_slope(double temperature, double saturation, double p)
+{
+    if (!(temperature > 150.0 && temperature < 400.0) || !(saturation > 0.0 && saturation < 0.2)) return 0.0;
+    const double pressure = kclamp(p, 100.0, 200000.0);
+    const double vapor = saturation * pressure / (0.62198 + saturation);
+    const double tc = temperature - kKT0;
+    const double den = 257.14 + tc;
+    const double num = (18.678 - tc / 234.5) * tc;
+    const double num_slope = 18.678 - 2.0 * tc / 234.5;
+    const double lps = (num_slope * den - num) / (den * den);
+    return saturation * pressure / kmax(pressure - vapor, 1.0) * lps;
+}
+
+// Coupled saturation adjustment (thermodynamics.hpp:282-466).
+__device__ double k_saturation_adjustment(double T_in, double p, double& qv, double& qc)
+{
+    double T = isfinite(T_in) ? kclamp(T_in, 150.0, 400.0) : kKT0;
+    qv = isfinite(qv) ? kmax(0.0, qv) : 0.0;
+    qc = isfinite(qc) ? kmax(0.0, qc) : 0.0;
+    double qvs = k_qvs_water(T, p);
+    if (!isfinite(qvs) || qvs < 0.0) qvs = 0.0;
+    const double L = kKLv / kKCp;
+    const double eps8 = 8.0 * 2.220446049250313e-16;
+    if (qv > qvs)
+    {
+        const double maximum = kmin(qv, kmax(0.0, (400.0 - T) / L));
+        double condensed = maximum;
+        if (qv - maximum - k_qvs_water(T + L * maximum, p) <= 0.0)
+        {
+            double lower = 0.0, upper = maximum;
+            condensed = kclamp((qv - qvs) / (1.0 + L * k_sat_slope(T, qvs, p)), lower, upper);
+            for (int it = 0; it < 10; ++it)
+            {
+                const double ta = T + L * condensed;
+                const double sa = k_qvs_water(ta, p);
+                const double value = qv - condensed - sa;
+                if (fabs(value) <= eps8 * kmax(kmax(1.0, fabs(qv)), fabs(sa))) break;
+                if (value > 0.0) lower = condensed;
+                else upper = condensed;
+                const double derivative = -1.0 - L * k_sat_slope(ta, sa, p);
+                const double candidate = condensed - value / derivative;
+                condensed = (candidate > lower && candidate < upper) ? candidate : 0.5 * (lower + upper);
+            }
+        }
+        qv -= condensed;
+        qc += condensed;
+        T += L * condensed;
+    }
+    else if (qv < qvs && qc > 0.0)
+    {
+        const double maximum = kmin(qc, kmax(0.0, (T - 150.0) / L));
+        double evaporated = maximum;
+        if (qv + maximum - k_qvs_water(T - L * maximum, p) >= 0.0)
+        {
+            double lower = 0.0, upper = maximum;
+            evaporated = kclamp((qvs - qv) / (1.0 + L * k_sat_slope(T, qvs, p)), lower, upper);
+            for (int it = 0; it < 10; ++it)
+            {
+                const double ta = T - L * evaporated;
+                const double sa = k_qvs_water(ta, p);
+                const double value = qv + evaporated - sa;
+                if (fabs(value) <= eps8 * kmax(kmax(1.0, fabs(qv)), fabs(sa))) break;
+                if (value < 0.0) lower = evaporated;
+                else upper = evaporated;
+                const double derivative = 1.0 + L * k_sat_slope(ta, sa, p);
+                const double candidate = evaporated - value / derivative;
+                evaporated = (candidate > lower && candidate < upper) ? candidate : 0.5 * (lower + upper);
+            }
+        }
+        qc -= evaporated;
+        qv += evaporated;
+        T -= L * evaporated;
+    }
+    qc = kmax(0.0, qc);
+    qv = kmax(0.0, qv);
+    return T;
+}
+
+// Rain fall flux Vt*qr of one cell, rounded to FP32 as the reference stores it.
+__device__ __forceinline__ float k_sed_flux(const KesslerParams& K, double qr_raw, double rho_k)
+{
+    const double q = kmax(0.0, qr_raw);
+    if (!(q > 0.0)) return 0.0f;
+    const double fall = sqrt(kFallRho / rho_k);
+    const double vt0 = (q < kRainMinQ) ? 0.0 : kRainA * pow(1.0e-3 * rho_k * q, kRainB);
+    const double vt = kmin(vt0 * fall, K.vt_max);
+    return (float)(vt * q);
+}
+
+template <bool kApply>
+__global__ void __launch_bounds__(256) kessler_kernel(KesslerParams K, float* __restrict__ theta, float* __restrict__ qv,
+                                                      float* __restrict__ qc, const float* __restrict__ qr,
+                                                      const float* __restrict__ p, const float* __restrict__ rho,
+                                                      float* __restrict__ qr_out, float* __restrict__ dth_out,
+                                                      float* __restrict__ dqv_out, float* __restrict__ dqc_out,
+                                                      float* __restrict__ dqr_out)
+{
+    const Dims d = K.d;
+    const int n = d.cells();
+    const double dt = K.dt;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+    {
+        int i, j, k;
+        decompose(d, c, i, j, k);
+        const bool inside = i >= K.i0 && i < K.i1 && j >= K.j0 && j < K.j1 && k >= K.k0 && k < K.k1;
+        float dth = 0.0f, dqv = 0.0f, dqc = 0.0f, dqr = 0.0f;
+        const float qr_c = qr[c];
+        if (inside && dt > 0.0)
+        {
+            const float p_c = p[c];
+            const float qv_c = qv[c], qc_c = qc[c];
+            // Saturation adjustment.
+            const float tv = (float)k_theta_to_temperature((double)theta[c], (double)p_c);
+            double qvd = (double)qv_c, qcd = (double)qc_c;
+            const float temp = (float)k_saturation_adjustment((double)tv, (double)p_c, qvd, qcd);
+            const float qv_adj = (float)qvd, qc_adj = (float)qcd;
+            const double dqa = (double)qc_adj - (double)qc_c;
+            if (dqa != 0.0)
+            {
+                const double rate = dqa * (1.0 / dt);
+                dqc = __fadd_rn(dqc, (float)rate);
+                dqv = __fsub_rn(dqv, (float)rate);
+                dth = __fadd_rn(dth, (float)(kKLv / kKCp * rate));
+            }
+            // Autoconversion + accretion, then rain evaporation.
+            float prod = 0.0f;
+            if (qc_adj > 0.0f)
+            {
+                const double factor =
+                    1.0 / (1.0 + K.c_accr * dt * pow((double)(0.0f < qr_c ? qr_c : 0.0f), 0.875));
+                const double amount =
+                    (double)qc_adj * (1.0 - factor) + factor * K.c_auto * dt * kmax((double)qc_adj - K.qc0, 0.0);
+                prod = (float)(kclamp(amount, 0.0, (double)qc_adj) / dt);
+                dqc = __fsub_rn(dqc, prod);
+                dqr = __fadd_rn(dqr, prod);
+            }
+            if (qr_c > 0.0f || prod > 0.0f)
+            {
+                const double pv = (double)p_c, rv = (double)rho[c];
+                const double qvsat = k_qvs_water((double)temp, pv);
+                if (qvsat > 0.0 && (double)qv_adj < qvsat && rv > 0.0 && pv > 0.0)
+                {
+                    const double qr_av = (double)qr_c + (double)prod * dt;
+                    const double rcgs = 1.0e-3 * rv;
+                    const double rain = rcgs * kmax(qr_av, 0.0);
+                    const double vent = (1.6 + 124.9 * pow(rain, 0.2046)) * pow(rain, 0.525);
+                    const double resist = 2.55e8 / (pv * qvsat) + 5.4e5;
+                    const double raw = K.evap_eff * (vent / resist) * ((qvsat - (double)qv_adj) / (rcgs * qvsat));
+                    const double gsat =
+                        (kKLv * kKLv * qvsat) / (kKCp * kKRv * kmax((double)temp * (double)temp, 1.0));
+                    const double bound = (qvsat - (double)qv_adj) / (1.0 + gsat);
+                    const double evap = kclamp(raw, 0.0, kmin(bound / dt, qr_av / dt));
+                    // Field3D's element proxy rounds the double operand to float first.
+                    dqv = __fadd_rn(dqv, (float)evap);
+                    dqr = __fsub_rn(dqr, (float)evap);
+                    dth = __fsub_rn(dth, (float)(kKLv / kKCp * evap));
+                }
+            }
+            // Sedimentation: lose the own fall flux, then gain the upper neighbour's.
+            const double rho_k = (double)rho[c];
+            if (kmax(0.0, (double)qr_c) > 0.0)
+                dqr = __fsub_rn(dqr, (float)((double)k_sed_flux(K, (double)qr_c, rho_k) / K.dz));
+            if (k + 1 < K.k1)
+            {
+                const double qr_up = (double)qr[c + 1];
+                if (kmax(0.0, qr_up) > 0.0)
+                {
+                    const double rho_up = (double)rho[c + 1];
+                    const float up = k_sed_flux(K, qr_up, rho_up);
+                    const double recv = rho_up / rho_k;
+                    dqr = __fadd_rn(dqr, (float)(recv * (double)up / K.dz));
+                }
+            }
+            // Temperature tendency to theta tendency.
+            {
+                const double dT = (double)dth, pv = (double)p_c;
+                double r = 0.0;
+                if (isfinite(dT) && isfinite(pv))
+                {
+                    const double ps = kclamp(pv, 100.0, 200000.0);
+                    r = dT * pow(kKP0 / ps, kKRd / kKCp);
+                    if (!isfinite(r)) r = 0.0;
+                }
+                dth = (float)r;
+            }
+        }
+        if (dth_out != nullptr)
+        {
+            dth_out[c] = dth;
+            dqv_out[c] = dqv;
+            dqc_out[c] = dqc;
+            dqr_out[c] = dqr;
+        }
+        if (kApply)
+        {
+            float qr_new = qr_c;
+            if (inside)
+            {
+                auto water = [&](float q, float dq) {
+                    const float raw = (float)((double)q + (double)dq * dt);
+                    return !isfinite(raw) ? 0.0f : (raw < 0.0f ? 0.0f : (0.05f < raw ? 0.05f : raw));
+                };
+                qv[c] = water(qv[c], dqv);
+                qc[c] = water(qc[c], dqc);
+                qr_new = water(qr_c, dqr);
+                theta[c] = (float)((double)theta[c] + (double)dth * dt);
+            }
+            qr_out[c] = qr_new;
+        }
+    }
+}
+
+// EOS pressure re-projection (eos_apply.cpp:50-175, pressure_fp64 in
+// eos_pressure.hpp:30-38): candidate p = clamp(float(p00 (rho R_d theta /
+// p00)^gamma)) for every cell.  With qv/qc/qr given, the cells of the
+// attributed domain (physical_scalar_domain: the one-cell lateral ring dropped
+// where the extent is >= 3, every level) are also checked as the energy
+// attribution checks them (eos_apply.cpp:139-158): old p finite and positive,
+// qv finite and non-negative, qc + qr (FP64) finite and non-negative.  Any
+// failure sets the status bit; eos_publish_kernel then leaves p untouched.
+__global__ void __launch_bounds__(256) eos_candidate_kernel(Dims d, const float* __restrict__ rho,
+                                                            const float* __restrict__ theta,
+                                                            const float* __restrict__ p_old,
+                                                            const float* __restrict__ qv, const float* __restrict__ qc,
+                                                            const float* __restrict__ qr, double gamma,
+                                                            float* __restrict__ p_candidate,
+                                                            unsigned* __restrict__ status)
+{
+    const int n = (int)d.cells();
+    const int ih = d.nx >= 3, jh = d.ny >= 3;
+    unsigned flags = 0;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+    {
+        const float r = rho[c], th = theta[c];
+        const double diagnosed = kP00 * pow((double)r * kRd * (double)th / kP00, gamma);
+        if (!isfinite(r) || !(r > 0.0f) || !isfinite(th) || !(th > 0.0f) || !isfinite(diagnosed) ||
+            diagnosed <= 0.0 || !isfinite((float)diagnosed))
+        {
+            flags |= kStatusInvalidEos;
+            continue;
+        }
+        p_candidate[c] = clamp_value((float)diagnosed, 101325.0f, 1000.0f, 200000.0f);
+        if (qv)
+        {
+            int i, j, k;
+            decompose(d, c, i, j, k);
+            if (i >= ih && i < d.nx - ih && j >= jh && j < d.ny - jh)
+            {
+                const float po = p_old[c], q = qv[c];
+                const double liquid = (double)qc[c] + (double)qr[c];
+                if (!isfinite(po) || po <= 0.0f || !isfinite(q) || q < 0.0f || !isfinite(liquid) || liquid < 0.0)
+                    flags |= kStatusInvalidEos;
+            }
+        }
+    }
+    if (flags) atomicOr(status, flags);
+}
+
+// Publishes the candidate pressure unless the projection was refused.
+__global__ void __launch_bounds__(256) eos_publish_kernel(long long n, const float* __restrict__ p_candidate,
+                                                          float* __restrict__ p, const unsigned* __restrict__ status)
+{
+    if (*status & kStatusInvalidEos) return;
+    const long long n4 = n / 4;
+    const float4* src = reinterpret_cast<const float4*>(p_candidate);
+    float4* dst = reinterpret_cast<float4*>(p);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if ((reinterpret_cast<uintptr_t>(p) & 15) == 0)
+    {
+        for (long long c = t; c < n4; c += stride) dst[c] = src[c];
+        for (long long c = 4 * n4 + t; c < n; c += stride) p[c] = p_candidate[c];
+    }
+    else
+    {
+        for (long long c = t; c < n; c += stride) p[c] = p_candidate[c];
+    }
+}
+
+}  // namespace nimbus

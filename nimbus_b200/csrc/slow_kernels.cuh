@@ -1,0 +1,224 @@
+// Slow (advective) tendencies of the flat C-grid KW scheme and the Heun slow
+// step, sm_100a.
+//
+// One slow step is two launches:
+//   slow_predict : k1 = L(u^n); writes k1 and the predictor state
+//                  x* = x^n + dt*k1 (u, v, w, p)            [prepare_slow_rk2_tendencies]
+//   slow_correct : k2 = L(x*); t = 0.5f*(k2 + k1) in FP32 as the reference
+//                  averages; x^n += dt*t                      [apply_slow_tendencies]
+// L is CartesianCGrid3DScheme::compute_slow_tendencies
+// (cartesian_cgrid_3d.cpp:1026-1401): fd5/fd3/fd1 upwind-biased momentum
+// advection (derivative_operators.hpp:324-395), f-plane Coriolis on the
+// perturbation wind, buoyancy -g(rho-rho0)/rho with vapour and hydrometeor
+// loading on w, and centred -u.grad p for p.
+#pragma once
+
+#include "acoustic_fused.cuh"
+
+namespace nimbus
+{
+
+struct SlowParams
+{
+    Dims d;
+    double inv_dx, inv_dy, inv_dz;
+    double dt;
+    double coriolis_f;
+    double frame_u, frame_v;
+    double gravity;
+    int moist;    // qv and qv0 present
+    int loading;  // qc, qr present
+};
+
+template <class real>
+__device__ __forceinline__ real upwind_deriv(const float* __restrict__ f, int c, int stride, int idx, int n, real a,
+                                             real inv_d)
+{
+    const int half = min(idx, n - 1 - idx);
+    const real cc = (real)f[c];
+    if (half <= 0) return (real)0;
+    const real m1 = (real)f[c - stride], p1 = (real)f[c + stride];
+    if (half == 1) return (a >= (real)0) ? (cc - m1) * inv_d : (p1 - cc) * inv_d;
+    const real m2 = (real)f[c - 2 * stride], p2 = (real)f[c + 2 * stride];
+    if (half == 2)
+        return (a >= (real)0) ? ((real)2 * p1 + (real)3 * cc - (real)6 * m1 + m2) * (inv_d / (real)6)
+                              : (-p2 + (real)6 * p1 - (real)3 * cc - (real)2 * m1) * (inv_d / (real)6);
+    const real m3 = (real)f[c - 3 * stride], p3 = (real)f[c + 3 * stride];
+    return (a >= (real)0)
+               ? ((real)-2 * m3 + (real)15 * m2 - (real)60 * m1 + (real)20 * cc + (real)30 * p1 - (real)3 * p2) *
+                     (inv_d / (real)60)
+               : ((real)2 * p3 - (real)15 * p2 + (real)60 * p1 - (real)20 * cc - (real)30 * m1 + (real)3 * m2) *
+                     (inv_d / (real)60);
+}
+
+// The four slow tendencies of cell c (zero outside their index ranges).
+template <class Policy>
+__device__ __forceinline__ void slow_tendencies_at(const SlowParams& S, int c, int i, int j, int k,
+                                                   const float* __restrict__ u, const float* __restrict__ v,
+                                                   const float* __restrict__ w, const float* __restrict__ rho,
+                                                   const float* __restrict__ p, const float* __restrict__ qv,
+                                                   const float* __restrict__ qc, const float* __restrict__ qr,
+                                                   const double* __restrict__ rho0, const double* __restrict__ qv0,
+                                                   const double* __restrict__ u0, const double* __restrict__ v0,
+                                                   float& out_u, float& out_v, float& out_w, float& out_p)
+{
+    using real = typename Policy::real;
+    const Dims d = S.d;
+    out_u = out_v = out_w = out_p = 0.0f;
+    if (!(i >= 1 && i < d.nx - 1 && j >= 1 && j < d.ny - 1 && k < d.nz - 1)) return;
+    const int sx = d.sx(), sy = d.sy();
+    const real q = (real)0.25, h = (real)0.5;
+    const real inv_dx = (real)S.inv_dx, inv_dy = (real)S.inv_dy, inv_dz = (real)S.inv_dz;
+    const real fu = (real)S.frame_u, fv = (real)S.frame_v, cf = (real)S.coriolis_f;
+    // du at the x-face
+    {
+        const real ux = (real)u[c];
+        const real uy = q * ((real)v[c - sy] + (real)v[c] + (real)v[c + sx - sy] + (real)v[c + sx]);
+        const real tux = ux - fu, tuy = uy - fv;
+        const real wx = (k == 0) ? q * ((real)w[c] + (real)w[c + sx])
+                                 : q * ((real)w[c - 1] + (real)w[c] + (real)w[c + sx - 1] + (real)w[c + sx]);
+        const real ddx = upwind_deriv<real>(u, c, sx, i, d.nx, tux, inv_dx);
+        const real ddy = upwind_deriv<real>(u, c, sy, j, d.ny, tuy, inv_dy);
+        const real ddz = (k == 0) ? ((wx >= (real)0) ? (real)0 : ((real)u[c + 1] - (real)u[c]) * inv_dz)
+                                  : upwind_deriv<real>(u, c, 1, k, d.nz, wx, inv_dz);
+        const real v0k = v0 ? (real)v0[k] : (real)0;
+        const real du = -tux * ddx - tuy * ddy - wx * ddz + cf * (uy - v0k);
+        out_u = (float)finite_or_zero((double)du);
+    }
+    // dv at the y-face
+    {
+        const real vy = (real)v[c];
+        const real ux = q * ((real)u[c - sx] + (real)u[c] + (real)u[c - sx + sy] + (real)u[c + sy]);
+        const real tvy = vy - fv, tux = ux - fu;
+        const real wy = (k == 0) ? q * ((real)w[c] + (real)w[c + sy])
+                                 : q * ((real)w[c - 1] + (real)w[c] + (real)w[c + sy - 1] + (real)w[c + sy]);
+        const real ddx = upwind_deriv<real>(v, c, sx, i, d.nx, tux, inv_dx);
+        const real ddy = upwind_deriv<real>(v, c, sy, j, d.ny, tvy, inv_dy);
+        const real ddz = (k == 0) ? ((wy >= (real)0) ? (real)0 : ((real)v[c + 1] - (real)v[c]) * inv_dz)
+                                  : upwind_deriv<real>(v, c, 1, k, d.nz, wy, inv_dz);
+        const real u0k = u0 ? (real)u0[k] : (real)0;
+        const real dv = -tux * ddx - tvy * ddy - wy * ddz - cf * (ux - u0k);
+        out_v = (float)finite_or_zero((double)dv);
+    }
+    // dw at the z-face
+    {
+        const real wz = (real)w[c];
+        const real ux = q * ((real)u[c - sx] + (real)u[c] + (real)u[c - sx + 1] + (real)u[c + 1]);
+        const real uy = q * ((real)v[c - sy] + (real)v[c] + (real)v[c - sy + 1] + (real)v[c + 1]);
+        const real tux = ux - fu, tuy = uy - fv;
+        const real ddx = upwind_deriv<real>(w, c, sx, i, d.nx, tux, inv_dx);
+        const real ddy = upwind_deriv<real>(w, c, sy, j, d.ny, tuy, inv_dy);
+        const real ddz = (k == 0) ? ((wz >= (real)0) ? ((real)w[c] - (real)0) * inv_dz : ((real)w[c + 1] - (real)w[c]) * inv_dz)
+                                  : upwind_deriv<real>(w, c, 1, k, d.nz, wz, inv_dz);
+        const double rho_face = 0.5 * ((double)rho[c] + (double)rho[c + 1]);
+        const double rho_s = safe_rho(rho_face);
+        const double rho0_face = 0.5 * (rho0[k] + rho0[k + 1]);
+        const double g = S.gravity;
+        const double buoy = -g * (rho_face - rho0_face) / rho_s;
+        double moist = 0.0;
+        if (S.moist)
+        {
+            const double qf = 0.5 * ((double)qv[c] + (double)qv[c + 1]);
+            const double q0f = 0.5 * ((double)(float)qv0[k] + (double)(float)qv0[k + 1]);
+            moist = g * 0.608 * (qf - q0f);
+        }
+        double load = 0.0;
+        if (S.loading)
+        {
+            const double lo = (double)qc[c] + (double)qr[c] + 0.0 + 0.0 + 0.0 + 0.0;
+            const double hi = (double)qc[c + 1] + (double)qr[c + 1] + 0.0 + 0.0 + 0.0 + 0.0;
+            load = -g * (0.5 * (lo + hi));
+        }
+        const real dw = -tux * ddx - tuy * ddy - wz * ddz + (real)buoy + (real)moist + (real)load;
+        out_w = (float)finite_or_zero((double)dw);
+    }
+    // dp at the centre
+    if (k >= 1)
+    {
+        const real uc = h * ((real)u[c] + (real)u[c - sx]);
+        const real vc = h * ((real)v[c] + (real)v[c - sy]);
+        const real tuc = uc - fu, tvc = vc - fv;
+        const real wc = h * ((real)w[c] + (real)w[c - 1]);
+        const real dpdx = ((real)p[c + sx] - (real)p[c - sx]) * (real)(0.5 * S.inv_dx);
+        const real dpdy = ((real)p[c + sy] - (real)p[c - sy]) * (real)(0.5 * S.inv_dy);
+        const real dpdz = ((real)p[c + 1] - (real)p[c - 1]) * (real)(0.5 * S.inv_dz);
+        out_p = (float)finite_or_zero((double)(-tuc * dpdx - tvc * dpdy - wc * dpdz));
+    }
+}
+
+__device__ __forceinline__ float slow_apply_one(float x, float t, double dt)
+{
+    return (float)((double)x + finite_or_zero((double)t) * dt);
+}
+
+// k1 and the predictor state; also the plain tendency evaluation (xs == null).
+template <class Policy>
+__global__ void __launch_bounds__(256) slow_predict_kernel(
+    SlowParams S, const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w,
+    const float* __restrict__ rho, const float* __restrict__ p, const float* __restrict__ qv,
+    const float* __restrict__ qc, const float* __restrict__ qr, const double* __restrict__ rho0,
+    const double* __restrict__ qv0, const double* __restrict__ u0, const double* __restrict__ v0,
+    float* __restrict__ k1u, float* __restrict__ k1v, float* __restrict__ k1w, float* __restrict__ k1p,
+    float* __restrict__ su, float* __restrict__ sv, float* __restrict__ sw, float* __restrict__ sp)
+{
+    const Dims d = S.d;
+    const int n = d.cells();
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+    {
+        int i, j, k;
+        decompose(d, c, i, j, k);
+        float tu, tv, tw, tp;
+        slow_tendencies_at<Policy>(S, c, i, j, k, u, v, w, rho, p, qv, qc, qr, rho0, qv0, u0, v0, tu, tv, tw, tp);
+        k1u[c] = tu;
+        k1v[c] = tv;
+        k1w[c] = tw;
+        k1p[c] = tp;
+        if (su != nullptr)
+        {
+            su[c] = slow_apply_one(u[c], tu, S.dt);
+            sv[c] = slow_apply_one(v[c], tv, S.dt);
+            sw[c] = slow_apply_one(w[c], tw, S.dt);
+            sp[c] = slow_apply_one(p[c], tp, S.dt);
+        }
+    }
+}
+
+// k2 at the predictor state, the FP32 Heun average, and the apply in place.
+template <class Policy>
+__global__ void __launch_bounds__(256) slow_correct_kernel(
+    SlowParams S, const float* __restrict__ su, const float* __restrict__ sv, const float* __restrict__ sw,
+    const float* __restrict__ rho, const float* __restrict__ sp, const float* __restrict__ qv,
+    const float* __restrict__ qc, const float* __restrict__ qr, const double* __restrict__ rho0,
+    const double* __restrict__ qv0, const double* __restrict__ u0, const double* __restrict__ v0,
+    const float* __restrict__ k1u, const float* __restrict__ k1v, const float* __restrict__ k1w,
+    const float* __restrict__ k1p, float* __restrict__ u, float* __restrict__ v, float* __restrict__ w,
+    float* __restrict__ p, float* __restrict__ tu_out, float* __restrict__ tv_out, float* __restrict__ tw_out,
+    float* __restrict__ tp_out)
+{
+    const Dims d = S.d;
+    const int n = d.cells();
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+    {
+        int i, j, k;
+        decompose(d, c, i, j, k);
+        float tu, tv, tw, tp;
+        slow_tendencies_at<Policy>(S, c, i, j, k, su, sv, sw, rho, sp, qv, qc, qr, rho0, qv0, u0, v0, tu, tv, tw, tp);
+        tu = __fmul_rn(0.5f, __fadd_rn(tu, k1u[c]));
+        tv = __fmul_rn(0.5f, __fadd_rn(tv, k1v[c]));
+        tw = __fmul_rn(0.5f, __fadd_rn(tw, k1w[c]));
+        tp = __fmul_rn(0.5f, __fadd_rn(tp, k1p[c]));
+        if (tu_out != nullptr)
+        {
+            tu_out[c] = tu;
+            tv_out[c] = tv;
+            tw_out[c] = tw;
+            tp_out[c] = tp;
+        }
+        u[c] = slow_apply_one(u[c], tu, S.dt);
+        v[c] = slow_apply_one(v[c], tv, S.dt);
+        w[c] = slow_apply_one(w[c], tw, S.dt);
+        p[c] = slow_apply_one(p[c], tp, S.dt);
+    }
+}
+
+}  // namespace nimbus

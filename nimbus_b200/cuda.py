@@ -87,6 +87,37 @@ class ScalarTransportArgs(ctypes.Structure):
     ]
 
 
+class SlowArgs(ctypes.Structure):
+    _fields_ = [
+        ("u", _fp), ("v", _fp), ("w", _fp), ("p", _fp), ("rho", _fp), ("qv", _fp), ("qc", _fp), ("qr", _fp),
+        ("rho0_base", _dp), ("qv0_base", _dp), ("u0_base", _dp), ("v0_base", _dp), ("base_len", ctypes.c_int),
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("dz", ctypes.c_double), ("dt_large", ctypes.c_double),
+        ("gravity", ctypes.c_double), ("coriolis_f", ctypes.c_double),
+        ("frame_velocity_u_ms", ctypes.c_float), ("frame_velocity_v_ms", ctypes.c_float),
+        ("du_dt", _fp), ("dv_dt", _fp), ("dw_dt", _fp), ("dp_dt", _fp),
+        ("memory", ctypes.c_int), ("stream", ctypes.c_void_p),
+    ]
+
+
+class KesslerArgs(ctypes.Structure):
+    _fields_ = [
+        ("theta", _fp), ("qv", _fp), ("qc", _fp), ("qr", _fp), ("p", _fp), ("rho", _fp),
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("dz", ctypes.c_double), ("dt", ctypes.c_double), ("domain", ctypes.c_int * 6),
+        ("dtheta_dt", _fp), ("dqv_dt", _fp), ("dqc_dt", _fp), ("dqr_dt", _fp),
+        ("memory", ctypes.c_int), ("stream", ctypes.c_void_p),
+    ]
+
+
+class EosArgs(ctypes.Structure):
+    _fields_ = [
+        ("p", _fp), ("rho", _fp), ("theta", _fp), ("qv", _fp), ("qc", _fp), ("qr", _fp),
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("gamma", ctypes.c_double),
+        ("memory", ctypes.c_int), ("stream", ctypes.c_void_p),
+    ]
+
+
 EXPORTED_SYMBOLS = (
     "nimbus_cuda_abi_version", "nimbus_cuda_create", "nimbus_cuda_destroy", "nimbus_cuda_last_error",
     "nimbus_cuda_kernel_launches", "nimbus_cuda_stream", "nimbus_cuda_synchronize",
@@ -94,12 +125,14 @@ EXPORTED_SYMBOLS = (
     "nimbus_cuda_set_kernel_timing", "nimbus_cuda_kernel_timing",
     "nimbus_cuda_acoustic_fused_static_scratch", "nimbus_cuda_set_precision",
     "nimbus_cuda_set_substep_form", "nimbus_cuda_autotune_substep",
+    "nimbus_cuda_slow_tendencies", "nimbus_cuda_slow_step",
+    "nimbus_cuda_kessler_tendencies", "nimbus_cuda_kessler_step", "nimbus_cuda_eos_projection",
 )
 SUBSTEP_AUTO, SUBSTEP_FUSED, SUBSTEP_SPLIT = 0, 1, 2
 PRECISION_REFERENCE, PRECISION_FP32 = 0, 1
 STATIC_SCRATCH_CELLS = 4194304  # NIMBUS_STATIC_SCRATCH_CELLS
 KERNEL_FAMILIES = ("acoustic_substep", "acoustic_momentum", "acoustic_boundary", "transport_faces",
-                   "transport_limiter", "transport_update")
+                   "transport_limiter", "transport_update", "slow", "microphysics")
 
 
 def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
@@ -124,6 +157,11 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
     lib.nimbus_cuda_autotune_substep.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                  ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
     lib.nimbus_cuda_acoustic_fused_static_scratch.argtypes = [ctypes.POINTER(AcousticFusedArgs)]
+    lib.nimbus_cuda_slow_tendencies.argtypes = [ctypes.c_void_p, ctypes.POINTER(SlowArgs)]
+    lib.nimbus_cuda_slow_step.argtypes = [ctypes.c_void_p, ctypes.POINTER(SlowArgs)]
+    lib.nimbus_cuda_kessler_tendencies.argtypes = [ctypes.c_void_p, ctypes.POINTER(KesslerArgs)]
+    lib.nimbus_cuda_kessler_step.argtypes = [ctypes.c_void_p, ctypes.POINTER(KesslerArgs)]
+    lib.nimbus_cuda_eos_projection.argtypes = [ctypes.c_void_p, ctypes.POINTER(EosArgs)]
     lib.nimbus_cuda_set_kernel_timing.argtypes = [ctypes.c_void_p, ctypes.c_int]
     lib.nimbus_cuda_kernel_timing.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64),
                                               ctypes.POINTER(ctypes.c_double)]
@@ -237,6 +275,21 @@ class Context:
     def scalar_transport(self, args: ScalarTransportArgs) -> int:
         return self.lib.nimbus_cuda_scalar_transport(self.handle, ctypes.byref(args))
 
+    def slow_tendencies(self, args: SlowArgs) -> int:
+        return self.lib.nimbus_cuda_slow_tendencies(self.handle, ctypes.byref(args))
+
+    def slow_step(self, args: SlowArgs) -> int:
+        return self.lib.nimbus_cuda_slow_step(self.handle, ctypes.byref(args))
+
+    def kessler_tendencies(self, args: KesslerArgs) -> int:
+        return self.lib.nimbus_cuda_kessler_tendencies(self.handle, ctypes.byref(args))
+
+    def kessler_step(self, args: KesslerArgs) -> int:
+        return self.lib.nimbus_cuda_kessler_step(self.handle, ctypes.byref(args))
+
+    def eos_projection(self, args: EosArgs) -> int:
+        return self.lib.nimbus_cuda_eos_projection(self.handle, ctypes.byref(args))
+
 
 def clamp_defaults() -> dict:
     """The reference's dispatch constants (dynamics.cpp:4560-4586, field_bounds.hpp)."""
@@ -309,6 +362,72 @@ def transport_args(q_in: Sequence, q_out: Sequence, pd: Sequence[int], rho_end, 
     a.weno = int(weno)
     a.top_open = int(top_open)
     a.rho_floor = initial.RHO_MIN
+    a.memory = memory
+    a.stream = stream
+    return a
+
+
+def slow_args(st, base, grid, dt_large=0.0, coriolis_f=0.0, moist=True, outputs=None, frame=(0.0, 0.0),
+              memory=MEMORY_HOST, stream=None) -> SlowArgs:
+    """Argument block for nimbus_cuda_slow_tendencies / nimbus_cuda_slow_step.
+    `outputs` is (du, dv, dw, dp) or None."""
+    nx, ny, nz = st["u"].shape
+    a = SlowArgs()
+    qv = st.get("qv") if moist else None
+    qc = st.get("qc") if moist else None
+    qr = st.get("qr") if moist else None
+    outs = outputs or (None, None, None, None)
+    a._keep = (dict(st), base["rho0"], base.get("qv0"), base.get("u0"), base.get("v0"), outs)
+    a.u, a.v, a.w, a.p, a.rho = (_f(st[k]) for k in ("u", "v", "w", "p", "rho"))
+    a.qv, a.qc, a.qr = _f(qv), _f(qc), _f(qr)
+    a.rho0_base = _d(base["rho0"])
+    a.qv0_base = _d(base["qv0"]) if moist else None
+    a.u0_base, a.v0_base = _d(base["u0"]), _d(base["v0"])
+    a.base_len = nz
+    a.nx, a.ny, a.nz = nx, ny, nz
+    a.dx, a.dy, a.dz = grid
+    a.dt_large = dt_large
+    a.gravity = initial.G
+    a.coriolis_f = coriolis_f
+    a.frame_velocity_u_ms, a.frame_velocity_v_ms = frame
+    a.du_dt, a.dv_dt, a.dw_dt, a.dp_dt = (_f(o) for o in outs)
+    a.memory = memory
+    a.stream = stream
+    return a
+
+
+def cgrid_cell_domain(nx: int, ny: int, nz: int) -> tuple:
+    """Physical cell domain of the C-grid microphysics step: the lateral
+    ghost ring is excluded, every level is kept (microphysics_step.cpp:86-96)."""
+    return (1, nx - 1, 1, ny - 1, 0, nz)
+
+
+def kessler_args(st, dz, dt, domain=None, outputs=None, memory=MEMORY_HOST, stream=None) -> KesslerArgs:
+    """Argument block for nimbus_cuda_kessler_tendencies / _step.  `st` holds
+    theta, qv, qc, qr, p, rho; `outputs` is (dtheta, dqv, dqc, dqr) or None."""
+    nx, ny, nz = st["theta"].shape
+    a = KesslerArgs()
+    outs = outputs or (None, None, None, None)
+    a._keep = (dict(st), outs)
+    a.theta, a.qv, a.qc, a.qr, a.p, a.rho = (_f(st[k]) for k in ("theta", "qv", "qc", "qr", "p", "rho"))
+    a.nx, a.ny, a.nz = nx, ny, nz
+    a.dz, a.dt = dz, dt
+    a.domain[:] = [int(x) for x in (domain or cgrid_cell_domain(nx, ny, nz))]
+    a.dtheta_dt, a.dqv_dt, a.dqc_dt, a.dqr_dt = (_f(o) for o in outs)
+    a.memory = memory
+    a.stream = stream
+    return a
+
+
+def eos_args(p, rho, theta, qv=None, qc=None, qr=None, memory=MEMORY_HOST, stream=None) -> EosArgs:
+    """Argument block for nimbus_cuda_eos_projection over every cell; qv/qc/qr
+    (all or none) add the moist-state checks."""
+    a = EosArgs()
+    a._keep = (p, rho, theta, qv, qc, qr)
+    a.p, a.rho, a.theta = _f(p), _f(rho), _f(theta)
+    a.qv, a.qc, a.qr = _f(qv), _f(qc), _f(qr)
+    a.nx, a.ny, a.nz = tuple(p.shape)
+    a.gamma = initial.GAMMA
     a.memory = memory
     a.stream = stream
     return a

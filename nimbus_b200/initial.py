@@ -197,6 +197,19 @@ def perturbed_state(case: Case, amplitude: float = 1.0, seed: int = 1):
     return st, base
 
 
+def cloudy_state(case: Case, seed: int = 1):
+    """perturbed_state with vapour scattered +/-30 % around the sounding and
+    cloud and rain in half of the cells: saturation adjustment, warm rain,
+    evaporation and sedimentation all act somewhere in the grid."""
+    st, base = perturbed_state(case, amplitude=1.0, seed=seed)
+    rng = np.random.default_rng(seed)
+    shape = case.shape
+    st["qv"] = (st["qv"] * (1.0 + 0.3 * rng.uniform(-1, 1, shape))).astype(np.float32)
+    st["qc"] = np.where(rng.uniform(0, 1, shape) < 0.5, 2e-3 * rng.uniform(0, 1, shape), 0).astype(np.float32)
+    st["qr"] = np.where(rng.uniform(0, 1, shape) < 0.5, 3e-3 * rng.uniform(0, 1, shape), 0).astype(np.float32)
+    return st, base
+
+
 def benchmark_case(name: str) -> Case:
     """Named workloads (grid, dt, acoustic substeps)."""
     if name == "supercell_1km_64x64x40":

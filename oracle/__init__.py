@@ -98,6 +98,62 @@ class Restatement:
             raise FloatingPointError("oracle mass-flux accumulation produced a non-finite flux")
         return out
 
+    def slow_tendencies(self, st, base, grid, coriolis_f=0.0, moist=True, frame=(0.0, 0.0)):
+        """(du, dv, dw, dp) of the slow operator at the given state."""
+        u, v, w, rho, p = (st[k] for k in ("u", "v", "w", "rho", "p"))
+        qv, qc, qr = _slow_inputs(st, base, moist)
+        self._chk(u, v, w, rho, p, qv, qc, qr)
+        nx, ny, nz = u.shape
+        out = [np.zeros_like(u) for _ in range(4)]
+        self.lib.oracle_slow_tendencies(
+            nx, ny, nz, ctypes.c_double(grid[0]), ctypes.c_double(grid[1]), ctypes.c_double(grid[2]),
+            _fp(u), _fp(v), _fp(w), _fp(rho), _fp(p), _opt(qv), _opt(qc), _opt(qr), _fp(base["rho0"]),
+            _fp(base["qv0"]) if moist else None, _fp(base["u0"]), _fp(base["v0"]), ctypes.c_double(coriolis_f),
+            ctypes.c_double(frame[0]), ctypes.c_double(frame[1]), *[_fp(o) for o in out])
+        return out
+
+    def slow_rk2_step(self, st, base, grid, dt, coriolis_f=0.0, moist=True, frame=(0.0, 0.0)):
+        """Heun slow step applied in place to u, v, w, p."""
+        u, v, w, rho, p = (st[k] for k in ("u", "v", "w", "rho", "p"))
+        qv, qc, qr = _slow_inputs(st, base, moist)
+        self._chk(u, v, w, rho, p, qv, qc, qr)
+        nx, ny, nz = u.shape
+        rc = self.lib.oracle_slow_rk2_step(
+            nx, ny, nz, ctypes.c_double(grid[0]), ctypes.c_double(grid[1]), ctypes.c_double(grid[2]),
+            _fp(u), _fp(v), _fp(w), _fp(rho), _fp(p), _opt(qv), _opt(qc), _opt(qr), _fp(base["rho0"]),
+            _fp(base["qv0"]) if moist else None, _fp(base["u0"]), _fp(base["v0"]), ctypes.c_double(coriolis_f),
+            ctypes.c_double(frame[0]), ctypes.c_double(frame[1]), ctypes.c_double(dt))
+        if rc != 0:
+            raise MemoryError("oracle slow-step scratch allocation failed")
+
+    def kessler_tendencies(self, st, dz, dt, domain):
+        th, p, rho, qv, qc, qr = (st[k] for k in ("theta", "p", "rho", "qv", "qc", "qr"))
+        self._chk(th, p, rho, qv, qc, qr)
+        nx, ny, nz = th.shape
+        out = [np.zeros_like(th) for _ in range(4)]
+        dom = (ctypes.c_int * 6)(*[int(x) for x in domain])
+        self.lib.oracle_kessler_tendencies(nx, ny, nz, ctypes.c_double(dz), ctypes.c_double(dt), _fp(th), _fp(p),
+                                           _fp(rho), _fp(qv), _fp(qc), _fp(qr), dom, *[_fp(o) for o in out])
+        return out
+
+    def kessler_step(self, st, dz, dt, domain):
+        """Kessler tendencies, then their application in place (theta, qv, qc, qr)."""
+        dth, dqv, dqc, dqr = self.kessler_tendencies(st, dz, dt, domain)
+        nx, ny, nz = st["theta"].shape
+        dom = (ctypes.c_int * 6)(*[int(x) for x in domain])
+        self.lib.oracle_kessler_apply(nx, ny, nz, ctypes.c_double(dt), dom, _fp(st["theta"]), _fp(st["qv"]),
+                                      _fp(st["qc"]), _fp(st["qr"]), _fp(dth), _fp(dqv), _fp(dqc), _fp(dqr))
+        return dth, dqv, dqc, dqr
+
+    def eos_projection(self, p, rho, theta, qv=None, qc=None, qr=None):
+        """EOS pressure re-projection in place; returns False (p untouched)
+        when the state is refused.  qv/qc/qr (all or none) add the moist-state
+        checks of the attributed domain."""
+        self._chk(p, rho, theta, qv, qc, qr)
+        nx, ny, nz = p.shape
+        return self.lib.oracle_eos_projection(nx, ny, nz, _fp(rho), _fp(theta), _fp(p), _opt(qv), _opt(qc),
+                                              _opt(qr)) == 0
+
     def scalar_transport(self, qs, pd, rho_end, rho_begin, mfx, mfy, mfz, dt, grid, weno=True, top_open=False):
         self._chk(rho_end, rho_begin, mfx, mfy, mfz, *qs)
         nx, ny, nz = rho_end.shape
@@ -111,6 +167,17 @@ class Restatement:
             ctypes.c_double(dt), int(weno), int(top_open))
         if rc != 0:
             raise MemoryError("oracle transport scratch allocation failed")
+
+
+def _opt(a):
+    return None if a is None else _fp(a)
+
+
+def _slow_inputs(st, base, moist=True):
+    qv = st.get("qv") if moist else None
+    qc = st.get("qc") if moist else None
+    qr = st.get("qr") if moist else None
+    return qv, qc, qr
 
 
 class ReferenceHarness:
@@ -151,6 +218,38 @@ class ReferenceHarness:
             ctypes.c_double(grid[0]), ctypes.c_double(grid[1]), ctypes.c_double(grid[2]),
             ctypes.c_double(dt_large), int(n_substeps), *[int(x) for x in bc],
             _fp(out["mfx"]), _fp(out["mfy"]), _fp(out["mfz"]), _fp(out["rho_begin"]), _fp(out["wave"])))
+        return out
+
+    def kessler_tendencies(self, st, dz, dt, domain):
+        th, p, rho, qv, qc, qr = (st[k] for k in ("theta", "p", "rho", "qv", "qc", "qr"))
+        nx, ny, nz = th.shape
+        out = [np.zeros_like(th) for _ in range(4)]
+        dom = (ctypes.c_int * 6)(*[int(x) for x in domain])
+        self._rc(self.lib.ref_kessler_tendencies(_fp(th), _fp(p), _fp(rho), _fp(qv), _fp(qc), _fp(qr), nx, ny, nz,
+                                                 ctypes.c_double(dz), ctypes.c_double(dt), dom,
+                                                 *[_fp(o) for o in out]))
+        return out
+
+    def eos_projection(self, p, rho, theta, grid, qv=None, qc=None, qr=None):
+        """apply_pressure_projection on p in place; False when refused."""
+        nx, ny, nz = p.shape
+        rc = self.lib.ref_eos_projection(_fp(rho), _fp(theta), _fp(p), _opt(qv), _opt(qc), _opt(qr), nx, ny, nz,
+                                         ctypes.c_double(grid[0]), ctypes.c_double(grid[1]),
+                                         ctypes.c_double(grid[2]))
+        if rc < 0:
+            self._rc(rc)
+        return rc == 0
+
+    def slow_tendencies(self, st, base, grid, coriolis_f=0.0, moist=True):
+        u, v, w, rho, p, th = (st[k] for k in ("u", "v", "w", "rho", "p", "theta"))
+        qv, qc, qr = _slow_inputs(st, base, moist)
+        nx, ny, nz = u.shape
+        out = [np.zeros_like(u) for _ in range(4)]
+        self._rc(self.lib.ref_slow_tendencies(
+            _fp(u), _fp(v), _fp(w), _fp(rho), _fp(p), _fp(th), _opt(qv), _opt(qc), _opt(qr), _fp(base["rho0"]),
+            _fp(base["p0"]), _fp(base["qv0"]) if moist else None, _fp(base["u0"]), _fp(base["v0"]),
+            _fp(base["theta0"]), nx, ny, nz, ctypes.c_double(grid[0]), ctypes.c_double(grid[1]),
+            ctypes.c_double(grid[2]), ctypes.c_double(coriolis_f), *[_fp(o) for o in out]))
         return out
 
     def scalar_transport(self, qs, pd, u, v, w, rho_end, rho_begin, mfx, mfy, mfz, dt, grid,

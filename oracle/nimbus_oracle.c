@@ -644,3 +644,497 @@ int oracle_scalar_transport(int nx, int ny, int nz, double dx, double dy, double
     free(rl);
     return 0;
 }
+
+/* ---------------------------------------------------------------------- */
+/* Slow tendencies and the Heun (RK2) slow step.                           */
+/* ---------------------------------------------------------------------- */
+
+/* Upwind-biased first derivatives, Wicker & Skamarock (2002):
+ * include/numerics/derivatives/derivative_operators.hpp:324-395.  `half` is
+ * the distance to the nearer boundary along the axis; the stencil order
+ * degrades 5 -> 3 -> 1 near it. */
+static double upwind_d(const REAL* f, size_t c, size_t stride, int idx, int n, double a, double inv_d)
+{
+    const int lo = idx, hi = n - 1 - idx;
+    const int half = lo < hi ? lo : hi;
+#define F(m) ((double)f[c + (ptrdiff_t)(m) * (ptrdiff_t)stride])
+    const double cc = F(0);
+    if (half <= 0) return 0.0;
+    const double m1 = F(-1), p1 = F(1);
+    if (half == 1) return (a >= 0.0) ? (cc - m1) * inv_d : (p1 - cc) * inv_d;
+    const double m2 = F(-2), p2 = F(2);
+    if (half == 2)
+        return (a >= 0.0) ? (2.0 * p1 + 3.0 * cc - 6.0 * m1 + m2) * (inv_d / 6.0)
+                          : (-p2 + 6.0 * p1 - 3.0 * cc - 2.0 * m1) * (inv_d / 6.0);
+    const double m3 = F(-3), p3 = F(3);
+    return (a >= 0.0) ? (-2.0 * m3 + 15.0 * m2 - 60.0 * m1 + 20.0 * cc + 30.0 * p1 - 3.0 * p2) * (inv_d / 60.0)
+                      : (2.0 * p3 - 15.0 * p2 + 60.0 * p1 - 20.0 * cc - 30.0 * m1 + 3.0 * m2) * (inv_d / 60.0);
+#undef F
+}
+
+/*
+ * Slow tendencies of the flat C-grid KW scheme:
+ * CartesianCGrid3DScheme::compute_slow_tendencies (cartesian_cgrid_3d.cpp:1026-1401)
+ * on the stationary flat branch.  du (x-faces), dv (y-faces), dw (z-faces)
+ * on 1<=i<=nx-2, 1<=j<=ny-2, 0<=k<=nz-2; dp (centres) on 1<=k<=nz-2; zero
+ * elsewhere.  qv/qc/qr may be NULL (no moisture / no loading); the loading
+ * sums qc+qr (the other hydrometeor species are absent for Kessler).
+ * qv0 enters rounded to FP32 (stored_base_value, cartesian_common.hpp:36-40).
+ */
+void oracle_slow_tendencies(int nx, int ny, int nz, double dx, double dy, double dz, const REAL* u, const REAL* v,
+                            const REAL* w, const REAL* rho, const REAL* p, const REAL* qv, const REAL* qc,
+                            const REAL* qr, const double* rho0, const double* qv0, const double* u0,
+                            const double* v0, double coriolis_f, double frame_u, double frame_v, REAL* du,
+                            REAL* dv, REAL* dw, REAL* dp)
+{
+    const size_t n = (size_t)nx * ny * nz;
+    const size_t SX = (size_t)ny * nz, SY = (size_t)nz;
+    const double inv_2dx = 1.0 / (2.0 * dx), inv_2dy = 1.0 / (2.0 * dy), inv_2dz = 1.0 / (2.0 * dz);
+    const double inv_dx = 1.0 / dx, inv_dy = 1.0 / dy, inv_dz = 1.0 / dz;
+    const double g = 9.81;
+    for (size_t c = 0; c < n; ++c) du[c] = dv[c] = dw[c] = dp[c] = 0;
+    for (int i = 1; i < nx - 1; ++i)
+        for (int j = 1; j < ny - 1; ++j)
+            for (int k = 0; k < nz - 1; ++k)
+            {
+                const size_t c = IDX(i, j, k);
+                /* du at the x-face */
+                {
+                    const double ux = (double)u[c];
+                    const double uy = 0.25 * ((double)v[IDX(i, j - 1, k)] + (double)v[c] + (double)v[IDX(i + 1, j - 1, k)] +
+                                              (double)v[IDX(i + 1, j, k)]);
+                    const double tux = ux - frame_u, tuy = uy - frame_v;
+                    const double wx = (k == 0) ? 0.25 * ((double)w[IDX(i, j, 0)] + (double)w[IDX(i + 1, j, 0)])
+                                               : 0.25 * ((double)w[IDX(i, j, k - 1)] + (double)w[c] +
+                                                         (double)w[IDX(i + 1, j, k - 1)] + (double)w[IDX(i + 1, j, k)]);
+                    const double ddx = upwind_d(u, c, SX, i, nx, tux, inv_dx);
+                    const double ddy = upwind_d(u, c, SY, j, ny, tuy, inv_dy);
+                    const double ddz = (k == 0) ? ((wx >= 0.0) ? 0.0 : ((double)u[IDX(i, j, 1)] - (double)u[IDX(i, j, 0)]) * inv_dz)
+                                                : upwind_d(u, c, 1, k, nz, wx, inv_dz);
+                    const double v0k = v0 ? v0[k] : 0.0;
+                    const double cor = coriolis_f * (uy - v0k);
+                    du[c] = (REAL)finite_or_zero(-tux * ddx - tuy * ddy - wx * ddz + cor);
+                }
+                /* dv at the y-face */
+                {
+                    const double vy = (double)v[c];
+                    const double ux = 0.25 * ((double)u[IDX(i - 1, j, k)] + (double)u[c] + (double)u[IDX(i - 1, j + 1, k)] +
+                                              (double)u[IDX(i, j + 1, k)]);
+                    const double tvy = vy - frame_v, tux = ux - frame_u;
+                    const double wy = (k == 0) ? 0.25 * ((double)w[IDX(i, j, 0)] + (double)w[IDX(i, j + 1, 0)])
+                                               : 0.25 * ((double)w[IDX(i, j, k - 1)] + (double)w[c] +
+                                                         (double)w[IDX(i, j + 1, k - 1)] + (double)w[IDX(i, j + 1, k)]);
+                    const double ddx = upwind_d(v, c, SX, i, nx, tux, inv_dx);
+                    const double ddy = upwind_d(v, c, SY, j, ny, tvy, inv_dy);
+                    const double ddz = (k == 0) ? ((wy >= 0.0) ? 0.0 : ((double)v[IDX(i, j, 1)] - (double)v[IDX(i, j, 0)]) * inv_dz)
+                                                : upwind_d(v, c, 1, k, nz, wy, inv_dz);
+                    const double u0k = u0 ? u0[k] : 0.0;
+                    const double cor = coriolis_f * (ux - u0k);
+                    dv[c] = (REAL)finite_or_zero(-tux * ddx - tvy * ddy - wy * ddz - cor);
+                }
+                /* dw at the z-face: advection, buoyancy, moisture, loading */
+                {
+                    const double wz = (double)w[c];
+                    const double ux = 0.25 * ((double)u[IDX(i - 1, j, k)] + (double)u[c] + (double)u[IDX(i - 1, j, k + 1)] +
+                                              (double)u[IDX(i, j, k + 1)]);
+                    const double uy = 0.25 * ((double)v[IDX(i, j - 1, k)] + (double)v[c] + (double)v[IDX(i, j - 1, k + 1)] +
+                                              (double)v[IDX(i, j, k + 1)]);
+                    const double tux = ux - frame_u, tuy = uy - frame_v;
+                    const double ddx = upwind_d(w, c, SX, i, nx, tux, inv_dx);
+                    const double ddy = upwind_d(w, c, SY, j, ny, tuy, inv_dy);
+                    const double ddz = (k == 0) ? ((wz >= 0.0) ? ((double)w[IDX(i, j, 0)] - 0.0) * inv_dz
+                                                               : ((double)w[IDX(i, j, 1)] - (double)w[IDX(i, j, 0)]) * inv_dz)
+                                                : upwind_d(w, c, 1, k, nz, wz, inv_dz);
+                    const double rho_face = 0.5 * ((double)rho[c] + (double)rho[IDX(i, j, k + 1)]);
+                    const double rho_s = safe_rho(rho_face);
+                    const double rho0_face = 0.5 * (rho0[k] + rho0[k + 1]);
+                    const double buoy = -g * (rho_face - rho0_face) / rho_s;
+                    double moist = 0.0;
+                    if (qv && qv0)
+                    {
+                        const double qf = 0.5 * ((double)qv[c] + (double)qv[IDX(i, j, k + 1)]);
+                        const double q0f = 0.5 * ((double)(float)qv0[k] + (double)(float)qv0[k + 1]);
+                        moist = g * 0.608 * (qf - q0f);
+                    }
+                    double load = 0.0;
+                    if (qc)
+                    {
+                        const double lo = (double)qc[c] + (double)qr[c] + 0.0 + 0.0 + 0.0 + 0.0;
+                        const double hi = (double)qc[IDX(i, j, k + 1)] + (double)qr[IDX(i, j, k + 1)] + 0.0 + 0.0 + 0.0 + 0.0;
+                        load = -g * (0.5 * (lo + hi));
+                    }
+                    dw[c] = (REAL)finite_or_zero(-tux * ddx - tuy * ddy - wz * ddz + buoy + moist + load);
+                }
+                /* dp at the centre: -u.grad p, centred */
+                if (k >= 1)
+                {
+                    const double uc = 0.5 * ((double)u[c] + (double)u[IDX(i - 1, j, k)]);
+                    const double vc = 0.5 * ((double)v[c] + (double)v[IDX(i, j - 1, k)]);
+                    const double tuc = uc - frame_u, tvc = vc - frame_v;
+                    const double wc = 0.5 * ((double)w[c] + (double)w[IDX(i, j, k - 1)]);
+                    const double dpdx = ((double)p[IDX(i + 1, j, k)] - (double)p[IDX(i - 1, j, k)]) * inv_2dx;
+                    const double dpdy = ((double)p[IDX(i, j + 1, k)] - (double)p[IDX(i, j - 1, k)]) * inv_2dy;
+                    const double dpdz = ((double)p[IDX(i, j, k + 1)] - (double)p[IDX(i, j, k - 1)]) * inv_2dz;
+                    dp[c] = (REAL)finite_or_zero(-tuc * dpdx - tvc * dpdy - wc * dpdz);
+                }
+            }
+}
+
+/* apply_slow_tendencies_cpu (dynamics.cpp:2066-2092): x += t * dt in FP64,
+ * rounded to the stored type; non-finite tendencies count as zero. */
+void oracle_slow_apply(size_t n, REAL* u, REAL* v, REAL* w, REAL* p, const REAL* du, const REAL* dv, const REAL* dw,
+                       const REAL* dp, double dt)
+{
+    for (size_t c = 0; c < n; ++c)
+    {
+        u[c] = (REAL)((double)u[c] + finite_or_zero((double)du[c]) * dt);
+        v[c] = (REAL)((double)v[c] + finite_or_zero((double)dv[c]) * dt);
+        w[c] = (REAL)((double)w[c] + finite_or_zero((double)dw[c]) * dt);
+        p[c] = (REAL)((double)p[c] + finite_or_zero((double)dp[c]) * dt);
+    }
+}
+
+/*
+ * The Heun slow step of one large step, then its application:
+ * prepare_slow_rk2_tendencies (dynamics.cpp:5123-5292) -- k1 at the state,
+ * predictor state + dt*k1, k2 at the predictor, tendency 0.5f*(k2 + k1) in
+ * the stored type -- followed by the split stepper's apply_slow_tendencies(dt)
+ * (split_explicit.cpp:186).  u, v, w, p are advanced in place.
+ */
+int oracle_slow_rk2_step(int nx, int ny, int nz, double dx, double dy, double dz, REAL* u, REAL* v, REAL* w,
+                         const REAL* rho, REAL* p, const REAL* qv, const REAL* qc, const REAL* qr, const double* rho0,
+                         const double* qv0, const double* u0, const double* v0, double coriolis_f, double frame_u,
+                         double frame_v, double dt)
+{
+    const size_t n = (size_t)nx * ny * nz;
+    REAL* buf = (REAL*)malloc(12 * n * sizeof(REAL));
+    if (!buf) return -1;
+    REAL *k1u = buf, *k1v = buf + n, *k1w = buf + 2 * n, *k1p = buf + 3 * n;
+    REAL *k2u = buf + 4 * n, *k2v = buf + 5 * n, *k2w = buf + 6 * n, *k2p = buf + 7 * n;
+    REAL *su = buf + 8 * n, *sv = buf + 9 * n, *sw = buf + 10 * n, *sp = buf + 11 * n;
+    oracle_slow_tendencies(nx, ny, nz, dx, dy, dz, u, v, w, rho, p, qv, qc, qr, rho0, qv0, u0, v0, coriolis_f, frame_u,
+                           frame_v, k1u, k1v, k1w, k1p);
+    memcpy(su, u, n * sizeof(REAL));
+    memcpy(sv, v, n * sizeof(REAL));
+    memcpy(sw, w, n * sizeof(REAL));
+    memcpy(sp, p, n * sizeof(REAL));
+    oracle_slow_apply(n, su, sv, sw, sp, k1u, k1v, k1w, k1p, dt);
+    oracle_slow_tendencies(nx, ny, nz, dx, dy, dz, su, sv, sw, rho, sp, qv, qc, qr, rho0, qv0, u0, v0, coriolis_f,
+                           frame_u, frame_v, k2u, k2v, k2w, k2p);
+    for (size_t c = 0; c < n; ++c)
+    {
+        k2u[c] = (REAL)((REAL)0.5 * (k2u[c] + k1u[c]));
+        k2v[c] = (REAL)((REAL)0.5 * (k2v[c] + k1v[c]));
+        k2w[c] = (REAL)((REAL)0.5 * (k2w[c] + k1w[c]));
+        k2p[c] = (REAL)((REAL)0.5 * (k2p[c] + k1p[c]));
+    }
+    oracle_slow_apply(n, u, v, w, p, k2u, k2v, k2w, k2p, dt);
+    free(buf);
+    return 0;
+}
+
+/* ---------------------------------------------------------------------- */
+/* Kessler warm-rain microphysics.                                         */
+/* ---------------------------------------------------------------------- */
+
+/* Constants: include/microphysics/microphysics_base.hpp:1073-1080,
+ * src/microphysics/base/fall_speeds.hpp:60-68, kessler.hpp:40-46. */
+static const double kT0 = 273.15, kLv = 2.5e6, kCpm = 1004.0, kRv = 461.5, kRdm = 287.0, kP0m = 100000.0;
+static const double kQc0 = 1.0e-3, kCauto = 1.0e-3, kCaccr = 2.2, kEvapEff = 1.0, kVtMax = 20.0;
+static const double kRainA = 36.34, kRainB = 0.1346, kMinQ = 1.0e-9, kRhoFall = 1.2;
+
+static double dclamp(double v, double lo, double hi) { return v < lo ? lo : (hi < v ? hi : v); }
+static double dmax(double a, double b) { return a < b ? b : a; }
+static double dmin(double a, double b) { return b < a ? b : a; }
+
+/* thermodynamics.hpp:29-44 */
+static double theta_to_temperature(double theta, double p)
+{
+    if (!isfinite(theta) || !isfinite(p)) return kT0;
+    const double th = dclamp(theta, 150.0, 700.0), ps = dclamp(p, 100.0, 200000.0);
+    const double T = th * pow(ps / kP0m, kRdm / kCpm);
+    return isfinite(T) ? T : kT0;
+}
+
+/* thermodynamics.hpp:67-85 (Buck, water at all temperatures) */
+static double svp_water(double T)
+{
+    if (!isfinite(T)) return 0.0;
+    T = dclamp(T, 150.0, 400.0);
+    const double tc = T - kT0;
+    const double value = 611.21 * exp((18.678 - tc / 234.5) * tc / (257.14 + tc));
+    return isfinite(value) ? dmax(0.0, value) : 0.0;
+}
+
+/* thermodynamics.hpp:106-118 */
+double oracle_qvs_water(double T, double p)
+{
+    const double e = svp_water(T);
+    if (!isfinite(e) || !isfinite(p)) return 0.0;
+    const double ps = dclamp(p, 100.0, 200000.0);
+    const double denom = dmax(ps - e, 1.0);
+    return dclamp(0.62198 * e / denom, 0.0, 0.2);
+}
+
+static double sat_slope(double temperature, double saturation, double p)
+{
+    if (!(temperature > 150.0 && temperature < 400.0) || !(saturation > 0.0 && saturation < 0.2)) return 0.0;
+    const double pressure = dclamp(p, 100.0, 200000.0);
+    const double vapor_pressure = saturation * pressure / (0.62198 + saturation);
+    const double tc = temperature - kT0;
+    const double denominator = 257.14 + tc;
+    const double numerator = (18.678 - tc / 234.5) * tc;
+    const double numerator_slope = 18.678 - 2.0 * tc / 234.5;
+    const double log_pressure_slope = (numerator_slope * denominator - numerator) / (denominator * denominator);
+    return saturation * pressure / dmax(pressure - vapor_pressure, 1.0) * log_pressure_slope;
+}
+
+/* Coupled saturation adjustment, bracketed Newton on qv' = qvs(T'):
+ * thermodynamics.hpp:282-466. */
+double oracle_saturation_adjustment(double T_in, double p, double* qv_io, double* qc_io)
+{
+    double T = isfinite(T_in) ? dclamp(T_in, 150.0, 400.0) : kT0;
+    double qv = isfinite(*qv_io) ? dmax(0.0, *qv_io) : 0.0;
+    double qc = isfinite(*qc_io) ? dmax(0.0, *qc_io) : 0.0;
+    double qvs = oracle_qvs_water(T, p);
+    if (!isfinite(qvs) || qvs < 0.0) qvs = 0.0;
+    const double L = kLv / kCpm;
+    const double eps8 = 8.0 * DBL_EPSILON;
+    if (qv > qvs)
+    {
+        const double maximum = dmin(qv, dmax(0.0, (400.0 - T) / L));
+        double condensed = maximum;
+        if (qv - maximum - oracle_qvs_water(T + L * maximum, p) <= 0.0)
+        {
+            double lower = 0.0, upper = maximum;
+            condensed = dclamp((qv - qvs) / (1.0 + L * sat_slope(T, qvs, p)), lower, upper);
+            for (int it = 0; it < 10; ++it)
+            {
+                const double ta = T + L * condensed;
+                const double sa = oracle_qvs_water(ta, p);
+                const double value = qv - condensed - sa;
+                const double scale = dmax(dmax(1.0, fabs(qv)), fabs(sa));
+                if (fabs(value) <= eps8 * scale) break;
+                if (value > 0.0) lower = condensed;
+                else upper = condensed;
+                const double derivative = -1.0 - L * sat_slope(ta, sa, p);
+                const double candidate = condensed - value / derivative;
+                condensed = (candidate > lower && candidate < upper) ? candidate : 0.5 * (lower + upper);
+            }
+        }
+        qv -= condensed;
+        qc += condensed;
+        T += L * condensed;
+    }
+    else if (qv < qvs && qc > 0.0)
+    {
+        const double maximum = dmin(qc, dmax(0.0, (T - 150.0) / L));
+        double evaporated = maximum;
+        if (qv + maximum - oracle_qvs_water(T - L * maximum, p) >= 0.0)
+        {
+            double lower = 0.0, upper = maximum;
+            evaporated = dclamp((qvs - qv) / (1.0 + L * sat_slope(T, qvs, p)), lower, upper);
+            for (int it = 0; it < 10; ++it)
+            {
+                const double ta = T - L * evaporated;
+                const double sa = oracle_qvs_water(ta, p);
+                const double value = qv + evaporated - sa;
+                const double scale = dmax(dmax(1.0, fabs(qv)), fabs(sa));
+                if (fabs(value) <= eps8 * scale) break;
+                if (value < 0.0) lower = evaporated;
+                else upper = evaporated;
+                const double derivative = 1.0 + L * sat_slope(ta, sa, p);
+                const double candidate = evaporated - value / derivative;
+                evaporated = (candidate > lower && candidate < upper) ? candidate : 0.5 * (lower + upper);
+            }
+        }
+        qc -= evaporated;
+        qv += evaporated;
+        T -= L * evaporated;
+    }
+    *qc_io = dmax(0.0, qc);
+    *qv_io = dmax(0.0, qv);
+    return T;
+}
+
+/*
+ * KesslerScheme::compute_tendencies on its CPU path (kessler.cpp:103-345,
+ * warm rain :346-464, sedimentation :465-520) over the cell domain
+ * [i0,i1)x[j0,j1)x[k0,k1) with uniform dz.  Tendencies are zero outside the
+ * domain; dtheta is converted from the accumulated temperature tendency at
+ * the end (temperature_tendency_to_theta, thermodynamics.hpp:225-236).
+ * Storage of the tendencies is FP32 in the reference (float fields).
+ */
+void oracle_kessler_tendencies(int nx, int ny, int nz, double dz, double dt, const REAL* theta, const REAL* p,
+                               const REAL* rho, const REAL* qv, const REAL* qc, const REAL* qr, const int* domain,
+                               REAL* dth, REAL* dqv, REAL* dqc, REAL* dqr)
+{
+    const size_t n = (size_t)nx * ny * nz;
+    for (size_t c = 0; c < n; ++c) dth[c] = dqv[c] = dqc[c] = dqr[c] = 0;
+    if (!(dt > 0.0) || !isfinite(dt)) return;
+    const int i0 = domain[0], i1 = domain[1], j0 = domain[2], j1 = domain[3], k0 = domain[4], k1 = domain[5];
+    const double inv_dt = 1.0 / dt;
+    const double Lcp = kLv / kCpm;
+    REAL* temp = (REAL*)malloc(3 * n * sizeof(REAL));
+    REAL* qv_adj = temp + n;
+    REAL* qc_adj = temp + 2 * n;
+    for (int i = i0; i < i1; ++i)
+        for (int j = j0; j < j1; ++j)
+            for (int k = k0; k < k1; ++k)
+            {
+                const size_t c = IDX(i, j, k);
+                const REAL tv = (REAL)theta_to_temperature((double)theta[c], (double)p[c]);
+                double qvd = (double)qv[c], qcd = (double)qc[c];
+                const double T = oracle_saturation_adjustment((double)tv, (double)p[c], &qvd, &qcd);
+                temp[c] = (REAL)T;
+                qv_adj[c] = (REAL)qvd;
+                qc_adj[c] = (REAL)qcd;
+                const double dqa = (double)qc_adj[c] - (double)qc[c];
+                if (dqa != 0.0)
+                {
+                    const double rate = dqa * inv_dt;
+                    dqc[c] += (REAL)rate;
+                    dqv[c] -= (REAL)rate;
+                    dth[c] += (REAL)(Lcp * rate);
+                }
+            }
+    for (int i = i0; i < i1; ++i)
+        for (int j = j0; j < j1; ++j)
+            for (int k = k0; k < k1; ++k)
+            {
+                const size_t c = IDX(i, j, k);
+                const REAL qcv = qc_adj[c], qrv = qr[c], qvv = qv_adj[c], T = temp[c];
+                REAL prod = 0;
+                if (dt > 0.0 && qcv > 0)
+                {
+                    const double factor = 1.0 / (1.0 + kCaccr * dt * pow((double)(qrv > 0 ? qrv : 0), 0.875));
+                    const double amount = (double)qcv * (1.0 - factor) + factor * kCauto * dt * dmax((double)qcv - kQc0, 0.0);
+                    prod = (REAL)(dclamp(amount, 0.0, (double)qcv) / dt);
+                    dqc[c] -= prod;
+                    dqr[c] += prod;
+                }
+                if (qrv > 0 || prod > 0)
+                {
+                    const double pv = (double)p[c], rv = (double)rho[c];
+                    const double qvsat = oracle_qvs_water((double)T, pv);
+                    if (qvsat > 0.0 && (double)qvv < qvsat && rv > 0.0 && pv > 0.0)
+                    {
+                        const double qr_av = (double)qrv + (double)prod * dt;
+                        const double rcgs = 1.0e-3 * rv;
+                        const double rain = rcgs * dmax(qr_av, 0.0);
+                        const double vent = (1.6 + 124.9 * pow(rain, 0.2046)) * pow(rain, 0.525);
+                        const double resist = 2.55e8 / (pv * qvsat) + 5.4e5;
+                        const double raw = kEvapEff * (vent / resist) * ((qvsat - (double)qvv) / (rcgs * qvsat));
+                        const double gsat = (kLv * kLv * qvsat) / (kCpm * kRv * dmax((double)T * (double)T, 1.0));
+                        const double bound = (qvsat - (double)qvv) / (1.0 + gsat);
+                        const double evap = dclamp(raw, 0.0, dmin(bound / dt, qr_av / dt));
+                        /* Field3D's element proxy rounds a double operand to float
+                         * before the compound add (field3d.hpp:391-397). */
+                        dqv[c] += (REAL)(float)evap;
+                        dqr[c] -= (REAL)(float)evap;
+                        dth[c] -= (REAL)(float)(kLv / kCpm * evap);
+                    }
+                }
+            }
+    for (int i = i0; i < i1; ++i)
+        for (int j = j0; j < j1; ++j)
+            for (int k = k0; k < k1; ++k)
+            {
+                const size_t c = IDX(i, j, k);
+                const double rk = (double)rho[c];
+                const double rkm = (k > k0) ? (double)rho[IDX(i, j, k - 1)] : rk;
+                const double fall = sqrt(kRhoFall / rk);
+                const double recv = rk / rkm;
+                const double q = dmax(0.0, (double)qr[c]);
+                if (q > 0.0)
+                {
+                    const double vt0 = (q < kMinQ) ? 0.0 : kRainA * pow(1.0e-3 * rk * q, kRainB);
+                    const double vt = dmin(vt0 * fall, kVtMax);
+                    const float sed = (float)(vt * q);
+                    dqr[c] -= (REAL)((double)sed / dz);
+                    if (k > k0) dqr[IDX(i, j, k - 1)] += (REAL)(recv * (double)sed / dz);
+                }
+            }
+    for (int i = i0; i < i1; ++i)
+        for (int j = j0; j < j1; ++j)
+            for (int k = k0; k < k1; ++k)
+            {
+                const size_t c = IDX(i, j, k);
+                const double dT = (double)(float)dth[c], pv = (double)(float)p[c];
+                double r = 0.0;
+                if (isfinite(dT) && isfinite(pv))
+                {
+                    const double ps = dclamp(pv, 100.0, 200000.0);
+                    r = dT * pow(kP0m / ps, kRdm / kCpm);
+                    if (!isfinite(r)) r = 0.0;
+                }
+                dth[c] = (REAL)r;
+            }
+    free(temp);
+}
+
+/* Application of the Kessler tendencies over the domain: water species as
+ * bounded_water_value (microphysics_step.cpp:503-532), clamp to [0, 0.05]
+ * with non-finite -> 0; theta as theta + dt*dtheta rounded once. */
+void oracle_kessler_apply(int nx, int ny, int nz, double dt, const int* domain, REAL* theta, REAL* qv, REAL* qc,
+                          REAL* qr, const REAL* dth, const REAL* dqv, const REAL* dqc, const REAL* dqr)
+{
+    for (int i = domain[0]; i < domain[1]; ++i)
+        for (int j = domain[2]; j < domain[3]; ++j)
+            for (int k = domain[4]; k < domain[5]; ++k)
+            {
+                const size_t c = IDX(i, j, k);
+#define WATER(q, dq)                                                       \
+    do {                                                                   \
+        const REAL raw = (REAL)((double)(q) + (double)(dq) * dt);          \
+        (q) = !isfinite(raw) ? (REAL)0 : (raw < 0 ? (REAL)0 : ((REAL)0.05f < raw ? (REAL)0.05f : raw)); \
+    } while (0)
+                WATER(qv[c], dqv[c]);
+                WATER(qc[c], dqc[c]);
+                WATER(qr[c], dqr[c]);
+#undef WATER
+                theta[c] = (REAL)((double)theta[c] + (double)dth[c] * dt);
+            }
+}
+
+/* EOS pressure re-projection (eos_apply.cpp:50-175 with pressure_fp64,
+ * eos_pressure.hpp:30-38): p = clamp(float(p00 (rho R_d theta / p00)^gamma))
+ * for every cell.  With qv/qc/qr given (a complete moist state) the cells of
+ * the attributed domain (physical_scalar_domain: a one-cell lateral ring
+ * dropped when the extent is >= 3, every level) are also checked as the energy
+ * attribution does (eos_apply.cpp:139-158): the old pressure finite and
+ * positive, qv finite and non-negative, qc + qr (FP64) finite and
+ * non-negative; the energy sums themselves are diagnostics and are not formed.
+ * Returns -1 (and leaves p unchanged) if any cell is invalid, as the
+ * reference throws before publishing. */
+static int eos_cell_invalid(size_t nx, size_t ny, size_t nz, size_t c, const REAL* rho, const REAL* theta,
+                            const REAL* p, const REAL* qv, const REAL* qc, const REAL* qr, double gamma)
+{
+    const float r = (float)rho[c], th = (float)theta[c];
+    const double diag = kP00 * pow((double)r * kRd * (double)th / kP00, gamma);
+    if (!isfinite(r) || !(r > 0.0f) || !isfinite(th) || !(th > 0.0f) || !isfinite(diag) || diag <= 0.0 ||
+        !isfinite((double)(float)diag))
+        return 1;
+    if (!qv) return 0;
+    const size_t j = (c / nz) % ny, i = c / (nz * ny);
+    const size_t ih = nx >= 3, jh = ny >= 3;
+    if (i < ih || i >= nx - ih || j < jh || j >= ny - jh) return 0;
+    const float p_old = (float)p[c], q = (float)qv[c];
+    const double liquid = (double)(float)qc[c] + (double)(float)qr[c];
+    return !isfinite(p_old) || p_old <= 0.0f || !isfinite(q) || q < 0.0f || !isfinite(liquid) || liquid < 0.0;
+}
+
+int oracle_eos_projection(int nx, int ny, int nz, const REAL* rho, const REAL* theta, REAL* p, const REAL* qv,
+                          const REAL* qc, const REAL* qr)
+{
+    const double gamma = oracle_gamma();
+    const size_t n = (size_t)nx * ny * nz;
+    for (size_t c = 0; c < n; ++c)
+        if (eos_cell_invalid(nx, ny, nz, c, rho, theta, p, qv, qc, qr, gamma)) return -1;
+    for (size_t c = 0; c < n; ++c)
+    {
+        const double diag = kP00 * pow((double)rho[c] * kRd * (double)theta[c] / kP00, gamma);
+        p[c] = clamp_store((REAL)(float)diag, (REAL)101325.0f, (REAL)kPMin, (REAL)kPMax);
+    }
+    return 0;
+}

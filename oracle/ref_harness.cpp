@@ -16,6 +16,13 @@
 //                           (advection_cartesian.cpp:610-870, Host precision, as
 //                           dynamics.cpp:4545-4557 calls it), fused substep, apply_acoustic(dt_s)
 //                           (boundary_conditions_cartesian_cgrid.cpp:141,884-1187)}
+//   ref_slow_tendencies     CartesianCGrid3DScheme::compute_slow_tendencies
+//                           (src/dynamics/schemes/klemp_wilhelmson_split/cartesian_cgrid_3d.cpp:724-1416)
+//                           on a stationary flat level with moisture and Kessler loading
+//   ref_kessler_tendencies  KesslerScheme::compute_tendencies
+//                           (src/microphysics/schemes/kessler/kessler.cpp:103-520)
+//   ref_eos_projection      tmv::dynamics_eos::apply_pressure_projection
+//                           (src/core/orchestration/dynamics/eos_apply.cpp:50-200)
 //   ref_scalar_transport    advect_scalars_conservative_3d_cartesian
 //                           (advection_cartesian.cpp:3532) on a retained context whose
 //                           face mass fluxes and beginning density are supplied
@@ -35,6 +42,9 @@
 #include "core/runtime/runtime_config.hpp"
 #include "dynamics/dynamics_base.hpp"
 #include "numerics/advection/advection_cartesian.hpp"
+#include "dynamics/schemes/klemp_wilhelmson_split/cartesian_cgrid_3d.hpp"
+#include "microphysics/schemes/kessler/kessler.hpp"
+#include "dynamics/eos_pressure.hpp"
 
 #include <cstring>
 #include <exception>
@@ -299,6 +309,134 @@ int ref_scalar_transport(float** q, const int* positive_definite, int n_scalars,
             weno ? tmv::CartesianFaceReconstruction::WENO5 : tmv::CartesianFaceReconstruction::MonotonicCentered);
         for (int s = 0; s < n_scalars; ++s)
             from_field(q[s], fields[s]);
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        return fail(e.what());
+    }
+}
+
+// Kessler warm-rain tendencies (dtheta, dqv, dqc, dqr) over the cell domain
+// {i0, i1, j0, j1, k0, k1} with uniform vertical spacing dz.
+int ref_kessler_tendencies(const float* theta, const float* p, const float* rho, const float* qv, const float* qc,
+                           const float* qr, int nx, int ny, int nz, double dz, double dt, const int* domain,
+                           float* dth, float* dqv, float* dqc, float* dqr)
+{
+    try
+    {
+        Field3D fth, fp, frho, fqv, fqc, fqr;
+        to_field(fth, theta, nx, ny, nz);
+        to_field(fp, p, nx, ny, nz);
+        to_field(frho, rho, nx, ny, nz);
+        to_field(fqv, qv, nx, ny, nz);
+        to_field(fqc, qc, nx, ny, nz);
+        to_field(fqr, qr, nx, ny, nz);
+        Field3D zero(nx, ny, nz, 0.0f);
+        Field3D o_th, o_qv, o_qc, o_qr, o_qi, o_qs, o_qg, o_qh;
+        tmv::KesslerScheme scheme;
+        scheme.set_vertical_spacing_m(dz);
+        PhysicalCellDomain d;
+        d.i_begin = domain[0]; d.i_end = domain[1];
+        d.j_begin = domain[2]; d.j_end = domain[3];
+        d.k_begin = domain[4]; d.k_end = domain[5];
+        scheme.set_physical_cell_domain(nx, ny, nz, d);
+        scheme.compute_tendencies(fp, fth, frho, fqv, fqc, fqr, zero, zero, zero, zero, dt, o_th, o_qv, o_qc, o_qr,
+                                  o_qi, o_qs, o_qg, o_qh);
+        from_field(dth, o_th);
+        from_field(dqv, o_qv);
+        from_field(dqc, o_qc);
+        from_field(dqr, o_qr);
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        return fail(e.what());
+    }
+}
+
+// EOS pressure re-projection on a level whose p is replaced in place.  With
+// qv/qc/qr given the state is complete (ice and TKE zero) and the reference's
+// moist energy attribution and its extra rejection checks run too.  Returns 0
+// when p was published, 1 when the reference refused the state (p untouched).
+int ref_eos_projection(const float* rho, const float* theta, float* p, const float* qv, const float* qc,
+                       const float* qr, int nx, int ny, int nz, double dx, double dy, double dz)
+{
+    try
+    {
+        Level L(nx, ny, nz, dx, dy, dz, 1.0);
+        auto& f = L.storage.fields;
+        for (Field3D* z : {&f.u, &f.v, &f.w}) z->resize(nx, ny, nz, 0.0f);
+        to_field(f.rho, rho, nx, ny, nz);
+        to_field(f.theta, theta, nx, ny, nz);
+        to_field(f.p, p, nx, ny, nz);
+        if (qv)
+        {
+            to_field(f.qv, qv, nx, ny, nz);
+            to_field(f.qc, qc, nx, ny, nz);
+            to_field(f.qr, qr, nx, ny, nz);
+            for (Field3D* z : {&f.qi, &f.qs, &f.qg, &f.qh, &f.tke}) z->resize(nx, ny, nz, 0.0f);
+        }
+        try
+        {
+            tmv::dynamics_eos::apply_pressure_projection(L.view);
+        }
+        catch (const std::runtime_error& e)
+        {
+            g_error = e.what();
+            return 1;
+        }
+        from_field(p, f.p);
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        return fail(e.what());
+    }
+}
+
+// Slow tendencies (du, dv, dw at faces; dp at centres) of the reference's
+// C-grid scheme.  qv/qc/qr may be null (dry / no loading); base profiles are
+// FP64 columns of length nz.
+int ref_slow_tendencies(const float* u, const float* v, const float* w, const float* rho, const float* p,
+                        const float* theta, const float* qv, const float* qc, const float* qr, const double* rho0,
+                        const double* p0b, const double* qv0, const double* u0, const double* v0,
+                        const double* theta0, int nx, int ny, int nz, double dx, double dy, double dz,
+                        double coriolis_f, float* du, float* dv, float* dw, float* dp)
+{
+    try
+    {
+        Level L(nx, ny, nz, dx, dy, dz, 1.0);
+        auto& f = L.storage.fields;
+        to_field(f.u, u, nx, ny, nz);
+        to_field(f.v, v, nx, ny, nz);
+        to_field(f.w, w, nx, ny, nz);
+        to_field(f.rho, rho, nx, ny, nz);
+        to_field(f.p, p, nx, ny, nz);
+        to_field(f.theta, theta, nx, ny, nz);
+        if (qv) to_field(f.qv, qv, nx, ny, nz);
+        if (qc)
+        {
+            to_field(f.qc, qc, nx, ny, nz);
+            to_field(f.qr, qr, nx, ny, nz);
+            for (Field3D* z : {&f.qi, &f.qs, &f.qg, &f.qh}) z->resize(nx, ny, nz, 0.0f);
+        }
+        auto& b = L.storage.base;
+        b.rho0.assign(rho0, rho0 + nz);
+        b.p0.assign(p0b, p0b + nz);
+        if (qv0) b.qv0.assign(qv0, qv0 + nz);
+        if (u0) b.u0.assign(u0, u0 + nz);
+        if (v0) b.v0.assign(v0, v0 + nz);
+        if (theta0) b.theta0.assign(theta0, theta0 + nz);
+        L.storage.coriolis_f = coriolis_f;
+        tmv::CartesianCGrid3DScheme scheme(L.view);
+        Field3D fdu(nx, ny, nz, 0.0f), fdv(nx, ny, nz, 0.0f), fdw(nx, ny, nz, 0.0f), fdr(nx, ny, nz, 0.0f),
+            fdp(nx, ny, nz, 0.0f);
+        scheme.compute_slow_tendencies(f.u, f.v, f.w, f.rho, f.p, f.theta, 1.0, fdu, fdv, fdw, fdr, fdp, nullptr);
+        from_field(du, fdu);
+        from_field(dv, fdv);
+        from_field(dw, fdw);
+        from_field(dp, fdp);
         return 0;
     }
     catch (const std::exception& e)

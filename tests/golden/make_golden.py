@@ -19,7 +19,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 sys.path.insert(0, str(HERE.parents[1]))
 
-from nimbus_b200.initial import Case, perturbed_state  # noqa: E402
+from nimbus_b200.initial import Case, cloudy_state, perturbed_state  # noqa: E402
 from oracle import ReferenceHarness  # noqa: E402
 
 GRID = (1000.0, 1000.0, 500.0)
@@ -84,6 +84,35 @@ def main():
             **{f"out_{k}": st2[k] for k in ("u", "v", "w", "rho", "p")},
             **{f"out_{k}": v for k, v in loop.items()}, **scalars)
         print("wrote", name)
+
+    # 4. Slow tendencies of the reference's C-grid scheme (moist, with Coriolis).
+    sc = Case(17, 14, 12, 800.0, 700.0, 400.0, 4.0, seed=6)
+    ss, sb = perturbed_state(sc, seed=12)
+    outs = ref.slow_tendencies(ss, sb, (800.0, 700.0, 400.0), coriolis_f=1e-4, moist=True)
+    dry = ref.slow_tendencies(ss, sb, (800.0, 700.0, 400.0), coriolis_f=0.0, moist=False)
+    np.savez_compressed(HERE / "slow_tendencies.npz", grid=np.array((800.0, 700.0, 400.0)), coriolis_f=1e-4,
+                        **{f"in_{k}": v for k, v in ss.items()}, **{f"base_{k}": v for k, v in sb.items()},
+                        **{f"out_{k}": o for k, o in zip(("du", "dv", "dw", "dp"), outs)},
+                        **{f"dry_{k}": o for k, o in zip(("du", "dv", "dw", "dp"), dry)})
+    print("wrote slow_tendencies")
+
+    # 5. Kessler tendencies on a cloudy state (C-grid cell domain and the full
+    #    grid), and the EOS re-projection of that state, dry and moist.
+    kc = Case(15, 13, 20, 1000.0, 1000.0, 500.0, 6.0, seed=3)
+    ks, _ = cloudy_state(kc, seed=3)
+    kdom = {"cgrid": (1, 14, 1, 12, 0, 20), "full": (0, 15, 0, 13, 0, 20)}
+    kout = {}
+    for name, dom in kdom.items():
+        for key, o in zip(("dtheta", "dqv", "dqc", "dqr"), ref.kessler_tendencies(ks, 500.0, 6.0, dom)):
+            kout[f"{name}_{key}"] = o
+    p_dry, p_moist = ks["p"].copy(), ks["p"].copy()
+    assert ref.eos_projection(p_dry, ks["rho"], ks["theta"], (kc.dx, kc.dy, kc.dz))
+    assert ref.eos_projection(p_moist, ks["rho"], ks["theta"], (kc.dx, kc.dy, kc.dz), ks["qv"], ks["qc"], ks["qr"])
+    np.savez_compressed(HERE / "kessler_eos.npz", dz=500.0, dt=6.0, grid=np.array((kc.dx, kc.dy, kc.dz)),
+                        **{f"dom_{k}": np.array(v) for k, v in kdom.items()},
+                        **{f"in_{k}": ks[k] for k in ("theta", "qv", "qc", "qr", "p", "rho")}, **kout,
+                        eos_p_dry=p_dry, eos_p_moist=p_moist)
+    print("wrote kessler_eos")
 
 
 if __name__ == "__main__":

@@ -49,6 +49,9 @@ def _c_layout(struct_name, fields, tmp_path):
     ("nimbus_acoustic_fused_args", cuda.AcousticFusedArgs),
     ("nimbus_acoustic_batched_args", cuda.AcousticBatchedArgs),
     ("nimbus_scalar_transport_args", cuda.ScalarTransportArgs),
+    ("nimbus_slow_args", cuda.SlowArgs),
+    ("nimbus_kessler_args", cuda.KesslerArgs),
+    ("nimbus_eos_args", cuda.EosArgs),
 ])
 def test_argument_block_layout_matches_header(struct_name, cls, tmp_path):
     fields = [f for f, _ in cls._fields_]

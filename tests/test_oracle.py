@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 import oracle
-from nimbus_b200.initial import Case, perturbed_state
+from nimbus_b200.initial import Case, cloudy_state, perturbed_state
 from tests.golden.make_golden import BC_SETS, close_walls
 
 pytestmark = pytest.mark.skipif(not oracle.restatement_available(),
@@ -164,3 +164,145 @@ def test_live_reference_pin(o32, bc_name, seed):
                          (800.0, 900.0, 400.0), top_open=bc[5] == 2)
     for x, y in zip(qa, qb):
         np.testing.assert_array_equal(x, y)
+
+
+def _slow_case(g):
+    st = {k[3:]: g[k].copy() for k in g.files if k.startswith("in_")}
+    base = {k[5:]: g[k] for k in g.files if k.startswith("base_")}
+    return st, base
+
+
+def test_golden_slow_tendencies(o32):
+    g = np.load("tests/golden/slow_tendencies.npz")
+    st, base = _slow_case(g)
+    grid = tuple(g["grid"])
+    got = o32.slow_tendencies(st, base, grid, coriolis_f=float(g["coriolis_f"]), moist=True)
+    for key, arr in zip(("du", "dv", "dw", "dp"), got):
+        np.testing.assert_array_equal(arr, g["out_" + key], err_msg=key)
+    dry = o32.slow_tendencies(st, base, grid, coriolis_f=0.0, moist=False)
+    for key, arr in zip(("du", "dv", "dw", "dp"), dry):
+        np.testing.assert_array_equal(arr, g["dry_" + key], err_msg="dry " + key)
+
+
+@pytest.mark.reference
+@pytest.mark.skipif(not oracle.reference_available(), reason="reference harness not built here")
+@pytest.mark.parametrize("seed", [31, 32])
+def test_live_reference_pin_slow(o32, seed):
+    ref = oracle.ReferenceHarness()
+    case = Case(19, 16, 13, 600.0, 650.0, 350.0, 3.0, seed=seed)
+    st, base = perturbed_state(case, seed=seed)
+    for cor, moist in ((1.2e-4, True), (0.0, False)):
+        a = ref.slow_tendencies(st, base, (600.0, 650.0, 350.0), cor, moist)
+        b = o32.slow_tendencies(st, base, (600.0, 650.0, 350.0), cor, moist)
+        for x, y in zip(a, b):
+            np.testing.assert_array_equal(x, y)
+
+
+def test_heun_step_is_average_of_two_evaluations(o32):
+    """The composition, checked on the CPU: one Heun step equals applying
+    0.5f*(k1 + k2) with k2 taken at the predictor state."""
+    g = np.load("tests/golden/slow_tendencies.npz")
+    st, base = _slow_case(g)
+    grid = tuple(g["grid"])
+    dt = 2.0
+    a = {k: v.copy() for k, v in st.items()}
+    o32.slow_rk2_step(a, base, grid, dt, coriolis_f=1e-4)
+    k1 = o32.slow_tendencies(st, base, grid, 1e-4)
+    star = {k: v.copy() for k, v in st.items()}
+    for key, t in zip(("u", "v", "w", "p"), k1):
+        star[key] = (star[key].astype(np.float64) + t.astype(np.float64) * dt).astype(np.float32)
+    k2 = o32.slow_tendencies(star, base, grid, 1e-4)
+    for key, t1, t2 in zip(("u", "v", "w", "p"), k1, k2):
+        avg = np.float32(0.5) * (t2 + t1)
+        want = (st[key].astype(np.float64) + avg.astype(np.float64) * dt).astype(np.float32)
+        np.testing.assert_array_equal(a[key], want, err_msg=key)
+
+
+def _kessler_case(g):
+    return {k[3:]: g[k].copy() for k in g.files if k.startswith("in_")}
+
+
+@pytest.mark.parametrize("dom", ["cgrid", "full"])
+def test_golden_kessler_tendencies(o32, dom):
+    g = np.load("tests/golden/kessler_eos.npz")
+    st = _kessler_case(g)
+    got = o32.kessler_tendencies(st, float(g["dz"]), float(g["dt"]), tuple(g["dom_" + dom]))
+    for key, arr in zip(("dtheta", "dqv", "dqc", "dqr"), got):
+        np.testing.assert_array_equal(arr, g[f"{dom}_{key}"], err_msg=key)
+    # every process acted somewhere: condensation and evaporation both present,
+    # rain gained (autoconversion/accretion) and lost (evaporation/fall-out)
+    dqv = g[f"{dom}_dqv"]
+    dqr = g[f"{dom}_dqr"]
+    assert (dqv > 0).any() and (dqv < 0).any() and (dqr > 0).any() and (dqr < 0).any()
+
+
+def test_golden_eos_projection(o32):
+    g = np.load("tests/golden/kessler_eos.npz")
+    st = _kessler_case(g)
+    p = st["p"].copy()
+    assert o32.eos_projection(p, st["rho"], st["theta"])
+    np.testing.assert_array_equal(p, g["eos_p_dry"])
+    p = st["p"].copy()
+    assert o32.eos_projection(p, st["rho"], st["theta"], st["qv"], st["qc"], st["qr"])
+    np.testing.assert_array_equal(p, g["eos_p_moist"])
+
+
+# (field, cell, value, refused when dry, refused when moist): invalid density or
+# temperature refuses everywhere; bad water or old pressure only inside the
+# attributed domain of a complete moist state (eos_apply.cpp:89-158).
+EOS_CASES = [
+    ("rho", (3, 3, 3), -1.0, True, True),
+    ("theta", (0, 0, 0), np.nan, True, True),
+    ("theta", (2, 2, 2), 3e38, True, True),
+    ("qv", (3, 3, 3), -1e-6, False, True),
+    ("qv", (0, 3, 3), -1e-6, False, False),
+    ("qc", (2, 2, 0), -1e-3, False, True),
+    ("qr", (1, 1, 1), np.inf, False, True),
+    ("p", (4, 4, 4), 0.0, False, True),
+    ("p", (8, 3, 3), np.nan, False, False),
+]
+
+
+@pytest.mark.parametrize("field,cell,value,dry_refused,moist_refused", EOS_CASES)
+def test_eos_refusal_rules(o32, field, cell, value, dry_refused, moist_refused):
+    case = Case(9, 7, 6, 1000.0, 1000.0, 500.0, 6.0, seed=1)
+    st, _ = cloudy_state(case, seed=3)
+    st[field][cell] = value
+    for moist, refused in ((False, dry_refused), (True, moist_refused)):
+        p = st["p"].copy()
+        q = (st["qv"], st["qc"], st["qr"]) if moist else (None, None, None)
+        ok = o32.eos_projection(p, st["rho"], st["theta"], *q)
+        assert ok == (not refused), (field, moist)
+        if refused:
+            np.testing.assert_array_equal(p.view(np.uint32), st["p"].view(np.uint32))
+
+
+@pytest.mark.reference
+@pytest.mark.skipif(not oracle.reference_available(), reason="reference harness not built here")
+@pytest.mark.parametrize("seed", [1, 2])
+def test_live_reference_pin_kessler(o32, seed):
+    ref = oracle.ReferenceHarness()
+    case = Case(15, 13, 20, 1000.0, 1000.0, 500.0, 6.0, seed=seed)
+    st, _ = cloudy_state(case, seed=seed)
+    for dom in ((1, 14, 1, 12, 0, 20), (2, 9, 0, 13, 3, 17)):
+        a = ref.kessler_tendencies(st, 500.0, 6.0, dom)
+        b = o32.kessler_tendencies(st, 500.0, 6.0, dom)
+        for x, y in zip(a, b):
+            np.testing.assert_array_equal(x, y)
+
+
+@pytest.mark.reference
+@pytest.mark.skipif(not oracle.reference_available(), reason="reference harness not built here")
+@pytest.mark.parametrize("field,cell,value,dry_refused,moist_refused", EOS_CASES)
+def test_live_reference_pin_eos(o32, field, cell, value, dry_refused, moist_refused):
+    ref = oracle.ReferenceHarness()
+    case = Case(9, 7, 6, 1000.0, 1000.0, 500.0, 6.0, seed=1)
+    st, _ = cloudy_state(case, seed=3)
+    st[field][cell] = value
+    for moist in (False, True):
+        q = (st["qv"], st["qc"], st["qr"]) if moist else (None, None, None)
+        a, b = st["p"].copy(), st["p"].copy()
+        ra = ref.eos_projection(a, st["rho"], st["theta"], (1000.0, 1000.0, 500.0), *q)
+        rb = o32.eos_projection(b, st["rho"], st["theta"], *q)
+        assert ra == rb
+        np.testing.assert_array_equal(a.view(np.uint32), b.view(np.uint32))

@@ -13,7 +13,7 @@ import pytest
 
 import oracle
 from nimbus_b200 import cuda
-from nimbus_b200.initial import Case, initial_state, perturbed_state
+from nimbus_b200.initial import Case, cloudy_state, initial_state, perturbed_state
 from tests.golden.make_golden import BC_SETS, close_walls
 
 pytestmark = pytest.mark.gpu
@@ -178,3 +178,124 @@ def test_nonfinite_mass_flux_is_reported_not_published(ctx):
     assert rc == 4, ctx.last_error   # NIMBUS_ERR_NONFINITE
     for k in st:
         assert_bitwise(st[k], before[k], k)
+
+
+def _slow_case(g):
+    st = {k[3:]: g[k].copy() for k in g.files if k.startswith("in_")}
+    base = {k[5:]: g[k] for k in g.files if k.startswith("base_")}
+    return st, base
+
+
+def test_slow_tendencies_match_reference(ctx):
+    g = np.load("tests/golden/slow_tendencies.npz")
+    st, base = _slow_case(g)
+    grid = tuple(g["grid"])
+    for moist, cor, prefix in ((True, float(g["coriolis_f"]), "out_"), (False, 0.0, "dry_")):
+        outs = tuple(np.zeros_like(st["u"]) for _ in range(4))
+        ctx.check(ctx.slow_tendencies(cuda.slow_args(st, base, grid, coriolis_f=cor, moist=moist, outputs=outs)))
+        for key, arr in zip(("du", "dv", "dw", "dp"), outs):
+            assert_bitwise(arr, g[prefix + key], prefix + key)
+
+
+def test_slow_heun_step_matches_oracle(ctx, o32):
+    case = Case(23, 19, 17, 500.0, 550.0, 300.0, 3.0, seed=13)
+    st, base = perturbed_state(case, seed=14)
+    gpu = {k: v.copy() for k, v in st.items()}
+    cpu = {k: v.copy() for k, v in st.items()}
+    outs = tuple(np.zeros_like(st["u"]) for _ in range(4))
+    ctx.check(ctx.slow_step(cuda.slow_args(gpu, base, (500.0, 550.0, 300.0), dt_large=3.0, coriolis_f=1e-4,
+                                           outputs=outs)))
+    o32.slow_rk2_step(cpu, base, (500.0, 550.0, 300.0), 3.0, coriolis_f=1e-4)
+    for k in ("u", "v", "w", "p"):
+        assert_bitwise(gpu[k], cpu[k], k)
+
+
+@pytest.mark.parametrize("dom", ["cgrid", "full"])
+def test_kessler_tendencies_match_reference(ctx, dom):
+    g = np.load("tests/golden/kessler_eos.npz")
+    st = _state(g)
+    outs = tuple(np.zeros_like(st["theta"]) for _ in range(4))
+    ctx.check(ctx.kessler_tendencies(cuda.kessler_args(st, float(g["dz"]), float(g["dt"]), tuple(g["dom_" + dom]),
+                                                       outputs=outs)))
+    for key, arr in zip(("dtheta", "dqv", "dqc", "dqr"), outs):
+        assert_bitwise(arr, g[f"{dom}_{key}"], key)
+
+
+def test_kessler_step_matches_oracle(ctx, o32):
+    case = Case(33, 27, 31, 700.0, 800.0, 350.0, 4.0, seed=21)
+    st, _ = cloudy_state(case, seed=21)
+    gpu = {k: v.copy() for k, v in st.items()}
+    cpu = {k: v.copy() for k, v in st.items()}
+    outs = tuple(np.zeros_like(st["theta"]) for _ in range(4))
+    ctx.check(ctx.kessler_step(cuda.kessler_args(gpu, 350.0, 4.0, outputs=outs)))
+    want = o32.kessler_step(cpu, 350.0, 4.0, cuda.cgrid_cell_domain(*case.shape))
+    for key, a, b in zip(("dtheta", "dqv", "dqc", "dqr"), outs, want):
+        assert_bitwise(a, b, key)
+    for k in ("theta", "qv", "qc", "qr"):
+        assert_bitwise(gpu[k], cpu[k], k)
+    # the step form without tendency outputs gives the same state
+    again = {k: v.copy() for k, v in st.items()}
+    ctx.check(ctx.kessler_step(cuda.kessler_args(again, 350.0, 4.0)))
+    for k in ("theta", "qv", "qc", "qr"):
+        assert_bitwise(again[k], cpu[k], k)
+
+
+def test_eos_projection_matches_reference(ctx):
+    g = np.load("tests/golden/kessler_eos.npz")
+    st = _state(g)
+    p = st["p"].copy()
+    ctx.check(ctx.eos_projection(cuda.eos_args(p, st["rho"], st["theta"])))
+    assert_bitwise(p, g["eos_p_dry"], "dry")
+    p = st["p"].copy()
+    ctx.check(ctx.eos_projection(cuda.eos_args(p, st["rho"], st["theta"], st["qv"], st["qc"], st["qr"])))
+    assert_bitwise(p, g["eos_p_moist"], "moist")
+
+
+# (field, cell, value, refused when dry, refused when moist), as pinned against
+# the reference in tests/test_oracle.py.
+EOS_CASES = [
+    ("rho", (3, 3, 3), -1.0, True, True),
+    ("theta", (0, 0, 0), np.nan, True, True),
+    ("qv", (3, 3, 3), -1e-6, False, True),
+    ("qv", (0, 3, 3), -1e-6, False, False),
+    ("qc", (2, 2, 0), -1e-3, False, True),
+    ("p", (4, 4, 4), 0.0, False, True),
+]
+
+
+@pytest.mark.parametrize("field,cell,value,dry_refused,moist_refused", EOS_CASES)
+def test_eos_refusal_matches_oracle(ctx, o32, field, cell, value, dry_refused, moist_refused):
+    case = Case(9, 7, 6, 1000.0, 1000.0, 500.0, 6.0, seed=1)
+    st, _ = cloudy_state(case, seed=3)
+    st[field][cell] = value
+    for moist, refused in ((False, dry_refused), (True, moist_refused)):
+        q = (st["qv"], st["qc"], st["qr"]) if moist else (None, None, None)
+        gpu, cpu = st["p"].copy(), st["p"].copy()
+        rc = ctx.eos_projection(cuda.eos_args(gpu, st["rho"], st["theta"], *q))
+        assert o32.eos_projection(cpu, st["rho"], st["theta"], *q) == (not refused)
+        assert rc == (4 if refused else 0), ctx.last_error
+        assert_bitwise(gpu, cpu, f"{field} moist={moist}")
+
+
+def test_eos_device_refusal_keeps_pressure(ctx):
+    """Device memory: a refused projection publishes nothing and the refusal
+    surfaces at synchronize."""
+    import torch
+    case = Case(12, 10, 8, 1000.0, 1000.0, 500.0, 6.0, seed=1)
+    st, _ = cloudy_state(case, seed=4)
+    st["rho"][5, 5, 5] = np.nan
+    dev = {k: torch.from_numpy(st[k]).cuda() for k in ("p", "rho", "theta")}
+    torch.cuda.synchronize()
+    args = cuda.eos_args(dev["p"], dev["rho"], dev["theta"], memory=cuda.MEMORY_DEVICE, stream=ctx.stream)
+    ctx.check(ctx.eos_projection(args))
+    assert ctx.lib.nimbus_cuda_synchronize(ctx.handle) == 4
+    assert_bitwise(dev["p"].cpu().numpy(), st["p"], "p")
+    # a clean state publishes afterwards
+    st["rho"][5, 5, 5] = 1.0
+    dev["rho"].copy_(torch.from_numpy(st["rho"]))
+    torch.cuda.synchronize()
+    ctx.check(ctx.eos_projection(args))
+    ctx.synchronize()
+    want = st["p"].copy()
+    oracle.Restatement("f32").eos_projection(want, st["rho"], st["theta"])
+    assert_bitwise(dev["p"].cpu().numpy(), want, "p")
