@@ -436,6 +436,101 @@ typedef struct nimbus_eos_args
 
 nimbus_status nimbus_cuda_eos_projection(nimbus_cuda_context* ctx, const nimbus_eos_args* a);
 
+/*
+ * Acoustic boundary closure on its own: CartesianCGridBCScheme::apply_acoustic
+ * (boundary_conditions_cartesian_cgrid.cpp:141-236) with the lateral faces in
+ * the order W, E, S, N and then the vertical closure.  dt_small == 0 only
+ * refreshes the ghosts (the closure the split stepper runs before seeding the
+ * KW78 history, dynamics.cpp:5384-5396); dt_small > 0 also integrates the
+ * radiative faces against wave_history (2*(nx+ny)*nz floats, the layout of
+ * nimbus_acoustic_batched_args).  Device memory only.
+ */
+typedef struct nimbus_boundary_args
+{
+    float *u, *v, *w, *rho, *p;
+    float* wave_history;     /* required when dt_small > 0 and a face is radiative */
+    int nx, ny, nz;
+    double dx, dy;
+    double dt_small;
+    int bc_west, bc_east, bc_south, bc_north, bc_bottom, bc_top;
+    float frame_velocity_u_ms, frame_velocity_v_ms;
+    void* stream;
+} nimbus_boundary_args;
+
+nimbus_status nimbus_cuda_acoustic_boundaries(nimbus_cuda_context* ctx, const nimbus_boundary_args* a);
+
+/*
+ * Member engine: many runs (ensemble members, served requests) resident in
+ * HBM and advanced together, each large step of every member in one batched
+ * launch per phase.  No counterpart in the reference, which advances one run
+ * per process; each member's arithmetic is exactly that of the per-operation
+ * entry points above (same kernels, same order), so a member's result does
+ * not depend on which other members share the launch.
+ *
+ * One large step of a member (the order of step_dynamics_new,
+ * dynamics.cpp:5123-7317, for the phases this backend owns):
+ *   Heun slow step; boundary refresh and KW78 seed; n_substeps acoustic
+ *   substeps (retained mass flux, continuity + EOS, momentum, boundaries);
+ *   conservative WENO5 transport of theta, qv, qc, qr; Kessler tendencies and
+ *   their application (microphysics == 1); EOS pressure re-projection.
+ * Members may differ in grid, spacing, dt and substep count.
+ */
+typedef struct nimbus_engine nimbus_engine;
+
+typedef struct nimbus_member_desc
+{
+    int nx, ny, nz;
+    double dx, dy, dz;
+    double dt;               /* large step */
+    int n_substeps;          /* acoustic substeps per large step, >= 1 */
+    int bc[6];               /* west, east, south, north, bottom, top */
+    double coriolis_f;
+    float frame_velocity_u_ms, frame_velocity_v_ms;
+    int microphysics;        /* 0 none, 1 Kessler */
+    /* FP64 base profiles of length nz in host memory (copied at admission) */
+    const double* rho0_base;
+    const double* p0_base;
+    const double* qv0_base;
+    const double* u0_base;   /* may be null: zero */
+    const double* v0_base;   /* may be null: zero */
+} nimbus_member_desc;
+
+/* Host arrays [nx][ny][nz] of one member's prognostic state. */
+typedef struct nimbus_member_state
+{
+    float *u, *v, *w, *rho, *p, *theta, *qv, *qc, *qr;
+} nimbus_member_state;
+
+nimbus_status nimbus_cuda_engine_create(nimbus_cuda_context* ctx, nimbus_engine** out);
+void nimbus_cuda_engine_destroy(nimbus_engine* e);
+/* Device bytes one member of this shape holds while resident. */
+size_t nimbus_cuda_engine_member_bytes(const nimbus_member_desc* desc);
+/* Admits a member with its initial state when its footprint plus
+ * reserve_bytes fits the free HBM (cudaMemGetInfo); otherwise returns
+ * NIMBUS_ERR_OUT_OF_MEMORY and changes nothing.  Waits for enqueued steps. */
+nimbus_status nimbus_cuda_engine_admit(nimbus_engine* e, const nimbus_member_desc* desc,
+                                       const nimbus_member_state* initial, size_t reserve_bytes, int* member_id);
+/* Frees a member's device memory (waits for enqueued steps). */
+nimbus_status nimbus_cuda_engine_retire(nimbus_engine* e, int member_id);
+/* Copies a member's current state to host arrays (waits for enqueued steps). */
+nimbus_status nimbus_cuda_engine_read(nimbus_engine* e, int member_id, const nimbus_member_state* out);
+/* Replaces a member's state with host arrays (waits for enqueued steps). */
+nimbus_status nimbus_cuda_engine_write(nimbus_engine* e, int member_id, const nimbus_member_state* in);
+/* Enqueues n_steps large steps of every resident member on the context's
+ * stream: replayed from a CUDA graph when graphs are on (the default), the
+ * graph rebuilt after admissions, retirements or a precision change. */
+nimbus_status nimbus_cuda_engine_step(nimbus_engine* e, int n_steps);
+/* Waits for the enqueued steps; NIMBUS_ERR_NONFINITE when a retained mass
+ * flux or transported scalar went non-finite or the EOS projection refused. */
+nimbus_status nimbus_cuda_engine_synchronize(nimbus_engine* e);
+/* A member's status bits (1 non-finite mass flux, 2 non-finite transported
+ * scalar, 4 EOS projection refused); waits for enqueued steps. */
+nimbus_status nimbus_cuda_engine_member_status(nimbus_engine* e, int member_id, unsigned* flags);
+nimbus_status nimbus_cuda_engine_set_graph(nimbus_engine* e, int enable);
+int nimbus_cuda_engine_members(const nimbus_engine* e);
+/* Kernel launches one large step enqueues (batched over all members). */
+int nimbus_cuda_engine_launches_per_step(const nimbus_engine* e);
+
 #ifdef __cplusplus
 }
 #endif

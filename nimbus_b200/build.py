@@ -40,7 +40,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     if out.exists() and not force and out.stat().st_mtime >= newest:
         return out
     cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-           str(CSRC / "nimbus_cuda.cu"), "-o", str(out)]
+           "--threads", "2", *[str(p) for p in sorted(CSRC.glob("*.cu"))], "-o", str(out)]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
         print(" ".join(cmd))

@@ -106,7 +106,7 @@ struct FusedSmem
 };
 
 template <int TJ, int BLOCK, class Policy>
-__global__ void __launch_bounds__(BLOCK, 3) acoustic_substep_fused_kernel(
+static __global__ void __launch_bounds__(BLOCK, 3) acoustic_substep_fused_kernel(
     FusedParams P, const float* __restrict__ rho_in, const float* __restrict__ u_in, const float* __restrict__ v_in,
     const float* __restrict__ w_in, const float* __restrict__ theta, const double* __restrict__ rho0,
     const double* __restrict__ p0, const float2* __restrict__ dp0_split, float* __restrict__ drho_out,

@@ -37,7 +37,7 @@ struct AcousticParams
 
 // Pass 1+2 of acoustic_cgrid_fast.cpp:47-157 and the Host-precision flux
 // accumulation of advection_cartesian.cpp:743-849 (cartesian_mass_flux.hpp:57-75,381-393).
-__global__ void __launch_bounds__(256) acoustic_continuity_eos_kernel(
+static __global__ void __launch_bounds__(256) acoustic_continuity_eos_kernel(
     AcousticParams P, const float* __restrict__ rho, const float* __restrict__ u, const float* __restrict__ v,
     const float* __restrict__ w, const float* __restrict__ theta, const double* __restrict__ rho0,
     float* __restrict__ rho_out, float* __restrict__ p_out, float* __restrict__ drho_out,
@@ -116,7 +116,7 @@ __global__ void __launch_bounds__(256) acoustic_continuity_eos_kernel(
 }
 
 // Pass 3 of acoustic_cgrid_fast.cpp:159-215, in place on u,v,w.
-__global__ void __launch_bounds__(256) acoustic_momentum_kernel(
+static __global__ void __launch_bounds__(256) acoustic_momentum_kernel(
     AcousticParams P, const float* __restrict__ rho, const float* __restrict__ p, const double* __restrict__ p0,
     float* __restrict__ u, float* __restrict__ v, float* __restrict__ w)
 {
@@ -166,15 +166,13 @@ __device__ __forceinline__ float kw78_updated_face(float previous, float phase, 
     return __fsub_rn(previous, increment);
 }
 
-// West then east faces for one (j,k) row: boundary_conditions_cartesian_cgrid.cpp:927-1032.
-__global__ void acoustic_bc_we_kernel(BoundaryParams B, float* __restrict__ u, float* __restrict__ v,
-                                      float* __restrict__ w, float* __restrict__ rho, float* __restrict__ p,
-                                      float* __restrict__ u_west, float* __restrict__ u_east)
+// West then east faces for one (j,k) row r: boundary_conditions_cartesian_cgrid.cpp:927-1032.
+__device__ __forceinline__ void bc_we_row(const BoundaryParams& B, float* __restrict__ u, float* __restrict__ v,
+                                          float* __restrict__ w, float* __restrict__ rho, float* __restrict__ p,
+                                          float* __restrict__ u_west, float* __restrict__ u_east, int r)
 {
     const Dims d = B.d;
-    const int rows = d.ny * d.nz;
     const bool radiate = B.dt_rad > 0.0f;
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x)
     {
         const int j = r / d.nz, k = r % d.nz;
         // ---- West: ghost i=0, wall face u[0] ----
@@ -234,15 +232,22 @@ __global__ void acoustic_bc_we_kernel(BoundaryParams B, float* __restrict__ u, f
     }
 }
 
-// South then north faces for one (i,k) row: boundary_conditions_cartesian_cgrid.cpp:1034-1121.
-__global__ void acoustic_bc_sn_kernel(BoundaryParams B, float* __restrict__ u, float* __restrict__ v,
+static __global__ void acoustic_bc_we_kernel(BoundaryParams B, float* __restrict__ u, float* __restrict__ v,
                                       float* __restrict__ w, float* __restrict__ rho, float* __restrict__ p,
-                                      float* __restrict__ v_south, float* __restrict__ v_north)
+                                      float* __restrict__ u_west, float* __restrict__ u_east)
+{
+    const int rows = B.d.ny * B.d.nz;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x)
+        bc_we_row(B, u, v, w, rho, p, u_west, u_east, r);
+}
+
+// South then north faces for one (i,k) row r: boundary_conditions_cartesian_cgrid.cpp:1034-1121.
+__device__ __forceinline__ void bc_sn_row(const BoundaryParams& B, float* __restrict__ u, float* __restrict__ v,
+                                          float* __restrict__ w, float* __restrict__ rho, float* __restrict__ p,
+                                          float* __restrict__ v_south, float* __restrict__ v_north, int r)
 {
     const Dims d = B.d;
-    const int rows = d.nx * d.nz;
     const bool radiate = B.dt_rad > 0.0f;
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x)
     {
         const int i = r / d.nz, k = r % d.nz;
         {
@@ -300,13 +305,20 @@ __global__ void acoustic_bc_sn_kernel(BoundaryParams B, float* __restrict__ u, f
     }
 }
 
+static __global__ void acoustic_bc_sn_kernel(BoundaryParams B, float* __restrict__ u, float* __restrict__ v,
+                                      float* __restrict__ w, float* __restrict__ rho, float* __restrict__ p,
+                                      float* __restrict__ v_south, float* __restrict__ v_north)
+{
+    const int rows = B.d.nx * B.d.nz;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x)
+        bc_sn_row(B, u, v, w, rho, p, v_south, v_north, r);
+}
+
 // Vertical closure for one (i,j) column: boundary_conditions_cartesian_cgrid.cpp:1124-1175.
-__global__ void acoustic_bc_vertical_kernel(BoundaryParams B, float* __restrict__ u, float* __restrict__ v,
-                                            float* __restrict__ w)
+__device__ __forceinline__ void bc_vertical_column(const BoundaryParams& B, float* __restrict__ u,
+                                                   float* __restrict__ v, float* __restrict__ w, int col)
 {
     const Dims d = B.d;
-    const int cols = d.nx * d.ny;
-    for (int col = blockIdx.x * blockDim.x + threadIdx.x; col < cols; col += gridDim.x * blockDim.x)
     {
         const int base = col * d.nz;
         if (B.bottom == kBottomNoSlip)
@@ -321,12 +333,20 @@ __global__ void acoustic_bc_vertical_kernel(BoundaryParams B, float* __restrict_
     }
 }
 
-// seed_radiative_state (boundary_conditions_cartesian_cgrid.cpp:798-822).
-__global__ void acoustic_seed_radiation_kernel(Dims d, const float* __restrict__ u, const float* __restrict__ v,
-                                               float* __restrict__ wave)
+static __global__ void acoustic_bc_vertical_kernel(BoundaryParams B, float* __restrict__ u, float* __restrict__ v,
+                                            float* __restrict__ w)
+{
+    const int cols = B.d.nx * B.d.ny;
+    for (int col = blockIdx.x * blockDim.x + threadIdx.x; col < cols; col += gridDim.x * blockDim.x)
+        bc_vertical_column(B, u, v, w, col);
+}
+
+// seed_radiative_state (boundary_conditions_cartesian_cgrid.cpp:798-822) for
+// history slot r of the west/east (r < ny*nz) and south/north rows.
+__device__ __forceinline__ void seed_radiation_row(const Dims& d, const float* __restrict__ u,
+                                                   const float* __restrict__ v, float* __restrict__ wave, int r)
 {
     const int yz = d.ny * d.nz, xz = d.nx * d.nz;
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < yz + xz; r += gridDim.x * blockDim.x)
     {
         if (r < yz)
         {
@@ -342,6 +362,14 @@ __global__ void acoustic_seed_radiation_kernel(Dims d, const float* __restrict__
             wave[2 * yz + xz + q] = v[d.at(i, d.ny - 2, k)];
         }
     }
+}
+
+static __global__ void acoustic_seed_radiation_kernel(Dims d, const float* __restrict__ u, const float* __restrict__ v,
+                                               float* __restrict__ wave)
+{
+    const int rows = d.ny * d.nz + d.nx * d.nz;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x)
+        seed_radiation_row(d, u, v, wave, r);
 }
 
 }  // namespace nimbus

@@ -17,40 +17,65 @@
 namespace nimbus
 {
 
+// First substep of a large step writes the retained flux instead of adding to
+// it: float(0.0 + w*flux) is bit-identical to accumulating into a zeroed slot
+// (the +0.0 turns a -0.0 product into +0.0 exactly as the add would).
+__device__ __forceinline__ void fused_store(float* slot, double weight, double flux, unsigned& flags)
+{
+    const float st = (float)(0.0 + weight * flux);
+    if (isfinite(st)) *slot = st;
+    else
+    {
+        *slot = 0.0f;
+        flags |= kStatusNonfiniteMassFlux;
+    }
+}
+
+__device__ __forceinline__ void retain_flux(float* slot, double weight, double flux, unsigned& flags, bool store)
+{
+    if (store) fused_store(slot, weight, flux, flags);
+    else fused_accumulate(slot, weight, flux, flags);
+}
+
+// Continuity, rho forward Euler and EOS for cell c.  With store_flux the
+// retained fluxes are written rather than accumulated and rho_copy (when
+// given) receives the pre-substep density (the transport context's
+// beginning density).
 template <class Policy>
-__global__ void __launch_bounds__(256) split_continuity_eos_kernel(
-    FusedParams P, const float* __restrict__ rho, const float* __restrict__ u, const float* __restrict__ v,
-    const float* __restrict__ w, const float* __restrict__ theta, const double* __restrict__ rho0,
-    float* __restrict__ rho_out, float* __restrict__ p_out, float* __restrict__ drho_out, float* __restrict__ mfx,
-    float* __restrict__ mfy, float* __restrict__ mfz, unsigned* __restrict__ status)
+__device__ __forceinline__ void continuity_eos_cell(const FusedParams& P, const float* __restrict__ rho,
+                                                    const float* __restrict__ u, const float* __restrict__ v,
+                                                    const float* __restrict__ w, const float* __restrict__ theta,
+                                                    const double* __restrict__ rho0, float* __restrict__ rho_out,
+                                                    float* __restrict__ p_out, float* __restrict__ drho_out,
+                                                    float* __restrict__ mfx, float* __restrict__ mfy,
+                                                    float* __restrict__ mfz, int c, unsigned& flags, bool store_flux,
+                                                    float* __restrict__ rho_copy)
 {
     using real = typename Policy::real;
     const Dims d = P.d;
-    const int n = d.cells();
     const int sx = d.sx(), sy = d.sy();
-    unsigned flags = 0;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
     {
         int i, j, k;
         decompose(d, c, i, j, k);
         const float rho_c = rho[c];
+        if (rho_copy != nullptr) rho_copy[c] = rho_c;
         if (mfx != nullptr)
         {
             if constexpr (sizeof(real) == 8)
             {
                 const double rc = (double)rho_c;
-                if (i < d.nx - 1) fused_accumulate(mfx + c, P.weight, 0.5 * (rc + (double)rho[c + sx]) * ((double)u[c] - P.frame_u), flags);
-                if (j < d.ny - 1) fused_accumulate(mfy + c, P.weight, 0.5 * (rc + (double)rho[c + sy]) * ((double)v[c] - P.frame_v), flags);
+                if (i < d.nx - 1) retain_flux(mfx + c, P.weight, 0.5 * (rc + (double)rho[c + sx]) * ((double)u[c] - P.frame_u), flags, store_flux);
+                if (j < d.ny - 1) retain_flux(mfy + c, P.weight, 0.5 * (rc + (double)rho[c + sy]) * ((double)v[c] - P.frame_v), flags, store_flux);
                 const double zf = (k == d.nz - 1) ? (P.top_open ? rc * (double)w[c] : 0.0)
                                                   : 0.5 * (rc + (double)rho[c + 1]) * (double)w[c];
-                fused_accumulate(mfz + c, P.weight, zf, flags);
+                retain_flux(mfz + c, P.weight, zf, flags, store_flux);
             }
             else
             {
-                if (i < d.nx - 1) fused_accumulate(mfx + c, P.weight, (double)(0.5f * (rho_c + rho[c + sx]) * (u[c] - (float)P.frame_u)), flags);
-                if (j < d.ny - 1) fused_accumulate(mfy + c, P.weight, (double)(0.5f * (rho_c + rho[c + sy]) * (v[c] - (float)P.frame_v)), flags);
+                if (i < d.nx - 1) retain_flux(mfx + c, P.weight, (double)(0.5f * (rho_c + rho[c + sx]) * (u[c] - (float)P.frame_u)), flags, store_flux);
+                if (j < d.ny - 1) retain_flux(mfy + c, P.weight, (double)(0.5f * (rho_c + rho[c + sy]) * (v[c] - (float)P.frame_v)), flags, store_flux);
                 const float zf = (k == d.nz - 1) ? (P.top_open ? rho_c * w[c] : 0.0f) : 0.5f * (rho_c + rho[c + 1]) * w[c];
-                fused_accumulate(mfz + c, P.weight, (double)zf, flags);
+                retain_flux(mfz + c, P.weight, (double)zf, flags, store_flux);
             }
         }
         double drho = 0.0;
@@ -87,20 +112,34 @@ __global__ void __launch_bounds__(256) split_continuity_eos_kernel(
         if (!isfinite(p_new) || p_new <= 0.0) p_new = (double)P.p_ref_fallback;
         p_out[c] = clamp_value((float)p_new, 101325.0f, P.p_min, P.p_max);
     }
-    if (flags) atomicOr(status, flags);
 }
 
 template <class Policy>
-__global__ void __launch_bounds__(256) split_momentum_kernel(
-    FusedParams P, const float* __restrict__ rho, const float* __restrict__ p, const double* __restrict__ p0,
-    const float2* __restrict__ dp0_split, const float* __restrict__ u, const float* __restrict__ v,
-    const float* __restrict__ w, float* __restrict__ u_out, float* __restrict__ v_out, float* __restrict__ w_out)
+static __global__ void __launch_bounds__(256) split_continuity_eos_kernel(
+    FusedParams P, const float* __restrict__ rho, const float* __restrict__ u, const float* __restrict__ v,
+    const float* __restrict__ w, const float* __restrict__ theta, const double* __restrict__ rho0,
+    float* __restrict__ rho_out, float* __restrict__ p_out, float* __restrict__ drho_out, float* __restrict__ mfx,
+    float* __restrict__ mfy, float* __restrict__ mfz, unsigned* __restrict__ status)
+{
+    const int n = P.d.cells();
+    unsigned flags = 0;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+        continuity_eos_cell<Policy>(P, rho, u, v, w, theta, rho0, rho_out, p_out, drho_out, mfx, mfy, mfz, c, flags,
+                                    false, nullptr);
+    if (flags) atomicOr(status, flags);
+}
+
+// Momentum forward Euler for the faces of cell c.  Face c reads only its own
+// old velocity, so u_out may alias u (in-place update).
+template <class Policy>
+__device__ __forceinline__ void momentum_cell(const FusedParams& P, const float* __restrict__ rho,
+                                              const float* __restrict__ p, const double* __restrict__ p0,
+                                              const float2* __restrict__ dp0_split, const float* u, const float* v,
+                                              const float* w, float* u_out, float* v_out, float* w_out, int c)
 {
     using real = typename Policy::real;
     const Dims d = P.d;
-    const int n = d.cells();
     const int sx = d.sx(), sy = d.sy();
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
     {
         int i, j, k;
         decompose(d, c, i, j, k);
@@ -153,6 +192,17 @@ __global__ void __launch_bounds__(256) split_momentum_kernel(
             w_out[c] = clamp_value(__fmaf_rn(dw, dt, w[c]), 0.0f, -P.wind_v, P.wind_v);
         }
     }
+}
+
+template <class Policy>
+static __global__ void __launch_bounds__(256) split_momentum_kernel(
+    FusedParams P, const float* __restrict__ rho, const float* __restrict__ p, const double* __restrict__ p0,
+    const float2* __restrict__ dp0_split, const float* __restrict__ u, const float* __restrict__ v,
+    const float* __restrict__ w, float* __restrict__ u_out, float* __restrict__ v_out, float* __restrict__ w_out)
+{
+    const int n = P.d.cells();
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+        momentum_cell<Policy>(P, rho, p, p0, dp0_split, u, v, w, u_out, v_out, w_out, c);
 }
 
 }  // namespace nimbus

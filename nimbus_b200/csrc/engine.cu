@@ -1,0 +1,693 @@
+// Member engine (include/nimbus_cuda.h): resident runs advanced together, one
+// batched launch per phase of the large step, replayed from a CUDA graph.
+//
+// Host bookkeeping.  Each member owns one device arena (state, retained
+// transport context, scratch, profiles, status word).  The device member
+// table is the authority for the ping-pong pointers (the swap kernels rotate
+// them on the device every step), so any host-side change to the membership
+// first waits for the stream and reads the table back.  The table is kept
+// sorted by substep count, descending, so the members still inside their
+// acoustic loop at substep s are a prefix of it.
+#include "../../include/nimbus_cuda.h"
+#include "context.cuh"
+#include "engine_kernels.cuh"
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <vector>
+
+using namespace nimbus;
+using namespace nimbus_host;
+
+namespace
+{
+
+constexpr int kEngineBlock = 256;
+constexpr size_t kAlign = 256;
+
+struct MemberSlot
+{
+    int id;
+    nimbus_member_desc desc;  // profile pointers cleared after admission
+    void* arena = nullptr;
+    size_t bytes = 0;
+    EngineMember m;           // host view of the device entry (refreshed before use)
+};
+
+size_t align_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
+
+// Byte layout of one member's arena.
+struct ArenaLayout
+{
+    size_t cells, history;
+    size_t off_state, off_ctxt, off_wave, off_sf, off_rl, off_k1, off_xs, off_eos, off_status, off_prof, off_dp0,
+        total;
+};
+
+ArenaLayout arena_layout(const nimbus_member_desc* d)
+{
+    ArenaLayout L{};
+    L.cells = static_cast<size_t>(d->nx) * d->ny * d->nz;
+    L.history = 2 * (static_cast<size_t>(d->nx) + d->ny) * d->nz;
+    const size_t field = align_up(L.cells * sizeof(float));
+    size_t off = 0;
+    L.off_state = off;  off += 11 * field;                  // u v w rho rho_alt p theta qv qc qr qr_alt
+    L.off_ctxt = off;   off += 4 * field;                   // rho_begin mfx mfy mfz
+    L.off_wave = off;   off += align_up(L.history * sizeof(float));
+    L.off_sf = off;     off += align_up(3 * kEngineScalars * L.cells * sizeof(float));
+    L.off_rl = off;     off += align_up(kEngineScalars * L.cells * sizeof(float));
+    L.off_k1 = off;     off += align_up(4 * L.cells * sizeof(float));
+    L.off_xs = off;     off += align_up(4 * L.cells * sizeof(float));
+    L.off_eos = off;    off += field;
+    L.off_status = off; off += kAlign;
+    L.off_prof = off;   off += align_up(5 * static_cast<size_t>(d->nz) * sizeof(double));
+    L.off_dp0 = off;    off += align_up(static_cast<size_t>(d->nz) * sizeof(float2));
+    L.total = off;
+    return L;
+}
+
+const char* check_desc(const nimbus_member_desc* d)
+{
+    if (d->nx < 4 || d->ny < 4 || d->nz < 2) return "member grid must be at least 4x4x2";
+    if (!cells_fit(d->nx, d->ny, d->nz)) return "member grid too large";
+    if (!finite_positive(d->dx) || !finite_positive(d->dy) || !finite_positive(d->dz) || !finite_positive(d->dt))
+        return "spacing and dt must be finite and positive";
+    if (d->n_substeps < 1 || d->n_substeps > 4096) return "n_substeps must be in [1, 4096]";
+    for (int a = 0; a < 4; ++a)
+        if (d->bc[a] < 0 || d->bc[a] > 4) return "lateral boundary code out of range";
+    if (d->bc[4] < 0 || d->bc[4] > 1 || d->bc[5] < 0 || d->bc[5] > 2) return "vertical boundary code out of range";
+    if (!std::isfinite(d->coriolis_f) || !std::isfinite(d->frame_velocity_u_ms) ||
+        !std::isfinite(d->frame_velocity_v_ms))
+        return "coriolis_f and frame velocity must be finite";
+    if (d->microphysics != 0 && d->microphysics != 1) return "microphysics must be 0 (none) or 1 (Kessler)";
+    if (!d->rho0_base || !d->p0_base || !d->qv0_base) return "rho0, p0 and qv0 base profiles are required";
+    return nullptr;
+}
+
+// Parameter blocks of one member: the values the per-operation entry points
+// receive from the reference-facing callers (dispatch constants of
+// dynamics.cpp:4560-4586 and field_bounds.hpp).
+void fill_params(EngineMember& M, const nimbus_member_desc* a)
+{
+    const double gamma = kCpd / (kCpd - kRd);
+    const double dt_small = a->dt / a->n_substeps;
+    FusedParams& F = M.F;
+    F = FusedParams{};
+    F.d = make_dims(a->nx, a->ny, a->nz);
+    F.inv_dx = 1.0 / a->dx;
+    F.inv_dy = 1.0 / a->dy;
+    F.inv_dz = 1.0 / a->dz;
+    F.dt_small = dt_small;
+    F.gamma = gamma;
+    F.rho_min = 0.05f;
+    F.rho_max = 2.0f;
+    F.p_min = 1000.0f;
+    F.p_max = 200000.0f;
+    F.p_ref_fallback = 100000.0f;
+    F.wind_h = 180.0f;
+    F.wind_v = 120.0f;
+    F.weight = dt_small / a->dt;
+    F.frame_u = a->frame_velocity_u_ms;
+    F.frame_v = a->frame_velocity_v_ms;
+    F.top_open = a->bc[5] == kTopOpen;
+    F.chunk = 1;
+
+    BoundaryParams& B = M.B;
+    B = BoundaryParams{};
+    B.d = F.d;
+    B.west = a->bc[0]; B.east = a->bc[1]; B.south = a->bc[2]; B.north = a->bc[3];
+    B.bottom = a->bc[4]; B.top = a->bc[5];
+    B.dt_rad = static_cast<float>(dt_small);
+    B.inv_dx = 1.0f / static_cast<float>(a->dx);
+    B.inv_dy = 1.0f / static_cast<float>(a->dy);
+    B.frame_u = a->frame_velocity_u_ms;
+    B.frame_v = a->frame_velocity_v_ms;
+
+    TransportParams& T = M.T;
+    T = TransportParams{};
+    T.d = F.d;
+    T.inv_dx = 1.0 / a->dx;
+    T.inv_dy = 1.0 / a->dy;
+    T.inv_dz = 1.0 / a->dz;
+    T.dt = a->dt;
+    T.rho_floor = static_cast<double>(0.05f);
+    T.weno = 1;
+    T.top_open = a->bc[5] == kTopOpen;
+    T.n_scalars = kEngineScalars;
+    T.positive_definite[0] = 0;  // theta (advection_batch.cpp:742-745)
+    for (int s = 1; s < kEngineScalars; ++s) T.positive_definite[s] = 1;
+
+    SlowParams& S = M.S;
+    S = SlowParams{};
+    S.d = F.d;
+    S.inv_dx = 1.0 / a->dx;
+    S.inv_dy = 1.0 / a->dy;
+    S.inv_dz = 1.0 / a->dz;
+    S.dt = a->dt;
+    S.coriolis_f = a->coriolis_f;
+    S.frame_u = a->frame_velocity_u_ms;
+    S.frame_v = a->frame_velocity_v_ms;
+    S.gravity = 9.81;
+    S.moist = 1;
+    S.loading = 1;
+
+    KesslerParams& K = M.K;
+    K = KesslerParams{};
+    K.d = F.d;
+    K.dz = a->dz;
+    K.dt = a->dt;
+    K.i0 = 1; K.i1 = a->nx - 1;  // physical_scalar_domain of the C-grid
+    K.j0 = 1; K.j1 = a->ny - 1;
+    K.k0 = 0; K.k1 = a->nz;
+    K.qc0 = 1.0e-3;
+    K.c_auto = 1.0e-3;
+    K.c_accr = 2.2;
+    K.evap_eff = 1.0;
+    K.vt_max = 20.0;
+
+    M.gamma = gamma;
+    M.n_substeps = a->n_substeps;
+    M.microphysics = a->microphysics;
+    M.items[kItemCells] = a->nx * a->ny * a->nz;
+    M.items[kItemRowsWE] = a->ny * a->nz;
+    M.items[kItemRowsSN] = a->nx * a->nz;
+    M.items[kItemColumns] = a->nx * a->ny;
+    M.items[kItemHistory] = (a->ny + a->nx) * a->nz;
+}
+
+}  // namespace
+
+struct nimbus_engine
+{
+    nimbus_cuda_context* ctx = nullptr;
+    std::vector<MemberSlot> slots;  // admission order
+    std::vector<int> order;         // slot indices in table order
+    int next_id = 1;
+    bool dirty = true;              // table / graph need a rebuild
+    bool table_current = true;      // host views match the device table
+    bool use_graph = true;
+    int built_precision = -1;
+    EngineMember* d_table = nullptr;
+    size_t table_cap = 0;
+    long long* d_prefix = nullptr;
+    size_t prefix_cap = 0;
+    std::vector<long long> prefix;  // [kItemKinds][members + 1]
+    std::vector<int> active;        // members inside the loop at substep s
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int launches_per_step = 0;
+    std::map<const void*, int> occupancy;
+};
+
+namespace
+{
+
+int blocks_per_sm(nimbus_engine* e, const void* kernel)
+{
+    auto it = e->occupancy.find(kernel);
+    if (it != e->occupancy.end()) return it->second;
+    int blocks = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, kEngineBlock, 0) != cudaSuccess || blocks < 1)
+        blocks = 1;
+    e->occupancy[kernel] = blocks;
+    return blocks;
+}
+
+// Persistent grid: one wave of resident CTAs, never more blocks than tiles.
+unsigned engine_grid(nimbus_engine* e, const void* kernel, long long tiles)
+{
+    const long long wave = static_cast<long long>(e->ctx->sm_count) * blocks_per_sm(e, kernel);
+    const long long g = tiles < wave ? tiles : wave;
+    return static_cast<unsigned>(g < 1 ? 1 : g);
+}
+
+const long long* prefix_of(const nimbus_engine* e, int kind)
+{
+    return e->d_prefix + static_cast<size_t>(kind) * (e->order.size() + 1);
+}
+
+long long tiles_of(const nimbus_engine* e, int kind, int members)
+{
+    return e->prefix[static_cast<size_t>(kind) * (e->order.size() + 1) + members];
+}
+
+nimbus_status sync_table_to_host(nimbus_engine* e)
+{
+    nimbus_cuda_context* ctx = e->ctx;
+    NB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (e->table_current || e->order.empty()) return NIMBUS_OK;
+    std::vector<EngineMember> host(e->order.size());
+    NB_CUDA(ctx, cudaMemcpy(host.data(), e->d_table, sizeof(EngineMember) * host.size(), cudaMemcpyDeviceToHost));
+    for (size_t r = 0; r < e->order.size(); ++r) e->slots[e->order[r]].m = host[r];
+    e->table_current = true;
+    return NIMBUS_OK;
+}
+
+nimbus_status rebuild_table(nimbus_engine* e)
+{
+    nimbus_cuda_context* ctx = e->ctx;
+    NB_TRY(sync_table_to_host(e));
+    const size_t n = e->slots.size();
+    e->order.resize(n);
+    for (size_t i = 0; i < n; ++i) e->order[i] = static_cast<int>(i);
+    std::stable_sort(e->order.begin(), e->order.end(), [&](int a, int b) {
+        return e->slots[a].desc.n_substeps > e->slots[b].desc.n_substeps;
+    });
+    if (n > e->table_cap)
+    {
+        if (e->d_table) cudaFree(e->d_table);
+        e->d_table = nullptr;
+        e->table_cap = 0;
+        const size_t cap = std::max<size_t>(n, 2 * e->table_cap + 8);
+        NB_CUDA(ctx, cudaMalloc(&e->d_table, sizeof(EngineMember) * cap));
+        e->table_cap = cap;
+    }
+    const size_t pre = static_cast<size_t>(kItemKinds) * (n + 1);
+    if (pre > e->prefix_cap)
+    {
+        if (e->d_prefix) cudaFree(e->d_prefix);
+        e->d_prefix = nullptr;
+        e->prefix_cap = 0;
+        NB_CUDA(ctx, cudaMalloc(&e->d_prefix, sizeof(long long) * (pre + 64)));
+        e->prefix_cap = pre + 64;
+    }
+    std::vector<EngineMember> host(n);
+    e->prefix.assign(pre, 0);
+    int max_n = 0;
+    for (size_t r = 0; r < n; ++r)
+    {
+        host[r] = e->slots[e->order[r]].m;
+        max_n = std::max(max_n, host[r].n_substeps);
+    }
+    for (int k = 0; k < kItemKinds; ++k)
+    {
+        long long* p = e->prefix.data() + static_cast<size_t>(k) * (n + 1);
+        p[0] = 0;
+        for (size_t r = 0; r < n; ++r) p[r + 1] = p[r] + (host[r].items[k] + kEngineBlock - 1) / kEngineBlock;
+    }
+    e->active.assign(max_n, 0);
+    for (int s = 0; s < max_n; ++s)
+    {
+        int a = 0;
+        while (a < static_cast<int>(n) && host[a].n_substeps > s) ++a;
+        e->active[s] = a;
+    }
+    if (n)
+    {
+        NB_CUDA(ctx, cudaMemcpy(e->d_table, host.data(), sizeof(EngineMember) * n, cudaMemcpyHostToDevice));
+        NB_CUDA(ctx, cudaMemcpy(e->d_prefix, e->prefix.data(), sizeof(long long) * pre, cudaMemcpyHostToDevice));
+    }
+    e->table_current = true;
+    if (e->exec)
+    {
+        cudaGraphExecDestroy(e->exec);
+        e->exec = nullptr;
+    }
+    if (e->graph)
+    {
+        cudaGraphDestroy(e->graph);
+        e->graph = nullptr;
+    }
+    e->dirty = false;
+    return NIMBUS_OK;
+}
+
+#define ENGINE_LAUNCH(family, kernel, tiles, gy, ...)                                                    \
+    do {                                                                                                 \
+        const long long tiles_ = (tiles);                                                                \
+        if (tiles_ > 0)                                                                                  \
+        {                                                                                                \
+            LaunchTimer t_(ctx, st, family);                                                             \
+            kernel<<<dim3(engine_grid(e, reinterpret_cast<const void*>(kernel), tiles_), gy), kEngineBlock, 0, \
+                     st>>>(__VA_ARGS__);                                                                 \
+            ++count;                                                                                     \
+        }                                                                                                \
+    } while (0)
+
+// Enqueues one large step of every member; returns the number of launches.
+template <class Policy, bool kFp32>
+int enqueue_step(nimbus_engine* e, cudaStream_t st)
+{
+    nimbus_cuda_context* ctx = e->ctx;
+    const int n = static_cast<int>(e->order.size());
+    int count = 0;
+    EngineMember* T = e->d_table;
+    const long long* pc = prefix_of(e, kItemCells);
+    const long long* pwe = prefix_of(e, kItemRowsWE);
+    const long long* psn = prefix_of(e, kItemRowsSN);
+    const long long* pcol = prefix_of(e, kItemColumns);
+    const long long* phist = prefix_of(e, kItemHistory);
+    const long long cells = tiles_of(e, kItemCells, n);
+
+    // Heun slow step (prepare_slow_rk2_tendencies + apply_slow_tendencies).
+    ENGINE_LAUNCH(NIMBUS_KERNEL_SLOW, engine_slow_predict_kernel<Policy>, cells, 1, T, pc, cells);
+    ENGINE_LAUNCH(NIMBUS_KERNEL_SLOW, engine_slow_correct_kernel<Policy>, cells, 1, T, pc, cells);
+    // seed_acoustic_radiation: apply_acoustic(0) then the KW78 seed.
+    ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_bc_we_kernel, tiles_of(e, kItemRowsWE, n), 1, T, pwe,
+                  tiles_of(e, kItemRowsWE, n), 0, 1);
+    ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_bc_sn_kernel, tiles_of(e, kItemRowsSN, n), 1, T, psn,
+                  tiles_of(e, kItemRowsSN, n), 0, 1);
+    ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_bc_vertical_kernel, tiles_of(e, kItemColumns, n), 1, T,
+                  pcol, tiles_of(e, kItemColumns, n));
+    ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_seed_kernel, tiles_of(e, kItemHistory, n), 1, T, phist,
+                  tiles_of(e, kItemHistory, n));
+    // The acoustic loop: members still inside it are a prefix of the table.
+    for (size_t s = 0; s < e->active.size(); ++s)
+    {
+        const int a = e->active[s];
+        const int si = static_cast<int>(s);
+        ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, engine_continuity_kernel<Policy>, tiles_of(e, kItemCells, a), 1,
+                      T, pc, tiles_of(e, kItemCells, a), si);
+        ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_MOMENTUM, engine_momentum_kernel<Policy>, tiles_of(e, kItemCells, a), 1,
+                      T, pc, tiles_of(e, kItemCells, a), si);
+        ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_bc_we_kernel, tiles_of(e, kItemRowsWE, a), 1, T, pwe,
+                      tiles_of(e, kItemRowsWE, a), si, 0);
+        ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_bc_sn_kernel, tiles_of(e, kItemRowsSN, a), 1, T, psn,
+                      tiles_of(e, kItemRowsSN, a), si, 0);
+        ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_bc_vertical_kernel, tiles_of(e, kItemColumns, a), 1, T,
+                      pcol, tiles_of(e, kItemColumns, a));
+    }
+    engine_swap_kernel<<<(n + 127) / 128, 128, 0, st>>>(T, n, 0);
+    ++count;
+    // Conservative transport of theta, qv, qc, qr against the retained fluxes.
+    ENGINE_LAUNCH(NIMBUS_KERNEL_TRANSPORT_FACES, engine_transport_faces_kernel<kFp32>, cells, kEngineScalars, T, pc,
+                  cells);
+    ENGINE_LAUNCH(NIMBUS_KERNEL_TRANSPORT_LIMITER, engine_transport_limiter_kernel, cells, kEngineScalars, T, pc,
+                  cells);
+    ENGINE_LAUNCH(NIMBUS_KERNEL_TRANSPORT_UPDATE, engine_transport_update_kernel, cells, kEngineScalars, T, pc,
+                  cells);
+    // Kessler step, then the EOS pressure re-projection.
+    ENGINE_LAUNCH(NIMBUS_KERNEL_MICROPHYSICS, engine_kessler_kernel, cells, 1, T, pc, cells);
+    engine_swap_kernel<<<(n + 127) / 128, 128, 0, st>>>(T, n, 1);
+    ++count;
+    ENGINE_LAUNCH(NIMBUS_KERNEL_MICROPHYSICS, engine_eos_kernel, cells, 1, T, pc, cells);
+    ENGINE_LAUNCH(NIMBUS_KERNEL_MICROPHYSICS, engine_eos_publish_kernel, cells, 1, T, pc, cells);
+    return count;
+}
+
+int enqueue(nimbus_engine* e, cudaStream_t st)
+{
+    if (e->ctx->precision == NIMBUS_PRECISION_FP32) return enqueue_step<Fp32Policy, true>(e, st);
+    return enqueue_step<RefPolicy, false>(e, st);
+}
+
+nimbus_status build_graph(nimbus_engine* e)
+{
+    nimbus_cuda_context* ctx = e->ctx;
+    cudaStream_t st = ctx->stream;
+    NB_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    const int launches = enqueue(e, st);
+    cudaGraph_t g = nullptr;
+    const cudaError_t end = cudaStreamEndCapture(st, &g);
+    if (end != cudaSuccess) return cuda_fail(ctx, end, "engine graph capture");
+    cudaGraphExec_t x = nullptr;
+    const cudaError_t inst = cudaGraphInstantiate(&x, g, 0);
+    if (inst != cudaSuccess)
+    {
+        cudaGraphDestroy(g);
+        return cuda_fail(ctx, inst, "engine graph instantiation");
+    }
+    e->graph = g;
+    e->exec = x;
+    e->launches_per_step = launches;
+    e->built_precision = ctx->precision;
+    return NIMBUS_OK;
+}
+
+void split_dp0(const double* p0, int nz, float2* out)
+{
+    for (int k = 0; k < nz; ++k)
+    {
+        const double dp = (k + 1 < nz) ? p0[k + 1] - p0[k] : 0.0;
+        const float hi = static_cast<float>(dp);
+        out[k] = make_float2(hi, static_cast<float>(dp - static_cast<double>(hi)));
+    }
+}
+
+MemberSlot* find_slot(nimbus_engine* e, int id, size_t* index = nullptr)
+{
+    for (size_t i = 0; i < e->slots.size(); ++i)
+        if (e->slots[i].id == id)
+        {
+            if (index) *index = i;
+            return &e->slots[i];
+        }
+    return nullptr;
+}
+
+const char* check_state(const nimbus_member_state* s)
+{
+    if (!s) return "state is null";
+    if (!s->u || !s->v || !s->w || !s->rho || !s->p || !s->theta || !s->qv || !s->qc || !s->qr)
+        return "a state array is null";
+    return nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+nimbus_status nimbus_cuda_engine_create(nimbus_cuda_context* ctx, nimbus_engine** out)
+{
+    if (!ctx || !out) return NIMBUS_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    auto* e = new (std::nothrow) nimbus_engine();
+    if (!e) return fail(ctx, NIMBUS_ERR_OUT_OF_MEMORY, "engine allocation failed");
+    e->ctx = ctx;
+    *out = e;
+    return NIMBUS_OK;
+}
+
+void nimbus_cuda_engine_destroy(nimbus_engine* e)
+{
+    if (!e) return;
+    cudaStreamSynchronize(e->ctx->stream);
+    if (e->exec) cudaGraphExecDestroy(e->exec);
+    if (e->graph) cudaGraphDestroy(e->graph);
+    for (auto& s : e->slots)
+        if (s.arena) cudaFree(s.arena);
+    if (e->d_table) cudaFree(e->d_table);
+    if (e->d_prefix) cudaFree(e->d_prefix);
+    delete e;
+}
+
+size_t nimbus_cuda_engine_member_bytes(const nimbus_member_desc* desc)
+{
+    if (!desc || check_desc(desc)) return 0;
+    return arena_layout(desc).total;
+}
+
+nimbus_status nimbus_cuda_engine_admit(nimbus_engine* e, const nimbus_member_desc* desc,
+                                       const nimbus_member_state* initial, size_t reserve_bytes, int* member_id)
+{
+    if (!e || !desc || !member_id) return NIMBUS_ERR_INVALID_ARGUMENT;
+    nimbus_cuda_context* ctx = e->ctx;
+    if (const char* why = check_desc(desc)) return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, why);
+    if (const char* why = check_state(initial)) return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, why);
+    NB_CUDA(ctx, cudaSetDevice(ctx->device));
+    const ArenaLayout L = arena_layout(desc);
+    size_t free_bytes = 0, total_bytes = 0;
+    NB_CUDA(ctx, cudaMemGetInfo(&free_bytes, &total_bytes));
+    if (L.total + reserve_bytes > free_bytes)
+        return fail(ctx, NIMBUS_ERR_OUT_OF_MEMORY, "member does not fit the free device memory");
+    NB_TRY(sync_table_to_host(e));
+
+    MemberSlot slot;
+    slot.id = e->next_id;
+    slot.desc = *desc;
+    slot.desc.rho0_base = slot.desc.p0_base = slot.desc.qv0_base = slot.desc.u0_base = slot.desc.v0_base = nullptr;
+    slot.bytes = L.total;
+    {
+        const cudaError_t err = cudaMalloc(&slot.arena, L.total);
+        if (err != cudaSuccess) return cuda_fail(ctx, err, "member allocation");
+    }
+    char* base = static_cast<char*>(slot.arena);
+    const size_t field = align_up(L.cells * sizeof(float));
+    auto fld = [&](size_t off, int idx) { return reinterpret_cast<float*>(base + off + idx * field); };
+    EngineMember& M = slot.m;
+    M = EngineMember{};
+    M.u = fld(L.off_state, 0);
+    M.v = fld(L.off_state, 1);
+    M.w = fld(L.off_state, 2);
+    M.rho = fld(L.off_state, 3);
+    M.rho_alt = fld(L.off_state, 4);
+    M.p = fld(L.off_state, 5);
+    M.theta = fld(L.off_state, 6);
+    M.qv = fld(L.off_state, 7);
+    M.qc = fld(L.off_state, 8);
+    M.qr = fld(L.off_state, 9);
+    M.qr_alt = fld(L.off_state, 10);
+    M.rho_begin = fld(L.off_ctxt, 0);
+    M.mfx = fld(L.off_ctxt, 1);
+    M.mfy = fld(L.off_ctxt, 2);
+    M.mfz = fld(L.off_ctxt, 3);
+    M.wave = reinterpret_cast<float*>(base + L.off_wave);
+    M.sf = reinterpret_cast<float*>(base + L.off_sf);
+    M.rl = reinterpret_cast<float*>(base + L.off_rl);
+    M.k1 = reinterpret_cast<float*>(base + L.off_k1);
+    M.xs = reinterpret_cast<float*>(base + L.off_xs);
+    M.eos = reinterpret_cast<float*>(base + L.off_eos);
+    M.status = reinterpret_cast<unsigned*>(base + L.off_status);
+    double* prof = reinterpret_cast<double*>(base + L.off_prof);
+    const size_t nz = static_cast<size_t>(desc->nz);
+    M.rho0 = prof;
+    M.p0 = prof + nz;
+    M.qv0 = prof + 2 * nz;
+    M.u0 = prof + 3 * nz;
+    M.v0 = prof + 4 * nz;
+    float2* dp0 = reinterpret_cast<float2*>(base + L.off_dp0);
+    M.dp0 = dp0;
+    fill_params(M, desc);
+
+    // Profiles, the split hydrostatic difference and the initial state.
+    std::vector<double> hp(5 * nz, 0.0);
+    std::memcpy(hp.data(), desc->rho0_base, nz * sizeof(double));
+    std::memcpy(hp.data() + nz, desc->p0_base, nz * sizeof(double));
+    std::memcpy(hp.data() + 2 * nz, desc->qv0_base, nz * sizeof(double));
+    if (desc->u0_base) std::memcpy(hp.data() + 3 * nz, desc->u0_base, nz * sizeof(double));
+    if (desc->v0_base) std::memcpy(hp.data() + 4 * nz, desc->v0_base, nz * sizeof(double));
+    std::vector<float2> hdp(nz);
+    split_dp0(desc->p0_base, desc->nz, hdp.data());
+    const size_t bytes = L.cells * sizeof(float);
+    cudaError_t err = cudaSuccess;
+    const float* src[9] = {initial->u, initial->v, initial->w, initial->rho, initial->p, initial->theta,
+                           initial->qv, initial->qc, initial->qr};
+    float* dst[9] = {M.u, M.v, M.w, M.rho, M.p, M.theta, M.qv, M.qc, M.qr};
+    for (int f = 0; f < 9 && err == cudaSuccess; ++f) err = cudaMemcpy(dst[f], src[f], bytes, cudaMemcpyHostToDevice);
+    if (err == cudaSuccess) err = cudaMemcpy(prof, hp.data(), hp.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (err == cudaSuccess) err = cudaMemcpy(dp0, hdp.data(), nz * sizeof(float2), cudaMemcpyHostToDevice);
+    if (err == cudaSuccess) err = cudaMemset(M.status, 0, sizeof(unsigned));
+    // Scratch that a step reads before writing: none, but keep it defined.
+    if (err == cudaSuccess) err = cudaMemset(M.wave, 0, L.history * sizeof(float));
+    if (err != cudaSuccess)
+    {
+        cudaFree(slot.arena);
+        return cuda_fail(ctx, err, "member upload");
+    }
+    e->slots.push_back(slot);
+    ++e->next_id;
+    e->dirty = true;
+    *member_id = slot.id;
+    return NIMBUS_OK;
+}
+
+nimbus_status nimbus_cuda_engine_retire(nimbus_engine* e, int member_id)
+{
+    if (!e) return NIMBUS_ERR_INVALID_ARGUMENT;
+    nimbus_cuda_context* ctx = e->ctx;
+    size_t index = 0;
+    if (!find_slot(e, member_id, &index)) return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "unknown member id");
+    NB_TRY(sync_table_to_host(e));
+    NB_CUDA(ctx, cudaFree(e->slots[index].arena));
+    e->slots.erase(e->slots.begin() + static_cast<long>(index));
+    e->dirty = true;
+    return NIMBUS_OK;
+}
+
+nimbus_status nimbus_cuda_engine_read(nimbus_engine* e, int member_id, const nimbus_member_state* out)
+{
+    if (!e) return NIMBUS_ERR_INVALID_ARGUMENT;
+    nimbus_cuda_context* ctx = e->ctx;
+    if (const char* why = check_state(out)) return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, why);
+    MemberSlot* s = find_slot(e, member_id);
+    if (!s) return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "unknown member id");
+    NB_TRY(sync_table_to_host(e));
+    const EngineMember& M = s->m;
+    const size_t bytes = static_cast<size_t>(M.items[kItemCells]) * sizeof(float);
+    const float* src[9] = {M.u, M.v, M.w, M.rho, M.p, M.theta, M.qv, M.qc, M.qr};
+    float* dst[9] = {out->u, out->v, out->w, out->rho, out->p, out->theta, out->qv, out->qc, out->qr};
+    for (int f = 0; f < 9; ++f)
+        NB_CUDA(ctx, cudaMemcpyAsync(dst[f], src[f], bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    NB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return NIMBUS_OK;
+}
+
+nimbus_status nimbus_cuda_engine_write(nimbus_engine* e, int member_id, const nimbus_member_state* in)
+{
+    if (!e) return NIMBUS_ERR_INVALID_ARGUMENT;
+    nimbus_cuda_context* ctx = e->ctx;
+    if (const char* why = check_state(in)) return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, why);
+    MemberSlot* s = find_slot(e, member_id);
+    if (!s) return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "unknown member id");
+    NB_TRY(sync_table_to_host(e));
+    const EngineMember& M = s->m;
+    const size_t bytes = static_cast<size_t>(M.items[kItemCells]) * sizeof(float);
+    const float* src[9] = {in->u, in->v, in->w, in->rho, in->p, in->theta, in->qv, in->qc, in->qr};
+    float* dst[9] = {M.u, M.v, M.w, M.rho, M.p, M.theta, M.qv, M.qc, M.qr};
+    for (int f = 0; f < 9; ++f)
+        NB_CUDA(ctx, cudaMemcpyAsync(dst[f], src[f], bytes, cudaMemcpyHostToDevice, ctx->stream));
+    NB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return NIMBUS_OK;
+}
+
+nimbus_status nimbus_cuda_engine_step(nimbus_engine* e, int n_steps)
+{
+    if (!e || n_steps < 0) return NIMBUS_ERR_INVALID_ARGUMENT;
+    nimbus_cuda_context* ctx = e->ctx;
+    NB_CUDA(ctx, cudaSetDevice(ctx->device));
+    if (e->dirty) NB_TRY(rebuild_table(e));
+    if (e->slots.empty() || n_steps == 0) return NIMBUS_OK;
+    const bool graph = e->use_graph && !ctx->timing;
+    if (graph && (!e->exec || e->built_precision != ctx->precision))
+    {
+        if (e->exec)
+        {
+            cudaGraphExecDestroy(e->exec);
+            e->exec = nullptr;
+            cudaGraphDestroy(e->graph);
+            e->graph = nullptr;
+        }
+        NB_TRY(build_graph(e));
+    }
+    for (int i = 0; i < n_steps; ++i)
+    {
+        if (graph) NB_CUDA(ctx, cudaGraphLaunch(e->exec, ctx->stream));
+        else e->launches_per_step = enqueue(e, ctx->stream);
+        ctx->launches += static_cast<uint64_t>(e->launches_per_step);
+    }
+    NB_CUDA(ctx, cudaGetLastError());
+    e->table_current = false;
+    return NIMBUS_OK;
+}
+
+nimbus_status nimbus_cuda_engine_synchronize(nimbus_engine* e)
+{
+    if (!e) return NIMBUS_ERR_INVALID_ARGUMENT;
+    nimbus_cuda_context* ctx = e->ctx;
+    NB_TRY(sync_table_to_host(e));
+    unsigned any = 0;
+    for (auto& s : e->slots)
+    {
+        unsigned f = 0;
+        NB_CUDA(ctx, cudaMemcpy(&f, s.m.status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+        any |= f;
+    }
+    if (any & kStatusNonfiniteMassFlux) return fail(ctx, NIMBUS_ERR_NONFINITE, "a member's retained mass flux went non-finite");
+    if (any & kStatusNonfiniteTransport) return fail(ctx, NIMBUS_ERR_NONFINITE, "a member's transported scalar went non-finite");
+    if (any & kStatusInvalidEos) return fail(ctx, NIMBUS_ERR_NONFINITE, "a member's EOS projection was refused");
+    return NIMBUS_OK;
+}
+
+nimbus_status nimbus_cuda_engine_member_status(nimbus_engine* e, int member_id, unsigned* flags)
+{
+    if (!e || !flags) return NIMBUS_ERR_INVALID_ARGUMENT;
+    MemberSlot* s = find_slot(e, member_id);
+    if (!s) return fail(e->ctx, NIMBUS_ERR_INVALID_ARGUMENT, "unknown member id");
+    NB_TRY(sync_table_to_host(e));
+    NB_CUDA(e->ctx, cudaMemcpy(flags, s->m.status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    return NIMBUS_OK;
+}
+
+nimbus_status nimbus_cuda_engine_set_graph(nimbus_engine* e, int enable)
+{
+    if (!e) return NIMBUS_ERR_INVALID_ARGUMENT;
+    e->use_graph = enable != 0;
+    return NIMBUS_OK;
+}
+
+int nimbus_cuda_engine_members(const nimbus_engine* e) { return e ? static_cast<int>(e->slots.size()) : 0; }
+
+int nimbus_cuda_engine_launches_per_step(const nimbus_engine* e) { return e ? e->launches_per_step : 0; }
+
+}  // extern "C"

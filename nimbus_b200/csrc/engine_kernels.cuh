@@ -1,0 +1,301 @@
+// Batched kernels of the member engine: one launch per phase advances that
+// phase for every resident member.
+//
+// Work layout.  Each phase has an item kind (cells, west/east boundary rows,
+// south/north rows, columns, KW78 history slots).  A member's items are cut
+// into tiles of one block (blockDim.x items) and the members' tiles are laid
+// end to end; prefix[kind][m] is the first tile of member m.  A persistent
+// grid (a few CTAs per SM) strides over the tiles, so the member of a tile is
+// uniform across its block and the per-member parameters are warp-broadcast
+// loads from the member table.  Members are kept sorted by substep count
+// (descending): at substep s the active members are a prefix of the table and
+// the launch covers prefix[kind][active_s] tiles -- a ragged ensemble wastes
+// no tiles on members that have finished their loop.
+//
+// Every item runs the same cell function as the per-operation kernels, with
+// the member's pointers and parameters, so a member's arithmetic does not
+// depend on the batch it shares.
+#pragma once
+
+#include "acoustic_kernels.cuh"
+#include "acoustic_split.cuh"
+#include "physics_kernels.cuh"
+#include "slow_kernels.cuh"
+#include "transport_kernels.cuh"
+
+namespace nimbus
+{
+
+enum ItemKind
+{
+    kItemCells = 0,
+    kItemRowsWE,     // ny*nz west/east boundary rows
+    kItemRowsSN,     // nx*nz south/north boundary rows
+    kItemColumns,    // nx*ny columns
+    kItemHistory,    // (ny + nx)*nz KW78 history slots
+    kItemKinds
+};
+
+constexpr int kEngineScalars = 4;  // theta, qv, qc, qr
+
+struct EngineMember
+{
+    // Prognostic state and the two ping-pong partners (swapped on the device
+    // at the end of the loop / after Kessler, see engine_swap_kernel).
+    float *u, *v, *w, *rho, *rho_alt, *p, *theta, *qv, *qc, *qr, *qr_alt;
+    // Retained transport context and per-step scratch.
+    float *rho_begin, *mfx, *mfy, *mfz, *wave;
+    float *sf;        // [kEngineScalars][3][cells] face fluxes
+    float *rl;        // [kEngineScalars][cells] limiter factors
+    float *k1, *xs;   // [4][cells] Heun k1 and predictor state
+    float *eos;       // EOS candidate pressure
+    unsigned* status; // this member's status word (kStatus* bits)
+    const double *rho0, *p0, *qv0, *u0, *v0;
+    const float2* dp0;
+    FusedParams F;
+    BoundaryParams B;
+    TransportParams T;  // geometry and flags; the scalar pointers are taken from the fields above
+    SlowParams S;
+    KesslerParams K;
+    double gamma;
+    int n_substeps;
+    int microphysics;
+    int items[kItemKinds];
+};
+
+__device__ __forceinline__ const float* engine_scalar(const EngineMember& M, int s)
+{
+    return s == 0 ? M.theta : (s == 1 ? M.qv : (s == 2 ? M.qc : M.qr));
+}
+
+__device__ __forceinline__ float* engine_scalar_out(const EngineMember& M, int s)
+{
+    return s == 0 ? M.theta : (s == 1 ? M.qv : (s == 2 ? M.qc : M.qr));
+}
+
+// Calls fn(member, item) for every item of the first tiles of a kind.
+template <class Fn>
+__device__ __forceinline__ void for_member_items(const EngineMember* __restrict__ table,
+                                                 const long long* __restrict__ prefix, long long tiles, int kind,
+                                                 Fn&& fn)
+{
+    int m = 0;
+    for (long long t = blockIdx.x; t < tiles; t += gridDim.x)
+    {
+        while (t >= prefix[m + 1]) ++m;
+        const EngineMember& M = table[m];
+        const int item = (int)((t - prefix[m]) * blockDim.x) + (int)threadIdx.x;
+        if (item < M.items[kind]) fn(M, item);
+    }
+}
+
+// ---- Heun slow step -------------------------------------------------------
+
+template <class Policy>
+static __global__ void __launch_bounds__(256) engine_slow_predict_kernel(const EngineMember* __restrict__ table,
+                                                                  const long long* __restrict__ prefix,
+                                                                  long long tiles)
+{
+    for_member_items(table, prefix, tiles, kItemCells, [&](const EngineMember& M, int c) {
+        const int n = M.items[kItemCells];
+        slow_predict_cell<Policy>(M.S, M.u, M.v, M.w, M.rho, M.p, M.qv, M.qc, M.qr, M.rho0, M.qv0, M.u0, M.v0, M.k1,
+                                  M.k1 + n, M.k1 + 2 * n, M.k1 + 3 * n, M.xs, M.xs + n, M.xs + 2 * n, M.xs + 3 * n,
+                                  c);
+    });
+}
+
+template <class Policy>
+static __global__ void __launch_bounds__(256) engine_slow_correct_kernel(const EngineMember* __restrict__ table,
+                                                                  const long long* __restrict__ prefix,
+                                                                  long long tiles)
+{
+    for_member_items(table, prefix, tiles, kItemCells, [&](const EngineMember& M, int c) {
+        const int n = M.items[kItemCells];
+        slow_correct_cell<Policy>(M.S, M.xs, M.xs + n, M.xs + 2 * n, M.rho, M.xs + 3 * n, M.qv, M.qc, M.qr, M.rho0,
+                                  M.qv0, M.u0, M.v0, M.k1, M.k1 + n, M.k1 + 2 * n, M.k1 + 3 * n, M.u, M.v, M.w,
+                                  M.p, nullptr, nullptr, nullptr, nullptr, c);
+    });
+}
+
+// ---- Boundaries and KW78 seed ---------------------------------------------
+//
+// The density buffer substep s reads (written == false) or writes: substep s
+// reads (s even ? rho : rho_alt) and writes the other one.  The boundary
+// closure after substep s works on the written buffer; the refresh before the
+// loop on the current density.
+
+__device__ __forceinline__ float* engine_density(const EngineMember& M, int s, bool written)
+{
+    const bool even = (s & 1) == 0;
+    return written ? (even ? M.rho_alt : M.rho) : (even ? M.rho : M.rho_alt);
+}
+
+static __global__ void __launch_bounds__(256) engine_bc_we_kernel(const EngineMember* __restrict__ table,
+                                                           const long long* __restrict__ prefix, long long tiles,
+                                                           int s, int refresh)
+{
+    for_member_items(table, prefix, tiles, kItemRowsWE, [&](const EngineMember& M, int r) {
+        BoundaryParams B = M.B;
+        if (refresh) B.dt_rad = 0.0f;
+        float* rho = refresh ? M.rho : engine_density(M, s, true);
+        const int yz = B.d.ny * B.d.nz;
+        bc_we_row(B, M.u, M.v, M.w, rho, M.p, M.wave, M.wave + yz, r);
+    });
+}
+
+static __global__ void __launch_bounds__(256) engine_bc_sn_kernel(const EngineMember* __restrict__ table,
+                                                           const long long* __restrict__ prefix, long long tiles,
+                                                           int s, int refresh)
+{
+    for_member_items(table, prefix, tiles, kItemRowsSN, [&](const EngineMember& M, int r) {
+        BoundaryParams B = M.B;
+        if (refresh) B.dt_rad = 0.0f;
+        float* rho = refresh ? M.rho : engine_density(M, s, true);
+        const int yz = B.d.ny * B.d.nz, xz = B.d.nx * B.d.nz;
+        bc_sn_row(B, M.u, M.v, M.w, rho, M.p, M.wave + 2 * yz, M.wave + 2 * yz + xz, r);
+    });
+}
+
+static __global__ void __launch_bounds__(256) engine_bc_vertical_kernel(const EngineMember* __restrict__ table,
+                                                                 const long long* __restrict__ prefix,
+                                                                 long long tiles)
+{
+    for_member_items(table, prefix, tiles, kItemColumns, [&](const EngineMember& M, int col) {
+        bc_vertical_column(M.B, M.u, M.v, M.w, col);
+    });
+}
+
+static __global__ void __launch_bounds__(256) engine_seed_kernel(const EngineMember* __restrict__ table,
+                                                          const long long* __restrict__ prefix, long long tiles)
+{
+    for_member_items(table, prefix, tiles, kItemHistory, [&](const EngineMember& M, int r) {
+        seed_radiation_row(M.B.d, M.u, M.v, M.wave, r);
+    });
+}
+
+// ---- Acoustic substep (split form, u/v/w in place, rho ping-pong) ---------
+
+template <class Policy>
+static __global__ void __launch_bounds__(256) engine_continuity_kernel(const EngineMember* __restrict__ table,
+                                                                const long long* __restrict__ prefix,
+                                                                long long tiles, int s)
+{
+    const bool first = s == 0;
+    for_member_items(table, prefix, tiles, kItemCells, [&](const EngineMember& M, int c) {
+        unsigned flags = 0;
+        continuity_eos_cell<Policy>(M.F, engine_density(M, s, false), M.u, M.v, M.w, M.theta, M.rho0,
+                                    engine_density(M, s, true), M.p, nullptr, M.mfx, M.mfy, M.mfz, c, flags, first,
+                                    first ? M.rho_begin : nullptr);
+        if (flags) atomicOr(M.status, flags);
+    });
+}
+
+template <class Policy>
+static __global__ void __launch_bounds__(256) engine_momentum_kernel(const EngineMember* __restrict__ table,
+                                                              const long long* __restrict__ prefix, long long tiles,
+                                                              int s)
+{
+    for_member_items(table, prefix, tiles, kItemCells, [&](const EngineMember& M, int c) {
+        momentum_cell<Policy>(M.F, engine_density(M, s, true), M.p, M.p0, M.dp0, M.u, M.v, M.w, M.u, M.v, M.w, c);
+    });
+}
+
+// Pointer rotation after the acoustic loop (rho, when the substep count is
+// odd the final density sits in the partner) and after Kessler (qr).
+static __global__ void engine_swap_kernel(EngineMember* table, int members, int which)
+{
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= members) return;
+    EngineMember& M = table[m];
+    if (which == 0)
+    {
+        if (M.n_substeps & 1)
+        {
+            float* t = M.rho;
+            M.rho = M.rho_alt;
+            M.rho_alt = t;
+        }
+    }
+    else if (M.microphysics)
+    {
+        float* t = M.qr;
+        M.qr = M.qr_alt;
+        M.qr_alt = t;
+    }
+}
+
+// ---- Transport (blockIdx.y = scalar) --------------------------------------
+
+template <bool kFp32>
+static __global__ void __launch_bounds__(256) engine_transport_faces_kernel(const EngineMember* __restrict__ table,
+                                                                     const long long* __restrict__ prefix,
+                                                                     long long tiles)
+{
+    const int s = blockIdx.y;
+    for_member_items(table, prefix, tiles, kItemCells, [&](const EngineMember& M, int c) {
+        const size_t n = (size_t)M.items[kItemCells];
+        transport_faces_cell<kFp32>(M.T, engine_scalar(M, s), M.mfx, M.mfy, M.mfz, M.sf + (size_t)s * 3 * n, c);
+    });
+}
+
+static __global__ void __launch_bounds__(256) engine_transport_limiter_kernel(const EngineMember* __restrict__ table,
+                                                                       const long long* __restrict__ prefix,
+                                                                       long long tiles)
+{
+    const int s = blockIdx.y;
+    if (s == 0) return;  // theta is not positive definite
+    for_member_items(table, prefix, tiles, kItemCells, [&](const EngineMember& M, int c) {
+        const size_t n = (size_t)M.items[kItemCells];
+        transport_limiter_cell(M.T, engine_scalar(M, s), M.rho_begin, M.sf + (size_t)s * 3 * n,
+                               M.rl + (size_t)s * n, c);
+    });
+}
+
+static __global__ void __launch_bounds__(256) engine_transport_update_kernel(const EngineMember* __restrict__ table,
+                                                                      const long long* __restrict__ prefix,
+                                                                      long long tiles)
+{
+    const int s = blockIdx.y;
+    for_member_items(table, prefix, tiles, kItemCells, [&](const EngineMember& M, int c) {
+        const size_t n = (size_t)M.items[kItemCells];
+        unsigned flags = 0;
+        transport_update_cell(M.T, s != 0, engine_scalar(M, s), engine_scalar_out(M, s), M.rho, M.rho_begin,
+                              M.sf + (size_t)s * 3 * n, M.rl + (size_t)s * n, c, flags);
+        if (flags) atomicOr(M.status, flags);
+    });
+}
+
+// ---- Kessler and EOS --------------------------------------------------------
+
+static __global__ void __launch_bounds__(256) engine_kessler_kernel(const EngineMember* __restrict__ table,
+                                                             const long long* __restrict__ prefix, long long tiles)
+{
+    for_member_items(table, prefix, tiles, kItemCells, [&](const EngineMember& M, int c) {
+        if (M.microphysics)
+            kessler_cell<true>(M.K, M.theta, M.qv, M.qc, M.qr, M.p, M.rho, M.qr_alt, nullptr, nullptr, nullptr,
+                               nullptr, c);
+    });
+}
+
+static __global__ void __launch_bounds__(256) engine_eos_kernel(const EngineMember* __restrict__ table,
+                                                         const long long* __restrict__ prefix, long long tiles)
+{
+    for_member_items(table, prefix, tiles, kItemCells, [&](const EngineMember& M, int c) {
+        unsigned flags = 0;
+        eos_candidate_cell(M.K.d, M.rho, M.theta, M.p, M.qv, M.qc, M.qr, M.gamma, M.eos, c, flags);
+        if (flags) atomicOr(M.status, flags);
+    });
+}
+
+// Publishes a member's candidate pressure unless its projection was refused
+// (then its whole grid keeps the old pressure, as the reference refuses).
+static __global__ void __launch_bounds__(256) engine_eos_publish_kernel(const EngineMember* __restrict__ table,
+                                                                 const long long* __restrict__ prefix,
+                                                                 long long tiles)
+{
+    for_member_items(table, prefix, tiles, kItemCells, [&](const EngineMember& M, int c) {
+        if (!(*M.status & kStatusInvalidEos)) M.p[c] = M.eos[c];
+    });
+}
+
+}  // namespace nimbus

@@ -5,6 +5,7 @@
 // (include/compute/dispatch/dynamics.hpp:682-683).  Device-memory calls only
 // enqueue; nimbus_cuda_synchronize() reports their status word.
 #include "../../include/nimbus_cuda.h"
+#include "context.cuh"
 
 #include "acoustic_fused.cuh"
 #include "acoustic_kernels.cuh"
@@ -24,167 +25,10 @@
 #include <vector>
 
 using namespace nimbus;
+using namespace nimbus_host;
 
 namespace
 {
-
-constexpr int kThreads = 256;
-
-struct DeviceBuffer
-{
-    void* ptr = nullptr;
-    size_t bytes = 0;
-};
-
-enum Slot
-{
-    kU, kV, kW, kRho, kP, kTheta, kRhoAlt, kDrho, kRho0, kP0, kMfx, kMfy, kMfz, kWave, kRhoBegin,
-    kRhoEnd, kSf, kRl, kUAlt, kVAlt, kWAlt, kDp0, kSlowK1, kSlowStar, kSlowOut, kQv, kQc, kQr, kQv0, kU0, kV0,
-    kQrAlt, kKesslerOut, kEosCandidate,
-    kQ0, kSlotCount = kQ0 + 2 * kMaxScalars
-};
-
-}  // namespace
-
-struct TimedLaunch
-{
-    int family;
-    cudaEvent_t start, stop;
-};
-
-struct nimbus_cuda_context
-{
-    int device = 0;
-    int precision = NIMBUS_PRECISION_REFERENCE;
-    int substep_form = NIMBUS_SUBSTEP_AUTO;
-    struct TunedShape
-    {
-        int nx, ny, nz, precision, form;
-    };
-    std::vector<TunedShape> tuned;
-    bool timing = false;
-    std::vector<TimedLaunch> pending;
-    std::vector<cudaEvent_t> event_pool;
-    uint64_t timed_launches[NIMBUS_KERNEL_FAMILIES] = {};
-    double timed_ms[NIMBUS_KERNEL_FAMILIES] = {};
-    int sm_count = 148;
-    cudaStream_t stream = nullptr;
-    unsigned* status = nullptr;  // device status word
-    uint64_t launches = 0;
-    std::string error;
-    DeviceBuffer ws[kSlotCount];
-};
-
-namespace
-{
-
-nimbus_status fail(nimbus_cuda_context* ctx, nimbus_status s, const std::string& msg)
-{
-    if (ctx) ctx->error = msg;
-    return s;
-}
-
-nimbus_status cuda_fail(nimbus_cuda_context* ctx, cudaError_t e, const char* where)
-{
-    return fail(ctx, e == cudaErrorMemoryAllocation ? NIMBUS_ERR_OUT_OF_MEMORY : NIMBUS_ERR_CUDA,
-                std::string(where) + ": " + cudaGetErrorString(e));
-}
-
-#define NB_CUDA(ctx, call)                                   \
-    do {                                                     \
-        cudaError_t e_ = (call);                             \
-        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
-    } while (0)
-
-template <class T>
-nimbus_status ensure(nimbus_cuda_context* ctx, Slot slot, size_t count, T** out)
-{
-    DeviceBuffer& b = ctx->ws[slot];
-    const size_t bytes = count * sizeof(T);
-    if (b.bytes < bytes)
-    {
-        if (b.ptr) cudaFree(b.ptr);
-        b.ptr = nullptr;
-        b.bytes = 0;
-        void* p = nullptr;
-        cudaError_t e = cudaMalloc(&p, bytes);
-        if (e != cudaSuccess) return cuda_fail(ctx, e, "workspace allocation");
-        b.ptr = p;
-        b.bytes = bytes;
-    }
-    *out = static_cast<T*>(b.ptr);
-    return NIMBUS_OK;
-}
-
-cudaEvent_t take_event(nimbus_cuda_context* ctx)
-{
-    if (!ctx->event_pool.empty())
-    {
-        cudaEvent_t e = ctx->event_pool.back();
-        ctx->event_pool.pop_back();
-        return e;
-    }
-    cudaEvent_t e = nullptr;
-    cudaEventCreate(&e);
-    return e;
-}
-
-// Brackets the launches issued between begin() and end() with CUDA events on
-// their stream when kernel timing is enabled.
-struct LaunchTimer
-{
-    nimbus_cuda_context* ctx;
-    cudaStream_t stream;
-    int family;
-    cudaEvent_t start = nullptr;
-    LaunchTimer(nimbus_cuda_context* c, cudaStream_t s, int f) : ctx(c), stream(s), family(f)
-    {
-        if (ctx->timing)
-        {
-            start = take_event(ctx);
-            cudaEventRecord(start, stream);
-        }
-    }
-    ~LaunchTimer()
-    {
-        if (start)
-        {
-            cudaEvent_t stop = take_event(ctx);
-            cudaEventRecord(stop, stream);
-            ctx->pending.push_back({family, start, stop});
-        }
-    }
-};
-
-void drain_timing(nimbus_cuda_context* ctx)
-{
-    for (auto& t : ctx->pending)
-    {
-        float ms = 0.0f;
-        cudaEventSynchronize(t.stop);
-        cudaEventElapsedTime(&ms, t.start, t.stop);
-        ctx->timed_launches[t.family] += 1;
-        ctx->timed_ms[t.family] += ms;
-        ctx->event_pool.push_back(t.start);
-        ctx->event_pool.push_back(t.stop);
-    }
-    ctx->pending.clear();
-}
-
-int grid_for(const nimbus_cuda_context* ctx, long long work)
-{
-    long long blocks = (work + kThreads - 1) / kThreads;
-    const long long cap = static_cast<long long>(ctx->sm_count) * 16;
-    if (blocks > cap) blocks = cap;
-    return blocks < 1 ? 1 : static_cast<int>(blocks);
-}
-
-bool finite_positive(double v) { return std::isfinite(v) && v > 0.0; }
-bool valid_bounds(float lo, float hi) { return std::isfinite(lo) && std::isfinite(hi) && lo > 0.0f && lo <= hi; }
-bool cells_fit(int nx, int ny, int nz)
-{
-    return static_cast<long long>(nx) * ny * nz < static_cast<long long>(std::numeric_limits<int>::max()) / 4;
-}
 
 // Mirrors valid_acoustic_cgrid_dispatch (src/compute/cpu/acoustic_cgrid.cpp:11-46).
 const char* check_acoustic_common(const float* u, const float* v, const float* w, const float* rho, const float* p,
@@ -233,34 +77,6 @@ AcousticParams acoustic_params(int nx, int ny, int nz, double dx, double dy, dou
     P.wind_v = wind_v;
     return P;
 }
-
-nimbus_status upload(nimbus_cuda_context* ctx, void* dst, const void* src, size_t bytes)
-{
-    NB_CUDA(ctx, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
-    return NIMBUS_OK;
-}
-
-nimbus_status download(nimbus_cuda_context* ctx, void* dst, const void* src, size_t bytes)
-{
-    NB_CUDA(ctx, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
-    return NIMBUS_OK;
-}
-
-nimbus_status read_status(nimbus_cuda_context* ctx, cudaStream_t stream, unsigned* flags)
-{
-    unsigned h = 0;
-    NB_CUDA(ctx, cudaMemcpyAsync(&h, ctx->status, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
-    NB_CUDA(ctx, cudaMemsetAsync(ctx->status, 0, sizeof(unsigned), stream));
-    NB_CUDA(ctx, cudaStreamSynchronize(stream));
-    *flags = h;
-    return NIMBUS_OK;
-}
-
-#define NB_TRY(expr)                         \
-    do {                                     \
-        nimbus_status s_ = (expr);           \
-        if (s_ != NIMBUS_OK) return s_;      \
-    } while (0)
 
 // ---------------------------------------------------------------------------
 // Device-side sequences (all pointers device memory).
@@ -608,9 +424,9 @@ nimbus_status run_transport_device(nimbus_cuda_context* ctx, cudaStream_t st, co
     {
         LaunchTimer t(ctx, st, NIMBUS_KERNEL_TRANSPORT_FACES);
         if (ctx->precision == NIMBUS_PRECISION_FP32)
-            transport_faces_f32_kernel<<<grid, kThreads, 0, st>>>(T, mfx, mfy, mfz, sf);
+            transport_faces_kernel<true><<<grid, kThreads, 0, st>>>(T, mfx, mfy, mfz, sf);
         else
-            transport_faces_kernel<<<grid, kThreads, 0, st>>>(T, mfx, mfy, mfz, sf);
+            transport_faces_kernel<false><<<grid, kThreads, 0, st>>>(T, mfx, mfy, mfz, sf);
     }
     {
         LaunchTimer t(ctx, st, NIMBUS_KERNEL_TRANSPORT_LIMITER);
@@ -982,6 +798,42 @@ nimbus_status nimbus_cuda_slow_tendencies(nimbus_cuda_context* ctx, const nimbus
 nimbus_status nimbus_cuda_slow_step(nimbus_cuda_context* ctx, const nimbus_slow_args* a)
 {
     return slow_entry(ctx, a, true);
+}
+
+nimbus_status nimbus_cuda_acoustic_boundaries(nimbus_cuda_context* ctx, const nimbus_boundary_args* a)
+{
+    if (!ctx || !a) return NIMBUS_ERR_INVALID_ARGUMENT;
+    if (!a->u || !a->v || !a->w || !a->rho || !a->p) return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "a field pointer is null");
+    if (a->nx < 4 || a->ny < 4 || a->nz < 2 || !cells_fit(a->nx, a->ny, a->nz))
+        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "boundary closure needs a grid of at least 4x4x2");
+    if (!finite_positive(a->dx) || !finite_positive(a->dy) || !std::isfinite(a->dt_small) || a->dt_small < 0.0)
+        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "invalid spacing or dt_small");
+    for (int bc : {a->bc_west, a->bc_east, a->bc_south, a->bc_north})
+        if (bc < 0 || bc > 4) return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "lateral boundary code out of range");
+    if (a->bc_bottom < 0 || a->bc_bottom > 1 || a->bc_top < 0 || a->bc_top > 2)
+        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "vertical boundary code out of range");
+    const bool radiative = a->bc_west == kBcRadiative || a->bc_east == kBcRadiative || a->bc_south == kBcRadiative ||
+                           a->bc_north == kBcRadiative;
+    if (a->dt_small > 0.0 && radiative && !a->wave_history)
+        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "radiative faces need the wave history");
+    NB_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = a->stream ? static_cast<cudaStream_t>(a->stream) : ctx->stream;
+    BoundaryParams B{};
+    B.d = make_dims(a->nx, a->ny, a->nz);
+    B.west = a->bc_west; B.east = a->bc_east; B.south = a->bc_south; B.north = a->bc_north;
+    B.bottom = a->bc_bottom; B.top = a->bc_top;
+    B.dt_rad = static_cast<float>(a->dt_small);
+    B.inv_dx = 1.0f / static_cast<float>(a->dx);
+    B.inv_dy = 1.0f / static_cast<float>(a->dy);
+    B.frame_u = a->frame_velocity_u_ms;
+    B.frame_v = a->frame_velocity_v_ms;
+    AcousticDevice D{};
+    D.u = a->u; D.v = a->v; D.w = a->w; D.rho = a->rho; D.p = a->p;
+    // Without radiation the history is never read; any valid pointer will do.
+    float* wave = a->wave_history ? a->wave_history : a->u;
+    launch_boundaries(ctx, st, B, D, a->rho, wave);
+    NB_CUDA(ctx, cudaGetLastError());
+    return NIMBUS_OK;
 }
 
 nimbus_status nimbus_cuda_kessler_tendencies(nimbus_cuda_context* ctx, const nimbus_kessler_args* a)

@@ -27,6 +27,7 @@ struct KesslerParams
 
 // Constants: microphysics_base.hpp:1073-1080, fall_speeds.hpp:60-68.
 constexpr double kKT0 = 273.15, kKLv = 2.5e6, kKCp = 1004.0, kKRv = 461.5, kKRd = 287.0, kKP0 = 100000.0;
+constexpr double kThetaStepMax = 50.0, kTheta0 = 300.0;  // max_theta_step_change_k, theta_reference_k
 constexpr double kRainA = 36.34, kRainB = 0.1346, kRainMinQ = 1.0e-9, kFallRho = 1.2;
 
 __device__ __forceinline__ double kclamp(double v, double lo, double hi) { return v < lo ? lo : (hi < v ? hi : v); }
@@ -69,7 +70,7 @@ __device__ __forceinline__ double k_sat_slope(double temperature, double saturat
 }
 
 // Coupled saturation adjustment (thermodynamics.hpp:282-466).
-__device__ double k_saturation_adjustment(double T_in, double p, double& qv, double& qc)
+static __device__ double k_saturation_adjustment(double T_in, double p, double& qv, double& qc)
 {
     double T = isfinite(T_in) ? kclamp(T_in, 150.0, 400.0) : kKT0;
     qv = isfinite(qv) ? kmax(0.0, qv) : 0.0;
@@ -144,18 +145,19 @@ __device__ __forceinline__ float k_sed_flux(const KesslerParams& K, double qr_ra
     return (float)(vt * q);
 }
 
+// Kessler tendencies of cell c and, with kApply, their application (theta,
+// qv, qc in place; the new qr to qr_out, since the cell below still reads
+// this cell's old qr for its sedimentation inflow).
 template <bool kApply>
-__global__ void __launch_bounds__(256) kessler_kernel(KesslerParams K, float* __restrict__ theta, float* __restrict__ qv,
-                                                      float* __restrict__ qc, const float* __restrict__ qr,
-                                                      const float* __restrict__ p, const float* __restrict__ rho,
-                                                      float* __restrict__ qr_out, float* __restrict__ dth_out,
-                                                      float* __restrict__ dqv_out, float* __restrict__ dqc_out,
-                                                      float* __restrict__ dqr_out)
+__device__ __forceinline__ void kessler_cell(const KesslerParams& K, float* __restrict__ theta,
+                                             float* __restrict__ qv, float* __restrict__ qc,
+                                             const float* __restrict__ qr, const float* __restrict__ p,
+                                             const float* __restrict__ rho, float* __restrict__ qr_out,
+                                             float* __restrict__ dth_out, float* __restrict__ dqv_out,
+                                             float* __restrict__ dqc_out, float* __restrict__ dqr_out, int c)
 {
     const Dims d = K.d;
-    const int n = d.cells();
     const double dt = K.dt;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
     {
         int i, j, k;
         decompose(d, c, i, j, k);
@@ -253,18 +255,42 @@ __global__ void __launch_bounds__(256) kessler_kernel(KesslerParams K, float* __
             float qr_new = qr_c;
             if (inside)
             {
+                // The CPU commit of step_microphysics_once with radiation,
+                // boundary layer and stochastic multipliers off
+                // (microphysics_step.cpp:3026-3245).
                 auto water = [&](float q, float dq) {
-                    const float raw = (float)((double)q + (double)dq * dt);
+                    const double dqs = isfinite(dq) ? (double)dq : 0.0;
+                    const float raw = (float)((double)q + dqs * dt);
                     return !isfinite(raw) ? 0.0f : (raw < 0.0f ? 0.0f : (0.05f < raw ? 0.05f : raw));
                 };
                 qv[c] = water(qv[c], dqv);
                 qc[c] = water(qc[c], dqc);
                 qr_new = water(qr_c, dqr);
-                theta[c] = (float)((double)theta[c] + (double)dth * dt);
+                const double told = (double)theta[c];
+                double total = (isfinite(dth) ? (double)dth : 0.0) * dt;
+                if (!isfinite(total)) total = 0.0;
+                const double limited = kclamp(total, -kThetaStepMax, kThetaStepMax);
+                double tn = told + limited;
+                if (!isfinite(tn)) tn = isfinite(told) ? told : kTheta0;
+                const float stored = (float)tn;
+                theta[c] = clamp_value(stored, (float)kTheta0, 200.0f, 700.0f);
             }
             qr_out[c] = qr_new;
         }
     }
+}
+
+template <bool kApply>
+static __global__ void __launch_bounds__(256) kessler_kernel(KesslerParams K, float* __restrict__ theta, float* __restrict__ qv,
+                                                      float* __restrict__ qc, const float* __restrict__ qr,
+                                                      const float* __restrict__ p, const float* __restrict__ rho,
+                                                      float* __restrict__ qr_out, float* __restrict__ dth_out,
+                                                      float* __restrict__ dqv_out, float* __restrict__ dqc_out,
+                                                      float* __restrict__ dqr_out)
+{
+    const int n = K.d.cells();
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+        kessler_cell<kApply>(K, theta, qv, qc, qr, p, rho, qr_out, dth_out, dqv_out, dqc_out, dqr_out, c);
 }
 
 // EOS pressure re-projection (eos_apply.cpp:50-175, pressure_fp64 in
@@ -275,7 +301,37 @@ __global__ void __launch_bounds__(256) kessler_kernel(KesslerParams K, float* __
 // attribution checks them (eos_apply.cpp:139-158): old p finite and positive,
 // qv finite and non-negative, qc + qr (FP64) finite and non-negative.  Any
 // failure sets the status bit; eos_publish_kernel then leaves p untouched.
-__global__ void __launch_bounds__(256) eos_candidate_kernel(Dims d, const float* __restrict__ rho,
+__device__ __forceinline__ void eos_candidate_cell(const Dims& d, const float* __restrict__ rho,
+                                                   const float* __restrict__ theta, const float* __restrict__ p_old,
+                                                   const float* __restrict__ qv, const float* __restrict__ qc,
+                                                   const float* __restrict__ qr, double gamma,
+                                                   float* __restrict__ p_candidate, int c, unsigned& flags)
+{
+    const float r = rho[c], th = theta[c];
+    const double diagnosed = kP00 * pow((double)r * kRd * (double)th / kP00, gamma);
+    if (!isfinite(r) || !(r > 0.0f) || !isfinite(th) || !(th > 0.0f) || !isfinite(diagnosed) || diagnosed <= 0.0 ||
+        !isfinite((float)diagnosed))
+    {
+        flags |= kStatusInvalidEos;
+        return;
+    }
+    p_candidate[c] = clamp_value((float)diagnosed, 101325.0f, 1000.0f, 200000.0f);
+    if (qv)
+    {
+        const int ih = d.nx >= 3, jh = d.ny >= 3;
+        int i, j, k;
+        decompose(d, c, i, j, k);
+        if (i >= ih && i < d.nx - ih && j >= jh && j < d.ny - jh)
+        {
+            const float po = p_old[c], q = qv[c];
+            const double liquid = (double)qc[c] + (double)qr[c];
+            if (!isfinite(po) || po <= 0.0f || !isfinite(q) || q < 0.0f || !isfinite(liquid) || liquid < 0.0)
+                flags |= kStatusInvalidEos;
+        }
+    }
+}
+
+static __global__ void __launch_bounds__(256) eos_candidate_kernel(Dims d, const float* __restrict__ rho,
                                                             const float* __restrict__ theta,
                                                             const float* __restrict__ p_old,
                                                             const float* __restrict__ qv, const float* __restrict__ qc,
@@ -284,37 +340,14 @@ __global__ void __launch_bounds__(256) eos_candidate_kernel(Dims d, const float*
                                                             unsigned* __restrict__ status)
 {
     const int n = (int)d.cells();
-    const int ih = d.nx >= 3, jh = d.ny >= 3;
     unsigned flags = 0;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
-    {
-        const float r = rho[c], th = theta[c];
-        const double diagnosed = kP00 * pow((double)r * kRd * (double)th / kP00, gamma);
-        if (!isfinite(r) || !(r > 0.0f) || !isfinite(th) || !(th > 0.0f) || !isfinite(diagnosed) ||
-            diagnosed <= 0.0 || !isfinite((float)diagnosed))
-        {
-            flags |= kStatusInvalidEos;
-            continue;
-        }
-        p_candidate[c] = clamp_value((float)diagnosed, 101325.0f, 1000.0f, 200000.0f);
-        if (qv)
-        {
-            int i, j, k;
-            decompose(d, c, i, j, k);
-            if (i >= ih && i < d.nx - ih && j >= jh && j < d.ny - jh)
-            {
-                const float po = p_old[c], q = qv[c];
-                const double liquid = (double)qc[c] + (double)qr[c];
-                if (!isfinite(po) || po <= 0.0f || !isfinite(q) || q < 0.0f || !isfinite(liquid) || liquid < 0.0)
-                    flags |= kStatusInvalidEos;
-            }
-        }
-    }
+        eos_candidate_cell(d, rho, theta, p_old, qv, qc, qr, gamma, p_candidate, c, flags);
     if (flags) atomicOr(status, flags);
 }
 
 // Publishes the candidate pressure unless the projection was refused.
-__global__ void __launch_bounds__(256) eos_publish_kernel(long long n, const float* __restrict__ p_candidate,
+static __global__ void __launch_bounds__(256) eos_publish_kernel(long long n, const float* __restrict__ p_candidate,
                                                           float* __restrict__ p, const unsigned* __restrict__ status)
 {
     if (*status & kStatusInvalidEos) return;

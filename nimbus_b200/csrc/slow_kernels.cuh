@@ -151,9 +151,36 @@ __device__ __forceinline__ float slow_apply_one(float x, float t, double dt)
     return (float)((double)x + finite_or_zero((double)t) * dt);
 }
 
-// k1 and the predictor state; also the plain tendency evaluation (xs == null).
+// k1 at cell c and, when su is given, the predictor state x* = x + dt*k1.
+// Also the plain tendency evaluation (su == null).
 template <class Policy>
-__global__ void __launch_bounds__(256) slow_predict_kernel(
+__device__ __forceinline__ void slow_predict_cell(
+    const SlowParams& S, const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w,
+    const float* __restrict__ rho, const float* __restrict__ p, const float* __restrict__ qv,
+    const float* __restrict__ qc, const float* __restrict__ qr, const double* __restrict__ rho0,
+    const double* __restrict__ qv0, const double* __restrict__ u0, const double* __restrict__ v0,
+    float* __restrict__ k1u, float* __restrict__ k1v, float* __restrict__ k1w, float* __restrict__ k1p,
+    float* __restrict__ su, float* __restrict__ sv, float* __restrict__ sw, float* __restrict__ sp, int c)
+{
+    int i, j, k;
+    decompose(S.d, c, i, j, k);
+    float tu, tv, tw, tp;
+    slow_tendencies_at<Policy>(S, c, i, j, k, u, v, w, rho, p, qv, qc, qr, rho0, qv0, u0, v0, tu, tv, tw, tp);
+    k1u[c] = tu;
+    k1v[c] = tv;
+    k1w[c] = tw;
+    k1p[c] = tp;
+    if (su != nullptr)
+    {
+        su[c] = slow_apply_one(u[c], tu, S.dt);
+        sv[c] = slow_apply_one(v[c], tv, S.dt);
+        sw[c] = slow_apply_one(w[c], tw, S.dt);
+        sp[c] = slow_apply_one(p[c], tp, S.dt);
+    }
+}
+
+template <class Policy>
+static __global__ void __launch_bounds__(256) slow_predict_kernel(
     SlowParams S, const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w,
     const float* __restrict__ rho, const float* __restrict__ p, const float* __restrict__ qv,
     const float* __restrict__ qc, const float* __restrict__ qr, const double* __restrict__ rho0,
@@ -161,31 +188,48 @@ __global__ void __launch_bounds__(256) slow_predict_kernel(
     float* __restrict__ k1u, float* __restrict__ k1v, float* __restrict__ k1w, float* __restrict__ k1p,
     float* __restrict__ su, float* __restrict__ sv, float* __restrict__ sw, float* __restrict__ sp)
 {
-    const Dims d = S.d;
-    const int n = d.cells();
+    const int n = S.d.cells();
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
-    {
-        int i, j, k;
-        decompose(d, c, i, j, k);
-        float tu, tv, tw, tp;
-        slow_tendencies_at<Policy>(S, c, i, j, k, u, v, w, rho, p, qv, qc, qr, rho0, qv0, u0, v0, tu, tv, tw, tp);
-        k1u[c] = tu;
-        k1v[c] = tv;
-        k1w[c] = tw;
-        k1p[c] = tp;
-        if (su != nullptr)
-        {
-            su[c] = slow_apply_one(u[c], tu, S.dt);
-            sv[c] = slow_apply_one(v[c], tv, S.dt);
-            sw[c] = slow_apply_one(w[c], tw, S.dt);
-            sp[c] = slow_apply_one(p[c], tp, S.dt);
-        }
-    }
+        slow_predict_cell<Policy>(S, u, v, w, rho, p, qv, qc, qr, rho0, qv0, u0, v0, k1u, k1v, k1w, k1p, su, sv, sw,
+                                  sp, c);
 }
 
-// k2 at the predictor state, the FP32 Heun average, and the apply in place.
+// k2 at the predictor state, the FP32 Heun average and its application to
+// cell c's own u, v, w, p (in place: the stencil reads only the predictor).
 template <class Policy>
-__global__ void __launch_bounds__(256) slow_correct_kernel(
+__device__ __forceinline__ void slow_correct_cell(
+    const SlowParams& S, const float* __restrict__ su, const float* __restrict__ sv, const float* __restrict__ sw,
+    const float* __restrict__ rho, const float* __restrict__ sp, const float* __restrict__ qv,
+    const float* __restrict__ qc, const float* __restrict__ qr, const double* __restrict__ rho0,
+    const double* __restrict__ qv0, const double* __restrict__ u0, const double* __restrict__ v0,
+    const float* __restrict__ k1u, const float* __restrict__ k1v, const float* __restrict__ k1w,
+    const float* __restrict__ k1p, float* __restrict__ u, float* __restrict__ v, float* __restrict__ w,
+    float* __restrict__ p, float* __restrict__ tu_out, float* __restrict__ tv_out, float* __restrict__ tw_out,
+    float* __restrict__ tp_out, int c)
+{
+    int i, j, k;
+    decompose(S.d, c, i, j, k);
+    float tu, tv, tw, tp;
+    slow_tendencies_at<Policy>(S, c, i, j, k, su, sv, sw, rho, sp, qv, qc, qr, rho0, qv0, u0, v0, tu, tv, tw, tp);
+    tu = __fmul_rn(0.5f, __fadd_rn(tu, k1u[c]));
+    tv = __fmul_rn(0.5f, __fadd_rn(tv, k1v[c]));
+    tw = __fmul_rn(0.5f, __fadd_rn(tw, k1w[c]));
+    tp = __fmul_rn(0.5f, __fadd_rn(tp, k1p[c]));
+    if (tu_out != nullptr)
+    {
+        tu_out[c] = tu;
+        tv_out[c] = tv;
+        tw_out[c] = tw;
+        tp_out[c] = tp;
+    }
+    u[c] = slow_apply_one(u[c], tu, S.dt);
+    v[c] = slow_apply_one(v[c], tv, S.dt);
+    w[c] = slow_apply_one(w[c], tw, S.dt);
+    p[c] = slow_apply_one(p[c], tp, S.dt);
+}
+
+template <class Policy>
+static __global__ void __launch_bounds__(256) slow_correct_kernel(
     SlowParams S, const float* __restrict__ su, const float* __restrict__ sv, const float* __restrict__ sw,
     const float* __restrict__ rho, const float* __restrict__ sp, const float* __restrict__ qv,
     const float* __restrict__ qc, const float* __restrict__ qr, const double* __restrict__ rho0,
@@ -195,30 +239,10 @@ __global__ void __launch_bounds__(256) slow_correct_kernel(
     float* __restrict__ p, float* __restrict__ tu_out, float* __restrict__ tv_out, float* __restrict__ tw_out,
     float* __restrict__ tp_out)
 {
-    const Dims d = S.d;
-    const int n = d.cells();
+    const int n = S.d.cells();
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
-    {
-        int i, j, k;
-        decompose(d, c, i, j, k);
-        float tu, tv, tw, tp;
-        slow_tendencies_at<Policy>(S, c, i, j, k, su, sv, sw, rho, sp, qv, qc, qr, rho0, qv0, u0, v0, tu, tv, tw, tp);
-        tu = __fmul_rn(0.5f, __fadd_rn(tu, k1u[c]));
-        tv = __fmul_rn(0.5f, __fadd_rn(tv, k1v[c]));
-        tw = __fmul_rn(0.5f, __fadd_rn(tw, k1w[c]));
-        tp = __fmul_rn(0.5f, __fadd_rn(tp, k1p[c]));
-        if (tu_out != nullptr)
-        {
-            tu_out[c] = tu;
-            tv_out[c] = tv;
-            tw_out[c] = tw;
-            tp_out[c] = tp;
-        }
-        u[c] = slow_apply_one(u[c], tu, S.dt);
-        v[c] = slow_apply_one(v[c], tv, S.dt);
-        w[c] = slow_apply_one(w[c], tw, S.dt);
-        p[c] = slow_apply_one(p[c], tp, S.dt);
-    }
+        slow_correct_cell<Policy>(S, su, sv, sw, rho, sp, qv, qc, qr, rho0, qv0, u0, v0, k1u, k1v, k1w, k1p, u, v, w,
+                                  p, tu_out, tv_out, tw_out, tp_out, c);
 }
 
 }  // namespace nimbus

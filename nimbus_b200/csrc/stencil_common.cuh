@@ -15,6 +15,7 @@ namespace nimbus
 
 // Physical constants: include/core/infra/physical_constants.hpp:15-34.
 constexpr double kRd = 287.0;
+constexpr double kCpd = 1004.0;
 constexpr double kP00 = 100000.0;
 // KW78 phase speed: boundary_conditions_cartesian_cgrid.cpp:266.
 constexpr float kCStar = 30.0f;

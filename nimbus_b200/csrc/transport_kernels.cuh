@@ -157,22 +157,25 @@ __device__ __forceinline__ float face_flux_f32(const float* __restrict__ q, int 
 #undef NQ
 }
 
-__global__ void __launch_bounds__(256) transport_faces_f32_kernel(TransportParams T, const float* __restrict__ mfx,
-                                                                  const float* __restrict__ mfy,
-                                                                  const float* __restrict__ mfz, float* __restrict__ sf)
+// Face fluxes of scalar s owned by cell c (its +x, +y and +z faces).
+// kFp32 selects the reference's FP32 GPU form (face_flux_f32), otherwise FP64
+// face values rounded once to the FP32 scratch.
+// sf points at the scalar's [3][cells] face-flux scratch (x, y, z).
+template <bool kFp32>
+__device__ __forceinline__ void transport_faces_cell(const TransportParams& T, const float* __restrict__ q,
+                                                     const float* __restrict__ mfx, const float* __restrict__ mfy,
+                                                     const float* __restrict__ mfz, float* __restrict__ sf, int c)
 {
     const Dims d = T.d;
     const int n = d.cells();
-    const int s = blockIdx.y;
-    const float* __restrict__ q = T.q_in[s];
-    float* __restrict__ sfx = sf + (size_t)s * 3 * n;
+    float* __restrict__ sfx = sf;
     float* __restrict__ sfy = sfx + n;
     float* __restrict__ sfz = sfy + n;
     const int kz_end = T.top_open ? d.nz : d.nz - 1;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+    int i, j, k;
+    decompose(d, c, i, j, k);
+    if constexpr (kFp32)
     {
-        int i, j, k;
-        decompose(d, c, i, j, k);
         if (i <= d.nx - 2) sfx[c] = face_flux_f32(q, c - i * d.sx(), d.sx(), i, d.nx, mfx[c], T.weno);
         if (j <= d.ny - 2) sfy[c] = face_flux_f32(q, c - j * d.sy(), d.sy(), j, d.ny, mfy[c], T.weno);
         if (k < kz_end)
@@ -181,24 +184,8 @@ __global__ void __launch_bounds__(256) transport_faces_f32_kernel(TransportParam
             sfz[c] = (k == d.nz - 1) ? mf * q[c] : face_flux_f32(q, c - k, 1, k, d.nz, mf, T.weno);
         }
     }
-}
-
-__global__ void __launch_bounds__(256) transport_faces_kernel(TransportParams T, const float* __restrict__ mfx,
-                                                              const float* __restrict__ mfy,
-                                                              const float* __restrict__ mfz, float* __restrict__ sf)
-{
-    const Dims d = T.d;
-    const int n = d.cells();
-    const int s = blockIdx.y;
-    const float* __restrict__ q = T.q_in[s];
-    float* __restrict__ sfx = sf + (size_t)s * 3 * n;
-    float* __restrict__ sfy = sfx + n;
-    float* __restrict__ sfz = sfy + n;
-    const int kz_end = T.top_open ? d.nz : d.nz - 1;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+    else
     {
-        int i, j, k;
-        decompose(d, c, i, j, k);
         if (i <= d.nx - 2)
         {
             const double mf = (double)mfx[c];
@@ -218,6 +205,16 @@ __global__ void __launch_bounds__(256) transport_faces_kernel(TransportParams T,
     }
 }
 
+template <bool kFp32>
+static __global__ void __launch_bounds__(256) transport_faces_kernel(TransportParams T, const float* __restrict__ mfx,
+                                                              const float* __restrict__ mfy,
+                                                              const float* __restrict__ mfz, float* __restrict__ sf)
+{
+    const int n = T.d.cells();
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+        transport_faces_cell<kFp32>(T, T.q_in[blockIdx.y], mfx, mfy, mfz, sf + (size_t)blockIdx.y * 3 * n, c);
+}
+
 // conservative_pd_limiter_factor (advection_cartesian.hpp:101-108), non-support path.
 __device__ __forceinline__ float pd_limiter_factor(double r)
 {
@@ -227,39 +224,45 @@ __device__ __forceinline__ float pd_limiter_factor(double r)
     return nextafterf(__fmul_rn(stored, roundoff), 0.0f);
 }
 
-__global__ void __launch_bounds__(256) transport_limiter_kernel(TransportParams T, const float* __restrict__ rho_begin,
-                                                                const float* __restrict__ sf, float* __restrict__ rl)
+// Positive-definite donor ratio of scalar s at cell c (advection_cartesian.cpp:2174-2240).
+// sf is the scalar's face-flux scratch, rl its [cells] limiter factors.
+__device__ __forceinline__ void transport_limiter_cell(const TransportParams& T, const float* __restrict__ q,
+                                                       const float* __restrict__ rho_begin,
+                                                       const float* __restrict__ sf, float* __restrict__ r_out, int c)
 {
     const Dims d = T.d;
     const int n = d.cells();
-    const int s = blockIdx.y;
-    if (!T.positive_definite[s]) return;
-    const float* __restrict__ q = T.q_in[s];
-    const float* __restrict__ sfx = sf + (size_t)s * 3 * n;
+    const float* __restrict__ sfx = sf;
     const float* __restrict__ sfy = sfx + n;
     const float* __restrict__ sfz = sfy + n;
-    float* __restrict__ r_out = rl + (size_t)s * n;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+    int i, j, k;
+    decompose(d, c, i, j, k);
+    double out = 0.0;
+    if (i <= d.nx - 2 && sfx[c] > 0.0f) out += (double)sfx[c] * T.inv_dx;
+    if (i >= 1 && sfx[c - d.sx()] < 0.0f) out -= (double)sfx[c - d.sx()] * T.inv_dx;
+    if (j <= d.ny - 2 && sfy[c] > 0.0f) out += (double)sfy[c] * T.inv_dy;
+    if (j >= 1 && sfy[c - d.sy()] < 0.0f) out -= (double)sfy[c - d.sy()] * T.inv_dy;
+    if ((k <= d.nz - 2 || (T.top_open && k == d.nz - 1)) && sfz[c] > 0.0f) out += (double)sfz[c] * T.inv_dz;
+    if (k >= 1 && sfz[c - 1] < 0.0f) out -= (double)sfz[c - 1] * T.inv_dz;
+    double r = 1.0;
+    if (out > 0.0)
     {
-        int i, j, k;
-        decompose(d, c, i, j, k);
-        double out = 0.0;
-        if (i <= d.nx - 2 && sfx[c] > 0.0f) out += (double)sfx[c] * T.inv_dx;
-        if (i >= 1 && sfx[c - d.sx()] < 0.0f) out -= (double)sfx[c - d.sx()] * T.inv_dx;
-        if (j <= d.ny - 2 && sfy[c] > 0.0f) out += (double)sfy[c] * T.inv_dy;
-        if (j >= 1 && sfy[c - d.sy()] < 0.0f) out -= (double)sfy[c - d.sy()] * T.inv_dy;
-        if ((k <= d.nz - 2 || (T.top_open && k == d.nz - 1)) && sfz[c] > 0.0f) out += (double)sfz[c] * T.inv_dz;
-        if (k >= 1 && sfz[c - 1] < 0.0f) out -= (double)sfz[c - 1] * T.inv_dz;
-        double r = 1.0;
-        if (out > 0.0)
-        {
-            const double qc = (double)q[c];
-            const double available = (double)rho_begin[c] * ((qc < 0.0) ? 0.0 : qc) / T.dt;  // std::max(q, 0.0)
-            const double ratio = available / out;
-            r = (ratio < 1.0) ? ratio : 1.0;  // std::min(1.0, ratio), NaN -> 1
-        }
-        r_out[c] = pd_limiter_factor(r);
+        const double qc = (double)q[c];
+        const double available = (double)rho_begin[c] * ((qc < 0.0) ? 0.0 : qc) / T.dt;  // std::max(q, 0.0)
+        const double ratio = available / out;
+        r = (ratio < 1.0) ? ratio : 1.0;  // std::min(1.0, ratio), NaN -> 1
     }
+    r_out[c] = pd_limiter_factor(r);
+}
+
+static __global__ void __launch_bounds__(256) transport_limiter_kernel(TransportParams T, const float* __restrict__ rho_begin,
+                                                                const float* __restrict__ sf, float* __restrict__ rl)
+{
+    const int s = blockIdx.y;
+    if (!T.positive_definite[s]) return;
+    const int n = T.d.cells();
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+        transport_limiter_cell(T, T.q_in[s], rho_begin, sf + (size_t)s * 3 * n, rl + (size_t)s * n, c);
 }
 
 __device__ __forceinline__ double limited_flux(float raw, bool pd, const float* __restrict__ rl, int lo, int hi)
@@ -269,64 +272,73 @@ __device__ __forceinline__ double limited_flux(float raw, bool pd, const float* 
     return (double)raw * (double)r;
 }
 
-__global__ void __launch_bounds__(256) transport_update_kernel(TransportParams T, const float* __restrict__ rho_end,
+// Donor-limited divergence and density recovery of scalar s at cell c
+// (advection_cartesian.cpp:2465-2640).  q_out may alias q_in: cell c reads
+// only its own old value, the fluxes live in the scratch.
+__device__ __forceinline__ void transport_update_cell(const TransportParams& T, bool pd, const float* q, float* qo,
+                                                      const float* __restrict__ rho_end,
+                                                      const float* __restrict__ rho_begin,
+                                                      const float* __restrict__ sf, const float* __restrict__ r,
+                                                      int c, unsigned& flags)
+{
+    const Dims d = T.d;
+    const int n = d.cells();
+    const float* __restrict__ sfx = sf;
+    const float* __restrict__ sfy = sfx + n;
+    const float* __restrict__ sfz = sfy + n;
+    int i, j, k;
+    decompose(d, c, i, j, k);
+    if (!(i >= 1 && i < d.nx - 1 && j >= 1 && j < d.ny - 1))
+    {
+        if (q != qo) qo[c] = q[c];  // seed_destination_from_source
+        return;
+    }
+    const int cxm = c - d.sx(), cxp = c + d.sx(), cym = c - d.sy(), cyp = c + d.sy();
+    const bool has_top = k <= d.nz - 2 || (T.top_open && k == d.nz - 1);
+    const double sxp = limited_flux(sfx[c], pd, r, c, cxp);
+    const double sxm = limited_flux(sfx[cxm], pd, r, cxm, c);
+    const double syp = limited_flux(sfy[c], pd, r, c, cyp);
+    const double sym = limited_flux(sfy[cym], pd, r, cym, c);
+    const double szp = has_top ? limited_flux(sfz[c], pd, r, c, k < d.nz - 1 ? c + 1 : c) : 0.0;
+    const double szm = (k >= 1) ? limited_flux(sfz[c - 1], pd, r, c - 1, c) : 0.0;
+    const double re = (double)rho_end[c];
+    const double rb = (double)rho_begin[c];
+    const double qc = (double)q[c];
+    double rho_phi;
+    if (pd)
+    {
+        double outgoing = 0.0, incoming = 0.0;
+        if (sxp >= 0.0) outgoing += sxp * T.inv_dx; else incoming -= sxp * T.inv_dx;
+        if (sxm <= 0.0) outgoing -= sxm * T.inv_dx; else incoming += sxm * T.inv_dx;
+        if (syp >= 0.0) outgoing += syp * T.inv_dy; else incoming -= syp * T.inv_dy;
+        if (sym <= 0.0) outgoing -= sym * T.inv_dy; else incoming += sym * T.inv_dy;
+        if (has_top) { if (szp >= 0.0) outgoing += szp * T.inv_dz; else incoming -= szp * T.inv_dz; }
+        if (k >= 1) { if (szm <= 0.0) outgoing -= szm * T.inv_dz; else incoming += szm * T.inv_dz; }
+        rho_phi = (rb * qc - T.dt * outgoing) + T.dt * incoming;
+    }
+    else
+    {
+        const double div = (sxp - sxm) * T.inv_dx + (syp - sym) * T.inv_dy + (szp - szm) * T.inv_dz;
+        rho_phi = rb * qc - T.dt * div;
+    }
+    const double denom = (re > T.rho_floor) ? re : T.rho_floor;
+    const float out = (float)(rho_phi / denom);
+    if (!isfinite(out)) flags |= kStatusNonfiniteTransport;
+    qo[c] = out;
+}
+
+static __global__ void __launch_bounds__(256) transport_update_kernel(TransportParams T, const float* __restrict__ rho_end,
                                                                const float* __restrict__ rho_begin,
                                                                const float* __restrict__ sf,
                                                                const float* __restrict__ rl, unsigned* status)
 {
-    const Dims d = T.d;
-    const int n = d.cells();
-    const int s = blockIdx.y;
-    const bool pd = T.positive_definite[s] != 0;
-    const float* q = T.q_in[s];
-    float* qo = T.q_out[s];
-    const float* __restrict__ sfx = sf + (size_t)s * 3 * n;
-    const float* __restrict__ sfy = sfx + n;
-    const float* __restrict__ sfz = sfy + n;
-    const float* __restrict__ r = rl + (size_t)s * n;
-    const bool copy_boundary = q != qo;
+    const int n = T.d.cells();
     unsigned flags = 0;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
     {
-        int i, j, k;
-        decompose(d, c, i, j, k);
-        if (!(i >= 1 && i < d.nx - 1 && j >= 1 && j < d.ny - 1))
-        {
-            if (copy_boundary) qo[c] = q[c];  // seed_destination_from_source
-            continue;
-        }
-        const int cxm = c - d.sx(), cxp = c + d.sx(), cym = c - d.sy(), cyp = c + d.sy();
-        const bool has_top = k <= d.nz - 2 || (T.top_open && k == d.nz - 1);
-        const double sxp = limited_flux(sfx[c], pd, r, c, cxp);
-        const double sxm = limited_flux(sfx[cxm], pd, r, cxm, c);
-        const double syp = limited_flux(sfy[c], pd, r, c, cyp);
-        const double sym = limited_flux(sfy[cym], pd, r, cym, c);
-        const double szp = has_top ? limited_flux(sfz[c], pd, r, c, k < d.nz - 1 ? c + 1 : c) : 0.0;
-        const double szm = (k >= 1) ? limited_flux(sfz[c - 1], pd, r, c - 1, c) : 0.0;
-        const double re = (double)rho_end[c];
-        const double rb = (double)rho_begin[c];
-        const double qc = (double)q[c];
-        double rho_phi;
-        if (pd)
-        {
-            double outgoing = 0.0, incoming = 0.0;
-            if (sxp >= 0.0) outgoing += sxp * T.inv_dx; else incoming -= sxp * T.inv_dx;
-            if (sxm <= 0.0) outgoing -= sxm * T.inv_dx; else incoming += sxm * T.inv_dx;
-            if (syp >= 0.0) outgoing += syp * T.inv_dy; else incoming -= syp * T.inv_dy;
-            if (sym <= 0.0) outgoing -= sym * T.inv_dy; else incoming += sym * T.inv_dy;
-            if (has_top) { if (szp >= 0.0) outgoing += szp * T.inv_dz; else incoming -= szp * T.inv_dz; }
-            if (k >= 1) { if (szm <= 0.0) outgoing -= szm * T.inv_dz; else incoming += szm * T.inv_dz; }
-            rho_phi = (rb * qc - T.dt * outgoing) + T.dt * incoming;
-        }
-        else
-        {
-            const double div = (sxp - sxm) * T.inv_dx + (syp - sym) * T.inv_dy + (szp - szm) * T.inv_dz;
-            rho_phi = rb * qc - T.dt * div;
-        }
-        const double denom = (re > T.rho_floor) ? re : T.rho_floor;
-        const float out = (float)(rho_phi / denom);
-        if (!isfinite(out)) flags |= kStatusNonfiniteTransport;
-        qo[c] = out;
+        const int s = blockIdx.y;
+        transport_update_cell(T, T.positive_definite[s] != 0, T.q_in[s], T.q_out[s], rho_end, rho_begin,
+                              sf + (size_t)s * 3 * n, rl + (size_t)s * n, c, flags);
     }
     if (flags) atomicOr(status, flags);
 }

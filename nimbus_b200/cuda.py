@@ -25,6 +25,8 @@ from . import initial
 LIB_PATH = Path(__file__).resolve().parent / "lib" / "libnimbus_cuda.so"
 
 NIMBUS_OK = 0
+NIMBUS_ERR_OUT_OF_MEMORY = 3
+NIMBUS_ERR_NONFINITE = 4
 STATUS_NAMES = {
     0: "NIMBUS_OK",
     1: "NIMBUS_ERR_INVALID_ARGUMENT",
@@ -118,6 +120,33 @@ class EosArgs(ctypes.Structure):
     ]
 
 
+class BoundaryArgs(ctypes.Structure):
+    _fields_ = [
+        ("u", _fp), ("v", _fp), ("w", _fp), ("rho", _fp), ("p", _fp), ("wave_history", _fp),
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("dt_small", ctypes.c_double),
+        ("bc_west", ctypes.c_int), ("bc_east", ctypes.c_int), ("bc_south", ctypes.c_int), ("bc_north", ctypes.c_int),
+        ("bc_bottom", ctypes.c_int), ("bc_top", ctypes.c_int),
+        ("frame_velocity_u_ms", ctypes.c_float), ("frame_velocity_v_ms", ctypes.c_float),
+        ("stream", ctypes.c_void_p),
+    ]
+
+
+class MemberDesc(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("dz", ctypes.c_double), ("dt", ctypes.c_double),
+        ("n_substeps", ctypes.c_int), ("bc", ctypes.c_int * 6), ("coriolis_f", ctypes.c_double),
+        ("frame_velocity_u_ms", ctypes.c_float), ("frame_velocity_v_ms", ctypes.c_float),
+        ("microphysics", ctypes.c_int),
+        ("rho0_base", _dp), ("p0_base", _dp), ("qv0_base", _dp), ("u0_base", _dp), ("v0_base", _dp),
+    ]
+
+
+class MemberState(ctypes.Structure):
+    _fields_ = [(k, _fp) for k in ("u", "v", "w", "rho", "p", "theta", "qv", "qc", "qr")]
+
+
 EXPORTED_SYMBOLS = (
     "nimbus_cuda_abi_version", "nimbus_cuda_create", "nimbus_cuda_destroy", "nimbus_cuda_last_error",
     "nimbus_cuda_kernel_launches", "nimbus_cuda_stream", "nimbus_cuda_synchronize",
@@ -127,6 +156,11 @@ EXPORTED_SYMBOLS = (
     "nimbus_cuda_set_substep_form", "nimbus_cuda_autotune_substep",
     "nimbus_cuda_slow_tendencies", "nimbus_cuda_slow_step",
     "nimbus_cuda_kessler_tendencies", "nimbus_cuda_kessler_step", "nimbus_cuda_eos_projection",
+    "nimbus_cuda_acoustic_boundaries",
+    "nimbus_cuda_engine_create", "nimbus_cuda_engine_destroy", "nimbus_cuda_engine_member_bytes",
+    "nimbus_cuda_engine_admit", "nimbus_cuda_engine_retire", "nimbus_cuda_engine_read", "nimbus_cuda_engine_write", "nimbus_cuda_engine_step",
+    "nimbus_cuda_engine_synchronize", "nimbus_cuda_engine_member_status", "nimbus_cuda_engine_set_graph",
+    "nimbus_cuda_engine_members", "nimbus_cuda_engine_launches_per_step",
 )
 SUBSTEP_AUTO, SUBSTEP_FUSED, SUBSTEP_SPLIT = 0, 1, 2
 PRECISION_REFERENCE, PRECISION_FP32 = 0, 1
@@ -162,6 +196,24 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
     lib.nimbus_cuda_kessler_tendencies.argtypes = [ctypes.c_void_p, ctypes.POINTER(KesslerArgs)]
     lib.nimbus_cuda_kessler_step.argtypes = [ctypes.c_void_p, ctypes.POINTER(KesslerArgs)]
     lib.nimbus_cuda_eos_projection.argtypes = [ctypes.c_void_p, ctypes.POINTER(EosArgs)]
+    lib.nimbus_cuda_acoustic_boundaries.argtypes = [ctypes.c_void_p, ctypes.POINTER(BoundaryArgs)]
+    vp = ctypes.c_void_p
+    lib.nimbus_cuda_engine_create.argtypes = [vp, ctypes.POINTER(vp)]
+    lib.nimbus_cuda_engine_destroy.argtypes = [vp]
+    lib.nimbus_cuda_engine_destroy.restype = None
+    lib.nimbus_cuda_engine_member_bytes.argtypes = [ctypes.POINTER(MemberDesc)]
+    lib.nimbus_cuda_engine_member_bytes.restype = ctypes.c_size_t
+    lib.nimbus_cuda_engine_admit.argtypes = [vp, ctypes.POINTER(MemberDesc), ctypes.POINTER(MemberState),
+                                             ctypes.c_size_t, ctypes.POINTER(ctypes.c_int)]
+    lib.nimbus_cuda_engine_retire.argtypes = [vp, ctypes.c_int]
+    lib.nimbus_cuda_engine_read.argtypes = [vp, ctypes.c_int, ctypes.POINTER(MemberState)]
+    lib.nimbus_cuda_engine_write.argtypes = [vp, ctypes.c_int, ctypes.POINTER(MemberState)]
+    lib.nimbus_cuda_engine_step.argtypes = [vp, ctypes.c_int]
+    lib.nimbus_cuda_engine_synchronize.argtypes = [vp]
+    lib.nimbus_cuda_engine_member_status.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_uint)]
+    lib.nimbus_cuda_engine_set_graph.argtypes = [vp, ctypes.c_int]
+    lib.nimbus_cuda_engine_members.argtypes = [vp]
+    lib.nimbus_cuda_engine_launches_per_step.argtypes = [vp]
     lib.nimbus_cuda_set_kernel_timing.argtypes = [ctypes.c_void_p, ctypes.c_int]
     lib.nimbus_cuda_kernel_timing.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64),
                                               ctypes.POINTER(ctypes.c_double)]
@@ -289,6 +341,9 @@ class Context:
 
     def eos_projection(self, args: EosArgs) -> int:
         return self.lib.nimbus_cuda_eos_projection(self.handle, ctypes.byref(args))
+
+    def acoustic_boundaries(self, args: BoundaryArgs) -> int:
+        return self.lib.nimbus_cuda_acoustic_boundaries(self.handle, ctypes.byref(args))
 
 
 def clamp_defaults() -> dict:
@@ -431,6 +486,151 @@ def eos_args(p, rho, theta, qv=None, qc=None, qr=None, memory=MEMORY_HOST, strea
     a.memory = memory
     a.stream = stream
     return a
+
+
+def boundary_args(st, grid, bc, dt_small=0.0, wave=None, frame=(0.0, 0.0), stream=None) -> BoundaryArgs:
+    """Argument block for nimbus_cuda_acoustic_boundaries (device tensors)."""
+    nx, ny, nz = tuple(st["u"].shape)
+    a = BoundaryArgs()
+    a._keep = (dict(st), wave)
+    a.u, a.v, a.w, a.rho, a.p = (_f(st[k]) for k in ("u", "v", "w", "rho", "p"))
+    a.wave_history = _f(wave)
+    a.nx, a.ny, a.nz = nx, ny, nz
+    a.dx, a.dy = grid[0], grid[1]
+    a.dt_small = dt_small
+    a.bc_west, a.bc_east, a.bc_south, a.bc_north, a.bc_bottom, a.bc_top = (int(x) for x in bc)
+    a.frame_velocity_u_ms, a.frame_velocity_v_ms = frame
+    a.stream = stream
+    return a
+
+
+MEMBER_FIELDS = ("u", "v", "w", "rho", "p", "theta", "qv", "qc", "qr")
+
+
+def member_desc(shape, grid, dt, n_substeps, bc, base, coriolis_f=0.0, frame=(0.0, 0.0),
+                microphysics=1) -> MemberDesc:
+    """Descriptor of one engine member; `base` holds the FP64 profiles
+    rho0, p0, qv0 (and optionally u0, v0)."""
+    d = MemberDesc()
+    d.nx, d.ny, d.nz = (int(x) for x in shape)
+    d.dx, d.dy, d.dz = grid
+    d.dt = dt
+    d.n_substeps = int(n_substeps)
+    d.bc[:] = [int(x) for x in bc]
+    d.coriolis_f = coriolis_f
+    d.frame_velocity_u_ms, d.frame_velocity_v_ms = frame
+    d.microphysics = int(microphysics)
+    prof = {k: np.ascontiguousarray(base[k], dtype=np.float64) for k in ("rho0", "p0", "qv0", "u0", "v0")
+            if base.get(k) is not None}
+    d._keep = prof
+    d.rho0_base, d.p0_base, d.qv0_base = _d(prof["rho0"]), _d(prof["p0"]), _d(prof["qv0"])
+    d.u0_base = _d(prof["u0"]) if "u0" in prof else None
+    d.v0_base = _d(prof["v0"]) if "v0" in prof else None
+    return d
+
+
+def member_state(st) -> MemberState:
+    s = MemberState()
+    s._keep = {k: np.ascontiguousarray(st[k], dtype=np.float32) for k in MEMBER_FIELDS}
+    for k in MEMBER_FIELDS:
+        setattr(s, k, _f(s._keep[k]))
+    return s
+
+
+class Engine:
+    """Resident members advanced together (nimbus_cuda_engine_*): one
+    batched launch per phase of the large step, replayed from a CUDA graph."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        h = ctypes.c_void_p()
+        ctx.check(self.lib.nimbus_cuda_engine_create(ctx.handle, ctypes.byref(h)))
+        self.handle = h.value
+        self.shapes = {}
+
+    def close(self):
+        if self.handle:
+            self.lib.nimbus_cuda_engine_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def member_bytes(self, desc: MemberDesc) -> int:
+        return int(self.lib.nimbus_cuda_engine_member_bytes(ctypes.byref(desc)))
+
+    def admit(self, desc: MemberDesc, state, reserve_bytes: int = 0) -> int:
+        """Admit a member with its initial state; raises NimbusCudaError
+        (OUT_OF_MEMORY) when it does not fit the free HBM."""
+        mid = ctypes.c_int(0)
+        st = member_state(state)
+        self.ctx.check(self.lib.nimbus_cuda_engine_admit(self.handle, ctypes.byref(desc), ctypes.byref(st),
+                                                         int(reserve_bytes), ctypes.byref(mid)))
+        self.shapes[mid.value] = (desc.nx, desc.ny, desc.nz)
+        return mid.value
+
+    def try_admit(self, desc: MemberDesc, state, reserve_bytes: int = 0) -> Optional[int]:
+        """Admission that returns None instead of raising when HBM is full."""
+        mid = ctypes.c_int(0)
+        st = member_state(state)
+        rc = self.lib.nimbus_cuda_engine_admit(self.handle, ctypes.byref(desc), ctypes.byref(st),
+                                               int(reserve_bytes), ctypes.byref(mid))
+        if rc == NIMBUS_ERR_OUT_OF_MEMORY:
+            return None
+        self.ctx.check(rc)
+        self.shapes[mid.value] = (desc.nx, desc.ny, desc.nz)
+        return mid.value
+
+    def retire(self, member_id: int):
+        self.ctx.check(self.lib.nimbus_cuda_engine_retire(self.handle, int(member_id)))
+        self.shapes.pop(member_id, None)
+
+    def read(self, member_id: int) -> dict:
+        shape = self.shapes[member_id]
+        out = {k: np.empty(shape, np.float32) for k in MEMBER_FIELDS}
+        self.ctx.check(self.lib.nimbus_cuda_engine_read(self.handle, int(member_id), ctypes.byref(member_state(out))))
+        return out
+
+    def read_into(self, member_id: int, out: dict):
+        st = MemberState()
+        for k in MEMBER_FIELDS:
+            setattr(st, k, _f(out[k]))
+        self.ctx.check(self.lib.nimbus_cuda_engine_read(self.handle, int(member_id), ctypes.byref(st)))
+
+    def write(self, member_id: int, state: dict):
+        """Replace a member's state from host arrays (pinned arrays copy fastest)."""
+        st = MemberState()
+        for k in MEMBER_FIELDS:
+            a = state[k]
+            assert a.dtype == np.float32 and a.flags["C_CONTIGUOUS"] and a.shape == self.shapes[member_id], k
+            setattr(st, k, _f(a))
+        self.ctx.check(self.lib.nimbus_cuda_engine_write(self.handle, int(member_id), ctypes.byref(st)))
+
+    def step(self, n: int = 1):
+        self.ctx.check(self.lib.nimbus_cuda_engine_step(self.handle, int(n)))
+
+    def synchronize(self):
+        self.ctx.check(self.lib.nimbus_cuda_engine_synchronize(self.handle))
+
+    def member_status(self, member_id: int) -> int:
+        f = ctypes.c_uint(0)
+        self.ctx.check(self.lib.nimbus_cuda_engine_member_status(self.handle, int(member_id), ctypes.byref(f)))
+        return f.value
+
+    def set_graph(self, enable: bool):
+        self.ctx.check(self.lib.nimbus_cuda_engine_set_graph(self.handle, int(bool(enable))))
+
+    @property
+    def members(self) -> int:
+        return int(self.lib.nimbus_cuda_engine_members(self.handle))
+
+    @property
+    def launches_per_step(self) -> int:
+        return int(self.lib.nimbus_cuda_engine_launches_per_step(self.handle))
 
 
 class CudaComputeBackend:

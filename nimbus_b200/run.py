@@ -1,22 +1,29 @@
-"""Device-resident single run: the state of one supercell stays in HBM and
-each large step of the hot path is enqueued through the C-ABI.
+"""Device-resident runs of the hot path.
 
-One large step (the order of step_dynamics_new, dynamics.cpp:6590-6961, for
-the hot path it owns):
-  1. open the retained transport context: zero the face mass-flux sums
-     (CartesianCGridTransportContext::begin);
-  2. the acoustic loop: N substeps, each with mass-flux accumulation, the
-     fused substep and the boundary closure; the KW78 radiation memory is
-     re-seeded from the live faces at the start of every large step, as
-     seed_acoustic_radiation does (split_explicit.cpp:174-205);
-  3. conservative WENO5 transport of theta, qv, qc, qr against the retained
-     fluxes and densities (advection_batch.cpp:565-760).
+One large step (the order of step_dynamics_new, dynamics.cpp:5123-7317, for
+the phases this backend owns):
+  1. Heun slow step: k1, predictor, k2, the FP32 average applied with dt
+     (prepare_slow_rk2_tendencies + apply_slow_tendencies);
+  2. boundary refresh apply_acoustic(0) and the KW78 seed
+     (seed_acoustic_radiation, dynamics.cpp:5384-5396);
+  3. the acoustic loop: N substeps, each with the retained mass-flux
+     accumulation, continuity + EOS, momentum and the boundary closure
+     (split_explicit.cpp:174-260);
+  4. conservative WENO5 transport of theta, qv, qc, qr against the retained
+     fluxes and densities (advection_batch.cpp:565-760);
+  5. the Kessler step over the C-grid cell domain (microphysics_step.cpp);
+  6. the EOS pressure re-projection (eos_apply.cpp).
 
-PyTorch is used only to own device memory; every kernel is the library's.
+Two drivers run it:
+  ResidentRun   the plain path: one run, each operation enqueued through its
+                own C-ABI entry point (the per-dispatch interface the
+                reference's compute backends expose);
+  EngineRun     the member engine: any number of runs, one batched launch per
+                phase, the step replayed from a CUDA graph.
+PyTorch only owns device memory for ResidentRun; every kernel is the
+library's.
 """
 from __future__ import annotations
-
-from dataclasses import dataclass
 
 import numpy as np
 import torch
@@ -29,9 +36,15 @@ POSITIVE = (0, 1, 1, 1)  # theta is the only non-positive-definite scalar (advec
 PROGNOSTIC = ("u", "v", "w", "rho", "p") + SCALARS
 
 
+def substeps_for(case: Case, state, base) -> int:
+    return resolve_substep_count(case.dt, max_sound_speed(state["p"], state["rho"], base), case.dx, case.dy,
+                                 case.dz, case.substeps)
+
+
 class ResidentRun:
     def __init__(self, ctx: cuda.Context, case: Case, state=None, base=None, device="cuda",
-                 precision: int = cuda.PRECISION_FP32, autotune: bool = True):
+                 precision: int = cuda.PRECISION_FP32, autotune: bool = True, coriolis_f: float = 0.0,
+                 microphysics: bool = True):
         self.ctx = ctx
         self.precision = precision
         self.tuned = None
@@ -42,25 +55,31 @@ class ResidentRun:
         if state is None:
             state, base = initial_state(case)
         self.base = base
-        self.n_substeps = resolve_substep_count(case.dt, max_sound_speed(state["p"], state["rho"], base), case.dx,
-                                                case.dy, case.dz, case.substeps)
+        self.microphysics = microphysics
+        self.n_substeps = substeps_for(case, state, base)
         dev = torch.device(device)
         self.fields = {k: torch.from_numpy(np.ascontiguousarray(state[k])).to(dev) for k in PROGNOSTIC}
         shape = case.shape
         self.mf = [torch.zeros(shape, dtype=torch.float32, device=dev) for _ in range(3)]
         self.rho_begin = torch.zeros(shape, dtype=torch.float32, device=dev)
         self.wave = torch.zeros(2 * (case.nx + case.ny) * case.nz, dtype=torch.float32, device=dev)
-        self.rho0 = torch.from_numpy(base["rho0"]).to(dev)
-        self.p0 = torch.from_numpy(base["p0"]).to(dev)
+        self.prof = {k: torch.from_numpy(np.ascontiguousarray(base[k], dtype=np.float64)).to(dev)
+                     for k in ("rho0", "p0", "qv0", "u0", "v0")}
         self.stream = ctx.stream
         grid = (case.dx, case.dy, case.dz)
         n = self.n_substeps
-        self._loop = cuda.batched_args(self.fields, self.rho0, self.p0, case.dt / n, n, grid, case.bc, *self.mf,
-                                       (case.dt / n) / case.dt, None, self.wave, self.rho_begin,
+        f = self.fields
+        self._slow = cuda.slow_args(f, self.prof, grid, dt_large=case.dt, coriolis_f=coriolis_f,
+                                    memory=cuda.MEMORY_DEVICE)
+        self._refresh = cuda.boundary_args(f, grid, case.bc, 0.0)
+        self._loop = cuda.batched_args(f, self.prof["rho0"], self.prof["p0"], case.dt / n, n, grid, case.bc,
+                                       *self.mf, (case.dt / n) / case.dt, None, self.wave, self.rho_begin,
                                        memory=cuda.MEMORY_DEVICE)
-        qs = [self.fields[k] for k in SCALARS]
-        self._transport = cuda.transport_args(qs, qs, POSITIVE, self.fields["rho"], self.rho_begin, *self.mf, case.dt,
+        qs = [f[k] for k in SCALARS]
+        self._transport = cuda.transport_args(qs, qs, POSITIVE, f["rho"], self.rho_begin, *self.mf, case.dt,
                                               grid, weno=True, top_open=case.bc[5] == 2, memory=cuda.MEMORY_DEVICE)
+        self._kessler = cuda.kessler_args(f, case.dz, case.dt, memory=cuda.MEMORY_DEVICE)
+        self._eos = cuda.eos_args(f["p"], f["rho"], f["theta"], f["qv"], f["qc"], f["qr"], memory=cuda.MEMORY_DEVICE)
         self.torch_stream = torch.cuda.ExternalStream(self.stream, device=dev)
 
     @property
@@ -69,12 +88,18 @@ class ResidentRun:
 
     def step(self):
         """Enqueue one large step on the context stream (no host synchronisation)."""
-        self.ctx.set_precision(self.precision)
+        c = self.ctx
+        c.set_precision(self.precision)
+        c.check(c.slow_step(self._slow))
+        c.check(c.acoustic_boundaries(self._refresh))
         with torch.cuda.stream(self.torch_stream):
             for m in self.mf:
                 m.zero_()
-        self.ctx.check(self.ctx.acoustic_batched(self._loop))
-        self.ctx.check(self.ctx.scalar_transport(self._transport))
+        c.check(c.acoustic_batched(self._loop))
+        c.check(c.scalar_transport(self._transport))
+        if self.microphysics:
+            c.check(c.kessler_step(self._kessler))
+        c.check(c.eos_projection(self._eos))
 
     def download(self) -> dict:
         torch.cuda.current_stream().wait_stream(self.torch_stream)
@@ -82,10 +107,46 @@ class ResidentRun:
         return {k: v.cpu().numpy() for k, v in self.fields.items()}
 
 
+class EngineRun:
+    """Runs resident in one member engine, advanced together."""
+
+    def __init__(self, ctx: cuda.Context, precision: int = cuda.PRECISION_FP32, graph: bool = True):
+        self.ctx = ctx
+        self.precision = precision
+        self.engine = cuda.Engine(ctx)
+        self.engine.set_graph(graph)
+        self.members = {}
+
+    def admit(self, case: Case, state=None, base=None, coriolis_f: float = 0.0, microphysics: bool = True,
+              reserve_bytes: int = 0, n_substeps: int | None = None):
+        if state is None:
+            state, base = initial_state(case)
+        n = n_substeps or substeps_for(case, state, base)
+        desc = cuda.member_desc(case.shape, (case.dx, case.dy, case.dz), case.dt, n, case.bc, base, coriolis_f,
+                                microphysics=int(microphysics))
+        mid = self.engine.admit(desc, state, reserve_bytes)
+        self.members[mid] = (case, n)
+        return mid
+
+    def step(self, n: int = 1):
+        self.ctx.set_precision(self.precision)
+        self.engine.step(n)
+
+    def read(self, member_id: int) -> dict:
+        return self.engine.read(member_id)
+
+    @property
+    def cells(self) -> int:
+        return sum(c.cells for c, _ in self.members.values())
+
+    def close(self):
+        self.engine.close()
+
+
 class HostStepper:
-    """The same large step through the reference-facing host-memory API:
-    every call uploads its inputs from (pinned) host arrays and returns the
-    results to them, as the reference's fence-confirmed dispatches do."""
+    """The same large step through the library's host-buffer API: every step
+    writes the member's state from pinned host arrays, advances it and reads
+    it back, so the host<->device copies are part of each step."""
 
     def __init__(self, ctx: cuda.Context, case: Case, state=None, base=None, pin=True,
                  precision: int = cuda.PRECISION_FP32):
@@ -94,44 +155,25 @@ class HostStepper:
         self.case = case
         if state is None:
             state, base = initial_state(case)
-        self.base = base
-        self.n_substeps = resolve_substep_count(case.dt, max_sound_speed(state["p"], state["rho"], base), case.dx,
-                                                case.dy, case.dz, case.substeps)
 
         def host(a):
             t = torch.from_numpy(np.ascontiguousarray(a))
             return (t.pin_memory() if pin else t.clone()).numpy()
 
         self.fields = {k: host(state[k]) for k in PROGNOSTIC}
-        shape = case.shape
-        self.mf = [host(np.zeros(shape, np.float32)) for _ in range(3)]
-        self.rho_begin = host(np.zeros(shape, np.float32))
-        self.wave = host(np.zeros(2 * (case.nx + case.ny) * case.nz, np.float32))
-        grid = (case.dx, case.dy, case.dz)
-        n = self.n_substeps
-        self._loop = cuda.batched_args(self.fields, base["rho0"], base["p0"], case.dt / n, n, grid, case.bc, *self.mf,
-                                       (case.dt / n) / case.dt, None, self.wave, self.rho_begin)
-        qs = [self.fields[k] for k in SCALARS]
-        self._transport = cuda.transport_args(qs, qs, POSITIVE, self.fields["rho"], self.rho_begin, *self.mf, case.dt,
-                                              grid, weno=True, top_open=case.bc[5] == 2)
+        self.run = EngineRun(ctx, precision)
+        self.member = self.run.admit(case, state, base)
+        self.n_substeps = self.run.members[self.member][1]
 
     def bytes_per_step(self):
-        """Host<->device bytes one step moves through the host API (counted
-        from the arrays each call stages)."""
-        n = self.case.cells * 4
-        w = self.wave.nbytes
-        prof = self.base["rho0"].nbytes + self.base["p0"].nbytes
-        # acoustic batch: in u,v,w,rho,p,theta + 3 mass fluxes + profiles (the KW78
-        #                 memory is seeded on the device); out u,v,w,rho,p + 3 mass
-        #                 fluxes + rho_begin + wave history
-        # transport:      in rho_end, rho_begin, 3 mass fluxes, 4 scalars; out 4 scalars
-        h2d = 9 * n + prof + 9 * n
-        d2h = 9 * n + w + 4 * n
-        return h2d, d2h
+        """Host<->device bytes one step moves (the nine prognostic fields each way)."""
+        n = self.case.cells * 4 * len(PROGNOSTIC)
+        return n, n
 
     def step(self):
-        self.ctx.set_precision(self.precision)
-        for m in self.mf:
-            m[...] = 0.0
-        self.ctx.check(self.ctx.acoustic_batched(self._loop))
-        self.ctx.check(self.ctx.scalar_transport(self._transport))
+        self.run.engine.write(self.member, self.fields)
+        self.run.step(1)
+        self.run.engine.read_into(self.member, self.fields)
+
+    def close(self):
+        self.run.close()

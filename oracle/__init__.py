@@ -145,6 +145,38 @@ class Restatement:
                                       _fp(st["qc"]), _fp(st["qr"]), _fp(dth), _fp(dqv), _fp(dqc), _fp(dqr))
         return dth, dqv, dqc, dqr
 
+    def acoustic_boundaries(self, st, grid, bc, dt_small=0.0, wave=None, frame=(0.0, 0.0)):
+        """apply_acoustic(dt_small) on u, v, w, rho, p in place (dt_small == 0:
+        refresh only, no wave history needed)."""
+        u, v, w, rho, p = (st[k] for k in ("u", "v", "w", "rho", "p"))
+        self._chk(u, v, w, rho, p)
+        nx, ny, nz = u.shape
+        if wave is None:
+            wave = np.zeros(2 * (nx + ny) * nz, self.dtype)
+        self.lib.oracle_acoustic_bcs(nx, ny, nz, ctypes.c_double(grid[0]), ctypes.c_double(grid[1]), _fp(u), _fp(v),
+                                     _fp(w), _fp(rho), _fp(p), _fp(wave), ctypes.c_double(dt_small), _bcs(bc),
+                                     ctypes.c_double(frame[0]), ctypes.c_double(frame[1]))
+
+    def large_step(self, st, base, grid, dt, n_substeps, bc, coriolis_f=0.0, microphysics=True):
+        """One large step of the hot path in the reference's order
+        (dynamics.cpp:5123-7317): Heun slow step, boundary refresh, the
+        acoustic loop (KW78 seed, N substeps with retained mass flux),
+        conservative WENO5 transport of theta, qv, qc, qr, the Kessler step
+        over the C-grid cell domain and the EOS re-projection.  In place on
+        the state dict; raises when the EOS projection refuses the state."""
+        self.slow_rk2_step(st, base, grid, dt, coriolis_f=coriolis_f)
+        self.acoustic_boundaries(st, grid, bc, 0.0)
+        loop = self.acoustic_loop(st, base["rho0"], base["p0"], dt, n_substeps, grid, bc)
+        qs = [st["theta"], st["qv"], st["qc"], st["qr"]]
+        self.scalar_transport(qs, [0, 1, 1, 1], st["rho"], loop["rho_begin"], loop["mfx"], loop["mfy"], loop["mfz"],
+                              dt, grid, weno=True, top_open=bc[5] == 2)
+        nx, ny, nz = st["u"].shape
+        if microphysics:
+            self.kessler_step(st, grid[2], dt, (1, nx - 1, 1, ny - 1, 0, nz))
+        if not self.eos_projection(st["p"], st["rho"], st["theta"], st["qv"], st["qc"], st["qr"]):
+            raise FloatingPointError("EOS pressure projection rejected an invalid physical state")
+        return loop
+
     def eos_projection(self, p, rho, theta, qv=None, qc=None, qr=None):
         """EOS pressure re-projection in place; returns False (p untouched)
         when the state is refused.  qv/qc/qr (all or none) add the moist-state

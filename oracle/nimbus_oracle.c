@@ -1073,9 +1073,17 @@ void oracle_kessler_tendencies(int nx, int ny, int nz, double dz, double dt, con
     free(temp);
 }
 
-/* Application of the Kessler tendencies over the domain: water species as
- * bounded_water_value (microphysics_step.cpp:503-532), clamp to [0, 0.05]
- * with non-finite -> 0; theta as theta + dt*dtheta rounded once. */
+/* Application of the Kessler tendencies over the domain, as the CPU commit
+ * of step_microphysics_once does it with radiation, boundary layer and
+ * stochastic multipliers off (microphysics_step.cpp:3026-3245):
+ *  - a non-finite tendency counts as zero;
+ *  - water species: bounded_water_value (:480-515), float(q + dq*dt) clamped
+ *    to [0, 0.05], non-finite -> 0;
+ *  - theta: theta + clamp(dtheta*dt, -50 K, 50 K) in FP64 (a non-finite sum
+ *    keeps theta, or theta0 = 300 K if theta itself is not finite), stored
+ *    through clamp_theta_k (field_bounds.hpp:68-71): [200, 700] K,
+ *    non-finite -> 300 K.  The theta storage residual is only carried with
+ *    radiation on and stays zero here. */
 void oracle_kessler_apply(int nx, int ny, int nz, double dt, const int* domain, REAL* theta, REAL* qv, REAL* qc,
                           REAL* qr, const REAL* dth, const REAL* dqv, const REAL* dqc, const REAL* dqr)
 {
@@ -1086,14 +1094,26 @@ void oracle_kessler_apply(int nx, int ny, int nz, double dt, const int* domain, 
                 const size_t c = IDX(i, j, k);
 #define WATER(q, dq)                                                       \
     do {                                                                   \
-        const REAL raw = (REAL)((double)(q) + (double)(dq) * dt);          \
+        const double dqs = isfinite((double)(dq)) ? (double)(dq) : 0.0;    \
+        const REAL raw = (REAL)((double)(q) + dqs * dt);                   \
         (q) = !isfinite(raw) ? (REAL)0 : (raw < 0 ? (REAL)0 : ((REAL)0.05f < raw ? (REAL)0.05f : raw)); \
     } while (0)
                 WATER(qv[c], dqv[c]);
                 WATER(qc[c], dqc[c]);
                 WATER(qr[c], dqr[c]);
 #undef WATER
-                theta[c] = (REAL)((double)theta[c] + (double)dth[c] * dt);
+                const double told = (double)theta[c];
+                const double rate = isfinite((double)dth[c]) ? (double)dth[c] : 0.0;
+                double total = rate * dt;
+                if (!isfinite(total)) total = 0.0;
+                const double limited = total < -50.0 ? -50.0 : (50.0 < total ? 50.0 : total);
+                double tn = told + limited;
+                if (!isfinite(tn)) tn = isfinite(told) ? told : 300.0;
+                const REAL stored = (REAL)tn;
+                theta[c] = !isfinite((double)stored) ? (REAL)300.0f
+                                                     : (stored < (REAL)200.0f ? (REAL)200.0f
+                                                                              : ((REAL)700.0f < stored ? (REAL)700.0f
+                                                                                                       : stored));
             }
 }
 

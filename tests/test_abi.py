@@ -17,7 +17,7 @@ HEADER = ROOT / "include" / "nimbus_cuda.h"
 
 def declared_functions():
     text = HEADER.read_text()
-    return sorted(set(re.findall(r"^\s*(?:nimbus_status|void\*?|const char\*|int|uint64_t)\s+(nimbus_cuda_\w+)\(",
+    return sorted(set(re.findall(r"^\s*(?:nimbus_status|void\*?|const char\*|int|uint64_t|size_t)\s+(nimbus_cuda_\w+)\(",
                                  text, re.M)))
 
 
@@ -52,6 +52,9 @@ def _c_layout(struct_name, fields, tmp_path):
     ("nimbus_slow_args", cuda.SlowArgs),
     ("nimbus_kessler_args", cuda.KesslerArgs),
     ("nimbus_eos_args", cuda.EosArgs),
+    ("nimbus_boundary_args", cuda.BoundaryArgs),
+    ("nimbus_member_desc", cuda.MemberDesc),
+    ("nimbus_member_state", cuda.MemberState),
 ])
 def test_argument_block_layout_matches_header(struct_name, cls, tmp_path):
     fields = [f for f, _ in cls._fields_]

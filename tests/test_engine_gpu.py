@@ -1,0 +1,213 @@
+"""The whole large step on the device, bit for bit against the oracle, and the
+member engine against the per-operation path.
+
+Reference precision: the plain path (one C-ABI call per operation) and the
+engine (batched launches under a CUDA graph) must both reproduce the oracle's
+composition of the pinned rows -- Heun slow step, boundary refresh, KW78 seed,
+acoustic loop, WENO5 transport, Kessler, EOS -- with zero ULP.  FP32 form:
+a member's result is identical alone and in any mix (no cross-member
+arithmetic), and identical to the plain FP32 path (same kernels)."""
+import numpy as np
+import pytest
+
+import oracle
+from nimbus_b200 import cuda
+from nimbus_b200.initial import Case, cloudy_state
+from nimbus_b200.run import PROGNOSTIC, EngineRun, ResidentRun
+
+pytestmark = pytest.mark.gpu
+
+BCS = {
+    "radiative": (1, 1, 1, 1, 1, 0),
+    "periodic_open": (0, 0, 0, 0, 0, 2),
+    "walls_sponge": (2, 3, 4, 1, 1, 1),
+}
+
+
+def assert_bitwise(a, b, what):
+    a = np.ascontiguousarray(a)
+    b = np.ascontiguousarray(b)
+    bad = np.count_nonzero(a.view(np.uint32) != b.view(np.uint32))
+    assert bad == 0, f"{what}: {bad}/{a.size} values differ, max |diff| {np.abs(a - b).max():.3e}"
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = cuda.Context(0)
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="module")
+def o32():
+    return oracle.Restatement("f32")
+
+
+def _case(shape, bc, seed, dt=4.0, grid=(700.0, 800.0, 350.0)):
+    return Case(*shape, *grid, dt, seed=seed, bc=bc)
+
+
+def _state(case, seed):
+    st, base = cloudy_state(case, seed=seed)
+    if case.bc[0] in (2, 3):
+        st["u"][0] = 0.0
+    if case.bc[1] in (2, 3):
+        st["u"][-2:] = 0.0
+    if case.bc[2] in (2, 3):
+        st["v"][:, 0] = 0.0
+    if case.bc[3] in (2, 3):
+        st["v"][:, -2:] = 0.0
+    return st, base
+
+
+def _oracle_steps(o32, case, st, base, n_sub, steps, coriolis_f):
+    ref = {k: v.copy() for k, v in st.items()}
+    for _ in range(steps):
+        o32.large_step(ref, base, (case.dx, case.dy, case.dz), case.dt, n_sub, case.bc, coriolis_f=coriolis_f)
+    return ref
+
+
+@pytest.mark.parametrize("bc_name", list(BCS))
+def test_plain_large_step_matches_oracle(ctx, o32, bc_name):
+    case = _case((21, 17, 15), BCS[bc_name], seed=3)
+    st, base = _state(case, 3)
+    run = ResidentRun(ctx, case, {k: v.copy() for k, v in st.items()}, base,
+                      precision=cuda.PRECISION_REFERENCE, autotune=False, coriolis_f=1e-4)
+    ctx.set_substep_form(cuda.SUBSTEP_SPLIT)
+    for _ in range(2):
+        run.step()
+    got = run.download()
+    ctx.set_substep_form(cuda.SUBSTEP_AUTO)
+    want = _oracle_steps(o32, case, st, base, run.n_substeps, 2, 1e-4)
+    for k in PROGNOSTIC:
+        assert_bitwise(got[k], want[k], f"{bc_name} {k}")
+
+
+@pytest.mark.parametrize("graph", [True, False], ids=["graph", "eager"])
+def test_engine_ragged_members_match_oracle(ctx, o32, graph):
+    """Three members of different shapes, spacings, dt and substep counts in
+    one engine, three large steps: each equals the oracle run alone."""
+    specs = [((19, 16, 13), BCS["radiative"], 4.0, 5), ((24, 14, 17), BCS["walls_sponge"], 3.0, 7),
+             ((12, 22, 9), BCS["periodic_open"], 5.0, 4)]
+    run = EngineRun(ctx, precision=cuda.PRECISION_REFERENCE, graph=graph)
+    members = []
+    for i, (shape, bc, dt, n_sub) in enumerate(specs):
+        case = _case(shape, bc, seed=10 + i, dt=dt)
+        st, base = _state(case, 10 + i)
+        mid = run.admit(case, st, base, coriolis_f=1e-4, n_substeps=n_sub)
+        members.append((mid, case, st, base, n_sub))
+    run.step(3)
+    run.engine.synchronize()
+    for mid, case, st, base, n_sub in members:
+        got = run.read(mid)
+        want = _oracle_steps(o32, case, st, base, n_sub, 3, 1e-4)
+        for k in PROGNOSTIC:
+            assert_bitwise(got[k], want[k], f"member {mid} {k}")
+    run.close()
+
+
+def test_engine_member_alone_equals_member_in_mix(ctx):
+    """FP32 form: the result of a member does not depend on its batch mates,
+    on admissions and retirements between steps, or on the graph."""
+    case = _case((26, 21, 18), BCS["radiative"], seed=40, dt=3.0)
+    st, base = _state(case, 40)
+    alone = EngineRun(ctx, precision=cuda.PRECISION_FP32)
+    a = alone.admit(case, st, base)
+    alone.step(4)
+    want = alone.read(a)
+    alone.close()
+
+    mix = EngineRun(ctx, precision=cuda.PRECISION_FP32)
+    others = []
+    for i, shape in enumerate([(40, 33, 25), (9, 11, 6)]):
+        c2 = _case(shape, BCS["periodic_open"], seed=50 + i, dt=2.5)
+        s2, b2 = _state(c2, 50 + i)
+        others.append(mix.admit(c2, s2, b2))
+    m = mix.admit(case, st, base)
+    mix.step(1)
+    mix.engine.retire(others[0])          # a batch mate leaves
+    mix.step(2)
+    c3 = _case((30, 12, 20), BCS["walls_sponge"], seed=60, dt=3.5)
+    s3, b3 = _state(c3, 60)
+    mix.admit(c3, s3, b3)                 # another arrives
+    mix.step(1)
+    got = mix.read(m)
+    mix.close()
+    for k in PROGNOSTIC:
+        assert_bitwise(got[k], want[k], k)
+
+
+def test_engine_matches_plain_fp32_path(ctx):
+    case = _case((23, 19, 16), BCS["radiative"], seed=70, dt=3.0)
+    st, base = _state(case, 70)
+    plain = ResidentRun(ctx, case, {k: v.copy() for k, v in st.items()}, base, precision=cuda.PRECISION_FP32,
+                        autotune=False)
+    ctx.set_substep_form(cuda.SUBSTEP_SPLIT)
+    for _ in range(2):
+        plain.step()
+    got_plain = plain.download()
+    ctx.set_substep_form(cuda.SUBSTEP_AUTO)
+    run = EngineRun(ctx, precision=cuda.PRECISION_FP32)
+    mid = run.admit(case, st, base)
+    run.step(2)
+    got = run.read(mid)
+    run.close()
+    for k in PROGNOSTIC:
+        assert_bitwise(got[k], got_plain[k], k)
+
+
+def test_admission_refuses_beyond_free_memory(ctx):
+    case = _case((10, 10, 8), BCS["radiative"], seed=1)
+    st, base = _state(case, 1)
+    run = EngineRun(ctx)
+    desc = cuda.member_desc(case.shape, (case.dx, case.dy, case.dz), case.dt, 4, case.bc, base)
+    assert run.engine.member_bytes(desc) > 40 * case.cells
+    assert run.engine.try_admit(desc, st, reserve_bytes=1 << 50) is None
+    assert run.engine.members == 0
+    mid = run.engine.admit(desc, st)
+    assert run.engine.members == 1
+    run.engine.retire(mid)
+    assert run.engine.members == 0
+    run.step(1)  # an empty engine steps as a no-op
+    run.close()
+
+
+def test_boundary_refresh_matches_oracle(ctx, o32):
+    import torch
+    case = _case((14, 12, 9), BCS["walls_sponge"], seed=5)
+    st, _ = _state(case, 5)
+    dev = {k: torch.from_numpy(st[k].copy()).cuda() for k in ("u", "v", "w", "rho", "p")}
+    torch.cuda.synchronize()
+    ctx.check(ctx.acoustic_boundaries(cuda.boundary_args(dev, (case.dx, case.dy), case.bc, 0.0, stream=ctx.stream)))
+    ctx.synchronize()
+    want = {k: st[k].copy() for k in ("u", "v", "w", "rho", "p")}
+    o32.acoustic_boundaries(want, (case.dx, case.dy, case.dz), case.bc, 0.0)
+    for k in want:
+        assert_bitwise(dev[k].cpu().numpy(), want[k], k)
+
+
+def test_engine_reports_a_refused_member_only(ctx):
+    """A member whose EOS projection is refused keeps its pressure and is
+    flagged; its batch mate is unaffected."""
+    good_case = _case((12, 11, 9), BCS["radiative"], seed=80)
+    gs, gb = _state(good_case, 80)
+    bad_case = _case((10, 13, 8), BCS["radiative"], seed=81)
+    bs, bb = _state(bad_case, 81)
+    bs["theta"][0, 5, 3] = -5.0   # a ghost-ring temperature nothing repairs; the EOS refuses it
+    run = EngineRun(ctx, precision=cuda.PRECISION_FP32)
+    g = run.admit(good_case, gs, gb)
+    b = run.admit(bad_case, bs, bb)
+    run.step(1)
+    with pytest.raises(cuda.NimbusCudaError):
+        run.engine.synchronize()
+    assert run.engine.member_status(b) & 4
+    assert run.engine.member_status(g) == 0
+    alone = EngineRun(ctx, precision=cuda.PRECISION_FP32)
+    a = alone.admit(good_case, gs, gb)
+    alone.step(1)
+    want = alone.read(a)
+    got = run.read(g)
+    for k in PROGNOSTIC:
+        assert_bitwise(got[k], want[k], k)
+    run.close()
+    alone.close()
