@@ -1,15 +1,22 @@
-"""Benchmark of the Nimbus hot path on B200: one large step = the
-split-explicit acoustic loop (N substeps with boundary closure and retained
-mass flux) + conservative WENO5 transport of theta, qv, qc, qr.
+"""Benchmark of the Nimbus hot path on B200.
+
+One step = one large step of every run in the workload: Heun slow step,
+boundary refresh and KW78 seed, N acoustic substeps (retained mass flux,
+continuity + EOS, momentum, boundary closure), conservative WENO5 transport
+of theta, qv, qc, qr, the Kessler step and the EOS re-projection.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload ensemble_64|supercell_250m_256x256x80|...]
 
 Prints one JSON line (rank 0).  `value` is device-timed whole-job throughput
-in cell-updates/s (one cell advanced one large step) with the state resident
-in HBM; `e2e` is the same metric through the reference-facing host-memory API
-(every step stages its inputs from pinned host memory and reads its results
-back).  Under torchrun each rank advances its own independent run (ensemble
-members share nothing), so scaling is weak.
+in cell-updates/s (one cell advanced one large step) of the batched FP32 form
+(member engine, CUDA graph) with the state resident in HBM.  `config` carries
+the plain per-operation path on the same runs, the reference-precision form,
+the error of the FP32 form against the FP64 oracle, and the serving numbers
+(p50/p99 completion latency beside throughput).  `e2e` is the same metric
+through the library's host-buffer API (every step writes each run's state
+from pinned host memory and reads it back).  Under torchrun each rank
+advances its own ensemble (members share nothing), so scaling is weak.
 """
 from __future__ import annotations
 
@@ -27,12 +34,18 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "cell-updates/s"
-WORKLOAD = "supercell_250m_256x256x80"
-# Algorithmic (compulsory) bytes per cell: one acoustic substep reads
-# u,v,w,rho,p,theta and the three retained mass fluxes and writes
-# u,v,w,rho,p and the three mass fluxes (17 FP32 fields).
-SUBSTEP_BYTES_PER_CELL = 68
-TRANSPORT_BYTES_PER_CELL = lambda scalars: 20 + 8 * scalars  # noqa: E731
+WORKLOAD = "ensemble_64"
+SINGLE_RUNS = ("supercell_1km_64x64x40", "supercell_250m_256x256x80", "supercell_100m_512x512x128")
+# Algorithmic (compulsory) bytes per cell (FP32 fields, each read once and
+# written once per named pass): acoustic substep 68 (reads u,v,w,rho,p,theta
+# and three retained fluxes; writes u,v,w,rho,p and the fluxes), WENO5
+# transport 20 + 8 per scalar, slow Heun 112, Kessler 40, EOS 12.
+SUBSTEP_BYTES = 68
+STEP_FIXED_BYTES = (20 + 8 * 4) + 112 + 40 + 12
+
+
+def step_bytes(n_substeps: int) -> int:
+    return SUBSTEP_BYTES * n_substeps + STEP_FIXED_BYTES
 
 
 def parse():
@@ -42,11 +55,15 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", default=WORKLOAD)
-    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--members", type=int, default=64)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--plain-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--substep-form", choices=("auto", "fused", "split"), default="auto",
-                    help="acoustic substep kernels: autotuned (default) or pinned (profiling runs pin the "
-                         "form the plain run chose, since a profiler distorts the autotuner's timings)")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-error", action="store_true")
+    ap.add_argument("--serving-requests", type=int, default=32)
+    ap.add_argument("--error-seconds", type=float, default=600.0)
     ap.add_argument("--precision", choices=("fp32", "reference"), default="fp32",
                     help="fp32: FP32 stencils on the FP64 base state (the timed form); "
                          "reference: FP64 interior arithmetic, bit-exact to the CPU solver")
@@ -57,53 +74,57 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
+def workload_cases(name, rank=0, members=64):
+    from nimbus_b200.ensemble import ensemble_cases
+    from nimbus_b200.initial import benchmark_case
+
+    if name == "ensemble_64":
+        return ensemble_cases(members, seed=2026 + 1000 * rank)
+    case = benchmark_case(name)
+    case.member = rank
+    case.seed = case.seed + 1000 * rank
+    return [case]
+
+
 # ---------------------------------------------------------------------------
-# CPU baseline: the reference CPU solver (oracle/_ref, built from the
-# reference's own sources) on a bounded sub-domain sample of the workload.
+# The reference CPU path: the reference solver's own objects (oracle/_ref,
+# built from its sources) assembled into one large step, on a bounded sample.
 # ---------------------------------------------------------------------------
 def sample_case(case):
     from nimbus_b200.initial import Case
 
-    nx = min(case.nx, 128)
-    ny = min(case.ny, 128)
+    nx, ny = min(case.nx, 96), min(case.ny, 96)
     return Case(nx, ny, case.nz, case.dx, case.dy, case.dz, case.dt, substeps=case.substeps,
                 noise_amp=case.noise_amp, seed=case.seed, bubble_rh=case.bubble_rh, bubble_rz=case.bubble_rz,
-                bubble_zc=case.bubble_zc, bc=case.bc)
+                bubble_zc=case.bubble_zc, bubble_amp=case.bubble_amp, bc=case.bc, member=case.member)
 
 
 def reference_step_runner(case, threads):
-    """Returns (step_fn, kind, cores, n_substeps): one large step of the
-    reference CPU path on the sample grid."""
+    """(step_fn, kind, cores, n_substeps): one large step of the reference CPU
+    path on `case`'s grid (the restatement when the reference is not built)."""
     import oracle
-    from nimbus_b200.initial import initial_state, max_sound_speed, resolve_substep_count
+    from nimbus_b200.initial import initial_state
+    from nimbus_b200.run import substeps_for
 
     st, base = initial_state(case)
-    n = resolve_substep_count(case.dt, max_sound_speed(st["p"], st["rho"], base), case.dx, case.dy, case.dz,
-                              case.substeps)
+    n = substeps_for(case, st, base)
     grid = (case.dx, case.dy, case.dz)
     if oracle.reference_available():
-        ref = oracle.ReferenceHarness(threads=threads)
-        kind, cores = "reference", ref.threads
-
-        def step():
-            out = ref.acoustic_loop(st, base["rho0"], base["p0"], case.dt, n, grid, case.bc)
-            qs = [st[k] for k in ("theta", "qv", "qc", "qr")]
-            ref.scalar_transport(qs, [0, 1, 1, 1], st["u"], st["v"], st["w"], st["rho"], out["rho_begin"],
-                                 out["mfx"], out["mfy"], out["mfz"], case.dt, grid, top_open=case.bc[5] == 2)
+        impl = oracle.ReferenceHarness(threads=threads)
+        kind, cores = "reference", impl.threads
     else:
-        port = oracle.Restatement("f32")
+        impl = oracle.Restatement("f32")
         kind, cores = "port", 1
 
-        def step():
-            out = port.acoustic_loop(st, base["rho0"], base["p0"], case.dt, n, grid, case.bc)
-            qs = [st[k] for k in ("theta", "qv", "qc", "qr")]
-            port.scalar_transport(qs, [0, 1, 1, 1], st["rho"], out["rho_begin"], out["mfx"], out["mfy"], out["mfz"],
-                                  case.dt, grid, top_open=case.bc[5] == 2)
+    def step():
+        impl.large_step(st, base, grid, case.dt, n, case.bc)
+
     return step, kind, cores, n
 
 
-def cpu_baseline(case, budget_s=12.0):
-    sc = sample_case(case)
+def cpu_baseline(cases, budget_s=12.0):
+    mid = sorted(cases, key=lambda c: c.cells)[len(cases) // 2]
+    sc = sample_case(mid)
     step, kind, cores, n = reference_step_runner(sc, os.cpu_count())
     step()  # warm-up
     t0 = time.perf_counter()
@@ -115,18 +136,18 @@ def cpu_baseline(case, budget_s=12.0):
             break
     el = time.perf_counter() - t0
     return {"value": sc.cells * steps / el, "unit": METRIC, "cores": cores, "kind": kind,
-            "sample": f"{steps} large steps of a {sc.nx}x{sc.ny}x{sc.nz} sub-domain of the workload "
-                      f"(N={n} acoustic substeps + WENO5 transport of 4 scalars), {el:.1f} s on {cores} host threads"}
+            "sample": f"{steps} large steps of a {sc.nx}x{sc.ny}x{sc.nz} grid (the workload's median run, "
+                      f"N={n} acoustic substeps, full step incl. slow Heun, transport, Kessler, EOS), "
+                      f"{el:.1f} s on {cores} host threads"}
 
 
 def run_reference_arm(args):
     rank, world, _ = dist_env()
-    from nimbus_b200.initial import benchmark_case
-
     if rank != 0:
         return 0
-    case = benchmark_case(args.workload)
-    sc = sample_case(case)
+    cases = workload_cases(args.workload, 0, args.members)
+    mid = sorted(cases, key=lambda c: c.cells)[len(cases) // 2]
+    sc = sample_case(mid)
     step, kind, cores, n = reference_step_runner(sc, os.cpu_count())
     for _ in range(args.warmup):
         step()
@@ -141,11 +162,12 @@ def run_reference_arm(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64 arithmetic, f32 storage",
-        "data": "synthetic (seeded WK82 supercell initial state)",
+        "data": "synthetic (seeded WK82 supercell initial states)",
         "config": {"workload": args.workload, "sample_grid": [sc.nx, sc.ny, sc.nz], "acoustic_substeps": n,
-                   "scalars": 4, "path": "acoustic loop + WENO5 transport (reference CPU solver)"},
+                   "scalars": 4, "path": "full large step assembled from the reference CPU solver's objects"},
         "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": kind,
-                         "sample": f"each step: one large step of a {sc.nx}x{sc.ny}x{sc.nz} sub-domain"},
+                         "sample": f"each step: one large step of a {sc.nx}x{sc.ny}x{sc.nz} grid (the workload's "
+                                   f"median run, capped at 96x96 columns)"},
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -200,9 +222,6 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-# ---------------------------------------------------------------------------
-# Our arm.
-# ---------------------------------------------------------------------------
 def load_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -218,14 +237,72 @@ def load_traffic():
     return {}
 
 
+# ---------------------------------------------------------------------------
+# Our arm.
+# ---------------------------------------------------------------------------
+def time_on_stream(torch, stream, fn, steps):
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(steps):
+        fn()
+    end.record(stream)
+    end.synchronize()
+    return start.elapsed_time(end)
+
+
+def error_study(ctx, seconds):
+    """FP32 form and reference-precision form on the device against the FP64
+    oracle, supercell_1km_64x64x40 (dt 6 s) for `seconds` of model time."""
+    import numpy as np
+
+    import oracle
+    from nimbus_b200 import cuda
+    from nimbus_b200.initial import benchmark_case, initial_state
+    from nimbus_b200.run import EngineRun, substeps_for
+
+    case = benchmark_case("supercell_1km_64x64x40")
+    st, base = initial_state(case)
+    n = substeps_for(case, st, base)
+    steps = int(round(seconds / case.dt))
+    o64 = oracle.Restatement("f64")
+    ref = {k: v.astype(np.float64) for k, v in st.items()}
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o64.large_step(ref, base, (case.dx, case.dy, case.dz), case.dt, n, case.bc)
+    oracle_s = time.perf_counter() - t0
+    theta0 = base["theta0"][None, None, :]
+    out = {"workload": "supercell_1km_64x64x40", "model_seconds": steps * case.dt, "steps": steps,
+           "acoustic_substeps": n, "oracle": "FP64 restatement (FP64 storage and arithmetic)",
+           "oracle_seconds": oracle_s, "metric": "relative L2 (max abs) per field; theta' = theta - theta0(z)"}
+    for name, prec in (("fp32", cuda.PRECISION_FP32), ("reference_precision", cuda.PRECISION_REFERENCE)):
+        run = EngineRun(ctx, prec)
+        mid = run.admit(case, st, base)
+        run.step(steps)
+        got = run.read(mid)
+        run.close()
+        fields = {}
+        for k in ("u", "v", "w", "theta", "qv", "p", "rho"):
+            a = got[k].astype(np.float64)
+            b = ref[k]
+            if k == "theta":
+                a, b = a - theta0, b - theta0
+            den = float(np.linalg.norm(b))
+            fields["theta'" if k == "theta" else k] = {
+                "rel_l2": float(np.linalg.norm(a - b) / den) if den > 0 else float(np.linalg.norm(a - b)),
+                "max_abs": float(np.abs(a - b).max())}
+        out[name] = fields
+    return out
+
+
 def run_ours(args):
     import numpy as np
     import torch
     import torch.distributed as dist
 
     from nimbus_b200 import cuda
-    from nimbus_b200.initial import benchmark_case
-    from nimbus_b200.run import HostStepper, ResidentRun
+    from nimbus_b200.initial import initial_state
+    from nimbus_b200.run import EngineRun, ResidentRun, substeps_for
 
     rank, world, local = dist_env()
     if world > 1:
@@ -233,135 +310,174 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     device = local if world > 1 else 0
     torch.cuda.set_device(device)
-    case = benchmark_case(args.workload)
-    case.member = rank  # each rank advances its own ensemble member
-    case.seed = case.seed + 1000 * rank
-    ctx = cuda.Context(device)
-    precision = cuda.PRECISION_FP32 if args.precision == "fp32" else cuda.PRECISION_REFERENCE
-    other = cuda.PRECISION_REFERENCE if precision == cuda.PRECISION_FP32 else cuda.PRECISION_FP32
-    form = {"auto": cuda.SUBSTEP_AUTO, "fused": cuda.SUBSTEP_FUSED, "split": cuda.SUBSTEP_SPLIT}[args.substep_form]
-    ctx.set_substep_form(form)
-    run = ResidentRun(ctx, case, device=f"cuda:{device}", precision=precision, autotune=form == cuda.SUBSTEP_AUTO)
-    stream = run.torch_stream
 
     def barrier():
         if world > 1:
             dist.barrier()
 
+    def max_over_ranks(x):
+        if world > 1:
+            t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{device}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+        return x
+
+    cases = workload_cases(args.workload, rank, args.members)
+    prepared = [initial_state(c) for c in cases]
+    subs = [substeps_for(c, *p) for c, p in zip(cases, prepared)]
+    cells = sum(c.cells for c in cases)
+    ctx = cuda.Context(device)
+    precision = cuda.PRECISION_FP32 if args.precision == "fp32" else cuda.PRECISION_REFERENCE
+    other = cuda.PRECISION_REFERENCE if precision == cuda.PRECISION_FP32 else cuda.PRECISION_FP32
+    stream = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{device}")
+
+    # ---- batched form: every run resident in one engine, CUDA graph ----
+    run = EngineRun(ctx, precision)
+    for c, (st, base), n in zip(cases, prepared, subs):
+        run.admit(c, st, base, n_substeps=n)
     for _ in range(max(args.warmup, 3)):
-        run.step()
-    stream.synchronize()
-    barrier()
-    torch.cuda.synchronize()
-    launches0 = ctx.kernel_launches
-    start = torch.cuda.Event(enable_timing=True)
-    end = torch.cuda.Event(enable_timing=True)
-    with ClockSampler(device) as clocks:
-        start.record(stream)
-        for _ in range(args.steps):
-            run.step()
-        end.record(stream)
-        end.synchronize()
+        run.step(1)
     ctx.synchronize()
     barrier()
     torch.cuda.synchronize()
+    launches0 = ctx.kernel_launches
+    with ClockSampler(device) as clocks:
+        ms = time_on_stream(torch, stream, lambda: run.step(1), args.steps)
+    run.engine.synchronize()
     launches = ctx.kernel_launches - launches0
-    ms = start.elapsed_time(end)
-    if world > 1:
-        t = torch.tensor([ms], device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    barrier()
+    ms = max_over_ranks(ms)
     clock = clocks.summary()
-    cells_total = case.cells * world
-    value = cells_total * args.steps / (ms / 1e3)
+    total_cells = cells * world
+    value = total_cells * args.steps / (ms / 1e3)
+    bytes_per_step = sum(c.cells * step_bytes(n) for c, n in zip(cases, subs))
 
-    # Per-kernel device time over an identical pass with event bracketing.
+    # ---- per-kernel device time (eager launches bracketed by events) ----
     ctx.set_kernel_timing(True)
     for _ in range(args.steps):
-        run.step()
+        run.step(1)
     timing = ctx.kernel_timing()
     ctx.set_kernel_timing(False)
-    n_sub = run.n_substeps
-    launches_sub, total_sub = timing["acoustic_substep"]
-    # One substep = the fused kernel, or the split form's two launches.
-    substep_ms = (total_sub + timing["acoustic_momentum"][1]) / max(launches_sub, 1)
-    achieved = SUBSTEP_BYTES_PER_CELL * case.cells / (substep_ms / 1e3) / 1e9
+    total_kernel_ms = sum(v[1] for v in timing.values())
+    shares = {k: round(v[1] / total_kernel_ms, 4) for k, v in timing.items()} if total_kernel_ms else {}
+    sub_ms = timing["acoustic_substep"][1] + timing["acoustic_momentum"][1]
+    sub_launches = timing["acoustic_substep"][0]
+    sub_bytes = sum(c.cells * n for c, n in zip(cases, subs)) * SUBSTEP_BYTES * args.steps
+    achieved = sub_bytes / (sub_ms / 1e3) / 1e9 if sub_ms else None
     peak, peak_kind = load_peaks()
-    traffic = load_traffic().get(args.workload, {}).get("acoustic_substep_bytes_per_substep")
-    total_ms = sum(v[1] for v in timing.values())
-    shares = {k: round(v[1] / total_ms, 4) for k, v in timing.items()} if total_ms else {}
+    traffic = load_traffic().get(args.workload, {})
+    step_gbs = bytes_per_step * args.steps / (ms / 1e3) / 1e9
 
-    # The other precision mode, same workload, device-timed (reported beside).
-    alt = ResidentRun(ctx, case, device=f"cuda:{device}", precision=other, autotune=form == cuda.SUBSTEP_AUTO)
-    for _ in range(3):
-        alt.step()
-    alt.torch_stream.synchronize()
-    a0 = torch.cuda.Event(enable_timing=True)
-    a1 = torch.cuda.Event(enable_timing=True)
-    a0.record(alt.torch_stream)
-    for _ in range(args.steps):
-        alt.step()
-    a1.record(alt.torch_stream)
-    a1.synchronize()
-    alt_ms = a0.elapsed_time(a1) / args.steps
-    del alt
+    # ---- the other precision, same runs ----
+    ctx.set_precision(other)
+    run.precision = other
+    for _ in range(2):
+        run.step(1)
+    alt_ms = time_on_stream(torch, stream, lambda: run.step(1), args.steps) / args.steps
+    run.precision = precision
     ctx.set_precision(precision)
 
-    # End-to-end through the reference-facing host API (pinned host arrays).
+    # ---- end to end through the host-buffer API ----
     e2e = None
     if args.e2e_steps > 0:
-        host = HostStepper(ctx, case, precision=precision)
-        host.step()
-        torch.cuda.synchronize()
+        host = {}
+        for mid, (c, _) in run.members.items():
+            host[mid] = {k: torch.from_numpy(v).pin_memory().numpy() for k, v in run.read(mid).items()}
+
+        def e2e_step():
+            for mid in run.members:
+                run.engine.write(mid, host[mid])
+            run.step(1)
+            for mid in run.members:
+                run.engine.read_into(mid, host[mid])
+
+        e2e_step()
         barrier()
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
-            host.step()
-        el = time.perf_counter() - t0
-        if world > 1:
-            t = torch.tensor([el], device=f"cuda:{device}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            el = float(t.item())
-        h2d, d2h = host.bytes_per_step()
-        e2e = {"value": cells_total * args.e2e_steps / el, "unit": METRIC, "h2d_bytes_per_step": h2d * world,
-               "d2h_bytes_per_step": d2h * world, "steps": args.e2e_steps,
-               "api": "nimbus_cuda_acoustic_batched + nimbus_cuda_scalar_transport, NIMBUS_MEMORY_HOST"}
+            e2e_step()
+        el = max_over_ranks(time.perf_counter() - t0)
+        io = cells * 4 * 9
+        e2e = {"value": total_cells * args.e2e_steps / el, "unit": METRIC, "h2d_bytes_per_step": io * world,
+               "d2h_bytes_per_step": io * world, "steps": args.e2e_steps,
+               "api": "nimbus_cuda_engine_write + nimbus_cuda_engine_step + nimbus_cuda_engine_read "
+                      "(pinned host arrays, nine prognostic fields each way per run per step)"}
+    run.close()
 
+    # ---- plain path: each run alone, one C-ABI call per operation ----
+    plain = None
+    if not args.no_plain:
+        ctx.set_substep_form(cuda.SUBSTEP_SPLIT)
+        runs = [ResidentRun(ctx, c, st, base, device=f"cuda:{device}", precision=precision, autotune=False)
+                for c, (st, base) in zip(cases, prepared)]
+
+        def plain_step():
+            for r in runs:
+                r.step()
+
+        plain_step()
+        ctx.synchronize()
+        p_ms = max_over_ranks(time_on_stream(torch, stream, plain_step, args.plain_steps))
+        plain = {"value": total_cells * args.plain_steps / (p_ms / 1e3), "ms_per_step": p_ms / args.plain_steps,
+                 "steps": args.plain_steps,
+                 "path": "each run alone through the per-operation entry points (slow_step, acoustic_boundaries, "
+                         "acoustic_batched, scalar_transport, kessler_step, eos_projection), host-enqueued launches"}
+        plain["batched_over_plain"] = value / plain["value"]
+        del runs
+        torch.cuda.empty_cache()
+        ctx.set_substep_form(cuda.SUBSTEP_AUTO)
+
+    serving = None
+    error = None
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        try:
-            cpu = cpu_baseline(case)
-        except Exception as exc:  # the baseline is reported, never required
-            cpu = {"value": None, "unit": METRIC, "cores": 0, "kind": "unavailable", "sample": str(exc)}
+    if rank == 0 and world == 1:
+        if not args.no_serving:
+            serving = serving_study(ctx, args, precision)
+        if not args.no_error:
+            error = error_study(ctx, args.error_seconds)
+        if not args.no_cpu_baseline:
+            try:
+                cpu = cpu_baseline(cases)
+            except Exception as exc:  # the baseline is reported, never required
+                cpu = {"value": None, "unit": METRIC, "cores": 0, "kind": "unavailable", "sample": str(exc)}
 
     if rank == 0:
+        nsub = sorted(set(subs))
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f32 (stencils), f64 (base state, EOS, mass-flux sums)" if precision == cuda.PRECISION_FP32
-            else "f64 arithmetic, f32 storage",
-            "data": "synthetic (seeded WK82 supercell: analytic sounding, cos^2 bubble, theta noise)",
-            "config": {"workload": args.workload, "grid": list(case.shape), "dx_m": case.dx, "dz_m": case.dz,
-                       "dt_s": case.dt, "acoustic_substeps": n_sub, "scalars": 4,
-                       "path": "acoustic loop (mass flux, fused substep, KW78 boundaries) + WENO5 transport",
-                       "precision": args.precision,
-                       "precision_modes": {
-                           args.precision: {"value": value, "ms_per_step": ms / args.steps},
-                           ("reference" if args.precision == "fp32" else "fp32"): {
-                               "value": cells_total * 1e3 / alt_ms if world == 1 else None, "ms_per_step": alt_ms}},
-                       "substep_form": {"chosen": args.substep_form if form != cuda.SUBSTEP_AUTO else
-                                        ("fused" if run.tuned and run.tuned[0] == 1 else "split"),
-                                        "autotune_ms_per_substep": run.tuned[1] if run.tuned else None},
-                       "parallelism": f"{world} independent member(s), one per GPU",
-                       "l2": "inputs larger than L2 (resident state ~%d MB per GPU)" % (case.cells * 4 * 17 // 2**20)},
-            "roofline": {"bound": "hbm",
-                         "kernel": "acoustic substep (%s form)" % (args.substep_form if form != cuda.SUBSTEP_AUTO else
-                                                                   ("fused" if run.tuned and run.tuned[0] == 1 else "split")),
-                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "peak_kind": peak_kind, "traffic": traffic,
-                         "algorithmic_bytes_per_cell": SUBSTEP_BYTES_PER_CELL,
-                         "substep_ms": substep_ms, "kernel_shares": shares},
+            "dtype": "f32 (stencils), f64 (base state, EOS, mass-flux sums, Kessler)"
+            if precision == cuda.PRECISION_FP32 else "f64 arithmetic, f32 storage",
+            "data": "synthetic (seeded WK82 supercells: analytic sounding, cos^2 bubble, theta noise)",
+            "config": {
+                "workload": args.workload, "runs_per_gpu": len(cases), "cells_per_gpu": cells,
+                "grids": "ragged: %d distinct shapes %s..%s" % (len({c.shape for c in cases}),
+                                                                min(c.shape for c in cases),
+                                                                max(c.shape for c in cases)),
+                "acoustic_substeps": nsub, "scalars": 4,
+                "path": "full large step: slow Heun, boundary refresh + KW78 seed, N split substeps "
+                        "(mass flux, continuity+EOS, momentum, boundaries), WENO5 transport, Kessler, EOS",
+                "form": "batched member engine, one launch per phase for all runs, CUDA graph replay",
+                "precision": args.precision,
+                "precision_modes": {
+                    args.precision: {"value": value, "ms_per_step": ms / args.steps},
+                    ("reference" if args.precision == "fp32" else "fp32"): {
+                        "value": total_cells * 1e3 / alt_ms if world == 1 else None, "ms_per_step": alt_ms}},
+                "plain": plain,
+                "serving": serving,
+                "error_vs_fp64": error,
+                "parallelism": f"{world} GPU(s), each with its own independent ensemble (no collective)",
+                "l2": "inputs larger than L2 (%.1f GB resident per GPU)" % (cells * 4 * 40 / 1e9),
+                "algorithmic_bytes_per_step": bytes_per_step,
+                "effective_step_bandwidth_gbs": step_gbs},
+            "roofline": {"bound": "hbm", "kernel": "acoustic substep (continuity+EOS and momentum kernels)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak if achieved else None, "peak_kind": peak_kind,
+                         "traffic": traffic.get("acoustic_substep_bytes_per_launch"),
+                         "algorithmic_bytes_per_cell_substep": SUBSTEP_BYTES,
+                         "launches": sub_launches, "substep_ms_total": sub_ms,
+                         "whole_step_frac": step_gbs / peak, "kernel_shares": shares},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches,
@@ -372,6 +488,27 @@ def run_ours(args):
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def serving_study(ctx, args, precision):
+    """Poisson stream (4 req/s) and a burst of the same requests: continuous
+    batching in the engine against running them one by one on the plain path."""
+    from nimbus_b200.ensemble import request_stream
+    from nimbus_b200.initial import initial_state
+    from nimbus_b200.serve import Server, serve_one_by_one, summarize
+
+    out = {}
+    for label, burst in (("poisson_4_per_s", False), ("burst", True)):
+        reqs = request_stream(args.serving_requests, rate_per_s=4.0, seed=7, burst=burst)
+        prepared = {r.rid: initial_state(r.case) for r in reqs}
+        server = Server(ctx, precision)
+        done, span = server.serve(reqs, prepared)
+        server.close()
+        plain, p_span = serve_one_by_one(ctx, reqs, precision, prepared)
+        out[label] = {"batched": summarize(done, span), "one_by_one_plain": summarize(plain, p_span)}
+    out["requests"] = ("%d runs, grids log-uniform 32x32x40..256x256x80, durations U(60,600) s at dt 3 s, "
+                       "seeded" % args.serving_requests)
+    return out
 
 
 def main():

@@ -262,6 +262,15 @@ class ReferenceHarness:
                                                  *[_fp(o) for o in out]))
         return out
 
+    def acoustic_boundaries(self, st, grid, bc, dt_small=0.0):
+        """apply_acoustic(dt_small) on u, v, w, rho, p in place."""
+        u, v, w, rho, p = (st[k] for k in ("u", "v", "w", "rho", "p"))
+        nx, ny, nz = u.shape
+        self._rc(self.lib.ref_acoustic_boundaries(_fp(u), _fp(v), _fp(w), _fp(rho), _fp(p), nx, ny, nz,
+                                                  ctypes.c_double(grid[0]), ctypes.c_double(grid[1]),
+                                                  ctypes.c_double(grid[2]), ctypes.c_double(dt_small),
+                                                  *[int(x) for x in bc]))
+
     def eos_projection(self, p, rho, theta, grid, qv=None, qc=None, qr=None):
         """apply_pressure_projection on p in place; False when refused."""
         nx, ny, nz = p.shape
@@ -271,6 +280,51 @@ class ReferenceHarness:
         if rc < 0:
             self._rc(rc)
         return rc == 0
+
+    def large_step(self, st, base, grid, dt, n_substeps, bc, coriolis_f=0.0):
+        """One large step of the hot path from the reference's own objects:
+        slow tendencies (k1, k2), boundary refresh, acoustic loop, transport,
+        Kessler tendencies and the EOS projection are the reference's calls;
+        the pointwise Heun combination and the microphysics commit between
+        them are written out here with the reference's rounding
+        (dynamics.cpp:1955-2408, microphysics_step.cpp:3026-3245)."""
+        f32, f64 = np.float32, np.float64
+
+        def apply(x, t):
+            t64 = np.where(np.isfinite(t), t, 0).astype(f64)
+            return (x.astype(f64) + t64 * dt).astype(f32)
+
+        keys = ("u", "v", "w", "p")
+        k1 = self.slow_tendencies(st, base, grid, coriolis_f)
+        star = dict(st)
+        for key, t in zip(keys, k1):
+            star[key] = apply(st[key], t)
+        k2 = self.slow_tendencies(star, base, grid, coriolis_f)
+        for key, a, b in zip(keys, k1, k2):
+            st[key][...] = apply(st[key], f32(0.5) * (b + a))
+        self.acoustic_boundaries(st, grid, bc, 0.0)
+        loop = self.acoustic_loop(st, base["rho0"], base["p0"], dt, n_substeps, grid, bc)
+        qs = [st["theta"], st["qv"], st["qc"], st["qr"]]
+        self.scalar_transport(qs, [0, 1, 1, 1], st["u"], st["v"], st["w"], st["rho"], loop["rho_begin"],
+                              loop["mfx"], loop["mfy"], loop["mfz"], dt, grid, top_open=bc[5] == 2)
+        nx, ny, nz = st["u"].shape
+        dth, dqv, dqc, dqr = self.kessler_tendencies(st, grid[2], dt, (1, nx - 1, 1, ny - 1, 0, nz))
+        sl = (slice(1, nx - 1), slice(1, ny - 1), slice(None))
+        with np.errstate(invalid="ignore", over="ignore"):
+            for key, d in (("qv", dqv), ("qc", dqc), ("qr", dqr)):
+                q = st[key][sl]
+                raw = (q.astype(f64) + np.where(np.isfinite(d[sl]), d[sl], 0).astype(f64) * dt).astype(f32)
+                st[key][sl] = np.where(np.isfinite(raw), np.clip(raw, f32(0), f32(0.05)), f32(0))
+            told = st["theta"][sl].astype(f64)
+            total = np.where(np.isfinite(dth[sl]), dth[sl], 0).astype(f64) * dt
+            total = np.where(np.isfinite(total), total, 0.0)
+            tn = told + np.clip(total, -50.0, 50.0)
+            tn = np.where(np.isfinite(tn), tn, np.where(np.isfinite(told), told, 300.0))
+            stored = tn.astype(f32)
+            st["theta"][sl] = np.where(np.isfinite(stored), np.clip(stored, f32(200), f32(700)), f32(300))
+        if not self.eos_projection(st["p"], st["rho"], st["theta"], grid, st["qv"], st["qc"], st["qr"]):
+            raise FloatingPointError("EOS pressure projection rejected an invalid physical state")
+        return loop
 
     def slow_tendencies(self, st, base, grid, coriolis_f=0.0, moist=True):
         u, v, w, rho, p, th = (st[k] for k in ("u", "v", "w", "rho", "p", "theta"))

@@ -21,6 +21,8 @@
 //                           on a stationary flat level with moisture and Kessler loading
 //   ref_kessler_tendencies  KesslerScheme::compute_tendencies
 //                           (src/microphysics/schemes/kessler/kessler.cpp:103-520)
+//   ref_acoustic_boundaries CartesianCGridBCScheme::apply_acoustic
+//                           (boundary_conditions_cartesian_cgrid.cpp:141-236)
 //   ref_eos_projection      tmv::dynamics_eos::apply_pressure_projection
 //                           (src/core/orchestration/dynamics/eos_apply.cpp:50-200)
 //   ref_scalar_transport    advect_scalars_conservative_3d_cartesian
@@ -187,6 +189,38 @@ int ref_acoustic_fused(float* u, float* v, float* w, float* rho, float* p, const
         d.drho_scratch = drho_scratch;
         if (!backend->dynamics_kernels()->dispatch_acoustic_substep_fused_cartesian_cgrid(d))
             return fail("reference CPU backend refused the fused acoustic dispatch");
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        return fail(e.what());
+    }
+}
+
+// The boundary closure alone: CartesianCGridBCScheme::apply_acoustic(dt_small)
+// on u, v, w, rho, p in place (dt_small == 0 refreshes the ghosts, the call
+// seed_acoustic_radiation's caller makes before seeding).
+int ref_acoustic_boundaries(float* u, float* v, float* w, float* rho, float* p, int nx, int ny, int nz, double dx,
+                            double dy, double dz, double dt_small, int bc_west, int bc_east, int bc_south,
+                            int bc_north, int bc_bottom, int bc_top)
+{
+    try
+    {
+        Level L(nx, ny, nz, dx, dy, dz, 1.0);
+        L.set_bcs(bc_west, bc_east, bc_south, bc_north, bc_bottom, bc_top);
+        auto& f = L.storage.fields;
+        to_field(f.u, u, nx, ny, nz);
+        to_field(f.v, v, nx, ny, nz);
+        to_field(f.w, w, nx, ny, nz);
+        to_field(f.rho, rho, nx, ny, nz);
+        to_field(f.p, p, nx, ny, nz);
+        auto bc = tmv::create_cartesian_cgrid_bc_scheme(L.view);
+        bc->apply_acoustic(dt_small);
+        from_field(u, f.u);
+        from_field(v, f.v);
+        from_field(w, f.w);
+        from_field(rho, f.rho);
+        from_field(p, f.p);
         return 0;
     }
     catch (const std::exception& e)

@@ -306,3 +306,42 @@ def test_live_reference_pin_eos(o32, field, cell, value, dry_refused, moist_refu
         rb = o32.eos_projection(b, st["rho"], st["theta"], *q)
         assert ra == rb
         np.testing.assert_array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+@pytest.mark.reference
+@pytest.mark.skipif(not oracle.reference_available(), reason="reference harness not built here")
+@pytest.mark.parametrize("bc_name", list(BC_SETS))
+def test_live_reference_pin_boundary_refresh(o32, bc_name):
+    """apply_acoustic(0): the ghost refresh before the KW78 seed."""
+    ref = oracle.ReferenceHarness()
+    case = Case(13, 11, 8, 1000.0, 1000.0, 500.0, 6.0, seed=4)
+    st, _ = perturbed_state(case, seed=21)
+    close_walls(st, BC_SETS[bc_name])
+    a = {k: st[k].copy() for k in ("u", "v", "w", "rho", "p")}
+    b = {k: st[k].copy() for k in ("u", "v", "w", "rho", "p")}
+    ref.acoustic_boundaries(a, (1000.0, 1000.0, 500.0), BC_SETS[bc_name], 0.0)
+    o32.acoustic_boundaries(b, (1000.0, 1000.0, 500.0), BC_SETS[bc_name], 0.0)
+    for k in a:
+        np.testing.assert_array_equal(a[k].view(np.uint32), b[k].view(np.uint32), err_msg=k)
+    assert any(not np.array_equal(a[k], st[k]) for k in a)  # the refresh did something
+
+
+@pytest.mark.reference
+@pytest.mark.skipif(not oracle.reference_available(), reason="reference harness not built here")
+@pytest.mark.parametrize("bc_name", list(BC_SETS))
+def test_live_reference_pin_large_step(o32, bc_name):
+    """The oracle's whole large step against the same step assembled from the
+    reference's own objects, two steps, every prognostic field bit for bit."""
+    from nimbus_b200.initial import cloudy_state
+    ref = oracle.ReferenceHarness()
+    case = Case(17, 15, 13, 800.0, 700.0, 400.0, 4.0, seed=8)
+    st, base = cloudy_state(case, seed=8)
+    close_walls(st, BC_SETS[bc_name])
+    a = {k: v.copy() for k, v in st.items()}
+    b = {k: v.copy() for k, v in st.items()}
+    grid = (800.0, 700.0, 400.0)
+    for _ in range(2):
+        ref.large_step(a, base, grid, 4.0, 5, BC_SETS[bc_name], coriolis_f=1e-4)
+        o32.large_step(b, base, grid, 4.0, 5, BC_SETS[bc_name], coriolis_f=1e-4)
+    for k in ("u", "v", "w", "rho", "p", "theta", "qv", "qc", "qr"):
+        np.testing.assert_array_equal(a[k].view(np.uint32), b[k].view(np.uint32), err_msg=k)
