@@ -16,11 +16,12 @@
 //   RefPolicy   FP64 interior arithmetic in the reference's operation order
 //               (acoustic_cgrid_fast.cpp:47-215), EOS via pow(): bit-identical
 //               to the CPU solver when compiled with --fmad=false.
-//   Fp32Policy  FP32 stencil arithmetic; the base state enters in FP64 (the
+//   Fp32Policy  FP32 arithmetic throughout; the base state enters in FP64 (the
 //               hydrostatic difference p0[k+1]-p0[k] as an FP32 hi+lo pair, so
 //               the w equation's cancellation stays exact to ~1e-7); the EOS is
-//               exp(gamma*log(x)) in FP64 and the retained mass-flux sums stay
-//               FP64 adds rounded once per substep.
+//               the compensated binomial form of substep_pressure (within
+//               about half an FP32 ulp of FP64), and the retained mass-flux
+//               sums and the density update are single-rounding FMAs.
 #pragma once
 
 #include "stencil_common.cuh"
@@ -41,7 +42,29 @@ struct FusedParams
     int chunk;               // i-planes per CTA
     unsigned nz_magic;       // fast t / nz (see fused_nz_magic)
     int vec4;                // 1: 16-byte copies (nz % 4 == 0 and 16-byte aligned bases)
+    // FP32 form: the scalars above rounded once, and the binomial-series
+    // coefficients binom(gamma, n), n = 1..6, of the EOS (substep_pressure).
+    float inv_dx_f, inv_dy_f, inv_dz_f, dt_f, weight_f, frame_u_f, frame_v_f;
+    float eos_c[6];
 };
+
+// Derives the FP32 copies of a filled parameter block.
+__host__ __device__ inline void finish_fp32(FusedParams& P)
+{
+    P.inv_dx_f = (float)P.inv_dx;
+    P.inv_dy_f = (float)P.inv_dy;
+    P.inv_dz_f = (float)P.inv_dz;
+    P.dt_f = (float)P.dt_small;
+    P.weight_f = (float)P.weight;
+    P.frame_u_f = (float)P.frame_u;
+    P.frame_v_f = (float)P.frame_v;
+    double c = 1.0;
+    for (int n = 1; n <= 6; ++n)
+    {
+        c *= (P.gamma - (n - 1)) / n;
+        P.eos_c[n - 1] = (float)c;
+    }
+}
 
 struct RefPolicy
 {
@@ -86,6 +109,119 @@ __device__ __forceinline__ void fused_accumulate(float* slot, double weight, dou
     else flags |= kStatusNonfiniteMassFlux;
 }
 
+// Per-level base data, from the FP64 pressure profile: the hydrostatic
+// difference p0[k+1] - p0[k] as an FP32 hi+lo pair (the w equation of the
+// FP32 form), and for the FP32 EOS p0 and b = (R_d / p00) / x0 as hi+lo pairs,
+// where x0 = (p0 / p00)^(1/gamma) is the EOS argument at the base pressure.
+static __global__ void level_base_kernel(const double* __restrict__ p0, int nz, double gamma,
+                                         float2* __restrict__ dp0, float4* __restrict__ eos0)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nz) return;
+    const double dp = (k + 1 < nz) ? p0[k + 1] - p0[k] : 0.0;
+    const float hi = (float)dp;
+    dp0[k] = make_float2(hi, (float)(dp - (double)hi));
+    const double x0 = pow(p0[k] / kP00, 1.0 / gamma);
+    const double b = (kRd / kP00) / x0;
+    const float ph = (float)p0[k], bh = (float)b;
+    eos0[k] = make_float4(ph, (float)(p0[k] - (double)ph), bh, (float)(b - (double)bh));
+}
+
+// The retained mass-flux increment of the FP32 form: one FMA, the weighted
+// flux added to the stored sum and rounded once to the FP32 slot -- the same
+// single rounding as the reference's FP64 add stored to FP32
+// (advection_cartesian.cpp:768-775), without leaving FP32.  With store the
+// slot starts from zero (first substep of a large step).
+__device__ __forceinline__ void retain_flux_f32(float* slot, float weight, float flux, unsigned& flags, bool store)
+{
+    const float st = __fmaf_rn(weight, flux, store ? 0.0f : *slot);
+    if (isfinite(st)) *slot = st;
+    else
+    {
+        if (store) *slot = 0.0f;
+        flags |= kStatusNonfiniteMassFlux;
+    }
+}
+
+// rho forward Euler + fallback + clamp (acoustic_cgrid_fast.cpp:120-135).
+// Reference policy: FP64 add rounded once; FP32 policy: one FMA.
+template <class Policy>
+__device__ __forceinline__ float substep_density(const FusedParams& P, float rho_c, float drho_stored,
+                                                 const double* __restrict__ rho0, int k)
+{
+    if constexpr (Policy::exact_pow)
+    {
+        double rho_new = (double)rho_c + (double)drho_stored * P.dt_small;
+        if (!isfinite(rho_new) || rho_new <= 0.0)
+        {
+            const double b = rho0[k];
+            rho_new = (0.1 < b) ? b : 0.1;
+        }
+        return clamp_value((float)rho_new, 1.0f, P.rho_min, P.rho_max);
+    }
+    else
+    {
+        float rn = __fmaf_rn(drho_stored, P.dt_f, rho_c);
+        if (!isfinite(rn) || rn <= 0.0f)
+        {
+            const double b = rho0[k];
+            rn = (float)((0.1 < b) ? b : 0.1);
+        }
+        return clamp_value(rn, 1.0f, P.rho_min, P.rho_max);
+    }
+}
+
+// EOS pressure p = p00 (rho R_d theta / p00)^gamma + fallback + clamp
+// (acoustic_cgrid_fast.cpp:136-157).  Reference policy: pow in FP64.  FP32
+// policy: p = p0 (1 + d)^gamma with 1 + d = rho theta b, the product formed
+// exactly as an FP32 hi+lo pair so d keeps full precision, and (1 + d)^gamma - 1
+// summed by its binomial series to the sixth power (|d| <= 1/16: the
+// truncation is below 2e-11 relative); the result is within about half an
+// FP32 ulp of the FP64 value.  Larger |d| take the FP64 route.
+template <class Policy>
+__device__ __forceinline__ float substep_pressure(const FusedParams& P, const float4* __restrict__ eos0, int k,
+                                                  float rho_stored, float th)
+{
+    if constexpr (Policy::exact_pow)
+    {
+        double p_new = (double)P.p_ref_fallback;
+        const double thv = (double)th;
+        if (thv > 0.0)
+        {
+            const double x = (double)rho_stored * kRd * thv / kP00;
+            p_new = kP00 * pow(x, P.gamma);
+        }
+        if (!isfinite(p_new) || p_new <= 0.0) p_new = (double)P.p_ref_fallback;
+        return clamp_value((float)p_new, 101325.0f, P.p_min, P.p_max);
+    }
+    else
+    {
+        float p = P.p_ref_fallback;
+        if (th > 0.0f)
+        {
+            const float4 e = eos0[k];
+            const float rt = rho_stored * th;
+            const float rt_lo = __fmaf_rn(rho_stored, th, -rt);
+            const float r = rt * e.z;
+            const float r_lo = __fmaf_rn(rt, e.z, -r) + __fmaf_rn(rt, e.w, rt_lo * e.z);
+            const float dl = (r - 1.0f) + r_lo;
+            if (fabsf(dl) <= 0.0625f)
+            {
+                float sum = P.eos_c[5];
+                for (int n = 4; n >= 0; --n) sum = __fmaf_rn(sum, dl, P.eos_c[n]);
+                p = e.x + __fmaf_rn(e.x, sum * dl, e.y);
+            }
+            else
+            {
+                double pd = kP00 * exp(P.gamma * log((double)rho_stored * kRd * (double)th / kP00));
+                if (!isfinite(pd) || pd <= 0.0) pd = (double)P.p_ref_fallback;
+                p = (float)pd;
+            }
+        }
+        return clamp_value(p, 101325.0f, P.p_min, P.p_max);
+    }
+}
+
 template <int TJ>
 struct FusedSmem
 {
@@ -109,7 +245,8 @@ template <int TJ, int BLOCK, class Policy>
 static __global__ void __launch_bounds__(BLOCK, 3) acoustic_substep_fused_kernel(
     FusedParams P, const float* __restrict__ rho_in, const float* __restrict__ u_in, const float* __restrict__ v_in,
     const float* __restrict__ w_in, const float* __restrict__ theta, const double* __restrict__ rho0,
-    const double* __restrict__ p0, const float2* __restrict__ dp0_split, float* __restrict__ drho_out,
+    const double* __restrict__ p0, const float2* __restrict__ dp0_split, const float4* __restrict__ eos0,
+    float* __restrict__ drho_out,
     float* __restrict__ rho_out, float* __restrict__ p_out, float* __restrict__ u_out, float* __restrict__ v_out,
     float* __restrict__ w_out, float* __restrict__ mfx, float* __restrict__ mfy, float* __restrict__ mfz,
     unsigned* __restrict__ status)
@@ -225,23 +362,9 @@ static __global__ void __launch_bounds__(BLOCK, 3) acoustic_substep_fused_kernel
             }
             const float drho_stored = (float)finite_or_zero(drho);
             if (drho_out != nullptr && r < tj) drho_out[(size_t)i * sx + (size_t)j * nz + k] = drho_stored;
-            double rho_new = (double)rho_c + (double)drho_stored * P.dt_small;
-            if (!isfinite(rho_new) || rho_new <= 0.0)
-            {
-                const double b = rho0[k];
-                rho_new = (0.1 < b) ? b : 0.1;
-            }
-            const float rho_stored = clamp_value((float)rho_new, 1.0f, P.rho_min, P.rho_max);
+            const float rho_stored = substep_density<Policy>(P, rho_c, drho_stored, rho0, k);
             rn[t] = rho_stored;
-            double p_new = (double)P.p_ref_fallback;
-            const double thv = (double)th[t];
-            if (thv > 0.0)
-            {
-                const double x = (double)rho_stored * kRd * thv / kP00;
-                p_new = Policy::exact_pow ? kP00 * pow(x, P.gamma) : kP00 * exp(P.gamma * log(x));
-            }
-            if (!isfinite(p_new) || p_new <= 0.0) p_new = (double)P.p_ref_fallback;
-            pn[t] = clamp_value((float)p_new, 101325.0f, P.p_min, P.p_max);
+            pn[t] = substep_pressure<Policy>(P, eos0, k, rho_stored, th[t]);
         }
     };
 
@@ -300,11 +423,11 @@ static __global__ void __launch_bounds__(BLOCK, 3) acoustic_substep_fused_kernel
                     else
                     {
                         if (i < d.nx - 1)
-                            fused_accumulate(mfx + g, P.weight, (double)(0.5f * (rho_c + rp[cr]) * (uc[t] - (float)P.frame_u)), flags);
+                            retain_flux_f32(mfx + g, P.weight_f, 0.5f * (rho_c + rp[cr]) * (uc[t] - P.frame_u_f), flags, false);
                         if (j < d.ny - 1)
-                            fused_accumulate(mfy + g, P.weight, (double)(0.5f * (rho_c + rc_[cr + nz]) * (vc[cr] - (float)P.frame_v)), flags);
+                            retain_flux_f32(mfy + g, P.weight_f, 0.5f * (rho_c + rc_[cr + nz]) * (vc[cr] - P.frame_v_f), flags, false);
                         const float zf = (k == nz - 1) ? (P.top_open ? rho_c * wc[t] : 0.0f) : 0.5f * (rho_c + rc_[cr + 1]) * wc[t];
-                        fused_accumulate(mfz + g, P.weight, (double)zf, flags);
+                        retain_flux_f32(mfz + g, P.weight_f, zf, flags, false);
                     }
                 }
                 rho_out[g] = rn[t];
@@ -356,9 +479,9 @@ static __global__ void __launch_bounds__(BLOCK, 3) acoustic_substep_fused_kernel
                         const float sxr = (isfinite(rho_x) && rho_x > 1.0e-6f) ? rho_x : 1.0f;
                         const float syr = (isfinite(rho_y) && rho_y > 1.0e-6f) ? rho_y : 1.0f;
                         const float szr = (isfinite(rho_z) && rho_z > 1.0e-6f) ? rho_z : 1.0f;
-                        const float a = __fdividef(-(pnx[t] - pc) * (float)P.inv_dx, sxr);
-                        const float b = __fdividef(-(pn[t + nz] - pc) * (float)P.inv_dy, syr);
-                        const float c = __fdividef(-dpz * (float)P.inv_dz, szr);
+                        const float a = __fdividef(-(pnx[t] - pc) * P.inv_dx_f, sxr);
+                        const float b = __fdividef(-(pn[t + nz] - pc) * P.inv_dy_f, syr);
+                        const float c = __fdividef(-dpz * P.inv_dz_f, szr);
                         du = isfinite(a) ? a : 0.0f;
                         dv = isfinite(b) ? b : 0.0f;
                         dw = isfinite(c) ? c : 0.0f;
@@ -373,7 +496,7 @@ static __global__ void __launch_bounds__(BLOCK, 3) acoustic_substep_fused_kernel
                 }
                 else
                 {
-                    const float dt = (float)P.dt_small;
+                    const float dt = P.dt_f;
                     u_out[g] = clamp_value(__fmaf_rn(du, dt, uc[t]), 0.0f, -P.wind_h, P.wind_h);
                     v_out[g] = clamp_value(__fmaf_rn(dv, dt, vc[t + nz]), 0.0f, -P.wind_h, P.wind_h);
                     w_out[g] = clamp_value(__fmaf_rn(dw, dt, wc[t]), 0.0f, -P.wind_v, P.wind_v);

@@ -45,7 +45,8 @@ template <class Policy>
 __device__ __forceinline__ void continuity_eos_cell(const FusedParams& P, const float* __restrict__ rho,
                                                     const float* __restrict__ u, const float* __restrict__ v,
                                                     const float* __restrict__ w, const float* __restrict__ theta,
-                                                    const double* __restrict__ rho0, float* __restrict__ rho_out,
+                                                    const double* __restrict__ rho0,
+                                                    const float4* __restrict__ eos0, float* __restrict__ rho_out,
                                                     float* __restrict__ p_out, float* __restrict__ drho_out,
                                                     float* __restrict__ mfx, float* __restrict__ mfy,
                                                     float* __restrict__ mfz, int c, unsigned& flags, bool store_flux,
@@ -72,13 +73,17 @@ __device__ __forceinline__ void continuity_eos_cell(const FusedParams& P, const 
             }
             else
             {
-                if (i < d.nx - 1) retain_flux(mfx + c, P.weight, (double)(0.5f * (rho_c + rho[c + sx]) * (u[c] - (float)P.frame_u)), flags, store_flux);
-                if (j < d.ny - 1) retain_flux(mfy + c, P.weight, (double)(0.5f * (rho_c + rho[c + sy]) * (v[c] - (float)P.frame_v)), flags, store_flux);
+                if (i < d.nx - 1)
+                    retain_flux_f32(mfx + c, P.weight_f, 0.5f * (rho_c + rho[c + sx]) * (u[c] - P.frame_u_f), flags,
+                                    store_flux);
+                if (j < d.ny - 1)
+                    retain_flux_f32(mfy + c, P.weight_f, 0.5f * (rho_c + rho[c + sy]) * (v[c] - P.frame_v_f), flags,
+                                    store_flux);
                 const float zf = (k == d.nz - 1) ? (P.top_open ? rho_c * w[c] : 0.0f) : 0.5f * (rho_c + rho[c + 1]) * w[c];
-                retain_flux(mfz + c, P.weight, (double)zf, flags, store_flux);
+                retain_flux_f32(mfz + c, P.weight_f, zf, flags, store_flux);
             }
         }
-        double drho = 0.0;
+        real drho = (real)0;
         if (i >= 1 && i < d.nx - 1 && j >= 1 && j < d.ny - 1)
         {
             const real rc = (real)rho_c;
@@ -89,28 +94,19 @@ __device__ __forceinline__ void continuity_eos_cell(const FusedParams& P, const 
             const real fy_neg = half * ((real)rho[c - sy] + rc) * (real)v[c - sy];
             const real fz_pos = (k + 1 < d.nz) ? half * (rc + (real)rho[c + 1]) * (real)w[c] : rc * (real)w[c];
             const real fz_neg = (k > 0) ? half * ((real)rho[c - 1] + rc) * (real)w[c - 1] : (real)0;
-            drho = (double)(-((fx_pos - fx_neg) * (real)P.inv_dx + (fy_pos - fy_neg) * (real)P.inv_dy +
-                              (fz_pos - fz_neg) * (real)P.inv_dz));
+            if constexpr (sizeof(real) == 8)
+                drho = -((fx_pos - fx_neg) * P.inv_dx + (fy_pos - fy_neg) * P.inv_dy + (fz_pos - fz_neg) * P.inv_dz);
+            else
+                drho = -((fx_pos - fx_neg) * P.inv_dx_f + (fy_pos - fy_neg) * P.inv_dy_f +
+                         (fz_pos - fz_neg) * P.inv_dz_f);
         }
-        const float drho_stored = (float)finite_or_zero(drho);
+        float drho_stored;
+        if constexpr (sizeof(real) == 8) drho_stored = (float)finite_or_zero(drho);
+        else drho_stored = isfinite(drho) ? drho : 0.0f;
         if (drho_out != nullptr) drho_out[c] = drho_stored;
-        double rho_new = (double)rho_c + (double)drho_stored * P.dt_small;
-        if (!isfinite(rho_new) || rho_new <= 0.0)
-        {
-            const double b = rho0[k];
-            rho_new = (0.1 < b) ? b : 0.1;
-        }
-        const float rho_stored = clamp_value((float)rho_new, 1.0f, P.rho_min, P.rho_max);
+        const float rho_stored = substep_density<Policy>(P, rho_c, drho_stored, rho0, k);
         rho_out[c] = rho_stored;
-        double p_new = (double)P.p_ref_fallback;
-        const double th = (double)theta[c];
-        if (th > 0.0)
-        {
-            const double x = (double)rho_stored * kRd * th / kP00;
-            p_new = Policy::exact_pow ? kP00 * pow(x, P.gamma) : kP00 * exp(P.gamma * log(x));
-        }
-        if (!isfinite(p_new) || p_new <= 0.0) p_new = (double)P.p_ref_fallback;
-        p_out[c] = clamp_value((float)p_new, 101325.0f, P.p_min, P.p_max);
+        p_out[c] = substep_pressure<Policy>(P, eos0, k, rho_stored, theta[c]);
     }
 }
 
@@ -118,14 +114,15 @@ template <class Policy>
 static __global__ void __launch_bounds__(256) split_continuity_eos_kernel(
     FusedParams P, const float* __restrict__ rho, const float* __restrict__ u, const float* __restrict__ v,
     const float* __restrict__ w, const float* __restrict__ theta, const double* __restrict__ rho0,
-    float* __restrict__ rho_out, float* __restrict__ p_out, float* __restrict__ drho_out, float* __restrict__ mfx,
-    float* __restrict__ mfy, float* __restrict__ mfz, unsigned* __restrict__ status)
+    const float4* __restrict__ eos0, float* __restrict__ rho_out, float* __restrict__ p_out,
+    float* __restrict__ drho_out, float* __restrict__ mfx, float* __restrict__ mfy, float* __restrict__ mfz,
+    unsigned* __restrict__ status)
 {
     const int n = P.d.cells();
     unsigned flags = 0;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
-        continuity_eos_cell<Policy>(P, rho, u, v, w, theta, rho0, rho_out, p_out, drho_out, mfx, mfy, mfz, c, flags,
-                                    false, nullptr);
+        continuity_eos_cell<Policy>(P, rho, u, v, w, theta, rho0, eos0, rho_out, p_out, drho_out, mfx, mfy, mfz, c,
+                                    flags, false, nullptr);
     if (flags) atomicOr(status, flags);
 }
 
@@ -170,9 +167,9 @@ __device__ __forceinline__ void momentum_cell(const FusedParams& P, const float*
                 const float sxr = (isfinite(rho_x) && rho_x > 1.0e-6f) ? rho_x : 1.0f;
                 const float syr = (isfinite(rho_y) && rho_y > 1.0e-6f) ? rho_y : 1.0f;
                 const float szr = (isfinite(rho_z) && rho_z > 1.0e-6f) ? rho_z : 1.0f;
-                const float a = __fdividef(-(p[c + sx] - pc) * (float)P.inv_dx, sxr);
-                const float b = __fdividef(-(p[c + sy] - pc) * (float)P.inv_dy, syr);
-                const float cz = __fdividef(-dpz * (float)P.inv_dz, szr);
+                const float a = __fdividef(-(p[c + sx] - pc) * P.inv_dx_f, sxr);
+                const float b = __fdividef(-(p[c + sy] - pc) * P.inv_dy_f, syr);
+                const float cz = __fdividef(-dpz * P.inv_dz_f, szr);
                 du = isfinite(a) ? a : 0.0f;
                 dv = isfinite(b) ? b : 0.0f;
                 dw = isfinite(cz) ? cz : 0.0f;
@@ -186,7 +183,7 @@ __device__ __forceinline__ void momentum_cell(const FusedParams& P, const float*
         }
         else
         {
-            const float dt = (float)P.dt_small;
+            const float dt = P.dt_f;
             u_out[c] = clamp_value(__fmaf_rn(du, dt, u[c]), 0.0f, -P.wind_h, P.wind_h);
             v_out[c] = clamp_value(__fmaf_rn(dv, dt, v[c]), 0.0f, -P.wind_h, P.wind_h);
             w_out[c] = clamp_value(__fmaf_rn(dw, dt, w[c]), 0.0f, -P.wind_v, P.wind_v);

@@ -42,7 +42,7 @@ struct ArenaLayout
 {
     size_t cells, history;
     size_t off_state, off_ctxt, off_wave, off_sf, off_rl, off_k1, off_xs, off_eos, off_status, off_prof, off_dp0,
-        total;
+        off_eos0, total;
 };
 
 ArenaLayout arena_layout(const nimbus_member_desc* d)
@@ -63,6 +63,7 @@ ArenaLayout arena_layout(const nimbus_member_desc* d)
     L.off_status = off; off += kAlign;
     L.off_prof = off;   off += align_up(5 * static_cast<size_t>(d->nz) * sizeof(double));
     L.off_dp0 = off;    off += align_up(static_cast<size_t>(d->nz) * sizeof(float2));
+    L.off_eos0 = off;   off += align_up(static_cast<size_t>(d->nz) * sizeof(float4));
     L.total = off;
     return L;
 }
@@ -112,6 +113,7 @@ void fill_params(EngineMember& M, const nimbus_member_desc* a)
     F.frame_v = a->frame_velocity_v_ms;
     F.top_open = a->bc[5] == kTopOpen;
     F.chunk = 1;
+    finish_fp32(F);
 
     BoundaryParams& B = M.B;
     B = BoundaryParams{};
@@ -137,6 +139,7 @@ void fill_params(EngineMember& M, const nimbus_member_desc* a)
     T.n_scalars = kEngineScalars;
     T.positive_definite[0] = 0;  // theta (advection_batch.cpp:742-745)
     for (int s = 1; s < kEngineScalars; ++s) T.positive_definite[s] = 1;
+    finish_fp32(T);
 
     SlowParams& S = M.S;
     S = SlowParams{};
@@ -151,6 +154,7 @@ void fill_params(EngineMember& M, const nimbus_member_desc* a)
     S.gravity = 9.81;
     S.moist = 1;
     S.loading = 1;
+    finish_fp32(S);
 
     KesslerParams& K = M.K;
     K = KesslerParams{};
@@ -371,18 +375,17 @@ int enqueue_step(nimbus_engine* e, cudaStream_t st)
     engine_swap_kernel<<<(n + 127) / 128, 128, 0, st>>>(T, n, 0);
     ++count;
     // Conservative transport of theta, qv, qc, qr against the retained fluxes.
-    ENGINE_LAUNCH(NIMBUS_KERNEL_TRANSPORT_FACES, engine_transport_faces_kernel<kFp32>, cells, kEngineScalars, T, pc,
+    ENGINE_LAUNCH(NIMBUS_KERNEL_TRANSPORT_FACES, engine_transport_faces_kernel<kFp32>, cells, 1, T, pc,
                   cells);
-    ENGINE_LAUNCH(NIMBUS_KERNEL_TRANSPORT_LIMITER, engine_transport_limiter_kernel, cells, kEngineScalars, T, pc,
+    ENGINE_LAUNCH(NIMBUS_KERNEL_TRANSPORT_LIMITER, engine_transport_limiter_kernel<kFp32>, cells, 1, T, pc,
                   cells);
-    ENGINE_LAUNCH(NIMBUS_KERNEL_TRANSPORT_UPDATE, engine_transport_update_kernel, cells, kEngineScalars, T, pc,
+    ENGINE_LAUNCH(NIMBUS_KERNEL_TRANSPORT_UPDATE, engine_transport_update_kernel<kFp32>, cells, 1, T, pc,
                   cells);
-    // Kessler step, then the EOS pressure re-projection.
-    ENGINE_LAUNCH(NIMBUS_KERNEL_MICROPHYSICS, engine_kessler_kernel, cells, 1, T, pc, cells);
+    // Kessler step and the EOS pressure re-projection (one pass), then the
+    // pointer rotation that publishes the new qr and pressure.
+    ENGINE_LAUNCH(NIMBUS_KERNEL_MICROPHYSICS, engine_microphysics_eos_kernel, cells, 1, T, pc, cells);
     engine_swap_kernel<<<(n + 127) / 128, 128, 0, st>>>(T, n, 1);
     ++count;
-    ENGINE_LAUNCH(NIMBUS_KERNEL_MICROPHYSICS, engine_eos_kernel, cells, 1, T, pc, cells);
-    ENGINE_LAUNCH(NIMBUS_KERNEL_MICROPHYSICS, engine_eos_publish_kernel, cells, 1, T, pc, cells);
     return count;
 }
 
@@ -413,16 +416,6 @@ nimbus_status build_graph(nimbus_engine* e)
     e->launches_per_step = launches;
     e->built_precision = ctx->precision;
     return NIMBUS_OK;
-}
-
-void split_dp0(const double* p0, int nz, float2* out)
-{
-    for (int k = 0; k < nz; ++k)
-    {
-        const double dp = (k + 1 < nz) ? p0[k + 1] - p0[k] : 0.0;
-        const float hi = static_cast<float>(dp);
-        out[k] = make_float2(hi, static_cast<float>(dp - static_cast<double>(hi)));
-    }
 }
 
 MemberSlot* find_slot(nimbus_engine* e, int id, size_t* index = nullptr)
@@ -537,7 +530,9 @@ nimbus_status nimbus_cuda_engine_admit(nimbus_engine* e, const nimbus_member_des
     M.u0 = prof + 3 * nz;
     M.v0 = prof + 4 * nz;
     float2* dp0 = reinterpret_cast<float2*>(base + L.off_dp0);
+    float4* eos0 = reinterpret_cast<float4*>(base + L.off_eos0);
     M.dp0 = dp0;
+    M.eos0 = eos0;
     fill_params(M, desc);
 
     // Profiles, the split hydrostatic difference and the initial state.
@@ -547,8 +542,6 @@ nimbus_status nimbus_cuda_engine_admit(nimbus_engine* e, const nimbus_member_des
     std::memcpy(hp.data() + 2 * nz, desc->qv0_base, nz * sizeof(double));
     if (desc->u0_base) std::memcpy(hp.data() + 3 * nz, desc->u0_base, nz * sizeof(double));
     if (desc->v0_base) std::memcpy(hp.data() + 4 * nz, desc->v0_base, nz * sizeof(double));
-    std::vector<float2> hdp(nz);
-    split_dp0(desc->p0_base, desc->nz, hdp.data());
     const size_t bytes = L.cells * sizeof(float);
     cudaError_t err = cudaSuccess;
     const float* src[9] = {initial->u, initial->v, initial->w, initial->rho, initial->p, initial->theta,
@@ -556,7 +549,14 @@ nimbus_status nimbus_cuda_engine_admit(nimbus_engine* e, const nimbus_member_des
     float* dst[9] = {M.u, M.v, M.w, M.rho, M.p, M.theta, M.qv, M.qc, M.qr};
     for (int f = 0; f < 9 && err == cudaSuccess; ++f) err = cudaMemcpy(dst[f], src[f], bytes, cudaMemcpyHostToDevice);
     if (err == cudaSuccess) err = cudaMemcpy(prof, hp.data(), hp.size() * sizeof(double), cudaMemcpyHostToDevice);
-    if (err == cudaSuccess) err = cudaMemcpy(dp0, hdp.data(), nz * sizeof(float2), cudaMemcpyHostToDevice);
+    if (err == cudaSuccess)
+    {
+        // The same per-level kernel the per-operation path runs, so both forms
+        // see identical base data.
+        level_base_kernel<<<(desc->nz + 127) / 128, 128, 0, ctx->stream>>>(M.p0, desc->nz, M.gamma, dp0, eos0);
+        err = cudaGetLastError();
+        if (err == cudaSuccess) err = cudaStreamSynchronize(ctx->stream);
+    }
     if (err == cudaSuccess) err = cudaMemset(M.status, 0, sizeof(unsigned));
     // Scratch that a step reads before writing: none, but keep it defined.
     if (err == cudaSuccess) err = cudaMemset(M.wave, 0, L.history * sizeof(float));

@@ -52,6 +52,7 @@ struct EngineMember
     unsigned* status; // this member's status word (kStatus* bits)
     const double *rho0, *p0, *qv0, *u0, *v0;
     const float2* dp0;
+    const float4* eos0;
     FusedParams F;
     BoundaryParams B;
     TransportParams T;  // geometry and flags; the scalar pointers are taken from the fields above
@@ -183,7 +184,7 @@ static __global__ void __launch_bounds__(256) engine_continuity_kernel(const Eng
     const bool first = s == 0;
     for_member_items(table, prefix, tiles, kItemCells, [&](const EngineMember& M, int c) {
         unsigned flags = 0;
-        continuity_eos_cell<Policy>(M.F, engine_density(M, s, false), M.u, M.v, M.w, M.theta, M.rho0,
+        continuity_eos_cell<Policy>(M.F, engine_density(M, s, false), M.u, M.v, M.w, M.theta, M.rho0, M.eos0,
                                     engine_density(M, s, true), M.p, nullptr, M.mfx, M.mfy, M.mfz, c, flags, first,
                                     first ? M.rho_begin : nullptr);
         if (flags) atomicOr(M.status, flags);
@@ -200,8 +201,9 @@ static __global__ void __launch_bounds__(256) engine_momentum_kernel(const Engin
     });
 }
 
-// Pointer rotation after the acoustic loop (rho, when the substep count is
-// odd the final density sits in the partner) and after Kessler (qr).
+// Pointer rotation after the acoustic loop (rho: with an odd substep count
+// the final density sits in the partner) and at the end of the step (qr after
+// Kessler; p and the EOS candidate, which publishes the projection).
 static __global__ void engine_swap_kernel(EngineMember* table, int members, int which)
 {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
@@ -216,85 +218,84 @@ static __global__ void engine_swap_kernel(EngineMember* table, int members, int 
             M.rho_alt = t;
         }
     }
-    else if (M.microphysics)
+    else
     {
-        float* t = M.qr;
-        M.qr = M.qr_alt;
-        M.qr_alt = t;
+        if (M.microphysics)
+        {
+            float* t = M.qr;
+            M.qr = M.qr_alt;
+            M.qr_alt = t;
+        }
+        if (!(*M.status & kStatusInvalidEos))
+        {
+            float* t = M.p;
+            M.p = M.eos;
+            M.eos = t;
+        }
     }
 }
 
-// ---- Transport (blockIdx.y = scalar) --------------------------------------
+// ---- Transport (every scalar of a cell in one thread) -----------------------
 
 template <bool kFp32>
 static __global__ void __launch_bounds__(256) engine_transport_faces_kernel(const EngineMember* __restrict__ table,
-                                                                     const long long* __restrict__ prefix,
-                                                                     long long tiles)
+                                                                            const long long* __restrict__ prefix,
+                                                                            long long tiles)
 {
-    const int s = blockIdx.y;
     for_member_items(table, prefix, tiles, kItemCells, [&](const EngineMember& M, int c) {
-        const size_t n = (size_t)M.items[kItemCells];
-        transport_faces_cell<kFp32>(M.T, engine_scalar(M, s), M.mfx, M.mfy, M.mfz, M.sf + (size_t)s * 3 * n, c);
+        transport_faces_cell<kFp32>(M.T, kEngineScalars, [&](int s) { return engine_scalar(M, s); }, M.mfx, M.mfy,
+                                    M.mfz, M.sf, c);
     });
 }
 
+template <bool kFp32>
 static __global__ void __launch_bounds__(256) engine_transport_limiter_kernel(const EngineMember* __restrict__ table,
-                                                                       const long long* __restrict__ prefix,
-                                                                       long long tiles)
+                                                                              const long long* __restrict__ prefix,
+                                                                              long long tiles)
 {
-    const int s = blockIdx.y;
-    if (s == 0) return;  // theta is not positive definite
     for_member_items(table, prefix, tiles, kItemCells, [&](const EngineMember& M, int c) {
-        const size_t n = (size_t)M.items[kItemCells];
-        transport_limiter_cell(M.T, engine_scalar(M, s), M.rho_begin, M.sf + (size_t)s * 3 * n,
-                               M.rl + (size_t)s * n, c);
+        transport_limiter_cell<kFp32>(M.T, kEngineScalars, [&](int s) { return engine_scalar(M, s); }, M.rho_begin, M.sf,
+                               M.rl, c);
     });
 }
 
+template <bool kFp32>
 static __global__ void __launch_bounds__(256) engine_transport_update_kernel(const EngineMember* __restrict__ table,
-                                                                      const long long* __restrict__ prefix,
-                                                                      long long tiles)
+                                                                             const long long* __restrict__ prefix,
+                                                                             long long tiles)
 {
-    const int s = blockIdx.y;
     for_member_items(table, prefix, tiles, kItemCells, [&](const EngineMember& M, int c) {
-        const size_t n = (size_t)M.items[kItemCells];
         unsigned flags = 0;
-        transport_update_cell(M.T, s != 0, engine_scalar(M, s), engine_scalar_out(M, s), M.rho, M.rho_begin,
-                              M.sf + (size_t)s * 3 * n, M.rl + (size_t)s * n, c, flags);
+        transport_update_cell<kFp32>(M.T, kEngineScalars, [&](int s) { return engine_scalar(M, s); },
+                              [&](int s) { return engine_scalar_out(M, s); }, M.rho, M.rho_begin, M.sf, M.rl, c,
+                              flags);
         if (flags) atomicOr(M.status, flags);
     });
 }
 
 // ---- Kessler and EOS --------------------------------------------------------
 
-static __global__ void __launch_bounds__(256) engine_kessler_kernel(const EngineMember* __restrict__ table,
-                                                             const long long* __restrict__ prefix, long long tiles)
-{
-    for_member_items(table, prefix, tiles, kItemCells, [&](const EngineMember& M, int c) {
-        if (M.microphysics)
-            kessler_cell<true>(M.K, M.theta, M.qv, M.qc, M.qr, M.p, M.rho, M.qr_alt, nullptr, nullptr, nullptr,
-                               nullptr, c);
-    });
-}
-
-static __global__ void __launch_bounds__(256) engine_eos_kernel(const EngineMember* __restrict__ table,
-                                                         const long long* __restrict__ prefix, long long tiles)
+// The Kessler step and the EOS re-projection in one pass: the candidate
+// pressure is formed from the applied state while it is still in registers
+// and written to the member's candidate buffer; engine_swap_kernel publishes
+// it by exchanging p and the candidate unless the projection was refused.
+static __global__ void __launch_bounds__(256) engine_microphysics_eos_kernel(const EngineMember* __restrict__ table,
+                                                                             const long long* __restrict__ prefix,
+                                                                             long long tiles)
 {
     for_member_items(table, prefix, tiles, kItemCells, [&](const EngineMember& M, int c) {
         unsigned flags = 0;
-        eos_candidate_cell(M.K.d, M.rho, M.theta, M.p, M.qv, M.qc, M.qr, M.gamma, M.eos, c, flags);
+        float4 s;
+        const float po = M.p[c];
+        if (M.microphysics)
+            kessler_cell<true>(M.K, M.theta, M.qv, M.qc, M.qr, M.p, M.rho, M.qr_alt, nullptr, nullptr, nullptr,
+                               nullptr, c, &s);
+        else
+            s = make_float4(M.theta[c], M.qv[c], M.qc[c], M.qr[c]);
+        float p_new;
+        if (eos_candidate_value(M.K.d, c, M.rho[c], s.x, M.gamma, true, po, s.y, s.z, s.w, p_new, flags))
+            M.eos[c] = p_new;
         if (flags) atomicOr(M.status, flags);
-    });
-}
-
-// Publishes a member's candidate pressure unless its projection was refused
-// (then its whole grid keeps the old pressure, as the reference refuses).
-static __global__ void __launch_bounds__(256) engine_eos_publish_kernel(const EngineMember* __restrict__ table,
-                                                                 const long long* __restrict__ prefix,
-                                                                 long long tiles)
-{
-    for_member_items(table, prefix, tiles, kItemCells, [&](const EngineMember& M, int c) {
-        if (!(*M.status & kStatusInvalidEos)) M.p[c] = M.eos[c];
     });
 }
 

@@ -117,7 +117,8 @@ bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) ==
 template <class Policy>
 nimbus_status launch_fused_impl(nimbus_cuda_context* ctx, cudaStream_t st, FusedParams F, const Prognostic& in,
                                 const Prognostic& out, float* p, const float* theta, const double* rho0,
-                                const double* p0, const float2* dp0, float* drho, float* mfx, float* mfy, float* mfz)
+                                const double* p0, const float2* dp0, const float4* eos0, float* drho, float* mfx,
+                                float* mfy, float* mfz)
 {
     const size_t smem = FusedSmem<kFusedTJ>::floats(F.d.nz) * sizeof(float);
     auto kernel = acoustic_substep_fused_kernel<kFusedTJ, kFusedBlock, Policy>;
@@ -145,7 +146,7 @@ nimbus_status launch_fused_impl(nimbus_cuda_context* ctx, cudaStream_t st, Fused
     F.vec4 = (F.d.nz % 4 == 0) && aligned16(in.rho) && aligned16(in.u) && aligned16(in.v) && aligned16(in.w) &&
              aligned16(theta);
     LaunchTimer t(ctx, st, NIMBUS_KERNEL_ACOUSTIC_SUBSTEP);
-    kernel<<<strips * chunks, kFusedBlock, smem, st>>>(F, in.rho, in.u, in.v, in.w, theta, rho0, p0, dp0, drho,
+    kernel<<<strips * chunks, kFusedBlock, smem, st>>>(F, in.rho, in.u, in.v, in.w, theta, rho0, p0, dp0, eos0, drho,
                                                        out.rho, p, out.u, out.v, out.w, mfx, mfy, mfz, ctx->status);
     ctx->launches += 1;
     return NIMBUS_OK;
@@ -154,7 +155,8 @@ nimbus_status launch_fused_impl(nimbus_cuda_context* ctx, cudaStream_t st, Fused
 template <class Policy>
 nimbus_status launch_split_impl(nimbus_cuda_context* ctx, cudaStream_t st, FusedParams F, const Prognostic& in,
                                 const Prognostic& out, float* p, const float* theta, const double* rho0,
-                                const double* p0, const float2* dp0, float* drho, float* mfx, float* mfy, float* mfz)
+                                const double* p0, const float2* dp0, const float4* eos0, float* drho, float* mfx,
+                                float* mfy, float* mfz)
 {
     const long long n = F.d.cells();
     long long blocks = (n + kThreads - 1) / kThreads;
@@ -163,7 +165,7 @@ nimbus_status launch_split_impl(nimbus_cuda_context* ctx, cudaStream_t st, Fused
     {
         LaunchTimer t(ctx, st, NIMBUS_KERNEL_ACOUSTIC_SUBSTEP);
         split_continuity_eos_kernel<Policy><<<static_cast<int>(blocks), kThreads, 0, st>>>(
-            F, in.rho, in.u, in.v, in.w, theta, rho0, out.rho, p, drho, mfx, mfy, mfz, ctx->status);
+            F, in.rho, in.u, in.v, in.w, theta, rho0, eos0, out.rho, p, drho, mfx, mfy, mfz, ctx->status);
     }
     {
         LaunchTimer t(ctx, st, NIMBUS_KERNEL_ACOUSTIC_MOMENTUM);
@@ -184,16 +186,16 @@ int resolve_form(const nimbus_cuda_context* ctx, const Dims& d)
 
 nimbus_status launch_fused(nimbus_cuda_context* ctx, cudaStream_t st, const FusedParams& F, const Prognostic& in,
                            const Prognostic& out, float* p, const float* theta, const double* rho0, const double* p0,
-                           const float2* dp0, float* drho, float* mfx, float* mfy, float* mfz)
+                           const float2* dp0, const float4* eos0, float* drho, float* mfx, float* mfy, float* mfz)
 {
     const bool fp32 = ctx->precision == NIMBUS_PRECISION_FP32;
     if (resolve_form(ctx, F.d) == NIMBUS_SUBSTEP_SPLIT)
     {
-        if (fp32) return launch_split_impl<Fp32Policy>(ctx, st, F, in, out, p, theta, rho0, p0, dp0, drho, mfx, mfy, mfz);
-        return launch_split_impl<RefPolicy>(ctx, st, F, in, out, p, theta, rho0, p0, dp0, drho, mfx, mfy, mfz);
+        if (fp32) return launch_split_impl<Fp32Policy>(ctx, st, F, in, out, p, theta, rho0, p0, dp0, eos0, drho, mfx, mfy, mfz);
+        return launch_split_impl<RefPolicy>(ctx, st, F, in, out, p, theta, rho0, p0, dp0, eos0, drho, mfx, mfy, mfz);
     }
-    if (fp32) return launch_fused_impl<Fp32Policy>(ctx, st, F, in, out, p, theta, rho0, p0, dp0, drho, mfx, mfy, mfz);
-    return launch_fused_impl<RefPolicy>(ctx, st, F, in, out, p, theta, rho0, p0, dp0, drho, mfx, mfy, mfz);
+    if (fp32) return launch_fused_impl<Fp32Policy>(ctx, st, F, in, out, p, theta, rho0, p0, dp0, eos0, drho, mfx, mfy, mfz);
+    return launch_fused_impl<RefPolicy>(ctx, st, F, in, out, p, theta, rho0, p0, dp0, eos0, drho, mfx, mfy, mfz);
 }
 
 // Resting state for the autotuner: rho=1.1, u=v=w=0, p=9e4, theta=300, zero
@@ -225,15 +227,6 @@ __global__ void fill_tuning_state(float* buf, size_t n, double* prof, int nz, fl
         }
 }
 
-__global__ void dp0_split_kernel(const double* __restrict__ p0, int nz, float2* __restrict__ out)
-{
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= nz) return;
-    const double dp = (k + 1 < nz) ? p0[k + 1] - p0[k] : 0.0;
-    const float hi = (float)dp;
-    out[k] = make_float2(hi, (float)(dp - (double)hi));
-}
-
 FusedParams fused_params(const nimbus_cuda_context* ctx, int nx, int ny, int nz, double dx, double dy, double dz,
                          double dt, double gamma, float rho_min, float rho_max, float p_min, float p_max, float p_ref,
                          float wind_h, float wind_v)
@@ -253,6 +246,7 @@ FusedParams fused_params(const nimbus_cuda_context* ctx, int nx, int ny, int nz,
     F.wind_h = wind_h;
     F.wind_v = wind_v;
     F.chunk = 1;  // set at launch from the kernel's occupancy
+    finish_fp32(F);
     return F;
 }
 
@@ -293,6 +287,7 @@ nimbus_status run_batched_device(nimbus_cuda_context* ctx, cudaStream_t st, cons
     F.frame_u = a->frame_velocity_u_ms;
     F.frame_v = a->frame_velocity_v_ms;
     F.top_open = a->bc_top == kTopOpen;
+    finish_fp32(F);
 
     BoundaryParams B{};
     B.d = d;
@@ -305,15 +300,18 @@ nimbus_status run_batched_device(nimbus_cuda_context* ctx, cudaStream_t st, cons
     B.frame_v = a->frame_velocity_v_ms;
 
     float2* dp0 = nullptr;
+    float4* eos0 = nullptr;
     NB_TRY(ensure(ctx, kDp0, static_cast<size_t>(d.nz), &dp0));
-    dp0_split_kernel<<<(d.nz + 127) / 128, 128, 0, st>>>(D.p0, d.nz, dp0);
+    NB_TRY(ensure(ctx, kEos0, static_cast<size_t>(d.nz), &eos0));
+    level_base_kernel<<<(d.nz + 127) / 128, 128, 0, st>>>(D.p0, d.nz, F.gamma, dp0, eos0);
     ctx->launches += 1;
     Prognostic user{D.u, D.v, D.w, D.rho};
     Prognostic work{D.u_alt, D.v_alt, D.w_alt, D.rho_alt};
     Prognostic cur = user, alt = work;
     for (int s = 0; s < a->n_substeps; ++s)
     {
-        NB_TRY(launch_fused(ctx, st, F, cur, alt, D.p, D.theta, D.rho0, D.p0, dp0, nullptr, D.mfx, D.mfy, D.mfz));
+        NB_TRY(launch_fused(ctx, st, F, cur, alt, D.p, D.theta, D.rho0, D.p0, dp0, eos0, nullptr, D.mfx, D.mfy,
+                            D.mfz));
         AcousticDevice E = D;
         E.u = alt.u; E.v = alt.v; E.w = alt.w;
         launch_boundaries(ctx, st, B, E, alt.rho, wave);
@@ -338,12 +336,15 @@ nimbus_status run_fused_device(nimbus_cuda_context* ctx, cudaStream_t st, const 
     FusedParams F = fused_params(ctx, a->nx, a->ny, a->nz, a->dx, a->dy, a->dz, a->dt_small, a->gamma, a->rho_min,
                                  a->rho_max, a->p_min, a->p_max, a->p_ref_fallback, a->wind_clamp_h, a->wind_clamp_v);
     float2* dp0 = nullptr;
+    float4* eos0 = nullptr;
     NB_TRY(ensure(ctx, kDp0, static_cast<size_t>(a->nz), &dp0));
-    dp0_split_kernel<<<(a->nz + 127) / 128, 128, 0, st>>>(D.p0, a->nz, dp0);
+    NB_TRY(ensure(ctx, kEos0, static_cast<size_t>(a->nz), &eos0));
+    level_base_kernel<<<(a->nz + 127) / 128, 128, 0, st>>>(D.p0, a->nz, F.gamma, dp0, eos0);
     ctx->launches += 1;
     Prognostic user{D.u, D.v, D.w, D.rho};
     Prognostic work{D.u_alt, D.v_alt, D.w_alt, D.rho_alt};
-    NB_TRY(launch_fused(ctx, st, F, user, work, D.p, D.theta, D.rho0, D.p0, dp0, D.drho, nullptr, nullptr, nullptr));
+    NB_TRY(launch_fused(ctx, st, F, user, work, D.p, D.theta, D.rho0, D.p0, dp0, eos0, D.drho, nullptr, nullptr,
+                        nullptr));
     NB_CUDA(ctx, cudaMemcpyAsync(user.u, work.u, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
     NB_CUDA(ctx, cudaMemcpyAsync(user.v, work.v, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
     NB_CUDA(ctx, cudaMemcpyAsync(user.w, work.w, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
@@ -408,6 +409,7 @@ TransportParams transport_params(const nimbus_scalar_transport_args* a)
     T.top_open = a->top_open != 0;
     T.n_scalars = a->n_scalars;
     for (int s = 0; s < a->n_scalars; ++s) T.positive_definite[s] = a->positive_definite[s] != 0;
+    finish_fp32(T);
     return T;
 }
 
@@ -420,7 +422,7 @@ nimbus_status run_transport_device(nimbus_cuda_context* ctx, cudaStream_t st, co
     float* rl = nullptr;
     NB_TRY(ensure(ctx, kSf, 3 * n * T.n_scalars, &sf));
     NB_TRY(ensure(ctx, kRl, n * T.n_scalars, &rl));
-    const dim3 grid(grid_for(ctx, T.d.cells()), T.n_scalars);
+    const dim3 grid(grid_for(ctx, T.d.cells()));
     {
         LaunchTimer t(ctx, st, NIMBUS_KERNEL_TRANSPORT_FACES);
         if (ctx->precision == NIMBUS_PRECISION_FP32)
@@ -428,13 +430,16 @@ nimbus_status run_transport_device(nimbus_cuda_context* ctx, cudaStream_t st, co
         else
             transport_faces_kernel<false><<<grid, kThreads, 0, st>>>(T, mfx, mfy, mfz, sf);
     }
+    const bool fp32 = ctx->precision == NIMBUS_PRECISION_FP32;
     {
         LaunchTimer t(ctx, st, NIMBUS_KERNEL_TRANSPORT_LIMITER);
-        transport_limiter_kernel<<<grid, kThreads, 0, st>>>(T, rho_begin, sf, rl);
+        if (fp32) transport_limiter_kernel<true><<<grid, kThreads, 0, st>>>(T, rho_begin, sf, rl);
+        else transport_limiter_kernel<false><<<grid, kThreads, 0, st>>>(T, rho_begin, sf, rl);
     }
     {
         LaunchTimer t(ctx, st, NIMBUS_KERNEL_TRANSPORT_UPDATE);
-        transport_update_kernel<<<grid, kThreads, 0, st>>>(T, rho_end, rho_begin, sf, rl, ctx->status);
+        if (fp32) transport_update_kernel<true><<<grid, kThreads, 0, st>>>(T, rho_end, rho_begin, sf, rl, ctx->status);
+        else transport_update_kernel<false><<<grid, kThreads, 0, st>>>(T, rho_end, rho_begin, sf, rl, ctx->status);
     }
     ctx->launches += 3;
     NB_CUDA(ctx, cudaGetLastError());
@@ -473,6 +478,7 @@ SlowParams slow_params(const nimbus_slow_args* a)
     S.gravity = a->gravity;
     S.moist = a->qv != nullptr;
     S.loading = a->qc != nullptr;
+    finish_fp32(S);
     return S;
 }
 
@@ -921,11 +927,14 @@ nimbus_status nimbus_cuda_autotune_substep(nimbus_cuda_context* ctx, int nx, int
     float* buf = nullptr;
     double* prof = nullptr;
     float2* dp0 = nullptr;
+    float4* eos0 = nullptr;
     NB_CUDA(ctx, cudaMalloc(&buf, sizeof(float) * n * 13));
-    if (cudaMalloc(&prof, sizeof(double) * 2 * nz) != cudaSuccess || cudaMalloc(&dp0, sizeof(float2) * nz) != cudaSuccess)
+    if (cudaMalloc(&prof, sizeof(double) * 2 * nz) != cudaSuccess || cudaMalloc(&dp0, sizeof(float2) * nz) != cudaSuccess ||
+        cudaMalloc(&eos0, sizeof(float4) * nz) != cudaSuccess)
     {
         cudaFree(buf);
         if (prof) cudaFree(prof);
+        if (dp0) cudaFree(dp0);
         return fail(ctx, NIMBUS_ERR_OUT_OF_MEMORY, "autotune scratch");
     }
     cudaStream_t st = ctx->stream;
@@ -938,6 +947,8 @@ nimbus_status nimbus_cuda_autotune_substep(nimbus_cuda_context* ctx, int nx, int
     FusedParams F = fused_params(ctx, nx, ny, nz, 250.0, 250.0, 250.0, 0.1, 1004.0 / 717.0, 0.05f, 2.0f, 1000.0f,
                                  200000.0f, 100000.0f, 180.0f, 120.0f);
     F.weight = 0.1;
+    finish_fp32(F);
+    level_base_kernel<<<(nz + 127) / 128, 128, 0, st>>>(prof + nz, nz, F.gamma, dp0, eos0);
     const int saved_form = ctx->substep_form;
     const bool saved_timing = ctx->timing;
     ctx->timing = false;
@@ -954,8 +965,8 @@ nimbus_status nimbus_cuda_autotune_substep(nimbus_cuda_context* ctx, int nx, int
         for (int w = 0; w < 2 + reps && rc == NIMBUS_OK; ++w)
         {
             if (w == 2) cudaEventRecord(e0, st);
-            rc = launch_fused(ctx, st, F, (w & 1) ? b : a, (w & 1) ? a : b, p, theta, prof, prof + nz, dp0, nullptr,
-                              mf, mf + n, mf + 2 * n);
+            rc = launch_fused(ctx, st, F, (w & 1) ? b : a, (w & 1) ? a : b, p, theta, prof, prof + nz, dp0, eos0,
+                              nullptr, mf, mf + n, mf + 2 * n);
         }
         cudaEventRecord(e1, st);
         if (rc != NIMBUS_OK) break;
@@ -976,6 +987,7 @@ nimbus_status nimbus_cuda_autotune_substep(nimbus_cuda_context* ctx, int nx, int
     cudaFree(buf);
     cudaFree(prof);
     cudaFree(dp0);
+    cudaFree(eos0);
     ctx->substep_form = saved_form;
     ctx->timing = saved_timing;
     if (rc != NIMBUS_OK) return rc;

@@ -148,13 +148,16 @@ __device__ __forceinline__ float k_sed_flux(const KesslerParams& K, double qr_ra
 // Kessler tendencies of cell c and, with kApply, their application (theta,
 // qv, qc in place; the new qr to qr_out, since the cell below still reads
 // this cell's old qr for its sedimentation inflow).
+// With `fresh` the applied state of the cell (theta, qv, qc, qr) is also
+// returned, for a pass that continues from it in registers.
 template <bool kApply>
 __device__ __forceinline__ void kessler_cell(const KesslerParams& K, float* __restrict__ theta,
                                              float* __restrict__ qv, float* __restrict__ qc,
                                              const float* __restrict__ qr, const float* __restrict__ p,
                                              const float* __restrict__ rho, float* __restrict__ qr_out,
                                              float* __restrict__ dth_out, float* __restrict__ dqv_out,
-                                             float* __restrict__ dqc_out, float* __restrict__ dqr_out, int c)
+                                             float* __restrict__ dqc_out, float* __restrict__ dqr_out, int c,
+                                             float4* fresh = nullptr)
 {
     const Dims d = K.d;
     const double dt = K.dt;
@@ -253,7 +256,17 @@ __device__ __forceinline__ void kessler_cell(const KesslerParams& K, float* __re
         if (kApply)
         {
             float qr_new = qr_c;
-            if (inside)
+            float th_new, qv_new, qc_new;
+            if (!inside)
+            {
+                if (fresh)
+                {
+                    th_new = theta[c];
+                    qv_new = qv[c];
+                    qc_new = qc[c];
+                }
+            }
+            else
             {
                 // The CPU commit of step_microphysics_once with radiation,
                 // boundary layer and stochastic multipliers off
@@ -263,8 +276,10 @@ __device__ __forceinline__ void kessler_cell(const KesslerParams& K, float* __re
                     const float raw = (float)((double)q + dqs * dt);
                     return !isfinite(raw) ? 0.0f : (raw < 0.0f ? 0.0f : (0.05f < raw ? 0.05f : raw));
                 };
-                qv[c] = water(qv[c], dqv);
-                qc[c] = water(qc[c], dqc);
+                qv_new = water(qv[c], dqv);
+                qc_new = water(qc[c], dqc);
+                qv[c] = qv_new;
+                qc[c] = qc_new;
                 qr_new = water(qr_c, dqr);
                 const double told = (double)theta[c];
                 double total = (isfinite(dth) ? (double)dth : 0.0) * dt;
@@ -273,9 +288,11 @@ __device__ __forceinline__ void kessler_cell(const KesslerParams& K, float* __re
                 double tn = told + limited;
                 if (!isfinite(tn)) tn = isfinite(told) ? told : kTheta0;
                 const float stored = (float)tn;
-                theta[c] = clamp_value(stored, (float)kTheta0, 200.0f, 700.0f);
+                th_new = clamp_value(stored, (float)kTheta0, 200.0f, 700.0f);
+                theta[c] = th_new;
             }
             qr_out[c] = qr_new;
+            if (fresh) *fresh = make_float4(th_new, qv_new, qc_new, qr_new);
         }
     }
 }
@@ -301,34 +318,46 @@ static __global__ void __launch_bounds__(256) kessler_kernel(KesslerParams K, fl
 // attribution checks them (eos_apply.cpp:139-158): old p finite and positive,
 // qv finite and non-negative, qc + qr (FP64) finite and non-negative.  Any
 // failure sets the status bit; eos_publish_kernel then leaves p untouched.
-__device__ __forceinline__ void eos_candidate_cell(const Dims& d, const float* __restrict__ rho,
-                                                   const float* __restrict__ theta, const float* __restrict__ p_old,
-                                                   const float* __restrict__ qv, const float* __restrict__ qc,
-                                                   const float* __restrict__ qr, double gamma,
-                                                   float* __restrict__ p_candidate, int c, unsigned& flags)
+// The candidate pressure of cell c from its values; sets the refusal bit and
+// returns false for an invalid cell.  moist adds the attributed-domain checks.
+__device__ __forceinline__ bool eos_candidate_value(const Dims& d, int c, float r, float th, double gamma, bool moist,
+                                                    float po, float q, float qc, float qr, float& p_new,
+                                                    unsigned& flags)
 {
-    const float r = rho[c], th = theta[c];
     const double diagnosed = kP00 * pow((double)r * kRd * (double)th / kP00, gamma);
     if (!isfinite(r) || !(r > 0.0f) || !isfinite(th) || !(th > 0.0f) || !isfinite(diagnosed) || diagnosed <= 0.0 ||
         !isfinite((float)diagnosed))
     {
         flags |= kStatusInvalidEos;
-        return;
+        return false;
     }
-    p_candidate[c] = clamp_value((float)diagnosed, 101325.0f, 1000.0f, 200000.0f);
-    if (qv)
+    p_new = clamp_value((float)diagnosed, 101325.0f, 1000.0f, 200000.0f);
+    if (moist)
     {
         const int ih = d.nx >= 3, jh = d.ny >= 3;
         int i, j, k;
         decompose(d, c, i, j, k);
         if (i >= ih && i < d.nx - ih && j >= jh && j < d.ny - jh)
         {
-            const float po = p_old[c], q = qv[c];
-            const double liquid = (double)qc[c] + (double)qr[c];
+            const double liquid = (double)qc + (double)qr;
             if (!isfinite(po) || po <= 0.0f || !isfinite(q) || q < 0.0f || !isfinite(liquid) || liquid < 0.0)
                 flags |= kStatusInvalidEos;
         }
     }
+    return true;
+}
+
+__device__ __forceinline__ void eos_candidate_cell(const Dims& d, const float* __restrict__ rho,
+                                                   const float* __restrict__ theta, const float* __restrict__ p_old,
+                                                   const float* __restrict__ qv, const float* __restrict__ qc,
+                                                   const float* __restrict__ qr, double gamma,
+                                                   float* __restrict__ p_candidate, int c, unsigned& flags)
+{
+    const bool moist = qv != nullptr;
+    float p_new;
+    if (eos_candidate_value(d, c, rho[c], theta[c], gamma, moist, moist ? p_old[c] : 0.0f, moist ? qv[c] : 0.0f,
+                            moist ? qc[c] : 0.0f, moist ? qr[c] : 0.0f, p_new, flags))
+        p_candidate[c] = p_new;
 }
 
 static __global__ void __launch_bounds__(256) eos_candidate_kernel(Dims d, const float* __restrict__ rho,

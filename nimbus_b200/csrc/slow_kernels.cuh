@@ -28,8 +28,32 @@ struct SlowParams
     double gravity;
     int moist;    // qv and qv0 present
     int loading;  // qc, qr present
+    // FP32 form: the scalars above rounded once.
+    float inv_dx_f, inv_dy_f, inv_dz_f, half_inv_dx_f, half_inv_dy_f, half_inv_dz_f, dt_f, coriolis_f_f, frame_u_f,
+        frame_v_f, gravity_f;
 };
 
+__host__ __device__ inline void finish_fp32(SlowParams& S)
+{
+    S.inv_dx_f = (float)S.inv_dx;
+    S.inv_dy_f = (float)S.inv_dy;
+    S.inv_dz_f = (float)S.inv_dz;
+    S.half_inv_dx_f = (float)(0.5 * S.inv_dx);
+    S.half_inv_dy_f = (float)(0.5 * S.inv_dy);
+    S.half_inv_dz_f = (float)(0.5 * S.inv_dz);
+    S.dt_f = (float)S.dt;
+    S.coriolis_f_f = (float)S.coriolis_f;
+    S.frame_u_f = (float)S.frame_u;
+    S.frame_v_f = (float)S.frame_v;
+    S.gravity_f = (float)S.gravity;
+}
+
+// upwind_dx/dy/dz (derivative_operators.hpp:324-395): fd5 upwind-biased in
+// the interior, fd3 two points from a boundary, fd1 next to it, 0 on it.
+// Away from the boundary the side is selected, not branched on: the a < 0
+// stencils of fd5 and fd1 are the a >= 0 ones on the mirrored points with
+// every intermediate negated (the reference's own operation order, so the
+// result is bit-identical), and lanes with opposite winds do not diverge.
 template <class real>
 __device__ __forceinline__ real upwind_deriv(const float* __restrict__ f, int c, int stride, int idx, int n, real a,
                                              real inv_d)
@@ -37,21 +61,31 @@ __device__ __forceinline__ real upwind_deriv(const float* __restrict__ f, int c,
     const int half = min(idx, n - 1 - idx);
     const real cc = (real)f[c];
     if (half <= 0) return (real)0;
-    const real m1 = (real)f[c - stride], p1 = (real)f[c + stride];
-    if (half == 1) return (a >= (real)0) ? (cc - m1) * inv_d : (p1 - cc) * inv_d;
-    const real m2 = (real)f[c - 2 * stride], p2 = (real)f[c + 2 * stride];
+    const bool pos = a >= (real)0;
+    const int s = pos ? stride : -stride;
+    const real x1 = (real)f[c - s], y1 = (real)f[c + s];
+    if (half == 1)
+    {
+        const real v = (cc - x1) * inv_d;
+        return pos ? v : -v;
+    }
     if (half == 2)
-        return (a >= (real)0) ? ((real)2 * p1 + (real)3 * cc - (real)6 * m1 + m2) * (inv_d / (real)6)
-                              : (-p2 + (real)6 * p1 - (real)3 * cc - (real)2 * m1) * (inv_d / (real)6);
-    const real m3 = (real)f[c - 3 * stride], p3 = (real)f[c + 3 * stride];
-    return (a >= (real)0)
-               ? ((real)-2 * m3 + (real)15 * m2 - (real)60 * m1 + (real)20 * cc + (real)30 * p1 - (real)3 * p2) *
-                     (inv_d / (real)60)
-               : ((real)2 * p3 - (real)15 * p2 + (real)60 * p1 - (real)20 * cc - (real)30 * m1 + (real)3 * m2) *
-                     (inv_d / (real)60);
+    {
+        const real m1 = (real)f[c - stride], p1 = (real)f[c + stride];
+        const real m2 = (real)f[c - 2 * stride], p2 = (real)f[c + 2 * stride];
+        return pos ? ((real)2 * p1 + (real)3 * cc - (real)6 * m1 + m2) * (inv_d / (real)6)
+                   : (-p2 + (real)6 * p1 - (real)3 * cc - (real)2 * m1) * (inv_d / (real)6);
+    }
+    const real x2 = (real)f[c - 2 * s], y2 = (real)f[c + 2 * s], x3 = (real)f[c - 3 * s];
+    const real v = ((real)-2 * x3 + (real)15 * x2 - (real)60 * x1 + (real)20 * cc + (real)30 * y1 - (real)3 * y2) *
+                   (inv_d / (real)60);
+    return pos ? v : -v;
 }
 
 // The four slow tendencies of cell c (zero outside their index ranges).
+// Reference policy: the reference's FP64 interior arithmetic and order.  FP32
+// policy: the same stencils in FP32, the base-state face averages formed in
+// FP64 and rounded once.
 template <class Policy>
 __device__ __forceinline__ void slow_tendencies_at(const SlowParams& S, int c, int i, int j, int k,
                                                    const float* __restrict__ u, const float* __restrict__ v,
@@ -63,13 +97,27 @@ __device__ __forceinline__ void slow_tendencies_at(const SlowParams& S, int c, i
                                                    float& out_u, float& out_v, float& out_w, float& out_p)
 {
     using real = typename Policy::real;
+    constexpr bool f32 = sizeof(real) == 4;
     const Dims d = S.d;
     out_u = out_v = out_w = out_p = 0.0f;
     if (!(i >= 1 && i < d.nx - 1 && j >= 1 && j < d.ny - 1 && k < d.nz - 1)) return;
     const int sx = d.sx(), sy = d.sy();
     const real q = (real)0.25, h = (real)0.5;
-    const real inv_dx = (real)S.inv_dx, inv_dy = (real)S.inv_dy, inv_dz = (real)S.inv_dz;
-    const real fu = (real)S.frame_u, fv = (real)S.frame_v, cf = (real)S.coriolis_f;
+    real inv_dx, inv_dy, inv_dz, fu, fv, cf;
+    if constexpr (f32)
+    {
+        inv_dx = S.inv_dx_f; inv_dy = S.inv_dy_f; inv_dz = S.inv_dz_f;
+        fu = S.frame_u_f; fv = S.frame_v_f; cf = S.coriolis_f_f;
+    }
+    else
+    {
+        inv_dx = S.inv_dx; inv_dy = S.inv_dy; inv_dz = S.inv_dz;
+        fu = S.frame_u; fv = S.frame_v; cf = S.coriolis_f;
+    }
+    auto store = [](real t) -> float {
+        if constexpr (f32) return isfinite(t) ? t : 0.0f;
+        else return (float)finite_or_zero((double)t);
+    };
     // du at the x-face
     {
         const real ux = (real)u[c];
@@ -83,7 +131,7 @@ __device__ __forceinline__ void slow_tendencies_at(const SlowParams& S, int c, i
                                   : upwind_deriv<real>(u, c, 1, k, d.nz, wx, inv_dz);
         const real v0k = v0 ? (real)v0[k] : (real)0;
         const real du = -tux * ddx - tuy * ddy - wx * ddz + cf * (uy - v0k);
-        out_u = (float)finite_or_zero((double)du);
+        out_u = store(du);
     }
     // dv at the y-face
     {
@@ -98,7 +146,7 @@ __device__ __forceinline__ void slow_tendencies_at(const SlowParams& S, int c, i
                                   : upwind_deriv<real>(v, c, 1, k, d.nz, wy, inv_dz);
         const real u0k = u0 ? (real)u0[k] : (real)0;
         const real dv = -tux * ddx - tvy * ddy - wy * ddz - cf * (ux - u0k);
-        out_v = (float)finite_or_zero((double)dv);
+        out_v = store(dv);
     }
     // dw at the z-face
     {
@@ -110,27 +158,53 @@ __device__ __forceinline__ void slow_tendencies_at(const SlowParams& S, int c, i
         const real ddy = upwind_deriv<real>(w, c, sy, j, d.ny, tuy, inv_dy);
         const real ddz = (k == 0) ? ((wz >= (real)0) ? ((real)w[c] - (real)0) * inv_dz : ((real)w[c + 1] - (real)w[c]) * inv_dz)
                                   : upwind_deriv<real>(w, c, 1, k, d.nz, wz, inv_dz);
-        const double rho_face = 0.5 * ((double)rho[c] + (double)rho[c + 1]);
-        const double rho_s = safe_rho(rho_face);
-        const double rho0_face = 0.5 * (rho0[k] + rho0[k + 1]);
-        const double g = S.gravity;
-        const double buoy = -g * (rho_face - rho0_face) / rho_s;
-        double moist = 0.0;
-        if (S.moist)
+        real forcing;
+        if constexpr (f32)
         {
-            const double qf = 0.5 * ((double)qv[c] + (double)qv[c + 1]);
-            const double q0f = 0.5 * ((double)(float)qv0[k] + (double)(float)qv0[k + 1]);
-            moist = g * 0.608 * (qf - q0f);
+            const float g = S.gravity_f;
+            const float rho_face = 0.5f * (rho[c] + rho[c + 1]);
+            const float rho_s = (isfinite(rho_face) && rho_face > 1.0e-6f) ? rho_face : 1.0f;
+            const float rho0_face = (float)(0.5 * (rho0[k] + rho0[k + 1]));
+            forcing = -g * (rho_face - rho0_face) / rho_s;
+            if (S.moist)
+            {
+                const float qf = 0.5f * (qv[c] + qv[c + 1]);
+                const float q0f = (float)(0.5 * ((double)(float)qv0[k] + (double)(float)qv0[k + 1]));
+                forcing += g * 0.608f * (qf - q0f);
+            }
+            if (S.loading)
+                forcing += -g * (0.5f * ((qc[c] + qr[c]) + (qc[c + 1] + qr[c + 1])));
         }
-        double load = 0.0;
-        if (S.loading)
+        else
         {
-            const double lo = (double)qc[c] + (double)qr[c] + 0.0 + 0.0 + 0.0 + 0.0;
-            const double hi = (double)qc[c + 1] + (double)qr[c + 1] + 0.0 + 0.0 + 0.0 + 0.0;
-            load = -g * (0.5 * (lo + hi));
+            const double rho_face = 0.5 * ((double)rho[c] + (double)rho[c + 1]);
+            const double rho_s = safe_rho(rho_face);
+            const double rho0_face = 0.5 * (rho0[k] + rho0[k + 1]);
+            const double g = S.gravity;
+            const double buoy = -g * (rho_face - rho0_face) / rho_s;
+            double moist = 0.0;
+            if (S.moist)
+            {
+                const double qf = 0.5 * ((double)qv[c] + (double)qv[c + 1]);
+                const double q0f = 0.5 * ((double)(float)qv0[k] + (double)(float)qv0[k + 1]);
+                moist = g * 0.608 * (qf - q0f);
+            }
+            double load = 0.0;
+            if (S.loading)
+            {
+                const double lo = (double)qc[c] + (double)qr[c] + 0.0 + 0.0 + 0.0 + 0.0;
+                const double hi = (double)qc[c + 1] + (double)qr[c + 1] + 0.0 + 0.0 + 0.0 + 0.0;
+                load = -g * (0.5 * (lo + hi));
+            }
+            forcing = 0;
+            const real dw = -tux * ddx - tuy * ddy - wz * ddz + (real)buoy + (real)moist + (real)load;
+            out_w = store(dw);
         }
-        const real dw = -tux * ddx - tuy * ddy - wz * ddz + (real)buoy + (real)moist + (real)load;
-        out_w = (float)finite_or_zero((double)dw);
+        if constexpr (f32)
+        {
+            const real dw = -tux * ddx - tuy * ddy - wz * ddz + forcing;
+            out_w = store(dw);
+        }
     }
     // dp at the centre
     if (k >= 1)
@@ -139,16 +213,30 @@ __device__ __forceinline__ void slow_tendencies_at(const SlowParams& S, int c, i
         const real vc = h * ((real)v[c] + (real)v[c - sy]);
         const real tuc = uc - fu, tvc = vc - fv;
         const real wc = h * ((real)w[c] + (real)w[c - 1]);
-        const real dpdx = ((real)p[c + sx] - (real)p[c - sx]) * (real)(0.5 * S.inv_dx);
-        const real dpdy = ((real)p[c + sy] - (real)p[c - sy]) * (real)(0.5 * S.inv_dy);
-        const real dpdz = ((real)p[c + 1] - (real)p[c - 1]) * (real)(0.5 * S.inv_dz);
-        out_p = (float)finite_or_zero((double)(-tuc * dpdx - tvc * dpdy - wc * dpdz));
+        real hx, hy, hz;
+        if constexpr (f32)
+        {
+            hx = S.half_inv_dx_f; hy = S.half_inv_dy_f; hz = S.half_inv_dz_f;
+        }
+        else
+        {
+            hx = (real)(0.5 * S.inv_dx); hy = (real)(0.5 * S.inv_dy); hz = (real)(0.5 * S.inv_dz);
+        }
+        const real dpdx = ((real)p[c + sx] - (real)p[c - sx]) * hx;
+        const real dpdy = ((real)p[c + sy] - (real)p[c - sy]) * hy;
+        const real dpdz = ((real)p[c + 1] - (real)p[c - 1]) * hz;
+        out_p = store(-tuc * dpdx - tvc * dpdy - wc * dpdz);
     }
 }
 
-__device__ __forceinline__ float slow_apply_one(float x, float t, double dt)
+// x + dt * t (apply_slow_tendencies_cpu, dynamics.cpp:1955-2080: a
+// non-finite tendency counts as zero).  Reference policy: FP64 add rounded
+// once; FP32 policy: one FMA.
+template <class Policy>
+__device__ __forceinline__ float slow_apply_one(const SlowParams& S, float x, float t)
 {
-    return (float)((double)x + finite_or_zero((double)t) * dt);
+    if constexpr (sizeof(typename Policy::real) == 4) return __fmaf_rn(isfinite(t) ? t : 0.0f, S.dt_f, x);
+    else return (float)((double)x + finite_or_zero((double)t) * S.dt);
 }
 
 // k1 at cell c and, when su is given, the predictor state x* = x + dt*k1.
@@ -172,10 +260,10 @@ __device__ __forceinline__ void slow_predict_cell(
     k1p[c] = tp;
     if (su != nullptr)
     {
-        su[c] = slow_apply_one(u[c], tu, S.dt);
-        sv[c] = slow_apply_one(v[c], tv, S.dt);
-        sw[c] = slow_apply_one(w[c], tw, S.dt);
-        sp[c] = slow_apply_one(p[c], tp, S.dt);
+        su[c] = slow_apply_one<Policy>(S, u[c], tu);
+        sv[c] = slow_apply_one<Policy>(S, v[c], tv);
+        sw[c] = slow_apply_one<Policy>(S, w[c], tw);
+        sp[c] = slow_apply_one<Policy>(S, p[c], tp);
     }
 }
 
@@ -222,10 +310,10 @@ __device__ __forceinline__ void slow_correct_cell(
         tw_out[c] = tw;
         tp_out[c] = tp;
     }
-    u[c] = slow_apply_one(u[c], tu, S.dt);
-    v[c] = slow_apply_one(v[c], tv, S.dt);
-    w[c] = slow_apply_one(w[c], tw, S.dt);
-    p[c] = slow_apply_one(p[c], tp, S.dt);
+    u[c] = slow_apply_one<Policy>(S, u[c], tu);
+    v[c] = slow_apply_one<Policy>(S, v[c], tv);
+    w[c] = slow_apply_one<Policy>(S, w[c], tw);
+    p[c] = slow_apply_one<Policy>(S, p[c], tp);
 }
 
 template <class Policy>

@@ -12,6 +12,8 @@
 
 #include "stencil_common.cuh"
 
+#include <type_traits>
+
 namespace nimbus
 {
 
@@ -29,7 +31,19 @@ struct TransportParams
     const float* q_in[kMaxScalars];
     float* q_out[kMaxScalars];
     int positive_definite[kMaxScalars];
+    // FP32 form: the scalars above rounded once.
+    float inv_dx_f, inv_dy_f, inv_dz_f, dt_f, inv_dt_f, rho_floor_f;
 };
+
+__host__ __device__ inline void finish_fp32(TransportParams& T)
+{
+    T.inv_dx_f = (float)T.inv_dx;
+    T.inv_dy_f = (float)T.inv_dy;
+    T.inv_dz_f = (float)T.inv_dz;
+    T.dt_f = (float)T.dt;
+    T.inv_dt_f = (float)(1.0 / T.dt);
+    T.rho_floor_f = (float)T.rho_floor;
+}
 
 // weno5_face_value (include/numerics/advection/weno5_face.hpp:43-86).
 __device__ __forceinline__ double weno5_face(double a, double b, double c, double d, double e)
@@ -72,19 +86,26 @@ __device__ __forceinline__ double mc_slope(double qm, double q0, double qp)
 }
 
 // Face value for face l+1/2 on an axis of extent n, cells at q[base + m*stride].
+// The upwind side is chosen by selecting the stencil, not by branching: with
+// s = +1 (mflux >= 0) or -1 and the donor cell l + (s < 0), the reference's
+// two calls weno5_face(q[l-2], q[l-1], q[l], q[l+1], q[l+2]) and
+// weno5_face(q[l+3], q[l+2], q[l+1], q[l], q[l-1]) are the one call on
+// q[donor - 2s .. donor + 2s], so lanes with opposite fluxes do not diverge.
 __device__ __forceinline__ double face_value(const float* __restrict__ q, int base, int stride, int l, int n,
                                              double mflux, int weno)
 {
 #define NQ(m) ((double)q[base + (m) * stride])
-    if (mflux >= 0.0)
+    const bool pos = mflux >= 0.0;
+    const int donor = pos ? l : l + 1;
+    const int s = pos ? 1 : -1;
+    const double q0 = NQ(donor);
+    if (weno && donor - 2 >= 0 && donor + 2 <= n - 1)
+        return weno5_face(NQ(donor - 2 * s), NQ(donor - s), q0, NQ(donor + s), NQ(donor + 2 * s));
+    if (pos)
     {
-        const double q0 = NQ(l);
-        if (weno && l >= 2 && l + 2 <= n - 1) return weno5_face(NQ(l - 2), NQ(l - 1), q0, NQ(l + 1), NQ(l + 2));
         const double sl = (l >= 1) ? mc_slope(NQ(l - 1), q0, NQ(l + 1)) : 0.0;
         return q0 + 0.5 * sl;
     }
-    const double q0 = NQ(l + 1);
-    if (weno && l - 1 >= 0 && l + 3 <= n - 1) return weno5_face(NQ(l + 3), NQ(l + 2), q0, NQ(l), NQ(l - 1));
     const double sl = (l + 1 <= n - 2) ? mc_slope(NQ(l), q0, NQ(l + 2)) : 0.0;
     return q0 - 0.5 * sl;
 #undef NQ
@@ -135,84 +156,77 @@ __device__ __forceinline__ float mc_slope_f32(float qm, float q0, float qp)
     return 0.0f;
 }
 
-// FP32 scalar face flux M*phi as M*base + M*offset (the reference's FP32 GPU form).
+// FP32 scalar face flux M*phi as M*base + M*offset (the reference's FP32 GPU
+// form), upwind side selected as in face_value.
 __device__ __forceinline__ float face_flux_f32(const float* __restrict__ q, int base, int stride, int l, int n,
                                                float mflux, int weno)
 {
 #define NQ(m) (q[base + (m) * stride])
-    float donor, offset;
-    if (mflux >= 0.0f)
-    {
-        donor = NQ(l);
-        if (weno && l >= 2 && l + 2 <= n - 1) offset = weno5_offset_f32(NQ(l - 2), NQ(l - 1), donor, NQ(l + 1), NQ(l + 2));
-        else offset = 0.5f * ((l >= 1) ? mc_slope_f32(NQ(l - 1), donor, NQ(l + 1)) : 0.0f);
-    }
+    const bool pos = mflux >= 0.0f;
+    const int donor = pos ? l : l + 1;
+    const int s = pos ? 1 : -1;
+    const float q0 = NQ(donor);
+    float offset;
+    if (weno && donor - 2 >= 0 && donor + 2 <= n - 1)
+        offset = weno5_offset_f32(NQ(donor - 2 * s), NQ(donor - s), q0, NQ(donor + s), NQ(donor + 2 * s));
+    else if (pos)
+        offset = 0.5f * ((l >= 1) ? mc_slope_f32(NQ(l - 1), q0, NQ(l + 1)) : 0.0f);
     else
-    {
-        donor = NQ(l + 1);
-        if (weno && l - 1 >= 0 && l + 3 <= n - 1) offset = weno5_offset_f32(NQ(l + 3), NQ(l + 2), donor, NQ(l), NQ(l - 1));
-        else offset = -0.5f * ((l + 1 <= n - 2) ? mc_slope_f32(NQ(l), donor, NQ(l + 2)) : 0.0f);
-    }
-    return __fmaf_rn(mflux, donor, mflux * offset);
+        offset = -0.5f * ((l + 1 <= n - 2) ? mc_slope_f32(NQ(l), q0, NQ(l + 2)) : 0.0f);
+    return __fmaf_rn(mflux, q0, mflux * offset);
 #undef NQ
 }
 
-// Face fluxes of scalar s owned by cell c (its +x, +y and +z faces).
+// Face fluxes owned by cell c (its +x, +y and +z faces) for every scalar:
+// the cell's index and mass fluxes are loaded once and the scalars follow.
 // kFp32 selects the reference's FP32 GPU form (face_flux_f32), otherwise FP64
-// face values rounded once to the FP32 scratch.
-// sf points at the scalar's [3][cells] face-flux scratch (x, y, z).
-template <bool kFp32>
-__device__ __forceinline__ void transport_faces_cell(const TransportParams& T, const float* __restrict__ q,
+// face values rounded once to the FP32 scratch.  q(s) gives scalar s's field;
+// sf is the [scalars][3][cells] face-flux scratch (x, y, z).
+template <bool kFp32, class QIn>
+__device__ __forceinline__ void transport_faces_cell(const TransportParams& T, int scalars, QIn&& q_of,
                                                      const float* __restrict__ mfx, const float* __restrict__ mfy,
                                                      const float* __restrict__ mfz, float* __restrict__ sf, int c)
 {
     const Dims d = T.d;
-    const int n = d.cells();
-    float* __restrict__ sfx = sf;
-    float* __restrict__ sfy = sfx + n;
-    float* __restrict__ sfz = sfy + n;
+    const size_t n = (size_t)d.cells();
     const int kz_end = T.top_open ? d.nz : d.nz - 1;
     int i, j, k;
     decompose(d, c, i, j, k);
-    if constexpr (kFp32)
+    const bool hx = i <= d.nx - 2, hy = j <= d.ny - 2, hz = k < kz_end, top = k == d.nz - 1;
+    const float fx = hx ? mfx[c] : 0.0f, fy = hy ? mfy[c] : 0.0f, fz = hz ? mfz[c] : 0.0f;
+    const int bx = c - i * d.sx(), by = c - j * d.sy(), bz = c - k;
+    for (int s = 0; s < scalars; ++s)
     {
-        if (i <= d.nx - 2) sfx[c] = face_flux_f32(q, c - i * d.sx(), d.sx(), i, d.nx, mfx[c], T.weno);
-        if (j <= d.ny - 2) sfy[c] = face_flux_f32(q, c - j * d.sy(), d.sy(), j, d.ny, mfy[c], T.weno);
-        if (k < kz_end)
+        const float* __restrict__ q = q_of(s);
+        float* __restrict__ sfx = sf + (size_t)s * 3 * n;
+        float* __restrict__ sfy = sfx + n;
+        float* __restrict__ sfz = sfy + n;
+        if constexpr (kFp32)
         {
-            const float mf = mfz[c];
-            sfz[c] = (k == d.nz - 1) ? mf * q[c] : face_flux_f32(q, c - k, 1, k, d.nz, mf, T.weno);
+            if (hx) sfx[c] = face_flux_f32(q, bx, d.sx(), i, d.nx, fx, T.weno);
+            if (hy) sfy[c] = face_flux_f32(q, by, d.sy(), j, d.ny, fy, T.weno);
+            if (hz) sfz[c] = top ? fz * q[c] : face_flux_f32(q, bz, 1, k, d.nz, fz, T.weno);
         }
-    }
-    else
-    {
-        if (i <= d.nx - 2)
+        else
         {
-            const double mf = (double)mfx[c];
-            sfx[c] = (float)(mf * face_value(q, c - i * d.sx(), d.sx(), i, d.nx, mf, T.weno));
-        }
-        if (j <= d.ny - 2)
-        {
-            const double mf = (double)mfy[c];
-            sfy[c] = (float)(mf * face_value(q, c - j * d.sy(), d.sy(), j, d.ny, mf, T.weno));
-        }
-        if (k < kz_end)
-        {
-            const double mf = (double)mfz[c];
-            if (k == d.nz - 1) sfz[c] = (float)(mf * (double)q[c]);
-            else sfz[c] = (float)(mf * face_value(q, c - k, 1, k, d.nz, mf, T.weno));
+            if (hx) sfx[c] = (float)((double)fx * face_value(q, bx, d.sx(), i, d.nx, (double)fx, T.weno));
+            if (hy) sfy[c] = (float)((double)fy * face_value(q, by, d.sy(), j, d.ny, (double)fy, T.weno));
+            if (hz)
+                sfz[c] = top ? (float)((double)fz * (double)q[c])
+                             : (float)((double)fz * face_value(q, bz, 1, k, d.nz, (double)fz, T.weno));
         }
     }
 }
 
 template <bool kFp32>
 static __global__ void __launch_bounds__(256) transport_faces_kernel(TransportParams T, const float* __restrict__ mfx,
-                                                              const float* __restrict__ mfy,
-                                                              const float* __restrict__ mfz, float* __restrict__ sf)
+                                                                     const float* __restrict__ mfy,
+                                                                     const float* __restrict__ mfz,
+                                                                     float* __restrict__ sf)
 {
     const int n = T.d.cells();
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
-        transport_faces_cell<kFp32>(T, T.q_in[blockIdx.y], mfx, mfy, mfz, sf + (size_t)blockIdx.y * 3 * n, c);
+        transport_faces_cell<kFp32>(T, T.n_scalars, [&](int s) { return T.q_in[s]; }, mfx, mfy, mfz, sf, c);
 }
 
 // conservative_pd_limiter_factor (advection_cartesian.hpp:101-108), non-support path.
@@ -224,45 +238,78 @@ __device__ __forceinline__ float pd_limiter_factor(double r)
     return nextafterf(__fmul_rn(stored, roundoff), 0.0f);
 }
 
-// Positive-definite donor ratio of scalar s at cell c (advection_cartesian.cpp:2174-2240).
-// sf is the scalar's face-flux scratch, rl its [cells] limiter factors.
-__device__ __forceinline__ void transport_limiter_cell(const TransportParams& T, const float* __restrict__ q,
+// Positive-definite donor ratio at cell c (advection_cartesian.cpp:2174-2240)
+// for every positive-definite scalar; rl is [scalars][cells].  kFp32: the
+// same sums in FP32 (the reference's FP32 GPU form); the factor's 32-ulp
+// roundoff margin covers the FP32 rounding of the update.
+template <bool kFp32, class QIn>
+__device__ __forceinline__ void transport_limiter_cell(const TransportParams& T, int scalars, QIn&& q_of,
                                                        const float* __restrict__ rho_begin,
-                                                       const float* __restrict__ sf, float* __restrict__ r_out, int c)
+                                                       const float* __restrict__ sf, float* __restrict__ rl, int c)
 {
+    using real = typename std::conditional<kFp32, float, double>::type;
     const Dims d = T.d;
-    const int n = d.cells();
-    const float* __restrict__ sfx = sf;
-    const float* __restrict__ sfy = sfx + n;
-    const float* __restrict__ sfz = sfy + n;
+    const size_t n = (size_t)d.cells();
     int i, j, k;
     decompose(d, c, i, j, k);
-    double out = 0.0;
-    if (i <= d.nx - 2 && sfx[c] > 0.0f) out += (double)sfx[c] * T.inv_dx;
-    if (i >= 1 && sfx[c - d.sx()] < 0.0f) out -= (double)sfx[c - d.sx()] * T.inv_dx;
-    if (j <= d.ny - 2 && sfy[c] > 0.0f) out += (double)sfy[c] * T.inv_dy;
-    if (j >= 1 && sfy[c - d.sy()] < 0.0f) out -= (double)sfy[c - d.sy()] * T.inv_dy;
-    if ((k <= d.nz - 2 || (T.top_open && k == d.nz - 1)) && sfz[c] > 0.0f) out += (double)sfz[c] * T.inv_dz;
-    if (k >= 1 && sfz[c - 1] < 0.0f) out -= (double)sfz[c - 1] * T.inv_dz;
-    double r = 1.0;
-    if (out > 0.0)
+    const bool xm = i >= 1, xp = i <= d.nx - 2, ym = j >= 1, yp = j <= d.ny - 2, zm = k >= 1;
+    const bool zp = k <= d.nz - 2 || (T.top_open && k == d.nz - 1);
+    const real rb = (real)rho_begin[c];
+    const real idx = kFp32 ? (real)T.inv_dx_f : (real)T.inv_dx;
+    const real idy = kFp32 ? (real)T.inv_dy_f : (real)T.inv_dy;
+    const real idz = kFp32 ? (real)T.inv_dz_f : (real)T.inv_dz;
+    for (int s = 0; s < scalars; ++s)
     {
-        const double qc = (double)q[c];
-        const double available = (double)rho_begin[c] * ((qc < 0.0) ? 0.0 : qc) / T.dt;  // std::max(q, 0.0)
-        const double ratio = available / out;
-        r = (ratio < 1.0) ? ratio : 1.0;  // std::min(1.0, ratio), NaN -> 1
+        if (!T.positive_definite[s]) continue;
+        const float* __restrict__ sfx = sf + (size_t)s * 3 * n;
+        const float* __restrict__ sfy = sfx + n;
+        const float* __restrict__ sfz = sfy + n;
+        real out = 0;
+        if (xp && sfx[c] > 0.0f) out += (real)sfx[c] * idx;
+        if (xm && sfx[c - d.sx()] < 0.0f) out -= (real)sfx[c - d.sx()] * idx;
+        if (yp && sfy[c] > 0.0f) out += (real)sfy[c] * idy;
+        if (ym && sfy[c - d.sy()] < 0.0f) out -= (real)sfy[c - d.sy()] * idy;
+        if (zp && sfz[c] > 0.0f) out += (real)sfz[c] * idz;
+        if (zm && sfz[c - 1] < 0.0f) out -= (real)sfz[c - 1] * idz;
+        float factor;
+        if constexpr (kFp32)
+        {
+            float r = 1.0f;
+            if (out > 0.0f)
+            {
+                const float qc = q_of(s)[c];
+                const float available = rb * ((qc < 0.0f) ? 0.0f : qc) * T.inv_dt_f;
+                const float ratio = __fdividef(available, out);
+                r = (ratio < 1.0f) ? ratio : 1.0f;
+            }
+            factor = (r > 0.0f && r < 1.0f) ? nextafterf(__fmul_rn(r, 1.0f - 32.0f * 1.1920928955078125e-7f), 0.0f)
+                                             : r;
+        }
+        else
+        {
+            double r = 1.0;
+            if (out > 0.0)
+            {
+                const double qc = (double)q_of(s)[c];
+                const double available = rb * ((qc < 0.0) ? 0.0 : qc) / T.dt;  // std::max(q, 0.0)
+                const double ratio = available / out;
+                r = (ratio < 1.0) ? ratio : 1.0;  // std::min(1.0, ratio), NaN -> 1
+            }
+            factor = pd_limiter_factor(r);
+        }
+        rl[(size_t)s * n + c] = factor;
     }
-    r_out[c] = pd_limiter_factor(r);
 }
 
-static __global__ void __launch_bounds__(256) transport_limiter_kernel(TransportParams T, const float* __restrict__ rho_begin,
-                                                                const float* __restrict__ sf, float* __restrict__ rl)
+template <bool kFp32>
+static __global__ void __launch_bounds__(256) transport_limiter_kernel(TransportParams T,
+                                                                       const float* __restrict__ rho_begin,
+                                                                       const float* __restrict__ sf,
+                                                                       float* __restrict__ rl)
 {
-    const int s = blockIdx.y;
-    if (!T.positive_definite[s]) return;
     const int n = T.d.cells();
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
-        transport_limiter_cell(T, T.q_in[s], rho_begin, sf + (size_t)s * 3 * n, rl + (size_t)s * n, c);
+        transport_limiter_cell<kFp32>(T, T.n_scalars, [&](int s) { return T.q_in[s]; }, rho_begin, sf, rl, c);
 }
 
 __device__ __forceinline__ double limited_flux(float raw, bool pd, const float* __restrict__ rl, int lo, int hi)
@@ -272,74 +319,101 @@ __device__ __forceinline__ double limited_flux(float raw, bool pd, const float* 
     return (double)raw * (double)r;
 }
 
-// Donor-limited divergence and density recovery of scalar s at cell c
-// (advection_cartesian.cpp:2465-2640).  q_out may alias q_in: cell c reads
-// only its own old value, the fluxes live in the scratch.
-__device__ __forceinline__ void transport_update_cell(const TransportParams& T, bool pd, const float* q, float* qo,
-                                                      const float* __restrict__ rho_end,
+// Donor-limited divergence and density recovery at cell c for every scalar
+// (advection_cartesian.cpp:2465-2640).  The output may alias the input: cell
+// c reads only its own old value, the fluxes live in the scratch.  kFp32: the
+// same sums in FP32.
+template <bool kFp32, class QIn, class QOut>
+__device__ __forceinline__ void transport_update_cell(const TransportParams& T, int scalars, QIn&& q_of,
+                                                      QOut&& qo_of, const float* __restrict__ rho_end,
                                                       const float* __restrict__ rho_begin,
-                                                      const float* __restrict__ sf, const float* __restrict__ r,
+                                                      const float* __restrict__ sf, const float* __restrict__ rl,
                                                       int c, unsigned& flags)
 {
+    using real = typename std::conditional<kFp32, float, double>::type;
     const Dims d = T.d;
-    const int n = d.cells();
-    const float* __restrict__ sfx = sf;
-    const float* __restrict__ sfy = sfx + n;
-    const float* __restrict__ sfz = sfy + n;
+    const size_t n = (size_t)d.cells();
     int i, j, k;
     decompose(d, c, i, j, k);
     if (!(i >= 1 && i < d.nx - 1 && j >= 1 && j < d.ny - 1))
     {
-        if (q != qo) qo[c] = q[c];  // seed_destination_from_source
+        for (int s = 0; s < scalars; ++s)
+        {
+            const float* q = q_of(s);
+            float* qo = qo_of(s);
+            if (q != qo) qo[c] = q[c];  // seed_destination_from_source
+        }
         return;
     }
     const int cxm = c - d.sx(), cxp = c + d.sx(), cym = c - d.sy(), cyp = c + d.sy();
     const bool has_top = k <= d.nz - 2 || (T.top_open && k == d.nz - 1);
-    const double sxp = limited_flux(sfx[c], pd, r, c, cxp);
-    const double sxm = limited_flux(sfx[cxm], pd, r, cxm, c);
-    const double syp = limited_flux(sfy[c], pd, r, c, cyp);
-    const double sym = limited_flux(sfy[cym], pd, r, cym, c);
-    const double szp = has_top ? limited_flux(sfz[c], pd, r, c, k < d.nz - 1 ? c + 1 : c) : 0.0;
-    const double szm = (k >= 1) ? limited_flux(sfz[c - 1], pd, r, c - 1, c) : 0.0;
-    const double re = (double)rho_end[c];
-    const double rb = (double)rho_begin[c];
-    const double qc = (double)q[c];
-    double rho_phi;
-    if (pd)
+    const real re = (real)rho_end[c];
+    const real rb = (real)rho_begin[c];
+    const real floor_ = kFp32 ? (real)T.rho_floor_f : (real)T.rho_floor;
+    const real denom = (re > floor_) ? re : floor_;
+    const real idx = kFp32 ? (real)T.inv_dx_f : (real)T.inv_dx;
+    const real idy = kFp32 ? (real)T.inv_dy_f : (real)T.inv_dy;
+    const real idz = kFp32 ? (real)T.inv_dz_f : (real)T.inv_dz;
+    const real dt = kFp32 ? (real)T.dt_f : (real)T.dt;
+    auto limited = [&](float raw, bool pd, const float* __restrict__ r, int lo, int hi) -> real {
+        if constexpr (kFp32)
+        {
+            if (!pd || raw == 0.0f) return raw;
+            return raw * (raw > 0.0f ? r[lo] : r[hi]);
+        }
+        else return limited_flux(raw, pd, r, lo, hi);
+    };
+    for (int s = 0; s < scalars; ++s)
     {
-        double outgoing = 0.0, incoming = 0.0;
-        if (sxp >= 0.0) outgoing += sxp * T.inv_dx; else incoming -= sxp * T.inv_dx;
-        if (sxm <= 0.0) outgoing -= sxm * T.inv_dx; else incoming += sxm * T.inv_dx;
-        if (syp >= 0.0) outgoing += syp * T.inv_dy; else incoming -= syp * T.inv_dy;
-        if (sym <= 0.0) outgoing -= sym * T.inv_dy; else incoming += sym * T.inv_dy;
-        if (has_top) { if (szp >= 0.0) outgoing += szp * T.inv_dz; else incoming -= szp * T.inv_dz; }
-        if (k >= 1) { if (szm <= 0.0) outgoing -= szm * T.inv_dz; else incoming += szm * T.inv_dz; }
-        rho_phi = (rb * qc - T.dt * outgoing) + T.dt * incoming;
+        const bool pd = T.positive_definite[s] != 0;
+        const float* __restrict__ sfx = sf + (size_t)s * 3 * n;
+        const float* __restrict__ sfy = sfx + n;
+        const float* __restrict__ sfz = sfy + n;
+        const float* __restrict__ r = rl + (size_t)s * n;
+        const real sxp = limited(sfx[c], pd, r, c, cxp);
+        const real sxm = limited(sfx[cxm], pd, r, cxm, c);
+        const real syp = limited(sfy[c], pd, r, c, cyp);
+        const real sym = limited(sfy[cym], pd, r, cym, c);
+        const real szp = has_top ? limited(sfz[c], pd, r, c, k < d.nz - 1 ? c + 1 : c) : (real)0;
+        const real szm = (k >= 1) ? limited(sfz[c - 1], pd, r, c - 1, c) : (real)0;
+        const real qc = (real)q_of(s)[c];
+        real rho_phi;
+        if (pd)
+        {
+            real outgoing = 0, incoming = 0;
+            if (sxp >= 0) outgoing += sxp * idx; else incoming -= sxp * idx;
+            if (sxm <= 0) outgoing -= sxm * idx; else incoming += sxm * idx;
+            if (syp >= 0) outgoing += syp * idy; else incoming -= syp * idy;
+            if (sym <= 0) outgoing -= sym * idy; else incoming += sym * idy;
+            if (has_top) { if (szp >= 0) outgoing += szp * idz; else incoming -= szp * idz; }
+            if (k >= 1) { if (szm <= 0) outgoing -= szm * idz; else incoming += szm * idz; }
+            rho_phi = (rb * qc - dt * outgoing) + dt * incoming;
+        }
+        else
+        {
+            const real div = (sxp - sxm) * idx + (syp - sym) * idy + (szp - szm) * idz;
+            rho_phi = rb * qc - dt * div;
+        }
+        float out;
+        if constexpr (kFp32) out = __fdividef(rho_phi, denom);
+        else out = (float)(rho_phi / denom);
+        if (!isfinite(out)) flags |= kStatusNonfiniteTransport;
+        qo_of(s)[c] = out;
     }
-    else
-    {
-        const double div = (sxp - sxm) * T.inv_dx + (syp - sym) * T.inv_dy + (szp - szm) * T.inv_dz;
-        rho_phi = rb * qc - T.dt * div;
-    }
-    const double denom = (re > T.rho_floor) ? re : T.rho_floor;
-    const float out = (float)(rho_phi / denom);
-    if (!isfinite(out)) flags |= kStatusNonfiniteTransport;
-    qo[c] = out;
 }
 
-static __global__ void __launch_bounds__(256) transport_update_kernel(TransportParams T, const float* __restrict__ rho_end,
-                                                               const float* __restrict__ rho_begin,
-                                                               const float* __restrict__ sf,
-                                                               const float* __restrict__ rl, unsigned* status)
+template <bool kFp32>
+static __global__ void __launch_bounds__(256) transport_update_kernel(TransportParams T,
+                                                                      const float* __restrict__ rho_end,
+                                                                      const float* __restrict__ rho_begin,
+                                                                      const float* __restrict__ sf,
+                                                                      const float* __restrict__ rl, unsigned* status)
 {
     const int n = T.d.cells();
     unsigned flags = 0;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
-    {
-        const int s = blockIdx.y;
-        transport_update_cell(T, T.positive_definite[s] != 0, T.q_in[s], T.q_out[s], rho_end, rho_begin,
-                              sf + (size_t)s * 3 * n, rl + (size_t)s * n, c, flags);
-    }
+        transport_update_cell<kFp32>(T, T.n_scalars, [&](int s) { return T.q_in[s]; }, [&](int s) { return T.q_out[s]; },
+                              rho_end, rho_begin, sf, rl, c, flags);
     if (flags) atomicOr(status, flags);
 }
 
