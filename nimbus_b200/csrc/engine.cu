@@ -288,7 +288,8 @@ nimbus_status rebuild_table(nimbus_engine* e)
     {
         long long* p = e->prefix.data() + static_cast<size_t>(k) * (n + 1);
         p[0] = 0;
-        for (size_t r = 0; r < n; ++r) p[r + 1] = p[r] + (host[r].items[k] + kEngineBlock - 1) / kEngineBlock;
+        const int tile = kEngineBlock * kItemsPerThread;
+        for (size_t r = 0; r < n; ++r) p[r + 1] = p[r] + (host[r].items[k] + tile - 1) / tile;
     }
     e->active.assign(max_n, 0);
     for (int s = 0; s < max_n; ++s)

@@ -74,6 +74,11 @@ __device__ __forceinline__ float* engine_scalar_out(const EngineMember& M, int s
     return s == 0 ? M.theta : (s == 1 ? M.qv : (s == 2 ? M.qc : M.qr));
 }
 
+// Items per thread in a tile: a tile is kTileItems = 4 * blockDim.x
+// consecutive items of one member, so the member lookup and its pointers are
+// loaded once for four items and each load instruction stays coalesced.
+constexpr int kItemsPerThread = 1;
+
 // Calls fn(member, item) for every item of the first tiles of a kind.
 template <class Fn>
 __device__ __forceinline__ void for_member_items(const EngineMember* __restrict__ table,
@@ -85,15 +90,21 @@ __device__ __forceinline__ void for_member_items(const EngineMember* __restrict_
     {
         while (t >= prefix[m + 1]) ++m;
         const EngineMember& M = table[m];
-        const int item = (int)((t - prefix[m]) * blockDim.x) + (int)threadIdx.x;
-        if (item < M.items[kind]) fn(M, item);
+        const int count = M.items[kind];
+        const int base = (int)((t - prefix[m]) * (kItemsPerThread * blockDim.x)) + (int)threadIdx.x;
+#pragma unroll
+        for (int q = 0; q < kItemsPerThread; ++q)
+        {
+            const int item = base + q * (int)blockDim.x;
+            if (item < count) fn(M, item);
+        }
     }
 }
 
 // ---- Heun slow step -------------------------------------------------------
 
 template <class Policy>
-static __global__ void __launch_bounds__(256) engine_slow_predict_kernel(const EngineMember* __restrict__ table,
+static __global__ void __launch_bounds__(256, 4) engine_slow_predict_kernel(const EngineMember* __restrict__ table,
                                                                   const long long* __restrict__ prefix,
                                                                   long long tiles)
 {
@@ -106,7 +117,7 @@ static __global__ void __launch_bounds__(256) engine_slow_predict_kernel(const E
 }
 
 template <class Policy>
-static __global__ void __launch_bounds__(256) engine_slow_correct_kernel(const EngineMember* __restrict__ table,
+static __global__ void __launch_bounds__(256, 4) engine_slow_correct_kernel(const EngineMember* __restrict__ table,
                                                                   const long long* __restrict__ prefix,
                                                                   long long tiles)
 {
@@ -177,7 +188,7 @@ static __global__ void __launch_bounds__(256) engine_seed_kernel(const EngineMem
 // ---- Acoustic substep (split form, u/v/w in place, rho ping-pong) ---------
 
 template <class Policy>
-static __global__ void __launch_bounds__(256) engine_continuity_kernel(const EngineMember* __restrict__ table,
+static __global__ void __launch_bounds__(256, 6) engine_continuity_kernel(const EngineMember* __restrict__ table,
                                                                 const long long* __restrict__ prefix,
                                                                 long long tiles, int s)
 {
@@ -279,7 +290,7 @@ static __global__ void __launch_bounds__(256) engine_transport_update_kernel(con
 // pressure is formed from the applied state while it is still in registers
 // and written to the member's candidate buffer; engine_swap_kernel publishes
 // it by exchanging p and the candidate unless the projection was refused.
-static __global__ void __launch_bounds__(256) engine_microphysics_eos_kernel(const EngineMember* __restrict__ table,
+static __global__ void __launch_bounds__(256, 4) engine_microphysics_eos_kernel(const EngineMember* __restrict__ table,
                                                                              const long long* __restrict__ prefix,
                                                                              long long tiles)
 {

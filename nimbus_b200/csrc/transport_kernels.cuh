@@ -392,10 +392,17 @@ __device__ __forceinline__ void transport_update_cell(const TransportParams& T, 
         else
         {
             const real div = (sxp - sxm) * idx + (syp - sym) * idy + (szp - szm) * idz;
-            rho_phi = rb * qc - dt * div;
+            if constexpr (kFp32)
+            {
+                // (rb q - dt div) / denom as q + ((rb - denom) q - dt div) / denom:
+                // the small increment carries the FP32 rounding instead of the
+                // full value (theta ~ 300 K would lose its perturbation bits).
+                rho_phi = (rb - denom) * qc - dt * div;
+            }
+            else rho_phi = rb * qc - dt * div;
         }
         float out;
-        if constexpr (kFp32) out = __fdividef(rho_phi, denom);
+        if constexpr (kFp32) out = pd ? __fdividef(rho_phi, denom) : qc + __fdividef(rho_phi, denom);
         else out = (float)(rho_phi / denom);
         if (!isfinite(out)) flags |= kStatusNonfiniteTransport;
         qo_of(s)[c] = out;
