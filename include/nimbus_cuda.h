@@ -473,7 +473,9 @@ nimbus_status nimbus_cuda_acoustic_boundaries(nimbus_cuda_context* ctx, const ni
  *   substeps (retained mass flux, continuity + EOS, momentum, boundaries);
  *   conservative WENO5 transport of theta, qv, qc, qr; Kessler tendencies and
  *   their application (microphysics == 1); EOS pressure re-projection.
- * Members may differ in grid, spacing, dt and substep count.
+ * Members may differ in grid, spacing, dt and substep count.  With Kessler
+ * on, dt must not exceed 0.8 dz / (20 m/s), the bound under which the
+ * reference runs the microphysics in one call instead of subcycling it.
  */
 typedef struct nimbus_engine nimbus_engine;
 

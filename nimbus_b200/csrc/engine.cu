@@ -82,6 +82,12 @@ const char* check_desc(const nimbus_member_desc* d)
         !std::isfinite(d->frame_velocity_v_ms))
         return "coriolis_f and frame velocity must be finite";
     if (d->microphysics != 0 && d->microphysics != 1) return "microphysics must be 0 (none) or 1 (Kessler)";
+    // step_microphysics subcycles when the interval exceeds the sedimentation
+    // limit 0.8 dz / max terminal velocity (microphysics_step.cpp:3500-3575,
+    // 3686-3740); Kessler's fall speed is capped at 20 m/s, so dt <= 0.04 dz
+    // guarantees the single call this engine makes.
+    if (d->microphysics == 1 && d->dt > 0.8 * d->dz / 20.0)
+        return "dt exceeds the Kessler sedimentation limit 0.8 dz / (20 m/s); the reference would subcycle";
     if (!d->rho0_base || !d->p0_base || !d->qv0_base) return "rho0, p0 and qv0 base profiles are required";
     return nullptr;
 }

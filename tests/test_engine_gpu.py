@@ -169,6 +169,10 @@ def test_admission_refuses_beyond_free_memory(ctx):
     run.engine.retire(mid)
     assert run.engine.members == 0
     run.step(1)  # an empty engine steps as a no-op
+    # a dt the reference would subcycle the microphysics for is refused
+    fast = cuda.member_desc(case.shape, (case.dx, case.dy, case.dz), 0.8 * case.dz / 20.0 + 1.0, 4, case.bc, base)
+    with pytest.raises(cuda.NimbusCudaError):
+        run.engine.admit(fast, st)
     run.close()
 
 
