@@ -17,30 +17,44 @@
 namespace nimbus
 {
 
-// First substep of a large step writes the retained flux instead of adding to
-// it: float(0.0 + w*flux) is bit-identical to accumulating into a zeroed slot
-// (the +0.0 turns a -0.0 product into +0.0 exactly as the add would).
-__device__ __forceinline__ void fused_store(float* slot, double weight, double flux, unsigned& flags)
+// Retained-flux update from an already loaded slot value.  Reference policy:
+// the FP64 weighted sum rounded once to the FP32 slot (fused_accumulate);
+// FP32 policy: one FMA (retain_flux_f32).  With store the slot starts from
+// zero -- the first substep of a large step writes instead of accumulating,
+// bit-identical to accumulating into a zeroed slot (the 0.0 + product turns a
+// -0.0 into +0.0 exactly as the add would).
+template <class Policy>
+__device__ __forceinline__ void retain_flux_from(float* slot, float old, const FusedParams& P, double flux64,
+                                                 float flux32, unsigned& flags, bool store)
 {
-    const float st = (float)(0.0 + weight * flux);
-    if (isfinite(st)) *slot = st;
+    if constexpr (Policy::exact_pow)
+    {
+        const float st = (float)((store ? 0.0 : (double)old) + P.weight * flux64);
+        if (isfinite(st)) *slot = st;
+        else
+        {
+            if (store) *slot = 0.0f;
+            flags |= kStatusNonfiniteMassFlux;
+        }
+    }
     else
     {
-        *slot = 0.0f;
-        flags |= kStatusNonfiniteMassFlux;
+        const float st = __fmaf_rn(P.weight_f, flux32, store ? 0.0f : old);
+        if (isfinite(st)) *slot = st;
+        else
+        {
+            if (store) *slot = 0.0f;
+            flags |= kStatusNonfiniteMassFlux;
+        }
     }
-}
-
-__device__ __forceinline__ void retain_flux(float* slot, double weight, double flux, unsigned& flags, bool store)
-{
-    if (store) fused_store(slot, weight, flux, flags);
-    else fused_accumulate(slot, weight, flux, flags);
 }
 
 // Continuity, rho forward Euler and EOS for cell c.  With store_flux the
 // retained fluxes are written rather than accumulated and rho_copy (when
 // given) receives the pre-substep density (the transport context's
-// beginning density).
+// beginning density).  Every load is issued before any arithmetic (indices of
+// neighbours outside the grid are clamped to the cell; those values are not
+// used), so a thread has all of its memory requests in flight at once.
 template <class Policy>
 __device__ __forceinline__ void continuity_eos_cell(const FusedParams& P, const float* __restrict__ rho,
                                                     const float* __restrict__ u, const float* __restrict__ v,
@@ -55,59 +69,72 @@ __device__ __forceinline__ void continuity_eos_cell(const FusedParams& P, const 
     using real = typename Policy::real;
     const Dims d = P.d;
     const int sx = d.sx(), sy = d.sy();
+    int i, j, k;
+    decompose(d, c, i, j, k);
+    const bool xlo = i >= 1, xhi = i < d.nx - 1, ylo = j >= 1, yhi = j < d.ny - 1;
+    const bool zlo = k > 0, zhi = k + 1 < d.nz;
+    const float rho_c = rho[c];
+    const float rxp = rho[xhi ? c + sx : c], rxm = rho[xlo ? c - sx : c];
+    const float ryp = rho[yhi ? c + sy : c], rym = rho[ylo ? c - sy : c];
+    const float rzp = rho[zhi ? c + 1 : c], rzm = rho[zlo ? c - 1 : c];
+    const float uc = u[c], uxm = u[xlo ? c - sx : c];
+    const float vc = v[c], vym = v[ylo ? c - sy : c];
+    const float wc = w[c], wzm = w[zlo ? c - 1 : c];
+    const float th = theta[c];
+    const bool flux = mfx != nullptr;
+    const bool acc = flux && !store_flux;
+    const float mx = acc ? mfx[c] : 0.0f, my = acc ? mfy[c] : 0.0f, mz = acc ? mfz[c] : 0.0f;
+
+    if (rho_copy != nullptr) rho_copy[c] = rho_c;
+    if (flux)
     {
-        int i, j, k;
-        decompose(d, c, i, j, k);
-        const float rho_c = rho[c];
-        if (rho_copy != nullptr) rho_copy[c] = rho_c;
-        if (mfx != nullptr)
+        if constexpr (sizeof(real) == 8)
         {
-            if constexpr (sizeof(real) == 8)
-            {
-                const double rc = (double)rho_c;
-                if (i < d.nx - 1) retain_flux(mfx + c, P.weight, 0.5 * (rc + (double)rho[c + sx]) * ((double)u[c] - P.frame_u), flags, store_flux);
-                if (j < d.ny - 1) retain_flux(mfy + c, P.weight, 0.5 * (rc + (double)rho[c + sy]) * ((double)v[c] - P.frame_v), flags, store_flux);
-                const double zf = (k == d.nz - 1) ? (P.top_open ? rc * (double)w[c] : 0.0)
-                                                  : 0.5 * (rc + (double)rho[c + 1]) * (double)w[c];
-                retain_flux(mfz + c, P.weight, zf, flags, store_flux);
-            }
-            else
-            {
-                if (i < d.nx - 1)
-                    retain_flux_f32(mfx + c, P.weight_f, 0.5f * (rho_c + rho[c + sx]) * (u[c] - P.frame_u_f), flags,
-                                    store_flux);
-                if (j < d.ny - 1)
-                    retain_flux_f32(mfy + c, P.weight_f, 0.5f * (rho_c + rho[c + sy]) * (v[c] - P.frame_v_f), flags,
-                                    store_flux);
-                const float zf = (k == d.nz - 1) ? (P.top_open ? rho_c * w[c] : 0.0f) : 0.5f * (rho_c + rho[c + 1]) * w[c];
-                retain_flux_f32(mfz + c, P.weight_f, zf, flags, store_flux);
-            }
+            const double rc = (double)rho_c;
+            if (xhi)
+                retain_flux_from<Policy>(mfx + c, mx, P, 0.5 * (rc + (double)rxp) * ((double)uc - P.frame_u), 0.0f,
+                                         flags, store_flux);
+            if (yhi)
+                retain_flux_from<Policy>(mfy + c, my, P, 0.5 * (rc + (double)ryp) * ((double)vc - P.frame_v), 0.0f,
+                                         flags, store_flux);
+            const double zf = !zhi ? (P.top_open ? rc * (double)wc : 0.0) : 0.5 * (rc + (double)rzp) * (double)wc;
+            retain_flux_from<Policy>(mfz + c, mz, P, zf, 0.0f, flags, store_flux);
         }
-        real drho = (real)0;
-        if (i >= 1 && i < d.nx - 1 && j >= 1 && j < d.ny - 1)
+        else
         {
-            const real rc = (real)rho_c;
-            const real half = (real)0.5;
-            const real fx_pos = half * (rc + (real)rho[c + sx]) * (real)u[c];
-            const real fx_neg = half * ((real)rho[c - sx] + rc) * (real)u[c - sx];
-            const real fy_pos = half * (rc + (real)rho[c + sy]) * (real)v[c];
-            const real fy_neg = half * ((real)rho[c - sy] + rc) * (real)v[c - sy];
-            const real fz_pos = (k + 1 < d.nz) ? half * (rc + (real)rho[c + 1]) * (real)w[c] : rc * (real)w[c];
-            const real fz_neg = (k > 0) ? half * ((real)rho[c - 1] + rc) * (real)w[c - 1] : (real)0;
-            if constexpr (sizeof(real) == 8)
-                drho = -((fx_pos - fx_neg) * P.inv_dx + (fy_pos - fy_neg) * P.inv_dy + (fz_pos - fz_neg) * P.inv_dz);
-            else
-                drho = -((fx_pos - fx_neg) * P.inv_dx_f + (fy_pos - fy_neg) * P.inv_dy_f +
-                         (fz_pos - fz_neg) * P.inv_dz_f);
+            if (xhi)
+                retain_flux_from<Policy>(mfx + c, mx, P, 0.0, 0.5f * (rho_c + rxp) * (uc - P.frame_u_f), flags,
+                                         store_flux);
+            if (yhi)
+                retain_flux_from<Policy>(mfy + c, my, P, 0.0, 0.5f * (rho_c + ryp) * (vc - P.frame_v_f), flags,
+                                         store_flux);
+            const float zf = !zhi ? (P.top_open ? rho_c * wc : 0.0f) : 0.5f * (rho_c + rzp) * wc;
+            retain_flux_from<Policy>(mfz + c, mz, P, 0.0, zf, flags, store_flux);
         }
-        float drho_stored;
-        if constexpr (sizeof(real) == 8) drho_stored = (float)finite_or_zero(drho);
-        else drho_stored = isfinite(drho) ? drho : 0.0f;
-        if (drho_out != nullptr) drho_out[c] = drho_stored;
-        const float rho_stored = substep_density<Policy>(P, rho_c, drho_stored, rho0, k);
-        rho_out[c] = rho_stored;
-        p_out[c] = substep_pressure<Policy>(P, eos0, k, rho_stored, theta[c]);
     }
+    real drho = (real)0;
+    if (xlo && xhi && ylo && yhi)
+    {
+        const real rc = (real)rho_c;
+        const real half = (real)0.5;
+        const real fx_pos = half * (rc + (real)rxp) * (real)uc;
+        const real fx_neg = half * ((real)rxm + rc) * (real)uxm;
+        const real fy_pos = half * (rc + (real)ryp) * (real)vc;
+        const real fy_neg = half * ((real)rym + rc) * (real)vym;
+        const real fz_pos = zhi ? half * (rc + (real)rzp) * (real)wc : rc * (real)wc;
+        const real fz_neg = zlo ? half * ((real)rzm + rc) * (real)wzm : (real)0;
+        if constexpr (sizeof(real) == 8)
+            drho = -((fx_pos - fx_neg) * P.inv_dx + (fy_pos - fy_neg) * P.inv_dy + (fz_pos - fz_neg) * P.inv_dz);
+        else
+            drho = -((fx_pos - fx_neg) * P.inv_dx_f + (fy_pos - fy_neg) * P.inv_dy_f + (fz_pos - fz_neg) * P.inv_dz_f);
+    }
+    float drho_stored;
+    if constexpr (sizeof(real) == 8) drho_stored = (float)finite_or_zero(drho);
+    else drho_stored = isfinite(drho) ? drho : 0.0f;
+    if (drho_out != nullptr) drho_out[c] = drho_stored;
+    const float rho_stored = substep_density<Policy>(P, rho_c, drho_stored, rho0, k);
+    rho_out[c] = rho_stored;
+    p_out[c] = substep_pressure<Policy>(P, eos0, k, rho_stored, th);
 }
 
 template <class Policy>
@@ -137,57 +164,57 @@ __device__ __forceinline__ void momentum_cell(const FusedParams& P, const float*
     using real = typename Policy::real;
     const Dims d = P.d;
     const int sx = d.sx(), sy = d.sy();
+    int i, j, k;
+    decompose(d, c, i, j, k);
+    const bool interior = i >= 1 && i < d.nx - 1 && j >= 1 && j < d.ny - 1 && k < d.nz - 1;
+    // Every load first; outside the interior the neighbour indices fall back
+    // to the cell itself (those values are not used).
+    const int cx = interior ? c + sx : c, cy = interior ? c + sy : c, cz1 = interior ? c + 1 : c;
+    const float rc = rho[c], rx = rho[cx], ry = rho[cy], rz = rho[cz1];
+    const float pc = p[c], px = p[cx], py = p[cy], pz = p[cz1];
+    const float uc = u[c], vc = v[c], wc = w[c];
+    float du = 0.0f, dv = 0.0f, dw = 0.0f;
+    if constexpr (sizeof(real) == 8)
     {
-        int i, j, k;
-        decompose(d, c, i, j, k);
-        float du = 0.0f, dv = 0.0f, dw = 0.0f;
-        if (i >= 1 && i < d.nx - 1 && j >= 1 && j < d.ny - 1 && k < d.nz - 1)
+        if (interior)
         {
-            if constexpr (sizeof(real) == 8)
-            {
-                const double rc = (double)rho[c];
-                const double rho_x = 0.5 * (rc + (double)rho[c + sx]);
-                const double rho_y = 0.5 * (rc + (double)rho[c + sy]);
-                const double rho_z = 0.5 * (rc + (double)rho[c + 1]);
-                const double pc = (double)p[c];
-                const double dp0_dz = (p0[k + 1] - p0[k]) * P.inv_dz;
-                du = (float)finite_or_zero(-((double)p[c + sx] - pc) * P.inv_dx / safe_rho(rho_x));
-                dv = (float)finite_or_zero(-((double)p[c + sy] - pc) * P.inv_dy / safe_rho(rho_y));
-                dw = (float)finite_or_zero(-((((double)p[c + 1] - pc) * P.inv_dz) - dp0_dz) / safe_rho(rho_z));
-            }
-            else
-            {
-                const float rc = rho[c];
-                const float rho_x = 0.5f * (rc + rho[c + sx]);
-                const float rho_y = 0.5f * (rc + rho[c + sy]);
-                const float rho_z = 0.5f * (rc + rho[c + 1]);
-                const float pc = p[c];
-                const float2 dp0 = dp0_split[k];
-                const float dpz = ((p[c + 1] - pc) - dp0.x) - dp0.y;
-                const float sxr = (isfinite(rho_x) && rho_x > 1.0e-6f) ? rho_x : 1.0f;
-                const float syr = (isfinite(rho_y) && rho_y > 1.0e-6f) ? rho_y : 1.0f;
-                const float szr = (isfinite(rho_z) && rho_z > 1.0e-6f) ? rho_z : 1.0f;
-                const float a = __fdividef(-(p[c + sx] - pc) * P.inv_dx_f, sxr);
-                const float b = __fdividef(-(p[c + sy] - pc) * P.inv_dy_f, syr);
-                const float cz = __fdividef(-dpz * P.inv_dz_f, szr);
-                du = isfinite(a) ? a : 0.0f;
-                dv = isfinite(b) ? b : 0.0f;
-                dw = isfinite(cz) ? cz : 0.0f;
-            }
+            const double rcd = (double)rc;
+            const double rho_x = 0.5 * (rcd + (double)rx);
+            const double rho_y = 0.5 * (rcd + (double)ry);
+            const double rho_z = 0.5 * (rcd + (double)rz);
+            const double pcd = (double)pc;
+            const double dp0_dz = (p0[k + 1] - p0[k]) * P.inv_dz;
+            du = (float)finite_or_zero(-((double)px - pcd) * P.inv_dx / safe_rho(rho_x));
+            dv = (float)finite_or_zero(-((double)py - pcd) * P.inv_dy / safe_rho(rho_y));
+            dw = (float)finite_or_zero(-((((double)pz - pcd) * P.inv_dz) - dp0_dz) / safe_rho(rho_z));
         }
-        if constexpr (sizeof(real) == 8)
+        u_out[c] = clamp_value((float)((double)uc + (double)du * P.dt_small), 0.0f, -P.wind_h, P.wind_h);
+        v_out[c] = clamp_value((float)((double)vc + (double)dv * P.dt_small), 0.0f, -P.wind_h, P.wind_h);
+        w_out[c] = clamp_value((float)((double)wc + (double)dw * P.dt_small), 0.0f, -P.wind_v, P.wind_v);
+    }
+    else
+    {
+        const float2 dp0 = dp0_split[k];
+        if (interior)
         {
-            u_out[c] = clamp_value((float)((double)u[c] + (double)du * P.dt_small), 0.0f, -P.wind_h, P.wind_h);
-            v_out[c] = clamp_value((float)((double)v[c] + (double)dv * P.dt_small), 0.0f, -P.wind_h, P.wind_h);
-            w_out[c] = clamp_value((float)((double)w[c] + (double)dw * P.dt_small), 0.0f, -P.wind_v, P.wind_v);
+            const float rho_x = 0.5f * (rc + rx);
+            const float rho_y = 0.5f * (rc + ry);
+            const float rho_z = 0.5f * (rc + rz);
+            const float dpz = ((pz - pc) - dp0.x) - dp0.y;
+            const float sxr = (isfinite(rho_x) && rho_x > 1.0e-6f) ? rho_x : 1.0f;
+            const float syr = (isfinite(rho_y) && rho_y > 1.0e-6f) ? rho_y : 1.0f;
+            const float szr = (isfinite(rho_z) && rho_z > 1.0e-6f) ? rho_z : 1.0f;
+            const float a = __fdividef(-(px - pc) * P.inv_dx_f, sxr);
+            const float b = __fdividef(-(py - pc) * P.inv_dy_f, syr);
+            const float cz = __fdividef(-dpz * P.inv_dz_f, szr);
+            du = isfinite(a) ? a : 0.0f;
+            dv = isfinite(b) ? b : 0.0f;
+            dw = isfinite(cz) ? cz : 0.0f;
         }
-        else
-        {
-            const float dt = P.dt_f;
-            u_out[c] = clamp_value(__fmaf_rn(du, dt, u[c]), 0.0f, -P.wind_h, P.wind_h);
-            v_out[c] = clamp_value(__fmaf_rn(dv, dt, v[c]), 0.0f, -P.wind_h, P.wind_h);
-            w_out[c] = clamp_value(__fmaf_rn(dw, dt, w[c]), 0.0f, -P.wind_v, P.wind_v);
-        }
+        const float dt = P.dt_f;
+        u_out[c] = clamp_value(__fmaf_rn(du, dt, uc), 0.0f, -P.wind_h, P.wind_h);
+        v_out[c] = clamp_value(__fmaf_rn(dv, dt, vc), 0.0f, -P.wind_h, P.wind_h);
+        w_out[c] = clamp_value(__fmaf_rn(dw, dt, wc), 0.0f, -P.wind_v, P.wind_v);
     }
 }
 

@@ -188,7 +188,7 @@ static __global__ void __launch_bounds__(256) engine_seed_kernel(const EngineMem
 // ---- Acoustic substep (split form, u/v/w in place, rho ping-pong) ---------
 
 template <class Policy>
-static __global__ void __launch_bounds__(256, 6) engine_continuity_kernel(const EngineMember* __restrict__ table,
+static __global__ void __launch_bounds__(256, 5) engine_continuity_kernel(const EngineMember* __restrict__ table,
                                                                 const long long* __restrict__ prefix,
                                                                 long long tiles, int s)
 {

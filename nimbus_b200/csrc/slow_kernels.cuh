@@ -62,21 +62,21 @@ __device__ __forceinline__ real upwind_deriv(const float* __restrict__ f, int c,
     const real cc = (real)f[c];
     if (half <= 0) return (real)0;
     const bool pos = a >= (real)0;
-    const int s = pos ? stride : -stride;
-    const real x1 = (real)f[c - s], y1 = (real)f[c + s];
+    // Both sides are loaded before the wind sign is known, so no load waits
+    // on the velocity arithmetic; the sign then only selects registers.
+    const real m1 = (real)f[c - stride], p1 = (real)f[c + stride];
     if (half == 1)
     {
-        const real v = (cc - x1) * inv_d;
+        const real v = (cc - (pos ? m1 : p1)) * inv_d;
         return pos ? v : -v;
     }
+    const real m2 = (real)f[c - 2 * stride], p2 = (real)f[c + 2 * stride];
     if (half == 2)
-    {
-        const real m1 = (real)f[c - stride], p1 = (real)f[c + stride];
-        const real m2 = (real)f[c - 2 * stride], p2 = (real)f[c + 2 * stride];
         return pos ? ((real)2 * p1 + (real)3 * cc - (real)6 * m1 + m2) * (inv_d / (real)6)
                    : (-p2 + (real)6 * p1 - (real)3 * cc - (real)2 * m1) * (inv_d / (real)6);
-    }
-    const real x2 = (real)f[c - 2 * s], y2 = (real)f[c + 2 * s], x3 = (real)f[c - 3 * s];
+    const real m3 = (real)f[c - 3 * stride], p3 = (real)f[c + 3 * stride];
+    const real x1 = pos ? m1 : p1, x2 = pos ? m2 : p2, x3 = pos ? m3 : p3;
+    const real y1 = pos ? p1 : m1, y2 = pos ? p2 : m2;
     const real v = ((real)-2 * x3 + (real)15 * x2 - (real)60 * x1 + (real)20 * cc + (real)30 * y1 - (real)3 * y2) *
                    (inv_d / (real)60);
     return pos ? v : -v;

@@ -355,14 +355,15 @@ __device__ __forceinline__ void transport_update_cell(const TransportParams& T, 
     const real idy = kFp32 ? (real)T.inv_dy_f : (real)T.inv_dy;
     const real idz = kFp32 ? (real)T.inv_dz_f : (real)T.inv_dz;
     const real dt = kFp32 ? (real)T.dt_f : (real)T.dt;
-    auto limited = [&](float raw, bool pd, const float* __restrict__ r, int lo, int hi) -> real {
-        if constexpr (kFp32)
-        {
-            if (!pd || raw == 0.0f) return raw;
-            return raw * (raw > 0.0f ? r[lo] : r[hi]);
-        }
-        else return limited_flux(raw, pd, r, lo, hi);
+    // The donor-side factor of a face (limited_flux): both candidates are
+    // loaded up front, so no load waits on the sign of a flux.
+    auto limited = [&](float raw, bool pd, float r_lo, float r_hi) -> real {
+        if (!pd || raw == 0.0f) return (real)raw;
+        const float r = raw > 0.0f ? r_lo : r_hi;
+        if constexpr (kFp32) return raw * r;
+        else return (double)raw * (double)r;
     };
+    const int czp = k < d.nz - 1 ? c + 1 : c, czm = k >= 1 ? c - 1 : c;
     for (int s = 0; s < scalars; ++s)
     {
         const bool pd = T.positive_definite[s] != 0;
@@ -370,13 +371,21 @@ __device__ __forceinline__ void transport_update_cell(const TransportParams& T, 
         const float* __restrict__ sfy = sfx + n;
         const float* __restrict__ sfz = sfy + n;
         const float* __restrict__ r = rl + (size_t)s * n;
-        const real sxp = limited(sfx[c], pd, r, c, cxp);
-        const real sxm = limited(sfx[cxm], pd, r, cxm, c);
-        const real syp = limited(sfy[c], pd, r, c, cyp);
-        const real sym = limited(sfy[cym], pd, r, cym, c);
-        const real szp = has_top ? limited(sfz[c], pd, r, c, k < d.nz - 1 ? c + 1 : c) : (real)0;
-        const real szm = (k >= 1) ? limited(sfz[c - 1], pd, r, c - 1, c) : (real)0;
-        const real qc = (real)q_of(s)[c];
+        const float fxp = sfx[c], fxm = sfx[cxm], fyp = sfy[c], fym = sfy[cym];
+        const float fzp = sfz[c], fzm = sfz[czm];
+        const float qraw = q_of(s)[c];
+        float rc = 1.0f, rxp = 1.0f, rxm = 1.0f, ryp = 1.0f, rym = 1.0f, rzp = 1.0f, rzm = 1.0f;
+        if (pd)
+        {
+            rc = r[c]; rxp = r[cxp]; rxm = r[cxm]; ryp = r[cyp]; rym = r[cym]; rzp = r[czp]; rzm = r[czm];
+        }
+        const real sxp = limited(fxp, pd, rc, rxp);
+        const real sxm = limited(fxm, pd, rxm, rc);
+        const real syp = limited(fyp, pd, rc, ryp);
+        const real sym = limited(fym, pd, rym, rc);
+        const real szp = has_top ? limited(fzp, pd, rc, rzp) : (real)0;
+        const real szm = (k >= 1) ? limited(fzm, pd, rzm, rc) : (real)0;
+        const real qc = (real)qraw;
         real rho_phi;
         if (pd)
         {
