@@ -365,7 +365,11 @@ def run_ours(args):
     sub_bytes = sum(c.cells * n for c, n in zip(cases, subs)) * SUBSTEP_BYTES * args.steps
     achieved = sub_bytes / (sub_ms / 1e3) / 1e9 if sub_ms else None
     peak, peak_kind = load_peaks()
-    traffic = load_traffic().get(args.workload, {})
+    # Measured DRAM bytes per cell-substep of the continuity + momentum pair
+    # (ncu, profiles/), scaled to this workload's average substep.
+    per_cell = load_traffic().get(args.workload, {}).get("acoustic_substep_dram_bytes_per_cell")
+    cells_per_substep = sum(c.cells * n for c, n in zip(cases, subs)) / max(subs)
+    traffic = per_cell * cells_per_substep if per_cell else None
     step_gbs = bytes_per_step * args.steps / (ms / 1e3) / 1e9
 
     # ---- the other precision, same runs ----
@@ -474,7 +478,8 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "kernel": "acoustic substep (continuity+EOS and momentum kernels)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak if achieved else None, "peak_kind": peak_kind,
-                         "traffic": traffic.get("acoustic_substep_bytes_per_launch"),
+                         "traffic": traffic, "traffic_unit": "DRAM bytes per substep (both kernels, all members)",
+                         "algorithmic_bytes_per_substep": SUBSTEP_BYTES * cells_per_substep,
                          "algorithmic_bytes_per_cell_substep": SUBSTEP_BYTES,
                          "launches": sub_launches, "substep_ms_total": sub_ms,
                          "whole_step_frac": step_gbs / peak, "kernel_shares": shares},
