@@ -3,10 +3,11 @@
     python -m nimbus_b200.build
 
 Produces nimbus_b200/lib/libnimbus_cuda.so from nimbus_b200/csrc with
-`nvcc -gencode arch=compute_100a,code=sm_100a`.  The reference-precision
-kernels are compiled with --fmad=false: the CPU solver they match performs
-every multiply and add separately, and a contracted FMA would change the
-rounding of stored values.
+`nvcc -gencode arch=compute_100a,code=sm_100a`, one object per translation
+unit.  The reference-precision units are compiled with --fmad=false: the CPU
+solver they match performs every multiply and add separately, and a
+contracted FMA would change the rounding of stored values.  The FP32 form's
+unit (fp32_*.cu) is compiled with --fmad=true.
 """
 from __future__ import annotations
 
@@ -39,12 +40,25 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     newest = max(p.stat().st_mtime for p in sources())
     if out.exists() and not force and out.stat().st_mtime >= newest:
         return out
-    cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-           "--threads", "2", *[str(p) for p in sorted(CSRC.glob("*.cu"))], "-o", str(out)]
+    obj_dir = LIB / "obj"
+    obj_dir.mkdir(exist_ok=True)
+    common = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]
     if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
+        common.append("-Xptxas=-v")
+    jobs, objs = [], []
+    for src in sorted(CSRC.glob("*.cu")):
+        obj = obj_dir / (src.stem + ".o")
+        # The FP32 form's unit contracts multiply-adds; every other unit keeps
+        # the reference's uncontracted arithmetic.
+        fmad = "--fmad=true" if src.name.startswith("fp32_") else "--fmad=false"
+        cmd = [*common, fmad, "-c", str(src), "-o", str(obj)]
+        if verbose:
+            print(" ".join(cmd))
+        jobs.append(subprocess.Popen(cmd))
+        objs.append(obj)
+    if any(j.wait() != 0 for j in jobs):
+        raise subprocess.CalledProcessError(1, "nvcc")
+    subprocess.run([nvcc(), *ARCH, "-shared", *[str(o) for o in objs], "-o", str(out)], check=True)
     return out
 
 

@@ -6,6 +6,7 @@
 // enqueue; nimbus_cuda_synchronize() reports their status word.
 #include "../../include/nimbus_cuda.h"
 #include "context.cuh"
+#include "launch.cuh"
 
 #include "acoustic_fused.cuh"
 #include "acoustic_kernels.cuh"
@@ -102,80 +103,6 @@ nimbus_status ensure_alts(nimbus_cuda_context* ctx, size_t n, AcousticDevice& D)
     return NIMBUS_OK;
 }
 
-// Fused one-launch substep: reads (u,v,w,rho)[cur], writes (u,v,w,rho)[alt],
-// p in place, mass fluxes in place.
-constexpr int kFusedTJ = 8;
-constexpr int kFusedBlock = 256;
-
-struct Prognostic
-{
-    float *u, *v, *w, *rho;
-};
-
-bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
-
-template <class Policy>
-nimbus_status launch_fused_impl(nimbus_cuda_context* ctx, cudaStream_t st, FusedParams F, const Prognostic& in,
-                                const Prognostic& out, float* p, const float* theta, const double* rho0,
-                                const double* p0, const float2* dp0, const float4* eos0, float* drho, float* mfx,
-                                float* mfy, float* mfz)
-{
-    const size_t smem = FusedSmem<kFusedTJ>::floats(F.d.nz) * sizeof(float);
-    auto kernel = acoustic_substep_fused_kernel<kFusedTJ, kFusedBlock, Policy>;
-    if (smem > 220 * 1024) return fail(ctx, NIMBUS_ERR_UNSUPPORTED, "nz too large for the fused substep's shared window");
-    static int occupancy_cache[2][512] = {};
-    const int pol = Policy::exact_pow ? 0 : 1;
-    int& occ = occupancy_cache[pol][F.d.nz < 512 ? F.d.nz : 511];
-    if (occ == 0)
-    {
-        NB_CUDA(ctx, cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
-        int blocks = 0;
-        NB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, kFusedBlock, smem));
-        occ = blocks > 0 ? blocks : 1;
-    }
-    // Chunk the i-march so the grid is about one full wave of resident CTAs
-    // (each chunk recomputes one plane, so longer chunks waste less).
-    const int strips = (F.d.ny + kFusedTJ - 1) / kFusedTJ;
-    const int resident = ctx->sm_count * occ;
-    int chunks = resident / strips;
-    if (chunks < 1) chunks = 1;
-    if (chunks > F.d.nx) chunks = F.d.nx;
-    F.chunk = (F.d.nx + chunks - 1) / chunks;
-    chunks = (F.d.nx + F.chunk - 1) / F.chunk;
-    F.nz_magic = fused_nz_magic(static_cast<unsigned>(F.d.nz));
-    F.vec4 = (F.d.nz % 4 == 0) && aligned16(in.rho) && aligned16(in.u) && aligned16(in.v) && aligned16(in.w) &&
-             aligned16(theta);
-    LaunchTimer t(ctx, st, NIMBUS_KERNEL_ACOUSTIC_SUBSTEP);
-    kernel<<<strips * chunks, kFusedBlock, smem, st>>>(F, in.rho, in.u, in.v, in.w, theta, rho0, p0, dp0, eos0, drho,
-                                                       out.rho, p, out.u, out.v, out.w, mfx, mfy, mfz, ctx->status);
-    ctx->launches += 1;
-    return NIMBUS_OK;
-}
-
-template <class Policy>
-nimbus_status launch_split_impl(nimbus_cuda_context* ctx, cudaStream_t st, FusedParams F, const Prognostic& in,
-                                const Prognostic& out, float* p, const float* theta, const double* rho0,
-                                const double* p0, const float2* dp0, const float4* eos0, float* drho, float* mfx,
-                                float* mfy, float* mfz)
-{
-    const long long n = F.d.cells();
-    long long blocks = (n + kThreads - 1) / kThreads;
-    const long long cap = static_cast<long long>(ctx->sm_count) * 32;
-    if (blocks > cap) blocks = cap;
-    {
-        LaunchTimer t(ctx, st, NIMBUS_KERNEL_ACOUSTIC_SUBSTEP);
-        split_continuity_eos_kernel<Policy><<<static_cast<int>(blocks), kThreads, 0, st>>>(
-            F, in.rho, in.u, in.v, in.w, theta, rho0, eos0, out.rho, p, drho, mfx, mfy, mfz, ctx->status);
-    }
-    {
-        LaunchTimer t(ctx, st, NIMBUS_KERNEL_ACOUSTIC_MOMENTUM);
-        split_momentum_kernel<Policy><<<static_cast<int>(blocks), kThreads, 0, st>>>(F, out.rho, p, p0, dp0, in.u,
-                                                                                      in.v, in.w, out.u, out.v, out.w);
-    }
-    ctx->launches += 2;
-    return NIMBUS_OK;
-}
-
 int resolve_form(const nimbus_cuda_context* ctx, const Dims& d)
 {
     if (ctx->substep_form != NIMBUS_SUBSTEP_AUTO) return ctx->substep_form;
@@ -191,10 +118,10 @@ nimbus_status launch_fused(nimbus_cuda_context* ctx, cudaStream_t st, const Fuse
     const bool fp32 = ctx->precision == NIMBUS_PRECISION_FP32;
     if (resolve_form(ctx, F.d) == NIMBUS_SUBSTEP_SPLIT)
     {
-        if (fp32) return launch_split_impl<Fp32Policy>(ctx, st, F, in, out, p, theta, rho0, p0, dp0, eos0, drho, mfx, mfy, mfz);
+        if (fp32) return nimbus_fp32::launch_split(ctx, st, F, in, out, p, theta, rho0, p0, dp0, eos0, drho, mfx, mfy, mfz);
         return launch_split_impl<RefPolicy>(ctx, st, F, in, out, p, theta, rho0, p0, dp0, eos0, drho, mfx, mfy, mfz);
     }
-    if (fp32) return launch_fused_impl<Fp32Policy>(ctx, st, F, in, out, p, theta, rho0, p0, dp0, eos0, drho, mfx, mfy, mfz);
+    if (fp32) return nimbus_fp32::launch_fused(ctx, st, F, in, out, p, theta, rho0, p0, dp0, eos0, drho, mfx, mfy, mfz);
     return launch_fused_impl<RefPolicy>(ctx, st, F, in, out, p, theta, rho0, p0, dp0, eos0, drho, mfx, mfy, mfz);
 }
 
@@ -422,28 +349,9 @@ nimbus_status run_transport_device(nimbus_cuda_context* ctx, cudaStream_t st, co
     float* rl = nullptr;
     NB_TRY(ensure(ctx, kSf, 3 * n * T.n_scalars, &sf));
     NB_TRY(ensure(ctx, kRl, n * T.n_scalars, &rl));
-    const dim3 grid(grid_for(ctx, T.d.cells()));
-    {
-        LaunchTimer t(ctx, st, NIMBUS_KERNEL_TRANSPORT_FACES);
-        if (ctx->precision == NIMBUS_PRECISION_FP32)
-            transport_faces_kernel<true><<<grid, kThreads, 0, st>>>(T, mfx, mfy, mfz, sf);
-        else
-            transport_faces_kernel<false><<<grid, kThreads, 0, st>>>(T, mfx, mfy, mfz, sf);
-    }
-    const bool fp32 = ctx->precision == NIMBUS_PRECISION_FP32;
-    {
-        LaunchTimer t(ctx, st, NIMBUS_KERNEL_TRANSPORT_LIMITER);
-        if (fp32) transport_limiter_kernel<true><<<grid, kThreads, 0, st>>>(T, rho_begin, sf, rl);
-        else transport_limiter_kernel<false><<<grid, kThreads, 0, st>>>(T, rho_begin, sf, rl);
-    }
-    {
-        LaunchTimer t(ctx, st, NIMBUS_KERNEL_TRANSPORT_UPDATE);
-        if (fp32) transport_update_kernel<true><<<grid, kThreads, 0, st>>>(T, rho_end, rho_begin, sf, rl, ctx->status);
-        else transport_update_kernel<false><<<grid, kThreads, 0, st>>>(T, rho_end, rho_begin, sf, rl, ctx->status);
-    }
-    ctx->launches += 3;
-    NB_CUDA(ctx, cudaGetLastError());
-    return NIMBUS_OK;
+    if (ctx->precision == NIMBUS_PRECISION_FP32)
+        return nimbus_fp32::launch_transport(ctx, st, T, rho_end, rho_begin, mfx, mfy, mfz, sf, rl);
+    return launch_transport_impl<false>(ctx, st, T, rho_end, rho_begin, mfx, mfy, mfz, sf, rl);
 }
 
 const char* check_slow(const nimbus_slow_args* a, bool step)
@@ -482,44 +390,6 @@ SlowParams slow_params(const nimbus_slow_args* a)
     return S;
 }
 
-struct SlowDevice
-{
-    float *u, *v, *w, *p;
-    const float *rho, *qv, *qc, *qr;
-    const double *rho0, *qv0, *u0, *v0;
-    float *du, *dv, *dw, *dp;
-};
-
-template <class Policy>
-nimbus_status run_slow_device(nimbus_cuda_context* ctx, cudaStream_t st, const SlowParams& S, const SlowDevice& D,
-                              bool step)
-{
-    const size_t n = static_cast<size_t>(S.d.cells());
-    const int blocks = grid_for(ctx, static_cast<long long>(n));
-    LaunchTimer t(ctx, st, NIMBUS_KERNEL_SLOW);
-    if (!step)
-    {
-        slow_predict_kernel<Policy><<<blocks, kThreads, 0, st>>>(S, D.u, D.v, D.w, D.rho, D.p, D.qv, D.qc, D.qr, D.rho0,
-                                                                 D.qv0, D.u0, D.v0, D.du, D.dv, D.dw, D.dp, nullptr,
-                                                                 nullptr, nullptr, nullptr);
-        ctx->launches += 1;
-        NB_CUDA(ctx, cudaGetLastError());
-        return NIMBUS_OK;
-    }
-    float *k1 = nullptr, *xs = nullptr;
-    NB_TRY(ensure(ctx, kSlowK1, 4 * n, &k1));
-    NB_TRY(ensure(ctx, kSlowStar, 4 * n, &xs));
-    slow_predict_kernel<Policy><<<blocks, kThreads, 0, st>>>(S, D.u, D.v, D.w, D.rho, D.p, D.qv, D.qc, D.qr, D.rho0,
-                                                             D.qv0, D.u0, D.v0, k1, k1 + n, k1 + 2 * n, k1 + 3 * n, xs,
-                                                             xs + n, xs + 2 * n, xs + 3 * n);
-    slow_correct_kernel<Policy><<<blocks, kThreads, 0, st>>>(S, xs, xs + n, xs + 2 * n, D.rho, xs + 3 * n, D.qv, D.qc,
-                                                             D.qr, D.rho0, D.qv0, D.u0, D.v0, k1, k1 + n, k1 + 2 * n,
-                                                             k1 + 3 * n, D.u, D.v, D.w, D.p, D.du, D.dv, D.dw, D.dp);
-    ctx->launches += 2;
-    NB_CUDA(ctx, cudaGetLastError());
-    return NIMBUS_OK;
-}
-
 nimbus_status slow_entry(nimbus_cuda_context* ctx, const nimbus_slow_args* a, bool step)
 {
     if (!ctx || !a) return NIMBUS_ERR_INVALID_ARGUMENT;
@@ -535,7 +405,7 @@ nimbus_status slow_entry(nimbus_cuda_context* ctx, const nimbus_slow_args* a, bo
         if (a->stream) st = static_cast<cudaStream_t>(a->stream);
         SlowDevice D{a->u, a->v, a->w, a->p, a->rho, a->qv, a->qc, a->qr, a->rho0_base, a->qv0_base, a->u0_base,
                      a->v0_base, a->du_dt, a->dv_dt, a->dw_dt, a->dp_dt};
-        return fp32 ? run_slow_device<Fp32Policy>(ctx, st, S, D, step) : run_slow_device<RefPolicy>(ctx, st, S, D, step);
+        return fp32 ? nimbus_fp32::run_slow(ctx, st, S, D, step) : run_slow_device<RefPolicy>(ctx, st, S, D, step);
     }
     const size_t n = static_cast<size_t>(a->nx) * a->ny * a->nz;
     const size_t bytes = n * sizeof(float);
@@ -582,7 +452,7 @@ nimbus_status slow_entry(nimbus_cuda_context* ctx, const nimbus_slow_args* a, bo
     if (want_out) NB_TRY(ensure(ctx, kSlowOut, 4 * n, &out));
     SlowDevice D{u, v, w, p, rho, qv, qc, qr, rho0, qv0, u0, v0, out, out ? out + n : nullptr,
                  out ? out + 2 * n : nullptr, out ? out + 3 * n : nullptr};
-    NB_TRY(fp32 ? run_slow_device<Fp32Policy>(ctx, st, S, D, step) : run_slow_device<RefPolicy>(ctx, st, S, D, step));
+    NB_TRY(fp32 ? nimbus_fp32::run_slow(ctx, st, S, D, step) : run_slow_device<RefPolicy>(ctx, st, S, D, step));
     NB_CUDA(ctx, cudaStreamSynchronize(st));
     if (step)
     {

@@ -31,6 +31,10 @@ struct SlowParams
     // FP32 form: the scalars above rounded once.
     float inv_dx_f, inv_dy_f, inv_dz_f, half_inv_dx_f, half_inv_dy_f, half_inv_dz_f, dt_f, coriolis_f_f, frame_u_f,
         frame_v_f, gravity_f;
+    // fd3 / fd5 stencil scales inv_d / 6 and inv_d / 60 per axis (x, y, z),
+    // formed once on the host exactly as the derivative operators form them.
+    double d6[3], d60[3];
+    float d6_f[3], d60_f[3];
 };
 
 __host__ __device__ inline void finish_fp32(SlowParams& S)
@@ -46,6 +50,15 @@ __host__ __device__ inline void finish_fp32(SlowParams& S)
     S.frame_u_f = (float)S.frame_u;
     S.frame_v_f = (float)S.frame_v;
     S.gravity_f = (float)S.gravity;
+    const double inv[3] = {S.inv_dx, S.inv_dy, S.inv_dz};
+    const float inv_f[3] = {S.inv_dx_f, S.inv_dy_f, S.inv_dz_f};
+    for (int a = 0; a < 3; ++a)
+    {
+        S.d6[a] = inv[a] / 6.0;
+        S.d60[a] = inv[a] / 60.0;
+        S.d6_f[a] = inv_f[a] / 6.0f;
+        S.d60_f[a] = inv_f[a] / 60.0f;
+    }
 }
 
 // upwind_dx/dy/dz (derivative_operators.hpp:324-395): fd5 upwind-biased in
@@ -56,7 +69,7 @@ __host__ __device__ inline void finish_fp32(SlowParams& S)
 // result is bit-identical), and lanes with opposite winds do not diverge.
 template <class real>
 __device__ __forceinline__ real upwind_deriv(const float* __restrict__ f, int c, int stride, int idx, int n, real a,
-                                             real inv_d)
+                                             real inv_d, real inv_d6, real inv_d60)
 {
     const int half = min(idx, n - 1 - idx);
     const real cc = (real)f[c];
@@ -72,13 +85,13 @@ __device__ __forceinline__ real upwind_deriv(const float* __restrict__ f, int c,
     }
     const real m2 = (real)f[c - 2 * stride], p2 = (real)f[c + 2 * stride];
     if (half == 2)
-        return pos ? ((real)2 * p1 + (real)3 * cc - (real)6 * m1 + m2) * (inv_d / (real)6)
-                   : (-p2 + (real)6 * p1 - (real)3 * cc - (real)2 * m1) * (inv_d / (real)6);
+        return pos ? ((real)2 * p1 + (real)3 * cc - (real)6 * m1 + m2) * inv_d6
+                   : (-p2 + (real)6 * p1 - (real)3 * cc - (real)2 * m1) * inv_d6;
     const real m3 = (real)f[c - 3 * stride], p3 = (real)f[c + 3 * stride];
     const real x1 = pos ? m1 : p1, x2 = pos ? m2 : p2, x3 = pos ? m3 : p3;
     const real y1 = pos ? p1 : m1, y2 = pos ? p2 : m2;
     const real v = ((real)-2 * x3 + (real)15 * x2 - (real)60 * x1 + (real)20 * cc + (real)30 * y1 - (real)3 * y2) *
-                   (inv_d / (real)60);
+                   inv_d60;
     return pos ? v : -v;
 }
 
@@ -103,16 +116,20 @@ __device__ __forceinline__ void slow_tendencies_at(const SlowParams& S, int c, i
     if (!(i >= 1 && i < d.nx - 1 && j >= 1 && j < d.ny - 1 && k < d.nz - 1)) return;
     const int sx = d.sx(), sy = d.sy();
     const real q = (real)0.25, h = (real)0.5;
-    real inv_dx, inv_dy, inv_dz, fu, fv, cf;
+    real inv_dx, inv_dy, inv_dz, fu, fv, cf, x6, y6, z6, x60, y60, z60;
     if constexpr (f32)
     {
         inv_dx = S.inv_dx_f; inv_dy = S.inv_dy_f; inv_dz = S.inv_dz_f;
         fu = S.frame_u_f; fv = S.frame_v_f; cf = S.coriolis_f_f;
+        x6 = S.d6_f[0]; y6 = S.d6_f[1]; z6 = S.d6_f[2];
+        x60 = S.d60_f[0]; y60 = S.d60_f[1]; z60 = S.d60_f[2];
     }
     else
     {
         inv_dx = S.inv_dx; inv_dy = S.inv_dy; inv_dz = S.inv_dz;
         fu = S.frame_u; fv = S.frame_v; cf = S.coriolis_f;
+        x6 = S.d6[0]; y6 = S.d6[1]; z6 = S.d6[2];
+        x60 = S.d60[0]; y60 = S.d60[1]; z60 = S.d60[2];
     }
     auto store = [](real t) -> float {
         if constexpr (f32) return isfinite(t) ? t : 0.0f;
@@ -125,10 +142,10 @@ __device__ __forceinline__ void slow_tendencies_at(const SlowParams& S, int c, i
         const real tux = ux - fu, tuy = uy - fv;
         const real wx = (k == 0) ? q * ((real)w[c] + (real)w[c + sx])
                                  : q * ((real)w[c - 1] + (real)w[c] + (real)w[c + sx - 1] + (real)w[c + sx]);
-        const real ddx = upwind_deriv<real>(u, c, sx, i, d.nx, tux, inv_dx);
-        const real ddy = upwind_deriv<real>(u, c, sy, j, d.ny, tuy, inv_dy);
+        const real ddx = upwind_deriv<real>(u, c, sx, i, d.nx, tux, inv_dx, x6, x60);
+        const real ddy = upwind_deriv<real>(u, c, sy, j, d.ny, tuy, inv_dy, y6, y60);
         const real ddz = (k == 0) ? ((wx >= (real)0) ? (real)0 : ((real)u[c + 1] - (real)u[c]) * inv_dz)
-                                  : upwind_deriv<real>(u, c, 1, k, d.nz, wx, inv_dz);
+                                  : upwind_deriv<real>(u, c, 1, k, d.nz, wx, inv_dz, z6, z60);
         const real v0k = v0 ? (real)v0[k] : (real)0;
         const real du = -tux * ddx - tuy * ddy - wx * ddz + cf * (uy - v0k);
         out_u = store(du);
@@ -140,10 +157,10 @@ __device__ __forceinline__ void slow_tendencies_at(const SlowParams& S, int c, i
         const real tvy = vy - fv, tux = ux - fu;
         const real wy = (k == 0) ? q * ((real)w[c] + (real)w[c + sy])
                                  : q * ((real)w[c - 1] + (real)w[c] + (real)w[c + sy - 1] + (real)w[c + sy]);
-        const real ddx = upwind_deriv<real>(v, c, sx, i, d.nx, tux, inv_dx);
-        const real ddy = upwind_deriv<real>(v, c, sy, j, d.ny, tvy, inv_dy);
+        const real ddx = upwind_deriv<real>(v, c, sx, i, d.nx, tux, inv_dx, x6, x60);
+        const real ddy = upwind_deriv<real>(v, c, sy, j, d.ny, tvy, inv_dy, y6, y60);
         const real ddz = (k == 0) ? ((wy >= (real)0) ? (real)0 : ((real)v[c + 1] - (real)v[c]) * inv_dz)
-                                  : upwind_deriv<real>(v, c, 1, k, d.nz, wy, inv_dz);
+                                  : upwind_deriv<real>(v, c, 1, k, d.nz, wy, inv_dz, z6, z60);
         const real u0k = u0 ? (real)u0[k] : (real)0;
         const real dv = -tux * ddx - tvy * ddy - wy * ddz - cf * (ux - u0k);
         out_v = store(dv);
@@ -154,10 +171,10 @@ __device__ __forceinline__ void slow_tendencies_at(const SlowParams& S, int c, i
         const real ux = q * ((real)u[c - sx] + (real)u[c] + (real)u[c - sx + 1] + (real)u[c + 1]);
         const real uy = q * ((real)v[c - sy] + (real)v[c] + (real)v[c - sy + 1] + (real)v[c + 1]);
         const real tux = ux - fu, tuy = uy - fv;
-        const real ddx = upwind_deriv<real>(w, c, sx, i, d.nx, tux, inv_dx);
-        const real ddy = upwind_deriv<real>(w, c, sy, j, d.ny, tuy, inv_dy);
+        const real ddx = upwind_deriv<real>(w, c, sx, i, d.nx, tux, inv_dx, x6, x60);
+        const real ddy = upwind_deriv<real>(w, c, sy, j, d.ny, tuy, inv_dy, y6, y60);
         const real ddz = (k == 0) ? ((wz >= (real)0) ? ((real)w[c] - (real)0) * inv_dz : ((real)w[c + 1] - (real)w[c]) * inv_dz)
-                                  : upwind_deriv<real>(w, c, 1, k, d.nz, wz, inv_dz);
+                                  : upwind_deriv<real>(w, c, 1, k, d.nz, wz, inv_dz, z6, z60);
         real forcing;
         if constexpr (f32)
         {
