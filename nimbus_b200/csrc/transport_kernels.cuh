@@ -85,47 +85,23 @@ __device__ __forceinline__ double mc_slope(double qm, double q0, double qp)
     return 0.0;
 }
 
-// Face value for face l+1/2 on an axis of extent n, cells at q[base + m*stride].
-// The upwind side is chosen by selecting the stencil, not by branching: with
-// s = +1 (mflux >= 0) or -1 and the donor cell l + (s < 0), the reference's
-// two calls weno5_face(q[l-2], q[l-1], q[l], q[l+1], q[l+2]) and
-// weno5_face(q[l+3], q[l+2], q[l+1], q[l], q[l-1]) are the one call on
-// q[donor - 2s .. donor + 2s], so lanes with opposite fluxes do not diverge.
-__device__ __forceinline__ double face_value(const float* __restrict__ q, int base, int stride, int l, int n,
-                                             double mflux, int weno)
-{
-#define NQ(m) ((double)q[base + (m) * stride])
-    const bool pos = mflux >= 0.0;
-    const int donor = pos ? l : l + 1;
-    const int s = pos ? 1 : -1;
-    const double q0 = NQ(donor);
-    if (weno && donor - 2 >= 0 && donor + 2 <= n - 1)
-        return weno5_face(NQ(donor - 2 * s), NQ(donor - s), q0, NQ(donor + s), NQ(donor + 2 * s));
-    if (pos)
-    {
-        const double sl = (l >= 1) ? mc_slope(NQ(l - 1), q0, NQ(l + 1)) : 0.0;
-        return q0 + 0.5 * sl;
-    }
-    const double sl = (l + 1 <= n - 2) ? mc_slope(NQ(l), q0, NQ(l + 2)) : 0.0;
-    return q0 - 0.5 * sl;
-#undef NQ
-}
-
-// FP32 face offset from the donor value: weno5_face_offset_fp32
-// (include/numerics/advection/weno5_face.hpp:88-120), the reference's own FP32
-// GPU reconstruction (scale-normalised, so moisture-scale fields keep their
-// nonlinear weights).
+// FP32 face offset from the donor value c (face = c + offset): WENO5-JS on
+// the stencil normalised by its largest magnitude, as the reference's FP32
+// GPU form normalises it (weno5_face_offset_fp32,
+// include/numerics/advection/weno5_face.hpp:88-120: differences from the
+// donor, eps = 1e-6 * relative^2 + (1e-20 / scale)^2, ideal weights 1/10,
+// 6/10, 3/10, p = 2), so moisture-scale fields keep their nonlinear weights.
+// After normalisation every eps + beta_k is at least 1e-6, so the weights
+// d_k / (eps + beta_k)^2 are formed directly from approximate reciprocals
+// instead of the reference's min-normalised ratios: the same weights to FP32
+// rounding in about half the instructions.  A non-finite result falls back to
+// the donor value (offset 0).
 __device__ __forceinline__ float weno5_offset_f32(float a, float b, float c, float d, float e)
 {
     const float magnitude = fmaxf(fmaxf(fmaxf(fabsf(a), fabsf(b)), fmaxf(fabsf(c), fabsf(d))), fabsf(e));
     const float scale = fmaxf(magnitude, 1e-20f);
-    if (!isfinite(scale)) return 0.0f;
-    const float inv = __frcp_rn(scale);
-    auto diff = [&](float value) {
-        const float delta = value - c;
-        return isfinite(delta) ? delta * inv : value * inv - c * inv;
-    };
-    const float ac = diff(a), bc = diff(b), dc = diff(d), ec = diff(e);
+    const float inv = __fdividef(1.0f, scale);
+    const float ac = (a - c) * inv, bc = (b - c) * inv, dc = (d - c) * inv, ec = (e - c) * inv;
     const float p0 = (1.0f / 3.0f) * ac - (7.0f / 6.0f) * bc;
     const float p1 = -(1.0f / 6.0f) * bc + (1.0f / 3.0f) * dc;
     const float p2 = (5.0f / 6.0f) * dc - (1.0f / 6.0f) * ec;
@@ -138,12 +114,10 @@ __device__ __forceinline__ float weno5_offset_f32(float a, float b, float c, flo
     const float relative = magnitude * inv;
     const float flo = 1e-20f * inv;
     const float epsilon = 1e-6f * relative * relative + flo * flo;
-    const float e0 = epsilon + b0, e1 = epsilon + b1, e2 = epsilon + b2;
-    const float minimum = fminf(fminf(e0, e1), e2);
-    const float r0 = __fdividef(minimum, e0), r1 = __fdividef(minimum, e1), r2 = __fdividef(minimum, e2);
+    const float r0 = __fdividef(1.0f, epsilon + b0), r1 = __fdividef(1.0f, epsilon + b1);
+    const float r2 = __fdividef(1.0f, epsilon + b2);
     const float a0 = 0.1f * r0 * r0, a1 = 0.6f * r1 * r1, a2 = 0.3f * r2 * r2;
-    const float sum = a0 + a1 + a2;
-    const float offset = scale * __fdividef(a0 * p0 + a1 * p1 + a2 * p2, sum);
+    const float offset = scale * __fdividef(a0 * p0 + a1 * p1 + a2 * p2, a0 + a1 + a2);
     return isfinite(offset) ? offset : 0.0f;
 }
 
@@ -156,32 +130,84 @@ __device__ __forceinline__ float mc_slope_f32(float qm, float q0, float qp)
     return 0.0f;
 }
 
-// FP32 scalar face flux M*phi as M*base + M*offset (the reference's FP32 GPU
-// form), upwind side selected as in face_value.
-__device__ __forceinline__ float face_flux_f32(const float* __restrict__ q, int base, int stride, int l, int n,
-                                               float mflux, int weno)
+// The stencil of one face, shared by every scalar (the upwind side follows
+// the mass flux, which all scalars share): the five cell offsets of the WENO5
+// stencil (donor - 2s .. donor + 2s), or for the MC fallback near a wall the
+// donor (o[2]) and its two neighbours in the reference's argument order.
+struct FaceStencil
 {
-#define NQ(m) (q[base + (m) * stride])
-    const bool pos = mflux >= 0.0f;
-    const int donor = pos ? l : l + 1;
-    const int s = pos ? 1 : -1;
-    const float q0 = NQ(donor);
-    float offset;
-    if (weno && donor - 2 >= 0 && donor + 2 <= n - 1)
-        offset = weno5_offset_f32(NQ(donor - 2 * s), NQ(donor - s), q0, NQ(donor + s), NQ(donor + 2 * s));
-    else if (pos)
-        offset = 0.5f * ((l >= 1) ? mc_slope_f32(NQ(l - 1), q0, NQ(l + 1)) : 0.0f);
+    int o[5];
+    bool pos;    // mflux >= 0
+    bool weno;   // the 5-point stencil fits
+    bool slope;  // MC: the slope's neighbours exist
+};
+
+__device__ __forceinline__ FaceStencil face_stencil(int base, int stride, int l, int n, bool mflux_pos, int weno)
+{
+    FaceStencil f;
+    f.pos = mflux_pos;
+    const int donor = f.pos ? l : l + 1;
+    const int s = f.pos ? stride : -stride;
+    f.weno = weno && donor - 2 >= 0 && donor + 2 <= n - 1;
+    const int cd = base + donor * stride;
+    if (f.weno)
+    {
+        f.o[0] = cd - 2 * s; f.o[1] = cd - s; f.o[2] = cd; f.o[3] = cd + s; f.o[4] = cd + 2 * s;
+        f.slope = false;
+    }
     else
-        offset = -0.5f * ((l + 1 <= n - 2) ? mc_slope_f32(NQ(l), q0, NQ(l + 2)) : 0.0f);
-    return __fmaf_rn(mflux, q0, mflux * offset);
-#undef NQ
+    {
+        // advection_cartesian.cpp:1971-2008: positive side
+        // mc(q[l-1], q[l], q[l+1]) when l >= 1, negative side
+        // mc(q[l], q[l+1], q[l+2]) when l + 1 <= n - 2.
+        f.slope = f.pos ? (l >= 1) : (l + 1 <= n - 2);
+        const int lo = f.pos ? l - 1 : l, hi = f.pos ? l + 1 : l + 2;
+        f.o[0] = f.slope ? base + lo * stride : cd;
+        f.o[1] = f.o[0]; f.o[2] = cd; f.o[3] = f.slope ? base + hi * stride : cd; f.o[4] = f.o[3];
+    }
+    return f;
+}
+
+// The face flux of one scalar on a prepared stencil
+// (advection_cartesian.cpp:1943-2172).  FP32 form: M * donor + M * offset
+// with the normalised WENO5 offset; reference precision: M times the FP64
+// face value (WENO5 where the stencil fits, else donor +- half the MC
+// slope), rounded once to the FP32 scratch.
+template <bool kFp32>
+__device__ __forceinline__ float stencil_flux(const float* __restrict__ q, const FaceStencil& f, float mflux)
+{
+    if constexpr (kFp32)
+    {
+        const float q0 = q[f.o[2]];
+        float offset;
+        if (f.weno) offset = weno5_offset_f32(q[f.o[0]], q[f.o[1]], q0, q[f.o[3]], q[f.o[4]]);
+        else
+        {
+            const float sl = f.slope ? mc_slope_f32(q[f.o[0]], q0, q[f.o[3]]) : 0.0f;
+            offset = (f.pos ? 0.5f : -0.5f) * sl;
+        }
+        return __fmaf_rn(mflux, q0, mflux * offset);
+    }
+    else
+    {
+        const double q0 = (double)q[f.o[2]];
+        double face;
+        if (f.weno)
+            face = weno5_face((double)q[f.o[0]], (double)q[f.o[1]], q0, (double)q[f.o[3]], (double)q[f.o[4]]);
+        else
+        {
+            const double sl = f.slope ? mc_slope((double)q[f.o[0]], q0, (double)q[f.o[3]]) : 0.0;
+            face = f.pos ? q0 + 0.5 * sl : q0 - 0.5 * sl;
+        }
+        return (float)((double)mflux * face);
+    }
 }
 
 // Face fluxes owned by cell c (its +x, +y and +z faces) for every scalar:
-// the cell's index and mass fluxes are loaded once and the scalars follow.
-// kFp32 selects the reference's FP32 GPU form (face_flux_f32), otherwise FP64
-// face values rounded once to the FP32 scratch.  q(s) gives scalar s's field;
-// sf is the [scalars][3][cells] face-flux scratch (x, y, z).
+// the cell's index, mass fluxes and face stencils are formed once and the
+// scalars follow.  kFp32 selects the FP32 form, otherwise FP64 face values
+// rounded once to the FP32 scratch.  q(s) gives scalar s's field; sf is the
+// [scalars][3][cells] face-flux scratch (x, y, z).
 template <bool kFp32, class QIn>
 __device__ __forceinline__ void transport_faces_cell(const TransportParams& T, int scalars, QIn&& q_of,
                                                      const float* __restrict__ mfx, const float* __restrict__ mfy,
@@ -194,26 +220,21 @@ __device__ __forceinline__ void transport_faces_cell(const TransportParams& T, i
     decompose(d, c, i, j, k);
     const bool hx = i <= d.nx - 2, hy = j <= d.ny - 2, hz = k < kz_end, top = k == d.nz - 1;
     const float fx = hx ? mfx[c] : 0.0f, fy = hy ? mfy[c] : 0.0f, fz = hz ? mfz[c] : 0.0f;
-    const int bx = c - i * d.sx(), by = c - j * d.sy(), bz = c - k;
+    const FaceStencil sx = face_stencil(c - i * d.sx(), d.sx(), i, d.nx, fx >= 0.0f, T.weno);
+    const FaceStencil sy = face_stencil(c - j * d.sy(), d.sy(), j, d.ny, fy >= 0.0f, T.weno);
+    const FaceStencil sz = face_stencil(c - k, 1, top ? k - 1 : k, d.nz, fz >= 0.0f, T.weno);
     for (int s = 0; s < scalars; ++s)
     {
         const float* __restrict__ q = q_of(s);
         float* __restrict__ sfx = sf + (size_t)s * 3 * n;
         float* __restrict__ sfy = sfx + n;
         float* __restrict__ sfz = sfy + n;
-        if constexpr (kFp32)
+        if (hx) sfx[c] = stencil_flux<kFp32>(q, sx, fx);
+        if (hy) sfy[c] = stencil_flux<kFp32>(q, sy, fy);
+        if (hz)
         {
-            if (hx) sfx[c] = face_flux_f32(q, bx, d.sx(), i, d.nx, fx, T.weno);
-            if (hy) sfy[c] = face_flux_f32(q, by, d.sy(), j, d.ny, fy, T.weno);
-            if (hz) sfz[c] = top ? fz * q[c] : face_flux_f32(q, bz, 1, k, d.nz, fz, T.weno);
-        }
-        else
-        {
-            if (hx) sfx[c] = (float)((double)fx * face_value(q, bx, d.sx(), i, d.nx, (double)fx, T.weno));
-            if (hy) sfy[c] = (float)((double)fy * face_value(q, by, d.sy(), j, d.ny, (double)fy, T.weno));
-            if (hz)
-                sfz[c] = top ? (float)((double)fz * (double)q[c])
-                             : (float)((double)fz * face_value(q, bz, 1, k, d.nz, (double)fz, T.weno));
+            if (top) sfz[c] = kFp32 ? fz * q[c] : (float)((double)fz * (double)q[c]);
+            else sfz[c] = stencil_flux<kFp32>(q, sz, fz);
         }
     }
 }
