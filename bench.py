@@ -56,7 +56,11 @@ def parse():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--members", type=int, default=64)
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--lanes", type=int, default=4,
+                    help="parallel member groups inside the engine's step graph")
+    ap.add_argument("--e2e-groups", type=int, default=8,
+                    help="engines (each on its own stream) the runs are split over for the end-to-end pass")
     ap.add_argument("--plain-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
@@ -302,7 +306,7 @@ def run_ours(args):
 
     from nimbus_b200 import cuda
     from nimbus_b200.initial import initial_state
-    from nimbus_b200.run import EngineRun, ResidentRun, substeps_for
+    from nimbus_b200.run import EngineRun, HostPipeline, ResidentRun, substeps_for
 
     rank, world, local = dist_env()
     if world > 1:
@@ -329,12 +333,11 @@ def run_ours(args):
     ctx = cuda.Context(device)
     precision = cuda.PRECISION_FP32 if args.precision == "fp32" else cuda.PRECISION_REFERENCE
     other = cuda.PRECISION_REFERENCE if precision == cuda.PRECISION_FP32 else cuda.PRECISION_FP32
-    stream = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{device}")
-
     # ---- batched form: every run resident in one engine, CUDA graph ----
-    run = EngineRun(ctx, precision)
+    run = EngineRun(ctx, precision, lanes=args.lanes)
     for c, (st, base), n in zip(cases, prepared, subs):
         run.admit(c, st, base, n_substeps=n)
+    stream = torch.cuda.ExternalStream(run.engine.stream, device=f"cuda:{device}")
     for _ in range(max(args.warmup, 3)):
         run.step(1)
     ctx.synchronize()
@@ -352,12 +355,17 @@ def run_ours(args):
     value = total_cells * args.steps / (ms / 1e3)
     bytes_per_step = sum(c.cells * step_bytes(n) for c, n in zip(cases, subs))
 
-    # ---- per-kernel device time (eager launches bracketed by events) ----
+    # ---- per-kernel device time (eager launches bracketed by events), one
+    # lane so that no two launches share the GPU ----
+    run.engine.set_lanes(1)
+    run.step(1)
+    ctx.synchronize()
     ctx.set_kernel_timing(True)
     for _ in range(args.steps):
         run.step(1)
     timing = ctx.kernel_timing()
     ctx.set_kernel_timing(False)
+    run.engine.set_lanes(args.lanes)
     total_kernel_ms = sum(v[1] for v in timing.values())
     shares = {k: round(v[1] / total_kernel_ms, 4) for k, v in timing.items()} if total_kernel_ms else {}
     sub_ms = timing["acoustic_substep"][1] + timing["acoustic_momentum"][1]
@@ -382,31 +390,24 @@ def run_ours(args):
     ctx.set_precision(precision)
 
     # ---- end to end through the host-buffer API ----
+    run.close()
     e2e = None
     if args.e2e_steps > 0:
-        host = {}
-        for mid, (c, _) in run.members.items():
-            host[mid] = {k: torch.from_numpy(v).pin_memory().numpy() for k, v in run.read(mid).items()}
-
-        def e2e_step():
-            for mid in run.members:
-                run.engine.write(mid, host[mid])
-            run.step(1)
-            for mid in run.members:
-                run.engine.read_into(mid, host[mid])
-
-        e2e_step()
+        pipe = HostPipeline(ctx, cases, prepared, groups=args.e2e_groups, precision=precision)
+        pipe.step()
         barrier()
         t0 = time.perf_counter()
-        for _ in range(args.e2e_steps):
-            e2e_step()
+        pipe.step(args.e2e_steps)
         el = max_over_ranks(time.perf_counter() - t0)
+        pipe.close()
         io = cells * 4 * 9
         e2e = {"value": total_cells * args.e2e_steps / el, "unit": METRIC, "h2d_bytes_per_step": io * world,
                "d2h_bytes_per_step": io * world, "steps": args.e2e_steps,
-               "api": "nimbus_cuda_engine_write + nimbus_cuda_engine_step + nimbus_cuda_engine_read "
-                      "(pinned host arrays, nine prognostic fields each way per run per step)"}
-    run.close()
+               "api": "nimbus_cuda_engine_upload_image_async + nimbus_cuda_engine_step + "
+                      "nimbus_cuda_engine_download_image_async, the runs split over "
+                      f"{args.e2e_groups} engines on their own streams (each engine's nine prognostic fields of "
+                      "every run in one pinned host block, one copy each way per step; uploads chained group "
+                      "after group, downloads likewise, so one group's copies overlap another's step)"}
 
     # ---- plain path: each run alone, one C-ABI call per operation ----
     plain = None
@@ -421,7 +422,8 @@ def run_ours(args):
 
         plain_step()
         ctx.synchronize()
-        p_ms = max_over_ranks(time_on_stream(torch, stream, plain_step, args.plain_steps))
+        ctx_stream = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{device}")
+        p_ms = max_over_ranks(time_on_stream(torch, ctx_stream, plain_step, args.plain_steps))
         plain = {"value": total_cells * args.plain_steps / (p_ms / 1e3), "ms_per_step": p_ms / args.plain_steps,
                  "steps": args.plain_steps,
                  "path": "each run alone through the per-operation entry points (slow_step, acoustic_boundaries, "
@@ -462,7 +464,9 @@ def run_ours(args):
                 "acoustic_substeps": nsub, "scalars": 4,
                 "path": "full large step: slow Heun, boundary refresh + KW78 seed, N split substeps "
                         "(mass flux, continuity+EOS, momentum, boundaries), WENO5 transport, Kessler, EOS",
-                "form": "batched member engine, one launch per phase for all runs, CUDA graph replay",
+                "form": f"batched member engine: the runs in {args.lanes} size-balanced lanes (parallel branches of "
+                        "one CUDA graph), one launch per phase per lane",
+                "lanes": args.lanes,
                 "precision": args.precision,
                 "precision_modes": {
                     args.precision: {"value": value, "ms_per_step": ms / args.steps},

@@ -518,7 +518,37 @@ nimbus_status nimbus_cuda_engine_retire(nimbus_engine* e, int member_id);
 nimbus_status nimbus_cuda_engine_read(nimbus_engine* e, int member_id, const nimbus_member_state* out);
 /* Replaces a member's state with host arrays (waits for enqueued steps). */
 nimbus_status nimbus_cuda_engine_write(nimbus_engine* e, int member_id, const nimbus_member_state* in);
-/* Enqueues n_steps large steps of every resident member on the context's
+/* The same copies enqueued on the engine's stream without waiting, ordered
+ * with its steps: host arrays should be pinned and must stay untouched until
+ * nimbus_cuda_engine_synchronize.  Several engines (each with its own stream)
+ * overlap one engine's copies with another's steps. */
+nimbus_status nimbus_cuda_engine_write_async(nimbus_engine* e, int member_id, const nimbus_member_state* in);
+nimbus_status nimbus_cuda_engine_read_async(nimbus_engine* e, int member_id, const nimbus_member_state* out);
+/* The engine's own CUDA stream (cudaStream_t), on which its steps run. */
+void* nimbus_cuda_engine_stream(const nimbus_engine* e);
+/* The state image: every member's nine prognostic fields in one block, members
+ * in admission order, each member's fields in nimbus_member_state order (u, v,
+ * w, rho, p, theta, qv, qc, qr), each nx*ny*nz floats.  Moving it costs one
+ * host<->device copy per direction plus one device pass that scatters it into
+ * (or gathers it from) the members' current buffers, where the per-member
+ * copies above cost nine each: many small copies in both directions at once
+ * run well below the bus rate, one large copy each way runs at it.
+ * image_bytes: the image size (0 for an empty engine); image_offset: a
+ * member's byte offset in it ((size_t)-1 for an unknown id). */
+size_t nimbus_cuda_engine_image_bytes(const nimbus_engine* e);
+size_t nimbus_cuda_engine_image_offset(const nimbus_engine* e, int member_id);
+/* Enqueue the image copies on the engine's stream, ordered with its steps
+ * (host memory should be pinned and stay untouched until synchronize). */
+nimbus_status nimbus_cuda_engine_upload_image_async(nimbus_engine* e, const void* host_image);
+nimbus_status nimbus_cuda_engine_download_image_async(nimbus_engine* e, void* host_image);
+/* Lanes: the members are split into up to `lanes` size-balanced groups whose
+ * launches run on parallel streams (branches of the one step graph), so one
+ * group's kernels fill the SMs another's launch tails leave idle.  Results do
+ * not depend on the lane count.  Default 4; takes effect at the next step.
+ * nimbus_cuda_engine_lanes: the lanes the current table uses. */
+nimbus_status nimbus_cuda_engine_set_lanes(nimbus_engine* e, int lanes);
+int nimbus_cuda_engine_lanes(const nimbus_engine* e);
+/* Enqueues n_steps large steps of every resident member on the engine's
  * stream: replayed from a CUDA graph when graphs are on (the default), the
  * graph rebuilt after admissions, retirements or a precision change. */
 nimbus_status nimbus_cuda_engine_step(nimbus_engine* e, int n_steps);

@@ -26,6 +26,7 @@ namespace
 
 constexpr size_t kAlign = 256;
 
+using nimbus_engine_detail::Lane;
 using nimbus_engine_detail::MemberSlot;
 
 size_t align_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
@@ -185,10 +186,28 @@ void fill_params(EngineMember& M, const nimbus_member_desc* a)
 namespace
 {
 
+// The host views track the device pointer rotations by replaying them
+// (rotate_host_views) after every enqueued step; only a refused EOS
+// projection (a member whose p is not rotated) makes them inexact, and then
+// the device table is read back.
+void rotate_host_views(nimbus_engine* e, int steps)
+{
+    for (auto& slot : e->slots)
+    {
+        EngineMember& M = slot.m;
+        for (int s = 0; s < steps; ++s)
+        {
+            if (M.n_substeps & 1) std::swap(M.rho, M.rho_alt);
+            if (M.microphysics) std::swap(M.qr, M.qr_alt);
+            std::swap(M.p, M.eos);
+        }
+    }
+}
+
 nimbus_status sync_table_to_host(nimbus_engine* e)
 {
     nimbus_cuda_context* ctx = e->ctx;
-    NB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    NB_CUDA(ctx, cudaStreamSynchronize(e->stream));
     if (e->table_current || e->order.empty()) return NIMBUS_OK;
     std::vector<EngineMember> host(e->order.size());
     NB_CUDA(ctx, cudaMemcpy(host.data(), e->d_table, sizeof(EngineMember) * host.size(), cudaMemcpyDeviceToHost));
@@ -197,26 +216,73 @@ nimbus_status sync_table_to_host(nimbus_engine* e)
     return NIMBUS_OK;
 }
 
+// Lane streams and events live as long as the engine; grown on demand.
+nimbus_status ensure_lane_streams(nimbus_engine* e, size_t extra)
+{
+    nimbus_cuda_context* ctx = e->ctx;
+    if (extra && !e->fork) NB_CUDA(ctx, cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming));
+    while (e->lane_streams.size() < extra)
+    {
+        cudaStream_t s = nullptr;
+        NB_CUDA(ctx, cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        e->lane_streams.push_back(s);
+        cudaEvent_t d = nullptr;
+        NB_CUDA(ctx, cudaEventCreateWithFlags(&d, cudaEventDisableTiming));
+        e->lane_done.push_back(d);
+    }
+    return NIMBUS_OK;
+}
+
 nimbus_status rebuild_table(nimbus_engine* e)
 {
     nimbus_cuda_context* ctx = e->ctx;
     NB_TRY(sync_table_to_host(e));
     const size_t n = e->slots.size();
-    e->order.resize(n);
-    for (size_t i = 0; i < n; ++i) e->order[i] = static_cast<int>(i);
-    std::stable_sort(e->order.begin(), e->order.end(), [&](int a, int b) {
-        return e->slots[a].desc.n_substeps > e->slots[b].desc.n_substeps;
-    });
+    // Lanes: members placed largest first on the least loaded lane (work =
+    // cells x (substeps + 3), the large step's cost in substep-equivalents),
+    // then each lane sorted by substep count, longest first.
+    const size_t lanes = std::min<size_t>(n, static_cast<size_t>(std::max(1, e->lane_target)));
+    std::vector<int> by_work(n);
+    for (size_t i = 0; i < n; ++i) by_work[i] = static_cast<int>(i);
+    auto work = [&](int i) {
+        return static_cast<double>(e->slots[i].m.items[kItemCells]) * (e->slots[i].desc.n_substeps + 3);
+    };
+    std::stable_sort(by_work.begin(), by_work.end(), [&](int a, int b) { return work(a) > work(b); });
+    std::vector<std::vector<int>> members(lanes);
+    std::vector<double> load(lanes, 0.0);
+    for (int i : by_work)
+    {
+        const size_t k = static_cast<size_t>(std::min_element(load.begin(), load.end()) - load.begin());
+        members[k].push_back(i);
+        load[k] += work(i);
+    }
+    e->order.clear();
+    e->lanes.assign(lanes, Lane());
+    size_t pre = 0;
+    for (size_t k = 0; k < lanes; ++k)
+    {
+        auto& m = members[k];
+        std::stable_sort(m.begin(), m.end(), [&](int a, int b) {
+            return e->slots[a].desc.n_substeps > e->slots[b].desc.n_substeps || (e->slots[a].desc.n_substeps ==
+                   e->slots[b].desc.n_substeps && a < b);
+        });
+        Lane& L = e->lanes[k];
+        L.first = static_cast<int>(e->order.size());
+        L.members = static_cast<int>(m.size());
+        L.prefix_first = pre;
+        pre += static_cast<size_t>(kItemKinds) * (m.size() + 1);
+        e->order.insert(e->order.end(), m.begin(), m.end());
+    }
+    NB_TRY(ensure_lane_streams(e, lanes ? lanes - 1 : 0));
     if (n > e->table_cap)
     {
+        const size_t cap = std::max<size_t>(n, 2 * e->table_cap);
         if (e->d_table) cudaFree(e->d_table);
         e->d_table = nullptr;
         e->table_cap = 0;
-        const size_t cap = std::max<size_t>(n, 2 * e->table_cap + 8);
         NB_CUDA(ctx, cudaMalloc(&e->d_table, sizeof(EngineMember) * cap));
         e->table_cap = cap;
     }
-    const size_t pre = static_cast<size_t>(kItemKinds) * (n + 1);
     if (pre > e->prefix_cap)
     {
         if (e->d_prefix) cudaFree(e->d_prefix);
@@ -225,27 +291,34 @@ nimbus_status rebuild_table(nimbus_engine* e)
         NB_CUDA(ctx, cudaMalloc(&e->d_prefix, sizeof(long long) * (pre + 64)));
         e->prefix_cap = pre + 64;
     }
+    long long image = 0;  // state-image offsets in admission order
+    for (auto& slot : e->slots)
+    {
+        slot.m.image_offset = image;
+        image += 9LL * slot.m.items[kItemCells];
+    }
     std::vector<EngineMember> host(n);
+    for (size_t r = 0; r < n; ++r) host[r] = e->slots[e->order[r]].m;
     e->prefix.assign(pre, 0);
-    int max_n = 0;
-    for (size_t r = 0; r < n; ++r)
+    const int tile = kEngineBlock * kItemsPerThread;
+    for (Lane& L : e->lanes)
     {
-        host[r] = e->slots[e->order[r]].m;
-        max_n = std::max(max_n, host[r].n_substeps);
-    }
-    for (int k = 0; k < kItemKinds; ++k)
-    {
-        long long* p = e->prefix.data() + static_cast<size_t>(k) * (n + 1);
-        p[0] = 0;
-        const int tile = kEngineBlock * kItemsPerThread;
-        for (size_t r = 0; r < n; ++r) p[r + 1] = p[r] + (host[r].items[k] + tile - 1) / tile;
-    }
-    e->active.assign(max_n, 0);
-    for (int s = 0; s < max_n; ++s)
-    {
-        int a = 0;
-        while (a < static_cast<int>(n) && host[a].n_substeps > s) ++a;
-        e->active[s] = a;
+        const EngineMember* rows = host.data() + L.first;
+        int max_n = 0;
+        for (int r = 0; r < L.members; ++r) max_n = std::max(max_n, rows[r].n_substeps);
+        for (int k = 0; k < kItemKinds; ++k)
+        {
+            long long* p = e->prefix.data() + L.prefix_first + static_cast<size_t>(k) * (L.members + 1);
+            p[0] = 0;
+            for (int r = 0; r < L.members; ++r) p[r + 1] = p[r] + (rows[r].items[k] + tile - 1) / tile;
+        }
+        L.active.assign(max_n, 0);
+        for (int st = 0; st < max_n; ++st)
+        {
+            int a = 0;
+            while (a < L.members && rows[a].n_substeps > st) ++a;
+            L.active[st] = a;
+        }
     }
     if (n)
     {
@@ -267,16 +340,38 @@ nimbus_status rebuild_table(nimbus_engine* e)
     return NIMBUS_OK;
 }
 
+int enqueue_lane(nimbus_engine* e, int lane, cudaStream_t st)
+{
+    if (e->ctx->precision == NIMBUS_PRECISION_FP32) return nimbus_fp32::engine_enqueue(e, lane, st);
+    return enqueue_step<RefPolicy, false>(e, lane, st);
+}
+
+// One large step of every lane: lanes 1.. forked from `st` onto their own
+// streams and joined back (inside a capture this builds parallel branches of
+// one graph).  Returns the launch count.
 int enqueue(nimbus_engine* e, cudaStream_t st)
 {
-    if (e->ctx->precision == NIMBUS_PRECISION_FP32) return nimbus_fp32::engine_enqueue(e, st);
-    return enqueue_step<RefPolicy, false>(e, st);
+    const size_t lanes = e->lanes.size();
+    if (lanes == 0) return 0;
+    if (lanes == 1) return enqueue_lane(e, 0, st);
+    int count = 0;
+    cudaEventRecord(e->fork, st);
+    for (size_t k = 1; k < lanes; ++k)
+    {
+        cudaStream_t ls = e->lane_streams[k - 1];
+        cudaStreamWaitEvent(ls, e->fork, 0);
+        count += enqueue_lane(e, static_cast<int>(k), ls);
+        cudaEventRecord(e->lane_done[k - 1], ls);
+    }
+    count += enqueue_lane(e, 0, st);
+    for (size_t k = 1; k < lanes; ++k) cudaStreamWaitEvent(st, e->lane_done[k - 1], 0);
+    return count;
 }
 
 nimbus_status build_graph(nimbus_engine* e)
 {
     nimbus_cuda_context* ctx = e->ctx;
-    cudaStream_t st = ctx->stream;
+    cudaStream_t st = e->stream;
     NB_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     const int launches = enqueue(e, st);
     cudaGraph_t g = nullptr;
@@ -307,6 +402,45 @@ MemberSlot* find_slot(nimbus_engine* e, int id, size_t* index = nullptr)
     return nullptr;
 }
 
+size_t image_bytes_of(const nimbus_engine* e)
+{
+    size_t floats = 0;
+    for (const auto& slot : e->slots) floats += 9ull * static_cast<size_t>(slot.m.items[kItemCells]);
+    return floats * sizeof(float);
+}
+
+// Table current, staging allocated: the common part of the image copies.
+nimbus_status prepare_image(nimbus_engine* e, size_t* bytes)
+{
+    nimbus_cuda_context* ctx = e->ctx;
+    NB_CUDA(ctx, cudaSetDevice(ctx->device));
+    if (e->dirty) NB_TRY(rebuild_table(e));
+    *bytes = image_bytes_of(e);
+    if (*bytes > e->image_cap)
+    {
+        NB_CUDA(ctx, cudaStreamSynchronize(e->stream));
+        if (e->d_image) cudaFree(e->d_image);
+        e->d_image = nullptr;
+        e->image_cap = 0;
+        NB_CUDA(ctx, cudaMalloc(&e->d_image, *bytes));
+        e->image_cap = *bytes;
+    }
+    return NIMBUS_OK;
+}
+
+void launch_image(nimbus_engine* e, int gather)
+{
+    for (const Lane& L : e->lanes)
+    {
+        const long long tiles = tiles_of(e, L, kItemCells, L.members);
+        if (tiles <= 0) continue;
+        engine_image_kernel<<<engine_grid(e, reinterpret_cast<const void*>(engine_image_kernel), tiles), kEngineBlock,
+                              0, e->stream>>>(e->d_table + L.first, prefix_of(e, L, kItemCells), tiles, e->d_image,
+                                              gather);
+        e->ctx->launches += 1;
+    }
+}
+
 const char* check_state(const nimbus_member_state* s)
 {
     if (!s) return "state is null";
@@ -335,9 +469,16 @@ nimbus_status nimbus_cuda_engine_create(nimbus_cuda_context* ctx, nimbus_engine*
 {
     if (!ctx || !out) return NIMBUS_ERR_INVALID_ARGUMENT;
     *out = nullptr;
+    NB_CUDA(ctx, cudaSetDevice(ctx->device));
     auto* e = new (std::nothrow) nimbus_engine();
     if (!e) return fail(ctx, NIMBUS_ERR_OUT_OF_MEMORY, "engine allocation failed");
     e->ctx = ctx;
+    const cudaError_t err = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+    if (err != cudaSuccess)
+    {
+        delete e;
+        return cuda_fail(ctx, err, "engine stream");
+    }
     *out = e;
     return NIMBUS_OK;
 }
@@ -345,13 +486,18 @@ nimbus_status nimbus_cuda_engine_create(nimbus_cuda_context* ctx, nimbus_engine*
 void nimbus_cuda_engine_destroy(nimbus_engine* e)
 {
     if (!e) return;
-    cudaStreamSynchronize(e->ctx->stream);
+    cudaStreamSynchronize(e->stream);
     if (e->exec) cudaGraphExecDestroy(e->exec);
     if (e->graph) cudaGraphDestroy(e->graph);
     for (auto& s : e->slots)
         if (s.arena) cudaFree(s.arena);
     if (e->d_table) cudaFree(e->d_table);
     if (e->d_prefix) cudaFree(e->d_prefix);
+    if (e->d_image) cudaFree(e->d_image);
+    for (cudaStream_t ls : e->lane_streams) cudaStreamDestroy(ls);
+    for (cudaEvent_t ev : e->lane_done) cudaEventDestroy(ev);
+    if (e->fork) cudaEventDestroy(e->fork);
+    if (e->stream) cudaStreamDestroy(e->stream);
     delete e;
 }
 
@@ -443,9 +589,9 @@ nimbus_status nimbus_cuda_engine_admit(nimbus_engine* e, const nimbus_member_des
     {
         // The same per-level kernel the per-operation path runs, so both forms
         // see identical base data.
-        level_base_kernel<<<(desc->nz + 127) / 128, 128, 0, ctx->stream>>>(M.p0, desc->nz, M.gamma, dp0, eos0);
+        level_base_kernel<<<(desc->nz + 127) / 128, 128, 0, e->stream>>>(M.p0, desc->nz, M.gamma, dp0, eos0);
         err = cudaGetLastError();
-        if (err == cudaSuccess) err = cudaStreamSynchronize(ctx->stream);
+        if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
     }
     if (err == cudaSuccess) err = cudaMemset(M.status, 0, sizeof(unsigned));
     // Scratch that a step reads before writing: none, but keep it defined.
@@ -475,39 +621,97 @@ nimbus_status nimbus_cuda_engine_retire(nimbus_engine* e, int member_id)
     return NIMBUS_OK;
 }
 
-nimbus_status nimbus_cuda_engine_read(nimbus_engine* e, int member_id, const nimbus_member_state* out)
+nimbus_status nimbus_cuda_engine_read_async(nimbus_engine* e, int member_id, const nimbus_member_state* out)
 {
     if (!e) return NIMBUS_ERR_INVALID_ARGUMENT;
     nimbus_cuda_context* ctx = e->ctx;
     if (const char* why = check_state(out)) return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, why);
     MemberSlot* s = find_slot(e, member_id);
     if (!s) return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "unknown member id");
-    NB_TRY(sync_table_to_host(e));
+    if (!e->mirror_exact) NB_TRY(sync_table_to_host(e));
     const EngineMember& M = s->m;
     const size_t bytes = static_cast<size_t>(M.items[kItemCells]) * sizeof(float);
     const float* src[9] = {M.u, M.v, M.w, M.rho, M.p, M.theta, M.qv, M.qc, M.qr};
     float* dst[9] = {out->u, out->v, out->w, out->rho, out->p, out->theta, out->qv, out->qc, out->qr};
     for (int f = 0; f < 9; ++f)
-        NB_CUDA(ctx, cudaMemcpyAsync(dst[f], src[f], bytes, cudaMemcpyDeviceToHost, ctx->stream));
-    NB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        NB_CUDA(ctx, cudaMemcpyAsync(dst[f], src[f], bytes, cudaMemcpyDeviceToHost, e->stream));
     return NIMBUS_OK;
 }
 
-nimbus_status nimbus_cuda_engine_write(nimbus_engine* e, int member_id, const nimbus_member_state* in)
+nimbus_status nimbus_cuda_engine_write_async(nimbus_engine* e, int member_id, const nimbus_member_state* in)
 {
     if (!e) return NIMBUS_ERR_INVALID_ARGUMENT;
     nimbus_cuda_context* ctx = e->ctx;
     if (const char* why = check_state(in)) return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, why);
     MemberSlot* s = find_slot(e, member_id);
     if (!s) return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "unknown member id");
-    NB_TRY(sync_table_to_host(e));
+    if (!e->mirror_exact) NB_TRY(sync_table_to_host(e));
     const EngineMember& M = s->m;
     const size_t bytes = static_cast<size_t>(M.items[kItemCells]) * sizeof(float);
     const float* src[9] = {in->u, in->v, in->w, in->rho, in->p, in->theta, in->qv, in->qc, in->qr};
     float* dst[9] = {M.u, M.v, M.w, M.rho, M.p, M.theta, M.qv, M.qc, M.qr};
     for (int f = 0; f < 9; ++f)
-        NB_CUDA(ctx, cudaMemcpyAsync(dst[f], src[f], bytes, cudaMemcpyHostToDevice, ctx->stream));
-    NB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        NB_CUDA(ctx, cudaMemcpyAsync(dst[f], src[f], bytes, cudaMemcpyHostToDevice, e->stream));
+    return NIMBUS_OK;
+}
+
+nimbus_status nimbus_cuda_engine_read(nimbus_engine* e, int member_id, const nimbus_member_state* out)
+{
+    if (!e) return NIMBUS_ERR_INVALID_ARGUMENT;
+    NB_TRY(sync_table_to_host(e));
+    NB_TRY(nimbus_cuda_engine_read_async(e, member_id, out));
+    NB_CUDA(e->ctx, cudaStreamSynchronize(e->stream));
+    return NIMBUS_OK;
+}
+
+nimbus_status nimbus_cuda_engine_write(nimbus_engine* e, int member_id, const nimbus_member_state* in)
+{
+    if (!e) return NIMBUS_ERR_INVALID_ARGUMENT;
+    NB_TRY(sync_table_to_host(e));
+    NB_TRY(nimbus_cuda_engine_write_async(e, member_id, in));
+    NB_CUDA(e->ctx, cudaStreamSynchronize(e->stream));
+    return NIMBUS_OK;
+}
+
+void* nimbus_cuda_engine_stream(const nimbus_engine* e) { return e ? static_cast<void*>(e->stream) : nullptr; }
+
+size_t nimbus_cuda_engine_image_bytes(const nimbus_engine* e) { return e ? image_bytes_of(e) : 0; }
+
+size_t nimbus_cuda_engine_image_offset(const nimbus_engine* e, int member_id)
+{
+    if (!e) return static_cast<size_t>(-1);
+    size_t floats = 0;
+    for (const auto& slot : e->slots)
+    {
+        if (slot.id == member_id) return floats * sizeof(float);
+        floats += 9ull * static_cast<size_t>(slot.m.items[kItemCells]);
+    }
+    return static_cast<size_t>(-1);
+}
+
+nimbus_status nimbus_cuda_engine_upload_image_async(nimbus_engine* e, const void* host_image)
+{
+    if (!e || !host_image) return NIMBUS_ERR_INVALID_ARGUMENT;
+    nimbus_cuda_context* ctx = e->ctx;
+    size_t bytes = 0;
+    NB_TRY(prepare_image(e, &bytes));
+    if (!bytes) return NIMBUS_OK;
+    NB_CUDA(ctx, cudaMemcpyAsync(e->d_image, host_image, bytes, cudaMemcpyHostToDevice, e->stream));
+    launch_image(e, 0);
+    NB_CUDA(ctx, cudaGetLastError());
+    return NIMBUS_OK;
+}
+
+nimbus_status nimbus_cuda_engine_download_image_async(nimbus_engine* e, void* host_image)
+{
+    if (!e || !host_image) return NIMBUS_ERR_INVALID_ARGUMENT;
+    nimbus_cuda_context* ctx = e->ctx;
+    size_t bytes = 0;
+    NB_TRY(prepare_image(e, &bytes));
+    if (!bytes) return NIMBUS_OK;
+    launch_image(e, 1);
+    NB_CUDA(ctx, cudaGetLastError());
+    NB_CUDA(ctx, cudaMemcpyAsync(host_image, e->d_image, bytes, cudaMemcpyDeviceToHost, e->stream));
     return NIMBUS_OK;
 }
 
@@ -532,12 +736,13 @@ nimbus_status nimbus_cuda_engine_step(nimbus_engine* e, int n_steps)
     }
     for (int i = 0; i < n_steps; ++i)
     {
-        if (graph) NB_CUDA(ctx, cudaGraphLaunch(e->exec, ctx->stream));
-        else e->launches_per_step = enqueue(e, ctx->stream);
+        if (graph) NB_CUDA(ctx, cudaGraphLaunch(e->exec, e->stream));
+        else e->launches_per_step = enqueue(e, e->stream);
         ctx->launches += static_cast<uint64_t>(e->launches_per_step);
     }
     NB_CUDA(ctx, cudaGetLastError());
-    e->table_current = false;
+    rotate_host_views(e, n_steps);
+    e->table_current = e->mirror_exact;
     return NIMBUS_OK;
 }
 
@@ -552,6 +757,14 @@ nimbus_status nimbus_cuda_engine_synchronize(nimbus_engine* e)
         unsigned f = 0;
         NB_CUDA(ctx, cudaMemcpy(&f, s.m.status, sizeof(unsigned), cudaMemcpyDeviceToHost));
         any |= f;
+    }
+    if (any & kStatusInvalidEos)
+    {
+        // A refused projection keeps that member's pressure buffer: read the
+        // true pointers back.
+        e->mirror_exact = false;
+        e->table_current = false;
+        NB_TRY(sync_table_to_host(e));
     }
     if (any & kStatusNonfiniteMassFlux) return fail(ctx, NIMBUS_ERR_NONFINITE, "a member's retained mass flux went non-finite");
     if (any & kStatusNonfiniteTransport) return fail(ctx, NIMBUS_ERR_NONFINITE, "a member's transported scalar went non-finite");
@@ -575,6 +788,20 @@ nimbus_status nimbus_cuda_engine_set_graph(nimbus_engine* e, int enable)
     e->use_graph = enable != 0;
     return NIMBUS_OK;
 }
+
+nimbus_status nimbus_cuda_engine_set_lanes(nimbus_engine* e, int lanes)
+{
+    if (!e || lanes < 1) return NIMBUS_ERR_INVALID_ARGUMENT;
+    if (lanes != e->lane_target)
+    {
+        NB_TRY(sync_table_to_host(e));
+        e->lane_target = lanes;
+        e->dirty = true;
+    }
+    return NIMBUS_OK;
+}
+
+int nimbus_cuda_engine_lanes(const nimbus_engine* e) { return e ? static_cast<int>(e->lanes.size()) : 0; }
 
 int nimbus_cuda_engine_members(const nimbus_engine* e) { return e ? static_cast<int>(e->slots.size()) : 0; }
 

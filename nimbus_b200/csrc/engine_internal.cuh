@@ -19,6 +19,19 @@ struct MemberSlot
     size_t bytes = 0;
     nimbus::EngineMember m;   // host view of the device entry (refreshed before use)
 };
+// A lane: a contiguous run of table rows whose members step together.  The
+// members are split into size-balanced lanes; each lane's launches go to its
+// own stream (forked from the engine stream and joined back, inside the one
+// captured graph), so one lane's kernels fill the SMs that another's
+// launch tails leave idle.  Within a lane rows are sorted by substep count,
+// so the members still inside the acoustic loop are a prefix of it.
+struct Lane
+{
+    int first = 0;            // first table row
+    int members = 0;
+    size_t prefix_first = 0;  // first entry of this lane's [kItemKinds][members + 1] prefix block
+    std::vector<int> active;  // members of this lane inside the loop at substep s
+};
 // The Kessler + EOS pass is FP64 in both forms and is launched from the
 // uncontracted unit (engine.cu), so both forms and the per-operation path
 // share its rounding.  Returns the launch count.
@@ -29,6 +42,8 @@ int launch_microphysics(nimbus_engine* e, cudaStream_t st, const nimbus::EngineM
 struct nimbus_engine
 {
     nimbus_cuda_context* ctx = nullptr;
+    cudaStream_t stream = nullptr;  // the engine's own stream (graphs, copies)
+    bool mirror_exact = true;       // host views predict the device pointer rotations
     std::vector<nimbus_engine_detail::MemberSlot> slots;  // admission order
     std::vector<int> order;         // slot indices in table order
     int next_id = 1;
@@ -40,12 +55,18 @@ struct nimbus_engine
     size_t table_cap = 0;
     long long* d_prefix = nullptr;
     size_t prefix_cap = 0;
-    std::vector<long long> prefix;  // [kItemKinds][members + 1]
-    std::vector<int> active;        // members inside the loop at substep s
+    std::vector<long long> prefix;  // the lanes' prefix blocks, back to back
+    std::vector<nimbus_engine_detail::Lane> lanes;
+    int lane_target = 4;            // lanes when there are at least that many members
+    std::vector<cudaStream_t> lane_streams;  // lanes 1.. (lane 0 runs on the engine stream)
+    std::vector<cudaEvent_t> lane_done;
+    cudaEvent_t fork = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int launches_per_step = 0;
     std::map<const void*, int> occupancy;
+    float* d_image = nullptr;       // device staging for the state image
+    size_t image_cap = 0;           // bytes
 };
 
 namespace
@@ -75,14 +96,14 @@ unsigned engine_grid(nimbus_engine* e, const void* kernel, long long tiles)
     return static_cast<unsigned>(g < 1 ? 1 : g);
 }
 
-const long long* prefix_of(const nimbus_engine* e, int kind)
+const long long* prefix_of(const nimbus_engine* e, const nimbus_engine_detail::Lane& L, int kind)
 {
-    return e->d_prefix + static_cast<size_t>(kind) * (e->order.size() + 1);
+    return e->d_prefix + L.prefix_first + static_cast<size_t>(kind) * (L.members + 1);
 }
 
-long long tiles_of(const nimbus_engine* e, int kind, int members)
+long long tiles_of(const nimbus_engine* e, const nimbus_engine_detail::Lane& L, int kind, int members)
 {
-    return e->prefix[static_cast<size_t>(kind) * (e->order.size() + 1) + members];
+    return e->prefix[L.prefix_first + static_cast<size_t>(kind) * (L.members + 1) + members];
 }
 
 #define ENGINE_LAUNCH(family, kernel, tiles, gy, ...)                                                    \
@@ -97,48 +118,50 @@ long long tiles_of(const nimbus_engine* e, int kind, int members)
         }                                                                                                \
     } while (0)
 
-// Enqueues one large step of every member; returns the number of launches.
+// Enqueues one large step of the members of one lane on `st`; returns the
+// number of launches.
 template <class Policy, bool kFp32>
-int enqueue_step(nimbus_engine* e, cudaStream_t st)
+int enqueue_step(nimbus_engine* e, int lane, cudaStream_t st)
 {
     nimbus_cuda_context* ctx = e->ctx;
-    const int n = static_cast<int>(e->order.size());
+    const nimbus_engine_detail::Lane& L = e->lanes[static_cast<size_t>(lane)];
+    const int n = L.members;
     int count = 0;
-    EngineMember* T = e->d_table;
-    const long long* pc = prefix_of(e, kItemCells);
-    const long long* pwe = prefix_of(e, kItemRowsWE);
-    const long long* psn = prefix_of(e, kItemRowsSN);
-    const long long* pcol = prefix_of(e, kItemColumns);
-    const long long* phist = prefix_of(e, kItemHistory);
-    const long long cells = tiles_of(e, kItemCells, n);
+    EngineMember* T = e->d_table + L.first;
+    const long long* pc = prefix_of(e, L, kItemCells);
+    const long long* pwe = prefix_of(e, L, kItemRowsWE);
+    const long long* psn = prefix_of(e, L, kItemRowsSN);
+    const long long* pcol = prefix_of(e, L, kItemColumns);
+    const long long* phist = prefix_of(e, L, kItemHistory);
+    const long long cells = tiles_of(e, L, kItemCells, n);
 
     // Heun slow step (prepare_slow_rk2_tendencies + apply_slow_tendencies).
     ENGINE_LAUNCH(NIMBUS_KERNEL_SLOW, engine_slow_predict_kernel<Policy>, cells, 1, T, pc, cells);
     ENGINE_LAUNCH(NIMBUS_KERNEL_SLOW, engine_slow_correct_kernel<Policy>, cells, 1, T, pc, cells);
     // seed_acoustic_radiation: apply_acoustic(0) then the KW78 seed.
-    ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_bc_we_kernel, tiles_of(e, kItemRowsWE, n), 1, T, pwe,
-                  tiles_of(e, kItemRowsWE, n), 0, 1);
-    ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_bc_sn_kernel, tiles_of(e, kItemRowsSN, n), 1, T, psn,
-                  tiles_of(e, kItemRowsSN, n), 0, 1);
-    ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_bc_vertical_kernel, tiles_of(e, kItemColumns, n), 1, T,
-                  pcol, tiles_of(e, kItemColumns, n));
-    ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_seed_kernel, tiles_of(e, kItemHistory, n), 1, T, phist,
-                  tiles_of(e, kItemHistory, n));
-    // The acoustic loop: members still inside it are a prefix of the table.
-    for (size_t s = 0; s < e->active.size(); ++s)
+    ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_bc_we_kernel, tiles_of(e, L, kItemRowsWE, n), 1, T, pwe,
+                  tiles_of(e, L, kItemRowsWE, n), 0, 1);
+    ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_bc_sn_kernel, tiles_of(e, L, kItemRowsSN, n), 1, T, psn,
+                  tiles_of(e, L, kItemRowsSN, n), 0, 1);
+    ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_bc_vertical_kernel, tiles_of(e, L, kItemColumns, n), 1, T,
+                  pcol, tiles_of(e, L, kItemColumns, n));
+    ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_seed_kernel, tiles_of(e, L, kItemHistory, n), 1, T, phist,
+                  tiles_of(e, L, kItemHistory, n));
+    // The acoustic loop: members still inside it are a prefix of the lane.
+    for (size_t s = 0; s < L.active.size(); ++s)
     {
-        const int a = e->active[s];
+        const int a = L.active[s];
         const int si = static_cast<int>(s);
-        ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, engine_continuity_kernel<Policy>, tiles_of(e, kItemCells, a), 1,
-                      T, pc, tiles_of(e, kItemCells, a), si);
-        ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_MOMENTUM, engine_momentum_kernel<Policy>, tiles_of(e, kItemCells, a), 1,
-                      T, pc, tiles_of(e, kItemCells, a), si);
-        ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_bc_we_kernel, tiles_of(e, kItemRowsWE, a), 1, T, pwe,
-                      tiles_of(e, kItemRowsWE, a), si, 0);
-        ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_bc_sn_kernel, tiles_of(e, kItemRowsSN, a), 1, T, psn,
-                      tiles_of(e, kItemRowsSN, a), si, 0);
-        ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_bc_vertical_kernel, tiles_of(e, kItemColumns, a), 1, T,
-                      pcol, tiles_of(e, kItemColumns, a));
+        ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, engine_continuity_kernel<Policy>, tiles_of(e, L, kItemCells, a), 1,
+                      T, pc, tiles_of(e, L, kItemCells, a), si);
+        ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_MOMENTUM, engine_momentum_kernel<Policy>, tiles_of(e, L, kItemCells, a), 1,
+                      T, pc, tiles_of(e, L, kItemCells, a), si);
+        ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_bc_we_kernel, tiles_of(e, L, kItemRowsWE, a), 1, T, pwe,
+                      tiles_of(e, L, kItemRowsWE, a), si, 0);
+        ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_bc_sn_kernel, tiles_of(e, L, kItemRowsSN, a), 1, T, psn,
+                      tiles_of(e, L, kItemRowsSN, a), si, 0);
+        ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_bc_vertical_kernel, tiles_of(e, L, kItemColumns, a), 1, T,
+                      pcol, tiles_of(e, L, kItemColumns, a));
     }
     engine_swap_kernel<<<(n + 127) / 128, 128, 0, st>>>(T, n, 0);
     ++count;

@@ -62,6 +62,7 @@ struct EngineMember
     int n_substeps;
     int microphysics;
     int items[kItemKinds];
+    long long image_offset;  // first float of this member's block in the engine's state image
 };
 
 __device__ __forceinline__ const float* engine_scalar(const EngineMember& M, int s)
@@ -209,6 +210,39 @@ static __global__ void __launch_bounds__(256) engine_momentum_kernel(const Engin
 {
     for_member_items(table, prefix, tiles, kItemCells, [&](const EngineMember& M, int c) {
         momentum_cell<Policy>(M.F, engine_density(M, s, true), M.p, M.p0, M.dp0, M.u, M.v, M.w, M.u, M.v, M.w, c);
+    });
+}
+
+// ---- state image ----------------------------------------------------------
+// The engine's state image holds every member's nine prognostic fields back to
+// back (u, v, w, rho, p, theta, qv, qc, qr, each items[kItemCells] floats) from
+// image + image_offset.  gather = 0 scatters the image into the members'
+// current buffers, gather = 1 collects them into it; one coalesced pass over
+// all cells of all members either way.
+static __global__ void __launch_bounds__(256) engine_image_kernel(const EngineMember* __restrict__ table,
+                                                                  const long long* __restrict__ prefix,
+                                                                  long long tiles, float* __restrict__ image,
+                                                                  int gather)
+{
+    for_member_items(table, prefix, tiles, kItemCells, [&](const EngineMember& M, int c) {
+        const long long n = M.items[kItemCells];
+        float* blk = image + M.image_offset + c;
+        float* const field[9] = {M.u, M.v, M.w, M.rho, M.p, M.theta, M.qv, M.qc, M.qr};
+        float x[9];
+        if (gather)
+        {
+#pragma unroll
+            for (int f = 0; f < 9; ++f) x[f] = field[f][c];
+#pragma unroll
+            for (int f = 0; f < 9; ++f) blk[f * n] = x[f];
+        }
+        else
+        {
+#pragma unroll
+            for (int f = 0; f < 9; ++f) x[f] = blk[f * n];
+#pragma unroll
+            for (int f = 0; f < 9; ++f) field[f][c] = x[f];
+        }
     });
 }
 

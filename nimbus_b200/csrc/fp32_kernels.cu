@@ -40,6 +40,9 @@ nimbus_status launch_transport(nimbus_cuda_context* ctx, cudaStream_t st, const 
     return launch_transport_impl<true>(ctx, st, T, rho_end, rho_begin, mfx, mfy, mfz, sf, rl);
 }
 
-int engine_enqueue(nimbus_engine* e, cudaStream_t st) { return enqueue_step<nimbus::Fp32Policy, true>(e, st); }
+int engine_enqueue(nimbus_engine* e, int lane, cudaStream_t st)
+{
+    return enqueue_step<nimbus::Fp32Policy, true>(e, lane, st);
+}
 
 }  // namespace nimbus_fp32

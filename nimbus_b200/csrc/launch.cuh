@@ -190,5 +190,5 @@ nimbus_status launch_transport(nimbus_cuda_context* ctx, cudaStream_t st, const 
                                const float* rho_end, const float* rho_begin, const float* mfx, const float* mfy,
                                const float* mfz, float* sf, float* rl);
 // One large step of every engine member (FP32 form); returns the launch count.
-int engine_enqueue(nimbus_engine* e, cudaStream_t st);
+int engine_enqueue(nimbus_engine* e, int lane, cudaStream_t st);
 }  // namespace nimbus_fp32

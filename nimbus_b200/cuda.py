@@ -159,6 +159,10 @@ EXPORTED_SYMBOLS = (
     "nimbus_cuda_acoustic_boundaries",
     "nimbus_cuda_engine_create", "nimbus_cuda_engine_destroy", "nimbus_cuda_engine_member_bytes",
     "nimbus_cuda_engine_admit", "nimbus_cuda_engine_retire", "nimbus_cuda_engine_read", "nimbus_cuda_engine_write", "nimbus_cuda_engine_step",
+    "nimbus_cuda_engine_read_async", "nimbus_cuda_engine_write_async", "nimbus_cuda_engine_stream",
+    "nimbus_cuda_engine_image_bytes", "nimbus_cuda_engine_image_offset",
+    "nimbus_cuda_engine_upload_image_async", "nimbus_cuda_engine_download_image_async",
+    "nimbus_cuda_engine_set_lanes", "nimbus_cuda_engine_lanes",
     "nimbus_cuda_engine_synchronize", "nimbus_cuda_engine_member_status", "nimbus_cuda_engine_set_graph",
     "nimbus_cuda_engine_members", "nimbus_cuda_engine_launches_per_step",
 )
@@ -208,6 +212,18 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
     lib.nimbus_cuda_engine_retire.argtypes = [vp, ctypes.c_int]
     lib.nimbus_cuda_engine_read.argtypes = [vp, ctypes.c_int, ctypes.POINTER(MemberState)]
     lib.nimbus_cuda_engine_write.argtypes = [vp, ctypes.c_int, ctypes.POINTER(MemberState)]
+    lib.nimbus_cuda_engine_write_async.argtypes = [vp, ctypes.c_int, ctypes.POINTER(MemberState)]
+    lib.nimbus_cuda_engine_read_async.argtypes = [vp, ctypes.c_int, ctypes.POINTER(MemberState)]
+    lib.nimbus_cuda_engine_stream.argtypes = [vp]
+    lib.nimbus_cuda_engine_stream.restype = vp
+    lib.nimbus_cuda_engine_image_bytes.argtypes = [vp]
+    lib.nimbus_cuda_engine_image_bytes.restype = ctypes.c_size_t
+    lib.nimbus_cuda_engine_image_offset.argtypes = [vp, ctypes.c_int]
+    lib.nimbus_cuda_engine_image_offset.restype = ctypes.c_size_t
+    lib.nimbus_cuda_engine_upload_image_async.argtypes = [vp, vp]
+    lib.nimbus_cuda_engine_download_image_async.argtypes = [vp, vp]
+    lib.nimbus_cuda_engine_set_lanes.argtypes = [vp, ctypes.c_int]
+    lib.nimbus_cuda_engine_lanes.argtypes = [vp]
     lib.nimbus_cuda_engine_step.argtypes = [vp, ctypes.c_int]
     lib.nimbus_cuda_engine_synchronize.argtypes = [vp]
     lib.nimbus_cuda_engine_member_status.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_uint)]
@@ -609,6 +625,69 @@ class Engine:
             assert a.dtype == np.float32 and a.flags["C_CONTIGUOUS"] and a.shape == self.shapes[member_id], k
             setattr(st, k, _f(a))
         self.ctx.check(self.lib.nimbus_cuda_engine_write(self.handle, int(member_id), ctypes.byref(st)))
+
+    def _state_of(self, member_id: int, arrays: dict) -> MemberState:
+        st = MemberState()
+        for k in MEMBER_FIELDS:
+            a = arrays[k]
+            assert a.dtype == np.float32 and a.flags["C_CONTIGUOUS"] and a.shape == self.shapes[member_id], k
+            setattr(st, k, _f(a))
+        return st
+
+    def write_async(self, member_id: int, state: dict):
+        """Enqueue the state upload on the engine's stream (pinned arrays; keep
+        them alive and unchanged until synchronize)."""
+        self.ctx.check(self.lib.nimbus_cuda_engine_write_async(self.handle, int(member_id),
+                                                               ctypes.byref(self._state_of(member_id, state))))
+
+    def read_async(self, member_id: int, out: dict):
+        """Enqueue the state download on the engine's stream into `out`."""
+        self.ctx.check(self.lib.nimbus_cuda_engine_read_async(self.handle, int(member_id),
+                                                              ctypes.byref(self._state_of(member_id, out))))
+
+    @property
+    def stream(self) -> int:
+        return int(self.lib.nimbus_cuda_engine_stream(self.handle) or 0)
+
+    def set_lanes(self, lanes: int):
+        """Split the members over up to `lanes` parallel streams (default 4)."""
+        self.ctx.check(self.lib.nimbus_cuda_engine_set_lanes(self.handle, int(lanes)))
+
+    @property
+    def lanes(self) -> int:
+        return int(self.lib.nimbus_cuda_engine_lanes(self.handle))
+
+    def image_bytes(self) -> int:
+        """Size of the state image (all members' nine fields in one block)."""
+        return int(self.lib.nimbus_cuda_engine_image_bytes(self.handle))
+
+    def image_offset(self, member_id: int) -> int:
+        off = int(self.lib.nimbus_cuda_engine_image_offset(self.handle, int(member_id)))
+        if off == ctypes.c_size_t(-1).value:
+            raise KeyError(member_id)
+        return off
+
+    def image_views(self, image: np.ndarray) -> dict:
+        """{member id: {field: array view}} into a host image of image_bytes()
+        bytes (any dtype, C-contiguous)."""
+        flat = image.reshape(-1).view(np.uint8)
+        assert flat.nbytes >= self.image_bytes()
+        views = {}
+        for mid, shape in self.shapes.items():
+            n = shape[0] * shape[1] * shape[2]
+            blk = flat[self.image_offset(mid):].view(np.float32)[:9 * n] if n else flat[:0].view(np.float32)
+            views[mid] = {k: blk[i * n:(i + 1) * n].reshape(shape) for i, k in enumerate(MEMBER_FIELDS)}
+        return views
+
+    def upload_image_async(self, image: np.ndarray):
+        """Enqueue the whole state image upload on the engine's stream (pinned
+        memory; keep it alive and unchanged until synchronize)."""
+        assert image.flags["C_CONTIGUOUS"] and image.nbytes >= self.image_bytes()
+        self.ctx.check(self.lib.nimbus_cuda_engine_upload_image_async(self.handle, image.ctypes.data))
+
+    def download_image_async(self, image: np.ndarray):
+        assert image.flags["C_CONTIGUOUS"] and image.nbytes >= self.image_bytes()
+        self.ctx.check(self.lib.nimbus_cuda_engine_download_image_async(self.handle, image.ctypes.data))
 
     def step(self, n: int = 1):
         self.ctx.check(self.lib.nimbus_cuda_engine_step(self.handle, int(n)))

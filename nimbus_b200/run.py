@@ -110,11 +110,14 @@ class ResidentRun:
 class EngineRun:
     """Runs resident in one member engine, advanced together."""
 
-    def __init__(self, ctx: cuda.Context, precision: int = cuda.PRECISION_FP32, graph: bool = True):
+    def __init__(self, ctx: cuda.Context, precision: int = cuda.PRECISION_FP32, graph: bool = True,
+                 lanes: int | None = None):
         self.ctx = ctx
         self.precision = precision
         self.engine = cuda.Engine(ctx)
         self.engine.set_graph(graph)
+        if lanes is not None:
+            self.engine.set_lanes(lanes)
         self.members = {}
 
     def admit(self, case: Case, state=None, base=None, coriolis_f: float = 0.0, microphysics: bool = True,
@@ -143,37 +146,62 @@ class EngineRun:
         self.engine.close()
 
 
-class HostStepper:
-    """The same large step through the library's host-buffer API: every step
-    writes the member's state from pinned host arrays, advances it and reads
-    it back, so the host<->device copies are part of each step."""
+class HostPipeline:
+    """Large steps through the library's host-buffer API: every step uploads
+    each run's state from pinned host memory, advances it and reads it back,
+    so all host<->device copies are inside the step.
 
-    def __init__(self, ctx: cuda.Context, case: Case, state=None, base=None, pin=True,
-                 precision: int = cuda.PRECISION_FP32):
+    The runs are split over `groups` engines, each on its own stream, and each
+    engine's runs live in one pinned host block laid out as its state image
+    (nimbus_cuda_engine_image_*): a step moves it with one copy each way, and
+    one group's copies overlap another group's step."""
+
+    def __init__(self, ctx: cuda.Context, cases, prepared=None, groups: int = 8,
+                 precision: int = cuda.PRECISION_FP32, lanes: int | None = 1):
         self.ctx = ctx
         self.precision = precision
-        self.case = case
-        if state is None:
-            state, base = initial_state(case)
-
-        def host(a):
-            t = torch.from_numpy(np.ascontiguousarray(a))
-            return (t.pin_memory() if pin else t.clone()).numpy()
-
-        self.fields = {k: host(state[k]) for k in PROGNOSTIC}
-        self.run = EngineRun(ctx, precision)
-        self.member = self.run.admit(case, state, base)
-        self.n_substeps = self.run.members[self.member][1]
+        prepared = prepared or [initial_state(c) for c in cases]
+        order = sorted(range(len(cases)), key=lambda i: -cases[i].cells)
+        groups = max(1, min(groups, len(cases)))
+        self.runs = [EngineRun(ctx, precision, lanes=lanes) for _ in range(groups)]
+        placed = []
+        for r, idx in enumerate(order):
+            run = self.runs[r % groups]
+            st, base = prepared[idx]
+            placed.append((run, run.admit(cases[idx], st, base), st))
+        self.images = []
+        views = {}
+        for run in self.runs:
+            img = torch.empty(max(run.engine.image_bytes(), 4), dtype=torch.uint8).pin_memory().numpy()
+            self.images.append(img)
+            views[id(run)] = run.engine.image_views(img)
+        self.host = []  # (run, member id, {field: view into the group's pinned image})
+        for run, mid, st in placed:
+            arrays = views[id(run)][mid]
+            for k in PROGNOSTIC:
+                arrays[k][...] = st[k]
+            self.host.append((run, mid, arrays))
+        self.cells = sum(c.cells for c in cases)
 
     def bytes_per_step(self):
         """Host<->device bytes one step moves (the nine prognostic fields each way)."""
-        n = self.case.cells * 4 * len(PROGNOSTIC)
+        n = self.cells * 4 * len(PROGNOSTIC)
         return n, n
 
-    def step(self):
-        self.run.engine.write(self.member, self.fields)
-        self.run.step(1)
-        self.run.engine.read_into(self.member, self.fields)
+    def step(self, n: int = 1):
+        """n large steps, each uploading every state, advancing it and reading it
+        back; each engine's stream orders step k's download before step k+1's
+        upload of the same host block, so consecutive steps of different groups
+        overlap.  Waits for all of them before returning."""
+        self.ctx.set_precision(self.precision)
+        for _ in range(n):
+            for run, image in zip(self.runs, self.images):
+                run.engine.upload_image_async(image)
+                run.engine.step(1)
+                run.engine.download_image_async(image)
+        for run in self.runs:
+            run.engine.synchronize()
 
     def close(self):
-        self.run.close()
+        for run in self.runs:
+            run.close()

@@ -13,7 +13,7 @@ import pytest
 import oracle
 from nimbus_b200 import cuda
 from nimbus_b200.initial import Case, cloudy_state
-from nimbus_b200.run import PROGNOSTIC, EngineRun, ResidentRun
+from nimbus_b200.run import PROGNOSTIC, EngineRun, HostPipeline, ResidentRun
 
 pytestmark = pytest.mark.gpu
 
@@ -215,3 +215,91 @@ def test_engine_reports_a_refused_member_only(ctx):
         assert_bitwise(got[k], want[k], k)
     run.close()
     alone.close()
+
+
+def test_host_pipeline_equals_resident_engine(ctx):
+    """Async host copies on several engine streams: uploading each state,
+    stepping and reading back every step gives the states the resident engine
+    reaches.  Odd and even substep counts and the Kessler step exercise the
+    rotated density, rain and pressure buffers the host side tracks."""
+    cases, prepared = [], []
+    for i, (shape, dt) in enumerate([((20, 17, 14), 3.0), ((12, 15, 10), 2.0), ((16, 16, 12), 3.5),
+                                     ((9, 14, 8), 2.5), ((18, 10, 11), 3.0)]):
+        c = _case(shape, BCS["radiative"] if i % 2 else BCS["periodic_open"], seed=90 + i, dt=dt)
+        cases.append(c)
+        prepared.append(_state(c, 90 + i))
+    pipe = HostPipeline(ctx, cases, prepared, groups=3)
+    for _ in range(3):
+        pipe.step()
+    order = sorted(range(len(cases)), key=lambda i: -cases[i].cells)
+    by_case = {idx: pipe.host[r][2] for r, idx in enumerate(order)}
+    pipe.close()
+    for i, (c, (st, base)) in enumerate(zip(cases, prepared)):
+        alone = EngineRun(ctx, precision=cuda.PRECISION_FP32)
+        mid = alone.admit(c, st, base)
+        alone.step(3)
+        want = alone.read(mid)
+        alone.close()
+        for k in PROGNOSTIC:
+            assert_bitwise(by_case[i][k], want[k], f"run {i} {k}")
+
+
+def test_state_image_round_trip(ctx):
+    """The state image holds each member's fields at its offset, in admission
+    order: a download right after admission returns the initial states, and an
+    uploaded image replaces them (retirements close the gaps)."""
+    run = EngineRun(ctx, precision=cuda.PRECISION_FP32)
+    states = {}
+    for i, shape in enumerate([(11, 9, 7), (6, 13, 5), (8, 8, 9)]):
+        c = _case(shape, BCS["radiative"], seed=100 + i)
+        st, base = _state(c, 100 + i)
+        states[run.admit(c, st, base)] = st
+    first = next(iter(states))
+    run.engine.retire(first)
+    states.pop(first)
+    eng = run.engine
+    want_bytes = sum(9 * 4 * st["u"].size for st in states.values())
+    assert eng.image_bytes() == want_bytes
+    img = np.zeros(want_bytes // 4, np.float32)
+    eng.download_image_async(img)
+    eng.synchronize()
+    views = eng.image_views(img)
+    for mid, st in states.items():
+        for k in PROGNOSTIC:
+            assert_bitwise(views[mid][k], st[k], f"{mid} {k}")
+    for mid in states:
+        for k in PROGNOSTIC:
+            views[mid][k][...] = views[mid][k] * np.float32(1.0 + 1e-3)
+    eng.upload_image_async(img)
+    eng.synchronize()
+    for mid in states:
+        got = eng.read(mid)
+        for k in PROGNOSTIC:
+            assert_bitwise(got[k], views[mid][k], f"{mid} {k} after upload")
+    with pytest.raises(KeyError):
+        eng.image_offset(first)
+    run.close()
+
+
+@pytest.mark.parametrize("graph", [True, False], ids=["graph", "eager"])
+def test_lanes_do_not_change_results(ctx, graph):
+    """Members split over parallel lanes (forked streams, one graph) reach the
+    states they reach in one lane; lanes above the member count collapse."""
+    specs = [((21, 17, 12), 3.0), ((9, 12, 7), 2.0), ((16, 14, 10), 3.5), ((12, 9, 11), 2.5),
+             ((19, 10, 9), 3.0), ((7, 7, 6), 4.0)]
+    members = []
+    for i, (shape, dt) in enumerate(specs):
+        c = _case(shape, list(BCS.values())[i % 3], seed=110 + i, dt=dt)
+        members.append((c, *_state(c, 110 + i)))
+    results = {}
+    for lanes in (1, 3, 16):
+        run = EngineRun(ctx, precision=cuda.PRECISION_FP32, graph=graph, lanes=lanes)
+        ids = [run.admit(c, st, base) for c, st, base in members]
+        run.step(2)
+        assert run.engine.lanes == min(lanes, len(members))
+        results[lanes] = [run.read(m) for m in ids]
+        run.close()
+    for lanes in (3, 16):
+        for i, (got, want) in enumerate(zip(results[lanes], results[1])):
+            for k in PROGNOSTIC:
+                assert_bitwise(got[k], want[k], f"lanes {lanes} member {i} {k}")
