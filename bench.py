@@ -406,8 +406,8 @@ def run_ours(args):
                "api": "nimbus_cuda_engine_upload_image_async + nimbus_cuda_engine_step + "
                       "nimbus_cuda_engine_download_image_async, the runs split over "
                       f"{args.e2e_groups} engines on their own streams (each engine's nine prognostic fields of "
-                      "every run in one pinned host block, one copy each way per step; uploads chained group "
-                      "after group, downloads likewise, so one group's copies overlap another's step)"}
+                      "every run in one pinned host block, one copy each way per step, stream-ordered, so one "
+                      "group's copies overlap another group's step)"}
 
     # ---- plain path: each run alone, one C-ABI call per operation ----
     plain = None
