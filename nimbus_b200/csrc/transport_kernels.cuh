@@ -85,6 +85,55 @@ __device__ __forceinline__ double mc_slope(double qm, double q0, double qp)
     return 0.0;
 }
 
+// Lane arithmetic for the FP32 face offset: one scalar stencil (float) or two
+// independent stencils at once (float2, Blackwell's paired f32x2 FMA / MUL /
+// ADD: two IEEE round-to-nearest operations per instruction).  Every operation
+// is an explicit round-to-nearest intrinsic, so the scalar and paired forms
+// run the same operation sequence and give the same bits; only the
+// reciprocals, the final quotient and the finiteness test act per lane.
+template <class V>
+struct Lanes;
+
+template <>
+struct Lanes<float>
+{
+    static __device__ __forceinline__ float splat(float x) { return x; }
+    static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+    static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+    static __device__ __forceinline__ float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+    static __device__ __forceinline__ float maxf(float a, float b) { return fmaxf(a, b); }
+    static __device__ __forceinline__ float absf(float a) { return fabsf(a); }
+    static __device__ __forceinline__ float rcp(float a) { return __fdividef(1.0f, a); }
+    static __device__ __forceinline__ float div(float a, float b) { return __fdividef(a, b); }
+    static __device__ __forceinline__ float finite_or_zero(float a) { return isfinite(a) ? a : 0.0f; }
+};
+
+template <>
+struct Lanes<float2>
+{
+    static __device__ __forceinline__ float2 splat(float x) { return make_float2(x, x); }
+    static __device__ __forceinline__ float2 add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+    static __device__ __forceinline__ float2 mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+    static __device__ __forceinline__ float2 fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+    static __device__ __forceinline__ float2 maxf(float2 a, float2 b)
+    {
+        return make_float2(fmaxf(a.x, b.x), fmaxf(a.y, b.y));
+    }
+    static __device__ __forceinline__ float2 absf(float2 a) { return make_float2(fabsf(a.x), fabsf(a.y)); }
+    static __device__ __forceinline__ float2 rcp(float2 a)
+    {
+        return make_float2(__fdividef(1.0f, a.x), __fdividef(1.0f, a.y));
+    }
+    static __device__ __forceinline__ float2 div(float2 a, float2 b)
+    {
+        return make_float2(__fdividef(a.x, b.x), __fdividef(a.y, b.y));
+    }
+    static __device__ __forceinline__ float2 finite_or_zero(float2 a)
+    {
+        return make_float2(isfinite(a.x) ? a.x : 0.0f, isfinite(a.y) ? a.y : 0.0f);
+    }
+};
+
 // FP32 face offset from the donor value c (face = c + offset): WENO5-JS on
 // the stencil normalised by its largest magnitude, as the reference's FP32
 // GPU form normalises it (weno5_face_offset_fp32,
@@ -95,30 +144,43 @@ __device__ __forceinline__ double mc_slope(double qm, double q0, double qp)
 // d_k / (eps + beta_k)^2 are formed directly from approximate reciprocals
 // instead of the reference's min-normalised ratios: the same weights to FP32
 // rounding in about half the instructions.  A non-finite result falls back to
-// the donor value (offset 0).
+// the donor value (offset 0).  V = float2 evaluates two stencils at once.
+template <class V>
+__device__ __forceinline__ V weno5_offset_lanes(V a, V b, V c, V d, V e)
+{
+    using L = Lanes<V>;
+    const V magnitude = L::maxf(L::maxf(L::maxf(L::absf(a), L::absf(b)), L::maxf(L::absf(c), L::absf(d))),
+                                L::absf(e));
+    const V scale = L::maxf(magnitude, L::splat(1e-20f));
+    const V inv = L::rcp(scale);
+    const V m1 = L::splat(-1.0f);
+    const V ac = L::mul(L::fma(c, m1, a), inv), bc = L::mul(L::fma(c, m1, b), inv);
+    const V dc = L::mul(L::fma(c, m1, d), inv), ec = L::mul(L::fma(c, m1, e), inv);
+    const V p0 = L::fma(ac, L::splat(1.0f / 3.0f), L::mul(bc, L::splat(-7.0f / 6.0f)));
+    const V p1 = L::fma(dc, L::splat(1.0f / 3.0f), L::mul(bc, L::splat(-1.0f / 6.0f)));
+    const V p2 = L::fma(dc, L::splat(5.0f / 6.0f), L::mul(ec, L::splat(-1.0f / 6.0f)));
+    const V s0a = L::fma(bc, L::splat(-2.0f), ac), s0b = L::fma(bc, L::splat(-4.0f), ac);
+    const V s1a = L::add(bc, dc), s1b = L::fma(dc, m1, bc);
+    const V s2a = L::fma(dc, L::splat(-2.0f), ec), s2b = L::fma(dc, L::splat(-4.0f), ec);
+    const V k13 = L::splat(13.0f / 12.0f), quarter = L::splat(0.25f);
+    const V b0 = L::fma(L::mul(s0a, k13), s0a, L::mul(L::mul(s0b, quarter), s0b));
+    const V b1 = L::fma(L::mul(s1a, k13), s1a, L::mul(L::mul(s1b, quarter), s1b));
+    const V b2 = L::fma(L::mul(s2a, k13), s2a, L::mul(L::mul(s2b, quarter), s2b));
+    const V relative = L::mul(magnitude, inv);
+    const V flo = L::mul(L::splat(1e-20f), inv);
+    const V epsilon = L::fma(L::mul(relative, L::splat(1e-6f)), relative, L::mul(flo, flo));
+    const V r0 = L::rcp(L::add(epsilon, b0)), r1 = L::rcp(L::add(epsilon, b1)), r2 = L::rcp(L::add(epsilon, b2));
+    const V a0 = L::mul(L::mul(r0, L::splat(0.1f)), r0);
+    const V a1 = L::mul(L::mul(r1, L::splat(0.6f)), r1);
+    const V a2 = L::mul(L::mul(r2, L::splat(0.3f)), r2);
+    const V num = L::fma(a2, p2, L::fma(a1, p1, L::mul(a0, p0)));
+    const V den = L::add(L::add(a0, a1), a2);
+    return L::finite_or_zero(L::mul(scale, L::div(num, den)));
+}
+
 __device__ __forceinline__ float weno5_offset_f32(float a, float b, float c, float d, float e)
 {
-    const float magnitude = fmaxf(fmaxf(fmaxf(fabsf(a), fabsf(b)), fmaxf(fabsf(c), fabsf(d))), fabsf(e));
-    const float scale = fmaxf(magnitude, 1e-20f);
-    const float inv = __fdividef(1.0f, scale);
-    const float ac = (a - c) * inv, bc = (b - c) * inv, dc = (d - c) * inv, ec = (e - c) * inv;
-    const float p0 = (1.0f / 3.0f) * ac - (7.0f / 6.0f) * bc;
-    const float p1 = -(1.0f / 6.0f) * bc + (1.0f / 3.0f) * dc;
-    const float p2 = (5.0f / 6.0f) * dc - (1.0f / 6.0f) * ec;
-    const float s0a = ac - 2.0f * bc, s0b = ac - 4.0f * bc;
-    const float s1a = bc + dc, s1b = bc - dc;
-    const float s2a = ec - 2.0f * dc, s2b = ec - 4.0f * dc;
-    const float b0 = (13.0f / 12.0f) * s0a * s0a + 0.25f * s0b * s0b;
-    const float b1 = (13.0f / 12.0f) * s1a * s1a + 0.25f * s1b * s1b;
-    const float b2 = (13.0f / 12.0f) * s2a * s2a + 0.25f * s2b * s2b;
-    const float relative = magnitude * inv;
-    const float flo = 1e-20f * inv;
-    const float epsilon = 1e-6f * relative * relative + flo * flo;
-    const float r0 = __fdividef(1.0f, epsilon + b0), r1 = __fdividef(1.0f, epsilon + b1);
-    const float r2 = __fdividef(1.0f, epsilon + b2);
-    const float a0 = 0.1f * r0 * r0, a1 = 0.6f * r1 * r1, a2 = 0.3f * r2 * r2;
-    const float offset = scale * __fdividef(a0 * p0 + a1 * p1 + a2 * p2, a0 + a1 + a2);
-    return isfinite(offset) ? offset : 0.0f;
+    return weno5_offset_lanes<float>(a, b, c, d, e);
 }
 
 __device__ __forceinline__ float mc_slope_f32(float qm, float q0, float qp)
@@ -203,6 +265,29 @@ __device__ __forceinline__ float stencil_flux(const float* __restrict__ q, const
     }
 }
 
+// FP32 face fluxes of two scalars on one stencil (same donor, same mass
+// flux): the WENO5 arithmetic of both in paired f32x2 instructions, with the
+// same bits as two stencil_flux<true> calls.
+__device__ __forceinline__ float2 stencil_flux_pair(const float* __restrict__ qa, const float* __restrict__ qb,
+                                                    const FaceStencil& f, float mflux)
+{
+    const float2 q0 = make_float2(qa[f.o[2]], qb[f.o[2]]);
+    float2 offset;
+    if (f.weno)
+        offset = weno5_offset_lanes<float2>(make_float2(qa[f.o[0]], qb[f.o[0]]), make_float2(qa[f.o[1]], qb[f.o[1]]),
+                                            q0, make_float2(qa[f.o[3]], qb[f.o[3]]),
+                                            make_float2(qa[f.o[4]], qb[f.o[4]]));
+    else
+    {
+        const float h = f.pos ? 0.5f : -0.5f;
+        const float sa = f.slope ? mc_slope_f32(qa[f.o[0]], q0.x, qa[f.o[3]]) : 0.0f;
+        const float sb = f.slope ? mc_slope_f32(qb[f.o[0]], q0.y, qb[f.o[3]]) : 0.0f;
+        offset = make_float2(h * sa, h * sb);
+    }
+    const float2 m = make_float2(mflux, mflux);
+    return __ffma2_rn(m, q0, __fmul2_rn(m, offset));
+}
+
 // Face fluxes owned by cell c (its +x, +y and +z faces) for every scalar:
 // the cell's index, mass fluxes and face stencils are formed once and the
 // scalars follow.  kFp32 selects the FP32 form, otherwise FP64 face values
@@ -223,7 +308,48 @@ __device__ __forceinline__ void transport_faces_cell(const TransportParams& T, i
     const FaceStencil sx = face_stencil(c - i * d.sx(), d.sx(), i, d.nx, fx >= 0.0f, T.weno);
     const FaceStencil sy = face_stencil(c - j * d.sy(), d.sy(), j, d.ny, fy >= 0.0f, T.weno);
     const FaceStencil sz = face_stencil(c - k, 1, top ? k - 1 : k, d.nz, fz >= 0.0f, T.weno);
-    for (int s = 0; s < scalars; ++s)
+    int s = 0;
+    if constexpr (kFp32)
+    {
+        for (; s + 1 < scalars; s += 2)
+        {
+            const float* __restrict__ qa = q_of(s);
+            const float* __restrict__ qb = q_of(s + 1);
+            float* __restrict__ sfx = sf + (size_t)s * 3 * n;
+            float* __restrict__ sfy = sfx + n;
+            float* __restrict__ sfz = sfy + n;
+            float* __restrict__ tfx = sfz + n;  // scalar s + 1
+            float* __restrict__ tfy = tfx + n;
+            float* __restrict__ tfz = tfy + n;
+            if (hx)
+            {
+                const float2 r = stencil_flux_pair(qa, qb, sx, fx);
+                sfx[c] = r.x;
+                tfx[c] = r.y;
+            }
+            if (hy)
+            {
+                const float2 r = stencil_flux_pair(qa, qb, sy, fy);
+                sfy[c] = r.x;
+                tfy[c] = r.y;
+            }
+            if (hz)
+            {
+                if (top)
+                {
+                    sfz[c] = fz * qa[c];
+                    tfz[c] = fz * qb[c];
+                }
+                else
+                {
+                    const float2 r = stencil_flux_pair(qa, qb, sz, fz);
+                    sfz[c] = r.x;
+                    tfz[c] = r.y;
+                }
+            }
+        }
+    }
+    for (; s < scalars; ++s)
     {
         const float* __restrict__ q = q_of(s);
         float* __restrict__ sfx = sf + (size_t)s * 3 * n;

@@ -347,6 +347,28 @@ def test_fp32_transport_tracks_fp64(ctx32, path):
             assert (a >= -1e-12).all(), name  # positive definite
 
 
+def test_fp32_paired_faces_equal_single_faces(ctx32):
+    """The FP32 faces evaluate scalars two at a time in paired f32x2
+    instructions; a scalar gets the same bits whether it is paired (either
+    lane) or evaluated alone."""
+    g = np.load(GOLDEN[0])
+    st = _state(g)
+    grid = tuple(g["grid"])
+
+    def run(names):
+        qs = [st[k].copy() for k in names]
+        ctx32.check(ctx32.scalar_transport(cuda.transport_args(
+            qs, qs, [1] * len(qs), g["out_rho"], g["out_rho_begin"], g["out_mfx"], g["out_mfy"], g["out_mfz"],
+            float(g["dt_large"]), grid, weno=True, top_open=int(g["bc"][5]) == 2)))
+        return dict(zip(names, qs))
+
+    runs = [run(("qv", "qc", "qr")), run(("qr", "qv", "qc")), run(("qc", "qr", "qv"))]
+    for k in ("qv", "qc", "qr"):
+        alone = run((k,))[k]
+        for r in runs:
+            assert np.array_equal(r[k].view(np.uint32), alone.view(np.uint32)), k
+
+
 @pytest.mark.parametrize("scale", [1e-30, 1e-10, 1e10, 1e30])
 def test_fp32_transport_across_scales(ctx32, scale):
     """Fields scaled anywhere from 1e-30 to 1e30 stay finite and track the
