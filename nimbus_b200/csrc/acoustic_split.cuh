@@ -155,11 +155,54 @@ static __global__ void __launch_bounds__(256) split_continuity_eos_kernel(
 
 // Momentum forward Euler for the faces of cell c.  Face c reads only its own
 // old velocity, so u_out may alias u (in-place update).
+// Stores the new face velocities of cell c, with the vertical closure of its
+// column when fuse_vertical asks for it (see momentum_cell).  (Handing the
+// top values to the cell above through a warp shuffle, so that every lane
+// stores its own cell, measured slower than these scattered stores.)
+__device__ __forceinline__ void momentum_store(const Dims& d, int i, int j, int k, int c, int fuse_vertical, float un,
+                                               float vn, float wn, float* u_out, float* v_out, float* w_out)
+{
+    if ((fuse_vertical & 1) && i >= 1 && i <= d.nx - 3 && j >= 1 && j <= d.ny - 3)
+    {
+        if (k == d.nz - 1) return;  // written by the cell below
+        if (k == 0 && (fuse_vertical & 2))
+        {
+            un = 0.0f;
+            vn = 0.0f;
+        }
+        if (k == d.nz - 2)
+        {
+            u_out[c + 1] = un;
+            v_out[c + 1] = vn;
+            w_out[c + 1] = (fuse_vertical & 4) ? wn : 0.0f;
+        }
+    }
+    u_out[c] = un;
+    v_out[c] = vn;
+    w_out[c] = wn;
+}
+
+// fuse_vertical (kFuse* bits): the momentum pass also applies the vertical
+// closure (bc_vertical_column) to the columns no lateral closure writes
+// (1 <= i <= nx-3, 1 <= j <= ny-3): the no-slip bottom zeros u and v at k = 0,
+// the cell at k = nz-2 writes its new u, v and w (or 0 under a rigid top)
+// into level nz-1 as well, and the cell at nz-1 does not store.  The lateral
+// closures that run in between neither write nor depend on those columns'
+// levels 0 and nz-1 for any value that survives the closure of their own
+// columns, so the state is the one the separate closure pass gives.
+enum : int
+{
+    kFuseVertical = 1,
+    kFuseNoSlipBottom = 2,
+    kFuseOpenTop = 4
+};
+
 template <class Policy>
 __device__ __forceinline__ void momentum_cell(const FusedParams& P, const float* __restrict__ rho,
                                               const float* __restrict__ p, const double* __restrict__ p0,
                                               const float2* __restrict__ dp0_split, const float* u, const float* v,
-                                              const float* w, float* u_out, float* v_out, float* w_out, int c)
+                                              const float* w, float* u_out, float* v_out, float* w_out, int c,
+                                              int fuse_vertical = 0)
 {
     using real = typename Policy::real;
     const Dims d = P.d;
@@ -188,9 +231,11 @@ __device__ __forceinline__ void momentum_cell(const FusedParams& P, const float*
             dv = (float)finite_or_zero(-((double)py - pcd) * P.inv_dy / safe_rho(rho_y));
             dw = (float)finite_or_zero(-((((double)pz - pcd) * P.inv_dz) - dp0_dz) / safe_rho(rho_z));
         }
-        u_out[c] = clamp_value((float)((double)uc + (double)du * P.dt_small), 0.0f, -P.wind_h, P.wind_h);
-        v_out[c] = clamp_value((float)((double)vc + (double)dv * P.dt_small), 0.0f, -P.wind_h, P.wind_h);
-        w_out[c] = clamp_value((float)((double)wc + (double)dw * P.dt_small), 0.0f, -P.wind_v, P.wind_v);
+        momentum_store(d, i, j, k, c, fuse_vertical,
+                       clamp_value((float)((double)uc + (double)du * P.dt_small), 0.0f, -P.wind_h, P.wind_h),
+                       clamp_value((float)((double)vc + (double)dv * P.dt_small), 0.0f, -P.wind_h, P.wind_h),
+                       clamp_value((float)((double)wc + (double)dw * P.dt_small), 0.0f, -P.wind_v, P.wind_v), u_out,
+                       v_out, w_out);
     }
     else
     {
@@ -212,9 +257,9 @@ __device__ __forceinline__ void momentum_cell(const FusedParams& P, const float*
             dw = isfinite(cz) ? cz : 0.0f;
         }
         const float dt = P.dt_f;
-        u_out[c] = clamp_value(__fmaf_rn(du, dt, uc), 0.0f, -P.wind_h, P.wind_h);
-        v_out[c] = clamp_value(__fmaf_rn(dv, dt, vc), 0.0f, -P.wind_h, P.wind_h);
-        w_out[c] = clamp_value(__fmaf_rn(dw, dt, wc), 0.0f, -P.wind_v, P.wind_v);
+        momentum_store(d, i, j, k, c, fuse_vertical, clamp_value(__fmaf_rn(du, dt, uc), 0.0f, -P.wind_h, P.wind_h),
+                       clamp_value(__fmaf_rn(dv, dt, vc), 0.0f, -P.wind_h, P.wind_h),
+                       clamp_value(__fmaf_rn(dw, dt, wc), 0.0f, -P.wind_v, P.wind_v), u_out, v_out, w_out);
     }
 }
 

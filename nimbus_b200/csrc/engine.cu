@@ -178,6 +178,7 @@ void fill_params(EngineMember& M, const nimbus_member_desc* a)
     M.items[kItemRowsSN] = a->nx * a->nz;
     M.items[kItemColumns] = a->nx * a->ny;
     M.items[kItemHistory] = (a->ny + a->nx) * a->nz;
+    M.items[kItemPerimeter] = 3 * a->nx + 3 * (a->ny - 3);
 }
 
 }  // namespace

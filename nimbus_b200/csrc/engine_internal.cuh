@@ -133,6 +133,7 @@ int enqueue_step(nimbus_engine* e, int lane, cudaStream_t st)
     const long long* psn = prefix_of(e, L, kItemRowsSN);
     const long long* pcol = prefix_of(e, L, kItemColumns);
     const long long* phist = prefix_of(e, L, kItemHistory);
+    const long long* pper = prefix_of(e, L, kItemPerimeter);
     const long long cells = tiles_of(e, L, kItemCells, n);
 
     // Heun slow step (prepare_slow_rk2_tendencies + apply_slow_tendencies).
@@ -160,8 +161,8 @@ int enqueue_step(nimbus_engine* e, int lane, cudaStream_t st)
                       tiles_of(e, L, kItemRowsWE, a), si, 0);
         ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_bc_sn_kernel, tiles_of(e, L, kItemRowsSN, a), 1, T, psn,
                       tiles_of(e, L, kItemRowsSN, a), si, 0);
-        ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_bc_vertical_kernel, tiles_of(e, L, kItemColumns, a), 1, T,
-                      pcol, tiles_of(e, L, kItemColumns, a));
+        ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_bc_vertical_perimeter_kernel,
+                      tiles_of(e, L, kItemPerimeter, a), 1, T, pper, tiles_of(e, L, kItemPerimeter, a));
     }
     engine_swap_kernel<<<(n + 127) / 128, 128, 0, st>>>(T, n, 0);
     ++count;

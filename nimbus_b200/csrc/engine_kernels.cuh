@@ -33,12 +33,13 @@ enum ItemKind
     kItemRowsSN,     // nx*nz south/north boundary rows
     kItemColumns,    // nx*ny columns
     kItemHistory,    // (ny + nx)*nz KW78 history slots
+    kItemPerimeter,  // 3 nx + 3 (ny - 3) columns the lateral closures write
     kItemKinds
 };
 
 constexpr int kEngineScalars = 4;  // theta, qv, qc, qr
 
-struct EngineMember
+struct __align__(16) EngineMember
 {
     // Prognostic state and the two ping-pong partners (swapped on the device
     // at the end of the loop / after Kessler, see engine_swap_kernel).
@@ -75,9 +76,10 @@ __device__ __forceinline__ float* engine_scalar_out(const EngineMember& M, int s
     return s == 0 ? M.theta : (s == 1 ? M.qv : (s == 2 ? M.qc : M.qr));
 }
 
-// Items per thread in a tile: a tile is kTileItems = 4 * blockDim.x
-// consecutive items of one member, so the member lookup and its pointers are
-// loaded once for four items and each load instruction stays coalesced.
+// Items per thread in a tile: a tile is kItemsPerThread * blockDim.x
+// consecutive items of one member (one item per thread measured fastest:
+// more items per thread cost more registers than the shared member lookup
+// saves).
 constexpr int kItemsPerThread = 1;
 
 // Calls fn(member, item) for every item of the first tiles of a kind.
@@ -178,6 +180,33 @@ static __global__ void __launch_bounds__(256) engine_bc_vertical_kernel(const En
     });
 }
 
+// The vertical closure inside the acoustic loop, for the columns the lateral
+// closures write (i in {0, nx-2, nx-1} or j in {0, ny-2, ny-1}); the momentum
+// kernel closes every other column itself (momentum_cell, fuse_vertical).
+// Item q: rows j = 0, ny-2, ny-1 for every i first, then i = 0, nx-2, nx-1
+// for j = 1 .. ny-3.
+static __global__ void __launch_bounds__(256) engine_bc_vertical_perimeter_kernel(
+    const EngineMember* __restrict__ table, const long long* __restrict__ prefix, long long tiles)
+{
+    for_member_items(table, prefix, tiles, kItemPerimeter, [&](const EngineMember& M, int q) {
+        const int nx = M.B.d.nx, ny = M.B.d.ny;
+        int i, j;
+        if (q < 3 * nx)
+        {
+            const int row = q / nx;
+            i = q - row * nx;
+            j = row == 0 ? 0 : ny - 3 + row;
+        }
+        else
+        {
+            const int r = q - 3 * nx, side = r % 3;
+            j = 1 + r / 3;
+            i = side == 0 ? 0 : nx - 3 + side;
+        }
+        bc_vertical_column(M.B, M.u, M.v, M.w, i * ny + j);
+    });
+}
+
 static __global__ void __launch_bounds__(256) engine_seed_kernel(const EngineMember* __restrict__ table,
                                                           const long long* __restrict__ prefix, long long tiles)
 {
@@ -209,7 +238,10 @@ static __global__ void __launch_bounds__(256) engine_momentum_kernel(const Engin
                                                               int s)
 {
     for_member_items(table, prefix, tiles, kItemCells, [&](const EngineMember& M, int c) {
-        momentum_cell<Policy>(M.F, engine_density(M, s, true), M.p, M.p0, M.dp0, M.u, M.v, M.w, M.u, M.v, M.w, c);
+        const int vertical = kFuseVertical | (M.B.bottom == kBottomNoSlip ? kFuseNoSlipBottom : 0) |
+                             (M.B.top == kTopOpen ? kFuseOpenTop : 0);
+        momentum_cell<Policy>(M.F, engine_density(M, s, true), M.p, M.p0, M.dp0, M.u, M.v, M.w, M.u, M.v, M.w, c,
+                              vertical);
     });
 }
 

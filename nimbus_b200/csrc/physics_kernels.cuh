@@ -239,9 +239,15 @@ __device__ __forceinline__ void kessler_cell(const KesslerParams& K, float* __re
                 double r = 0.0;
                 if (isfinite(dT) && isfinite(pv))
                 {
-                    const double ps = kclamp(pv, 100.0, 200000.0);
-                    r = dT * pow(kKP0 / ps, kKRd / kKCp);
-                    if (!isfinite(r)) r = 0.0;
+                    // The factor is finite and positive (ps is clamped), so a
+                    // zero tendency keeps its own signed zero without it.
+                    if (dT == 0.0) r = dT;
+                    else
+                    {
+                        const double ps = kclamp(pv, 100.0, 200000.0);
+                        r = dT * pow(kKP0 / ps, kKRd / kKCp);
+                        if (!isfinite(r)) r = 0.0;
+                    }
                 }
                 dth = (float)r;
             }
