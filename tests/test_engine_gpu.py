@@ -303,3 +303,38 @@ def test_lanes_do_not_change_results(ctx, graph):
         for i, (got, want) in enumerate(zip(results[lanes], results[1])):
             for k in PROGNOSTIC:
                 assert_bitwise(got[k], want[k], f"lanes {lanes} member {i} {k}")
+
+
+def test_fp32_form_error_against_fp64_is_the_reference_forms(ctx):
+    """Several large steps of a cloudy, radiative-boundary run: the FP32 form
+    and the reference-precision form (FP32 storage, the reference's own
+    arithmetic) both against the FP64 restatement of the same step.  Per
+    field, the FP32 form's relative L2 error stays within 1.5x the reference
+    form's (plus a 1e-7 floor): reduced-precision arithmetic adds no error
+    beyond what FP32 storage already costs."""
+    case = _case((28, 26, 20), BCS["radiative"], seed=130, dt=3.0)
+    st, base = _state(case, 130)
+    n_sub, steps = 6, 12
+    o64 = oracle.Restatement("f64")
+    ref = {k: v.astype(np.float64) for k, v in st.items()}
+    for _ in range(steps):
+        o64.large_step(ref, base, (case.dx, case.dy, case.dz), case.dt, n_sub, case.bc)
+    theta0 = base["theta0"][None, None, :]
+    errors = {}
+    for prec in (cuda.PRECISION_FP32, cuda.PRECISION_REFERENCE):
+        run = EngineRun(ctx, precision=prec)
+        mid = run.admit(case, st, base, n_substeps=n_sub)
+        run.step(steps)
+        got = run.read(mid)
+        run.close()
+        err = {}
+        for k in ("u", "v", "w", "theta", "qv", "qc", "p", "rho"):
+            a, b = got[k].astype(np.float64), ref[k]
+            if k == "theta":
+                a, b = a - theta0, b - theta0
+            den = max(float(np.linalg.norm(b)), 1e-30)
+            err[k] = float(np.linalg.norm(a - b)) / den
+        errors[prec] = err
+    for k, e32 in errors[cuda.PRECISION_FP32].items():
+        eref = errors[cuda.PRECISION_REFERENCE][k]
+        assert np.isfinite(e32) and e32 <= 1.5 * eref + 1e-7, (k, e32, eref)
