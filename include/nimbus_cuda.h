@@ -432,6 +432,11 @@ typedef struct nimbus_eos_args
     double gamma;
     int memory;
     void* stream;
+    /* Optional FP64 base pressure per level (nz; host or device as `memory`).
+     * Under NIMBUS_PRECISION_FP32 the projection is then evaluated around it
+     * in the compensated FP32 form of the acoustic substeps (within about
+     * half an FP32 ulp of the FP64 value); NULL keeps the FP64 evaluation. */
+    const double* p0_base;
 } nimbus_eos_args;
 
 nimbus_status nimbus_cuda_eos_projection(nimbus_cuda_context* ctx, const nimbus_eos_args* a);

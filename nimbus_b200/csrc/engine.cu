@@ -169,8 +169,10 @@ void fill_params(EngineMember& M, const nimbus_member_desc* a)
     K.c_accr = 2.2;
     K.evap_eff = 1.0;
     K.vt_max = 20.0;
+    finish_fp32(K);
 
     M.gamma = gamma;
+    M.eos_series = eos_series(gamma);
     M.n_substeps = a->n_substeps;
     M.microphysics = a->microphysics;
     M.items[kItemCells] = a->nx * a->ny * a->nz;
@@ -458,9 +460,14 @@ int nimbus_engine_detail::launch_microphysics(nimbus_engine* e, cudaStream_t st,
     if (tiles <= 0) return 0;
     nimbus_cuda_context* ctx = e->ctx;
     LaunchTimer t(ctx, st, NIMBUS_KERNEL_MICROPHYSICS);
-    engine_microphysics_eos_kernel<<<engine_grid(e, reinterpret_cast<const void*>(engine_microphysics_eos_kernel),
-                                                 tiles),
-                                     kEngineBlock, 0, st>>>(table, prefix, tiles);
+    if (ctx->precision == NIMBUS_PRECISION_FP32)
+        engine_microphysics_eos_kernel<true>
+            <<<engine_grid(e, reinterpret_cast<const void*>(engine_microphysics_eos_kernel<true>), tiles),
+               kEngineBlock, 0, st>>>(table, prefix, tiles);
+    else
+        engine_microphysics_eos_kernel<false>
+            <<<engine_grid(e, reinterpret_cast<const void*>(engine_microphysics_eos_kernel<false>), tiles),
+               kEngineBlock, 0, st>>>(table, prefix, tiles);
     return 1;
 }
 

@@ -60,6 +60,7 @@ struct __align__(16) EngineMember
     SlowParams S;
     KesslerParams K;
     double gamma;
+    EosSeries eos_series;  // FP32 EOS coefficients binom(gamma, n)
     int n_substeps;
     int microphysics;
     int items[kItemKinds];
@@ -356,6 +357,7 @@ static __global__ void __launch_bounds__(256) engine_transport_update_kernel(con
 // pressure is formed from the applied state while it is still in registers
 // and written to the member's candidate buffer; engine_swap_kernel publishes
 // it by exchanging p and the candidate unless the projection was refused.
+template <bool kFp32>
 static __global__ void __launch_bounds__(256, 4) engine_microphysics_eos_kernel(const EngineMember* __restrict__ table,
                                                                              const long long* __restrict__ prefix,
                                                                              long long tiles)
@@ -365,13 +367,24 @@ static __global__ void __launch_bounds__(256, 4) engine_microphysics_eos_kernel(
         float4 s;
         const float po = M.p[c];
         if (M.microphysics)
-            kessler_cell<true>(M.K, M.theta, M.qv, M.qc, M.qr, M.p, M.rho, M.qr_alt, nullptr, nullptr, nullptr,
-                               nullptr, c, &s);
+        {
+            if constexpr (kFp32)
+                kessler_cell_f32<true>(M.K, M.theta, M.qv, M.qc, M.qr, M.p, M.rho, M.qr_alt, nullptr, nullptr,
+                                       nullptr, nullptr, c, &s);
+            else
+                kessler_cell<true>(M.K, M.theta, M.qv, M.qc, M.qr, M.p, M.rho, M.qr_alt, nullptr, nullptr, nullptr,
+                                   nullptr, c, &s);
+        }
         else
             s = make_float4(M.theta[c], M.qv[c], M.qc[c], M.qr[c]);
         float p_new;
-        if (eos_candidate_value(M.K.d, c, M.rho[c], s.x, M.gamma, true, po, s.y, s.z, s.w, p_new, flags))
-            M.eos[c] = p_new;
+        bool ok;
+        if constexpr (kFp32)
+            ok = eos_candidate_value_f32(M.K.d, c, c % M.K.d.nz, M.rho[c], s.x, M.eos0, M.eos_series, M.gamma, true,
+                                         po, s.y, s.z, s.w, p_new, flags);
+        else
+            ok = eos_candidate_value(M.K.d, c, M.rho[c], s.x, M.gamma, true, po, s.y, s.z, s.w, p_new, flags);
+        if (ok) M.eos[c] = p_new;
         if (flags) atomicOr(M.status, flags);
     });
 }

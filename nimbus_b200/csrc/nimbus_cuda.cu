@@ -504,6 +504,7 @@ KesslerParams kessler_params(const nimbus_kessler_args* a)
     K.c_accr = 2.2;
     K.evap_eff = 1.0;
     K.vt_max = 20.0;
+    finish_fp32(K);
     return K;
 }
 
@@ -516,16 +517,27 @@ nimbus_status run_kessler_device(nimbus_cuda_context* ctx, cudaStream_t st, cons
     const size_t n = static_cast<size_t>(K.d.cells());
     const int blocks = grid_for(ctx, static_cast<long long>(n));
     LaunchTimer t(ctx, st, NIMBUS_KERNEL_MICROPHYSICS);
+    const bool fp32 = ctx->precision == NIMBUS_PRECISION_FP32;
     if (!step)
     {
-        kessler_kernel<false><<<blocks, kThreads, 0, st>>>(K, theta, qv, qc, qr, p, rho, nullptr, dth, dqv, dqc, dqr);
+        if (fp32)
+            kessler_f32_kernel<false><<<blocks, kThreads, 0, st>>>(K, theta, qv, qc, qr, p, rho, nullptr, dth, dqv, dqc,
+                                                                  dqr);
+        else
+            kessler_kernel<false><<<blocks, kThreads, 0, st>>>(K, theta, qv, qc, qr, p, rho, nullptr, dth, dqv, dqc,
+                                                              dqr);
         ctx->launches += 1;
     }
     else
     {
         float* qr_new = nullptr;
         NB_TRY(ensure(ctx, kQrAlt, n, &qr_new));
-        kessler_kernel<true><<<blocks, kThreads, 0, st>>>(K, theta, qv, qc, qr, p, rho, qr_new, dth, dqv, dqc, dqr);
+        if (fp32)
+            kessler_f32_kernel<true><<<blocks, kThreads, 0, st>>>(K, theta, qv, qc, qr, p, rho, qr_new, dth, dqv, dqc,
+                                                                 dqr);
+        else
+            kessler_kernel<true><<<blocks, kThreads, 0, st>>>(K, theta, qv, qc, qr, p, rho, qr_new, dth, dqv, dqc,
+                                                             dqr);
         NB_CUDA(ctx, cudaMemcpyAsync(qr, qr_new, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
         ctx->launches += 1;
     }
@@ -588,15 +600,32 @@ nimbus_status kessler_entry(nimbus_cuda_context* ctx, const nimbus_kessler_args*
 
 nimbus_status run_eos_device(nimbus_cuda_context* ctx, cudaStream_t st, const nimbus_eos_args* a, float* p,
                              const float* rho, const float* theta, const float* qv, const float* qc,
-                             const float* qr)
+                             const float* qr, const double* p0_device)
 {
     const Dims d = make_dims(a->nx, a->ny, a->nz);
     const long long n = d.cells();
     float* candidate = nullptr;
     NB_TRY(ensure(ctx, kEosCandidate, static_cast<size_t>(n), &candidate));
+    // The FP32 form evaluates the EOS around the base pressure profile when
+    // the caller gives it (the compensated form of the acoustic substeps).
+    const bool fp32 = ctx->precision == NIMBUS_PRECISION_FP32 && p0_device != nullptr;
+    float4* eos0 = nullptr;
+    if (fp32)
+    {
+        float2* dp0 = nullptr;
+        NB_TRY(ensure(ctx, kDp0, static_cast<size_t>(d.nz), &dp0));
+        NB_TRY(ensure(ctx, kEos0, static_cast<size_t>(d.nz), &eos0));
+        level_base_kernel<<<(d.nz + 127) / 128, 128, 0, st>>>(p0_device, d.nz, a->gamma, dp0, eos0);
+        ctx->launches += 1;
+    }
     LaunchTimer t(ctx, st, NIMBUS_KERNEL_MICROPHYSICS);
-    eos_candidate_kernel<<<grid_for(ctx, n), kThreads, 0, st>>>(d, rho, theta, p, qv, qc, qr, a->gamma, candidate,
-                                                                 ctx->status);
+    if (fp32)
+        eos_candidate_f32_kernel<<<grid_for(ctx, n), kThreads, 0, st>>>(d, rho, theta, p, qv, qc, qr, eos0,
+                                                                         eos_series(a->gamma), a->gamma, candidate,
+                                                                         ctx->status);
+    else
+        eos_candidate_kernel<<<grid_for(ctx, n), kThreads, 0, st>>>(d, rho, theta, p, qv, qc, qr, a->gamma,
+                                                                     candidate, ctx->status);
     eos_publish_kernel<<<grid_for(ctx, (n + 3) / 4), kThreads, 0, st>>>(n, candidate, p, ctx->status);
     ctx->launches += 2;
     NB_CUDA(ctx, cudaGetLastError());
@@ -737,7 +766,7 @@ nimbus_status nimbus_cuda_eos_projection(nimbus_cuda_context* ctx, const nimbus_
     if (a->memory == NIMBUS_MEMORY_DEVICE)
     {
         if (a->stream) st = static_cast<cudaStream_t>(a->stream);
-        return run_eos_device(ctx, st, a, a->p, a->rho, a->theta, a->qv, a->qc, a->qr);
+        return run_eos_device(ctx, st, a, a->p, a->rho, a->theta, a->qv, a->qc, a->qr, a->p0_base);
     }
     const size_t n = static_cast<size_t>(a->nx) * a->ny * a->nz;
     const size_t bytes = n * sizeof(float);
@@ -757,7 +786,13 @@ nimbus_status nimbus_cuda_eos_projection(nimbus_cuda_context* ctx, const nimbus_
         NB_TRY(upload(ctx, qc, a->qc, bytes));
         NB_TRY(upload(ctx, qr, a->qr, bytes));
     }
-    NB_TRY(run_eos_device(ctx, st, a, p, rho, th, qv, qc, qr));
+    double* p0 = nullptr;
+    if (a->p0_base)
+    {
+        NB_TRY(ensure(ctx, kP0, static_cast<size_t>(a->nz), &p0));
+        NB_TRY(upload(ctx, p0, a->p0_base, sizeof(double) * static_cast<size_t>(a->nz)));
+    }
+    NB_TRY(run_eos_device(ctx, st, a, p, rho, th, qv, qc, qr, p0));
     unsigned flags = 0;
     NB_TRY(read_status(ctx, st, &flags));
     if (flags & kStatusInvalidEos)

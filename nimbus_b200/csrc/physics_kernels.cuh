@@ -23,7 +23,20 @@ struct KesslerParams
     double dt;
     int i0, i1, j0, j1, k0, k1;  // cell domain
     double qc0, c_auto, c_accr, evap_eff, vt_max;
+    // FP32 form: the scalars above rounded once.
+    float dz_f, dt_f, qc0_f, c_auto_f, c_accr_f, evap_eff_f, vt_max_f;
 };
+
+__host__ __device__ inline void finish_fp32(KesslerParams& K)
+{
+    K.dz_f = (float)K.dz;
+    K.dt_f = (float)K.dt;
+    K.qc0_f = (float)K.qc0;
+    K.c_auto_f = (float)K.c_auto;
+    K.c_accr_f = (float)K.c_accr;
+    K.evap_eff_f = (float)K.evap_eff;
+    K.vt_max_f = (float)K.vt_max;
+}
 
 // Constants: microphysics_base.hpp:1073-1080, fall_speeds.hpp:60-68.
 constexpr double kKT0 = 273.15, kKLv = 2.5e6, kKCp = 1004.0, kKRv = 461.5, kKRd = 287.0, kKP0 = 100000.0;
@@ -303,6 +316,242 @@ __device__ __forceinline__ void kessler_cell(const KesslerParams& K, float* __re
     }
 }
 
+// ---- FP32 form -------------------------------------------------------------
+// The same scheme in FP32 arithmetic (the reference's GPU microphysics
+// dispatch takes FP32 parameters, src/compute/dispatch/microphysics.cpp):
+// the same clamps, branches and order, FP32 powf/expf/sqrtf, and a saturation
+// adjustment whose Newton iteration stops at a few FP32 ulps of the vapour
+// rather than at the FP64 epsilon.  Used by the FP32 precision form only.
+constexpr float kfT0 = 273.15f, kfP0 = 100000.0f;
+constexpr float kfKappa = (float)(kKRd / kKCp), kfLvCp = (float)(kKLv / kKCp);
+constexpr float kfLv2CpRv = (float)(kKLv * kKLv / (kKCp * kKRv));
+
+__device__ __forceinline__ float kfclamp(float v, float lo, float hi) { return v < lo ? lo : (hi < v ? hi : v); }
+
+__device__ __forceinline__ float kf_theta_to_temperature(float theta, float p)
+{
+    if (!isfinite(theta) || !isfinite(p)) return kfT0;
+    const float th = kfclamp(theta, 150.0f, 700.0f), ps = kfclamp(p, 100.0f, 200000.0f);
+    const float T = th * powf(ps / kfP0, kfKappa);
+    return isfinite(T) ? T : kfT0;
+}
+
+__device__ __forceinline__ float kf_qvs_water(float T, float p)
+{
+    float e = 0.0f;
+    if (isfinite(T))
+    {
+        const float tc = kfclamp(T, 150.0f, 400.0f) - kfT0;
+        const float value = 611.21f * expf((18.678f - tc / 234.5f) * tc / (257.14f + tc));
+        e = isfinite(value) ? fmaxf(0.0f, value) : 0.0f;
+    }
+    if (!isfinite(e) || !isfinite(p)) return 0.0f;
+    const float ps = kfclamp(p, 100.0f, 200000.0f);
+    return kfclamp(0.62198f * e / fmaxf(ps - e, 1.0f), 0.0f, 0.2f);
+}
+
+__device__ __forceinline__ float kf_sat_slope(float temperature, float saturation, float p)
+{
+    if (!(temperature > 150.0f && temperature < 400.0f) || !(saturation > 0.0f && saturation < 0.2f)) return 0.0f;
+    const float pressure = kfclamp(p, 100.0f, 200000.0f);
+    const float vapor = saturation * pressure / (0.62198f + saturation);
+    const float tc = temperature - kfT0;
+    const float den = 257.14f + tc;
+    const float num = (18.678f - tc / 234.5f) * tc;
+    const float num_slope = 18.678f - 2.0f * tc / 234.5f;
+    const float lps = (num_slope * den - num) / (den * den);
+    return saturation * pressure / fmaxf(pressure - vapor, 1.0f) * lps;
+}
+
+// One Newton-bisection solve of the coupled adjustment (k_saturation_adjustment
+// in FP32): sign = +1 condenses vapour, -1 evaporates cloud.
+__device__ __forceinline__ float kf_adjust(float T, float p, float qv, float qvs, float maximum, float sign)
+{
+    const float L = kfLvCp;
+    float amount = maximum;
+    if (sign * (qv - sign * maximum - kf_qvs_water(T + sign * L * maximum, p)) <= 0.0f)
+    {
+        float lower = 0.0f, upper = maximum;
+        amount = kfclamp(sign * (qv - qvs) / (1.0f + L * kf_sat_slope(T, qvs, p)), lower, upper);
+        for (int it = 0; it < 10; ++it)
+        {
+            const float ta = T + sign * L * amount;
+            const float sa = kf_qvs_water(ta, p);
+            const float value = qv - sign * amount - sa;
+            if (fabsf(value) <= 4.0f * 1.1920929e-7f * fmaxf(fmaxf(fabsf(qv), fabsf(sa)), 1.0e-12f)) break;
+            if (sign * value > 0.0f) lower = amount;
+            else upper = amount;
+            const float derivative = -1.0f - L * kf_sat_slope(ta, sa, p);
+            const float candidate = amount + sign * value / (-derivative);
+            amount = (candidate > lower && candidate < upper) ? candidate : 0.5f * (lower + upper);
+        }
+    }
+    return amount;
+}
+
+static __device__ float kf_saturation_adjustment(float T_in, float p, float& qv, float& qc)
+{
+    float T = isfinite(T_in) ? kfclamp(T_in, 150.0f, 400.0f) : kfT0;
+    qv = isfinite(qv) ? fmaxf(0.0f, qv) : 0.0f;
+    qc = isfinite(qc) ? fmaxf(0.0f, qc) : 0.0f;
+    float qvs = kf_qvs_water(T, p);
+    if (!isfinite(qvs) || qvs < 0.0f) qvs = 0.0f;
+    const float L = kfLvCp;
+    if (qv > qvs)
+    {
+        const float condensed = kf_adjust(T, p, qv, qvs, fminf(qv, fmaxf(0.0f, (400.0f - T) / L)), 1.0f);
+        qv -= condensed;
+        qc += condensed;
+        T += L * condensed;
+    }
+    else if (qv < qvs && qc > 0.0f)
+    {
+        const float evaporated = kf_adjust(T, p, qv, qvs, fminf(qc, fmaxf(0.0f, (T - 150.0f) / L)), -1.0f);
+        qc -= evaporated;
+        qv += evaporated;
+        T -= L * evaporated;
+    }
+    qc = fmaxf(0.0f, qc);
+    qv = fmaxf(0.0f, qv);
+    return T;
+}
+
+__device__ __forceinline__ float kf_sed_flux(const KesslerParams& K, float qr_raw, float rho_k)
+{
+    const float q = fmaxf(0.0f, qr_raw);
+    if (!(q > 0.0f)) return 0.0f;
+    const float fall = sqrtf((float)kFallRho / rho_k);
+    const float vt0 = (q < (float)kRainMinQ) ? 0.0f : (float)kRainA * powf(1.0e-3f * rho_k * q, (float)kRainB);
+    return fminf(vt0 * fall, K.vt_max_f) * q;
+}
+
+template <bool kApply>
+__device__ __forceinline__ void kessler_cell_f32(const KesslerParams& K, float* __restrict__ theta,
+                                                 float* __restrict__ qv, float* __restrict__ qc,
+                                                 const float* __restrict__ qr, const float* __restrict__ p,
+                                                 const float* __restrict__ rho, float* __restrict__ qr_out,
+                                                 float* __restrict__ dth_out, float* __restrict__ dqv_out,
+                                                 float* __restrict__ dqc_out, float* __restrict__ dqr_out, int c,
+                                                 float4* fresh = nullptr)
+{
+    const Dims d = K.d;
+    const float dt = K.dt_f;
+    int i, j, k;
+    decompose(d, c, i, j, k);
+    const bool inside = i >= K.i0 && i < K.i1 && j >= K.j0 && j < K.j1 && k >= K.k0 && k < K.k1;
+    float dth = 0.0f, dqv = 0.0f, dqc = 0.0f, dqr = 0.0f;
+    const float qr_c = qr[c];
+    const float th_c = theta[c], qv_c = qv[c], qc_c = qc[c];
+    if (inside && dt > 0.0f)
+    {
+        const float p_c = p[c], rho_k = rho[c];
+        const bool up_exists = k + 1 < K.k1;
+        const float qr_up = up_exists ? qr[c + 1] : 0.0f, rho_up = up_exists ? rho[c + 1] : 1.0f;
+        // Saturation adjustment.
+        float qv_adj = qv_c, qc_adj = qc_c;
+        const float temp = kf_saturation_adjustment(kf_theta_to_temperature(th_c, p_c), p_c, qv_adj, qc_adj);
+        const float dqa = qc_adj - qc_c;
+        if (dqa != 0.0f)
+        {
+            const float rate = dqa / dt;
+            dqc += rate;
+            dqv -= rate;
+            dth += kfLvCp * rate;
+        }
+        // Autoconversion + accretion, then rain evaporation.
+        float prod = 0.0f;
+        if (qc_adj > 0.0f)
+        {
+            const float factor = 1.0f / (1.0f + K.c_accr_f * dt * powf(fmaxf(qr_c, 0.0f), 0.875f));
+            const float amount = qc_adj * (1.0f - factor) + factor * K.c_auto_f * dt * fmaxf(qc_adj - K.qc0_f, 0.0f);
+            prod = kfclamp(amount, 0.0f, qc_adj) / dt;
+            dqc -= prod;
+            dqr += prod;
+        }
+        if (qr_c > 0.0f || prod > 0.0f)
+        {
+            const float qvsat = kf_qvs_water(temp, p_c);
+            if (qvsat > 0.0f && qv_adj < qvsat && rho_k > 0.0f && p_c > 0.0f)
+            {
+                const float qr_av = qr_c + prod * dt;
+                const float rcgs = 1.0e-3f * rho_k;
+                const float rain = rcgs * fmaxf(qr_av, 0.0f);
+                const float vent = (1.6f + 124.9f * powf(rain, 0.2046f)) * powf(rain, 0.525f);
+                const float resist = 2.55e8f / (p_c * qvsat) + 5.4e5f;
+                const float raw = K.evap_eff_f * (vent / resist) * ((qvsat - qv_adj) / (rcgs * qvsat));
+                const float gsat = kfLv2CpRv * qvsat / fmaxf(temp * temp, 1.0f);
+                const float bound = (qvsat - qv_adj) / (1.0f + gsat);
+                const float evap = kfclamp(raw, 0.0f, fminf(bound / dt, qr_av / dt));
+                dqv += evap;
+                dqr -= evap;
+                dth -= kfLvCp * evap;
+            }
+        }
+        // Sedimentation: lose the own fall flux, then gain the upper neighbour's.
+        if (qr_c > 0.0f) dqr -= kf_sed_flux(K, qr_c, rho_k) / K.dz_f;
+        if (up_exists && qr_up > 0.0f) dqr += (rho_up / rho_k) * kf_sed_flux(K, qr_up, rho_up) / K.dz_f;
+        // Temperature tendency to theta tendency (a zero tendency needs no factor).
+        if (isfinite(dth) && isfinite(p_c))
+        {
+            if (dth != 0.0f)
+            {
+                const float r = dth * powf(kfP0 / kfclamp(p_c, 100.0f, 200000.0f), kfKappa);
+                dth = isfinite(r) ? r : 0.0f;
+            }
+        }
+        else dth = 0.0f;
+    }
+    if (dth_out != nullptr)
+    {
+        dth_out[c] = dth;
+        dqv_out[c] = dqv;
+        dqc_out[c] = dqc;
+        dqr_out[c] = dqr;
+    }
+    if (kApply)
+    {
+        float th_new = th_c, qv_new = qv_c, qc_new = qc_c, qr_new = qr_c;
+        if (inside)
+        {
+            // step_microphysics_once's commit (microphysics_step.cpp:3026-3245).
+            auto water = [&](float q, float dq) {
+                const float raw = __fmaf_rn(isfinite(dq) ? dq : 0.0f, dt, q);
+                return !isfinite(raw) ? 0.0f : (raw < 0.0f ? 0.0f : (0.05f < raw ? 0.05f : raw));
+            };
+            qv_new = water(qv_c, dqv);
+            qc_new = water(qc_c, dqc);
+            qr_new = water(qr_c, dqr);
+            float total = (isfinite(dth) ? dth : 0.0f) * dt;
+            if (!isfinite(total)) total = 0.0f;
+            float tn = th_c + kfclamp(total, -(float)kThetaStepMax, (float)kThetaStepMax);
+            if (!isfinite(tn)) tn = isfinite(th_c) ? th_c : (float)kTheta0;
+            th_new = clamp_value(tn, (float)kTheta0, 200.0f, 700.0f);
+            theta[c] = th_new;
+            qv[c] = qv_new;
+            qc[c] = qc_new;
+        }
+        qr_out[c] = qr_new;
+        if (fresh) *fresh = make_float4(th_new, qv_new, qc_new, qr_new);
+    }
+}
+
+template <bool kApply>
+static __global__ void __launch_bounds__(256) kessler_f32_kernel(KesslerParams K, float* __restrict__ theta,
+                                                                 float* __restrict__ qv, float* __restrict__ qc,
+                                                                 const float* __restrict__ qr,
+                                                                 const float* __restrict__ p,
+                                                                 const float* __restrict__ rho,
+                                                                 float* __restrict__ qr_out,
+                                                                 float* __restrict__ dth_out,
+                                                                 float* __restrict__ dqv_out,
+                                                                 float* __restrict__ dqc_out,
+                                                                 float* __restrict__ dqr_out)
+{
+    const int n = K.d.cells();
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+        kessler_cell_f32<kApply>(K, theta, qv, qc, qr, p, rho, qr_out, dth_out, dqv_out, dqc_out, dqr_out, c);
+}
+
 template <bool kApply>
 static __global__ void __launch_bounds__(256) kessler_kernel(KesslerParams K, float* __restrict__ theta, float* __restrict__ qv,
                                                       float* __restrict__ qc, const float* __restrict__ qr,
@@ -351,6 +600,99 @@ __device__ __forceinline__ bool eos_candidate_value(const Dims& d, int c, float 
         }
     }
     return true;
+}
+
+// The binomial-series coefficients binom(gamma, n), n = 1..6, rounded once.
+struct EosSeries
+{
+    float c[6];
+};
+
+__host__ inline EosSeries eos_series(double gamma)
+{
+    EosSeries e;
+    double c = 1.0;
+    for (int n = 1; n <= 6; ++n)
+    {
+        c *= (gamma - (n - 1)) / n;
+        e.c[n - 1] = (float)c;
+    }
+    return e;
+}
+
+// FP32 form of eos_candidate_value: p = p0 (1 + d)^gamma around the level's
+// base state (eos0[k] = {p0 hi, p0 lo, b hi, b lo}, b = R_d / (p00 x0),
+// x0 = (p0 / p00)^(1/gamma)), with 1 + d = rho theta b formed exactly as a
+// hi+lo pair and the series summed to the sixth power for |d| <= 1/16 (within
+// about half an FP32 ulp of the FP64 value; larger |d| take FP64).  The same
+// refusal rules and clamp as the FP64 form.
+__device__ __forceinline__ bool eos_candidate_value_f32(const Dims& d, int c, int k, float r, float th,
+                                                        const float4* __restrict__ eos0, const EosSeries& series,
+                                                        double gamma, bool moist, float po, float q, float qc,
+                                                        float qr, float& p_new, unsigned& flags)
+{
+    bool ok = isfinite(r) && r > 0.0f && isfinite(th) && th > 0.0f;
+    float pressure = 0.0f;
+    if (ok)
+    {
+        const float4 e = eos0[k];
+        const float rt = r * th;
+        const float rt_lo = __fmaf_rn(r, th, -rt);
+        const float x = rt * e.z;
+        const float x_lo = __fmaf_rn(rt, e.z, -x) + __fmaf_rn(rt, e.w, rt_lo * e.z);
+        const float dl = (x - 1.0f) + x_lo;
+        if (fabsf(dl) <= 0.0625f)
+        {
+            float sum = series.c[5];
+            for (int n = 4; n >= 0; --n) sum = __fmaf_rn(sum, dl, series.c[n]);
+            pressure = e.x + __fmaf_rn(e.x, sum * dl, e.y);
+        }
+        else
+        {
+            const double diagnosed = kP00 * pow((double)r * kRd * (double)th / kP00, gamma);
+            ok = isfinite(diagnosed) && diagnosed > 0.0 && isfinite((float)diagnosed);
+            pressure = (float)diagnosed;
+        }
+    }
+    if (!ok)
+    {
+        flags |= kStatusInvalidEos;
+        return false;
+    }
+    p_new = clamp_value(pressure, 101325.0f, 1000.0f, 200000.0f);
+    if (moist)
+    {
+        const int ih = d.nx >= 3, jh = d.ny >= 3;
+        int i, j, kk;
+        decompose(d, c, i, j, kk);
+        if (i >= ih && i < d.nx - ih && j >= jh && j < d.ny - jh)
+        {
+            const double liquid = (double)qc + (double)qr;
+            if (!isfinite(po) || po <= 0.0f || !isfinite(q) || q < 0.0f || !isfinite(liquid) || liquid < 0.0)
+                flags |= kStatusInvalidEos;
+        }
+    }
+    return true;
+}
+
+static __global__ void __launch_bounds__(256) eos_candidate_f32_kernel(
+    Dims d, const float* __restrict__ rho, const float* __restrict__ theta, const float* __restrict__ p_old,
+    const float* __restrict__ qv, const float* __restrict__ qc, const float* __restrict__ qr,
+    const float4* __restrict__ eos0, EosSeries series, double gamma, float* __restrict__ p_candidate,
+    unsigned* __restrict__ status)
+{
+    const int n = (int)d.cells();
+    const bool moist = qv != nullptr;
+    unsigned flags = 0;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+    {
+        const int k = c % d.nz;
+        float p_new;
+        if (eos_candidate_value_f32(d, c, k, rho[c], theta[c], eos0, series, gamma, moist, moist ? p_old[c] : 0.0f,
+                                    moist ? qv[c] : 0.0f, moist ? qc[c] : 0.0f, moist ? qr[c] : 0.0f, p_new, flags))
+            p_candidate[c] = p_new;
+    }
+    if (flags) atomicOr(status, flags);
 }
 
 __device__ __forceinline__ void eos_candidate_cell(const Dims& d, const float* __restrict__ rho,

@@ -116,7 +116,7 @@ class EosArgs(ctypes.Structure):
     _fields_ = [
         ("p", _fp), ("rho", _fp), ("theta", _fp), ("qv", _fp), ("qc", _fp), ("qr", _fp),
         ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("gamma", ctypes.c_double),
-        ("memory", ctypes.c_int), ("stream", ctypes.c_void_p),
+        ("memory", ctypes.c_int), ("stream", ctypes.c_void_p), ("p0_base", _dp),
     ]
 
 
@@ -490,11 +490,13 @@ def kessler_args(st, dz, dt, domain=None, outputs=None, memory=MEMORY_HOST, stre
     return a
 
 
-def eos_args(p, rho, theta, qv=None, qc=None, qr=None, memory=MEMORY_HOST, stream=None) -> EosArgs:
+def eos_args(p, rho, theta, qv=None, qc=None, qr=None, memory=MEMORY_HOST, stream=None, p0=None) -> EosArgs:
     """Argument block for nimbus_cuda_eos_projection over every cell; qv/qc/qr
-    (all or none) add the moist-state checks."""
+    (all or none) add the moist-state checks; p0 (FP64 per level) lets the
+    FP32 form evaluate around the base pressure."""
     a = EosArgs()
-    a._keep = (p, rho, theta, qv, qc, qr)
+    a._keep = (p, rho, theta, qv, qc, qr, p0)
+    a.p0_base = _d(p0) if p0 is not None else None
     a.p, a.rho, a.theta = _f(p), _f(rho), _f(theta)
     a.qv, a.qc, a.qr = _f(qv), _f(qc), _f(qr)
     a.nx, a.ny, a.nz = tuple(p.shape)

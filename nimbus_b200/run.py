@@ -79,7 +79,8 @@ class ResidentRun:
         self._transport = cuda.transport_args(qs, qs, POSITIVE, f["rho"], self.rho_begin, *self.mf, case.dt,
                                               grid, weno=True, top_open=case.bc[5] == 2, memory=cuda.MEMORY_DEVICE)
         self._kessler = cuda.kessler_args(f, case.dz, case.dt, memory=cuda.MEMORY_DEVICE)
-        self._eos = cuda.eos_args(f["p"], f["rho"], f["theta"], f["qv"], f["qc"], f["qr"], memory=cuda.MEMORY_DEVICE)
+        self._eos = cuda.eos_args(f["p"], f["rho"], f["theta"], f["qv"], f["qc"], f["qr"], memory=cuda.MEMORY_DEVICE,
+                                  p0=self.prof["p0"])
         self.torch_stream = torch.cuda.ExternalStream(self.stream, device=dev)
 
     @property
