@@ -453,7 +453,7 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f32 (stencils), f64 (base state, EOS, mass-flux sums, Kessler)"
+            "dtype": "f32 (f64 only in the per-level base-state data and out-of-range EOS fallbacks)"
             if precision == cuda.PRECISION_FP32 else "f64 arithmetic, f32 storage",
             "data": "synthetic (seeded WK82 supercells: analytic sounding, cos^2 bubble, theta noise)",
             "config": {

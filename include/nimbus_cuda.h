@@ -102,10 +102,12 @@ nimbus_status nimbus_cuda_synchronize(nimbus_cuda_context* ctx);
  *   NIMBUS_PRECISION_REFERENCE (default): FP64 interior arithmetic over FP32
  *     storage in the reference CPU solver's operation order -- bit-identical
  *     results to the reference.
- *   NIMBUS_PRECISION_FP32: FP32 stencil arithmetic with the FP64 base state
- *     (hydrostatic pressure differences carried as FP32 hi+lo pairs), FP64
- *     EOS power law and FP64 retained mass-flux sums; errors against the FP64
- *     oracle are stated, not zero. */
+ *   NIMBUS_PRECISION_FP32: FP32 arithmetic throughout (stencils, WENO5 in
+ *     paired f32x2 instructions, Kessler), with the FP64 base state entering
+ *     as per-level FP32 hi+lo pairs: the hydrostatic pressure differences and
+ *     the compensated EOS p = p0 (1 + d)^gamma; the retained mass-flux sums
+ *     are single-rounding FMAs.  Errors against the FP64 oracle are stated,
+ *     not zero. */
 enum
 {
     NIMBUS_PRECISION_REFERENCE = 0,

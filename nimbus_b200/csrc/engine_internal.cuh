@@ -32,9 +32,9 @@ struct Lane
     size_t prefix_first = 0;  // first entry of this lane's [kItemKinds][members + 1] prefix block
     std::vector<int> active;  // members of this lane inside the loop at substep s
 };
-// The Kessler + EOS pass is FP64 in both forms and is launched from the
-// uncontracted unit (engine.cu), so both forms and the per-operation path
-// share its rounding.  Returns the launch count.
+// The Kessler + EOS pass (FP64 in the reference-precision form, FP32 in the
+// FP32 form) is launched from the uncontracted unit (engine.cu), so the engine
+// and the per-operation path share its rounding.  Returns the launch count.
 int launch_microphysics(nimbus_engine* e, cudaStream_t st, const nimbus::EngineMember* table,
                         const long long* prefix, long long tiles);
 }  // namespace nimbus_engine_detail
