@@ -46,8 +46,8 @@ struct __align__(16) EngineMember
     float *u, *v, *w, *rho, *rho_alt, *p, *theta, *qv, *qc, *qr, *qr_alt;
     // Retained transport context and per-step scratch.
     float *rho_begin, *mfx, *mfy, *mfz, *wave;
-    float *sf;        // [kEngineScalars][3][cells] face fluxes
-    float *rl;        // [kEngineScalars][cells] limiter factors
+    float *sf;        // [3][cells] float4 face fluxes (one lane per scalar)
+    float *rl;        // [cells] float4 limiter factors
     float *k1, *xs;   // [4][cells] Heun k1 and predictor state
     float *eos;       // EOS candidate pressure
     unsigned* status; // this member's status word (kStatus* bits)
@@ -321,8 +321,8 @@ static __global__ void __launch_bounds__(256) engine_transport_faces_kernel(cons
                                                                             long long tiles)
 {
     for_member_items(table, prefix, tiles, kItemCells, [&](const EngineMember& M, int c) {
-        transport_faces_cell<kFp32>(M.T, kEngineScalars, [&](int s) { return engine_scalar(M, s); }, M.mfx, M.mfy,
-                                    M.mfz, M.sf, c);
+        transport_faces_cell4<kFp32>(M.T, [&](int s) { return engine_scalar(M, s); }, M.mfx, M.mfy, M.mfz,
+                                     reinterpret_cast<float4*>(M.sf), c);
     });
 }
 
@@ -332,8 +332,8 @@ static __global__ void __launch_bounds__(256) engine_transport_limiter_kernel(co
                                                                               long long tiles)
 {
     for_member_items(table, prefix, tiles, kItemCells, [&](const EngineMember& M, int c) {
-        transport_limiter_cell<kFp32>(M.T, kEngineScalars, [&](int s) { return engine_scalar(M, s); }, M.rho_begin, M.sf,
-                               M.rl, c);
+        transport_limiter_cell4<kFp32>(M.T, [&](int s) { return engine_scalar(M, s); }, M.rho_begin,
+                                       reinterpret_cast<const float4*>(M.sf), reinterpret_cast<float4*>(M.rl), c);
     });
 }
 
@@ -344,9 +344,10 @@ static __global__ void __launch_bounds__(256) engine_transport_update_kernel(con
 {
     for_member_items(table, prefix, tiles, kItemCells, [&](const EngineMember& M, int c) {
         unsigned flags = 0;
-        transport_update_cell<kFp32>(M.T, kEngineScalars, [&](int s) { return engine_scalar(M, s); },
-                              [&](int s) { return engine_scalar_out(M, s); }, M.rho, M.rho_begin, M.sf, M.rl, c,
-                              flags);
+        transport_update_cell4<kFp32>(M.T, [&](int s) { return engine_scalar(M, s); },
+                                      [&](int s) { return engine_scalar_out(M, s); }, M.rho, M.rho_begin,
+                                      reinterpret_cast<const float4*>(M.sf), reinterpret_cast<const float4*>(M.rl), c,
+                                      flags);
         if (flags) atomicOr(M.status, flags);
     });
 }

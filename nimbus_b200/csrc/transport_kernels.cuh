@@ -385,66 +385,76 @@ __device__ __forceinline__ float pd_limiter_factor(double r)
     return nextafterf(__fmul_rn(stored, roundoff), 0.0f);
 }
 
-// Positive-definite donor ratio at cell c (advection_cartesian.cpp:2174-2240)
-// for every positive-definite scalar; rl is [scalars][cells].  kFp32: the
-// same sums in FP32 (the reference's FP32 GPU form); the factor's 32-ulp
-// roundoff margin covers the FP32 rounding of the update.
+// Positive-definite donor ratio of one scalar at a cell from its six face
+// fluxes (advection_cartesian.cpp:2174-2240): x+, x-, y+, y-, z+, z- faces,
+// each counted only where it exists (the has_* flags).  kFp32: the same sums
+// in FP32 (the reference's FP32 GPU form); the factor's 32-ulp roundoff
+// margin covers the FP32 rounding of the update.
+template <bool kFp32>
+__device__ __forceinline__ float limiter_factor(const TransportParams& T, float fxp, float fxm, float fyp, float fym,
+                                                float fzp, float fzm, bool xp, bool xm, bool yp, bool ym, bool zp,
+                                                bool zm, float rho_b, float q)
+{
+    using real = typename std::conditional<kFp32, float, double>::type;
+    const real rb = (real)rho_b;
+    const real idx = kFp32 ? (real)T.inv_dx_f : (real)T.inv_dx;
+    const real idy = kFp32 ? (real)T.inv_dy_f : (real)T.inv_dy;
+    const real idz = kFp32 ? (real)T.inv_dz_f : (real)T.inv_dz;
+    real out = 0;
+    if (xp && fxp > 0.0f) out += (real)fxp * idx;
+    if (xm && fxm < 0.0f) out -= (real)fxm * idx;
+    if (yp && fyp > 0.0f) out += (real)fyp * idy;
+    if (ym && fym < 0.0f) out -= (real)fym * idy;
+    if (zp && fzp > 0.0f) out += (real)fzp * idz;
+    if (zm && fzm < 0.0f) out -= (real)fzm * idz;
+    if constexpr (kFp32)
+    {
+        float r = 1.0f;
+        if (out > 0.0f)
+        {
+            const float available = rb * ((q < 0.0f) ? 0.0f : q) * T.inv_dt_f;
+            const float ratio = __fdividef(available, out);
+            r = (ratio < 1.0f) ? ratio : 1.0f;
+        }
+        return (r > 0.0f && r < 1.0f) ? nextafterf(__fmul_rn(r, 1.0f - 32.0f * 1.1920928955078125e-7f), 0.0f) : r;
+    }
+    else
+    {
+        double r = 1.0;
+        if (out > 0.0)
+        {
+            const double qc = (double)q;
+            const double available = rb * ((qc < 0.0) ? 0.0 : qc) / T.dt;  // std::max(q, 0.0)
+            const double ratio = available / out;
+            r = (ratio < 1.0) ? ratio : 1.0;  // std::min(1.0, ratio), NaN -> 1
+        }
+        return pd_limiter_factor(r);
+    }
+}
+
+// The limiter factor of every positive-definite scalar at cell c; sf is
+// [scalars][3][cells], rl [scalars][cells].
 template <bool kFp32, class QIn>
 __device__ __forceinline__ void transport_limiter_cell(const TransportParams& T, int scalars, QIn&& q_of,
                                                        const float* __restrict__ rho_begin,
                                                        const float* __restrict__ sf, float* __restrict__ rl, int c)
 {
-    using real = typename std::conditional<kFp32, float, double>::type;
     const Dims d = T.d;
     const size_t n = (size_t)d.cells();
     int i, j, k;
     decompose(d, c, i, j, k);
     const bool xm = i >= 1, xp = i <= d.nx - 2, ym = j >= 1, yp = j <= d.ny - 2, zm = k >= 1;
     const bool zp = k <= d.nz - 2 || (T.top_open && k == d.nz - 1);
-    const real rb = (real)rho_begin[c];
-    const real idx = kFp32 ? (real)T.inv_dx_f : (real)T.inv_dx;
-    const real idy = kFp32 ? (real)T.inv_dy_f : (real)T.inv_dy;
-    const real idz = kFp32 ? (real)T.inv_dz_f : (real)T.inv_dz;
+    const int cxm = xm ? c - d.sx() : c, cym = ym ? c - d.sy() : c, czm = zm ? c - 1 : c;
+    const float rb = rho_begin[c];
     for (int s = 0; s < scalars; ++s)
     {
         if (!T.positive_definite[s]) continue;
         const float* __restrict__ sfx = sf + (size_t)s * 3 * n;
         const float* __restrict__ sfy = sfx + n;
         const float* __restrict__ sfz = sfy + n;
-        real out = 0;
-        if (xp && sfx[c] > 0.0f) out += (real)sfx[c] * idx;
-        if (xm && sfx[c - d.sx()] < 0.0f) out -= (real)sfx[c - d.sx()] * idx;
-        if (yp && sfy[c] > 0.0f) out += (real)sfy[c] * idy;
-        if (ym && sfy[c - d.sy()] < 0.0f) out -= (real)sfy[c - d.sy()] * idy;
-        if (zp && sfz[c] > 0.0f) out += (real)sfz[c] * idz;
-        if (zm && sfz[c - 1] < 0.0f) out -= (real)sfz[c - 1] * idz;
-        float factor;
-        if constexpr (kFp32)
-        {
-            float r = 1.0f;
-            if (out > 0.0f)
-            {
-                const float qc = q_of(s)[c];
-                const float available = rb * ((qc < 0.0f) ? 0.0f : qc) * T.inv_dt_f;
-                const float ratio = __fdividef(available, out);
-                r = (ratio < 1.0f) ? ratio : 1.0f;
-            }
-            factor = (r > 0.0f && r < 1.0f) ? nextafterf(__fmul_rn(r, 1.0f - 32.0f * 1.1920928955078125e-7f), 0.0f)
-                                             : r;
-        }
-        else
-        {
-            double r = 1.0;
-            if (out > 0.0)
-            {
-                const double qc = (double)q_of(s)[c];
-                const double available = rb * ((qc < 0.0) ? 0.0 : qc) / T.dt;  // std::max(q, 0.0)
-                const double ratio = available / out;
-                r = (ratio < 1.0) ? ratio : 1.0;  // std::min(1.0, ratio), NaN -> 1
-            }
-            factor = pd_limiter_factor(r);
-        }
-        rl[(size_t)s * n + c] = factor;
+        rl[(size_t)s * n + c] = limiter_factor<kFp32>(T, sfx[c], sfx[cxm], sfy[c], sfy[cym], sfz[c], sfz[czm], xp,
+                                                      xm, yp, ym, zp, zm, rb, q_of(s)[c]);
     }
 }
 
@@ -459,17 +469,78 @@ static __global__ void __launch_bounds__(256) transport_limiter_kernel(Transport
         transport_limiter_cell<kFp32>(T, T.n_scalars, [&](int s) { return T.q_in[s]; }, rho_begin, sf, rl, c);
 }
 
-__device__ __forceinline__ double limited_flux(float raw, bool pd, const float* __restrict__ rl, int lo, int hi)
+// The donor-side factor of a face (limited_flux in the reference): the factor
+// of the cell the flux leaves.
+template <bool kFp32>
+__device__ __forceinline__ typename std::conditional<kFp32, float, double>::type limited_face(float raw, bool pd,
+                                                                                             float r_lo, float r_hi)
 {
-    if (!pd || raw == 0.0f) return (double)raw;
-    const float r = raw > 0.0f ? rl[lo] : rl[hi];
-    return (double)raw * (double)r;
+    if (!pd || raw == 0.0f) return raw;
+    const float r = raw > 0.0f ? r_lo : r_hi;
+    if constexpr (kFp32) return raw * r;
+    else return (double)raw * (double)r;
+}
+
+// The new value of one scalar at an interior cell from its six face fluxes
+// (x+, x-, y+, y-, z+, z-), the limiter factors of the cell and its six
+// neighbours (positive-definite scalars only) and its old value
+// (advection_cartesian.cpp:2465-2640).  kFp32: the same sums in FP32.
+template <bool kFp32>
+__device__ __forceinline__ float update_value(const TransportParams& T, bool pd, float fxp, float fxm, float fyp,
+                                              float fym, float fzp, float fzm, float rc, float rxp, float rxm,
+                                              float ryp, float rym, float rzp, float rzm, float qraw, bool has_top,
+                                              bool has_bottom, float rho_e, float rho_b, unsigned& flags)
+{
+    using real = typename std::conditional<kFp32, float, double>::type;
+    const real re = (real)rho_e;
+    const real rb = (real)rho_b;
+    const real floor_ = kFp32 ? (real)T.rho_floor_f : (real)T.rho_floor;
+    const real denom = (re > floor_) ? re : floor_;
+    const real idx = kFp32 ? (real)T.inv_dx_f : (real)T.inv_dx;
+    const real idy = kFp32 ? (real)T.inv_dy_f : (real)T.inv_dy;
+    const real idz = kFp32 ? (real)T.inv_dz_f : (real)T.inv_dz;
+    const real dt = kFp32 ? (real)T.dt_f : (real)T.dt;
+    const real sxp = limited_face<kFp32>(fxp, pd, rc, rxp);
+    const real sxm = limited_face<kFp32>(fxm, pd, rxm, rc);
+    const real syp = limited_face<kFp32>(fyp, pd, rc, ryp);
+    const real sym = limited_face<kFp32>(fym, pd, rym, rc);
+    const real szp = has_top ? limited_face<kFp32>(fzp, pd, rc, rzp) : (real)0;
+    const real szm = has_bottom ? limited_face<kFp32>(fzm, pd, rzm, rc) : (real)0;
+    const real qc = (real)qraw;
+    real rho_phi;
+    if (pd)
+    {
+        real outgoing = 0, incoming = 0;
+        if (sxp >= 0) outgoing += sxp * idx; else incoming -= sxp * idx;
+        if (sxm <= 0) outgoing -= sxm * idx; else incoming += sxm * idx;
+        if (syp >= 0) outgoing += syp * idy; else incoming -= syp * idy;
+        if (sym <= 0) outgoing -= sym * idy; else incoming += sym * idy;
+        if (has_top) { if (szp >= 0) outgoing += szp * idz; else incoming -= szp * idz; }
+        if (has_bottom) { if (szm <= 0) outgoing -= szm * idz; else incoming += szm * idz; }
+        rho_phi = (rb * qc - dt * outgoing) + dt * incoming;
+    }
+    else
+    {
+        const real div = (sxp - sxm) * idx + (syp - sym) * idy + (szp - szm) * idz;
+        if constexpr (kFp32)
+        {
+            // (rb q - dt div) / denom as q + ((rb - denom) q - dt div) / denom:
+            // the small increment carries the FP32 rounding instead of the
+            // full value (theta ~ 300 K would lose its perturbation bits).
+            rho_phi = (rb - denom) * qc - dt * div;
+        }
+        else rho_phi = rb * qc - dt * div;
+    }
+    float out;
+    if constexpr (kFp32) out = pd ? __fdividef(rho_phi, denom) : qc + __fdividef(rho_phi, denom);
+    else out = (float)(rho_phi / denom);
+    if (!isfinite(out)) flags |= kStatusNonfiniteTransport;
+    return out;
 }
 
 // Donor-limited divergence and density recovery at cell c for every scalar
 // (advection_cartesian.cpp:2465-2640).  The output may alias the input: cell
-// c reads only its own old value, the fluxes live in the scratch.  kFp32: the
-// same sums in FP32.
+// c reads only its own old value, the fluxes live in the scratch.
 template <bool kFp32, class QIn, class QOut>
 __device__ __forceinline__ void transport_update_cell(const TransportParams& T, int scalars, QIn&& q_of,
                                                       QOut&& qo_of, const float* __restrict__ rho_end,
@@ -477,7 +548,6 @@ __device__ __forceinline__ void transport_update_cell(const TransportParams& T, 
                                                       const float* __restrict__ sf, const float* __restrict__ rl,
                                                       int c, unsigned& flags)
 {
-    using real = typename std::conditional<kFp32, float, double>::type;
     const Dims d = T.d;
     const size_t n = (size_t)d.cells();
     int i, j, k;
@@ -494,22 +564,8 @@ __device__ __forceinline__ void transport_update_cell(const TransportParams& T, 
     }
     const int cxm = c - d.sx(), cxp = c + d.sx(), cym = c - d.sy(), cyp = c + d.sy();
     const bool has_top = k <= d.nz - 2 || (T.top_open && k == d.nz - 1);
-    const real re = (real)rho_end[c];
-    const real rb = (real)rho_begin[c];
-    const real floor_ = kFp32 ? (real)T.rho_floor_f : (real)T.rho_floor;
-    const real denom = (re > floor_) ? re : floor_;
-    const real idx = kFp32 ? (real)T.inv_dx_f : (real)T.inv_dx;
-    const real idy = kFp32 ? (real)T.inv_dy_f : (real)T.inv_dy;
-    const real idz = kFp32 ? (real)T.inv_dz_f : (real)T.inv_dz;
-    const real dt = kFp32 ? (real)T.dt_f : (real)T.dt;
-    // The donor-side factor of a face (limited_flux): both candidates are
-    // loaded up front, so no load waits on the sign of a flux.
-    auto limited = [&](float raw, bool pd, float r_lo, float r_hi) -> real {
-        if (!pd || raw == 0.0f) return (real)raw;
-        const float r = raw > 0.0f ? r_lo : r_hi;
-        if constexpr (kFp32) return raw * r;
-        else return (double)raw * (double)r;
-    };
+    const float re = rho_end[c], rb = rho_begin[c];
+    // Every candidate is loaded up front, so no load waits on a flux sign.
     const int czp = k < d.nz - 1 ? c + 1 : c, czm = k >= 1 ? c - 1 : c;
     for (int s = 0; s < scalars; ++s)
     {
@@ -526,42 +582,8 @@ __device__ __forceinline__ void transport_update_cell(const TransportParams& T, 
         {
             rc = r[c]; rxp = r[cxp]; rxm = r[cxm]; ryp = r[cyp]; rym = r[cym]; rzp = r[czp]; rzm = r[czm];
         }
-        const real sxp = limited(fxp, pd, rc, rxp);
-        const real sxm = limited(fxm, pd, rxm, rc);
-        const real syp = limited(fyp, pd, rc, ryp);
-        const real sym = limited(fym, pd, rym, rc);
-        const real szp = has_top ? limited(fzp, pd, rc, rzp) : (real)0;
-        const real szm = (k >= 1) ? limited(fzm, pd, rzm, rc) : (real)0;
-        const real qc = (real)qraw;
-        real rho_phi;
-        if (pd)
-        {
-            real outgoing = 0, incoming = 0;
-            if (sxp >= 0) outgoing += sxp * idx; else incoming -= sxp * idx;
-            if (sxm <= 0) outgoing -= sxm * idx; else incoming += sxm * idx;
-            if (syp >= 0) outgoing += syp * idy; else incoming -= syp * idy;
-            if (sym <= 0) outgoing -= sym * idy; else incoming += sym * idy;
-            if (has_top) { if (szp >= 0) outgoing += szp * idz; else incoming -= szp * idz; }
-            if (k >= 1) { if (szm <= 0) outgoing -= szm * idz; else incoming += szm * idz; }
-            rho_phi = (rb * qc - dt * outgoing) + dt * incoming;
-        }
-        else
-        {
-            const real div = (sxp - sxm) * idx + (syp - sym) * idy + (szp - szm) * idz;
-            if constexpr (kFp32)
-            {
-                // (rb q - dt div) / denom as q + ((rb - denom) q - dt div) / denom:
-                // the small increment carries the FP32 rounding instead of the
-                // full value (theta ~ 300 K would lose its perturbation bits).
-                rho_phi = (rb - denom) * qc - dt * div;
-            }
-            else rho_phi = rb * qc - dt * div;
-        }
-        float out;
-        if constexpr (kFp32) out = pd ? __fdividef(rho_phi, denom) : qc + __fdividef(rho_phi, denom);
-        else out = (float)(rho_phi / denom);
-        if (!isfinite(out)) flags |= kStatusNonfiniteTransport;
-        qo_of(s)[c] = out;
+        qo_of(s)[c] = update_value<kFp32>(T, pd, fxp, fxm, fyp, fym, fzp, fzm, rc, rxp, rxm, ryp, rym, rzp, rzm, qraw,
+                                          has_top, k >= 1, re, rb, flags);
     }
 }
 
@@ -578,6 +600,154 @@ static __global__ void __launch_bounds__(256) transport_update_kernel(TransportP
         transport_update_cell<kFp32>(T, T.n_scalars, [&](int s) { return T.q_in[s]; }, [&](int s) { return T.q_out[s]; },
                               rho_end, rho_begin, sf, rl, c, flags);
     if (flags) atomicOr(status, flags);
+}
+
+// ---- Four scalars interleaved (the member engine) -------------------------
+// The engine transports exactly four scalars (theta, qv, qc, qr) and keeps
+// their face fluxes as [3][cells] float4 (x, y, z faces; one lane per scalar)
+// and their limiter factors as [cells] float4, so a cell's fluxes of one
+// direction, or one cell's factors, are one 16-byte load.  The arithmetic is
+// the per-scalar helpers above, so the values equal the planar form's.
+
+__device__ __forceinline__ float lane4(const float4& v, int s)
+{
+    return s == 0 ? v.x : (s == 1 ? v.y : (s == 2 ? v.z : v.w));
+}
+
+template <bool kFp32, class QIn>
+__device__ __forceinline__ void transport_faces_cell4(const TransportParams& T, QIn&& q_of,
+                                                      const float* __restrict__ mfx, const float* __restrict__ mfy,
+                                                      const float* __restrict__ mfz, float4* __restrict__ sf4, int c)
+{
+    const Dims d = T.d;
+    const size_t n = (size_t)d.cells();
+    const int kz_end = T.top_open ? d.nz : d.nz - 1;
+    int i, j, k;
+    decompose(d, c, i, j, k);
+    const bool hx = i <= d.nx - 2, hy = j <= d.ny - 2, hz = k < kz_end, top = k == d.nz - 1;
+    const float fx = hx ? mfx[c] : 0.0f, fy = hy ? mfy[c] : 0.0f, fz = hz ? mfz[c] : 0.0f;
+    const FaceStencil sx = face_stencil(c - i * d.sx(), d.sx(), i, d.nx, fx >= 0.0f, T.weno);
+    const FaceStencil sy = face_stencil(c - j * d.sy(), d.sy(), j, d.ny, fy >= 0.0f, T.weno);
+    const FaceStencil sz = face_stencil(c - k, 1, top ? k - 1 : k, d.nz, fz >= 0.0f, T.weno);
+    const float *q0 = q_of(0), *q1 = q_of(1), *q2 = q_of(2), *q3 = q_of(3);
+    float4 ox = make_float4(0.0f, 0.0f, 0.0f, 0.0f), oy = ox, oz = ox;
+    if constexpr (kFp32)
+    {
+        if (hx)
+        {
+            const float2 a = stencil_flux_pair(q0, q1, sx, fx), b = stencil_flux_pair(q2, q3, sx, fx);
+            ox = make_float4(a.x, a.y, b.x, b.y);
+        }
+        if (hy)
+        {
+            const float2 a = stencil_flux_pair(q0, q1, sy, fy), b = stencil_flux_pair(q2, q3, sy, fy);
+            oy = make_float4(a.x, a.y, b.x, b.y);
+        }
+        if (hz)
+        {
+            if (top) oz = make_float4(fz * q0[c], fz * q1[c], fz * q2[c], fz * q3[c]);
+            else
+            {
+                const float2 a = stencil_flux_pair(q0, q1, sz, fz), b = stencil_flux_pair(q2, q3, sz, fz);
+                oz = make_float4(a.x, a.y, b.x, b.y);
+            }
+        }
+    }
+    else
+    {
+        if (hx)
+            ox = make_float4(stencil_flux<false>(q0, sx, fx), stencil_flux<false>(q1, sx, fx),
+                             stencil_flux<false>(q2, sx, fx), stencil_flux<false>(q3, sx, fx));
+        if (hy)
+            oy = make_float4(stencil_flux<false>(q0, sy, fy), stencil_flux<false>(q1, sy, fy),
+                             stencil_flux<false>(q2, sy, fy), stencil_flux<false>(q3, sy, fy));
+        if (hz)
+        {
+            if (top)
+            {
+                const double f = (double)fz;
+                oz = make_float4((float)(f * (double)q0[c]), (float)(f * (double)q1[c]), (float)(f * (double)q2[c]),
+                                 (float)(f * (double)q3[c]));
+            }
+            else
+                oz = make_float4(stencil_flux<false>(q0, sz, fz), stencil_flux<false>(q1, sz, fz),
+                                 stencil_flux<false>(q2, sz, fz), stencil_flux<false>(q3, sz, fz));
+        }
+    }
+    sf4[c] = ox;
+    sf4[n + c] = oy;
+    sf4[2 * n + c] = oz;
+}
+
+template <bool kFp32, class QIn>
+__device__ __forceinline__ void transport_limiter_cell4(const TransportParams& T, QIn&& q_of,
+                                                        const float* __restrict__ rho_begin,
+                                                        const float4* __restrict__ sf4, float4* __restrict__ rl4,
+                                                        int c)
+{
+    const Dims d = T.d;
+    const size_t n = (size_t)d.cells();
+    int i, j, k;
+    decompose(d, c, i, j, k);
+    const bool xm = i >= 1, xp = i <= d.nx - 2, ym = j >= 1, yp = j <= d.ny - 2, zm = k >= 1;
+    const bool zp = k <= d.nz - 2 || (T.top_open && k == d.nz - 1);
+    const int cxm = xm ? c - d.sx() : c, cym = ym ? c - d.sy() : c, czm = zm ? c - 1 : c;
+    const float4 fxp = sf4[c], fxm = sf4[cxm], fyp = sf4[n + c], fym = sf4[n + cym];
+    const float4 fzp = sf4[2 * n + c], fzm = sf4[2 * n + czm];
+    const float rb = rho_begin[c];
+    float r[4];
+#pragma unroll
+    for (int s = 0; s < 4; ++s)
+        r[s] = T.positive_definite[s]
+                   ? limiter_factor<kFp32>(T, lane4(fxp, s), lane4(fxm, s), lane4(fyp, s), lane4(fym, s),
+                                           lane4(fzp, s), lane4(fzm, s), xp, xm, yp, ym, zp, zm, rb, q_of(s)[c])
+                   : 1.0f;
+    rl4[c] = make_float4(r[0], r[1], r[2], r[3]);
+}
+
+template <bool kFp32, class QIn, class QOut>
+__device__ __forceinline__ void transport_update_cell4(const TransportParams& T, QIn&& q_of, QOut&& qo_of,
+                                                       const float* __restrict__ rho_end,
+                                                       const float* __restrict__ rho_begin,
+                                                       const float4* __restrict__ sf4,
+                                                       const float4* __restrict__ rl4, int c, unsigned& flags)
+{
+    const Dims d = T.d;
+    const size_t n = (size_t)d.cells();
+    int i, j, k;
+    decompose(d, c, i, j, k);
+    if (!(i >= 1 && i < d.nx - 1 && j >= 1 && j < d.ny - 1))
+    {
+#pragma unroll
+        for (int s = 0; s < 4; ++s)
+        {
+            const float* q = q_of(s);
+            float* qo = qo_of(s);
+            if (q != qo) qo[c] = q[c];  // seed_destination_from_source
+        }
+        return;
+    }
+    const int cxm = c - d.sx(), cxp = c + d.sx(), cym = c - d.sy(), cyp = c + d.sy();
+    const int czp = k < d.nz - 1 ? c + 1 : c, czm = k >= 1 ? c - 1 : c;
+    const bool has_top = k <= d.nz - 2 || (T.top_open && k == d.nz - 1);
+    const float4 fxp = sf4[c], fxm = sf4[cxm], fyp = sf4[n + c], fym = sf4[n + cym];
+    const float4 fzp = sf4[2 * n + c], fzm = sf4[2 * n + czm];
+    const float4 rc = rl4[c], rxp = rl4[cxp], rxm = rl4[cxm], ryp = rl4[cyp], rym = rl4[cym];
+    const float4 rzp = rl4[czp], rzm = rl4[czm];
+    const float re = rho_end[c], rb = rho_begin[c];
+    float qraw[4];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) qraw[s] = q_of(s)[c];
+#pragma unroll
+    for (int s = 0; s < 4; ++s)
+    {
+        const bool pd = T.positive_definite[s] != 0;
+        qo_of(s)[c] = update_value<kFp32>(
+            T, pd, lane4(fxp, s), lane4(fxm, s), lane4(fyp, s), lane4(fym, s), lane4(fzp, s), lane4(fzm, s),
+            pd ? lane4(rc, s) : 1.0f, pd ? lane4(rxp, s) : 1.0f, pd ? lane4(rxm, s) : 1.0f, pd ? lane4(ryp, s) : 1.0f,
+            pd ? lane4(rym, s) : 1.0f, pd ? lane4(rzp, s) : 1.0f, pd ? lane4(rzm, s) : 1.0f, qraw[s], has_top, k >= 1,
+            re, rb, flags);
+    }
 }
 
 }  // namespace nimbus
