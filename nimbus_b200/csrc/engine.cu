@@ -35,7 +35,7 @@ size_t align_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
 struct ArenaLayout
 {
     size_t cells, history;
-    size_t off_state, off_ctxt, off_wave, off_sf, off_rl, off_k1, off_xs, off_eos, off_status, off_prof, off_dp0,
+    size_t off_state, off_ctxt, off_wave, off_sf, off_rl, off_q4, off_k1, off_xs, off_eos, off_status, off_prof, off_dp0,
         off_eos0, total;
 };
 
@@ -51,6 +51,7 @@ ArenaLayout arena_layout(const nimbus_member_desc* d)
     L.off_wave = off;   off += align_up(L.history * sizeof(float));
     L.off_sf = off;     off += align_up(3 * kEngineScalars * L.cells * sizeof(float));
     L.off_rl = off;     off += align_up(kEngineScalars * L.cells * sizeof(float));
+    L.off_q4 = off;     off += align_up(kEngineScalars * L.cells * sizeof(float));
     L.off_k1 = off;     off += align_up(4 * L.cells * sizeof(float));
     L.off_xs = off;     off += align_up(4 * L.cells * sizeof(float));
     L.off_eos = off;    off += field;
@@ -562,6 +563,7 @@ nimbus_status nimbus_cuda_engine_admit(nimbus_engine* e, const nimbus_member_des
     M.wave = reinterpret_cast<float*>(base + L.off_wave);
     M.sf = reinterpret_cast<float*>(base + L.off_sf);
     M.rl = reinterpret_cast<float*>(base + L.off_rl);
+    M.q4 = reinterpret_cast<float*>(base + L.off_q4);
     M.k1 = reinterpret_cast<float*>(base + L.off_k1);
     M.xs = reinterpret_cast<float*>(base + L.off_xs);
     M.eos = reinterpret_cast<float*>(base + L.off_eos);

@@ -48,6 +48,7 @@ struct __align__(16) EngineMember
     float *rho_begin, *mfx, *mfy, *mfz, *wave;
     float *sf;        // [3][cells] float4 face fluxes (one lane per scalar)
     float *rl;        // [cells] float4 limiter factors
+    float *q4;        // [cells] float4 theta, qv, qc, qr before transport (written by the slow predictor)
     float *k1, *xs;   // [4][cells] Heun k1 and predictor state
     float *eos;       // EOS candidate pressure
     unsigned* status; // this member's status word (kStatus* bits)
@@ -117,6 +118,9 @@ static __global__ void __launch_bounds__(256, 4) engine_slow_predict_kernel(cons
         slow_predict_cell<Policy>(M.S, M.u, M.v, M.w, M.rho, M.p, M.qv, M.qc, M.qr, M.rho0, M.qv0, M.u0, M.v0, M.k1,
                                   M.k1 + n, M.k1 + 2 * n, M.k1 + 3 * n, M.xs, M.xs + n, M.xs + 2 * n, M.xs + 3 * n,
                                   c);
+        // The transported scalars do not change before transport: keep their
+        // interleaved copy for the transport kernels.
+        reinterpret_cast<float4*>(M.q4)[c] = make_float4(M.theta[c], M.qv[c], M.qc[c], M.qr[c]);
     });
 }
 
@@ -321,7 +325,7 @@ static __global__ void __launch_bounds__(256) engine_transport_faces_kernel(cons
                                                                             long long tiles)
 {
     for_member_items(table, prefix, tiles, kItemCells, [&](const EngineMember& M, int c) {
-        transport_faces_cell4<kFp32>(M.T, [&](int s) { return engine_scalar(M, s); }, M.mfx, M.mfy, M.mfz,
+        transport_faces_cell4<kFp32>(M.T, reinterpret_cast<const float4*>(M.q4), M.mfx, M.mfy, M.mfz,
                                      reinterpret_cast<float4*>(M.sf), c);
     });
 }
@@ -332,7 +336,7 @@ static __global__ void __launch_bounds__(256) engine_transport_limiter_kernel(co
                                                                               long long tiles)
 {
     for_member_items(table, prefix, tiles, kItemCells, [&](const EngineMember& M, int c) {
-        transport_limiter_cell4<kFp32>(M.T, [&](int s) { return engine_scalar(M, s); }, M.rho_begin,
+        transport_limiter_cell4<kFp32>(M.T, reinterpret_cast<const float4*>(M.q4), M.rho_begin,
                                        reinterpret_cast<const float4*>(M.sf), reinterpret_cast<float4*>(M.rl), c);
     });
 }
@@ -344,7 +348,7 @@ static __global__ void __launch_bounds__(256) engine_transport_update_kernel(con
 {
     for_member_items(table, prefix, tiles, kItemCells, [&](const EngineMember& M, int c) {
         unsigned flags = 0;
-        transport_update_cell4<kFp32>(M.T, [&](int s) { return engine_scalar(M, s); },
+        transport_update_cell4<kFp32>(M.T, reinterpret_cast<const float4*>(M.q4), [&](int s) { return engine_scalar(M, s); },
                                       [&](int s) { return engine_scalar_out(M, s); }, M.rho, M.rho_begin,
                                       reinterpret_cast<const float4*>(M.sf), reinterpret_cast<const float4*>(M.rl), c,
                                       flags);

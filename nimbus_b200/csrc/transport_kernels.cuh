@@ -235,57 +235,70 @@ __device__ __forceinline__ FaceStencil face_stencil(int base, int stride, int l,
 // with the normalised WENO5 offset; reference precision: M times the FP64
 // face value (WENO5 where the stencil fits, else donor +- half the MC
 // slope), rounded once to the FP32 scratch.
+// The same from the five stencil values v[m] = q[f.o[m]] (for the MC
+// fallback v[0], v[2], v[3] are the slope's points).
 template <bool kFp32>
-__device__ __forceinline__ float stencil_flux(const float* __restrict__ q, const FaceStencil& f, float mflux)
+__device__ __forceinline__ float stencil_flux_values(const float (&v)[5], const FaceStencil& f, float mflux)
 {
     if constexpr (kFp32)
     {
-        const float q0 = q[f.o[2]];
+        const float q0 = v[2];
         float offset;
-        if (f.weno) offset = weno5_offset_f32(q[f.o[0]], q[f.o[1]], q0, q[f.o[3]], q[f.o[4]]);
+        if (f.weno) offset = weno5_offset_f32(v[0], v[1], q0, v[3], v[4]);
         else
         {
-            const float sl = f.slope ? mc_slope_f32(q[f.o[0]], q0, q[f.o[3]]) : 0.0f;
+            const float sl = f.slope ? mc_slope_f32(v[0], q0, v[3]) : 0.0f;
             offset = (f.pos ? 0.5f : -0.5f) * sl;
         }
         return __fmaf_rn(mflux, q0, mflux * offset);
     }
     else
     {
-        const double q0 = (double)q[f.o[2]];
+        const double q0 = (double)v[2];
         double face;
-        if (f.weno)
-            face = weno5_face((double)q[f.o[0]], (double)q[f.o[1]], q0, (double)q[f.o[3]], (double)q[f.o[4]]);
+        if (f.weno) face = weno5_face((double)v[0], (double)v[1], q0, (double)v[3], (double)v[4]);
         else
         {
-            const double sl = f.slope ? mc_slope((double)q[f.o[0]], q0, (double)q[f.o[3]]) : 0.0;
+            const double sl = f.slope ? mc_slope((double)v[0], q0, (double)v[3]) : 0.0;
             face = f.pos ? q0 + 0.5 * sl : q0 - 0.5 * sl;
         }
         return (float)((double)mflux * face);
     }
 }
 
+template <bool kFp32>
+__device__ __forceinline__ float stencil_flux(const float* __restrict__ q, const FaceStencil& f, float mflux)
+{
+    const float v[5] = {q[f.o[0]], q[f.o[1]], q[f.o[2]], q[f.o[3]], q[f.o[4]]};
+    return stencil_flux_values<kFp32>(v, f, mflux);
+}
+
 // FP32 face fluxes of two scalars on one stencil (same donor, same mass
 // flux): the WENO5 arithmetic of both in paired f32x2 instructions, with the
 // same bits as two stencil_flux<true> calls.
-__device__ __forceinline__ float2 stencil_flux_pair(const float* __restrict__ qa, const float* __restrict__ qb,
-                                                    const FaceStencil& f, float mflux)
+__device__ __forceinline__ float2 stencil_flux_pair_values(const float2 (&v)[5], const FaceStencil& f, float mflux)
 {
-    const float2 q0 = make_float2(qa[f.o[2]], qb[f.o[2]]);
+    const float2 q0 = v[2];
     float2 offset;
-    if (f.weno)
-        offset = weno5_offset_lanes<float2>(make_float2(qa[f.o[0]], qb[f.o[0]]), make_float2(qa[f.o[1]], qb[f.o[1]]),
-                                            q0, make_float2(qa[f.o[3]], qb[f.o[3]]),
-                                            make_float2(qa[f.o[4]], qb[f.o[4]]));
+    if (f.weno) offset = weno5_offset_lanes<float2>(v[0], v[1], q0, v[3], v[4]);
     else
     {
         const float h = f.pos ? 0.5f : -0.5f;
-        const float sa = f.slope ? mc_slope_f32(qa[f.o[0]], q0.x, qa[f.o[3]]) : 0.0f;
-        const float sb = f.slope ? mc_slope_f32(qb[f.o[0]], q0.y, qb[f.o[3]]) : 0.0f;
+        const float sa = f.slope ? mc_slope_f32(v[0].x, q0.x, v[3].x) : 0.0f;
+        const float sb = f.slope ? mc_slope_f32(v[0].y, q0.y, v[3].y) : 0.0f;
         offset = make_float2(h * sa, h * sb);
     }
     const float2 m = make_float2(mflux, mflux);
     return __ffma2_rn(m, q0, __fmul2_rn(m, offset));
+}
+
+__device__ __forceinline__ float2 stencil_flux_pair(const float* __restrict__ qa, const float* __restrict__ qb,
+                                                    const FaceStencil& f, float mflux)
+{
+    float2 v[5];
+#pragma unroll
+    for (int m = 0; m < 5; ++m) v[m] = make_float2(qa[f.o[m]], qb[f.o[m]]);
+    return stencil_flux_pair_values(v, f, mflux);
 }
 
 // Face fluxes owned by cell c (its +x, +y and +z faces) for every scalar:
@@ -603,19 +616,53 @@ static __global__ void __launch_bounds__(256) transport_update_kernel(TransportP
 }
 
 // ---- Four scalars interleaved (the member engine) -------------------------
-// The engine transports exactly four scalars (theta, qv, qc, qr) and keeps
-// their face fluxes as [3][cells] float4 (x, y, z faces; one lane per scalar)
-// and their limiter factors as [cells] float4, so a cell's fluxes of one
-// direction, or one cell's factors, are one 16-byte load.  The arithmetic is
-// the per-scalar helpers above, so the values equal the planar form's.
+// The engine transports exactly four scalars (theta, qv, qc, qr).  It reads
+// them from q4, a [cells] float4 copy of their values before transport (one
+// 16-byte load per stencil point instead of four), keeps their face fluxes as
+// [3][cells] float4 (x, y, z faces; one lane per scalar) and their limiter
+// factors as [cells] float4.  The arithmetic is the per-scalar helpers above,
+// so the values equal the planar form's.
 
 __device__ __forceinline__ float lane4(const float4& v, int s)
 {
     return s == 0 ? v.x : (s == 1 ? v.y : (s == 2 ? v.z : v.w));
 }
 
-template <bool kFp32, class QIn>
-__device__ __forceinline__ void transport_faces_cell4(const TransportParams& T, QIn&& q_of,
+// The four face fluxes of one face from its stencil: q4 holds the four
+// scalars of every cell.
+template <bool kFp32>
+__device__ __forceinline__ float4 stencil_flux4(const float4* __restrict__ q4, const FaceStencil& f, float mflux)
+{
+    float4 p[5];
+#pragma unroll
+    for (int m = 0; m < 5; ++m) p[m] = q4[f.o[m]];
+    if constexpr (kFp32)
+    {
+        float2 a[5], b[5];
+#pragma unroll
+        for (int m = 0; m < 5; ++m)
+        {
+            a[m] = make_float2(p[m].x, p[m].y);
+            b[m] = make_float2(p[m].z, p[m].w);
+        }
+        const float2 ra = stencil_flux_pair_values(a, f, mflux), rb = stencil_flux_pair_values(b, f, mflux);
+        return make_float4(ra.x, ra.y, rb.x, rb.y);
+    }
+    else
+    {
+        float r[4];
+#pragma unroll
+        for (int s = 0; s < 4; ++s)
+        {
+            const float v[5] = {lane4(p[0], s), lane4(p[1], s), lane4(p[2], s), lane4(p[3], s), lane4(p[4], s)};
+            r[s] = stencil_flux_values<false>(v, f, mflux);
+        }
+        return make_float4(r[0], r[1], r[2], r[3]);
+    }
+}
+
+template <bool kFp32>
+__device__ __forceinline__ void transport_faces_cell4(const TransportParams& T, const float4* __restrict__ q4,
                                                       const float* __restrict__ mfx, const float* __restrict__ mfy,
                                                       const float* __restrict__ mfz, float4* __restrict__ sf4, int c)
 {
@@ -629,58 +676,31 @@ __device__ __forceinline__ void transport_faces_cell4(const TransportParams& T, 
     const FaceStencil sx = face_stencil(c - i * d.sx(), d.sx(), i, d.nx, fx >= 0.0f, T.weno);
     const FaceStencil sy = face_stencil(c - j * d.sy(), d.sy(), j, d.ny, fy >= 0.0f, T.weno);
     const FaceStencil sz = face_stencil(c - k, 1, top ? k - 1 : k, d.nz, fz >= 0.0f, T.weno);
-    const float *q0 = q_of(0), *q1 = q_of(1), *q2 = q_of(2), *q3 = q_of(3);
     float4 ox = make_float4(0.0f, 0.0f, 0.0f, 0.0f), oy = ox, oz = ox;
-    if constexpr (kFp32)
+    if (hx) ox = stencil_flux4<kFp32>(q4, sx, fx);
+    if (hy) oy = stencil_flux4<kFp32>(q4, sy, fy);
+    if (hz)
     {
-        if (hx)
+        if (top)
         {
-            const float2 a = stencil_flux_pair(q0, q1, sx, fx), b = stencil_flux_pair(q2, q3, sx, fx);
-            ox = make_float4(a.x, a.y, b.x, b.y);
-        }
-        if (hy)
-        {
-            const float2 a = stencil_flux_pair(q0, q1, sy, fy), b = stencil_flux_pair(q2, q3, sy, fy);
-            oy = make_float4(a.x, a.y, b.x, b.y);
-        }
-        if (hz)
-        {
-            if (top) oz = make_float4(fz * q0[c], fz * q1[c], fz * q2[c], fz * q3[c]);
+            const float4 q = q4[c];
+            if constexpr (kFp32) oz = make_float4(fz * q.x, fz * q.y, fz * q.z, fz * q.w);
             else
-            {
-                const float2 a = stencil_flux_pair(q0, q1, sz, fz), b = stencil_flux_pair(q2, q3, sz, fz);
-                oz = make_float4(a.x, a.y, b.x, b.y);
-            }
-        }
-    }
-    else
-    {
-        if (hx)
-            ox = make_float4(stencil_flux<false>(q0, sx, fx), stencil_flux<false>(q1, sx, fx),
-                             stencil_flux<false>(q2, sx, fx), stencil_flux<false>(q3, sx, fx));
-        if (hy)
-            oy = make_float4(stencil_flux<false>(q0, sy, fy), stencil_flux<false>(q1, sy, fy),
-                             stencil_flux<false>(q2, sy, fy), stencil_flux<false>(q3, sy, fy));
-        if (hz)
-        {
-            if (top)
             {
                 const double f = (double)fz;
-                oz = make_float4((float)(f * (double)q0[c]), (float)(f * (double)q1[c]), (float)(f * (double)q2[c]),
-                                 (float)(f * (double)q3[c]));
+                oz = make_float4((float)(f * (double)q.x), (float)(f * (double)q.y), (float)(f * (double)q.z),
+                                 (float)(f * (double)q.w));
             }
-            else
-                oz = make_float4(stencil_flux<false>(q0, sz, fz), stencil_flux<false>(q1, sz, fz),
-                                 stencil_flux<false>(q2, sz, fz), stencil_flux<false>(q3, sz, fz));
         }
+        else oz = stencil_flux4<kFp32>(q4, sz, fz);
     }
     sf4[c] = ox;
     sf4[n + c] = oy;
     sf4[2 * n + c] = oz;
 }
 
-template <bool kFp32, class QIn>
-__device__ __forceinline__ void transport_limiter_cell4(const TransportParams& T, QIn&& q_of,
+template <bool kFp32>
+__device__ __forceinline__ void transport_limiter_cell4(const TransportParams& T, const float4* __restrict__ q4,
                                                         const float* __restrict__ rho_begin,
                                                         const float4* __restrict__ sf4, float4* __restrict__ rl4,
                                                         int c)
@@ -695,18 +715,20 @@ __device__ __forceinline__ void transport_limiter_cell4(const TransportParams& T
     const float4 fxp = sf4[c], fxm = sf4[cxm], fyp = sf4[n + c], fym = sf4[n + cym];
     const float4 fzp = sf4[2 * n + c], fzm = sf4[2 * n + czm];
     const float rb = rho_begin[c];
+    const float4 q = q4[c];
     float r[4];
 #pragma unroll
     for (int s = 0; s < 4; ++s)
         r[s] = T.positive_definite[s]
                    ? limiter_factor<kFp32>(T, lane4(fxp, s), lane4(fxm, s), lane4(fyp, s), lane4(fym, s),
-                                           lane4(fzp, s), lane4(fzm, s), xp, xm, yp, ym, zp, zm, rb, q_of(s)[c])
+                                           lane4(fzp, s), lane4(fzm, s), xp, xm, yp, ym, zp, zm, rb, lane4(q, s))
                    : 1.0f;
     rl4[c] = make_float4(r[0], r[1], r[2], r[3]);
 }
 
 template <bool kFp32, class QIn, class QOut>
-__device__ __forceinline__ void transport_update_cell4(const TransportParams& T, QIn&& q_of, QOut&& qo_of,
+__device__ __forceinline__ void transport_update_cell4(const TransportParams& T, const float4* __restrict__ q4,
+                                                       QIn&& q_of, QOut&& qo_of,
                                                        const float* __restrict__ rho_end,
                                                        const float* __restrict__ rho_begin,
                                                        const float4* __restrict__ sf4,
@@ -735,9 +757,8 @@ __device__ __forceinline__ void transport_update_cell4(const TransportParams& T,
     const float4 rc = rl4[c], rxp = rl4[cxp], rxm = rl4[cxm], ryp = rl4[cyp], rym = rl4[cym];
     const float4 rzp = rl4[czp], rzm = rl4[czm];
     const float re = rho_end[c], rb = rho_begin[c];
-    float qraw[4];
-#pragma unroll
-    for (int s = 0; s < 4; ++s) qraw[s] = q_of(s)[c];
+    const float4 q = q4[c];
+    const float qraw[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
     for (int s = 0; s < 4; ++s)
     {
