@@ -49,7 +49,7 @@ struct __align__(16) EngineMember
     float *sf;        // [3][cells] float4 face fluxes (one lane per scalar)
     float *rl;        // [cells] float4 limiter factors
     float *q4;        // [cells] float4 theta, qv, qc, qr before transport (written by the slow predictor)
-    float *k1, *xs;   // [4][cells] Heun k1 and predictor state
+    float *k1, *xs;   // [cells] float4 {u, v, w, p}: Heun k1 and predictor state
     float *eos;       // EOS candidate pressure
     unsigned* status; // this member's status word (kStatus* bits)
     const double *rho0, *p0, *qv0, *u0, *v0;
@@ -114,10 +114,8 @@ static __global__ void __launch_bounds__(256, 4) engine_slow_predict_kernel(cons
                                                                   long long tiles)
 {
     for_member_items(table, prefix, tiles, kItemCells, [&](const EngineMember& M, int c) {
-        const int n = M.items[kItemCells];
-        slow_predict_cell<Policy>(M.S, M.u, M.v, M.w, M.rho, M.p, M.qv, M.qc, M.qr, M.rho0, M.qv0, M.u0, M.v0, M.k1,
-                                  M.k1 + n, M.k1 + 2 * n, M.k1 + 3 * n, M.xs, M.xs + n, M.xs + 2 * n, M.xs + 3 * n,
-                                  c);
+        slow_predict_packed<Policy>(M.S, M.u, M.v, M.w, M.rho, M.p, M.qv, M.qc, M.qr, M.rho0, M.qv0, M.u0, M.v0,
+                                    reinterpret_cast<float4*>(M.k1), reinterpret_cast<float4*>(M.xs), c);
         // The transported scalars do not change before transport: keep their
         // interleaved copy for the transport kernels.
         reinterpret_cast<float4*>(M.q4)[c] = make_float4(M.theta[c], M.qv[c], M.qc[c], M.qr[c]);
@@ -130,10 +128,8 @@ static __global__ void __launch_bounds__(256, 4) engine_slow_correct_kernel(cons
                                                                   long long tiles)
 {
     for_member_items(table, prefix, tiles, kItemCells, [&](const EngineMember& M, int c) {
-        const int n = M.items[kItemCells];
-        slow_correct_cell<Policy>(M.S, M.xs, M.xs + n, M.xs + 2 * n, M.rho, M.xs + 3 * n, M.qv, M.qc, M.qr, M.rho0,
-                                  M.qv0, M.u0, M.v0, M.k1, M.k1 + n, M.k1 + 2 * n, M.k1 + 3 * n, M.u, M.v, M.w,
-                                  M.p, nullptr, nullptr, nullptr, nullptr, c);
+        slow_correct_packed<Policy>(M.S, reinterpret_cast<const float4*>(M.xs), M.rho, M.qv, M.qc, M.qr, M.rho0,
+                                    M.qv0, M.u0, M.v0, reinterpret_cast<const float4*>(M.k1), M.u, M.v, M.w, M.p, c);
     });
 }
 

@@ -68,26 +68,19 @@ __host__ __device__ inline void finish_fp32(SlowParams& S)
 // every intermediate negated (the reference's own operation order, so the
 // result is bit-identical), and lanes with opposite winds do not diverge.
 template <class real>
-__device__ __forceinline__ real upwind_deriv(const float* __restrict__ f, int c, int stride, int idx, int n, real a,
-                                             real inv_d, real inv_d6, real inv_d60)
+__device__ __forceinline__ real upwind_from(int half, real cc, real m1, real p1, real m2, real p2, real m3, real p3,
+                                            real a, real inv_d, real inv_d6, real inv_d60)
 {
-    const int half = min(idx, n - 1 - idx);
-    const real cc = (real)f[c];
     if (half <= 0) return (real)0;
     const bool pos = a >= (real)0;
-    // Both sides are loaded before the wind sign is known, so no load waits
-    // on the velocity arithmetic; the sign then only selects registers.
-    const real m1 = (real)f[c - stride], p1 = (real)f[c + stride];
     if (half == 1)
     {
         const real v = (cc - (pos ? m1 : p1)) * inv_d;
         return pos ? v : -v;
     }
-    const real m2 = (real)f[c - 2 * stride], p2 = (real)f[c + 2 * stride];
     if (half == 2)
         return pos ? ((real)2 * p1 + (real)3 * cc - (real)6 * m1 + m2) * inv_d6
                    : (-p2 + (real)6 * p1 - (real)3 * cc - (real)2 * m1) * inv_d6;
-    const real m3 = (real)f[c - 3 * stride], p3 = (real)f[c + 3 * stride];
     const real x1 = pos ? m1 : p1, x2 = pos ? m2 : p2, x3 = pos ? m3 : p3;
     const real y1 = pos ? p1 : m1, y2 = pos ? p2 : m2;
     const real v = ((real)-2 * x3 + (real)15 * x2 - (real)60 * x1 + (real)20 * cc + (real)30 * y1 - (real)3 * y2) *
@@ -95,15 +88,76 @@ __device__ __forceinline__ real upwind_deriv(const float* __restrict__ f, int c,
     return pos ? v : -v;
 }
 
+// The velocity and pressure fields seen from one cell: uvw(off) / p(off) are
+// the values `off` cells away (k fastest).  PlanarState reads four arrays;
+// PackedState one array of float4 {u, v, w, p} cells (the member engine's
+// Heun predictor), where a stencil point's three velocities are one 16-byte
+// load.
+struct PlanarState
+{
+    const float* __restrict__ u;  // each at the cell
+    const float* __restrict__ v;
+    const float* __restrict__ w;
+    const float* __restrict__ pr;
+    __device__ __forceinline__ float3 uvw(int o) const { return make_float3(u[o], v[o], w[o]); }
+    __device__ __forceinline__ float U(int o) const { return u[o]; }
+    __device__ __forceinline__ float V(int o) const { return v[o]; }
+    __device__ __forceinline__ float W(int o) const { return w[o]; }
+    __device__ __forceinline__ float P(int o) const { return pr[o]; }
+};
+
+struct PackedState
+{
+    const float4* __restrict__ x;  // at the cell
+    __device__ __forceinline__ float3 uvw(int o) const
+    {
+        const float4 t = x[o];
+        return make_float3(t.x, t.y, t.z);
+    }
+    __device__ __forceinline__ float U(int o) const { return x[o].x; }
+    __device__ __forceinline__ float V(int o) const { return x[o].y; }
+    __device__ __forceinline__ float W(int o) const { return x[o].z; }
+    __device__ __forceinline__ float P(int o) const { return x[o].w; }
+};
+
+// The upwind derivatives of u, v and w along one axis (stride, index idx of
+// n), each with its own advecting wind: one set of stencil-point loads for
+// the three fields.  Only points inside the grid are read (the half-width
+// decides the order, as in the reference).
+template <class real, class State>
+__device__ __forceinline__ void upwind3(const State& X, int stride, int idx, int n, real au, real av, real aw,
+                                        real inv_d, real inv_d6, real inv_d60, real& du, real& dv, real& dw)
+{
+    const int half = min(idx, n - 1 - idx);
+    if (half <= 0)
+    {
+        du = dv = dw = (real)0;
+        return;
+    }
+    const float3 cc = X.uvw(0), m1 = X.uvw(-stride), p1 = X.uvw(stride);
+    float3 m2 = cc, p2 = cc, m3 = cc, p3 = cc;
+    if (half >= 2)
+    {
+        m2 = X.uvw(-2 * stride);
+        p2 = X.uvw(2 * stride);
+    }
+    if (half >= 3)
+    {
+        m3 = X.uvw(-3 * stride);
+        p3 = X.uvw(3 * stride);
+    }
+    du = upwind_from<real>(half, cc.x, m1.x, p1.x, m2.x, p2.x, m3.x, p3.x, au, inv_d, inv_d6, inv_d60);
+    dv = upwind_from<real>(half, cc.y, m1.y, p1.y, m2.y, p2.y, m3.y, p3.y, av, inv_d, inv_d6, inv_d60);
+    dw = upwind_from<real>(half, cc.z, m1.z, p1.z, m2.z, p2.z, m3.z, p3.z, aw, inv_d, inv_d6, inv_d60);
+}
+
 // The four slow tendencies of cell c (zero outside their index ranges).
 // Reference policy: the reference's FP64 interior arithmetic and order.  FP32
 // policy: the same stencils in FP32, the base-state face averages formed in
 // FP64 and rounded once.
-template <class Policy>
-__device__ __forceinline__ void slow_tendencies_at(const SlowParams& S, int c, int i, int j, int k,
-                                                   const float* __restrict__ u, const float* __restrict__ v,
-                                                   const float* __restrict__ w, const float* __restrict__ rho,
-                                                   const float* __restrict__ p, const float* __restrict__ qv,
+template <class Policy, class State>
+__device__ __forceinline__ void slow_tendencies_at(const SlowParams& S, int c, int i, int j, int k, const State& X,
+                                                   const float* __restrict__ rho, const float* __restrict__ qv,
                                                    const float* __restrict__ qc, const float* __restrict__ qr,
                                                    const double* __restrict__ rho0, const double* __restrict__ qv0,
                                                    const double* __restrict__ u0, const double* __restrict__ v0,
@@ -135,54 +189,53 @@ __device__ __forceinline__ void slow_tendencies_at(const SlowParams& S, int c, i
         if constexpr (f32) return isfinite(t) ? t : 0.0f;
         else return (float)finite_or_zero((double)t);
     };
+    // Advecting winds of du (x-face), dv (y-face) and dw (z-face).
+    const real ux_u = (real)X.U(0);
+    const real uy_u = q * ((real)X.V(-sy) + (real)X.V(0) + (real)X.V(sx - sy) + (real)X.V(sx));
+    const real tux_u = ux_u - fu, tuy_u = uy_u - fv;
+    const real wx = (k == 0) ? q * ((real)X.W(0) + (real)X.W(sx))
+                             : q * ((real)X.W(-1) + (real)X.W(0) + (real)X.W(sx - 1) + (real)X.W(sx));
+    const real vy = (real)X.V(0);
+    const real ux_v = q * ((real)X.U(-sx) + (real)X.U(0) + (real)X.U(sy - sx) + (real)X.U(sy));
+    const real tvy = vy - fv, tux_v = ux_v - fu;
+    const real wy = (k == 0) ? q * ((real)X.W(0) + (real)X.W(sy))
+                             : q * ((real)X.W(-1) + (real)X.W(0) + (real)X.W(sy - 1) + (real)X.W(sy));
+    const real wz = (real)X.W(0);
+    const real ux_w = q * ((real)X.U(-sx) + (real)X.U(0) + (real)X.U(1 - sx) + (real)X.U(1));
+    const real uy_w = q * ((real)X.V(-sy) + (real)X.V(0) + (real)X.V(1 - sy) + (real)X.V(1));
+    const real tux_w = ux_w - fu, tuy_w = uy_w - fv;
+    // Upwind derivatives, one axis at a time for the three fields.
+    real dxu, dxv, dxw, dyu, dyv, dyw, dzu, dzv, dzw;
+    upwind3<real>(X, sx, i, d.nx, tux_u, tux_v, tux_w, inv_dx, x6, x60, dxu, dxv, dxw);
+    upwind3<real>(X, sy, j, d.ny, tuy_u, tvy, tuy_w, inv_dy, y6, y60, dyu, dyv, dyw);
+    if (k == 0)
+    {
+        dzu = (wx >= (real)0) ? (real)0 : ((real)X.U(1) - (real)X.U(0)) * inv_dz;
+        dzv = (wy >= (real)0) ? (real)0 : ((real)X.V(1) - (real)X.V(0)) * inv_dz;
+        dzw = (wz >= (real)0) ? ((real)X.W(0) - (real)0) * inv_dz : ((real)X.W(1) - (real)X.W(0)) * inv_dz;
+    }
+    else upwind3<real>(X, 1, k, d.nz, wx, wy, wz, inv_dz, z6, z60, dzu, dzv, dzw);
     // du at the x-face
     {
-        const real ux = (real)u[c];
-        const real uy = q * ((real)v[c - sy] + (real)v[c] + (real)v[c + sx - sy] + (real)v[c + sx]);
-        const real tux = ux - fu, tuy = uy - fv;
-        const real wx = (k == 0) ? q * ((real)w[c] + (real)w[c + sx])
-                                 : q * ((real)w[c - 1] + (real)w[c] + (real)w[c + sx - 1] + (real)w[c + sx]);
-        const real ddx = upwind_deriv<real>(u, c, sx, i, d.nx, tux, inv_dx, x6, x60);
-        const real ddy = upwind_deriv<real>(u, c, sy, j, d.ny, tuy, inv_dy, y6, y60);
-        const real ddz = (k == 0) ? ((wx >= (real)0) ? (real)0 : ((real)u[c + 1] - (real)u[c]) * inv_dz)
-                                  : upwind_deriv<real>(u, c, 1, k, d.nz, wx, inv_dz, z6, z60);
         const real v0k = v0 ? (real)v0[k] : (real)0;
-        const real du = -tux * ddx - tuy * ddy - wx * ddz + cf * (uy - v0k);
+        const real du = -tux_u * dxu - tuy_u * dyu - wx * dzu + cf * (uy_u - v0k);
         out_u = store(du);
     }
     // dv at the y-face
     {
-        const real vy = (real)v[c];
-        const real ux = q * ((real)u[c - sx] + (real)u[c] + (real)u[c - sx + sy] + (real)u[c + sy]);
-        const real tvy = vy - fv, tux = ux - fu;
-        const real wy = (k == 0) ? q * ((real)w[c] + (real)w[c + sy])
-                                 : q * ((real)w[c - 1] + (real)w[c] + (real)w[c + sy - 1] + (real)w[c + sy]);
-        const real ddx = upwind_deriv<real>(v, c, sx, i, d.nx, tux, inv_dx, x6, x60);
-        const real ddy = upwind_deriv<real>(v, c, sy, j, d.ny, tvy, inv_dy, y6, y60);
-        const real ddz = (k == 0) ? ((wy >= (real)0) ? (real)0 : ((real)v[c + 1] - (real)v[c]) * inv_dz)
-                                  : upwind_deriv<real>(v, c, 1, k, d.nz, wy, inv_dz, z6, z60);
         const real u0k = u0 ? (real)u0[k] : (real)0;
-        const real dv = -tux * ddx - tvy * ddy - wy * ddz - cf * (ux - u0k);
+        const real dv = -tux_v * dxv - tvy * dyv - wy * dzv - cf * (ux_v - u0k);
         out_v = store(dv);
     }
     // dw at the z-face
     {
-        const real wz = (real)w[c];
-        const real ux = q * ((real)u[c - sx] + (real)u[c] + (real)u[c - sx + 1] + (real)u[c + 1]);
-        const real uy = q * ((real)v[c - sy] + (real)v[c] + (real)v[c - sy + 1] + (real)v[c + 1]);
-        const real tux = ux - fu, tuy = uy - fv;
-        const real ddx = upwind_deriv<real>(w, c, sx, i, d.nx, tux, inv_dx, x6, x60);
-        const real ddy = upwind_deriv<real>(w, c, sy, j, d.ny, tuy, inv_dy, y6, y60);
-        const real ddz = (k == 0) ? ((wz >= (real)0) ? ((real)w[c] - (real)0) * inv_dz : ((real)w[c + 1] - (real)w[c]) * inv_dz)
-                                  : upwind_deriv<real>(w, c, 1, k, d.nz, wz, inv_dz, z6, z60);
-        real forcing;
         if constexpr (f32)
         {
             const float g = S.gravity_f;
             const float rho_face = 0.5f * (rho[c] + rho[c + 1]);
             const float rho_s = (isfinite(rho_face) && rho_face > 1.0e-6f) ? rho_face : 1.0f;
             const float rho0_face = (float)(0.5 * (rho0[k] + rho0[k + 1]));
-            forcing = -g * (rho_face - rho0_face) / rho_s;
+            float forcing = -g * (rho_face - rho0_face) / rho_s;
             if (S.moist)
             {
                 const float qf = 0.5f * (qv[c] + qv[c + 1]);
@@ -191,6 +244,8 @@ __device__ __forceinline__ void slow_tendencies_at(const SlowParams& S, int c, i
             }
             if (S.loading)
                 forcing += -g * (0.5f * ((qc[c] + qr[c]) + (qc[c + 1] + qr[c + 1])));
+            const real dw = -tux_w * dxw - tuy_w * dyw - wz * dzw + forcing;
+            out_w = store(dw);
         }
         else
         {
@@ -213,23 +268,17 @@ __device__ __forceinline__ void slow_tendencies_at(const SlowParams& S, int c, i
                 const double hi = (double)qc[c + 1] + (double)qr[c + 1] + 0.0 + 0.0 + 0.0 + 0.0;
                 load = -g * (0.5 * (lo + hi));
             }
-            forcing = 0;
-            const real dw = -tux * ddx - tuy * ddy - wz * ddz + (real)buoy + (real)moist + (real)load;
-            out_w = store(dw);
-        }
-        if constexpr (f32)
-        {
-            const real dw = -tux * ddx - tuy * ddy - wz * ddz + forcing;
+            const real dw = -tux_w * dxw - tuy_w * dyw - wz * dzw + (real)buoy + (real)moist + (real)load;
             out_w = store(dw);
         }
     }
     // dp at the centre
     if (k >= 1)
     {
-        const real uc = h * ((real)u[c] + (real)u[c - sx]);
-        const real vc = h * ((real)v[c] + (real)v[c - sy]);
+        const real uc = h * ((real)X.U(0) + (real)X.U(-sx));
+        const real vc = h * ((real)X.V(0) + (real)X.V(-sy));
         const real tuc = uc - fu, tvc = vc - fv;
-        const real wc = h * ((real)w[c] + (real)w[c - 1]);
+        const real wc = h * ((real)X.W(0) + (real)X.W(-1));
         real hx, hy, hz;
         if constexpr (f32)
         {
@@ -239,9 +288,9 @@ __device__ __forceinline__ void slow_tendencies_at(const SlowParams& S, int c, i
         {
             hx = (real)(0.5 * S.inv_dx); hy = (real)(0.5 * S.inv_dy); hz = (real)(0.5 * S.inv_dz);
         }
-        const real dpdx = ((real)p[c + sx] - (real)p[c - sx]) * hx;
-        const real dpdy = ((real)p[c + sy] - (real)p[c - sy]) * hy;
-        const real dpdz = ((real)p[c + 1] - (real)p[c - 1]) * hz;
+        const real dpdx = ((real)X.P(sx) - (real)X.P(-sx)) * hx;
+        const real dpdy = ((real)X.P(sy) - (real)X.P(-sy)) * hy;
+        const real dpdz = ((real)X.P(1) - (real)X.P(-1)) * hz;
         out_p = store(-tuc * dpdx - tvc * dpdy - wc * dpdz);
     }
 }
@@ -270,7 +319,8 @@ __device__ __forceinline__ void slow_predict_cell(
     int i, j, k;
     decompose(S.d, c, i, j, k);
     float tu, tv, tw, tp;
-    slow_tendencies_at<Policy>(S, c, i, j, k, u, v, w, rho, p, qv, qc, qr, rho0, qv0, u0, v0, tu, tv, tw, tp);
+    slow_tendencies_at<Policy>(S, c, i, j, k, PlanarState{u + c, v + c, w + c, p + c}, rho, qv, qc, qr, rho0, qv0, u0,
+                               v0, tu, tv, tw, tp);
     k1u[c] = tu;
     k1v[c] = tv;
     k1w[c] = tw;
@@ -315,7 +365,8 @@ __device__ __forceinline__ void slow_correct_cell(
     int i, j, k;
     decompose(S.d, c, i, j, k);
     float tu, tv, tw, tp;
-    slow_tendencies_at<Policy>(S, c, i, j, k, su, sv, sw, rho, sp, qv, qc, qr, rho0, qv0, u0, v0, tu, tv, tw, tp);
+    slow_tendencies_at<Policy>(S, c, i, j, k, PlanarState{su + c, sv + c, sw + c, sp + c}, rho, qv, qc, qr, rho0, qv0,
+                               u0, v0, tu, tv, tw, tp);
     tu = __fmul_rn(0.5f, __fadd_rn(tu, k1u[c]));
     tv = __fmul_rn(0.5f, __fadd_rn(tv, k1v[c]));
     tw = __fmul_rn(0.5f, __fadd_rn(tw, k1w[c]));
@@ -327,6 +378,50 @@ __device__ __forceinline__ void slow_correct_cell(
         tw_out[c] = tw;
         tp_out[c] = tp;
     }
+    u[c] = slow_apply_one<Policy>(S, u[c], tu);
+    v[c] = slow_apply_one<Policy>(S, v[c], tv);
+    w[c] = slow_apply_one<Policy>(S, w[c], tw);
+    p[c] = slow_apply_one<Policy>(S, p[c], tp);
+}
+
+// The member engine's form: k1 and the predictor as one float4 {u, v, w, p}
+// per cell, so the corrector reads a stencil point's predictor velocities
+// with one load.  Same arithmetic as slow_predict_cell / slow_correct_cell.
+template <class Policy>
+__device__ __forceinline__ void slow_predict_packed(
+    const SlowParams& S, const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w,
+    const float* __restrict__ rho, const float* __restrict__ p, const float* __restrict__ qv,
+    const float* __restrict__ qc, const float* __restrict__ qr, const double* __restrict__ rho0,
+    const double* __restrict__ qv0, const double* __restrict__ u0, const double* __restrict__ v0,
+    float4* __restrict__ k1, float4* __restrict__ xs, int c)
+{
+    int i, j, k;
+    decompose(S.d, c, i, j, k);
+    float tu, tv, tw, tp;
+    slow_tendencies_at<Policy>(S, c, i, j, k, PlanarState{u + c, v + c, w + c, p + c}, rho, qv, qc, qr, rho0, qv0, u0,
+                               v0, tu, tv, tw, tp);
+    k1[c] = make_float4(tu, tv, tw, tp);
+    xs[c] = make_float4(slow_apply_one<Policy>(S, u[c], tu), slow_apply_one<Policy>(S, v[c], tv),
+                        slow_apply_one<Policy>(S, w[c], tw), slow_apply_one<Policy>(S, p[c], tp));
+}
+
+template <class Policy>
+__device__ __forceinline__ void slow_correct_packed(
+    const SlowParams& S, const float4* __restrict__ xs, const float* __restrict__ rho, const float* __restrict__ qv,
+    const float* __restrict__ qc, const float* __restrict__ qr, const double* __restrict__ rho0,
+    const double* __restrict__ qv0, const double* __restrict__ u0, const double* __restrict__ v0,
+    const float4* __restrict__ k1, float* __restrict__ u, float* __restrict__ v, float* __restrict__ w,
+    float* __restrict__ p, int c)
+{
+    int i, j, k;
+    decompose(S.d, c, i, j, k);
+    float tu, tv, tw, tp;
+    slow_tendencies_at<Policy>(S, c, i, j, k, PackedState{xs + c}, rho, qv, qc, qr, rho0, qv0, u0, v0, tu, tv, tw, tp);
+    const float4 a = k1[c];
+    tu = __fmul_rn(0.5f, __fadd_rn(tu, a.x));
+    tv = __fmul_rn(0.5f, __fadd_rn(tv, a.y));
+    tw = __fmul_rn(0.5f, __fadd_rn(tw, a.z));
+    tp = __fmul_rn(0.5f, __fadd_rn(tp, a.w));
     u[c] = slow_apply_one<Policy>(S, u[c], tu);
     v[c] = slow_apply_one<Policy>(S, v[c], tv);
     w[c] = slow_apply_one<Policy>(S, w[c], tw);
