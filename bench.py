@@ -56,7 +56,7 @@ def parse():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--members", type=int, default=64)
-    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--lanes", type=int, default=4,
                     help="parallel member groups inside the engine's step graph")
     ap.add_argument("--e2e-groups", type=int, default=8,
