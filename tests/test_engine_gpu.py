@@ -338,3 +338,53 @@ def test_fp32_form_error_against_fp64_is_the_reference_forms(ctx):
     for k, e32 in errors[cuda.PRECISION_FP32].items():
         eref = errors[cuda.PRECISION_REFERENCE][k]
         assert np.isfinite(e32) and e32 <= 1.5 * eref + 1e-7, (k, e32, eref)
+
+
+def test_engine_minimal_members_match_oracle(ctx, o32):
+    """Members at the admission minimum (4x4 columns, 2 levels) and just
+    above: the vertical closure that the momentum pass applies to interior
+    columns meets nz = 2 (level 0 is also level nz - 2), one interior column
+    and a perimeter of all but one column.  Reference precision, bit-exact
+    against the oracle run alone; the FP32 form gives each member the same
+    bits alone and in the mix."""
+    specs = [((4, 4, 2), "radiative"), ((5, 4, 3), "walls_sponge"), ((4, 6, 2), "periodic_open"),
+             ((4, 4, 5), "walls_sponge")]
+    members = []
+    for i, (shape, bc) in enumerate(specs):
+        case = _case(shape, BCS[bc], seed=140 + i, dt=3.0)
+        members.append((case, *_state(case, 140 + i)))
+    run = EngineRun(ctx, precision=cuda.PRECISION_REFERENCE)
+    ids = [run.admit(c, st, base, coriolis_f=1e-4, n_substeps=4) for c, st, base in members]
+    run.step(3)
+    for mid, (case, st, base) in zip(ids, members):
+        got = run.read(mid)
+        want = _oracle_steps(o32, case, st, base, 4, 3, 1e-4)
+        for k in PROGNOSTIC:
+            assert_bitwise(got[k], want[k], f"{case.shape} {k}")
+    run.close()
+    mix = EngineRun(ctx, precision=cuda.PRECISION_FP32, lanes=2)
+    ids = [mix.admit(c, st, base, n_substeps=4) for c, st, base in members]
+    mix.step(2)
+    for mid, (case, st, base) in zip(ids, members):
+        alone = EngineRun(ctx, precision=cuda.PRECISION_FP32)
+        a = alone.admit(case, st, base, n_substeps=4)
+        alone.step(2)
+        want = alone.read(a)
+        alone.close()
+        got = mix.read(mid)
+        for k in PROGNOSTIC:
+            assert_bitwise(got[k], want[k], f"fp32 {case.shape} {k}")
+    mix.close()
+
+
+def test_empty_engine_steps_and_copies_nothing(ctx):
+    eng = cuda.Engine(ctx)
+    eng.step(2)
+    eng.synchronize()
+    assert eng.members == 0 and eng.image_bytes() == 0
+    img = np.zeros(4, np.float32)
+    eng.upload_image_async(img)
+    eng.download_image_async(img)
+    eng.synchronize()
+    assert eng.lanes == 0 and not img.any()
+    eng.close()
