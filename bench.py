@@ -66,6 +66,7 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-error", action="store_true")
+    ap.add_argument("--no-relaxation", action="store_true")
     ap.add_argument("--serving-requests", type=int, default=32)
     ap.add_argument("--error-seconds", type=float, default=600.0)
     ap.add_argument("--precision", choices=("fp32", "reference"), default="fp32",
@@ -299,6 +300,44 @@ def error_study(ctx, seconds):
     return out
 
 
+def relaxation_study(ctx, device):
+    """The end-of-step sponge (nimbus_cuda_state_relaxation, the next row
+    after the large step) on one 512x512x80 level (four fields of 84 MB, larger
+    than L2) with the reference's default sponge: device-timed, against the
+    HBM roofline.  Algorithmic bytes: 16 read + 16 written per cell the sponge
+    touches (upper levels, lid levels, lateral band); untouched cells move
+    nothing."""
+    import numpy as np
+    import torch
+
+    from nimbus_b200 import cuda
+    from nimbus_b200.initial import Case, initial_state
+    from nimbus_b200.sponge import SpongeConfig, build_profiles
+
+    case = Case(512, 512, 80, 500.0, 500.0, 20000.0 / 80, 3.0, seed=11)
+    st, base = initial_state(case)
+    P = build_profiles(SpongeConfig(wind=(0.0, 0.0, 5.0, 2.0, 15.0, 6.0)), case.nz, case.dz, base["theta0"])
+    dev = {k: torch.from_numpy(np.ascontiguousarray(st[k])).to(f"cuda:{device}") for k in ("u", "v", "w", "theta")}
+    args = cuda.state_relaxation_args(dev, P, case.dt, memory=cuda.MEMORY_DEVICE)
+    on = (P.alpha > 0) | (P.upper_w_alpha > 0) | (P.w_only_alpha > 0)
+    i = np.arange(case.nx)[:, None]
+    j = np.arange(case.ny)[None, :]
+    band = np.minimum(np.minimum(i, case.nx - 1 - i), np.minimum(j, case.ny - 1 - j)) < len(P.lateral_alpha)
+    touched = int(on.sum()) * case.nx * case.ny + int(band.sum()) * int((~on).sum())
+    stream = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{device}")
+    for _ in range(3):
+        ctx.check(ctx.state_relaxation(args))
+    launches = 20
+    ms = time_on_stream(torch, stream, lambda: ctx.check(ctx.state_relaxation(args)), launches) / launches
+    ctx.synchronize()
+    peak, kind = load_peaks()
+    achieved = 32.0 * touched / (ms / 1e3) / 1e9
+    return {"grid": list(case.shape), "cells": case.cells, "cells_touched": touched,
+            "ms_per_call": ms, "achieved_gbs": achieved, "peak_gbs": peak, "frac": achieved / peak,
+            "peak_kind": kind, "algorithmic_bytes_per_touched_cell": 32,
+            "note": "includes the host forming the per-level factors and staging the tables each call"}
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -436,7 +475,10 @@ def run_ours(args):
     serving = None
     error = None
     cpu = None
+    relaxation = None
     if rank == 0 and world == 1:
+        if not args.no_relaxation:
+            relaxation = relaxation_study(ctx, device)
         if not args.no_serving:
             serving = serving_study(ctx, args, precision)
         if not args.no_error:
@@ -475,6 +517,7 @@ def run_ours(args):
                 "plain": plain,
                 "serving": serving,
                 "error_vs_fp64": error,
+                "state_relaxation": relaxation,
                 "parallelism": f"{world} GPU(s), each with its own independent ensemble (no collective)",
                 "l2": "inputs larger than L2 (%.1f GB resident per GPU)" % (cells * 4 * 40 / 1e9),
                 "algorithmic_bytes_per_step": bytes_per_step,

@@ -148,7 +148,7 @@ enum
     NIMBUS_KERNEL_TRANSPORT_LIMITER = 4,
     NIMBUS_KERNEL_TRANSPORT_UPDATE = 5,
     NIMBUS_KERNEL_SLOW = 6,               /* slow tendencies (k1+predictor, k2+apply) */
-    NIMBUS_KERNEL_MICROPHYSICS = 7,       /* Kessler and the EOS re-projection */
+    NIMBUS_KERNEL_MICROPHYSICS = 7,       /* Kessler, the EOS re-projection and the end-of-step sponge */
     NIMBUS_KERNEL_FAMILIES = 8
 };
 /* When enabled, every launch is bracketed by CUDA events on its own stream
@@ -442,6 +442,50 @@ typedef struct nimbus_eos_args
 } nimbus_eos_args;
 
 nimbus_status nimbus_cuda_eos_projection(nimbus_cuda_context* ctx, const nimbus_eos_args* a);
+
+/*
+ * End-of-step sponge (state relaxation) on a flat C-grid level: the upper
+ * Rayleigh sponge, the w-only lid absorber and the lateral band, in that
+ * order, relaxing u, v, w toward (u_ref, v_ref, 0) and theta toward
+ * theta_ref (rho and p are not relaxed).  Replaces apply_rayleigh_damping +
+ * apply_lateral_damping (src/core/infra/rayleigh_damping.cpp:720-1119,
+ * 1194-1476) as dynamics.cpp:7323-7340 calls them after the EOS projection,
+ * and the fused device dispatch dispatch_state_relaxation_cartesian_backend
+ * (src/compute/dispatch/dynamics.cpp:432-470).  Profiles are the reference
+ * runtime's FP64 per-level values (host memory): alpha / upper_w_alpha are
+ * the upper sponge's rates at scalar and w levels (a level takes part when
+ * either is > 0; upper_w_alpha applies to w when staggered), w_only_alpha the
+ * lid absorber's (levels with a rate > 0), lateral_alpha the band's rate by
+ * distance from the nearest lateral face.  A factor is -expm1(-alpha dt)
+ * (implicit_mode: alpha dt / (1 + alpha dt)); a cell adds factor * (ref -
+ * old) formed in FP64, rounded to FP32, in FP32: the reference's results bit
+ * for bit.  Invalid rates or dt where the reference would evaluate them:
+ * NIMBUS_ERR_INVALID_ARGUMENT, nothing changed.
+ */
+typedef struct nimbus_state_relaxation_args
+{
+    float* u;
+    float* v;
+    float* w;
+    float* theta;
+    int nx, ny, nz;
+    const double* alpha;          /* [nz] upper sponge, scalar levels */
+    const double* upper_w_alpha;  /* [nz] upper sponge, w levels */
+    const double* w_only_alpha;   /* [nz] w-only lid absorber */
+    const double* u_ref;          /* [nz] */
+    const double* v_ref;          /* [nz] */
+    const double* theta_ref;      /* [nz] theta0 base profile */
+    int lateral_width;            /* cells from each lateral face */
+    const double* lateral_alpha;  /* [lateral_width] */
+    int do_upper, do_w_only, do_lateral;
+    int staggered;                /* 1: w takes upper_w_alpha (C-grid) */
+    int implicit_mode;
+    double dt;
+    int memory;
+    void* stream;
+} nimbus_state_relaxation_args;
+
+nimbus_status nimbus_cuda_state_relaxation(nimbus_cuda_context* ctx, const nimbus_state_relaxation_args* a);
 
 /*
  * Acoustic boundary closure on its own: CartesianCGridBCScheme::apply_acoustic

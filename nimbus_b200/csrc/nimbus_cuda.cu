@@ -13,6 +13,7 @@
 #include "acoustic_split.cuh"
 #include "slow_kernels.cuh"
 #include "physics_kernels.cuh"
+#include "relaxation_kernels.cuh"
 #include "transport_kernels.cuh"
 
 #include <cmath>
@@ -749,6 +750,132 @@ nimbus_status nimbus_cuda_kessler_tendencies(nimbus_cuda_context* ctx, const nim
 nimbus_status nimbus_cuda_kessler_step(nimbus_cuda_context* ctx, const nimbus_kessler_args* a)
 {
     return kessler_entry(ctx, a, true);
+}
+
+// damping_relaxation_factor (rayleigh_damping.cpp:145-163): false where the
+// reference throws.
+static bool relaxation_factor(double alpha, double dt, int implicit_mode, double* out)
+{
+    if (!std::isfinite(alpha) || alpha < 0.0 || !std::isfinite(dt) || dt <= 0.0) return false;
+    const double scaled = alpha * dt;
+    if (!std::isfinite(scaled)) return false;
+    *out = implicit_mode ? scaled / (1.0 + scaled) : -std::expm1(-scaled);
+    return true;
+}
+
+nimbus_status nimbus_cuda_state_relaxation(nimbus_cuda_context* ctx, const nimbus_state_relaxation_args* a)
+{
+    if (!ctx || !a) return NIMBUS_ERR_INVALID_ARGUMENT;
+    if (!a->u || !a->v || !a->w || !a->theta || a->nx < 1 || a->ny < 1 || a->nz < 1 ||
+        !cells_fit(a->nx, a->ny, a->nz) || a->lateral_width < 0)
+        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "invalid state relaxation arguments");
+    if (a->memory != NIMBUS_MEMORY_HOST && a->memory != NIMBUS_MEMORY_DEVICE)
+        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "unknown memory kind");
+    const int nz = a->nz;
+    const bool upper = a->do_upper != 0, lid = a->do_w_only != 0;
+    const bool lateral = a->do_lateral != 0 && a->lateral_width > 0;
+    if ((upper && (!a->alpha || !a->upper_w_alpha)) || (lid && !a->w_only_alpha) || (lateral && !a->lateral_alpha) ||
+        ((upper || lateral) && (!a->u_ref || !a->v_ref || !a->theta_ref)))
+        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "a profile of an enabled sponge pass is null");
+    // Per-level tables: the factors the reference forms cell by cell depend
+    // on the level (or lateral distance) only; formed here once with the same
+    // expm1, and checked where the reference would evaluate them.
+    const int width = lateral ? a->lateral_width : 0;
+    std::vector<double> tab(6 * static_cast<size_t>(nz) + static_cast<size_t>(width > 0 ? width : 1), 0.0);
+    std::vector<unsigned char> on(2 * static_cast<size_t>(nz), 0);
+    double* up = tab.data();
+    double* up_w = up + nz;
+    double* lid_f = up_w + nz;
+    double* refs = lid_f + nz;  // u_ref, v_ref, theta_ref
+    double* lat = refs + 3 * nz;
+    for (int k = 0; k < nz; ++k)
+    {
+        if (upper && !(a->alpha[k] <= 0.0 && a->upper_w_alpha[k] <= 0.0))
+        {
+            on[k] = 1;
+            if (!relaxation_factor(a->alpha[k], a->dt, a->implicit_mode, &up[k]))
+                return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "upper sponge: alpha and dt must be finite, alpha >= 0, dt > 0");
+            if (!a->staggered) up_w[k] = up[k];
+            else if (!relaxation_factor(a->upper_w_alpha[k], a->dt, a->implicit_mode, &up_w[k]))
+                return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "upper sponge: alpha and dt must be finite, alpha >= 0, dt > 0");
+        }
+        if (lid && a->w_only_alpha[k] > 0.0)
+        {
+            on[nz + k] = 1;
+            if (!relaxation_factor(a->w_only_alpha[k], a->dt, a->implicit_mode, &lid_f[k]))
+                return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "w-only sponge: alpha and dt must be finite, dt > 0");
+        }
+        if (upper || lateral)
+        {
+            refs[k] = a->u_ref[k];
+            refs[nz + k] = a->v_ref[k];
+            refs[2 * nz + k] = a->theta_ref[k];
+        }
+    }
+    // Distances that occur on this grid (a band wider than half the domain
+    // is never reached by its inner entries, which the reference then never
+    // evaluates).
+    const int reach = std::min((a->nx - 1) / 2, (a->ny - 1) / 2);
+    for (int dd = 0; dd < width && dd <= reach; ++dd)
+        if (!relaxation_factor(a->lateral_alpha[dd], a->dt, a->implicit_mode, &lat[dd]))
+            return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "lateral sponge: alpha and dt must be finite, alpha >= 0, dt > 0");
+    if (!upper && !lid && !lateral) return NIMBUS_OK;
+
+    NB_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    if (a->memory == NIMBUS_MEMORY_DEVICE && a->stream) st = static_cast<cudaStream_t>(a->stream);
+    const size_t tab_bytes = tab.size() * sizeof(double);
+    unsigned char* dev = nullptr;
+    NB_TRY(ensure(ctx, kRelaxTables, tab_bytes + on.size(), &dev));
+    // Pageable sources: the call returns once the tables are staged.
+    NB_CUDA(ctx, cudaMemcpyAsync(dev, tab.data(), tab_bytes, cudaMemcpyHostToDevice, st));
+    NB_CUDA(ctx, cudaMemcpyAsync(dev + tab_bytes, on.data(), on.size(), cudaMemcpyHostToDevice, st));
+    const double* dt_ = reinterpret_cast<const double*>(dev);
+    RelaxTables R;
+    R.upper = dt_;
+    R.upper_w = dt_ + nz;
+    R.w_only = dt_ + 2 * nz;
+    R.u_ref = dt_ + 3 * nz;
+    R.v_ref = dt_ + 4 * nz;
+    R.th_ref = dt_ + 5 * nz;
+    R.lateral = dt_ + 6 * nz;
+    R.upper_on = dev + tab_bytes;
+    R.w_only_on = dev + tab_bytes + nz;
+    R.lateral_width = width;
+    R.do_upper = upper;
+    R.do_w_only = lid;
+    R.do_lateral = lateral;
+    const Dims d = make_dims(a->nx, a->ny, a->nz);
+    const long long n = d.cells();
+    float *u = a->u, *v = a->v, *w = a->w, *th = a->theta;
+    const size_t bytes = static_cast<size_t>(n) * sizeof(float);
+    if (a->memory == NIMBUS_MEMORY_HOST)
+    {
+        NB_TRY(ensure(ctx, kU, static_cast<size_t>(n), &u));
+        NB_TRY(ensure(ctx, kV, static_cast<size_t>(n), &v));
+        NB_TRY(ensure(ctx, kW, static_cast<size_t>(n), &w));
+        NB_TRY(ensure(ctx, kTheta, static_cast<size_t>(n), &th));
+        NB_TRY(upload(ctx, u, a->u, bytes));
+        NB_TRY(upload(ctx, v, a->v, bytes));
+        NB_TRY(upload(ctx, w, a->w, bytes));
+        NB_TRY(upload(ctx, th, a->theta, bytes));
+    }
+    {
+        LaunchTimer t(ctx, st, NIMBUS_KERNEL_MICROPHYSICS);
+        state_relaxation_kernel<<<grid_for(ctx, n), kThreads, 0, st>>>(d, R, u, v, w, th);
+        ctx->launches += 1;
+    }
+    NB_CUDA(ctx, cudaGetLastError());
+    if (a->memory == NIMBUS_MEMORY_HOST)
+    {
+        NB_CUDA(ctx, cudaStreamSynchronize(st));
+        NB_TRY(download(ctx, a->u, u, bytes));
+        NB_TRY(download(ctx, a->v, v, bytes));
+        NB_TRY(download(ctx, a->w, w, bytes));
+        NB_TRY(download(ctx, a->theta, th, bytes));
+        NB_CUDA(ctx, cudaStreamSynchronize(st));
+    }
+    return NIMBUS_OK;
 }
 
 nimbus_status nimbus_cuda_eos_projection(nimbus_cuda_context* ctx, const nimbus_eos_args* a)

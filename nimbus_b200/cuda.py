@@ -25,6 +25,7 @@ from . import initial
 LIB_PATH = Path(__file__).resolve().parent / "lib" / "libnimbus_cuda.so"
 
 NIMBUS_OK = 0
+NIMBUS_ERR_INVALID_ARGUMENT = 1
 NIMBUS_ERR_OUT_OF_MEMORY = 3
 NIMBUS_ERR_NONFINITE = 4
 STATUS_NAMES = {
@@ -120,6 +121,18 @@ class EosArgs(ctypes.Structure):
     ]
 
 
+class StateRelaxationArgs(ctypes.Structure):
+    _fields_ = [
+        ("u", _fp), ("v", _fp), ("w", _fp), ("theta", _fp),
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("alpha", _dp), ("upper_w_alpha", _dp), ("w_only_alpha", _dp), ("u_ref", _dp), ("v_ref", _dp),
+        ("theta_ref", _dp), ("lateral_width", ctypes.c_int), ("lateral_alpha", _dp),
+        ("do_upper", ctypes.c_int), ("do_w_only", ctypes.c_int), ("do_lateral", ctypes.c_int),
+        ("staggered", ctypes.c_int), ("implicit_mode", ctypes.c_int), ("dt", ctypes.c_double),
+        ("memory", ctypes.c_int), ("stream", ctypes.c_void_p),
+    ]
+
+
 class BoundaryArgs(ctypes.Structure):
     _fields_ = [
         ("u", _fp), ("v", _fp), ("w", _fp), ("rho", _fp), ("p", _fp), ("wave_history", _fp),
@@ -156,7 +169,7 @@ EXPORTED_SYMBOLS = (
     "nimbus_cuda_set_substep_form", "nimbus_cuda_autotune_substep",
     "nimbus_cuda_slow_tendencies", "nimbus_cuda_slow_step",
     "nimbus_cuda_kessler_tendencies", "nimbus_cuda_kessler_step", "nimbus_cuda_eos_projection",
-    "nimbus_cuda_acoustic_boundaries",
+    "nimbus_cuda_acoustic_boundaries", "nimbus_cuda_state_relaxation",
     "nimbus_cuda_engine_create", "nimbus_cuda_engine_destroy", "nimbus_cuda_engine_member_bytes",
     "nimbus_cuda_engine_admit", "nimbus_cuda_engine_retire", "nimbus_cuda_engine_read", "nimbus_cuda_engine_write", "nimbus_cuda_engine_step",
     "nimbus_cuda_engine_read_async", "nimbus_cuda_engine_write_async", "nimbus_cuda_engine_stream",
@@ -201,6 +214,7 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
     lib.nimbus_cuda_kessler_step.argtypes = [ctypes.c_void_p, ctypes.POINTER(KesslerArgs)]
     lib.nimbus_cuda_eos_projection.argtypes = [ctypes.c_void_p, ctypes.POINTER(EosArgs)]
     lib.nimbus_cuda_acoustic_boundaries.argtypes = [ctypes.c_void_p, ctypes.POINTER(BoundaryArgs)]
+    lib.nimbus_cuda_state_relaxation.argtypes = [ctypes.c_void_p, ctypes.POINTER(StateRelaxationArgs)]
     vp = ctypes.c_void_p
     lib.nimbus_cuda_engine_create.argtypes = [vp, ctypes.POINTER(vp)]
     lib.nimbus_cuda_engine_destroy.argtypes = [vp]
@@ -361,6 +375,9 @@ class Context:
     def acoustic_boundaries(self, args: BoundaryArgs) -> int:
         return self.lib.nimbus_cuda_acoustic_boundaries(self.handle, ctypes.byref(args))
 
+    def state_relaxation(self, args: StateRelaxationArgs) -> int:
+        return self.lib.nimbus_cuda_state_relaxation(self.handle, ctypes.byref(args))
+
 
 def clamp_defaults() -> dict:
     """The reference's dispatch constants (dynamics.cpp:4560-4586, field_bounds.hpp)."""
@@ -485,6 +502,28 @@ def kessler_args(st, dz, dt, domain=None, outputs=None, memory=MEMORY_HOST, stre
     a.dz, a.dt = dz, dt
     a.domain[:] = [int(x) for x in (domain or cgrid_cell_domain(nx, ny, nz))]
     a.dtheta_dt, a.dqv_dt, a.dqc_dt, a.dqr_dt = (_f(o) for o in outs)
+    a.memory = memory
+    a.stream = stream
+    return a
+
+
+def state_relaxation_args(fields, profiles, dt, memory=MEMORY_HOST, stream=None) -> StateRelaxationArgs:
+    """Argument block for nimbus_cuda_state_relaxation on fields' u, v, w,
+    theta with a nimbus_b200.sponge.SpongeProfiles."""
+    P = profiles
+    d = lambda x: np.ascontiguousarray(x, dtype=np.float64)  # noqa: E731
+    prof = [d(P.alpha), d(P.upper_w_alpha), d(P.w_only_alpha), d(P.u_ref), d(P.v_ref), d(P.theta_ref)]
+    lateral = d(P.lateral_alpha) if len(P.lateral_alpha) else None
+    a = StateRelaxationArgs()
+    a._keep = (fields, prof, lateral)
+    a.u, a.v, a.w, a.theta = (_f(fields[k]) for k in ("u", "v", "w", "theta"))
+    a.nx, a.ny, a.nz = tuple(fields["u"].shape)
+    a.alpha, a.upper_w_alpha, a.w_only_alpha, a.u_ref, a.v_ref, a.theta_ref = (_d(x) for x in prof)
+    a.lateral_width = len(P.lateral_alpha)
+    a.lateral_alpha = _d(lateral)
+    a.do_upper, a.do_w_only, a.do_lateral = int(P.do_upper), int(P.do_w_only), int(P.do_lateral)
+    a.staggered, a.implicit_mode = int(P.staggered), int(P.implicit_mode)
+    a.dt = float(dt)
     a.memory = memory
     a.stream = stream
     return a

@@ -186,6 +186,23 @@ class Restatement:
         return self.lib.oracle_eos_projection(nx, ny, nz, _fp(rho), _fp(theta), _fp(p), _opt(qv), _opt(qc),
                                               _opt(qr)) == 0
 
+    def state_relaxation(self, st, profiles, dt):
+        """The end-of-step sponge on st's u, v, w, theta in place
+        (oracle_state_relaxation); profiles as nimbus_b200.sponge.SpongeProfiles."""
+        u, v, w, th = (st[k] for k in ("u", "v", "w", "theta"))
+        self._chk(u, v, w, th)
+        nx, ny, nz = u.shape
+        P = profiles
+        d = lambda a: np.ascontiguousarray(a, dtype=np.float64)  # noqa: E731
+        arrs = [d(P.theta_ref), d(P.alpha), d(P.upper_w_alpha), d(P.w_only_alpha), d(P.u_ref), d(P.v_ref)]
+        lat = d(P.lateral_alpha) if len(P.lateral_alpha) else np.zeros(1)
+        rc = self.lib.oracle_state_relaxation(
+            nx, ny, nz, _fp(u), _fp(v), _fp(w), _fp(th), *[_fp(a) for a in arrs], int(len(P.lateral_alpha)), _fp(lat),
+            int(P.do_upper), int(P.do_w_only), int(P.do_lateral), int(P.staggered), int(P.implicit_mode),
+            ctypes.c_double(dt))
+        if rc != 0:
+            raise ValueError("state relaxation: invalid alpha or dt")
+
     def scalar_transport(self, qs, pd, rho_end, rho_begin, mfx, mfy, mfz, dt, grid, weno=True, top_open=False):
         self._chk(rho_end, rho_begin, mfx, mfy, mfz, *qs)
         nx, ny, nz = rho_end.shape
@@ -280,6 +297,27 @@ class ReferenceHarness:
         if rc < 0:
             self._rc(rc)
         return rc == 0
+
+    def state_relaxation(self, st, theta0, grid, dt, config):
+        """apply_rayleigh_damping then apply_lateral_damping on st's u, v, w,
+        theta in place, configured from a nimbus_b200.sponge.SpongeConfig;
+        returns the reference runtime's own profiles
+        (alpha, upper_w_alpha, w_only_alpha, u_ref, v_ref, lateral_alpha)."""
+        u, v, w, th = (st[k] for k in ("u", "v", "w", "theta"))
+        nx, ny, nz = u.shape
+        c = config
+        out = [np.zeros(nz) for _ in range(5)] + [np.zeros(max(c.lateral_width, 1))]
+        wind = (ctypes.c_double * 6)(*[float(x) for x in c.wind])
+        self._rc(self.lib.ref_state_relaxation(
+            _fp(u), _fp(v), _fp(w), _fp(th), _fp(np.ascontiguousarray(theta0, dtype=np.float64)), nx, ny, nz,
+            ctypes.c_double(grid[0]), ctypes.c_double(grid[1]), ctypes.c_double(grid[2]), ctypes.c_double(dt),
+            ctypes.c_double(c.z_damp), ctypes.c_double(c.alpha_max), int(c.w_only_cells),
+            ctypes.c_double(c.w_only_alpha_max), int(c.lateral_width), ctypes.c_double(c.lateral_alpha_max),
+            int(c.implicit_mode), wind, *[_fp(o) for o in out]))
+        names = ("alpha", "upper_w_alpha", "w_only_alpha", "u_ref", "v_ref", "lateral_alpha")
+        prof = dict(zip(names, out))
+        prof["lateral_alpha"] = prof["lateral_alpha"][:c.lateral_width]
+        return prof
 
     def large_step(self, st, base, grid, dt, n_substeps, bc, coriolis_f=0.0):
         """One large step of the hot path from the reference's own objects:

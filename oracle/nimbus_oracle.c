@@ -1158,3 +1158,86 @@ int oracle_eos_projection(int nx, int ny, int nz, const REAL* rho, const REAL* t
     }
     return 0;
 }
+
+/* ---- End-of-step sponge (state relaxation) ------------------------------
+ * apply_rayleigh_damping then apply_lateral_damping on a flat C-grid level
+ * (src/core/infra/rayleigh_damping.cpp:720-1119 upper + w-only passes,
+ * 1194-1476 lateral pass; relaxation factor :145-163).  Three passes over the
+ * whole grid in the reference's order; each cell's increment factor *
+ * (ref - old) is formed in FP64 and added to the stored value as the
+ * reference's Field3D proxy adds it (rounded to the storage type, then one
+ * storage-type add).  Profiles are the reference runtime's: alpha, upper_w_alpha,
+ * w_only_alpha, u_ref, v_ref, theta_ref per level; lateral_alpha by distance
+ * from the nearest lateral face.  Returns -1 (fields untouched from that pass
+ * on) where the reference would throw. */
+static int relax_factor(double alpha, double dt, int implicit_mode, double* out)
+{
+    if (!isfinite(alpha) || alpha < 0.0 || !isfinite(dt) || dt <= 0.0) return -1;
+    const double scaled = alpha * dt;
+    if (!isfinite(scaled)) return -1;
+    *out = implicit_mode ? scaled / (1.0 + scaled) : -expm1(-scaled);
+    return 0;
+}
+
+static void relax_add(REAL* x, double delta)
+{
+    *x = (REAL)(*x + (REAL)delta);
+}
+
+int oracle_state_relaxation(int nx, int ny, int nz, REAL* u, REAL* v, REAL* w, REAL* theta,
+                            const double* theta_ref, const double* alpha, const double* upper_w_alpha,
+                            const double* w_only_alpha, const double* u_ref, const double* v_ref,
+                            int lateral_width, const double* lateral_alpha, int do_upper, int do_w_only,
+                            int do_lateral, int staggered, int implicit_mode, double dt)
+{
+    const size_t cells = (size_t)nx * ny * nz;
+    if (do_upper)
+        for (size_t c = 0; c < cells; ++c)
+        {
+            const int k = (int)(c % (size_t)nz);
+            if (alpha[k] <= 0.0 && upper_w_alpha[k] <= 0.0) continue;
+            double f, fw;
+            if (relax_factor(alpha[k], dt, implicit_mode, &f)) return -1;
+            if (staggered)
+            {
+                if (relax_factor(upper_w_alpha[k], dt, implicit_mode, &fw)) return -1;
+            }
+            else fw = f;
+            const double u_old = u[c], v_old = v[c], w_old = w[c], th_old = theta[c];
+            relax_add(&u[c], f * (u_ref[k] - u_old));
+            relax_add(&v[c], f * (v_ref[k] - v_old));
+            relax_add(&w[c], fw * (0.0 - w_old));
+            relax_add(&theta[c], f * (theta_ref[k] - th_old));
+        }
+    if (do_w_only)
+        for (size_t c = 0; c < cells; ++c)
+        {
+            const int k = (int)(c % (size_t)nz);
+            if (w_only_alpha[k] <= 0.0) continue;
+            double fw;
+            if (relax_factor(w_only_alpha[k], dt, implicit_mode, &fw)) return -1;
+            const double w_old = w[c];
+            relax_add(&w[c], fw * (0.0 - w_old));
+        }
+    if (do_lateral && lateral_width > 0)
+        for (int i = 0; i < nx; ++i)
+            for (int j = 0; j < ny; ++j)
+            {
+                const int di = i < nx - 1 - i ? i : nx - 1 - i;
+                const int dj = j < ny - 1 - j ? j : ny - 1 - j;
+                const int dist = di < dj ? di : dj;
+                if (dist >= lateral_width) continue;
+                double f;
+                if (relax_factor(lateral_alpha[dist], dt, implicit_mode, &f)) return -1;
+                for (int k = 0; k < nz; ++k)
+                {
+                    const size_t c = ((size_t)i * ny + j) * nz + k;
+                    const double u_old = u[c], v_old = v[c], w_old = w[c], th_old = theta[c];
+                    relax_add(&u[c], f * (u_ref[k] - u_old));
+                    relax_add(&v[c], f * (v_ref[k] - v_old));
+                    relax_add(&w[c], f * (0.0 - w_old));
+                    relax_add(&theta[c], f * (theta_ref[k] - th_old));
+                }
+            }
+    return 0;
+}

@@ -25,6 +25,10 @@
 //                           (boundary_conditions_cartesian_cgrid.cpp:141-236)
 //   ref_eos_projection      tmv::dynamics_eos::apply_pressure_projection
 //                           (src/core/orchestration/dynamics/eos_apply.cpp:50-200)
+//   ref_state_relaxation    apply_rayleigh_damping then apply_lateral_damping
+//                           (src/core/infra/rayleigh_damping.cpp:720-1119,1194-1476),
+//                           the end-of-step sponge of dynamics.cpp:7323-7340, with
+//                           the per-level profiles its runtime built
 //   ref_scalar_transport    advect_scalars_conservative_3d_cartesian
 //                           (advection_cartesian.cpp:3532) on a retained context whose
 //                           face mass fluxes and beginning density are supplied
@@ -47,6 +51,7 @@
 #include "dynamics/schemes/klemp_wilhelmson_split/cartesian_cgrid_3d.hpp"
 #include "microphysics/schemes/kessler/kessler.hpp"
 #include "dynamics/eos_pressure.hpp"
+#include "core/infra/rayleigh_damping.hpp"
 
 #include <cstring>
 #include <exception>
@@ -471,6 +476,67 @@ int ref_slow_tendencies(const float* u, const float* v, const float* w, const fl
         from_field(dv, fdv);
         from_field(dw, fdw);
         from_field(dp, fdp);
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        return fail(e.what());
+    }
+}
+
+// The end-of-step sponge on a flat C-grid level: the upper Rayleigh sponge
+// (and the w-only lid absorber when w_only_cells > 0), then the lateral
+// sponge of lateral_width cells, exactly as dynamics.cpp calls them.  u, v,
+// w, theta are relaxed in place; theta0 is the base profile (nz).  The
+// reference's own per-level profiles are returned: alpha, upper_w_alpha,
+// w_only_alpha, u_ref, v_ref (nz each) and lateral_alpha (lateral_width).
+int ref_state_relaxation(float* u, float* v, float* w, float* theta, const double* theta0, int nx, int ny, int nz,
+                         double dx, double dy, double dz, double dt, double z_damp, double alpha_max,
+                         int w_only_cells, double w_only_alpha_max, int lateral_width, double lateral_alpha_max,
+                         int implicit_mode, const double* wind /* u_sfc v_sfc u_1km v_1km u_6km v_6km */,
+                         double* alpha, double* upper_w_alpha, double* w_only_alpha, double* u_ref, double* v_ref,
+                         double* lateral_alpha)
+{
+    try
+    {
+        Level L(nx, ny, nz, dx, dy, dz, dt);
+        auto& f = L.storage.fields;
+        to_field(f.u, u, nx, ny, nz);
+        to_field(f.v, v, nx, ny, nz);
+        to_field(f.w, w, nx, ny, nz);
+        to_field(f.theta, theta, nx, ny, nz);
+        L.storage.base.theta0.assign(theta0, theta0 + nz);
+        auto& c = L.storage.configuration;
+        c.damping_enabled = true;
+        c.damping_z_d = z_damp;
+        c.damping_alpha = alpha_max;
+        c.w_only_top_sponge = w_only_cells > 0;
+        c.w_only_depth_cells = w_only_cells;
+        c.w_only_alpha_max = w_only_alpha_max;
+        c.lateral_sponge_enabled = lateral_width > 0;
+        c.lateral_sponge_width = lateral_width;
+        c.lateral_sponge_alpha = lateral_alpha_max;
+        c.damping_mode = implicit_mode ? tmv::init::config::DampingMode::Implicit
+                                       : tmv::init::config::DampingMode::Explicit;
+        c.wind_profile = WindProfile{wind[0], wind[1], wind[2], wind[3], wind[4], wind[5]};
+        RayleighDampingRuntimeState runtime;
+        L.view.rayleigh_runtime = &runtime;
+        apply_rayleigh_damping(L.view, dt);
+        apply_lateral_damping(L.view, dt);
+        from_field(u, f.u);
+        from_field(v, f.v);
+        from_field(w, f.w);
+        from_field(theta, f.theta);
+        for (int k = 0; k < nz; ++k)
+        {
+            alpha[k] = runtime.alpha[k];
+            upper_w_alpha[k] = runtime.upper_w_alpha[k];
+            w_only_alpha[k] = runtime.w_only_alpha[k];
+            u_ref[k] = runtime.u_ref[k];
+            v_ref[k] = runtime.v_ref[k];
+        }
+        for (int d = 0; d < lateral_width && d < static_cast<int>(runtime.lateral_alpha.size()); ++d)
+            lateral_alpha[d] = runtime.lateral_alpha[d];
         return 0;
     }
     catch (const std::exception& e)

@@ -115,5 +115,41 @@ def main():
     print("wrote kessler_eos")
 
 
+# The end-of-step sponge: two configurations on one seeded level, each with
+# the reference runtime's own profiles and the relaxed fields.
+SPONGE_CONFIGS = {
+    "explicit": dict(z_damp=-1.0, alpha_max=0.05, w_only_cells=4, w_only_alpha_max=0.2, lateral_width=5,
+                     lateral_alpha_max=0.08, implicit_mode=0, wind=(2.0, -1.0, 8.0, 3.0, 15.0, 7.0)),
+    "implicit": dict(z_damp=2500.0, alpha_max=0.1, w_only_cells=0, w_only_alpha_max=0.0, lateral_width=3,
+                     lateral_alpha_max=0.3, implicit_mode=1, wind=(0.5, 1.0, 4.0, -2.0, 9.0, 3.0)),
+}
+
+
+def make_state_relaxation():
+    from nimbus_b200.sponge import SpongeConfig
+
+    ref = ReferenceHarness()
+    case = Case(18, 15, 12, 500.0, 600.0, 400.0, 6.0, seed=21)
+    st, base = cloudy_state(case, seed=21)
+    out = {"grid": np.array((case.dx, case.dy, case.dz)), "dt": 6.0, "theta0": base["theta0"],
+           **{f"in_{k}": st[k] for k in ("u", "v", "w", "theta")}}
+    for name, kw in SPONGE_CONFIGS.items():
+        fields = {k: st[k].copy() for k in ("u", "v", "w", "theta")}
+        prof = ref.state_relaxation(fields, base["theta0"], (case.dx, case.dy, case.dz), 6.0, SpongeConfig(**kw))
+        for k, v in kw.items():
+            out[f"{name}_cfg_{k}"] = np.array(v)
+        for k, v in prof.items():
+            out[f"{name}_prof_{k}"] = v
+        for k, v in fields.items():
+            out[f"{name}_out_{k}"] = v
+    np.savez_compressed(HERE / "state_relaxation.npz", **out)
+    print("wrote state_relaxation")
+
+
 if __name__ == "__main__":
-    main()
+    # `make_golden.py state_relaxation` writes only that fixture.
+    if sys.argv[1:] == ["state_relaxation"]:
+        make_state_relaxation()
+    else:
+        main()
+        make_state_relaxation()

@@ -345,3 +345,77 @@ def test_live_reference_pin_large_step(o32, bc_name):
         o32.large_step(b, base, grid, 4.0, 5, BC_SETS[bc_name], coriolis_f=1e-4)
     for k in ("u", "v", "w", "rho", "p", "theta", "qv", "qc", "qr"):
         np.testing.assert_array_equal(a[k].view(np.uint32), b[k].view(np.uint32), err_msg=k)
+
+
+# ---- End-of-step sponge (state relaxation) ------------------------------------
+def _sponge_config(g, name):
+    from nimbus_b200.sponge import SpongeConfig
+
+    kw = {k[len(name) + 5:]: g[k] for k in g.files if k.startswith(f"{name}_cfg_")}
+    kw = {k: (tuple(float(x) for x in v) if k == "wind" else v.item()) for k, v in kw.items()}
+    return SpongeConfig(**kw)
+
+
+@pytest.mark.parametrize("name", ["explicit", "implicit"])
+def test_golden_state_relaxation(o32, name):
+    """The profile builder reproduces the reference runtime's profiles, and the
+    restatement the reference's relaxed fields, bit for bit (fixture from the
+    reference's own apply_rayleigh_damping + apply_lateral_damping)."""
+    from nimbus_b200.sponge import build_profiles
+
+    g = np.load("tests/golden/state_relaxation.npz")
+    cfg = _sponge_config(g, name)
+    nz = g["in_u"].shape[2]
+    P = build_profiles(cfg, nz, float(g["grid"][2]), g["theta0"])
+    for k in ("alpha", "upper_w_alpha", "w_only_alpha", "u_ref", "v_ref", "lateral_alpha"):
+        want = g[f"{name}_prof_{k}"]
+        got = getattr(P, k)
+        assert got.shape == want.shape and np.array_equal(got.view(np.uint64), want.view(np.uint64)), k
+    st = {k: g[f"in_{k}"].copy() for k in ("u", "v", "w", "theta")}
+    o32.state_relaxation(st, P, float(g["dt"]))
+    for k in st:
+        want = g[f"{name}_out_{k}"]
+        assert np.count_nonzero(st[k].view(np.uint32) != want.view(np.uint32)) == 0, k
+        assert np.count_nonzero(want != g[f"in_{k}"]) > 0, k  # the sponge acted on every field
+
+
+@pytest.mark.skipif(not oracle.reference_available(), reason="reference harness not built here")
+@pytest.mark.parametrize("seed", [31, 32, 33])
+def test_live_reference_pin_state_relaxation(o32, seed):
+    """Seeded configurations (explicit and implicit, with and without the lid
+    absorber and the lateral band, default and set damping heights) against
+    the reference objects: profiles and fields bit-exact."""
+    from nimbus_b200.sponge import SpongeConfig, build_profiles
+
+    rng = np.random.default_rng(seed)
+    cfg = SpongeConfig(z_damp=float(rng.choice([-1.0, 1800.0])), alpha_max=float(rng.uniform(0.01, 0.2)),
+                       w_only_cells=int(rng.integers(0, 6)), w_only_alpha_max=float(rng.uniform(0.05, 0.5)),
+                       lateral_width=int(rng.integers(0, 9)), lateral_alpha_max=float(rng.uniform(0.0, 0.4)),
+                       implicit_mode=int(rng.integers(0, 2)), wind=tuple(rng.uniform(-10, 20, 6)))
+    case = Case(int(rng.integers(5, 20)), int(rng.integers(5, 20)), int(rng.integers(4, 16)), 500.0, 700.0,
+                350.0, 4.0, seed=seed)
+    st, base = cloudy_state(case, seed=seed)
+    ref_fields = {k: st[k].copy() for k in ("u", "v", "w", "theta")}
+    prof = oracle.ReferenceHarness().state_relaxation(ref_fields, base["theta0"], (case.dx, case.dy, case.dz), 4.0,
+                                                      cfg)
+    P = build_profiles(cfg, case.nz, case.dz, base["theta0"])
+    for k, want in prof.items():
+        assert np.array_equal(getattr(P, k).view(np.uint64), want.view(np.uint64)), k
+    mine = {k: st[k].copy() for k in ref_fields}
+    o32.state_relaxation(mine, P, 4.0)
+    for k in mine:
+        assert np.count_nonzero(mine[k].view(np.uint32) != ref_fields[k].view(np.uint32)) == 0, k
+
+
+def test_state_relaxation_rejects_invalid_rates(o32):
+    from nimbus_b200.sponge import SpongeConfig, build_profiles
+
+    case = Case(8, 8, 6, 500.0, 500.0, 400.0, 3.0, seed=2)
+    st, base = cloudy_state(case, seed=2)
+    P = build_profiles(SpongeConfig(z_damp=100.0), case.nz, case.dz, base["theta0"])
+    P.alpha[3] = -1.0
+    with pytest.raises(ValueError):
+        o32.state_relaxation({k: st[k].copy() for k in ("u", "v", "w", "theta")}, P, 3.0)
+    P = build_profiles(SpongeConfig(), case.nz, case.dz, base["theta0"])
+    with pytest.raises(ValueError):
+        o32.state_relaxation({k: st[k].copy() for k in ("u", "v", "w", "theta")}, P, 0.0)

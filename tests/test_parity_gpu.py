@@ -381,3 +381,69 @@ def test_fp32_transport_across_scales(ctx32, scale):
     for a, b in zip(got, ref):
         assert np.isfinite(a).all()
         assert _rel(a, b) <= 1e-5
+
+
+# ---- End-of-step sponge (state relaxation) ------------------------------------
+@pytest.fixture(scope="module")
+def rctx():
+    c = cuda.Context(0)
+    yield c
+    c.close()
+
+
+@pytest.mark.parametrize("name", ["explicit", "implicit"])
+def test_state_relaxation_matches_reference(rctx, name):
+    """nimbus_cuda_state_relaxation on host arrays against the reference's own
+    apply_rayleigh_damping + apply_lateral_damping (golden fixture): 0 ULP."""
+    from nimbus_b200.sponge import build_profiles
+    from tests.test_oracle import _sponge_config
+
+    g = np.load("tests/golden/state_relaxation.npz")
+    P = build_profiles(_sponge_config(g, name), g["in_u"].shape[2], float(g["grid"][2]), g["theta0"])
+    st = {k: g[f"in_{k}"].copy() for k in ("u", "v", "w", "theta")}
+    rctx.check(rctx.state_relaxation(cuda.state_relaxation_args(st, P, float(g["dt"]))))
+    for k in st:
+        want = g[f"{name}_out_{k}"]
+        assert np.count_nonzero(st[k].view(np.uint32) != want.view(np.uint32)) == 0, k
+
+
+@pytest.mark.parametrize("seed", [41, 42, 43, 44])
+def test_state_relaxation_device_memory_matches_oracle(rctx, o32, seed):
+    """Device arrays, seeded configurations (lid absorber and lateral band on or
+    off, explicit or implicit, unstaggered w): equal to the restatement, which
+    the reference pins."""
+    import torch
+
+    from nimbus_b200.sponge import SpongeConfig, build_profiles
+
+    rng = np.random.default_rng(seed)
+    cfg = SpongeConfig(z_damp=float(rng.choice([-1.0, 1500.0])), alpha_max=float(rng.uniform(0.01, 0.3)),
+                       w_only_cells=int(rng.integers(0, 7)), w_only_alpha_max=float(rng.uniform(0.05, 0.5)),
+                       lateral_width=int(rng.integers(0, 12)), lateral_alpha_max=float(rng.uniform(0.0, 0.5)),
+                       implicit_mode=int(rng.integers(0, 2)), wind=tuple(rng.uniform(-10, 20, 6)))
+    case = Case(int(rng.integers(4, 40)), int(rng.integers(4, 40)), int(rng.integers(2, 30)), 500.0, 600.0, 300.0,
+                4.0, seed=seed)
+    st, base = cloudy_state(case, seed=seed)
+    P = build_profiles(cfg, case.nz, case.dz, base["theta0"], staggered=bool(seed % 2))
+    want = {k: st[k].copy() for k in ("u", "v", "w", "theta")}
+    o32.state_relaxation(want, P, 4.0)
+    dev = {k: torch.from_numpy(st[k].copy()).cuda() for k in want}
+    rctx.check(rctx.state_relaxation(cuda.state_relaxation_args(dev, P, 4.0, memory=cuda.MEMORY_DEVICE)))
+    rctx.synchronize()
+    for k in want:
+        got = dev[k].cpu().numpy()
+        assert np.count_nonzero(got.view(np.uint32) != want[k].view(np.uint32)) == 0, k
+
+
+def test_state_relaxation_refuses_invalid_rates(rctx):
+    from nimbus_b200.sponge import SpongeConfig, build_profiles
+
+    case = Case(10, 9, 8, 500.0, 500.0, 400.0, 3.0, seed=5)
+    st, base = cloudy_state(case, seed=5)
+    P = build_profiles(SpongeConfig(z_damp=200.0), case.nz, case.dz, base["theta0"])
+    P.alpha[2] = float("nan")
+    fields = {k: st[k].copy() for k in ("u", "v", "w", "theta")}
+    rc = rctx.state_relaxation(cuda.state_relaxation_args(fields, P, 3.0))
+    assert rc == cuda.NIMBUS_ERR_INVALID_ARGUMENT
+    for k in fields:
+        assert np.array_equal(fields[k], st[k]), k
