@@ -530,6 +530,25 @@ nimbus_status nimbus_cuda_acoustic_boundaries(nimbus_cuda_context* ctx, const ni
  */
 typedef struct nimbus_engine nimbus_engine;
 
+/* Optional end-of-step sponge of an engine member: the profiles and switches
+ * of nimbus_state_relaxation_args (FP64, host memory, copied at admission),
+ * applied with the member's dt after the EOS projection, as
+ * dynamics.cpp:7323-7340 applies it. */
+typedef struct nimbus_sponge_desc
+{
+    const double* alpha;
+    const double* upper_w_alpha;
+    const double* w_only_alpha;
+    const double* u_ref;
+    const double* v_ref;
+    const double* theta_ref;
+    int lateral_width;
+    const double* lateral_alpha;
+    int do_upper, do_w_only, do_lateral;
+    int staggered;
+    int implicit_mode;
+} nimbus_sponge_desc;
+
 typedef struct nimbus_member_desc
 {
     int nx, ny, nz;
@@ -546,6 +565,7 @@ typedef struct nimbus_member_desc
     const double* qv0_base;
     const double* u0_base;   /* may be null: zero */
     const double* v0_base;   /* may be null: zero */
+    const nimbus_sponge_desc* sponge;  /* may be null: no end-of-step sponge */
 } nimbus_member_desc;
 
 /* Host arrays [nx][ny][nz] of one member's prognostic state. */

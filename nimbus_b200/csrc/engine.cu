@@ -36,7 +36,7 @@ struct ArenaLayout
 {
     size_t cells, history;
     size_t off_state, off_ctxt, off_wave, off_sf, off_rl, off_q4, off_k1, off_xs, off_eos, off_status, off_prof, off_dp0,
-        off_eos0, total;
+        off_eos0, off_sponge, sponge_bytes, total;
 };
 
 ArenaLayout arena_layout(const nimbus_member_desc* d)
@@ -59,6 +59,15 @@ ArenaLayout arena_layout(const nimbus_member_desc* d)
     L.off_prof = off;   off += align_up(5 * static_cast<size_t>(d->nz) * sizeof(double));
     L.off_dp0 = off;    off += align_up(static_cast<size_t>(d->nz) * sizeof(float2));
     L.off_eos0 = off;   off += align_up(static_cast<size_t>(d->nz) * sizeof(float4));
+    L.off_sponge = off;
+    if (const nimbus_sponge_desc* sp = d->sponge)
+    {
+        // RelaxImage: 6 nz + max(width, 1) doubles, then 2 nz level flags.
+        const int width = (sp->do_lateral && sp->lateral_width > 0) ? sp->lateral_width : 0;
+        L.sponge_bytes = (6 * static_cast<size_t>(d->nz) + static_cast<size_t>(width > 0 ? width : 1)) *
+                             sizeof(double) + 2 * static_cast<size_t>(d->nz);
+        off += align_up(L.sponge_bytes);
+    }
     L.total = off;
     return L;
 }
@@ -84,6 +93,15 @@ const char* check_desc(const nimbus_member_desc* d)
     if (d->microphysics == 1 && d->dt > 0.8 * d->dz / 20.0)
         return "dt exceeds the Kessler sedimentation limit 0.8 dz / (20 m/s); the reference would subcycle";
     if (!d->rho0_base || !d->p0_base || !d->qv0_base) return "rho0, p0 and qv0 base profiles are required";
+    if (const nimbus_sponge_desc* sp = d->sponge)
+    {
+        RelaxImage img;
+        if (const char* why = build_relax_image(d->nx, d->ny, d->nz, sp->alpha, sp->upper_w_alpha, sp->w_only_alpha,
+                                                sp->u_ref, sp->v_ref, sp->theta_ref, sp->lateral_width,
+                                                sp->lateral_alpha, sp->do_upper, sp->do_w_only, sp->do_lateral,
+                                                sp->staggered, sp->implicit_mode, d->dt, img))
+            return why;
+    }
     return nullptr;
 }
 
@@ -535,6 +553,7 @@ nimbus_status nimbus_cuda_engine_admit(nimbus_engine* e, const nimbus_member_des
     slot.id = e->next_id;
     slot.desc = *desc;
     slot.desc.rho0_base = slot.desc.p0_base = slot.desc.qv0_base = slot.desc.u0_base = slot.desc.v0_base = nullptr;
+    slot.desc.sponge = nullptr;
     slot.bytes = L.total;
     {
         const cudaError_t err = cudaMalloc(&slot.arena, L.total);
@@ -595,6 +614,20 @@ nimbus_status nimbus_cuda_engine_admit(nimbus_engine* e, const nimbus_member_des
     float* dst[9] = {M.u, M.v, M.w, M.rho, M.p, M.theta, M.qv, M.qc, M.qr};
     for (int f = 0; f < 9 && err == cudaSuccess; ++f) err = cudaMemcpy(dst[f], src[f], bytes, cudaMemcpyHostToDevice);
     if (err == cudaSuccess) err = cudaMemcpy(prof, hp.data(), hp.size() * sizeof(double), cudaMemcpyHostToDevice);
+    M.R = RelaxTables{};
+    if (err == cudaSuccess && desc->sponge)
+    {
+        const nimbus_sponge_desc* sp = desc->sponge;
+        RelaxImage img;  // validated by check_desc
+        build_relax_image(desc->nx, desc->ny, desc->nz, sp->alpha, sp->upper_w_alpha, sp->w_only_alpha, sp->u_ref,
+                          sp->v_ref, sp->theta_ref, sp->lateral_width, sp->lateral_alpha, sp->do_upper, sp->do_w_only,
+                          sp->do_lateral, sp->staggered, sp->implicit_mode, desc->dt, img);
+        unsigned char* dev = reinterpret_cast<unsigned char*>(base + L.off_sponge);
+        const size_t tab_bytes = img.tab.size() * sizeof(double);
+        err = cudaMemcpy(dev, img.tab.data(), tab_bytes, cudaMemcpyHostToDevice);
+        if (err == cudaSuccess) err = cudaMemcpy(dev + tab_bytes, img.on.data(), img.on.size(), cudaMemcpyHostToDevice);
+        M.R = relax_tables(img, dev, desc->nz);
+    }
     if (err == cudaSuccess)
     {
         // The same per-level kernel the per-operation path runs, so both forms

@@ -20,6 +20,7 @@
 #include "acoustic_kernels.cuh"
 #include "acoustic_split.cuh"
 #include "physics_kernels.cuh"
+#include "relaxation_kernels.cuh"
 #include "slow_kernels.cuh"
 #include "transport_kernels.cuh"
 
@@ -62,6 +63,7 @@ struct __align__(16) EngineMember
     KesslerParams K;
     double gamma;
     EosSeries eos_series;  // FP32 EOS coefficients binom(gamma, n)
+    RelaxTables R;         // end-of-step sponge (all do_* zero: none)
     int n_substeps;
     int microphysics;
     int items[kItemKinds];
@@ -387,6 +389,20 @@ static __global__ void __launch_bounds__(256, 4) engine_microphysics_eos_kernel(
             ok = eos_candidate_value(M.K.d, c, M.rho[c], s.x, M.gamma, true, po, s.y, s.z, s.w, p_new, flags);
         if (ok) M.eos[c] = p_new;
         if (flags) atomicOr(M.status, flags);
+        // The end-of-step sponge after the EOS projection (dynamics.cpp:7323-7340).
+        if (M.R.do_upper | M.R.do_w_only | M.R.do_lateral)
+        {
+            int i, j, k;
+            decompose(M.K.d, c, i, j, k);
+            float uu = M.u[c], vv = M.v[c], ww = M.w[c], th = s.x;
+            if (relax_cell(M.R, M.K.d.nx, M.K.d.ny, i, j, k, uu, vv, ww, th))
+            {
+                M.u[c] = uu;
+                M.v[c] = vv;
+                M.w[c] = ww;
+                M.theta[c] = th;
+            }
+        }
     });
 }
 

@@ -752,17 +752,6 @@ nimbus_status nimbus_cuda_kessler_step(nimbus_cuda_context* ctx, const nimbus_ke
     return kessler_entry(ctx, a, true);
 }
 
-// damping_relaxation_factor (rayleigh_damping.cpp:145-163): false where the
-// reference throws.
-static bool relaxation_factor(double alpha, double dt, int implicit_mode, double* out)
-{
-    if (!std::isfinite(alpha) || alpha < 0.0 || !std::isfinite(dt) || dt <= 0.0) return false;
-    const double scaled = alpha * dt;
-    if (!std::isfinite(scaled)) return false;
-    *out = implicit_mode ? scaled / (1.0 + scaled) : -std::expm1(-scaled);
-    return true;
-}
-
 nimbus_status nimbus_cuda_state_relaxation(nimbus_cuda_context* ctx, const nimbus_state_relaxation_args* a)
 {
     if (!ctx || !a) return NIMBUS_ERR_INVALID_ARGUMENT;
@@ -772,79 +761,23 @@ nimbus_status nimbus_cuda_state_relaxation(nimbus_cuda_context* ctx, const nimbu
     if (a->memory != NIMBUS_MEMORY_HOST && a->memory != NIMBUS_MEMORY_DEVICE)
         return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "unknown memory kind");
     const int nz = a->nz;
-    const bool upper = a->do_upper != 0, lid = a->do_w_only != 0;
-    const bool lateral = a->do_lateral != 0 && a->lateral_width > 0;
-    if ((upper && (!a->alpha || !a->upper_w_alpha)) || (lid && !a->w_only_alpha) || (lateral && !a->lateral_alpha) ||
-        ((upper || lateral) && (!a->u_ref || !a->v_ref || !a->theta_ref)))
-        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "a profile of an enabled sponge pass is null");
-    // Per-level tables: the factors the reference forms cell by cell depend
-    // on the level (or lateral distance) only; formed here once with the same
-    // expm1, and checked where the reference would evaluate them.
-    const int width = lateral ? a->lateral_width : 0;
-    std::vector<double> tab(6 * static_cast<size_t>(nz) + static_cast<size_t>(width > 0 ? width : 1), 0.0);
-    std::vector<unsigned char> on(2 * static_cast<size_t>(nz), 0);
-    double* up = tab.data();
-    double* up_w = up + nz;
-    double* lid_f = up_w + nz;
-    double* refs = lid_f + nz;  // u_ref, v_ref, theta_ref
-    double* lat = refs + 3 * nz;
-    for (int k = 0; k < nz; ++k)
-    {
-        if (upper && !(a->alpha[k] <= 0.0 && a->upper_w_alpha[k] <= 0.0))
-        {
-            on[k] = 1;
-            if (!relaxation_factor(a->alpha[k], a->dt, a->implicit_mode, &up[k]))
-                return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "upper sponge: alpha and dt must be finite, alpha >= 0, dt > 0");
-            if (!a->staggered) up_w[k] = up[k];
-            else if (!relaxation_factor(a->upper_w_alpha[k], a->dt, a->implicit_mode, &up_w[k]))
-                return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "upper sponge: alpha and dt must be finite, alpha >= 0, dt > 0");
-        }
-        if (lid && a->w_only_alpha[k] > 0.0)
-        {
-            on[nz + k] = 1;
-            if (!relaxation_factor(a->w_only_alpha[k], a->dt, a->implicit_mode, &lid_f[k]))
-                return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "w-only sponge: alpha and dt must be finite, dt > 0");
-        }
-        if (upper || lateral)
-        {
-            refs[k] = a->u_ref[k];
-            refs[nz + k] = a->v_ref[k];
-            refs[2 * nz + k] = a->theta_ref[k];
-        }
-    }
-    // Distances that occur on this grid (a band wider than half the domain
-    // is never reached by its inner entries, which the reference then never
-    // evaluates).
-    const int reach = std::min((a->nx - 1) / 2, (a->ny - 1) / 2);
-    for (int dd = 0; dd < width && dd <= reach; ++dd)
-        if (!relaxation_factor(a->lateral_alpha[dd], a->dt, a->implicit_mode, &lat[dd]))
-            return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "lateral sponge: alpha and dt must be finite, alpha >= 0, dt > 0");
-    if (!upper && !lid && !lateral) return NIMBUS_OK;
+    RelaxImage img;
+    if (const char* why = build_relax_image(a->nx, a->ny, nz, a->alpha, a->upper_w_alpha, a->w_only_alpha, a->u_ref,
+                                            a->v_ref, a->theta_ref, a->lateral_width, a->lateral_alpha, a->do_upper,
+                                            a->do_w_only, a->do_lateral, a->staggered, a->implicit_mode, a->dt, img))
+        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, why);
+    if (!img.upper && !img.lid && !img.lateral) return NIMBUS_OK;
 
     NB_CUDA(ctx, cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
     if (a->memory == NIMBUS_MEMORY_DEVICE && a->stream) st = static_cast<cudaStream_t>(a->stream);
-    const size_t tab_bytes = tab.size() * sizeof(double);
     unsigned char* dev = nullptr;
-    NB_TRY(ensure(ctx, kRelaxTables, tab_bytes + on.size(), &dev));
+    NB_TRY(ensure(ctx, kRelaxTables, img.bytes(), &dev));
     // Pageable sources: the call returns once the tables are staged.
-    NB_CUDA(ctx, cudaMemcpyAsync(dev, tab.data(), tab_bytes, cudaMemcpyHostToDevice, st));
-    NB_CUDA(ctx, cudaMemcpyAsync(dev + tab_bytes, on.data(), on.size(), cudaMemcpyHostToDevice, st));
-    const double* dt_ = reinterpret_cast<const double*>(dev);
-    RelaxTables R;
-    R.upper = dt_;
-    R.upper_w = dt_ + nz;
-    R.w_only = dt_ + 2 * nz;
-    R.u_ref = dt_ + 3 * nz;
-    R.v_ref = dt_ + 4 * nz;
-    R.th_ref = dt_ + 5 * nz;
-    R.lateral = dt_ + 6 * nz;
-    R.upper_on = dev + tab_bytes;
-    R.w_only_on = dev + tab_bytes + nz;
-    R.lateral_width = width;
-    R.do_upper = upper;
-    R.do_w_only = lid;
-    R.do_lateral = lateral;
+    const size_t tab_bytes = img.tab.size() * sizeof(double);
+    NB_CUDA(ctx, cudaMemcpyAsync(dev, img.tab.data(), tab_bytes, cudaMemcpyHostToDevice, st));
+    NB_CUDA(ctx, cudaMemcpyAsync(dev + tab_bytes, img.on.data(), img.on.size(), cudaMemcpyHostToDevice, st));
+    const RelaxTables R = relax_tables(img, dev, nz);
     const Dims d = make_dims(a->nx, a->ny, a->nz);
     const long long n = d.cells();
     float *u = a->u, *v = a->v, *w = a->w, *th = a->theta;

@@ -145,6 +145,15 @@ class BoundaryArgs(ctypes.Structure):
     ]
 
 
+class SpongeDesc(ctypes.Structure):
+    _fields_ = [
+        ("alpha", _dp), ("upper_w_alpha", _dp), ("w_only_alpha", _dp), ("u_ref", _dp), ("v_ref", _dp),
+        ("theta_ref", _dp), ("lateral_width", ctypes.c_int), ("lateral_alpha", _dp),
+        ("do_upper", ctypes.c_int), ("do_w_only", ctypes.c_int), ("do_lateral", ctypes.c_int),
+        ("staggered", ctypes.c_int), ("implicit_mode", ctypes.c_int),
+    ]
+
+
 class MemberDesc(ctypes.Structure):
     _fields_ = [
         ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
@@ -153,6 +162,7 @@ class MemberDesc(ctypes.Structure):
         ("frame_velocity_u_ms", ctypes.c_float), ("frame_velocity_v_ms", ctypes.c_float),
         ("microphysics", ctypes.c_int),
         ("rho0_base", _dp), ("p0_base", _dp), ("qv0_base", _dp), ("u0_base", _dp), ("v0_base", _dp),
+        ("sponge", ctypes.POINTER(SpongeDesc)),
     ]
 
 
@@ -564,10 +574,27 @@ def boundary_args(st, grid, bc, dt_small=0.0, wave=None, frame=(0.0, 0.0), strea
 MEMBER_FIELDS = ("u", "v", "w", "rho", "p", "theta", "qv", "qc", "qr")
 
 
+def sponge_desc(profiles) -> SpongeDesc:
+    """nimbus_sponge_desc from a nimbus_b200.sponge.SpongeProfiles."""
+    P = profiles
+    d = lambda x: np.ascontiguousarray(x, dtype=np.float64)  # noqa: E731
+    prof = [d(P.alpha), d(P.upper_w_alpha), d(P.w_only_alpha), d(P.u_ref), d(P.v_ref), d(P.theta_ref)]
+    lateral = d(P.lateral_alpha) if len(P.lateral_alpha) else None
+    s = SpongeDesc()
+    s._keep = (prof, lateral)
+    s.alpha, s.upper_w_alpha, s.w_only_alpha, s.u_ref, s.v_ref, s.theta_ref = (_d(x) for x in prof)
+    s.lateral_width = len(P.lateral_alpha)
+    s.lateral_alpha = _d(lateral)
+    s.do_upper, s.do_w_only, s.do_lateral = int(P.do_upper), int(P.do_w_only), int(P.do_lateral)
+    s.staggered, s.implicit_mode = int(P.staggered), int(P.implicit_mode)
+    return s
+
+
 def member_desc(shape, grid, dt, n_substeps, bc, base, coriolis_f=0.0, frame=(0.0, 0.0),
-                microphysics=1) -> MemberDesc:
+                microphysics=1, sponge=None) -> MemberDesc:
     """Descriptor of one engine member; `base` holds the FP64 profiles
-    rho0, p0, qv0 (and optionally u0, v0)."""
+    rho0, p0, qv0 (and optionally u0, v0); `sponge` (SpongeProfiles) adds the
+    end-of-step sponge."""
     d = MemberDesc()
     d.nx, d.ny, d.nz = (int(x) for x in shape)
     d.dx, d.dy, d.dz = grid
@@ -583,6 +610,10 @@ def member_desc(shape, grid, dt, n_substeps, bc, base, coriolis_f=0.0, frame=(0.
     d.rho0_base, d.p0_base, d.qv0_base = _d(prof["rho0"]), _d(prof["p0"]), _d(prof["qv0"])
     d.u0_base = _d(prof["u0"]) if "u0" in prof else None
     d.v0_base = _d(prof["v0"]) if "v0" in prof else None
+    if sponge is not None:
+        sd = sponge_desc(sponge)
+        d._sponge = sd
+        d.sponge = ctypes.pointer(sd)
     return d
 
 

@@ -12,7 +12,9 @@ the phases this backend owns):
   4. conservative WENO5 transport of theta, qv, qc, qr against the retained
      fluxes and densities (advection_batch.cpp:565-760);
   5. the Kessler step over the C-grid cell domain (microphysics_step.cpp);
-  6. the EOS pressure re-projection (eos_apply.cpp).
+  6. the EOS pressure re-projection (eos_apply.cpp);
+  7. optionally the end-of-step sponge (rayleigh_damping.cpp, called at
+     dynamics.cpp:7323-7340).
 
 Two drivers run it:
   ResidentRun   the plain path: one run, each operation enqueued through its
@@ -44,7 +46,7 @@ def substeps_for(case: Case, state, base) -> int:
 class ResidentRun:
     def __init__(self, ctx: cuda.Context, case: Case, state=None, base=None, device="cuda",
                  precision: int = cuda.PRECISION_FP32, autotune: bool = True, coriolis_f: float = 0.0,
-                 microphysics: bool = True):
+                 microphysics: bool = True, sponge=None):
         self.ctx = ctx
         self.precision = precision
         self.tuned = None
@@ -81,6 +83,9 @@ class ResidentRun:
         self._kessler = cuda.kessler_args(f, case.dz, case.dt, memory=cuda.MEMORY_DEVICE)
         self._eos = cuda.eos_args(f["p"], f["rho"], f["theta"], f["qv"], f["qc"], f["qr"], memory=cuda.MEMORY_DEVICE,
                                   p0=self.prof["p0"])
+        # The end-of-step sponge (SpongeProfiles), after the EOS projection.
+        self._sponge = (cuda.state_relaxation_args(f, sponge, case.dt, memory=cuda.MEMORY_DEVICE)
+                        if sponge is not None else None)
         self.torch_stream = torch.cuda.ExternalStream(self.stream, device=dev)
 
     @property
@@ -101,6 +106,8 @@ class ResidentRun:
         if self.microphysics:
             c.check(c.kessler_step(self._kessler))
         c.check(c.eos_projection(self._eos))
+        if self._sponge is not None:
+            c.check(c.state_relaxation(self._sponge))
 
     def download(self) -> dict:
         torch.cuda.current_stream().wait_stream(self.torch_stream)
@@ -122,12 +129,12 @@ class EngineRun:
         self.members = {}
 
     def admit(self, case: Case, state=None, base=None, coriolis_f: float = 0.0, microphysics: bool = True,
-              reserve_bytes: int = 0, n_substeps: int | None = None):
+              reserve_bytes: int = 0, n_substeps: int | None = None, sponge=None):
         if state is None:
             state, base = initial_state(case)
         n = n_substeps or substeps_for(case, state, base)
         desc = cuda.member_desc(case.shape, (case.dx, case.dy, case.dz), case.dt, n, case.bc, base, coriolis_f,
-                                microphysics=int(microphysics))
+                                microphysics=int(microphysics), sponge=sponge)
         mid = self.engine.admit(desc, state, reserve_bytes)
         self.members[mid] = (case, n)
         return mid

@@ -157,7 +157,7 @@ class Restatement:
                                      _fp(w), _fp(rho), _fp(p), _fp(wave), ctypes.c_double(dt_small), _bcs(bc),
                                      ctypes.c_double(frame[0]), ctypes.c_double(frame[1]))
 
-    def large_step(self, st, base, grid, dt, n_substeps, bc, coriolis_f=0.0, microphysics=True):
+    def large_step(self, st, base, grid, dt, n_substeps, bc, coriolis_f=0.0, microphysics=True, sponge=None):
         """One large step of the hot path in the reference's order
         (dynamics.cpp:5123-7317): Heun slow step, boundary refresh, the
         acoustic loop (KW78 seed, N substeps with retained mass flux),
@@ -175,6 +175,8 @@ class Restatement:
             self.kessler_step(st, grid[2], dt, (1, nx - 1, 1, ny - 1, 0, nz))
         if not self.eos_projection(st["p"], st["rho"], st["theta"], st["qv"], st["qc"], st["qr"]):
             raise FloatingPointError("EOS pressure projection rejected an invalid physical state")
+        if sponge is not None:
+            self.state_relaxation(st, sponge, dt)
         return loop
 
     def eos_projection(self, p, rho, theta, qv=None, qc=None, qr=None):

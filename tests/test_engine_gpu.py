@@ -388,3 +388,62 @@ def test_empty_engine_steps_and_copies_nothing(ctx):
     eng.synchronize()
     assert eng.lanes == 0 and not img.any()
     eng.close()
+
+
+def _sponge_profiles(case, base, seed):
+    from nimbus_b200.sponge import SpongeConfig, build_profiles
+
+    rng = np.random.default_rng(seed)
+    cfg = SpongeConfig(z_damp=float(case.nz * case.dz * rng.uniform(0.3, 0.8)), alpha_max=float(rng.uniform(0.02, 0.2)),
+                       w_only_cells=int(rng.integers(0, 4)), w_only_alpha_max=0.3, lateral_width=int(rng.integers(1, 5)),
+                       lateral_alpha_max=float(rng.uniform(0.05, 0.3)), implicit_mode=int(seed % 2),
+                       wind=tuple(rng.uniform(-8, 15, 6)))
+    return build_profiles(cfg, case.nz, case.dz, base["theta0"])
+
+
+@pytest.mark.parametrize("graph", [True, False], ids=["graph", "eager"])
+def test_engine_sponge_matches_oracle(ctx, o32, graph):
+    """Members with the end-of-step sponge (different configurations) beside
+    one without: each equals the oracle large step followed by the sponge,
+    reference precision, bit-exact."""
+    specs = [((17, 14, 12), BCS["radiative"], 3.0, 5, True), ((13, 19, 10), BCS["walls_sponge"], 4.0, 4, True),
+             ((11, 12, 9), BCS["periodic_open"], 3.0, 4, False)]
+    run = EngineRun(ctx, precision=cuda.PRECISION_REFERENCE, graph=graph)
+    members = []
+    for i, (shape, bc, dt, n_sub, with_sponge) in enumerate(specs):
+        case = _case(shape, bc, seed=150 + i, dt=dt)
+        st, base = _state(case, 150 + i)
+        P = _sponge_profiles(case, base, 150 + i) if with_sponge else None
+        mid = run.admit(case, st, base, coriolis_f=1e-4, n_substeps=n_sub, sponge=P)
+        members.append((mid, case, st, base, n_sub, P))
+    run.step(2)
+    for mid, case, st, base, n_sub, P in members:
+        want = {k: v.copy() for k, v in st.items()}
+        for _ in range(2):
+            o32.large_step(want, base, (case.dx, case.dy, case.dz), case.dt, n_sub, case.bc, coriolis_f=1e-4,
+                           sponge=P)
+        got = run.read(mid)
+        for k in PROGNOSTIC:
+            assert_bitwise(got[k], want[k], f"member {mid} {k}")
+    run.close()
+
+
+def test_engine_sponge_fp32_matches_plain(ctx):
+    case = _case((20, 16, 14), BCS["radiative"], seed=160, dt=3.0)
+    st, base = _state(case, 160)
+    P = _sponge_profiles(case, base, 160)
+    plain = ResidentRun(ctx, case, {k: v.copy() for k, v in st.items()}, base, precision=cuda.PRECISION_FP32,
+                        autotune=False, sponge=P)
+    ctx.set_substep_form(cuda.SUBSTEP_SPLIT)
+    for _ in range(2):
+        plain.step()
+    got_plain = plain.download()
+    ctx.set_substep_form(cuda.SUBSTEP_AUTO)
+    run = EngineRun(ctx, precision=cuda.PRECISION_FP32)
+    mid = run.admit(case, st, base, sponge=P)
+    run.step(2)
+    got = run.read(mid)
+    run.close()
+    for k in PROGNOSTIC:
+        assert_bitwise(got[k], got_plain[k], k)
+    assert np.count_nonzero(got["theta"][:, :, -1] != got_plain["theta"][:, :, -1]) == 0
