@@ -566,6 +566,9 @@ typedef struct nimbus_member_desc
     const double* u0_base;   /* may be null: zero */
     const double* v0_base;   /* may be null: zero */
     const nimbus_sponge_desc* sponge;  /* may be null: no end-of-step sponge */
+    int final_closure;       /* 1: end the step with the boundary closure
+                                apply_full_attributed (= apply_acoustic(0) on u, v,
+                                w, rho, p; dynamics.cpp:7415, after the sponge) */
 } nimbus_member_desc;
 
 /* Host arrays [nx][ny][nz] of one member's prognostic state. */

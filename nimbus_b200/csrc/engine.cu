@@ -86,6 +86,7 @@ const char* check_desc(const nimbus_member_desc* d)
         !std::isfinite(d->frame_velocity_v_ms))
         return "coriolis_f and frame velocity must be finite";
     if (d->microphysics != 0 && d->microphysics != 1) return "microphysics must be 0 (none) or 1 (Kessler)";
+    if (d->final_closure != 0 && d->final_closure != 1) return "final_closure must be 0 or 1";
     // step_microphysics subcycles when the interval exceeds the sedimentation
     // limit 0.8 dz / max terminal velocity (microphysics_step.cpp:3500-3575,
     // 3686-3740); Kessler's fall speed is capped at 20 m/s, so dt <= 0.04 dz
@@ -334,6 +335,8 @@ nimbus_status rebuild_table(nimbus_engine* e)
             p[0] = 0;
             for (int r = 0; r < L.members; ++r) p[r + 1] = p[r] + (rows[r].items[k] + tile - 1) / tile;
         }
+        L.closing = false;
+        for (int r = 0; r < L.members; ++r) L.closing = L.closing || rows[r].close_step != 0;
         L.active.assign(max_n, 0);
         for (int st = 0; st < max_n; ++st)
         {
@@ -615,6 +618,7 @@ nimbus_status nimbus_cuda_engine_admit(nimbus_engine* e, const nimbus_member_des
     for (int f = 0; f < 9 && err == cudaSuccess; ++f) err = cudaMemcpy(dst[f], src[f], bytes, cudaMemcpyHostToDevice);
     if (err == cudaSuccess) err = cudaMemcpy(prof, hp.data(), hp.size() * sizeof(double), cudaMemcpyHostToDevice);
     M.R = RelaxTables{};
+    M.close_step = desc->final_closure != 0;
     if (err == cudaSuccess && desc->sponge)
     {
         const nimbus_sponge_desc* sp = desc->sponge;

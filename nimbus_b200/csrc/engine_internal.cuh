@@ -31,6 +31,7 @@ struct Lane
     int members = 0;
     size_t prefix_first = 0;  // first entry of this lane's [kItemKinds][members + 1] prefix block
     std::vector<int> active;  // members of this lane inside the loop at substep s
+    bool closing = false;     // some member ends its step with the boundary closure
 };
 // The Kessler + EOS pass (FP64 in the reference-precision form, FP32 in the
 // FP32 form) is launched from the uncontracted unit (engine.cu), so the engine
@@ -145,7 +146,7 @@ int enqueue_step(nimbus_engine* e, int lane, cudaStream_t st)
     ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_bc_sn_kernel, tiles_of(e, L, kItemRowsSN, n), 1, T, psn,
                   tiles_of(e, L, kItemRowsSN, n), 0, 1);
     ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_bc_vertical_kernel, tiles_of(e, L, kItemColumns, n), 1, T,
-                  pcol, tiles_of(e, L, kItemColumns, n));
+                  pcol, tiles_of(e, L, kItemColumns, n), 1);
     ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_seed_kernel, tiles_of(e, L, kItemHistory, n), 1, T, phist,
                   tiles_of(e, L, kItemHistory, n));
     // The acoustic loop: members still inside it are a prefix of the lane.
@@ -178,6 +179,17 @@ int enqueue_step(nimbus_engine* e, int lane, cudaStream_t st)
     count += nimbus_engine_detail::launch_microphysics(e, st, T, pc, cells);
     engine_swap_kernel<<<(n + 127) / 128, 128, 0, st>>>(T, n, 1);
     ++count;
+    // The closing boundary refresh (apply_full_attributed, after the sponge)
+    // for the members that ask for it, on the published density and pressure.
+    if (L.closing)
+    {
+        ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_bc_we_kernel, tiles_of(e, L, kItemRowsWE, n), 1, T, pwe,
+                      tiles_of(e, L, kItemRowsWE, n), 0, 2);
+        ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_bc_sn_kernel, tiles_of(e, L, kItemRowsSN, n), 1, T, psn,
+                      tiles_of(e, L, kItemRowsSN, n), 0, 2);
+        ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_bc_vertical_kernel, tiles_of(e, L, kItemColumns, n), 1,
+                      T, pcol, tiles_of(e, L, kItemColumns, n), 2);
+    }
     return count;
 }
 

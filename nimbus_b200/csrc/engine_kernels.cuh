@@ -64,6 +64,7 @@ struct __align__(16) EngineMember
     double gamma;
     EosSeries eos_series;  // FP32 EOS coefficients binom(gamma, n)
     RelaxTables R;         // end-of-step sponge (all do_* zero: none)
+    int close_step;        // end the step with the boundary closure
     int n_substeps;
     int microphysics;
     int items[kItemKinds];
@@ -153,6 +154,7 @@ static __global__ void __launch_bounds__(256) engine_bc_we_kernel(const EngineMe
                                                            int s, int refresh)
 {
     for_member_items(table, prefix, tiles, kItemRowsWE, [&](const EngineMember& M, int r) {
+        if (refresh == 2 && !M.close_step) return;  // the closing refresh only where asked
         BoundaryParams B = M.B;
         if (refresh) B.dt_rad = 0.0f;
         float* rho = refresh ? M.rho : engine_density(M, s, true);
@@ -166,6 +168,7 @@ static __global__ void __launch_bounds__(256) engine_bc_sn_kernel(const EngineMe
                                                            int s, int refresh)
 {
     for_member_items(table, prefix, tiles, kItemRowsSN, [&](const EngineMember& M, int r) {
+        if (refresh == 2 && !M.close_step) return;
         BoundaryParams B = M.B;
         if (refresh) B.dt_rad = 0.0f;
         float* rho = refresh ? M.rho : engine_density(M, s, true);
@@ -174,11 +177,14 @@ static __global__ void __launch_bounds__(256) engine_bc_sn_kernel(const EngineMe
     });
 }
 
+// refresh: 1 before the acoustic loop, 2 the closing refresh at the end of the
+// step (members with close_step only).
 static __global__ void __launch_bounds__(256) engine_bc_vertical_kernel(const EngineMember* __restrict__ table,
                                                                  const long long* __restrict__ prefix,
-                                                                 long long tiles)
+                                                                 long long tiles, int refresh)
 {
     for_member_items(table, prefix, tiles, kItemColumns, [&](const EngineMember& M, int col) {
+        if (refresh == 2 && !M.close_step) return;
         bc_vertical_column(M.B, M.u, M.v, M.w, col);
     });
 }

@@ -162,7 +162,7 @@ class MemberDesc(ctypes.Structure):
         ("frame_velocity_u_ms", ctypes.c_float), ("frame_velocity_v_ms", ctypes.c_float),
         ("microphysics", ctypes.c_int),
         ("rho0_base", _dp), ("p0_base", _dp), ("qv0_base", _dp), ("u0_base", _dp), ("v0_base", _dp),
-        ("sponge", ctypes.POINTER(SpongeDesc)),
+        ("sponge", ctypes.POINTER(SpongeDesc)), ("final_closure", ctypes.c_int),
     ]
 
 
@@ -591,10 +591,10 @@ def sponge_desc(profiles) -> SpongeDesc:
 
 
 def member_desc(shape, grid, dt, n_substeps, bc, base, coriolis_f=0.0, frame=(0.0, 0.0),
-                microphysics=1, sponge=None) -> MemberDesc:
+                microphysics=1, sponge=None, final_closure=False) -> MemberDesc:
     """Descriptor of one engine member; `base` holds the FP64 profiles
     rho0, p0, qv0 (and optionally u0, v0); `sponge` (SpongeProfiles) adds the
-    end-of-step sponge."""
+    end-of-step sponge, `final_closure` the closing boundary refresh."""
     d = MemberDesc()
     d.nx, d.ny, d.nz = (int(x) for x in shape)
     d.dx, d.dy, d.dz = grid
@@ -614,6 +614,7 @@ def member_desc(shape, grid, dt, n_substeps, bc, base, coriolis_f=0.0, frame=(0.
         sd = sponge_desc(sponge)
         d._sponge = sd
         d.sponge = ctypes.pointer(sd)
+    d.final_closure = int(bool(final_closure))
     return d
 
 

@@ -14,7 +14,8 @@ the phases this backend owns):
   5. the Kessler step over the C-grid cell domain (microphysics_step.cpp);
   6. the EOS pressure re-projection (eos_apply.cpp);
   7. optionally the end-of-step sponge (rayleigh_damping.cpp, called at
-     dynamics.cpp:7323-7340).
+     dynamics.cpp:7323-7340) and the closing boundary refresh
+     (apply_full_attributed, dynamics.cpp:7415).
 
 Two drivers run it:
   ResidentRun   the plain path: one run, each operation enqueued through its
@@ -46,7 +47,7 @@ def substeps_for(case: Case, state, base) -> int:
 class ResidentRun:
     def __init__(self, ctx: cuda.Context, case: Case, state=None, base=None, device="cuda",
                  precision: int = cuda.PRECISION_FP32, autotune: bool = True, coriolis_f: float = 0.0,
-                 microphysics: bool = True, sponge=None):
+                 microphysics: bool = True, sponge=None, final_closure: bool = False):
         self.ctx = ctx
         self.precision = precision
         self.tuned = None
@@ -86,6 +87,7 @@ class ResidentRun:
         # The end-of-step sponge (SpongeProfiles), after the EOS projection.
         self._sponge = (cuda.state_relaxation_args(f, sponge, case.dt, memory=cuda.MEMORY_DEVICE)
                         if sponge is not None else None)
+        self.final_closure = final_closure
         self.torch_stream = torch.cuda.ExternalStream(self.stream, device=dev)
 
     @property
@@ -108,6 +110,8 @@ class ResidentRun:
         c.check(c.eos_projection(self._eos))
         if self._sponge is not None:
             c.check(c.state_relaxation(self._sponge))
+        if self.final_closure:  # apply_full_attributed = apply_acoustic(0)
+            c.check(c.acoustic_boundaries(self._refresh))
 
     def download(self) -> dict:
         torch.cuda.current_stream().wait_stream(self.torch_stream)
@@ -129,12 +133,12 @@ class EngineRun:
         self.members = {}
 
     def admit(self, case: Case, state=None, base=None, coriolis_f: float = 0.0, microphysics: bool = True,
-              reserve_bytes: int = 0, n_substeps: int | None = None, sponge=None):
+              reserve_bytes: int = 0, n_substeps: int | None = None, sponge=None, final_closure: bool = False):
         if state is None:
             state, base = initial_state(case)
         n = n_substeps or substeps_for(case, state, base)
         desc = cuda.member_desc(case.shape, (case.dx, case.dy, case.dz), case.dt, n, case.bc, base, coriolis_f,
-                                microphysics=int(microphysics), sponge=sponge)
+                                microphysics=int(microphysics), sponge=sponge, final_closure=final_closure)
         mid = self.engine.admit(desc, state, reserve_bytes)
         self.members[mid] = (case, n)
         return mid

@@ -157,7 +157,8 @@ class Restatement:
                                      _fp(w), _fp(rho), _fp(p), _fp(wave), ctypes.c_double(dt_small), _bcs(bc),
                                      ctypes.c_double(frame[0]), ctypes.c_double(frame[1]))
 
-    def large_step(self, st, base, grid, dt, n_substeps, bc, coriolis_f=0.0, microphysics=True, sponge=None):
+    def large_step(self, st, base, grid, dt, n_substeps, bc, coriolis_f=0.0, microphysics=True, sponge=None,
+                   final_closure=False):
         """One large step of the hot path in the reference's order
         (dynamics.cpp:5123-7317): Heun slow step, boundary refresh, the
         acoustic loop (KW78 seed, N substeps with retained mass flux),
@@ -177,6 +178,8 @@ class Restatement:
             raise FloatingPointError("EOS pressure projection rejected an invalid physical state")
         if sponge is not None:
             self.state_relaxation(st, sponge, dt)
+        if final_closure:  # apply_full_attributed (dynamics.cpp:7415) = apply_acoustic(0)
+            self.acoustic_boundaries(st, grid, bc, 0.0)
         return loop
 
     def eos_projection(self, p, rho, theta, qv=None, qc=None, qr=None):
