@@ -67,6 +67,7 @@ def parse():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-error", action="store_true")
     ap.add_argument("--no-relaxation", action="store_true")
+    ap.add_argument("--no-output", action="store_true")
     ap.add_argument("--serving-requests", type=int, default=32)
     ap.add_argument("--error-seconds", type=float, default=600.0)
     ap.add_argument("--precision", choices=("fp32", "reference"), default="fp32",
@@ -338,6 +339,80 @@ def relaxation_study(ctx, device):
             "note": "includes the host forming the per-level factors and staging the tables each call"}
 
 
+def output_study(ctx, device):
+    """Device-side output of one 512x512x80 level (84 MB per field, larger
+    than L2): the cell-centre kernel (nimbus_cuda_cell_centre_velocity)
+    device-timed against the HBM roofline, 24 algorithmic bytes per cell
+    (three face fields read once, three centre fields written); a whole
+    history frame (nimbus_cuda_history_snapshot: the kernel and the copies of
+    all nine fields into pinned host memory) device-timed against the host
+    link; the nine npy files of one frame written by nimbus_history_write,
+    wall-timed; and the reference's own interpolate_*_face_to_center and
+    npy::write_3d on the same fields, on the host cores."""
+    import shutil
+    import tempfile
+
+    import numpy as np
+    import torch
+
+    import oracle
+    from nimbus_b200 import cuda
+    from nimbus_b200.initial import Case, initial_state
+
+    case = Case(512, 512, 80, 500.0, 500.0, 20000.0 / 80, 3.0, seed=13)
+    st, _ = initial_state(case)
+    dev = {k: torch.from_numpy(np.ascontiguousarray(st[k])).to(f"cuda:{device}") for k in cuda.HISTORY_FIELDS}
+    centre = tuple(torch.empty_like(dev[k]) for k in "uvw")
+    args = cuda.cell_centre_args(dev["u"], dev["v"], dev["w"], outputs=centre, memory=cuda.MEMORY_DEVICE)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{device}")
+    for _ in range(3):
+        ctx.check(ctx.cell_centre_velocity(args))
+    launches = 20
+    k_ms = time_on_stream(torch, stream, lambda: ctx.check(ctx.cell_centre_velocity(args)), launches) / launches
+    peak, kind = load_peaks()
+    achieved = 24.0 * case.cells / (k_ms / 1e3) / 1e9
+    image = torch.empty(9 * case.cells, dtype=torch.float32).pin_memory().numpy()
+    hargs = cuda.history_args(dev, cuda.HISTORY_CORE, image, case.shape)
+    for _ in range(2):
+        ctx.check(ctx.history_snapshot(hargs))
+    frames = 5
+    f_ms = time_on_stream(torch, stream, lambda: ctx.check(ctx.history_snapshot(hargs)), frames) / frames
+    ctx.synchronize()
+    frame_bytes = 36 * case.cells
+    tmp = Path(tempfile.mkdtemp(prefix="nimbus_history_"))
+    try:
+        t0 = time.perf_counter()
+        rc = cuda.history_write(image, cuda.HISTORY_CORE, case.shape, tmp, ctx.lib)
+        write_s = time.perf_counter() - t0
+        ref = None
+        if oracle.reference_available():
+            h = oracle.ReferenceHarness(os.cpu_count())
+            host = {k: st[k] for k in "uvw"}
+            h.cell_centre(host["u"], host["v"], host["w"])
+            t0 = time.perf_counter()
+            uc, vc, wc = h.cell_centre(host["u"], host["v"], host["w"])
+            r_interp = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            for k, a in zip(cuda.HISTORY_FIELDS, (uc, vc, wc, *[st[k] for k in cuda.HISTORY_FIELDS[3:]])):
+                h.npy_write_3d(a, tmp / f"ref_{k}.npy")
+            r_write = time.perf_counter() - t0
+            ref = {"kind": "reference", "cores": h.threads, "interpolate_ms": 1e3 * r_interp,
+                   "npy_write_s": r_write, "sample": "interpolate_u/v/w_face_to_center on the same three fields, "
+                                                     "then npy::write_3d of the nine fields of one frame"}
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    return {"grid": list(case.shape), "cells": case.cells,
+            "cell_centre": {"ms_per_call": k_ms, "achieved_gbs": achieved, "peak_gbs": peak,
+                            "frac": achieved / peak, "peak_kind": kind, "algorithmic_bytes_per_cell": 24},
+            "history_frame": {"fields": 9, "bytes": frame_bytes, "ms_per_frame": f_ms,
+                              "d2h_gbs": frame_bytes / (f_ms / 1e3) / 1e9,
+                              "path": "one centring launch + one device-to-host copy per adjacent run of fields, "
+                                      "into pinned host memory"},
+            "npy_write": {"status": cuda.STATUS_NAMES.get(rc, rc), "seconds": write_s,
+                          "gbs": frame_bytes / write_s / 1e9, "target": "local temporary directory"},
+            "reference_cpu": ref}
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -476,9 +551,12 @@ def run_ours(args):
     error = None
     cpu = None
     relaxation = None
+    output = None
     if rank == 0 and world == 1:
         if not args.no_relaxation:
             relaxation = relaxation_study(ctx, device)
+        if not args.no_output:
+            output = output_study(ctx, device)
         if not args.no_serving:
             serving = serving_study(ctx, args, precision)
         if not args.no_error:
@@ -518,6 +596,7 @@ def run_ours(args):
                 "serving": serving,
                 "error_vs_fp64": error,
                 "state_relaxation": relaxation,
+                "output": output,
                 "parallelism": f"{world} GPU(s), each with its own independent ensemble (no collective)",
                 "l2": "inputs larger than L2 (%.1f GB resident per GPU)" % (cells * 4 * 40 / 1e9),
                 "algorithmic_bytes_per_step": bytes_per_step,

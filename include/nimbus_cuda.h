@@ -45,7 +45,8 @@ typedef enum nimbus_status
     NIMBUS_ERR_NONFINITE = 4,        /* a produced value was non-finite; outputs not published */
     NIMBUS_ERR_UNSUPPORTED = 5,      /* valid request outside this backend's contract */
     NIMBUS_ERR_NO_DEVICE = 6,        /* no usable sm_100 device */
-    NIMBUS_ERR_TOO_LARGE = 7         /* grid exceeds a fixed capacity (see NIMBUS_STATIC_SCRATCH_CELLS) */
+    NIMBUS_ERR_TOO_LARGE = 7,        /* grid exceeds a fixed capacity (see NIMBUS_STATIC_SCRATCH_CELLS) */
+    NIMBUS_ERR_IO = 8                /* a history file could not be written */
 } nimbus_status;
 
 typedef enum nimbus_memory
@@ -149,7 +150,8 @@ enum
     NIMBUS_KERNEL_TRANSPORT_UPDATE = 5,
     NIMBUS_KERNEL_SLOW = 6,               /* slow tendencies (k1+predictor, k2+apply) */
     NIMBUS_KERNEL_MICROPHYSICS = 7,       /* Kessler, the EOS re-projection and the end-of-step sponge */
-    NIMBUS_KERNEL_FAMILIES = 8
+    NIMBUS_KERNEL_OUTPUT = 8,             /* cell-centre velocities for output */
+    NIMBUS_KERNEL_FAMILIES = 9
 };
 /* When enabled, every launch is bracketed by CUDA events on its own stream
  * and nimbus_cuda_kernel_timing() returns, per family, the launch count and
@@ -511,6 +513,91 @@ typedef struct nimbus_boundary_args
 nimbus_status nimbus_cuda_acoustic_boundaries(nimbus_cuda_context* ctx, const nimbus_boundary_args* a);
 
 /*
+ * Cell-centre velocities for output.  Replaces interpolate_u_face_to_center,
+ * interpolate_v_face_to_center and both interpolate_w_face_to_center forms
+ * (src/core/output/stagger_interpolation.cpp), which the reference runs
+ * before every history or live export of a C-grid level
+ * (headless_runtime.cpp:2577-2601).  Centre i of u is 0.5f * (face i-1 +
+ * face i) and cell 0 keeps face 0; v likewise in j; centre k of w is
+ * 0.5f * (face k-1 + face k) for k > 0 and 0.5 * (ground_w + face 0) in FP64,
+ * rounded once, for k = 0: bit-identical to the reference.  A NULL output
+ * skips that component (its input may then be NULL too).  ground_w: the
+ * terrain lower-face velocity of each column ([nx][ny] FP64, host memory),
+ * NULL on flat ground (0).  Refused with NIMBUS_ERR_INVALID_ARGUMENT, nothing
+ * written: a non-finite ground_w value (the reference's invalid_argument), an
+ * output overlapping an input or another output.  Zero cells: nothing to do.
+ */
+typedef struct nimbus_cell_centre_args
+{
+    const float* u;           /* face fields [nx][ny][nz] */
+    const float* v;
+    const float* w;
+    float* u_centre;          /* [nx][ny][nz]; NULL: skipped */
+    float* v_centre;
+    float* w_centre;
+    const double* ground_w;   /* [nx][ny], host memory; NULL: flat ground */
+    int nx, ny, nz;
+    int memory;
+    void* stream;
+} nimbus_cell_centre_args;
+
+nimbus_status nimbus_cuda_cell_centre_velocity(nimbus_cuda_context* ctx, const nimbus_cell_centre_args* a);
+
+/* History fields, in the order of the reference's core volume bindings
+ * (core_field_binding_array, headless_runtime.cpp:588-600). */
+enum
+{
+    NIMBUS_HISTORY_U = 1u << 0,
+    NIMBUS_HISTORY_V = 1u << 1,
+    NIMBUS_HISTORY_W = 1u << 2,
+    NIMBUS_HISTORY_RHO = 1u << 3,
+    NIMBUS_HISTORY_P = 1u << 4,
+    NIMBUS_HISTORY_THETA = 1u << 5,
+    NIMBUS_HISTORY_QV = 1u << 6,
+    NIMBUS_HISTORY_QC = 1u << 7,
+    NIMBUS_HISTORY_QR = 1u << 8,
+    NIMBUS_HISTORY_CORE = 0x1ffu
+};
+
+/*
+ * One history frame of a resident level, fed from device memory: the
+ * selected fields with u, v, w cell-centred (as above, on flat ground unless
+ * ground_w is given), copied to host_image in the order of the bits, each
+ * nx*ny*nz floats -- the payloads the reference's export writes
+ * (write_or_snapshot_core_volume_fields, include/core/output/core_volume_writer.hpp:26-64).
+ * Enqueued on `stream` (NULL: the context's): one centring launch into device
+ * staging and one device-to-host copy per contiguous run of fields; the image
+ * is complete once the stream is synchronised.  host_image should be pinned
+ * (cudaHostAlloc) for the copies to run at bus rate and overlap later work.
+ * A field whose bit is set must be non-NULL.
+ */
+typedef struct nimbus_history_args
+{
+    const float *u, *v, *w, *rho, *p, *theta, *qv, *qc, *qr;  /* device memory */
+    unsigned fields;          /* NIMBUS_HISTORY_* bits */
+    const double* ground_w;   /* [nx][ny], host memory; NULL: flat ground */
+    int nx, ny, nz;
+    float* host_image;
+    void* stream;
+} nimbus_history_args;
+
+nimbus_status nimbus_cuda_history_snapshot(nimbus_cuda_context* ctx, const nimbus_history_args* a);
+
+/* Host-side npy writers, byte for byte those of the reference
+ * (src/core/output/npy_writer.cpp): NPY 1.0, header dict
+ * "{'descr': '<f4', 'fortran_order': False, 'shape': (d0, d1, d2), }" padded
+ * with spaces to a 16-byte boundary, C-order float32 payload.
+ * nimbus_npy_write_3d replaces npy::write_3d (npy_writer.cpp:143-156):
+ * NIMBUS_ERR_INVALID_ARGUMENT for a NULL pointer or a dimension <= 0,
+ * NIMBUS_ERR_IO when the file cannot be written.  nimbus_history_write writes
+ * the fields of one history image as <step_dir>/<name>.npy (u, v, w, rho, p,
+ * theta, qv, qc, qr), the reference's synchronous npy export
+ * (core_volume_writer.hpp:60-63); the directory must exist. */
+nimbus_status nimbus_npy_write_3d(const float* data, int dim0, int dim1, int dim2, const char* path);
+nimbus_status nimbus_history_write(const float* host_image, unsigned fields, int nx, int ny, int nz,
+                                   const char* step_dir);
+
+/*
  * Member engine: many runs (ensemble members, served requests) resident in
  * HBM and advanced together, each large step of every member in one batched
  * launch per phase.  No counterpart in the reference, which advances one run
@@ -615,6 +702,12 @@ size_t nimbus_cuda_engine_image_offset(const nimbus_engine* e, int member_id);
  * (host memory should be pinned and stay untouched until synchronize). */
 nimbus_status nimbus_cuda_engine_upload_image_async(nimbus_engine* e, const void* host_image);
 nimbus_status nimbus_cuda_engine_download_image_async(nimbus_engine* e, void* host_image);
+/* One history frame of a member (flat ground), enqueued on the engine's
+ * stream after its enqueued steps: the nimbus_cuda_history_snapshot image of
+ * the member's current state (fields as NIMBUS_HISTORY_* bits, nx*ny*nz floats
+ * each).  host_image should be pinned and is complete after
+ * nimbus_cuda_engine_synchronize. */
+nimbus_status nimbus_cuda_engine_history_async(nimbus_engine* e, int member_id, unsigned fields, void* host_image);
 /* Lanes: the members are split into up to `lanes` size-balanced groups whose
  * launches run on parallel streams (branches of the one step graph), so one
  * group's kernels fill the SMs another's launch tails leave idle.  Results do

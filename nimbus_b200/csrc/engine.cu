@@ -12,6 +12,7 @@
 #include "context.cuh"
 #include "engine_internal.cuh"
 #include "launch.cuh"
+#include "output_host.cuh"
 
 #include <algorithm>
 #include <cstring>
@@ -524,6 +525,7 @@ void nimbus_cuda_engine_destroy(nimbus_engine* e)
     if (e->d_table) cudaFree(e->d_table);
     if (e->d_prefix) cudaFree(e->d_prefix);
     if (e->d_image) cudaFree(e->d_image);
+    if (e->d_centre) cudaFree(e->d_centre);
     for (cudaStream_t ls : e->lane_streams) cudaStreamDestroy(ls);
     for (cudaEvent_t ev : e->lane_done) cudaEventDestroy(ev);
     if (e->fork) cudaEventDestroy(e->fork);
@@ -700,6 +702,34 @@ nimbus_status nimbus_cuda_engine_write_async(nimbus_engine* e, int member_id, co
     for (int f = 0; f < 9; ++f)
         NB_CUDA(ctx, cudaMemcpyAsync(dst[f], src[f], bytes, cudaMemcpyHostToDevice, e->stream));
     return NIMBUS_OK;
+}
+
+nimbus_status nimbus_cuda_engine_history_async(nimbus_engine* e, int member_id, unsigned fields, void* host_image)
+{
+    if (!e) return NIMBUS_ERR_INVALID_ARGUMENT;
+    nimbus_cuda_context* ctx = e->ctx;
+    if (fields & ~static_cast<unsigned>(NIMBUS_HISTORY_CORE))
+        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "unknown history field bit");
+    if (fields && !host_image) return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "host_image is null");
+    MemberSlot* s = find_slot(e, member_id);
+    if (!s) return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "unknown member id");
+    if (!fields) return NIMBUS_OK;
+    NB_CUDA(ctx, cudaSetDevice(ctx->device));
+    if (!e->mirror_exact) NB_TRY(sync_table_to_host(e));
+    const EngineMember& M = s->m;
+    const size_t need = 3 * static_cast<size_t>(M.items[kItemCells]) * sizeof(float);
+    if (need > e->centre_cap)
+    {
+        NB_CUDA(ctx, cudaStreamSynchronize(e->stream));
+        if (e->d_centre) cudaFree(e->d_centre);
+        e->d_centre = nullptr;
+        e->centre_cap = 0;
+        NB_CUDA(ctx, cudaMalloc(&e->d_centre, need));
+        e->centre_cap = need;
+    }
+    const float* src[kHistoryFields] = {M.u, M.v, M.w, M.rho, M.p, M.theta, M.qv, M.qc, M.qr};
+    return enqueue_history(ctx, e->stream, src, fields, nullptr, s->desc.nx, s->desc.ny, s->desc.nz, e->d_centre,
+                           static_cast<float*>(host_image));
 }
 
 nimbus_status nimbus_cuda_engine_read(nimbus_engine* e, int member_id, const nimbus_member_state* out)

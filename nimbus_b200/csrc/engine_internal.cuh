@@ -68,6 +68,8 @@ struct nimbus_engine
     std::map<const void*, int> occupancy;
     float* d_image = nullptr;       // device staging for the state image
     size_t image_cap = 0;           // bytes
+    float* d_centre = nullptr;      // device staging for history frames
+    size_t centre_cap = 0;          // bytes
 };
 
 namespace

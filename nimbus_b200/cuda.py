@@ -28,6 +28,7 @@ NIMBUS_OK = 0
 NIMBUS_ERR_INVALID_ARGUMENT = 1
 NIMBUS_ERR_OUT_OF_MEMORY = 3
 NIMBUS_ERR_NONFINITE = 4
+NIMBUS_ERR_IO = 8
 STATUS_NAMES = {
     0: "NIMBUS_OK",
     1: "NIMBUS_ERR_INVALID_ARGUMENT",
@@ -37,6 +38,7 @@ STATUS_NAMES = {
     5: "NIMBUS_ERR_UNSUPPORTED",
     6: "NIMBUS_ERR_NO_DEVICE",
     7: "NIMBUS_ERR_TOO_LARGE",
+    8: "NIMBUS_ERR_IO",
 }
 MEMORY_HOST, MEMORY_DEVICE = 0, 1
 
@@ -166,6 +168,22 @@ class MemberDesc(ctypes.Structure):
     ]
 
 
+class CellCentreArgs(ctypes.Structure):
+    _fields_ = [
+        ("u", _fp), ("v", _fp), ("w", _fp), ("u_centre", _fp), ("v_centre", _fp), ("w_centre", _fp),
+        ("ground_w", _dp), ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("memory", ctypes.c_int), ("stream", ctypes.c_void_p),
+    ]
+
+
+class HistoryArgs(ctypes.Structure):
+    _fields_ = [
+        *[(k, _fp) for k in ("u", "v", "w", "rho", "p", "theta", "qv", "qc", "qr")],
+        ("fields", ctypes.c_uint), ("ground_w", _dp), ("nx", ctypes.c_int), ("ny", ctypes.c_int),
+        ("nz", ctypes.c_int), ("host_image", _fp), ("stream", ctypes.c_void_p),
+    ]
+
+
 class MemberState(ctypes.Structure):
     _fields_ = [(k, _fp) for k in ("u", "v", "w", "rho", "p", "theta", "qv", "qc", "qr")]
 
@@ -180,6 +198,8 @@ EXPORTED_SYMBOLS = (
     "nimbus_cuda_slow_tendencies", "nimbus_cuda_slow_step",
     "nimbus_cuda_kessler_tendencies", "nimbus_cuda_kessler_step", "nimbus_cuda_eos_projection",
     "nimbus_cuda_acoustic_boundaries", "nimbus_cuda_state_relaxation",
+    "nimbus_cuda_cell_centre_velocity", "nimbus_cuda_history_snapshot", "nimbus_npy_write_3d",
+    "nimbus_history_write", "nimbus_cuda_engine_history_async",
     "nimbus_cuda_engine_create", "nimbus_cuda_engine_destroy", "nimbus_cuda_engine_member_bytes",
     "nimbus_cuda_engine_admit", "nimbus_cuda_engine_retire", "nimbus_cuda_engine_read", "nimbus_cuda_engine_write", "nimbus_cuda_engine_step",
     "nimbus_cuda_engine_read_async", "nimbus_cuda_engine_write_async", "nimbus_cuda_engine_stream",
@@ -193,7 +213,24 @@ SUBSTEP_AUTO, SUBSTEP_FUSED, SUBSTEP_SPLIT = 0, 1, 2
 PRECISION_REFERENCE, PRECISION_FP32 = 0, 1
 STATIC_SCRATCH_CELLS = 4194304  # NIMBUS_STATIC_SCRATCH_CELLS
 KERNEL_FAMILIES = ("acoustic_substep", "acoustic_momentum", "acoustic_boundary", "transport_faces",
-                   "transport_limiter", "transport_update", "slow", "microphysics")
+                   "transport_limiter", "transport_update", "slow", "microphysics", "output")
+# History fields (NIMBUS_HISTORY_* bit order): the reference's core volume
+# bindings, headless_runtime.cpp:588-600.
+HISTORY_FIELDS = ("u", "v", "w", "rho", "p", "theta", "qv", "qc", "qr")
+HISTORY_CORE = (1 << len(HISTORY_FIELDS)) - 1
+
+
+def history_mask(names) -> int:
+    """NIMBUS_HISTORY_* bits of field names (any order)."""
+    mask = 0
+    for name in names:
+        mask |= 1 << HISTORY_FIELDS.index(name)
+    return mask
+
+
+def history_names(mask: int) -> tuple:
+    """Field names of a NIMBUS_HISTORY_* mask, in image order."""
+    return tuple(k for i, k in enumerate(HISTORY_FIELDS) if mask >> i & 1)
 
 
 def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
@@ -225,7 +262,13 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
     lib.nimbus_cuda_eos_projection.argtypes = [ctypes.c_void_p, ctypes.POINTER(EosArgs)]
     lib.nimbus_cuda_acoustic_boundaries.argtypes = [ctypes.c_void_p, ctypes.POINTER(BoundaryArgs)]
     lib.nimbus_cuda_state_relaxation.argtypes = [ctypes.c_void_p, ctypes.POINTER(StateRelaxationArgs)]
+    lib.nimbus_cuda_cell_centre_velocity.argtypes = [ctypes.c_void_p, ctypes.POINTER(CellCentreArgs)]
+    lib.nimbus_cuda_history_snapshot.argtypes = [ctypes.c_void_p, ctypes.POINTER(HistoryArgs)]
+    lib.nimbus_npy_write_3d.argtypes = [_fp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_char_p]
+    lib.nimbus_history_write.argtypes = [_fp, ctypes.c_uint, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_char_p]
     vp = ctypes.c_void_p
+    lib.nimbus_cuda_engine_history_async.argtypes = [vp, ctypes.c_int, ctypes.c_uint, vp]
     lib.nimbus_cuda_engine_create.argtypes = [vp, ctypes.POINTER(vp)]
     lib.nimbus_cuda_engine_destroy.argtypes = [vp]
     lib.nimbus_cuda_engine_destroy.restype = None
@@ -385,6 +428,12 @@ class Context:
     def acoustic_boundaries(self, args: BoundaryArgs) -> int:
         return self.lib.nimbus_cuda_acoustic_boundaries(self.handle, ctypes.byref(args))
 
+    def cell_centre_velocity(self, args: CellCentreArgs) -> int:
+        return self.lib.nimbus_cuda_cell_centre_velocity(self.handle, ctypes.byref(args))
+
+    def history_snapshot(self, args: HistoryArgs) -> int:
+        return self.lib.nimbus_cuda_history_snapshot(self.handle, ctypes.byref(args))
+
     def state_relaxation(self, args: StateRelaxationArgs) -> int:
         return self.lib.nimbus_cuda_state_relaxation(self.handle, ctypes.byref(args))
 
@@ -537,6 +586,64 @@ def state_relaxation_args(fields, profiles, dt, memory=MEMORY_HOST, stream=None)
     a.memory = memory
     a.stream = stream
     return a
+
+
+def cell_centre_args(u=None, v=None, w=None, outputs=None, ground_w=None, memory=MEMORY_HOST,
+                     stream=None) -> CellCentreArgs:
+    """Argument block for nimbus_cuda_cell_centre_velocity.  outputs: (uc, vc,
+    wc) arrays or tensors, None entries skipped; by default one array (host) or
+    tensor (device) per given face field."""
+    faces = (u, v, w)
+    face = next(x for x in faces if x is not None)
+    if outputs is None:
+        outputs = tuple(None if x is None else (np.empty_like(x) if isinstance(x, np.ndarray) else x.new_empty(x.shape))
+                        for x in faces)
+    g = None if ground_w is None else np.ascontiguousarray(ground_w, dtype=np.float64)
+    a = CellCentreArgs()
+    a._keep = (faces, outputs, g)
+    a.outputs = outputs
+    a.u, a.v, a.w = (_f(x) for x in faces)
+    a.u_centre, a.v_centre, a.w_centre = (_f(x) for x in outputs)
+    a.ground_w = _d(g)
+    a.nx, a.ny, a.nz = tuple(face.shape)
+    a.memory = memory
+    a.stream = stream
+    return a
+
+
+def history_args(fields: dict, mask: int, host_image, shape, ground_w=None, stream=None) -> HistoryArgs:
+    """Argument block for nimbus_cuda_history_snapshot: fields maps names to
+    device tensors (or addresses); host_image a C-contiguous float32 array of
+    at least popcount(mask) * cells floats (pinned for overlap)."""
+    g = None if ground_w is None else np.ascontiguousarray(ground_w, dtype=np.float64)
+    a = HistoryArgs()
+    a._keep = (fields, host_image, g)
+    for k in HISTORY_FIELDS:
+        setattr(a, k, _f(fields.get(k)))
+    a.fields = int(mask)
+    a.ground_w = _d(g)
+    a.nx, a.ny, a.nz = (int(x) for x in shape)
+    a.host_image = _f(host_image)
+    a.stream = stream
+    return a
+
+
+def npy_write_3d(data: np.ndarray, path, lib: Optional[ctypes.CDLL] = None) -> int:
+    """nimbus_npy_write_3d of a C-contiguous float32 [d0][d1][d2] array; the
+    status code."""
+    lib = lib or load_library()
+    a = np.ascontiguousarray(data, dtype=np.float32)
+    d = tuple(a.shape) if a.ndim == 3 else (0, 0, 0)
+    return lib.nimbus_npy_write_3d(a.ctypes.data_as(_fp), *[int(x) for x in d], str(path).encode())
+
+
+def history_write(image: np.ndarray, mask: int, shape, step_dir, lib: Optional[ctypes.CDLL] = None) -> int:
+    """nimbus_history_write: <step_dir>/<name>.npy for each field of mask
+    from a history image; the status code."""
+    lib = lib or load_library()
+    assert image.dtype == np.float32 and image.flags["C_CONTIGUOUS"]
+    return lib.nimbus_history_write(image.ctypes.data_as(_fp), int(mask), *[int(x) for x in shape],
+                                    str(step_dir).encode())
 
 
 def eos_args(p, rho, theta, qv=None, qc=None, qr=None, memory=MEMORY_HOST, stream=None, p0=None) -> EosArgs:
@@ -761,6 +868,16 @@ class Engine:
     def download_image_async(self, image: np.ndarray):
         assert image.flags["C_CONTIGUOUS"] and image.nbytes >= self.image_bytes()
         self.ctx.check(self.lib.nimbus_cuda_engine_download_image_async(self.handle, image.ctypes.data))
+
+    def history_async(self, member_id: int, mask: int, image: np.ndarray):
+        """Enqueue a history frame of the member (cell-centred u, v, w and the
+        scalars of mask, image order) into a pinned float32 image on the
+        engine's stream; complete after synchronize."""
+        shape = self.shapes.get(member_id, (0, 0, 0))  # an unknown id is the library's to refuse
+        assert image.dtype == np.float32 and image.flags["C_CONTIGUOUS"]
+        assert image.size >= bin(mask).count("1") * shape[0] * shape[1] * shape[2]
+        self.ctx.check(self.lib.nimbus_cuda_engine_history_async(self.handle, int(member_id), int(mask),
+                                                                 image.ctypes.data))
 
     def step(self, n: int = 1):
         self.ctx.check(self.lib.nimbus_cuda_engine_step(self.handle, int(n)))

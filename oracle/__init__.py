@@ -208,6 +208,21 @@ class Restatement:
         if rc != 0:
             raise ValueError("state relaxation: invalid alpha or dt")
 
+    def cell_centre(self, u, v, w, ground_w=None):
+        """Cell-centre u, v, w of face fields (oracle_cell_centre); a None
+        input skips that component (its output is None).  ground_w: the
+        terrain lower-face w per column ([nx][ny] FP64) or None (flat)."""
+        face = next(a for a in (u, v, w) if a is not None)
+        self._chk(*[a for a in (u, v, w) if a is not None])
+        nx, ny, nz = face.shape
+        outs = [None if a is None else np.empty_like(a) for a in (u, v, w)]
+        g = None if ground_w is None else np.ascontiguousarray(ground_w, dtype=np.float64)
+        rc = self.lib.oracle_cell_centre(nx, ny, nz, *[_opt(a) for a in (u, v, w)], *[_opt(o) for o in outs],
+                                         _opt(g))
+        if rc != 0:
+            raise ValueError("terrain lower-boundary velocity must contain only finite values")
+        return tuple(outs)
+
     def scalar_transport(self, qs, pd, rho_end, rho_begin, mfx, mfy, mfz, dt, grid, weno=True, top_open=False):
         self._chk(rho_end, rho_begin, mfx, mfy, mfz, *qs)
         nx, ny, nz = rho_end.shape
@@ -225,6 +240,27 @@ class Restatement:
 
 def _opt(a):
     return None if a is None else _fp(a)
+
+
+def npy_header(shape, descr: str = "<f4") -> bytes:
+    """The header npy::write_3d / write_2d write (src/core/output/npy_writer.cpp:27-118):
+    magic, version 1.0, a little-endian uint16 header length, the dict
+    "{'descr': '<f4', 'fortran_order': False, 'shape': (a, b, c), }" padded
+    with spaces so that the preamble, dict and newline end on a 16-byte
+    boundary."""
+    dims = ", ".join(str(int(x)) for x in shape) + ("," if len(shape) == 1 else "")
+    head = "{'descr': '" + descr + "', 'fortran_order': False, 'shape': (" + dims + "), }"
+    pad = (16 - (10 + len(head) + 1) % 16) % 16
+    body = (head + " " * pad + "\n").encode("ascii")
+    return b"\x93NUMPY\x01\x00" + len(body).to_bytes(2, "little") + body
+
+
+def npy_bytes(data) -> bytes:
+    """The whole file the reference's writer produces for a float32 (or
+    float64) array: npy_header, then the C-order little-endian payload."""
+    a = np.ascontiguousarray(data)
+    descr = {np.dtype(np.float32): "<f4", np.dtype(np.float64): "<f8"}[a.dtype]
+    return npy_header(a.shape, descr) + a.astype(a.dtype.newbyteorder("<")).tobytes()
 
 
 def _slow_inputs(st, base, moist=True):
@@ -323,6 +359,23 @@ class ReferenceHarness:
         prof = dict(zip(names, out))
         prof["lateral_alpha"] = prof["lateral_alpha"][:c.lateral_width]
         return prof
+
+    def cell_centre(self, u, v, w, ground_w=None):
+        """interpolate_u/v/w_face_to_center on face fields; a None input
+        skips that component.  A non-finite ground_w raises (the reference's
+        invalid_argument)."""
+        face = next(a for a in (u, v, w) if a is not None)
+        nx, ny, nz = face.shape
+        outs = [None if a is None else np.empty_like(a) for a in (u, v, w)]
+        g = None if ground_w is None else np.ascontiguousarray(ground_w, dtype=np.float64)
+        self._rc(self.lib.ref_cell_centre(*[_opt(a) for a in (u, v, w)], *[_opt(o) for o in outs], _opt(g),
+                                          nx, ny, nz))
+        return tuple(outs)
+
+    def npy_write_3d(self, data, path):
+        """npy::write_3d of a float32 [d0][d1][d2] array to path."""
+        a = np.ascontiguousarray(data, dtype=np.float32)
+        self._rc(self.lib.ref_npy_write_3d(_fp(a), *[int(x) for x in a.shape], str(path).encode()))
 
     def large_step(self, st, base, grid, dt, n_substeps, bc, coriolis_f=0.0):
         """One large step of the hot path from the reference's own objects:

@@ -1241,3 +1241,34 @@ int oracle_state_relaxation(int nx, int ny, int nz, REAL* u, REAL* v, REAL* w, R
             }
     return 0;
 }
+
+/* ------------------------------------------------------------------------- */
+/* Cell-centre velocities for output (src/core/output/stagger_interpolation.cpp):
+ * u: centre i is the mean of faces i-1 and i, cell 0 keeps face 0 (the west
+ * boundary face); v likewise in j; w: centre k > 0 is the mean of faces k-1
+ * and k, centre 0 is 0.5 (ground_w + w[0]) formed in FP64 and rounded once,
+ * with ground_w the column's lower-face velocity (0 on flat ground).  Interior
+ * means are 0.5f * (a + b) in storage precision.  A null output skips that
+ * component.  Returns -1 when ground_w holds a non-finite value (the
+ * reference's invalid_argument), before anything is written. */
+int oracle_cell_centre(int nx, int ny, int nz, const REAL* u, const REAL* v, const REAL* w, REAL* uc, REAL* vc,
+                       REAL* wc, const double* ground_w)
+{
+    if (wc && ground_w)
+        for (size_t c = 0; c < (size_t)nx * (size_t)ny; ++c)
+            if (!isfinite(ground_w[c])) return -1;
+    const REAL half = (REAL)0.5;
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j)
+        {
+            const double lower = ground_w ? ground_w[(size_t)i * (size_t)ny + (size_t)j] : 0.0;
+            for (int k = 0; k < nz; ++k)
+            {
+                const size_t c = IDX(i, j, k);
+                if (uc) uc[c] = i == 0 ? u[c] : half * (u[IDX(i - 1, j, k)] + u[c]);
+                if (vc) vc[c] = j == 0 ? v[c] : half * (v[IDX(i, j - 1, k)] + v[c]);
+                if (wc) wc[c] = k == 0 ? (REAL)(0.5 * (lower + (double)w[c])) : half * (w[c - 1] + w[c]);
+            }
+        }
+    return 0;
+}

@@ -29,6 +29,11 @@
 //                           (src/core/infra/rayleigh_damping.cpp:720-1119,1194-1476),
 //                           the end-of-step sponge of dynamics.cpp:7323-7340, with
 //                           the per-level profiles its runtime built
+//   ref_cell_centre         interpolate_u/v/w_face_to_center
+//                           (src/core/output/stagger_interpolation.cpp), the C-grid
+//                           output staging of the history and live export
+//                           (headless_runtime.cpp:2577-2601)
+//   ref_npy_write_3d        npy::write_3d (src/core/output/npy_writer.cpp:143-156)
 //   ref_scalar_transport    advect_scalars_conservative_3d_cartesian
 //                           (advection_cartesian.cpp:3532) on a retained context whose
 //                           face mass fluxes and beginning density are supplied
@@ -52,11 +57,14 @@
 #include "microphysics/schemes/kessler/kessler.hpp"
 #include "dynamics/eos_pressure.hpp"
 #include "core/infra/rayleigh_damping.hpp"
+#include "core/output/npy_writer.hpp"
+#include "core/output/stagger_interpolation.hpp"
 
 #include <cstring>
 #include <exception>
 #include <memory>
 #include <string>
+#include <vector>
 
 #ifdef _OPENMP
 #include <omp.h>
@@ -543,6 +551,51 @@ int ref_state_relaxation(float* u, float* v, float* w, float* theta, const doubl
     {
         return fail(e.what());
     }
+}
+
+// Cell-centre velocities of face fields u, v, w ([nx][ny][nz] each); a null
+// output skips that component; ground_w (nx*ny, may be null) is the terrain
+// lower-face w the reference's terrain form takes.
+int ref_cell_centre(const float* u, const float* v, const float* w, float* uc, float* vc, float* wc,
+                    const double* ground_w, int nx, int ny, int nz)
+{
+    try
+    {
+        Field3D face, centre;
+        if (uc)
+        {
+            to_field(face, u, nx, ny, nz);
+            interpolate_u_face_to_center(face, centre);
+            from_field(uc, centre);
+        }
+        if (vc)
+        {
+            to_field(face, v, nx, ny, nz);
+            interpolate_v_face_to_center(face, centre);
+            from_field(vc, centre);
+        }
+        if (wc)
+        {
+            to_field(face, w, nx, ny, nz);
+            if (ground_w)
+                interpolate_w_face_to_center(
+                    face, centre, std::vector<double>(ground_w, ground_w + static_cast<std::size_t>(nx) * ny));
+            else
+                interpolate_w_face_to_center(face, centre);
+            from_field(wc, centre);
+        }
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        return fail(e.what());
+    }
+}
+
+// npy::write_3d of a float32 array; 0 on success.
+int ref_npy_write_3d(const float* data, int dim0, int dim1, int dim2, const char* path)
+{
+    return npy::write_3d(data, dim0, dim1, dim2, std::string(path)) ? 0 : fail("npy::write_3d failed");
 }
 
 } // extern "C"

@@ -146,10 +146,41 @@ def make_state_relaxation():
     print("wrote state_relaxation")
 
 
+# Output: cell-centre velocities on grids whose nz takes every run width of
+# the device kernel (4, 2, 1) plus a single cell, flat and with a terrain
+# lower-face velocity; and one npy file written by the reference's writer.
+OUTPUT_SHAPES = ((6, 5, 8), (9, 7, 6), (5, 4, 7), (1, 1, 1), (1, 6, 3), (4, 1, 5))
+
+
+def make_output():
+    ref = ReferenceHarness()
+    rng = np.random.default_rng(61)
+    out = {}
+    for n, shape in enumerate(OUTPUT_SHAPES):
+        faces = [(rng.standard_normal(shape) * 12.0).astype(np.float32) for _ in range(3)]
+        ground = rng.standard_normal(shape[:2]) * 2.5
+        flat = ref.cell_centre(*faces)
+        terrain = ref.cell_centre(None, None, faces[2], ground)
+        for k, a in zip("uvw", faces):
+            out[f"s{n}_{k}"] = a
+        for k, a in zip("uvw", flat):
+            out[f"s{n}_{k}c"] = a
+        out[f"s{n}_ground"] = ground
+        out[f"s{n}_wc_terrain"] = terrain[2]
+    data = (rng.standard_normal((3, 4, 5)) * 100.0).astype(np.float32)
+    out["npy_data"] = data
+    np.savez_compressed(HERE / "cell_centre.npz", **out)
+    ref.npy_write_3d(data, HERE / "npy_write_3d.npy")
+    print("wrote cell_centre, npy_write_3d")
+
+
 if __name__ == "__main__":
-    # `make_golden.py state_relaxation` writes only that fixture.
+    # `make_golden.py state_relaxation` (or `output`) writes only that fixture.
     if sys.argv[1:] == ["state_relaxation"]:
         make_state_relaxation()
+    elif sys.argv[1:] == ["output"]:
+        make_output()
     else:
         main()
         make_state_relaxation()
+        make_output()

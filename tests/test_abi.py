@@ -17,7 +17,7 @@ HEADER = ROOT / "include" / "nimbus_cuda.h"
 
 def declared_functions():
     text = HEADER.read_text()
-    return sorted(set(re.findall(r"^\s*(?:nimbus_status|void\*?|const char\*|int|uint64_t|size_t)\s+(nimbus_cuda_\w+)\(",
+    return sorted(set(re.findall(r"^\s*(?:nimbus_status|void\*?|const char\*|int|uint64_t|size_t)\s+(nimbus_\w+)\(",
                                  text, re.M)))
 
 
@@ -54,6 +54,8 @@ def _c_layout(struct_name, fields, tmp_path):
     ("nimbus_eos_args", cuda.EosArgs),
     ("nimbus_boundary_args", cuda.BoundaryArgs),
     ("nimbus_state_relaxation_args", cuda.StateRelaxationArgs),
+    ("nimbus_cell_centre_args", cuda.CellCentreArgs),
+    ("nimbus_history_args", cuda.HistoryArgs),
     ("nimbus_member_desc", cuda.MemberDesc),
     ("nimbus_member_state", cuda.MemberState),
 ])
