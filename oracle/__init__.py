@@ -223,6 +223,63 @@ class Restatement:
             raise ValueError("terrain lower-boundary velocity must contain only finite values")
         return tuple(outs)
 
+    def smagorinsky(self, st, dz, grid, sgs):
+        """The Smagorinsky producer (oracle_smagorinsky) on st's u, v, w,
+        theta, rho and optional qv; dz: FP64 cell thickness per level; sgs: a
+        nimbus_b200.sgs.SgsConfig.  Returns {nu_t, K_theta, K_q, dudt, dvdt,
+        dwdt, dthdt, dqvdt}; raises ValueError where the reference throws."""
+        u = st["u"]
+        qv = st.get("qv")
+        self._chk(u, st["v"], st["w"], st["theta"], st["rho"], qv)
+        nx, ny, nz = u.shape
+        dz = np.ascontiguousarray(dz, dtype=np.float64)
+        delta = np.array([sgs_filter_width(sgs.filter_width, grid[0], grid[1], float(dz[k])) for k in range(nz)])
+        out = {k: np.empty_like(u) for k in SGS_OUTPUTS}
+        opened = (ctypes.c_int * 4)(*[int(x) for x in sgs.open_lateral])
+        rc = self.lib.oracle_smagorinsky(
+            nx, ny, nz, _fp(u), _fp(st["v"]), _fp(st["w"]), _fp(st["theta"]), _opt(qv), _fp(st["rho"]), _fp(dz),
+            _fp(delta), ctypes.c_double(grid[0]), ctypes.c_double(grid[1]), int(sgs.use_horizontal),
+            int(sgs.use_vertical), int(sgs.periodic_x), int(sgs.periodic_y), opened, ctypes.c_double(sgs.Cs),
+            ctypes.c_double(sgs.Pr_t), ctypes.c_double(sgs.Sc_t), ctypes.c_double(sgs.nu_t_max),
+            ctypes.c_double(sgs.K_max), *[_fp(out[k]) for k in SGS_OUTPUTS])
+        if rc == -2:
+            raise ValueError("turbulence field violates its finite physical domain")
+        if rc != 0:
+            raise ValueError("Smagorinsky coefficient is not finite")
+        return out
+
+    def sgs_apply(self, st, rates, dt, theta0=None, repairs=True, theta_ref=300.0):
+        """Forward-Euler SGS application in place on st's u, v, w, theta and
+        optional qv (oracle_sgs_apply); rates as smagorinsky() returns."""
+        u = st["u"]
+        qv = st.get("qv")
+        nx, ny, nz = u.shape
+        t0 = None if theta0 is None else np.ascontiguousarray(theta0, dtype=np.float64)
+        self.lib.oracle_sgs_apply(
+            nx, ny, nz, _fp(u), _fp(st["v"]), _fp(st["w"]), _fp(st["theta"]), _opt(qv), None,
+            _fp(rates["dudt"]), _fp(rates["dvdt"]), _fp(rates["dwdt"]), _fp(rates["dthdt"]),
+            _opt(rates["dqvdt"] if qv is not None else None), None, None, _opt(t0), ctypes.c_double(dt),
+            int(bool(repairs)), ctypes.c_double(theta_ref), ctypes.c_float(200.0), ctypes.c_float(700.0),
+            ctypes.c_float(0.05), ctypes.c_float(180.0), ctypes.c_float(120.0))
+
+    def sgs_stability(self, st, rates, grid, dz, sgs):
+        """oracle_sgs_stability (periodic or closed lateral faces only): the
+        same dict as ReferenceHarness.sgs_stability."""
+        u = st["u"]
+        qv = st.get("qv")
+        nx, ny, nz = u.shape
+        out = np.zeros(5)
+        rc = self.lib.oracle_sgs_stability(
+            nx, ny, nz, _fp(u), _fp(st["v"]), _fp(st["w"]), _fp(st["theta"]), _opt(qv), _fp(st["rho"]),
+            _fp(rates["dudt"]), _fp(rates["dvdt"]), _fp(rates["dwdt"]), _fp(rates["dthdt"]),
+            _opt(rates["dqvdt"] if qv is not None else None), ctypes.c_double(grid[0]), ctypes.c_double(grid[1]),
+            _fp(np.ascontiguousarray(dz, dtype=np.float64)), int(sgs.periodic_x), int(sgs.periodic_y), _fp(out))
+        if rc == -2:
+            raise ValueError("SGS stability evaluation requires a finite, positive state")
+        if rc != 0:
+            raise ValueError("realized SGS tendency has no positive stable timestep")
+        return dict(zip(("maximum", "momentum_energy", "theta_monotonic", "qv_monotonic", "dissipation_w"), out))
+
     def scalar_transport(self, qs, pd, rho_end, rho_begin, mfx, mfy, mfz, dt, grid, weno=True, top_open=False):
         self._chk(rho_end, rho_begin, mfx, mfy, mfz, *qs)
         nx, ny, nz = rho_end.shape
@@ -240,6 +297,22 @@ class Restatement:
 
 def _opt(a):
     return None if a is None else _fp(a)
+
+
+SGS_OUTPUTS = ("nu_t", "K_theta", "K_q", "dudt", "dvdt", "dwdt", "dthdt", "dqvdt")
+SGS_MODES = {(1, 1): 0, (1, 0): 1, (0, 1): 2}
+
+
+def sgs_filter_width(kind: str, dx: float, dy: float, dz: float) -> float:
+    """compute_filter_width (src/turbulence/base/eddy_viscosity.cpp:1414-1468),
+    flat grid: sqrt(dx dy) for "dx", cbrt(dx dy dz) for "cubic_root"
+    (math.sqrt / math.cbrt are the C library's, as in the reference)."""
+    import math
+    if kind == "dx":
+        return math.sqrt(dx * dy)
+    if kind == "cubic_root":
+        return math.cbrt(dx * dy * dz)
+    raise ValueError(kind)
 
 
 def npy_header(shape, descr: str = "<f4") -> bytes:
@@ -376,6 +449,53 @@ class ReferenceHarness:
         """npy::write_3d of a float32 [d0][d1][d2] array to path."""
         a = np.ascontiguousarray(data, dtype=np.float32)
         self._rc(self.lib.ref_npy_write_3d(_fp(a), *[int(x) for x in a.shape], str(path).encode()))
+
+    def smagorinsky(self, st, dz, grid, sgs):
+        """SmagorinskyScheme::compute on the flat C-grid CPU path; same
+        outputs as Restatement.smagorinsky."""
+        u = st["u"]
+        qv = st.get("qv")
+        nx, ny, nz = u.shape
+        out = {k: np.empty_like(u) for k in SGS_OUTPUTS}
+        opened = (ctypes.c_int * 4)(*[int(x) for x in sgs.open_lateral])
+        self._rc(self.lib.ref_smagorinsky(
+            _fp(u), _fp(st["v"]), _fp(st["w"]), _fp(st["theta"]), _opt(qv), _fp(st["rho"]),
+            _fp(np.ascontiguousarray(dz, dtype=np.float64)), nx, ny, nz, ctypes.c_double(grid[0]),
+            ctypes.c_double(grid[1]), SGS_MODES[(int(sgs.use_horizontal), int(sgs.use_vertical))],
+            int(sgs.filter_width == "dx"), int(sgs.periodic_x), int(sgs.periodic_y), opened,
+            ctypes.c_double(sgs.Cs), ctypes.c_double(sgs.Pr_t), ctypes.c_double(sgs.Sc_t),
+            ctypes.c_double(sgs.nu_t_max), ctypes.c_double(sgs.K_max), *[_fp(out[k]) for k in SGS_OUTPUTS]))
+        return out
+
+    def sgs_apply(self, st, rates, dt, theta0=None, repairs=True):
+        """apply_admitted_sgs_substep (CPU path) in place on st's u, v, w,
+        theta and optional qv."""
+        u = st["u"]
+        qv = st.get("qv")
+        nx, ny, nz = u.shape
+        t0 = None if theta0 is None else np.ascontiguousarray(theta0, dtype=np.float64)
+        self._rc(self.lib.ref_sgs_apply(
+            _fp(u), _fp(st["v"]), _fp(st["w"]), _fp(st["theta"]), _opt(qv), _fp(rates["dudt"]),
+            _fp(rates["dvdt"]), _fp(rates["dwdt"]), _fp(rates["dthdt"]),
+            _opt(rates["dqvdt"] if qv is not None else None), _opt(t0), nx, ny, nz, ctypes.c_double(dt),
+            int(bool(repairs))))
+
+    def sgs_stability(self, st, rates, grid, bc, sgs):
+        """compute_sgs_explicit_stability with deterministic reductions:
+        {maximum, momentum_energy, theta_monotonic, qv_monotonic,
+        dissipation_w}."""
+        u = st["u"]
+        qv = st.get("qv")
+        nx, ny, nz = u.shape
+        out = np.zeros(5)
+        bcs = (ctypes.c_int * 6)(*[int(x) for x in bc])
+        self._rc(self.lib.ref_sgs_stability(
+            _fp(u), _fp(st["v"]), _fp(st["w"]), _fp(st["theta"]), _opt(qv), _fp(st["rho"]), _fp(rates["dudt"]),
+            _fp(rates["dvdt"]), _fp(rates["dwdt"]), _fp(rates["dthdt"]),
+            _opt(rates["dqvdt"] if qv is not None else None), nx, ny, nz, ctypes.c_double(grid[0]),
+            ctypes.c_double(grid[1]), ctypes.c_double(grid[2]), bcs,
+            SGS_MODES[(int(sgs.use_horizontal), int(sgs.use_vertical))], _fp(out)))
+        return dict(zip(("maximum", "momentum_energy", "theta_monotonic", "qv_monotonic", "dissipation_w"), out))
 
     def large_step(self, st, base, grid, dt, n_substeps, bc, coriolis_f=0.0):
         """One large step of the hot path from the reference's own objects:

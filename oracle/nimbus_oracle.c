@@ -1272,3 +1272,576 @@ int oracle_cell_centre(int nx, int ny, int nz, const REAL* u, const REAL* v, con
         }
     return 0;
 }
+
+/* ------------------------------------------------------------------------- */
+/* Smagorinsky SGS closure on a flat C-grid (stability correction "none").
+ *
+ * Neighbours (src/turbulence/base/eddy_viscosity.cpp:69-105): clamped to the
+ * allocated range, or on a periodic axis wrapped over the physical rows
+ * 1..n-2 (the ghost rows 0 and n-1 never take part). */
+static int sgs_prev(int i, int n, int periodic)
+{
+    if (!periodic) return i > 0 ? i - 1 : 0;
+    return i <= 1 ? n - 2 : (i - 1 < n - 2 ? i - 1 : n - 2);
+}
+
+static int sgs_next(int i, int n, int periodic)
+{
+    if (!periodic) return i + 1 < n - 1 ? i + 1 : n - 1;
+    return i >= n - 2 ? 1 : (i + 1 > 1 ? i + 1 : 1);
+}
+
+typedef struct
+{
+    int nx, ny, nz, use_h, use_v, px, py;
+    double dx, dy;
+    const double* dz; /* cell thickness per level */
+} sgs_grid;
+
+/* Distance between scalar centres k and k+1 (grid_metric_utils.hpp:157-181). */
+static double sgs_dzc(const sgs_grid* g, int k) { return 0.5 * (g->dz[k] + g->dz[k + 1]); }
+
+#define SIDX(i, j, k) (((size_t)(i) * (size_t)G->ny + (size_t)(j)) * (size_t)G->nz + (size_t)(k))
+
+static double sgs_w(const sgs_grid* G, const REAL* w, int i, int j, int k)
+{
+    return k < 0 ? 0.0 : (double)w[SIDX(i, j, k)];
+}
+
+/* Strain-rate square at a scalar centre, each component where it lives on
+ * the C-grid and the off-diagonal squares averaged from the four edges
+ * (compute_directional_strain_sq_centered, eddy_viscosity.cpp:1253-1400).
+ * mode: use_h && use_v "3d", use_h alone "horizontal_only", use_v alone
+ * "vertical_only". */
+static double sgs_strain_sq(const sgs_grid* G, const REAL* u, const REAL* v, const REAL* w, int i, int j, int k)
+{
+    const int nx = G->nx, ny = G->ny, nz = G->nz;
+    const double dx = G->dx, dy = G->dy, dzk = G->dz[k];
+    const int jm = sgs_prev(j, ny, G->py), im = sgs_prev(i, nx, G->px);
+    const double s11 = ((double)u[SIDX(i, j, k)] - (double)u[SIDX(im, j, k)]) / dx;
+    const double s22 = ((double)v[SIDX(i, j, k)] - (double)v[SIDX(i, jm, k)]) / dy;
+    const double s33 = (sgs_w(G, w, i, j, k) - sgs_w(G, w, i, j, k - 1)) / dzk;
+    double s12[4];
+    const int ie[4] = {im, im, i, i}, je[4] = {jm, j, jm, j};
+    for (int e = 0; e < 4; ++e)
+    {
+        const int ii = ie[e], jj = je[e];
+        const int jj1 = sgs_next(jj, ny, G->py), ii1 = sgs_next(ii, nx, G->px);
+        const double dudy = ((double)u[SIDX(ii, jj1, k)] - (double)u[SIDX(ii, jj, k)]) / dy;
+        const double dvdx = ((double)v[SIDX(ii1, jj, k)] - (double)v[SIDX(ii, jj, k)]) / dx;
+        s12[e] = 0.5 * (dudy + dvdx);
+    }
+    /* xz edges (x-face, z-face) and yz edges (y-face, z-face): {d/dz, d w/dx}. */
+    double xz[4][2], yz[4][2];
+    const int xi[4] = {im, im, i, i}, yj[4] = {jm, jm, j, j}, ke[4] = {k - 1, k, k - 1, k};
+    for (int e = 0; e < 4; ++e)
+    {
+        const int kk = ke[e];
+        if (kk < 0 || kk >= nz - 1)
+        {
+            xz[e][0] = xz[e][1] = yz[e][0] = yz[e][1] = 0.0;
+            continue;
+        }
+        const double dzc = sgs_dzc(G, kk);
+        const int ii = xi[e], ii1 = sgs_next(ii, nx, G->px);
+        xz[e][0] = ((double)u[SIDX(ii, j, kk + 1)] - (double)u[SIDX(ii, j, kk)]) / dzc;
+        xz[e][1] = (sgs_w(G, w, ii1, j, kk) - sgs_w(G, w, ii, j, kk)) / dx;
+        const int jj = yj[e], jj1 = sgs_next(jj, ny, G->py);
+        yz[e][0] = ((double)v[SIDX(i, jj, kk + 1)] - (double)v[SIDX(i, jj, kk)]) / dzc;
+        yz[e][1] = (sgs_w(G, w, i, jj1, kk) - sgs_w(G, w, i, jj, kk)) / dy;
+    }
+    const double s12_sq = 0.25 * (s12[0] * s12[0] + s12[1] * s12[1] + s12[2] * s12[2] + s12[3] * s12[3]);
+#define SGS_AVG_SQ(a, c) (0.25 * (a[0][c] * a[0][c] + a[1][c] * a[1][c] + a[2][c] * a[2][c] + a[3][c] * a[3][c]))
+    if (G->use_h && !G->use_v)
+        return 2.0 * (s11 * s11 + s22 * s22) + 4.0 * s12_sq + SGS_AVG_SQ(xz, 1) + SGS_AVG_SQ(yz, 1);
+    if (G->use_v && !G->use_h)
+        return SGS_AVG_SQ(xz, 0) + SGS_AVG_SQ(yz, 0) + 2.0 * s33 * s33;
+#undef SGS_AVG_SQ
+    double sym_xz[4], sym_yz[4];
+    for (int e = 0; e < 4; ++e)
+    {
+        const double a = 0.5 * (xz[e][0] + xz[e][1]);
+        const double b = 0.5 * (yz[e][0] + yz[e][1]);
+        sym_xz[e] = a * a;
+        sym_yz[e] = b * b;
+    }
+    const double s13_sq = 0.25 * (sym_xz[0] + sym_xz[1] + sym_xz[2] + sym_xz[3]);
+    const double s23_sq = 0.25 * (sym_yz[0] + sym_yz[1] + sym_yz[2] + sym_yz[3]);
+    return 2.0 * (s11 * s11 + s22 * s22 + s33 * s33) + 4.0 * (s12_sq + s13_sq + s23_sq);
+}
+
+static double sgs_min(double a, double b) { return b < a ? b : a; } /* std::min */
+
+/* Eddy coefficients of every cell (SmagorinskyScheme::compute_eddy_coefficients,
+ * smagorinsky.cpp:494-571): nu = Cs^2 Delta^2 |S| (Delta per level: sqrt(dx dy)
+ * or cbrt(dx dy dz), precomputed by the caller as the reference does), capped
+ * at nu_max; K_theta = nu / Pr_t, K_q = nu / Sc_t, capped at K_max.  Returns
+ * -1 at the first cell whose strain, viscosity or diffusivity is not finite
+ * (the reference throws), else 0. */
+static int sgs_coefficients(const sgs_grid* G, const REAL* u, const REAL* v, const REAL* w, const double* delta,
+                            double Cs, double Pr_t, double Sc_t, double nu_max, double K_max, REAL* nu_t,
+                            REAL* K_theta, REAL* K_q)
+{
+    for (int i = 0; i < G->nx; ++i)
+        for (int j = 0; j < G->ny; ++j)
+            for (int k = 0; k < G->nz; ++k)
+            {
+                const double strain = sqrt(sgs_strain_sq(G, u, v, w, i, j, k));
+                if (!isfinite(strain) || strain < 0.0) return -1;
+                double nu = Cs * Cs * delta[k] * delta[k] * strain * 1.0;
+                if (!isfinite(nu)) return -1;
+                nu = sgs_min(nu, nu_max);
+                const double kt = nu / Pr_t, kq = nu / Sc_t;
+                if (!isfinite(kt) || !isfinite(kq)) return -1;
+                const size_t c = SIDX(i, j, k);
+                nu_t[c] = (REAL)nu;
+                K_theta[c] = (REAL)sgs_min(kt, K_max);
+                K_q[c] = (REAL)sgs_min(kq, K_max);
+            }
+    return 0;
+}
+
+/* Conservative live-density stress divergence (compute_momentum_diffusion_tendencies,
+ * eddy_viscosity.cpp:1532-1948, flat C-grid): du_i/dt = (1/rho_face) d_j (2 mu S_ij)
+ * with mu = rho nu, diagonal stresses at centres, off-diagonal ones at edges
+ * (mu four-point averaged, thickness-weighted across z), zero shear stress at
+ * the ground and the lid.  Cells outside the updated faces are zero. */
+static void sgs_momentum(const sgs_grid* G, const REAL* u, const REAL* v, const REAL* w, const REAL* rho,
+                         const REAL* nu, REAL* dudt, REAL* dvdt, REAL* dwdt)
+{
+    const int nx = G->nx, ny = G->ny, nz = G->nz, px = G->px, py = G->py;
+    const double dx = G->dx, dy = G->dy;
+    const size_t n = (size_t)nx * ny * nz;
+    for (size_t c = 0; c < n; ++c) dudt[c] = dvdt[c] = dwdt[c] = (REAL)0;
+#define MU(ii, jj, kk) ((double)rho[SIDX(ii, jj, kk)] * (double)nu[SIDX(ii, jj, kk)])
+#define U(ii, jj, kk) ((double)u[SIDX(ii, jj, kk)])
+#define V(ii, jj, kk) ((double)v[SIDX(ii, jj, kk)])
+#define W(ii, jj, kk) sgs_w(G, w, ii, jj, kk)
+    /* mu on an xy edge (x-face ii, y-face jj) and on xz / yz edges (z-face kk). */
+#define MU_XY(ii, jj, kk) (0.25 * (MU(ii, jj, kk) + MU(sgs_next(ii, nx, px), jj, kk) + MU(ii, sgs_next(jj, ny, py), kk) + \
+                                   MU(sgs_next(ii, nx, px), sgs_next(jj, ny, py), kk)))
+    double lo, up;
+    for (int i = 1; i <= (px ? nx - 2 : nx - 3); ++i)
+        for (int j = 1; j <= ny - 2; ++j)
+        {
+            const int jmm = sgs_prev(j, ny, py), imm = sgs_prev(i, nx, px), ipp = sgs_next(i, nx, px);
+            double lower = 0.0;
+            for (int k = 0; k < nz - 1; ++k)
+            {
+                double div = 0.0;
+                if (G->use_h)
+                {
+                    const double s_r = (U(ipp, j, k) - U(i, j, k)) / dx;
+                    const double s_l = (U(i, j, k) - U(imm, j, k)) / dx;
+                    div += (2.0 * MU(ipp, j, k) * s_r - 2.0 * MU(i, j, k) * s_l) / dx;
+                    double t12[2];
+                    const int jes[2] = {j, jmm};
+                    for (int e = 0; e < 2; ++e)
+                    {
+                        const int je = jes[e], je1 = sgs_next(je, ny, py);
+                        const double s12 = 0.5 * ((U(i, je1, k) - U(i, je, k)) / dy + (V(ipp, je, k) - V(i, je, k)) / dx);
+                        t12[e] = 2.0 * MU_XY(i, je, k) * s12;
+                    }
+                    div += (t12[0] - t12[1]) / dy;
+                }
+                if (G->use_v)
+                {
+                    double upper = 0.0;
+                    if (k < nz - 1)
+                    {
+                        const double dudz = (U(i, j, k + 1) - U(i, j, k)) / sgs_dzc(G, k);
+                        const double grad = G->use_h ? dudz + (W(ipp, j, k) - W(i, j, k)) / dx : dudz;
+                        lo = 0.5 * (MU(i, j, k) + MU(ipp, j, k));
+                        up = 0.5 * (MU(i, j, k + 1) + MU(ipp, j, k + 1));
+                        const double mu_e = (G->dz[k + 1] * lo + G->dz[k] * up) / (G->dz[k] + G->dz[k + 1]);
+                        upper = mu_e * grad;
+                    }
+                    div += (upper - lower) / G->dz[k];
+                    lower = upper;
+                }
+                dudt[SIDX(i, j, k)] = (REAL)(div / (0.5 * ((double)rho[SIDX(i, j, k)] + (double)rho[SIDX(ipp, j, k)])));
+            }
+        }
+    for (int i = 1; i <= nx - 2; ++i)
+        for (int j = 1; j <= (py ? ny - 2 : ny - 3); ++j)
+        {
+            const int jmm = sgs_prev(j, ny, py), jpp = sgs_next(j, ny, py), imm = sgs_prev(i, nx, px);
+            double lower = 0.0;
+            for (int k = 0; k < nz - 1; ++k)
+            {
+                double div = 0.0;
+                if (G->use_h)
+                {
+                    const double s_n = (V(i, jpp, k) - V(i, j, k)) / dy;
+                    const double s_s = (V(i, j, k) - V(i, jmm, k)) / dy;
+                    div += (2.0 * MU(i, jpp, k) * s_n - 2.0 * MU(i, j, k) * s_s) / dy;
+                    double t21[2];
+                    const int ies[2] = {i, imm};
+                    for (int e = 0; e < 2; ++e)
+                    {
+                        const int ie = ies[e], ie1 = sgs_next(ie, nx, px);
+                        const double s12 = 0.5 * ((U(ie, jpp, k) - U(ie, j, k)) / dy + (V(ie1, j, k) - V(ie, j, k)) / dx);
+                        t21[e] = 2.0 * MU_XY(ie, j, k) * s12;
+                    }
+                    div += (t21[0] - t21[1]) / dx;
+                }
+                if (G->use_v)
+                {
+                    const double dvdz = (V(i, j, k + 1) - V(i, j, k)) / sgs_dzc(G, k);
+                    const double grad = G->use_h ? dvdz + (W(i, jpp, k) - W(i, j, k)) / dy : dvdz;
+                    lo = 0.5 * (MU(i, j, k) + MU(i, jpp, k));
+                    up = 0.5 * (MU(i, j, k + 1) + MU(i, jpp, k + 1));
+                    const double upper = (G->dz[k + 1] * lo + G->dz[k] * up) / (G->dz[k] + G->dz[k + 1]) * grad;
+                    div += (upper - lower) / G->dz[k];
+                    lower = upper;
+                }
+                dvdt[SIDX(i, j, k)] = (REAL)(div / (0.5 * ((double)rho[SIDX(i, j, k)] + (double)rho[SIDX(i, jpp, k)])));
+            }
+        }
+    for (int i = 1; i <= nx - 2; ++i)
+        for (int j = 1; j <= ny - 2; ++j)
+        {
+            const int imm = sgs_prev(i, nx, px), jmm = sgs_prev(j, ny, py);
+            double lower = 0.0;
+            if (G->use_v) lower = 2.0 * MU(i, j, 0) * ((W(i, j, 0) - W(i, j, -1)) / G->dz[0]);
+            for (int k = 0; k < nz - 1; ++k)
+            {
+                const double dzb = G->dz[k], dzt = G->dz[k + 1], dzd = sgs_dzc(G, k);
+                const double mass = 0.5 * ((double)rho[SIDX(i, j, k)] * dzb + (double)rho[SIDX(i, j, k + 1)] * dzt);
+                double force = 0.0;
+                if (G->use_v)
+                {
+                    const double t33 = 2.0 * MU(i, j, k + 1) * ((W(i, j, k + 1) - W(i, j, k)) / dzt);
+                    force += t33 - lower;
+                    lower = t33;
+                }
+                if (G->use_h)
+                {
+                    double t31[2], t32[2];
+                    const int ies[2] = {i, imm}, jes[2] = {j, jmm};
+                    for (int e = 0; e < 2; ++e)
+                    {
+                        const int ie = ies[e], ie1 = sgs_next(ie, nx, px);
+                        const double dwdx = (W(ie1, j, k) - W(ie, j, k)) / dx;
+                        const double gx = G->use_v ? (U(ie, j, k + 1) - U(ie, j, k)) / dzd + dwdx : dwdx;
+                        lo = 0.5 * (MU(ie, j, k) + MU(ie1, j, k));
+                        up = 0.5 * (MU(ie, j, k + 1) + MU(ie1, j, k + 1));
+                        t31[e] = (G->dz[k + 1] * lo + G->dz[k] * up) / (G->dz[k] + G->dz[k + 1]) * gx;
+                        const int je = jes[e], je1 = sgs_next(je, ny, py);
+                        const double dwdy = (W(i, je1, k) - W(i, je, k)) / dy;
+                        const double gy = G->use_v ? (V(i, je, k + 1) - V(i, je, k)) / dzd + dwdy : dwdy;
+                        lo = 0.5 * (MU(i, je, k) + MU(i, je1, k));
+                        up = 0.5 * (MU(i, je, k + 1) + MU(i, je1, k + 1));
+                        t32[e] = (G->dz[k + 1] * lo + G->dz[k] * up) / (G->dz[k] + G->dz[k + 1]) * gy;
+                    }
+                    force += dzd * (t31[0] - t31[1]) / dx;
+                    force += dzd * (t32[0] - t32[1]) / dy;
+                }
+                dwdt[SIDX(i, j, k)] = (REAL)(force / mass);
+            }
+        }
+#undef MU_XY
+#undef W
+#undef V
+#undef U
+#undef MU
+}
+
+/* Conservative scalar diffusion (compute_scalar_diffusion_tendencies,
+ * eddy_viscosity.cpp:1953-2090, flat C-grid): d phi/dt = (1/rho) d_j (rho_face
+ * K_face d phi/dx_j), zero flux at the ground and lid; a lateral face that is
+ * neither periodic nor open reflects its first physical row (zero flux).
+ * open: W, E, S, N. */
+static void sgs_scalar(const sgs_grid* G, const int* open, const REAL* rho, const REAL* K, const REAL* phi, REAL* out)
+{
+    const int nx = G->nx, ny = G->ny, nz = G->nz, px = G->px, py = G->py;
+    const size_t n = (size_t)nx * ny * nz;
+    for (size_t c = 0; c < n; ++c) out[c] = (REAL)0;
+#define TR(ii, jj, kk) ((double)rho[SIDX(ii, jj, kk)] * (double)K[SIDX(ii, jj, kk)])
+#define PH(ii, jj, kk) ((double)phi[SIDX(ii, jj, kk)])
+    for (int i = 1; i <= nx - 2; ++i)
+        for (int j = 1; j <= ny - 2; ++j)
+        {
+            const int jmm = !py && !open[2] && j == 1 ? j : sgs_prev(j, ny, py);
+            const int jpp = !py && !open[3] && j == ny - 2 ? j : sgs_next(j, ny, py);
+            const int imm = !px && !open[0] && i == 1 ? i : sgs_prev(i, nx, px);
+            const int ipp = !px && !open[1] && i == nx - 2 ? i : sgs_next(i, nx, px);
+            for (int k = 0; k < nz; ++k)
+            {
+                double div = 0.0;
+                if (G->use_h)
+                {
+                    const double fe = 0.5 * (TR(i, j, k) + TR(ipp, j, k)) * (PH(ipp, j, k) - PH(i, j, k)) / G->dx;
+                    const double fw = 0.5 * (TR(imm, j, k) + TR(i, j, k)) * (PH(i, j, k) - PH(imm, j, k)) / G->dx;
+                    const double fn = 0.5 * (TR(i, j, k) + TR(i, jpp, k)) * (PH(i, jpp, k) - PH(i, j, k)) / G->dy;
+                    const double fs = 0.5 * (TR(i, jmm, k) + TR(i, j, k)) * (PH(i, j, k) - PH(i, jmm, k)) / G->dy;
+                    div += (fe - fw) / G->dx + (fn - fs) / G->dy;
+                }
+                if (G->use_v)
+                {
+                    const double ft = k < nz - 1
+                        ? 0.5 * (TR(i, j, k) + TR(i, j, k + 1)) * (PH(i, j, k + 1) - PH(i, j, k)) / sgs_dzc(G, k)
+                        : 0.0;
+                    const double fb = k > 0
+                        ? 0.5 * (TR(i, j, k - 1) + TR(i, j, k)) * (PH(i, j, k) - PH(i, j, k - 1)) / sgs_dzc(G, k - 1)
+                        : 0.0;
+                    div += (ft - fb) / G->dz[k];
+                }
+                out[SIDX(i, j, k)] = (REAL)(div / (double)rho[SIDX(i, j, k)]);
+            }
+        }
+#undef PH
+#undef TR
+}
+
+/* The fused Smagorinsky producer: coefficients, then the momentum, theta and
+ * (when qv is given) qv tendencies; dqvdt is zero without qv.  Returns -2
+ * when an input violates the reference's field contract (u, v, w finite;
+ * theta and rho finite and positive; qv finite and non-negative;
+ * validate_scheme_inputs, eddy_viscosity.cpp:1088-1175) and nothing is
+ * written, -1 when a coefficient is not finite (the outputs are then
+ * partial, as the reference's are when it throws).  Else 0. */
+int oracle_smagorinsky(int nx, int ny, int nz, const REAL* u, const REAL* v, const REAL* w, const REAL* theta,
+                       const REAL* qv, const REAL* rho, const double* dz, const double* delta, double dx, double dy,
+                       int use_h, int use_v, int periodic_x, int periodic_y, const int* open_lateral, double Cs,
+                       double Pr_t, double Sc_t, double nu_max, double K_max, REAL* nu_t, REAL* K_theta, REAL* K_q,
+                       REAL* dudt, REAL* dvdt, REAL* dwdt, REAL* dthdt, REAL* dqvdt)
+{
+    const sgs_grid g = {nx, ny, nz, use_h, use_v, periodic_x, periodic_y, dx, dy, dz};
+    for (size_t c = 0; c < (size_t)nx * ny * nz; ++c)
+        if (!isfinite(u[c]) || !isfinite(v[c]) || !isfinite(w[c]) || !isfinite(theta[c]) || !(theta[c] > 0) ||
+            !isfinite(rho[c]) || !(rho[c] > 0) || (qv && (!isfinite(qv[c]) || qv[c] < 0)))
+            return -2;
+    if (sgs_coefficients(&g, u, v, w, delta, Cs, Pr_t, Sc_t, nu_max, K_max, nu_t, K_theta, K_q) != 0) return -1;
+    sgs_momentum(&g, u, v, w, rho, nu_t, dudt, dvdt, dwdt);
+    sgs_scalar(&g, open_lateral, rho, K_theta, theta, dthdt);
+    if (qv)
+        sgs_scalar(&g, open_lateral, rho, K_q, qv, dqvdt);
+    else
+        for (size_t c = 0; c < (size_t)nx * ny * nz; ++c) dqvdt[c] = (REAL)0;
+    return 0;
+}
+
+/* sanitize_value (include/core/field/field_bounds.hpp:40-56). */
+static REAL sgs_sanitize(REAL x, int repairs, REAL fallback, REAL lo, REAL hi)
+{
+    if (!repairs) return x;
+    if (!isfinite(x)) return fallback;
+    return x < lo ? lo : (hi < x ? hi : x);
+}
+
+/* Forward-Euler application of the SGS tendencies to every cell
+ * (apply_sgs_tendencies_cpu, src/core/orchestration/dynamics/sgs_apply.cpp:436-
+ * 956, without the work ledger): x += dt * dx/dt in FP64, rounded to FP32 and
+ * clamped (winds to +-wind_h / +-wind_v, theta to [theta_lo, theta_hi], qv to
+ * [0, qv_hi]); with repairs on, non-finite tendencies count as zero and a
+ * non-finite sum falls back (winds and qv to 0, theta to its old value, else
+ * the level's base theta, else theta_ref; a non-finite stored theta to
+ * (float) theta_ref).  qv and tke (with dtke_pbl) are optional. */
+void oracle_sgs_apply(int nx, int ny, int nz, REAL* u, REAL* v, REAL* w, REAL* theta, REAL* qv, REAL* tke,
+                      const REAL* dudt, const REAL* dvdt, const REAL* dwdt, const REAL* dthdt, const REAL* dqvdt,
+                      const REAL* dtkedt, const REAL* dtke_pbl, const double* theta0_base, double dt, int repairs,
+                      double theta_ref, float theta_lo, float theta_hi, float qv_hi, float wind_h, float wind_v)
+{
+    const size_t plane = (size_t)nz;
+    for (size_t c = 0; c < (size_t)nx * ny * nz; ++c)
+    {
+        double rates[4] = {(double)dudt[c], (double)dvdt[c], (double)dwdt[c], (double)dthdt[c]};
+        for (int r = 0; r < 4; ++r)
+            if (repairs && !isfinite(rates[r])) rates[r] = 0.0;
+        REAL* fields[3] = {u, v, w};
+        for (int r = 0; r < 3; ++r)
+        {
+            double x = (double)fields[r][c] + rates[r] * dt;
+            if (repairs && !isfinite(x)) x = 0.0;
+            const REAL lim = (REAL)(r == 2 ? wind_v : wind_h);
+            fields[r][c] = sgs_sanitize((REAL)x, repairs, (REAL)0, -lim, lim);
+        }
+        const double th_old = (double)theta[c];
+        double th = th_old + rates[3] * dt;
+        if (repairs && !isfinite(th))
+            th = isfinite(th_old) ? th_old : (theta0_base ? theta0_base[c % plane] : theta_ref);
+        theta[c] = sgs_sanitize((REAL)th, repairs, (REAL)(float)theta_ref, (REAL)theta_lo, (REAL)theta_hi);
+        if (qv)
+        {
+            double rq = (double)dqvdt[c];
+            if (repairs && !isfinite(rq)) rq = 0.0;
+            double q = (double)qv[c] + rq * dt;
+            if (repairs && !isfinite(q)) q = 0.0;
+            qv[c] = sgs_sanitize((REAL)q, repairs, (REAL)0, (REAL)0, (REAL)qv_hi);
+        }
+        if (tke)
+        {
+            const double old = (double)tke[c];
+            double a = (double)dtkedt[c], b = (double)dtke_pbl[c];
+            if (repairs && !isfinite(a)) a = 0.0;
+            if (repairs && !isfinite(b)) b = 0.0;
+            double t = old + (a + b) * dt;
+            if (repairs && !isfinite(t)) t = isfinite(old) ? old : 0.0;
+            tke[c] = (REAL)(repairs ? (t < 0.0 ? 0.0 : t) : t);
+        }
+    }
+}
+
+/* Compensated (Neumaier) sum of the reference's deterministic reductions
+ * (CompensatedSum, include/diagnostics/deterministic_reduction.hpp:28-53). */
+typedef struct
+{
+    double sum, corr;
+} sgs_csum;
+
+static void sgs_csum_add(sgs_csum* s, double x)
+{
+    const double next = s->sum + x;
+    if (fabs(s->sum) >= fabs(x))
+        s->corr += (s->sum - next) + x;
+    else
+        s->corr += (x - next) + s->sum;
+    s->sum = next;
+}
+
+/* Explicit stability limit of one SGS substep (compute_sgs_explicit_stability,
+ * src/core/orchestration/dynamics/sgs_apply.cpp:1483-1973) on a flat C-grid
+ * whose lateral faces are periodic or closed and whose lid carries no open
+ * stress, with the reference's deterministic reductions: each x-slab i of the
+ * physical cells sums its momentum power (mass u du/dt, per face, in j-k
+ * order) and acceleration norm serially, the slabs merge in increasing i with
+ * the compensated sum; theta / qv extrema and their monotonic limits are
+ * exact min / max reductions.  Limits carry the 0.9 safety factor.
+ * dz: per-level thickness (uniform grids: the reference's scalar dz).
+ * out: maximum, momentum-energy, theta-monotonic, qv-monotonic timesteps and
+ * the irreversible dissipation power.  Returns -2 for an invalid state (the
+ * reference's invalid_argument), -4 for a non-dissipative tendency or a
+ * non-positive limit (its runtime_error), else 0. */
+int oracle_sgs_stability(int nx, int ny, int nz, const REAL* u, const REAL* v, const REAL* w, const REAL* theta,
+                         const REAL* qv, const REAL* rho, const REAL* dudt, const REAL* dvdt, const REAL* dwdt,
+                         const REAL* dthdt, const REAL* dqvdt, double dx, double dy, const double* dz, int wrap_x,
+                         int wrap_y, double* out)
+{
+    const sgs_grid gg = {nx, ny, nz, 1, 1, wrap_x, wrap_y, dx, dy, dz};
+    const sgs_grid* G = &gg;
+    for (int i = 1; i < nx - 1; ++i)
+        for (int j = 1; j < ny - 1; ++j)
+            for (int k = 0; k < nz; ++k)
+            {
+                const size_t c = SIDX(i, j, k);
+                const double vals[9] = {rho[c], u[c], v[c], w[c], theta[c], dudt[c], dvdt[c], dwdt[c], dthdt[c]};
+                for (int q = 0; q < 9; ++q)
+                    if (!isfinite(vals[q])) return -2;
+                if (vals[0] <= 0.0 || vals[4] <= 0.0) return -2;
+                if (qv && (!isfinite(qv[c]) || qv[c] < 0 || !isfinite(dqvdt[c]))) return -2;
+            }
+    const double area = dx * dy;
+    sgs_csum power = {0.0, 0.0}, norm = {0.0, 0.0};
+    double th_lo = INFINITY, th_hi = -INFINITY, q_lo = INFINITY, q_hi = -INFINITY;
+    for (int i = 1; i < nx - 1; ++i)
+    {
+        double p = 0.0, a = 0.0, slo = INFINITY, shi = -INFINITY, qlo = INFINITY, qhi = -INFINITY;
+        for (int j = 1; j < ny - 1; ++j)
+            for (int k = 0; k < nz; ++k)
+            {
+                if (k < nz - 1)
+                {
+                    const double vol = area * dz[k];
+                    if (wrap_x || i <= nx - 3)
+                    {
+                        const int i1 = wrap_x && i >= nx - 2 ? 1 : i + 1;
+                        const double m = 0.5 * ((double)rho[SIDX(i, j, k)] * vol + (double)rho[SIDX(i1, j, k)] * vol);
+                        const double acc = (double)dudt[SIDX(i, j, k)];
+                        p += m * (double)u[SIDX(i, j, k)] * acc;
+                        a += m * acc * acc;
+                    }
+                    if (wrap_y || j < ny - 2)
+                    {
+                        const int j1 = wrap_y && j >= ny - 2 ? 1 : j + 1;
+                        const double m = 0.5 * ((double)rho[SIDX(i, j, k)] * vol + (double)rho[SIDX(i, j1, k)] * vol);
+                        const double acc = (double)dvdt[SIDX(i, j, k)];
+                        p += m * (double)v[SIDX(i, j, k)] * acc;
+                        a += m * acc * acc;
+                    }
+                    const double m = 0.5 * ((double)rho[SIDX(i, j, k)] * vol +
+                                            (double)rho[SIDX(i, j, k + 1)] * (area * dz[k + 1]));
+                    const double acc = (double)dwdt[SIDX(i, j, k)];
+                    p += m * (double)w[SIDX(i, j, k)] * acc;
+                    a += m * acc * acc;
+                }
+                const double th = (double)theta[SIDX(i, j, k)];
+                slo = th < slo ? th : slo;
+                shi = shi < th ? th : shi;
+                if (qv)
+                {
+                    const double q = (double)qv[SIDX(i, j, k)];
+                    qlo = q < qlo ? q : qlo;
+                    qhi = qhi < q ? q : qhi;
+                }
+            }
+        sgs_csum_add(&power, p);
+        sgs_csum_add(&norm, a);
+        th_lo = slo < th_lo ? slo : th_lo;
+        th_hi = th_hi < shi ? shi : th_hi;
+        q_lo = qlo < q_lo ? qlo : q_lo;
+        q_hi = q_hi < qhi ? qhi : q_hi;
+    }
+    const double linear = power.sum + power.corr, anorm = norm.sum + norm.corr;
+    if (!isfinite(linear) || !isfinite(anorm) || anorm < 0.0) return -4;
+    double mom = INFINITY, dissipation = 0.0;
+    if (anorm > 0.0)
+    {
+        if (!(linear < 0.0)) return -4;
+        dissipation = -linear;
+        mom = 0.9 * (-2.0 * linear / anorm);
+    }
+    double tl = INFINITY, ql = INFINITY;
+    for (int i = 1; i < nx - 1; ++i)
+        for (int j = 1; j < ny - 1; ++j)
+            for (int k = 0; k < nz; ++k)
+            {
+                const size_t c = SIDX(i, j, k);
+                const double th = theta[c], r = dthdt[c];
+                double x;
+                if (r > 0.0)
+                {
+                    x = (th_hi - th) / r;
+                    tl = x < tl ? x : tl;
+                }
+                else if (r < 0.0)
+                {
+                    x = (th - th_lo) / -r;
+                    tl = x < tl ? x : tl;
+                }
+                if (qv)
+                {
+                    const double q = qv[c], rq = dqvdt[c];
+                    if (rq > 0.0)
+                    {
+                        x = (q_hi - q) / rq;
+                        ql = x < ql ? x : ql;
+                    }
+                    else if (rq < 0.0)
+                    {
+                        x = (q - q_lo) / -rq;
+                        ql = x < ql ? x : ql;
+                    }
+                }
+            }
+    double lim[2] = {tl, ql};
+    for (int q = 0; q < 2; ++q)
+    {
+        if (isinf(lim[q]) || lim[q] >= 0.5 * DBL_MAX)
+            lim[q] = INFINITY;
+        else if (!isfinite(lim[q]) || lim[q] <= 0.0)
+            return -4;
+        else
+            lim[q] = 0.9 * lim[q];
+    }
+    double best = mom;
+    if (lim[0] < best) best = lim[0];
+    if (lim[1] < best) best = lim[1];
+    if (!(best > 0.0)) return -4;
+    out[0] = best;
+    out[1] = mom;
+    out[2] = lim[0];
+    out[3] = lim[1];
+    out[4] = dissipation;
+    return 0;
+}

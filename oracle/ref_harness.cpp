@@ -34,6 +34,14 @@
 //                           output staging of the history and live export
 //                           (headless_runtime.cpp:2577-2601)
 //   ref_npy_write_3d        npy::write_3d (src/core/output/npy_writer.cpp:143-156)
+//   ref_smagorinsky         SmagorinskyScheme::compute on the flat C-grid CPU path
+//                           (src/turbulence/schemes/smagorinsky/smagorinsky.cpp:96-440:
+//                           eddy coefficients, then compute_momentum_diffusion_tendencies
+//                           and compute_scalar_diffusion_tendencies,
+//                           src/turbulence/base/eddy_viscosity.cpp:1532-2090)
+//   ref_sgs_apply           apply_admitted_sgs_substep, CPU path
+//                           (src/core/orchestration/dynamics/sgs_apply.cpp:436-956,1975-2029)
+//   ref_sgs_stability       compute_sgs_explicit_stability (sgs_apply.cpp:1483-1973)
 //   ref_scalar_transport    advect_scalars_conservative_3d_cartesian
 //                           (advection_cartesian.cpp:3532) on a retained context whose
 //                           face mass fluxes and beginning density are supplied
@@ -59,6 +67,11 @@
 #include "core/infra/rayleigh_damping.hpp"
 #include "core/output/npy_writer.hpp"
 #include "core/output/stagger_interpolation.hpp"
+#include "core/orchestration/dynamics/sgs_apply.hpp"
+#include "core/orchestration/dynamics/sgs_apply_internal.hpp"
+#include "compute/backend_runtime.hpp"
+#include "diagnostics/deterministic_reduction.hpp"
+#include "turbulence/schemes/smagorinsky/smagorinsky.hpp"
 
 #include <cstring>
 #include <exception>
@@ -596,6 +609,198 @@ int ref_cell_centre(const float* u, const float* v, const float* w, float* uc, f
 int ref_npy_write_3d(const float* data, int dim0, int dim1, int dim2, const char* path)
 {
     return npy::write_3d(data, dim0, dim1, dim2, std::string(path)) ? 0 : fail("npy::write_3d failed");
+}
+
+namespace
+{
+const char* const kSgsModes[3] = {"3d", "horizontal_only", "vertical_only"};
+}
+
+// The Smagorinsky producer on host arrays: mode 0 3d, 1 horizontal_only,
+// 2 vertical_only; filter 0 cubic_root, 1 dx; open: W, E, S, N.  qv may be
+// null.  Outputs: the coefficients (from the scheme's diagnostics) and the
+// five tendencies.
+int ref_smagorinsky(const float* u, const float* v, const float* w, const float* theta, const float* qv,
+                    const float* rho, const double* dz, int nx, int ny, int nz, double dx, double dy, int mode,
+                    int filter, int periodic_x, int periodic_y, const int* open, double Cs, double Pr_t, double Sc_t,
+                    double nu_max, double K_max, float* nu_t, float* K_theta, float* K_q, float* dudt, float* dvdt,
+                    float* dwdt, float* dthdt, float* dqvdt)
+{
+    try
+    {
+        Field3D fu, fv, fw, fth, fqv, frho;
+        to_field(fu, u, nx, ny, nz);
+        to_field(fv, v, nx, ny, nz);
+        to_field(fw, w, nx, ny, nz);
+        to_field(fth, theta, nx, ny, nz);
+        to_field(frho, rho, nx, ny, nz);
+        if (qv) to_field(fqv, qv, nx, ny, nz);
+        std::vector<double> rho0(static_cast<std::size_t>(nz), 1.0);
+        TurbulenceStateView sv;
+        sv.u = &fu;
+        sv.v = &fv;
+        sv.w = &fw;
+        sv.theta = &fth;
+        sv.rho = &frho;
+        sv.qv = qv ? &fqv : nullptr;
+        sv.rho0 = &rho0;
+        sv.c_grid = true;
+        sv.NR = nx;
+        sv.NTH = ny;
+        sv.NZ = nz;
+        sv.periodic_x = periodic_x != 0;
+        sv.periodic_y = periodic_y != 0;
+        sv.open_lateral = {open[0] != 0, open[1] != 0, open[2] != 0, open[3] != 0};
+        GridMetrics g;
+        g.dx = dx;
+        g.dy = dy;
+        g.dz.assign(dz, dz + nz);
+        TurbulenceConfig cfg;
+        cfg.mode = kSgsModes[mode];
+        cfg.filter_width = filter ? "dx" : "cubic_root";
+        cfg.Cs = Cs;
+        cfg.Pr_t = Pr_t;
+        cfg.Sc_t = Sc_t;
+        cfg.nu_t_max = nu_max;
+        cfg.K_max = K_max;
+        SmagorinskyScheme scheme;
+        scheme.initialize(cfg);
+        TurbulenceTendencies t;
+        TurbulenceDiagnostics d;
+        scheme.compute(cfg, g, sv, t, &d);
+        from_field(nu_t, d.nu_t);
+        from_field(K_theta, d.K_theta);
+        from_field(K_q, d.K_q);
+        from_field(dudt, t.dudt_sgs);
+        from_field(dvdt, t.dvdt_sgs);
+        from_field(dwdt, t.dwdt_sgs);
+        from_field(dthdt, t.dthetadt_sgs);
+        if (qv)
+            from_field(dqvdt, t.dqvdt_sgs);
+        else
+            std::memset(dqvdt, 0, sizeof(float) * static_cast<std::size_t>(nx) * ny * nz);
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        return fail(e.what());
+    }
+}
+
+namespace
+{
+// A level with the turbulence and compute runtimes the SGS apply and
+// stability code expect (CPU kind, no scheme: no work ledger).
+struct SgsLevel
+{
+    Level L;
+    ComputeBackendRuntimeState compute;
+    tmv::TurbulenceRuntimeState turbulence;
+    TurbulenceTendencies tend;
+    SgsLevel(int nx, int ny, int nz, double dx, double dy, double dz, double dt) : L(nx, ny, nz, dx, dy, dz, dt)
+    {
+        L.view.compute_runtime = &compute;
+        L.view.turbulence_runtime = &turbulence;
+    }
+    void load(const float* const rates[6], int nx, int ny, int nz)
+    {
+        Field3D* out[6] = {&tend.dudt_sgs, &tend.dvdt_sgs, &tend.dwdt_sgs, &tend.dthetadt_sgs, &tend.dqvdt_sgs,
+                           &tend.dtkedt_sgs};
+        for (int f = 0; f < 6; ++f)
+        {
+            if (rates[f])
+                to_field(*out[f], rates[f], nx, ny, nz);
+            else
+                out[f]->resize(nx, ny, nz, 0.0f);
+        }
+    }
+};
+}  // namespace
+
+// apply_admitted_sgs_substep on host arrays in place (u, v, w, theta, qv; qv
+// may be null, which leaves the level without moisture); repairs sets the
+// writer repair policy for the call.
+int ref_sgs_apply(float* u, float* v, float* w, float* theta, float* qv, const float* dudt, const float* dvdt,
+                  const float* dwdt, const float* dthdt, const float* dqvdt, const double* theta0, int nx, int ny,
+                  int nz, double dt, int repairs)
+{
+    const bool saved = primary_state_repairs_enabled;
+    try
+    {
+        SgsLevel S(nx, ny, nz, 1000.0, 1000.0, 500.0, dt);
+        auto& f = S.L.storage.fields;
+        to_field(f.u, u, nx, ny, nz);
+        to_field(f.v, v, nx, ny, nz);
+        to_field(f.w, w, nx, ny, nz);
+        to_field(f.theta, theta, nx, ny, nz);
+        if (qv)
+            to_field(f.qv, qv, nx, ny, nz);
+        else
+            f.qv = Field3D();
+        f.tke = Field3D();
+        if (theta0) S.L.storage.base.theta0.assign(theta0, theta0 + nz);
+        const float* rates[6] = {dudt, dvdt, dwdt, dthdt, dqvdt, nullptr};
+        S.load(rates, nx, ny, nz);
+        set_primary_state_repairs_enabled(repairs != 0);
+        apply_admitted_sgs_substep(S.L.view, dt, S.tend);
+        set_primary_state_repairs_enabled(saved);
+        from_field(u, f.u);
+        from_field(v, f.v);
+        from_field(w, f.w);
+        from_field(theta, f.theta);
+        if (qv) from_field(qv, f.qv);
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        set_primary_state_repairs_enabled(saved);
+        return fail(e.what());
+    }
+}
+
+// compute_sgs_explicit_stability with the reference's deterministic
+// (thread-count independent) reductions.  bc: W, E, S, N, bottom, top codes.
+// out: maximum, momentum-energy, theta-monotonic and qv-monotonic timesteps,
+// then the irreversible dissipation power.
+int ref_sgs_stability(const float* u, const float* v, const float* w, const float* theta, const float* qv,
+                      const float* rho, const float* dudt, const float* dvdt, const float* dwdt, const float* dthdt,
+                      const float* dqvdt, int nx, int ny, int nz, double dx, double dy, double dz, const int* bc,
+                      int mode, double* out)
+{
+    const bool saved = tmv::diagnostics::deterministic_reductions_enabled();
+    try
+    {
+        SgsLevel S(nx, ny, nz, dx, dy, dz, 1.0);
+        S.L.set_bcs(bc[0], bc[1], bc[2], bc[3], bc[4], bc[5]);
+        S.turbulence.config.mode = kSgsModes[mode];
+        auto& f = S.L.storage.fields;
+        to_field(f.u, u, nx, ny, nz);
+        to_field(f.v, v, nx, ny, nz);
+        to_field(f.w, w, nx, ny, nz);
+        to_field(f.theta, theta, nx, ny, nz);
+        to_field(f.rho, rho, nx, ny, nz);
+        if (qv)
+            to_field(f.qv, qv, nx, ny, nz);
+        else
+            f.qv = Field3D();
+        f.tke = Field3D();
+        const float* rates[6] = {dudt, dvdt, dwdt, dthdt, dqvdt, nullptr};
+        S.load(rates, nx, ny, nz);
+        tmv::diagnostics::set_deterministic_reductions(true);
+        const SgsExplicitStability r = compute_sgs_explicit_stability(S.L.view, S.tend);
+        tmv::diagnostics::set_deterministic_reductions(saved);
+        out[0] = r.maximum_timestep_s;
+        out[1] = r.momentum_energy_timestep_s;
+        out[2] = r.theta_monotonic_timestep_s;
+        out[3] = r.qv_monotonic_timestep_s;
+        out[4] = r.momentum_irreversible_dissipation_w;
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        tmv::diagnostics::set_deterministic_reductions(saved);
+        return fail(e.what());
+    }
 }
 
 } // extern "C"
