@@ -151,7 +151,8 @@ enum
     NIMBUS_KERNEL_SLOW = 6,               /* slow tendencies (k1+predictor, k2+apply) */
     NIMBUS_KERNEL_MICROPHYSICS = 7,       /* Kessler, the EOS re-projection and the end-of-step sponge */
     NIMBUS_KERNEL_OUTPUT = 8,             /* cell-centre velocities for output */
-    NIMBUS_KERNEL_FAMILIES = 9
+    NIMBUS_KERNEL_SGS = 9,                /* Smagorinsky closure, SGS apply and stability */
+    NIMBUS_KERNEL_FAMILIES = 10
 };
 /* When enabled, every launch is bracketed by CUDA events on its own stream
  * and nimbus_cuda_kernel_timing() returns, per family, the launch count and
@@ -511,6 +512,121 @@ typedef struct nimbus_boundary_args
 } nimbus_boundary_args;
 
 nimbus_status nimbus_cuda_acoustic_boundaries(nimbus_cuda_context* ctx, const nimbus_boundary_args* a);
+
+/*
+ * Smagorinsky SGS closure on a flat C-grid (stability correction "none"),
+ * the operations of TurbulenceComputeKernels
+ * (include/compute/dispatch/turbulence.hpp:100-195,200-285) with the CPU
+ * solver's arithmetic: FP64 over FP32 storage in the reference's order, so
+ * every output is bit-identical to SmagorinskyScheme::compute and
+ * apply_sgs_tendencies_cpu.  The flat filter width is formed per level on
+ * the host (sqrt(dx dy) or cbrt(dx dy dz_k), the C library's functions, as
+ * compute_filter_width calls them, eddy_viscosity.cpp:1414-1468).
+ *
+ * nimbus_cuda_smagorinsky_fused replaces dispatch_smagorinsky_fused: eddy
+ * coefficients of every cell (nu = Cs^2 Delta^2 |S| capped at nu_t_max;
+ * K_theta = nu / Pr_t, K_q = nu / Sc_t capped at K_max), then the
+ * live-density stress divergence for u, v, w and the flux-form diffusion of
+ * theta and qv (zero flux at the ground and lid; a lateral face that is
+ * neither periodic nor open reflects).  nu_t / K_theta / K_q may be NULL
+ * (kept in device scratch); dqvdt_sgs is zero-filled when qv is NULL.  A
+ * state outside the reference's contract (u, v, w finite; theta, rho finite
+ * and positive; qv finite and non-negative) or a non-finite coefficient:
+ * NIMBUS_ERR_INVALID_ARGUMENT with host outputs untouched (host memory), or
+ * reported by nimbus_cuda_synchronize (device memory).
+ */
+typedef struct nimbus_smagorinsky_args
+{
+    const float *u, *v, *w, *theta, *qv, *rho;  /* [nx][ny][nz]; qv may be NULL */
+    const double* dz;          /* [nz] cell thickness (host memory, FP64) */
+    int nx, ny, nz;            /* >= 3, 3, 2 */
+    int filter_mode;           /* 0 cubic root of the cell volume, 1 sqrt(dx dy) */
+    int use_horizontal, use_vertical;  /* mode: both "3d", one of them horizontal_only / vertical_only */
+    int periodic_x, periodic_y;
+    int open_lateral[4];       /* W, E, S, N: radiative or zero-gradient face */
+    int open_top;              /* open lid (stability only) */
+    double dx, dy, Cs, Pr_t, Sc_t, nu_t_max, K_max;
+    float *nu_t, *K_theta, *K_q;  /* outputs, may be NULL */
+    float *dudt_sgs, *dvdt_sgs, *dwdt_sgs, *dthetadt_sgs, *dqvdt_sgs;  /* outputs (inputs of the stability call) */
+    int memory;
+    void* stream;
+} nimbus_smagorinsky_args;
+
+nimbus_status nimbus_cuda_smagorinsky_fused(nimbus_cuda_context* ctx, const nimbus_smagorinsky_args* a);
+
+/*
+ * SGS tendency application, replacing dispatch_sgs_apply (SgsApplyDispatch,
+ * turbulence.hpp:62-98) with the CPU semantics of apply_sgs_tendencies_cpu
+ * (src/core/orchestration/dynamics/sgs_apply.cpp:436-956, without the energy
+ * ledger): every cell, x += dt dx/dt formed in FP64, rounded to FP32 and
+ * clamped (u, v to +-wind_h_max, w to +-wind_v_max, theta to [theta_min,
+ * theta_max], qv to [0, qv_max]).  sanitize = primary_state_repairs_enabled:
+ * non-finite tendencies count as zero, a non-finite sum falls back (winds and
+ * qv to 0, theta to its old value, else theta0_base[k], else
+ * theta_reference), tke stays non-negative.  qv and tke (with dtkedt and
+ * dtkedt_pbl) may be NULL.  dt must be finite and positive.
+ */
+typedef struct nimbus_sgs_apply_args
+{
+    float *u, *v, *w, *theta, *qv, *tke;
+    const float *dudt, *dvdt, *dwdt, *dthetadt, *dqvdt, *dtkedt, *dtkedt_pbl;
+    const double* theta0_base;  /* [nz] host memory, may be NULL */
+    int nx, ny, nz;
+    double dt;
+    int sanitize;
+    double theta_reference;     /* 300 K in the reference (theta0) */
+    float theta_min, theta_max, qv_max, wind_h_max, wind_v_max;  /* 200, 700, 0.05, 180, 120 */
+    int memory;
+    void* stream;
+} nimbus_sgs_apply_args;
+
+nimbus_status nimbus_cuda_sgs_apply(nimbus_cuda_context* ctx, const nimbus_sgs_apply_args* a);
+
+/*
+ * Explicit stability limit of the realized SGS tendencies
+ * (compute_sgs_explicit_stability, sgs_apply.cpp:1483-1973) with the
+ * reference's deterministic reductions (each x-slab summed serially in j-k
+ * order, slabs merged in increasing i with its compensated sum): the same
+ * binary64 results.  Reads the state and the five rates of `a`.  Lateral
+ * faces must be periodic or closed and the lid closed to shear stress (an
+ * open one needs the realized boundary-power term): NIMBUS_ERR_UNSUPPORTED
+ * otherwise.  NIMBUS_ERR_INVALID_ARGUMENT for a state the reference rejects,
+ * NIMBUS_ERR_NONFINITE for a non-dissipative tendency or no positive limit.
+ * Synchronous.
+ */
+typedef struct nimbus_sgs_stability
+{
+    double maximum_timestep_s;
+    double momentum_energy_timestep_s;
+    double theta_monotonic_timestep_s;
+    double qv_monotonic_timestep_s;
+    double momentum_irreversible_dissipation_w;
+} nimbus_sgs_stability;
+
+nimbus_status nimbus_cuda_sgs_stability(nimbus_cuda_context* ctx, const nimbus_smagorinsky_args* a,
+                                        nimbus_sgs_stability* out);
+
+/*
+ * The explicit SGS integration of one large step (dynamics.cpp:7159-7217):
+ * until dt is covered, refresh the closure from the live state
+ * (nimbus_cuda_smagorinsky_fused), bound the substep by the stability limit
+ * and dt_sgs, and apply it (nimbus_cuda_sgs_apply).  Device memory; u, v, w,
+ * theta, qv updated in place; the rate and coefficient pointers of `closure`
+ * may be NULL (device scratch).  One host synchronisation per substep (the
+ * limit decides its length).  time_s: the model time at the start (enters
+ * the reference's progress floor).  substeps / stability_limit_s (may be
+ * NULL) receive the substep count and the smallest limit seen.
+ */
+typedef struct nimbus_sgs_step_args
+{
+    nimbus_smagorinsky_args closure;  /* memory must be NIMBUS_MEMORY_DEVICE */
+    const double* theta0_base;        /* [nz] host memory, may be NULL */
+    double dt, dt_sgs, time_s;
+    int sanitize;
+} nimbus_sgs_step_args;
+
+nimbus_status nimbus_cuda_sgs_step(nimbus_cuda_context* ctx, const nimbus_sgs_step_args* a, int* substeps,
+                                   double* stability_limit_s);
 
 /*
  * Cell-centre velocities for output.  Replaces interpolate_u_face_to_center,

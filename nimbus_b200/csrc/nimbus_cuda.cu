@@ -693,6 +693,9 @@ nimbus_status nimbus_cuda_synchronize(nimbus_cuda_context* ctx)
     if (flags & kStatusNonfiniteMassFlux) return fail(ctx, NIMBUS_ERR_NONFINITE, "non-finite retained face mass flux");
     if (flags & kStatusNonfiniteTransport) return fail(ctx, NIMBUS_ERR_NONFINITE, "non-finite transported scalar");
     if (flags & kStatusInvalidEos) return fail(ctx, NIMBUS_ERR_NONFINITE, "EOS projection met an invalid state");
+    if (flags & kStatusSgsInvalid)
+        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT,
+                    "SGS closure met a state outside its contract or a non-finite coefficient");
     return NIMBUS_OK;
 }
 

@@ -1,0 +1,616 @@
+// Smagorinsky SGS closure on a flat C-grid (stability correction "none"):
+// eddy coefficients, conservative live-density stress and scalar diffusion
+// tendencies, the forward-Euler application and the explicit stability
+// reductions.  Reference: SmagorinskyScheme::compute_eddy_coefficients
+// (src/turbulence/schemes/smagorinsky/smagorinsky.cpp:494-571),
+// compute_directional_strain_sq_centered, compute_momentum_diffusion_tendencies
+// and compute_scalar_diffusion_tendencies
+// (src/turbulence/base/eddy_viscosity.cpp:1253-1400,1532-2090),
+// apply_sgs_tendencies_cpu and compute_sgs_explicit_stability
+// (src/core/orchestration/dynamics/sgs_apply.cpp:436-956,1483-1973).
+//
+// FP64 arithmetic over FP32 storage in the reference's operation order
+// (compiled without FMA contraction): bit-identical to the CPU solver.  Every
+// stress or flux the reference carries along a column (its rolling lower
+// T13 / T23 / T33) is recomputed here from the same expression, which gives
+// the same binary64 value, so each cell is independent: one thread per cell.
+#pragma once
+
+#include "stencil_common.cuh"
+
+namespace nimbus
+{
+
+struct SgsParams
+{
+    Dims d;
+    double dx, dy;
+    const double* dz;     // [nz] cell thickness (device)
+    const double* delta;  // [nz] filter width (device, formed on the host)
+    int use_h, use_v;
+    int px, py;           // periodic x / y
+    int open[4];          // W, E, S, N lateral faces open (scalar fluxes pass)
+    double Cs, Pr_t, Sc_t, nu_max, K_max;
+};
+
+// Neighbour rows (eddy_viscosity.cpp:69-105): clamped to the allocated
+// range, or on a periodic axis wrapped over the physical rows 1..n-2.
+__device__ __forceinline__ int sgs_prev(int i, int n, int periodic)
+{
+    if (!periodic) return i > 0 ? i - 1 : 0;
+    return i <= 1 ? n - 2 : (i - 1 < n - 2 ? i - 1 : n - 2);
+}
+
+__device__ __forceinline__ int sgs_next(int i, int n, int periodic)
+{
+    if (!periodic) return i + 1 < n - 1 ? i + 1 : n - 1;
+    return i >= n - 2 ? 1 : (i + 1 > 1 ? i + 1 : 1);
+}
+
+struct SgsAt
+{
+    const SgsParams& P;
+    __device__ __forceinline__ int at(int i, int j, int k) const { return P.d.at(i, j, k); }
+    __device__ __forceinline__ double f(const float* x, int i, int j, int k) const
+    {
+        return (double)__ldg(x + at(i, j, k));
+    }
+    // w with the implicit ground face w[-1] = 0.
+    __device__ __forceinline__ double wf(const float* w, int i, int j, int k) const
+    {
+        return k < 0 ? 0.0 : f(w, i, j, k);
+    }
+    __device__ __forceinline__ double dzc(int k) const { return 0.5 * (P.dz[k] + P.dz[k + 1]); }
+    // mu = rho nu at a centre; on an xy edge (four-point mean); on an xz or yz
+    // edge (pair means of the two levels, weighted by the other level's
+    // thickness).
+    __device__ __forceinline__ double mu(const float* rho, const float* nu, int i, int j, int k) const
+    {
+        return f(rho, i, j, k) * f(nu, i, j, k);
+    }
+    __device__ __forceinline__ double mu_xy(const float* rho, const float* nu, int i, int j, int k) const
+    {
+        const int i1 = sgs_next(i, P.d.nx, P.px), j1 = sgs_next(j, P.d.ny, P.py);
+        return 0.25 * (mu(rho, nu, i, j, k) + mu(rho, nu, i1, j, k) + mu(rho, nu, i, j1, k) + mu(rho, nu, i1, j1, k));
+    }
+    __device__ __forceinline__ double mu_z(const float* rho, const float* nu, int i, int j, int i1, int j1,
+                                           int k) const
+    {
+        const double lo = 0.5 * (mu(rho, nu, i, j, k) + mu(rho, nu, i1, j1, k));
+        const double up = 0.5 * (mu(rho, nu, i, j, k + 1) + mu(rho, nu, i1, j1, k + 1));
+        return (P.dz[k + 1] * lo + P.dz[k] * up) / (P.dz[k] + P.dz[k + 1]);
+    }
+};
+
+// Strain-rate square at a scalar centre (compute_directional_strain_sq_centered).
+__device__ double sgs_strain_sq(const SgsParams& P, const float* u, const float* v, const float* w, int i, int j,
+                                int k)
+{
+    const SgsAt A{P};
+    const int nx = P.d.nx, ny = P.d.ny, nz = P.d.nz;
+    const int jm = sgs_prev(j, ny, P.py), im = sgs_prev(i, nx, P.px);
+    const double s11 = (A.f(u, i, j, k) - A.f(u, im, j, k)) / P.dx;
+    const double s22 = (A.f(v, i, j, k) - A.f(v, i, jm, k)) / P.dy;
+    const double s33 = (A.wf(w, i, j, k) - A.wf(w, i, j, k - 1)) / P.dz[k];
+    double s12[4];
+    {
+        const int ie[4] = {im, im, i, i}, je[4] = {jm, j, jm, j};
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+        {
+            const int ii = ie[e], jj = je[e];
+            const int jj1 = sgs_next(jj, ny, P.py), ii1 = sgs_next(ii, nx, P.px);
+            const double dudy = (A.f(u, ii, jj1, k) - A.f(u, ii, jj, k)) / P.dy;
+            const double dvdx = (A.f(v, ii1, jj, k) - A.f(v, ii, jj, k)) / P.dx;
+            s12[e] = 0.5 * (dudy + dvdx);
+        }
+    }
+    double xz0[4], xz1[4], yz0[4], yz1[4];
+    {
+        const int xi[4] = {im, im, i, i}, yj[4] = {jm, jm, j, j}, ke[4] = {k - 1, k, k - 1, k};
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+        {
+            const int kk = ke[e];
+            if (kk < 0 || kk >= nz - 1)
+            {
+                xz0[e] = xz1[e] = yz0[e] = yz1[e] = 0.0;
+                continue;
+            }
+            const double dzc = A.dzc(kk);
+            const int ii = xi[e], ii1 = sgs_next(ii, nx, P.px);
+            xz0[e] = (A.f(u, ii, j, kk + 1) - A.f(u, ii, j, kk)) / dzc;
+            xz1[e] = (A.wf(w, ii1, j, kk) - A.wf(w, ii, j, kk)) / P.dx;
+            const int jj = yj[e], jj1 = sgs_next(jj, ny, P.py);
+            yz0[e] = (A.f(v, i, jj, kk + 1) - A.f(v, i, jj, kk)) / dzc;
+            yz1[e] = (A.wf(w, i, jj1, kk) - A.wf(w, i, jj, kk)) / P.dy;
+        }
+    }
+    const double s12_sq = 0.25 * (s12[0] * s12[0] + s12[1] * s12[1] + s12[2] * s12[2] + s12[3] * s12[3]);
+    auto avg_sq = [](const double (&g)[4]) { return 0.25 * (g[0] * g[0] + g[1] * g[1] + g[2] * g[2] + g[3] * g[3]); };
+    if (P.use_h && !P.use_v) return 2.0 * (s11 * s11 + s22 * s22) + 4.0 * s12_sq + avg_sq(xz1) + avg_sq(yz1);
+    if (P.use_v && !P.use_h) return avg_sq(xz0) + avg_sq(yz0) + 2.0 * s33 * s33;
+    double sxz[4], syz[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e)
+    {
+        const double a = 0.5 * (xz0[e] + xz1[e]);
+        const double b = 0.5 * (yz0[e] + yz1[e]);
+        sxz[e] = a * a;
+        syz[e] = b * b;
+    }
+    const double s13_sq = 0.25 * (sxz[0] + sxz[1] + sxz[2] + sxz[3]);
+    const double s23_sq = 0.25 * (syz[0] + syz[1] + syz[2] + syz[3]);
+    return 2.0 * (s11 * s11 + s22 * s22 + s33 * s33) + 4.0 * (s12_sq + s13_sq + s23_sq);
+}
+
+__device__ __forceinline__ double sgs_min(double a, double b) { return b < a ? b : a; }  // std::min
+
+// Eddy coefficients of every cell; a cell whose inputs break the reference's
+// field contract (validate_scheme_inputs, eddy_viscosity.cpp:1088-1175) or
+// whose coefficient is not finite raises kStatusSgsInvalid.
+__global__ void __launch_bounds__(256) sgs_coefficients_kernel(SgsParams P, const float* __restrict__ u,
+                                                               const float* __restrict__ v,
+                                                               const float* __restrict__ w,
+                                                               const float* __restrict__ theta,
+                                                               const float* __restrict__ qv,
+                                                               const float* __restrict__ rho, float* __restrict__ nu_t,
+                                                               float* __restrict__ K_theta, float* __restrict__ K_q,
+                                                               unsigned* status)
+{
+    const int n = P.d.cells();
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+    {
+        int i, j, k;
+        decompose(P.d, c, i, j, k);
+        const float th = theta[c], r = rho[c];
+        bool bad = !isfinite(u[c]) || !isfinite(v[c]) || !isfinite(w[c]) || !isfinite(th) || !(th > 0.0f) ||
+                   !isfinite(r) || !(r > 0.0f) || (qv && (!isfinite(qv[c]) || qv[c] < 0.0f));
+        const double strain = sqrt(sgs_strain_sq(P, u, v, w, i, j, k));
+        double nu = P.Cs * P.Cs * P.delta[k] * P.delta[k] * strain * 1.0;
+        bad |= !isfinite(strain) || !isfinite(nu);
+        nu = sgs_min(nu, P.nu_max);
+        const double kt = nu / P.Pr_t, kq = nu / P.Sc_t;
+        bad |= !isfinite(kt) || !isfinite(kq);
+        if (bad) atomicOr(status, kStatusSgsInvalid);
+        nu_t[c] = (float)nu;
+        K_theta[c] = (float)sgs_min(kt, P.K_max);
+        K_q[c] = (float)sgs_min(kq, P.K_max);
+    }
+}
+
+// Scalar diffusion tendency at one cell (compute_scalar_diffusion_tendencies).
+__device__ double sgs_scalar_rate(const SgsParams& P, const float* rho, const float* K, const float* phi, int i,
+                                  int j, int k)
+{
+    const SgsAt A{P};
+    const int nx = P.d.nx, ny = P.d.ny, nz = P.d.nz;
+    const int jmm = !P.py && !P.open[2] && j == 1 ? j : sgs_prev(j, ny, P.py);
+    const int jpp = !P.py && !P.open[3] && j == ny - 2 ? j : sgs_next(j, ny, P.py);
+    const int imm = !P.px && !P.open[0] && i == 1 ? i : sgs_prev(i, nx, P.px);
+    const int ipp = !P.px && !P.open[1] && i == nx - 2 ? i : sgs_next(i, nx, P.px);
+    auto tr = [&](int ii, int jj, int kk) { return A.f(rho, ii, jj, kk) * A.f(K, ii, jj, kk); };
+    double div = 0.0;
+    if (P.use_h)
+    {
+        const double ph = A.f(phi, i, j, k), tc = tr(i, j, k);
+        const double fe = 0.5 * (tc + tr(ipp, j, k)) * (A.f(phi, ipp, j, k) - ph) / P.dx;
+        const double fw = 0.5 * (tr(imm, j, k) + tc) * (ph - A.f(phi, imm, j, k)) / P.dx;
+        const double fn = 0.5 * (tc + tr(i, jpp, k)) * (A.f(phi, i, jpp, k) - ph) / P.dy;
+        const double fs = 0.5 * (tr(i, jmm, k) + tc) * (ph - A.f(phi, i, jmm, k)) / P.dy;
+        div += (fe - fw) / P.dx + (fn - fs) / P.dy;
+    }
+    if (P.use_v)
+    {
+        const double ft = k < nz - 1 ? 0.5 * (tr(i, j, k) + tr(i, j, k + 1)) *
+                                           (A.f(phi, i, j, k + 1) - A.f(phi, i, j, k)) / A.dzc(k)
+                                     : 0.0;
+        const double fb = k > 0 ? 0.5 * (tr(i, j, k - 1) + tr(i, j, k)) *
+                                      (A.f(phi, i, j, k) - A.f(phi, i, j, k - 1)) / A.dzc(k - 1)
+                                : 0.0;
+        div += (ft - fb) / P.dz[k];
+    }
+    return div / A.f(rho, i, j, k);
+}
+
+// du/dt at x-face (i, j, k) (compute_momentum_diffusion_tendencies, first loop).
+__device__ double sgs_du(const SgsParams& P, const float* u, const float* v, const float* w, const float* rho,
+                         const float* nu, int i, int j, int k)
+{
+    const SgsAt A{P};
+    const int nx = P.d.nx, ny = P.d.ny;
+    const int jmm = sgs_prev(j, ny, P.py), imm = sgs_prev(i, nx, P.px), ipp = sgs_next(i, nx, P.px);
+    double div = 0.0;
+    if (P.use_h)
+    {
+        const double s_r = (A.f(u, ipp, j, k) - A.f(u, i, j, k)) / P.dx;
+        const double s_l = (A.f(u, i, j, k) - A.f(u, imm, j, k)) / P.dx;
+        div += (2.0 * A.mu(rho, nu, ipp, j, k) * s_r - 2.0 * A.mu(rho, nu, i, j, k) * s_l) / P.dx;
+        double t12[2];
+        const int jes[2] = {j, jmm};
+#pragma unroll
+        for (int e = 0; e < 2; ++e)
+        {
+            const int je = jes[e], je1 = sgs_next(je, ny, P.py);
+            const double s12 =
+                0.5 * ((A.f(u, i, je1, k) - A.f(u, i, je, k)) / P.dy + (A.f(v, ipp, je, k) - A.f(v, i, je, k)) / P.dx);
+            t12[e] = 2.0 * A.mu_xy(rho, nu, i, je, k) * s12;
+        }
+        div += (t12[0] - t12[1]) / P.dy;
+    }
+    if (P.use_v)
+    {
+        // T13 on the z-faces k (upper) and k-1 (lower; zero at the ground).
+        double t13[2];
+#pragma unroll
+        for (int e = 0; e < 2; ++e)
+        {
+            const int ke = k - e;
+            if (ke < 0)
+            {
+                t13[e] = 0.0;
+                continue;
+            }
+            const double dudz = (A.f(u, i, j, ke + 1) - A.f(u, i, j, ke)) / A.dzc(ke);
+            const double grad = P.use_h ? dudz + (A.wf(w, ipp, j, ke) - A.wf(w, i, j, ke)) / P.dx : dudz;
+            t13[e] = A.mu_z(rho, nu, i, j, ipp, j, ke) * grad;
+        }
+        div += (t13[0] - t13[1]) / P.dz[k];
+    }
+    return div / (0.5 * (A.f(rho, i, j, k) + A.f(rho, ipp, j, k)));
+}
+
+// dv/dt at y-face (i, j, k) (second loop).
+__device__ double sgs_dv(const SgsParams& P, const float* u, const float* v, const float* w, const float* rho,
+                         const float* nu, int i, int j, int k)
+{
+    const SgsAt A{P};
+    const int nx = P.d.nx, ny = P.d.ny;
+    const int jmm = sgs_prev(j, ny, P.py), jpp = sgs_next(j, ny, P.py), imm = sgs_prev(i, nx, P.px);
+    double div = 0.0;
+    if (P.use_h)
+    {
+        const double s_n = (A.f(v, i, jpp, k) - A.f(v, i, j, k)) / P.dy;
+        const double s_s = (A.f(v, i, j, k) - A.f(v, i, jmm, k)) / P.dy;
+        div += (2.0 * A.mu(rho, nu, i, jpp, k) * s_n - 2.0 * A.mu(rho, nu, i, j, k) * s_s) / P.dy;
+        double t21[2];
+        const int ies[2] = {i, imm};
+#pragma unroll
+        for (int e = 0; e < 2; ++e)
+        {
+            const int ie = ies[e], ie1 = sgs_next(ie, nx, P.px);
+            const double s12 = 0.5 * ((A.f(u, ie, jpp, k) - A.f(u, ie, j, k)) / P.dy +
+                                      (A.f(v, ie1, j, k) - A.f(v, ie, j, k)) / P.dx);
+            t21[e] = 2.0 * A.mu_xy(rho, nu, ie, j, k) * s12;
+        }
+        div += (t21[0] - t21[1]) / P.dx;
+    }
+    if (P.use_v)
+    {
+        double t23[2];
+#pragma unroll
+        for (int e = 0; e < 2; ++e)
+        {
+            const int ke = k - e;
+            if (ke < 0)
+            {
+                t23[e] = 0.0;
+                continue;
+            }
+            const double dvdz = (A.f(v, i, j, ke + 1) - A.f(v, i, j, ke)) / A.dzc(ke);
+            const double grad = P.use_h ? dvdz + (A.wf(w, i, jpp, ke) - A.wf(w, i, j, ke)) / P.dy : dvdz;
+            t23[e] = A.mu_z(rho, nu, i, j, i, jpp, ke) * grad;
+        }
+        div += (t23[0] - t23[1]) / P.dz[k];
+    }
+    return div / (0.5 * (A.f(rho, i, j, k) + A.f(rho, i, jpp, k)));
+}
+
+// dw/dt at z-face (i, j, k) (third loop): stress divergence over the dual
+// column mass.
+__device__ double sgs_dw(const SgsParams& P, const float* u, const float* v, const float* w, const float* rho,
+                         const float* nu, int i, int j, int k)
+{
+    const SgsAt A{P};
+    const int nx = P.d.nx, ny = P.d.ny;
+    const int imm = sgs_prev(i, nx, P.px), jmm = sgs_prev(j, ny, P.py);
+    const double dzb = P.dz[k], dzt = P.dz[k + 1], dzd = A.dzc(k);
+    const double mass = 0.5 * (A.f(rho, i, j, k) * dzb + A.f(rho, i, j, k + 1) * dzt);
+    double force = 0.0;
+    if (P.use_v)
+    {
+        const double t33_t = 2.0 * A.mu(rho, nu, i, j, k + 1) * ((A.wf(w, i, j, k + 1) - A.wf(w, i, j, k)) / dzt);
+        const double t33_b = 2.0 * A.mu(rho, nu, i, j, k) * ((A.wf(w, i, j, k) - A.wf(w, i, j, k - 1)) / dzb);
+        force += t33_t - t33_b;
+    }
+    if (P.use_h)
+    {
+        double t31[2], t32[2];
+        const int ies[2] = {i, imm}, jes[2] = {j, jmm};
+#pragma unroll
+        for (int e = 0; e < 2; ++e)
+        {
+            const int ie = ies[e], ie1 = sgs_next(ie, nx, P.px);
+            const double dwdx = (A.wf(w, ie1, j, k) - A.wf(w, ie, j, k)) / P.dx;
+            const double gx = P.use_v ? (A.f(u, ie, j, k + 1) - A.f(u, ie, j, k)) / dzd + dwdx : dwdx;
+            t31[e] = A.mu_z(rho, nu, ie, j, ie1, j, k) * gx;
+            const int je = jes[e], je1 = sgs_next(je, ny, P.py);
+            const double dwdy = (A.wf(w, i, je1, k) - A.wf(w, i, je, k)) / P.dy;
+            const double gy = P.use_v ? (A.f(v, i, je, k + 1) - A.f(v, i, je, k)) / dzd + dwdy : dwdy;
+            t32[e] = A.mu_z(rho, nu, i, je, i, je1, k) * gy;
+        }
+        force += dzd * (t31[0] - t31[1]) / P.dx;
+        force += dzd * (t32[0] - t32[1]) / P.dy;
+    }
+    return force / mass;
+}
+
+// The five tendencies of every cell; zero where the reference leaves its
+// pre-cleared outputs untouched.
+__global__ void __launch_bounds__(256) sgs_tendencies_kernel(
+    SgsParams P, const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w,
+    const float* __restrict__ theta, const float* __restrict__ qv, const float* __restrict__ rho,
+    const float* __restrict__ nu_t, const float* __restrict__ K_theta, const float* __restrict__ K_q,
+    float* __restrict__ dudt, float* __restrict__ dvdt, float* __restrict__ dwdt, float* __restrict__ dthdt,
+    float* __restrict__ dqvdt)
+{
+    const int n = P.d.cells();
+    const int nx = P.d.nx, ny = P.d.ny, nz = P.d.nz;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+    {
+        int i, j, k;
+        decompose(P.d, c, i, j, k);
+        const bool column = i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2;
+        const bool below_lid = k <= nz - 2;
+        float ru = 0.0f, rv = 0.0f, rw = 0.0f, rt = 0.0f, rq = 0.0f;
+        if (column && below_lid)
+        {
+            if (i <= (P.px ? nx - 2 : nx - 3)) ru = (float)sgs_du(P, u, v, w, rho, nu_t, i, j, k);
+            if (j <= (P.py ? ny - 2 : ny - 3)) rv = (float)sgs_dv(P, u, v, w, rho, nu_t, i, j, k);
+            rw = (float)sgs_dw(P, u, v, w, rho, nu_t, i, j, k);
+        }
+        if (column)
+        {
+            rt = (float)sgs_scalar_rate(P, rho, K_theta, theta, i, j, k);
+            if (qv) rq = (float)sgs_scalar_rate(P, rho, K_q, qv, i, j, k);
+        }
+        dudt[c] = ru;
+        dvdt[c] = rv;
+        dwdt[c] = rw;
+        dthdt[c] = rt;
+        if (dqvdt) dqvdt[c] = rq;
+    }
+}
+
+struct SgsApplyParams
+{
+    int n, nz;
+    double dt;
+    int repairs;
+    double theta_ref;
+    float theta_lo, theta_hi, qv_hi, wind_h, wind_v;
+    const double* theta0;  // [nz] base theta or null (device)
+};
+
+// sanitize_value (include/core/field/field_bounds.hpp:40-56).
+__device__ __forceinline__ float sgs_sanitize(float x, int repairs, float fallback, float lo, float hi)
+{
+    if (!repairs) return x;
+    if (!isfinite(x)) return fallback;
+    return x < lo ? lo : (hi < x ? hi : x);
+}
+
+__device__ __forceinline__ double sgs_rate(float r, int repairs)
+{
+    const double x = (double)r;
+    return repairs && !isfinite(x) ? 0.0 : x;
+}
+
+// Forward Euler of every cell (apply_sgs_tendencies_cpu without the work
+// ledger): x += dt dx/dt in FP64, rounded once, clamped and repaired.
+__global__ void __launch_bounds__(256) sgs_apply_kernel(SgsApplyParams A, float* __restrict__ u,
+                                                        float* __restrict__ v, float* __restrict__ w,
+                                                        float* __restrict__ theta, float* __restrict__ qv,
+                                                        float* __restrict__ tke, const float* __restrict__ dudt,
+                                                        const float* __restrict__ dvdt, const float* __restrict__ dwdt,
+                                                        const float* __restrict__ dthdt,
+                                                        const float* __restrict__ dqvdt,
+                                                        const float* __restrict__ dtkedt,
+                                                        const float* __restrict__ dtke_pbl)
+{
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < A.n; c += gridDim.x * blockDim.x)
+    {
+        float* wind[3] = {u, v, w};
+        const float* rate[3] = {dudt, dvdt, dwdt};
+#pragma unroll
+        for (int f = 0; f < 3; ++f)
+        {
+            double x = (double)wind[f][c] + sgs_rate(rate[f][c], A.repairs) * A.dt;
+            if (A.repairs && !isfinite(x)) x = 0.0;
+            const float lim = f == 2 ? A.wind_v : A.wind_h;
+            wind[f][c] = sgs_sanitize((float)x, A.repairs, 0.0f, -lim, lim);
+        }
+        const double th_old = (double)theta[c];
+        double th = th_old + sgs_rate(dthdt[c], A.repairs) * A.dt;
+        if (A.repairs && !isfinite(th))
+            th = isfinite(th_old) ? th_old : (A.theta0 ? A.theta0[c % A.nz] : A.theta_ref);
+        theta[c] = sgs_sanitize((float)th, A.repairs, (float)A.theta_ref, A.theta_lo, A.theta_hi);
+        if (qv)
+        {
+            double q = (double)qv[c] + sgs_rate(dqvdt[c], A.repairs) * A.dt;
+            if (A.repairs && !isfinite(q)) q = 0.0;
+            qv[c] = sgs_sanitize((float)q, A.repairs, 0.0f, 0.0f, A.qv_hi);
+        }
+        if (tke)
+        {
+            const double old = (double)tke[c];
+            double t = old + (sgs_rate(dtkedt[c], A.repairs) + sgs_rate(dtke_pbl[c], A.repairs)) * A.dt;
+            if (A.repairs && !isfinite(t)) t = isfinite(old) ? old : 0.0;
+            tke[c] = (float)(A.repairs ? (t < 0.0 ? 0.0 : t) : t);
+        }
+    }
+}
+
+// ---- explicit stability (closed or periodic lateral faces) ----
+
+// One thread per physical x-slab i: the slab's momentum power and
+// acceleration norm summed serially in j-k order (the reference's
+// deterministic slab reduction), its theta / qv extrema, and its part of the
+// input check.  partial: [slab][6] = power, norm, theta min, max, qv min, max.
+__global__ void __launch_bounds__(128) sgs_stability_slab_kernel(SgsParams P, const float* __restrict__ u,
+                                                                 const float* __restrict__ v,
+                                                                 const float* __restrict__ w,
+                                                                 const float* __restrict__ theta,
+                                                                 const float* __restrict__ qv,
+                                                                 const float* __restrict__ rho,
+                                                                 const float* __restrict__ dudt,
+                                                                 const float* __restrict__ dvdt,
+                                                                 const float* __restrict__ dwdt,
+                                                                 const float* __restrict__ dthdt,
+                                                                 const float* __restrict__ dqvdt,
+                                                                 double* __restrict__ partial, unsigned* status)
+{
+    const int slab = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nx = P.d.nx, ny = P.d.ny, nz = P.d.nz;
+    if (slab >= nx - 2) return;
+    const int i = slab + 1;
+    const double area = P.dx * P.dy;
+    double p = 0.0, a = 0.0, tlo = INFINITY, thi = -INFINITY, qlo = INFINITY, qhi = -INFINITY;
+    bool bad = false;
+    const int i1 = P.px && i >= nx - 2 ? 1 : i + 1;
+    const bool has_u = P.px || i <= nx - 3;
+    for (int j = 1; j < ny - 1; ++j)
+    {
+        const int j1 = P.py && j >= ny - 2 ? 1 : j + 1;
+        const bool has_v = P.py || j < ny - 2;
+        for (int k = 0; k < nz; ++k)
+        {
+            const int c = P.d.at(i, j, k);
+            const double r = rho[c], th = theta[c];
+            bad |= !isfinite(r) || !isfinite(u[c]) || !isfinite(v[c]) || !isfinite(w[c]) || !isfinite(th) ||
+                   !isfinite(dudt[c]) || !isfinite(dvdt[c]) || !isfinite(dwdt[c]) || !isfinite(dthdt[c]) ||
+                   !(r > 0.0) || !(th > 0.0);
+            if (k < nz - 1)
+            {
+                const double vol = area * P.dz[k];
+                if (has_u)
+                {
+                    const double m = 0.5 * (r * vol + (double)rho[P.d.at(i1, j, k)] * vol);
+                    const double acc = (double)dudt[c];
+                    p += m * (double)u[c] * acc;
+                    a += m * acc * acc;
+                }
+                if (has_v)
+                {
+                    const double m = 0.5 * (r * vol + (double)rho[P.d.at(i, j1, k)] * vol);
+                    const double acc = (double)dvdt[c];
+                    p += m * (double)v[c] * acc;
+                    a += m * acc * acc;
+                }
+                const double m = 0.5 * (r * vol + (double)rho[c + 1] * (area * P.dz[k + 1]));
+                const double acc = (double)dwdt[c];
+                p += m * (double)w[c] * acc;
+                a += m * acc * acc;
+            }
+            tlo = th < tlo ? th : tlo;
+            thi = thi < th ? th : thi;
+            if (qv)
+            {
+                const double q = qv[c];
+                bad |= !isfinite(q) || q < 0.0 || !isfinite(dqvdt[c]);
+                qlo = q < qlo ? q : qlo;
+                qhi = qhi < q ? q : qhi;
+            }
+        }
+    }
+    if (bad) atomicOr(status, kStatusSgsInvalid);
+    double* o = partial + 6 * slab;
+    o[0] = p;
+    o[1] = a;
+    o[2] = tlo;
+    o[3] = thi;
+    o[4] = qlo;
+    o[5] = qhi;
+}
+
+// Merge of the slab partials in increasing i: compensated sums of power and
+// norm (CompensatedSum, include/diagnostics/deterministic_reduction.hpp:28-53)
+// and the extrema.  out: power, norm, theta min, max, qv min, max; one thread.
+__global__ void sgs_stability_merge_kernel(int slabs, const double* __restrict__ partial, double* __restrict__ out)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    double sums[2] = {0.0, 0.0}, corr[2] = {0.0, 0.0};
+    double tlo = INFINITY, thi = -INFINITY, qlo = INFINITY, qhi = -INFINITY;
+    for (int s = 0; s < slabs; ++s)
+    {
+        const double* o = partial + 6 * s;
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+        {
+            const double x = o[q], next = sums[q] + x;
+            if (fabs(sums[q]) >= fabs(x))
+                corr[q] += (sums[q] - next) + x;
+            else
+                corr[q] += (x - next) + sums[q];
+            sums[q] = next;
+        }
+        tlo = o[2] < tlo ? o[2] : tlo;
+        thi = thi < o[3] ? o[3] : thi;
+        qlo = o[4] < qlo ? o[4] : qlo;
+        qhi = qhi < o[5] ? o[5] : qhi;
+    }
+    out[0] = sums[0] + corr[0];
+    out[1] = sums[1] + corr[1];
+    out[2] = tlo;
+    out[3] = thi;
+    out[4] = qlo;
+    out[5] = qhi;
+}
+
+// The theta / qv monotonic limits: min over the physical cells of the time to
+// reach the field's current extremum.  Every candidate is >= 0, so the
+// minimum is an unsigned min over the bit patterns (atomicMin).  ext: the
+// merged extrema (out[2..5] above); lim: two u64 slots preset to +inf.
+__global__ void __launch_bounds__(256) sgs_stability_limit_kernel(SgsParams P, const float* __restrict__ theta,
+                                                                  const float* __restrict__ qv,
+                                                                  const float* __restrict__ dthdt,
+                                                                  const float* __restrict__ dqvdt,
+                                                                  const double* __restrict__ ext,
+                                                                  unsigned long long* lim)
+{
+    const int nx = P.d.nx, ny = P.d.ny, nz = P.d.nz;
+    const int n = (nx - 2) * (ny - 2) * nz;
+    double tl = INFINITY, ql = INFINITY;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+    {
+        const int k = t % nz, col = t / nz;
+        const int j = 1 + col % (ny - 2), i = 1 + col / (ny - 2);
+        const int c = P.d.at(i, j, k);
+        const double th = theta[c], r = dthdt[c];
+        if (r > 0.0)
+            tl = fmin(tl, (ext[1] - th) / r);
+        else if (r < 0.0)
+            tl = fmin(tl, (th - ext[0]) / -r);
+        if (qv)
+        {
+            const double q = qv[c], rq = dqvdt[c];
+            if (rq > 0.0)
+                ql = fmin(ql, (ext[3] - q) / rq);
+            else if (rq < 0.0)
+                ql = fmin(ql, (q - ext[2]) / -rq);
+        }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+    {
+        tl = fmin(tl, __shfl_down_sync(0xffffffffu, tl, off));
+        ql = fmin(ql, __shfl_down_sync(0xffffffffu, ql, off));
+    }
+    if ((threadIdx.x & 31) == 0)
+    {
+        atomicMin(lim, (unsigned long long)__double_as_longlong(tl));
+        atomicMin(lim + 1, (unsigned long long)__double_as_longlong(ql));
+    }
+}
+
+}  // namespace nimbus

@@ -46,6 +46,7 @@ enum : unsigned
     kStatusNonfiniteMassFlux = 1u << 0,
     kStatusNonfiniteTransport = 1u << 1,
     kStatusInvalidEos = 1u << 2,
+    kStatusSgsInvalid = 1u << 3,
 };
 
 struct Dims

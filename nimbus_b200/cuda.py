@@ -168,6 +168,41 @@ class MemberDesc(ctypes.Structure):
     ]
 
 
+class SmagorinskyArgs(ctypes.Structure):
+    _fields_ = [
+        *[(k, _fp) for k in ("u", "v", "w", "theta", "qv", "rho")], ("dz", _dp),
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("filter_mode", ctypes.c_int),
+        ("use_horizontal", ctypes.c_int), ("use_vertical", ctypes.c_int), ("periodic_x", ctypes.c_int),
+        ("periodic_y", ctypes.c_int), ("open_lateral", ctypes.c_int * 4), ("open_top", ctypes.c_int),
+        *[(k, ctypes.c_double) for k in ("dx", "dy", "Cs", "Pr_t", "Sc_t", "nu_t_max", "K_max")],
+        *[(k, _fp) for k in ("nu_t", "K_theta", "K_q", "dudt_sgs", "dvdt_sgs", "dwdt_sgs", "dthetadt_sgs",
+                             "dqvdt_sgs")],
+        ("memory", ctypes.c_int), ("stream", ctypes.c_void_p),
+    ]
+
+
+class SgsApplyArgs(ctypes.Structure):
+    _fields_ = [
+        *[(k, _fp) for k in ("u", "v", "w", "theta", "qv", "tke", "dudt", "dvdt", "dwdt", "dthetadt", "dqvdt",
+                             "dtkedt", "dtkedt_pbl")],
+        ("theta0_base", _dp), ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("dt", ctypes.c_double), ("sanitize", ctypes.c_int), ("theta_reference", ctypes.c_double),
+        *[(k, ctypes.c_float) for k in ("theta_min", "theta_max", "qv_max", "wind_h_max", "wind_v_max")],
+        ("memory", ctypes.c_int), ("stream", ctypes.c_void_p),
+    ]
+
+
+class SgsStability(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_double) for k in ("maximum_timestep_s", "momentum_energy_timestep_s",
+                                               "theta_monotonic_timestep_s", "qv_monotonic_timestep_s",
+                                               "momentum_irreversible_dissipation_w")]
+
+
+class SgsStepArgs(ctypes.Structure):
+    _fields_ = [("closure", SmagorinskyArgs), ("theta0_base", _dp), ("dt", ctypes.c_double),
+                ("dt_sgs", ctypes.c_double), ("time_s", ctypes.c_double), ("sanitize", ctypes.c_int)]
+
+
 class CellCentreArgs(ctypes.Structure):
     _fields_ = [
         ("u", _fp), ("v", _fp), ("w", _fp), ("u_centre", _fp), ("v_centre", _fp), ("w_centre", _fp),
@@ -198,6 +233,7 @@ EXPORTED_SYMBOLS = (
     "nimbus_cuda_slow_tendencies", "nimbus_cuda_slow_step",
     "nimbus_cuda_kessler_tendencies", "nimbus_cuda_kessler_step", "nimbus_cuda_eos_projection",
     "nimbus_cuda_acoustic_boundaries", "nimbus_cuda_state_relaxation",
+    "nimbus_cuda_smagorinsky_fused", "nimbus_cuda_sgs_apply", "nimbus_cuda_sgs_stability", "nimbus_cuda_sgs_step",
     "nimbus_cuda_cell_centre_velocity", "nimbus_cuda_history_snapshot", "nimbus_npy_write_3d",
     "nimbus_history_write", "nimbus_cuda_engine_history_async",
     "nimbus_cuda_engine_create", "nimbus_cuda_engine_destroy", "nimbus_cuda_engine_member_bytes",
@@ -213,7 +249,7 @@ SUBSTEP_AUTO, SUBSTEP_FUSED, SUBSTEP_SPLIT = 0, 1, 2
 PRECISION_REFERENCE, PRECISION_FP32 = 0, 1
 STATIC_SCRATCH_CELLS = 4194304  # NIMBUS_STATIC_SCRATCH_CELLS
 KERNEL_FAMILIES = ("acoustic_substep", "acoustic_momentum", "acoustic_boundary", "transport_faces",
-                   "transport_limiter", "transport_update", "slow", "microphysics", "output")
+                   "transport_limiter", "transport_update", "slow", "microphysics", "output", "sgs")
 # History fields (NIMBUS_HISTORY_* bit order): the reference's core volume
 # bindings, headless_runtime.cpp:588-600.
 HISTORY_FIELDS = ("u", "v", "w", "rho", "p", "theta", "qv", "qc", "qr")
@@ -262,6 +298,12 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
     lib.nimbus_cuda_eos_projection.argtypes = [ctypes.c_void_p, ctypes.POINTER(EosArgs)]
     lib.nimbus_cuda_acoustic_boundaries.argtypes = [ctypes.c_void_p, ctypes.POINTER(BoundaryArgs)]
     lib.nimbus_cuda_state_relaxation.argtypes = [ctypes.c_void_p, ctypes.POINTER(StateRelaxationArgs)]
+    lib.nimbus_cuda_smagorinsky_fused.argtypes = [ctypes.c_void_p, ctypes.POINTER(SmagorinskyArgs)]
+    lib.nimbus_cuda_sgs_apply.argtypes = [ctypes.c_void_p, ctypes.POINTER(SgsApplyArgs)]
+    lib.nimbus_cuda_sgs_stability.argtypes = [ctypes.c_void_p, ctypes.POINTER(SmagorinskyArgs),
+                                              ctypes.POINTER(SgsStability)]
+    lib.nimbus_cuda_sgs_step.argtypes = [ctypes.c_void_p, ctypes.POINTER(SgsStepArgs), ctypes.POINTER(ctypes.c_int),
+                                         ctypes.POINTER(ctypes.c_double)]
     lib.nimbus_cuda_cell_centre_velocity.argtypes = [ctypes.c_void_p, ctypes.POINTER(CellCentreArgs)]
     lib.nimbus_cuda_history_snapshot.argtypes = [ctypes.c_void_p, ctypes.POINTER(HistoryArgs)]
     lib.nimbus_npy_write_3d.argtypes = [_fp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_char_p]
@@ -428,6 +470,28 @@ class Context:
     def acoustic_boundaries(self, args: BoundaryArgs) -> int:
         return self.lib.nimbus_cuda_acoustic_boundaries(self.handle, ctypes.byref(args))
 
+    def smagorinsky_fused(self, args: SmagorinskyArgs) -> int:
+        return self.lib.nimbus_cuda_smagorinsky_fused(self.handle, ctypes.byref(args))
+
+    def sgs_apply(self, args: SgsApplyArgs) -> int:
+        return self.lib.nimbus_cuda_sgs_apply(self.handle, ctypes.byref(args))
+
+    def sgs_stability(self, args: SmagorinskyArgs) -> dict:
+        """The stability limits of args' state and rates; raises on refusal."""
+        out = SgsStability()
+        self.check(self.lib.nimbus_cuda_sgs_stability(self.handle, ctypes.byref(args), ctypes.byref(out)))
+        return {"maximum": out.maximum_timestep_s, "momentum_energy": out.momentum_energy_timestep_s,
+                "theta_monotonic": out.theta_monotonic_timestep_s, "qv_monotonic": out.qv_monotonic_timestep_s,
+                "dissipation_w": out.momentum_irreversible_dissipation_w}
+
+    def sgs_step(self, args: SgsStepArgs) -> tuple:
+        """(substeps, smallest stability limit) of one explicit SGS integration."""
+        count = ctypes.c_int(0)
+        limit = ctypes.c_double(0.0)
+        self.check(self.lib.nimbus_cuda_sgs_step(self.handle, ctypes.byref(args), ctypes.byref(count),
+                                                 ctypes.byref(limit)))
+        return count.value, limit.value
+
     def cell_centre_velocity(self, args: CellCentreArgs) -> int:
         return self.lib.nimbus_cuda_cell_centre_velocity(self.handle, ctypes.byref(args))
 
@@ -585,6 +649,89 @@ def state_relaxation_args(fields, profiles, dt, memory=MEMORY_HOST, stream=None)
     a.dt = float(dt)
     a.memory = memory
     a.stream = stream
+    return a
+
+
+SGS_RATES = ("dudt", "dvdt", "dwdt", "dthdt", "dqvdt")
+
+
+def _empty_like(x):
+    return np.empty_like(x) if isinstance(x, np.ndarray) else x.new_empty(x.shape)
+
+
+def smagorinsky_args(st, dz, grid, sgs, outputs=None, rates=None, memory=MEMORY_HOST, stream=None,
+                     open_top=False) -> SmagorinskyArgs:
+    """Argument block for nimbus_cuda_smagorinsky_fused / _sgs_stability on st's
+    u, v, w, theta, rho and optional qv with a nimbus_b200.sgs.SgsConfig.
+    outputs: {nu_t, K_theta, K_q, dudt, dvdt, dwdt, dthdt, dqvdt} arrays or
+    tensors (default: new ones like u); rates: the five rates for the
+    stability call instead."""
+    u = st["u"]
+    qv = st.get("qv")
+    if outputs is None:
+        outputs = {k: _empty_like(u) for k in ("nu_t", "K_theta", "K_q", *SGS_RATES)}
+    if rates is not None:
+        outputs = {**outputs, **rates}
+    dzh = np.ascontiguousarray(dz, dtype=np.float64)
+    a = SmagorinskyArgs()
+    a._keep = (st, dzh, outputs)
+    a.outputs = outputs
+    for k in ("u", "v", "w", "theta", "rho"):
+        setattr(a, k, _f(st[k]))
+    a.qv = _f(qv)
+    a.dz = _d(dzh)
+    a.nx, a.ny, a.nz = tuple(u.shape)
+    a.filter_mode = 1 if sgs.filter_width == "dx" else 0
+    a.use_horizontal, a.use_vertical = int(sgs.use_horizontal), int(sgs.use_vertical)
+    a.periodic_x, a.periodic_y = int(sgs.periodic_x), int(sgs.periodic_y)
+    for f in range(4):
+        a.open_lateral[f] = int(bool(sgs.open_lateral[f]))
+    a.open_top = int(bool(open_top))
+    a.dx, a.dy = float(grid[0]), float(grid[1])
+    a.Cs, a.Pr_t, a.Sc_t, a.nu_t_max, a.K_max = (float(x) for x in (sgs.Cs, sgs.Pr_t, sgs.Sc_t, sgs.nu_t_max,
+                                                                    sgs.K_max))
+    a.nu_t, a.K_theta, a.K_q = (_f(outputs.get(k)) for k in ("nu_t", "K_theta", "K_q"))
+    a.dudt_sgs, a.dvdt_sgs, a.dwdt_sgs, a.dthetadt_sgs, a.dqvdt_sgs = (_f(outputs.get(k)) for k in SGS_RATES)
+    a.memory = memory
+    a.stream = stream
+    return a
+
+
+def sgs_apply_args(st, rates, dt, theta0=None, sanitize=True, memory=MEMORY_HOST, stream=None) -> SgsApplyArgs:
+    """Argument block for nimbus_cuda_sgs_apply on st's u, v, w, theta and
+    optional qv with the reference's clamp bounds."""
+    t0 = None if theta0 is None else np.ascontiguousarray(theta0, dtype=np.float64)
+    a = SgsApplyArgs()
+    a._keep = (st, rates, t0)
+    for k in ("u", "v", "w", "theta"):
+        setattr(a, k, _f(st[k]))
+    a.qv = _f(st.get("qv"))
+    a.dudt, a.dvdt, a.dwdt, a.dthetadt = (_f(rates[k]) for k in ("dudt", "dvdt", "dwdt", "dthdt"))
+    a.dqvdt = _f(rates.get("dqvdt")) if st.get("qv") is not None else None
+    a.theta0_base = _d(t0)
+    a.nx, a.ny, a.nz = tuple(st["u"].shape)
+    a.dt = float(dt)
+    a.sanitize = int(bool(sanitize))
+    a.theta_reference = 300.0
+    a.theta_min, a.theta_max, a.qv_max, a.wind_h_max, a.wind_v_max = 200.0, 700.0, 0.05, 180.0, 120.0
+    a.memory = memory
+    a.stream = stream
+    return a
+
+
+def sgs_step_args(st, dz, grid, sgs, dt, theta0=None, time_s=0.0, sanitize=True, stream=None,
+                  open_top=False) -> SgsStepArgs:
+    """Argument block for nimbus_cuda_sgs_step on device tensors (scratch for
+    the coefficients and rates comes from the context)."""
+    closure = smagorinsky_args(st, dz, grid, sgs, outputs={}, memory=MEMORY_DEVICE, stream=stream,
+                               open_top=open_top)
+    t0 = None if theta0 is None else np.ascontiguousarray(theta0, dtype=np.float64)
+    a = SgsStepArgs()
+    a._keep = (closure, t0)
+    a.closure = closure
+    a.theta0_base = _d(t0)
+    a.dt, a.dt_sgs, a.time_s = float(dt), float(sgs.dt_sgs), float(time_s)
+    a.sanitize = int(bool(sanitize))
     return a
 
 

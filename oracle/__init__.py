@@ -280,6 +280,29 @@ class Restatement:
             raise ValueError("realized SGS tendency has no positive stable timestep")
         return dict(zip(("maximum", "momentum_energy", "theta_monotonic", "qv_monotonic", "dissipation_w"), out))
 
+    def sgs_step(self, st, dz, grid, sgs, dt, theta0=None, time_s=0.0, repairs=True):
+        """The explicit SGS integration of one large step in place
+        (dynamics.cpp:7159-7217): refresh the closure, bound the substep by
+        the stability limit and dt_sgs, apply; returns (substeps, smallest
+        limit)."""
+        import sys
+        eps = sys.float_info.epsilon
+        floor_s = 64.0 * eps * max(1.0, dt, abs(time_s))
+        advanced, seen, count = 0.0, float("inf"), 0
+        while advanced < dt:
+            rates = self.smagorinsky(st, dz, grid, sgs)
+            limit = self.sgs_stability(st, rates, grid, dz, sgs)["maximum"]
+            seen = min(seen, limit)
+            sub = min(dt - advanced, sgs.dt_sgs, limit)
+            count += 1
+            if not np.isfinite(sub) or sub <= floor_s:
+                raise ValueError("SGS explicit integration cannot make stable progress")
+            self.sgs_apply(st, rates, sub, theta0=theta0, repairs=repairs)
+            advanced += sub
+            if dt - advanced <= floor_s:
+                advanced = dt
+        return count, seen
+
     def scalar_transport(self, qs, pd, rho_end, rho_begin, mfx, mfy, mfz, dt, grid, weno=True, top_open=False):
         self._chk(rho_end, rho_begin, mfx, mfy, mfz, *qs)
         nx, ny, nz = rho_end.shape

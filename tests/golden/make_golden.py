@@ -174,13 +174,64 @@ def make_output():
     print("wrote cell_centre, npy_write_3d")
 
 
+# Smagorinsky SGS: one seeded level with strong wind noise, four closure
+# configurations (bc W, E, S, N, bottom, top; keyword overrides), each with
+# the reference's coefficients and tendencies, one applied SGS substep and,
+# where the lateral faces are periodic or closed, its stability limits.
+SGS_CASES = {
+    "closed_3d_cubic": ((2, 2, 2, 2, 1, 0), {}),
+    "periodic_3d_dx": ((0, 0, 0, 0, 1, 0), {"filter_width": "dx"}),
+    "open_horizontal": ((1, 1, 4, 1, 1, 0), {"use_vertical": False, "Cs": 0.2}),
+    "mixed_vertical": ((0, 0, 2, 3, 1, 0), {"use_horizontal": False, "nu_t_max": 50.0, "K_max": 40.0}),
+}
+SGS_SHAPE = (12, 11, 8)
+SGS_GRID = (500.0, 600.0, 400.0)
+
+
+def sgs_state(seed=41):
+    case = Case(*SGS_SHAPE, *SGS_GRID, 3.0, seed=seed)
+    st, base = cloudy_state(case, seed=seed)
+    rng = np.random.default_rng(seed)
+    for k in "uvw":
+        st[k] = (st[k] + rng.standard_normal(SGS_SHAPE).astype(np.float32) * 3.0).astype(np.float32)
+    return st, base
+
+
+def make_sgs():
+    from nimbus_b200.sgs import SgsConfig
+
+    ref = ReferenceHarness()
+    st, base = sgs_state()
+    dz = np.full(SGS_SHAPE[2], SGS_GRID[2])
+    out = {"grid": np.array(SGS_GRID), "dz": dz, "theta0": base["theta0"],
+           **{f"in_{k}": st[k] for k in ("u", "v", "w", "theta", "qv", "rho")}}
+    for name, (bc, kw) in SGS_CASES.items():
+        cfg = SgsConfig.from_bc(bc, **kw)
+        rates = ref.smagorinsky(st, dz, SGS_GRID, cfg)
+        for k, v in rates.items():
+            out[f"{name}_{k}"] = v
+        applied = {k: st[k].copy() for k in ("u", "v", "w", "theta", "qv")}
+        ref.sgs_apply(applied, rates, 2.5, theta0=base["theta0"])
+        for k, v in applied.items():
+            out[f"{name}_applied_{k}"] = v
+        if not any(cfg.open_lateral):
+            stab = ref.sgs_stability({**st}, rates, SGS_GRID, bc, cfg)
+            out[f"{name}_stability"] = np.array([stab[k] for k in ("maximum", "momentum_energy", "theta_monotonic",
+                                                                    "qv_monotonic", "dissipation_w")])
+    np.savez_compressed(HERE / "smagorinsky.npz", **out)
+    print("wrote smagorinsky")
+
+
 if __name__ == "__main__":
-    # `make_golden.py state_relaxation` (or `output`) writes only that fixture.
+    # `make_golden.py state_relaxation` (or `output`, `sgs`) writes only that fixture.
     if sys.argv[1:] == ["state_relaxation"]:
         make_state_relaxation()
     elif sys.argv[1:] == ["output"]:
         make_output()
+    elif sys.argv[1:] == ["sgs"]:
+        make_sgs()
     else:
         main()
         make_state_relaxation()
         make_output()
+        make_sgs()

@@ -55,6 +55,10 @@ def _c_layout(struct_name, fields, tmp_path):
     ("nimbus_boundary_args", cuda.BoundaryArgs),
     ("nimbus_state_relaxation_args", cuda.StateRelaxationArgs),
     ("nimbus_cell_centre_args", cuda.CellCentreArgs),
+    ("nimbus_smagorinsky_args", cuda.SmagorinskyArgs),
+    ("nimbus_sgs_apply_args", cuda.SgsApplyArgs),
+    ("nimbus_sgs_stability", cuda.SgsStability),
+    ("nimbus_sgs_step_args", cuda.SgsStepArgs),
     ("nimbus_history_args", cuda.HistoryArgs),
     ("nimbus_member_desc", cuda.MemberDesc),
     ("nimbus_member_state", cuda.MemberState),
