@@ -68,6 +68,7 @@ def parse():
     ap.add_argument("--no-error", action="store_true")
     ap.add_argument("--no-relaxation", action="store_true")
     ap.add_argument("--no-output", action="store_true")
+    ap.add_argument("--no-sgs", action="store_true")
     ap.add_argument("--serving-requests", type=int, default=32)
     ap.add_argument("--error-seconds", type=float, default=600.0)
     ap.add_argument("--precision", choices=("fp32", "reference"), default="fp32",
@@ -413,6 +414,84 @@ def output_study(ctx, device):
             "reference_cpu": ref}
 
 
+def sgs_study(ctx, device):
+    """The Smagorinsky SGS path on one 512x512x80 level with rigid lateral
+    walls (84 MB per field, larger than L2), reference precision: the fused
+    closure (nimbus_cuda_smagorinsky_fused: eddy coefficients + stress and
+    scalar diffusion tendencies, 92 algorithmic bytes per cell: u, v, w,
+    theta, qv, rho read and nu_t, K_theta, K_q written by the coefficient
+    pass, u, v, w, rho, nu_t, K_theta, K_q, theta, qv read and five rates
+    written by the tendency pass), the stability limit
+    (nimbus_cuda_sgs_stability, synchronous) and the SGS apply, each
+    device-timed; the explicit SGS integration of a 3 s step with dt_sgs =
+    1 s (three substeps: closure, stability, apply); and the reference's
+    SmagorinskyScheme::compute on the same level on the host cores."""
+    import numpy as np
+    import torch
+
+    import oracle
+    from nimbus_b200 import cuda
+    from nimbus_b200.initial import Case, cloudy_state
+    from nimbus_b200.sgs import SgsConfig
+
+    case = Case(512, 512, 80, 500.0, 500.0, 250.0, 3.0, seed=17, bc=(2, 2, 2, 2, 1, 0))
+    st, base = cloudy_state(case, seed=17)
+    rng = np.random.default_rng(17)
+    for k in "uvw":
+        st[k] = (st[k] + rng.standard_normal(case.shape).astype(np.float32)).astype(np.float32)
+    cfg = SgsConfig.from_bc(case.bc, dt_sgs=1.0)
+    dz = np.full(case.nz, case.dz)
+    grid = (case.dx, case.dy, case.dz)
+    dev = {k: torch.from_numpy(np.ascontiguousarray(st[k])).to(f"cuda:{device}")
+           for k in ("u", "v", "w", "theta", "qv", "rho")}
+    ctx.set_precision(cuda.PRECISION_REFERENCE)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{device}")
+    closure = cuda.smagorinsky_args(dev, dz, grid, cfg, memory=cuda.MEMORY_DEVICE)
+    for _ in range(3):
+        ctx.check(ctx.smagorinsky_fused(closure))
+    calls = 10
+    c_ms = time_on_stream(torch, stream, lambda: ctx.check(ctx.smagorinsky_fused(closure)), calls) / calls
+    ctx.synchronize()
+    peak, kind = load_peaks()
+    achieved = 92.0 * case.cells / (c_ms / 1e3) / 1e9
+    stab_args = cuda.smagorinsky_args(dev, dz, grid, cfg, rates={k: closure.outputs[k] for k in cuda.SGS_RATES},
+                                      memory=cuda.MEMORY_DEVICE)
+    ctx.sgs_stability(stab_args)
+    t0 = time.perf_counter()
+    for _ in range(3):
+        limits = ctx.sgs_stability(stab_args)
+    s_ms = 1e3 * (time.perf_counter() - t0) / 3
+    state = {k: v.clone() for k, v in dev.items()}
+    apply = cuda.sgs_apply_args(state, {k: closure.outputs[k] for k in cuda.SGS_RATES}, 1.0,
+                                theta0=base["theta0"], memory=cuda.MEMORY_DEVICE)
+    ctx.check(ctx.sgs_apply(apply))
+    a_ms = time_on_stream(torch, stream, lambda: ctx.check(ctx.sgs_apply(apply)), calls) / calls
+    step = cuda.sgs_step_args(state, dz, grid, cfg, case.dt, theta0=base["theta0"])
+    ctx.sgs_step(step)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    substeps, _ = ctx.sgs_step(step)
+    torch.cuda.synchronize()
+    step_ms = 1e3 * (time.perf_counter() - t0)
+    ref = None
+    if oracle.reference_available():
+        h = oracle.ReferenceHarness(os.cpu_count())
+        t0 = time.perf_counter()
+        h.smagorinsky(st, dz, grid, cfg)
+        r_s = time.perf_counter() - t0
+        ref = {"kind": "reference", "cores": h.threads, "closure_s": r_s,
+               "sample": "SmagorinskyScheme::compute (coefficients + momentum, theta, qv tendencies) on the same "
+                         "512x512x80 level, one call"}
+    return {"grid": list(case.shape), "cells": case.cells, "precision": "reference (FP64 arithmetic, FP32 storage)",
+            "closure": {"ms_per_call": c_ms, "achieved_gbs": achieved, "peak_gbs": peak, "frac": achieved / peak,
+                        "peak_kind": kind, "algorithmic_bytes_per_cell": 92},
+            "stability": {"ms_per_call": s_ms, "limit_s": limits["maximum"],
+                          "note": "wall time incl. one host synchronisation; slab sums are serial per x-slab"},
+            "apply": {"ms_per_call": a_ms, "algorithmic_bytes_per_cell": 60},
+            "sgs_step": {"dt_s": case.dt, "dt_sgs_s": cfg.dt_sgs, "substeps": substeps, "ms": step_ms},
+            "reference_cpu": ref}
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -552,11 +631,15 @@ def run_ours(args):
     cpu = None
     relaxation = None
     output = None
+    sgs = None
     if rank == 0 and world == 1:
         if not args.no_relaxation:
             relaxation = relaxation_study(ctx, device)
         if not args.no_output:
             output = output_study(ctx, device)
+        if not args.no_sgs:
+            sgs = sgs_study(ctx, device)
+            ctx.set_precision(precision)
         if not args.no_serving:
             serving = serving_study(ctx, args, precision)
         if not args.no_error:
@@ -597,6 +680,7 @@ def run_ours(args):
                 "error_vs_fp64": error,
                 "state_relaxation": relaxation,
                 "output": output,
+                "smagorinsky_sgs": sgs,
                 "parallelism": f"{world} GPU(s), each with its own independent ensemble (no collective)",
                 "l2": "inputs larger than L2 (%.1f GB resident per GPU)" % (cells * 4 * 40 / 1e9),
                 "algorithmic_bytes_per_step": bytes_per_step,

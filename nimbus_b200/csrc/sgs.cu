@@ -142,7 +142,7 @@ nimbus_status run_stability(nimbus_cuda_context* ctx, cudaStream_t st, const Sgs
     NB_CUDA(ctx, cudaMemsetAsync(S.status, 0, sizeof(unsigned), st));
     {
         LaunchTimer t(ctx, st, NIMBUS_KERNEL_SGS);
-        sgs_stability_slab_kernel<<<(slabs + 127) / 128, 128, 0, st>>>(
+        sgs_stability_slab_kernel<<<(slabs + kSlabWarps - 1) / kSlabWarps, 32 * kSlabWarps, 0, st>>>(
             P, D.u, D.v, D.w, D.theta, D.qv, D.rho, R.du, R.dv, R.dw, R.dth, R.dqv, S.partial, S.status);
         sgs_stability_merge_kernel<<<1, 32, 0, st>>>(slabs, S.partial, S.merged);
         const long long cells = static_cast<long long>(slabs) * (P.d.ny - 2) * P.d.nz;

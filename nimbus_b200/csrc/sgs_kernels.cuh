@@ -149,7 +149,7 @@ __device__ __forceinline__ double sgs_min(double a, double b) { return b < a ? b
 // Eddy coefficients of every cell; a cell whose inputs break the reference's
 // field contract (validate_scheme_inputs, eddy_viscosity.cpp:1088-1175) or
 // whose coefficient is not finite raises kStatusSgsInvalid.
-__global__ void __launch_bounds__(256) sgs_coefficients_kernel(SgsParams P, const float* __restrict__ u,
+__global__ void __launch_bounds__(256, 3) sgs_coefficients_kernel(SgsParams P, const float* __restrict__ u,
                                                                const float* __restrict__ v,
                                                                const float* __restrict__ w,
                                                                const float* __restrict__ theta,
@@ -347,7 +347,7 @@ __device__ double sgs_dw(const SgsParams& P, const float* u, const float* v, con
 
 // The five tendencies of every cell; zero where the reference leaves its
 // pre-cleared outputs untouched.
-__global__ void __launch_bounds__(256) sgs_tendencies_kernel(
+__global__ void __launch_bounds__(256, 4) sgs_tendencies_kernel(
     SgsParams P, const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w,
     const float* __restrict__ theta, const float* __restrict__ qv, const float* __restrict__ rho,
     const float* __restrict__ nu_t, const float* __restrict__ K_theta, const float* __restrict__ K_q,
@@ -453,84 +453,168 @@ __global__ void __launch_bounds__(256) sgs_apply_kernel(SgsApplyParams A, float*
 
 // ---- explicit stability (closed or periodic lateral faces) ----
 
-// One thread per physical x-slab i: the slab's momentum power and
+// One warp per physical x-slab i: the slab's momentum power and
 // acceleration norm summed serially in j-k order (the reference's
 // deterministic slab reduction), its theta / qv extrema, and its part of the
 // input check.  partial: [slab][6] = power, norm, theta min, max, qv min, max.
-__global__ void __launch_bounds__(128) sgs_stability_slab_kernel(SgsParams P, const float* __restrict__ u,
-                                                                 const float* __restrict__ v,
-                                                                 const float* __restrict__ w,
-                                                                 const float* __restrict__ theta,
-                                                                 const float* __restrict__ qv,
-                                                                 const float* __restrict__ rho,
-                                                                 const float* __restrict__ dudt,
-                                                                 const float* __restrict__ dvdt,
-                                                                 const float* __restrict__ dwdt,
-                                                                 const float* __restrict__ dthdt,
-                                                                 const float* __restrict__ dqvdt,
-                                                                 double* __restrict__ partial, unsigned* status)
+// The lanes load 32 consecutive levels of a row (coalesced) and form each
+// cell's six terms (mass * velocity * acceleration and mass * acceleration^2
+// of its u, v and w faces) in parallel; lane 0 then adds them to the two
+// running sums in the reference's order, while the lanes already hold the
+// next chunk's loads.  A face the reference skips contributes +0.0, which
+// leaves a sum that started at +0.0 unchanged bit for bit.
+constexpr int kSlabWarps = 4;
+
+struct SlabChunk
 {
-    const int slab = blockIdx.x * blockDim.x + threadIdx.x;
+    float u, v, w, r, ri, rj, rk, du, dv, dw, th, dth, q, dq;
+};
+
+__device__ __forceinline__ SlabChunk slab_load(const SgsParams& P, const float* u, const float* v, const float* w,
+                                               const float* theta, const float* qv, const float* rho,
+                                               const float* dudt, const float* dvdt, const float* dwdt,
+                                               const float* dthdt, const float* dqvdt, int i, int i1, int j, int j1,
+                                               int k)
+{
+    SlabChunk x{};
+    if (k >= P.d.nz) return x;
+    const int c = P.d.at(i, j, k);
+    x.u = __ldg(u + c);
+    x.v = __ldg(v + c);
+    x.w = __ldg(w + c);
+    x.r = __ldg(rho + c);
+    x.ri = __ldg(rho + P.d.at(i1, j, k));
+    x.rj = __ldg(rho + P.d.at(i, j1, k));
+    x.rk = k + 1 < P.d.nz ? __ldg(rho + c + 1) : 1.0f;
+    x.du = __ldg(dudt + c);
+    x.dv = __ldg(dvdt + c);
+    x.dw = __ldg(dwdt + c);
+    x.th = __ldg(theta + c);
+    x.dth = __ldg(dthdt + c);
+    if (qv)
+    {
+        x.q = __ldg(qv + c);
+        x.dq = __ldg(dqvdt + c);
+    }
+    return x;
+}
+
+__global__ void __launch_bounds__(32 * kSlabWarps) sgs_stability_slab_kernel(
+    SgsParams P, const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w,
+    const float* __restrict__ theta, const float* __restrict__ qv, const float* __restrict__ rho,
+    const float* __restrict__ dudt, const float* __restrict__ dvdt, const float* __restrict__ dwdt,
+    const float* __restrict__ dthdt, const float* __restrict__ dqvdt, double* __restrict__ partial,
+    unsigned* status)
+{
+    __shared__ double terms[kSlabWarps][6][32];
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int slab = blockIdx.x * kSlabWarps + wib;
     const int nx = P.d.nx, ny = P.d.ny, nz = P.d.nz;
-    if (slab >= nx - 2) return;
+    if (slab >= nx - 2) return;  // uniform across the warp
     const int i = slab + 1;
     const double area = P.dx * P.dy;
-    double p = 0.0, a = 0.0, tlo = INFINITY, thi = -INFINITY, qlo = INFINITY, qhi = -INFINITY;
-    bool bad = false;
     const int i1 = P.px && i >= nx - 2 ? 1 : i + 1;
     const bool has_u = P.px || i <= nx - 3;
-    for (int j = 1; j < ny - 1; ++j)
+    double (*t)[32] = terms[wib];
+    double p = 0.0, a = 0.0, tlo = INFINITY, thi = -INFINITY, qlo = INFINITY, qhi = -INFINITY;
+    bool bad = false;
+    const int chunks = (nz + 31) / 32;
+    const int total = (ny - 2) * chunks;
+    // Chunk n covers row j = 1 + n / chunks, levels (n % chunks) * 32 + lane.
+    auto row_of = [&](int n, int& j, int& j1, int& k) {
+        j = 1 + n / chunks;
+        j1 = P.py && j >= ny - 2 ? 1 : j + 1;
+        k = (n % chunks) * 32 + lane;
+    };
+    int j, j1, k;
+    row_of(0, j, j1, k);
+    SlabChunk x = slab_load(P, u, v, w, theta, qv, rho, dudt, dvdt, dwdt, dthdt, dqvdt, i, i1, j, j1, k);
+    for (int n = 0; n < total; ++n)
     {
-        const int j1 = P.py && j >= ny - 2 ? 1 : j + 1;
-        const bool has_v = P.py || j < ny - 2;
-        for (int k = 0; k < nz; ++k)
+        const int jc = j, kc = k;
+        const SlabChunk cur = x;
+        if (n + 1 < total)
         {
-            const int c = P.d.at(i, j, k);
-            const double r = rho[c], th = theta[c];
-            bad |= !isfinite(r) || !isfinite(u[c]) || !isfinite(v[c]) || !isfinite(w[c]) || !isfinite(th) ||
-                   !isfinite(dudt[c]) || !isfinite(dvdt[c]) || !isfinite(dwdt[c]) || !isfinite(dthdt[c]) ||
+            row_of(n + 1, j, j1, k);
+            x = slab_load(P, u, v, w, theta, qv, rho, dudt, dvdt, dwdt, dthdt, dqvdt, i, i1, j, j1, k);
+        }
+        double tm[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        if (kc < nz)
+        {
+            const double r = cur.r, th = cur.th;
+            bad |= !isfinite(r) || !isfinite(cur.u) || !isfinite(cur.v) || !isfinite(cur.w) || !isfinite(th) ||
+                   !isfinite(cur.du) || !isfinite(cur.dv) || !isfinite(cur.dw) || !isfinite(cur.dth) ||
                    !(r > 0.0) || !(th > 0.0);
-            if (k < nz - 1)
+            if (kc < nz - 1)
             {
-                const double vol = area * P.dz[k];
+                const double vol = area * P.dz[kc];
                 if (has_u)
                 {
-                    const double m = 0.5 * (r * vol + (double)rho[P.d.at(i1, j, k)] * vol);
-                    const double acc = (double)dudt[c];
-                    p += m * (double)u[c] * acc;
-                    a += m * acc * acc;
+                    const double m = 0.5 * (r * vol + (double)cur.ri * vol);
+                    const double acc = cur.du;
+                    tm[0] = m * (double)cur.u * acc;
+                    tm[1] = m * acc * acc;
                 }
-                if (has_v)
+                if (P.py || jc < ny - 2)
                 {
-                    const double m = 0.5 * (r * vol + (double)rho[P.d.at(i, j1, k)] * vol);
-                    const double acc = (double)dvdt[c];
-                    p += m * (double)v[c] * acc;
-                    a += m * acc * acc;
+                    const double m = 0.5 * (r * vol + (double)cur.rj * vol);
+                    const double acc = cur.dv;
+                    tm[2] = m * (double)cur.v * acc;
+                    tm[3] = m * acc * acc;
                 }
-                const double m = 0.5 * (r * vol + (double)rho[c + 1] * (area * P.dz[k + 1]));
-                const double acc = (double)dwdt[c];
-                p += m * (double)w[c] * acc;
-                a += m * acc * acc;
+                const double m = 0.5 * (r * vol + (double)cur.rk * (area * P.dz[kc + 1]));
+                const double acc = cur.dw;
+                tm[4] = m * (double)cur.w * acc;
+                tm[5] = m * acc * acc;
             }
             tlo = th < tlo ? th : tlo;
             thi = thi < th ? th : thi;
             if (qv)
             {
-                const double q = qv[c];
-                bad |= !isfinite(q) || q < 0.0 || !isfinite(dqvdt[c]);
+                const double q = cur.q;
+                bad |= !isfinite(q) || q < 0.0 || !isfinite(cur.dq);
                 qlo = q < qlo ? q : qlo;
                 qhi = qhi < q ? q : qhi;
             }
         }
+#pragma unroll
+        for (int q = 0; q < 6; ++q) t[q][lane] = tm[q];
+        __syncwarp();
+        if (lane == 0)
+        {
+            const int cells = min(32, nz - (kc - lane));
+            for (int c = 0; c < cells; ++c)
+            {
+                p += t[0][c];
+                a += t[1][c];
+                p += t[2][c];
+                a += t[3][c];
+                p += t[4][c];
+                a += t[5][c];
+            }
+        }
+        __syncwarp();
     }
-    if (bad) atomicOr(status, kStatusSgsInvalid);
-    double* o = partial + 6 * slab;
-    o[0] = p;
-    o[1] = a;
-    o[2] = tlo;
-    o[3] = thi;
-    o[4] = qlo;
-    o[5] = qhi;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+    {
+        tlo = fmin(tlo, __shfl_down_sync(0xffffffffu, tlo, off));
+        thi = fmax(thi, __shfl_down_sync(0xffffffffu, thi, off));
+        qlo = fmin(qlo, __shfl_down_sync(0xffffffffu, qlo, off));
+        qhi = fmax(qhi, __shfl_down_sync(0xffffffffu, qhi, off));
+    }
+    bad = __any_sync(0xffffffffu, bad);
+    if (lane == 0)
+    {
+        if (bad) atomicOr(status, kStatusSgsInvalid);
+        double* o = partial + 6 * slab;
+        o[0] = p;
+        o[1] = a;
+        o[2] = tlo;
+        o[3] = thi;
+        o[4] = qlo;
+        o[5] = qhi;
+    }
 }
 
 // Merge of the slab partials in increasing i: compensated sums of power and

@@ -11,7 +11,9 @@ the phases this backend owns):
      (split_explicit.cpp:174-260);
   4. conservative WENO5 transport of theta, qv, qc, qr against the retained
      fluxes and densities (advection_batch.cpp:565-760);
-  5. the Kessler step over the C-grid cell domain (microphysics_step.cpp);
+  5. the Kessler step over the C-grid cell domain (microphysics_step.cpp),
+     then optionally the explicit Smagorinsky SGS integration
+     (dynamics.cpp:7151-7250; ResidentRun only);
   6. the EOS pressure re-projection (eos_apply.cpp);
   7. optionally the end-of-step sponge (rayleigh_damping.cpp, called at
      dynamics.cpp:7323-7340) and the closing boundary refresh
@@ -47,7 +49,7 @@ def substeps_for(case: Case, state, base) -> int:
 class ResidentRun:
     def __init__(self, ctx: cuda.Context, case: Case, state=None, base=None, device="cuda",
                  precision: int = cuda.PRECISION_FP32, autotune: bool = True, coriolis_f: float = 0.0,
-                 microphysics: bool = True, sponge=None, final_closure: bool = False):
+                 microphysics: bool = True, sponge=None, final_closure: bool = False, sgs=None):
         self.ctx = ctx
         self.precision = precision
         self.tuned = None
@@ -88,6 +90,11 @@ class ResidentRun:
         self._sponge = (cuda.state_relaxation_args(f, sponge, case.dt, memory=cuda.MEMORY_DEVICE)
                         if sponge is not None else None)
         self.final_closure = final_closure
+        # The explicit Smagorinsky SGS integration (nimbus_b200.sgs.SgsConfig).
+        self.time_s = 0.0
+        self.sgs_substeps = 0
+        self._sgs = (cuda.sgs_step_args(f, np.full(case.nz, case.dz), grid, sgs, case.dt, theta0=base["theta0"])
+                     if sgs is not None else None)
         self.torch_stream = torch.cuda.ExternalStream(self.stream, device=dev)
 
     @property
@@ -107,11 +114,16 @@ class ResidentRun:
         c.check(c.scalar_transport(self._transport))
         if self.microphysics:
             c.check(c.kessler_step(self._kessler))
+        if self._sgs is not None:  # synchronises once per SGS substep
+            self._sgs.time_s = self.time_s
+            count, _ = c.sgs_step(self._sgs)
+            self.sgs_substeps += count
         c.check(c.eos_projection(self._eos))
         if self._sponge is not None:
             c.check(c.state_relaxation(self._sponge))
         if self.final_closure:  # apply_full_attributed = apply_acoustic(0)
             c.check(c.acoustic_boundaries(self._refresh))
+        self.time_s += self.case.dt
 
     def download(self) -> dict:
         torch.cuda.current_stream().wait_stream(self.torch_stream)

@@ -158,13 +158,16 @@ class Restatement:
                                      ctypes.c_double(frame[0]), ctypes.c_double(frame[1]))
 
     def large_step(self, st, base, grid, dt, n_substeps, bc, coriolis_f=0.0, microphysics=True, sponge=None,
-                   final_closure=False):
+                   final_closure=False, sgs=None, time_s=0.0):
         """One large step of the hot path in the reference's order
         (dynamics.cpp:5123-7317): Heun slow step, boundary refresh, the
         acoustic loop (KW78 seed, N substeps with retained mass flux),
         conservative WENO5 transport of theta, qv, qc, qr, the Kessler step
         over the C-grid cell domain and the EOS re-projection.  In place on
-        the state dict; raises when the EOS projection refuses the state."""
+        the state dict; raises when the EOS projection refuses the state.
+        sgs (a nimbus_b200.sgs.SgsConfig) adds the explicit Smagorinsky
+        integration between the Kessler step and the EOS projection, as the
+        reference orders them; time_s is the model time at the step start."""
         self.slow_rk2_step(st, base, grid, dt, coriolis_f=coriolis_f)
         self.acoustic_boundaries(st, grid, bc, 0.0)
         loop = self.acoustic_loop(st, base["rho0"], base["p0"], dt, n_substeps, grid, bc)
@@ -174,6 +177,8 @@ class Restatement:
         nx, ny, nz = st["u"].shape
         if microphysics:
             self.kessler_step(st, grid[2], dt, (1, nx - 1, 1, ny - 1, 0, nz))
+        if sgs is not None:  # the explicit SGS integration (dynamics.cpp:7151-7250)
+            self.sgs_step(st, np.full(nz, grid[2]), grid, sgs, dt, theta0=base["theta0"], time_s=time_s)
         if not self.eos_projection(st["p"], st["rho"], st["theta"], st["qv"], st["qc"], st["qr"]):
             raise FloatingPointError("EOS pressure projection rejected an invalid physical state")
         if sponge is not None:

@@ -198,9 +198,9 @@ def test_refusals(ctx, golden):
 
 
 def test_full_level(ctx, o32):
-    """A 256x256x64 level (16 MB per field) bit for bit; the closure's ncu
-    capture uses this case."""
-    st, _ = _case((256, 256, 64), 77)
+    """A 320x320x64 level (26 MB per field, 14 fields read or written: more
+    than L2) bit for bit; the closure's ncu capture uses this case."""
+    st, _ = _case((320, 320, 64), 77)
     dz = _dz(64, "uniform")
     cfg = SgsConfig.from_bc((2, 2, 2, 2, 1, 0))
     dev = on_device({k: st[k] for k in ("u", "v", "w", "theta", "rho", "qv")})
@@ -211,3 +211,26 @@ def test_full_level(ctx, o32):
     want = o32.smagorinsky(st, dz, SGS_GRID, cfg)
     for k, v in args.outputs.items():
         assert_bitwise(v.cpu().numpy(), want[k], k)
+
+
+@pytest.mark.parametrize("bc,dt_sgs", [((2, 2, 2, 2, 1, 0), 1.0), ((0, 0, 2, 3, 0, 0), 4.0)])
+def test_resident_run_with_sgs_matches_oracle(ctx, o32, bc, dt_sgs):
+    """Two large steps of the plain path with the Smagorinsky integration
+    between the Kessler step and the EOS projection, against the oracle's
+    large step with the same closure: bit for bit."""
+    from nimbus_b200.run import PROGNOSTIC, ResidentRun
+
+    case = Case(24, 20, 16, 1000.0, 1000.0, 500.0, 3.0, seed=12, bc=bc, substeps=6)
+    st, base = cloudy_state(case, seed=12)
+    cfg = SgsConfig.from_bc(bc, dt_sgs=dt_sgs)
+    run = ResidentRun(ctx, case, {k: v.copy() for k, v in st.items()}, base, precision=cuda.PRECISION_REFERENCE,
+                      autotune=False, sgs=cfg)
+    want = {k: v.copy() for k, v in st.items()}
+    for step in range(2):
+        run.step()
+        o32.large_step(want, base, (case.dx, case.dy, case.dz), case.dt, run.n_substeps, case.bc, sgs=cfg,
+                       time_s=step * case.dt)
+    got = run.download()
+    for k in PROGNOSTIC:
+        assert_bitwise(got[k], want[k], k)
+    assert run.sgs_substeps == 2 * int(np.ceil(case.dt / dt_sgs))
