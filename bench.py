@@ -407,7 +407,7 @@ def output_study(ctx, device):
                             "frac": achieved / peak, "peak_kind": kind, "algorithmic_bytes_per_cell": 24},
             "history_frame": {"fields": 9, "bytes": frame_bytes, "ms_per_frame": f_ms,
                               "d2h_gbs": frame_bytes / (f_ms / 1e3) / 1e9,
-                              "path": "one centring launch + one device-to-host copy per adjacent run of fields, "
+                              "path": "one centring launch + one device-to-host copy for the velocities and one per scalar, "
                                       "into pinned host memory"},
             "npy_write": {"status": cuda.STATUS_NAMES.get(rc, rc), "seconds": write_s,
                           "gbs": frame_bytes / write_s / 1e9, "target": "local temporary directory"},

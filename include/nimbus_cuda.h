@@ -682,7 +682,8 @@ enum
  * nx*ny*nz floats -- the payloads the reference's export writes
  * (write_or_snapshot_core_volume_fields, include/core/output/core_volume_writer.hpp:26-64).
  * Enqueued on `stream` (NULL: the context's): one centring launch into device
- * staging and one device-to-host copy per contiguous run of fields; the image
+ * staging, one device-to-host copy for the staged velocities and one per
+ * scalar field; the image
  * is complete once the stream is synchronised.  host_image should be pinned
  * (cudaHostAlloc) for the copies to run at bus rate and overlap later work.
  * A field whose bit is set must be non-NULL.

@@ -110,7 +110,9 @@ nimbus_status enqueue_history(nimbus_cuda_context* ctx, cudaStream_t st, const f
     NB_TRY(launch_centre(ctx, st, d, F));
     for (int f = 3; f < kHistoryFields; ++f)
         if (fields & (1u << f)) from[f] = src[f];
-    // One copy per run of selected fields whose sources are adjacent.
+    // One copy for the staged velocities (one allocation), one per scalar
+    // field: a copy may not span two allocations, and adjacent caller
+    // buffers can belong to different ones.
     size_t slot = 0;
     for (int f = 0; f < kHistoryFields;)
     {
@@ -120,7 +122,7 @@ nimbus_status enqueue_history(nimbus_cuda_context* ctx, cudaStream_t st, const f
             continue;
         }
         int last = f;
-        while (last + 1 < kHistoryFields && (fields & (1u << (last + 1))) && from[last + 1] == from[last] + n) ++last;
+        while (last + 1 < 3 && (fields & (1u << (last + 1))) && from[last + 1] == from[last] + n) ++last;
         const size_t count = static_cast<size_t>(last - f + 1);
         NB_CUDA(ctx, cudaMemcpyAsync(host_image + slot * n, from[f], count * n * sizeof(float),
                                      cudaMemcpyDeviceToHost, st));

@@ -7,11 +7,11 @@ by recreating <outdir>/step_NNNNNN, staging cell-centre u, v, w
 <name>.npy with npy::write_3d, either at once or from its asynchronous
 writer's thread (src/core/output/output_writer.cpp:1330-1350).
 
-Here a frame is enqueued on the run's own stream -- nimbus_cuda_history_snapshot
+Here a frame is enqueued on the run's own stream (nimbus_cuda_history_snapshot
 for a ResidentRun, nimbus_cuda_engine_history_async for an engine member: one
-centring launch and one copy per run of adjacent fields into a pinned image --
-and a writer thread waits for that frame's event and writes the files with
-nimbus_history_write.  The steps enqueued after a frame overlap both its copy
+centring launch, one copy for the velocities and one per scalar field into a
+pinned image), and a writer thread waits for that frame's event and writes the
+files with nimbus_history_write.  The steps enqueued after a frame overlap both its copy
 and its file writes; the writer blocks new frames only when every pinned
 image is still in flight.
 """
