@@ -8,6 +8,11 @@ unit.  The reference-precision units are compiled with --fmad=false: the CPU
 solver they match performs every multiply and add separately, and a
 contracted FMA would change the rounding of stored values.  The FP32 form's
 unit (fp32_*.cu) is compiled with --fmad=true.
+
+Where the reference solver's headers are present it also builds
+nimbus_b200/lib/libnimbus_reference_backend.so, the ComputeBackend adapter
+(reference_backend/nimbus_compute_backend.cpp) that plugs this library into
+the reference's own backend interface.
 """
 from __future__ import annotations
 
@@ -32,6 +37,28 @@ def nvcc() -> str:
 
 def sources():
     return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cuh")) + [PKG.parent / "include" / "nimbus_cuda.h"]
+
+
+# The reference's headers, for the ComputeBackend adapter (built when present).
+REFERENCE = Path(os.environ.get("NIMBUS_REFERENCE_ROOT", "/root/reference"))
+ADAPTER = PKG / "reference_backend" / "nimbus_compute_backend.cpp"
+
+
+def build_reference_backend(force: bool = False) -> Path | None:
+    """nimbus_b200/lib/libnimbus_reference_backend.so: the CUDA backend as a
+    ComputeBackend of the reference solver, compiled against its headers and
+    linked to libnimbus_cuda.so.  Skipped (None) without the reference tree."""
+    if not (REFERENCE / "include" / "compute" / "backend_interface.hpp").exists():
+        return None
+    out = LIB / "libnimbus_reference_backend.so"
+    cuda_lib = LIB / "libnimbus_cuda.so"
+    if out.exists() and not force and out.stat().st_mtime >= max(ADAPTER.stat().st_mtime, cuda_lib.stat().st_mtime):
+        return out
+    cxx = os.environ.get("CXX", "g++")
+    subprocess.run([cxx, "-std=c++17", "-O2", "-fPIC", "-shared", "-w", "-I", str(REFERENCE / "include"),
+                    "-I", str(REFERENCE / "src"), str(ADAPTER), "-o", str(out), "-L", str(LIB), "-lnimbus_cuda",
+                    "-Wl,-rpath,$ORIGIN", "-Wl,--no-undefined"], check=True)
+    return out
 
 
 def build(force: bool = False, verbose: bool = False) -> Path:
@@ -59,8 +86,10 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     if any(j.wait() != 0 for j in jobs):
         raise subprocess.CalledProcessError(1, "nvcc")
     subprocess.run([nvcc(), *ARCH, "-shared", *[str(o) for o in objs], "-o", str(out)], check=True)
+    build_reference_backend(force=True)
     return out
 
 
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))
+    print(build_reference_backend())

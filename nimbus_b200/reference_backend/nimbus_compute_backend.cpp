@@ -1,0 +1,218 @@
+// The CUDA backend as a ComputeBackend of the reference solver: the class a
+// maintainer registers beside CpuComputeBackend (src/compute/compute_backend.cpp:76-88,
+// include/compute/backend_types.hpp:27-32 gain a Cuda kind).  It implements
+// the reference's own interfaces (include/compute/backend_interface.hpp,
+// include/compute/dispatch/dynamics.hpp, include/compute/dispatch/turbulence.hpp)
+// and forwards each dispatch struct to the C-ABI in include/nimbus_cuda.h;
+// nothing here computes.  Built against the reference's headers only (every
+// virtual it overrides is declared inline there), linked to libnimbus_cuda.so.
+//
+// Dispatches follow the reference's contract: false leaves host fields
+// untouched and the caller decides between its CPU path and an error
+// (dynamics.cpp:4453,4604).
+//   AcousticSubstepFusedCartesianCgrid  the dispatch carries the CPU solver's
+//       FP64 profiles and spacings (rho0_base_host, dx_host, ...): the result
+//       is the CPU backend's, bit for bit.
+//   Smagorinsky (dispatch_smagorinsky_fused)  the bridge passes FP32 copies of
+//       dz, dx, dy and the closure constants (src/compute/dispatch/turbulence.cpp:87-146);
+//       they are widened to FP64, so the result equals the CPU scheme's
+//       exactly when those values are FP32-representable (dz = 250 m, Cs =
+//       0.25, ...), and differs by their FP32 rounding otherwise.
+//   SgsApply  the same widening of dt_step and the bounds; a dispatch that
+//       asks for a completion observer is declined (false).
+#include "compute/backend_interface.hpp"
+#include "compute/dispatch/dynamics.hpp"
+#include "compute/dispatch/turbulence.hpp"
+
+#include "../../include/nimbus_cuda.h"
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace
+{
+
+class NimbusCudaComputeBackend final : public ComputeBackend,
+                                       public DynamicsComputeKernels,
+                                       public TurbulenceComputeKernels
+{
+public:
+    ~NimbusCudaComputeBackend() override { shutdown(); }
+
+    std::string name() const override { return "cuda"; }
+
+    bool initialize(std::string& error) override
+    {
+        if (ctx_) return true;
+        if (nimbus_cuda_create(0, &ctx_) != NIMBUS_OK)
+        {
+            ctx_ = nullptr;
+            error = "no sm_100 CUDA device (the CUDA backend has no CPU fallback)";
+            return false;
+        }
+        nimbus_cuda_set_precision(ctx_, NIMBUS_PRECISION_REFERENCE);
+        return true;
+    }
+
+    void shutdown() override
+    {
+        if (ctx_) nimbus_cuda_destroy(ctx_);
+        ctx_ = nullptr;
+    }
+
+    std::uint64_t successful_dispatch_count() const override { return dispatches_; }
+
+    DynamicsComputeKernels* dynamics_kernels() override { return ctx_ ? this : nullptr; }
+    const DynamicsComputeKernels* dynamics_kernels() const override { return ctx_ ? this : nullptr; }
+    TurbulenceComputeKernels* turbulence_kernels() override { return ctx_ ? this : nullptr; }
+    const TurbulenceComputeKernels* turbulence_kernels() const override { return ctx_ ? this : nullptr; }
+
+    bool supports(DynamicsKernelOp op) const override
+    {
+        return op == DynamicsKernelOp::AcousticSubstepFusedCartesianCgrid;
+    }
+
+    bool supports(TurbulenceKernelOp op) const override
+    {
+        return op == TurbulenceKernelOp::Smagorinsky || op == TurbulenceKernelOp::SgsApply;
+    }
+
+    bool dispatch_acoustic_substep_fused_cartesian_cgrid(const AcousticSubstepFusedCartesianCgridDispatch& d) override
+    {
+        if (!ctx_ || !d.rho0_base_host || !d.p0_base_host) return false;
+        nimbus_acoustic_fused_args a{};
+        a.u = d.u;
+        a.v = d.v;
+        a.w = d.w;
+        a.rho = d.rho;
+        a.p = d.p;
+        a.theta = d.theta_data;
+        a.rho0_base = d.rho0_base_host;
+        a.p0_base = d.p0_base_host;
+        a.base_len = d.base_len;
+        a.nx = d.nx;
+        a.ny = d.ny;
+        a.nz = d.nz;
+        a.dx = d.dx_host;
+        a.dy = d.dy_host;
+        a.dz = d.dz_host;
+        a.dt_small = d.dt_small_host;
+        a.gamma = d.gamma_host;
+        a.rho_min = d.rho_min;
+        a.rho_max = d.rho_max;
+        a.p_min = d.p_min;
+        a.p_max = d.p_max;
+        a.p_ref_fallback = d.p_ref_fallback;
+        a.wind_clamp_h = d.wind_clamp_h;
+        a.wind_clamp_v = d.wind_clamp_v;
+        a.drho_scratch = d.drho_scratch;
+        a.memory = NIMBUS_MEMORY_HOST;
+        return count(nimbus_cuda_acoustic_fused(ctx_, &a));
+    }
+
+    bool dispatch_smagorinsky_fused(const SmagorinskyFusedDispatch& d) override
+    {
+        if (!ctx_ || !d.dz_prof || d.prof_len < d.nz) return false;
+        std::vector<double> dz(static_cast<size_t>(d.nz));
+        for (int k = 0; k < d.nz; ++k) dz[k] = static_cast<double>(d.dz_prof[k]);
+        // The scheme sizes its coefficient fields only when it wants them back.
+        std::vector<float> scratch;
+        const size_t n = static_cast<size_t>(d.nx) * d.ny * d.nz;
+        const bool coefficients = d.download_coefficients && d.nu_t && d.K_theta && d.K_q;
+        nimbus_smagorinsky_args a{};
+        a.u = d.u_data;
+        a.v = d.v_data;
+        a.w = d.w_data;
+        a.theta = d.theta_data;
+        a.qv = d.has_qv ? d.qv_data : nullptr;
+        a.rho = d.rho;
+        a.dz = dz.data();
+        a.nx = d.nx;
+        a.ny = d.ny;
+        a.nz = d.nz;
+        a.filter_mode = d.filter_mode;
+        a.use_horizontal = d.use_horizontal;
+        a.use_vertical = d.use_vertical;
+        a.periodic_x = d.periodic_x;
+        a.periodic_y = d.periodic_y;
+        for (int f = 0; f < 4; ++f) a.open_lateral[f] = d.open_lateral[f];
+        a.dx = d.dx_val;
+        a.dy = d.dy_val;
+        a.Cs = d.Cs;
+        a.Pr_t = d.Pr_t;
+        a.Sc_t = d.Sc_t;
+        a.nu_t_max = d.nu_t_max;
+        a.K_max = d.K_max;
+        a.nu_t = coefficients ? d.nu_t : nullptr;
+        a.K_theta = coefficients ? d.K_theta : nullptr;
+        a.K_q = coefficients ? d.K_q : nullptr;
+        a.dudt_sgs = d.dudt_sgs;
+        a.dvdt_sgs = d.dvdt_sgs;
+        a.dwdt_sgs = d.dwdt_sgs;
+        a.dthetadt_sgs = d.dthetadt_sgs;
+        if (!d.has_qv && d.dqvdt_sgs)
+        {
+            scratch.assign(n, 0.0f);  // the reference leaves dqvdt untouched without qv
+            a.dqvdt_sgs = scratch.data();
+        }
+        else
+        {
+            a.dqvdt_sgs = d.dqvdt_sgs;
+        }
+        a.memory = NIMBUS_MEMORY_HOST;
+        return count(nimbus_cuda_smagorinsky_fused(ctx_, &a));
+    }
+
+    bool dispatch_sgs_apply(const SgsApplyDispatch& d) override
+    {
+        if (!ctx_ || d.completed_observer || d.collocated) return false;
+        nimbus_sgs_apply_args a{};
+        a.u = d.u;
+        a.v = d.v;
+        a.w = d.w;
+        a.theta = d.theta_data;
+        a.qv = d.has_qv ? d.qv_data : nullptr;
+        a.tke = d.has_tke ? d.tke_data : nullptr;
+        a.dudt = d.dudt;
+        a.dvdt = d.dvdt;
+        a.dwdt = d.dwdt;
+        a.dthetadt = d.dthetadt;
+        a.dqvdt = d.dqvdt;
+        a.dtkedt = d.dtkedt;
+        a.dtkedt_pbl = d.dtkedt_pbl;
+        a.nx = d.nx;
+        a.ny = d.ny;
+        a.nz = d.nz;
+        a.dt = d.dt_step;
+        a.sanitize = d.sanitize;
+        a.theta_reference = d.theta_fallback;
+        a.theta_min = d.theta_min;
+        a.theta_max = d.theta_max;
+        a.qv_max = d.qv_max_val;
+        a.wind_h_max = d.wind_h_max;
+        a.wind_v_max = d.wind_v_max;
+        a.memory = NIMBUS_MEMORY_HOST;
+        return count(nimbus_cuda_sgs_apply(ctx_, &a));
+    }
+
+private:
+    bool count(nimbus_status s)
+    {
+        if (s != NIMBUS_OK) return false;
+        ++dispatches_;
+        return true;
+    }
+
+    nimbus_cuda_context* ctx_ = nullptr;
+    std::uint64_t dispatches_ = 0;
+};
+
+}  // namespace
+
+// Factory hooks: the maintainer's create_compute_backend(ComputeBackendKind::Cuda)
+// returns nimbus_cuda_create_compute_backend(); a plugin loader can dlopen
+// this library and resolve the same symbol.
+extern "C" ComputeBackend* nimbus_cuda_create_compute_backend() { return new NimbusCudaComputeBackend(); }
+
+extern "C" void nimbus_cuda_destroy_compute_backend(ComputeBackend* backend) { delete backend; }

@@ -390,12 +390,16 @@ class ReferenceHarness:
         if rc != 0:
             raise RuntimeError(self.lib.ref_last_error().decode())
 
-    def acoustic_fused(self, st, rho0, p0, dt_small, grid, drho=None):
+    def acoustic_fused(self, st, rho0, p0, dt_small, grid, drho=None, backend=None):
+        """One fused substep through a ComputeBackend: the reference's CPU
+        backend, or the one a shared library's nimbus_cuda_create_compute_backend
+        makes (backend: its path)."""
         u, v, w, rho, p, th = (st[k] for k in ("u", "v", "w", "rho", "p", "theta"))
         nx, ny, nz = u.shape
         scratch = drho if drho is not None else np.zeros_like(u)
-        self._rc(self.lib.ref_acoustic_fused(
-            _fp(u), _fp(v), _fp(w), _fp(rho), _fp(p), _fp(th), _fp(rho0), _fp(p0), nx, ny, nz,
+        lib_path = None if backend is None else str(backend).encode()
+        self._rc(self.lib.ref_backend_acoustic_fused(
+            lib_path, _fp(u), _fp(v), _fp(w), _fp(rho), _fp(p), _fp(th), _fp(rho0), _fp(p0), nx, ny, nz,
             ctypes.c_double(grid[0]), ctypes.c_double(grid[1]), ctypes.c_double(grid[2]),
             ctypes.c_double(dt_small), _fp(scratch)))
 
@@ -478,16 +482,18 @@ class ReferenceHarness:
         a = np.ascontiguousarray(data, dtype=np.float32)
         self._rc(self.lib.ref_npy_write_3d(_fp(a), *[int(x) for x in a.shape], str(path).encode()))
 
-    def smagorinsky(self, st, dz, grid, sgs):
-        """SmagorinskyScheme::compute on the flat C-grid CPU path; same
-        outputs as Restatement.smagorinsky."""
+    def smagorinsky(self, st, dz, grid, sgs, backend=None):
+        """SmagorinskyScheme::compute on the flat C-grid: the CPU path, or
+        (backend: a shared library's path) the scheme's native path through
+        that library's ComputeBackend.  Same outputs as Restatement.smagorinsky."""
         u = st["u"]
         qv = st.get("qv")
         nx, ny, nz = u.shape
         out = {k: np.empty_like(u) for k in SGS_OUTPUTS}
         opened = (ctypes.c_int * 4)(*[int(x) for x in sgs.open_lateral])
-        self._rc(self.lib.ref_smagorinsky(
-            _fp(u), _fp(st["v"]), _fp(st["w"]), _fp(st["theta"]), _opt(qv), _fp(st["rho"]),
+        lib_path = None if backend is None else str(backend).encode()
+        self._rc(self.lib.ref_backend_smagorinsky(
+            lib_path, _fp(u), _fp(st["v"]), _fp(st["w"]), _fp(st["theta"]), _opt(qv), _fp(st["rho"]),
             _fp(np.ascontiguousarray(dz, dtype=np.float64)), nx, ny, nz, ctypes.c_double(grid[0]),
             ctypes.c_double(grid[1]), SGS_MODES[(int(sgs.use_horizontal), int(sgs.use_vertical))],
             int(sgs.filter_width == "dx"), int(sgs.periodic_x), int(sgs.periodic_y), opened,

@@ -42,6 +42,13 @@
 //   ref_sgs_apply           apply_admitted_sgs_substep, CPU path
 //                           (src/core/orchestration/dynamics/sgs_apply.cpp:436-956,1975-2029)
 //   ref_sgs_stability       compute_sgs_explicit_stability (sgs_apply.cpp:1483-1973)
+//   ref_backend_acoustic_fused, ref_backend_smagorinsky
+//                           the same reference calls with a ComputeBackend loaded
+//                           from a shared library (the CUDA backend's adapter,
+//                           nimbus_cuda_create_compute_backend): the reference's own
+//                           dispatch structs and, for the closure, its own
+//                           SmagorinskyScheme::compute routing to the backend
+//                           through dispatch_smagorinsky_fused_backend
 //   ref_scalar_transport    advect_scalars_conservative_3d_cartesian
 //                           (advection_cartesian.cpp:3532) on a retained context whose
 //                           face mass fluxes and beginning density are supplied
@@ -73,6 +80,8 @@
 #include "diagnostics/deterministic_reduction.hpp"
 #include "turbulence/schemes/smagorinsky/smagorinsky.hpp"
 
+#include <dlfcn.h>
+
 #include <cstring>
 #include <exception>
 #include <memory>
@@ -102,6 +111,19 @@ void to_field(Field3D& f, const float* src, int nx, int ny, int nz)
 void from_field(float* dst, const Field3D& f)
 {
     std::memcpy(dst, const_cast<Field3D&>(f).data(), sizeof(float) * f.size());
+}
+
+// A compute backend: the reference's CPU backend, or one created by the
+// factory symbol of a shared library (loaded once, never unloaded).
+std::unique_ptr<ComputeBackend> load_backend(const char* library)
+{
+    if (!library) return create_cpu_compute_backend();
+    void* handle = dlopen(library, RTLD_NOW | RTLD_LOCAL);
+    if (!handle) throw std::runtime_error(std::string("dlopen: ") + dlerror());
+    using Factory = ComputeBackend* (*)();
+    auto make = reinterpret_cast<Factory>(dlsym(handle, "nimbus_cuda_create_compute_backend"));
+    if (!make) throw std::runtime_error("library has no nimbus_cuda_create_compute_backend");
+    return std::unique_ptr<ComputeBackend>(make());
 }
 
 using tmv::init::config::BottomBC;
@@ -191,14 +213,15 @@ int ref_set_threads(int n)
 #endif
 }
 
-// One fused acoustic substep on host arrays, in place.
-int ref_acoustic_fused(float* u, float* v, float* w, float* rho, float* p, const float* theta,
-                       const double* rho0, const double* p0b, int nx, int ny, int nz,
-                       double dx, double dy, double dz, double dt_small, float* drho_scratch)
+// One fused acoustic substep on host arrays, in place, through `library`'s
+// backend (null: the reference's CPU backend).
+int ref_backend_acoustic_fused(const char* library, float* u, float* v, float* w, float* rho, float* p,
+                               const float* theta, const double* rho0, const double* p0b, int nx, int ny, int nz,
+                               double dx, double dy, double dz, double dt_small, float* drho_scratch)
 {
     try
     {
-        auto backend = create_cpu_compute_backend();
+        auto backend = load_backend(library);
         std::string err;
         if (!backend->initialize(err)) return fail(err.c_str());
         AcousticSubstepFusedCartesianCgridDispatch d;
@@ -214,13 +237,22 @@ int ref_acoustic_fused(float* u, float* v, float* w, float* rho, float* p, const
         d.gamma_host = dynamics_constants::gamma;
         d.drho_scratch = drho_scratch;
         if (!backend->dynamics_kernels()->dispatch_acoustic_substep_fused_cartesian_cgrid(d))
-            return fail("reference CPU backend refused the fused acoustic dispatch");
+            return fail("the backend refused the fused acoustic dispatch");
         return 0;
     }
     catch (const std::exception& e)
     {
         return fail(e.what());
     }
+}
+
+// The reference CPU backend's fused substep (see ref_backend_acoustic_fused).
+int ref_acoustic_fused(float* u, float* v, float* w, float* rho, float* p, const float* theta,
+                       const double* rho0, const double* p0b, int nx, int ny, int nz,
+                       double dx, double dy, double dz, double dt_small, float* drho_scratch)
+{
+    return ref_backend_acoustic_fused(nullptr, u, v, w, rho, p, theta, rho0, p0b, nx, ny, nz, dx, dy, dz, dt_small,
+                                      drho_scratch);
 }
 
 // The boundary closure alone: CartesianCGridBCScheme::apply_acoustic(dt_small)
@@ -294,7 +326,7 @@ int ref_acoustic_loop(float* u, float* v, float* w, float* rho, float* p, const 
             ctx.accumulate(L.view, f.rho, f.u, f.v, f.w, dt_small);
             auto d = make_fused(L, rho0, p0b, dt_small, scratch.data());
             if (!backend->dynamics_kernels()->dispatch_acoustic_substep_fused_cartesian_cgrid(d))
-                return fail("reference CPU backend refused the fused acoustic dispatch");
+                return fail("the backend refused the fused acoustic dispatch");
             bc->apply_acoustic(dt_small);
         }
         ctx.complete(L.view);
@@ -620,14 +652,26 @@ const char* const kSgsModes[3] = {"3d", "horizontal_only", "vertical_only"};
 // 2 vertical_only; filter 0 cubic_root, 1 dx; open: W, E, S, N.  qv may be
 // null.  Outputs: the coefficients (from the scheme's diagnostics) and the
 // five tendencies.
-int ref_smagorinsky(const float* u, const float* v, const float* w, const float* theta, const float* qv,
-                    const float* rho, const double* dz, int nx, int ny, int nz, double dx, double dy, int mode,
-                    int filter, int periodic_x, int periodic_y, const int* open, double Cs, double Pr_t, double Sc_t,
-                    double nu_max, double K_max, float* nu_t, float* K_theta, float* K_q, float* dudt, float* dvdt,
-                    float* dwdt, float* dthdt, float* dqvdt)
+int ref_backend_smagorinsky(const char* library, const float* u, const float* v, const float* w,
+                            const float* theta, const float* qv, const float* rho, const double* dz, int nx, int ny,
+                            int nz, double dx, double dy, int mode, int filter, int periodic_x, int periodic_y,
+                            const int* open, double Cs, double Pr_t, double Sc_t, double nu_max, double K_max,
+                            float* nu_t, float* K_theta, float* K_q, float* dudt, float* dvdt, float* dwdt,
+                            float* dthdt, float* dqvdt)
 {
     try
     {
+        // With a library, the scheme sees it as the level's active backend and
+        // takes its native path (smagorinsky.cpp:170-176,276-318).
+        ComputeBackendRuntimeState runtime;
+        if (library)
+        {
+            runtime.backend = load_backend(library);
+            std::string err;
+            if (!runtime.backend->initialize(err)) return fail(err.c_str());
+            runtime.active_kind = ComputeBackendKind::Vulkan;  // any accelerator kind
+            runtime.requested_kind = runtime.active_kind;
+        }
         Field3D fu, fv, fw, fth, fqv, frho;
         to_field(fu, u, nx, ny, nz);
         to_field(fv, v, nx, ny, nz);
@@ -651,6 +695,11 @@ int ref_smagorinsky(const float* u, const float* v, const float* w, const float*
         sv.periodic_x = periodic_x != 0;
         sv.periodic_y = periodic_y != 0;
         sv.open_lateral = {open[0] != 0, open[1] != 0, open[2] != 0, open[3] != 0};
+        if (library)
+        {
+            sv.compute_runtime = &runtime;
+            sv.require_native_dispatch = true;  // the scheme throws rather than fall back to its CPU path
+        }
         GridMetrics g;
         g.dx = dx;
         g.dy = dy;
@@ -685,6 +734,18 @@ int ref_smagorinsky(const float* u, const float* v, const float* w, const float*
     {
         return fail(e.what());
     }
+}
+
+// SmagorinskyScheme::compute on the reference's CPU path.
+int ref_smagorinsky(const float* u, const float* v, const float* w, const float* theta, const float* qv,
+                    const float* rho, const double* dz, int nx, int ny, int nz, double dx, double dy, int mode,
+                    int filter, int periodic_x, int periodic_y, const int* open, double Cs, double Pr_t, double Sc_t,
+                    double nu_max, double K_max, float* nu_t, float* K_theta, float* K_q, float* dudt, float* dvdt,
+                    float* dwdt, float* dthdt, float* dqvdt)
+{
+    return ref_backend_smagorinsky(nullptr, u, v, w, theta, qv, rho, dz, nx, ny, nz, dx, dy, mode, filter, periodic_x,
+                                   periodic_y, open, Cs, Pr_t, Sc_t, nu_max, K_max, nu_t, K_theta, K_q, dudt, dvdt,
+                                   dwdt, dthdt, dqvdt);
 }
 
 namespace

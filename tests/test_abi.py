@@ -70,6 +70,17 @@ def test_argument_block_layout_matches_header(struct_name, cls, tmp_path):
     assert offsets == [getattr(cls, f).offset for f in fields]
 
 
+def test_reference_backend_adapter_exports():
+    """The ComputeBackend adapter loads and exposes its factory hooks (no
+    backend is created here)."""
+    path = ROOT / "nimbus_b200" / "lib" / "libnimbus_reference_backend.so"
+    if not path.exists():
+        pytest.skip("adapter not built (no reference headers)")
+    lib = ctypes.CDLL(str(path))
+    assert hasattr(lib, "nimbus_cuda_create_compute_backend")
+    assert hasattr(lib, "nimbus_cuda_destroy_compute_backend")
+
+
 def test_no_device_is_an_error_not_a_fallback():
     import torch
     if torch.cuda.is_available():
