@@ -13,7 +13,8 @@
 // (compiled without FMA contraction): bit-identical to the CPU solver.  Every
 // stress or flux the reference carries along a column (its rolling lower
 // T13 / T23 / T33) is recomputed here from the same expression, which gives
-// the same binary64 value, so each cell is independent: one thread per cell.
+// the same binary64 value, so each cell is independent: one thread per cell;
+// within a cell the three corner edge stresses two faces share are formed once.
 #pragma once
 
 #include "stencil_common.cuh"
@@ -213,9 +214,57 @@ __device__ double sgs_scalar_rate(const SgsParams& P, const float* rho, const fl
     return div / A.f(rho, i, j, k);
 }
 
-// du/dt at x-face (i, j, k) (compute_momentum_diffusion_tendencies, first loop).
+// The stresses on the three edges that meet at cell (i, j, k)'s upper-east-
+// north corner, each used by two of the cell's faces with the same binary64
+// value: T12 on the xy edge (x-face i, y-face j), shared by du (its north
+// edge) and dv (its east edge); T13 on the xz edge (x-face i, z-face k),
+// shared by du (its upper edge) and dw (its east edge); T23 likewise on the
+// yz edge.  In each stress mode the reference's du / dw (dv / dw) forms of
+// T13 (T23) reduce to the same expression.
+__device__ __forceinline__ double sgs_t12(const SgsParams& P, const float* u, const float* v, const float* rho,
+                                          const float* nu, int i, int j, int k)
+{
+    const SgsAt A{P};
+    const int i1 = sgs_next(i, P.d.nx, P.px), j1 = sgs_next(j, P.d.ny, P.py);
+    const double s12 =
+        0.5 * ((A.f(u, i, j1, k) - A.f(u, i, j, k)) / P.dy + (A.f(v, i1, j, k) - A.f(v, i, j, k)) / P.dx);
+    return 2.0 * A.mu_xy(rho, nu, i, j, k) * s12;
+}
+
+__device__ __forceinline__ double sgs_t13(const SgsParams& P, const float* u, const float* w, const float* rho,
+                                          const float* nu, int i, int j, int k)
+{
+    const SgsAt A{P};
+    const int i1 = sgs_next(i, P.d.nx, P.px);
+    const double dwdx = (A.wf(w, i1, j, k) - A.wf(w, i, j, k)) / P.dx;
+    double grad = dwdx;
+    if (P.use_v)
+    {
+        const double dudz = (A.f(u, i, j, k + 1) - A.f(u, i, j, k)) / A.dzc(k);
+        grad = P.use_h ? dudz + dwdx : dudz;
+    }
+    return A.mu_z(rho, nu, i, j, i1, j, k) * grad;
+}
+
+__device__ __forceinline__ double sgs_t23(const SgsParams& P, const float* v, const float* w, const float* rho,
+                                          const float* nu, int i, int j, int k)
+{
+    const SgsAt A{P};
+    const int j1 = sgs_next(j, P.d.ny, P.py);
+    const double dwdy = (A.wf(w, i, j1, k) - A.wf(w, i, j, k)) / P.dy;
+    double grad = dwdy;
+    if (P.use_v)
+    {
+        const double dvdz = (A.f(v, i, j, k + 1) - A.f(v, i, j, k)) / A.dzc(k);
+        grad = P.use_h ? dvdz + dwdy : dvdz;
+    }
+    return A.mu_z(rho, nu, i, j, i, j1, k) * grad;
+}
+
+// du/dt at x-face (i, j, k) (compute_momentum_diffusion_tendencies, first
+// loop); t12 / t13: the shared corner stresses above.
 __device__ double sgs_du(const SgsParams& P, const float* u, const float* v, const float* w, const float* rho,
-                         const float* nu, int i, int j, int k)
+                         const float* nu, int i, int j, int k, double t12, double t13)
 {
     const SgsAt A{P};
     const int nx = P.d.nx, ny = P.d.ny;
@@ -226,43 +275,20 @@ __device__ double sgs_du(const SgsParams& P, const float* u, const float* v, con
         const double s_r = (A.f(u, ipp, j, k) - A.f(u, i, j, k)) / P.dx;
         const double s_l = (A.f(u, i, j, k) - A.f(u, imm, j, k)) / P.dx;
         div += (2.0 * A.mu(rho, nu, ipp, j, k) * s_r - 2.0 * A.mu(rho, nu, i, j, k) * s_l) / P.dx;
-        double t12[2];
-        const int jes[2] = {j, jmm};
-#pragma unroll
-        for (int e = 0; e < 2; ++e)
-        {
-            const int je = jes[e], je1 = sgs_next(je, ny, P.py);
-            const double s12 =
-                0.5 * ((A.f(u, i, je1, k) - A.f(u, i, je, k)) / P.dy + (A.f(v, ipp, je, k) - A.f(v, i, je, k)) / P.dx);
-            t12[e] = 2.0 * A.mu_xy(rho, nu, i, je, k) * s12;
-        }
-        div += (t12[0] - t12[1]) / P.dy;
+        div += (t12 - sgs_t12(P, u, v, rho, nu, i, jmm, k)) / P.dy;
     }
     if (P.use_v)
     {
         // T13 on the z-faces k (upper) and k-1 (lower; zero at the ground).
-        double t13[2];
-#pragma unroll
-        for (int e = 0; e < 2; ++e)
-        {
-            const int ke = k - e;
-            if (ke < 0)
-            {
-                t13[e] = 0.0;
-                continue;
-            }
-            const double dudz = (A.f(u, i, j, ke + 1) - A.f(u, i, j, ke)) / A.dzc(ke);
-            const double grad = P.use_h ? dudz + (A.wf(w, ipp, j, ke) - A.wf(w, i, j, ke)) / P.dx : dudz;
-            t13[e] = A.mu_z(rho, nu, i, j, ipp, j, ke) * grad;
-        }
-        div += (t13[0] - t13[1]) / P.dz[k];
+        const double lower = k > 0 ? sgs_t13(P, u, w, rho, nu, i, j, k - 1) : 0.0;
+        div += (t13 - lower) / P.dz[k];
     }
     return div / (0.5 * (A.f(rho, i, j, k) + A.f(rho, ipp, j, k)));
 }
 
 // dv/dt at y-face (i, j, k) (second loop).
 __device__ double sgs_dv(const SgsParams& P, const float* u, const float* v, const float* w, const float* rho,
-                         const float* nu, int i, int j, int k)
+                         const float* nu, int i, int j, int k, double t12, double t23)
 {
     const SgsAt A{P};
     const int nx = P.d.nx, ny = P.d.ny;
@@ -273,35 +299,12 @@ __device__ double sgs_dv(const SgsParams& P, const float* u, const float* v, con
         const double s_n = (A.f(v, i, jpp, k) - A.f(v, i, j, k)) / P.dy;
         const double s_s = (A.f(v, i, j, k) - A.f(v, i, jmm, k)) / P.dy;
         div += (2.0 * A.mu(rho, nu, i, jpp, k) * s_n - 2.0 * A.mu(rho, nu, i, j, k) * s_s) / P.dy;
-        double t21[2];
-        const int ies[2] = {i, imm};
-#pragma unroll
-        for (int e = 0; e < 2; ++e)
-        {
-            const int ie = ies[e], ie1 = sgs_next(ie, nx, P.px);
-            const double s12 = 0.5 * ((A.f(u, ie, jpp, k) - A.f(u, ie, j, k)) / P.dy +
-                                      (A.f(v, ie1, j, k) - A.f(v, ie, j, k)) / P.dx);
-            t21[e] = 2.0 * A.mu_xy(rho, nu, ie, j, k) * s12;
-        }
-        div += (t21[0] - t21[1]) / P.dx;
+        div += (t12 - sgs_t12(P, u, v, rho, nu, imm, j, k)) / P.dx;
     }
     if (P.use_v)
     {
-        double t23[2];
-#pragma unroll
-        for (int e = 0; e < 2; ++e)
-        {
-            const int ke = k - e;
-            if (ke < 0)
-            {
-                t23[e] = 0.0;
-                continue;
-            }
-            const double dvdz = (A.f(v, i, j, ke + 1) - A.f(v, i, j, ke)) / A.dzc(ke);
-            const double grad = P.use_h ? dvdz + (A.wf(w, i, jpp, ke) - A.wf(w, i, j, ke)) / P.dy : dvdz;
-            t23[e] = A.mu_z(rho, nu, i, j, i, jpp, ke) * grad;
-        }
-        div += (t23[0] - t23[1]) / P.dz[k];
+        const double lower = k > 0 ? sgs_t23(P, v, w, rho, nu, i, j, k - 1) : 0.0;
+        div += (t23 - lower) / P.dz[k];
     }
     return div / (0.5 * (A.f(rho, i, j, k) + A.f(rho, i, jpp, k)));
 }
@@ -309,11 +312,10 @@ __device__ double sgs_dv(const SgsParams& P, const float* u, const float* v, con
 // dw/dt at z-face (i, j, k) (third loop): stress divergence over the dual
 // column mass.
 __device__ double sgs_dw(const SgsParams& P, const float* u, const float* v, const float* w, const float* rho,
-                         const float* nu, int i, int j, int k)
+                         const float* nu, int i, int j, int k, double t13, double t23)
 {
     const SgsAt A{P};
-    const int nx = P.d.nx, ny = P.d.ny;
-    const int imm = sgs_prev(i, nx, P.px), jmm = sgs_prev(j, ny, P.py);
+    const int imm = sgs_prev(i, P.d.nx, P.px), jmm = sgs_prev(j, P.d.ny, P.py);
     const double dzb = P.dz[k], dzt = P.dz[k + 1], dzd = A.dzc(k);
     const double mass = 0.5 * (A.f(rho, i, j, k) * dzb + A.f(rho, i, j, k + 1) * dzt);
     double force = 0.0;
@@ -325,22 +327,8 @@ __device__ double sgs_dw(const SgsParams& P, const float* u, const float* v, con
     }
     if (P.use_h)
     {
-        double t31[2], t32[2];
-        const int ies[2] = {i, imm}, jes[2] = {j, jmm};
-#pragma unroll
-        for (int e = 0; e < 2; ++e)
-        {
-            const int ie = ies[e], ie1 = sgs_next(ie, nx, P.px);
-            const double dwdx = (A.wf(w, ie1, j, k) - A.wf(w, ie, j, k)) / P.dx;
-            const double gx = P.use_v ? (A.f(u, ie, j, k + 1) - A.f(u, ie, j, k)) / dzd + dwdx : dwdx;
-            t31[e] = A.mu_z(rho, nu, ie, j, ie1, j, k) * gx;
-            const int je = jes[e], je1 = sgs_next(je, ny, P.py);
-            const double dwdy = (A.wf(w, i, je1, k) - A.wf(w, i, je, k)) / P.dy;
-            const double gy = P.use_v ? (A.f(v, i, je, k + 1) - A.f(v, i, je, k)) / dzd + dwdy : dwdy;
-            t32[e] = A.mu_z(rho, nu, i, je, i, je1, k) * gy;
-        }
-        force += dzd * (t31[0] - t31[1]) / P.dx;
-        force += dzd * (t32[0] - t32[1]) / P.dy;
+        force += dzd * (t13 - sgs_t13(P, u, w, rho, nu, imm, j, k)) / P.dx;
+        force += dzd * (t23 - sgs_t23(P, v, w, rho, nu, i, jmm, k)) / P.dy;
     }
     return force / mass;
 }
@@ -365,9 +353,14 @@ __global__ void __launch_bounds__(256, 4) sgs_tendencies_kernel(
         float ru = 0.0f, rv = 0.0f, rw = 0.0f, rt = 0.0f, rq = 0.0f;
         if (column && below_lid)
         {
-            if (i <= (P.px ? nx - 2 : nx - 3)) ru = (float)sgs_du(P, u, v, w, rho, nu_t, i, j, k);
-            if (j <= (P.py ? ny - 2 : ny - 3)) rv = (float)sgs_dv(P, u, v, w, rho, nu_t, i, j, k);
-            rw = (float)sgs_dw(P, u, v, w, rho, nu_t, i, j, k);
+            const bool du_on = i <= (P.px ? nx - 2 : nx - 3);
+            const bool dv_on = j <= (P.py ? ny - 2 : ny - 3);
+            const double t12 = P.use_h && (du_on || dv_on) ? sgs_t12(P, u, v, rho, nu_t, i, j, k) : 0.0;
+            const double t13 = (du_on && P.use_v) || P.use_h ? sgs_t13(P, u, w, rho, nu_t, i, j, k) : 0.0;
+            const double t23 = (dv_on && P.use_v) || P.use_h ? sgs_t23(P, v, w, rho, nu_t, i, j, k) : 0.0;
+            if (du_on) ru = (float)sgs_du(P, u, v, w, rho, nu_t, i, j, k, t12, t13);
+            if (dv_on) rv = (float)sgs_dv(P, u, v, w, rho, nu_t, i, j, k, t12, t23);
+            rw = (float)sgs_dw(P, u, v, w, rho, nu_t, i, j, k, t13, t23);
         }
         if (column)
         {
