@@ -13,6 +13,13 @@
 //   AcousticSubstepFusedCartesianCgrid  the dispatch carries the CPU solver's
 //       FP64 profiles and spacings (rho0_base_host, dx_host, ...): the result
 //       is the CPU backend's, bit for bit.
+//   AcousticSubstepsBatchedCartesianCgrid  the whole acoustic loop of a large
+//       step (split_explicit.cpp's GPU route); this dispatch carries only FP32
+//       base profiles, spacings and dt_small, which are widened to FP64, so the
+//       result is the C-ABI's on those widened values (and differs from the
+//       CPU loop by that FP32 narrowing of its inputs, as the reference's own
+//       accelerator backends do).  A dispatch that turns the state repairs
+//       off, or accumulates mass flux without a positive weight, is declined.
 //   Smagorinsky (dispatch_smagorinsky_fused)  the bridge passes FP32 copies of
 //       dz, dx, dy and the closure constants (src/compute/dispatch/turbulence.cpp:87-146);
 //       they are widened to FP64, so the result equals the CPU scheme's
@@ -70,8 +77,11 @@ public:
 
     bool supports(DynamicsKernelOp op) const override
     {
-        return op == DynamicsKernelOp::AcousticSubstepFusedCartesianCgrid;
+        return op == DynamicsKernelOp::AcousticSubstepFusedCartesianCgrid ||
+               op == DynamicsKernelOp::AcousticSubstepsBatchedCartesianCgrid;
     }
+
+    bool supports_batched_cartesian_cgrid_mass_flux_export() const override { return true; }
 
     bool supports(TurbulenceKernelOp op) const override
     {
@@ -109,6 +119,65 @@ public:
         a.drho_scratch = d.drho_scratch;
         a.memory = NIMBUS_MEMORY_HOST;
         return count(nimbus_cuda_acoustic_fused(ctx_, &a));
+    }
+
+    bool dispatch_acoustic_substeps_batched_cartesian_cgrid(const AcousticSubstepsBatchedCartesianCgridDispatch& d) override
+    {
+        if (!ctx_ || !d.rho0_base_data || !d.p0_base_data || d.nz < 1 || d.base_len < d.nz || !d.repair_primary_state)
+            return false;
+        if (d.accumulate_mass_flux && !(d.mass_flux_weight > 0.0)) return false;
+        std::vector<double> rho0(d.rho0_base_data, d.rho0_base_data + d.nz);
+        std::vector<double> p0(d.p0_base_data, d.p0_base_data + d.nz);
+        std::vector<float> wave_out;
+        float* wave_output = d.wave_history_output;
+        if (!wave_output)
+        {
+            wave_out.assign(2 * (static_cast<size_t>(d.nx) + d.ny) * d.nz, 0.0f);
+            wave_output = wave_out.data();
+        }
+        nimbus_acoustic_batched_args a{};
+        a.u = d.u;
+        a.v = d.v;
+        a.w = d.w;
+        a.rho = d.rho;
+        a.p = d.p;
+        a.theta = d.theta_data;
+        a.rho0_base = rho0.data();
+        a.p0_base = p0.data();
+        a.base_len = d.nz;
+        a.nx = d.nx;
+        a.ny = d.ny;
+        a.nz = d.nz;
+        a.dx = d.dx;
+        a.dy = d.dy;
+        a.dz = d.dz;
+        a.dt_small = d.dt_small;
+        a.n_substeps = d.n_substeps;
+        a.gamma = d.gamma_val;
+        a.rho_min = d.rho_min;
+        a.rho_max = d.rho_max;
+        a.p_min = d.p_min;
+        a.p_max = d.p_max;
+        a.p_ref_fallback = d.p_ref_fallback;
+        a.wind_clamp_h = d.wind_clamp_h;
+        a.wind_clamp_v = d.wind_clamp_v;
+        a.bc_west = d.bc_west;
+        a.bc_east = d.bc_east;
+        a.bc_south = d.bc_south;
+        a.bc_north = d.bc_north;
+        a.bc_bottom = d.bc_bottom;
+        a.bc_top = d.bc_top;
+        a.mass_flux_x = d.mass_flux_x;
+        a.mass_flux_y = d.mass_flux_y;
+        a.mass_flux_z = d.mass_flux_z;
+        a.accumulate_mass_flux = d.accumulate_mass_flux;
+        a.mass_flux_weight = d.mass_flux_weight;
+        a.frame_velocity_u_ms = d.frame_velocity_u_ms;
+        a.frame_velocity_v_ms = d.frame_velocity_v_ms;
+        a.wave_history = d.wave_history;
+        a.wave_history_output = wave_output;
+        a.memory = NIMBUS_MEMORY_HOST;
+        return count(nimbus_cuda_acoustic_batched(ctx_, &a));
     }
 
     bool dispatch_smagorinsky_fused(const SmagorinskyFusedDispatch& d) override

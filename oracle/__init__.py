@@ -126,6 +126,23 @@ class Restatement:
         if rc != 0:
             raise MemoryError("oracle slow-step scratch allocation failed")
 
+    def acoustic_batched(self, st, rho0, p0, dt_small, n_substeps, grid, bc, backend, wave_in=None):
+        """The acoustic loop as one AcousticSubstepsBatchedCartesianCgridDispatch
+        (FP32 profiles, spacings and dt_small) through the ComputeBackend of
+        the shared library at `backend`, in place; returns the mass fluxes and
+        the KW78 history."""
+        u, v, w, rho, p, th = (st[k] for k in ("u", "v", "w", "rho", "p", "theta"))
+        nx, ny, nz = u.shape
+        out = {k: np.zeros_like(u) for k in ("mfx", "mfy", "mfz")}
+        out["wave"] = np.zeros(2 * (nx + ny) * nz, np.float32)
+        bcs = (ctypes.c_int * 6)(*[int(x) for x in bc])
+        self._rc(self.lib.ref_backend_acoustic_batched(
+            str(backend).encode(), _fp(u), _fp(v), _fp(w), _fp(rho), _fp(p), _fp(th), _fp(rho0), _fp(p0), nx, ny,
+            nz, ctypes.c_double(grid[0]), ctypes.c_double(grid[1]), ctypes.c_double(grid[2]),
+            ctypes.c_double(dt_small), int(n_substeps), bcs, _fp(out["mfx"]), _fp(out["mfy"]), _fp(out["mfz"]),
+            _opt(wave_in), _fp(out["wave"])))
+        return out
+
     def kessler_tendencies(self, st, dz, dt, domain):
         th, p, rho, qv, qc, qr = (st[k] for k in ("theta", "p", "rho", "qv", "qc", "qr"))
         self._chk(th, p, rho, qv, qc, qr)
@@ -413,6 +430,23 @@ class ReferenceHarness:
             ctypes.c_double(grid[0]), ctypes.c_double(grid[1]), ctypes.c_double(grid[2]),
             ctypes.c_double(dt_large), int(n_substeps), *[int(x) for x in bc],
             _fp(out["mfx"]), _fp(out["mfy"]), _fp(out["mfz"]), _fp(out["rho_begin"]), _fp(out["wave"])))
+        return out
+
+    def acoustic_batched(self, st, rho0, p0, dt_small, n_substeps, grid, bc, backend, wave_in=None):
+        """The acoustic loop as one AcousticSubstepsBatchedCartesianCgridDispatch
+        (FP32 profiles, spacings and dt_small) through the ComputeBackend of
+        the shared library at `backend`, in place; returns the mass fluxes and
+        the KW78 history."""
+        u, v, w, rho, p, th = (st[k] for k in ("u", "v", "w", "rho", "p", "theta"))
+        nx, ny, nz = u.shape
+        out = {k: np.zeros_like(u) for k in ("mfx", "mfy", "mfz")}
+        out["wave"] = np.zeros(2 * (nx + ny) * nz, np.float32)
+        bcs = (ctypes.c_int * 6)(*[int(x) for x in bc])
+        self._rc(self.lib.ref_backend_acoustic_batched(
+            str(backend).encode(), _fp(u), _fp(v), _fp(w), _fp(rho), _fp(p), _fp(th), _fp(rho0), _fp(p0), nx, ny,
+            nz, ctypes.c_double(grid[0]), ctypes.c_double(grid[1]), ctypes.c_double(grid[2]),
+            ctypes.c_double(dt_small), int(n_substeps), bcs, _fp(out["mfx"]), _fp(out["mfy"]), _fp(out["mfz"]),
+            _opt(wave_in), _fp(out["wave"])))
         return out
 
     def kessler_tendencies(self, st, dz, dt, domain):

@@ -42,7 +42,7 @@
 //   ref_sgs_apply           apply_admitted_sgs_substep, CPU path
 //                           (src/core/orchestration/dynamics/sgs_apply.cpp:436-956,1975-2029)
 //   ref_sgs_stability       compute_sgs_explicit_stability (sgs_apply.cpp:1483-1973)
-//   ref_backend_acoustic_fused, ref_backend_smagorinsky
+//   ref_backend_acoustic_fused, ref_backend_acoustic_batched, ref_backend_smagorinsky
 //                           the same reference calls with a ComputeBackend loaded
 //                           from a shared library (the CUDA backend's adapter,
 //                           nimbus_cuda_create_compute_backend): the reference's own
@@ -238,6 +238,53 @@ int ref_backend_acoustic_fused(const char* library, float* u, float* v, float* w
         d.drho_scratch = drho_scratch;
         if (!backend->dynamics_kernels()->dispatch_acoustic_substep_fused_cartesian_cgrid(d))
             return fail("the backend refused the fused acoustic dispatch");
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        return fail(e.what());
+    }
+}
+
+// The whole acoustic loop of a large step through `library`'s backend as the
+// reference's accelerator route hands it over: an
+// AcousticSubstepsBatchedCartesianCgridDispatch with FP32 base profiles,
+// spacings and dt_small (narrowed here from the FP64 inputs), the strict
+// contract's KW78 history in and out and the mass-flux weight 1/n.
+int ref_backend_acoustic_batched(const char* library, float* u, float* v, float* w, float* rho, float* p,
+                                 const float* theta, const double* rho0, const double* p0b, int nx, int ny, int nz,
+                                 double dx, double dy, double dz, double dt_small, int n_substeps, const int* bc,
+                                 float* mfx, float* mfy, float* mfz, const float* wave_in, float* wave_out)
+{
+    try
+    {
+        auto backend = load_backend(library);
+        std::string err;
+        if (!backend->initialize(err)) return fail(err.c_str());
+        std::vector<float> r0(rho0, rho0 + nz), pb(p0b, p0b + nz);
+        AcousticSubstepsBatchedCartesianCgridDispatch d;
+        d.u = u; d.v = v; d.w = w; d.rho = rho; d.p = p; d.theta_data = theta;
+        d.rho0_base_data = r0.data(); d.p0_base_data = pb.data(); d.base_len = nz;
+        d.nx = nx; d.ny = ny; d.nz = nz;
+        d.dx = static_cast<float>(dx); d.dy = static_cast<float>(dy); d.dz = static_cast<float>(dz);
+        d.gamma_val = static_cast<float>(dynamics_constants::gamma);
+        d.dt_small = static_cast<float>(dt_small); d.n_substeps = n_substeps;
+        d.rho_min = density_min_kgm3; d.rho_max = density_max_kgm3;
+        d.p_min = pressure_min_pa; d.p_max = pressure_max_pa;
+        d.p_ref_fallback = static_cast<float>(p0);
+        d.wind_clamp_h = wind_horizontal_abs_max_ms; d.wind_clamp_v = wind_vertical_abs_max_ms;
+        d.bc_west = bc[0]; d.bc_east = bc[1]; d.bc_south = bc[2]; d.bc_north = bc[3];
+        d.bc_bottom = bc[4]; d.bc_top = bc[5];
+        d.mass_flux_x = mfx; d.mass_flux_y = mfy; d.mass_flux_z = mfz;
+        d.accumulate_mass_flux = true;
+        d.mass_flux_weight = 1.0 / n_substeps;
+        d.wave_history = wave_in;
+        d.wave_history_output = wave_out;
+        if (!backend->dynamics_kernels() ||
+            !backend->dynamics_kernels()->supports(DynamicsKernelOp::AcousticSubstepsBatchedCartesianCgrid))
+            return fail("the backend does not offer the batched acoustic loop");
+        if (!backend->dynamics_kernels()->dispatch_acoustic_substeps_batched_cartesian_cgrid(d))
+            return fail("the backend refused the batched acoustic dispatch");
         return 0;
     }
     catch (const std::exception& e)

@@ -12,6 +12,7 @@ import pytest
 import oracle
 from nimbus_b200.initial import Case, cloudy_state, perturbed_state
 from nimbus_b200.sgs import SgsConfig
+from tests.golden.make_golden import close_walls
 
 pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not oracle.reference_available(),
                                                    reason="reference harness not built")]
@@ -69,3 +70,44 @@ def test_smagorinsky_scheme_takes_the_cuda_backend(ref, bc, kw):
     gpu = ref.smagorinsky(st, dz, grid, cfg, backend=ADAPTER)
     for k in cpu:
         assert np.array_equal(bits(cpu[k]), bits(gpu[k])), k
+
+
+@pytest.mark.parametrize("bc", [(1, 1, 1, 1, 1, 0), (0, 0, 2, 3, 0, 2)])
+def test_batched_loop_through_the_reference_interface(ref, bc):
+    """AcousticSubstepsBatchedCartesianCgridDispatch (the reference's
+    accelerator route for the acoustic loop) through the adapter.  The
+    dispatch carries FP32 profiles, spacings and dt_small: the adapter's
+    result equals the C-ABI loop given those values widened to FP64, bit for
+    bit, and the reference's CPU loop within the FP32 narrowing of its inputs."""
+    from nimbus_b200 import cuda
+
+    case = Case(36, 30, 20, 1000.0, 1000.0, 500.0, 6.0, seed=5, bc=bc)
+    st, base = perturbed_state(case, seed=5)
+    close_walls(st, bc)  # rigid walls start impermeable, as the solver's initial closure leaves them
+    n, dt = 6, 6.0
+    grid = (case.dx, case.dy, case.dz)
+    got = {k: v.copy() for k, v in st.items()}
+    out = ref.acoustic_batched(got, base["rho0"], base["p0"], dt / n, n, grid, bc, ADAPTER)
+    # The same loop through the C-ABI on the widened FP32 inputs.
+    ctx = cuda.Context(0)
+    want = {k: v.copy() for k, v in st.items()}
+    widen = lambda x: np.asarray(x, np.float32).astype(np.float64)  # noqa: E731
+    mf = [np.zeros(case.shape, np.float32) for _ in range(3)]
+    wave = np.zeros(2 * (case.nx + case.ny) * case.nz, np.float32)
+    args = cuda.batched_args(want, widen(base["rho0"]), widen(base["p0"]), float(np.float32(dt / n)), n,
+                             tuple(float(np.float32(g)) for g in grid), bc, *mf, 1.0 / n, None, wave)
+    args.gamma = float(np.float32(args.gamma))
+    ctx.check(ctx.acoustic_batched(args))
+    ctx.close()
+    for k in ("u", "v", "w", "rho", "p"):
+        assert np.array_equal(bits(got[k]), bits(want[k])), k
+    for k, m in zip(("mfx", "mfy", "mfz"), mf):
+        assert np.array_equal(bits(out[k]), bits(m)), k
+    assert np.array_equal(bits(out["wave"]), bits(wave))
+    # Against the reference's CPU loop on the FP64 inputs.
+    cpu = {k: v.copy() for k, v in st.items()}
+    ref.acoustic_loop(cpu, base["rho0"], base["p0"], dt, n, grid, bc)
+    for k in ("u", "v", "w", "rho", "p"):
+        a, b = got[k].astype(np.float64), cpu[k].astype(np.float64)
+        scale = max(np.abs(b).max(), 1e-30)
+        assert np.abs(a - b).max() <= 1e-4 * scale, (k, np.abs(a - b).max(), scale)
