@@ -454,6 +454,14 @@ def sgs_study(ctx, device):
     ctx.synchronize()
     peak, kind = load_peaks()
     achieved = 92.0 * case.cells / (c_ms / 1e3) / 1e9
+    # The FP32 form of the closure (same call on an FP32-precision context).
+    ctx.set_precision(cuda.PRECISION_FP32)
+    ctx.check(ctx.smagorinsky_fused(closure))
+    f_ms = time_on_stream(torch, stream, lambda: ctx.check(ctx.smagorinsky_fused(closure)), calls) / calls
+    ctx.synchronize()
+    ctx.set_precision(cuda.PRECISION_REFERENCE)
+    ctx.check(ctx.smagorinsky_fused(closure))
+    ctx.synchronize()
     stab_args = cuda.smagorinsky_args(dev, dz, grid, cfg, rates={k: closure.outputs[k] for k in cuda.SGS_RATES},
                                       memory=cuda.MEMORY_DEVICE)
     ctx.sgs_stability(stab_args)
@@ -485,6 +493,8 @@ def sgs_study(ctx, device):
     return {"grid": list(case.shape), "cells": case.cells, "precision": "reference (FP64 arithmetic, FP32 storage)",
             "closure": {"ms_per_call": c_ms, "achieved_gbs": achieved, "peak_gbs": peak, "frac": achieved / peak,
                         "peak_kind": kind, "algorithmic_bytes_per_cell": 92},
+            "closure_fp32": {"ms_per_call": f_ms, "achieved_gbs": 92.0 * case.cells / (f_ms / 1e3) / 1e9,
+                             "frac": 92.0 * case.cells / (f_ms / 1e3) / 1e9 / peak},
             "stability": {"ms_per_call": s_ms, "limit_s": limits["maximum"],
                           "note": "wall time incl. one host synchronisation; slab sums are serial per x-slab"},
             "apply": {"ms_per_call": a_ms, "algorithmic_bytes_per_cell": 60},

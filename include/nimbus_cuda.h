@@ -523,6 +523,10 @@ nimbus_status nimbus_cuda_acoustic_boundaries(nimbus_cuda_context* ctx, const ni
  * the host (sqrt(dx dy) or cbrt(dx dy dz_k), the C library's functions, as
  * compute_filter_width calls them, eddy_viscosity.cpp:1414-1468).
  *
+ * On a context in NIMBUS_PRECISION_FP32 the closure (coefficients and
+ * tendencies) computes in FP32 instead: within 1e-6 relative of the FP64
+ * result; the apply and the stability limit stay FP64.
+ *
  * nimbus_cuda_smagorinsky_fused replaces dispatch_smagorinsky_fused: eddy
  * coefficients of every cell (nu = Cs^2 Delta^2 |S| capped at nu_t_max;
  * K_theta = nu / Pr_t, K_q = nu / Sc_t capped at K_max), then the

@@ -90,10 +90,20 @@ nimbus_status launch_closure(nimbus_cuda_context* ctx, cudaStream_t st, const Sg
 {
     const int grid = grid_for(ctx, P.d.cells());
     LaunchTimer t(ctx, st, NIMBUS_KERNEL_SGS);
-    sgs_coefficients_kernel<<<grid, kThreads, 0, st>>>(P, D.u, D.v, D.w, D.theta, D.qv, D.rho, D.nu, D.kt, D.kq,
-                                                       status);
-    sgs_tendencies_kernel<<<grid, kThreads, 0, st>>>(P, D.u, D.v, D.w, D.theta, D.qv, D.rho, D.nu, D.kt, D.kq, D.du,
-                                                     D.dv, D.dw, D.dth, D.dqv);
+    if (ctx->precision == NIMBUS_PRECISION_FP32)
+    {
+        sgs_coefficients_kernel<float><<<grid, kThreads, 0, st>>>(P, D.u, D.v, D.w, D.theta, D.qv, D.rho, D.nu,
+                                                                  D.kt, D.kq, status);
+        sgs_tendencies_kernel<float><<<grid, kThreads, 0, st>>>(P, D.u, D.v, D.w, D.theta, D.qv, D.rho, D.nu, D.kt,
+                                                                D.kq, D.du, D.dv, D.dw, D.dth, D.dqv);
+    }
+    else
+    {
+        sgs_coefficients_kernel<double><<<grid, kThreads, 0, st>>>(P, D.u, D.v, D.w, D.theta, D.qv, D.rho, D.nu,
+                                                                   D.kt, D.kq, status);
+        sgs_tendencies_kernel<double><<<grid, kThreads, 0, st>>>(P, D.u, D.v, D.w, D.theta, D.qv, D.rho, D.nu, D.kt,
+                                                                 D.kq, D.du, D.dv, D.dw, D.dth, D.dqv);
+    }
     ctx->launches += 2;
     NB_CUDA(ctx, cudaGetLastError());
     return NIMBUS_OK;

@@ -10,7 +10,9 @@
 // (src/core/orchestration/dynamics/sgs_apply.cpp:436-956,1483-1973).
 //
 // FP64 arithmetic over FP32 storage in the reference's operation order
-// (compiled without FMA contraction): bit-identical to the CPU solver.  Every
+// (compiled without FMA contraction): bit-identical to the CPU solver.  The
+// closure kernels are templated on their arithmetic type R: R = double is that
+// reference form, R = float the FP32 form (same operations in FP32).  Every
 // stress or flux the reference carries along a column (its rolling lower
 // T13 / T23 / T33) is recomputed here from the same expression, which gives
 // the same binary64 value, so each cell is independent: one thread per cell;
@@ -48,52 +50,54 @@ __device__ __forceinline__ int sgs_next(int i, int n, int periodic)
     return i >= n - 2 ? 1 : (i + 1 > 1 ? i + 1 : 1);
 }
 
+template <class R>
 struct SgsAt
 {
     const SgsParams& P;
     __device__ __forceinline__ int at(int i, int j, int k) const { return P.d.at(i, j, k); }
-    __device__ __forceinline__ double f(const float* x, int i, int j, int k) const
+    __device__ __forceinline__ R f(const float* x, int i, int j, int k) const
     {
-        return (double)__ldg(x + at(i, j, k));
+        return (R)__ldg(x + at(i, j, k));
     }
     // w with the implicit ground face w[-1] = 0.
-    __device__ __forceinline__ double wf(const float* w, int i, int j, int k) const
+    __device__ __forceinline__ R wf(const float* w, int i, int j, int k) const
     {
-        return k < 0 ? 0.0 : f(w, i, j, k);
+        return k < 0 ? R(0.0) : f(w, i, j, k);
     }
-    __device__ __forceinline__ double dzc(int k) const { return 0.5 * (P.dz[k] + P.dz[k + 1]); }
+    __device__ __forceinline__ R dzc(int k) const { return R(0.5) * (R(P.dz[k]) + R(P.dz[k + 1])); }
     // mu = rho nu at a centre; on an xy edge (four-point mean); on an xz or yz
     // edge (pair means of the two levels, weighted by the other level's
     // thickness).
-    __device__ __forceinline__ double mu(const float* rho, const float* nu, int i, int j, int k) const
+    __device__ __forceinline__ R mu(const float* rho, const float* nu, int i, int j, int k) const
     {
         return f(rho, i, j, k) * f(nu, i, j, k);
     }
-    __device__ __forceinline__ double mu_xy(const float* rho, const float* nu, int i, int j, int k) const
+    __device__ __forceinline__ R mu_xy(const float* rho, const float* nu, int i, int j, int k) const
     {
         const int i1 = sgs_next(i, P.d.nx, P.px), j1 = sgs_next(j, P.d.ny, P.py);
-        return 0.25 * (mu(rho, nu, i, j, k) + mu(rho, nu, i1, j, k) + mu(rho, nu, i, j1, k) + mu(rho, nu, i1, j1, k));
+        return R(0.25) * (mu(rho, nu, i, j, k) + mu(rho, nu, i1, j, k) + mu(rho, nu, i, j1, k) + mu(rho, nu, i1, j1, k));
     }
-    __device__ __forceinline__ double mu_z(const float* rho, const float* nu, int i, int j, int i1, int j1,
+    __device__ __forceinline__ R mu_z(const float* rho, const float* nu, int i, int j, int i1, int j1,
                                            int k) const
     {
-        const double lo = 0.5 * (mu(rho, nu, i, j, k) + mu(rho, nu, i1, j1, k));
-        const double up = 0.5 * (mu(rho, nu, i, j, k + 1) + mu(rho, nu, i1, j1, k + 1));
-        return (P.dz[k + 1] * lo + P.dz[k] * up) / (P.dz[k] + P.dz[k + 1]);
+        const R lo = R(0.5) * (mu(rho, nu, i, j, k) + mu(rho, nu, i1, j1, k));
+        const R up = R(0.5) * (mu(rho, nu, i, j, k + 1) + mu(rho, nu, i1, j1, k + 1));
+        return (R(P.dz[k + 1]) * lo + R(P.dz[k]) * up) / (R(P.dz[k]) + R(P.dz[k + 1]));
     }
 };
 
 // Strain-rate square at a scalar centre (compute_directional_strain_sq_centered).
-__device__ double sgs_strain_sq(const SgsParams& P, const float* u, const float* v, const float* w, int i, int j,
+template <class R>
+__device__ R sgs_strain_sq(const SgsParams& P, const float* u, const float* v, const float* w, int i, int j,
                                 int k)
 {
-    const SgsAt A{P};
+    const SgsAt<R> A{P};
     const int nx = P.d.nx, ny = P.d.ny, nz = P.d.nz;
     const int jm = sgs_prev(j, ny, P.py), im = sgs_prev(i, nx, P.px);
-    const double s11 = (A.f(u, i, j, k) - A.f(u, im, j, k)) / P.dx;
-    const double s22 = (A.f(v, i, j, k) - A.f(v, i, jm, k)) / P.dy;
-    const double s33 = (A.wf(w, i, j, k) - A.wf(w, i, j, k - 1)) / P.dz[k];
-    double s12[4];
+    const R s11 = (A.f(u, i, j, k) - A.f(u, im, j, k)) / R(P.dx);
+    const R s22 = (A.f(v, i, j, k) - A.f(v, i, jm, k)) / R(P.dy);
+    const R s33 = (A.wf(w, i, j, k) - A.wf(w, i, j, k - 1)) / R(P.dz[k]);
+    R s12[4];
     {
         const int ie[4] = {im, im, i, i}, je[4] = {jm, j, jm, j};
 #pragma unroll
@@ -101,12 +105,12 @@ __device__ double sgs_strain_sq(const SgsParams& P, const float* u, const float*
         {
             const int ii = ie[e], jj = je[e];
             const int jj1 = sgs_next(jj, ny, P.py), ii1 = sgs_next(ii, nx, P.px);
-            const double dudy = (A.f(u, ii, jj1, k) - A.f(u, ii, jj, k)) / P.dy;
-            const double dvdx = (A.f(v, ii1, jj, k) - A.f(v, ii, jj, k)) / P.dx;
-            s12[e] = 0.5 * (dudy + dvdx);
+            const R dudy = (A.f(u, ii, jj1, k) - A.f(u, ii, jj, k)) / R(P.dy);
+            const R dvdx = (A.f(v, ii1, jj, k) - A.f(v, ii, jj, k)) / R(P.dx);
+            s12[e] = R(0.5) * (dudy + dvdx);
         }
     }
-    double xz0[4], xz1[4], yz0[4], yz1[4];
+    R xz0[4], xz1[4], yz0[4], yz1[4];
     {
         const int xi[4] = {im, im, i, i}, yj[4] = {jm, jm, j, j}, ke[4] = {k - 1, k, k - 1, k};
 #pragma unroll
@@ -115,41 +119,43 @@ __device__ double sgs_strain_sq(const SgsParams& P, const float* u, const float*
             const int kk = ke[e];
             if (kk < 0 || kk >= nz - 1)
             {
-                xz0[e] = xz1[e] = yz0[e] = yz1[e] = 0.0;
+                xz0[e] = xz1[e] = yz0[e] = yz1[e] = R(0.0);
                 continue;
             }
-            const double dzc = A.dzc(kk);
+            const R dzc = A.dzc(kk);
             const int ii = xi[e], ii1 = sgs_next(ii, nx, P.px);
             xz0[e] = (A.f(u, ii, j, kk + 1) - A.f(u, ii, j, kk)) / dzc;
-            xz1[e] = (A.wf(w, ii1, j, kk) - A.wf(w, ii, j, kk)) / P.dx;
+            xz1[e] = (A.wf(w, ii1, j, kk) - A.wf(w, ii, j, kk)) / R(P.dx);
             const int jj = yj[e], jj1 = sgs_next(jj, ny, P.py);
             yz0[e] = (A.f(v, i, jj, kk + 1) - A.f(v, i, jj, kk)) / dzc;
-            yz1[e] = (A.wf(w, i, jj1, kk) - A.wf(w, i, jj, kk)) / P.dy;
+            yz1[e] = (A.wf(w, i, jj1, kk) - A.wf(w, i, jj, kk)) / R(P.dy);
         }
     }
-    const double s12_sq = 0.25 * (s12[0] * s12[0] + s12[1] * s12[1] + s12[2] * s12[2] + s12[3] * s12[3]);
-    auto avg_sq = [](const double (&g)[4]) { return 0.25 * (g[0] * g[0] + g[1] * g[1] + g[2] * g[2] + g[3] * g[3]); };
-    if (P.use_h && !P.use_v) return 2.0 * (s11 * s11 + s22 * s22) + 4.0 * s12_sq + avg_sq(xz1) + avg_sq(yz1);
-    if (P.use_v && !P.use_h) return avg_sq(xz0) + avg_sq(yz0) + 2.0 * s33 * s33;
-    double sxz[4], syz[4];
+    const R s12_sq = R(0.25) * (s12[0] * s12[0] + s12[1] * s12[1] + s12[2] * s12[2] + s12[3] * s12[3]);
+    auto avg_sq = [](const R (&g)[4]) { return R(0.25) * (g[0] * g[0] + g[1] * g[1] + g[2] * g[2] + g[3] * g[3]); };
+    if (P.use_h && !P.use_v) return R(2.0) * (s11 * s11 + s22 * s22) + R(4.0) * s12_sq + avg_sq(xz1) + avg_sq(yz1);
+    if (P.use_v && !P.use_h) return avg_sq(xz0) + avg_sq(yz0) + R(2.0) * s33 * s33;
+    R sxz[4], syz[4];
 #pragma unroll
     for (int e = 0; e < 4; ++e)
     {
-        const double a = 0.5 * (xz0[e] + xz1[e]);
-        const double b = 0.5 * (yz0[e] + yz1[e]);
+        const R a = R(0.5) * (xz0[e] + xz1[e]);
+        const R b = R(0.5) * (yz0[e] + yz1[e]);
         sxz[e] = a * a;
         syz[e] = b * b;
     }
-    const double s13_sq = 0.25 * (sxz[0] + sxz[1] + sxz[2] + sxz[3]);
-    const double s23_sq = 0.25 * (syz[0] + syz[1] + syz[2] + syz[3]);
-    return 2.0 * (s11 * s11 + s22 * s22 + s33 * s33) + 4.0 * (s12_sq + s13_sq + s23_sq);
+    const R s13_sq = R(0.25) * (sxz[0] + sxz[1] + sxz[2] + sxz[3]);
+    const R s23_sq = R(0.25) * (syz[0] + syz[1] + syz[2] + syz[3]);
+    return R(2.0) * (s11 * s11 + s22 * s22 + s33 * s33) + R(4.0) * (s12_sq + s13_sq + s23_sq);
 }
 
-__device__ __forceinline__ double sgs_min(double a, double b) { return b < a ? b : a; }  // std::min
+template <class R>
+__device__ __forceinline__ R sgs_min(R a, R b) { return b < a ? b : a; }  // std::min
 
 // Eddy coefficients of every cell; a cell whose inputs break the reference's
 // field contract (validate_scheme_inputs, eddy_viscosity.cpp:1088-1175) or
 // whose coefficient is not finite raises kStatusSgsInvalid.
+template <class R>
 __global__ void __launch_bounds__(256, 3) sgs_coefficients_kernel(SgsParams P, const float* __restrict__ u,
                                                                const float* __restrict__ v,
                                                                const float* __restrict__ w,
@@ -167,49 +173,50 @@ __global__ void __launch_bounds__(256, 3) sgs_coefficients_kernel(SgsParams P, c
         const float th = theta[c], r = rho[c];
         bool bad = !isfinite(u[c]) || !isfinite(v[c]) || !isfinite(w[c]) || !isfinite(th) || !(th > 0.0f) ||
                    !isfinite(r) || !(r > 0.0f) || (qv && (!isfinite(qv[c]) || qv[c] < 0.0f));
-        const double strain = sqrt(sgs_strain_sq(P, u, v, w, i, j, k));
-        double nu = P.Cs * P.Cs * P.delta[k] * P.delta[k] * strain * 1.0;
+        const R strain = sqrt(sgs_strain_sq<R>(P, u, v, w, i, j, k));
+        R nu = R(P.Cs) * R(P.Cs) * R(P.delta[k]) * R(P.delta[k]) * strain * R(1.0);
         bad |= !isfinite(strain) || !isfinite(nu);
-        nu = sgs_min(nu, P.nu_max);
-        const double kt = nu / P.Pr_t, kq = nu / P.Sc_t;
+        nu = sgs_min(nu, R(P.nu_max));
+        const R kt = nu / R(P.Pr_t), kq = nu / R(P.Sc_t);
         bad |= !isfinite(kt) || !isfinite(kq);
         if (bad) atomicOr(status, kStatusSgsInvalid);
         nu_t[c] = (float)nu;
-        K_theta[c] = (float)sgs_min(kt, P.K_max);
-        K_q[c] = (float)sgs_min(kq, P.K_max);
+        K_theta[c] = (float)sgs_min(kt, R(P.K_max));
+        K_q[c] = (float)sgs_min(kq, R(P.K_max));
     }
 }
 
 // Scalar diffusion tendency at one cell (compute_scalar_diffusion_tendencies).
-__device__ double sgs_scalar_rate(const SgsParams& P, const float* rho, const float* K, const float* phi, int i,
+template <class R>
+__device__ R sgs_scalar_rate(const SgsParams& P, const float* rho, const float* K, const float* phi, int i,
                                   int j, int k)
 {
-    const SgsAt A{P};
+    const SgsAt<R> A{P};
     const int nx = P.d.nx, ny = P.d.ny, nz = P.d.nz;
     const int jmm = !P.py && !P.open[2] && j == 1 ? j : sgs_prev(j, ny, P.py);
     const int jpp = !P.py && !P.open[3] && j == ny - 2 ? j : sgs_next(j, ny, P.py);
     const int imm = !P.px && !P.open[0] && i == 1 ? i : sgs_prev(i, nx, P.px);
     const int ipp = !P.px && !P.open[1] && i == nx - 2 ? i : sgs_next(i, nx, P.px);
     auto tr = [&](int ii, int jj, int kk) { return A.f(rho, ii, jj, kk) * A.f(K, ii, jj, kk); };
-    double div = 0.0;
+    R div = R(0.0);
     if (P.use_h)
     {
-        const double ph = A.f(phi, i, j, k), tc = tr(i, j, k);
-        const double fe = 0.5 * (tc + tr(ipp, j, k)) * (A.f(phi, ipp, j, k) - ph) / P.dx;
-        const double fw = 0.5 * (tr(imm, j, k) + tc) * (ph - A.f(phi, imm, j, k)) / P.dx;
-        const double fn = 0.5 * (tc + tr(i, jpp, k)) * (A.f(phi, i, jpp, k) - ph) / P.dy;
-        const double fs = 0.5 * (tr(i, jmm, k) + tc) * (ph - A.f(phi, i, jmm, k)) / P.dy;
-        div += (fe - fw) / P.dx + (fn - fs) / P.dy;
+        const R ph = A.f(phi, i, j, k), tc = tr(i, j, k);
+        const R fe = R(0.5) * (tc + tr(ipp, j, k)) * (A.f(phi, ipp, j, k) - ph) / R(P.dx);
+        const R fw = R(0.5) * (tr(imm, j, k) + tc) * (ph - A.f(phi, imm, j, k)) / R(P.dx);
+        const R fn = R(0.5) * (tc + tr(i, jpp, k)) * (A.f(phi, i, jpp, k) - ph) / R(P.dy);
+        const R fs = R(0.5) * (tr(i, jmm, k) + tc) * (ph - A.f(phi, i, jmm, k)) / R(P.dy);
+        div += (fe - fw) / R(P.dx) + (fn - fs) / R(P.dy);
     }
     if (P.use_v)
     {
-        const double ft = k < nz - 1 ? 0.5 * (tr(i, j, k) + tr(i, j, k + 1)) *
+        const R ft = k < nz - 1 ? R(0.5) * (tr(i, j, k) + tr(i, j, k + 1)) *
                                            (A.f(phi, i, j, k + 1) - A.f(phi, i, j, k)) / A.dzc(k)
-                                     : 0.0;
-        const double fb = k > 0 ? 0.5 * (tr(i, j, k - 1) + tr(i, j, k)) *
+                                     : R(0.0);
+        const R fb = k > 0 ? R(0.5) * (tr(i, j, k - 1) + tr(i, j, k)) *
                                       (A.f(phi, i, j, k) - A.f(phi, i, j, k - 1)) / A.dzc(k - 1)
-                                : 0.0;
-        div += (ft - fb) / P.dz[k];
+                                : R(0.0);
+        div += (ft - fb) / R(P.dz[k]);
     }
     return div / A.f(rho, i, j, k);
 }
@@ -221,41 +228,44 @@ __device__ double sgs_scalar_rate(const SgsParams& P, const float* rho, const fl
 // shared by du (its upper edge) and dw (its east edge); T23 likewise on the
 // yz edge.  In each stress mode the reference's du / dw (dv / dw) forms of
 // T13 (T23) reduce to the same expression.
-__device__ __forceinline__ double sgs_t12(const SgsParams& P, const float* u, const float* v, const float* rho,
+template <class R>
+__device__ __forceinline__ R sgs_t12(const SgsParams& P, const float* u, const float* v, const float* rho,
                                           const float* nu, int i, int j, int k)
 {
-    const SgsAt A{P};
+    const SgsAt<R> A{P};
     const int i1 = sgs_next(i, P.d.nx, P.px), j1 = sgs_next(j, P.d.ny, P.py);
-    const double s12 =
-        0.5 * ((A.f(u, i, j1, k) - A.f(u, i, j, k)) / P.dy + (A.f(v, i1, j, k) - A.f(v, i, j, k)) / P.dx);
-    return 2.0 * A.mu_xy(rho, nu, i, j, k) * s12;
+    const R s12 =
+        R(0.5) * ((A.f(u, i, j1, k) - A.f(u, i, j, k)) / R(P.dy) + (A.f(v, i1, j, k) - A.f(v, i, j, k)) / R(P.dx));
+    return R(2.0) * A.mu_xy(rho, nu, i, j, k) * s12;
 }
 
-__device__ __forceinline__ double sgs_t13(const SgsParams& P, const float* u, const float* w, const float* rho,
+template <class R>
+__device__ __forceinline__ R sgs_t13(const SgsParams& P, const float* u, const float* w, const float* rho,
                                           const float* nu, int i, int j, int k)
 {
-    const SgsAt A{P};
+    const SgsAt<R> A{P};
     const int i1 = sgs_next(i, P.d.nx, P.px);
-    const double dwdx = (A.wf(w, i1, j, k) - A.wf(w, i, j, k)) / P.dx;
-    double grad = dwdx;
+    const R dwdx = (A.wf(w, i1, j, k) - A.wf(w, i, j, k)) / R(P.dx);
+    R grad = dwdx;
     if (P.use_v)
     {
-        const double dudz = (A.f(u, i, j, k + 1) - A.f(u, i, j, k)) / A.dzc(k);
+        const R dudz = (A.f(u, i, j, k + 1) - A.f(u, i, j, k)) / A.dzc(k);
         grad = P.use_h ? dudz + dwdx : dudz;
     }
     return A.mu_z(rho, nu, i, j, i1, j, k) * grad;
 }
 
-__device__ __forceinline__ double sgs_t23(const SgsParams& P, const float* v, const float* w, const float* rho,
+template <class R>
+__device__ __forceinline__ R sgs_t23(const SgsParams& P, const float* v, const float* w, const float* rho,
                                           const float* nu, int i, int j, int k)
 {
-    const SgsAt A{P};
+    const SgsAt<R> A{P};
     const int j1 = sgs_next(j, P.d.ny, P.py);
-    const double dwdy = (A.wf(w, i, j1, k) - A.wf(w, i, j, k)) / P.dy;
-    double grad = dwdy;
+    const R dwdy = (A.wf(w, i, j1, k) - A.wf(w, i, j, k)) / R(P.dy);
+    R grad = dwdy;
     if (P.use_v)
     {
-        const double dvdz = (A.f(v, i, j, k + 1) - A.f(v, i, j, k)) / A.dzc(k);
+        const R dvdz = (A.f(v, i, j, k + 1) - A.f(v, i, j, k)) / A.dzc(k);
         grad = P.use_h ? dvdz + dwdy : dvdz;
     }
     return A.mu_z(rho, nu, i, j, i, j1, k) * grad;
@@ -263,78 +273,82 @@ __device__ __forceinline__ double sgs_t23(const SgsParams& P, const float* v, co
 
 // du/dt at x-face (i, j, k) (compute_momentum_diffusion_tendencies, first
 // loop); t12 / t13: the shared corner stresses above.
-__device__ double sgs_du(const SgsParams& P, const float* u, const float* v, const float* w, const float* rho,
-                         const float* nu, int i, int j, int k, double t12, double t13)
+template <class R>
+__device__ R sgs_du(const SgsParams& P, const float* u, const float* v, const float* w, const float* rho,
+                         const float* nu, int i, int j, int k, R t12, R t13)
 {
-    const SgsAt A{P};
+    const SgsAt<R> A{P};
     const int nx = P.d.nx, ny = P.d.ny;
     const int jmm = sgs_prev(j, ny, P.py), imm = sgs_prev(i, nx, P.px), ipp = sgs_next(i, nx, P.px);
-    double div = 0.0;
+    R div = R(0.0);
     if (P.use_h)
     {
-        const double s_r = (A.f(u, ipp, j, k) - A.f(u, i, j, k)) / P.dx;
-        const double s_l = (A.f(u, i, j, k) - A.f(u, imm, j, k)) / P.dx;
-        div += (2.0 * A.mu(rho, nu, ipp, j, k) * s_r - 2.0 * A.mu(rho, nu, i, j, k) * s_l) / P.dx;
-        div += (t12 - sgs_t12(P, u, v, rho, nu, i, jmm, k)) / P.dy;
+        const R s_r = (A.f(u, ipp, j, k) - A.f(u, i, j, k)) / R(P.dx);
+        const R s_l = (A.f(u, i, j, k) - A.f(u, imm, j, k)) / R(P.dx);
+        div += (R(2.0) * A.mu(rho, nu, ipp, j, k) * s_r - R(2.0) * A.mu(rho, nu, i, j, k) * s_l) / R(P.dx);
+        div += (t12 - sgs_t12<R>(P, u, v, rho, nu, i, jmm, k)) / R(P.dy);
     }
     if (P.use_v)
     {
         // T13 on the z-faces k (upper) and k-1 (lower; zero at the ground).
-        const double lower = k > 0 ? sgs_t13(P, u, w, rho, nu, i, j, k - 1) : 0.0;
-        div += (t13 - lower) / P.dz[k];
+        const R lower = k > 0 ? sgs_t13<R>(P, u, w, rho, nu, i, j, k - 1) : R(0.0);
+        div += (t13 - lower) / R(P.dz[k]);
     }
-    return div / (0.5 * (A.f(rho, i, j, k) + A.f(rho, ipp, j, k)));
+    return div / (R(0.5) * (A.f(rho, i, j, k) + A.f(rho, ipp, j, k)));
 }
 
 // dv/dt at y-face (i, j, k) (second loop).
-__device__ double sgs_dv(const SgsParams& P, const float* u, const float* v, const float* w, const float* rho,
-                         const float* nu, int i, int j, int k, double t12, double t23)
+template <class R>
+__device__ R sgs_dv(const SgsParams& P, const float* u, const float* v, const float* w, const float* rho,
+                         const float* nu, int i, int j, int k, R t12, R t23)
 {
-    const SgsAt A{P};
+    const SgsAt<R> A{P};
     const int nx = P.d.nx, ny = P.d.ny;
     const int jmm = sgs_prev(j, ny, P.py), jpp = sgs_next(j, ny, P.py), imm = sgs_prev(i, nx, P.px);
-    double div = 0.0;
+    R div = R(0.0);
     if (P.use_h)
     {
-        const double s_n = (A.f(v, i, jpp, k) - A.f(v, i, j, k)) / P.dy;
-        const double s_s = (A.f(v, i, j, k) - A.f(v, i, jmm, k)) / P.dy;
-        div += (2.0 * A.mu(rho, nu, i, jpp, k) * s_n - 2.0 * A.mu(rho, nu, i, j, k) * s_s) / P.dy;
-        div += (t12 - sgs_t12(P, u, v, rho, nu, imm, j, k)) / P.dx;
+        const R s_n = (A.f(v, i, jpp, k) - A.f(v, i, j, k)) / R(P.dy);
+        const R s_s = (A.f(v, i, j, k) - A.f(v, i, jmm, k)) / R(P.dy);
+        div += (R(2.0) * A.mu(rho, nu, i, jpp, k) * s_n - R(2.0) * A.mu(rho, nu, i, j, k) * s_s) / R(P.dy);
+        div += (t12 - sgs_t12<R>(P, u, v, rho, nu, imm, j, k)) / R(P.dx);
     }
     if (P.use_v)
     {
-        const double lower = k > 0 ? sgs_t23(P, v, w, rho, nu, i, j, k - 1) : 0.0;
-        div += (t23 - lower) / P.dz[k];
+        const R lower = k > 0 ? sgs_t23<R>(P, v, w, rho, nu, i, j, k - 1) : R(0.0);
+        div += (t23 - lower) / R(P.dz[k]);
     }
-    return div / (0.5 * (A.f(rho, i, j, k) + A.f(rho, i, jpp, k)));
+    return div / (R(0.5) * (A.f(rho, i, j, k) + A.f(rho, i, jpp, k)));
 }
 
 // dw/dt at z-face (i, j, k) (third loop): stress divergence over the dual
 // column mass.
-__device__ double sgs_dw(const SgsParams& P, const float* u, const float* v, const float* w, const float* rho,
-                         const float* nu, int i, int j, int k, double t13, double t23)
+template <class R>
+__device__ R sgs_dw(const SgsParams& P, const float* u, const float* v, const float* w, const float* rho,
+                         const float* nu, int i, int j, int k, R t13, R t23)
 {
-    const SgsAt A{P};
+    const SgsAt<R> A{P};
     const int imm = sgs_prev(i, P.d.nx, P.px), jmm = sgs_prev(j, P.d.ny, P.py);
-    const double dzb = P.dz[k], dzt = P.dz[k + 1], dzd = A.dzc(k);
-    const double mass = 0.5 * (A.f(rho, i, j, k) * dzb + A.f(rho, i, j, k + 1) * dzt);
-    double force = 0.0;
+    const R dzb = R(P.dz[k]), dzt = R(P.dz[k + 1]), dzd = A.dzc(k);
+    const R mass = R(0.5) * (A.f(rho, i, j, k) * dzb + A.f(rho, i, j, k + 1) * dzt);
+    R force = R(0.0);
     if (P.use_v)
     {
-        const double t33_t = 2.0 * A.mu(rho, nu, i, j, k + 1) * ((A.wf(w, i, j, k + 1) - A.wf(w, i, j, k)) / dzt);
-        const double t33_b = 2.0 * A.mu(rho, nu, i, j, k) * ((A.wf(w, i, j, k) - A.wf(w, i, j, k - 1)) / dzb);
+        const R t33_t = R(2.0) * A.mu(rho, nu, i, j, k + 1) * ((A.wf(w, i, j, k + 1) - A.wf(w, i, j, k)) / dzt);
+        const R t33_b = R(2.0) * A.mu(rho, nu, i, j, k) * ((A.wf(w, i, j, k) - A.wf(w, i, j, k - 1)) / dzb);
         force += t33_t - t33_b;
     }
     if (P.use_h)
     {
-        force += dzd * (t13 - sgs_t13(P, u, w, rho, nu, imm, j, k)) / P.dx;
-        force += dzd * (t23 - sgs_t23(P, v, w, rho, nu, i, jmm, k)) / P.dy;
+        force += dzd * (t13 - sgs_t13<R>(P, u, w, rho, nu, imm, j, k)) / R(P.dx);
+        force += dzd * (t23 - sgs_t23<R>(P, v, w, rho, nu, i, jmm, k)) / R(P.dy);
     }
     return force / mass;
 }
 
 // The five tendencies of every cell; zero where the reference leaves its
 // pre-cleared outputs untouched.
+template <class R>
 __global__ void __launch_bounds__(256, 4) sgs_tendencies_kernel(
     SgsParams P, const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w,
     const float* __restrict__ theta, const float* __restrict__ qv, const float* __restrict__ rho,
@@ -355,17 +369,17 @@ __global__ void __launch_bounds__(256, 4) sgs_tendencies_kernel(
         {
             const bool du_on = i <= (P.px ? nx - 2 : nx - 3);
             const bool dv_on = j <= (P.py ? ny - 2 : ny - 3);
-            const double t12 = P.use_h && (du_on || dv_on) ? sgs_t12(P, u, v, rho, nu_t, i, j, k) : 0.0;
-            const double t13 = (du_on && P.use_v) || P.use_h ? sgs_t13(P, u, w, rho, nu_t, i, j, k) : 0.0;
-            const double t23 = (dv_on && P.use_v) || P.use_h ? sgs_t23(P, v, w, rho, nu_t, i, j, k) : 0.0;
-            if (du_on) ru = (float)sgs_du(P, u, v, w, rho, nu_t, i, j, k, t12, t13);
-            if (dv_on) rv = (float)sgs_dv(P, u, v, w, rho, nu_t, i, j, k, t12, t23);
-            rw = (float)sgs_dw(P, u, v, w, rho, nu_t, i, j, k, t13, t23);
+            const R t12 = P.use_h && (du_on || dv_on) ? sgs_t12<R>(P, u, v, rho, nu_t, i, j, k) : R(0.0);
+            const R t13 = (du_on && P.use_v) || P.use_h ? sgs_t13<R>(P, u, w, rho, nu_t, i, j, k) : R(0.0);
+            const R t23 = (dv_on && P.use_v) || P.use_h ? sgs_t23<R>(P, v, w, rho, nu_t, i, j, k) : R(0.0);
+            if (du_on) ru = (float)sgs_du<R>(P, u, v, w, rho, nu_t, i, j, k, t12, t13);
+            if (dv_on) rv = (float)sgs_dv<R>(P, u, v, w, rho, nu_t, i, j, k, t12, t23);
+            rw = (float)sgs_dw<R>(P, u, v, w, rho, nu_t, i, j, k, t13, t23);
         }
         if (column)
         {
-            rt = (float)sgs_scalar_rate(P, rho, K_theta, theta, i, j, k);
-            if (qv) rq = (float)sgs_scalar_rate(P, rho, K_q, qv, i, j, k);
+            rt = (float)sgs_scalar_rate<R>(P, rho, K_theta, theta, i, j, k);
+            if (qv) rq = (float)sgs_scalar_rate<R>(P, rho, K_q, qv, i, j, k);
         }
         dudt[c] = ru;
         dvdt[c] = rv;

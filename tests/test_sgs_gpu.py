@@ -234,3 +234,32 @@ def test_resident_run_with_sgs_matches_oracle(ctx, o32, bc, dt_sgs):
     for k in PROGNOSTIC:
         assert_bitwise(got[k], want[k], k)
     assert run.sgs_substeps == 2 * int(np.ceil(case.dt / dt_sgs))
+
+
+@pytest.mark.parametrize("shape,bc,kw,dzkind", DEVICE_CASES[:4], ids=[str(c[0]) for c in DEVICE_CASES[:4]])
+def test_fp32_closure_error_against_fp64(shape, bc, kw, dzkind):
+    """The FP32 form of the closure (an FP32-precision context) against the
+    FP64 oracle on the same FP32 inputs: every output within 1e-6 relative L2
+    and 1e-6 of its largest magnitude (measured: at most 2.7e-7 and 4.2e-7),
+    where the reference-precision closure's error is only its final FP32
+    rounding (about 3e-8)."""
+    o64 = oracle.Restatement("f64")
+    st, _ = _case(shape, sum(shape))
+    dz = _dz(shape[2], dzkind)
+    cfg = SgsConfig.from_bc(bc, **kw)
+    c32 = cuda.Context(0)
+    c32.set_precision(cuda.PRECISION_FP32)
+    dev = on_device({k: st[k] for k in ("u", "v", "w", "theta", "rho", "qv")})
+    args = cuda.smagorinsky_args(dev, dz, SGS_GRID, cfg, memory=cuda.MEMORY_DEVICE)
+    c32.check(c32.smagorinsky_fused(args))
+    c32.synchronize()
+    ref = o64.smagorinsky({k: v.astype(np.float64) for k, v in st.items()}, dz, SGS_GRID, cfg)
+    for k, v in args.outputs.items():
+        got = v.cpu().numpy().astype(np.float64)
+        norm = np.linalg.norm(ref[k])
+        if norm == 0.0:
+            assert np.all(got == 0.0), k
+            continue
+        assert np.linalg.norm(got - ref[k]) / norm <= 1e-6, k
+        assert np.abs(got - ref[k]).max() <= 1e-6 * np.abs(ref[k]).max(), k
+    c32.close()
