@@ -466,9 +466,9 @@ __global__ void __launch_bounds__(256) sgs_apply_kernel(SgsApplyParams A, float*
 // input check.  partial: [slab][6] = power, norm, theta min, max, qv min, max.
 // The lanes load 32 consecutive levels of a row (coalesced) and form each
 // cell's six terms (mass * velocity * acceleration and mass * acceleration^2
-// of its u, v and w faces) in parallel; lane 0 then adds them to the two
-// running sums in the reference's order, while the lanes already hold the
-// next chunk's loads.  A face the reference skips contributes +0.0, which
+// of its u, v and w faces) in parallel; lanes 0 and 1 then add them to the
+// power and norm sums (one each) in the reference's order, while the lanes
+// already hold the next chunk's loads.  A face the reference skips contributes +0.0, which
 // leaves a sum that started at +0.0 unchanged bit for bit.
 constexpr int kSlabWarps = 4;
 
@@ -587,18 +587,22 @@ __global__ void __launch_bounds__(32 * kSlabWarps) sgs_stability_slab_kernel(
 #pragma unroll
         for (int q = 0; q < 6; ++q) t[q][lane] = tm[q];
         __syncwarp();
-        if (lane == 0)
+        if (lane < 2)
         {
+            // Lane 0 carries the power sum, lane 1 the norm sum: two
+            // independent serial chains, each in the reference's order.
             const int cells = min(32, nz - (kc - lane));
+            double acc = lane == 0 ? p : a;
             for (int c = 0; c < cells; ++c)
             {
-                p += t[0][c];
-                a += t[1][c];
-                p += t[2][c];
-                a += t[3][c];
-                p += t[4][c];
-                a += t[5][c];
+                acc += t[lane][c];
+                acc += t[lane + 2][c];
+                acc += t[lane + 4][c];
             }
+            if (lane == 0)
+                p = acc;
+            else
+                a = acc;
         }
         __syncwarp();
     }
@@ -611,6 +615,7 @@ __global__ void __launch_bounds__(32 * kSlabWarps) sgs_stability_slab_kernel(
         qhi = fmax(qhi, __shfl_down_sync(0xffffffffu, qhi, off));
     }
     bad = __any_sync(0xffffffffu, bad);
+    a = __shfl_sync(0xffffffffu, a, 1);
     if (lane == 0)
     {
         if (bad) atomicOr(status, kStatusSgsInvalid);
