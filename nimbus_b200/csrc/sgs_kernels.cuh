@@ -534,16 +534,28 @@ __global__ void __launch_bounds__(32 * kSlabWarps) sgs_stability_slab_kernel(
         k = (n % chunks) * 32 + lane;
     };
     int j, j1, k;
+    // Two chunks in flight ahead of the one being summed.
+    int jb = 0, j1b = 0, kb = 0;
     row_of(0, j, j1, k);
     SlabChunk x = slab_load(P, u, v, w, theta, qv, rho, dudt, dvdt, dwdt, dthdt, dqvdt, i, i1, j, j1, k);
+    SlabChunk y{};
+    if (total > 1)
+    {
+        row_of(1, jb, j1b, kb);
+        y = slab_load(P, u, v, w, theta, qv, rho, dudt, dvdt, dwdt, dthdt, dqvdt, i, i1, jb, j1b, kb);
+    }
     for (int n = 0; n < total; ++n)
     {
         const int jc = j, kc = k;
         const SlabChunk cur = x;
-        if (n + 1 < total)
+        x = y;
+        j = jb;
+        j1 = j1b;
+        k = kb;
+        if (n + 2 < total)
         {
-            row_of(n + 1, j, j1, k);
-            x = slab_load(P, u, v, w, theta, qv, rho, dudt, dvdt, dwdt, dthdt, dqvdt, i, i1, j, j1, k);
+            row_of(n + 2, jb, j1b, kb);
+            y = slab_load(P, u, v, w, theta, qv, rho, dudt, dvdt, dwdt, dthdt, dqvdt, i, i1, jb, j1b, kb);
         }
         double tm[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         if (kc < nz)
