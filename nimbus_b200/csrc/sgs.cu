@@ -50,11 +50,16 @@ nimbus_status stage_tables(nimbus_cuda_context* ctx, cudaStream_t st, const doub
 {
     const size_t nz = delta.size();
     double* dev = nullptr;
-    NB_TRY(ensure(ctx, kSgsTables, 2 * nz, &dev));
+    NB_TRY(ensure(ctx, kSgsTables, 3 * nz, &dev));  // dz, delta, then the FP32 reciprocals of dz
+    std::vector<float> inv(nz);
+    for (size_t k = 0; k < nz; ++k) inv[k] = static_cast<float>(1.0 / dz[k]);
     NB_CUDA(ctx, cudaMemcpyAsync(dev, dz, nz * sizeof(double), cudaMemcpyHostToDevice, st));
     NB_CUDA(ctx, cudaMemcpyAsync(dev + nz, delta.data(), nz * sizeof(double), cudaMemcpyHostToDevice, st));
+    float* inv_dev = reinterpret_cast<float*>(dev + 2 * nz);
+    NB_CUDA(ctx, cudaMemcpyAsync(inv_dev, inv.data(), nz * sizeof(float), cudaMemcpyHostToDevice, st));
     P.dz = dev;
     P.delta = dev + nz;
+    P.inv_dz_f = inv_dev;
     return NIMBUS_OK;
 }
 
@@ -74,6 +79,8 @@ SgsParams params_of(const nimbus_smagorinsky_args* a)
     P.Sc_t = a->Sc_t;
     P.nu_max = a->nu_t_max;
     P.K_max = a->K_max;
+    P.inv_dx_f = static_cast<float>(1.0 / a->dx);
+    P.inv_dy_f = static_cast<float>(1.0 / a->dy);
     return P;
 }
 

@@ -34,7 +34,29 @@ struct SgsParams
     int px, py;           // periodic x / y
     int open[4];          // W, E, S, N lateral faces open (scalar fluxes pass)
     double Cs, Pr_t, Sc_t, nu_max, K_max;
+    // FP32 form: reciprocals of the spacings (it multiplies where the
+    // reference form divides).
+    float inv_dx_f, inv_dy_f;
+    const float* inv_dz_f;  // [nz] (device)
 };
+
+// A divisor: the reference form divides by d; the FP32 form multiplies by the
+// FP32 reciprocal (one rounding more, no division sequence).
+template <class R>
+struct Recip
+{
+    double d;
+    float inv;
+};
+
+template <class R>
+__device__ __forceinline__ R operator/(R x, Recip<R> r)
+{
+    if constexpr (sizeof(R) == sizeof(float))
+        return x * r.inv;
+    else
+        return x / R(r.d);
+}
 
 // Neighbour rows (eddy_viscosity.cpp:69-105): clamped to the allocated
 // range, or on a periodic axis wrapped over the physical rows 1..n-2.
@@ -64,6 +86,9 @@ struct SgsAt
     {
         return k < 0 ? R(0.0) : f(w, i, j, k);
     }
+    __device__ __forceinline__ Recip<R> DX() const { return {P.dx, P.inv_dx_f}; }
+    __device__ __forceinline__ Recip<R> DY() const { return {P.dy, P.inv_dy_f}; }
+    __device__ __forceinline__ Recip<R> DZ(int k) const { return {P.dz[k], P.inv_dz_f[k]}; }
     __device__ __forceinline__ R dzc(int k) const { return R(0.5) * (R(P.dz[k]) + R(P.dz[k + 1])); }
     // mu = rho nu at a centre; on an xy edge (four-point mean); on an xz or yz
     // edge (pair means of the two levels, weighted by the other level's
@@ -94,9 +119,9 @@ __device__ R sgs_strain_sq(const SgsParams& P, const float* u, const float* v, c
     const SgsAt<R> A{P};
     const int nx = P.d.nx, ny = P.d.ny, nz = P.d.nz;
     const int jm = sgs_prev(j, ny, P.py), im = sgs_prev(i, nx, P.px);
-    const R s11 = (A.f(u, i, j, k) - A.f(u, im, j, k)) / R(P.dx);
-    const R s22 = (A.f(v, i, j, k) - A.f(v, i, jm, k)) / R(P.dy);
-    const R s33 = (A.wf(w, i, j, k) - A.wf(w, i, j, k - 1)) / R(P.dz[k]);
+    const R s11 = (A.f(u, i, j, k) - A.f(u, im, j, k)) / A.DX();
+    const R s22 = (A.f(v, i, j, k) - A.f(v, i, jm, k)) / A.DY();
+    const R s33 = (A.wf(w, i, j, k) - A.wf(w, i, j, k - 1)) / A.DZ(k);
     R s12[4];
     {
         const int ie[4] = {im, im, i, i}, je[4] = {jm, j, jm, j};
@@ -105,8 +130,8 @@ __device__ R sgs_strain_sq(const SgsParams& P, const float* u, const float* v, c
         {
             const int ii = ie[e], jj = je[e];
             const int jj1 = sgs_next(jj, ny, P.py), ii1 = sgs_next(ii, nx, P.px);
-            const R dudy = (A.f(u, ii, jj1, k) - A.f(u, ii, jj, k)) / R(P.dy);
-            const R dvdx = (A.f(v, ii1, jj, k) - A.f(v, ii, jj, k)) / R(P.dx);
+            const R dudy = (A.f(u, ii, jj1, k) - A.f(u, ii, jj, k)) / A.DY();
+            const R dvdx = (A.f(v, ii1, jj, k) - A.f(v, ii, jj, k)) / A.DX();
             s12[e] = R(0.5) * (dudy + dvdx);
         }
     }
@@ -125,10 +150,10 @@ __device__ R sgs_strain_sq(const SgsParams& P, const float* u, const float* v, c
             const R dzc = A.dzc(kk);
             const int ii = xi[e], ii1 = sgs_next(ii, nx, P.px);
             xz0[e] = (A.f(u, ii, j, kk + 1) - A.f(u, ii, j, kk)) / dzc;
-            xz1[e] = (A.wf(w, ii1, j, kk) - A.wf(w, ii, j, kk)) / R(P.dx);
+            xz1[e] = (A.wf(w, ii1, j, kk) - A.wf(w, ii, j, kk)) / A.DX();
             const int jj = yj[e], jj1 = sgs_next(jj, ny, P.py);
             yz0[e] = (A.f(v, i, jj, kk + 1) - A.f(v, i, jj, kk)) / dzc;
-            yz1[e] = (A.wf(w, i, jj1, kk) - A.wf(w, i, jj, kk)) / R(P.dy);
+            yz1[e] = (A.wf(w, i, jj1, kk) - A.wf(w, i, jj, kk)) / A.DY();
         }
     }
     const R s12_sq = R(0.25) * (s12[0] * s12[0] + s12[1] * s12[1] + s12[2] * s12[2] + s12[3] * s12[3]);
@@ -202,11 +227,11 @@ __device__ R sgs_scalar_rate(const SgsParams& P, const float* rho, const float* 
     if (P.use_h)
     {
         const R ph = A.f(phi, i, j, k), tc = tr(i, j, k);
-        const R fe = R(0.5) * (tc + tr(ipp, j, k)) * (A.f(phi, ipp, j, k) - ph) / R(P.dx);
-        const R fw = R(0.5) * (tr(imm, j, k) + tc) * (ph - A.f(phi, imm, j, k)) / R(P.dx);
-        const R fn = R(0.5) * (tc + tr(i, jpp, k)) * (A.f(phi, i, jpp, k) - ph) / R(P.dy);
-        const R fs = R(0.5) * (tr(i, jmm, k) + tc) * (ph - A.f(phi, i, jmm, k)) / R(P.dy);
-        div += (fe - fw) / R(P.dx) + (fn - fs) / R(P.dy);
+        const R fe = R(0.5) * (tc + tr(ipp, j, k)) * (A.f(phi, ipp, j, k) - ph) / A.DX();
+        const R fw = R(0.5) * (tr(imm, j, k) + tc) * (ph - A.f(phi, imm, j, k)) / A.DX();
+        const R fn = R(0.5) * (tc + tr(i, jpp, k)) * (A.f(phi, i, jpp, k) - ph) / A.DY();
+        const R fs = R(0.5) * (tr(i, jmm, k) + tc) * (ph - A.f(phi, i, jmm, k)) / A.DY();
+        div += (fe - fw) / A.DX() + (fn - fs) / A.DY();
     }
     if (P.use_v)
     {
@@ -216,7 +241,7 @@ __device__ R sgs_scalar_rate(const SgsParams& P, const float* rho, const float* 
         const R fb = k > 0 ? R(0.5) * (tr(i, j, k - 1) + tr(i, j, k)) *
                                       (A.f(phi, i, j, k) - A.f(phi, i, j, k - 1)) / A.dzc(k - 1)
                                 : R(0.0);
-        div += (ft - fb) / R(P.dz[k]);
+        div += (ft - fb) / A.DZ(k);
     }
     return div / A.f(rho, i, j, k);
 }
@@ -235,7 +260,7 @@ __device__ __forceinline__ R sgs_t12(const SgsParams& P, const float* u, const f
     const SgsAt<R> A{P};
     const int i1 = sgs_next(i, P.d.nx, P.px), j1 = sgs_next(j, P.d.ny, P.py);
     const R s12 =
-        R(0.5) * ((A.f(u, i, j1, k) - A.f(u, i, j, k)) / R(P.dy) + (A.f(v, i1, j, k) - A.f(v, i, j, k)) / R(P.dx));
+        R(0.5) * ((A.f(u, i, j1, k) - A.f(u, i, j, k)) / A.DY() + (A.f(v, i1, j, k) - A.f(v, i, j, k)) / A.DX());
     return R(2.0) * A.mu_xy(rho, nu, i, j, k) * s12;
 }
 
@@ -245,7 +270,7 @@ __device__ __forceinline__ R sgs_t13(const SgsParams& P, const float* u, const f
 {
     const SgsAt<R> A{P};
     const int i1 = sgs_next(i, P.d.nx, P.px);
-    const R dwdx = (A.wf(w, i1, j, k) - A.wf(w, i, j, k)) / R(P.dx);
+    const R dwdx = (A.wf(w, i1, j, k) - A.wf(w, i, j, k)) / A.DX();
     R grad = dwdx;
     if (P.use_v)
     {
@@ -261,7 +286,7 @@ __device__ __forceinline__ R sgs_t23(const SgsParams& P, const float* v, const f
 {
     const SgsAt<R> A{P};
     const int j1 = sgs_next(j, P.d.ny, P.py);
-    const R dwdy = (A.wf(w, i, j1, k) - A.wf(w, i, j, k)) / R(P.dy);
+    const R dwdy = (A.wf(w, i, j1, k) - A.wf(w, i, j, k)) / A.DY();
     R grad = dwdy;
     if (P.use_v)
     {
@@ -283,16 +308,16 @@ __device__ R sgs_du(const SgsParams& P, const float* u, const float* v, const fl
     R div = R(0.0);
     if (P.use_h)
     {
-        const R s_r = (A.f(u, ipp, j, k) - A.f(u, i, j, k)) / R(P.dx);
-        const R s_l = (A.f(u, i, j, k) - A.f(u, imm, j, k)) / R(P.dx);
-        div += (R(2.0) * A.mu(rho, nu, ipp, j, k) * s_r - R(2.0) * A.mu(rho, nu, i, j, k) * s_l) / R(P.dx);
-        div += (t12 - sgs_t12<R>(P, u, v, rho, nu, i, jmm, k)) / R(P.dy);
+        const R s_r = (A.f(u, ipp, j, k) - A.f(u, i, j, k)) / A.DX();
+        const R s_l = (A.f(u, i, j, k) - A.f(u, imm, j, k)) / A.DX();
+        div += (R(2.0) * A.mu(rho, nu, ipp, j, k) * s_r - R(2.0) * A.mu(rho, nu, i, j, k) * s_l) / A.DX();
+        div += (t12 - sgs_t12<R>(P, u, v, rho, nu, i, jmm, k)) / A.DY();
     }
     if (P.use_v)
     {
         // T13 on the z-faces k (upper) and k-1 (lower; zero at the ground).
         const R lower = k > 0 ? sgs_t13<R>(P, u, w, rho, nu, i, j, k - 1) : R(0.0);
-        div += (t13 - lower) / R(P.dz[k]);
+        div += (t13 - lower) / A.DZ(k);
     }
     return div / (R(0.5) * (A.f(rho, i, j, k) + A.f(rho, ipp, j, k)));
 }
@@ -308,15 +333,15 @@ __device__ R sgs_dv(const SgsParams& P, const float* u, const float* v, const fl
     R div = R(0.0);
     if (P.use_h)
     {
-        const R s_n = (A.f(v, i, jpp, k) - A.f(v, i, j, k)) / R(P.dy);
-        const R s_s = (A.f(v, i, j, k) - A.f(v, i, jmm, k)) / R(P.dy);
-        div += (R(2.0) * A.mu(rho, nu, i, jpp, k) * s_n - R(2.0) * A.mu(rho, nu, i, j, k) * s_s) / R(P.dy);
-        div += (t12 - sgs_t12<R>(P, u, v, rho, nu, imm, j, k)) / R(P.dx);
+        const R s_n = (A.f(v, i, jpp, k) - A.f(v, i, j, k)) / A.DY();
+        const R s_s = (A.f(v, i, j, k) - A.f(v, i, jmm, k)) / A.DY();
+        div += (R(2.0) * A.mu(rho, nu, i, jpp, k) * s_n - R(2.0) * A.mu(rho, nu, i, j, k) * s_s) / A.DY();
+        div += (t12 - sgs_t12<R>(P, u, v, rho, nu, imm, j, k)) / A.DX();
     }
     if (P.use_v)
     {
         const R lower = k > 0 ? sgs_t23<R>(P, v, w, rho, nu, i, j, k - 1) : R(0.0);
-        div += (t23 - lower) / R(P.dz[k]);
+        div += (t23 - lower) / A.DZ(k);
     }
     return div / (R(0.5) * (A.f(rho, i, j, k) + A.f(rho, i, jpp, k)));
 }
@@ -340,8 +365,8 @@ __device__ R sgs_dw(const SgsParams& P, const float* u, const float* v, const fl
     }
     if (P.use_h)
     {
-        force += dzd * (t13 - sgs_t13<R>(P, u, w, rho, nu, imm, j, k)) / R(P.dx);
-        force += dzd * (t23 - sgs_t23<R>(P, v, w, rho, nu, i, jmm, k)) / R(P.dy);
+        force += dzd * (t13 - sgs_t13<R>(P, u, w, rho, nu, imm, j, k)) / A.DX();
+        force += dzd * (t23 - sgs_t23<R>(P, v, w, rho, nu, i, jmm, k)) / A.DY();
     }
     return force / mass;
 }
