@@ -50,16 +50,18 @@ nimbus_status stage_tables(nimbus_cuda_context* ctx, cudaStream_t st, const doub
 {
     const size_t nz = delta.size();
     double* dev = nullptr;
-    NB_TRY(ensure(ctx, kSgsTables, 3 * nz, &dev));  // dz, delta, then the FP32 reciprocals of dz
-    std::vector<float> inv(nz);
+    NB_TRY(ensure(ctx, kSgsTables, 3 * nz, &dev));  // dz, delta, then the FP32 reciprocals of dz and dzc
+    std::vector<float> inv(2 * nz, 0.0f);
     for (size_t k = 0; k < nz; ++k) inv[k] = static_cast<float>(1.0 / dz[k]);
+    for (size_t k = 0; k + 1 < nz; ++k) inv[nz + k] = static_cast<float>(1.0 / (0.5 * (dz[k] + dz[k + 1])));
     NB_CUDA(ctx, cudaMemcpyAsync(dev, dz, nz * sizeof(double), cudaMemcpyHostToDevice, st));
     NB_CUDA(ctx, cudaMemcpyAsync(dev + nz, delta.data(), nz * sizeof(double), cudaMemcpyHostToDevice, st));
     float* inv_dev = reinterpret_cast<float*>(dev + 2 * nz);
-    NB_CUDA(ctx, cudaMemcpyAsync(inv_dev, inv.data(), nz * sizeof(float), cudaMemcpyHostToDevice, st));
+    NB_CUDA(ctx, cudaMemcpyAsync(inv_dev, inv.data(), 2 * nz * sizeof(float), cudaMemcpyHostToDevice, st));
     P.dz = dev;
     P.delta = dev + nz;
     P.inv_dz_f = inv_dev;
+    P.inv_dzc_f = inv_dev + nz;
     return NIMBUS_OK;
 }
 

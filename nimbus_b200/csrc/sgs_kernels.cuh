@@ -37,7 +37,8 @@ struct SgsParams
     // FP32 form: reciprocals of the spacings (it multiplies where the
     // reference form divides).
     float inv_dx_f, inv_dy_f;
-    const float* inv_dz_f;  // [nz] (device)
+    const float* inv_dz_f;   // [nz] (device)
+    const float* inv_dzc_f;  // [nz] (device): 1 / distance between centres k and k+1
 };
 
 // A divisor: the reference form divides by d; the FP32 form multiplies by the
@@ -89,6 +90,9 @@ struct SgsAt
     __device__ __forceinline__ Recip<R> DX() const { return {P.dx, P.inv_dx_f}; }
     __device__ __forceinline__ Recip<R> DY() const { return {P.dy, P.inv_dy_f}; }
     __device__ __forceinline__ Recip<R> DZ(int k) const { return {P.dz[k], P.inv_dz_f[k]}; }
+    // Distance between centres k and k+1 as a divisor (the reference form
+    // divides by 0.5 (dz_k + dz_k+1)).
+    __device__ __forceinline__ Recip<R> DZC(int k) const { return {0.5 * (P.dz[k] + P.dz[k + 1]), P.inv_dzc_f[k]}; }
     __device__ __forceinline__ R dzc(int k) const { return R(0.5) * (R(P.dz[k]) + R(P.dz[k + 1])); }
     // mu = rho nu at a centre; on an xy edge (four-point mean); on an xz or yz
     // edge (pair means of the two levels, weighted by the other level's
@@ -147,7 +151,7 @@ __device__ R sgs_strain_sq(const SgsParams& P, const float* u, const float* v, c
                 xz0[e] = xz1[e] = yz0[e] = yz1[e] = R(0.0);
                 continue;
             }
-            const R dzc = A.dzc(kk);
+            const Recip<R> dzc = A.DZC(kk);
             const int ii = xi[e], ii1 = sgs_next(ii, nx, P.px);
             xz0[e] = (A.f(u, ii, j, kk + 1) - A.f(u, ii, j, kk)) / dzc;
             xz1[e] = (A.wf(w, ii1, j, kk) - A.wf(w, ii, j, kk)) / A.DX();
@@ -236,10 +240,10 @@ __device__ R sgs_scalar_rate(const SgsParams& P, const float* rho, const float* 
     if (P.use_v)
     {
         const R ft = k < nz - 1 ? R(0.5) * (tr(i, j, k) + tr(i, j, k + 1)) *
-                                           (A.f(phi, i, j, k + 1) - A.f(phi, i, j, k)) / A.dzc(k)
+                                           (A.f(phi, i, j, k + 1) - A.f(phi, i, j, k)) / A.DZC(k)
                                      : R(0.0);
         const R fb = k > 0 ? R(0.5) * (tr(i, j, k - 1) + tr(i, j, k)) *
-                                      (A.f(phi, i, j, k) - A.f(phi, i, j, k - 1)) / A.dzc(k - 1)
+                                      (A.f(phi, i, j, k) - A.f(phi, i, j, k - 1)) / A.DZC(k - 1)
                                 : R(0.0);
         div += (ft - fb) / A.DZ(k);
     }
@@ -274,7 +278,7 @@ __device__ __forceinline__ R sgs_t13(const SgsParams& P, const float* u, const f
     R grad = dwdx;
     if (P.use_v)
     {
-        const R dudz = (A.f(u, i, j, k + 1) - A.f(u, i, j, k)) / A.dzc(k);
+        const R dudz = (A.f(u, i, j, k + 1) - A.f(u, i, j, k)) / A.DZC(k);
         grad = P.use_h ? dudz + dwdx : dudz;
     }
     return A.mu_z(rho, nu, i, j, i1, j, k) * grad;
@@ -290,7 +294,7 @@ __device__ __forceinline__ R sgs_t23(const SgsParams& P, const float* v, const f
     R grad = dwdy;
     if (P.use_v)
     {
-        const R dvdz = (A.f(v, i, j, k + 1) - A.f(v, i, j, k)) / A.dzc(k);
+        const R dvdz = (A.f(v, i, j, k + 1) - A.f(v, i, j, k)) / A.DZC(k);
         grad = P.use_h ? dvdz + dwdy : dvdz;
     }
     return A.mu_z(rho, nu, i, j, i, j1, k) * grad;
@@ -359,8 +363,8 @@ __device__ R sgs_dw(const SgsParams& P, const float* u, const float* v, const fl
     R force = R(0.0);
     if (P.use_v)
     {
-        const R t33_t = R(2.0) * A.mu(rho, nu, i, j, k + 1) * ((A.wf(w, i, j, k + 1) - A.wf(w, i, j, k)) / dzt);
-        const R t33_b = R(2.0) * A.mu(rho, nu, i, j, k) * ((A.wf(w, i, j, k) - A.wf(w, i, j, k - 1)) / dzb);
+        const R t33_t = R(2.0) * A.mu(rho, nu, i, j, k + 1) * ((A.wf(w, i, j, k + 1) - A.wf(w, i, j, k)) / A.DZ(k + 1));
+        const R t33_b = R(2.0) * A.mu(rho, nu, i, j, k) * ((A.wf(w, i, j, k) - A.wf(w, i, j, k - 1)) / A.DZ(k));
         force += t33_t - t33_b;
     }
     if (P.use_h)
