@@ -447,6 +447,38 @@ typedef struct nimbus_eos_args
 nimbus_status nimbus_cuda_eos_projection(nimbus_cuda_context* ctx, const nimbus_eos_args* a);
 
 /*
+ * Acoustic substep count before a large step.  The reference re-derives it
+ * before every large step from the live state: choose_runtime_timestep
+ * (src/numerics/runtime.cpp:712-880) samples c_max = max sqrt(gamma p / rho)
+ * over every cell (the flat Cartesian CFL scan, runtime.cpp:346-401) and the
+ * base columns (:854-870), and SplitExplicitScheme::resolve_substep_count
+ * (src/numerics/time_stepping/schemes/split_explicit/split_explicit.cpp:67-170)
+ * turns it into N = max(requested, ceil(dt c_max / (0.5 min(dx,dy,dz))) + 1, 2).
+ *
+ * nimbus_cuda_max_sound_speed scans p and rho (host or device memory as
+ * `memory`) on the device and returns c_max in *max_sound_speed after waiting
+ * for the scan; base columns (host memory, length nz) may be NULL.  A
+ * non-finite or non-positive pressure or density: NIMBUS_ERR_NONFINITE
+ * (where the reference throws).
+ * nimbus_cuda_resolve_substep_count: the count, or -1 where the reference
+ * throws (dt, c_max or spacing non-finite or non-positive; unrepresentable N).
+ */
+typedef struct nimbus_sound_speed_args
+{
+    const float* p;
+    const float* rho;
+    int nx, ny, nz;
+    const double* p0_base;    /* host, nz values, or NULL */
+    const double* rho0_base;  /* host, nz values, or NULL */
+    int memory;
+    void* stream;
+    double max_sound_speed;   /* out */
+} nimbus_sound_speed_args;
+
+nimbus_status nimbus_cuda_max_sound_speed(nimbus_cuda_context* ctx, nimbus_sound_speed_args* a);
+int nimbus_cuda_resolve_substep_count(double dt_large, double max_sound_speed, double min_spacing, int requested);
+
+/*
  * End-of-step sponge (state relaxation) on a flat C-grid level: the upper
  * Rayleigh sponge, the w-only lid absorber and the lateral band, in that
  * order, relaxing u, v, w toward (u_ref, v_ref, 0) and theta toward
@@ -777,6 +809,15 @@ typedef struct nimbus_member_desc
     int final_closure;       /* 1: end the step with the boundary closure
                                 apply_full_attributed (= apply_acoustic(0) on u, v,
                                 w, rho, p; dynamics.cpp:7415, after the sponge) */
+    int resolve_substeps;    /* 1: re-derive the substep count before every large
+                                step from the live state, as the reference does
+                                (choose_runtime_timestep, src/numerics/runtime.cpp:
+                                846-880, then SplitExplicitScheme::resolve_substep_count,
+                                split_explicit.cpp:67-170): N = max(n_substeps,
+                                ceil(dt c_max / (0.5 min(dx, dy, dz))) + 1, 2) with
+                                c_max = max sqrt(gamma p / rho) over the member's cells
+                                and base columns; n_substeps is then the requested
+                                minimum (0: the rule alone).  0: n_substeps every step. */
 } nimbus_member_desc;
 
 /* Host arrays [nx][ny][nz] of one member's prognostic state. */
@@ -838,14 +879,22 @@ nimbus_status nimbus_cuda_engine_set_lanes(nimbus_engine* e, int lanes);
 int nimbus_cuda_engine_lanes(const nimbus_engine* e);
 /* Enqueues n_steps large steps of every resident member on the engine's
  * stream: replayed from a CUDA graph when graphs are on (the default), the
- * graph rebuilt after admissions, retirements or a precision change. */
+ * graph rebuilt after admissions, retirements, a precision change or a
+ * changed substep count.  With resolve_substeps members, each step first
+ * scans every member's acoustic speed on the device and waits for the
+ * per-member maxima (a few bytes) before enqueuing the step, since the
+ * step's launches depend on the counts. */
 nimbus_status nimbus_cuda_engine_step(nimbus_engine* e, int n_steps);
 /* Waits for the enqueued steps; NIMBUS_ERR_NONFINITE when a retained mass
  * flux or transported scalar went non-finite or the EOS projection refused. */
 nimbus_status nimbus_cuda_engine_synchronize(nimbus_engine* e);
 /* A member's status bits (1 non-finite mass flux, 2 non-finite transported
- * scalar, 4 EOS projection refused); waits for enqueued steps. */
+ * scalar, 4 EOS projection refused, 16 a pressure or density failed the
+ * acoustic speed scan); waits for enqueued steps. */
 nimbus_status nimbus_cuda_engine_member_status(nimbus_engine* e, int member_id, unsigned* flags);
+/* The acoustic substep count of a member's last enqueued (or, before any,
+ * its first) large step. */
+nimbus_status nimbus_cuda_engine_member_substeps(nimbus_engine* e, int member_id, int* n_substeps);
 nimbus_status nimbus_cuda_engine_set_graph(nimbus_engine* e, int enable);
 int nimbus_cuda_engine_members(const nimbus_engine* e);
 /* Kernel launches one large step enqueues (batched over all members). */

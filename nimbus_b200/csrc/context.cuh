@@ -32,7 +32,7 @@ enum Slot
     kU, kV, kW, kRho, kP, kTheta, kRhoAlt, kDrho, kRho0, kP0, kMfx, kMfy, kMfz, kWave, kRhoBegin,
     kRhoEnd, kSf, kRl, kUAlt, kVAlt, kWAlt, kDp0, kSlowK1, kSlowStar, kSlowOut, kQv, kQc, kQr, kQv0, kU0, kV0,
     kQrAlt, kKesslerOut, kEosCandidate, kEos0, kRelaxTables, kCentre, kGround,
-    kSgsTables, kSgsCoef, kSgsRates, kSgsScratch, kSgsTheta0, kTke, kTkeRates,
+    kSgsTables, kSgsCoef, kSgsRates, kSgsScratch, kSgsTheta0, kTke, kTkeRates, kSoundSpeed,
     kQ0, kSlotCount = kQ0 + 2 * kMaxScalars
 };
 

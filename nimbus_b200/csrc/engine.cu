@@ -79,7 +79,9 @@ const char* check_desc(const nimbus_member_desc* d)
     if (!cells_fit(d->nx, d->ny, d->nz)) return "member grid too large";
     if (!finite_positive(d->dx) || !finite_positive(d->dy) || !finite_positive(d->dz) || !finite_positive(d->dt))
         return "spacing and dt must be finite and positive";
-    if (d->n_substeps < 1 || d->n_substeps > 4096) return "n_substeps must be in [1, 4096]";
+    if (d->resolve_substeps != 0 && d->resolve_substeps != 1) return "resolve_substeps must be 0 or 1";
+    if (d->resolve_substeps ? (d->n_substeps < 0 || d->n_substeps > 4096) : (d->n_substeps < 1 || d->n_substeps > 4096))
+        return "n_substeps must be in [1, 4096] ([0, 4096] as the requested minimum of resolve_substeps)";
     for (int a = 0; a < 4; ++a)
         if (d->bc[a] < 0 || d->bc[a] > 4) return "lateral boundary code out of range";
     if (d->bc[4] < 0 || d->bc[4] > 1 || d->bc[5] < 0 || d->bc[5] > 2) return "vertical boundary code out of range";
@@ -269,7 +271,7 @@ nimbus_status rebuild_table(nimbus_engine* e)
     std::vector<int> by_work(n);
     for (size_t i = 0; i < n; ++i) by_work[i] = static_cast<int>(i);
     auto work = [&](int i) {
-        return static_cast<double>(e->slots[i].m.items[kItemCells]) * (e->slots[i].desc.n_substeps + 3);
+        return static_cast<double>(e->slots[i].m.items[kItemCells]) * (e->slots[i].m.n_substeps + 3);
     };
     std::stable_sort(by_work.begin(), by_work.end(), [&](int a, int b) { return work(a) > work(b); });
     std::vector<std::vector<int>> members(lanes);
@@ -287,8 +289,8 @@ nimbus_status rebuild_table(nimbus_engine* e)
     {
         auto& m = members[k];
         std::stable_sort(m.begin(), m.end(), [&](int a, int b) {
-            return e->slots[a].desc.n_substeps > e->slots[b].desc.n_substeps || (e->slots[a].desc.n_substeps ==
-                   e->slots[b].desc.n_substeps && a < b);
+            const int na = e->slots[a].m.n_substeps, nb = e->slots[b].m.n_substeps;
+            return na > nb || (na == nb && a < b);
         });
         Lane& L = e->lanes[k];
         L.first = static_cast<int>(e->order.size());
@@ -363,6 +365,65 @@ nimbus_status rebuild_table(nimbus_engine* e)
         e->graph = nullptr;
     }
     e->dirty = false;
+    return NIMBUS_OK;
+}
+
+// Substep counts of the resolve_substeps members for the next large step
+// (the reference's choose_runtime_timestep + resolve_substep_count before
+// every step): scan every member's (gamma p) / rho on the device, wait for the
+// per-member maxima, and give each member whose count changed its new count
+// and substep parameters (the table and graph are then rebuilt).
+nimbus_status resolve_substeps(nimbus_engine* e)
+{
+    nimbus_cuda_context* ctx = e->ctx;
+    if (e->dirty) NB_TRY(rebuild_table(e));
+    const size_t n = e->order.size();
+    if (n == 0) return NIMBUS_OK;
+    if (n > e->c2_cap)
+    {
+        NB_CUDA(ctx, cudaStreamSynchronize(e->stream));
+        if (e->d_c2) cudaFree(e->d_c2);
+        if (e->h_c2) cudaFreeHost(e->h_c2);
+        e->d_c2 = nullptr;
+        e->h_c2 = nullptr;
+        e->c2_cap = 0;
+        const size_t cap = std::max<size_t>(n, 64);
+        NB_CUDA(ctx, cudaMalloc(&e->d_c2, cap * sizeof(unsigned long long)));
+        NB_CUDA(ctx, cudaMallocHost(&e->h_c2, cap * sizeof(unsigned long long)));
+        e->c2_cap = cap;
+    }
+    NB_CUDA(ctx, cudaMemsetAsync(e->d_c2, 0, n * sizeof(unsigned long long), e->stream));
+    for (const Lane& L : e->lanes)
+    {
+        const long long tiles = tiles_of(e, L, kItemCells, L.members);
+        if (tiles <= 0) continue;
+        engine_sound_speed_kernel<<<engine_grid(e, reinterpret_cast<const void*>(engine_sound_speed_kernel), tiles),
+                                    kEngineBlock, 0, e->stream>>>(e->d_table + L.first, prefix_of(e, L, kItemCells),
+                                                                  tiles, e->d_c2 + L.first);
+        ctx->launches += 1;
+    }
+    NB_CUDA(ctx, cudaGetLastError());
+    NB_CUDA(ctx, cudaMemcpyAsync(e->h_c2, e->d_c2, n * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                 e->stream));
+    NB_TRY(sync_table_to_host(e));  // waits for the copy; host views exact
+    for (size_t r = 0; r < n; ++r)
+    {
+        MemberSlot& slot = e->slots[static_cast<size_t>(e->order[r])];
+        if (!slot.desc.resolve_substeps) continue;
+        // 0: every cell failed the scan (flagged in the member's status word);
+        // the member keeps its count.
+        if (e->h_c2[r] == 0) continue;
+        const double c = std::max(std::sqrt(ordered_bits_to_double(e->h_c2[r])), slot.c_base);
+        const double spacing = std::min({slot.desc.dx, slot.desc.dy, slot.desc.dz});
+        const int count = resolve_substep_count(slot.desc.dt, c, spacing, slot.desc.n_substeps);
+        if (count < 1 || count > 4096)
+            return fail(ctx, NIMBUS_ERR_UNSUPPORTED, "a member's acoustic CFL needs an unsupported substep count");
+        if (count == slot.m.n_substeps) continue;
+        nimbus_member_desc d = slot.desc;
+        d.n_substeps = count;
+        fill_params(slot.m, &d);
+        e->dirty = true;
+    }
     return NIMBUS_OK;
 }
 
@@ -526,6 +587,8 @@ void nimbus_cuda_engine_destroy(nimbus_engine* e)
     if (e->d_prefix) cudaFree(e->d_prefix);
     if (e->d_image) cudaFree(e->d_image);
     if (e->d_centre) cudaFree(e->d_centre);
+    if (e->d_c2) cudaFree(e->d_c2);
+    if (e->h_c2) cudaFreeHost(e->h_c2);
     for (cudaStream_t ls : e->lane_streams) cudaStreamDestroy(ls);
     for (cudaEvent_t ev : e->lane_done) cudaEventDestroy(ev);
     if (e->fork) cudaEventDestroy(e->fork);
@@ -554,9 +617,37 @@ nimbus_status nimbus_cuda_engine_admit(nimbus_engine* e, const nimbus_member_des
         return fail(ctx, NIMBUS_ERR_OUT_OF_MEMORY, "member does not fit the free device memory");
     NB_TRY(sync_table_to_host(e));
 
+    // A resolve_substeps member starts with the count its initial state gives
+    // (the same scan the device repeats before every step).
+    nimbus_member_desc first = *desc;
+    double c_base = 0.0;
+    if (desc->resolve_substeps)
+    {
+        const double gamma = kCpd / (kCpd - kRd);
+        for (int k = 0; k < desc->nz; ++k)
+            if (!finite_positive(desc->p0_base[k]) || !finite_positive(desc->rho0_base[k]))
+                return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "base pressure and density must be positive and finite");
+        c_base = base_sound_speed(desc->p0_base, desc->rho0_base, desc->nz, gamma);
+        double best = 0.0;
+        for (size_t c = 0; c < L.cells; ++c)
+        {
+            const double ph = initial->p[c], rh = initial->rho[c];
+            if (!finite_positive(ph) || !finite_positive(rh))
+                return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT,
+                            "CFL scan requires finite wind and positive finite pressure/density");
+            best = std::max(best, gamma * ph / rh);
+        }
+        const int count = resolve_substep_count(desc->dt, std::max(std::sqrt(best), c_base),
+                                                std::min({desc->dx, desc->dy, desc->dz}), desc->n_substeps);
+        if (count < 1 || count > 4096)
+            return fail(ctx, NIMBUS_ERR_UNSUPPORTED, "the acoustic CFL needs an unsupported substep count");
+        first.n_substeps = count;
+    }
+
     MemberSlot slot;
     slot.id = e->next_id;
     slot.desc = *desc;
+    slot.c_base = c_base;
     slot.desc.rho0_base = slot.desc.p0_base = slot.desc.qv0_base = slot.desc.u0_base = slot.desc.v0_base = nullptr;
     slot.desc.sponge = nullptr;
     slot.bytes = L.total;
@@ -603,7 +694,7 @@ nimbus_status nimbus_cuda_engine_admit(nimbus_engine* e, const nimbus_member_des
     float4* eos0 = reinterpret_cast<float4*>(base + L.off_eos0);
     M.dp0 = dp0;
     M.eos0 = eos0;
-    fill_params(M, desc);
+    fill_params(M, &first);
 
     // Profiles, the split hydrostatic difference and the initial state.
     std::vector<double> hp(5 * nz, 0.0);
@@ -811,15 +902,32 @@ nimbus_status nimbus_cuda_engine_step(nimbus_engine* e, int n_steps)
         }
         NB_TRY(build_graph(e));
     }
+    bool resolving = false;
+    for (const auto& slot : e->slots) resolving = resolving || slot.desc.resolve_substeps;
     for (int i = 0; i < n_steps; ++i)
     {
+        if (resolving)
+        {
+            NB_TRY(resolve_substeps(e));
+            if (e->dirty) NB_TRY(rebuild_table(e));
+            if (graph && !e->exec) NB_TRY(build_graph(e));
+        }
         if (graph) NB_CUDA(ctx, cudaGraphLaunch(e->exec, e->stream));
         else e->launches_per_step = enqueue(e, e->stream);
         ctx->launches += static_cast<uint64_t>(e->launches_per_step);
+        rotate_host_views(e, 1);
+        e->table_current = e->mirror_exact;
     }
     NB_CUDA(ctx, cudaGetLastError());
-    rotate_host_views(e, n_steps);
-    e->table_current = e->mirror_exact;
+    return NIMBUS_OK;
+}
+
+nimbus_status nimbus_cuda_engine_member_substeps(nimbus_engine* e, int member_id, int* n_substeps)
+{
+    if (!e || !n_substeps) return NIMBUS_ERR_INVALID_ARGUMENT;
+    MemberSlot* s = find_slot(e, member_id);
+    if (!s) return fail(e->ctx, NIMBUS_ERR_INVALID_ARGUMENT, "unknown member id");
+    *n_substeps = s->m.n_substeps;
     return NIMBUS_OK;
 }
 

@@ -18,6 +18,7 @@ struct MemberSlot
     void* arena = nullptr;
     size_t bytes = 0;
     nimbus::EngineMember m;   // host view of the device entry (refreshed before use)
+    double c_base = 0.0;      // largest sound speed of the base columns (resolve_substeps members)
 };
 // A lane: a contiguous run of table rows whose members step together.  The
 // members are split into size-balanced lanes; each lane's launches go to its
@@ -70,6 +71,9 @@ struct nimbus_engine
     size_t image_cap = 0;           // bytes
     float* d_centre = nullptr;      // device staging for history frames
     size_t centre_cap = 0;          // bytes
+    unsigned long long* d_c2 = nullptr;  // per table row: max (gamma p) / rho before a step
+    unsigned long long* h_c2 = nullptr;  // pinned host copy
+    size_t c2_cap = 0;                   // rows
 };
 
 namespace

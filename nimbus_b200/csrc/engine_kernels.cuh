@@ -360,6 +360,48 @@ static __global__ void __launch_bounds__(256) engine_transport_update_kernel(con
     });
 }
 
+// ---- Acoustic speed scan before a large step --------------------------------
+// Per member the largest (gamma p) / rho of its cells, as ordered double bits
+// into c2[row] (row = the member's table row in this launch), for the
+// substep count the reference re-derives before every large step
+// (src/numerics/runtime.cpp:346-401,854-880).  The member of a tile is
+// block-uniform, so a block keeps a running maximum while it walks one
+// member's tiles and publishes it with one atomicMax when it moves on.
+static __global__ void __launch_bounds__(256) engine_sound_speed_kernel(const EngineMember* __restrict__ table,
+                                                                        const long long* __restrict__ prefix,
+                                                                        long long tiles, unsigned long long* c2)
+{
+    int m = 0, held = -1;
+    unsigned long long best = 0;
+    for (long long t = blockIdx.x; t < tiles; t += gridDim.x)
+    {
+        while (t >= prefix[m + 1]) ++m;
+        if (m != held)
+        {
+            if (held >= 0)
+            {
+                const unsigned long long b = block_max_u64(best);
+                if (threadIdx.x == 0 && b) atomicMax(c2 + held, b);
+            }
+            held = m;
+            best = 0;
+        }
+        const EngineMember& M = table[m];
+        const int c = (int)((t - prefix[m]) * blockDim.x) + (int)threadIdx.x;
+        if (c < M.items[kItemCells])
+        {
+            unsigned flags = 0;
+            best = max(best, sound_speed_sq_bits(M.gamma, M.p[c], M.rho[c], flags));
+            if (flags) atomicOr(M.status, flags);
+        }
+    }
+    if (held >= 0)
+    {
+        const unsigned long long b = block_max_u64(best);
+        if (threadIdx.x == 0 && b) atomicMax(c2 + held, b);
+    }
+}
+
 // ---- Kessler and EOS --------------------------------------------------------
 
 // The Kessler step and the EOS re-projection in one pass: the candidate

@@ -865,6 +865,63 @@ nimbus_status nimbus_cuda_eos_projection(nimbus_cuda_context* ctx, const nimbus_
     return NIMBUS_OK;
 }
 
+nimbus_status nimbus_cuda_max_sound_speed(nimbus_cuda_context* ctx, nimbus_sound_speed_args* a)
+{
+    if (!ctx || !a) return NIMBUS_ERR_INVALID_ARGUMENT;
+    if (!a->p || !a->rho || a->nx < 1 || a->ny < 1 || a->nz < 1 || !cells_fit(a->nx, a->ny, a->nz))
+        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "invalid sound speed scan arguments");
+    if ((a->p0_base == nullptr) != (a->rho0_base == nullptr))
+        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "p0_base and rho0_base come together");
+    if (a->memory != NIMBUS_MEMORY_HOST && a->memory != NIMBUS_MEMORY_DEVICE)
+        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "unknown memory kind");
+    NB_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const size_t n = static_cast<size_t>(a->nx) * a->ny * a->nz;
+    const float* p = a->p;
+    const float* rho = a->rho;
+    if (a->memory == NIMBUS_MEMORY_DEVICE)
+    {
+        if (a->stream) st = static_cast<cudaStream_t>(a->stream);
+    }
+    else
+    {
+        float *dp, *drho;
+        NB_TRY(ensure(ctx, kP, n, &dp));
+        NB_TRY(ensure(ctx, kRho, n, &drho));
+        NB_TRY(upload(ctx, dp, a->p, n * sizeof(float)));
+        NB_TRY(upload(ctx, drho, a->rho, n * sizeof(float)));
+        if (st != ctx->stream) NB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        p = dp;
+        rho = drho;
+    }
+    // Its own result slot and flag word: the context's status word keeps the
+    // flags of work enqueued before this call for nimbus_cuda_synchronize.
+    unsigned long long* slot = nullptr;
+    NB_TRY(ensure(ctx, kSoundSpeed, 2, &slot));
+    NB_CUDA(ctx, cudaMemsetAsync(slot, 0, 2 * sizeof(unsigned long long), st));
+    const double gamma = kCpd / (kCpd - kRd);
+    max_sound_speed_kernel<<<grid_for(ctx, static_cast<long long>(n)), kThreads, 0, st>>>(
+        p, rho, static_cast<long long>(n), gamma, slot, reinterpret_cast<unsigned*>(slot + 1));
+    NB_CUDA(ctx, cudaGetLastError());
+    ctx->launches += 1;
+    unsigned long long result[2] = {0, 0};
+    NB_CUDA(ctx, cudaMemcpyAsync(result, slot, sizeof result, cudaMemcpyDeviceToHost, st));
+    NB_CUDA(ctx, cudaStreamSynchronize(st));
+    const unsigned long long bits = result[0];
+    const unsigned flags = static_cast<unsigned>(result[1]);
+    if (flags & kStatusInvalidState)
+        return fail(ctx, NIMBUS_ERR_NONFINITE, "CFL scan requires finite wind and positive finite pressure/density");
+    double c = std::sqrt(ordered_bits_to_double(bits));
+    if (a->p0_base) c = std::max(c, base_sound_speed(a->p0_base, a->rho0_base, a->nz, gamma));
+    a->max_sound_speed = c;
+    return NIMBUS_OK;
+}
+
+int nimbus_cuda_resolve_substep_count(double dt_large, double max_sound_speed, double min_spacing, int requested)
+{
+    return resolve_substep_count(dt_large, max_sound_speed, min_spacing, requested);
+}
+
 nimbus_status nimbus_cuda_set_precision(nimbus_cuda_context* ctx, int precision)
 {
     if (!ctx) return NIMBUS_ERR_INVALID_ARGUMENT;

@@ -7,7 +7,9 @@
 // dependencies allow.
 #pragma once
 
+#include <cmath>
 #include <cstdint>
+#include <cstring>
 #include <cuda_runtime.h>
 
 namespace nimbus
@@ -47,6 +49,7 @@ enum : unsigned
     kStatusNonfiniteTransport = 1u << 1,
     kStatusInvalidEos = 1u << 2,
     kStatusSgsInvalid = 1u << 3,
+    kStatusInvalidState = 1u << 4,  // a pressure or density failed the CFL scan (non-finite or <= 0)
 };
 
 struct Dims
@@ -117,4 +120,100 @@ __device__ __forceinline__ float clamp_value(float v, float fallback, float lo, 
     return v < lo ? lo : (hi < v ? hi : v);
 }
 
+// ---- Acoustic speed scan ------------------------------------------------
+// Before every large step the reference samples c_max = max sqrt(gamma p / rho)
+// over the state (the flat Cartesian CFL scan, src/numerics/runtime.cpp:346-401,
+// the product formed as (gamma * p) / rho in FP64) and derives the substep
+// count from it.  sqrt is monotone and correctly rounded, so the maximum of
+// (gamma p) / rho followed by one sqrt is that maximum exactly; a
+// non-negative double's bits order like its value, so the maximum is an
+// integer atomicMax.
+
+// (gamma p) / rho of one cell as ordered double bits; 0 and an invalid-state
+// flag where p or rho is non-finite or non-positive (where the reference throws).
+__device__ __forceinline__ unsigned long long sound_speed_sq_bits(double gamma, float p, float rho, unsigned& flags)
+{
+    const double ph = (double)p, rh = (double)rho;
+    if (!(isfinite(ph) && ph > 0.0 && isfinite(rh) && rh > 0.0))
+    {
+        flags |= kStatusInvalidState;
+        return 0ull;
+    }
+    return (unsigned long long)__double_as_longlong(gamma * ph / rh);
+}
+
+// Maximum of v over the block, valid in thread 0.  Every thread of the block
+// calls it (it synchronises the block).
+__device__ __forceinline__ unsigned long long block_max_u64(unsigned long long v)
+{
+    __shared__ unsigned long long part[32];
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();  // an earlier call may still read part[]
+    if (lane == 0) part[warp] = v;
+    __syncthreads();
+    if (warp == 0)
+    {
+        const int warps = (blockDim.x + 31) >> 5;
+        v = lane < warps ? part[lane] : 0ull;
+        for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    }
+    return v;
+}
+
+// Grid-stride scan of one field pair: the maximum into *out (atomicMax of
+// the ordered bits), invalid cells into *status.
+static __global__ void __launch_bounds__(256) max_sound_speed_kernel(const float* __restrict__ p,
+                                                                     const float* __restrict__ rho, long long n,
+                                                                     double gamma, unsigned long long* out,
+                                                                     unsigned* status)
+{
+    unsigned long long best = 0;
+    unsigned flags = 0;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x)
+        best = max(best, sound_speed_sq_bits(gamma, p[c], rho[c], flags));
+    best = block_max_u64(best);
+    if (threadIdx.x == 0 && best) atomicMax(out, best);
+    if (flags) atomicOr(status, flags);
+}
+
 }  // namespace nimbus
+
+namespace nimbus_host
+{
+// SplitExplicitScheme::resolve_substep_count
+// (src/numerics/time_stepping/schemes/split_explicit/split_explicit.cpp:67-170)
+// with a positive minimum spacing: N = max(requested, max(ceil(dt c_max /
+// (0.5 min_spacing)) + 1, 2)), requested <= 0 meaning the CFL rule alone;
+// -1 where the reference throws.
+inline int resolve_substep_count(double dt_large, double c_max, double min_spacing, int requested)
+{
+    if (!(dt_large > 0.0) || !std::isfinite(dt_large)) return -1;
+    if (!(c_max > 0.0) || !std::isfinite(c_max)) return -1;
+    if (!(min_spacing > 0.0) || !std::isfinite(min_spacing)) return -1;
+    const double required_real = dt_large * c_max / (0.5 * min_spacing);
+    if (!std::isfinite(required_real) || required_real >= 2147483646.0) return -1;
+    int required = static_cast<int>(std::ceil(required_real)) + 1;
+    if (required < 2) required = 2;
+    return requested > 0 ? (requested > required ? requested : required) : required;
+}
+
+// Largest sqrt(gamma p0 / rho0) of the base columns (runtime.cpp:854-870).
+inline double base_sound_speed(const double* p0, const double* rho0, int nz, double gamma)
+{
+    double best = 0.0;
+    for (int k = 0; k < nz; ++k)
+    {
+        const double s = std::sqrt(gamma * p0[k] / rho0[k]);
+        if (best < s) best = s;
+    }
+    return best;
+}
+
+inline double ordered_bits_to_double(unsigned long long b)
+{
+    double x;
+    std::memcpy(&x, &b, sizeof x);
+    return x;
+}
+}  // namespace nimbus_host

@@ -165,6 +165,15 @@ class MemberDesc(ctypes.Structure):
         ("microphysics", ctypes.c_int),
         ("rho0_base", _dp), ("p0_base", _dp), ("qv0_base", _dp), ("u0_base", _dp), ("v0_base", _dp),
         ("sponge", ctypes.POINTER(SpongeDesc)), ("final_closure", ctypes.c_int),
+        ("resolve_substeps", ctypes.c_int),
+    ]
+
+
+class SoundSpeedArgs(ctypes.Structure):
+    _fields_ = [
+        ("p", _fp), ("rho", _fp), ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("p0_base", _dp), ("rho0_base", _dp), ("memory", ctypes.c_int), ("stream", ctypes.c_void_p),
+        ("max_sound_speed", ctypes.c_double),
     ]
 
 
@@ -243,7 +252,8 @@ EXPORTED_SYMBOLS = (
     "nimbus_cuda_engine_upload_image_async", "nimbus_cuda_engine_download_image_async",
     "nimbus_cuda_engine_set_lanes", "nimbus_cuda_engine_lanes",
     "nimbus_cuda_engine_synchronize", "nimbus_cuda_engine_member_status", "nimbus_cuda_engine_set_graph",
-    "nimbus_cuda_engine_members", "nimbus_cuda_engine_launches_per_step",
+    "nimbus_cuda_engine_members", "nimbus_cuda_engine_launches_per_step", "nimbus_cuda_engine_member_substeps",
+    "nimbus_cuda_max_sound_speed", "nimbus_cuda_resolve_substep_count",
 )
 SUBSTEP_AUTO, SUBSTEP_FUSED, SUBSTEP_SPLIT = 0, 1, 2
 PRECISION_REFERENCE, PRECISION_FP32 = 0, 1
@@ -339,6 +349,10 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
     lib.nimbus_cuda_engine_set_graph.argtypes = [vp, ctypes.c_int]
     lib.nimbus_cuda_engine_members.argtypes = [vp]
     lib.nimbus_cuda_engine_launches_per_step.argtypes = [vp]
+    lib.nimbus_cuda_engine_member_substeps.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    lib.nimbus_cuda_max_sound_speed.argtypes = [vp, ctypes.POINTER(SoundSpeedArgs)]
+    lib.nimbus_cuda_resolve_substep_count.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                                      ctypes.c_int]
     lib.nimbus_cuda_set_kernel_timing.argtypes = [ctypes.c_void_p, ctypes.c_int]
     lib.nimbus_cuda_kernel_timing.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64),
                                               ctypes.POINTER(ctypes.c_double)]
@@ -466,6 +480,29 @@ class Context:
 
     def eos_projection(self, args: EosArgs) -> int:
         return self.lib.nimbus_cuda_eos_projection(self.handle, ctypes.byref(args))
+
+    def max_sound_speed(self, p, rho, shape, base=None, stream=None) -> float:
+        """Largest sqrt(gamma p / rho) over the fields (host float32 arrays or
+        device tensors) and, with `base`, its p0/rho0 columns; waits for it."""
+        a = SoundSpeedArgs()
+        a.p, a.rho = _f(p), _f(rho)
+        a.nx, a.ny, a.nz = (int(x) for x in shape)
+        keep = None
+        if base is not None:
+            keep = (np.ascontiguousarray(base["p0"], np.float64), np.ascontiguousarray(base["rho0"], np.float64))
+            a.p0_base, a.rho0_base = _d(keep[0]), _d(keep[1])
+        a.memory = MEMORY_DEVICE if hasattr(p, "data_ptr") else MEMORY_HOST
+        a.stream = stream
+        self.check(self.lib.nimbus_cuda_max_sound_speed(self.handle, ctypes.byref(a)))
+        return a.max_sound_speed
+
+    def resolve_substep_count(self, dt, c_max, min_spacing, requested=0) -> int:
+        """The reference's substep-count rule (split_explicit.cpp:67-170)."""
+        n = int(self.lib.nimbus_cuda_resolve_substep_count(float(dt), float(c_max), float(min_spacing),
+                                                             int(requested)))
+        if n < 1:
+            raise ValueError("split-explicit acoustic CFL cannot be resolved")
+        return n
 
     def acoustic_boundaries(self, args: BoundaryArgs) -> int:
         return self.lib.nimbus_cuda_acoustic_boundaries(self.handle, ctypes.byref(args))
@@ -845,10 +882,12 @@ def sponge_desc(profiles) -> SpongeDesc:
 
 
 def member_desc(shape, grid, dt, n_substeps, bc, base, coriolis_f=0.0, frame=(0.0, 0.0),
-                microphysics=1, sponge=None, final_closure=False) -> MemberDesc:
+                microphysics=1, sponge=None, final_closure=False, resolve_substeps=False) -> MemberDesc:
     """Descriptor of one engine member; `base` holds the FP64 profiles
     rho0, p0, qv0 (and optionally u0, v0); `sponge` (SpongeProfiles) adds the
-    end-of-step sponge, `final_closure` the closing boundary refresh."""
+    end-of-step sponge, `final_closure` the closing boundary refresh.  With
+    resolve_substeps the substep count is re-derived from the state before
+    every large step and n_substeps is the requested minimum (0: none)."""
     d = MemberDesc()
     d.nx, d.ny, d.nz = (int(x) for x in shape)
     d.dx, d.dy, d.dz = grid
@@ -869,6 +908,7 @@ def member_desc(shape, grid, dt, n_substeps, bc, base, coriolis_f=0.0, frame=(0.
         d._sponge = sd
         d.sponge = ctypes.pointer(sd)
     d.final_closure = int(bool(final_closure))
+    d.resolve_substeps = int(bool(resolve_substeps))
     return d
 
 
@@ -927,6 +967,12 @@ class Engine:
         self.ctx.check(rc)
         self.shapes[mid.value] = (desc.nx, desc.ny, desc.nz)
         return mid.value
+
+    def member_substeps(self, member_id: int) -> int:
+        """Substep count of the member's last enqueued (or first) large step."""
+        n = ctypes.c_int(0)
+        self.ctx.check(self.lib.nimbus_cuda_engine_member_substeps(self.handle, int(member_id), ctypes.byref(n)))
+        return n.value
 
     def retire(self, member_id: int):
         self.ctx.check(self.lib.nimbus_cuda_engine_retire(self.handle, int(member_id)))

@@ -163,10 +163,13 @@ def initial_state(case: Case):
 
 
 def max_sound_speed(p: np.ndarray, rho: np.ndarray, base) -> float:
-    """Largest sqrt(gamma p / rho) over the state and the base columns
-    (the acoustic speed sampled by src/numerics/runtime.cpp:846-878)."""
-    c_state = float(np.sqrt(GAMMA * np.max(p.astype(np.float64) / rho.astype(np.float64))))
-    c_base = float(np.sqrt(GAMMA * np.max(base["p0"] / base["rho0"])))
+    """Largest sqrt(gamma p / rho) over the state and the base columns (the
+    acoustic speed choose_runtime_timestep samples before every large step,
+    src/numerics/runtime.cpp:346-401,854-870), each product formed as
+    (gamma * p) / rho in FP64; the maximum is taken before the (monotone,
+    correctly rounded) square root, which gives the same value."""
+    c_state = float(np.sqrt(np.max(GAMMA * p.astype(np.float64) / rho.astype(np.float64))))
+    c_base = float(np.sqrt(np.max(GAMMA * np.asarray(base["p0"], np.float64) / np.asarray(base["rho0"], np.float64))))
     return max(c_state, c_base)
 
 

@@ -27,9 +27,16 @@
 //       0.25, ...), and differs by their FP32 rounding otherwise.
 //   SgsApply  the same widening of dt_step and the bounds; a dispatch that
 //       asks for a completion observer is declined (false).
+//   ConservativeCartesianCgridTransport  the coupled WENO5/MC transport of the
+//       retained acoustic context (advection_batch.cpp's route): FP64 spacings
+//       from the level's state view and dt_step_host, so the result is the CPU
+//       backend's bit for bit; see the dispatch for what it declines.
 #include "compute/backend_interface.hpp"
+#include "compute/dispatch/advection.hpp"
 #include "compute/dispatch/dynamics.hpp"
 #include "compute/dispatch/turbulence.hpp"
+#include "core/runtime/runtime_config.hpp"
+#include "core/runtime/simulation_state.hpp"
 
 #include "../../include/nimbus_cuda.h"
 
@@ -41,6 +48,7 @@ namespace
 {
 
 class NimbusCudaComputeBackend final : public ComputeBackend,
+                                       public AdvectionComputeKernels,
                                        public DynamicsComputeKernels,
                                        public TurbulenceComputeKernels
 {
@@ -70,10 +78,74 @@ public:
 
     std::uint64_t successful_dispatch_count() const override { return dispatches_; }
 
+    AdvectionComputeKernels* advection_kernels() override { return ctx_ ? this : nullptr; }
+    const AdvectionComputeKernels* advection_kernels() const override { return ctx_ ? this : nullptr; }
     DynamicsComputeKernels* dynamics_kernels() override { return ctx_ ? this : nullptr; }
     const DynamicsComputeKernels* dynamics_kernels() const override { return ctx_ ? this : nullptr; }
     TurbulenceComputeKernels* turbulence_kernels() override { return ctx_ ? this : nullptr; }
     const TurbulenceComputeKernels* turbulence_kernels() const override { return ctx_ ? this : nullptr; }
+
+    bool supports(AdvectionKernelOp op) const override
+    {
+        return op == AdvectionKernelOp::ConservativeCartesianCgridTransport;
+    }
+
+    bool supports_supplied_cartesian_cgrid_mass_flux() const override { return true; }
+
+    // The coupled transport of the retained acoustic context: the face mass
+    // fluxes and beginning density the split continuity solve accumulated.
+    // The raw ABI carries FP32 inverse spacings and dt; the level's state
+    // view (execution_state) and dt_step_host carry the FP64 values the CPU
+    // backend uses, and its configuration the open-top flag, so the result is
+    // the CPU backend's bit for bit.  Declined (false, nothing written): no
+    // state view, the instantaneous-flux mode, a positive-support
+    // reconstruction, non-zero kappas, terrain, a collocated grid, or any
+    // requested boundary / energy report or interface-flux register (this
+    // backend produces none, and a non-null report must be produced or the
+    // dispatch refused).
+    bool dispatch_advect_scalars_conservative_cartesian_cgrid(
+        const ConservativeCartesianCgridTransportDispatch& d) override
+    {
+        if (!ctx_ || d.n_scalars < 0 || d.n_scalars > 16) return false;
+        if (d.n_scalars == 0) return true;
+        if (!d.use_supplied_mass_flux || !d.density_begin || !d.mass_flux_x || !d.mass_flux_y || !d.mass_flux_z)
+            return false;
+        if (!d.q_in || !d.q_out || !d.positive_definite || !d.rho_data || d.preserve_positive_support) return false;
+        const SimulationStateView* es = d.execution_state;
+        if (!es || !es->configuration || es->configuration->stagger_type != StaggerType::CGrid) return false;
+        if (es->process_grid_metrics && es->process_grid_metrics->terrain_metrics_active) return false;
+        for (int s = 0; s < d.n_scalars; ++s)
+        {
+            if (d.dt_kappas && d.dt_kappas[s] != 0.0f) return false;
+            if (d.host_kappas && d.host_kappas[s] != 0.0) return false;
+            if (d.host_boundary_reports && d.host_boundary_reports[s]) return false;
+            if (d.host_energy_reports && d.host_energy_reports[s]) return false;
+            if (d.host_energy_kinds && d.host_energy_kinds[s] != tmv::ScalarMoistEnergyKind::None) return false;
+            if (d.host_interface_registers && d.host_interface_registers[s]) return false;
+        }
+        nimbus_scalar_transport_args a{};
+        a.q_in = d.q_in;
+        a.q_out = d.q_out;
+        a.positive_definite = d.positive_definite;
+        a.n_scalars = d.n_scalars;
+        a.nx = d.nx;
+        a.ny = d.ny;
+        a.nz = d.nz;
+        a.dx = es->grid.dr;
+        a.dy = es->grid.dtheta;
+        a.dz = es->grid.dz;
+        a.dt = d.dt_step_host > 0.0 ? d.dt_step_host : static_cast<double>(d.dt_step);
+        a.rho_end = d.rho_data;
+        a.rho_begin = d.density_begin;
+        a.mass_flux_x = d.mass_flux_x;
+        a.mass_flux_y = d.mass_flux_y;
+        a.mass_flux_z = d.mass_flux_z;
+        a.weno = d.weno ? 1 : 0;
+        a.top_open = es->configuration->top_bc == tmv::init::config::TopBC::Open ? 1 : 0;
+        a.rho_floor = d.rho_floor;
+        a.memory = NIMBUS_MEMORY_HOST;
+        return count(nimbus_cuda_scalar_transport(ctx_, &a));
+    }
 
     bool supports(DynamicsKernelOp op) const override
     {

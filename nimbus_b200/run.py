@@ -49,7 +49,8 @@ def substeps_for(case: Case, state, base) -> int:
 class ResidentRun:
     def __init__(self, ctx: cuda.Context, case: Case, state=None, base=None, device="cuda",
                  precision: int = cuda.PRECISION_FP32, autotune: bool = True, coriolis_f: float = 0.0,
-                 microphysics: bool = True, sponge=None, final_closure: bool = False, sgs=None):
+                 microphysics: bool = True, sponge=None, final_closure: bool = False, sgs=None,
+                 resolve: bool = True):
         self.ctx = ctx
         self.precision = precision
         self.tuned = None
@@ -77,9 +78,12 @@ class ResidentRun:
         self._slow = cuda.slow_args(f, self.prof, grid, dt_large=case.dt, coriolis_f=coriolis_f,
                                     memory=cuda.MEMORY_DEVICE)
         self._refresh = cuda.boundary_args(f, grid, case.bc, 0.0)
-        self._loop = cuda.batched_args(f, self.prof["rho0"], self.prof["p0"], case.dt / n, n, grid, case.bc,
-                                       *self.mf, (case.dt / n) / case.dt, None, self.wave, self.rho_begin,
-                                       memory=cuda.MEMORY_DEVICE)
+        # resolve: the substep count re-derived from the state before every
+        # large step, as the reference does (one device scan of p and rho and
+        # a host wait per step); otherwise the admission count throughout.
+        self.resolve = resolve
+        self.substep_counts = []
+        self._loop = self._loop_args(n)
         qs = [f[k] for k in SCALARS]
         self._transport = cuda.transport_args(qs, qs, POSITIVE, f["rho"], self.rho_begin, *self.mf, case.dt,
                                               grid, weno=True, top_open=case.bc[5] == 2, memory=cuda.MEMORY_DEVICE)
@@ -97,14 +101,35 @@ class ResidentRun:
                      if sgs is not None else None)
         self.torch_stream = torch.cuda.ExternalStream(self.stream, device=dev)
 
+    def _loop_args(self, n: int):
+        case = self.case
+        grid = (case.dx, case.dy, case.dz)
+        return cuda.batched_args(self.fields, self.prof["rho0"], self.prof["p0"], case.dt / n, n, grid, case.bc,
+                                 *self.mf, (case.dt / n) / case.dt, None, self.wave, self.rho_begin,
+                                 memory=cuda.MEMORY_DEVICE)
+
     @property
     def cells(self) -> int:
         return self.case.cells
 
+    def resolve_substeps(self) -> int:
+        """The substep count the reference would use for the next large step
+        from the current device state (waits for enqueued work)."""
+        case, c = self.case, self.ctx
+        c_max = c.max_sound_speed(self.fields["p"], self.fields["rho"], case.shape, self.base)
+        return c.resolve_substep_count(case.dt, c_max, min(case.dx, case.dy, case.dz), case.substeps)
+
     def step(self):
-        """Enqueue one large step on the context stream (no host synchronisation)."""
+        """Enqueue one large step on the context stream (without resolve, no
+        host synchronisation)."""
         c = self.ctx
         c.set_precision(self.precision)
+        if self.resolve:
+            n = self.resolve_substeps()
+            if n != self.n_substeps:
+                self.n_substeps = n
+                self._loop = self._loop_args(n)
+        self.substep_counts.append(self.n_substeps)
         c.check(c.slow_step(self._slow))
         c.check(c.acoustic_boundaries(self._refresh))
         with torch.cuda.stream(self.torch_stream):
@@ -145,15 +170,27 @@ class EngineRun:
         self.members = {}
 
     def admit(self, case: Case, state=None, base=None, coriolis_f: float = 0.0, microphysics: bool = True,
-              reserve_bytes: int = 0, n_substeps: int | None = None, sponge=None, final_closure: bool = False):
+              reserve_bytes: int = 0, n_substeps: int | None = None, sponge=None, final_closure: bool = False,
+              resolve: bool | None = None):
+        """Admit a run.  Without n_substeps (or with resolve=True) the engine
+        re-derives its substep count before every large step from the live
+        state, with case.substeps (or n_substeps) as the requested minimum,
+        as the reference does; an explicit n_substeps alone fixes the count."""
         if state is None:
             state, base = initial_state(case)
-        n = n_substeps or substeps_for(case, state, base)
+        if resolve is None:
+            resolve = n_substeps is None
+        n = n_substeps if n_substeps is not None else (case.substeps if resolve else substeps_for(case, state, base))
         desc = cuda.member_desc(case.shape, (case.dx, case.dy, case.dz), case.dt, n, case.bc, base, coriolis_f,
-                                microphysics=int(microphysics), sponge=sponge, final_closure=final_closure)
+                                microphysics=int(microphysics), sponge=sponge, final_closure=final_closure,
+                                resolve_substeps=resolve)
         mid = self.engine.admit(desc, state, reserve_bytes)
-        self.members[mid] = (case, n)
+        self.members[mid] = (case, self.engine.member_substeps(mid))
         return mid
+
+    def substeps(self, member_id: int) -> int:
+        """Substep count of the member's last enqueued (or first) large step."""
+        return self.engine.member_substeps(member_id)
 
     def step(self, n: int = 1):
         self.ctx.set_precision(self.precision)
@@ -219,8 +256,12 @@ class HostPipeline:
         overlap.  Waits for all of them before returning."""
         self.ctx.set_precision(self.precision)
         for _ in range(n):
+            # Every group's upload first: a step waits for its group's
+            # acoustic speed scan (the substep counts depend on the uploaded
+            # state), and the other groups' copies proceed meanwhile.
             for run, image in zip(self.runs, self.images):
                 run.engine.upload_image_async(image)
+            for run, image in zip(self.runs, self.images):
                 run.engine.step(1)
                 run.engine.download_image_async(image)
         for run in self.runs:

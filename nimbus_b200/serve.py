@@ -21,7 +21,7 @@ import numpy as np
 
 from . import cuda
 from .initial import initial_state
-from .run import EngineRun, ResidentRun, substeps_for
+from .run import EngineRun, ResidentRun
 
 
 @dataclass
@@ -79,9 +79,9 @@ class Server:
             while queue:  # FIFO admission while the head fits
                 r = queue[0]
                 state, base = prepared[r.rid] if prepared else initial_state(r.case)
-                n_sub = substeps_for(r.case, state, base)
-                desc = cuda.member_desc(r.case.shape, (r.case.dx, r.case.dy, r.case.dz), r.case.dt, n_sub,
-                                        r.case.bc, base)
+                # the substep count is re-derived before every step, as the reference does
+                desc = cuda.member_desc(r.case.shape, (r.case.dx, r.case.dy, r.case.dz), r.case.dt,
+                                        r.case.substeps, r.case.bc, base, resolve_substeps=True)
                 mid = eng.try_admit(desc, state, self.reserve)
                 if mid is None:
                     if not active:

@@ -204,6 +204,42 @@ class Restatement:
             self.acoustic_boundaries(st, grid, bc, 0.0)
         return loop
 
+    def max_sound_speed(self, st, base):
+        """Largest sqrt(gamma p / rho) over the state and the base columns
+        (runtime.cpp:346-401, 854-870); raises on a non-finite or
+        non-positive pressure or density, where the reference throws."""
+        self._chk(st["p"], st["rho"])
+        nx, ny, nz = st["p"].shape
+        out = ctypes.c_double(0.0)
+        p0 = np.ascontiguousarray(base["p0"], np.float64)
+        rho0 = np.ascontiguousarray(base["rho0"], np.float64)
+        if self.lib.oracle_max_sound_speed(nx, ny, nz, _fp(st["p"]), _fp(st["rho"]), _fp(p0), _fp(rho0),
+                                           ctypes.byref(out)) != 0:
+            raise ValueError("CFL scan requires finite wind and positive finite pressure/density")
+        return out.value
+
+    def resolve_substeps(self, dt, c_max, min_spacing, requested=0):
+        """split_explicit.cpp:67-170 with a positive diagnosed spacing."""
+        self.lib.oracle_resolve_substeps.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int]
+        n = self.lib.oracle_resolve_substeps(dt, c_max, min_spacing, int(requested))
+        if n < 1:
+            raise ValueError("split-explicit acoustic CFL cannot be resolved")
+        return n
+
+    def substeps(self, st, base, grid, dt, requested=0):
+        """The substep count the reference uses for a large step from this state."""
+        return self.resolve_substeps(dt, self.max_sound_speed(st, base), min(grid), requested)
+
+    def run(self, st, base, grid, dt, steps, bc, requested=0, **kw):
+        """`steps` large steps in place, the substep count re-derived from the
+        state before each one as the reference does; returns the counts."""
+        counts = []
+        for _ in range(steps):
+            n = self.substeps(st, base, grid, dt, requested)
+            counts.append(n)
+            self.large_step(st, base, grid, dt, n, bc, **kw)
+        return counts
+
     def eos_projection(self, p, rho, theta, qv=None, qc=None, qr=None):
         """EOS pressure re-projection in place; returns False (p untouched)
         when the state is refused.  qv/qc/qr (all or none) add the moist-state
@@ -610,6 +646,39 @@ class ReferenceHarness:
             raise FloatingPointError("EOS pressure projection rejected an invalid physical state")
         return loop
 
+    def max_sound_speed(self, st, base, grid, dt):
+        """(c_max, min spacing) that choose_runtime_timestep (runtime.cpp:712-880)
+        hands the split-explicit scheme for this state."""
+        nx, ny, nz = st["p"].shape
+        out = np.zeros(2, np.float64)
+        self._rc(self.lib.ref_max_sound_speed(
+            _fp(st["u"]), _fp(st["v"]), _fp(st["w"]), _fp(st["rho"]), _fp(st["p"]), nx, ny, nz,
+            ctypes.c_double(grid[0]), ctypes.c_double(grid[1]), ctypes.c_double(grid[2]), ctypes.c_double(dt),
+            _fp(np.ascontiguousarray(base["rho0"], np.float64)), _fp(np.ascontiguousarray(base["p0"], np.float64)),
+            _fp(out)))
+        return float(out[0]), float(out[1])
+
+    def resolve_substep_count(self, dt, c_max, min_spacing, requested=0):
+        """SplitExplicitScheme::resolve_substep_count (split_explicit.cpp:67-170)."""
+        n = ctypes.c_int(0)
+        self._rc(self.lib.ref_resolve_substep_count(ctypes.c_double(dt), ctypes.c_double(c_max),
+                                                    ctypes.c_double(min_spacing), int(requested), ctypes.byref(n)))
+        return n.value
+
+    def substeps(self, st, base, grid, dt, requested=0):
+        c, spacing = self.max_sound_speed(st, base, grid, dt)
+        return self.resolve_substep_count(dt, c, spacing, requested)
+
+    def run(self, st, base, grid, dt, steps, bc, requested=0, coriolis_f=0.0):
+        """`steps` large steps in place with the substep count re-derived
+        before each one; returns the counts."""
+        counts = []
+        for _ in range(steps):
+            n = self.substeps(st, base, grid, dt, requested)
+            counts.append(n)
+            self.large_step(st, base, grid, dt, n, bc, coriolis_f=coriolis_f)
+        return counts
+
     def slow_tendencies(self, st, base, grid, coriolis_f=0.0, moist=True):
         u, v, w, rho, p, th = (st[k] for k in ("u", "v", "w", "rho", "p", "theta"))
         qv, qc, qr = _slow_inputs(st, base, moist)
@@ -632,6 +701,28 @@ class ReferenceHarness:
             arr, flags, n, _fp(u), _fp(v), _fp(w), _fp(rho_end), _fp(rho_begin), _fp(mfx), _fp(mfy),
             _fp(mfz), nx, ny, nz, ctypes.c_double(grid[0]), ctypes.c_double(grid[1]),
             ctypes.c_double(grid[2]), ctypes.c_double(dt), int(weno), int(top_open)))
+
+
+    def bridge_scalar_transport(self, qs, pd, u, v, w, rho_end, rho_begin, mfx, mfy, mfz, dt, grid,
+                                weno=True, top_open=False, backend=None):
+        """The transport through the reference's bridge
+        dispatch_advect_scalars_conservative_cartesian_cgrid_backend to the
+        CPU backend (backend=None) or a shared library's ComputeBackend, with
+        the arguments advection_batch.cpp passes; in place.  Returns False when
+        the backend declined the dispatch (fields untouched)."""
+        nx, ny, nz = rho_end.shape
+        n = len(qs)
+        arr = (_F * max(n, 1))(*[_ptr(q, ctypes.c_float) for q in qs])
+        flags = (ctypes.c_int * max(n, 1))(*[int(x) for x in pd])
+        lib = str(backend).encode() if backend is not None else None
+        rc = self.lib.ref_backend_scalar_transport(
+            lib, arr, flags, n, _fp(u), _fp(v), _fp(w), _fp(rho_end), _fp(rho_begin), _fp(mfx), _fp(mfy),
+            _fp(mfz), nx, ny, nz, ctypes.c_double(grid[0]), ctypes.c_double(grid[1]),
+            ctypes.c_double(grid[2]), ctypes.c_double(dt), int(weno), int(top_open))
+        if rc == 1:
+            return False
+        self._rc(rc)
+        return True
 
 
 def reference_available() -> bool:

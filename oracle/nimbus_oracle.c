@@ -1845,3 +1845,50 @@ int oracle_sgs_stability(int nx, int ny, int nz, const REAL* u, const REAL* v, c
     out[4] = dissipation;
     return 0;
 }
+
+/* ---- Acoustic substep count, re-derived before every large step ----------
+ * The largest sound speed the split-explicit scheme must resolve: the flat
+ * Cartesian CFL scan's max sqrt(gamma p / rho) over every cell
+ * (src/numerics/runtime.cpp:346-401, the product formed as (gamma*p)/rho),
+ * raised to that of the base columns (runtime.cpp:854-870).  Returns -1 when
+ * a pressure or density is non-finite or non-positive (the reference throws
+ * "CFL scan requires finite wind and positive finite pressure/density"). */
+int oracle_max_sound_speed(int nx, int ny, int nz, const REAL* p, const REAL* rho, const double* p0,
+                           const double* rho0, double* out)
+{
+    const double gamma = oracle_gamma();
+    double best = 0.0;
+    const size_t n = (size_t)nx * (size_t)ny * (size_t)nz;
+    for (size_t c = 0; c < n; ++c)
+    {
+        const double ph = (double)p[c], rh = (double)rho[c];
+        if (!isfinite(ph) || ph <= 0.0 || !isfinite(rh) || rh <= 0.0) return -1;
+        const double s = sqrt(gamma * ph / rh);
+        if (best < s) best = s;
+    }
+    for (int k = 0; k < nz; ++k)
+    {
+        const double s = sqrt(gamma * p0[k] / rho0[k]);
+        if (best < s) best = s;
+    }
+    *out = best;
+    return 0;
+}
+
+/* SplitExplicitScheme::resolve_substep_count
+ * (src/numerics/time_stepping/schemes/split_explicit/split_explicit.cpp:67-170)
+ * with a positive diagnosed minimum spacing: N = max(requested,
+ * max(ceil(dt c_max / (0.5 min_spacing)) + 1, 2)); requested <= 0 means the
+ * CFL rule alone.  Returns -1 where the reference throws. */
+int oracle_resolve_substeps(double dt_large, double c_max, double min_spacing, int requested)
+{
+    if (!isfinite(dt_large) || dt_large <= 0.0) return -1;
+    if (!isfinite(c_max) || c_max <= 0.0) return -1;
+    if (!isfinite(min_spacing) || min_spacing <= 0.0) return -1;
+    const double required_real = dt_large * c_max / (0.5 * min_spacing);
+    if (!isfinite(required_real) || required_real >= (double)(2147483647 - 1)) return -1;
+    int required = (int)ceil(required_real) + 1;
+    if (required < 2) required = 2;
+    if (requested > 0) return requested > required ? requested : required;
+    return required;
+}

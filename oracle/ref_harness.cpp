@@ -49,6 +49,11 @@
 //                           dispatch structs and, for the closure, its own
 //                           SmagorinskyScheme::compute routing to the backend
 //                           through dispatch_smagorinsky_fused_backend
+//   ref_backend_scalar_transport  the same transport through the reference's bridge
+//                           dispatch_advect_scalars_conservative_cartesian_cgrid_backend
+//                           (src/compute/dispatch/advection.cpp:95-150) to a loaded backend
+//   ref_resolve_substep_count, ref_max_sound_speed  SplitExplicitScheme::resolve_substep_count
+//                           and the acoustic speed choose_runtime_timestep samples
 //   ref_scalar_transport    advect_scalars_conservative_3d_cartesian
 //                           (advection_cartesian.cpp:3532) on a retained context whose
 //                           face mass fluxes and beginning density are supplied
@@ -79,6 +84,9 @@
 #include "compute/backend_runtime.hpp"
 #include "diagnostics/deterministic_reduction.hpp"
 #include "turbulence/schemes/smagorinsky/smagorinsky.hpp"
+#include "numerics/runtime.hpp"
+#include "compute/bridge/advection.hpp"
+#include "numerics/time_stepping/schemes/split_explicit/split_explicit.hpp"
 
 #include <dlfcn.h>
 
@@ -907,6 +915,136 @@ int ref_sgs_stability(const float* u, const float* v, const float* w, const floa
     catch (const std::exception& e)
     {
         tmv::diagnostics::set_deterministic_reductions(saved);
+        return fail(e.what());
+    }
+}
+
+// Conservative transport of n_scalars scalars routed through the reference's
+// own bridge dispatch_advect_scalars_conservative_cartesian_cgrid_backend
+// (src/compute/dispatch/advection.cpp:95-150) to the backend `library` holds
+// (NULL: the reference's CPU backend), with the arguments
+// advect_thermodynamics_impl passes (advection_batch.cpp:832-886): inverse
+// spacings divided in FP64 and rounded once, the retained context's face
+// mass fluxes and beginning density, the host fields, zero kappas, the FP64
+// dt and the level's state view.  Returns 1 when the backend declined.
+int ref_backend_scalar_transport(const char* library, float** q, const int* positive_definite, int n_scalars,
+                                 const float* u, const float* v, const float* w, const float* rho_end,
+                                 const float* rho_begin, const float* mfx, const float* mfy, const float* mfz,
+                                 int nx, int ny, int nz, double dx, double dy, double dz, double dt, int weno,
+                                 int top_open)
+{
+    try
+    {
+        if (n_scalars < 0 || n_scalars > 16) return fail("n_scalars out of range");
+        ComputeBackendRuntimeState runtime;
+        runtime.backend = load_backend(library);
+        std::string err;
+        if (!runtime.backend->initialize(err)) return fail(err.c_str());
+        Level L(nx, ny, nz, dx, dy, dz, dt);
+        L.set_bcs(4, 4, 4, 4, 1, top_open ? 2 : 0);
+        auto& f = L.storage.fields;
+        to_field(f.u, u, nx, ny, nz);
+        to_field(f.v, v, nx, ny, nz);
+        to_field(f.w, w, nx, ny, nz);
+        to_field(f.rho, rho_end, nx, ny, nz);
+        tmv::CartesianCGridTransportContext ctx;
+        ctx.begin(L.view, nx, ny, nz, dt);
+        Field3D begin_density;
+        to_field(begin_density, rho_begin, nx, ny, nz);
+        ctx.capture_density_begin(begin_density);
+        std::memcpy(ctx.mass_flux_x.data(), mfx, sizeof(float) * f.u.size());
+        std::memcpy(ctx.mass_flux_y.data(), mfy, sizeof(float) * f.u.size());
+        std::memcpy(ctx.mass_flux_z.data(), mfz, sizeof(float) * f.u.size());
+        ctx.record_external_accumulation(dt, 1);
+        ctx.complete(L.view);
+
+        std::unique_ptr<Field3D[]> fields(new Field3D[n_scalars > 0 ? n_scalars : 1]);
+        Field3D* field_ptrs[16] = {};
+        const float* q_in[16] = {};
+        float* q_out[16] = {};
+        float dt_kappas[16] = {};
+        double kappas[16] = {};
+        for (int s = 0; s < n_scalars; ++s)
+        {
+            to_field(fields[s], q[s], nx, ny, nz);
+            field_ptrs[s] = &fields[s];
+            q_in[s] = fields[s].data();
+            q_out[s] = fields[s].data();
+        }
+        const bool done = dispatch_advect_scalars_conservative_cartesian_cgrid_backend(
+            runtime, f.u.data(), f.v.data(), f.w.data(), f.rho.data(), q_in, q_out, dt_kappas, positive_definite,
+            n_scalars, nx, ny, nz, static_cast<float>(1.0 / dx), static_cast<float>(1.0 / dy),
+            static_cast<float>(1.0 / dz), static_cast<float>(1.0 / (dx * dx)), static_cast<float>(1.0 / (dy * dy)),
+            static_cast<float>(1.0 / (dz * dz)), static_cast<float>(dt), density_min_kgm3,
+            ctx.density_begin.data(), ctx.mass_flux_x.data(), ctx.mass_flux_y.data(), ctx.mass_flux_z.data(), true,
+            field_ptrs, kappas, &ctx, dt, nullptr, nullptr, nullptr, 0.0f, 0.0f, &L.view, nullptr, weno != 0);
+        if (!done) return 1;
+        for (int s = 0; s < n_scalars; ++s)
+            from_field(q[s], fields[s]);
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        return fail(e.what());
+    }
+}
+
+// SplitExplicitScheme::resolve_substep_count
+// (src/numerics/time_stepping/schemes/split_explicit/split_explicit.cpp:67-170)
+// with the runtime's sampled sound speed and diagnosed minimum spacing.
+int ref_resolve_substep_count(double dt_large, double max_acoustic_speed, double min_spacing, int requested,
+                              int* out)
+{
+    try
+    {
+        tmv::SplitExplicitScheme scheme;
+        TimeSteppingConfig cfg;
+        cfg.split_acoustic = true;
+        cfg.n_acoustic_substeps = requested;
+        cfg.max_acoustic_speed_ms = max_acoustic_speed;
+        cfg.min_acoustic_spacing_m = min_spacing;
+        *out = scheme.resolve_substep_count(cfg, dt_large);
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        return fail(e.what());
+    }
+}
+
+// The acoustic speed and spacing choose_runtime_timestep
+// (src/numerics/runtime.cpp:712-880) hands the split-explicit scheme before a
+// large step: the Cartesian CFL scan's max sqrt(gamma p / rho) over the state
+// (runtime.cpp:346-401), raised to the base columns' (runtime.cpp:854-870),
+// and min(dx, dy, dz).
+int ref_max_sound_speed(const float* u, const float* v, const float* w, const float* rho, const float* p, int nx,
+                        int ny, int nz, double dx, double dy, double dz, double dt, const double* rho0,
+                        const double* p0, double* out)
+{
+    try
+    {
+        Level L(nx, ny, nz, dx, dy, dz, dt);
+        auto& f = L.storage.fields;
+        to_field(f.u, u, nx, ny, nz);
+        to_field(f.v, v, nx, ny, nz);
+        to_field(f.w, w, nx, ny, nz);
+        to_field(f.rho, rho, nx, ny, nz);
+        to_field(f.p, p, nx, ny, nz);
+        L.storage.base.rho0.assign(rho0, rho0 + nz);
+        L.storage.base.p0.assign(p0, p0 + nz);
+        auto& metrics = tmv::require_level_runtime(L.view.process_grid_metrics, "grid metrics");
+        metrics.dx = dx;
+        metrics.dy = dy;
+        metrics.dz.assign(static_cast<std::size_t>(nz), dz);
+        auto& ts = tmv::require_level_runtime(L.view.time_stepping_runtime, "time_stepping_runtime");
+        ts.config.split_acoustic = true;
+        (void)choose_runtime_timestep(L.view);
+        out[0] = ts.config.max_acoustic_speed_ms;
+        out[1] = ts.config.min_acoustic_spacing_m;
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
         return fail(e.what());
     }
 }

@@ -52,6 +52,7 @@ def _c_layout(struct_name, fields, tmp_path):
     ("nimbus_slow_args", cuda.SlowArgs),
     ("nimbus_kessler_args", cuda.KesslerArgs),
     ("nimbus_eos_args", cuda.EosArgs),
+    ("nimbus_sound_speed_args", cuda.SoundSpeedArgs),
     ("nimbus_boundary_args", cuda.BoundaryArgs),
     ("nimbus_state_relaxation_args", cuda.StateRelaxationArgs),
     ("nimbus_cell_centre_args", cuda.CellCentreArgs),

@@ -419,3 +419,26 @@ def test_state_relaxation_rejects_invalid_rates(o32):
     P = build_profiles(SpongeConfig(), case.nz, case.dz, base["theta0"])
     with pytest.raises(ValueError):
         o32.state_relaxation({k: st[k].copy() for k in ("u", "v", "w", "theta")}, P, 0.0)
+
+
+@pytest.mark.reference
+@pytest.mark.skipif(not oracle.reference_available(), reason="reference harness not built here")
+def test_transport_bridge_route_equals_the_direct_call(o32):
+    """The reference's transport bridge with its CPU backend (the route a
+    device backend replaces) gives the direct call's bits: the harness's route
+    arguments are the ones advection_batch.cpp passes."""
+    ref = oracle.ReferenceHarness()
+    bc = BC_SETS["periodic_noslip_open"]
+    case = Case(18, 15, 11, 800.0, 900.0, 400.0, 4.0, seed=23)
+    st, base = perturbed_state(case, seed=23)
+    close_walls(st, bc)
+    a = {k: v.copy() for k, v in st.items()}
+    loop = o32.acoustic_loop(a, base["rho0"], base["p0"], 4.0, 9, (800.0, 900.0, 400.0), bc)
+    args = (a["u"], a["v"], a["w"], a["rho"], loop["rho_begin"], loop["mfx"], loop["mfy"], loop["mfz"], 4.0,
+            (800.0, 900.0, 400.0))
+    qa = [a[k].copy() for k in ("theta", "qv", "qc", "qr")]
+    qb = [q.copy() for q in qa]
+    ref.scalar_transport(qa, [0, 1, 1, 1], *args, top_open=True)
+    assert ref.bridge_scalar_transport(qb, [0, 1, 1, 1], *args, top_open=True)
+    for x, y in zip(qa, qb):
+        np.testing.assert_array_equal(x.view(np.uint32), y.view(np.uint32))

@@ -111,3 +111,34 @@ def test_batched_loop_through_the_reference_interface(ref, bc):
         a, b = got[k].astype(np.float64), cpu[k].astype(np.float64)
         scale = max(np.abs(b).max(), 1e-30)
         assert np.abs(a - b).max() <= 1e-4 * scale, (k, np.abs(a - b).max(), scale)
+
+
+@pytest.mark.parametrize("bc_name", ["radiative_slip_rigidlid", "periodic_noslip_open", "mixed_walls_sponge"])
+@pytest.mark.parametrize("weno", [True, False], ids=["weno5", "mc"])
+def test_transport_through_the_reference_bridge(ref, bc_name, weno):
+    """The coupled scalar transport through the reference's own bridge
+    (dispatch_advect_scalars_conservative_cartesian_cgrid_backend) with the
+    arguments advect_thermodynamics_impl passes: the CUDA backend's adapter
+    against the reference's CPU backend on the same retained fluxes, and both
+    against the direct CPU call.  Bit for bit."""
+    from tests.golden.make_golden import BC_SETS
+    bc = BC_SETS[bc_name]
+    o32 = oracle.Restatement("f32")
+    case = Case(29, 23, 17, 800.0, 900.0, 400.0, 4.0, seed=21)
+    st, base = cloudy_state(case, seed=21)
+    close_walls(st, bc)
+    grid = (case.dx, case.dy, case.dz)
+    a = {k: v.copy() for k, v in st.items()}
+    loop = o32.acoustic_loop(a, base["rho0"], base["p0"], 4.0, 9, grid, bc)
+    args = (a["u"], a["v"], a["w"], a["rho"], loop["rho_begin"], loop["mfx"], loop["mfy"], loop["mfz"], 4.0, grid)
+    names = ("theta", "qv", "qc", "qr")
+    direct = [a[k].copy() for k in names]
+    cpu = [a[k].copy() for k in names]
+    cuda_route = [a[k].copy() for k in names]
+    ref.scalar_transport(direct, [0, 1, 1, 1], *args, weno=weno, top_open=bc[5] == 2)
+    assert ref.bridge_scalar_transport(cpu, [0, 1, 1, 1], *args, weno=weno, top_open=bc[5] == 2)
+    assert ref.bridge_scalar_transport(cuda_route, [0, 1, 1, 1], *args, weno=weno, top_open=bc[5] == 2,
+                                       backend=ADAPTER)
+    for k, x, y, z in zip(names, direct, cpu, cuda_route):
+        assert np.array_equal(bits(x), bits(y)), k
+        assert np.array_equal(bits(y), bits(z)), k
