@@ -539,7 +539,7 @@ def run_ours(args):
     # ---- batched form: every run resident in one engine, CUDA graph ----
     run = EngineRun(ctx, precision, lanes=args.lanes)
     for c, (st, base), n in zip(cases, prepared, subs):
-        run.admit(c, st, base, n_substeps=n)
+        run.admit(c, st, base)  # substep count re-derived before every step
     stream = torch.cuda.ExternalStream(run.engine.stream, device=f"cuda:{device}")
     for _ in range(max(args.warmup, 3)):
         run.step(1)
@@ -716,22 +716,36 @@ def run_ours(args):
 
 
 def serving_study(ctx, args, precision):
-    """Poisson stream (4 req/s) and a burst of the same requests: continuous
-    batching in the engine against running them one by one on the plain path."""
+    """Poisson streams of increasing rate (4, 16 and 64 requests per second,
+    the last past saturation) and a burst of the same requests: continuous
+    batching in the engine against running them one by one on the plain path.
+    Initial states are prepared (and pinned) before each stream starts."""
+    import torch
+
     from nimbus_b200.ensemble import request_stream
     from nimbus_b200.initial import initial_state
     from nimbus_b200.serve import Server, serve_one_by_one, summarize
 
+    def pinned(st):
+        return {k: torch.from_numpy(v).pin_memory().numpy() for k, v in st.items()}
+
     out = {}
-    for label, burst in (("poisson_4_per_s", False), ("burst", True)):
-        reqs = request_stream(args.serving_requests, rate_per_s=4.0, seed=7, burst=burst)
-        prepared = {r.rid: initial_state(r.case) for r in reqs}
+    streams = [("poisson_%d_per_s" % rate, rate, False) for rate in (4, 16, 64)] + [("burst", 4, True)]
+    for label, rate, burst in streams:
+        reqs = request_stream(args.serving_requests, rate_per_s=float(rate), seed=7, burst=burst)
+        prepared = {}
+        for r in reqs:
+            st, base = initial_state(r.case)
+            prepared[r.rid] = (pinned(st), base)
         server = Server(ctx, precision)
         done, span = server.serve(reqs, prepared)
+        builds = server.run.engine.graph_builds()
         server.close()
         plain, p_span = serve_one_by_one(ctx, reqs, precision, prepared)
-        out[label] = {"batched": summarize(done, span), "one_by_one_plain": summarize(plain, p_span)}
-    out["requests"] = ("%d runs, grids log-uniform 32x32x40..256x256x80, durations U(60,600) s at dt 3 s, "
+        batched = summarize(done, span)
+        batched["graph_instantiations"], batched["graph_updates"] = builds
+        out[label] = {"batched": batched, "one_by_one_plain": summarize(plain, p_span)}
+    out["requests"] = ("%d runs per stream, grids log-uniform 32x32x40..256x256x80, durations U(60,600) s at dt 3 s, "
                        "seeded" % args.serving_requests)
     return out
 

@@ -149,7 +149,8 @@ enum
     NIMBUS_KERNEL_TRANSPORT_LIMITER = 4,
     NIMBUS_KERNEL_TRANSPORT_UPDATE = 5,
     NIMBUS_KERNEL_SLOW = 6,               /* slow tendencies (k1+predictor, k2+apply) */
-    NIMBUS_KERNEL_MICROPHYSICS = 7,       /* Kessler, the EOS re-projection and the end-of-step sponge */
+    NIMBUS_KERNEL_MICROPHYSICS = 7,       /* Kessler, the EOS re-projection, the end-of-step sponge and the
+                                             engine's acoustic speed scan */
     NIMBUS_KERNEL_OUTPUT = 8,             /* cell-centre velocities for output */
     NIMBUS_KERNEL_SGS = 9,                /* Smagorinsky closure, SGS apply and stability */
     NIMBUS_KERNEL_FAMILIES = 10
@@ -831,11 +832,16 @@ void nimbus_cuda_engine_destroy(nimbus_engine* e);
 /* Device bytes one member of this shape holds while resident. */
 size_t nimbus_cuda_engine_member_bytes(const nimbus_member_desc* desc);
 /* Admits a member with its initial state when its footprint plus
- * reserve_bytes fits the free HBM (cudaMemGetInfo); otherwise returns
- * NIMBUS_ERR_OUT_OF_MEMORY and changes nothing.  Waits for enqueued steps. */
+ * reserve_bytes fits the free HBM (cudaMemGetInfo's free bytes plus what the
+ * default memory pool holds unused); otherwise returns
+ * NIMBUS_ERR_OUT_OF_MEMORY and changes nothing.  Does not wait for enqueued
+ * steps: the arena is allocated and the state copied in stream order on the
+ * engine's stream (pageable arrays are staged before the call returns, pinned
+ * ones must stay untouched until the member's first step has run). */
 nimbus_status nimbus_cuda_engine_admit(nimbus_engine* e, const nimbus_member_desc* desc,
                                        const nimbus_member_state* initial, size_t reserve_bytes, int* member_id);
-/* Frees a member's device memory (waits for enqueued steps). */
+/* Frees a member's device memory in stream order, after the enqueued steps
+ * and copies that use it (does not wait). */
 nimbus_status nimbus_cuda_engine_retire(nimbus_engine* e, int member_id);
 /* Copies a member's current state to host arrays (waits for enqueued steps). */
 nimbus_status nimbus_cuda_engine_read(nimbus_engine* e, int member_id, const nimbus_member_state* out);
@@ -877,6 +883,30 @@ nimbus_status nimbus_cuda_engine_history_async(nimbus_engine* e, int member_id, 
  * nimbus_cuda_engine_lanes: the lanes the current table uses. */
 nimbus_status nimbus_cuda_engine_set_lanes(nimbus_engine* e, int lanes);
 int nimbus_cuda_engine_lanes(const nimbus_engine* e);
+/* Kernel form of the acoustic substep's continuity and momentum passes (the
+ * bulk of a step).  Results do not depend on it; it takes effect at the next
+ * step.
+ *   NIMBUS_ACOUSTIC_TABLE  one thread per cell, each member's parameters and
+ *                          buffers read from the member table in HBM;
+ *   NIMBUS_ACOUSTIC_CONST  one thread per cell, each lane's members' constants
+ *                          passed as one kernel parameter (the constant bank),
+ *                          only the rotating buffers read from the table
+ *                          (default; lanes of more than 64 members fall back
+ *                          to the table form);
+ *   NIMBUS_ACOUSTIC_MARCH  one thread advances nimbus_cuda_engine_set_march
+ *                          consecutive cells of a row along x (default 16),
+ *                          neighbour data of the previous cell carried over in
+ *                          registers. */
+enum
+{
+    NIMBUS_ACOUSTIC_TABLE = 0,
+    NIMBUS_ACOUSTIC_CONST = 1,
+    NIMBUS_ACOUSTIC_MARCH = 2
+};
+nimbus_status nimbus_cuda_engine_set_acoustic_form(nimbus_engine* e, int form);
+int nimbus_cuda_engine_acoustic_form(const nimbus_engine* e);
+nimbus_status nimbus_cuda_engine_set_march(nimbus_engine* e, int planes);
+int nimbus_cuda_engine_march(const nimbus_engine* e);
 /* Enqueues n_steps large steps of every resident member on the engine's
  * stream: replayed from a CUDA graph when graphs are on (the default), the
  * graph rebuilt after admissions, retirements, a precision change or a
@@ -892,6 +922,14 @@ nimbus_status nimbus_cuda_engine_synchronize(nimbus_engine* e);
  * scalar, 4 EOS projection refused, 16 a pressure or density failed the
  * acoustic speed scan); waits for enqueued steps. */
 nimbus_status nimbus_cuda_engine_member_status(nimbus_engine* e, int member_id, unsigned* flags);
+/* The same status bits copied into pinned host memory in stream order (after
+ * the enqueued steps), without waiting: read them once the stream has passed
+ * that point (an event recorded after the call, or a synchronisation). */
+nimbus_status nimbus_cuda_engine_member_status_async(nimbus_engine* e, int member_id, unsigned* host_flags);
+/* How often the engine instantiated its step graphs and how often it updated
+ * an instantiated graph in place (an admission or retirement that keeps the
+ * graphs' shape). */
+nimbus_status nimbus_cuda_engine_graph_builds(const nimbus_engine* e, uint64_t* instantiations, uint64_t* updates);
 /* The acoustic substep count of a member's last enqueued (or, before any,
  * its first) large step. */
 nimbus_status nimbus_cuda_engine_member_substeps(nimbus_engine* e, int member_id, int* n_substeps);

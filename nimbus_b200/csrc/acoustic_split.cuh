@@ -49,6 +49,92 @@ __device__ __forceinline__ void retain_flux_from(float* slot, float old, const F
     }
 }
 
+// The old-state neighbourhood one cell's continuity reads: density at the
+// cell and its six face neighbours, the velocities on the cell's upper and
+// lower faces, theta, and the stored retained-flux sums.  Neighbours outside
+// the grid hold the cell's own value (they are never used).
+struct ContinuityStencil
+{
+    float rho_c, rxp, rxm, ryp, rym, rzp, rzm;
+    float uc, uxm, vc, vym, wc, wzm;
+    float th;
+    float mx, my, mz;
+};
+
+// Continuity, rho forward Euler and EOS of cell c = (i, j, k) from its loaded
+// stencil: the retained fluxes of its three upper faces (written when
+// store_flux, else accumulated), the new density into rho_out[c] and the
+// pressure into p_out[c].  Every way of loading the stencil (one thread per
+// cell, or marching along i) ends here, so the arithmetic is one sequence.
+template <class Policy>
+__device__ __forceinline__ void continuity_eos_values(const FusedParams& P, const ContinuityStencil& s, int i, int j,
+                                                      int k, int c, const double* __restrict__ rho0,
+                                                      const float4* __restrict__ eos0, float* __restrict__ rho_out,
+                                                      float* __restrict__ p_out, float* __restrict__ drho_out,
+                                                      float* __restrict__ mfx, float* __restrict__ mfy,
+                                                      float* __restrict__ mfz, unsigned& flags, bool store_flux,
+                                                      float* __restrict__ rho_copy)
+{
+    using real = typename Policy::real;
+    const Dims d = P.d;
+    const bool xlo = i >= 1, xhi = i < d.nx - 1, ylo = j >= 1, yhi = j < d.ny - 1;
+    const bool zlo = k > 0, zhi = k + 1 < d.nz;
+    const float rho_c = s.rho_c;
+    const bool flux = mfx != nullptr;
+
+    if (rho_copy != nullptr) rho_copy[c] = rho_c;
+    if (flux)
+    {
+        if constexpr (sizeof(real) == 8)
+        {
+            const double rc = (double)rho_c;
+            if (xhi)
+                retain_flux_from<Policy>(mfx + c, s.mx, P, 0.5 * (rc + (double)s.rxp) * ((double)s.uc - P.frame_u),
+                                         0.0f, flags, store_flux);
+            if (yhi)
+                retain_flux_from<Policy>(mfy + c, s.my, P, 0.5 * (rc + (double)s.ryp) * ((double)s.vc - P.frame_v),
+                                         0.0f, flags, store_flux);
+            const double zf =
+                !zhi ? (P.top_open ? rc * (double)s.wc : 0.0) : 0.5 * (rc + (double)s.rzp) * (double)s.wc;
+            retain_flux_from<Policy>(mfz + c, s.mz, P, zf, 0.0f, flags, store_flux);
+        }
+        else
+        {
+            if (xhi)
+                retain_flux_from<Policy>(mfx + c, s.mx, P, 0.0, 0.5f * (rho_c + s.rxp) * (s.uc - P.frame_u_f), flags,
+                                         store_flux);
+            if (yhi)
+                retain_flux_from<Policy>(mfy + c, s.my, P, 0.0, 0.5f * (rho_c + s.ryp) * (s.vc - P.frame_v_f), flags,
+                                         store_flux);
+            const float zf = !zhi ? (P.top_open ? rho_c * s.wc : 0.0f) : 0.5f * (rho_c + s.rzp) * s.wc;
+            retain_flux_from<Policy>(mfz + c, s.mz, P, 0.0, zf, flags, store_flux);
+        }
+    }
+    real drho = (real)0;
+    if (xlo && xhi && ylo && yhi)
+    {
+        const real rc = (real)rho_c;
+        const real half = (real)0.5;
+        const real fx_pos = half * (rc + (real)s.rxp) * (real)s.uc;
+        const real fx_neg = half * ((real)s.rxm + rc) * (real)s.uxm;
+        const real fy_pos = half * (rc + (real)s.ryp) * (real)s.vc;
+        const real fy_neg = half * ((real)s.rym + rc) * (real)s.vym;
+        const real fz_pos = zhi ? half * (rc + (real)s.rzp) * (real)s.wc : rc * (real)s.wc;
+        const real fz_neg = zlo ? half * ((real)s.rzm + rc) * (real)s.wzm : (real)0;
+        if constexpr (sizeof(real) == 8)
+            drho = -((fx_pos - fx_neg) * P.inv_dx + (fy_pos - fy_neg) * P.inv_dy + (fz_pos - fz_neg) * P.inv_dz);
+        else
+            drho = -((fx_pos - fx_neg) * P.inv_dx_f + (fy_pos - fy_neg) * P.inv_dy_f + (fz_pos - fz_neg) * P.inv_dz_f);
+    }
+    float drho_stored;
+    if constexpr (sizeof(real) == 8) drho_stored = (float)finite_or_zero(drho);
+    else drho_stored = isfinite(drho) ? drho : 0.0f;
+    if (drho_out != nullptr) drho_out[c] = drho_stored;
+    const float rho_stored = substep_density<Policy>(P, rho_c, drho_stored, rho0, k);
+    rho_out[c] = rho_stored;
+    p_out[c] = substep_pressure<Policy>(P, eos0, k, rho_stored, s.th);
+}
+
 // Continuity, rho forward Euler and EOS for cell c.  With store_flux the
 // retained fluxes are written rather than accumulated and rho_copy (when
 // given) receives the pre-substep density (the transport context's
@@ -66,75 +152,86 @@ __device__ __forceinline__ void continuity_eos_cell(const FusedParams& P, const 
                                                     float* __restrict__ mfz, int c, unsigned& flags, bool store_flux,
                                                     float* __restrict__ rho_copy)
 {
-    using real = typename Policy::real;
     const Dims d = P.d;
     const int sx = d.sx(), sy = d.sy();
     int i, j, k;
     decompose(d, c, i, j, k);
     const bool xlo = i >= 1, xhi = i < d.nx - 1, ylo = j >= 1, yhi = j < d.ny - 1;
     const bool zlo = k > 0, zhi = k + 1 < d.nz;
-    const float rho_c = rho[c];
-    const float rxp = rho[xhi ? c + sx : c], rxm = rho[xlo ? c - sx : c];
-    const float ryp = rho[yhi ? c + sy : c], rym = rho[ylo ? c - sy : c];
-    const float rzp = rho[zhi ? c + 1 : c], rzm = rho[zlo ? c - 1 : c];
-    const float uc = u[c], uxm = u[xlo ? c - sx : c];
-    const float vc = v[c], vym = v[ylo ? c - sy : c];
-    const float wc = w[c], wzm = w[zlo ? c - 1 : c];
-    const float th = theta[c];
-    const bool flux = mfx != nullptr;
-    const bool acc = flux && !store_flux;
-    const float mx = acc ? mfx[c] : 0.0f, my = acc ? mfy[c] : 0.0f, mz = acc ? mfz[c] : 0.0f;
+    ContinuityStencil s;
+    s.rho_c = rho[c];
+    s.rxp = rho[xhi ? c + sx : c];
+    s.rxm = rho[xlo ? c - sx : c];
+    s.ryp = rho[yhi ? c + sy : c];
+    s.rym = rho[ylo ? c - sy : c];
+    s.rzp = rho[zhi ? c + 1 : c];
+    s.rzm = rho[zlo ? c - 1 : c];
+    s.uc = u[c];
+    s.uxm = u[xlo ? c - sx : c];
+    s.vc = v[c];
+    s.vym = v[ylo ? c - sy : c];
+    s.wc = w[c];
+    s.wzm = w[zlo ? c - 1 : c];
+    s.th = theta[c];
+    const bool acc = mfx != nullptr && !store_flux;
+    s.mx = acc ? mfx[c] : 0.0f;
+    s.my = acc ? mfy[c] : 0.0f;
+    s.mz = acc ? mfz[c] : 0.0f;
+    continuity_eos_values<Policy>(P, s, i, j, k, c, rho0, eos0, rho_out, p_out, drho_out, mfx, mfy, mfz, flags,
+                                  store_flux, rho_copy);
+}
 
-    if (rho_copy != nullptr) rho_copy[c] = rho_c;
-    if (flux)
+// The same continuity for the cells (i0 .. i1-1, j, k) of one grid row along
+// x, marching in i: the density of planes i-1, i and the x-velocity of plane
+// i-1 carry over in registers from the previous cell, so a cell loads one new
+// x-neighbour instead of three, and its neighbour offsets and boundary flags
+// in j and k are formed once per row.  q = j nz + k.
+template <class Policy>
+__device__ __forceinline__ void continuity_eos_march(const FusedParams& P, const float* __restrict__ rho,
+                                                     const float* __restrict__ u, const float* __restrict__ v,
+                                                     const float* __restrict__ w, const float* __restrict__ theta,
+                                                     const double* __restrict__ rho0,
+                                                     const float4* __restrict__ eos0, float* __restrict__ rho_out,
+                                                     float* __restrict__ p_out, float* __restrict__ mfx,
+                                                     float* __restrict__ mfy, float* __restrict__ mfz, int i0, int i1,
+                                                     int j, int k, int q, unsigned& flags, bool store_flux,
+                                                     float* __restrict__ rho_copy)
+{
+    const Dims d = P.d;
+    const int sx = d.sx();
+    const int oyp = j < d.ny - 1 ? d.nz : 0, oym = j >= 1 ? -d.nz : 0;
+    const int ozp = k + 1 < d.nz ? 1 : 0, ozm = k > 0 ? -1 : 0;
+    const bool acc = mfx != nullptr && !store_flux;
+    int c = i0 * sx + q;
+    float r_m = rho[i0 >= 1 ? c - sx : c];
+    float r_c = rho[c];
+    float u_m = u[i0 >= 1 ? c - sx : c];
+    for (int i = i0; i < i1; ++i, c += sx)
     {
-        if constexpr (sizeof(real) == 8)
-        {
-            const double rc = (double)rho_c;
-            if (xhi)
-                retain_flux_from<Policy>(mfx + c, mx, P, 0.5 * (rc + (double)rxp) * ((double)uc - P.frame_u), 0.0f,
-                                         flags, store_flux);
-            if (yhi)
-                retain_flux_from<Policy>(mfy + c, my, P, 0.5 * (rc + (double)ryp) * ((double)vc - P.frame_v), 0.0f,
-                                         flags, store_flux);
-            const double zf = !zhi ? (P.top_open ? rc * (double)wc : 0.0) : 0.5 * (rc + (double)rzp) * (double)wc;
-            retain_flux_from<Policy>(mfz + c, mz, P, zf, 0.0f, flags, store_flux);
-        }
-        else
-        {
-            if (xhi)
-                retain_flux_from<Policy>(mfx + c, mx, P, 0.0, 0.5f * (rho_c + rxp) * (uc - P.frame_u_f), flags,
-                                         store_flux);
-            if (yhi)
-                retain_flux_from<Policy>(mfy + c, my, P, 0.0, 0.5f * (rho_c + ryp) * (vc - P.frame_v_f), flags,
-                                         store_flux);
-            const float zf = !zhi ? (P.top_open ? rho_c * wc : 0.0f) : 0.5f * (rho_c + rzp) * wc;
-            retain_flux_from<Policy>(mfz + c, mz, P, 0.0, zf, flags, store_flux);
-        }
+        ContinuityStencil s;
+        s.rho_c = r_c;
+        s.rxm = r_m;
+        s.rxp = rho[i < d.nx - 1 ? c + sx : c];
+        s.ryp = rho[c + oyp];
+        s.rym = rho[c + oym];
+        s.rzp = rho[c + ozp];
+        s.rzm = rho[c + ozm];
+        s.uc = u[c];
+        s.uxm = u_m;
+        s.vc = v[c];
+        s.vym = v[c + oym];
+        s.wc = w[c];
+        s.wzm = w[c + ozm];
+        s.th = theta[c];
+        s.mx = acc ? mfx[c] : 0.0f;
+        s.my = acc ? mfy[c] : 0.0f;
+        s.mz = acc ? mfz[c] : 0.0f;
+        continuity_eos_values<Policy>(P, s, i, j, k, c, rho0, eos0, rho_out, p_out, nullptr, mfx, mfy, mfz, flags,
+                                      store_flux, rho_copy);
+        r_m = r_c;
+        r_c = s.rxp;
+        u_m = s.uc;
     }
-    real drho = (real)0;
-    if (xlo && xhi && ylo && yhi)
-    {
-        const real rc = (real)rho_c;
-        const real half = (real)0.5;
-        const real fx_pos = half * (rc + (real)rxp) * (real)uc;
-        const real fx_neg = half * ((real)rxm + rc) * (real)uxm;
-        const real fy_pos = half * (rc + (real)ryp) * (real)vc;
-        const real fy_neg = half * ((real)rym + rc) * (real)vym;
-        const real fz_pos = zhi ? half * (rc + (real)rzp) * (real)wc : rc * (real)wc;
-        const real fz_neg = zlo ? half * ((real)rzm + rc) * (real)wzm : (real)0;
-        if constexpr (sizeof(real) == 8)
-            drho = -((fx_pos - fx_neg) * P.inv_dx + (fy_pos - fy_neg) * P.inv_dy + (fz_pos - fz_neg) * P.inv_dz);
-        else
-            drho = -((fx_pos - fx_neg) * P.inv_dx_f + (fy_pos - fy_neg) * P.inv_dy_f + (fz_pos - fz_neg) * P.inv_dz_f);
-    }
-    float drho_stored;
-    if constexpr (sizeof(real) == 8) drho_stored = (float)finite_or_zero(drho);
-    else drho_stored = isfinite(drho) ? drho : 0.0f;
-    if (drho_out != nullptr) drho_out[c] = drho_stored;
-    const float rho_stored = substep_density<Policy>(P, rho_c, drho_stored, rho0, k);
-    rho_out[c] = rho_stored;
-    p_out[c] = substep_pressure<Policy>(P, eos0, k, rho_stored, th);
 }
 
 template <class Policy>
@@ -197,6 +294,74 @@ enum : int
     kFuseOpenTop = 4
 };
 
+// The new-state neighbourhood of one cell's momentum: density and pressure at
+// the cell and its upper x, y and z neighbours, and the cell's old face
+// velocities.
+struct MomentumStencil
+{
+    float rc, rx, ry, rz;
+    float pc, px, py, pz;
+    float uc, vc, wc;
+};
+
+// Momentum forward Euler of the faces of cell c = (i, j, k) from its loaded
+// stencil (see momentum_cell).
+template <class Policy>
+__device__ __forceinline__ void momentum_values(const FusedParams& P, const MomentumStencil& s, int i, int j, int k,
+                                                int c, const double* __restrict__ p0,
+                                                const float2* __restrict__ dp0_split, float* u_out, float* v_out,
+                                                float* w_out, int fuse_vertical)
+{
+    using real = typename Policy::real;
+    const Dims d = P.d;
+    const bool interior = i >= 1 && i < d.nx - 1 && j >= 1 && j < d.ny - 1 && k < d.nz - 1;
+    float du = 0.0f, dv = 0.0f, dw = 0.0f;
+    if constexpr (sizeof(real) == 8)
+    {
+        if (interior)
+        {
+            const double rcd = (double)s.rc;
+            const double rho_x = 0.5 * (rcd + (double)s.rx);
+            const double rho_y = 0.5 * (rcd + (double)s.ry);
+            const double rho_z = 0.5 * (rcd + (double)s.rz);
+            const double pcd = (double)s.pc;
+            const double dp0_dz = (p0[k + 1] - p0[k]) * P.inv_dz;
+            du = (float)finite_or_zero(-((double)s.px - pcd) * P.inv_dx / safe_rho(rho_x));
+            dv = (float)finite_or_zero(-((double)s.py - pcd) * P.inv_dy / safe_rho(rho_y));
+            dw = (float)finite_or_zero(-((((double)s.pz - pcd) * P.inv_dz) - dp0_dz) / safe_rho(rho_z));
+        }
+        momentum_store(d, i, j, k, c, fuse_vertical,
+                       clamp_value((float)((double)s.uc + (double)du * P.dt_small), 0.0f, -P.wind_h, P.wind_h),
+                       clamp_value((float)((double)s.vc + (double)dv * P.dt_small), 0.0f, -P.wind_h, P.wind_h),
+                       clamp_value((float)((double)s.wc + (double)dw * P.dt_small), 0.0f, -P.wind_v, P.wind_v),
+                       u_out, v_out, w_out);
+    }
+    else
+    {
+        const float2 dp0 = dp0_split[k];
+        if (interior)
+        {
+            const float rho_x = 0.5f * (s.rc + s.rx);
+            const float rho_y = 0.5f * (s.rc + s.ry);
+            const float rho_z = 0.5f * (s.rc + s.rz);
+            const float dpz = ((s.pz - s.pc) - dp0.x) - dp0.y;
+            const float sxr = (isfinite(rho_x) && rho_x > 1.0e-6f) ? rho_x : 1.0f;
+            const float syr = (isfinite(rho_y) && rho_y > 1.0e-6f) ? rho_y : 1.0f;
+            const float szr = (isfinite(rho_z) && rho_z > 1.0e-6f) ? rho_z : 1.0f;
+            const float a = __fdividef(-(s.px - s.pc) * P.inv_dx_f, sxr);
+            const float b = __fdividef(-(s.py - s.pc) * P.inv_dy_f, syr);
+            const float cz = __fdividef(-dpz * P.inv_dz_f, szr);
+            du = isfinite(a) ? a : 0.0f;
+            dv = isfinite(b) ? b : 0.0f;
+            dw = isfinite(cz) ? cz : 0.0f;
+        }
+        const float dt = P.dt_f;
+        momentum_store(d, i, j, k, c, fuse_vertical, clamp_value(__fmaf_rn(du, dt, s.uc), 0.0f, -P.wind_h, P.wind_h),
+                       clamp_value(__fmaf_rn(dv, dt, s.vc), 0.0f, -P.wind_h, P.wind_h),
+                       clamp_value(__fmaf_rn(dw, dt, s.wc), 0.0f, -P.wind_v, P.wind_v), u_out, v_out, w_out);
+    }
+}
+
 template <class Policy>
 __device__ __forceinline__ void momentum_cell(const FusedParams& P, const float* __restrict__ rho,
                                               const float* __restrict__ p, const double* __restrict__ p0,
@@ -204,7 +369,6 @@ __device__ __forceinline__ void momentum_cell(const FusedParams& P, const float*
                                               const float* w, float* u_out, float* v_out, float* w_out, int c,
                                               int fuse_vertical = 0)
 {
-    using real = typename Policy::real;
     const Dims d = P.d;
     const int sx = d.sx(), sy = d.sy();
     int i, j, k;
@@ -213,53 +377,53 @@ __device__ __forceinline__ void momentum_cell(const FusedParams& P, const float*
     // Every load first; outside the interior the neighbour indices fall back
     // to the cell itself (those values are not used).
     const int cx = interior ? c + sx : c, cy = interior ? c + sy : c, cz1 = interior ? c + 1 : c;
-    const float rc = rho[c], rx = rho[cx], ry = rho[cy], rz = rho[cz1];
-    const float pc = p[c], px = p[cx], py = p[cy], pz = p[cz1];
-    const float uc = u[c], vc = v[c], wc = w[c];
-    float du = 0.0f, dv = 0.0f, dw = 0.0f;
-    if constexpr (sizeof(real) == 8)
+    MomentumStencil s;
+    s.rc = rho[c];
+    s.rx = rho[cx];
+    s.ry = rho[cy];
+    s.rz = rho[cz1];
+    s.pc = p[c];
+    s.px = p[cx];
+    s.py = p[cy];
+    s.pz = p[cz1];
+    s.uc = u[c];
+    s.vc = v[c];
+    s.wc = w[c];
+    momentum_values<Policy>(P, s, i, j, k, c, p0, dp0_split, u_out, v_out, w_out, fuse_vertical);
+}
+
+// The same momentum for the cells (i0 .. i1-1, j, k) of one row along x,
+// marching in i: the new density and pressure of plane i+1 loaded for cell i
+// are those of cell i+1, so they carry over in registers.  q = j nz + k.
+template <class Policy>
+__device__ __forceinline__ void momentum_march(const FusedParams& P, const float* __restrict__ rho,
+                                               const float* __restrict__ p, const double* __restrict__ p0,
+                                               const float2* __restrict__ dp0_split, float* u, float* v, float* w,
+                                               int i0, int i1, int j, int k, int q, int fuse_vertical)
+{
+    const Dims d = P.d;
+    const int sx = d.sx();
+    const int oy = j < d.ny - 1 ? d.nz : 0, oz = k < d.nz - 1 ? 1 : 0;
+    int c = i0 * sx + q;
+    float rc = rho[c], pc = p[c];
+    for (int i = i0; i < i1; ++i, c += sx)
     {
-        if (interior)
-        {
-            const double rcd = (double)rc;
-            const double rho_x = 0.5 * (rcd + (double)rx);
-            const double rho_y = 0.5 * (rcd + (double)ry);
-            const double rho_z = 0.5 * (rcd + (double)rz);
-            const double pcd = (double)pc;
-            const double dp0_dz = (p0[k + 1] - p0[k]) * P.inv_dz;
-            du = (float)finite_or_zero(-((double)px - pcd) * P.inv_dx / safe_rho(rho_x));
-            dv = (float)finite_or_zero(-((double)py - pcd) * P.inv_dy / safe_rho(rho_y));
-            dw = (float)finite_or_zero(-((((double)pz - pcd) * P.inv_dz) - dp0_dz) / safe_rho(rho_z));
-        }
-        momentum_store(d, i, j, k, c, fuse_vertical,
-                       clamp_value((float)((double)uc + (double)du * P.dt_small), 0.0f, -P.wind_h, P.wind_h),
-                       clamp_value((float)((double)vc + (double)dv * P.dt_small), 0.0f, -P.wind_h, P.wind_h),
-                       clamp_value((float)((double)wc + (double)dw * P.dt_small), 0.0f, -P.wind_v, P.wind_v), u_out,
-                       v_out, w_out);
-    }
-    else
-    {
-        const float2 dp0 = dp0_split[k];
-        if (interior)
-        {
-            const float rho_x = 0.5f * (rc + rx);
-            const float rho_y = 0.5f * (rc + ry);
-            const float rho_z = 0.5f * (rc + rz);
-            const float dpz = ((pz - pc) - dp0.x) - dp0.y;
-            const float sxr = (isfinite(rho_x) && rho_x > 1.0e-6f) ? rho_x : 1.0f;
-            const float syr = (isfinite(rho_y) && rho_y > 1.0e-6f) ? rho_y : 1.0f;
-            const float szr = (isfinite(rho_z) && rho_z > 1.0e-6f) ? rho_z : 1.0f;
-            const float a = __fdividef(-(px - pc) * P.inv_dx_f, sxr);
-            const float b = __fdividef(-(py - pc) * P.inv_dy_f, syr);
-            const float cz = __fdividef(-dpz * P.inv_dz_f, szr);
-            du = isfinite(a) ? a : 0.0f;
-            dv = isfinite(b) ? b : 0.0f;
-            dw = isfinite(cz) ? cz : 0.0f;
-        }
-        const float dt = P.dt_f;
-        momentum_store(d, i, j, k, c, fuse_vertical, clamp_value(__fmaf_rn(du, dt, uc), 0.0f, -P.wind_h, P.wind_h),
-                       clamp_value(__fmaf_rn(dv, dt, vc), 0.0f, -P.wind_h, P.wind_h),
-                       clamp_value(__fmaf_rn(dw, dt, wc), 0.0f, -P.wind_v, P.wind_v), u_out, v_out, w_out);
+        MomentumStencil s;
+        const int cx = i < d.nx - 1 ? c + sx : c;
+        s.rc = rc;
+        s.pc = pc;
+        s.rx = rho[cx];
+        s.px = p[cx];
+        s.ry = rho[c + oy];
+        s.py = p[c + oy];
+        s.rz = rho[c + oz];
+        s.pz = p[c + oz];
+        s.uc = u[c];
+        s.vc = v[c];
+        s.wc = w[c];
+        momentum_values<Policy>(P, s, i, j, k, c, p0, dp0_split, u, v, w, fuse_vertical);
+        rc = s.rx;
+        pc = s.px;
     }
 }
 

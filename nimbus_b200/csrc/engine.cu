@@ -204,6 +204,7 @@ void fill_params(EngineMember& M, const nimbus_member_desc* a)
     M.items[kItemColumns] = a->nx * a->ny;
     M.items[kItemHistory] = (a->ny + a->nx) * a->nz;
     M.items[kItemPerimeter] = 3 * a->nx + 3 * (a->ny - 3);
+    M.items[kItemScan] = (M.items[kItemCells] + kScanCells - 1) / kScanCells;
 }
 
 }  // namespace
@@ -230,15 +231,35 @@ void rotate_host_views(nimbus_engine* e, int steps)
     }
 }
 
+// Makes the host views exact: when they already are (the mirror replayed
+// every enqueued rotation), returns at once without waiting for the stream;
+// otherwise waits for the stream and reads the table back.
 nimbus_status sync_table_to_host(nimbus_engine* e)
 {
     nimbus_cuda_context* ctx = e->ctx;
-    NB_CUDA(ctx, cudaStreamSynchronize(e->stream));
     if (e->table_current || e->order.empty()) return NIMBUS_OK;
+    NB_CUDA(ctx, cudaStreamSynchronize(e->stream));
     std::vector<EngineMember> host(e->order.size());
     NB_CUDA(ctx, cudaMemcpy(host.data(), e->d_table, sizeof(EngineMember) * host.size(), cudaMemcpyDeviceToHost));
     for (size_t r = 0; r < e->order.size(); ++r) e->slots[e->order[r]].m = host[r];
     e->table_current = true;
+    return NIMBUS_OK;
+}
+
+// Free device memory for admission (the rule of
+// include/compute/compute_memory_admission.hpp): cudaMemGetInfo's free bytes
+// plus what the device's default memory pool holds reserved but unused
+// (arenas of retired members freed in stream order return there first).
+nimbus_status free_device_bytes(nimbus_cuda_context* ctx, size_t* out)
+{
+    size_t free_bytes = 0, total_bytes = 0;
+    NB_CUDA(ctx, cudaMemGetInfo(&free_bytes, &total_bytes));
+    cudaMemPool_t pool = nullptr;
+    NB_CUDA(ctx, cudaDeviceGetDefaultMemPool(&pool, ctx->device));
+    unsigned long long reserved = 0, used = 0;  // the attributes are 64-bit
+    NB_CUDA(ctx, cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
+    NB_CUDA(ctx, cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used));
+    *out = free_bytes + static_cast<size_t>(reserved > used ? reserved - used : 0);
     return NIMBUS_OK;
 }
 
@@ -257,6 +278,17 @@ nimbus_status ensure_lane_streams(nimbus_engine* e, size_t extra)
         e->lane_done.push_back(d);
     }
     return NIMBUS_OK;
+}
+
+void destroy_graphs(nimbus_engine* e)
+{
+    for (int part = 0; part < 2; ++part)
+    {
+        if (e->exec[part]) cudaGraphExecDestroy(e->exec[part]);
+        if (e->graph[part]) cudaGraphDestroy(e->graph[part]);
+        e->exec[part] = nullptr;
+        e->graph[part] = nullptr;
+    }
 }
 
 nimbus_status rebuild_table(nimbus_engine* e)
@@ -303,6 +335,7 @@ nimbus_status rebuild_table(nimbus_engine* e)
     if (n > e->table_cap)
     {
         const size_t cap = std::max<size_t>(n, 2 * e->table_cap);
+        NB_CUDA(ctx, cudaStreamSynchronize(e->stream));  // enqueued steps still read the old table
         if (e->d_table) cudaFree(e->d_table);
         e->d_table = nullptr;
         e->table_cap = 0;
@@ -311,6 +344,7 @@ nimbus_status rebuild_table(nimbus_engine* e)
     }
     if (pre > e->prefix_cap)
     {
+        NB_CUDA(ctx, cudaStreamSynchronize(e->stream));
         if (e->d_prefix) cudaFree(e->d_prefix);
         e->d_prefix = nullptr;
         e->prefix_cap = 0;
@@ -322,6 +356,13 @@ nimbus_status rebuild_table(nimbus_engine* e)
     {
         slot.m.image_offset = image;
         image += 9LL * slot.m.items[kItemCells];
+        // Marching tiles: (j, k) blocks of one CTA times i-chunks of march_len planes.
+        EngineMember& M = slot.m;
+        const int blocks = (M.F.d.ny * M.F.d.nz + kEngineBlock - 1) / kEngineBlock;
+        const int chunks = (M.F.d.nx + e->march_len - 1) / e->march_len;
+        M.march_len = e->march_len;
+        M.march_blocks = blocks;
+        M.items[kItemMarch] = blocks * kEngineBlock * chunks;
     }
     std::vector<EngineMember> host(n);
     for (size_t r = 0; r < n; ++r) host[r] = e->slots[e->order[r]].m;
@@ -350,36 +391,21 @@ nimbus_status rebuild_table(nimbus_engine* e)
     }
     if (n)
     {
-        NB_CUDA(ctx, cudaMemcpy(e->d_table, host.data(), sizeof(EngineMember) * n, cudaMemcpyHostToDevice));
-        NB_CUDA(ctx, cudaMemcpy(e->d_prefix, e->prefix.data(), sizeof(long long) * pre, cudaMemcpyHostToDevice));
+        // Stream-ordered after every enqueued step (the host views already
+        // include their rotations); pageable sources are staged before the
+        // calls return, so the vectors may go.
+        NB_CUDA(ctx, cudaMemcpyAsync(e->d_table, host.data(), sizeof(EngineMember) * n, cudaMemcpyHostToDevice,
+                                     e->stream));
+        NB_CUDA(ctx, cudaMemcpyAsync(e->d_prefix, e->prefix.data(), sizeof(long long) * pre,
+                                     cudaMemcpyHostToDevice, e->stream));
     }
     e->table_current = true;
-    if (e->exec)
-    {
-        cudaGraphExecDestroy(e->exec);
-        e->exec = nullptr;
-    }
-    if (e->graph)
-    {
-        cudaGraphDestroy(e->graph);
-        e->graph = nullptr;
-    }
-    e->dirty = false;
-    return NIMBUS_OK;
-}
-
-// Substep counts of the resolve_substeps members for the next large step
-// (the reference's choose_runtime_timestep + resolve_substep_count before
-// every step): scan every member's (gamma p) / rho on the device, wait for the
-// per-member maxima, and give each member whose count changed its new count
-// and substep parameters (the table and graph are then rebuilt).
-nimbus_status resolve_substeps(nimbus_engine* e)
-{
-    nimbus_cuda_context* ctx = e->ctx;
-    if (e->dirty) NB_TRY(rebuild_table(e));
-    const size_t n = e->order.size();
-    if (n == 0) return NIMBUS_OK;
-    if (n > e->c2_cap)
+    e->graphs_stale = true;
+    // The acoustic speed scan's per-row maxima (device) and their pinned host copy.
+    e->resolving = false;
+    for (const auto& slot : e->slots) e->resolving = e->resolving || slot.desc.resolve_substeps;
+    e->scan_pending = false;  // rows moved: an earlier scan no longer matches them
+    if (e->resolving && n > e->c2_cap)
     {
         NB_CUDA(ctx, cudaStreamSynchronize(e->stream));
         if (e->d_c2) cudaFree(e->d_c2);
@@ -387,26 +413,53 @@ nimbus_status resolve_substeps(nimbus_engine* e)
         e->d_c2 = nullptr;
         e->h_c2 = nullptr;
         e->c2_cap = 0;
-        const size_t cap = std::max<size_t>(n, 64);
+        const size_t cap = std::max<size_t>(2 * n, 64);
         NB_CUDA(ctx, cudaMalloc(&e->d_c2, cap * sizeof(unsigned long long)));
         NB_CUDA(ctx, cudaMallocHost(&e->h_c2, cap * sizeof(unsigned long long)));
         e->c2_cap = cap;
     }
+    if (e->resolving && !e->scan_done) NB_CUDA(ctx, cudaEventCreateWithFlags(&e->scan_done, cudaEventDisableTiming));
+    e->dirty = false;
+    return NIMBUS_OK;
+}
+
+// The acoustic speed scan outside a step (after admissions, writes or
+// uploads changed the state the next step starts from): every member's
+// maximum (gamma p) / rho into d_c2 by table row, copied to the pinned h_c2.
+// Inside a step the scan is part 1's last launch.
+nimbus_status enqueue_scan(nimbus_engine* e)
+{
+    nimbus_cuda_context* ctx = e->ctx;
+    const size_t n = e->order.size();
     NB_CUDA(ctx, cudaMemsetAsync(e->d_c2, 0, n * sizeof(unsigned long long), e->stream));
     for (const Lane& L : e->lanes)
     {
-        const long long tiles = tiles_of(e, L, kItemCells, L.members);
+        const long long tiles = tiles_of(e, L, kItemScan, L.members);
         if (tiles <= 0) continue;
         engine_sound_speed_kernel<<<engine_grid(e, reinterpret_cast<const void*>(engine_sound_speed_kernel), tiles),
-                                    kEngineBlock, 0, e->stream>>>(e->d_table + L.first, prefix_of(e, L, kItemCells),
+                                    kEngineBlock, 0, e->stream>>>(e->d_table + L.first, prefix_of(e, L, kItemScan),
                                                                   tiles, e->d_c2 + L.first);
         ctx->launches += 1;
     }
     NB_CUDA(ctx, cudaGetLastError());
     NB_CUDA(ctx, cudaMemcpyAsync(e->h_c2, e->d_c2, n * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                                  e->stream));
-    NB_TRY(sync_table_to_host(e));  // waits for the copy; host views exact
-    for (size_t r = 0; r < n; ++r)
+    NB_CUDA(ctx, cudaEventRecord(e->scan_done, e->stream));
+    e->scan_pending = true;
+    return NIMBUS_OK;
+}
+
+// Substep counts of the resolve_substeps members for the step whose part 0 is
+// enqueued (the reference's choose_runtime_timestep + resolve_substep_count
+// before every step): waits for the pending scan of that step's starting
+// state and gives each member whose count changed its new count and substep
+// parameters (the table and graphs are then rebuilt).
+nimbus_status apply_scan(nimbus_engine* e)
+{
+    nimbus_cuda_context* ctx = e->ctx;
+    NB_CUDA(ctx, cudaEventSynchronize(e->scan_done));
+    e->scan_pending = false;
+    for (size_t r = 0; r < e->order.size(); ++r)
     {
         MemberSlot& slot = e->slots[static_cast<size_t>(e->order[r])];
         if (!slot.desc.resolve_substeps) continue;
@@ -419,6 +472,7 @@ nimbus_status resolve_substeps(nimbus_engine* e)
         if (count < 1 || count > 4096)
             return fail(ctx, NIMBUS_ERR_UNSUPPORTED, "a member's acoustic CFL needs an unsupported substep count");
         if (count == slot.m.n_substeps) continue;
+        if (!e->dirty) NB_TRY(sync_table_to_host(e));  // exact host views before editing a row
         nimbus_member_desc d = slot.desc;
         d.n_substeps = count;
         fill_params(slot.m, &d);
@@ -427,54 +481,101 @@ nimbus_status resolve_substeps(nimbus_engine* e)
     return NIMBUS_OK;
 }
 
-int enqueue_lane(nimbus_engine* e, int lane, cudaStream_t st)
+int enqueue_lane(nimbus_engine* e, int lane, cudaStream_t st, int part)
 {
-    if (e->ctx->precision == NIMBUS_PRECISION_FP32) return nimbus_fp32::engine_enqueue(e, lane, st);
-    return enqueue_step<RefPolicy, false>(e, lane, st);
+    if (e->ctx->precision == NIMBUS_PRECISION_FP32) return nimbus_fp32::engine_enqueue(e, lane, st, part);
+    return enqueue_step<RefPolicy, false>(e, lane, st, part);
 }
 
-// One large step of every lane: lanes 1.. forked from `st` onto their own
-// streams and joined back (inside a capture this builds parallel branches of
-// one graph).  Returns the launch count.
-int enqueue(nimbus_engine* e, cudaStream_t st)
+// Part `part` of one large step of every lane: lanes 1.. forked from `st`
+// onto their own streams and joined back (inside a capture this builds
+// parallel branches of one graph).  Part 1 with resolving members ends with
+// the copy of the scan maxima to the host.  Returns the launch count.
+int enqueue(nimbus_engine* e, cudaStream_t st, int part)
 {
     const size_t lanes = e->lanes.size();
     if (lanes == 0) return 0;
-    if (lanes == 1) return enqueue_lane(e, 0, st);
+    const bool scan = part == 1 && e->resolving;
+    if (scan) cudaMemsetAsync(e->d_c2, 0, e->order.size() * sizeof(unsigned long long), st);
     int count = 0;
-    cudaEventRecord(e->fork, st);
-    for (size_t k = 1; k < lanes; ++k)
+    if (lanes == 1) count = enqueue_lane(e, 0, st, part);
+    else
     {
-        cudaStream_t ls = e->lane_streams[k - 1];
-        cudaStreamWaitEvent(ls, e->fork, 0);
-        count += enqueue_lane(e, static_cast<int>(k), ls);
-        cudaEventRecord(e->lane_done[k - 1], ls);
+        cudaEventRecord(e->fork, st);
+        for (size_t k = 1; k < lanes; ++k)
+        {
+            cudaStream_t ls = e->lane_streams[k - 1];
+            cudaStreamWaitEvent(ls, e->fork, 0);
+            count += enqueue_lane(e, static_cast<int>(k), ls, part);
+            cudaEventRecord(e->lane_done[k - 1], ls);
+        }
+        count += enqueue_lane(e, 0, st, part);
+        for (size_t k = 1; k < lanes; ++k) cudaStreamWaitEvent(st, e->lane_done[k - 1], 0);
     }
-    count += enqueue_lane(e, 0, st);
-    for (size_t k = 1; k < lanes; ++k) cudaStreamWaitEvent(st, e->lane_done[k - 1], 0);
+    if (scan)
+        cudaMemcpyAsync(e->h_c2, e->d_c2, e->order.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
     return count;
 }
 
-nimbus_status build_graph(nimbus_engine* e)
+// Captures both parts of a step.  An admission or retirement that keeps the
+// graphs' shape (lanes, launches per lane) only changes launch parameters
+// (grid sizes, table rows, tile counts): the instantiated graph is updated in
+// place (cudaGraphExecUpdate) rather than instantiated again.
+nimbus_status build_graphs(nimbus_engine* e)
 {
     nimbus_cuda_context* ctx = e->ctx;
     cudaStream_t st = e->stream;
-    NB_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    const int launches = enqueue(e, st);
-    cudaGraph_t g = nullptr;
-    const cudaError_t end = cudaStreamEndCapture(st, &g);
-    if (end != cudaSuccess) return cuda_fail(ctx, end, "engine graph capture");
-    cudaGraphExec_t x = nullptr;
-    const cudaError_t inst = cudaGraphInstantiate(&x, g, 0);
-    if (inst != cudaSuccess)
+    if (e->built_precision != ctx->precision) destroy_graphs(e);
+    for (int part = 0; part < 2; ++part)
     {
-        cudaGraphDestroy(g);
-        return cuda_fail(ctx, inst, "engine graph instantiation");
+        NB_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        const int launches = enqueue(e, st, part);
+        cudaGraph_t g = nullptr;
+        const cudaError_t end = cudaStreamEndCapture(st, &g);
+        if (end != cudaSuccess) return cuda_fail(ctx, end, "engine graph capture");
+        bool updated = false;
+        if (e->exec[part])
+        {
+            cudaGraphExecUpdateResultInfo info{};
+            updated = cudaGraphExecUpdate(e->exec[part], g, &info) == cudaSuccess;
+            if (!updated)
+            {
+                (void)cudaGetLastError();  // a refused update is not an error of the engine
+                cudaGraphExecDestroy(e->exec[part]);
+                e->exec[part] = nullptr;
+            }
+        }
+        if (!updated)
+        {
+            cudaGraphExec_t x = nullptr;
+            const cudaError_t inst = cudaGraphInstantiate(&x, g, 0);
+            if (inst != cudaSuccess)
+            {
+                cudaGraphDestroy(g);
+                return cuda_fail(ctx, inst, "engine graph instantiation");
+            }
+            e->exec[part] = x;
+            ++e->graph_instantiations;
+        }
+        else
+            ++e->graph_updates;
+        if (e->graph[part]) cudaGraphDestroy(e->graph[part]);
+        e->graph[part] = g;
+        e->launches_part[part] = launches;
     }
-    e->graph = g;
-    e->exec = x;
-    e->launches_per_step = launches;
+    e->graphs_stale = false;
+    e->launches_per_step = e->launches_part[0] + e->launches_part[1];
     e->built_precision = ctx->precision;
+    return NIMBUS_OK;
+}
+
+// Enqueues part `part` of one step (graph or eager launches).
+nimbus_status launch_part(nimbus_engine* e, bool graph, int part)
+{
+    nimbus_cuda_context* ctx = e->ctx;
+    if (graph) NB_CUDA(ctx, cudaGraphLaunch(e->exec[part], e->stream));
+    else e->launches_part[part] = enqueue(e, e->stream, part);
+    ctx->launches += static_cast<uint64_t>(e->launches_part[part]);
     return NIMBUS_OK;
 }
 
@@ -562,6 +663,15 @@ nimbus_status nimbus_cuda_engine_create(nimbus_cuda_context* ctx, nimbus_engine*
     if (!ctx || !out) return NIMBUS_ERR_INVALID_ARGUMENT;
     *out = nullptr;
     NB_CUDA(ctx, cudaSetDevice(ctx->device));
+    // Member arenas come from the device's default memory pool (stream-ordered
+    // allocation); keep what retirements free there, so that admissions reuse
+    // it without mapping memory again.  free_device_bytes counts it as free.
+    {
+        cudaMemPool_t pool = nullptr;
+        NB_CUDA(ctx, cudaDeviceGetDefaultMemPool(&pool, ctx->device));
+        unsigned long long keep = ~0ull;
+        NB_CUDA(ctx, cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    }
     auto* e = new (std::nothrow) nimbus_engine();
     if (!e) return fail(ctx, NIMBUS_ERR_OUT_OF_MEMORY, "engine allocation failed");
     e->ctx = ctx;
@@ -579,10 +689,11 @@ void nimbus_cuda_engine_destroy(nimbus_engine* e)
 {
     if (!e) return;
     cudaStreamSynchronize(e->stream);
-    if (e->exec) cudaGraphExecDestroy(e->exec);
-    if (e->graph) cudaGraphDestroy(e->graph);
+    destroy_graphs(e);
+    if (e->scan_done) cudaEventDestroy(e->scan_done);
     for (auto& s : e->slots)
-        if (s.arena) cudaFree(s.arena);
+        if (s.arena) cudaFreeAsync(s.arena, e->stream);
+    cudaStreamSynchronize(e->stream);
     if (e->d_table) cudaFree(e->d_table);
     if (e->d_prefix) cudaFree(e->d_prefix);
     if (e->d_image) cudaFree(e->d_image);
@@ -611,14 +722,15 @@ nimbus_status nimbus_cuda_engine_admit(nimbus_engine* e, const nimbus_member_des
     if (const char* why = check_state(initial)) return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, why);
     NB_CUDA(ctx, cudaSetDevice(ctx->device));
     const ArenaLayout L = arena_layout(desc);
-    size_t free_bytes = 0, total_bytes = 0;
-    NB_CUDA(ctx, cudaMemGetInfo(&free_bytes, &total_bytes));
+    size_t free_bytes = 0;
+    NB_TRY(free_device_bytes(ctx, &free_bytes));
     if (L.total + reserve_bytes > free_bytes)
         return fail(ctx, NIMBUS_ERR_OUT_OF_MEMORY, "member does not fit the free device memory");
-    NB_TRY(sync_table_to_host(e));
 
-    // A resolve_substeps member starts with the count its initial state gives
-    // (the same scan the device repeats before every step).
+    // A resolve_substeps member starts with the count of its base columns'
+    // sound speed; the device scan of its initial state, which runs before
+    // its first step, settles the count of that step (admission does no pass
+    // over the state on the host).
     nimbus_member_desc first = *desc;
     double c_base = 0.0;
     if (desc->resolve_substeps)
@@ -628,17 +740,8 @@ nimbus_status nimbus_cuda_engine_admit(nimbus_engine* e, const nimbus_member_des
             if (!finite_positive(desc->p0_base[k]) || !finite_positive(desc->rho0_base[k]))
                 return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "base pressure and density must be positive and finite");
         c_base = base_sound_speed(desc->p0_base, desc->rho0_base, desc->nz, gamma);
-        double best = 0.0;
-        for (size_t c = 0; c < L.cells; ++c)
-        {
-            const double ph = initial->p[c], rh = initial->rho[c];
-            if (!finite_positive(ph) || !finite_positive(rh))
-                return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT,
-                            "CFL scan requires finite wind and positive finite pressure/density");
-            best = std::max(best, gamma * ph / rh);
-        }
-        const int count = resolve_substep_count(desc->dt, std::max(std::sqrt(best), c_base),
-                                                std::min({desc->dx, desc->dy, desc->dz}), desc->n_substeps);
+        const int count = resolve_substep_count(desc->dt, c_base, std::min({desc->dx, desc->dy, desc->dz}),
+                                                desc->n_substeps);
         if (count < 1 || count > 4096)
             return fail(ctx, NIMBUS_ERR_UNSUPPORTED, "the acoustic CFL needs an unsupported substep count");
         first.n_substeps = count;
@@ -652,7 +755,9 @@ nimbus_status nimbus_cuda_engine_admit(nimbus_engine* e, const nimbus_member_des
     slot.desc.sponge = nullptr;
     slot.bytes = L.total;
     {
-        const cudaError_t err = cudaMalloc(&slot.arena, L.total);
+        // Stream-ordered: the arena is ready for everything later on the
+        // engine stream, and admission does not wait for enqueued steps.
+        const cudaError_t err = cudaMallocAsync(&slot.arena, L.total, e->stream);
         if (err != cudaSuccess) return cuda_fail(ctx, err, "member allocation");
     }
     char* base = static_cast<char*>(slot.arena);
@@ -708,8 +813,12 @@ nimbus_status nimbus_cuda_engine_admit(nimbus_engine* e, const nimbus_member_des
     const float* src[9] = {initial->u, initial->v, initial->w, initial->rho, initial->p, initial->theta,
                            initial->qv, initial->qc, initial->qr};
     float* dst[9] = {M.u, M.v, M.w, M.rho, M.p, M.theta, M.qv, M.qc, M.qr};
-    for (int f = 0; f < 9 && err == cudaSuccess; ++f) err = cudaMemcpy(dst[f], src[f], bytes, cudaMemcpyHostToDevice);
-    if (err == cudaSuccess) err = cudaMemcpy(prof, hp.data(), hp.size() * sizeof(double), cudaMemcpyHostToDevice);
+    // Pageable sources are staged before each call returns (the caller's
+    // arrays and the local vectors may go); pinned ones are read by the copy.
+    for (int f = 0; f < 9 && err == cudaSuccess; ++f)
+        err = cudaMemcpyAsync(dst[f], src[f], bytes, cudaMemcpyHostToDevice, e->stream);
+    if (err == cudaSuccess)
+        err = cudaMemcpyAsync(prof, hp.data(), hp.size() * sizeof(double), cudaMemcpyHostToDevice, e->stream);
     M.R = RelaxTables{};
     M.close_step = desc->final_closure != 0;
     if (err == cudaSuccess && desc->sponge)
@@ -721,8 +830,9 @@ nimbus_status nimbus_cuda_engine_admit(nimbus_engine* e, const nimbus_member_des
                           sp->do_lateral, sp->staggered, sp->implicit_mode, desc->dt, img);
         unsigned char* dev = reinterpret_cast<unsigned char*>(base + L.off_sponge);
         const size_t tab_bytes = img.tab.size() * sizeof(double);
-        err = cudaMemcpy(dev, img.tab.data(), tab_bytes, cudaMemcpyHostToDevice);
-        if (err == cudaSuccess) err = cudaMemcpy(dev + tab_bytes, img.on.data(), img.on.size(), cudaMemcpyHostToDevice);
+        err = cudaMemcpyAsync(dev, img.tab.data(), tab_bytes, cudaMemcpyHostToDevice, e->stream);
+        if (err == cudaSuccess)
+            err = cudaMemcpyAsync(dev + tab_bytes, img.on.data(), img.on.size(), cudaMemcpyHostToDevice, e->stream);
         M.R = relax_tables(img, dev, desc->nz);
     }
     if (err == cudaSuccess)
@@ -731,14 +841,13 @@ nimbus_status nimbus_cuda_engine_admit(nimbus_engine* e, const nimbus_member_des
         // see identical base data.
         level_base_kernel<<<(desc->nz + 127) / 128, 128, 0, e->stream>>>(M.p0, desc->nz, M.gamma, dp0, eos0);
         err = cudaGetLastError();
-        if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
     }
-    if (err == cudaSuccess) err = cudaMemset(M.status, 0, sizeof(unsigned));
+    if (err == cudaSuccess) err = cudaMemsetAsync(M.status, 0, sizeof(unsigned), e->stream);
     // Scratch that a step reads before writing: none, but keep it defined.
-    if (err == cudaSuccess) err = cudaMemset(M.wave, 0, L.history * sizeof(float));
+    if (err == cudaSuccess) err = cudaMemsetAsync(M.wave, 0, L.history * sizeof(float), e->stream);
     if (err != cudaSuccess)
     {
-        cudaFree(slot.arena);
+        cudaFreeAsync(slot.arena, e->stream);
         return cuda_fail(ctx, err, "member upload");
     }
     e->slots.push_back(slot);
@@ -754,8 +863,8 @@ nimbus_status nimbus_cuda_engine_retire(nimbus_engine* e, int member_id)
     nimbus_cuda_context* ctx = e->ctx;
     size_t index = 0;
     if (!find_slot(e, member_id, &index)) return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "unknown member id");
-    NB_TRY(sync_table_to_host(e));
-    NB_CUDA(ctx, cudaFree(e->slots[index].arena));
+    // Freed in stream order after the enqueued steps that still use it; no wait.
+    NB_CUDA(ctx, cudaFreeAsync(e->slots[index].arena, e->stream));
     e->slots.erase(e->slots.begin() + static_cast<long>(index));
     e->dirty = true;
     return NIMBUS_OK;
@@ -781,6 +890,7 @@ nimbus_status nimbus_cuda_engine_read_async(nimbus_engine* e, int member_id, con
 nimbus_status nimbus_cuda_engine_write_async(nimbus_engine* e, int member_id, const nimbus_member_state* in)
 {
     if (!e) return NIMBUS_ERR_INVALID_ARGUMENT;
+    e->scan_pending = false;  // the next step's starting state changes
     nimbus_cuda_context* ctx = e->ctx;
     if (const char* why = check_state(in)) return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, why);
     MemberSlot* s = find_slot(e, member_id);
@@ -860,6 +970,7 @@ size_t nimbus_cuda_engine_image_offset(const nimbus_engine* e, int member_id)
 nimbus_status nimbus_cuda_engine_upload_image_async(nimbus_engine* e, const void* host_image)
 {
     if (!e || !host_image) return NIMBUS_ERR_INVALID_ARGUMENT;
+    e->scan_pending = false;  // the next step's starting state changes
     nimbus_cuda_context* ctx = e->ctx;
     size_t bytes = 0;
     NB_TRY(prepare_image(e, &bytes));
@@ -891,34 +1002,53 @@ nimbus_status nimbus_cuda_engine_step(nimbus_engine* e, int n_steps)
     if (e->dirty) NB_TRY(rebuild_table(e));
     if (e->slots.empty() || n_steps == 0) return NIMBUS_OK;
     const bool graph = e->use_graph && !ctx->timing;
-    if (graph && (!e->exec || e->built_precision != ctx->precision))
-    {
-        if (e->exec)
-        {
-            cudaGraphExecDestroy(e->exec);
-            e->exec = nullptr;
-            cudaGraphDestroy(e->graph);
-            e->graph = nullptr;
-        }
-        NB_TRY(build_graph(e));
-    }
-    bool resolving = false;
-    for (const auto& slot : e->slots) resolving = resolving || slot.desc.resolve_substeps;
+    if (graph && (!e->exec[0] || e->graphs_stale || e->built_precision != ctx->precision)) NB_TRY(build_graphs(e));
     for (int i = 0; i < n_steps; ++i)
     {
-        if (resolving)
+        // Part 0 needs no substep count; with resolving members the counts
+        // are derived while it runs, from the scan of the step's starting
+        // state (part 1 of the previous step, or an explicit scan).
+        if (e->resolving && !e->scan_pending) NB_TRY(enqueue_scan(e));
+        NB_TRY(launch_part(e, graph, 0));
+        if (e->resolving)
         {
-            NB_TRY(resolve_substeps(e));
-            if (e->dirty) NB_TRY(rebuild_table(e));
-            if (graph && !e->exec) NB_TRY(build_graph(e));
+            NB_TRY(apply_scan(e));
+            if (e->dirty)
+            {
+                // The new rows take effect after part 0, whose work is per
+                // member and independent of the row order.
+                NB_TRY(rebuild_table(e));
+                if (graph) NB_TRY(build_graphs(e));
+            }
         }
-        if (graph) NB_CUDA(ctx, cudaGraphLaunch(e->exec, e->stream));
-        else e->launches_per_step = enqueue(e, e->stream);
-        ctx->launches += static_cast<uint64_t>(e->launches_per_step);
+        NB_TRY(launch_part(e, graph, 1));
+        if (e->resolving)
+        {
+            NB_CUDA(ctx, cudaEventRecord(e->scan_done, e->stream));
+            e->scan_pending = true;
+        }
+        e->launches_per_step = e->launches_part[0] + e->launches_part[1];
         rotate_host_views(e, 1);
         e->table_current = e->mirror_exact;
     }
     NB_CUDA(ctx, cudaGetLastError());
+    return NIMBUS_OK;
+}
+
+nimbus_status nimbus_cuda_engine_member_status_async(nimbus_engine* e, int member_id, unsigned* host_flags)
+{
+    if (!e || !host_flags) return NIMBUS_ERR_INVALID_ARGUMENT;
+    MemberSlot* s = find_slot(e, member_id);
+    if (!s) return fail(e->ctx, NIMBUS_ERR_INVALID_ARGUMENT, "unknown member id");
+    NB_CUDA(e->ctx, cudaMemcpyAsync(host_flags, s->m.status, sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream));
+    return NIMBUS_OK;
+}
+
+nimbus_status nimbus_cuda_engine_graph_builds(const nimbus_engine* e, uint64_t* instantiations, uint64_t* updates)
+{
+    if (!e || !instantiations || !updates) return NIMBUS_ERR_INVALID_ARGUMENT;
+    *instantiations = e->graph_instantiations;
+    *updates = e->graph_updates;
     return NIMBUS_OK;
 }
 
@@ -935,6 +1065,7 @@ nimbus_status nimbus_cuda_engine_synchronize(nimbus_engine* e)
 {
     if (!e) return NIMBUS_ERR_INVALID_ARGUMENT;
     nimbus_cuda_context* ctx = e->ctx;
+    NB_CUDA(ctx, cudaStreamSynchronize(e->stream));
     NB_TRY(sync_table_to_host(e));
     unsigned any = 0;
     for (auto& s : e->slots)
@@ -962,6 +1093,7 @@ nimbus_status nimbus_cuda_engine_member_status(nimbus_engine* e, int member_id, 
     if (!e || !flags) return NIMBUS_ERR_INVALID_ARGUMENT;
     MemberSlot* s = find_slot(e, member_id);
     if (!s) return fail(e->ctx, NIMBUS_ERR_INVALID_ARGUMENT, "unknown member id");
+    NB_CUDA(e->ctx, cudaStreamSynchronize(e->stream));
     NB_TRY(sync_table_to_host(e));
     NB_CUDA(e->ctx, cudaMemcpy(flags, s->m.status, sizeof(unsigned), cudaMemcpyDeviceToHost));
     return NIMBUS_OK;
@@ -987,6 +1119,34 @@ nimbus_status nimbus_cuda_engine_set_lanes(nimbus_engine* e, int lanes)
 }
 
 int nimbus_cuda_engine_lanes(const nimbus_engine* e) { return e ? static_cast<int>(e->lanes.size()) : 0; }
+
+nimbus_status nimbus_cuda_engine_set_acoustic_form(nimbus_engine* e, int form)
+{
+    if (!e || form < NIMBUS_ACOUSTIC_TABLE || form > NIMBUS_ACOUSTIC_MARCH) return NIMBUS_ERR_INVALID_ARGUMENT;
+    if (form != e->acoustic_form)
+    {
+        NB_TRY(sync_table_to_host(e));
+        e->acoustic_form = form;
+        e->dirty = true;
+    }
+    return NIMBUS_OK;
+}
+
+int nimbus_cuda_engine_acoustic_form(const nimbus_engine* e) { return e ? e->acoustic_form : -1; }
+
+nimbus_status nimbus_cuda_engine_set_march(nimbus_engine* e, int planes)
+{
+    if (!e || planes < 1 || planes > 4096) return NIMBUS_ERR_INVALID_ARGUMENT;
+    if (planes != e->march_len)
+    {
+        NB_TRY(sync_table_to_host(e));
+        e->march_len = planes;
+        e->dirty = true;
+    }
+    return NIMBUS_OK;
+}
+
+int nimbus_cuda_engine_march(const nimbus_engine* e) { return e ? e->march_len : -1; }
 
 int nimbus_cuda_engine_members(const nimbus_engine* e) { return e ? static_cast<int>(e->slots.size()) : 0; }
 

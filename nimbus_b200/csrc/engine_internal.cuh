@@ -7,6 +7,7 @@
 #include "engine_kernels.cuh"
 
 #include <map>
+#include <memory>
 #include <vector>
 
 namespace nimbus_engine_detail
@@ -60,12 +61,25 @@ struct nimbus_engine
     std::vector<long long> prefix;  // the lanes' prefix blocks, back to back
     std::vector<nimbus_engine_detail::Lane> lanes;
     int lane_target = 4;            // lanes when there are at least that many members
+    int march_len = 16;             // i-planes per thread of the marching acoustic kernels
+    int acoustic_form = NIMBUS_ACOUSTIC_CONST;  // nimbus_acoustic_form of the continuity and momentum passes
     std::vector<cudaStream_t> lane_streams;  // lanes 1.. (lane 0 runs on the engine stream)
     std::vector<cudaEvent_t> lane_done;
     cudaEvent_t fork = nullptr;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
+    // One large step as two graphs: part 0 (Heun slow step, boundary refresh
+    // and KW78 seed) needs no substep count; part 1 (the acoustic loop and the
+    // rest of the step) does.  With resolve_substeps members, part 1 ends with
+    // the acoustic speed scan of the state the next step starts from, so the
+    // host reads the next step's counts while that step's part 0 runs.
+    cudaGraph_t graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
     int launches_per_step = 0;
+    int launches_part[2] = {0, 0};
+    bool graphs_stale = true;       // the table changed since the graphs were captured
+    uint64_t graph_instantiations = 0, graph_updates = 0;
+    bool resolving = false;         // some member re-derives its substep count every step
+    bool scan_pending = false;      // h_c2 will hold the current rows' scan once scan_done completes
+    cudaEvent_t scan_done = nullptr;
     std::map<const void*, int> occupancy;
     float* d_image = nullptr;       // device staging for the state image
     size_t image_cap = 0;           // bytes
@@ -125,10 +139,12 @@ long long tiles_of(const nimbus_engine* e, const nimbus_engine_detail::Lane& L, 
         }                                                                                                \
     } while (0)
 
-// Enqueues one large step of the members of one lane on `st`; returns the
-// number of launches.
+// Enqueues part `part` of one large step of the members of one lane on `st`
+// (0: Heun slow step, boundary refresh and KW78 seed; 1: the acoustic loop,
+// transport, microphysics and EOS, the closing refresh); returns the number
+// of launches.
 template <class Policy, bool kFp32>
-int enqueue_step(nimbus_engine* e, int lane, cudaStream_t st)
+int enqueue_step(nimbus_engine* e, int lane, cudaStream_t st, int part)
 {
     nimbus_cuda_context* ctx = e->ctx;
     const nimbus_engine_detail::Lane& L = e->lanes[static_cast<size_t>(lane)];
@@ -143,6 +159,8 @@ int enqueue_step(nimbus_engine* e, int lane, cudaStream_t st)
     const long long* pper = prefix_of(e, L, kItemPerimeter);
     const long long cells = tiles_of(e, L, kItemCells, n);
 
+    if (part == 0)
+    {
     // Heun slow step (prepare_slow_rk2_tendencies + apply_slow_tendencies).
     ENGINE_LAUNCH(NIMBUS_KERNEL_SLOW, engine_slow_predict_kernel<Policy>, cells, 1, T, pc, cells);
     ENGINE_LAUNCH(NIMBUS_KERNEL_SLOW, engine_slow_correct_kernel<Policy>, cells, 1, T, pc, cells);
@@ -155,15 +173,73 @@ int enqueue_step(nimbus_engine* e, int lane, cudaStream_t st)
                   pcol, tiles_of(e, L, kItemColumns, n), 1);
     ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_seed_kernel, tiles_of(e, L, kItemHistory, n), 1, T, phist,
                   tiles_of(e, L, kItemHistory, n));
+    return count;
+    }
     // The acoustic loop: members still inside it are a prefix of the lane.
+    const long long* pm = prefix_of(e, L, kItemMarch);
+    // The constant-bank form: the lane's members' constants as one kernel
+    // parameter (lanes of at most kConstMembers members; larger ones take the
+    // member-table form).
+    const int form = (e->acoustic_form == NIMBUS_ACOUSTIC_CONST && n > kConstMembers) ? NIMBUS_ACOUSTIC_TABLE
+                                                                                       : e->acoustic_form;
+    std::unique_ptr<AcousticLaunch> al;
+    if (form == NIMBUS_ACOUSTIC_CONST)
+    {
+        al.reset(new AcousticLaunch());
+        const long long* p = e->prefix.data() + L.prefix_first + static_cast<size_t>(kItemCells) * (n + 1);
+        for (int r = 0; r <= n; ++r) al->prefix[r] = p[r];
+        for (int r = 0; r < n; ++r)
+        {
+            const EngineMember& H = e->slots[static_cast<size_t>(e->order[static_cast<size_t>(L.first + r)])].m;
+            AcousticConst& A = al->m[r];
+            A.F = H.F;
+            A.u = H.u;
+            A.v = H.v;
+            A.w = H.w;
+            A.theta = H.theta;
+            A.mfx = H.mfx;
+            A.mfy = H.mfy;
+            A.mfz = H.mfz;
+            A.rho_begin = H.rho_begin;
+            A.status = H.status;
+            A.rho0 = H.rho0;
+            A.p0 = H.p0;
+            A.dp0 = H.dp0;
+            A.eos0 = H.eos0;
+            A.vertical = kFuseVertical | (H.B.bottom == kBottomNoSlip ? kFuseNoSlipBottom : 0) |
+                         (H.B.top == kTopOpen ? kFuseOpenTop : 0);
+        }
+    }
     for (size_t s = 0; s < L.active.size(); ++s)
     {
         const int a = L.active[s];
         const int si = static_cast<int>(s);
-        ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, engine_continuity_kernel<Policy>, tiles_of(e, L, kItemCells, a), 1,
-                      T, pc, tiles_of(e, L, kItemCells, a), si);
-        ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_MOMENTUM, engine_momentum_kernel<Policy>, tiles_of(e, L, kItemCells, a), 1,
-                      T, pc, tiles_of(e, L, kItemCells, a), si);
+        if (form == NIMBUS_ACOUSTIC_CONST)
+        {
+            const long long tiles = tiles_of(e, L, kItemCells, a);
+            if (s == 0)
+                ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, (engine_continuity_const_kernel<Policy, true>), tiles, 1,
+                              *al, T, tiles, si);
+            else
+                ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, (engine_continuity_const_kernel<Policy, false>), tiles,
+                              1, *al, T, tiles, si);
+            ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_MOMENTUM, engine_momentum_const_kernel<Policy>, tiles, 1, *al, T,
+                          tiles, si);
+        }
+        else if (form == NIMBUS_ACOUSTIC_MARCH)
+        {
+            ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, engine_continuity_march_kernel<Policy>,
+                          tiles_of(e, L, kItemMarch, a), 1, T, pm, tiles_of(e, L, kItemMarch, a), si);
+            ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_MOMENTUM, engine_momentum_march_kernel<Policy>,
+                          tiles_of(e, L, kItemMarch, a), 1, T, pm, tiles_of(e, L, kItemMarch, a), si);
+        }
+        else
+        {
+            ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, engine_continuity_kernel<Policy>,
+                          tiles_of(e, L, kItemCells, a), 1, T, pc, tiles_of(e, L, kItemCells, a), si);
+            ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_MOMENTUM, engine_momentum_kernel<Policy>,
+                          tiles_of(e, L, kItemCells, a), 1, T, pc, tiles_of(e, L, kItemCells, a), si);
+        }
         ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_bc_we_kernel, tiles_of(e, L, kItemRowsWE, a), 1, T, pwe,
                       tiles_of(e, L, kItemRowsWE, a), si, 0);
         ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_bc_sn_kernel, tiles_of(e, L, kItemRowsSN, a), 1, T, psn,
@@ -196,6 +272,10 @@ int enqueue_step(nimbus_engine* e, int lane, cudaStream_t st)
         ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_bc_vertical_kernel, tiles_of(e, L, kItemColumns, n), 1,
                       T, pcol, tiles_of(e, L, kItemColumns, n), 2);
     }
+    // The acoustic speed scan of the state the next step starts from.
+    if (e->resolving)
+        ENGINE_LAUNCH(NIMBUS_KERNEL_MICROPHYSICS, engine_sound_speed_kernel, tiles_of(e, L, kItemScan, n), 1, T,
+                      prefix_of(e, L, kItemScan), tiles_of(e, L, kItemScan, n), e->d_c2 + L.first);
     return count;
 }
 

@@ -35,8 +35,12 @@ enum ItemKind
     kItemColumns,    // nx*ny columns
     kItemHistory,    // (ny + nx)*nz KW78 history slots
     kItemPerimeter,  // 3 nx + 3 (ny - 3) columns the lateral closures write
+    kItemMarch,      // rows along x: (j, k) positions in blocks times i-chunks (for_member_rows)
+    kItemScan,       // cells in groups of kScanCells (engine_sound_speed_kernel)
     kItemKinds
 };
+
+constexpr int kScanCells = 8;  // cells one thread of the acoustic speed scan reads
 
 constexpr int kEngineScalars = 4;  // theta, qv, qc, qr
 
@@ -67,6 +71,8 @@ struct __align__(16) EngineMember
     int close_step;        // end the step with the boundary closure
     int n_substeps;
     int microphysics;
+    int march_len;         // i-planes one thread of a marching kernel advances (kItemMarch tiles)
+    int march_blocks;      // blocks of blockDim.x (j, k) positions per i-chunk
     int items[kItemKinds];
     long long image_offset;  // first float of this member's block in the engine's state image
 };
@@ -106,6 +112,32 @@ __device__ __forceinline__ void for_member_items(const EngineMember* __restrict_
             const int item = base + q * (int)blockDim.x;
             if (item < count) fn(M, item);
         }
+    }
+}
+
+// Calls fn(member, i0, i1, j, k, q) for the rows of the first tiles of
+// kItemMarch: a member's (j, k) positions q = j nz + k are cut into blocks of
+// blockDim.x (a warp reads 32 consecutive floats of a plane) and its x range
+// into chunks of march_len planes; tile = chunk * march_blocks + block.  The
+// thread of position q advances the cells (i0 .. i1-1, j, k) of its row.
+template <class Fn>
+__device__ __forceinline__ void for_member_rows(const EngineMember* __restrict__ table,
+                                                const long long* __restrict__ prefix, long long tiles, Fn&& fn)
+{
+    int m = 0;
+    for (long long t = blockIdx.x; t < tiles; t += gridDim.x)
+    {
+        while (t >= prefix[m + 1]) ++m;
+        const EngineMember& M = table[m];
+        const int local = (int)(t - prefix[m]);
+        const int chunk = local / M.march_blocks;
+        const int q = (local - chunk * M.march_blocks) * (int)blockDim.x + (int)threadIdx.x;
+        const Dims d = M.F.d;
+        if (q >= d.ny * d.nz) continue;
+        int i, j, k;
+        decompose(d, q, i, j, k);
+        const int i0 = chunk * M.march_len;
+        fn(M, i0, min(d.nx, i0 + M.march_len), j, k, q);
     }
 }
 
@@ -254,6 +286,124 @@ static __global__ void __launch_bounds__(256) engine_momentum_kernel(const Engin
     });
 }
 
+// The same two passes marching along x (continuity_eos_march, momentum_march):
+// one thread per (j, k) row segment of march_len cells.
+#ifndef NIMBUS_MARCH_MINB
+#define NIMBUS_MARCH_MINB 4
+#endif
+template <class Policy>
+static __global__ void __launch_bounds__(256, NIMBUS_MARCH_MINB) engine_continuity_march_kernel(const EngineMember* __restrict__ table,
+                                                                      const long long* __restrict__ prefix,
+                                                                      long long tiles, int s)
+{
+    const bool first = s == 0;
+    for_member_rows(table, prefix, tiles, [&](const EngineMember& M, int i0, int i1, int j, int k, int q) {
+        unsigned flags = 0;
+        continuity_eos_march<Policy>(M.F, engine_density(M, s, false), M.u, M.v, M.w, M.theta, M.rho0, M.eos0,
+                                     engine_density(M, s, true), M.p, M.mfx, M.mfy, M.mfz, i0, i1, j, k, q, flags,
+                                     first, first ? M.rho_begin : nullptr);
+        if (flags) atomicOr(M.status, flags);
+    });
+}
+
+template <class Policy>
+static __global__ void __launch_bounds__(256) engine_momentum_march_kernel(const EngineMember* __restrict__ table,
+                                                                    const long long* __restrict__ prefix,
+                                                                    long long tiles, int s)
+{
+    for_member_rows(table, prefix, tiles, [&](const EngineMember& M, int i0, int i1, int j, int k, int q) {
+        const int vertical = kFuseVertical | (M.B.bottom == kBottomNoSlip ? kFuseNoSlipBottom : 0) |
+                             (M.B.top == kTopOpen ? kFuseOpenTop : 0);
+        momentum_march<Policy>(M.F, engine_density(M, s, true), M.p, M.p0, M.dp0, M.u, M.v, M.w, i0, i1, j, k, q,
+                               vertical);
+    });
+}
+
+// ---- Acoustic passes with the members' constants in the constant bank ----
+//
+// A kernel that reads a member's parameters and pointers from the member
+// table holds them in registers (about 50 values for continuity), which caps
+// it at 5-6 resident CTAs per SM; the per-operation kernels take the same
+// values from the constant bank as instruction operands and run at full
+// occupancy with 32 registers.  So each launch of a lane gets its members'
+// constants as one kernel parameter (__grid_constant__, the constant bank):
+// the parameter blocks and every buffer that does not rotate.  The rotating
+// buffers (density ping-pong, pressure) are read from the member table.
+struct AcousticConst
+{
+    FusedParams F;
+    float *u, *v, *w, *theta, *mfx, *mfy, *mfz, *rho_begin;
+    unsigned* status;
+    const double *rho0, *p0;
+    const float2* dp0;
+    const float4* eos0;
+    int vertical;  // kFuse* bits of the momentum pass
+};
+
+constexpr int kConstMembers = 64;  // members one launch can carry in its parameter
+
+// Resident CTAs per SM the launch bounds ask for (continuity, momentum):
+// measured on the 64-member ensemble, FP32, ms per step: natural register
+// counts (48 / 36 registers) 14.41, 6 / 7 CTAs (40 / 36) 13.49, 8 / 8 (32
+// registers, spilling) 14.49.
+#ifndef NIMBUS_CONST_MINB
+#define NIMBUS_CONST_MINB 6
+#endif
+#ifndef NIMBUS_CONST_MINB_MOM
+#define NIMBUS_CONST_MINB_MOM 7
+#endif
+
+struct AcousticLaunch
+{
+    long long prefix[kConstMembers + 1];  // first cell tile of each member
+    AcousticConst m[kConstMembers];
+};
+static_assert(sizeof(AcousticLaunch) <= 32000, "a kernel parameter block holds at most 32764 bytes");
+
+// kFirst: the first substep of the step (the retained fluxes are written, not
+// accumulated, and the beginning density is kept).
+template <class Policy, bool kFirst>
+static __global__ void __launch_bounds__(256, NIMBUS_CONST_MINB) engine_continuity_const_kernel(const __grid_constant__ AcousticLaunch L,
+                                                                      const EngineMember* __restrict__ table,
+                                                                      long long tiles, int s)
+{
+    constexpr bool first = kFirst;
+    const bool even = (s & 1) == 0;
+    int m = 0;
+    for (long long t = blockIdx.x; t < tiles; t += gridDim.x)
+    {
+        while (t >= L.prefix[m + 1]) ++m;
+        const AcousticConst& A = L.m[m];
+        const int c = (int)((t - L.prefix[m]) * blockDim.x) + (int)threadIdx.x;
+        if (c >= A.F.d.cells()) continue;
+        const EngineMember& M = table[m];
+        unsigned flags = 0;
+        continuity_eos_cell<Policy>(A.F, even ? M.rho : M.rho_alt, A.u, A.v, A.w, A.theta, A.rho0, A.eos0,
+                                    even ? M.rho_alt : M.rho, M.p, nullptr, A.mfx, A.mfy, A.mfz, c, flags, first,
+                                    first ? A.rho_begin : nullptr);
+        if (flags) atomicOr(A.status, flags);
+    }
+}
+
+template <class Policy>
+static __global__ void __launch_bounds__(256, NIMBUS_CONST_MINB_MOM) engine_momentum_const_kernel(const __grid_constant__ AcousticLaunch L,
+                                                                    const EngineMember* __restrict__ table,
+                                                                    long long tiles, int s)
+{
+    const bool even = (s & 1) == 0;
+    int m = 0;
+    for (long long t = blockIdx.x; t < tiles; t += gridDim.x)
+    {
+        while (t >= L.prefix[m + 1]) ++m;
+        const AcousticConst& A = L.m[m];
+        const int c = (int)((t - L.prefix[m]) * blockDim.x) + (int)threadIdx.x;
+        if (c >= A.F.d.cells()) continue;
+        const EngineMember& M = table[m];
+        momentum_cell<Policy>(A.F, even ? M.rho_alt : M.rho, M.p, A.p0, A.dp0, A.u, A.v, A.w, A.u, A.v, A.w, c,
+                              A.vertical);
+    }
+}
+
 // ---- state image ----------------------------------------------------------
 // The engine's state image holds every member's nine prognostic fields back to
 // back (u, v, w, rho, p, theta, qv, qc, qr, each items[kItemCells] floats) from
@@ -367,6 +517,8 @@ static __global__ void __launch_bounds__(256) engine_transport_update_kernel(con
 // (src/numerics/runtime.cpp:346-401,854-880).  The member of a tile is
 // block-uniform, so a block keeps a running maximum while it walks one
 // member's tiles and publishes it with one atomicMax when it moves on.
+// One thread reads kScanCells cells (kItemScan tiles), which keeps the
+// per-tile member lookup off the scan's critical path.
 static __global__ void __launch_bounds__(256) engine_sound_speed_kernel(const EngineMember* __restrict__ table,
                                                                         const long long* __restrict__ prefix,
                                                                         long long tiles, unsigned long long* c2)
@@ -387,13 +539,15 @@ static __global__ void __launch_bounds__(256) engine_sound_speed_kernel(const En
             best = 0;
         }
         const EngineMember& M = table[m];
-        const int c = (int)((t - prefix[m]) * blockDim.x) + (int)threadIdx.x;
-        if (c < M.items[kItemCells])
+        const int c0 = (int)((t - prefix[m]) * blockDim.x * kScanCells) + (int)threadIdx.x;
+        unsigned flags = 0;
+#pragma unroll
+        for (int q = 0; q < kScanCells; ++q)
         {
-            unsigned flags = 0;
-            best = max(best, sound_speed_sq_bits(M.gamma, M.p[c], M.rho[c], flags));
-            if (flags) atomicOr(M.status, flags);
+            const int c = c0 + q * (int)blockDim.x;
+            if (c < M.items[kItemCells]) best = max(best, sound_speed_sq_bits(M.gamma, M.p[c], M.rho[c], flags));
         }
+        if (flags) atomicOr(M.status, flags);
     }
     if (held >= 0)
     {

@@ -40,9 +40,9 @@ nimbus_status launch_transport(nimbus_cuda_context* ctx, cudaStream_t st, const 
     return launch_transport_impl<true>(ctx, st, T, rho_end, rho_begin, mfx, mfy, mfz, sf, rl);
 }
 
-int engine_enqueue(nimbus_engine* e, int lane, cudaStream_t st)
+int engine_enqueue(nimbus_engine* e, int lane, cudaStream_t st, int part)
 {
-    return enqueue_step<nimbus::Fp32Policy, true>(e, lane, st);
+    return enqueue_step<nimbus::Fp32Policy, true>(e, lane, st, part);
 }
 
 }  // namespace nimbus_fp32

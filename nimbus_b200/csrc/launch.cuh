@@ -189,6 +189,7 @@ nimbus_status run_slow(nimbus_cuda_context* ctx, cudaStream_t st, const nimbus::
 nimbus_status launch_transport(nimbus_cuda_context* ctx, cudaStream_t st, const nimbus::TransportParams& T,
                                const float* rho_end, const float* rho_begin, const float* mfx, const float* mfy,
                                const float* mfz, float* sf, float* rl);
-// One large step of every engine member (FP32 form); returns the launch count.
-int engine_enqueue(nimbus_engine* e, int lane, cudaStream_t st);
+// Part `part` of one large step of every engine member of a lane (FP32 form);
+// returns the launch count.
+int engine_enqueue(nimbus_engine* e, int lane, cudaStream_t st, int part);
 }  // namespace nimbus_fp32

@@ -254,7 +254,10 @@ EXPORTED_SYMBOLS = (
     "nimbus_cuda_engine_synchronize", "nimbus_cuda_engine_member_status", "nimbus_cuda_engine_set_graph",
     "nimbus_cuda_engine_members", "nimbus_cuda_engine_launches_per_step", "nimbus_cuda_engine_member_substeps",
     "nimbus_cuda_max_sound_speed", "nimbus_cuda_resolve_substep_count",
+    "nimbus_cuda_engine_set_march", "nimbus_cuda_engine_march", "nimbus_cuda_engine_set_acoustic_form",
+    "nimbus_cuda_engine_acoustic_form", "nimbus_cuda_engine_member_status_async", "nimbus_cuda_engine_graph_builds",
 )
+ACOUSTIC_TABLE, ACOUSTIC_CONST, ACOUSTIC_MARCH = 0, 1, 2
 SUBSTEP_AUTO, SUBSTEP_FUSED, SUBSTEP_SPLIT = 0, 1, 2
 PRECISION_REFERENCE, PRECISION_FP32 = 0, 1
 STATIC_SCRATCH_CELLS = 4194304  # NIMBUS_STATIC_SCRATCH_CELLS
@@ -350,6 +353,13 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
     lib.nimbus_cuda_engine_members.argtypes = [vp]
     lib.nimbus_cuda_engine_launches_per_step.argtypes = [vp]
     lib.nimbus_cuda_engine_member_substeps.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    lib.nimbus_cuda_engine_set_march.argtypes = [vp, ctypes.c_int]
+    lib.nimbus_cuda_engine_march.argtypes = [vp]
+    lib.nimbus_cuda_engine_set_acoustic_form.argtypes = [vp, ctypes.c_int]
+    lib.nimbus_cuda_engine_member_status_async.argtypes = [vp, ctypes.c_int, ctypes.c_void_p]
+    lib.nimbus_cuda_engine_graph_builds.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64),
+                                                    ctypes.POINTER(ctypes.c_uint64)]
+    lib.nimbus_cuda_engine_acoustic_form.argtypes = [vp]
     lib.nimbus_cuda_max_sound_speed.argtypes = [vp, ctypes.POINTER(SoundSpeedArgs)]
     lib.nimbus_cuda_resolve_substep_count.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                                       ctypes.c_int]
@@ -968,6 +978,18 @@ class Engine:
         self.shapes[mid.value] = (desc.nx, desc.ny, desc.nz)
         return mid.value
 
+    def member_status_async(self, member_id: int, host_flags) -> None:
+        """Enqueue the copy of a member's status word into host_flags (a pinned
+        uint32 array of one element), in stream order."""
+        self.ctx.check(self.lib.nimbus_cuda_engine_member_status_async(self.handle, int(member_id),
+                                                                      ctypes.c_void_p(host_flags.ctypes.data)))
+
+    def graph_builds(self) -> tuple:
+        """(instantiations, in-place updates) of the step graphs so far."""
+        a, b = ctypes.c_uint64(), ctypes.c_uint64()
+        self.ctx.check(self.lib.nimbus_cuda_engine_graph_builds(self.handle, ctypes.byref(a), ctypes.byref(b)))
+        return int(a.value), int(b.value)
+
     def member_substeps(self, member_id: int) -> int:
         """Substep count of the member's last enqueued (or first) large step."""
         n = ctypes.c_int(0)
@@ -1029,6 +1051,23 @@ class Engine:
     @property
     def lanes(self) -> int:
         return int(self.lib.nimbus_cuda_engine_lanes(self.handle))
+
+    def set_acoustic_form(self, form: int):
+        """ACOUSTIC_TABLE / ACOUSTIC_CONST / ACOUSTIC_MARCH kernels for the
+        continuity and momentum passes; results do not depend on it."""
+        self.ctx.check(self.lib.nimbus_cuda_engine_set_acoustic_form(self.handle, int(form)))
+
+    @property
+    def acoustic_form(self) -> int:
+        return int(self.lib.nimbus_cuda_engine_acoustic_form(self.handle))
+
+    def set_march(self, planes: int):
+        """Cells one thread of the marching acoustic passes advances along x."""
+        self.ctx.check(self.lib.nimbus_cuda_engine_set_march(self.handle, int(planes)))
+
+    @property
+    def march(self) -> int:
+        return int(self.lib.nimbus_cuda_engine_march(self.handle))
 
     def image_bytes(self) -> int:
         """Size of the state image (all members' nine fields in one block)."""

@@ -64,15 +64,37 @@ class Server:
     def serve(self, requests: list, prepared=None) -> tuple:
         """Serve a request stream in real time; returns (completions, makespan_s).
         `prepared` maps rid -> (state, base) to keep host-side set-up out of the
-        measured loop."""
+        measured loop (pinned arrays upload without blocking the loop).
+
+        Nothing here waits for the device except to learn a completion: the
+        engine admits with stream-ordered allocation and copies, retires with
+        a stream-ordered free, and rebuilds its step graphs in place; a
+        finished run's final state (when kept) is read asynchronously behind
+        its last step, and its completion is the moment the event recorded
+        there fires.  The engine itself stays at most about one step ahead of
+        the device (it reads each step's substep counts from the scan of the
+        state that step starts from)."""
+        import torch
+
         eng = self.run.engine
+        stream = torch.cuda.ExternalStream(eng.stream)
         pending = sorted(requests, key=lambda r: (r.arrival_s, r.rid))
         queue = []
-        active = {}  # member id -> [request, remaining steps, admitted_s]
+        active = {}     # member id -> [request, remaining steps, admitted_s]
+        finishing = []  # (request, admitted_s, event, kept state, member id)
         done = []
         t0 = time.perf_counter()
         now = lambda: time.perf_counter() - t0  # noqa: E731
-        while pending or queue or active:
+
+        def harvest(block=False):
+            while finishing and (block or finishing[0][2].query()):
+                r, admitted, ev, state, flags = finishing.pop(0)
+                ev.synchronize()
+                done.append(Completion(r.rid, r.arrival_s, admitted, now(), r.case.cells, r.steps, int(flags[0]),
+                                       state))
+                block = False
+
+        while pending or queue or active or finishing:
             t = now()
             while pending and pending[0].arrival_s <= t:
                 queue.append(pending.pop(0))
@@ -84,39 +106,44 @@ class Server:
                                         r.case.substeps, r.case.bc, base, resolve_substeps=True)
                 mid = eng.try_admit(desc, state, self.reserve)
                 if mid is None:
-                    if not active:
+                    if not active and not finishing:
                         raise RuntimeError(f"request {r.rid} does not fit an empty device")
                     break
                 queue.pop(0)
                 eng.shapes[mid] = r.case.shape
                 active[mid] = [r, r.steps, now()]
+            harvest()
             if not active:
-                if pending:
+                if finishing:
+                    harvest(block=True)
+                elif pending:
                     time.sleep(max(0.0, min(pending[0].arrival_s - now(), 0.05)))
                 continue
-            # Advance every resident run; take several steps at once when no
+            # Advance every resident run; several steps at once when no
             # arrival is due and no run finishes sooner.
             soonest = min(v[1] for v in active.values())
-            chunk = 1 if (queue or (pending and pending[0].arrival_s <= now() + 0.005)) else min(soonest,
-                                                                                                   self.max_chunk)
+            due = queue or (pending and pending[0].arrival_s <= now() + 0.005)
+            chunk = 1 if due else min(soonest, self.max_chunk)
             self.ctx.set_precision(self.run.precision)
             eng.step(chunk)
-            try:
-                eng.synchronize()
-                failed = set()
-            except cuda.NimbusCudaError:
-                failed = {mid for mid in active if eng.member_status(mid)}
-            t_done = now()
             for mid in list(active):
                 rec = active[mid]
                 rec[1] -= chunk
-                if rec[1] <= 0 or mid in failed:
+                if rec[1] <= 0:
                     r = rec[0]
-                    state = eng.read(mid) if self.keep else None
-                    status = eng.member_status(mid) if mid in failed else 0
+                    state = None
+                    if self.keep:
+                        state = {k: np.empty(r.case.shape, np.float32) for k in cuda.MEMBER_FIELDS}
+                        eng.read_async(mid, state)
+                    # the run's status bits (refused EOS projection, non-finite
+                    # flux) land in pinned memory behind its last step
+                    flags = torch.zeros(1, dtype=torch.int32).pin_memory().numpy().view(np.uint32)
+                    eng.member_status_async(mid, flags)
+                    ev = torch.cuda.Event()
+                    ev.record(stream)
                     eng.retire(mid)
                     del active[mid]
-                    done.append(Completion(r.rid, r.arrival_s, rec[2], t_done, r.case.cells, r.steps, status, state))
+                    finishing.append((r, rec[2], ev, state, flags))
         return done, now()
 
 
