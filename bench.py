@@ -22,6 +22,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -65,6 +66,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-single", action="store_true", help="skip the 250 m and 100 m single-run legs")
+    ap.add_argument("--no-autotune", action="store_true", help="keep --lanes and the default kernel form")
+    ap.add_argument("--scaling", choices=("weak", "strong"), default="weak",
+                    help="weak: each rank its own ensemble; strong: one ensemble split over the ranks")
     ap.add_argument("--no-error", action="store_true")
     ap.add_argument("--no-relaxation", action="store_true")
     ap.add_argument("--no-output", action="store_true")
@@ -81,11 +86,17 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
-def workload_cases(name, rank=0, members=64):
-    from nimbus_b200.ensemble import ensemble_cases
+def workload_cases(name, rank=0, members=64, world=1, strong=False):
+    """This rank's runs.  Weak scaling: every rank its own seeded ensemble.
+    Strong scaling: one ensemble, its members split over the ranks by the
+    greedy size-balanced placement (nimbus_b200.ensemble.shard)."""
+    from nimbus_b200.ensemble import ensemble_cases, shard
     from nimbus_b200.initial import benchmark_case
 
     if name == "ensemble_64":
+        if strong:
+            cases = ensemble_cases(members, seed=2026)
+            return [cases[i] for i in shard(cases, world, rank)]
         return ensemble_cases(members, seed=2026 + 1000 * rank)
     case = benchmark_case(name)
     case.member = rank
@@ -129,10 +140,58 @@ def reference_step_runner(case, threads):
     return step, kind, cores, n
 
 
+REF_CLI = ROOT / "oracle" / "_ref" / "nimbus_sim_ref"
+REF_CLI_TEMPLATE = ROOT / "oracle" / "configs" / "supercell_1km_64x64x40.yaml"
+
+
+def reference_cli_run(case, steps, warmup, threads):
+    """The reference solver's own command-line program (built from its sources
+    into oracle/_ref) run headless on the host cores, the stock CPU path: the
+    1 km supercell preset (oracle/configs/) with this run's grid, spacing, dt
+    and requested substeps, `warmup` untimed then `steps` timed large steps;
+    returns (avg_step_ms, acoustic substeps after the scheme's promotion, log
+    lines).  Its [PERF SUMMARY] times whole model steps excluding file output."""
+    import re
+
+    text = REF_CLI_TEMPLATE.read_text()
+    repl = {"nx": case.nx, "ny": case.ny, "nz": case.nz, "dx": case.dx, "dy": case.dy, "dz": case.dz,
+            "ztop": case.dz * case.nz, "dt_large": case.dt, "acoustic_substeps": max(case.substeps, 1),
+            "warmup_steps": warmup, "center_x_m": 0.5 * case.nx * case.dx, "center_y_m": 0.5 * case.ny * case.dy}
+    for key, val in repl.items():
+        text = re.sub(rf"^(\s*{key}:)\s*\S+", rf"\g<1> {val}", text, count=1, flags=re.M)
+    with tempfile.TemporaryDirectory() as tmp:
+        cfg = Path(tmp) / "run.yaml"
+        cfg.write_text(text)
+        out = Path(tmp) / "out"
+        out.mkdir()
+        cmd = [str(REF_CLI), "--config", str(cfg), "--headless", "--timing", "--threads", str(threads),
+               "--write-every=0", f"--outdir={out}", "--guard-mode", "sanitize",
+               "--duration", str(int(math.ceil(case.dt * (steps + warmup))))]
+        proc = subprocess.run(cmd, capture_output=True, text=True, cwd=tmp, timeout=1800)
+    log = proc.stdout + proc.stderr
+    m = re.search(r"\[PERF SUMMARY\].*?avg_step_ms=([0-9.eE+-]+)", log)
+    if proc.returncode != 0 or not m:
+        raise RuntimeError("reference CLI run failed: " + log[-400:])
+    promoted = re.search(r"promoting to (\d+)", log)
+    n = int(promoted.group(1)) if promoted else max(case.substeps, 1)
+    return float(m.group(1)), n, log
+
+
 def cpu_baseline(cases, budget_s=12.0):
+    """The reference's stock CPU path (its own program, all host threads) on
+    the workload's median run; the reference objects through the harness when
+    the program was not built."""
     mid = sorted(cases, key=lambda c: c.cells)[len(cases) // 2]
+    threads = os.cpu_count()
+    if REF_CLI.exists():
+        steps = 20
+        ms, n, _ = reference_cli_run(mid, steps, 5, threads)
+        return {"value": mid.cells / (ms / 1e3), "unit": METRIC, "cores": threads, "kind": "reference",
+                "sample": f"{steps} timed large steps (after 5 warm-up steps) of the workload's median run "
+                          f"({mid.nx}x{mid.ny}x{mid.nz}, N={n}) in the reference's own program, headless, "
+                          f"on {threads} host threads: {ms:.1f} ms per step"}
     sc = sample_case(mid)
-    step, kind, cores, n = reference_step_runner(sc, os.cpu_count())
+    step, kind, cores, n = reference_step_runner(sc, threads)
     step()  # warm-up
     t0 = time.perf_counter()
     steps = 0
@@ -149,32 +208,54 @@ def cpu_baseline(cases, budget_s=12.0):
 
 
 def run_reference_arm(args):
+    """The reference's own CPU implementation of the path on the host cores:
+    its stock command-line program (headless, --timing) on the workload's
+    median run, every host thread, args.warmup untimed then args.steps timed
+    large steps; beside it, the same grid through the reference objects the
+    parity harness drives (the hot path alone, without the runtime around it).
+    Without the built program the harness rate is the line's value."""
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
     cases = workload_cases(args.workload, 0, args.members)
     mid = sorted(cases, key=lambda c: c.cells)[len(cases) // 2]
+    threads = os.cpu_count()
+    # the hot path alone, through the reference's objects (bounded sample)
     sc = sample_case(mid)
-    step, kind, cores, n = reference_step_runner(sc, os.cpu_count())
-    for _ in range(args.warmup):
+    step, kind, cores, n = reference_step_runner(sc, threads)
+    for _ in range(min(args.warmup, 3)):
         step()
-    times = []
+    t0 = time.perf_counter()
     for _ in range(args.steps):
-        t0 = time.perf_counter()
         step()
-        times.append(time.perf_counter() - t0)
-    total = sum(times)
-    value = sc.cells * args.steps / total
+    harness_value = sc.cells * args.steps / (time.perf_counter() - t0)
+    harness = {"value": harness_value, "grid": [sc.nx, sc.ny, sc.nz], "acoustic_substeps": n, "cores": cores,
+               "path": "slow Heun, boundary refresh, acoustic loop, transport, Kessler, EOS from the reference "
+                       "solver's objects (oracle/_ref harness)"}
+    value, ms, grid, path, n_used = harness_value, 1e3 * sc.cells / harness_value, [sc.nx, sc.ny, sc.nz], \
+        harness["path"], n
+    sample = (f"each step: one large step of a {sc.nx}x{sc.ny}x{sc.nz} grid through the reference's objects "
+              f"(the workload's median run, capped at 96x96 columns)")
+    cli = None
+    if REF_CLI.exists():
+        ms, n_used, _ = reference_cli_run(mid, args.steps, max(args.warmup, 3), threads)
+        value, grid = mid.cells / (ms / 1e3), list(mid.shape)
+        path = ("the reference's stock CLI (nimbus_sim built from its sources), headless, --timing, "
+                "--guard-mode sanitize; [PERF SUMMARY] avg_step_ms after its warm-up steps")
+        sample = (f"{args.steps} timed large steps of the workload's median run ({mid.nx}x{mid.ny}x{mid.nz}, "
+                  f"dx {mid.dx:g} m, dt {mid.dt:g} s, N={n_used}) in the reference's own program")
+        cli = {"value": value, "avg_step_ms": ms, "grid": grid, "acoustic_substeps": n_used, "threads": threads}
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64 arithmetic, f32 storage",
-        "data": "synthetic (seeded WK82 supercell initial states)",
-        "config": {"workload": args.workload, "sample_grid": [sc.nx, sc.ny, sc.nz], "acoustic_substeps": n,
-                   "scalars": 4, "path": "full large step assembled from the reference CPU solver's objects"},
-        "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": kind,
-                         "sample": f"each step: one large step of a {sc.nx}x{sc.ny}x{sc.nz} grid (the workload's "
-                                   f"median run, capped at 96x96 columns)"},
+        "data": "synthetic (the reference's parametric supercell preset with this run's grid)" if cli else
+                "synthetic (seeded WK82 supercell initial states)",
+        "config": {"workload": args.workload, "sample_grid": grid, "acoustic_substeps": n_used, "scalars": 4,
+                   "path": path, "per_cell_rate": "cell-updates/s of one run: the ensemble's runs are independent "
+                   "and the reference advances one run per process", "reference_cli": cli,
+                   "reference_objects": harness},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -529,7 +610,8 @@ def run_ours(args):
             return float(t.item())
         return x
 
-    cases = workload_cases(args.workload, rank, args.members)
+    strong = args.scaling == "strong" and args.workload == "ensemble_64"
+    cases = workload_cases(args.workload, rank, args.members, world, strong)
     prepared = [initial_state(c) for c in cases]
     subs = [substeps_for(c, *p) for c, p in zip(cases, prepared)]
     cells = sum(c.cells for c in cases)
@@ -540,6 +622,13 @@ def run_ours(args):
     run = EngineRun(ctx, precision, lanes=args.lanes)
     for c, (st, base), n in zip(cases, prepared, subs):
         run.admit(c, st, base)  # substep count re-derived before every step
+    # The engine autotuner picks lanes and the acoustic kernel form on these
+    # runs (their states are restored afterwards); --lanes fixes the lanes.
+    tuned = None
+    if not args.no_autotune:
+        ctx.set_precision(precision)
+        tuned = run.engine.autotune(steps=2)
+    lanes_used = run.engine.lanes
     stream = torch.cuda.ExternalStream(run.engine.stream, device=f"cuda:{device}")
     for _ in range(max(args.warmup, 3)):
         run.step(1)
@@ -554,7 +643,11 @@ def run_ours(args):
     barrier()
     ms = max_over_ranks(ms)
     clock = clocks.summary()
-    total_cells = cells * world
+    if strong:  # the whole ensemble, whichever rank holds a member
+        from nimbus_b200.ensemble import ensemble_cases
+        total_cells = sum(c.cells for c in ensemble_cases(args.members, seed=2026))
+    else:
+        total_cells = cells * world
     value = total_cells * args.steps / (ms / 1e3)
     bytes_per_step = sum(c.cells * step_bytes(n) for c, n in zip(cases, subs))
 
@@ -568,7 +661,7 @@ def run_ours(args):
         run.step(1)
     timing = ctx.kernel_timing()
     ctx.set_kernel_timing(False)
-    run.engine.set_lanes(args.lanes)
+    run.engine.set_lanes(lanes_used)
     total_kernel_ms = sum(v[1] for v in timing.values())
     shares = {k: round(v[1] / total_kernel_ms, 4) for k, v in timing.items()} if total_kernel_ms else {}
     sub_ms = timing["acoustic_substep"][1] + timing["acoustic_momentum"][1]
@@ -603,9 +696,8 @@ def run_ours(args):
         pipe.step(args.e2e_steps)
         el = max_over_ranks(time.perf_counter() - t0)
         pipe.close()
-        io = cells * 4 * 9
-        e2e = {"value": total_cells * args.e2e_steps / el, "unit": METRIC, "h2d_bytes_per_step": io * world,
-               "d2h_bytes_per_step": io * world, "steps": args.e2e_steps,
+        e2e = {"value": total_cells * args.e2e_steps / el, "unit": METRIC, "h2d_bytes_per_step": total_cells * 4 * 9,
+               "d2h_bytes_per_step": total_cells * 4 * 9, "steps": args.e2e_steps,
                "api": "nimbus_cuda_engine_upload_image_async + nimbus_cuda_engine_step + "
                       "nimbus_cuda_engine_download_image_async, the runs split over "
                       f"{args.e2e_groups} engines on their own streams (each engine's nine prognostic fields of "
@@ -637,6 +729,7 @@ def run_ours(args):
         ctx.set_substep_form(cuda.SUBSTEP_AUTO)
 
     serving = None
+    single = None
     error = None
     cpu = None
     relaxation = None
@@ -652,6 +745,8 @@ def run_ours(args):
             ctx.set_precision(precision)
         if not args.no_serving:
             serving = serving_study(ctx, args, precision)
+        if not args.no_single:
+            single = single_run_study(ctx, args, precision)
         if not args.no_error:
             error = error_study(ctx, args.error_seconds)
         if not args.no_cpu_baseline:
@@ -664,7 +759,8 @@ def run_ours(args):
         nsub = sorted(set(subs))
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "strong" if strong else "weak",
             "vs_baseline": None,
             "dtype": "f32 (f64 only in the per-level base-state data and out-of-range EOS fallbacks)"
             if precision == cuda.PRECISION_FP32 else "f64 arithmetic, f32 storage",
@@ -677,9 +773,10 @@ def run_ours(args):
                 "acoustic_substeps": nsub, "scalars": 4,
                 "path": "full large step: slow Heun, boundary refresh + KW78 seed, N split substeps "
                         "(mass flux, continuity+EOS, momentum, boundaries), WENO5 transport, Kessler, EOS",
-                "form": f"batched member engine: the runs in {args.lanes} size-balanced lanes (parallel branches of "
+                "form": f"batched member engine: the runs in {lanes_used} size-balanced lanes (parallel branches of "
                         "one CUDA graph), one launch per phase per lane",
-                "lanes": args.lanes,
+                "lanes": lanes_used,
+                "autotune": tuned,
                 "precision": args.precision,
                 "precision_modes": {
                     args.precision: {"value": value, "ms_per_step": ms / args.steps},
@@ -687,11 +784,14 @@ def run_ours(args):
                         "value": total_cells * 1e3 / alt_ms if world == 1 else None, "ms_per_step": alt_ms}},
                 "plain": plain,
                 "serving": serving,
+                "single_runs": single,
                 "error_vs_fp64": error,
                 "state_relaxation": relaxation,
                 "output": output,
                 "smagorinsky_sgs": sgs,
-                "parallelism": f"{world} GPU(s), each with its own independent ensemble (no collective)",
+                "parallelism": (f"{world} GPU(s) sharing one {args.members}-member ensemble, members placed by "
+                                "size-balanced greedy partition (no data-path collective)") if strong else
+                               f"{world} GPU(s), each with its own independent ensemble (no collective)",
                 "l2": "inputs larger than L2 (%.1f GB resident per GPU)" % (cells * 4 * 40 / 1e9),
                 "algorithmic_bytes_per_step": bytes_per_step,
                 "effective_step_bandwidth_gbs": step_gbs},
@@ -713,6 +813,98 @@ def run_ours(args):
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+# Algorithmic bytes per cell of each kernel family's pass (see SUBSTEP_BYTES);
+# the acoustic pair's per substep.
+FAMILY_BYTES = {"acoustic": SUBSTEP_BYTES, "transport": 20 + 8 * 4, "slow": 112, "microphysics": 40 + 12}
+
+
+def single_run_study(ctx, args, precision):
+    """The single-run configurations: the 250 m supercell (256x256x80, dt
+    1.5 s, 8 substeps) and the 100 m supercell (512x512x128, dt 0.6 s, 10
+    substeps), each as one member of the engine (graph) and on the plain
+    per-operation path, with every kernel family's event-timed duration and
+    HBM rate (its algorithmic bytes over that duration, against the measured
+    copy rate).  The reference CPU solver runs one large step of the 250 m
+    grid on the host cores; the 100 m grid's CPU time is that rate scaled by
+    cells and algorithmic bytes per cell (labelled as an extrapolation)."""
+    import torch
+
+    from nimbus_b200 import cuda
+    from nimbus_b200.initial import benchmark_case, initial_state
+    from nimbus_b200.run import EngineRun, ResidentRun
+
+    peak, peak_kind = load_peaks()
+    out = {}
+    cpu_rate = None
+    for name in ("supercell_250m_256x256x80", "supercell_100m_512x512x128"):
+        case = benchmark_case(name)
+        st, base = initial_state(case)
+        run = EngineRun(ctx, precision)
+        mid = run.admit(case, st, base)
+        stream = torch.cuda.ExternalStream(run.engine.stream)
+        for _ in range(3):
+            run.step(1)
+        ctx.synchronize()
+        steps = max(3, min(args.steps, 10))
+        ms = time_on_stream(torch, stream, lambda: run.step(1), steps) / steps
+        n = run.substeps(mid)
+        ctx.set_kernel_timing(True)
+        for _ in range(steps):
+            run.step(1)
+        timing = ctx.kernel_timing()
+        ctx.set_kernel_timing(False)
+        run.close()
+        fam_ms = {k: v[1] / steps for k, v in timing.items() if v[1] > 0}
+        groups = {"acoustic": ("acoustic_substep", "acoustic_momentum"),
+                  "transport": ("transport_faces", "transport_limiter", "transport_update"),
+                  "slow": ("slow",), "microphysics": ("microphysics",)}
+        kernels = {}
+        for g, fams in groups.items():
+            t = sum(fam_ms.get(f, 0.0) for f in fams)
+            nbytes = case.cells * FAMILY_BYTES[g] * (n if g == "acoustic" else 1)
+            if t > 0:
+                gbs = nbytes / (t / 1e3) / 1e9
+                kernels[g] = {"ms_per_step": round(t, 4), "algorithmic_gb": round(nbytes / 1e9, 4),
+                              "achieved_gbs": round(gbs, 1), "frac": round(gbs / peak, 4)}
+        kernels["acoustic_boundary"] = {"ms_per_step": round(fam_ms.get("acoustic_boundary", 0.0), 4)}
+        # plain path: one C-ABI call per operation
+        ctx.set_substep_form(cuda.SUBSTEP_SPLIT)
+        plain = ResidentRun(ctx, case, {k: v.copy() for k, v in st.items()}, base, precision=precision,
+                            autotune=False)
+        plain.step()
+        ctx.synchronize()
+        cstream = torch.cuda.ExternalStream(ctx.stream)
+        p_ms = time_on_stream(torch, cstream, plain.step, steps) / steps
+        del plain
+        torch.cuda.empty_cache()
+        ctx.set_substep_form(cuda.SUBSTEP_AUTO)
+        bytes_step = case.cells * step_bytes(n)
+        entry = {"grid": list(case.shape), "dt_s": case.dt, "acoustic_substeps": n, "cells": case.cells,
+                 "engine": {"ms_per_step": round(ms, 4), "value": case.cells / (ms / 1e3), "unit": METRIC,
+                            "whole_step_gbs": round(bytes_step / (ms / 1e3) / 1e9, 1),
+                            "whole_step_frac": round(bytes_step / (ms / 1e3) / 1e9 / peak, 4)},
+                 "plain": {"ms_per_step": round(p_ms, 4), "value": case.cells / (p_ms / 1e3)},
+                 "kernels": kernels, "peak_gbs": peak, "peak_kind": peak_kind}
+        if not args.no_cpu_baseline:
+            if cpu_rate is None:
+                step, kind, cores, n_ref = reference_step_runner(case, os.cpu_count())
+                t0 = time.perf_counter()
+                step()
+                el = time.perf_counter() - t0
+                cpu_rate = (case.cells / el, kind, cores, el, case.cells * step_bytes(n_ref))
+                entry["cpu_reference"] = {"value": cpu_rate[0], "unit": METRIC, "kind": kind, "cores": cores,
+                                          "sample": f"one large step of this grid (N={n_ref}), {el:.1f} s"}
+            else:
+                rate, kind, cores, _, ref_bytes = cpu_rate
+                per_byte = rate * step_bytes(8) / step_bytes(n)
+                entry["cpu_reference"] = {"value": per_byte, "unit": METRIC, "kind": kind, "cores": cores,
+                                          "sample": "extrapolated from the 250 m grid's measured step: that "
+                                                    "rate scaled by algorithmic bytes per cell (N=8 there, "
+                                                    f"N={n} here); not run on this grid"}
+        out[name] = entry
+    return out
 
 
 def serving_study(ctx, args, precision):

@@ -211,7 +211,10 @@ nimbus_status nimbus_cuda_acoustic_fused(nimbus_cuda_context* ctx, const nimbus_
  * other entry point may grow the context workspace; this one allocates
  * nothing and needs no context.
  *
- * Same arithmetic and results as nimbus_cuda_acoustic_fused.  Requirements:
+ * It always computes in reference precision (FP64 interior arithmetic on
+ * FP32 storage): its results equal nimbus_cuda_acoustic_fused's for a context
+ * in NIMBUS_PRECISION_REFERENCE, bit for bit; the FP32 form is not offered
+ * here.  Requirements:
  *   - memory == NIMBUS_MEMORY_DEVICE: every field pointer is device memory on
  *     the current device; the substep is enqueued on `stream` (NULL = the
  *     default stream) and the call returns without synchronising;
@@ -225,6 +228,10 @@ nimbus_status nimbus_cuda_acoustic_fused(nimbus_cuda_context* ctx, const nimbus_
  * threads on the same device) race and must be serialised by the caller.
  * Each call overwrites the whole scratch range it reads, so no clearing is
  * needed between calls.
+ * Errors: an error left by earlier work of the process is cleared, not
+ * reported; NIMBUS_ERR_CUDA from a launch means nothing was enqueued after
+ * it; if the final copy of the new density fails, p, u, v and w are already
+ * advanced while rho still holds its old values.
  */
 #define NIMBUS_STATIC_SCRATCH_CELLS 4194304
 nimbus_status nimbus_cuda_acoustic_fused_static_scratch(const nimbus_acoustic_fused_args* a);
@@ -765,6 +772,9 @@ nimbus_status nimbus_history_write(const float* host_image, unsigned fields, int
  *   substeps (retained mass flux, continuity + EOS, momentum, boundaries);
  *   conservative WENO5 transport of theta, qv, qc, qr; Kessler tendencies and
  *   their application (microphysics == 1); EOS pressure re-projection.
+ * Several engines may share one context, and each may be driven from its own
+ * host thread (one thread per engine at a time): an engine's step waits only
+ * for its own acoustic speed scans.
  * Members may differ in grid, spacing, dt and substep count.  With Kessler
  * on, dt must not exceed 0.8 dz / (20 m/s), the bound under which the
  * reference runs the microphysics in one call instead of subcycling it.
@@ -907,6 +917,28 @@ nimbus_status nimbus_cuda_engine_set_acoustic_form(nimbus_engine* e, int form);
 int nimbus_cuda_engine_acoustic_form(const nimbus_engine* e);
 nimbus_status nimbus_cuda_engine_set_march(nimbus_engine* e, int planes);
 int nimbus_cuda_engine_march(const nimbus_engine* e);
+
+/* The engine autotuner (no counterpart in the reference).  Times candidate
+ * launch configurations -- lanes {1, 2, 4, 6, 8} (at most the member count) x
+ * acoustic kernel form {constant-bank, member-table, marching 16 planes} --
+ * on the resident members themselves, `steps` timed steps each after one
+ * warm-up step, keeps the fastest and reports every candidate's time.  The
+ * members' states are saved on the device before and restored after, so the
+ * runs are where they were (status words and substep counts may reflect the
+ * tuning steps).  Waits for the device. */
+#define NIMBUS_TUNING_CANDIDATES 16
+typedef struct nimbus_engine_tuning
+{
+    int lanes, acoustic_form, march;  /* the chosen configuration (now set) */
+    double ms_per_step;               /* its time */
+    int candidates;
+    int candidate_lanes[NIMBUS_TUNING_CANDIDATES];
+    int candidate_form[NIMBUS_TUNING_CANDIDATES];
+    int candidate_march[NIMBUS_TUNING_CANDIDATES];
+    double candidate_ms[NIMBUS_TUNING_CANDIDATES];
+} nimbus_engine_tuning;
+
+nimbus_status nimbus_cuda_engine_autotune(nimbus_engine* e, int steps, nimbus_engine_tuning* out);
 /* Enqueues n_steps large steps of every resident member on the engine's
  * stream: replayed from a CUDA graph when graphs are on (the default), the
  * graph rebuilt after admissions, retirements, a precision change or a

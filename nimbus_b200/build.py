@@ -39,16 +39,24 @@ def sources():
     return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cuh")) + [PKG.parent / "include" / "nimbus_cuda.h"]
 
 
-# The reference's headers, for the ComputeBackend adapter (built when present).
-REFERENCE = Path(os.environ.get("NIMBUS_REFERENCE_ROOT", "/root/reference"))
+# The reference solver's source tree (its headers, for the ComputeBackend
+# adapter): the directory NIMBUS_REFERENCE_DIR names; the adapter is skipped
+# without it.
 ADAPTER = PKG / "reference_backend" / "nimbus_compute_backend.cpp"
+
+
+def reference_dir() -> Path | None:
+    value = os.environ.get("NIMBUS_REFERENCE_DIR")
+    return Path(value) if value else None
 
 
 def build_reference_backend(force: bool = False) -> Path | None:
     """nimbus_b200/lib/libnimbus_reference_backend.so: the CUDA backend as a
     ComputeBackend of the reference solver, compiled against its headers and
-    linked to libnimbus_cuda.so.  Skipped (None) without the reference tree."""
-    if not (REFERENCE / "include" / "compute" / "backend_interface.hpp").exists():
+    linked to libnimbus_cuda.so.  Skipped (None) without the reference tree
+    (NIMBUS_REFERENCE_DIR)."""
+    REFERENCE = reference_dir()
+    if REFERENCE is None or not (REFERENCE / "include" / "compute" / "backend_interface.hpp").exists():
         return None
     out = LIB / "libnimbus_reference_backend.so"
     cuda_lib = LIB / "libnimbus_cuda.so"

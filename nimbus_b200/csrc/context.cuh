@@ -6,6 +6,7 @@
 #include "../../include/nimbus_cuda.h"
 #include "transport_kernels.cuh"
 
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <limits>
@@ -62,7 +63,7 @@ struct nimbus_cuda_context
     int sm_count = 148;
     cudaStream_t stream = nullptr;
     unsigned* status = nullptr;  // device status word
-    uint64_t launches = 0;
+    std::atomic<uint64_t> launches{0};  // engines of this context may step from their own host threads
     std::string error;
     nimbus_host::DeviceBuffer ws[nimbus_host::kSlotCount];
 };

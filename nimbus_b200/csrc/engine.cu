@@ -616,15 +616,15 @@ nimbus_status prepare_image(nimbus_engine* e, size_t* bytes)
     return NIMBUS_OK;
 }
 
-void launch_image(nimbus_engine* e, int gather)
+void launch_image(nimbus_engine* e, int gather, float* image = nullptr)
 {
     for (const Lane& L : e->lanes)
     {
         const long long tiles = tiles_of(e, L, kItemCells, L.members);
         if (tiles <= 0) continue;
         engine_image_kernel<<<engine_grid(e, reinterpret_cast<const void*>(engine_image_kernel), tiles), kEngineBlock,
-                              0, e->stream>>>(e->d_table + L.first, prefix_of(e, L, kItemCells), tiles, e->d_image,
-                                              gather);
+                              0, e->stream>>>(e->d_table + L.first, prefix_of(e, L, kItemCells), tiles,
+                                              image ? image : e->d_image, gather);
         e->ctx->launches += 1;
     }
 }
@@ -1049,6 +1049,106 @@ nimbus_status nimbus_cuda_engine_graph_builds(const nimbus_engine* e, uint64_t* 
     if (!e || !instantiations || !updates) return NIMBUS_ERR_INVALID_ARGUMENT;
     *instantiations = e->graph_instantiations;
     *updates = e->graph_updates;
+    return NIMBUS_OK;
+}
+
+// The engine autotuner: times candidate launch configurations on the
+// resident members themselves and keeps the fastest.  The members' states are
+// saved before (a device copy through the state-image kernel) and restored
+// after, so tuning leaves every run where it was.
+nimbus_status nimbus_cuda_engine_autotune(nimbus_engine* e, int steps, nimbus_engine_tuning* out)
+{
+    if (!e || !out || steps < 1 || steps > 100) return NIMBUS_ERR_INVALID_ARGUMENT;
+    nimbus_cuda_context* ctx = e->ctx;
+    NB_CUDA(ctx, cudaSetDevice(ctx->device));
+    *out = nimbus_engine_tuning{};
+    if (e->dirty) NB_TRY(rebuild_table(e));
+    if (e->slots.empty())
+    {
+        out->lanes = e->lane_target;
+        out->acoustic_form = e->acoustic_form;
+        out->march = e->march_len;
+        return NIMBUS_OK;
+    }
+    const size_t bytes = image_bytes_of(e);
+    float* backup = nullptr;
+    NB_CUDA(ctx, cudaMallocAsync(reinterpret_cast<void**>(&backup), bytes, e->stream));
+    launch_image(e, 1, backup);  // save
+    struct Candidate
+    {
+        int lanes, form, march;
+    };
+    std::vector<Candidate> cands;
+    const int members = static_cast<int>(e->slots.size());
+    for (int lanes : {1, 2, 4, 6, 8})
+    {
+        if (lanes > members && lanes != 1) continue;
+        cands.push_back({lanes, NIMBUS_ACOUSTIC_CONST, e->march_len});
+        cands.push_back({lanes, NIMBUS_ACOUSTIC_TABLE, e->march_len});
+        cands.push_back({lanes, NIMBUS_ACOUSTIC_MARCH, 16});
+    }
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    NB_CUDA(ctx, cudaEventCreate(&t0));
+    NB_CUDA(ctx, cudaEventCreate(&t1));
+    const int saved_lanes = e->lane_target, saved_form = e->acoustic_form, saved_march = e->march_len;
+    double best = 1e300;
+    Candidate chosen{saved_lanes, saved_form, saved_march};
+    nimbus_status status = NIMBUS_OK;
+    int n = 0;
+    for (const Candidate& c : cands)
+    {
+        e->lane_target = c.lanes;
+        e->acoustic_form = c.form;
+        e->march_len = c.march;
+        e->dirty = true;
+        status = nimbus_cuda_engine_step(e, 1);  // builds the table and graphs, warms up
+        if (status != NIMBUS_OK) break;
+        cudaEventRecord(t0, e->stream);
+        status = nimbus_cuda_engine_step(e, steps);
+        if (status != NIMBUS_OK) break;
+        cudaEventRecord(t1, e->stream);
+        if (cudaEventSynchronize(t1) != cudaSuccess)
+        {
+            status = cuda_fail(ctx, cudaGetLastError(), "autotune timing");
+            break;
+        }
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, t0, t1);
+        const double per_step = ms / steps;
+        if (n < NIMBUS_TUNING_CANDIDATES)
+        {
+            out->candidate_lanes[n] = c.lanes;
+            out->candidate_form[n] = c.form;
+            out->candidate_march[n] = c.march;
+            out->candidate_ms[n] = per_step;
+            ++n;
+        }
+        if (per_step < best)
+        {
+            best = per_step;
+            chosen = c;
+        }
+        // Restore the saved states for the next candidate (rows may have
+        // moved with the lane split: the image follows admission order).
+        launch_image(e, 0, backup);
+    }
+    out->candidates = n;
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    e->lane_target = status == NIMBUS_OK ? chosen.lanes : saved_lanes;
+    e->acoustic_form = status == NIMBUS_OK ? chosen.form : saved_form;
+    e->march_len = status == NIMBUS_OK ? chosen.march : saved_march;
+    e->dirty = true;
+    NB_TRY(rebuild_table(e));
+    launch_image(e, 0, backup);  // every run back to its state before tuning
+    e->scan_pending = false;     // the state changed
+    NB_CUDA(ctx, cudaFreeAsync(backup, e->stream));
+    NB_CUDA(ctx, cudaStreamSynchronize(e->stream));
+    NB_TRY(status);
+    out->lanes = e->lane_target;
+    out->acoustic_form = e->acoustic_form;
+    out->march = e->march_len;
+    out->ms_per_step = best;
     return NIMBUS_OK;
 }
 

@@ -682,7 +682,7 @@ void nimbus_cuda_destroy(nimbus_cuda_context* ctx)
 }
 
 const char* nimbus_cuda_last_error(const nimbus_cuda_context* ctx) { return ctx ? ctx->error.c_str() : "null context"; }
-uint64_t nimbus_cuda_kernel_launches(const nimbus_cuda_context* ctx) { return ctx ? ctx->launches : 0; }
+uint64_t nimbus_cuda_kernel_launches(const nimbus_cuda_context* ctx) { return ctx ? ctx->launches.load() : 0; }
 void* nimbus_cuda_stream(const nimbus_cuda_context* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
 
 nimbus_status nimbus_cuda_synchronize(nimbus_cuda_context* ctx)
@@ -1281,13 +1281,21 @@ extern "C" nimbus_status nimbus_cuda_acoustic_fused_static_scratch(const nimbus_
         std::lock_guard<std::mutex> lock(g_static_scratch_mutex);
         if (!g_static_scratch_ptr[dev])
         {
-            // Set-up, once per device, with that device current.
+            // Set-up, once per device, with that device current.  A failed
+            // set-up clears the error it raised, so that a later call of any
+            // entry point does not report it as its own.
             void* ptr = nullptr;
             if (cudaGetSymbolAddress(&ptr, g_static_rho_scratch) != cudaSuccess || ptr == nullptr)
+            {
+                (void)cudaGetLastError();
                 return NIMBUS_ERR_CUDA;
+            }
             int count = 0;
             if (cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || count <= 0)
+            {
+                (void)cudaGetLastError();
                 return NIMBUS_ERR_CUDA;
+            }
             g_static_scratch_ptr[dev] = static_cast<float*>(ptr);
             g_static_scratch_sms[dev] = count;
         }
@@ -1301,14 +1309,20 @@ extern "C" nimbus_status nimbus_cuda_acoustic_fused_static_scratch(const nimbus_
     cudaStream_t st = static_cast<cudaStream_t>(a->stream);
     long long blocks = (cells + kThreads - 1) / kThreads;
     if (blocks > static_cast<long long>(sms) * 16) blocks = static_cast<long long>(sms) * 16;
+    // An error left by earlier, unrelated work of the process is not this
+    // call's failure: drop it before the first launch, then check each step.
+    (void)cudaGetLastError();
     acoustic_continuity_eos_kernel<<<static_cast<int>(blocks), kThreads, 0, st>>>(
         P, a->rho, a->u, a->v, a->w, a->theta, a->rho0_base, scratch, a->p, a->drho_scratch, nullptr, nullptr,
         nullptr, nullptr);
+    if (cudaGetLastError() != cudaSuccess) return NIMBUS_ERR_CUDA;
     acoustic_momentum_kernel<<<static_cast<int>(blocks), kThreads, 0, st>>>(P, scratch, a->p, a->p0_base, a->u,
                                                                              a->v, a->w);
+    if (cudaGetLastError() != cudaSuccess) return NIMBUS_ERR_CUDA;
+    // A failure from here on leaves p, u, v, w already advanced while rho
+    // keeps its old values (the new density is still in the scratch array).
     if (cudaMemcpyAsync(a->rho, scratch, sizeof(float) * static_cast<size_t>(cells), cudaMemcpyDeviceToDevice, st) !=
         cudaSuccess)
         return NIMBUS_ERR_CUDA;
-    if (cudaGetLastError() != cudaSuccess) return NIMBUS_ERR_CUDA;
     return NIMBUS_OK;
 }

@@ -54,6 +54,8 @@ nimbus_status stage_tables(nimbus_cuda_context* ctx, cudaStream_t st, const doub
     std::vector<float> inv(2 * nz, 0.0f);
     for (size_t k = 0; k < nz; ++k) inv[k] = static_cast<float>(1.0 / dz[k]);
     for (size_t k = 0; k + 1 < nz; ++k) inv[nz + k] = static_cast<float>(1.0 / (0.5 * (dz[k] + dz[k + 1])));
+    // No centre above the top level: a use of DZC(nz - 1) shows up as NaN.
+    inv[2 * nz - 1] = std::numeric_limits<float>::quiet_NaN();
     NB_CUDA(ctx, cudaMemcpyAsync(dev, dz, nz * sizeof(double), cudaMemcpyHostToDevice, st));
     NB_CUDA(ctx, cudaMemcpyAsync(dev + nz, delta.data(), nz * sizeof(double), cudaMemcpyHostToDevice, st));
     float* inv_dev = reinterpret_cast<float*>(dev + 2 * nz);

@@ -91,7 +91,9 @@ struct SgsAt
     __device__ __forceinline__ Recip<R> DY() const { return {P.dy, P.inv_dy_f}; }
     __device__ __forceinline__ Recip<R> DZ(int k) const { return {P.dz[k], P.inv_dz_f[k]}; }
     // Distance between centres k and k+1 as a divisor (the reference form
-    // divides by 0.5 (dz_k + dz_k+1)).
+    // divides by 0.5 (dz_k + dz_k+1)).  Defined for k < nz - 1 only: every
+    // caller guards that; the FP32 table holds NaN at nz - 1 and dz has no
+    // element nz.
     __device__ __forceinline__ Recip<R> DZC(int k) const { return {0.5 * (P.dz[k] + P.dz[k + 1]), P.inv_dzc_f[k]}; }
     __device__ __forceinline__ R dzc(int k) const { return R(0.5) * (R(P.dz[k]) + R(P.dz[k + 1])); }
     // mu = rho nu at a centre; on an xy edge (four-point mean); on an xz or yz

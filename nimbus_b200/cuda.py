@@ -169,6 +169,15 @@ class MemberDesc(ctypes.Structure):
     ]
 
 
+class EngineTuning(ctypes.Structure):
+    _fields_ = [
+        ("lanes", ctypes.c_int), ("acoustic_form", ctypes.c_int), ("march", ctypes.c_int),
+        ("ms_per_step", ctypes.c_double), ("candidates", ctypes.c_int),
+        ("candidate_lanes", ctypes.c_int * 16), ("candidate_form", ctypes.c_int * 16),
+        ("candidate_march", ctypes.c_int * 16), ("candidate_ms", ctypes.c_double * 16),
+    ]
+
+
 class SoundSpeedArgs(ctypes.Structure):
     _fields_ = [
         ("p", _fp), ("rho", _fp), ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
@@ -256,7 +265,9 @@ EXPORTED_SYMBOLS = (
     "nimbus_cuda_max_sound_speed", "nimbus_cuda_resolve_substep_count",
     "nimbus_cuda_engine_set_march", "nimbus_cuda_engine_march", "nimbus_cuda_engine_set_acoustic_form",
     "nimbus_cuda_engine_acoustic_form", "nimbus_cuda_engine_member_status_async", "nimbus_cuda_engine_graph_builds",
+    "nimbus_cuda_engine_autotune",
 )
+ACOUSTIC_FORM_NAMES = {0: "member-table", 1: "constant-bank", 2: "marching"}
 ACOUSTIC_TABLE, ACOUSTIC_CONST, ACOUSTIC_MARCH = 0, 1, 2
 SUBSTEP_AUTO, SUBSTEP_FUSED, SUBSTEP_SPLIT = 0, 1, 2
 PRECISION_REFERENCE, PRECISION_FP32 = 0, 1
@@ -357,6 +368,7 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
     lib.nimbus_cuda_engine_march.argtypes = [vp]
     lib.nimbus_cuda_engine_set_acoustic_form.argtypes = [vp, ctypes.c_int]
     lib.nimbus_cuda_engine_member_status_async.argtypes = [vp, ctypes.c_int, ctypes.c_void_p]
+    lib.nimbus_cuda_engine_autotune.argtypes = [vp, ctypes.c_int, ctypes.POINTER(EngineTuning)]
     lib.nimbus_cuda_engine_graph_builds.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64),
                                                     ctypes.POINTER(ctypes.c_uint64)]
     lib.nimbus_cuda_engine_acoustic_form.argtypes = [vp]
@@ -983,6 +995,18 @@ class Engine:
         uint32 array of one element), in stream order."""
         self.ctx.check(self.lib.nimbus_cuda_engine_member_status_async(self.handle, int(member_id),
                                                                       ctypes.c_void_p(host_flags.ctypes.data)))
+
+    def autotune(self, steps: int = 3) -> dict:
+        """Time lanes x acoustic kernel form on the resident members (states
+        restored afterwards), keep the fastest; returns the choice and every
+        candidate's ms per step."""
+        t = EngineTuning()
+        self.ctx.check(self.lib.nimbus_cuda_engine_autotune(self.handle, int(steps), ctypes.byref(t)))
+        cands = [{"lanes": t.candidate_lanes[i], "form": ACOUSTIC_FORM_NAMES[t.candidate_form[i]],
+                  "march": t.candidate_march[i], "ms_per_step": round(t.candidate_ms[i], 4)}
+                 for i in range(t.candidates)]
+        return {"lanes": t.lanes, "acoustic_form": ACOUSTIC_FORM_NAMES[t.acoustic_form], "march": t.march,
+                "ms_per_step": round(t.ms_per_step, 4), "steps_per_candidate": int(steps), "candidates": cands}
 
     def graph_builds(self) -> tuple:
         """(instantiations, in-place updates) of the step graphs so far."""

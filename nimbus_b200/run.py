@@ -243,6 +243,7 @@ class HostPipeline:
                 arrays[k][...] = st[k]
             self.host.append((run, mid, arrays))
         self.cells = sum(c.cells for c in cases)
+        self._pool = None
 
     def bytes_per_step(self):
         """Host<->device bytes one step moves (the nine prognostic fields each way)."""
@@ -253,20 +254,31 @@ class HostPipeline:
         """n large steps, each uploading every state, advancing it and reading it
         back; each engine's stream orders step k's download before step k+1's
         upload of the same host block, so consecutive steps of different groups
-        overlap.  Waits for all of them before returning."""
+        overlap.  Each group is driven from its own host thread: a step waits
+        for its group's acoustic speed scan (the substep counts depend on the
+        uploaded state), and the other groups keep enqueuing meanwhile (the
+        library calls release the interpreter lock).  Waits for all of them
+        before returning."""
+        from concurrent.futures import ThreadPoolExecutor
+
         self.ctx.set_precision(self.precision)
-        for _ in range(n):
-            # Every group's upload first: a step waits for its group's
-            # acoustic speed scan (the substep counts depend on the uploaded
-            # state), and the other groups' copies proceed meanwhile.
-            for run, image in zip(self.runs, self.images):
+
+        def drive(pair):
+            run, image = pair
+            for _ in range(n):
                 run.engine.upload_image_async(image)
-            for run, image in zip(self.runs, self.images):
                 run.engine.step(1)
                 run.engine.download_image_async(image)
-        for run in self.runs:
             run.engine.synchronize()
 
+        if self._pool is None:
+            self._pool = ThreadPoolExecutor(max_workers=len(self.runs))
+        for f in [self._pool.submit(drive, pair) for pair in zip(self.runs, self.images)]:
+            f.result()
+
     def close(self):
+        if self._pool is not None:
+            self._pool.shutdown()
+            self._pool = None
         for run in self.runs:
             run.close()

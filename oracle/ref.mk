@@ -6,10 +6,15 @@
 #
 #   make -f oracle/ref.mk REF=/path/to/reference -j8
 #
+# REF is required (the build recipe passes NIMBUS_REFERENCE_DIR).
+#
 # Portability: no -march=native (the archive must run on any x86-64 host the
 # library travels to) and -ffp-contract=off (no FMA contraction), so the
 # reference's arithmetic is the plain IEEE sequence its sources spell out.
-REF      ?= /root/reference
+REF      ?= $(NIMBUS_REFERENCE_DIR)
+ifeq ($(strip $(REF)),)
+$(error REF (or NIMBUS_REFERENCE_DIR) must name the reference solver's source tree)
+endif
 OUT      ?= oracle/_ref
 OBJDIR   := $(OUT)/obj
 CXX      ?= g++
@@ -45,3 +50,13 @@ $(OUT)/libnimbus_ref_harness.so: oracle/ref_harness.cpp $(OUT)/libnimbus_ref.a
 	$(CXX) -shared $(OUT)/ref_harness.o -o $@ $(OUT)/libnimbus_ref.a $(GOMP_LIBS) -Wl,--no-undefined
 
 .PHONY: harness
+
+# The reference's command-line program from the same objects (its main() is
+# compiled as nimbus_reference_cli_main): the stock CPU path bench.py times.
+cli: $(OUT)/nimbus_sim_ref
+
+$(OUT)/nimbus_sim_ref: oracle/ref_cli.cpp $(OUT)/libnimbus_ref.a
+	$(CXX) -std=c++17 -O2 -c oracle/ref_cli.cpp -o $(OUT)/ref_cli.o
+	$(CXX) $(OUT)/ref_cli.o -o $@ -Wl,--whole-archive $(OUT)/libnimbus_ref.a -Wl,--no-whole-archive $(GOMP_LIBS)
+
+.PHONY: cli

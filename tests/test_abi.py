@@ -62,6 +62,7 @@ def _c_layout(struct_name, fields, tmp_path):
     ("nimbus_sgs_step_args", cuda.SgsStepArgs),
     ("nimbus_history_args", cuda.HistoryArgs),
     ("nimbus_member_desc", cuda.MemberDesc),
+    ("nimbus_engine_tuning", cuda.EngineTuning),
     ("nimbus_member_state", cuda.MemberState),
 ])
 def test_argument_block_layout_matches_header(struct_name, cls, tmp_path):

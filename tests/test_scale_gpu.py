@@ -290,3 +290,21 @@ def test_engine_substep_counts_of_closing_members(ctx, o32):
     for k in PROGNOSTIC:
         assert_bitwise(got_c[k], ref_c[k], f"closing {k}")
         assert_bitwise(got_p[k], ref_p[k], f"plain {k}")
+
+
+def test_engine_autotune_restores_states_and_keeps_results(ctx, multi_tile):
+    """The autotuner steps the resident members under every candidate
+    configuration, restores their states, and leaves the fastest
+    configuration set; the runs then continue exactly as an untuned engine's."""
+    members, want = multi_tile
+    run = EngineRun(ctx, precision=cuda.PRECISION_REFERENCE)
+    ids = [run.admit(case, st, base, coriolis_f=1e-4) for case, st, base in members[:5]]
+    tuned = run.engine.autotune(steps=1)
+    assert tuned["candidates"] and tuned["ms_per_step"] == min(c["ms_per_step"] for c in tuned["candidates"])
+    assert run.engine.lanes == min(tuned["lanes"], 5)
+    run.step(2)
+    for mid, (case, _, _), (ref, _) in zip(ids, members, want):
+        got = run.read(mid)
+        for k in PROGNOSTIC:
+            assert_bitwise(got[k], ref[k], f"after autotune member {mid} {k}")
+    run.close()

@@ -90,3 +90,77 @@ def test_two_ranks_agree_on_the_placement():
     assert sorted(sizes[0] + sizes[1]) == list(range(16)) and not set(sizes[0]) & set(sizes[1])
     works = _works(ensemble_cases(16, seed=5))
     assert slowest == max(sum(works[i] for i in sizes[r]) for r in range(2))
+
+
+def _small_ensemble():
+    """Six small supercells of different grids (the ensemble's generator at
+    a reduced size), for stepping on the CPU oracle."""
+    from nimbus_b200.initial import Case
+    rng = np.random.default_rng(12)
+    out = []
+    for m in range(6):
+        n = int(rng.integers(10, 17))
+        nz = int(rng.integers(8, 13))
+        out.append(Case(n, n + m % 2, nz, 1000.0, 1000.0, 8000.0 / nz, 5.0, bubble_rh=4000.0, noise_amp=0.2,
+                        seed=3, member=m, bubble_amp=float(rng.uniform(2, 4))))
+    return out
+
+
+def _advance(cases, indices, steps=2):
+    """Advance the members `indices` with the oracle, substep counts
+    re-derived before every step; returns {index: state}."""
+    import oracle
+    from nimbus_b200.initial import initial_state
+    o = oracle.Restatement("f32")
+    out = {}
+    for i in indices:
+        c = cases[i]
+        st, base = initial_state(c)
+        o.run(st, base, (c.dx, c.dy, c.dz), c.dt, steps, c.bc)
+        out[i] = st
+    return out
+
+
+def _shard_main(rank, world, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    cases = _small_ensemble()
+    works = [member_work(c, 6) for c in cases]
+    mine = shard(cases, world, rank, works)
+    states = _advance(cases, mine)
+    gathered = [None] * world
+    dist.all_gather_object(gathered, states)
+    if rank == 0:
+        merged = {}
+        for part in gathered:
+            merged.update(part)
+        out.put(merged)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.skipif(not __import__("oracle").restatement_available(), reason="oracle restatement not built")
+def test_sharded_ensemble_equals_single_rank_run():
+    """Strong scaling's data path: each of two gloo ranks advances only the
+    members the size-balanced placement gives it; the gathered states equal a
+    single-rank run of the whole ensemble bit for bit (members share nothing,
+    so no collective exists on the data path)."""
+    import socket
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    procs = [ctx.Process(target=_shard_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    merged = q.get(timeout=300)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    cases = _small_ensemble()
+    assert sorted(merged) == list(range(len(cases)))
+    alone = _advance(cases, range(len(cases)))
+    for i in range(len(cases)):
+        for k, a in alone[i].items():
+            assert np.array_equal(a.view(np.uint32), merged[i][k].view(np.uint32)), (i, k)

@@ -63,6 +63,36 @@ def test_static_scratch_substeps_match_allocating_entry_point():
     ctx.close()
 
 
+def test_static_scratch_at_capacity_matches_allocating_entry_point():
+    """A grid of exactly NIMBUS_STATIC_SCRATCH_CELLS cells (256x256x64) is
+    accepted, and its grid-stride launch (capped at 16 blocks per SM) gives
+    the allocating entry point's bits."""
+    import torch
+
+    lib = cuda.load_library()
+    case = Case(256, 256, 64, 500.0, 500.0, 300.0, 3.0, seed=4)
+    assert case.cells == cuda.STATIC_SCRATCH_CELLS
+    st, base = perturbed_state(case, seed=5)
+    rho0 = torch.from_numpy(base["rho0"]).cuda()
+    p0 = torch.from_numpy(base["p0"]).cuda()
+    grid = (case.dx, case.dy, case.dz)
+    ctx = cuda.Context(0)
+    ctx.set_precision(cuda.PRECISION_REFERENCE)
+    want = _device_state(torch, st)
+    got = _device_state(torch, st)
+    torch.cuda.synchronize()
+    for _ in range(2):
+        ctx.check(ctx.acoustic_fused(cuda.fused_args(want, rho0, p0, 0.3, grid, memory=cuda.MEMORY_DEVICE)))
+        ctx.synchronize()
+        b = cuda.fused_args(got, rho0, p0, 0.3, grid, memory=cuda.MEMORY_DEVICE)
+        rc = lib.nimbus_cuda_acoustic_fused_static_scratch(ctypes.byref(b))
+        assert rc == 0, cuda.STATUS_NAMES.get(rc, rc)
+        torch.cuda.synchronize()
+    for k in FIELDS:
+        assert torch.equal(want[k].view(torch.int32), got[k].view(torch.int32)), k
+    ctx.close()
+
+
 def test_static_scratch_refuses_grids_beyond_capacity():
     import torch
 
@@ -77,6 +107,13 @@ def test_static_scratch_refuses_grids_beyond_capacity():
     a.nx, a.ny, a.nz, a.base_len = 1024, 1024, 8, 64
     assert 1024 * 1024 * 8 > cuda.STATIC_SCRATCH_CELLS
     assert lib.nimbus_cuda_acoustic_fused_static_scratch(ctypes.byref(a)) == 7  # NIMBUS_ERR_TOO_LARGE
+    # One cell beyond the capacity (5 x 397 x 2113 = 4,194,305) is refused too.
+    rho0_long = torch.from_numpy(np.resize(base["rho0"], 2113)).cuda()
+    p0_long = torch.from_numpy(np.resize(base["p0"], 2113)).cuda()
+    c = cuda.fused_args(dev, rho0_long, p0_long, 0.5, (1000.0, 1000.0, 500.0), memory=cuda.MEMORY_DEVICE)
+    c.nx, c.ny, c.nz, c.base_len = 5, 397, 2113, 2113
+    assert 5 * 397 * 2113 == cuda.STATIC_SCRATCH_CELLS + 1
+    assert lib.nimbus_cuda_acoustic_fused_static_scratch(ctypes.byref(c)) == 7
     # Host memory is not accepted either: the entry point never stages.
     host = {k: np.ascontiguousarray(st[k]) for k in FIELDS}
     h = cuda.fused_args(host, base["rho0"], base["p0"], 0.5, (1000.0, 1000.0, 500.0))
