@@ -383,6 +383,36 @@ typedef struct nimbus_slow_args
 } nimbus_slow_args;
 
 nimbus_status nimbus_cuda_slow_tendencies(nimbus_cuda_context* ctx, const nimbus_slow_args* a);
+
+/*
+ * The slow tendencies applied over the large step.  Replaces
+ * DynamicsComputeKernels::dispatch_slow_apply (include/compute/dispatch/
+ * dynamics.hpp:328-352,760) with the CPU semantics of apply_slow_tendencies_cpu
+ * (src/core/orchestration/dynamics/dynamics.cpp:1955-2095): u and v take
+ * their tendency plus the boundary-layer one (du_dt_pbl, dv_dt_pbl; NULL =
+ * zero), w and p their own; with sanitize a non-finite tendency counts as
+ * zero; each field becomes x + t dt formed in FP64 and rounded once.
+ */
+typedef struct nimbus_slow_apply_args
+{
+    float* u;
+    float* v;
+    float* w;
+    float* p;
+    const float* du_dt;
+    const float* dv_dt;
+    const float* dw_dt;
+    const float* dp_dt;
+    const float* du_dt_pbl;  /* may be NULL */
+    const float* dv_dt_pbl;  /* may be NULL */
+    int nx, ny, nz;
+    double dt_large;
+    int sanitize;            /* the runtime's primary-state repairs */
+    int memory;
+    void* stream;
+} nimbus_slow_apply_args;
+
+nimbus_status nimbus_cuda_slow_apply(nimbus_cuda_context* ctx, const nimbus_slow_apply_args* a);
 nimbus_status nimbus_cuda_slow_step(nimbus_cuda_context* ctx, const nimbus_slow_args* a);
 
 /*

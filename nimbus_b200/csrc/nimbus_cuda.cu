@@ -865,6 +865,59 @@ nimbus_status nimbus_cuda_eos_projection(nimbus_cuda_context* ctx, const nimbus_
     return NIMBUS_OK;
 }
 
+nimbus_status nimbus_cuda_slow_apply(nimbus_cuda_context* ctx, const nimbus_slow_apply_args* a)
+{
+    if (!ctx || !a) return NIMBUS_ERR_INVALID_ARGUMENT;
+    if (!a->u || !a->v || !a->w || !a->p || !a->du_dt || !a->dv_dt || !a->dw_dt || !a->dp_dt || a->nx < 1 ||
+        a->ny < 1 || a->nz < 1 || !cells_fit(a->nx, a->ny, a->nz) || !std::isfinite(a->dt_large))
+        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "invalid slow apply arguments");
+    if (a->memory != NIMBUS_MEMORY_HOST && a->memory != NIMBUS_MEMORY_DEVICE)
+        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "unknown memory kind");
+    NB_CUDA(ctx, cudaSetDevice(ctx->device));
+    const size_t n = static_cast<size_t>(a->nx) * a->ny * a->nz;
+    const int blocks = grid_for(ctx, static_cast<long long>(n));
+    if (a->memory == NIMBUS_MEMORY_DEVICE)
+    {
+        cudaStream_t st = a->stream ? static_cast<cudaStream_t>(a->stream) : ctx->stream;
+        slow_apply_kernel<<<blocks, kThreads, 0, st>>>(a->u, a->v, a->w, a->p, a->du_dt, a->dv_dt, a->dw_dt, a->dp_dt,
+                                                       a->du_dt_pbl, a->dv_dt_pbl, static_cast<long long>(n),
+                                                       a->dt_large, a->sanitize);
+        NB_CUDA(ctx, cudaGetLastError());
+        ctx->launches += 1;
+        return NIMBUS_OK;
+    }
+    const size_t bytes = n * sizeof(float);
+    float *u, *v, *w, *p, *t, *pbl = nullptr;
+    NB_TRY(ensure(ctx, kU, n, &u));
+    NB_TRY(ensure(ctx, kV, n, &v));
+    NB_TRY(ensure(ctx, kW, n, &w));
+    NB_TRY(ensure(ctx, kP, n, &p));
+    NB_TRY(ensure(ctx, kSlowK1, 4 * n, &t));
+    if (a->du_dt_pbl || a->dv_dt_pbl) NB_TRY(ensure(ctx, kSlowStar, 2 * n, &pbl));
+    NB_TRY(upload(ctx, u, a->u, bytes));
+    NB_TRY(upload(ctx, v, a->v, bytes));
+    NB_TRY(upload(ctx, w, a->w, bytes));
+    NB_TRY(upload(ctx, p, a->p, bytes));
+    NB_TRY(upload(ctx, t, a->du_dt, bytes));
+    NB_TRY(upload(ctx, t + n, a->dv_dt, bytes));
+    NB_TRY(upload(ctx, t + 2 * n, a->dw_dt, bytes));
+    NB_TRY(upload(ctx, t + 3 * n, a->dp_dt, bytes));
+    if (a->du_dt_pbl) NB_TRY(upload(ctx, pbl, a->du_dt_pbl, bytes));
+    if (a->dv_dt_pbl) NB_TRY(upload(ctx, pbl + n, a->dv_dt_pbl, bytes));
+    slow_apply_kernel<<<blocks, kThreads, 0, ctx->stream>>>(u, v, w, p, t, t + n, t + 2 * n, t + 3 * n,
+                                                            a->du_dt_pbl ? pbl : nullptr,
+                                                            a->dv_dt_pbl ? pbl + n : nullptr,
+                                                            static_cast<long long>(n), a->dt_large, a->sanitize);
+    NB_CUDA(ctx, cudaGetLastError());
+    ctx->launches += 1;
+    NB_TRY(download(ctx, a->u, u, bytes));
+    NB_TRY(download(ctx, a->v, v, bytes));
+    NB_TRY(download(ctx, a->w, w, bytes));
+    NB_TRY(download(ctx, a->p, p, bytes));
+    NB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return NIMBUS_OK;
+}
+
 nimbus_status nimbus_cuda_max_sound_speed(nimbus_cuda_context* ctx, nimbus_sound_speed_args* a)
 {
     if (!ctx || !a) return NIMBUS_ERR_INVALID_ARGUMENT;

@@ -305,6 +305,38 @@ __device__ __forceinline__ float slow_apply_one(const SlowParams& S, float x, fl
     else return (float)((double)x + finite_or_zero((double)t) * S.dt);
 }
 
+// The slow tendencies applied over dt with the CPU's arithmetic
+// (apply_slow_tendencies_cpu, dynamics.cpp:1955-2095): the horizontal
+// tendencies gain the boundary-layer ones (du + du_pbl in FP64; a missing
+// field counts as zero, added all the same so that a -0.0 sums as it does
+// there), a non-finite tendency counts as zero when sanitize is on, and each
+// field takes x + t dt in FP64 rounded once to FP32.
+static __global__ void __launch_bounds__(256) slow_apply_kernel(
+    float* __restrict__ u, float* __restrict__ v, float* __restrict__ w, float* __restrict__ p,
+    const float* __restrict__ du, const float* __restrict__ dv, const float* __restrict__ dw,
+    const float* __restrict__ dp, const float* __restrict__ du_pbl, const float* __restrict__ dv_pbl, long long n,
+    double dt, int sanitize)
+{
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x)
+    {
+        double tu = (double)du[c] + (du_pbl ? (double)du_pbl[c] : 0.0);
+        double tv = (double)dv[c] + (dv_pbl ? (double)dv_pbl[c] : 0.0);
+        double tw = (double)dw[c];
+        double tp = (double)dp[c];
+        if (sanitize)
+        {
+            tu = finite_or_zero(tu);
+            tv = finite_or_zero(tv);
+            tw = finite_or_zero(tw);
+            tp = finite_or_zero(tp);
+        }
+        u[c] = (float)((double)u[c] + tu * dt);
+        v[c] = (float)((double)v[c] + tv * dt);
+        w[c] = (float)((double)w[c] + tw * dt);
+        p[c] = (float)((double)p[c] + tp * dt);
+    }
+}
+
 // k1 at cell c and, when su is given, the predictor state x* = x + dt*k1.
 // Also the plain tendency evaluation (su == null).
 template <class Policy>

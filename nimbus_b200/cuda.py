@@ -169,6 +169,14 @@ class MemberDesc(ctypes.Structure):
     ]
 
 
+class SlowApplyArgs(ctypes.Structure):
+    _fields_ = [
+        *[(k, _fp) for k in ("u", "v", "w", "p", "du_dt", "dv_dt", "dw_dt", "dp_dt", "du_dt_pbl", "dv_dt_pbl")],
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("dt_large", ctypes.c_double),
+        ("sanitize", ctypes.c_int), ("memory", ctypes.c_int), ("stream", ctypes.c_void_p),
+    ]
+
+
 class EngineTuning(ctypes.Structure):
     _fields_ = [
         ("lanes", ctypes.c_int), ("acoustic_form", ctypes.c_int), ("march", ctypes.c_int),
@@ -265,7 +273,7 @@ EXPORTED_SYMBOLS = (
     "nimbus_cuda_max_sound_speed", "nimbus_cuda_resolve_substep_count",
     "nimbus_cuda_engine_set_march", "nimbus_cuda_engine_march", "nimbus_cuda_engine_set_acoustic_form",
     "nimbus_cuda_engine_acoustic_form", "nimbus_cuda_engine_member_status_async", "nimbus_cuda_engine_graph_builds",
-    "nimbus_cuda_engine_autotune",
+    "nimbus_cuda_engine_autotune", "nimbus_cuda_slow_apply",
 )
 ACOUSTIC_FORM_NAMES = {0: "member-table", 1: "constant-bank", 2: "marching"}
 ACOUSTIC_TABLE, ACOUSTIC_CONST, ACOUSTIC_MARCH = 0, 1, 2
@@ -369,6 +377,7 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
     lib.nimbus_cuda_engine_set_acoustic_form.argtypes = [vp, ctypes.c_int]
     lib.nimbus_cuda_engine_member_status_async.argtypes = [vp, ctypes.c_int, ctypes.c_void_p]
     lib.nimbus_cuda_engine_autotune.argtypes = [vp, ctypes.c_int, ctypes.POINTER(EngineTuning)]
+    lib.nimbus_cuda_slow_apply.argtypes = [vp, ctypes.POINTER(SlowApplyArgs)]
     lib.nimbus_cuda_engine_graph_builds.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64),
                                                     ctypes.POINTER(ctypes.c_uint64)]
     lib.nimbus_cuda_engine_acoustic_form.argtypes = [vp]
@@ -517,6 +526,19 @@ class Context:
         a.stream = stream
         self.check(self.lib.nimbus_cuda_max_sound_speed(self.handle, ctypes.byref(a)))
         return a.max_sound_speed
+
+    def slow_apply(self, u, v, w, p, du, dv, dw, dp, dt, du_pbl=None, dv_pbl=None, sanitize=True) -> None:
+        """apply_slow_tendencies_cpu on host float32 arrays (in place) or device tensors."""
+        a = SlowApplyArgs()
+        a._keep = (u, v, w, p, du, dv, dw, dp, du_pbl, dv_pbl)
+        for name, x in zip(("u", "v", "w", "p", "du_dt", "dv_dt", "dw_dt", "dp_dt", "du_dt_pbl", "dv_dt_pbl"),
+                           a._keep):
+            setattr(a, name, _f(x))
+        a.nx, a.ny, a.nz = (int(x) for x in u.shape)
+        a.dt_large = float(dt)
+        a.sanitize = int(bool(sanitize))
+        a.memory = MEMORY_DEVICE if hasattr(u, "data_ptr") else MEMORY_HOST
+        self.check(self.lib.nimbus_cuda_slow_apply(self.handle, ctypes.byref(a)))
 
     def resolve_substep_count(self, dt, c_max, min_spacing, requested=0) -> int:
         """The reference's substep-count rule (split_explicit.cpp:67-170)."""

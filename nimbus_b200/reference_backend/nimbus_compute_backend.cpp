@@ -40,6 +40,7 @@
 
 #include "../../include/nimbus_cuda.h"
 
+#include <algorithm>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -150,8 +151,130 @@ public:
     bool supports(DynamicsKernelOp op) const override
     {
         return op == DynamicsKernelOp::AcousticSubstepFusedCartesianCgrid ||
-               op == DynamicsKernelOp::AcousticSubstepsBatchedCartesianCgrid;
+               op == DynamicsKernelOp::AcousticSubstepsBatchedCartesianCgrid ||
+               op == DynamicsKernelOp::SlowApply || op == DynamicsKernelOp::StateRelaxationCartesian;
     }
+
+    // apply_slow_tendencies_cpu's arithmetic on the dispatched fields (the
+    // FP32 dt_large widened to FP64: the CPU's result bit for bit when dt is
+    // FP32-representable, as 1.5, 3 or 6 s are).  With a completion
+    // observer, the committed fields are handed to it before the host fields
+    // change, as the contract asks.
+    bool dispatch_slow_apply(const SlowApplyDispatch& d) override
+    {
+        if (!ctx_ || !d.u || !d.v || !d.w || !d.p_data || !d.du_dt || !d.dv_dt || !d.dw_dt || !d.dp_dt) return false;
+        const size_t n = static_cast<size_t>(d.nx) * d.ny * d.nz;
+        std::vector<float> fields;
+        float* out[4] = {d.u, d.v, d.w, d.p_data};
+        if (d.completed_observer)
+        {
+            fields.resize(4 * n);
+            for (int f = 0; f < 4; ++f)
+            {
+                std::copy(out[f], out[f] + n, fields.begin() + f * n);
+                out[f] = fields.data() + f * n;
+            }
+        }
+        nimbus_slow_apply_args a{};
+        a.u = out[0];
+        a.v = out[1];
+        a.w = out[2];
+        a.p = out[3];
+        a.du_dt = d.du_dt;
+        a.dv_dt = d.dv_dt;
+        a.dw_dt = d.dw_dt;
+        a.dp_dt = d.dp_dt;
+        a.du_dt_pbl = d.du_dt_pbl;
+        a.dv_dt_pbl = d.dv_dt_pbl;
+        a.nx = d.nx;
+        a.ny = d.ny;
+        a.nz = d.nz;
+        a.dt_large = static_cast<double>(d.dt_large);
+        a.sanitize = d.sanitize ? 1 : 0;
+        a.memory = NIMBUS_MEMORY_HOST;
+        if (!count(nimbus_cuda_slow_apply(ctx_, &a))) return false;
+        if (d.completed_observer)
+        {
+            d.completed_observer(d.completed_observer_context, out[0], out[1], out[2], out[3]);
+            std::copy(out[0], out[0] + n, d.u);
+            std::copy(out[1], out[1] + n, d.v);
+            std::copy(out[2], out[2] + n, d.w);
+            std::copy(out[3], out[3] + n, d.p_data);
+        }
+        return true;
+    }
+
+    // The end-of-step sponge from the dispatch's packed FP32 profile block
+    // (rows of nz: upper alpha, w-only alpha, u_ref, v_ref, theta0, lateral
+    // alpha by distance, stagger-aware upper-w alpha; dynamics.cpp:538-567),
+    // widened to FP64, with the exact exponential factor and C-grid
+    // staggering the compact device ABI implies (the caller keeps the
+    // implicit mode on its CPU writer, dynamics.cpp:478-485).  The result is
+    // the C-ABI's on those widened profiles; it differs from the CPU writer by
+    // their FP32 rounding, as the reference's accelerator backends do.
+    bool dispatch_state_relaxation_cartesian(const StateRelaxationDispatch& d) override
+    {
+        if (!ctx_ || !d.u || !d.v || !d.w || !d.theta_data || !d.profiles) return false;
+        const int nz = d.nz;
+        if (d.profiles_len < 7 * nz || d.lateral_width < 0 || d.lateral_width > nz) return false;
+        std::vector<double> rows(static_cast<size_t>(7 * nz));
+        for (int r = 0; r < 7 * nz; ++r) rows[static_cast<size_t>(r)] = static_cast<double>(d.profiles[r]);
+        const size_t n = static_cast<size_t>(d.nx) * d.ny * nz;
+        std::vector<float> fields;
+        float* out[4] = {d.u, d.v, d.w, d.theta_data};
+        if (d.completed_observer)
+        {
+            fields.resize(4 * n);
+            for (int f = 0; f < 4; ++f)
+            {
+                std::copy(out[f], out[f] + n, fields.begin() + f * n);
+                out[f] = fields.data() + f * n;
+            }
+        }
+        nimbus_state_relaxation_args a{};
+        a.u = out[0];
+        a.v = out[1];
+        a.w = out[2];
+        a.theta = out[3];
+        a.nx = d.nx;
+        a.ny = d.ny;
+        a.nz = nz;
+        a.alpha = rows.data();
+        a.w_only_alpha = rows.data() + nz;
+        a.u_ref = rows.data() + 2 * nz;
+        a.v_ref = rows.data() + 3 * nz;
+        a.theta_ref = rows.data() + 4 * nz;
+        a.lateral_alpha = rows.data() + 5 * nz;
+        a.upper_w_alpha = rows.data() + 6 * nz;
+        a.lateral_width = d.lateral_width;
+        a.do_upper = d.do_upper ? 1 : 0;
+        a.do_w_only = d.do_w_only ? 1 : 0;
+        a.do_lateral = d.do_lateral ? 1 : 0;
+        a.staggered = 1;
+        a.implicit_mode = 0;
+        a.dt = static_cast<double>(d.dt_step);
+        a.memory = NIMBUS_MEMORY_HOST;
+        if (!count(nimbus_cuda_state_relaxation(ctx_, &a))) return false;
+        if (d.completed_observer)
+        {
+            d.completed_observer(d.completed_observer_context, out[0], out[1], out[2], out[3]);
+            for (int f = 0; f < 4; ++f)
+            {
+                float* dst = f == 0 ? d.u : f == 1 ? d.v : f == 2 ? d.w : d.theta_data;
+                std::copy(out[f], out[f] + n, dst);
+            }
+        }
+        return true;
+    }
+
+    // Residency: every dispatch uploads the host fields it is given and
+    // writes its results back before returning, and no device copy outlives
+    // a dispatch, so there is nothing to keep or invalidate between them.
+    void begin_resident_step() override {}
+    void select_residency_scope(ComputeResidencyScope) noexcept override {}
+    void invalidate_residency_scope(ComputeResidencyScope) noexcept override {}
+    void invalidate_resident_field(const char*) noexcept override {}
+    void invalidate_all_resident_fields() noexcept override {}
 
     bool supports_batched_cartesian_cgrid_mass_flux_export() const override { return true; }
 

@@ -725,6 +725,42 @@ class ReferenceHarness:
         return True
 
 
+    def bridge_slow_apply(self, st, tend, dt, pbl=None, sanitize=True, observed=False, backend=None):
+        """apply through the reference's bridge dispatch_slow_apply_backend to
+        `backend` (a shared library; None: the CPU backend, which declines it);
+        in place on st's u, v, w, p.  Returns (False, None) when declined,
+        else (True, the committed fields the observer saw or None)."""
+        u, v, w, p = (st[k] for k in ("u", "v", "w", "p"))
+        nx, ny, nz = u.shape
+        outs = [np.zeros_like(u) for _ in range(4)] if observed else [None] * 4
+        calls = ctypes.c_int(0)
+        lib = str(backend).encode() if backend is not None else None
+        du_pbl, dv_pbl = (pbl if pbl is not None else (None, None))
+        rc = self.lib.ref_backend_slow_apply(
+            lib, _fp(u), _fp(v), _fp(w), _fp(p), *[_fp(t) for t in tend], _opt(du_pbl), _opt(dv_pbl), nx, ny, nz,
+            ctypes.c_float(dt), int(sanitize), int(observed), *[_opt(o) for o in outs], ctypes.byref(calls))
+        if rc == 1:
+            return False, None
+        self._rc(rc)
+        return True, (dict(zip("uvwp", outs)) if observed else None, calls.value)
+
+    def bridge_state_relaxation(self, st, profiles_block, lateral_width, flags, dt, backend=None):
+        """the sponge through dispatch_state_relaxation_cartesian_backend with a
+        packed FP32 profile block (7 rows of nz) and a completion observer;
+        in place.  Returns False when declined, else the observer's call count."""
+        u, v, w, th = (st[k] for k in ("u", "v", "w", "theta"))
+        nx, ny, nz = u.shape
+        calls = ctypes.c_int(0)
+        lib = str(backend).encode() if backend is not None else None
+        rc = self.lib.ref_backend_state_relaxation(
+            lib, _fp(u), _fp(v), _fp(w), _fp(th), _fp(np.ascontiguousarray(profiles_block, np.float32)), nx, ny, nz,
+            int(lateral_width), *[int(bool(x)) for x in flags], ctypes.c_float(dt), ctypes.byref(calls))
+        if rc == 1:
+            return False
+        self._rc(rc)
+        return calls.value
+
+
 def reference_available() -> bool:
     return (REF / "libnimbus_ref_harness.so").exists()
 

@@ -86,10 +86,12 @@
 #include "turbulence/schemes/smagorinsky/smagorinsky.hpp"
 #include "numerics/runtime.hpp"
 #include "compute/bridge/advection.hpp"
+#include "compute/bridge/dynamics.hpp"
 #include "numerics/time_stepping/schemes/split_explicit/split_explicit.hpp"
 
 #include <dlfcn.h>
 
+#include <algorithm>
 #include <cstring>
 #include <exception>
 #include <memory>
@@ -981,6 +983,95 @@ int ref_backend_scalar_transport(const char* library, float** q, const int* posi
         if (!done) return 1;
         for (int s = 0; s < n_scalars; ++s)
             from_field(q[s], fields[s]);
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        return fail(e.what());
+    }
+}
+
+// A completion observer that keeps the committed fields the backend hands it.
+struct ObservedCommit
+{
+    std::vector<float>* out = nullptr;
+    std::size_t n = 0;
+    int calls = 0;
+};
+
+void observe_commit(void* context, const float* a, const float* b, const float* c, const float* d)
+{
+    auto* o = static_cast<ObservedCommit*>(context);
+    const float* committed[4] = {a, b, c, d};
+    for (int f = 0; f < 4; ++f) std::copy(committed[f], committed[f] + o->n, o->out[f].begin());
+    ++o->calls;
+}
+
+// The slow tendencies applied through the reference's bridge
+// dispatch_slow_apply_backend (src/compute/dispatch/dynamics.cpp:489-513) to
+// the backend `library` holds (NULL: the CPU backend), with the arguments
+// dynamics.cpp:2346-2364 passes; observed != 0 adds a completion observer
+// whose committed fields are written to out_*.  Returns 1 when declined.
+int ref_backend_slow_apply(const char* library, float* u, float* v, float* w, float* p, const float* du,
+                           const float* dv, const float* dw, const float* dp, const float* du_pbl,
+                           const float* dv_pbl, int nx, int ny, int nz, float dt, int sanitize, int observed,
+                           float* out_u, float* out_v, float* out_w, float* out_p, int* observer_calls)
+{
+    try
+    {
+        ComputeBackendRuntimeState runtime;
+        runtime.backend = load_backend(library);
+        std::string err;
+        if (!runtime.backend->initialize(err)) return fail(err.c_str());
+        const std::size_t n = static_cast<std::size_t>(nx) * ny * nz;
+        std::vector<float> kept[4];
+        for (auto& k : kept) k.assign(n, 0.0f);
+        ObservedCommit obs;
+        obs.out = kept;
+        obs.n = n;
+        const bool done = dispatch_slow_apply_backend(runtime, u, v, w, p, du, dv, dw, dp, du_pbl, dv_pbl, nx, ny, nz,
+                                                      dt, observed ? &observe_commit : nullptr,
+                                                      observed ? &obs : nullptr, sanitize != 0);
+        if (!done) return 1;
+        float* outs[4] = {out_u, out_v, out_w, out_p};
+        for (int f = 0; f < 4; ++f)
+            if (outs[f]) std::copy(kept[f].begin(), kept[f].end(), outs[f]);
+        *observer_calls = obs.calls;
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        return fail(e.what());
+    }
+}
+
+// The end-of-step sponge through the reference's bridge
+// dispatch_state_relaxation_cartesian_backend (src/compute/dispatch/dynamics.cpp:
+// 440-470) with a packed FP32 profile block laid out as dynamics.cpp:538-567
+// builds it (rows of nz: upper alpha, w-only alpha, u_ref, v_ref, theta0,
+// lateral alpha by distance, upper-w alpha) and a completion observer, as
+// try_state_relaxation_gpu calls it.  Returns 1 when declined.
+int ref_backend_state_relaxation(const char* library, float* u, float* v, float* w, float* theta,
+                                 const float* profiles, int nx, int ny, int nz, int lateral_width, int do_upper,
+                                 int do_w_only, int do_lateral, float dt, int* observer_calls)
+{
+    try
+    {
+        ComputeBackendRuntimeState runtime;
+        runtime.backend = load_backend(library);
+        std::string err;
+        if (!runtime.backend->initialize(err)) return fail(err.c_str());
+        const std::size_t n = static_cast<std::size_t>(nx) * ny * nz;
+        std::vector<float> kept[4];
+        for (auto& k : kept) k.assign(n, 0.0f);
+        ObservedCommit obs;
+        obs.out = kept;
+        obs.n = n;
+        const bool done = dispatch_state_relaxation_cartesian_backend(
+            runtime, u, v, w, theta, profiles, 7 * nz, nx, ny, nz, lateral_width, do_upper != 0, do_w_only != 0,
+            do_lateral != 0, dt, &observe_commit, &obs);
+        if (!done) return 1;
+        *observer_calls = obs.calls;
         return 0;
     }
     catch (const std::exception& e)

@@ -53,6 +53,7 @@ def _c_layout(struct_name, fields, tmp_path):
     ("nimbus_kessler_args", cuda.KesslerArgs),
     ("nimbus_eos_args", cuda.EosArgs),
     ("nimbus_sound_speed_args", cuda.SoundSpeedArgs),
+    ("nimbus_slow_apply_args", cuda.SlowApplyArgs),
     ("nimbus_boundary_args", cuda.BoundaryArgs),
     ("nimbus_state_relaxation_args", cuda.StateRelaxationArgs),
     ("nimbus_cell_centre_args", cuda.CellCentreArgs),

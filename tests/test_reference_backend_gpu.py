@@ -142,3 +142,89 @@ def test_transport_through_the_reference_bridge(ref, bc_name, weno):
     for k, x, y, z in zip(names, direct, cpu, cuda_route):
         assert np.array_equal(bits(x), bits(y)), k
         assert np.array_equal(bits(y), bits(z)), k
+
+
+@pytest.mark.parametrize("sanitize,observed,pbl", [(True, False, True), (True, True, False), (False, True, True)])
+def test_slow_apply_through_the_reference_bridge(ref, sanitize, observed, pbl):
+    """dispatch_slow_apply_backend (the accelerator route of the slow apply;
+    the reference's CPU backend declines it) with the CUDA backend's adapter:
+    apply_slow_tendencies_cpu's arithmetic bit for bit (dt FP32-representable),
+    boundary-layer tendencies added, non-finite tendencies zeroed under the
+    repairs, and the committed fields handed to the completion observer
+    before the host fields change."""
+    rng = np.random.default_rng(5)
+    shape = (23, 17, 11)
+    st = {k: rng.uniform(-30, 30, shape).astype(np.float32) for k in "uvw"}
+    st["p"] = rng.uniform(5e4, 1e5, shape).astype(np.float32)
+    tend = [rng.uniform(-1, 1, shape).astype(np.float32) for _ in range(3)] + \
+        [rng.uniform(-20, 20, shape).astype(np.float32)]
+    tend[0][1, 2, 3] = np.nan
+    tend[3][4, 4, 4] = np.inf
+    tend[1][0, 0, 0] = -0.0
+    st["v"][0, 0, 0] = -0.0
+    pbl_fields = (rng.uniform(-0.1, 0.1, shape).astype(np.float32),
+                  rng.uniform(-0.1, 0.1, shape).astype(np.float32)) if pbl else None
+    dt = 3.0
+    f64 = np.float64
+    want = {}
+    for k, t, extra in (("u", tend[0], pbl_fields[0] if pbl else None), ("v", tend[1], pbl_fields[1] if pbl else None),
+                        ("w", tend[2], None), ("p", tend[3], None)):
+        ts = t.astype(f64) + (extra.astype(f64) if extra is not None else 0.0)
+        if sanitize:
+            ts = np.where(np.isfinite(ts), ts, 0.0)
+        with np.errstate(invalid="ignore"):
+            want[k] = (st[k].astype(f64) + ts * dt).astype(np.float32)
+    cpu = {k: v.copy() for k, v in st.items()}
+    assert ref.bridge_slow_apply(cpu, tend, dt, pbl_fields, sanitize) == (False, None)
+    for k in st:
+        assert np.array_equal(bits(cpu[k]), bits(st[k])), "a declined dispatch leaves the fields untouched"
+    got = {k: v.copy() for k, v in st.items()}
+    ok, extra = ref.bridge_slow_apply(got, tend, dt, pbl_fields, sanitize, observed=observed, backend=ADAPTER)
+    assert ok
+    for k in st:
+        assert np.array_equal(bits(got[k]), bits(want[k])), k
+    if observed:
+        committed, calls = extra
+        assert calls == 1
+        for k in st:
+            assert np.array_equal(bits(committed[k]), bits(want[k])), k
+
+
+def test_state_relaxation_through_the_reference_bridge(ref):
+    """dispatch_state_relaxation_cartesian_backend with the profile block
+    try_state_relaxation_gpu packs (FP32 rows) and its completion observer:
+    the adapter equals the C-ABI on the widened FP32 profiles bit for bit, and
+    the reference's CPU sponge (FP64 profiles) within that narrowing."""
+    from nimbus_b200 import cuda
+    from nimbus_b200.sponge import SpongeConfig, SpongeProfiles
+
+    cfg = SpongeConfig(z_damp=-1.0, alpha_max=0.05, w_only_cells=6, w_only_alpha_max=0.2, lateral_width=7,
+                       lateral_alpha_max=0.05, implicit_mode=0, wind=(2.0, 1.0, 8.0, 4.0, 20.0, 10.0))
+    case = Case(30, 26, 24, 500.0, 600.0, 400.0, 3.0, seed=6)
+    st, base = cloudy_state(case, seed=6)
+    fields = {k: st[k].copy() for k in ("u", "v", "w", "theta")}
+    cpu = {k: v.copy() for k, v in fields.items()}
+    prof = ref.state_relaxation(cpu, base["theta0"], (case.dx, case.dy, case.dz), case.dt, cfg)
+    nz = case.nz
+    block = np.zeros((7, nz), np.float32)
+    block[0], block[1] = prof["alpha"], prof["w_only_alpha"]
+    block[2], block[3] = prof["u_ref"], prof["v_ref"]
+    block[4] = base["theta0"]
+    block[5, :cfg.lateral_width] = prof["lateral_alpha"]
+    block[6] = prof["upper_w_alpha"]
+    flags = (1, 1, 1)
+    got = {k: v.copy() for k, v in fields.items()}
+    calls = ref.bridge_state_relaxation(got, block, cfg.lateral_width, flags, np.float32(case.dt), backend=ADAPTER)
+    assert calls == 1
+    wide = block.astype(np.float64)
+    P = SpongeProfiles(alpha=wide[0], upper_w_alpha=wide[6], w_only_alpha=wide[1], u_ref=wide[2], v_ref=wide[3],
+                       theta_ref=wide[4], lateral_alpha=wide[5, :cfg.lateral_width].copy(), staggered=1,
+                       implicit_mode=0)
+    ctx = cuda.Context(0)
+    mine = {k: v.copy() for k, v in fields.items()}
+    ctx.check(ctx.state_relaxation(cuda.state_relaxation_args(mine, P, float(np.float32(case.dt)))))
+    ctx.close()
+    for k in fields:
+        assert np.array_equal(bits(got[k]), bits(mine[k])), k
+        scale = np.abs(cpu[k]).max() + 1e-30
+        assert np.abs(got[k].astype(np.float64) - cpu[k]).max() / scale < 1e-5, k
