@@ -936,34 +936,46 @@ int nimbus_cuda_engine_lanes(const nimbus_engine* e);
  *   NIMBUS_ACOUSTIC_MARCH  one thread advances nimbus_cuda_engine_set_march
  *                          consecutive cells of a row along x (default 16),
  *                          neighbour data of the previous cell carried over in
- *                          registers. */
+ *                          registers;
+ *   NIMBUS_ACOUSTIC_PAIR   the constant-bank form with two cells per thread
+ *                          (both cells' loads issued before either's
+ *                          arithmetic).
+ * nimbus_cuda_engine_set_acoustic_form sets both passes; set_pass_forms sets
+ * each; nimbus_cuda_engine_acoustic_form reports the continuity pass's. */
 enum
 {
     NIMBUS_ACOUSTIC_TABLE = 0,
     NIMBUS_ACOUSTIC_CONST = 1,
-    NIMBUS_ACOUSTIC_MARCH = 2
+    NIMBUS_ACOUSTIC_MARCH = 2,
+    NIMBUS_ACOUSTIC_PAIR = 3
 };
 nimbus_status nimbus_cuda_engine_set_acoustic_form(nimbus_engine* e, int form);
 int nimbus_cuda_engine_acoustic_form(const nimbus_engine* e);
+nimbus_status nimbus_cuda_engine_set_pass_forms(nimbus_engine* e, int continuity_form, int momentum_form);
+nimbus_status nimbus_cuda_engine_pass_forms(const nimbus_engine* e, int* continuity_form, int* momentum_form);
 nimbus_status nimbus_cuda_engine_set_march(nimbus_engine* e, int planes);
 int nimbus_cuda_engine_march(const nimbus_engine* e);
 
 /* The engine autotuner (no counterpart in the reference).  Times candidate
- * launch configurations -- lanes {1, 2, 4, 6, 8} (at most the member count) x
- * acoustic kernel form {constant-bank, member-table, marching 16 planes} --
- * on the resident members themselves, `steps` timed steps each after one
- * warm-up step, keeps the fastest and reports every candidate's time.  The
- * members' states are saved on the device before and restored after, so the
- * runs are where they were (status words and substep counts may reflect the
- * tuning steps).  Waits for the device. */
-#define NIMBUS_TUNING_CANDIDATES 16
+ * launch configurations on the resident members themselves, `steps` timed
+ * steps each after one warm-up step, keeps the fastest and reports every
+ * candidate's time: first the lane count {1, 2, 4, 6, 8} (at most the member
+ * count) with the constant-bank form, then, at the fastest lane count, every
+ * pair of pass forms (continuity x momentum, each of constant bank, member
+ * table, marching 16 planes, two cells per thread).  The members' states are
+ * saved on the device before and restored after, so the runs are where they
+ * were (status words and substep counts may reflect the tuning steps).
+ * Waits for the device. */
+#define NIMBUS_TUNING_CANDIDATES 32
 typedef struct nimbus_engine_tuning
 {
-    int lanes, acoustic_form, march;  /* the chosen configuration (now set) */
+    int lanes, acoustic_form, march;  /* the chosen configuration (now set); acoustic_form: continuity */
+    int momentum_form;
     double ms_per_step;               /* its time */
     int candidates;
     int candidate_lanes[NIMBUS_TUNING_CANDIDATES];
     int candidate_form[NIMBUS_TUNING_CANDIDATES];
+    int candidate_momentum_form[NIMBUS_TUNING_CANDIDATES];
     int candidate_march[NIMBUS_TUNING_CANDIDATES];
     double candidate_ms[NIMBUS_TUNING_CANDIDATES];
 } nimbus_engine_tuning;

@@ -135,27 +135,17 @@ __device__ __forceinline__ void continuity_eos_values(const FusedParams& P, cons
     p_out[c] = substep_pressure<Policy>(P, eos0, k, rho_stored, s.th);
 }
 
-// Continuity, rho forward Euler and EOS for cell c.  With store_flux the
-// retained fluxes are written rather than accumulated and rho_copy (when
-// given) receives the pre-substep density (the transport context's
-// beginning density).  Every load is issued before any arithmetic (indices of
-// neighbours outside the grid are clamped to the cell; those values are not
-// used), so a thread has all of its memory requests in flight at once.
-template <class Policy>
-__device__ __forceinline__ void continuity_eos_cell(const FusedParams& P, const float* __restrict__ rho,
-                                                    const float* __restrict__ u, const float* __restrict__ v,
-                                                    const float* __restrict__ w, const float* __restrict__ theta,
-                                                    const double* __restrict__ rho0,
-                                                    const float4* __restrict__ eos0, float* __restrict__ rho_out,
-                                                    float* __restrict__ p_out, float* __restrict__ drho_out,
-                                                    float* __restrict__ mfx, float* __restrict__ mfy,
-                                                    float* __restrict__ mfz, int c, unsigned& flags, bool store_flux,
-                                                    float* __restrict__ rho_copy)
+// Loads cell c = (i, j, k)'s continuity stencil (acc: the stored retained-flux
+// sums too).  Neighbours outside the grid read the cell itself.
+__device__ __forceinline__ ContinuityStencil continuity_load(const Dims& d, const float* __restrict__ rho,
+                                                             const float* __restrict__ u,
+                                                             const float* __restrict__ v,
+                                                             const float* __restrict__ w,
+                                                             const float* __restrict__ theta, const float* mfx,
+                                                             const float* mfy, const float* mfz, bool acc, int c,
+                                                             int i, int j, int k)
 {
-    const Dims d = P.d;
     const int sx = d.sx(), sy = d.sy();
-    int i, j, k;
-    decompose(d, c, i, j, k);
     const bool xlo = i >= 1, xhi = i < d.nx - 1, ylo = j >= 1, yhi = j < d.ny - 1;
     const bool zlo = k > 0, zhi = k + 1 < d.nz;
     ContinuityStencil s;
@@ -173,10 +163,33 @@ __device__ __forceinline__ void continuity_eos_cell(const FusedParams& P, const 
     s.wc = w[c];
     s.wzm = w[zlo ? c - 1 : c];
     s.th = theta[c];
-    const bool acc = mfx != nullptr && !store_flux;
     s.mx = acc ? mfx[c] : 0.0f;
     s.my = acc ? mfy[c] : 0.0f;
     s.mz = acc ? mfz[c] : 0.0f;
+    return s;
+}
+
+// Continuity, rho forward Euler and EOS for cell c.  With store_flux the
+// retained fluxes are written rather than accumulated and rho_copy (when
+// given) receives the pre-substep density (the transport context's
+// beginning density).  Every load is issued before any arithmetic (indices of
+// neighbours outside the grid are clamped to the cell; those values are not
+// used), so a thread has all of its memory requests in flight at once.
+template <class Policy>
+__device__ __forceinline__ void continuity_eos_cell(const FusedParams& P, const float* __restrict__ rho,
+                                                    const float* __restrict__ u, const float* __restrict__ v,
+                                                    const float* __restrict__ w, const float* __restrict__ theta,
+                                                    const double* __restrict__ rho0,
+                                                    const float4* __restrict__ eos0, float* __restrict__ rho_out,
+                                                    float* __restrict__ p_out, float* __restrict__ drho_out,
+                                                    float* __restrict__ mfx, float* __restrict__ mfy,
+                                                    float* __restrict__ mfz, int c, unsigned& flags, bool store_flux,
+                                                    float* __restrict__ rho_copy)
+{
+    int i, j, k;
+    decompose(P.d, c, i, j, k);
+    const ContinuityStencil s =
+        continuity_load(P.d, rho, u, v, w, theta, mfx, mfy, mfz, mfx != nullptr && !store_flux, c, i, j, k);
     continuity_eos_values<Policy>(P, s, i, j, k, c, rho0, eos0, rho_out, p_out, drho_out, mfx, mfy, mfz, flags,
                                   store_flux, rho_copy);
 }
@@ -362,21 +375,14 @@ __device__ __forceinline__ void momentum_values(const FusedParams& P, const Mome
     }
 }
 
-template <class Policy>
-__device__ __forceinline__ void momentum_cell(const FusedParams& P, const float* __restrict__ rho,
-                                              const float* __restrict__ p, const double* __restrict__ p0,
-                                              const float2* __restrict__ dp0_split, const float* u, const float* v,
-                                              const float* w, float* u_out, float* v_out, float* w_out, int c,
-                                              int fuse_vertical = 0)
+// Loads cell c = (i, j, k)'s momentum stencil; outside the interior the
+// neighbour indices fall back to the cell itself (those values are not used).
+__device__ __forceinline__ MomentumStencil momentum_load(const Dims& d, const float* __restrict__ rho,
+                                                         const float* __restrict__ p, const float* u, const float* v,
+                                                         const float* w, int c, int i, int j, int k)
 {
-    const Dims d = P.d;
-    const int sx = d.sx(), sy = d.sy();
-    int i, j, k;
-    decompose(d, c, i, j, k);
     const bool interior = i >= 1 && i < d.nx - 1 && j >= 1 && j < d.ny - 1 && k < d.nz - 1;
-    // Every load first; outside the interior the neighbour indices fall back
-    // to the cell itself (those values are not used).
-    const int cx = interior ? c + sx : c, cy = interior ? c + sy : c, cz1 = interior ? c + 1 : c;
+    const int cx = interior ? c + d.sx() : c, cy = interior ? c + d.sy() : c, cz1 = interior ? c + 1 : c;
     MomentumStencil s;
     s.rc = rho[c];
     s.rx = rho[cx];
@@ -389,6 +395,19 @@ __device__ __forceinline__ void momentum_cell(const FusedParams& P, const float*
     s.uc = u[c];
     s.vc = v[c];
     s.wc = w[c];
+    return s;
+}
+
+template <class Policy>
+__device__ __forceinline__ void momentum_cell(const FusedParams& P, const float* __restrict__ rho,
+                                              const float* __restrict__ p, const double* __restrict__ p0,
+                                              const float2* __restrict__ dp0_split, const float* u, const float* v,
+                                              const float* w, float* u_out, float* v_out, float* w_out, int c,
+                                              int fuse_vertical = 0)
+{
+    int i, j, k;
+    decompose(P.d, c, i, j, k);
+    const MomentumStencil s = momentum_load(P.d, rho, p, u, v, w, c, i, j, k);
     momentum_values<Policy>(P, s, i, j, k, c, p0, dp0_split, u_out, v_out, w_out, fuse_vertical);
 }
 

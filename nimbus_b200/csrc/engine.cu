@@ -1067,6 +1067,7 @@ nimbus_status nimbus_cuda_engine_autotune(nimbus_engine* e, int steps, nimbus_en
     {
         out->lanes = e->lane_target;
         out->acoustic_form = e->acoustic_form;
+        out->momentum_form = e->momentum_form;
         out->march = e->march_len;
         return NIMBUS_OK;
     }
@@ -1076,41 +1077,33 @@ nimbus_status nimbus_cuda_engine_autotune(nimbus_engine* e, int steps, nimbus_en
     launch_image(e, 1, backup);  // save
     struct Candidate
     {
-        int lanes, form, march;
+        int lanes, form, momentum, march;
     };
-    std::vector<Candidate> cands;
-    const int members = static_cast<int>(e->slots.size());
-    for (int lanes : {1, 2, 4, 6, 8})
-    {
-        if (lanes > members && lanes != 1) continue;
-        cands.push_back({lanes, NIMBUS_ACOUSTIC_CONST, e->march_len});
-        cands.push_back({lanes, NIMBUS_ACOUSTIC_TABLE, e->march_len});
-        cands.push_back({lanes, NIMBUS_ACOUSTIC_MARCH, 16});
-    }
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     NB_CUDA(ctx, cudaEventCreate(&t0));
     NB_CUDA(ctx, cudaEventCreate(&t1));
-    const int saved_lanes = e->lane_target, saved_form = e->acoustic_form, saved_march = e->march_len;
+    const Candidate saved{e->lane_target, e->acoustic_form, e->momentum_form, e->march_len};
     double best = 1e300;
-    Candidate chosen{saved_lanes, saved_form, saved_march};
+    Candidate chosen = saved;
     nimbus_status status = NIMBUS_OK;
     int n = 0;
-    for (const Candidate& c : cands)
-    {
+    // Times one candidate; false when a step failed (status set).
+    auto trial = [&](const Candidate& c) {
         e->lane_target = c.lanes;
         e->acoustic_form = c.form;
+        e->momentum_form = c.momentum;
         e->march_len = c.march;
         e->dirty = true;
         status = nimbus_cuda_engine_step(e, 1);  // builds the table and graphs, warms up
-        if (status != NIMBUS_OK) break;
+        if (status != NIMBUS_OK) return false;
         cudaEventRecord(t0, e->stream);
         status = nimbus_cuda_engine_step(e, steps);
-        if (status != NIMBUS_OK) break;
+        if (status != NIMBUS_OK) return false;
         cudaEventRecord(t1, e->stream);
         if (cudaEventSynchronize(t1) != cudaSuccess)
         {
             status = cuda_fail(ctx, cudaGetLastError(), "autotune timing");
-            break;
+            return false;
         }
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, t0, t1);
@@ -1119,6 +1112,7 @@ nimbus_status nimbus_cuda_engine_autotune(nimbus_engine* e, int steps, nimbus_en
         {
             out->candidate_lanes[n] = c.lanes;
             out->candidate_form[n] = c.form;
+            out->candidate_momentum_form[n] = c.momentum;
             out->candidate_march[n] = c.march;
             out->candidate_ms[n] = per_step;
             ++n;
@@ -1131,13 +1125,37 @@ nimbus_status nimbus_cuda_engine_autotune(nimbus_engine* e, int steps, nimbus_en
         // Restore the saved states for the next candidate (rows may have
         // moved with the lane split: the image follows admission order).
         launch_image(e, 0, backup);
+        return true;
+    };
+    // Lanes first (constant-bank form), then every pair of pass forms at the
+    // fastest lane count.
+    const int members = static_cast<int>(e->slots.size());
+    bool ok = true;
+    for (int lanes : {1, 2, 4, 6, 8})
+    {
+        if (lanes > members && lanes != 1) continue;
+        if (!(ok = trial({lanes, NIMBUS_ACOUSTIC_CONST, NIMBUS_ACOUSTIC_CONST, saved.march}))) break;
+    }
+    const int forms[] = {NIMBUS_ACOUSTIC_CONST, NIMBUS_ACOUSTIC_PAIR, NIMBUS_ACOUSTIC_TABLE, NIMBUS_ACOUSTIC_MARCH};
+    const int lanes = chosen.lanes;
+    for (int cf : forms)
+    {
+        if (!ok) break;
+        for (int mf : forms)
+        {
+            if (cf == NIMBUS_ACOUSTIC_CONST && mf == NIMBUS_ACOUSTIC_CONST) continue;  // timed above
+            const int march = (cf == NIMBUS_ACOUSTIC_MARCH || mf == NIMBUS_ACOUSTIC_MARCH) ? 16 : saved.march;
+            if (!(ok = trial({lanes, cf, mf, march}))) break;
+        }
     }
     out->candidates = n;
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
-    e->lane_target = status == NIMBUS_OK ? chosen.lanes : saved_lanes;
-    e->acoustic_form = status == NIMBUS_OK ? chosen.form : saved_form;
-    e->march_len = status == NIMBUS_OK ? chosen.march : saved_march;
+    const Candidate& keep = status == NIMBUS_OK ? chosen : saved;
+    e->lane_target = keep.lanes;
+    e->acoustic_form = keep.form;
+    e->momentum_form = keep.momentum;
+    e->march_len = keep.march;
     e->dirty = true;
     NB_TRY(rebuild_table(e));
     launch_image(e, 0, backup);  // every run back to its state before tuning
@@ -1147,6 +1165,7 @@ nimbus_status nimbus_cuda_engine_autotune(nimbus_engine* e, int steps, nimbus_en
     NB_TRY(status);
     out->lanes = e->lane_target;
     out->acoustic_form = e->acoustic_form;
+    out->momentum_form = e->momentum_form;
     out->march = e->march_len;
     out->ms_per_step = best;
     return NIMBUS_OK;
@@ -1220,16 +1239,31 @@ nimbus_status nimbus_cuda_engine_set_lanes(nimbus_engine* e, int lanes)
 
 int nimbus_cuda_engine_lanes(const nimbus_engine* e) { return e ? static_cast<int>(e->lanes.size()) : 0; }
 
-nimbus_status nimbus_cuda_engine_set_acoustic_form(nimbus_engine* e, int form)
+nimbus_status nimbus_cuda_engine_set_pass_forms(nimbus_engine* e, int continuity_form, int momentum_form)
 {
-    if (!e || form < NIMBUS_ACOUSTIC_TABLE || form > NIMBUS_ACOUSTIC_MARCH) return NIMBUS_ERR_INVALID_ARGUMENT;
-    if (form != e->acoustic_form)
+    auto valid = [](int f) { return f >= NIMBUS_ACOUSTIC_TABLE && f <= NIMBUS_ACOUSTIC_PAIR; };
+    if (!e || !valid(continuity_form) || !valid(momentum_form)) return NIMBUS_ERR_INVALID_ARGUMENT;
+    if (continuity_form != e->acoustic_form || momentum_form != e->momentum_form)
     {
         NB_TRY(sync_table_to_host(e));
-        e->acoustic_form = form;
+        e->acoustic_form = continuity_form;
+        e->momentum_form = momentum_form;
         e->dirty = true;
     }
     return NIMBUS_OK;
+}
+
+nimbus_status nimbus_cuda_engine_pass_forms(const nimbus_engine* e, int* continuity_form, int* momentum_form)
+{
+    if (!e || !continuity_form || !momentum_form) return NIMBUS_ERR_INVALID_ARGUMENT;
+    *continuity_form = e->acoustic_form;
+    *momentum_form = e->momentum_form;
+    return NIMBUS_OK;
+}
+
+nimbus_status nimbus_cuda_engine_set_acoustic_form(nimbus_engine* e, int form)
+{
+    return nimbus_cuda_engine_set_pass_forms(e, form, form);
 }
 
 int nimbus_cuda_engine_acoustic_form(const nimbus_engine* e) { return e ? e->acoustic_form : -1; }

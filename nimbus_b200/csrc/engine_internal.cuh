@@ -62,7 +62,8 @@ struct nimbus_engine
     std::vector<nimbus_engine_detail::Lane> lanes;
     int lane_target = 4;            // lanes when there are at least that many members
     int march_len = 16;             // i-planes per thread of the marching acoustic kernels
-    int acoustic_form = NIMBUS_ACOUSTIC_CONST;  // nimbus_acoustic_form of the continuity and momentum passes
+    int acoustic_form = NIMBUS_ACOUSTIC_CONST;  // nimbus_acoustic_form of the continuity pass
+    int momentum_form = NIMBUS_ACOUSTIC_CONST;  // and of the momentum pass
     std::vector<cudaStream_t> lane_streams;  // lanes 1.. (lane 0 runs on the engine stream)
     std::vector<cudaEvent_t> lane_done;
     cudaEvent_t fork = nullptr;
@@ -98,21 +99,21 @@ using namespace nimbus_host;
 
 constexpr int kEngineBlock = 256;
 
-int blocks_per_sm(nimbus_engine* e, const void* kernel)
+int blocks_per_sm(nimbus_engine* e, const void* kernel, int block = kEngineBlock)
 {
     auto it = e->occupancy.find(kernel);
     if (it != e->occupancy.end()) return it->second;
     int blocks = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, kEngineBlock, 0) != cudaSuccess || blocks < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, block, 0) != cudaSuccess || blocks < 1)
         blocks = 1;
     e->occupancy[kernel] = blocks;
     return blocks;
 }
 
 // Persistent grid: one wave of resident CTAs, never more blocks than tiles.
-unsigned engine_grid(nimbus_engine* e, const void* kernel, long long tiles)
+unsigned engine_grid(nimbus_engine* e, const void* kernel, long long tiles, int block = kEngineBlock)
 {
-    const long long wave = static_cast<long long>(e->ctx->sm_count) * blocks_per_sm(e, kernel);
+    const long long wave = static_cast<long long>(e->ctx->sm_count) * blocks_per_sm(e, kernel, block);
     const long long g = tiles < wave ? tiles : wave;
     return static_cast<unsigned>(g < 1 ? 1 : g);
 }
@@ -127,17 +128,21 @@ long long tiles_of(const nimbus_engine* e, const nimbus_engine_detail::Lane& L, 
     return e->prefix[L.prefix_first + static_cast<size_t>(kind) * (L.members + 1) + members];
 }
 
-#define ENGINE_LAUNCH(family, kernel, tiles, gy, ...)                                                    \
+#define ENGINE_LAUNCH_GRID(family, kernel, tiles, gy, block, ...)                                       \
     do {                                                                                                 \
         const long long tiles_ = (tiles);                                                                \
         if (tiles_ > 0)                                                                                  \
         {                                                                                                \
             LaunchTimer t_(ctx, st, family);                                                             \
-            kernel<<<dim3(engine_grid(e, reinterpret_cast<const void*>(kernel), tiles_), gy), kEngineBlock, 0, \
-                     st>>>(__VA_ARGS__);                                                                 \
+            kernel<<<dim3(engine_grid(e, reinterpret_cast<const void*>(kernel), tiles_, (block)), gy),   \
+                     (block), 0, st>>>(__VA_ARGS__);                                                     \
             ++count;                                                                                     \
         }                                                                                                \
     } while (0)
+#define ENGINE_LAUNCH(family, kernel, tiles, gy, ...) \
+    ENGINE_LAUNCH_GRID(family, kernel, tiles, gy, kEngineBlock, __VA_ARGS__)
+#define ENGINE_LAUNCH_BLOCK(family, kernel, tiles, block, ...) \
+    ENGINE_LAUNCH_GRID(family, kernel, tiles, 1, block, __VA_ARGS__)
 
 // Enqueues part `part` of one large step of the members of one lane on `st`
 // (0: Heun slow step, boundary refresh and KW78 seed; 1: the acoustic loop,
@@ -177,13 +182,17 @@ int enqueue_step(nimbus_engine* e, int lane, cudaStream_t st, int part)
     }
     // The acoustic loop: members still inside it are a prefix of the lane.
     const long long* pm = prefix_of(e, L, kItemMarch);
-    // The constant-bank form: the lane's members' constants as one kernel
+    // The constant-bank forms: the lane's members' constants as one kernel
     // parameter (lanes of at most kConstMembers members; larger ones take the
     // member-table form).
-    const int form = (e->acoustic_form == NIMBUS_ACOUSTIC_CONST && n > kConstMembers) ? NIMBUS_ACOUSTIC_TABLE
-                                                                                       : e->acoustic_form;
+    auto resolve_form = [n](int f) {
+        const bool bank = f == NIMBUS_ACOUSTIC_CONST || f == NIMBUS_ACOUSTIC_PAIR;
+        return (bank && n > kConstMembers) ? static_cast<int>(NIMBUS_ACOUSTIC_TABLE) : f;
+    };
+    const int cform = resolve_form(e->acoustic_form), mform = resolve_form(e->momentum_form);
+    auto in_bank = [](int f) { return f == NIMBUS_ACOUSTIC_CONST || f == NIMBUS_ACOUSTIC_PAIR; };
     std::unique_ptr<AcousticLaunch> al;
-    if (form == NIMBUS_ACOUSTIC_CONST)
+    if (in_bank(cform) || in_bank(mform))
     {
         al.reset(new AcousticLaunch());
         const long long* p = e->prefix.data() + L.prefix_first + static_cast<size_t>(kItemCells) * (n + 1);
@@ -214,31 +223,51 @@ int enqueue_step(nimbus_engine* e, int lane, cudaStream_t st, int part)
     {
         const int a = L.active[s];
         const int si = static_cast<int>(s);
-        if (form == NIMBUS_ACOUSTIC_CONST)
+        const long long tiles = tiles_of(e, L, kItemCells, a);
+        const long long march_tiles = tiles_of(e, L, kItemMarch, a);
+        switch (cform)
         {
-            const long long tiles = tiles_of(e, L, kItemCells, a);
+        case NIMBUS_ACOUSTIC_CONST:
             if (s == 0)
                 ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, (engine_continuity_const_kernel<Policy, true>), tiles, 1,
                               *al, T, tiles, si);
             else
                 ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, (engine_continuity_const_kernel<Policy, false>), tiles,
                               1, *al, T, tiles, si);
+            break;
+        case NIMBUS_ACOUSTIC_PAIR:
+            if (s == 0)
+                ENGINE_LAUNCH_BLOCK(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, (engine_continuity_pair_kernel<Policy, true>),
+                                    tiles, kEngineBlock / 2, *al, T, tiles, si);
+            else
+                ENGINE_LAUNCH_BLOCK(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, (engine_continuity_pair_kernel<Policy, false>),
+                                    tiles, kEngineBlock / 2, *al, T, tiles, si);
+            break;
+        case NIMBUS_ACOUSTIC_MARCH:
+            ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, engine_continuity_march_kernel<Policy>, march_tiles, 1, T,
+                          pm, march_tiles, si);
+            break;
+        default:
+            ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, engine_continuity_kernel<Policy>, tiles, 1, T, pc, tiles,
+                          si);
+        }
+        switch (mform)
+        {
+        case NIMBUS_ACOUSTIC_CONST:
             ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_MOMENTUM, engine_momentum_const_kernel<Policy>, tiles, 1, *al, T,
                           tiles, si);
-        }
-        else if (form == NIMBUS_ACOUSTIC_MARCH)
-        {
-            ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, engine_continuity_march_kernel<Policy>,
-                          tiles_of(e, L, kItemMarch, a), 1, T, pm, tiles_of(e, L, kItemMarch, a), si);
-            ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_MOMENTUM, engine_momentum_march_kernel<Policy>,
-                          tiles_of(e, L, kItemMarch, a), 1, T, pm, tiles_of(e, L, kItemMarch, a), si);
-        }
-        else
-        {
-            ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, engine_continuity_kernel<Policy>,
-                          tiles_of(e, L, kItemCells, a), 1, T, pc, tiles_of(e, L, kItemCells, a), si);
-            ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_MOMENTUM, engine_momentum_kernel<Policy>,
-                          tiles_of(e, L, kItemCells, a), 1, T, pc, tiles_of(e, L, kItemCells, a), si);
+            break;
+        case NIMBUS_ACOUSTIC_PAIR:
+            ENGINE_LAUNCH_BLOCK(NIMBUS_KERNEL_ACOUSTIC_MOMENTUM, engine_momentum_pair_kernel<Policy>, tiles,
+                                kEngineBlock / 2, *al, T, tiles, si);
+            break;
+        case NIMBUS_ACOUSTIC_MARCH:
+            ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_MOMENTUM, engine_momentum_march_kernel<Policy>, march_tiles, 1, T,
+                          pm, march_tiles, si);
+            break;
+        default:
+            ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_MOMENTUM, engine_momentum_kernel<Policy>, tiles, 1, T, pc, tiles,
+                          si);
         }
         ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_bc_we_kernel, tiles_of(e, L, kItemRowsWE, a), 1, T, pwe,
                       tiles_of(e, L, kItemRowsWE, a), si, 0);

@@ -404,6 +404,86 @@ static __global__ void __launch_bounds__(256, NIMBUS_CONST_MINB_MOM) engine_mome
     }
 }
 
+// The same two passes with two cells per thread: a CTA of half a tile's
+// threads takes cells c and c + blockDim.x of each tile, issuing both
+// stencils' loads before either cell's arithmetic, so a thread has twice the
+// bytes in flight (the passes are memory-latency bound at one cell per
+// thread).  Each cell's arithmetic is the one-cell form's.
+#ifndef NIMBUS_PAIR_MINB
+#define NIMBUS_PAIR_MINB 8
+#endif
+#ifndef NIMBUS_PAIR_MINB_MOM
+#define NIMBUS_PAIR_MINB_MOM 8
+#endif
+
+template <class Policy, bool kFirst>
+static __global__ void __launch_bounds__(128, NIMBUS_PAIR_MINB) engine_continuity_pair_kernel(const __grid_constant__ AcousticLaunch L,
+                                                                     const EngineMember* __restrict__ table,
+                                                                     long long tiles, int s)
+{
+    const bool even = (s & 1) == 0;
+    const int half = (int)blockDim.x;
+    int m = 0;
+    for (long long t = blockIdx.x; t < tiles; t += gridDim.x)
+    {
+        while (t >= L.prefix[m + 1]) ++m;
+        const AcousticConst& A = L.m[m];
+        const Dims d = A.F.d;
+        const int n = d.cells();
+        const int c0 = (int)((t - L.prefix[m]) * (2 * half)) + (int)threadIdx.x;
+        if (c0 >= n) continue;
+        const bool two = c0 + half < n;
+        const int c1 = two ? c0 + half : c0;
+        const EngineMember& M = table[m];
+        const float* rho = even ? M.rho : M.rho_alt;
+        float* rho_out = even ? M.rho_alt : M.rho;
+        int i0, j0, k0, i1, j1, k1;
+        decompose(d, c0, i0, j0, k0);
+        decompose(d, c1, i1, j1, k1);
+        const ContinuityStencil s0 = continuity_load(d, rho, A.u, A.v, A.w, A.theta, A.mfx, A.mfy, A.mfz, !kFirst, c0,
+                                                     i0, j0, k0);
+        const ContinuityStencil s1 = continuity_load(d, rho, A.u, A.v, A.w, A.theta, A.mfx, A.mfy, A.mfz, !kFirst, c1,
+                                                     i1, j1, k1);
+        unsigned flags = 0;
+        continuity_eos_values<Policy>(A.F, s0, i0, j0, k0, c0, A.rho0, A.eos0, rho_out, M.p, nullptr, A.mfx, A.mfy,
+                                      A.mfz, flags, kFirst, kFirst ? A.rho_begin : nullptr);
+        if (two)
+            continuity_eos_values<Policy>(A.F, s1, i1, j1, k1, c1, A.rho0, A.eos0, rho_out, M.p, nullptr, A.mfx,
+                                          A.mfy, A.mfz, flags, kFirst, kFirst ? A.rho_begin : nullptr);
+        if (flags) atomicOr(A.status, flags);
+    }
+}
+
+template <class Policy>
+static __global__ void __launch_bounds__(128, NIMBUS_PAIR_MINB_MOM) engine_momentum_pair_kernel(const __grid_constant__ AcousticLaunch L,
+                                                                       const EngineMember* __restrict__ table,
+                                                                       long long tiles, int s)
+{
+    const bool even = (s & 1) == 0;
+    const int half = (int)blockDim.x;
+    int m = 0;
+    for (long long t = blockIdx.x; t < tiles; t += gridDim.x)
+    {
+        while (t >= L.prefix[m + 1]) ++m;
+        const AcousticConst& A = L.m[m];
+        const Dims d = A.F.d;
+        const int n = d.cells();
+        const int c0 = (int)((t - L.prefix[m]) * (2 * half)) + (int)threadIdx.x;
+        if (c0 >= n) continue;
+        const bool two = c0 + half < n;
+        const int c1 = two ? c0 + half : c0;
+        const EngineMember& M = table[m];
+        const float* rho = even ? M.rho_alt : M.rho;
+        int i0, j0, k0, i1, j1, k1;
+        decompose(d, c0, i0, j0, k0);
+        decompose(d, c1, i1, j1, k1);
+        const MomentumStencil s0 = momentum_load(d, rho, M.p, A.u, A.v, A.w, c0, i0, j0, k0);
+        const MomentumStencil s1 = momentum_load(d, rho, M.p, A.u, A.v, A.w, c1, i1, j1, k1);
+        momentum_values<Policy>(A.F, s0, i0, j0, k0, c0, A.p0, A.dp0, A.u, A.v, A.w, A.vertical);
+        if (two) momentum_values<Policy>(A.F, s1, i1, j1, k1, c1, A.p0, A.dp0, A.u, A.v, A.w, A.vertical);
+    }
+}
+
 // ---- state image ----------------------------------------------------------
 // The engine's state image holds every member's nine prognostic fields back to
 // back (u, v, w, rho, p, theta, qv, qc, qr, each items[kItemCells] floats) from

@@ -177,12 +177,17 @@ class SlowApplyArgs(ctypes.Structure):
     ]
 
 
+TUNING_CANDIDATES = 32
+
+
 class EngineTuning(ctypes.Structure):
     _fields_ = [
         ("lanes", ctypes.c_int), ("acoustic_form", ctypes.c_int), ("march", ctypes.c_int),
-        ("ms_per_step", ctypes.c_double), ("candidates", ctypes.c_int),
-        ("candidate_lanes", ctypes.c_int * 16), ("candidate_form", ctypes.c_int * 16),
-        ("candidate_march", ctypes.c_int * 16), ("candidate_ms", ctypes.c_double * 16),
+        ("momentum_form", ctypes.c_int), ("ms_per_step", ctypes.c_double), ("candidates", ctypes.c_int),
+        ("candidate_lanes", ctypes.c_int * TUNING_CANDIDATES), ("candidate_form", ctypes.c_int * TUNING_CANDIDATES),
+        ("candidate_momentum_form", ctypes.c_int * TUNING_CANDIDATES),
+        ("candidate_march", ctypes.c_int * TUNING_CANDIDATES),
+        ("candidate_ms", ctypes.c_double * TUNING_CANDIDATES),
     ]
 
 
@@ -273,10 +278,11 @@ EXPORTED_SYMBOLS = (
     "nimbus_cuda_max_sound_speed", "nimbus_cuda_resolve_substep_count",
     "nimbus_cuda_engine_set_march", "nimbus_cuda_engine_march", "nimbus_cuda_engine_set_acoustic_form",
     "nimbus_cuda_engine_acoustic_form", "nimbus_cuda_engine_member_status_async", "nimbus_cuda_engine_graph_builds",
+    "nimbus_cuda_engine_set_pass_forms", "nimbus_cuda_engine_pass_forms",
     "nimbus_cuda_engine_autotune", "nimbus_cuda_slow_apply",
 )
-ACOUSTIC_FORM_NAMES = {0: "member-table", 1: "constant-bank", 2: "marching"}
-ACOUSTIC_TABLE, ACOUSTIC_CONST, ACOUSTIC_MARCH = 0, 1, 2
+ACOUSTIC_FORM_NAMES = {0: "member-table", 1: "constant-bank", 2: "marching", 3: "constant-bank, two cells per thread"}
+ACOUSTIC_TABLE, ACOUSTIC_CONST, ACOUSTIC_MARCH, ACOUSTIC_PAIR = 0, 1, 2, 3
 SUBSTEP_AUTO, SUBSTEP_FUSED, SUBSTEP_SPLIT = 0, 1, 2
 PRECISION_REFERENCE, PRECISION_FP32 = 0, 1
 STATIC_SCRATCH_CELLS = 4194304  # NIMBUS_STATIC_SCRATCH_CELLS
@@ -381,6 +387,8 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
     lib.nimbus_cuda_engine_graph_builds.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64),
                                                     ctypes.POINTER(ctypes.c_uint64)]
     lib.nimbus_cuda_engine_acoustic_form.argtypes = [vp]
+    lib.nimbus_cuda_engine_set_pass_forms.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    lib.nimbus_cuda_engine_pass_forms.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
     lib.nimbus_cuda_max_sound_speed.argtypes = [vp, ctypes.POINTER(SoundSpeedArgs)]
     lib.nimbus_cuda_resolve_substep_count.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                                       ctypes.c_int]
@@ -1019,15 +1027,17 @@ class Engine:
                                                                       ctypes.c_void_p(host_flags.ctypes.data)))
 
     def autotune(self, steps: int = 3) -> dict:
-        """Time lanes x acoustic kernel form on the resident members (states
-        restored afterwards), keep the fastest; returns the choice and every
-        candidate's ms per step."""
+        """Time the lane count, then the continuity x momentum kernel forms,
+        on the resident members (states restored afterwards), keep the
+        fastest; returns the choice and every candidate's ms per step."""
         t = EngineTuning()
         self.ctx.check(self.lib.nimbus_cuda_engine_autotune(self.handle, int(steps), ctypes.byref(t)))
-        cands = [{"lanes": t.candidate_lanes[i], "form": ACOUSTIC_FORM_NAMES[t.candidate_form[i]],
+        cands = [{"lanes": t.candidate_lanes[i], "continuity": ACOUSTIC_FORM_NAMES[t.candidate_form[i]],
+                  "momentum": ACOUSTIC_FORM_NAMES[t.candidate_momentum_form[i]],
                   "march": t.candidate_march[i], "ms_per_step": round(t.candidate_ms[i], 4)}
                  for i in range(t.candidates)]
-        return {"lanes": t.lanes, "acoustic_form": ACOUSTIC_FORM_NAMES[t.acoustic_form], "march": t.march,
+        return {"lanes": t.lanes, "continuity_form": ACOUSTIC_FORM_NAMES[t.acoustic_form],
+                "momentum_form": ACOUSTIC_FORM_NAMES[t.momentum_form], "march": t.march,
                 "ms_per_step": round(t.ms_per_step, 4), "steps_per_candidate": int(steps), "candidates": cands}
 
     def graph_builds(self) -> tuple:
@@ -1099,13 +1109,23 @@ class Engine:
         return int(self.lib.nimbus_cuda_engine_lanes(self.handle))
 
     def set_acoustic_form(self, form: int):
-        """ACOUSTIC_TABLE / ACOUSTIC_CONST / ACOUSTIC_MARCH kernels for the
-        continuity and momentum passes; results do not depend on it."""
+        """ACOUSTIC_TABLE / _CONST / _MARCH / _PAIR kernels for the continuity
+        and momentum passes; results do not depend on it."""
         self.ctx.check(self.lib.nimbus_cuda_engine_set_acoustic_form(self.handle, int(form)))
 
     @property
     def acoustic_form(self) -> int:
         return int(self.lib.nimbus_cuda_engine_acoustic_form(self.handle))
+
+    def set_pass_forms(self, continuity: int, momentum: int):
+        """Kernel form of each acoustic pass."""
+        self.ctx.check(self.lib.nimbus_cuda_engine_set_pass_forms(self.handle, int(continuity), int(momentum)))
+
+    @property
+    def pass_forms(self) -> tuple:
+        a, b = ctypes.c_int(), ctypes.c_int()
+        self.ctx.check(self.lib.nimbus_cuda_engine_pass_forms(self.handle, ctypes.byref(a), ctypes.byref(b)))
+        return int(a.value), int(b.value)
 
     def set_march(self, planes: int):
         """Cells one thread of the marching acoustic passes advances along x."""

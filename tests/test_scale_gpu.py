@@ -246,23 +246,32 @@ def test_device_sound_speed_scan_matches_oracle(ctx, o32):
         ctx.max_sound_speed(bad, st["rho"], case.shape, base)
 
 
-@pytest.mark.parametrize("form,march", [(cuda.ACOUSTIC_TABLE, 16), (cuda.ACOUSTIC_MARCH, 5),
-                                        (cuda.ACOUSTIC_MARCH, 1000)], ids=["table", "march5", "whole-rows"])
-def test_engine_acoustic_kernel_form_does_not_change_results(ctx, multi_tile, form, march):
+T, C, M, P2 = cuda.ACOUSTIC_TABLE, cuda.ACOUSTIC_CONST, cuda.ACOUSTIC_MARCH, cuda.ACOUSTIC_PAIR
+
+
+@pytest.mark.parametrize("forms,march", [((T, T), 16), ((M, M), 5), ((M, M), 1000), ((P2, P2), 16),
+                                         ((C, M), 16), ((P2, T), 7), ((T, P2), 16)],
+                         ids=["table", "march5", "whole-rows", "pair", "const-march", "pair-table", "table-pair"])
+def test_engine_acoustic_kernel_form_does_not_change_results(ctx, multi_tile, forms, march):
     """The continuity and momentum passes in each kernel form (member table,
-    constant-bank parameters -- the default, covered above -- or marching along
-    x over chunks of `march` planes) give the oracle's bits."""
+    constant-bank parameters -- the default, covered above -- marching along x
+    over chunks of `march` planes, or two cells per thread), alone and mixed
+    between the passes, give the oracle's bits."""
     members, want = multi_tile
     run = EngineRun(ctx, precision=cuda.PRECISION_REFERENCE)
-    run.engine.set_acoustic_form(form)
+    if forms[0] == forms[1]:
+        run.engine.set_acoustic_form(forms[0])
+    else:
+        run.engine.set_pass_forms(*forms)
     run.engine.set_march(march)
-    assert run.engine.acoustic_form == form and run.engine.march == march
+    assert run.engine.pass_forms == forms and run.engine.march == march
+    assert run.engine.acoustic_form == forms[0]
     ids = [run.admit(case, st, base, coriolis_f=1e-4) for case, st, base in members[:4]]
     run.step(2)
     for mid, (case, _, _), (ref, _) in zip(ids, members, want):
         got = run.read(mid)
         for k in PROGNOSTIC:
-            assert_bitwise(got[k], ref[k], f"form {form} march {march} member {mid} {case.shape} {k}")
+            assert_bitwise(got[k], ref[k], f"forms {forms} march {march} member {mid} {case.shape} {k}")
     run.close()
 
 
