@@ -1136,7 +1136,8 @@ nimbus_status nimbus_cuda_engine_autotune(nimbus_engine* e, int steps, nimbus_en
         if (lanes > members && lanes != 1) continue;
         if (!(ok = trial({lanes, NIMBUS_ACOUSTIC_CONST, NIMBUS_ACOUSTIC_CONST, saved.march}))) break;
     }
-    const int forms[] = {NIMBUS_ACOUSTIC_CONST, NIMBUS_ACOUSTIC_PAIR, NIMBUS_ACOUSTIC_TABLE, NIMBUS_ACOUSTIC_MARCH};
+    const int forms[] = {NIMBUS_ACOUSTIC_CONST, NIMBUS_ACOUSTIC_PAIR, NIMBUS_ACOUSTIC_TABLE, NIMBUS_ACOUSTIC_MARCH,
+                         NIMBUS_ACOUSTIC_BULK};
     const int lanes = chosen.lanes;
     for (int cf : forms)
     {
@@ -1204,6 +1205,7 @@ nimbus_status nimbus_cuda_engine_synchronize(nimbus_engine* e)
     if (any & kStatusNonfiniteMassFlux) return fail(ctx, NIMBUS_ERR_NONFINITE, "a member's retained mass flux went non-finite");
     if (any & kStatusNonfiniteTransport) return fail(ctx, NIMBUS_ERR_NONFINITE, "a member's transported scalar went non-finite");
     if (any & kStatusInvalidEos) return fail(ctx, NIMBUS_ERR_NONFINITE, "a member's EOS projection was refused");
+    if (any & kStatusStagingTimeout) return fail(ctx, NIMBUS_ERR_CUDA, "a bulk-staged tile's copies did not complete");
     return NIMBUS_OK;
 }
 
@@ -1241,7 +1243,7 @@ int nimbus_cuda_engine_lanes(const nimbus_engine* e) { return e ? static_cast<in
 
 nimbus_status nimbus_cuda_engine_set_pass_forms(nimbus_engine* e, int continuity_form, int momentum_form)
 {
-    auto valid = [](int f) { return f >= NIMBUS_ACOUSTIC_TABLE && f <= NIMBUS_ACOUSTIC_PAIR; };
+    auto valid = [](int f) { return f >= NIMBUS_ACOUSTIC_TABLE && f <= NIMBUS_ACOUSTIC_BULK; };
     if (!e || !valid(continuity_form) || !valid(momentum_form)) return NIMBUS_ERR_INVALID_ARGUMENT;
     if (continuity_form != e->acoustic_form || momentum_form != e->momentum_form)
     {

@@ -6,6 +6,7 @@
 #include "context.cuh"
 #include "engine_kernels.cuh"
 
+#include <algorithm>
 #include <map>
 #include <memory>
 #include <vector>
@@ -82,6 +83,7 @@ struct nimbus_engine
     bool scan_pending = false;      // h_c2 will hold the current rows' scan once scan_done completes
     cudaEvent_t scan_done = nullptr;
     std::map<const void*, int> occupancy;
+    std::map<std::pair<const void*, size_t>, int> occupancy_smem;  // (kernel, dynamic shared bytes)
     float* d_image = nullptr;       // device staging for the state image
     size_t image_cap = 0;           // bytes
     float* d_centre = nullptr;      // device staging for history frames
@@ -118,6 +120,39 @@ unsigned engine_grid(nimbus_engine* e, const void* kernel, long long tiles, int 
     return static_cast<unsigned>(g < 1 ? 1 : g);
 }
 
+// The bulk-staged acoustic forms: dynamic shared memory of kBulkStages
+// stages plus their barriers, at most kBulkSmemLimit (a lane whose members
+// need more takes the constant-bank form).
+constexpr size_t kBulkSmemLimit = 200 * 1024;
+static_assert(kBulkTile == kEngineBlock * kItemsPerThread, "a bulk-staged tile is one cell tile");
+
+size_t bulk_smem_bytes(int stage_floats)
+{
+    return kBulkBarrierBytes + static_cast<size_t>(kBulkStages) * stage_floats * sizeof(float);
+}
+
+// Persistent grid of a launch with dynamic shared memory.
+unsigned engine_grid_smem(nimbus_engine* e, const void* kernel, long long tiles, size_t smem)
+{
+    const auto key = std::make_pair(kernel, smem);
+    auto it = e->occupancy_smem.find(key);
+    int blocks = 0;
+    if (it != e->occupancy_smem.end()) blocks = it->second;
+    else
+    {
+        // The opt-in limit is a ceiling only (occupancy follows each launch's
+        // own size), so every size this kernel is launched with fits under it.
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kBulkSmemLimit));
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, kEngineBlock, smem) != cudaSuccess ||
+            blocks < 1)
+            blocks = 1;
+        e->occupancy_smem[key] = blocks;
+    }
+    const long long wave = static_cast<long long>(e->ctx->sm_count) * blocks;
+    const long long g = tiles < wave ? tiles : wave;
+    return static_cast<unsigned>(g < 1 ? 1 : g);
+}
+
 const long long* prefix_of(const nimbus_engine* e, const nimbus_engine_detail::Lane& L, int kind)
 {
     return e->d_prefix + L.prefix_first + static_cast<size_t>(kind) * (L.members + 1);
@@ -136,6 +171,17 @@ long long tiles_of(const nimbus_engine* e, const nimbus_engine_detail::Lane& L, 
             LaunchTimer t_(ctx, st, family);                                                             \
             kernel<<<dim3(engine_grid(e, reinterpret_cast<const void*>(kernel), tiles_, (block)), gy),   \
                      (block), 0, st>>>(__VA_ARGS__);                                                     \
+            ++count;                                                                                     \
+        }                                                                                                \
+    } while (0)
+#define ENGINE_LAUNCH_SMEM(family, kernel, tiles, smem, ...)                                            \
+    do {                                                                                                 \
+        const long long tiles_ = (tiles);                                                                \
+        if (tiles_ > 0)                                                                                  \
+        {                                                                                                \
+            LaunchTimer t_(ctx, st, family);                                                             \
+            kernel<<<engine_grid_smem(e, reinterpret_cast<const void*>(kernel), tiles_, (smem)),         \
+                     kEngineBlock, (smem), st>>>(__VA_ARGS__);                                           \
             ++count;                                                                                     \
         }                                                                                                \
     } while (0)
@@ -185,18 +231,37 @@ int enqueue_step(nimbus_engine* e, int lane, cudaStream_t st, int part)
     // The constant-bank forms: the lane's members' constants as one kernel
     // parameter (lanes of at most kConstMembers members; larger ones take the
     // member-table form).
-    auto resolve_form = [n](int f) {
-        const bool bank = f == NIMBUS_ACOUSTIC_CONST || f == NIMBUS_ACOUSTIC_PAIR;
-        return (bank && n > kConstMembers) ? static_cast<int>(NIMBUS_ACOUSTIC_TABLE) : f;
+    auto in_bank = [](int f) {
+        return f == NIMBUS_ACOUSTIC_CONST || f == NIMBUS_ACOUSTIC_PAIR || f == NIMBUS_ACOUSTIC_BULK;
+    };
+    // Bulk copies move 16-byte units between 16-byte-aligned addresses: every
+    // member field starts on a 256-byte boundary of its arena, so the arenas
+    // themselves must be 16-byte aligned.
+    int sy4 = 4;
+    bool arenas_aligned = true;
+    for (int r = 0; r < n; ++r)
+    {
+        const nimbus_engine_detail::MemberSlot& slot =
+            e->slots[static_cast<size_t>(e->order[static_cast<size_t>(L.first + r)])];
+        sy4 = std::max(sy4, (slot.m.F.d.sy() + 3) & ~3);
+        arenas_aligned = arenas_aligned && reinterpret_cast<uintptr_t>(slot.arena) % 16 == 0;
+    }
+    const size_t smem_cont = bulk_smem_bytes(continuity_stage_floats(sy4));
+    const size_t smem_mom = bulk_smem_bytes(momentum_stage_floats(sy4));
+    auto resolve_form = [&](int f) {
+        if (in_bank(f) && n > kConstMembers) return static_cast<int>(NIMBUS_ACOUSTIC_TABLE);
+        if (f == NIMBUS_ACOUSTIC_BULK && (smem_cont > kBulkSmemLimit || !arenas_aligned))
+            return static_cast<int>(NIMBUS_ACOUSTIC_CONST);
+        return f;
     };
     const int cform = resolve_form(e->acoustic_form), mform = resolve_form(e->momentum_form);
-    auto in_bank = [](int f) { return f == NIMBUS_ACOUSTIC_CONST || f == NIMBUS_ACOUSTIC_PAIR; };
     std::unique_ptr<AcousticLaunch> al;
     if (in_bank(cform) || in_bank(mform))
     {
         al.reset(new AcousticLaunch());
         const long long* p = e->prefix.data() + L.prefix_first + static_cast<size_t>(kItemCells) * (n + 1);
         for (int r = 0; r <= n; ++r) al->prefix[r] = p[r];
+        al->bulk_sy4 = sy4;
         for (int r = 0; r < n; ++r)
         {
             const EngineMember& H = e->slots[static_cast<size_t>(e->order[static_cast<size_t>(L.first + r)])].m;
@@ -247,6 +312,14 @@ int enqueue_step(nimbus_engine* e, int lane, cudaStream_t st, int part)
             ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, engine_continuity_march_kernel<Policy>, march_tiles, 1, T,
                           pm, march_tiles, si);
             break;
+        case NIMBUS_ACOUSTIC_BULK:
+            if (s == 0)
+                ENGINE_LAUNCH_SMEM(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, (engine_continuity_bulk_kernel<Policy, true>),
+                                   tiles, smem_cont, *al, T, tiles, si);
+            else
+                ENGINE_LAUNCH_SMEM(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, (engine_continuity_bulk_kernel<Policy, false>),
+                                   tiles, smem_cont, *al, T, tiles, si);
+            break;
         default:
             ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, engine_continuity_kernel<Policy>, tiles, 1, T, pc, tiles,
                           si);
@@ -264,6 +337,10 @@ int enqueue_step(nimbus_engine* e, int lane, cudaStream_t st, int part)
         case NIMBUS_ACOUSTIC_MARCH:
             ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_MOMENTUM, engine_momentum_march_kernel<Policy>, march_tiles, 1, T,
                           pm, march_tiles, si);
+            break;
+        case NIMBUS_ACOUSTIC_BULK:
+            ENGINE_LAUNCH_SMEM(NIMBUS_KERNEL_ACOUSTIC_MOMENTUM, engine_momentum_bulk_kernel<Policy>, tiles, smem_mom,
+                               *al, T, tiles, si);
             break;
         default:
             ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_MOMENTUM, engine_momentum_kernel<Policy>, tiles, 1, T, pc, tiles,

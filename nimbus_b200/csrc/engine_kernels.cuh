@@ -19,6 +19,7 @@
 
 #include "acoustic_kernels.cuh"
 #include "acoustic_split.cuh"
+#include "bulk_stage.cuh"
 #include "physics_kernels.cuh"
 #include "relaxation_kernels.cuh"
 #include "slow_kernels.cuh"
@@ -357,6 +358,7 @@ struct AcousticLaunch
 {
     long long prefix[kConstMembers + 1];  // first cell tile of each member
     AcousticConst m[kConstMembers];
+    int bulk_sy4;                         // the members' largest nz rounded up to 4 (bulk-staged forms)
 };
 static_assert(sizeof(AcousticLaunch) <= 32000, "a kernel parameter block holds at most 32764 bytes");
 
@@ -481,6 +483,333 @@ static __global__ void __launch_bounds__(128, NIMBUS_PAIR_MINB_MOM) engine_momen
         const MomentumStencil s1 = momentum_load(d, rho, M.p, A.u, A.v, A.w, c1, i1, j1, k1);
         momentum_values<Policy>(A.F, s0, i0, j0, k0, c0, A.p0, A.dp0, A.u, A.v, A.w, A.vertical);
         if (two) momentum_values<Policy>(A.F, s1, i1, j1, k1, c1, A.p0, A.dp0, A.u, A.v, A.w, A.vertical);
+    }
+}
+
+// The same two passes with each tile's stencil data staged in shared memory
+// by bulk copies (bulk_stage.cuh).  A tile is 256 consecutive cells of one
+// member (one per thread); its stencils read, per field, the tile itself and
+// the tile shifted by the neighbour strides, each a contiguous run of cells,
+// so one CTA stages a tile with a handful of bulk copies issued by one thread
+// and keeps kBulkStages tiles in flight while it computes.  Each cell's
+// arithmetic is the one-cell form's, on the same values.
+constexpr int kBulkStages = 4;
+constexpr int kBulkTile = 256;
+constexpr int kBulkCap = kBulkTile + 8;  // a run of the tile's length widened to 16-byte units
+constexpr int kBulkBarrierBytes = 64;
+#ifndef NIMBUS_BULK_MINB
+#define NIMBUS_BULK_MINB 4
+#endif
+
+// Floats of one continuity stage: eleven runs, R0 (rho at -x), R1 (rho at
+// the tile, +-1, +-y), R2 (rho at +x), U1 (u at the tile), U0 (u at -x), V (v
+// at the tile and -y), W (w at the tile and -1), TH, MX, MY, MZ.
+__host__ __device__ constexpr int continuity_stage_floats(int sy4) { return 11 * kBulkCap + 3 * sy4; }
+// Floats of one momentum stage: RA, PA (tile, +1, +y), RB, PB (+x), U, V, W.
+__host__ __device__ constexpr int momentum_stage_floats(int sy4) { return 7 * kBulkCap + 2 * sy4; }
+
+// Slot offsets of the two stage layouts (floats), the last entry the stage end.
+__host__ __device__ constexpr int continuity_slot(int slot, int sy4)
+{
+    // R0, R1 (+2 sy4), R2, U1, U0, V (+sy4), W, TH, MX, MY, MZ
+    return slot * kBulkCap + (slot >= 2 ? 2 * sy4 : 0) + (slot >= 6 ? sy4 : 0);
+}
+__host__ __device__ constexpr int momentum_slot(int slot, int sy4)
+{
+    // RA (+sy4), PA (+sy4), RB, PB, U, V, W
+    return slot * kBulkCap + (slot >= 1 ? sy4 : 0) + (slot >= 2 ? sy4 : 0);
+}
+static_assert(continuity_slot(11, 8) == continuity_stage_floats(8) && continuity_slot(11, 64) == continuity_stage_floats(64),
+              "continuity stage layout");
+static_assert(momentum_slot(7, 8) == momentum_stage_floats(8) && momentum_slot(7, 64) == momentum_stage_floats(64),
+              "momentum stage layout");
+
+__device__ __forceinline__ unsigned run_bytes(const CellRun& r) { return r.hi > r.lo ? 4u * (r.hi - r.lo) : 0u; }
+
+__device__ __forceinline__ void stage_run(float* dst, const float* field, const CellRun& r, uint64_t* bar)
+{
+    if (r.hi > r.lo) bulk_copy_g2s(dst, field + r.lo, run_bytes(r), bar);
+}
+
+struct ContinuityRuns
+{
+    CellRun r0, r1, r2, t, v, w;  // r0 also serves u at -x; t the tile (u, theta, mx, my, mz)
+};
+
+__device__ __forceinline__ ContinuityRuns continuity_runs(int c0, int c1, int n, int sx, int sy)
+{
+    ContinuityRuns R;
+    R.r0 = cell_run((long long)c0 - sx, (long long)c1 - sx, n);
+    R.r1 = cell_run((long long)c0 - sy, (long long)c1 + sy, n);
+    R.r2 = cell_run((long long)c0 + sx, (long long)c1 + sx, n);
+    R.t = cell_run(c0, c1, n);
+    R.v = cell_run((long long)c0 - sy, c1, n);
+    R.w = cell_run((long long)c0 - 1, c1, n);
+    return R;
+}
+
+struct MomentumRuns
+{
+    CellRun a, b, t;  // a: tile .. +y (rho, p); b: +x (rho, p); t: the tile (u, v, w)
+};
+
+__device__ __forceinline__ MomentumRuns momentum_runs(int c0, int c1, int n, int sx, int sy)
+{
+    MomentumRuns R;
+    R.a = cell_run(c0, (long long)c1 + sy, n);
+    R.b = cell_run((long long)c0 + sx, (long long)c1 + sx, n);
+    R.t = cell_run(c0, c1, n);
+    return R;
+}
+
+// Ends a CTA whose stage wait timed out: the member's status gets
+// kStatusStagingTimeout and thread 0 waits (bounded) for the copies of the
+// stages it issued that are still outstanding before the CTA leaves.
+__device__ __forceinline__ void bulk_abandon(uint64_t* bar, unsigned parity_bits, int pending, unsigned* status)
+{
+    if (threadIdx.x == 0)
+    {
+        atomicOr(status, kStatusStagingTimeout);
+        for (int q = 0; q < kBulkStages; ++q)
+            if (pending & (1 << q)) (void)mbar_wait(&bar[q], (parity_bits >> q) & 1u);
+    }
+    __syncthreads();
+}
+
+template <class Policy, bool kFirst>
+static __global__ void __launch_bounds__(256, NIMBUS_BULK_MINB) engine_continuity_bulk_kernel(const __grid_constant__ AcousticLaunch L,
+                                                                     const EngineMember* __restrict__ table,
+                                                                     long long tiles, int s)
+{
+    extern __shared__ __align__(16) unsigned char bulk_smem[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(bulk_smem);
+    float* stages = reinterpret_cast<float*>(bulk_smem + kBulkBarrierBytes);
+    const int sy4 = L.bulk_sy4;
+    const int o_r1 = continuity_slot(1, sy4), o_r2 = continuity_slot(2, sy4), o_u1 = continuity_slot(3, sy4),
+              o_u0 = continuity_slot(4, sy4), o_v = continuity_slot(5, sy4), o_w = continuity_slot(6, sy4),
+              o_th = continuity_slot(7, sy4), o_mx = continuity_slot(8, sy4), o_my = continuity_slot(9, sy4),
+              o_mz = continuity_slot(10, sy4);
+    const int stage_floats = continuity_stage_floats(sy4);
+    const bool even = (s & 1) == 0;
+    if (threadIdx.x == 0)
+    {
+        for (int q = 0; q < kBulkStages; ++q) mbar_init(&bar[q], 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+
+    int pm = 0;                        // the producer's member cursor
+    unsigned parity = 0;               // bit q: the parity of stage q's next phase
+    int pending = 0;                   // stages issued and not yet consumed (thread 0's view)
+    // Thread 0: stage tile t into stage q.
+    auto issue = [&](long long t, int q) {
+        while (t >= L.prefix[pm + 1]) ++pm;
+        const AcousticConst& A = L.m[pm];
+        const Dims d = A.F.d;
+        const int n = d.cells();
+        const int c0 = (int)((t - L.prefix[pm]) * kBulkTile), c1 = min(c0 + kBulkTile, n);
+        const EngineMember& M = table[pm];
+        const float* rho = even ? M.rho : M.rho_alt;
+        const ContinuityRuns R = continuity_runs(c0, c1, n, d.sx(), d.sy());
+        unsigned bytes = 2 * run_bytes(R.r0) + run_bytes(R.r1) + run_bytes(R.r2) + 2 * run_bytes(R.t) +
+                         run_bytes(R.v) + run_bytes(R.w);
+        if (!kFirst) bytes += 3 * run_bytes(R.t);
+        float* S = stages + q * stage_floats;
+        mbar_arrive_expect_tx(&bar[q], bytes);
+        stage_run(S, rho, R.r0, &bar[q]);
+        stage_run(S + o_r1, rho, R.r1, &bar[q]);
+        stage_run(S + o_r2, rho, R.r2, &bar[q]);
+        stage_run(S + o_u1, A.u, R.t, &bar[q]);
+        stage_run(S + o_u0, A.u, R.r0, &bar[q]);
+        stage_run(S + o_v, A.v, R.v, &bar[q]);
+        stage_run(S + o_w, A.w, R.w, &bar[q]);
+        stage_run(S + o_th, A.theta, R.t, &bar[q]);
+        if (!kFirst)
+        {
+            stage_run(S + o_mx, A.mfx, R.t, &bar[q]);
+            stage_run(S + o_my, A.mfy, R.t, &bar[q]);
+            stage_run(S + o_mz, A.mfz, R.t, &bar[q]);
+        }
+        pending |= 1 << q;
+    };
+    const long long stride = gridDim.x;
+    if (threadIdx.x == 0)
+        for (int q = 0; q < kBulkStages; ++q)
+        {
+            const long long t = blockIdx.x + q * stride;
+            if (t < tiles) issue(t, q);
+        }
+
+    int m = 0;
+    int it = 0;
+    for (long long t = blockIdx.x; t < tiles; t += stride, ++it)
+    {
+        const int q = it % kBulkStages;
+        while (t >= L.prefix[m + 1]) ++m;
+        const AcousticConst& A = L.m[m];
+        const bool ok = mbar_wait(&bar[q], (parity >> q) & 1u);
+        if (ok)
+        {
+            const Dims d = A.F.d;
+            const int n = d.cells(), sx = d.sx(), sy = d.sy();
+            const int c0 = (int)((t - L.prefix[m]) * kBulkTile), c1 = min(c0 + kBulkTile, n);
+            const int c = c0 + (int)threadIdx.x;
+            if (c < c1)
+            {
+                const ContinuityRuns R = continuity_runs(c0, c1, n, sx, sy);
+                const float* S = stages + q * stage_floats;
+                int i, j, k;
+                decompose(d, c, i, j, k);
+                const bool xlo = i >= 1, xhi = i < d.nx - 1, ylo = j >= 1, yhi = j < d.ny - 1;
+                const bool zlo = k > 0, zhi = k + 1 < d.nz;
+                const float* r1 = S + o_r1 + (c - R.r1.lo);  // rho at the cell
+                ContinuityStencil st;
+                st.rho_c = r1[0];
+                st.rxp = xhi ? S[o_r2 + (c + sx - R.r2.lo)] : st.rho_c;
+                st.rxm = xlo ? S[c - sx - R.r0.lo] : st.rho_c;
+                st.ryp = yhi ? r1[sy] : st.rho_c;
+                st.rym = ylo ? r1[-sy] : st.rho_c;
+                st.rzp = zhi ? r1[1] : st.rho_c;
+                st.rzm = zlo ? r1[-1] : st.rho_c;
+                const int ct = c - R.t.lo;
+                st.uc = S[o_u1 + ct];
+                st.uxm = xlo ? S[o_u0 + c - sx - R.r0.lo] : st.uc;
+                st.vc = S[o_v + c - R.v.lo];
+                st.vym = ylo ? S[o_v + c - sy - R.v.lo] : st.vc;
+                st.wc = S[o_w + c - R.w.lo];
+                st.wzm = zlo ? S[o_w + c - 1 - R.w.lo] : st.wc;
+                st.th = S[o_th + ct];
+                st.mx = kFirst ? 0.0f : S[o_mx + ct];
+                st.my = kFirst ? 0.0f : S[o_my + ct];
+                st.mz = kFirst ? 0.0f : S[o_mz + ct];
+                const EngineMember& M = table[m];
+                unsigned flags = 0;
+                continuity_eos_values<Policy>(A.F, st, i, j, k, c, A.rho0, A.eos0, even ? M.rho_alt : M.rho, M.p,
+                                              nullptr, A.mfx, A.mfy, A.mfz, flags, kFirst,
+                                              kFirst ? A.rho_begin : nullptr);
+                if (flags) atomicOr(A.status, flags);
+            }
+        }
+        // Every thread is done with stage q (and agrees whether its wait
+        // completed) before it is refilled.
+        if (!__syncthreads_and(ok))
+        {
+            bulk_abandon(bar, parity, pending, A.status);
+            return;
+        }
+        parity ^= 1u << q;
+        if (threadIdx.x == 0)
+        {
+            pending &= ~(1 << q);
+            const long long next = t + kBulkStages * stride;
+            if (next < tiles) issue(next, q);
+        }
+    }
+}
+
+template <class Policy>
+static __global__ void __launch_bounds__(256, NIMBUS_BULK_MINB) engine_momentum_bulk_kernel(const __grid_constant__ AcousticLaunch L,
+                                                                   const EngineMember* __restrict__ table,
+                                                                   long long tiles, int s)
+{
+    extern __shared__ __align__(16) unsigned char bulk_smem[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(bulk_smem);
+    float* stages = reinterpret_cast<float*>(bulk_smem + kBulkBarrierBytes);
+    const int sy4 = L.bulk_sy4;
+    const int o_pa = momentum_slot(1, sy4), o_rb = momentum_slot(2, sy4), o_pb = momentum_slot(3, sy4),
+              o_u = momentum_slot(4, sy4), o_v = momentum_slot(5, sy4), o_w = momentum_slot(6, sy4);
+    const int stage_floats = momentum_stage_floats(sy4);
+    const bool even = (s & 1) == 0;
+    if (threadIdx.x == 0)
+    {
+        for (int q = 0; q < kBulkStages; ++q) mbar_init(&bar[q], 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+
+    int pm = 0;
+    unsigned parity = 0;
+    int pending = 0;
+    auto issue = [&](long long t, int q) {
+        while (t >= L.prefix[pm + 1]) ++pm;
+        const AcousticConst& A = L.m[pm];
+        const Dims d = A.F.d;
+        const int n = d.cells();
+        const int c0 = (int)((t - L.prefix[pm]) * kBulkTile), c1 = min(c0 + kBulkTile, n);
+        const EngineMember& M = table[pm];
+        const float* rho = even ? M.rho_alt : M.rho;
+        const MomentumRuns R = momentum_runs(c0, c1, n, d.sx(), d.sy());
+        const unsigned bytes = 2 * run_bytes(R.a) + 2 * run_bytes(R.b) + 3 * run_bytes(R.t);
+        float* S = stages + q * stage_floats;
+        mbar_arrive_expect_tx(&bar[q], bytes);
+        stage_run(S, rho, R.a, &bar[q]);
+        stage_run(S + o_pa, M.p, R.a, &bar[q]);
+        stage_run(S + o_rb, rho, R.b, &bar[q]);
+        stage_run(S + o_pb, M.p, R.b, &bar[q]);
+        stage_run(S + o_u, A.u, R.t, &bar[q]);
+        stage_run(S + o_v, A.v, R.t, &bar[q]);
+        stage_run(S + o_w, A.w, R.t, &bar[q]);
+        pending |= 1 << q;
+    };
+    const long long stride = gridDim.x;
+    if (threadIdx.x == 0)
+        for (int q = 0; q < kBulkStages; ++q)
+        {
+            const long long t = blockIdx.x + q * stride;
+            if (t < tiles) issue(t, q);
+        }
+
+    int m = 0;
+    int it = 0;
+    for (long long t = blockIdx.x; t < tiles; t += stride, ++it)
+    {
+        const int q = it % kBulkStages;
+        while (t >= L.prefix[m + 1]) ++m;
+        const AcousticConst& A = L.m[m];
+        const bool ok = mbar_wait(&bar[q], (parity >> q) & 1u);
+        if (ok)
+        {
+            const Dims d = A.F.d;
+            const int n = d.cells(), sx = d.sx(), sy = d.sy();
+            const int c0 = (int)((t - L.prefix[m]) * kBulkTile), c1 = min(c0 + kBulkTile, n);
+            const int c = c0 + (int)threadIdx.x;
+            if (c < c1)
+            {
+                const MomentumRuns R = momentum_runs(c0, c1, n, sx, sy);
+                const float* S = stages + q * stage_floats;
+                int i, j, k;
+                decompose(d, c, i, j, k);
+                const bool interior = i >= 1 && i < d.nx - 1 && j >= 1 && j < d.ny - 1 && k < d.nz - 1;
+                const float* ra = S + (c - R.a.lo);  // rho at the cell
+                const float* pa = S + o_pa + (c - R.a.lo);
+                MomentumStencil st;
+                st.rc = ra[0];
+                st.pc = pa[0];
+                st.rx = interior ? S[o_rb + (c + sx - R.b.lo)] : st.rc;
+                st.px = interior ? S[o_pb + (c + sx - R.b.lo)] : st.pc;
+                st.ry = interior ? ra[sy] : st.rc;
+                st.py = interior ? pa[sy] : st.pc;
+                st.rz = interior ? ra[1] : st.rc;
+                st.pz = interior ? pa[1] : st.pc;
+                const int ct = c - R.t.lo;
+                st.uc = S[o_u + ct];
+                st.vc = S[o_v + ct];
+                st.wc = S[o_w + ct];
+                momentum_values<Policy>(A.F, st, i, j, k, c, A.p0, A.dp0, A.u, A.v, A.w, A.vertical);
+            }
+        }
+        if (!__syncthreads_and(ok))
+        {
+            bulk_abandon(bar, parity, pending, A.status);
+            return;
+        }
+        parity ^= 1u << q;
+        if (threadIdx.x == 0)
+        {
+            pending &= ~(1 << q);
+            const long long next = t + kBulkStages * stride;
+            if (next < tiles) issue(next, q);
+        }
     }
 }
 

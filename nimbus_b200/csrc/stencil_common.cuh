@@ -50,6 +50,7 @@ enum : unsigned
     kStatusInvalidEos = 1u << 2,
     kStatusSgsInvalid = 1u << 3,
     kStatusInvalidState = 1u << 4,  // a pressure or density failed the CFL scan (non-finite or <= 0)
+    kStatusStagingTimeout = 1u << 5,  // a bulk-staged tile's copies did not complete (the step is void)
 };
 
 struct Dims

@@ -281,8 +281,9 @@ EXPORTED_SYMBOLS = (
     "nimbus_cuda_engine_set_pass_forms", "nimbus_cuda_engine_pass_forms",
     "nimbus_cuda_engine_autotune", "nimbus_cuda_slow_apply",
 )
-ACOUSTIC_FORM_NAMES = {0: "member-table", 1: "constant-bank", 2: "marching", 3: "constant-bank, two cells per thread"}
-ACOUSTIC_TABLE, ACOUSTIC_CONST, ACOUSTIC_MARCH, ACOUSTIC_PAIR = 0, 1, 2, 3
+ACOUSTIC_FORM_NAMES = {0: "member-table", 1: "constant-bank", 2: "marching", 3: "constant-bank, two cells per thread",
+                       4: "bulk-staged tiles"}
+ACOUSTIC_TABLE, ACOUSTIC_CONST, ACOUSTIC_MARCH, ACOUSTIC_PAIR, ACOUSTIC_BULK = 0, 1, 2, 3, 4
 SUBSTEP_AUTO, SUBSTEP_FUSED, SUBSTEP_SPLIT = 0, 1, 2
 PRECISION_REFERENCE, PRECISION_FP32 = 0, 1
 STATIC_SCRATCH_CELLS = 4194304  # NIMBUS_STATIC_SCRATCH_CELLS
@@ -1109,8 +1110,8 @@ class Engine:
         return int(self.lib.nimbus_cuda_engine_lanes(self.handle))
 
     def set_acoustic_form(self, form: int):
-        """ACOUSTIC_TABLE / _CONST / _MARCH / _PAIR kernels for the continuity
-        and momentum passes; results do not depend on it."""
+        """ACOUSTIC_TABLE / _CONST / _MARCH / _PAIR / _BULK kernels for the
+        continuity and momentum passes; results do not depend on it."""
         self.ctx.check(self.lib.nimbus_cuda_engine_set_acoustic_form(self.handle, int(form)))
 
     @property

@@ -246,17 +246,20 @@ def test_device_sound_speed_scan_matches_oracle(ctx, o32):
         ctx.max_sound_speed(bad, st["rho"], case.shape, base)
 
 
-T, C, M, P2 = cuda.ACOUSTIC_TABLE, cuda.ACOUSTIC_CONST, cuda.ACOUSTIC_MARCH, cuda.ACOUSTIC_PAIR
+T, C, M, P2, B = cuda.ACOUSTIC_TABLE, cuda.ACOUSTIC_CONST, cuda.ACOUSTIC_MARCH, cuda.ACOUSTIC_PAIR, cuda.ACOUSTIC_BULK
 
 
 @pytest.mark.parametrize("forms,march", [((T, T), 16), ((M, M), 5), ((M, M), 1000), ((P2, P2), 16),
-                                         ((C, M), 16), ((P2, T), 7), ((T, P2), 16)],
-                         ids=["table", "march5", "whole-rows", "pair", "const-march", "pair-table", "table-pair"])
+                                         ((C, M), 16), ((P2, T), 7), ((T, P2), 16), ((B, B), 16), ((B, M), 16),
+                                         ((C, B), 16)],
+                         ids=["table", "march5", "whole-rows", "pair", "const-march", "pair-table", "table-pair",
+                              "bulk", "bulk-march", "const-bulk"])
 def test_engine_acoustic_kernel_form_does_not_change_results(ctx, multi_tile, forms, march):
     """The continuity and momentum passes in each kernel form (member table,
     constant-bank parameters -- the default, covered above -- marching along x
-    over chunks of `march` planes, or two cells per thread), alone and mixed
-    between the passes, give the oracle's bits."""
+    over chunks of `march` planes, two cells per thread, or tiles staged in
+    shared memory by bulk copies), alone and mixed between the passes, give
+    the oracle's bits."""
     members, want = multi_tile
     run = EngineRun(ctx, precision=cuda.PRECISION_REFERENCE)
     if forms[0] == forms[1]:
