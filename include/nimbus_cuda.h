@@ -453,6 +453,60 @@ nimbus_status nimbus_cuda_kessler_tendencies(nimbus_cuda_context* ctx, const nim
 nimbus_status nimbus_cuda_kessler_step(nimbus_cuda_context* ctx, const nimbus_kessler_args* a);
 
 /*
+ * The Kessler operators of the reference's device route
+ * (KesslerScheme::compute_tendencies, kessler.cpp:152-300, when the active
+ * backend supports MicrophysicsKernelOp::KesslerPointwise): the host runs the
+ * saturation adjustment, the pointwise operator takes the adjusted
+ * temperature, qv and qc and writes the warm-rain tendencies (production and
+ * rain evaporation; dtheta_dt is the temperature tendency before the theta
+ * conversion) over the whole grid, zero outside the cell domain; the
+ * sedimentation operator adds the rain fallout to dqr_dt in place.  FP32
+ * arithmetic, the reference's device operator
+ * (vulkan/shaders/compute/microphysics/kessler_pointwise.comp,
+ * kessler_sedimentation.comp).  Mirror KesslerPointwiseDispatch and
+ * KesslerSedimentationDispatch (include/compute/dispatch/microphysics.hpp:436-492);
+ * the inert qg/qh slots are dropped (dqg_dt/dqh_dt, when given, are written
+ * zero).
+ */
+typedef struct nimbus_kessler_pointwise_args
+{
+    const float* temperature;
+    const float* p;
+    const float* qv;
+    const float* qc;
+    const float* qr;
+    const float* rho_d;
+    float* dtheta_dt;
+    float* dqv_dt;
+    float* dqc_dt;
+    float* dqr_dt;
+    float* dqg_dt;           /* optional */
+    float* dqh_dt;           /* optional */
+    int nx, ny, nz;
+    int i_begin, i_end, j_begin, j_end, k_begin, k_end;
+    float qc0, c_auto, c_accr, evaporation_efficiency, lv_cp, t0, dt_step;
+    int memory;
+    void* stream;
+} nimbus_kessler_pointwise_args;
+
+typedef struct nimbus_kessler_sedimentation_args
+{
+    const float* qr;
+    const float* rho_d;              /* optional: density-corrected fall speeds and receiver weights */
+    const float* layer_thickness_m;  /* optional: per-cell layer thickness instead of dz */
+    float* dqr_dt;                   /* read and updated in place */
+    int nx, ny, nz;
+    int i_begin, i_end, j_begin, j_end, k_begin, k_end;
+    float dz, vt_max_rain, vt_cap, dt_step;
+    int memory;
+    void* stream;
+} nimbus_kessler_sedimentation_args;
+
+nimbus_status nimbus_cuda_kessler_pointwise(nimbus_cuda_context* ctx, const nimbus_kessler_pointwise_args* a);
+nimbus_status nimbus_cuda_kessler_sedimentation(nimbus_cuda_context* ctx,
+                                                const nimbus_kessler_sedimentation_args* a);
+
+/*
  * EOS pressure re-projection after transport and microphysics
  * (tmv::dynamics_eos::apply_pressure_projection, eos_apply.cpp:50-200):
  * p = clamp(float(p00 (rho R_d theta / p00)^gamma), 1000, 2e5) in FP64 for

@@ -918,6 +918,114 @@ nimbus_status nimbus_cuda_slow_apply(nimbus_cuda_context* ctx, const nimbus_slow
     return NIMBUS_OK;
 }
 
+namespace
+{
+bool domain_ok(int nx, int ny, int nz, int i0, int i1, int j0, int j1, int k0, int k1)
+{
+    return 0 <= i0 && i0 <= i1 && i1 <= nx && 0 <= j0 && j0 <= j1 && j1 <= ny && 0 <= k0 && k0 <= k1 && k1 <= nz;
+}
+}  // namespace
+
+nimbus_status nimbus_cuda_kessler_pointwise(nimbus_cuda_context* ctx, const nimbus_kessler_pointwise_args* a)
+{
+    if (!ctx || !a) return NIMBUS_ERR_INVALID_ARGUMENT;
+    if (!a->temperature || !a->p || !a->qv || !a->qc || !a->qr || !a->rho_d || !a->dtheta_dt || !a->dqv_dt ||
+        !a->dqc_dt || !a->dqr_dt || a->nx < 1 || a->ny < 1 || a->nz < 1 || !cells_fit(a->nx, a->ny, a->nz) ||
+        !domain_ok(a->nx, a->ny, a->nz, a->i_begin, a->i_end, a->j_begin, a->j_end, a->k_begin, a->k_end))
+        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "invalid Kessler pointwise arguments");
+    if (a->memory != NIMBUS_MEMORY_HOST && a->memory != NIMBUS_MEMORY_DEVICE)
+        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "unknown memory kind");
+    NB_CUDA(ctx, cudaSetDevice(ctx->device));
+    KesslerPointwiseParams P{a->nx, a->ny, a->nz, a->i_begin, a->i_end, a->j_begin, a->j_end, a->k_begin, a->k_end,
+                             a->qc0, a->c_auto, a->c_accr, a->evaporation_efficiency, a->lv_cp, a->t0, a->dt_step};
+    const size_t n = static_cast<size_t>(a->nx) * a->ny * a->nz;
+    const int blocks = grid_for(ctx, static_cast<long long>(n));
+    if (a->memory == NIMBUS_MEMORY_DEVICE)
+    {
+        cudaStream_t st = a->stream ? static_cast<cudaStream_t>(a->stream) : ctx->stream;
+        kessler_pointwise_kernel<<<blocks, kThreads, 0, st>>>(P, a->temperature, a->p, a->qv, a->qc, a->qr, a->rho_d,
+                                                              a->dtheta_dt, a->dqv_dt, a->dqc_dt, a->dqr_dt,
+                                                              a->dqg_dt, a->dqh_dt);
+        NB_CUDA(ctx, cudaGetLastError());
+        ctx->launches += 1;
+        return NIMBUS_OK;
+    }
+    const size_t bytes = n * sizeof(float);
+    float *T, *p, *qv, *qc, *qr, *rho, *out;
+    NB_TRY(ensure(ctx, kTheta, n, &T));
+    NB_TRY(ensure(ctx, kP, n, &p));
+    NB_TRY(ensure(ctx, kQv, n, &qv));
+    NB_TRY(ensure(ctx, kQc, n, &qc));
+    NB_TRY(ensure(ctx, kQr, n, &qr));
+    NB_TRY(ensure(ctx, kRho, n, &rho));
+    NB_TRY(ensure(ctx, kKesslerOut, 4 * n, &out));
+    NB_TRY(upload(ctx, T, a->temperature, bytes));
+    NB_TRY(upload(ctx, p, a->p, bytes));
+    NB_TRY(upload(ctx, qv, a->qv, bytes));
+    NB_TRY(upload(ctx, qc, a->qc, bytes));
+    NB_TRY(upload(ctx, qr, a->qr, bytes));
+    NB_TRY(upload(ctx, rho, a->rho_d, bytes));
+    kessler_pointwise_kernel<<<blocks, kThreads, 0, ctx->stream>>>(P, T, p, qv, qc, qr, rho, out, out + n, out + 2 * n,
+                                                                   out + 3 * n, nullptr, nullptr);
+    NB_CUDA(ctx, cudaGetLastError());
+    ctx->launches += 1;
+    NB_TRY(download(ctx, a->dtheta_dt, out, bytes));
+    NB_TRY(download(ctx, a->dqv_dt, out + n, bytes));
+    NB_TRY(download(ctx, a->dqc_dt, out + 2 * n, bytes));
+    NB_TRY(download(ctx, a->dqr_dt, out + 3 * n, bytes));
+    NB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (a->dqg_dt) std::memset(a->dqg_dt, 0, bytes);
+    if (a->dqh_dt) std::memset(a->dqh_dt, 0, bytes);
+    return NIMBUS_OK;
+}
+
+nimbus_status nimbus_cuda_kessler_sedimentation(nimbus_cuda_context* ctx, const nimbus_kessler_sedimentation_args* a)
+{
+    if (!ctx || !a) return NIMBUS_ERR_INVALID_ARGUMENT;
+    if (!a->qr || !a->dqr_dt || a->nx < 1 || a->ny < 1 || a->nz < 1 || !cells_fit(a->nx, a->ny, a->nz) ||
+        !domain_ok(a->nx, a->ny, a->nz, a->i_begin, a->i_end, a->j_begin, a->j_end, a->k_begin, a->k_end) ||
+        (!a->layer_thickness_m && !(a->dz > 0.0f)))
+        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "invalid Kessler sedimentation arguments");
+    if (a->memory != NIMBUS_MEMORY_HOST && a->memory != NIMBUS_MEMORY_DEVICE)
+        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "unknown memory kind");
+    NB_CUDA(ctx, cudaSetDevice(ctx->device));
+    KesslerSedimentationParams P{a->nx, a->ny, a->nz, a->i_begin, a->i_end, a->j_begin, a->j_end, a->k_begin,
+                                 a->k_end, a->dz, a->vt_max_rain, a->vt_cap};
+    const size_t n = static_cast<size_t>(a->nx) * a->ny * a->nz;
+    const int blocks = grid_for(ctx, static_cast<long long>(n));
+    if (a->memory == NIMBUS_MEMORY_DEVICE)
+    {
+        cudaStream_t st = a->stream ? static_cast<cudaStream_t>(a->stream) : ctx->stream;
+        kessler_sedimentation_kernel<<<blocks, kThreads, 0, st>>>(P, a->qr, a->rho_d, a->layer_thickness_m,
+                                                                  a->dqr_dt);
+        NB_CUDA(ctx, cudaGetLastError());
+        ctx->launches += 1;
+        return NIMBUS_OK;
+    }
+    const size_t bytes = n * sizeof(float);
+    float *qr, *dqr, *rho = nullptr, *layers = nullptr;
+    NB_TRY(ensure(ctx, kQr, n, &qr));
+    NB_TRY(ensure(ctx, kKesslerOut, 4 * n, &dqr));
+    NB_TRY(upload(ctx, qr, a->qr, bytes));
+    NB_TRY(upload(ctx, dqr, a->dqr_dt, bytes));
+    if (a->rho_d)
+    {
+        NB_TRY(ensure(ctx, kRho, n, &rho));
+        NB_TRY(upload(ctx, rho, a->rho_d, bytes));
+    }
+    if (a->layer_thickness_m)
+    {
+        layers = dqr + n;
+        NB_TRY(upload(ctx, layers, a->layer_thickness_m, bytes));
+    }
+    kessler_sedimentation_kernel<<<blocks, kThreads, 0, ctx->stream>>>(P, qr, rho, layers, dqr);
+    NB_CUDA(ctx, cudaGetLastError());
+    ctx->launches += 1;
+    NB_TRY(download(ctx, a->dqr_dt, dqr, bytes));
+    NB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return NIMBUS_OK;
+}
+
 nimbus_status nimbus_cuda_max_sound_speed(nimbus_cuda_context* ctx, nimbus_sound_speed_args* a)
 {
     if (!ctx || !a) return NIMBUS_ERR_INVALID_ARGUMENT;

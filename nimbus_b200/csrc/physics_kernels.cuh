@@ -744,4 +744,161 @@ static __global__ void __launch_bounds__(256) eos_publish_kernel(long long n, co
     }
 }
 
+// ---- The Kessler dispatches of the device route ---------------------------
+//
+// KesslerScheme::compute_tendencies (kessler.cpp:152-300) has a second route
+// when the active backend supports the Kessler operators: it runs the
+// saturation adjustment on the host, hands the adjusted temperature, qv and
+// qc to dispatch_kessler_pointwise (warm-rain production and rain
+// evaporation, FP32, outputs written over the whole grid, zero outside the
+// cell domain), books the adjustment's tendencies itself and then calls
+// dispatch_kessler_sedimentation, which adds the rain fallout to dqr_dt in
+// place.  The operators' arithmetic is the reference's device form of them
+// (vulkan/shaders/compute/microphysics/kessler_pointwise.comp:70-172,
+// kessler_sedimentation.comp:44-117): FP32 throughout.
+
+struct KesslerPointwiseParams
+{
+    int nx, ny, nz;
+    int i0, i1, j0, j1, k0, k1;
+    float qc0, c_auto, c_accr, evaporation_efficiency, lv_cp, t0, dt;
+};
+
+// Buck's saturation vapour pressure over water (all temperatures) and the
+// saturation mixing ratio bounded to [0, 0.2] (kessler_pointwise.comp:55-69).
+__device__ __forceinline__ float kessler_qvsat_f32(float T, float p, float t0)
+{
+    const float tc = T - t0;
+    const float es = 611.21f * expf((18.678f - tc / 234.5f) * tc / (257.14f + tc));
+    const float denom = fmaxf(p - es, 1.0f);
+    return fminf(fmaxf(0.62198f * es / denom, 0.0f), 0.2f);
+}
+
+static __global__ void __launch_bounds__(256) kessler_pointwise_kernel(
+    KesslerPointwiseParams P, const float* __restrict__ temperature, const float* __restrict__ pres,
+    const float* __restrict__ qv, const float* __restrict__ qc, const float* __restrict__ qr,
+    const float* __restrict__ rho_d, float* __restrict__ dth, float* __restrict__ dqv, float* __restrict__ dqc,
+    float* __restrict__ dqr, float* __restrict__ dqg, float* __restrict__ dqh)
+{
+    const long long n = (long long)P.nx * P.ny * P.nz;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x)
+    {
+        const int k = (int)(c % P.nz);
+        const long long col = c / P.nz;
+        const int j = (int)(col % P.ny), i = (int)(col / P.ny);
+        float d_th = 0.0f, d_qv = 0.0f, d_qc = 0.0f, d_qr = 0.0f;
+        if (i >= P.i0 && i < P.i1 && j >= P.j0 && j < P.j1 && k >= P.k0 && k < P.k1)
+        {
+            const float T = temperature[c], pv = pres[c], qvv = qv[c], qcv = qc[c], qrv = qr[c], rho = rho_d[c];
+            const float dt = P.dt;
+            // Finite-step production: implicit accretion plus autoconversion.
+            float production = 0.0f;
+            if (dt > 0.0f && qcv > 0.0f)
+            {
+                const float factor = 1.0f / (1.0f + P.c_accr * dt * powf(fmaxf(qrv, 0.0f), 0.875f));
+                float amount = qcv * (1.0f - factor) + factor * P.c_auto * dt * fmaxf(qcv - P.qc0, 0.0f);
+                amount = fminf(fmaxf(amount, 0.0f), qcv);
+                production = amount / dt;
+                d_qc -= production;
+                d_qr += production;
+            }
+            // Rain evaporation in sub-saturated air, bounded by the
+            // saturation deficit and the rain available over the step.
+            if (qrv > 0.0f || production > 0.0f)
+            {
+                const float qvsat = kessler_qvsat_f32(T, pv, P.t0);
+                if (qvsat > 0.0f && qvv < qvsat && rho > 0.0f && pv > 0.0f)
+                {
+                    const float available = qrv + production * dt;
+                    const float rcgs = 1.0e-3f * rho;
+                    const float content = rcgs * fmaxf(available, 0.0f);
+                    const float ventilation = (1.6f + 124.9f * powf(content, 0.2046f)) * powf(content, 0.525f);
+                    const float resistance = 2.55e8f / (pv * qvsat) + 5.4e5f;
+                    const float raw = P.evaporation_efficiency * (ventilation / resistance) *
+                                      ((qvsat - qvv) / (rcgs * qvsat));
+                    const float gamma_sat = P.lv_cp * (2.5e6f / 461.5f) * qvsat / fmaxf(T * T, 1.0f);
+                    const float bound = (qvsat - qvv) / (1.0f + gamma_sat);
+                    const float evap = fminf(fmaxf(raw, 0.0f), fminf(bound / dt, available / dt));
+                    d_qv += evap;
+                    d_qr -= evap;
+                    d_th -= P.lv_cp * evap;
+                }
+            }
+        }
+        dth[c] = d_th;
+        dqv[c] = d_qv;
+        dqc[c] = d_qc;
+        dqr[c] = d_qr;
+        if (dqg) dqg[c] = 0.0f;
+        if (dqh) dqh[c] = 0.0f;
+    }
+}
+
+struct KesslerSedimentationParams
+{
+    int nx, ny, nz;
+    int i0, i1, j0, j1, k0, k1;
+    float dz, vt_max, vt_cap;
+};
+
+// The rain fallout out of level k (kessler_sedimentation.comp:83-115): zero
+// below the species threshold; *donor_dz and *recv_scale receive the donor
+// layer's thickness and the density weight over the receiver's thickness.
+__device__ __forceinline__ float kessler_fallout_f32(const KesslerSedimentationParams& P, const float* qr,
+                                                     const float* rho_d, const float* layers, long long idx, int k,
+                                                     float& donor_dz, float& recv_scale_num, float& receiver_dz)
+{
+    donor_dz = P.dz;
+    receiver_dz = P.dz;
+    if (layers)
+    {
+        donor_dz = layers[idx];
+        receiver_dz = k > P.k0 ? layers[idx - 1] : donor_dz;
+    }
+    float fall = 1.0f, weight = 1.0f, rho_air = 1.2f;
+    if (rho_d)
+    {
+        const float rk = rho_d[idx];
+        const float rkm = k > P.k0 ? rho_d[idx - 1] : rk;
+        fall = sqrtf(1.2f / rk);
+        weight = rk / rkm;
+        rho_air = rk;
+    }
+    recv_scale_num = weight;
+    const float q = fmaxf(qr[idx], 0.0f);
+    if (!(q > 1.0e-9f)) return 0.0f;
+    float vt = 36.34f * powf(1.0e-3f * rho_air * q, 0.1346f);
+    vt = fminf(vt * fall, P.vt_max);
+    vt = fminf(vt, P.vt_cap);
+    return vt * q;
+}
+
+// One thread per cell of the domain: the column's sequential update of
+// dqr_dt[k] is (dqr - fallout_k / donor_dz_k) + w_{k+1} fallout_{k+1} /
+// receiver_dz_{k+1}, evaluated here per level in that order.
+static __global__ void __launch_bounds__(256) kessler_sedimentation_kernel(
+    KesslerSedimentationParams P, const float* __restrict__ qr, const float* __restrict__ rho_d,
+    const float* __restrict__ layers, float* __restrict__ dqr)
+{
+    const long long n = (long long)P.nx * P.ny * P.nz;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x)
+    {
+        const int k = (int)(c % P.nz);
+        const long long col = c / P.nz;
+        const int j = (int)(col % P.ny), i = (int)(col / P.ny);
+        if (i < P.i0 || i >= P.i1 || j < P.j0 || j >= P.j1 || k < P.k0 || k >= P.k1) continue;
+        float donor, weight, receiver;
+        const float out = kessler_fallout_f32(P, qr, rho_d, layers, c, k, donor, weight, receiver);
+        float t = dqr[c];
+        if (fmaxf(qr[c], 0.0f) > 1.0e-9f) t -= out / donor;
+        if (k + 1 < P.k1)
+        {
+            float d2, w2, r2;
+            const float in = kessler_fallout_f32(P, qr, rho_d, layers, c + 1, k + 1, d2, w2, r2);
+            if (fmaxf(qr[c + 1], 0.0f) > 1.0e-9f) t += w2 * in / r2;
+        }
+        dqr[c] = t;
+    }
+}
+
 }  // namespace nimbus

@@ -177,6 +177,26 @@ class SlowApplyArgs(ctypes.Structure):
     ]
 
 
+class KesslerPointwiseArgs(ctypes.Structure):
+    _fields_ = [
+        *[(k, _fp) for k in ("temperature", "p", "qv", "qc", "qr", "rho_d", "dtheta_dt", "dqv_dt", "dqc_dt", "dqr_dt",
+                             "dqg_dt", "dqh_dt")],
+        *[(k, ctypes.c_int) for k in ("nx", "ny", "nz", "i_begin", "i_end", "j_begin", "j_end", "k_begin", "k_end")],
+        *[(k, ctypes.c_float) for k in ("qc0", "c_auto", "c_accr", "evaporation_efficiency", "lv_cp", "t0",
+                                        "dt_step")],
+        ("memory", ctypes.c_int), ("stream", ctypes.c_void_p),
+    ]
+
+
+class KesslerSedimentationArgs(ctypes.Structure):
+    _fields_ = [
+        *[(k, _fp) for k in ("qr", "rho_d", "layer_thickness_m", "dqr_dt")],
+        *[(k, ctypes.c_int) for k in ("nx", "ny", "nz", "i_begin", "i_end", "j_begin", "j_end", "k_begin", "k_end")],
+        *[(k, ctypes.c_float) for k in ("dz", "vt_max_rain", "vt_cap", "dt_step")],
+        ("memory", ctypes.c_int), ("stream", ctypes.c_void_p),
+    ]
+
+
 TUNING_CANDIDATES = 32
 
 
@@ -279,7 +299,8 @@ EXPORTED_SYMBOLS = (
     "nimbus_cuda_engine_set_march", "nimbus_cuda_engine_march", "nimbus_cuda_engine_set_acoustic_form",
     "nimbus_cuda_engine_acoustic_form", "nimbus_cuda_engine_member_status_async", "nimbus_cuda_engine_graph_builds",
     "nimbus_cuda_engine_set_pass_forms", "nimbus_cuda_engine_pass_forms",
-    "nimbus_cuda_engine_autotune", "nimbus_cuda_slow_apply",
+    "nimbus_cuda_engine_autotune", "nimbus_cuda_slow_apply", "nimbus_cuda_kessler_pointwise",
+    "nimbus_cuda_kessler_sedimentation",
 )
 ACOUSTIC_FORM_NAMES = {0: "member-table", 1: "constant-bank", 2: "marching", 3: "constant-bank, two cells per thread",
                        4: "bulk-staged tiles"}
@@ -385,6 +406,8 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
     lib.nimbus_cuda_engine_member_status_async.argtypes = [vp, ctypes.c_int, ctypes.c_void_p]
     lib.nimbus_cuda_engine_autotune.argtypes = [vp, ctypes.c_int, ctypes.POINTER(EngineTuning)]
     lib.nimbus_cuda_slow_apply.argtypes = [vp, ctypes.POINTER(SlowApplyArgs)]
+    lib.nimbus_cuda_kessler_pointwise.argtypes = [vp, ctypes.POINTER(KesslerPointwiseArgs)]
+    lib.nimbus_cuda_kessler_sedimentation.argtypes = [vp, ctypes.POINTER(KesslerSedimentationArgs)]
     lib.nimbus_cuda_engine_graph_builds.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64),
                                                     ctypes.POINTER(ctypes.c_uint64)]
     lib.nimbus_cuda_engine_acoustic_form.argtypes = [vp]
@@ -548,6 +571,40 @@ class Context:
         a.sanitize = int(bool(sanitize))
         a.memory = MEMORY_DEVICE if hasattr(u, "data_ptr") else MEMORY_HOST
         self.check(self.lib.nimbus_cuda_slow_apply(self.handle, ctypes.byref(a)))
+
+    def kessler_pointwise(self, T, p, qv, qc, qr, rho_d, outs, domain, qc0=1.0e-3, c_auto=1.0e-3, c_accr=2.2,
+                          evaporation_efficiency=1.0, lv_cp=2.5e6 / 1004.0, t0=273.15, dt=3.0) -> None:
+        """The device route's Kessler pointwise operator: outs = (dtheta, dqv,
+        dqc, dqr[, dqg, dqh]) written over the whole grid (host float32 arrays
+        or device tensors)."""
+        a = KesslerPointwiseArgs()
+        outs = list(outs) + [None] * (6 - len(outs))
+        a._keep = (T, p, qv, qc, qr, rho_d, outs)
+        for name, x in zip(("temperature", "p", "qv", "qc", "qr", "rho_d"), (T, p, qv, qc, qr, rho_d)):
+            setattr(a, name, _f(x))
+        for name, x in zip(("dtheta_dt", "dqv_dt", "dqc_dt", "dqr_dt", "dqg_dt", "dqh_dt"), outs):
+            setattr(a, name, _f(x) if x is not None else None)
+        a.nx, a.ny, a.nz = (int(x) for x in T.shape)
+        a.i_begin, a.i_end, a.j_begin, a.j_end, a.k_begin, a.k_end = (int(x) for x in domain)
+        a.qc0, a.c_auto, a.c_accr = qc0, c_auto, c_accr
+        a.evaporation_efficiency, a.lv_cp, a.t0, a.dt_step = evaporation_efficiency, lv_cp, t0, dt
+        a.memory = MEMORY_DEVICE if hasattr(T, "data_ptr") else MEMORY_HOST
+        self.check(self.lib.nimbus_cuda_kessler_pointwise(self.handle, ctypes.byref(a)))
+
+    def kessler_sedimentation(self, qr, dqr, domain, dz, vt_max=20.0, vt_cap=3.4028234663852886e38, rho_d=None,
+                              layers=None, dt=3.0) -> None:
+        """The device route's Kessler sedimentation operator: the rain fallout
+        added to dqr in place."""
+        a = KesslerSedimentationArgs()
+        a._keep = (qr, dqr, rho_d, layers)
+        a.qr, a.dqr_dt = _f(qr), _f(dqr)
+        a.rho_d = _f(rho_d) if rho_d is not None else None
+        a.layer_thickness_m = _f(layers) if layers is not None else None
+        a.nx, a.ny, a.nz = (int(x) for x in qr.shape)
+        a.i_begin, a.i_end, a.j_begin, a.j_end, a.k_begin, a.k_end = (int(x) for x in domain)
+        a.dz, a.vt_max_rain, a.vt_cap, a.dt_step = dz, vt_max, vt_cap, dt
+        a.memory = MEMORY_DEVICE if hasattr(qr, "data_ptr") else MEMORY_HOST
+        self.check(self.lib.nimbus_cuda_kessler_sedimentation(self.handle, ctypes.byref(a)))
 
     def resolve_substep_count(self, dt, c_max, min_spacing, requested=0) -> int:
         """The reference's substep-count rule (split_explicit.cpp:67-170)."""

@@ -31,9 +31,16 @@
 //       retained acoustic context (advection_batch.cpp's route): FP64 spacings
 //       from the level's state view and dt_step_host, so the result is the CPU
 //       backend's bit for bit; see the dispatch for what it declines.
+//   KesslerPointwise / KesslerSedimentation  the two operators of
+//       KesslerScheme's device route (kessler.cpp:152-300), FP32 as the
+//       reference's device operators compute them; the scheme's result then
+//       matches its CPU route within FP32 rounding (the routes book the
+//       saturation adjustment in a different order and the CPU one computes
+//       in FP64).
 #include "compute/backend_interface.hpp"
 #include "compute/dispatch/advection.hpp"
 #include "compute/dispatch/dynamics.hpp"
+#include "compute/dispatch/microphysics.hpp"
 #include "compute/dispatch/turbulence.hpp"
 #include "core/runtime/runtime_config.hpp"
 #include "core/runtime/simulation_state.hpp"
@@ -51,6 +58,7 @@ namespace
 class NimbusCudaComputeBackend final : public ComputeBackend,
                                        public AdvectionComputeKernels,
                                        public DynamicsComputeKernels,
+                                       public MicrophysicsComputeKernels,
                                        public TurbulenceComputeKernels
 {
 public:
@@ -83,6 +91,8 @@ public:
     const AdvectionComputeKernels* advection_kernels() const override { return ctx_ ? this : nullptr; }
     DynamicsComputeKernels* dynamics_kernels() override { return ctx_ ? this : nullptr; }
     const DynamicsComputeKernels* dynamics_kernels() const override { return ctx_ ? this : nullptr; }
+    MicrophysicsComputeKernels* microphysics_kernels() override { return ctx_ ? this : nullptr; }
+    const MicrophysicsComputeKernels* microphysics_kernels() const override { return ctx_ ? this : nullptr; }
     TurbulenceComputeKernels* turbulence_kernels() override { return ctx_ ? this : nullptr; }
     const TurbulenceComputeKernels* turbulence_kernels() const override { return ctx_ ? this : nullptr; }
 
@@ -146,6 +156,72 @@ public:
         a.rho_floor = d.rho_floor;
         a.memory = NIMBUS_MEMORY_HOST;
         return count(nimbus_cuda_scalar_transport(ctx_, &a));
+    }
+
+    bool supports(MicrophysicsKernelOp op) const override
+    {
+        return op == MicrophysicsKernelOp::KesslerPointwise || op == MicrophysicsKernelOp::KesslerSedimentation;
+    }
+
+    bool dispatch_kessler_pointwise(const KesslerPointwiseDispatch& d) override
+    {
+        if (!ctx_) return false;
+        nimbus_kessler_pointwise_args a{};
+        a.temperature = d.temperature_data;
+        a.p = d.p_data;
+        a.qv = d.qv_data;
+        a.qc = d.qc_data;
+        a.qr = d.qr_data;
+        a.rho_d = d.rho_d_data;
+        a.dtheta_dt = d.dtheta_dt_data;
+        a.dqv_dt = d.dqv_dt_data;
+        a.dqc_dt = d.dqc_dt_data;
+        a.dqr_dt = d.dqr_dt_data;
+        a.dqg_dt = d.dqg_dt_data;
+        a.dqh_dt = d.dqh_dt_data;
+        a.nx = d.nr;
+        a.ny = d.nth;
+        a.nz = d.nz;
+        a.i_begin = d.i_begin;
+        a.i_end = d.i_end;
+        a.j_begin = d.j_begin;
+        a.j_end = d.j_end;
+        a.k_begin = d.k_begin;
+        a.k_end = d.k_end;
+        a.qc0 = d.qc0;
+        a.c_auto = d.c_auto;
+        a.c_accr = d.c_accr;
+        a.evaporation_efficiency = d.evaporation_efficiency;
+        a.lv_cp = d.Lv_cp;
+        a.t0 = d.T0;
+        a.dt_step = d.dt_step;
+        a.memory = NIMBUS_MEMORY_HOST;
+        return count(nimbus_cuda_kessler_pointwise(ctx_, &a));
+    }
+
+    bool dispatch_kessler_sedimentation(const KesslerSedimentationDispatch& d) override
+    {
+        if (!ctx_) return false;
+        nimbus_kessler_sedimentation_args a{};
+        a.qr = d.qr_data;
+        a.rho_d = d.rho_d_data;
+        a.layer_thickness_m = d.layer_thickness_m;
+        a.dqr_dt = d.dqr_dt_data;
+        a.nx = d.nr;
+        a.ny = d.nth;
+        a.nz = d.nz;
+        a.i_begin = d.i_begin;
+        a.i_end = d.i_end;
+        a.j_begin = d.j_begin;
+        a.j_end = d.j_end;
+        a.k_begin = d.k_begin;
+        a.k_end = d.k_end;
+        a.dz = d.dz_val;
+        a.vt_max_rain = d.Vt_max_rain;
+        a.vt_cap = d.vt_cap;
+        a.dt_step = d.dt_step;
+        a.memory = NIMBUS_MEMORY_HOST;
+        return count(nimbus_cuda_kessler_sedimentation(ctx_, &a));
     }
 
     bool supports(DynamicsKernelOp op) const override

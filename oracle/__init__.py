@@ -485,14 +485,18 @@ class ReferenceHarness:
             _opt(wave_in), _fp(out["wave"])))
         return out
 
-    def kessler_tendencies(self, st, dz, dt, domain):
+    def kessler_tendencies(self, st, dz, dt, domain, backend=None):
+        """KesslerScheme::compute_tendencies: the CPU route, or (backend: a
+        shared library's path) the device route through that library's
+        ComputeBackend (the pointwise and sedimentation dispatches)."""
         th, p, rho, qv, qc, qr = (st[k] for k in ("theta", "p", "rho", "qv", "qc", "qr"))
         nx, ny, nz = th.shape
         out = [np.zeros_like(th) for _ in range(4)]
         dom = (ctypes.c_int * 6)(*[int(x) for x in domain])
-        self._rc(self.lib.ref_kessler_tendencies(_fp(th), _fp(p), _fp(rho), _fp(qv), _fp(qc), _fp(qr), nx, ny, nz,
-                                                 ctypes.c_double(dz), ctypes.c_double(dt), dom,
-                                                 *[_fp(o) for o in out]))
+        lib = str(backend).encode() if backend is not None else None
+        self._rc(self.lib.ref_backend_kessler_tendencies(lib, _fp(th), _fp(p), _fp(rho), _fp(qv), _fp(qc), _fp(qr),
+                                                         nx, ny, nz, ctypes.c_double(dz), ctypes.c_double(dt), dom,
+                                                         *[_fp(o) for o in out]))
         return out
 
     def acoustic_boundaries(self, st, grid, bc, dt_small=0.0):

@@ -21,6 +21,9 @@
 //                           on a stationary flat level with moisture and Kessler loading
 //   ref_kessler_tendencies  KesslerScheme::compute_tendencies
 //                           (src/microphysics/schemes/kessler/kessler.cpp:103-520)
+//   ref_backend_kessler_tendencies  the same scheme on its device route through a
+//                           loaded backend (kessler.cpp:152-300: the Kessler pointwise
+//                           and sedimentation dispatches)
 //   ref_acoustic_boundaries CartesianCGridBCScheme::apply_acoustic
 //                           (boundary_conditions_cartesian_cgrid.cpp:141-236)
 //   ref_eos_projection      tmv::dynamics_eos::apply_pressure_projection
@@ -467,13 +470,26 @@ int ref_scalar_transport(float** q, const int* positive_definite, int n_scalars,
 }
 
 // Kessler warm-rain tendencies (dtheta, dqv, dqc, dqr) over the cell domain
-// {i0, i1, j0, j1, k0, k1} with uniform vertical spacing dz.
-int ref_kessler_tendencies(const float* theta, const float* p, const float* rho, const float* qv, const float* qc,
-                           const float* qr, int nx, int ny, int nz, double dz, double dt, const int* domain,
-                           float* dth, float* dqv, float* dqc, float* dqr)
+// {i0, i1, j0, j1, k0, k1} with uniform vertical spacing dz: the scheme's CPU
+// route, or (library given) its device route through that library's
+// ComputeBackend (kessler.cpp:152-300: the pointwise and sedimentation
+// dispatches, the scheme throwing rather than falling back).
+int ref_backend_kessler_tendencies(const char* library, const float* theta, const float* p, const float* rho,
+                                   const float* qv, const float* qc, const float* qr, int nx, int ny, int nz,
+                                   double dz, double dt, const int* domain, float* dth, float* dqv, float* dqc,
+                                   float* dqr)
 {
     try
     {
+        ComputeBackendRuntimeState runtime;
+        if (library)
+        {
+            runtime.backend = load_backend(library);
+            std::string err;
+            if (!runtime.backend->initialize(err)) return fail(err.c_str());
+            runtime.active_kind = ComputeBackendKind::Vulkan;  // any accelerator kind
+            runtime.requested_kind = runtime.active_kind;
+        }
         Field3D fth, fp, frho, fqv, fqc, fqr;
         to_field(fth, theta, nx, ny, nz);
         to_field(fp, p, nx, ny, nz);
@@ -490,6 +506,11 @@ int ref_kessler_tendencies(const float* theta, const float* p, const float* rho,
         d.j_begin = domain[2]; d.j_end = domain[3];
         d.k_begin = domain[4]; d.k_end = domain[5];
         scheme.set_physical_cell_domain(nx, ny, nz, d);
+        if (library)
+        {
+            scheme.bind_execution_owners(runtime, nullptr);
+            scheme.set_require_native_dispatch(true);
+        }
         scheme.compute_tendencies(fp, fth, frho, fqv, fqc, fqr, zero, zero, zero, zero, dt, o_th, o_qv, o_qc, o_qr,
                                   o_qi, o_qs, o_qg, o_qh);
         from_field(dth, o_th);
@@ -502,6 +523,14 @@ int ref_kessler_tendencies(const float* theta, const float* p, const float* rho,
     {
         return fail(e.what());
     }
+}
+
+int ref_kessler_tendencies(const float* theta, const float* p, const float* rho, const float* qv, const float* qc,
+                           const float* qr, int nx, int ny, int nz, double dz, double dt, const int* domain,
+                           float* dth, float* dqv, float* dqc, float* dqr)
+{
+    return ref_backend_kessler_tendencies(nullptr, theta, p, rho, qv, qc, qr, nx, ny, nz, dz, dt, domain, dth, dqv,
+                                          dqc, dqr);
 }
 
 // EOS pressure re-projection on a level whose p is replaced in place.  With

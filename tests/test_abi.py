@@ -54,6 +54,8 @@ def _c_layout(struct_name, fields, tmp_path):
     ("nimbus_eos_args", cuda.EosArgs),
     ("nimbus_sound_speed_args", cuda.SoundSpeedArgs),
     ("nimbus_slow_apply_args", cuda.SlowApplyArgs),
+    ("nimbus_kessler_pointwise_args", cuda.KesslerPointwiseArgs),
+    ("nimbus_kessler_sedimentation_args", cuda.KesslerSedimentationArgs),
     ("nimbus_boundary_args", cuda.BoundaryArgs),
     ("nimbus_state_relaxation_args", cuda.StateRelaxationArgs),
     ("nimbus_cell_centre_args", cuda.CellCentreArgs),

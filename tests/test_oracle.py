@@ -442,3 +442,25 @@ def test_transport_bridge_route_equals_the_direct_call(o32):
     assert ref.bridge_scalar_transport(qb, [0, 1, 1, 1], *args, top_open=True)
     for x, y in zip(qa, qb):
         np.testing.assert_array_equal(x.view(np.uint32), y.view(np.uint32))
+
+
+def test_kessler_device_restatement_fp32_floor():
+    """The device-route Kessler operators' FP64 statement against an FP32
+    evaluation of the same sequence (numpy, IEEE single): the FP32 floor the
+    CUDA operators' tolerances are set above (6e-6 of each field's scale for
+    the pointwise operator, 3e-7 for the fallout)."""
+    from oracle.kessler_device import kessler_pointwise, kessler_sedimentation
+    from tests.test_kessler_dispatch_gpu import PARAMS, VT_CAP, kessler_inputs
+
+    st = kessler_inputs((24, 20, 30), 1)
+    dom = (1, 23, 1, 19, 0, 30)
+    args = [PARAMS[k] for k in ("qc0", "c_auto", "c_accr", "evaporation_efficiency", "lv_cp", "t0", "dt")]
+    ins = [st[k] for k in ("T", "p", "qv", "qc", "qr", "rho")]
+    f64 = kessler_pointwise(*ins, dom, *args)
+    f32 = kessler_pointwise(*ins, dom, *args, dtype=np.float32)
+    for a, b in zip(f64, f32):
+        assert np.abs(a - b).max() <= 1e-5 * np.abs(a).max()
+    s64 = kessler_sedimentation(st["qr"], f64[3], dom, 400.0, 20.0, VT_CAP, rho_d=st["rho"])
+    s32 = kessler_sedimentation(st["qr"], f64[3].astype(np.float32), dom, 400.0, 20.0, VT_CAP, rho_d=st["rho"],
+                                dtype=np.float32)
+    assert np.abs(s64 - s32).max() <= 1e-6 * np.abs(s64).max()
