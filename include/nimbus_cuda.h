@@ -413,6 +413,53 @@ typedef struct nimbus_slow_apply_args
 } nimbus_slow_apply_args;
 
 nimbus_status nimbus_cuda_slow_apply(nimbus_cuda_context* ctx, const nimbus_slow_apply_args* a);
+
+/*
+ * The slow-tendency operator of the reference's device route
+ * (CartesianCGrid3DScheme::compute_slow_tendencies, cartesian_cgrid_3d.cpp:835-925,
+ * when the backend supports DynamicsKernelOp::CartesianCgridSlowTendencies):
+ * FP32 fields and spacings, FP32 base profiles (rho0 of at least nz levels;
+ * qv0 when has_moisture; u0/v0 used when wind0_base_len >= nz, else zero),
+ * the host-summed hydrometeor loading, f at grid y = 0 and the beta-plane
+ * df/dy.  Every output is written (zero where the scheme does not act;
+ * drho_dt zero); the three advection outputs come together or not at all.
+ * FP32 arithmetic, the reference's device operator
+ * (vulkan/shaders/compute/dynamics/cartesian_cgrid_slow_tendencies.comp).
+ * Mirrors CartesianCgridSlowTendenciesDispatch (include/compute/dispatch/dynamics.hpp:374-420).
+ */
+typedef struct nimbus_cgrid_slow_tendencies_args
+{
+    const float* u;
+    const float* v;
+    const float* w;
+    const float* rho;
+    const float* p;
+    const float* rho0_base;
+    int rho0_base_len;
+    const float* qv0_base;
+    int qv0_base_len;
+    const float* u0_base;
+    const float* v0_base;
+    int wind0_base_len;
+    const float* qv;
+    const float* loading;
+    float* du_dt;
+    float* dv_dt;
+    float* dw_dt;
+    float* drho_dt;          /* optional */
+    float* dp_dt;
+    int nx, ny, nz;
+    float dx, dy, dz, g, coriolis_f;
+    int has_moisture, has_loading;
+    float* du_advection_dt;  /* optional, all three or none */
+    float* dv_advection_dt;
+    float* dw_advection_dt;
+    float frame_velocity_u, frame_velocity_v, coriolis_beta;
+    int memory;
+    void* stream;
+} nimbus_cgrid_slow_tendencies_args;
+
+nimbus_status nimbus_cuda_cgrid_slow_tendencies(nimbus_cuda_context* ctx, const nimbus_cgrid_slow_tendencies_args* a);
 nimbus_status nimbus_cuda_slow_step(nimbus_cuda_context* ctx, const nimbus_slow_args* a);
 
 /*

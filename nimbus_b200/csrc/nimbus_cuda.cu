@@ -1026,6 +1026,113 @@ nimbus_status nimbus_cuda_kessler_sedimentation(nimbus_cuda_context* ctx, const 
     return NIMBUS_OK;
 }
 
+nimbus_status nimbus_cuda_cgrid_slow_tendencies(nimbus_cuda_context* ctx, const nimbus_cgrid_slow_tendencies_args* a)
+{
+    if (!ctx || !a) return NIMBUS_ERR_INVALID_ARGUMENT;
+    const bool adv = a->du_advection_dt || a->dv_advection_dt || a->dw_advection_dt;
+    const bool winds = a->wind0_base_len >= a->nz;
+    if (!a->u || !a->v || !a->w || !a->rho || !a->p || !a->rho0_base || !a->du_dt || !a->dv_dt || !a->dw_dt ||
+        !a->dp_dt || a->nx < 3 || a->ny < 3 || a->nz < 2 || !cells_fit(a->nx, a->ny, a->nz) ||
+        a->rho0_base_len < a->nz || (a->has_moisture && (!a->qv || !a->qv0_base || a->qv0_base_len < a->nz)) ||
+        (a->has_loading && !a->loading) || (winds && (!a->u0_base || !a->v0_base)) ||
+        (adv && !(a->du_advection_dt && a->dv_advection_dt && a->dw_advection_dt)) || !(a->dx > 0.0f) ||
+        !(a->dy > 0.0f) || !(a->dz > 0.0f))
+        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "invalid slow tendency arguments");
+    if (a->memory != NIMBUS_MEMORY_HOST && a->memory != NIMBUS_MEMORY_DEVICE)
+        return fail(ctx, NIMBUS_ERR_INVALID_ARGUMENT, "unknown memory kind");
+    NB_CUDA(ctx, cudaSetDevice(ctx->device));
+    SlowDispatchParams S{};
+    S.d = Dims{a->nx, a->ny, a->nz};
+    // The operator's FP32 constants, formed as it forms them.
+    S.inv_dx = 1.0f / a->dx;
+    S.inv_dy = 1.0f / a->dy;
+    S.inv_dz = 1.0f / a->dz;
+    S.inv_2dx = 0.5f / a->dx;
+    S.inv_2dy = 0.5f / a->dy;
+    S.inv_2dz = 0.5f / a->dz;
+    const float inv[3] = {S.inv_dx, S.inv_dy, S.inv_dz};
+    for (int q = 0; q < 3; ++q)
+    {
+        S.d6[q] = inv[q] / 6.0f;
+        S.d60[q] = inv[q] / 60.0f;
+    }
+    S.dy = a->dy;
+    S.g = a->g;
+    S.f0 = a->coriolis_f;
+    S.beta = a->coriolis_beta;
+    S.frame_u = a->frame_velocity_u;
+    S.frame_v = a->frame_velocity_v;
+    S.has_moisture = a->has_moisture ? 1 : 0;
+    S.has_loading = a->has_loading ? 1 : 0;
+    S.wind_profiles = winds ? 1 : 0;
+    S.emit_advection = adv ? 1 : 0;
+    const size_t n = static_cast<size_t>(a->nx) * a->ny * a->nz;
+    const int blocks = grid_for(ctx, static_cast<long long>(n));
+    if (a->memory == NIMBUS_MEMORY_DEVICE)
+    {
+        cudaStream_t st = a->stream ? static_cast<cudaStream_t>(a->stream) : ctx->stream;
+        slow_tendencies_dispatch_kernel<<<blocks, kThreads, 0, st>>>(
+            S, a->u, a->v, a->w, a->rho, a->p, a->rho0_base, a->qv0_base, a->u0_base, a->v0_base, a->qv, a->loading,
+            a->du_dt, a->dv_dt, a->dw_dt, a->drho_dt, a->dp_dt, a->du_advection_dt, a->dv_advection_dt,
+            a->dw_advection_dt);
+        NB_CUDA(ctx, cudaGetLastError());
+        ctx->launches += 1;
+        return NIMBUS_OK;
+    }
+    const size_t bytes = n * sizeof(float);
+    const size_t nzb = static_cast<size_t>(a->nz) * sizeof(float);
+    float *u, *v, *w, *rho, *p, *prof, *qv = nullptr, *load = nullptr, *out, *advo = nullptr;
+    NB_TRY(ensure(ctx, kU, n, &u));
+    NB_TRY(ensure(ctx, kV, n, &v));
+    NB_TRY(ensure(ctx, kW, n, &w));
+    NB_TRY(ensure(ctx, kRho, n, &rho));
+    NB_TRY(ensure(ctx, kP, n, &p));
+    NB_TRY(ensure(ctx, kRelaxTables, 4 * static_cast<size_t>(a->nz), &prof));
+    NB_TRY(ensure(ctx, kSlowK1, 4 * n, &out));
+    NB_TRY(upload(ctx, u, a->u, bytes));
+    NB_TRY(upload(ctx, v, a->v, bytes));
+    NB_TRY(upload(ctx, w, a->w, bytes));
+    NB_TRY(upload(ctx, rho, a->rho, bytes));
+    NB_TRY(upload(ctx, p, a->p, bytes));
+    NB_TRY(upload(ctx, prof, a->rho0_base, nzb));
+    if (a->has_moisture)
+    {
+        NB_TRY(ensure(ctx, kQv, n, &qv));
+        NB_TRY(upload(ctx, qv, a->qv, bytes));
+        NB_TRY(upload(ctx, prof + a->nz, a->qv0_base, nzb));
+    }
+    if (winds)
+    {
+        NB_TRY(upload(ctx, prof + 2 * static_cast<size_t>(a->nz), a->u0_base, nzb));
+        NB_TRY(upload(ctx, prof + 3 * static_cast<size_t>(a->nz), a->v0_base, nzb));
+    }
+    if (a->has_loading)
+    {
+        NB_TRY(ensure(ctx, kQc, n, &load));
+        NB_TRY(upload(ctx, load, a->loading, bytes));
+    }
+    if (adv) NB_TRY(ensure(ctx, kSlowStar, 3 * n, &advo));
+    slow_tendencies_dispatch_kernel<<<blocks, kThreads, 0, ctx->stream>>>(
+        S, u, v, w, rho, p, prof, prof + a->nz, prof + 2 * static_cast<size_t>(a->nz),
+        prof + 3 * static_cast<size_t>(a->nz), qv, load, out, out + n, out + 2 * n, nullptr, out + 3 * n,
+        adv ? advo : nullptr, adv ? advo + n : nullptr, adv ? advo + 2 * n : nullptr);
+    NB_CUDA(ctx, cudaGetLastError());
+    ctx->launches += 1;
+    NB_TRY(download(ctx, a->du_dt, out, bytes));
+    NB_TRY(download(ctx, a->dv_dt, out + n, bytes));
+    NB_TRY(download(ctx, a->dw_dt, out + 2 * n, bytes));
+    NB_TRY(download(ctx, a->dp_dt, out + 3 * n, bytes));
+    if (adv)
+    {
+        NB_TRY(download(ctx, a->du_advection_dt, advo, bytes));
+        NB_TRY(download(ctx, a->dv_advection_dt, advo + n, bytes));
+        NB_TRY(download(ctx, a->dw_advection_dt, advo + 2 * n, bytes));
+    }
+    NB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (a->drho_dt) std::memset(a->drho_dt, 0, bytes);
+    return NIMBUS_OK;
+}
+
 nimbus_status nimbus_cuda_max_sound_speed(nimbus_cuda_context* ctx, nimbus_sound_speed_args* a)
 {
     if (!ctx || !a) return NIMBUS_ERR_INVALID_ARGUMENT;

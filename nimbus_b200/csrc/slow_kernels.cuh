@@ -477,4 +477,125 @@ static __global__ void __launch_bounds__(256) slow_correct_kernel(
                                   p, tu_out, tv_out, tw_out, tp_out, c);
 }
 
+// ---- The slow-tendency operator of the device route ------------------------
+//
+// CartesianCGrid3DScheme::compute_slow_tendencies (cartesian_cgrid_3d.cpp:835-925)
+// hands a supporting backend dispatch_cartesian_cgrid_slow_tendencies: FP32
+// fields, FP32 base profiles (rho0, qv0, u0, v0 -- the wind profiles one zero
+// when the sounding has none), the host-summed hydrometeor loading, FP32
+// spacings, f at grid y = 0 and the beta-plane df/dy.  The operator's
+// arithmetic is the reference's device form of the scheme
+// (vulkan/shaders/compute/dynamics/cartesian_cgrid_slow_tendencies.comp:139-391):
+// the same upwind-biased momentum advection and centred pressure advection
+// as the CPU route, in FP32, every output written (zero where the scheme
+// does not act; drho_dt is zero on this path).
+struct SlowDispatchParams
+{
+    Dims d;
+    float inv_dx, inv_dy, inv_dz, inv_2dx, inv_2dy, inv_2dz;
+    float d6[3], d60[3];  // inv_d / 6 and inv_d / 60 per axis, as the operator forms them
+    float dy, g, f0, beta, frame_u, frame_v;
+    int has_moisture, has_loading, wind_profiles, emit_advection;
+};
+
+static __global__ void __launch_bounds__(256) slow_tendencies_dispatch_kernel(
+    SlowDispatchParams S, const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w,
+    const float* __restrict__ rho, const float* __restrict__ p, const float* __restrict__ rho0,
+    const float* __restrict__ qv0, const float* __restrict__ u0, const float* __restrict__ v0,
+    const float* __restrict__ qv, const float* __restrict__ loading, float* __restrict__ du_dt,
+    float* __restrict__ dv_dt, float* __restrict__ dw_dt, float* __restrict__ drho_dt, float* __restrict__ dp_dt,
+    float* __restrict__ du_adv, float* __restrict__ dv_adv, float* __restrict__ dw_adv)
+{
+    const Dims d = S.d;
+    const int n = d.cells(), sx = d.sx(), sy = d.sy();
+    auto clean = [](float t) { return isfinite(t) ? t : 0.0f; };
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+    {
+        int i, j, k;
+        decompose(d, c, i, j, k);
+        float du = 0.0f, dv = 0.0f, dw = 0.0f, dp = 0.0f, au = 0.0f, av = 0.0f, aw = 0.0f;
+        if (i >= 1 && i <= d.nx - 2 && j >= 1 && j <= d.ny - 2 && k <= d.nz - 2)
+        {
+            const PlanarState X{u + c, v + c, w + c, p + c};
+            const float u0k = S.wind_profiles ? u0[k] : 0.0f, v0k = S.wind_profiles ? v0[k] : 0.0f;
+            // Advecting winds at the x-, y- and z-faces.
+            const float ux = X.U(0);
+            const float uy_x = 0.25f * (X.V(-sy) + X.V(0) + X.V(sx - sy) + X.V(sx));
+            const float w_x = (k == 0) ? 0.25f * (X.W(0) + X.W(sx))
+                                       : 0.25f * (X.W(-1) + X.W(0) + X.W(sx - 1) + X.W(sx));
+            const float vy = X.V(0);
+            const float ux_y = 0.25f * (X.U(-sx) + X.U(0) + X.U(sy - sx) + X.U(sy));
+            const float w_y = (k == 0) ? 0.25f * (X.W(0) + X.W(sy))
+                                       : 0.25f * (X.W(-1) + X.W(0) + X.W(sy - 1) + X.W(sy));
+            const float wz = X.W(0);
+            const float ux_w = 0.25f * (X.U(-sx) + X.U(0) + X.U(1 - sx) + X.U(1));
+            const float uy_w = 0.25f * (X.V(-sy) + X.V(0) + X.V(1 - sy) + X.V(1));
+            float dxu, dxv, dxw, dyu, dyv, dyw, dzu, dzv, dzw;
+            upwind3<float>(X, sx, i, d.nx, ux, ux_y, ux_w, S.inv_dx, S.d6[0], S.d60[0], dxu, dxv, dxw);
+            upwind3<float>(X, sy, j, d.ny, uy_x, vy, uy_w, S.inv_dy, S.d6[1], S.d60[1], dyu, dyv, dyw);
+            if (k == 0)
+            {
+                dzu = (w_x >= 0.0f) ? 0.0f : (X.U(1) - ux) * S.inv_dz;
+                dzv = (w_y >= 0.0f) ? 0.0f : (X.V(1) - vy) * S.inv_dz;
+                dzw = (wz >= 0.0f) ? X.W(0) * S.inv_dz : (X.W(1) - X.W(0)) * S.inv_dz;
+            }
+            else upwind3<float>(X, 1, k, d.nz, w_x, w_y, wz, S.inv_dz, S.d6[2], S.d60[2], dzu, dzv, dzw);
+            // du at the x-face
+            au = -(ux - S.frame_u) * dxu - (uy_x - S.frame_v) * dyu - w_x * dzu;
+            float cor_x = S.f0 * (uy_x - v0k);
+            if (S.beta != 0.0f)
+            {
+                const float f_lo = S.f0 + S.beta * ((float)j + 0.25f) * S.dy;
+                const float f_hi = S.f0 + S.beta * ((float)j + 0.75f) * S.dy;
+                cor_x = 0.25f * (f_lo * (X.V(-sy) + X.V(sx - sy) - 2.0f * v0k) +
+                                 f_hi * (X.V(0) + X.V(sx) - 2.0f * v0k));
+            }
+            du = au + cor_x;
+            // dv at the y-face
+            av = -(ux_y - S.frame_u) * dxv - (vy - S.frame_v) * dyv - w_y * dzv;
+            float cor_y = S.f0 * (ux_y - u0k);
+            if (S.beta != 0.0f)
+            {
+                const float f_lo = S.f0 + S.beta * ((float)j + 0.75f) * S.dy;
+                const float f_hi = S.f0 + S.beta * ((float)j + 1.25f) * S.dy;
+                cor_y = 0.25f * (f_lo * (X.U(-sx) + X.U(0) - 2.0f * u0k) + f_hi * (X.U(sy - sx) + X.U(sy) - 2.0f * u0k));
+            }
+            dv = av - cor_y;
+            // dw at the z-face: advection, buoyancy, vapour and loading
+            aw = -(ux_w - S.frame_u) * dxw - (uy_w - S.frame_v) * dyw - wz * dzw;
+            const float rho_face = 0.5f * (rho[c] + rho[c + 1]);
+            const float rho_safe = (isfinite(rho_face) && rho_face > 1.0e-6f) ? rho_face : 1.0f;
+            const float rho0_face = 0.5f * (rho0[k] + rho0[k + 1]);
+            const float buoyancy = -S.g * (rho_face - rho0_face) / rho_safe;
+            float moisture = 0.0f, load = 0.0f;
+            if (S.has_moisture)
+                moisture = S.g * 0.608f * (0.5f * (qv[c] + qv[c + 1]) - 0.5f * (qv0[k] + qv0[k + 1]));
+            if (S.has_loading) load = -S.g * 0.5f * (loading[c] + loading[c + 1]);
+            dw = aw + buoyancy + moisture + load;
+            // dp at the cell centre (centred advection), levels 1 .. nz-2
+            if (k >= 1)
+            {
+                const float uc = 0.5f * (X.U(0) + X.U(-sx));
+                const float vc = 0.5f * (X.V(0) + X.V(-sy));
+                const float wc = 0.5f * (X.W(0) + X.W(-1));
+                const float dpdx = (X.P(sx) - X.P(-sx)) * S.inv_2dx;
+                const float dpdy = (X.P(sy) - X.P(-sy)) * S.inv_2dy;
+                const float dpdz = (X.P(1) - X.P(-1)) * S.inv_2dz;
+                dp = -(uc - S.frame_u) * dpdx - (vc - S.frame_v) * dpdy - wc * dpdz;
+            }
+        }
+        du_dt[c] = clean(du);
+        dv_dt[c] = clean(dv);
+        dw_dt[c] = clean(dw);
+        dp_dt[c] = clean(dp);
+        if (drho_dt) drho_dt[c] = 0.0f;
+        if (S.emit_advection)
+        {
+            du_adv[c] = clean(au);
+            dv_adv[c] = clean(av);
+            dw_adv[c] = clean(aw);
+        }
+    }
+}
+
 }  // namespace nimbus

@@ -197,6 +197,21 @@ class KesslerSedimentationArgs(ctypes.Structure):
     ]
 
 
+class CgridSlowTendenciesArgs(ctypes.Structure):
+    _fields_ = [
+        *[(k, _fp) for k in ("u", "v", "w", "rho", "p", "rho0_base")], ("rho0_base_len", ctypes.c_int),
+        ("qv0_base", _fp), ("qv0_base_len", ctypes.c_int), ("u0_base", _fp), ("v0_base", _fp),
+        ("wind0_base_len", ctypes.c_int),
+        *[(k, _fp) for k in ("qv", "loading", "du_dt", "dv_dt", "dw_dt", "drho_dt", "dp_dt")],
+        *[(k, ctypes.c_int) for k in ("nx", "ny", "nz")],
+        *[(k, ctypes.c_float) for k in ("dx", "dy", "dz", "g", "coriolis_f")],
+        ("has_moisture", ctypes.c_int), ("has_loading", ctypes.c_int),
+        *[(k, _fp) for k in ("du_advection_dt", "dv_advection_dt", "dw_advection_dt")],
+        *[(k, ctypes.c_float) for k in ("frame_velocity_u", "frame_velocity_v", "coriolis_beta")],
+        ("memory", ctypes.c_int), ("stream", ctypes.c_void_p),
+    ]
+
+
 TUNING_CANDIDATES = 32
 
 
@@ -300,7 +315,7 @@ EXPORTED_SYMBOLS = (
     "nimbus_cuda_engine_acoustic_form", "nimbus_cuda_engine_member_status_async", "nimbus_cuda_engine_graph_builds",
     "nimbus_cuda_engine_set_pass_forms", "nimbus_cuda_engine_pass_forms",
     "nimbus_cuda_engine_autotune", "nimbus_cuda_slow_apply", "nimbus_cuda_kessler_pointwise",
-    "nimbus_cuda_kessler_sedimentation",
+    "nimbus_cuda_kessler_sedimentation", "nimbus_cuda_cgrid_slow_tendencies",
 )
 ACOUSTIC_FORM_NAMES = {0: "member-table", 1: "constant-bank", 2: "marching", 3: "constant-bank, two cells per thread",
                        4: "bulk-staged tiles"}
@@ -408,6 +423,7 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
     lib.nimbus_cuda_slow_apply.argtypes = [vp, ctypes.POINTER(SlowApplyArgs)]
     lib.nimbus_cuda_kessler_pointwise.argtypes = [vp, ctypes.POINTER(KesslerPointwiseArgs)]
     lib.nimbus_cuda_kessler_sedimentation.argtypes = [vp, ctypes.POINTER(KesslerSedimentationArgs)]
+    lib.nimbus_cuda_cgrid_slow_tendencies.argtypes = [vp, ctypes.POINTER(CgridSlowTendenciesArgs)]
     lib.nimbus_cuda_engine_graph_builds.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64),
                                                     ctypes.POINTER(ctypes.c_uint64)]
     lib.nimbus_cuda_engine_acoustic_form.argtypes = [vp]
@@ -605,6 +621,39 @@ class Context:
         a.dz, a.vt_max_rain, a.vt_cap, a.dt_step = dz, vt_max, vt_cap, dt
         a.memory = MEMORY_DEVICE if hasattr(qr, "data_ptr") else MEMORY_HOST
         self.check(self.lib.nimbus_cuda_kessler_sedimentation(self.handle, ctypes.byref(a)))
+
+    def cgrid_slow_tendencies(self, st, profiles, outs, grid, g=9.81, coriolis_f=0.0, beta=0.0, loading=None,
+                              advection=None, frame=(0.0, 0.0)) -> None:
+        """The device route's slow-tendency operator.  st: u, v, w, rho, p
+        (and qv for moisture); profiles: FP32 rho0 (and qv0, u0, v0); outs:
+        du, dv, dw, drho (or None), dp; advection: three outputs or None.
+        Host float32 arrays or device tensors."""
+        a = CgridSlowTendenciesArgs()
+        a._keep = (dict(st), dict(profiles), list(outs), loading, advection)
+        for k in ("u", "v", "w", "rho", "p"):
+            setattr(a, k, _f(st[k]))
+        nz = int(st["u"].shape[2])
+        a.rho0_base, a.rho0_base_len = _f(profiles["rho0"]), int(profiles["rho0"].shape[0])
+        moist = st.get("qv") is not None and profiles.get("qv0") is not None
+        if moist:
+            a.qv, a.qv0_base, a.qv0_base_len = _f(st["qv"]), _f(profiles["qv0"]), int(profiles["qv0"].shape[0])
+        if profiles.get("u0") is not None:
+            a.u0_base, a.v0_base = _f(profiles["u0"]), _f(profiles["v0"])
+            a.wind0_base_len = int(profiles["u0"].shape[0])
+        if loading is not None:
+            a.loading = _f(loading)
+        for name, x in zip(("du_dt", "dv_dt", "dw_dt", "drho_dt", "dp_dt"), outs):
+            setattr(a, name, _f(x) if x is not None else None)
+        if advection is not None:
+            a.du_advection_dt, a.dv_advection_dt, a.dw_advection_dt = (_f(x) for x in advection)
+        a.nx, a.ny, a.nz = (int(x) for x in st["u"].shape)
+        a.dx, a.dy, a.dz = (float(x) for x in grid)
+        a.g, a.coriolis_f, a.coriolis_beta = g, coriolis_f, beta
+        a.has_moisture, a.has_loading = int(moist), int(loading is not None)
+        a.frame_velocity_u, a.frame_velocity_v = frame
+        a.memory = MEMORY_DEVICE if hasattr(st["u"], "data_ptr") else MEMORY_HOST
+        assert nz >= 2
+        self.check(self.lib.nimbus_cuda_cgrid_slow_tendencies(self.handle, ctypes.byref(a)))
 
     def resolve_substep_count(self, dt, c_max, min_spacing, requested=0) -> int:
         """The reference's substep-count rule (split_explicit.cpp:67-170)."""

@@ -31,6 +31,10 @@
 //       retained acoustic context (advection_batch.cpp's route): FP64 spacings
 //       from the level's state view and dt_step_host, so the result is the CPU
 //       backend's bit for bit; see the dispatch for what it declines.
+//   CartesianCgridSlowTendencies  the scheme's device route for the slow
+//       tendencies (cartesian_cgrid_3d.cpp:835-925), FP32 as the reference's
+//       device operator computes it: within the reference's own stencil
+//       parity tier of the CPU route.
 //   KesslerPointwise / KesslerSedimentation  the two operators of
 //       KesslerScheme's device route (kessler.cpp:152-300), FP32 as the
 //       reference's device operators compute them; the scheme's result then
@@ -228,7 +232,53 @@ public:
     {
         return op == DynamicsKernelOp::AcousticSubstepFusedCartesianCgrid ||
                op == DynamicsKernelOp::AcousticSubstepsBatchedCartesianCgrid ||
-               op == DynamicsKernelOp::SlowApply || op == DynamicsKernelOp::StateRelaxationCartesian;
+               op == DynamicsKernelOp::SlowApply || op == DynamicsKernelOp::StateRelaxationCartesian ||
+               op == DynamicsKernelOp::CartesianCgridSlowTendencies;
+    }
+
+    // The scheme's device route for the slow tendencies (FP32 operator; the
+    // residency hint is moot: every dispatch uploads what it is given).
+    bool dispatch_cartesian_cgrid_slow_tendencies(const CartesianCgridSlowTendenciesDispatch& d) override
+    {
+        if (!ctx_) return false;
+        nimbus_cgrid_slow_tendencies_args a{};
+        a.u = d.u_data;
+        a.v = d.v_data;
+        a.w = d.w_data;
+        a.rho = d.rho_data;
+        a.p = d.p_data;
+        a.rho0_base = d.rho0_base_data;
+        a.rho0_base_len = d.rho0_base_len;
+        a.qv0_base = d.qv0_base_data;
+        a.qv0_base_len = d.qv0_base_len;
+        a.u0_base = d.u0_base_data;
+        a.v0_base = d.v0_base_data;
+        a.wind0_base_len = d.wind0_base_len;
+        a.qv = d.qv_data;
+        a.loading = d.loading_data;
+        a.du_dt = d.du_dt_data;
+        a.dv_dt = d.dv_dt_data;
+        a.dw_dt = d.dw_dt_data;
+        a.drho_dt = d.drho_dt_data;
+        a.dp_dt = d.dp_dt_data;
+        a.nx = d.nr;
+        a.ny = d.nth;
+        a.nz = d.nz;
+        a.dx = d.dx;
+        a.dy = d.dy;
+        a.dz = d.dz;
+        a.g = d.g;
+        a.coriolis_f = d.coriolis_f_val;
+        a.has_moisture = d.has_moisture ? 1 : 0;
+        a.has_loading = d.has_loading ? 1 : 0;
+        a.du_advection_dt = d.du_advection_dt_data;
+        a.dv_advection_dt = d.dv_advection_dt_data;
+        a.dw_advection_dt = d.dw_advection_dt_data;
+        a.frame_velocity_u = d.frame_velocity_u_ms;
+        a.frame_velocity_v = d.frame_velocity_v_ms;
+        a.coriolis_beta = d.coriolis_beta;
+        a.memory = NIMBUS_MEMORY_HOST;
+        return count(nimbus_cuda_cgrid_slow_tendencies(ctx_, &a));
     }
 
     // apply_slow_tendencies_cpu's arithmetic on the dispatched fields (the

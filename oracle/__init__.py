@@ -683,16 +683,20 @@ class ReferenceHarness:
             self.large_step(st, base, grid, dt, n, bc, coriolis_f=coriolis_f)
         return counts
 
-    def slow_tendencies(self, st, base, grid, coriolis_f=0.0, moist=True):
+    def slow_tendencies(self, st, base, grid, coriolis_f=0.0, moist=True, beta=0.0, backend=None):
+        """CartesianCGrid3DScheme::compute_slow_tendencies: the CPU route, or
+        (backend: a shared library's path) the scheme's device route through
+        that library's ComputeBackend.  Returns du, dv, dw, dp."""
         u, v, w, rho, p, th = (st[k] for k in ("u", "v", "w", "rho", "p", "theta"))
         qv, qc, qr = _slow_inputs(st, base, moist)
         nx, ny, nz = u.shape
         out = [np.zeros_like(u) for _ in range(4)]
-        self._rc(self.lib.ref_slow_tendencies(
-            _fp(u), _fp(v), _fp(w), _fp(rho), _fp(p), _fp(th), _opt(qv), _opt(qc), _opt(qr), _fp(base["rho0"]),
+        lib = str(backend).encode() if backend is not None else None
+        self._rc(self.lib.ref_backend_slow_tendencies(
+            lib, _fp(u), _fp(v), _fp(w), _fp(rho), _fp(p), _fp(th), _opt(qv), _opt(qc), _opt(qr), _fp(base["rho0"]),
             _fp(base["p0"]), _fp(base["qv0"]) if moist else None, _fp(base["u0"]), _fp(base["v0"]),
             _fp(base["theta0"]), nx, ny, nz, ctypes.c_double(grid[0]), ctypes.c_double(grid[1]),
-            ctypes.c_double(grid[2]), ctypes.c_double(coriolis_f), *[_fp(o) for o in out]))
+            ctypes.c_double(grid[2]), ctypes.c_double(coriolis_f), ctypes.c_double(beta), *[_fp(o) for o in out]))
         return out
 
     def scalar_transport(self, qs, pd, u, v, w, rho_end, rho_begin, mfx, mfy, mfz, dt, grid,

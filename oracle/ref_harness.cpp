@@ -19,6 +19,8 @@
 //   ref_slow_tendencies     CartesianCGrid3DScheme::compute_slow_tendencies
 //                           (src/dynamics/schemes/klemp_wilhelmson_split/cartesian_cgrid_3d.cpp:724-1416)
 //                           on a stationary flat level with moisture and Kessler loading
+//   ref_backend_slow_tendencies  the same on the scheme's device route through a
+//                           loaded backend (cartesian_cgrid_3d.cpp:835-925)
 //   ref_kessler_tendencies  KesslerScheme::compute_tendencies
 //                           (src/microphysics/schemes/kessler/kessler.cpp:103-520)
 //   ref_backend_kessler_tendencies  the same scheme on its device route through a
@@ -90,6 +92,7 @@
 #include "numerics/runtime.hpp"
 #include "compute/bridge/advection.hpp"
 #include "compute/bridge/dynamics.hpp"
+#include "dynamics/coriolis.hpp"
 #include "numerics/time_stepping/schemes/split_explicit/split_explicit.hpp"
 
 #include <dlfcn.h>
@@ -576,15 +579,30 @@ int ref_eos_projection(const float* rho, const float* theta, float* p, const flo
 // Slow tendencies (du, dv, dw at faces; dp at centres) of the reference's
 // C-grid scheme.  qv/qc/qr may be null (dry / no loading); base profiles are
 // FP64 columns of length nz.
-int ref_slow_tendencies(const float* u, const float* v, const float* w, const float* rho, const float* p,
-                        const float* theta, const float* qv, const float* qc, const float* qr, const double* rho0,
-                        const double* p0b, const double* qv0, const double* u0, const double* v0,
-                        const double* theta0, int nx, int ny, int nz, double dx, double dy, double dz,
-                        double coriolis_f, float* du, float* dv, float* dw, float* dp)
+// The slow tendencies on the CPU route, or (library given) on the scheme's
+// device route through that library's ComputeBackend
+// (cartesian_cgrid_3d.cpp:835-925, dispatch_cartesian_cgrid_slow_tendencies);
+// beta != 0 sets a beta-plane Coriolis profile (f at grid y = 0, df/dy).
+int ref_backend_slow_tendencies(const char* library, const float* u, const float* v, const float* w,
+                                const float* rho, const float* p, const float* theta, const float* qv,
+                                const float* qc, const float* qr, const double* rho0, const double* p0b,
+                                const double* qv0, const double* u0, const double* v0, const double* theta0, int nx,
+                                int ny, int nz, double dx, double dy, double dz, double coriolis_f, double beta,
+                                float* du, float* dv, float* dw, float* dp)
 {
     try
     {
+        ComputeBackendRuntimeState runtime;
+        if (library)
+        {
+            runtime.backend = load_backend(library);
+            std::string err;
+            if (!runtime.backend->initialize(err)) return fail(err.c_str());
+            runtime.active_kind = ComputeBackendKind::Vulkan;  // any accelerator kind
+            runtime.requested_kind = runtime.active_kind;
+        }
         Level L(nx, ny, nz, dx, dy, dz, 1.0);
+        if (library) L.view.compute_runtime = &runtime;
         auto& f = L.storage.fields;
         to_field(f.u, u, nx, ny, nz);
         to_field(f.v, v, nx, ny, nz);
@@ -608,9 +626,12 @@ int ref_slow_tendencies(const float* u, const float* v, const float* w, const fl
         if (theta0) b.theta0.assign(theta0, theta0 + nz);
         L.storage.coriolis_f = coriolis_f;
         tmv::CartesianCGrid3DScheme scheme(L.view);
+        if (beta != 0.0) scheme.set_coriolis_profile(tmv::CartesianCoriolisProfile{coriolis_f, beta});
         Field3D fdu(nx, ny, nz, 0.0f), fdv(nx, ny, nz, 0.0f), fdw(nx, ny, nz, 0.0f), fdr(nx, ny, nz, 0.0f),
             fdp(nx, ny, nz, 0.0f);
         scheme.compute_slow_tendencies(f.u, f.v, f.w, f.rho, f.p, f.theta, 1.0, fdu, fdv, fdw, fdr, fdp, nullptr);
+        if (library && runtime.backend->successful_dispatch_count() == 0)
+            return fail("the scheme did not take its device route");
         from_field(du, fdu);
         from_field(dv, fdv);
         from_field(dw, fdw);
@@ -621,6 +642,16 @@ int ref_slow_tendencies(const float* u, const float* v, const float* w, const fl
     {
         return fail(e.what());
     }
+}
+
+int ref_slow_tendencies(const float* u, const float* v, const float* w, const float* rho, const float* p,
+                        const float* theta, const float* qv, const float* qc, const float* qr, const double* rho0,
+                        const double* p0b, const double* qv0, const double* u0, const double* v0,
+                        const double* theta0, int nx, int ny, int nz, double dx, double dy, double dz,
+                        double coriolis_f, float* du, float* dv, float* dw, float* dp)
+{
+    return ref_backend_slow_tendencies(nullptr, u, v, w, rho, p, theta, qv, qc, qr, rho0, p0b, qv0, u0, v0, theta0,
+                                       nx, ny, nz, dx, dy, dz, coriolis_f, 0.0, du, dv, dw, dp);
 }
 
 // The end-of-step sponge on a flat C-grid level: the upper Rayleigh sponge

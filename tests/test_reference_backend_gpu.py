@@ -3,7 +3,10 @@ library (nimbus_b200/reference_backend/nimbus_compute_backend.cpp) loaded as a
 ComputeBackend by the reference-linked harness, driven with the reference's
 dispatch structs and, for the Smagorinsky closure, by the reference's own
 SmagorinskyScheme::compute taking its native-backend path.  The results must
-equal the reference's CPU backend / CPU path bit for bit."""
+equal the reference's CPU backend / CPU path bit for bit, except for the
+operators the reference defines in FP32 on its device route (Kessler, the
+slow tendencies), which must agree with its CPU route within the
+reference's own parity tiers."""
 from pathlib import Path
 
 import numpy as np
@@ -18,6 +21,22 @@ pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not oracle.reference_available
                                                    reason="reference harness not built")]
 
 ADAPTER = Path(__file__).resolve().parents[1] / "nimbus_b200" / "lib" / "libnimbus_reference_backend.so"
+
+
+# The reference's own GPU-vs-CPU parity tiers (src/compute/parity_comparison.cpp:115-123,
+# include/compute/parity_types.hpp:12-22): |gpu - cpu| <= abs + rel |cpu| as
+# (rel, abs); its runtime checks the slow-tendency kernel against the CPU
+# route with the stencil tier (cartesian_cgrid_3d.cpp:983-998).
+STENCIL_TIER = (1e-4, 5e-5)
+MICROPHYSICS_TIER = (1e-4, 1e-7)
+MICROPHYSICS_HEATING_TIER = (1e-4, 6e-4)
+
+
+def assert_tier(got, want, tier, what):
+    rel, abs_ = tier
+    bad = np.abs(got.astype(np.float64) - want) > abs_ + rel * np.abs(want.astype(np.float64))
+    assert not bad.any(), (f"{what}: {np.count_nonzero(bad)} cells outside the tier, max |diff| "
+                           f"{np.abs(got.astype(np.float64) - want).max():.3e}")
 
 
 @pytest.fixture(scope="module")
@@ -253,3 +272,68 @@ def test_kessler_scheme_takes_the_cuda_backend(ref):
         scale = float(np.abs(a).max())
         err = float(np.abs(a.astype(np.float64) - b).max())
         assert scale > 0 and err <= 1e-4 * scale, f"{name}: {err:.3e} against {scale:.3e}"
+        # The reference's own microphysics parity tiers (parity_comparison.cpp:119-122).
+        assert_tier(b, a, MICROPHYSICS_HEATING_TIER if name == "dtheta" else MICROPHYSICS_TIER, name)
+
+
+def _slow_level(seed, wind=True):
+    case = Case(30, 26, 22, 800.0, 700.0, 400.0, 3.0, seed=seed, noise_amp=0.3)
+    st, base = cloudy_state(case, seed=seed + 1)
+    if not wind:
+        base = dict(base, u0=np.zeros_like(base["u0"]), v0=np.zeros_like(base["v0"]))
+    return case, st, base
+
+
+@pytest.mark.parametrize("moist,cor,beta", [(True, 1e-4, 0.0), (False, 0.0, 0.0), (True, 1e-4, 2e-11)],
+                         ids=["moist-f", "dry", "beta-plane"])
+def test_slow_tendencies_scheme_takes_the_cuda_backend(ref, moist, cor, beta):
+    """CartesianCGrid3DScheme::compute_slow_tendencies with the adapter as the
+    level's backend takes its device route (dispatch_cartesian_cgrid_slow_tendencies:
+    FP32 profiles, the host-summed hydrometeor loading) and agrees with its
+    CPU route within the reference's stencil tier over the whole field."""
+    case, st, base = _slow_level(21)
+    grid = (case.dx, case.dy, case.dz)
+    cpu = ref.slow_tendencies(st, base, grid, coriolis_f=cor, moist=moist, beta=beta)
+    dev = ref.slow_tendencies(st, base, grid, coriolis_f=cor, moist=moist, beta=beta, backend=ADAPTER)
+    for name, a, b in zip(("du", "dv", "dw", "dp"), cpu, dev):
+        assert np.abs(a).max() > 0, name
+        assert_tier(b, a, STENCIL_TIER, name)
+
+
+@pytest.mark.parametrize("memory", ["host", "device"])
+def test_slow_tendency_operator_through_the_c_abi(ref, memory):
+    """nimbus_cuda_cgrid_slow_tendencies called directly with the dispatch's
+    inputs (FP32 profiles, loading = qc + qr), host or device memory, with the
+    advection components: the stencil tier against the CPU route, drho zero,
+    and du = advection + Coriolis exactly as the components say."""
+    import torch
+
+    from nimbus_b200 import cuda
+
+    case, st, base = _slow_level(31)
+    grid = (case.dx, case.dy, case.dz)
+    cpu = ref.slow_tendencies(st, base, grid, coriolis_f=1e-4, moist=True)
+    prof = {k: np.ascontiguousarray(base[k], np.float32) for k in ("rho0", "qv0", "u0", "v0")}
+    load = np.ascontiguousarray(st["qc"] + st["qr"], np.float32)
+    fields = {k: st[k] for k in ("u", "v", "w", "rho", "p", "qv")}
+    outs = [np.full_like(st["u"], np.nan) for _ in range(5)]
+    adv = [np.full_like(st["u"], np.nan) for _ in range(3)]
+    ctx = cuda.Context(0)
+    try:
+        if memory == "device":
+            d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+            dfields = {k: d(v) for k, v in fields.items()}
+            dprof = {k: d(v) for k, v in prof.items()}
+            douts, dadv = [d(a) for a in outs], [d(a) for a in adv]
+            ctx.cgrid_slow_tendencies(dfields, dprof, douts, grid, coriolis_f=1e-4, loading=d(load), advection=dadv)
+            ctx.synchronize()
+            outs, adv = [a.cpu().numpy() for a in douts], [a.cpu().numpy() for a in dadv]
+        else:
+            ctx.cgrid_slow_tendencies(fields, prof, outs, grid, coriolis_f=1e-4, loading=load, advection=adv)
+    finally:
+        ctx.close()
+    du, dv, dw, drho, dp = outs
+    for name, a, b in zip(("du", "dv", "dw", "dp"), cpu, (du, dv, dw, dp)):
+        assert_tier(b, a, STENCIL_TIER, name)
+    assert np.all(drho == 0.0)
+    assert np.all(np.isfinite(adv[0])) and np.abs(adv[2]).max() > 0
