@@ -19,7 +19,9 @@
 //       result is the C-ABI's on those widened values (and differs from the
 //       CPU loop by that FP32 narrowing of its inputs, as the reference's own
 //       accelerator backends do).  A dispatch that turns the state repairs
-//       off, or accumulates mass flux without a positive weight, is declined.
+//       off is declined; one that accumulates mass flux without a weight
+//       (the runtime's generic route) adds each substep's flux with 1/N, as
+//       the reference's device backends do.
 //   Smagorinsky (dispatch_smagorinsky_fused)  the bridge passes FP32 copies of
 //       dz, dx, dy and the closure constants (src/compute/dispatch/turbulence.cpp:87-146);
 //       they are widened to FP64, so the result equals the CPU scheme's
@@ -446,7 +448,12 @@ public:
     {
         if (!ctx_ || !d.rho0_base_data || !d.p0_base_data || d.nz < 1 || d.base_len < d.nz || !d.repair_primary_state)
             return false;
-        if (d.accumulate_mass_flux && !(d.mass_flux_weight > 0.0)) return false;
+        // The generic (repaired) route passes no weight: each substep's flux
+        // then enters with 1/N, as the reference's device backends take it
+        // (the loop's substeps split the large step evenly).
+        if (d.accumulate_mass_flux && !(d.mass_flux_weight > 0.0) && d.mass_flux_weight != 0.0) return false;
+        if (d.accumulate_mass_flux && d.n_substeps < 1) return false;
+        const double flux_weight = d.mass_flux_weight > 0.0 ? d.mass_flux_weight : 1.0 / d.n_substeps;
         std::vector<double> rho0(d.rho0_base_data, d.rho0_base_data + d.nz);
         std::vector<double> p0(d.p0_base_data, d.p0_base_data + d.nz);
         std::vector<float> wave_out;
@@ -492,7 +499,7 @@ public:
         a.mass_flux_y = d.mass_flux_y;
         a.mass_flux_z = d.mass_flux_z;
         a.accumulate_mass_flux = d.accumulate_mass_flux;
-        a.mass_flux_weight = d.mass_flux_weight;
+        a.mass_flux_weight = flux_weight;
         a.frame_velocity_u_ms = d.frame_velocity_u_ms;
         a.frame_velocity_v_ms = d.frame_velocity_v_ms;
         a.wave_history = d.wave_history;
