@@ -58,6 +58,7 @@ def test_reference_program_runs_on_the_cuda_backend_and_passes_its_parity_check(
     kernels = set(re.findall(r"^\S*\s*\[PARITY\] (\w+)\s+\w+\s+(?:pointwise|stencil|microphys|mp-heating)", log,
                              flags=re.M))
     report = "\n".join(line for line in log.splitlines() if "[PARITY]" in line)
+    print(report)
     assert result.group(1) == "PASS", report
     # The device dispatches the run took and the reference replayed.
     for k in ("acoustic_batched_cartesian_cgrid", "cartesian_cgrid_slow_tendencies"):
