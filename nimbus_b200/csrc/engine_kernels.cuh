@@ -145,7 +145,11 @@ __device__ __forceinline__ void for_member_rows(const EngineMember* __restrict__
 // ---- Heun slow step -------------------------------------------------------
 
 template <class Policy>
-static __global__ void __launch_bounds__(256, 4) engine_slow_predict_kernel(const EngineMember* __restrict__ table,
+// Resident CTAs per SM of the slow Heun pair (64 registers at 4).
+#ifndef NIMBUS_SLOW_MINB
+#define NIMBUS_SLOW_MINB 4
+#endif
+static __global__ void __launch_bounds__(256, NIMBUS_SLOW_MINB) engine_slow_predict_kernel(const EngineMember* __restrict__ table,
                                                                   const long long* __restrict__ prefix,
                                                                   long long tiles)
 {
@@ -159,7 +163,7 @@ static __global__ void __launch_bounds__(256, 4) engine_slow_predict_kernel(cons
 }
 
 template <class Policy>
-static __global__ void __launch_bounds__(256, 4) engine_slow_correct_kernel(const EngineMember* __restrict__ table,
+static __global__ void __launch_bounds__(256, NIMBUS_SLOW_MINB) engine_slow_correct_kernel(const EngineMember* __restrict__ table,
                                                                   const long long* __restrict__ prefix,
                                                                   long long tiles)
 {
@@ -883,7 +887,10 @@ static __global__ void engine_swap_kernel(EngineMember* table, int members, int 
 // ---- Transport (every scalar of a cell in one thread) -----------------------
 
 template <bool kFp32>
-static __global__ void __launch_bounds__(256) engine_transport_faces_kernel(const EngineMember* __restrict__ table,
+#ifndef NIMBUS_FACES_MINB
+#define NIMBUS_FACES_MINB 1
+#endif
+static __global__ void __launch_bounds__(256, NIMBUS_FACES_MINB) engine_transport_faces_kernel(const EngineMember* __restrict__ table,
                                                                             const long long* __restrict__ prefix,
                                                                             long long tiles)
 {
