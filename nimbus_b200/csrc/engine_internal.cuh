@@ -101,6 +101,11 @@ using namespace nimbus_host;
 
 constexpr int kEngineBlock = 256;
 
+// The slow Heun pair's constant-bank form (1) or member-table form (0).
+#ifndef NIMBUS_SLOW_CONST
+#define NIMBUS_SLOW_CONST 1
+#endif
+
 int blocks_per_sm(nimbus_engine* e, const void* kernel, int block = kEngineBlock)
 {
     auto it = e->occupancy.find(kernel);
@@ -212,9 +217,40 @@ int enqueue_step(nimbus_engine* e, int lane, cudaStream_t st, int part)
 
     if (part == 0)
     {
-    // Heun slow step (prepare_slow_rk2_tendencies + apply_slow_tendencies).
-    ENGINE_LAUNCH(NIMBUS_KERNEL_SLOW, engine_slow_predict_kernel<Policy>, cells, 1, T, pc, cells);
-    ENGINE_LAUNCH(NIMBUS_KERNEL_SLOW, engine_slow_correct_kernel<Policy>, cells, 1, T, pc, cells);
+    // Heun slow step (prepare_slow_rk2_tendencies + apply_slow_tendencies):
+    // the constant-bank form for lanes of at most kSlowConstMembers members.
+    if (NIMBUS_SLOW_CONST && n <= kSlowConstMembers)
+    {
+        std::unique_ptr<SlowLaunch> sl(new SlowLaunch());
+        const long long* p = e->prefix.data() + L.prefix_first + static_cast<size_t>(kItemCells) * (n + 1);
+        for (int r = 0; r <= n; ++r) sl->prefix[r] = p[r];
+        for (int r = 0; r < n; ++r)
+        {
+            const EngineMember& H = e->slots[static_cast<size_t>(e->order[static_cast<size_t>(L.first + r)])].m;
+            SlowConst& A = sl->m[r];
+            A.S = H.S;
+            A.u = H.u;
+            A.v = H.v;
+            A.w = H.w;
+            A.theta = H.theta;
+            A.qv = H.qv;
+            A.qc = H.qc;
+            A.k1 = reinterpret_cast<float4*>(H.k1);
+            A.xs = reinterpret_cast<float4*>(H.xs);
+            A.q4 = reinterpret_cast<float4*>(H.q4);
+            A.rho0 = H.rho0;
+            A.qv0 = H.qv0;
+            A.u0 = H.u0;
+            A.v0 = H.v0;
+        }
+        ENGINE_LAUNCH(NIMBUS_KERNEL_SLOW, engine_slow_predict_const_kernel<Policy>, cells, 1, *sl, T, cells);
+        ENGINE_LAUNCH(NIMBUS_KERNEL_SLOW, engine_slow_correct_const_kernel<Policy>, cells, 1, *sl, T, cells);
+    }
+    else
+    {
+        ENGINE_LAUNCH(NIMBUS_KERNEL_SLOW, engine_slow_predict_kernel<Policy>, cells, 1, T, pc, cells);
+        ENGINE_LAUNCH(NIMBUS_KERNEL_SLOW, engine_slow_correct_kernel<Policy>, cells, 1, T, pc, cells);
+    }
     // seed_acoustic_radiation: apply_acoustic(0) then the KW78 seed.
     ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_BOUNDARY, engine_bc_we_kernel, tiles_of(e, L, kItemRowsWE, n), 1, T, pwe,
                   tiles_of(e, L, kItemRowsWE, n), 0, 1);

@@ -173,6 +173,64 @@ static __global__ void __launch_bounds__(256, NIMBUS_SLOW_MINB) engine_slow_corr
     });
 }
 
+// The Heun pair with the members' constants in the constant bank (the
+// acoustic passes' reason, below: parameters read from the member table sit
+// in registers, and the pair spilled at 64 registers).  Each lane's launch
+// gets its members' SlowParams and every buffer that does not rotate as one
+// __grid_constant__ parameter; density, pressure and rain, which rotate, are
+// read from the table.
+struct SlowConst
+{
+    SlowParams S;
+    float *u, *v, *w, *theta, *qv, *qc;
+    float4 *k1, *xs, *q4;
+    const double *rho0, *qv0, *u0, *v0;
+};
+
+constexpr int kSlowConstMembers = 64;
+
+struct SlowLaunch
+{
+    long long prefix[kSlowConstMembers + 1];  // first cell tile of each member
+    SlowConst m[kSlowConstMembers];
+};
+static_assert(sizeof(SlowLaunch) <= 32000, "a kernel parameter block holds at most 32764 bytes");
+
+template <class Policy>
+static __global__ void __launch_bounds__(256, NIMBUS_SLOW_MINB) engine_slow_predict_const_kernel(
+    const __grid_constant__ SlowLaunch L, const EngineMember* __restrict__ table, long long tiles)
+{
+    int m = 0;
+    for (long long t = blockIdx.x; t < tiles; t += gridDim.x)
+    {
+        while (t >= L.prefix[m + 1]) ++m;
+        const SlowConst& A = L.m[m];
+        const int c = (int)((t - L.prefix[m]) * blockDim.x) + (int)threadIdx.x;
+        if (c >= A.S.d.cells()) continue;
+        const EngineMember& M = table[m];
+        slow_predict_packed<Policy>(A.S, A.u, A.v, A.w, M.rho, M.p, A.qv, A.qc, M.qr, A.rho0, A.qv0, A.u0, A.v0, A.k1,
+                                    A.xs, c);
+        A.q4[c] = make_float4(A.theta[c], A.qv[c], A.qc[c], M.qr[c]);
+    }
+}
+
+template <class Policy>
+static __global__ void __launch_bounds__(256, NIMBUS_SLOW_MINB) engine_slow_correct_const_kernel(
+    const __grid_constant__ SlowLaunch L, const EngineMember* __restrict__ table, long long tiles)
+{
+    int m = 0;
+    for (long long t = blockIdx.x; t < tiles; t += gridDim.x)
+    {
+        while (t >= L.prefix[m + 1]) ++m;
+        const SlowConst& A = L.m[m];
+        const int c = (int)((t - L.prefix[m]) * blockDim.x) + (int)threadIdx.x;
+        if (c >= A.S.d.cells()) continue;
+        const EngineMember& M = table[m];
+        slow_correct_packed<Policy>(A.S, A.xs, M.rho, A.qv, A.qc, M.qr, A.rho0, A.qv0, A.u0, A.v0, A.k1, A.u, A.v,
+                                    A.w, M.p, c);
+    }
+}
+
 // ---- Boundaries and KW78 seed ---------------------------------------------
 //
 // The density buffer substep s reads (written == false) or writes: substep s
