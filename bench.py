@@ -628,11 +628,11 @@ def run_ours(args):
     if not args.no_autotune:
         ctx.set_precision(precision)
         tuned = run.engine.autotune(steps=2)
-    lanes_used = run.engine.lanes
     stream = torch.cuda.ExternalStream(run.engine.stream, device=f"cuda:{device}")
     for _ in range(max(args.warmup, 3)):
         run.step(1)
     ctx.synchronize()
+    lanes_used = run.engine.lanes  # the lanes the built table uses
     barrier()
     torch.cuda.synchronize()
     launches0 = ctx.kernel_launches

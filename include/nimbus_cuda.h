@@ -1032,12 +1032,12 @@ int nimbus_cuda_engine_lanes(const nimbus_engine* e);
  *   NIMBUS_ACOUSTIC_CONST  one thread per cell, each lane's members' constants
  *                          passed as one kernel parameter (the constant bank),
  *                          only the rotating buffers read from the table
- *                          (default; lanes of more than 64 members fall back
- *                          to the table form);
+ *                          (the continuity pass's default; lanes of more than
+ *                          64 members fall back to the table form);
  *   NIMBUS_ACOUSTIC_MARCH  one thread advances nimbus_cuda_engine_set_march
  *                          consecutive cells of a row along x (default 16),
  *                          neighbour data of the previous cell carried over in
- *                          registers;
+ *                          registers (the momentum pass's default);
  *   NIMBUS_ACOUSTIC_PAIR   the constant-bank form with two cells per thread
  *                          (both cells' loads issued before either's
  *                          arithmetic);

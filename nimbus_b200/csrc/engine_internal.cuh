@@ -64,7 +64,7 @@ struct nimbus_engine
     int lane_target = 4;            // lanes when there are at least that many members
     int march_len = 16;             // i-planes per thread of the marching acoustic kernels
     int acoustic_form = NIMBUS_ACOUSTIC_CONST;  // nimbus_acoustic_form of the continuity pass
-    int momentum_form = NIMBUS_ACOUSTIC_CONST;  // and of the momentum pass
+    int momentum_form = NIMBUS_ACOUSTIC_MARCH;  // and of the momentum pass (marching measured fastest)
     std::vector<cudaStream_t> lane_streams;  // lanes 1.. (lane 0 runs on the engine stream)
     std::vector<cudaEvent_t> lane_done;
     cudaEvent_t fork = nullptr;
@@ -101,9 +101,13 @@ using namespace nimbus_host;
 
 constexpr int kEngineBlock = 256;
 
-// The slow Heun pair's constant-bank form (1) or member-table form (0).
+// The slow Heun pair's and the transport passes' constant-bank forms (1) or
+// member-table forms (0).
 #ifndef NIMBUS_SLOW_CONST
 #define NIMBUS_SLOW_CONST 1
+#endif
+#ifndef NIMBUS_TRANSPORT_CONST
+#define NIMBUS_TRANSPORT_CONST 1
 #endif
 
 int blocks_per_sm(nimbus_engine* e, const void* kernel, int block = kEngineBlock)
@@ -391,13 +395,59 @@ int enqueue_step(nimbus_engine* e, int lane, cudaStream_t st, int part)
     }
     engine_swap_kernel<<<(n + 127) / 128, 128, 0, st>>>(T, n, 0);
     ++count;
-    // Conservative transport of theta, qv, qc, qr against the retained fluxes.
-    ENGINE_LAUNCH(NIMBUS_KERNEL_TRANSPORT_FACES, engine_transport_faces_kernel<kFp32>, cells, 1, T, pc,
-                  cells);
-    ENGINE_LAUNCH(NIMBUS_KERNEL_TRANSPORT_LIMITER, engine_transport_limiter_kernel<kFp32>, cells, 1, T, pc,
-                  cells);
-    ENGINE_LAUNCH(NIMBUS_KERNEL_TRANSPORT_UPDATE, engine_transport_update_kernel<kFp32>, cells, 1, T, pc,
-                  cells);
+    // Conservative transport of theta, qv, qc, qr against the retained fluxes
+    // (the constant-bank form for lanes of at most kTransportConstMembers).
+    if (NIMBUS_TRANSPORT_CONST && n <= kTransportConstMembers)
+    {
+        std::unique_ptr<TransportLaunch> tl(new TransportLaunch());
+        const long long* p = e->prefix.data() + L.prefix_first + static_cast<size_t>(kItemCells) * (n + 1);
+        for (int r = 0; r <= n; ++r) tl->prefix[r] = p[r];
+        for (int r = 0; r < n; ++r)
+        {
+            const EngineMember& H = e->slots[static_cast<size_t>(e->order[static_cast<size_t>(L.first + r)])].m;
+            TransportConst& A = tl->m[r];
+            TransportCompact& C = A.T;
+            C.d = H.T.d;
+            C.inv_dx = H.T.inv_dx;
+            C.inv_dy = H.T.inv_dy;
+            C.inv_dz = H.T.inv_dz;
+            C.dt = H.T.dt;
+            C.rho_floor = H.T.rho_floor;
+            C.weno = H.T.weno;
+            C.top_open = H.T.top_open;
+            for (int q = 0; q < 4; ++q) C.positive_definite[q] = H.T.positive_definite[q];
+            C.inv_dx_f = H.T.inv_dx_f;
+            C.inv_dy_f = H.T.inv_dy_f;
+            C.inv_dz_f = H.T.inv_dz_f;
+            C.dt_f = H.T.dt_f;
+            C.inv_dt_f = H.T.inv_dt_f;
+            C.rho_floor_f = H.T.rho_floor_f;
+            A.q4 = reinterpret_cast<const float4*>(H.q4);
+            A.mfx = H.mfx;
+            A.mfy = H.mfy;
+            A.mfz = H.mfz;
+            A.rho_begin = H.rho_begin;
+            A.sf = reinterpret_cast<float4*>(H.sf);
+            A.rl = reinterpret_cast<float4*>(H.rl);
+            A.theta = H.theta;
+            A.qv = H.qv;
+            A.qc = H.qc;
+            A.status = H.status;
+        }
+        ENGINE_LAUNCH(NIMBUS_KERNEL_TRANSPORT_FACES, engine_transport_faces_const_kernel<kFp32>, cells, 1, *tl, T,
+                      cells);
+        ENGINE_LAUNCH(NIMBUS_KERNEL_TRANSPORT_LIMITER, engine_transport_limiter_const_kernel<kFp32>, cells, 1, *tl, T,
+                      cells);
+        ENGINE_LAUNCH(NIMBUS_KERNEL_TRANSPORT_UPDATE, engine_transport_update_const_kernel<kFp32>, cells, 1, *tl, T,
+                      cells);
+    }
+    else
+    {
+        ENGINE_LAUNCH(NIMBUS_KERNEL_TRANSPORT_FACES, engine_transport_faces_kernel<kFp32>, cells, 1, T, pc, cells);
+        ENGINE_LAUNCH(NIMBUS_KERNEL_TRANSPORT_LIMITER, engine_transport_limiter_kernel<kFp32>, cells, 1, T, pc,
+                      cells);
+        ENGINE_LAUNCH(NIMBUS_KERNEL_TRANSPORT_UPDATE, engine_transport_update_kernel<kFp32>, cells, 1, T, pc, cells);
+    }
     // Kessler step and the EOS pressure re-projection (one pass), then the
     // pointer rotation that publishes the new qr and pressure.
     count += nimbus_engine_detail::launch_microphysics(e, st, T, pc, cells);

@@ -984,6 +984,76 @@ static __global__ void __launch_bounds__(256) engine_transport_update_kernel(con
     });
 }
 
+// The three transport passes with the members' constants in the constant
+// bank: a compact copy of each member's transport parameters and its buffers
+// that do not rotate; the end-of-loop density and the rain, which rotate,
+// are read from the table.
+struct TransportConst
+{
+    TransportCompact T;
+    const float4* q4;
+    const float *mfx, *mfy, *mfz, *rho_begin;
+    float4 *sf, *rl;
+    float *theta, *qv, *qc;
+    unsigned* status;
+};
+
+constexpr int kTransportConstMembers = 64;
+
+struct TransportLaunch
+{
+    long long prefix[kTransportConstMembers + 1];
+    TransportConst m[kTransportConstMembers];
+};
+static_assert(sizeof(TransportLaunch) <= 32000, "a kernel parameter block holds at most 32764 bytes");
+
+// Calls fn(A, M, c) for every cell of the first tiles of the launch.
+template <class Fn>
+__device__ __forceinline__ void for_transport_cells(const TransportLaunch& L, const EngineMember* __restrict__ table,
+                                                    long long tiles, Fn&& fn)
+{
+    int m = 0;
+    for (long long t = blockIdx.x; t < tiles; t += gridDim.x)
+    {
+        while (t >= L.prefix[m + 1]) ++m;
+        const TransportConst& A = L.m[m];
+        const int c = (int)((t - L.prefix[m]) * blockDim.x) + (int)threadIdx.x;
+        if (c >= A.T.d.cells()) continue;
+        fn(A, table[m], c);
+    }
+}
+
+template <bool kFp32>
+static __global__ void __launch_bounds__(256, NIMBUS_FACES_MINB) engine_transport_faces_const_kernel(
+    const __grid_constant__ TransportLaunch L, const EngineMember* __restrict__ table, long long tiles)
+{
+    for_transport_cells(L, table, tiles, [&](const TransportConst& A, const EngineMember&, int c) {
+        transport_faces_cell4<kFp32>(A.T, A.q4, A.mfx, A.mfy, A.mfz, A.sf, c);
+    });
+}
+
+template <bool kFp32>
+static __global__ void __launch_bounds__(256) engine_transport_limiter_const_kernel(
+    const __grid_constant__ TransportLaunch L, const EngineMember* __restrict__ table, long long tiles)
+{
+    for_transport_cells(L, table, tiles, [&](const TransportConst& A, const EngineMember&, int c) {
+        transport_limiter_cell4<kFp32>(A.T, A.q4, A.rho_begin, A.sf, A.rl, c);
+    });
+}
+
+template <bool kFp32>
+static __global__ void __launch_bounds__(256) engine_transport_update_const_kernel(
+    const __grid_constant__ TransportLaunch L, const EngineMember* __restrict__ table, long long tiles)
+{
+    for_transport_cells(L, table, tiles, [&](const TransportConst& A, const EngineMember& M, int c) {
+        unsigned flags = 0;
+        float* const in_place[4] = {A.theta, A.qv, A.qc, M.qr};
+        transport_update_cell4<kFp32>(A.T, A.q4, [&](int s) { return (const float*)in_place[s]; },
+                                      [&](int s) { return in_place[s]; }, M.rho, A.rho_begin, A.sf, A.rl, c, flags);
+        if (flags) atomicOr(A.status, flags);
+    });
+}
+
 // ---- Acoustic speed scan before a large step --------------------------------
 // Per member the largest (gamma p) / rho of its cells, as ordered double bits
 // into c2[row] (row = the member's table row in this launch), for the

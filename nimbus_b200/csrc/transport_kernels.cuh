@@ -35,6 +35,21 @@ struct TransportParams
     float inv_dx_f, inv_dy_f, inv_dz_f, dt_f, inv_dt_f, rho_floor_f;
 };
 
+// The fields of TransportParams the interleaved (float4) cell functions read:
+// geometry, spacings, dt, the density floor, the reconstruction and top
+// flags and the first four scalars' positive-definite flags.
+struct TransportCompact
+{
+    Dims d;
+    double inv_dx, inv_dy, inv_dz;
+    double dt;
+    double rho_floor;
+    int weno;
+    int top_open;
+    int positive_definite[4];
+    float inv_dx_f, inv_dy_f, inv_dz_f, dt_f, inv_dt_f, rho_floor_f;
+};
+
 __host__ __device__ inline void finish_fp32(TransportParams& T)
 {
     T.inv_dx_f = (float)T.inv_dx;
@@ -403,8 +418,8 @@ __device__ __forceinline__ float pd_limiter_factor(double r)
 // each counted only where it exists (the has_* flags).  kFp32: the same sums
 // in FP32 (the reference's FP32 GPU form); the factor's 32-ulp roundoff
 // margin covers the FP32 rounding of the update.
-template <bool kFp32>
-__device__ __forceinline__ float limiter_factor(const TransportParams& T, float fxp, float fxm, float fyp, float fym,
+template <bool kFp32, class TP>
+__device__ __forceinline__ float limiter_factor(const TP& T, float fxp, float fxm, float fyp, float fym,
                                                 float fzp, float fzm, bool xp, bool xm, bool yp, bool ym, bool zp,
                                                 bool zm, float rho_b, float q)
 {
@@ -498,8 +513,8 @@ __device__ __forceinline__ typename std::conditional<kFp32, float, double>::type
 // (x+, x-, y+, y-, z+, z-), the limiter factors of the cell and its six
 // neighbours (positive-definite scalars only) and its old value
 // (advection_cartesian.cpp:2465-2640).  kFp32: the same sums in FP32.
-template <bool kFp32>
-__device__ __forceinline__ float update_value(const TransportParams& T, bool pd, float fxp, float fxm, float fyp,
+template <bool kFp32, class TP>
+__device__ __forceinline__ float update_value(const TP& T, bool pd, float fxp, float fxm, float fyp,
                                               float fym, float fzp, float fzm, float rc, float rxp, float rxm,
                                               float ryp, float rym, float rzp, float rzm, float qraw, bool has_top,
                                               bool has_bottom, float rho_e, float rho_b, unsigned& flags)
@@ -661,8 +676,11 @@ __device__ __forceinline__ float4 stencil_flux4(const float4* __restrict__ q4, c
     }
 }
 
-template <bool kFp32>
-__device__ __forceinline__ void transport_faces_cell4(const TransportParams& T, const float4* __restrict__ q4,
+// The cell functions below take the transport parameters as any type with
+// TransportParams' geometry and flag fields (the member engine passes a
+// compact copy through the constant bank).
+template <bool kFp32, class TP>
+__device__ __forceinline__ void transport_faces_cell4(const TP& T, const float4* __restrict__ q4,
                                                       const float* __restrict__ mfx, const float* __restrict__ mfy,
                                                       const float* __restrict__ mfz, float4* __restrict__ sf4, int c)
 {
@@ -699,8 +717,8 @@ __device__ __forceinline__ void transport_faces_cell4(const TransportParams& T, 
     sf4[2 * n + c] = oz;
 }
 
-template <bool kFp32>
-__device__ __forceinline__ void transport_limiter_cell4(const TransportParams& T, const float4* __restrict__ q4,
+template <bool kFp32, class TP>
+__device__ __forceinline__ void transport_limiter_cell4(const TP& T, const float4* __restrict__ q4,
                                                         const float* __restrict__ rho_begin,
                                                         const float4* __restrict__ sf4, float4* __restrict__ rl4,
                                                         int c)
@@ -726,8 +744,8 @@ __device__ __forceinline__ void transport_limiter_cell4(const TransportParams& T
     rl4[c] = make_float4(r[0], r[1], r[2], r[3]);
 }
 
-template <bool kFp32, class QIn, class QOut>
-__device__ __forceinline__ void transport_update_cell4(const TransportParams& T, const float4* __restrict__ q4,
+template <bool kFp32, class TP, class QIn, class QOut>
+__device__ __forceinline__ void transport_update_cell4(const TP& T, const float4* __restrict__ q4,
                                                        QIn&& q_of, QOut&& qo_of,
                                                        const float* __restrict__ rho_end,
                                                        const float* __restrict__ rho_begin,
