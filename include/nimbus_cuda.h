@@ -1046,7 +1046,9 @@ int nimbus_cuda_engine_lanes(const nimbus_engine* e);
  *                          copies (cp.async.bulk on an mbarrier, four tiles in
  *                          flight per CTA); a staged copy that does not
  *                          complete sets member status bit 32 and the step
- *                          fails with NIMBUS_ERR_CUDA at synchronisation.
+ *                          fails with NIMBUS_ERR_CUDA at synchronisation;
+ *   NIMBUS_ACOUSTIC_CMARCH the marching form with the constant-bank
+ *                          parameters.
  * nimbus_cuda_engine_set_acoustic_form sets both passes; set_pass_forms sets
  * each; nimbus_cuda_engine_acoustic_form reports the continuity pass's. */
 enum
@@ -1055,7 +1057,8 @@ enum
     NIMBUS_ACOUSTIC_CONST = 1,
     NIMBUS_ACOUSTIC_MARCH = 2,
     NIMBUS_ACOUSTIC_PAIR = 3,
-    NIMBUS_ACOUSTIC_BULK = 4
+    NIMBUS_ACOUSTIC_BULK = 4,
+    NIMBUS_ACOUSTIC_CMARCH = 5
 };
 nimbus_status nimbus_cuda_engine_set_acoustic_form(nimbus_engine* e, int form);
 int nimbus_cuda_engine_acoustic_form(const nimbus_engine* e);
@@ -1070,11 +1073,12 @@ int nimbus_cuda_engine_march(const nimbus_engine* e);
  * candidate's time: first the lane count {1, 2, 4, 6, 8} (at most the member
  * count) with the constant-bank form, then, at the fastest lane count, every
  * pair of pass forms (continuity x momentum, each of constant bank, member
- * table, marching 16 planes, two cells per thread, bulk-staged tiles).  The members' states are
+ * table, marching 16 planes, two cells per thread, bulk-staged tiles,
+ * constant-bank marching).  The members' states are
  * saved on the device before and restored after, so the runs are where they
  * were (status words and substep counts may reflect the tuning steps).
  * Waits for the device. */
-#define NIMBUS_TUNING_CANDIDATES 32
+#define NIMBUS_TUNING_CANDIDATES 48
 typedef struct nimbus_engine_tuning
 {
     int lanes, acoustic_form, march;  /* the chosen configuration (now set); acoustic_form: continuity */

@@ -1137,7 +1137,7 @@ nimbus_status nimbus_cuda_engine_autotune(nimbus_engine* e, int steps, nimbus_en
         if (!(ok = trial({lanes, NIMBUS_ACOUSTIC_CONST, NIMBUS_ACOUSTIC_CONST, saved.march}))) break;
     }
     const int forms[] = {NIMBUS_ACOUSTIC_CONST, NIMBUS_ACOUSTIC_PAIR, NIMBUS_ACOUSTIC_TABLE, NIMBUS_ACOUSTIC_MARCH,
-                         NIMBUS_ACOUSTIC_BULK};
+                         NIMBUS_ACOUSTIC_BULK, NIMBUS_ACOUSTIC_CMARCH};
     const int lanes = chosen.lanes;
     for (int cf : forms)
     {
@@ -1145,7 +1145,8 @@ nimbus_status nimbus_cuda_engine_autotune(nimbus_engine* e, int steps, nimbus_en
         for (int mf : forms)
         {
             if (cf == NIMBUS_ACOUSTIC_CONST && mf == NIMBUS_ACOUSTIC_CONST) continue;  // timed above
-            const int march = (cf == NIMBUS_ACOUSTIC_MARCH || mf == NIMBUS_ACOUSTIC_MARCH) ? 16 : saved.march;
+            auto marching = [](int f) { return f == NIMBUS_ACOUSTIC_MARCH || f == NIMBUS_ACOUSTIC_CMARCH; };
+            const int march = (marching(cf) || marching(mf)) ? 16 : saved.march;
             if (!(ok = trial({lanes, cf, mf, march}))) break;
         }
     }
@@ -1243,7 +1244,7 @@ int nimbus_cuda_engine_lanes(const nimbus_engine* e) { return e ? static_cast<in
 
 nimbus_status nimbus_cuda_engine_set_pass_forms(nimbus_engine* e, int continuity_form, int momentum_form)
 {
-    auto valid = [](int f) { return f >= NIMBUS_ACOUSTIC_TABLE && f <= NIMBUS_ACOUSTIC_BULK; };
+    auto valid = [](int f) { return f >= NIMBUS_ACOUSTIC_TABLE && f <= NIMBUS_ACOUSTIC_CMARCH; };
     if (!e || !valid(continuity_form) || !valid(momentum_form)) return NIMBUS_ERR_INVALID_ARGUMENT;
     if (continuity_form != e->acoustic_form || momentum_form != e->momentum_form)
     {

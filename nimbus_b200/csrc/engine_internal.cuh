@@ -272,7 +272,8 @@ int enqueue_step(nimbus_engine* e, int lane, cudaStream_t st, int part)
     // parameter (lanes of at most kConstMembers members; larger ones take the
     // member-table form).
     auto in_bank = [](int f) {
-        return f == NIMBUS_ACOUSTIC_CONST || f == NIMBUS_ACOUSTIC_PAIR || f == NIMBUS_ACOUSTIC_BULK;
+        return f == NIMBUS_ACOUSTIC_CONST || f == NIMBUS_ACOUSTIC_PAIR || f == NIMBUS_ACOUSTIC_BULK ||
+               f == NIMBUS_ACOUSTIC_CMARCH;
     };
     // Bulk copies move 16-byte units between 16-byte-aligned addresses: every
     // member field starts on a 256-byte boundary of its arena, so the arenas
@@ -301,6 +302,8 @@ int enqueue_step(nimbus_engine* e, int lane, cudaStream_t st, int part)
         al.reset(new AcousticLaunch());
         const long long* p = e->prefix.data() + L.prefix_first + static_cast<size_t>(kItemCells) * (n + 1);
         for (int r = 0; r <= n; ++r) al->prefix[r] = p[r];
+        const long long* pmr = e->prefix.data() + L.prefix_first + static_cast<size_t>(kItemMarch) * (n + 1);
+        for (int r = 0; r <= n; ++r) al->march_prefix[r] = pmr[r];
         al->bulk_sy4 = sy4;
         for (int r = 0; r < n; ++r)
         {
@@ -322,6 +325,8 @@ int enqueue_step(nimbus_engine* e, int lane, cudaStream_t st, int part)
             A.eos0 = H.eos0;
             A.vertical = kFuseVertical | (H.B.bottom == kBottomNoSlip ? kFuseNoSlipBottom : 0) |
                          (H.B.top == kTopOpen ? kFuseOpenTop : 0);
+            A.march_len = H.march_len;
+            A.march_blocks = H.march_blocks;
         }
     }
     for (size_t s = 0; s < L.active.size(); ++s)
@@ -352,6 +357,14 @@ int enqueue_step(nimbus_engine* e, int lane, cudaStream_t st, int part)
             ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, engine_continuity_march_kernel<Policy>, march_tiles, 1, T,
                           pm, march_tiles, si);
             break;
+        case NIMBUS_ACOUSTIC_CMARCH:
+            if (s == 0)
+                ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, (engine_continuity_cmarch_kernel<Policy, true>),
+                              march_tiles, 1, *al, T, march_tiles, si);
+            else
+                ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, (engine_continuity_cmarch_kernel<Policy, false>),
+                              march_tiles, 1, *al, T, march_tiles, si);
+            break;
         case NIMBUS_ACOUSTIC_BULK:
             if (s == 0)
                 ENGINE_LAUNCH_SMEM(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, (engine_continuity_bulk_kernel<Policy, true>),
@@ -381,6 +394,10 @@ int enqueue_step(nimbus_engine* e, int lane, cudaStream_t st, int part)
         case NIMBUS_ACOUSTIC_BULK:
             ENGINE_LAUNCH_SMEM(NIMBUS_KERNEL_ACOUSTIC_MOMENTUM, engine_momentum_bulk_kernel<Policy>, tiles, smem_mom,
                                *al, T, tiles, si);
+            break;
+        case NIMBUS_ACOUSTIC_CMARCH:
+            ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_MOMENTUM, engine_momentum_cmarch_kernel<Policy>, march_tiles, 1, *al,
+                          T, march_tiles, si);
             break;
         default:
             ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_MOMENTUM, engine_momentum_kernel<Policy>, tiles, 1, T, pc, tiles,

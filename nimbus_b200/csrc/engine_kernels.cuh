@@ -144,11 +144,11 @@ __device__ __forceinline__ void for_member_rows(const EngineMember* __restrict__
 
 // ---- Heun slow step -------------------------------------------------------
 
-template <class Policy>
 // Resident CTAs per SM of the slow Heun pair (64 registers at 4).
 #ifndef NIMBUS_SLOW_MINB
 #define NIMBUS_SLOW_MINB 4
 #endif
+template <class Policy>
 static __global__ void __launch_bounds__(256, NIMBUS_SLOW_MINB) engine_slow_predict_kernel(const EngineMember* __restrict__ table,
                                                                   const long long* __restrict__ prefix,
                                                                   long long tiles)
@@ -401,6 +401,7 @@ struct AcousticConst
     const float2* dp0;
     const float4* eos0;
     int vertical;  // kFuse* bits of the momentum pass
+    int march_len, march_blocks;  // the marching forms' row tiling (kItemMarch)
 };
 
 constexpr int kConstMembers = 64;  // members one launch can carry in its parameter
@@ -418,9 +419,10 @@ constexpr int kConstMembers = 64;  // members one launch can carry in its parame
 
 struct AcousticLaunch
 {
-    long long prefix[kConstMembers + 1];  // first cell tile of each member
+    long long prefix[kConstMembers + 1];        // first cell tile of each member
+    long long march_prefix[kConstMembers + 1];  // first row tile of each member (marching forms)
     AcousticConst m[kConstMembers];
-    int bulk_sy4;                         // the members' largest nz rounded up to 4 (bulk-staged forms)
+    int bulk_sy4;                               // the members' largest nz rounded up to 4 (bulk-staged forms)
 };
 static_assert(sizeof(AcousticLaunch) <= 32000, "a kernel parameter block holds at most 32764 bytes");
 
@@ -466,6 +468,58 @@ static __global__ void __launch_bounds__(256, NIMBUS_CONST_MINB_MOM) engine_mome
         momentum_cell<Policy>(A.F, even ? M.rho_alt : M.rho, M.p, A.p0, A.dp0, A.u, A.v, A.w, A.u, A.v, A.w, c,
                               A.vertical);
     }
+}
+
+// The marching passes with the members' constants in the constant bank.
+#ifndef NIMBUS_CMARCH_MINB
+#define NIMBUS_CMARCH_MINB 5
+#endif
+template <class Fn>
+__device__ __forceinline__ void for_const_rows(const AcousticLaunch& L, const EngineMember* __restrict__ table,
+                                               long long tiles, Fn&& fn)
+{
+    int m = 0;
+    for (long long t = blockIdx.x; t < tiles; t += gridDim.x)
+    {
+        while (t >= L.march_prefix[m + 1]) ++m;
+        const AcousticConst& A = L.m[m];
+        const int local = (int)(t - L.march_prefix[m]);
+        const int chunk = local / A.march_blocks;
+        const int q = (local - chunk * A.march_blocks) * (int)blockDim.x + (int)threadIdx.x;
+        const Dims d = A.F.d;
+        if (q >= d.ny * d.nz) continue;
+        int i, j, k;
+        decompose(d, q, i, j, k);
+        const int i0 = chunk * A.march_len;
+        fn(A, table[m], i0, min(d.nx, i0 + A.march_len), j, k, q);
+    }
+}
+
+template <class Policy, bool kFirst>
+static __global__ void __launch_bounds__(256, NIMBUS_CMARCH_MINB) engine_continuity_cmarch_kernel(
+    const __grid_constant__ AcousticLaunch L, const EngineMember* __restrict__ table, long long tiles, int s)
+{
+    const bool even = (s & 1) == 0;
+    for_const_rows(L, table, tiles, [&](const AcousticConst& A, const EngineMember& M, int i0, int i1, int j, int k,
+                                        int q) {
+        unsigned flags = 0;
+        continuity_eos_march<Policy>(A.F, even ? M.rho : M.rho_alt, A.u, A.v, A.w, A.theta, A.rho0, A.eos0,
+                                     even ? M.rho_alt : M.rho, M.p, A.mfx, A.mfy, A.mfz, i0, i1, j, k, q, flags, kFirst,
+                                     kFirst ? A.rho_begin : nullptr);
+        if (flags) atomicOr(A.status, flags);
+    });
+}
+
+template <class Policy>
+static __global__ void __launch_bounds__(256, NIMBUS_CMARCH_MINB) engine_momentum_cmarch_kernel(
+    const __grid_constant__ AcousticLaunch L, const EngineMember* __restrict__ table, long long tiles, int s)
+{
+    const bool even = (s & 1) == 0;
+    for_const_rows(L, table, tiles, [&](const AcousticConst& A, const EngineMember& M, int i0, int i1, int j, int k,
+                                        int q) {
+        momentum_march<Policy>(A.F, even ? M.rho_alt : M.rho, M.p, A.p0, A.dp0, A.u, A.v, A.w, i0, i1, j, k, q,
+                               A.vertical);
+    });
 }
 
 // The same two passes with two cells per thread: a CTA of half a tile's

@@ -212,7 +212,7 @@ class CgridSlowTendenciesArgs(ctypes.Structure):
     ]
 
 
-TUNING_CANDIDATES = 32
+TUNING_CANDIDATES = 48
 
 
 class EngineTuning(ctypes.Structure):
@@ -318,8 +318,8 @@ EXPORTED_SYMBOLS = (
     "nimbus_cuda_kessler_sedimentation", "nimbus_cuda_cgrid_slow_tendencies",
 )
 ACOUSTIC_FORM_NAMES = {0: "member-table", 1: "constant-bank", 2: "marching", 3: "constant-bank, two cells per thread",
-                       4: "bulk-staged tiles"}
-ACOUSTIC_TABLE, ACOUSTIC_CONST, ACOUSTIC_MARCH, ACOUSTIC_PAIR, ACOUSTIC_BULK = 0, 1, 2, 3, 4
+                       4: "bulk-staged tiles", 5: "constant-bank marching"}
+ACOUSTIC_TABLE, ACOUSTIC_CONST, ACOUSTIC_MARCH, ACOUSTIC_PAIR, ACOUSTIC_BULK, ACOUSTIC_CMARCH = 0, 1, 2, 3, 4, 5
 SUBSTEP_AUTO, SUBSTEP_FUSED, SUBSTEP_SPLIT = 0, 1, 2
 PRECISION_REFERENCE, PRECISION_FP32 = 0, 1
 STATIC_SCRATCH_CELLS = 4194304  # NIMBUS_STATIC_SCRATCH_CELLS

@@ -246,14 +246,15 @@ def test_device_sound_speed_scan_matches_oracle(ctx, o32):
         ctx.max_sound_speed(bad, st["rho"], case.shape, base)
 
 
-T, C, M, P2, B = cuda.ACOUSTIC_TABLE, cuda.ACOUSTIC_CONST, cuda.ACOUSTIC_MARCH, cuda.ACOUSTIC_PAIR, cuda.ACOUSTIC_BULK
+T, C, M, P2, B, CM = (cuda.ACOUSTIC_TABLE, cuda.ACOUSTIC_CONST, cuda.ACOUSTIC_MARCH, cuda.ACOUSTIC_PAIR,
+                      cuda.ACOUSTIC_BULK, cuda.ACOUSTIC_CMARCH)
 
 
 @pytest.mark.parametrize("forms,march", [((T, T), 16), ((M, M), 5), ((M, M), 1000), ((P2, P2), 16),
                                          ((C, M), 16), ((P2, T), 7), ((T, P2), 16), ((B, B), 16), ((B, M), 16),
-                                         ((C, B), 16)],
+                                         ((C, B), 16), ((CM, CM), 16), ((CM, M), 3), ((T, CM), 1000)],
                          ids=["table", "march5", "whole-rows", "pair", "const-march", "pair-table", "table-pair",
-                              "bulk", "bulk-march", "const-bulk"])
+                              "bulk", "bulk-march", "const-bulk", "cmarch", "cmarch-march3", "table-cmarch-rows"])
 def test_engine_acoustic_kernel_form_does_not_change_results(ctx, multi_tile, forms, march):
     """The continuity and momentum passes in each kernel form (member table,
     constant-bank parameters -- the default, covered above -- marching along x
