@@ -301,7 +301,11 @@ int enqueue_step(nimbus_engine* e, int lane, cudaStream_t st, int part)
     {
         al.reset(new AcousticLaunch());
         const long long* p = e->prefix.data() + L.prefix_first + static_cast<size_t>(kItemCells) * (n + 1);
-        for (int r = 0; r <= n; ++r) al->prefix[r] = p[r];
+        for (int r = 0; r <= n; ++r)
+        {
+            al->prefix[r] = p[r];
+            al->prefix32[r] = static_cast<int>(p[r]);
+        }
         const long long* pmr = e->prefix.data() + L.prefix_first + static_cast<size_t>(kItemMarch) * (n + 1);
         for (int r = 0; r <= n; ++r) al->march_prefix[r] = pmr[r];
         al->bulk_sy4 = sy4;

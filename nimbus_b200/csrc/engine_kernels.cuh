@@ -420,6 +420,7 @@ constexpr int kConstMembers = 64;  // members one launch can carry in its parame
 struct AcousticLaunch
 {
     long long prefix[kConstMembers + 1];        // first cell tile of each member
+    int prefix32[kConstMembers + 1];            // the same as 32-bit values (a lane's tiles fit)
     long long march_prefix[kConstMembers + 1];  // first row tile of each member (marching forms)
     AcousticConst m[kConstMembers];
     int bulk_sy4;                               // the members' largest nz rounded up to 4 (bulk-staged forms)
@@ -436,11 +437,12 @@ static __global__ void __launch_bounds__(256, NIMBUS_CONST_MINB) engine_continui
     constexpr bool first = kFirst;
     const bool even = (s & 1) == 0;
     int m = 0;
-    for (long long t = blockIdx.x; t < tiles; t += gridDim.x)
+    const int ntiles = (int)tiles;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x)
     {
-        while (t >= L.prefix[m + 1]) ++m;
+        while (t >= L.prefix32[m + 1]) ++m;
         const AcousticConst& A = L.m[m];
-        const int c = (int)((t - L.prefix[m]) * blockDim.x) + (int)threadIdx.x;
+        const int c = (t - L.prefix32[m]) * (int)blockDim.x + (int)threadIdx.x;
         if (c >= A.F.d.cells()) continue;
         const EngineMember& M = table[m];
         unsigned flags = 0;
@@ -458,11 +460,12 @@ static __global__ void __launch_bounds__(256, NIMBUS_CONST_MINB_MOM) engine_mome
 {
     const bool even = (s & 1) == 0;
     int m = 0;
-    for (long long t = blockIdx.x; t < tiles; t += gridDim.x)
+    const int ntiles = (int)tiles;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x)
     {
-        while (t >= L.prefix[m + 1]) ++m;
+        while (t >= L.prefix32[m + 1]) ++m;
         const AcousticConst& A = L.m[m];
-        const int c = (int)((t - L.prefix[m]) * blockDim.x) + (int)threadIdx.x;
+        const int c = (t - L.prefix32[m]) * (int)blockDim.x + (int)threadIdx.x;
         if (c >= A.F.d.cells()) continue;
         const EngineMember& M = table[m];
         momentum_cell<Policy>(A.F, even ? M.rho_alt : M.rho, M.p, A.p0, A.dp0, A.u, A.v, A.w, A.u, A.v, A.w, c,
