@@ -93,6 +93,18 @@ int nimbus_cuda_abi_version(void);
 uint64_t nimbus_cuda_kernel_launches(const nimbus_cuda_context* ctx);
 /* The context's stream, as a cudaStream_t. */
 void* nimbus_cuda_stream(const nimbus_cuda_context* ctx);
+/* The context's device: its name, SM count, compute capability and memory
+ * (total, and free now); what ComputeBackend::populate_hardware_info and
+ * memory_properties report (backend_interface.hpp:39-44). */
+typedef struct nimbus_device_info
+{
+    char name[256];
+    int sm_count;
+    int cc_major, cc_minor;
+    unsigned long long total_bytes;
+    unsigned long long free_bytes;
+} nimbus_device_info;
+nimbus_status nimbus_cuda_device_info(nimbus_cuda_context* ctx, nimbus_device_info* out);
 /* Waits for all work on the context's stream, then reads and clears the
  * device status word that NIMBUS_MEMORY_DEVICE calls accumulate: returns
  * NIMBUS_ERR_NONFINITE if any enqueued call produced a non-finite retained

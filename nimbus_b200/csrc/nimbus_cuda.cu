@@ -667,6 +667,24 @@ nimbus_status nimbus_cuda_create(int device, nimbus_cuda_context** out)
     return NIMBUS_OK;
 }
 
+nimbus_status nimbus_cuda_device_info(nimbus_cuda_context* ctx, nimbus_device_info* out)
+{
+    if (!ctx || !out) return NIMBUS_ERR_INVALID_ARGUMENT;
+    NB_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaDeviceProp prop{};
+    NB_CUDA(ctx, cudaGetDeviceProperties(&prop, ctx->device));
+    size_t free_b = 0, total_b = 0;
+    NB_CUDA(ctx, cudaMemGetInfo(&free_b, &total_b));
+    *out = nimbus_device_info{};
+    std::strncpy(out->name, prop.name, sizeof(out->name) - 1);
+    out->sm_count = prop.multiProcessorCount;
+    out->cc_major = prop.major;
+    out->cc_minor = prop.minor;
+    out->total_bytes = total_b;
+    out->free_bytes = free_b;
+    return NIMBUS_OK;
+}
+
 void nimbus_cuda_destroy(nimbus_cuda_context* ctx)
 {
     if (!ctx) return;

@@ -212,6 +212,11 @@ class CgridSlowTendenciesArgs(ctypes.Structure):
     ]
 
 
+class DeviceInfo(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 256), ("sm_count", ctypes.c_int), ("cc_major", ctypes.c_int),
+                ("cc_minor", ctypes.c_int), ("total_bytes", ctypes.c_ulonglong), ("free_bytes", ctypes.c_ulonglong)]
+
+
 TUNING_CANDIDATES = 48
 
 
@@ -315,7 +320,7 @@ EXPORTED_SYMBOLS = (
     "nimbus_cuda_engine_acoustic_form", "nimbus_cuda_engine_member_status_async", "nimbus_cuda_engine_graph_builds",
     "nimbus_cuda_engine_set_pass_forms", "nimbus_cuda_engine_pass_forms",
     "nimbus_cuda_engine_autotune", "nimbus_cuda_slow_apply", "nimbus_cuda_kessler_pointwise",
-    "nimbus_cuda_kessler_sedimentation", "nimbus_cuda_cgrid_slow_tendencies",
+    "nimbus_cuda_kessler_sedimentation", "nimbus_cuda_cgrid_slow_tendencies", "nimbus_cuda_device_info",
 )
 ACOUSTIC_FORM_NAMES = {0: "member-table", 1: "constant-bank", 2: "marching", 3: "constant-bank, two cells per thread",
                        4: "bulk-staged tiles", 5: "constant-bank marching"}
@@ -424,6 +429,7 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
     lib.nimbus_cuda_kessler_pointwise.argtypes = [vp, ctypes.POINTER(KesslerPointwiseArgs)]
     lib.nimbus_cuda_kessler_sedimentation.argtypes = [vp, ctypes.POINTER(KesslerSedimentationArgs)]
     lib.nimbus_cuda_cgrid_slow_tendencies.argtypes = [vp, ctypes.POINTER(CgridSlowTendenciesArgs)]
+    lib.nimbus_cuda_device_info.argtypes = [vp, ctypes.POINTER(DeviceInfo)]
     lib.nimbus_cuda_engine_graph_builds.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64),
                                                     ctypes.POINTER(ctypes.c_uint64)]
     lib.nimbus_cuda_engine_acoustic_form.argtypes = [vp]
@@ -654,6 +660,13 @@ class Context:
         a.memory = MEMORY_DEVICE if hasattr(st["u"], "data_ptr") else MEMORY_HOST
         assert nz >= 2
         self.check(self.lib.nimbus_cuda_cgrid_slow_tendencies(self.handle, ctypes.byref(a)))
+
+    def device_info(self) -> dict:
+        """Name, SM count, compute capability and memory of the context's device."""
+        d = DeviceInfo()
+        self.check(self.lib.nimbus_cuda_device_info(self.handle, ctypes.byref(d)))
+        return {"name": d.name.decode(), "sm_count": d.sm_count, "cc": (d.cc_major, d.cc_minor),
+                "total_bytes": d.total_bytes, "free_bytes": d.free_bytes}
 
     def resolve_substep_count(self, dt, c_max, min_spacing, requested=0) -> int:
         """The reference's substep-count rule (split_explicit.cpp:67-170)."""

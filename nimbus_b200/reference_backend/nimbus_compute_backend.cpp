@@ -44,6 +44,7 @@
 //       saturation adjustment in a different order and the CPU one computes
 //       in FP64).
 #include "compute/backend_interface.hpp"
+#include "core/infra/hardware_info.hpp"
 #include "compute/dispatch/advection.hpp"
 #include "compute/dispatch/dynamics.hpp"
 #include "compute/dispatch/microphysics.hpp"
@@ -72,10 +73,13 @@ public:
 
     std::string name() const override { return "cuda"; }
 
+    // The configured device (device_index < 0: the first one).
+    void configure(const ComputeBackendConfig& config) override { device_ = config.device_index > 0 ? config.device_index : 0; }
+
     bool initialize(std::string& error) override
     {
         if (ctx_) return true;
-        if (nimbus_cuda_create(0, &ctx_) != NIMBUS_OK)
+        if (nimbus_cuda_create(device_, &ctx_) != NIMBUS_OK)
         {
             ctx_ = nullptr;
             error = "no sm_100 CUDA device (the CUDA backend has no CPU fallback)";
@@ -92,6 +96,31 @@ public:
     }
 
     std::uint64_t successful_dispatch_count() const override { return dispatches_; }
+
+    void populate_hardware_info(HardwareInfo& info) const override
+    {
+        nimbus_device_info d{};
+        if (!ctx_ || nimbus_cuda_device_info(ctx_, &d) != NIMBUS_OK) return;
+        info.gpu_available = true;
+        info.gpu_device_name = d.name;
+    }
+
+    // Device-separated HBM, its whole size addressable by one buffer; the
+    // free bytes are a live estimate.  Dispatches stage through a
+    // per-context workspace sized by the largest call.
+    ComputeMemoryProperties memory_properties() const override
+    {
+        ComputeMemoryProperties m{};
+        nimbus_device_info d{};
+        if (!ctx_ || nimbus_cuda_device_info(ctx_, &d) != NIMBUS_OK) return m;
+        m.accelerator = true;
+        m.unified_host_device_memory = false;
+        m.device_local_heap_bytes = d.total_bytes;
+        m.max_storage_buffer_bytes = d.total_bytes;
+        m.device_budget_is_live = true;
+        m.device_available_budget_bytes = d.free_bytes;
+        return m;
+    }
 
     AdvectionComputeKernels* advection_kernels() override { return ctx_ ? this : nullptr; }
     const AdvectionComputeKernels* advection_kernels() const override { return ctx_ ? this : nullptr; }
@@ -602,6 +631,7 @@ private:
     }
 
     nimbus_cuda_context* ctx_ = nullptr;
+    int device_ = 0;
     std::uint64_t dispatches_ = 0;
 };
 

@@ -57,6 +57,7 @@ def _c_layout(struct_name, fields, tmp_path):
     ("nimbus_kessler_pointwise_args", cuda.KesslerPointwiseArgs),
     ("nimbus_kessler_sedimentation_args", cuda.KesslerSedimentationArgs),
     ("nimbus_cgrid_slow_tendencies_args", cuda.CgridSlowTendenciesArgs),
+    ("nimbus_device_info", cuda.DeviceInfo),
     ("nimbus_boundary_args", cuda.BoundaryArgs),
     ("nimbus_state_relaxation_args", cuda.StateRelaxationArgs),
     ("nimbus_cell_centre_args", cuda.CellCentreArgs),

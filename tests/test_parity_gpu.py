@@ -447,3 +447,11 @@ def test_state_relaxation_refuses_invalid_rates(rctx):
     assert rc == cuda.NIMBUS_ERR_INVALID_ARGUMENT
     for k in fields:
         assert np.array_equal(fields[k], st[k]), k
+
+
+def test_device_info_reports_the_b200(ctx):
+    """nimbus_cuda_device_info: what the adapter's populate_hardware_info and
+    memory_properties report to the reference runtime."""
+    info = ctx.device_info()
+    assert info["cc"][0] == 10 and info["sm_count"] > 0 and info["name"]
+    assert 0 < info["free_bytes"] <= info["total_bytes"]
