@@ -76,3 +76,13 @@ def test_reference_program_cuda_backend_step_time(tmp_path):
         times[backend] = float(m.group(1))
     print(f"reference program, 64x64x40 supercell, avg_step_ms: {times}")
     assert all(t > 0 for t in times.values())
+
+
+def test_reference_program_runs_on_the_cuda_backend_with_fallback_off(tmp_path):
+    """allow_fallback: false -- every dispatch the runtime requires natively on
+    an accelerator backend must be served (a declined one is an error): the
+    run completes on the CUDA backend."""
+    log = _run(tmp_path, "cuda", parity=False, steps=4, strict=True)
+    assert re.search(r"\[COMPUTE\] backend=cuda, requested=cuda, .*fallback=off, fallback_allowed=off", log), \
+        log[-3000:]
+    assert re.search(r"\[PERF SUMMARY\].*avg_step_ms=", log), log[-2000:]
