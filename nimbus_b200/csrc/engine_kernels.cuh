@@ -144,10 +144,21 @@ __device__ __forceinline__ void for_member_rows(const EngineMember* __restrict__
 
 // ---- Heun slow step -------------------------------------------------------
 
-// Resident CTAs per SM of the slow Heun pair (64 registers at 4).
+// Resident CTAs per SM of the slow Heun pair: the FP32 form at 5 (48
+// registers; measured 3.14 -> 2.88 ms per ensemble step against 4), the
+// reference-precision form at 4 (64 registers; its FP64 arithmetic spills
+// heavily at 48).
 #ifndef NIMBUS_SLOW_MINB
 #define NIMBUS_SLOW_MINB 4
 #endif
+#ifndef NIMBUS_SLOW_MINB_F32
+#define NIMBUS_SLOW_MINB_F32 5
+#endif
+template <class Policy>
+constexpr int slow_min_blocks()
+{
+    return sizeof(typename Policy::real) == 4 ? NIMBUS_SLOW_MINB_F32 : NIMBUS_SLOW_MINB;
+}
 template <class Policy>
 static __global__ void __launch_bounds__(256, NIMBUS_SLOW_MINB) engine_slow_predict_kernel(const EngineMember* __restrict__ table,
                                                                   const long long* __restrict__ prefix,
@@ -197,7 +208,7 @@ struct SlowLaunch
 static_assert(sizeof(SlowLaunch) <= 32000, "a kernel parameter block holds at most 32764 bytes");
 
 template <class Policy>
-static __global__ void __launch_bounds__(256, NIMBUS_SLOW_MINB) engine_slow_predict_const_kernel(
+static __global__ void __launch_bounds__(256, slow_min_blocks<Policy>()) engine_slow_predict_const_kernel(
     const __grid_constant__ SlowLaunch L, const EngineMember* __restrict__ table, long long tiles)
 {
     int m = 0;
@@ -215,7 +226,7 @@ static __global__ void __launch_bounds__(256, NIMBUS_SLOW_MINB) engine_slow_pred
 }
 
 template <class Policy>
-static __global__ void __launch_bounds__(256, NIMBUS_SLOW_MINB) engine_slow_correct_const_kernel(
+static __global__ void __launch_bounds__(256, slow_min_blocks<Policy>()) engine_slow_correct_const_kernel(
     const __grid_constant__ SlowLaunch L, const EngineMember* __restrict__ table, long long tiles)
 {
     int m = 0;
@@ -1002,8 +1013,14 @@ static __global__ void engine_swap_kernel(EngineMember* table, int members, int 
 // ---- Transport (every scalar of a cell in one thread) -----------------------
 
 template <bool kFp32>
+// Resident CTAs per SM of the face-flux pass: the FP32 form at 4 (64
+// registers; 1.85 -> 1.81 ms per ensemble step), the reference-precision
+// form unbounded.
 #ifndef NIMBUS_FACES_MINB
 #define NIMBUS_FACES_MINB 1
+#endif
+#ifndef NIMBUS_FACES_MINB_F32
+#define NIMBUS_FACES_MINB_F32 4
 #endif
 static __global__ void __launch_bounds__(256, NIMBUS_FACES_MINB) engine_transport_faces_kernel(const EngineMember* __restrict__ table,
                                                                             const long long* __restrict__ prefix,
@@ -1081,7 +1098,7 @@ __device__ __forceinline__ void for_transport_cells(const TransportLaunch& L, co
 }
 
 template <bool kFp32>
-static __global__ void __launch_bounds__(256, NIMBUS_FACES_MINB) engine_transport_faces_const_kernel(
+static __global__ void __launch_bounds__(256, kFp32 ? NIMBUS_FACES_MINB_F32 : NIMBUS_FACES_MINB) engine_transport_faces_const_kernel(
     const __grid_constant__ TransportLaunch L, const EngineMember* __restrict__ table, long long tiles)
 {
     for_transport_cells(L, table, tiles, [&](const TransportConst& A, const EngineMember&, int c) {
