@@ -1015,9 +1015,9 @@ static __global__ void engine_swap_kernel(EngineMember* table, int members, int 
 template <bool kFp32>
 // Resident CTAs per SM of the face-flux pass: the FP32 form at 4 (64
 // registers; 1.85 -> 1.81 ms per ensemble step), the reference-precision
-// form unbounded.
+// form at 2 (its natural 90 registers).
 #ifndef NIMBUS_FACES_MINB
-#define NIMBUS_FACES_MINB 1
+#define NIMBUS_FACES_MINB 2
 #endif
 #ifndef NIMBUS_FACES_MINB_F32
 #define NIMBUS_FACES_MINB_F32 4
@@ -1115,8 +1115,14 @@ static __global__ void __launch_bounds__(256) engine_transport_limiter_const_ker
     });
 }
 
+// Resident CTAs per SM of the update pass: the FP32 form at 4 (64
+// registers; 0.88 -> 0.83 ms per ensemble step), the reference-precision
+// form at 3 (at most 85 registers).
+#ifndef NIMBUS_UPDATE_MINB_F32
+#define NIMBUS_UPDATE_MINB_F32 4
+#endif
 template <bool kFp32>
-static __global__ void __launch_bounds__(256) engine_transport_update_const_kernel(
+static __global__ void __launch_bounds__(256, kFp32 ? NIMBUS_UPDATE_MINB_F32 : 3) engine_transport_update_const_kernel(
     const __grid_constant__ TransportLaunch L, const EngineMember* __restrict__ table, long long tiles)
 {
     for_transport_cells(L, table, tiles, [&](const TransportConst& A, const EngineMember& M, int c) {
@@ -1180,8 +1186,14 @@ static __global__ void __launch_bounds__(256) engine_sound_speed_kernel(const En
 // pressure is formed from the applied state while it is still in registers
 // and written to the member's candidate buffer; engine_swap_kernel publishes
 // it by exchanging p and the candidate unless the projection was refused.
+// Resident CTAs per SM of the Kessler + EOS pass: the FP32 form at 5 (48
+// registers; 1.03 -> 0.99 ms per ensemble step), the reference-precision
+// form at 4.
+#ifndef NIMBUS_MICRO_MINB_F32
+#define NIMBUS_MICRO_MINB_F32 5
+#endif
 template <bool kFp32>
-static __global__ void __launch_bounds__(256, 4) engine_microphysics_eos_kernel(const EngineMember* __restrict__ table,
+static __global__ void __launch_bounds__(256, kFp32 ? NIMBUS_MICRO_MINB_F32 : 4) engine_microphysics_eos_kernel(const EngineMember* __restrict__ table,
                                                                              const long long* __restrict__ prefix,
                                                                              long long tiles)
 {
