@@ -1106,8 +1106,11 @@ static __global__ void __launch_bounds__(256, kFp32 ? NIMBUS_FACES_MINB_F32 : NI
     });
 }
 
+#ifndef NIMBUS_LIMITER_MINB_F32
+#define NIMBUS_LIMITER_MINB_F32 6
+#endif
 template <bool kFp32>
-static __global__ void __launch_bounds__(256) engine_transport_limiter_const_kernel(
+static __global__ void __launch_bounds__(256, kFp32 ? NIMBUS_LIMITER_MINB_F32 : 3) engine_transport_limiter_const_kernel(
     const __grid_constant__ TransportLaunch L, const EngineMember* __restrict__ table, long long tiles)
 {
     for_transport_cells(L, table, tiles, [&](const TransportConst& A, const EngineMember&, int c) {
