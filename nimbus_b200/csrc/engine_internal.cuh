@@ -7,6 +7,7 @@
 #include "engine_kernels.cuh"
 
 #include <algorithm>
+#include <cstring>
 #include <map>
 #include <memory>
 #include <vector>
@@ -297,6 +298,10 @@ int enqueue_step(nimbus_engine* e, int lane, cudaStream_t st, int part)
     };
     const int cform = resolve_form(e->acoustic_form), mform = resolve_form(e->momentum_form);
     std::unique_ptr<AcousticLaunch> al;
+#ifndef NIMBUS_ACOUSTIC_SHARED
+#define NIMBUS_ACOUSTIC_SHARED 1
+#endif
+    bool shared = NIMBUS_ACOUSTIC_SHARED != 0;  // every member's shared values equal al->shared
     if (in_bank(cform) || in_bank(mform))
     {
         al.reset(new AcousticLaunch());
@@ -309,6 +314,13 @@ int enqueue_step(nimbus_engine* e, int lane, cudaStream_t st, int part)
         const long long* pmr = e->prefix.data() + L.prefix_first + static_cast<size_t>(kItemMarch) * (n + 1);
         for (int r = 0; r <= n; ++r) al->march_prefix[r] = pmr[r];
         al->bulk_sy4 = sy4;
+        for (int r = 0; r < n; ++r)
+        {
+            const EngineMember& H = e->slots[static_cast<size_t>(e->order[static_cast<size_t>(L.first + r)])].m;
+            const AcousticShared own = acoustic_shared_of(H.F);
+            if (r == 0) al->shared = own;
+            else if (std::memcmp(&own, &al->shared, sizeof(AcousticShared)) != 0) shared = false;
+        }
         for (int r = 0; r < n; ++r)
         {
             const EngineMember& H = e->slots[static_cast<size_t>(e->order[static_cast<size_t>(L.first + r)])].m;
@@ -342,12 +354,18 @@ int enqueue_step(nimbus_engine* e, int lane, cudaStream_t st, int part)
         switch (cform)
         {
         case NIMBUS_ACOUSTIC_CONST:
-            if (s == 0)
-                ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, (engine_continuity_const_kernel<Policy, true>), tiles, 1,
-                              *al, T, tiles, si);
+            if (s == 0 && shared)
+                ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, (engine_continuity_const_kernel<Policy, true, true>),
+                              tiles, 1, *al, T, tiles, si);
+            else if (s == 0)
+                ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, (engine_continuity_const_kernel<Policy, true, false>),
+                              tiles, 1, *al, T, tiles, si);
+            else if (shared)
+                ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, (engine_continuity_const_kernel<Policy, false, true>),
+                              tiles, 1, *al, T, tiles, si);
             else
-                ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, (engine_continuity_const_kernel<Policy, false>), tiles,
-                              1, *al, T, tiles, si);
+                ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, (engine_continuity_const_kernel<Policy, false, false>),
+                              tiles, 1, *al, T, tiles, si);
             break;
         case NIMBUS_ACOUSTIC_PAIR:
             if (s == 0)

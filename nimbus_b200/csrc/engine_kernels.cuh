@@ -417,6 +417,57 @@ struct AcousticConst
 
 constexpr int kConstMembers = 64;  // members one launch can carry in its parameter
 
+// The part of the parameter block every member of a launch holds alike (field
+// bounds, EOS exponent and coefficients, frame velocity, top condition).  A
+// member's own block is indexed by the member, so each value it supplies is an
+// indexed constant load per cell; from here the kernel takes them as operands
+// at fixed constant-bank offsets.
+struct AcousticShared
+{
+    double gamma, frame_u, frame_v;
+    float rho_min, rho_max, p_min, p_max, p_ref_fallback, frame_u_f, frame_v_f;
+    int top_open;
+    float eos_c[6];
+};
+
+inline AcousticShared acoustic_shared_of(const FusedParams& F)
+{
+    AcousticShared S{};
+    S.gamma = F.gamma;
+    S.frame_u = F.frame_u;
+    S.frame_v = F.frame_v;
+    S.rho_min = F.rho_min;
+    S.rho_max = F.rho_max;
+    S.p_min = F.p_min;
+    S.p_max = F.p_max;
+    S.p_ref_fallback = F.p_ref_fallback;
+    S.frame_u_f = F.frame_u_f;
+    S.frame_v_f = F.frame_v_f;
+    S.top_open = F.top_open;
+    for (int n = 0; n < 6; ++n) S.eos_c[n] = F.eos_c[n];
+    return S;
+}
+
+// A member's block with the shared values read from S (bitwise equal to its
+// own: the launch checks that before choosing a kernel that uses this).
+__device__ __forceinline__ FusedParams with_shared(const FusedParams& F, const AcousticShared& S)
+{
+    FusedParams P = F;
+    P.gamma = S.gamma;
+    P.frame_u = S.frame_u;
+    P.frame_v = S.frame_v;
+    P.rho_min = S.rho_min;
+    P.rho_max = S.rho_max;
+    P.p_min = S.p_min;
+    P.p_max = S.p_max;
+    P.p_ref_fallback = S.p_ref_fallback;
+    P.frame_u_f = S.frame_u_f;
+    P.frame_v_f = S.frame_v_f;
+    P.top_open = S.top_open;
+    for (int n = 0; n < 6; ++n) P.eos_c[n] = S.eos_c[n];
+    return P;
+}
+
 // Resident CTAs per SM the launch bounds ask for (continuity, momentum):
 // measured on the 64-member ensemble, FP32, ms per step: natural register
 // counts (48 / 36 registers) 14.41, 6 / 7 CTAs (40 / 36) 13.49, 8 / 8 (32
@@ -435,12 +486,18 @@ struct AcousticLaunch
     long long march_prefix[kConstMembers + 1];  // first row tile of each member (marching forms)
     AcousticConst m[kConstMembers];
     int bulk_sy4;                               // the members' largest nz rounded up to 4 (bulk-staged forms)
+    AcousticShared shared;                      // every member's shared values (kernels with kShared)
 };
 static_assert(sizeof(AcousticLaunch) <= 32000, "a kernel parameter block holds at most 32764 bytes");
 
 // kFirst: the first substep of the step (the retained fluxes are written, not
 // accumulated, and the beginning density is kept).
-template <class Policy, bool kFirst>
+// kShared: every member's shared values equal L.shared (acoustic_shared_of).
+// Measured on the 64-member ensemble, FP32: continuity 3.58 -> 3.49 ms per
+// step.  (Deriving the member's buffers from one pointer and the arena's field
+// stride as well, two indexed loads instead of eight, spilled at the launch
+// bound and took 3.78 ms.)
+template <class Policy, bool kFirst, bool kShared>
 static __global__ void __launch_bounds__(256, NIMBUS_CONST_MINB) engine_continuity_const_kernel(const __grid_constant__ AcousticLaunch L,
                                                                       const EngineMember* __restrict__ table,
                                                                       long long tiles, int s)
@@ -457,9 +514,17 @@ static __global__ void __launch_bounds__(256, NIMBUS_CONST_MINB) engine_continui
         if (c >= A.F.d.cells()) continue;
         const EngineMember& M = table[m];
         unsigned flags = 0;
-        continuity_eos_cell<Policy>(A.F, even ? M.rho : M.rho_alt, A.u, A.v, A.w, A.theta, A.rho0, A.eos0,
-                                    even ? M.rho_alt : M.rho, M.p, nullptr, A.mfx, A.mfy, A.mfz, c, flags, first,
-                                    first ? A.rho_begin : nullptr);
+        if constexpr (kShared)
+        {
+            const FusedParams F = with_shared(A.F, L.shared);
+            continuity_eos_cell<Policy>(F, even ? M.rho : M.rho_alt, A.u, A.v, A.w, A.theta, A.rho0, A.eos0,
+                                        even ? M.rho_alt : M.rho, M.p, nullptr, A.mfx, A.mfy, A.mfz, c, flags, first,
+                                        first ? A.rho_begin : nullptr);
+        }
+        else
+            continuity_eos_cell<Policy>(A.F, even ? M.rho : M.rho_alt, A.u, A.v, A.w, A.theta, A.rho0, A.eos0,
+                                        even ? M.rho_alt : M.rho, M.p, nullptr, A.mfx, A.mfy, A.mfz, c, flags, first,
+                                        first ? A.rho_begin : nullptr);
         if (flags) atomicOr(A.status, flags);
     }
 }
