@@ -496,7 +496,9 @@ static_assert(sizeof(AcousticLaunch) <= 32000, "a kernel parameter block holds a
 // Measured on the 64-member ensemble, FP32: continuity 3.58 -> 3.49 ms per
 // step.  (Deriving the member's buffers from one pointer and the arena's field
 // stride as well, two indexed loads instead of eight, spilled at the launch
-// bound and took 3.78 ms.)
+// bound and took 3.78 ms; an inner loop over one member's tiles, so that its
+// values could be loaded once per member, kept the loads per cell and took
+// 3.58 ms.)
 template <class Policy, bool kFirst, bool kShared>
 static __global__ void __launch_bounds__(256, NIMBUS_CONST_MINB) engine_continuity_const_kernel(const __grid_constant__ AcousticLaunch L,
                                                                       const EngineMember* __restrict__ table,
