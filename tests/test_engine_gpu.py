@@ -137,6 +137,32 @@ def test_engine_member_alone_equals_member_in_mix(ctx):
         assert_bitwise(got[k], want[k], k)
 
 
+@pytest.mark.parametrize("precision", [cuda.PRECISION_FP32, cuda.PRECISION_REFERENCE], ids=["fp32", "reference"])
+def test_continuity_kernel_with_and_without_launch_shared_values(ctx, precision):
+    """A launch whose members all hold the same bounds, EOS coefficients,
+    frame velocity and top condition reads those from the launch-wide block;
+    one lane that mixes a rigid and an open top reads them per member.  A
+    member's result is the same either way."""
+    case = _case((26, 21, 18), BCS["radiative"], seed=41, dt=3.0)
+    st, base = _state(case, 41)
+    alone = EngineRun(ctx, precision=precision, lanes=1)
+    a = alone.admit(case, st, base)
+    alone.step(3)
+    want = alone.read(a)
+    alone.close()
+
+    mix = EngineRun(ctx, precision=precision, lanes=1)
+    mate = _case((30, 24, 20), BCS["periodic_open"], seed=42, dt=3.0)
+    s2, b2 = _state(mate, 42)
+    mix.admit(mate, s2, b2)
+    m = mix.admit(case, st, base)
+    mix.step(3)
+    got = mix.read(m)
+    mix.close()
+    for k in PROGNOSTIC:
+        assert_bitwise(got[k], want[k], k)
+
+
 def test_engine_matches_plain_fp32_path(ctx):
     case = _case((23, 19, 16), BCS["radiative"], seed=70, dt=3.0)
     st, base = _state(case, 70)
