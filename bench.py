@@ -823,7 +823,8 @@ FAMILY_BYTES = {"acoustic": SUBSTEP_BYTES, "transport": 20 + 8 * 4, "slow": 112,
 def single_run_study(ctx, args, precision):
     """The single-run configurations: the 250 m supercell (256x256x80, dt
     1.5 s, 8 substeps) and the 100 m supercell (512x512x128, dt 0.6 s, 10
-    substeps), each as one member of the engine (graph) and on the plain
+    substeps), each as one member of the engine (graph, its kernel forms
+    autotuned on the grid) and on the plain
     per-operation path, with every kernel family's event-timed duration and
     HBM rate (its algorithmic bytes over that duration, against the measured
     copy rate).  The reference CPU solver runs one large step of the 250 m
@@ -843,6 +844,8 @@ def single_run_study(ctx, args, precision):
         st, base = initial_state(case)
         run = EngineRun(ctx, precision)
         mid = run.admit(case, st, base)
+        ctx.set_precision(precision)
+        tuned = run.engine.autotune(steps=2)  # the kernel forms for this grid (states restored)
         stream = torch.cuda.ExternalStream(run.engine.stream)
         for _ in range(3):
             run.step(1)
@@ -886,7 +889,8 @@ def single_run_study(ctx, args, precision):
                             "whole_step_gbs": round(bytes_step / (ms / 1e3) / 1e9, 1),
                             "whole_step_frac": round(bytes_step / (ms / 1e3) / 1e9 / peak, 4)},
                  "plain": {"ms_per_step": round(p_ms, 4), "value": case.cells / (p_ms / 1e3)},
-                 "kernels": kernels, "peak_gbs": peak, "peak_kind": peak_kind}
+                 "kernels": kernels, "peak_gbs": peak, "peak_kind": peak_kind,
+                 "forms": {"continuity": tuned["continuity_form"], "momentum": tuned["momentum_form"]}}
         if not args.no_cpu_baseline:
             if cpu_rate is None:
                 step, kind, cores, n_ref = reference_step_runner(case, os.cpu_count())

@@ -1050,9 +1050,11 @@ int nimbus_cuda_engine_lanes(const nimbus_engine* e);
  *                          consecutive cells of a row along x (default 16),
  *                          neighbour data of the previous cell carried over in
  *                          registers (the momentum pass's default);
- *   NIMBUS_ACOUSTIC_PAIR   the constant-bank form with two cells per thread
- *                          (both cells' loads issued before either's
- *                          arithmetic);
+ *   NIMBUS_ACOUSTIC_PAIR   the constant-bank form with two vertically
+ *                          adjacent cells per thread (in members with an even
+ *                          nz the pair's values are one 8-byte load per field
+ *                          and neighbour; both cells' loads are issued before
+ *                          either's arithmetic);
  *   NIMBUS_ACOUSTIC_BULK   the constant-bank form with each 256-cell tile's
  *                          stencil data staged in shared memory by bulk
  *                          copies (cp.async.bulk on an mbarrier, four tiles in

@@ -446,6 +446,95 @@ __device__ __forceinline__ void momentum_march(const FusedParams& P, const float
     }
 }
 
+// ---- Two vertically adjacent cells per thread ------------------------------
+// Cells c and c + 1 with c even, of a grid whose nz is even: both lie in one
+// column (k even, k + 1 <= nz - 1), share i and j, and every field's values at
+// the pair and at the pair shifted by +-sx or +-sy are one aligned 8-byte load
+// (member fields start on 256-byte boundaries; sx and sy are even).  Each
+// cell's stencil holds the values the one-cell loads give, clamped
+// neighbours included, and its arithmetic is the one-cell form's.
+__device__ __forceinline__ float2 load_pair(const float* __restrict__ f, int c)
+{
+    return *reinterpret_cast<const float2*>(f + c);
+}
+
+template <class Policy>
+__device__ __forceinline__ void continuity_eos_kpair(const FusedParams& P, const float* __restrict__ rho,
+                                                     const float* __restrict__ u, const float* __restrict__ v,
+                                                     const float* __restrict__ w, const float* __restrict__ theta,
+                                                     const double* __restrict__ rho0,
+                                                     const float4* __restrict__ eos0, float* __restrict__ rho_out,
+                                                     float* __restrict__ p_out, float* __restrict__ mfx,
+                                                     float* __restrict__ mfy, float* __restrict__ mfz, int c,
+                                                     unsigned& flags, bool store_flux, float* __restrict__ rho_copy)
+{
+    const Dims d = P.d;
+    int i, j, k;
+    decompose(d, c, i, j, k);
+    const int sx = d.sx(), sy = d.sy();
+    const bool xlo = i >= 1, xhi = i < d.nx - 1, ylo = j >= 1, yhi = j < d.ny - 1;
+    const bool acc = mfx != nullptr && !store_flux;
+    const float2 r = load_pair(rho, c);
+    const float2 rxp = load_pair(rho, xhi ? c + sx : c), rxm = load_pair(rho, xlo ? c - sx : c);
+    const float2 ryp = load_pair(rho, yhi ? c + sy : c), rym = load_pair(rho, ylo ? c - sy : c);
+    const float rzm = rho[k > 0 ? c - 1 : c];
+    const float rzp = rho[k + 2 < d.nz ? c + 2 : c + 1];
+    const float2 uc = load_pair(u, c), uxm = load_pair(u, xlo ? c - sx : c);
+    const float2 vc = load_pair(v, c), vym = load_pair(v, ylo ? c - sy : c);
+    const float2 wc = load_pair(w, c);
+    const float wzm = w[k > 0 ? c - 1 : c];
+    const float2 th = load_pair(theta, c);
+    float2 mx = make_float2(0.0f, 0.0f), my = mx, mz = mx;
+    if (acc)
+    {
+        mx = load_pair(mfx, c);
+        my = load_pair(mfy, c);
+        mz = load_pair(mfz, c);
+    }
+    ContinuityStencil a, b;
+    a.rho_c = r.x; a.rxp = rxp.x; a.rxm = rxm.x; a.ryp = ryp.x; a.rym = rym.x; a.rzp = r.y; a.rzm = rzm;
+    a.uc = uc.x; a.uxm = uxm.x; a.vc = vc.x; a.vym = vym.x; a.wc = wc.x; a.wzm = wzm; a.th = th.x;
+    a.mx = mx.x; a.my = my.x; a.mz = mz.x;
+    b.rho_c = r.y; b.rxp = rxp.y; b.rxm = rxm.y; b.ryp = ryp.y; b.rym = rym.y; b.rzp = rzp; b.rzm = r.x;
+    b.uc = uc.y; b.uxm = uxm.y; b.vc = vc.y; b.vym = vym.y; b.wc = wc.y; b.wzm = wc.x; b.th = th.y;
+    b.mx = mx.y; b.my = my.y; b.mz = mz.y;
+    continuity_eos_values<Policy>(P, a, i, j, k, c, rho0, eos0, rho_out, p_out, nullptr, mfx, mfy, mfz, flags,
+                                  store_flux, rho_copy);
+    continuity_eos_values<Policy>(P, b, i, j, k + 1, c + 1, rho0, eos0, rho_out, p_out, nullptr, mfx, mfy, mfz, flags,
+                                  store_flux, rho_copy);
+}
+
+// Momentum of the pair (c, c + 1), in place.  Both stencils are loaded before
+// either cell stores: under the vertical closure the cell at nz - 2 writes
+// level nz - 1, which is the pair's second cell when nz - 2 is even, and that
+// cell stores nothing.
+template <class Policy>
+__device__ __forceinline__ void momentum_kpair(const FusedParams& P, const float* __restrict__ rho,
+                                               const float* __restrict__ p, const double* __restrict__ p0,
+                                               const float2* __restrict__ dp0_split, float* u, float* v, float* w,
+                                               int c, int fuse_vertical)
+{
+    const Dims d = P.d;
+    int i, j, k;
+    decompose(d, c, i, j, k);
+    const bool ij = i >= 1 && i < d.nx - 1 && j >= 1 && j < d.ny - 1;
+    const int cx = ij ? c + d.sx() : c, cy = ij ? c + d.sy() : c;
+    const float2 r = load_pair(rho, c), rx = load_pair(rho, cx), ry = load_pair(rho, cy);
+    const float2 pc = load_pair(p, c), px = load_pair(p, cx), py = load_pair(p, cy);
+    const int cz2 = ij && k + 2 < d.nz ? c + 2 : c + 1;
+    const float rz2 = rho[cz2], pz2 = p[cz2];
+    const float2 uc = load_pair(u, c), vc = load_pair(v, c), wc = load_pair(w, c);
+    MomentumStencil a, b;
+    a.rc = r.x; a.rx = rx.x; a.ry = ry.x; a.rz = r.y;
+    a.pc = pc.x; a.px = px.x; a.py = py.x; a.pz = pc.y;
+    a.uc = uc.x; a.vc = vc.x; a.wc = wc.x;
+    b.rc = r.y; b.rx = rx.y; b.ry = ry.y; b.rz = rz2;
+    b.pc = pc.y; b.px = px.y; b.py = py.y; b.pz = pz2;
+    b.uc = uc.y; b.vc = vc.y; b.wc = wc.y;
+    momentum_values<Policy>(P, a, i, j, k, c, p0, dp0_split, u, v, w, fuse_vertical);
+    momentum_values<Policy>(P, b, i, j, k + 1, c + 1, p0, dp0_split, u, v, w, fuse_vertical);
+}
+
 template <class Policy>
 static __global__ void __launch_bounds__(256) split_momentum_kernel(
     FusedParams P, const float* __restrict__ rho, const float* __restrict__ p, const double* __restrict__ p0,

@@ -368,12 +368,22 @@ int enqueue_step(nimbus_engine* e, int lane, cudaStream_t st, int part)
                               tiles, 1, *al, T, tiles, si);
             break;
         case NIMBUS_ACOUSTIC_PAIR:
-            if (s == 0)
-                ENGINE_LAUNCH_BLOCK(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, (engine_continuity_pair_kernel<Policy, true>),
-                                    tiles, kEngineBlock / 2, *al, T, tiles, si);
+            if (s == 0 && shared)
+                ENGINE_LAUNCH_BLOCK(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP,
+                                    (engine_continuity_pair_kernel<Policy, true, true>), tiles, kEngineBlock / 2, *al,
+                                    T, tiles, si);
+            else if (s == 0)
+                ENGINE_LAUNCH_BLOCK(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP,
+                                    (engine_continuity_pair_kernel<Policy, true, false>), tiles, kEngineBlock / 2, *al,
+                                    T, tiles, si);
+            else if (shared)
+                ENGINE_LAUNCH_BLOCK(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP,
+                                    (engine_continuity_pair_kernel<Policy, false, true>), tiles, kEngineBlock / 2, *al,
+                                    T, tiles, si);
             else
-                ENGINE_LAUNCH_BLOCK(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, (engine_continuity_pair_kernel<Policy, false>),
-                                    tiles, kEngineBlock / 2, *al, T, tiles, si);
+                ENGINE_LAUNCH_BLOCK(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP,
+                                    (engine_continuity_pair_kernel<Policy, false, false>), tiles, kEngineBlock / 2,
+                                    *al, T, tiles, si);
             break;
         case NIMBUS_ACOUSTIC_MARCH:
             ENGINE_LAUNCH(NIMBUS_KERNEL_ACOUSTIC_SUBSTEP, engine_continuity_march_kernel<Policy>, march_tiles, 1, T,

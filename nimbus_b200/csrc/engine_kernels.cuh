@@ -603,11 +603,16 @@ static __global__ void __launch_bounds__(256, NIMBUS_CMARCH_MINB) engine_momentu
     });
 }
 
-// The same two passes with two cells per thread: a CTA of half a tile's
-// threads takes cells c and c + blockDim.x of each tile, issuing both
-// stencils' loads before either cell's arithmetic, so a thread has twice the
-// bytes in flight (the passes are memory-latency bound at one cell per
-// thread).  Each cell's arithmetic is the one-cell form's.
+// The same two passes with two vertically adjacent cells per thread: a CTA
+// of half a tile's threads takes cells c and c + 1 (c even) of each tile.  In
+// a member whose nz is even the pair lies in one column, so the pair's index,
+// neighbour offsets and member constants are formed once and every field's
+// values at the pair (and at the pair shifted by +-sx or +-sy) are one 8-byte
+// load (continuity_eos_kpair, momentum_kpair); in a member with an odd nz the
+// thread advances its two cells one after the other.  Each cell's arithmetic
+// is the one-cell form's.  ensemble_64, FP32, one lane: continuity
+// 3.49 -> 3.30 ms per step against the one-cell constant-bank form (cells c
+// and c + 128 per thread instead: 3.97), momentum 2.38 against 2.33 marching.
 #ifndef NIMBUS_PAIR_MINB
 #define NIMBUS_PAIR_MINB 8
 #endif
@@ -615,7 +620,7 @@ static __global__ void __launch_bounds__(256, NIMBUS_CMARCH_MINB) engine_momentu
 #define NIMBUS_PAIR_MINB_MOM 8
 #endif
 
-template <class Policy, bool kFirst>
+template <class Policy, bool kFirst, bool kShared>
 static __global__ void __launch_bounds__(128, NIMBUS_PAIR_MINB) engine_continuity_pair_kernel(const __grid_constant__ AcousticLaunch L,
                                                                      const EngineMember* __restrict__ table,
                                                                      long long tiles, int s)
@@ -623,32 +628,31 @@ static __global__ void __launch_bounds__(128, NIMBUS_PAIR_MINB) engine_continuit
     const bool even = (s & 1) == 0;
     const int half = (int)blockDim.x;
     int m = 0;
-    for (long long t = blockIdx.x; t < tiles; t += gridDim.x)
+    const int ntiles = (int)tiles;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x)
     {
-        while (t >= L.prefix[m + 1]) ++m;
+        while (t >= L.prefix32[m + 1]) ++m;
         const AcousticConst& A = L.m[m];
-        const Dims d = A.F.d;
-        const int n = d.cells();
-        const int c0 = (int)((t - L.prefix[m]) * (2 * half)) + (int)threadIdx.x;
+        const FusedParams F = kShared ? with_shared(A.F, L.shared) : A.F;
+        const int n = F.d.cells();
+        const int c0 = (t - L.prefix32[m]) * (2 * half) + 2 * (int)threadIdx.x;
         if (c0 >= n) continue;
-        const bool two = c0 + half < n;
-        const int c1 = two ? c0 + half : c0;
         const EngineMember& M = table[m];
         const float* rho = even ? M.rho : M.rho_alt;
         float* rho_out = even ? M.rho_alt : M.rho;
-        int i0, j0, k0, i1, j1, k1;
-        decompose(d, c0, i0, j0, k0);
-        decompose(d, c1, i1, j1, k1);
-        const ContinuityStencil s0 = continuity_load(d, rho, A.u, A.v, A.w, A.theta, A.mfx, A.mfy, A.mfz, !kFirst, c0,
-                                                     i0, j0, k0);
-        const ContinuityStencil s1 = continuity_load(d, rho, A.u, A.v, A.w, A.theta, A.mfx, A.mfy, A.mfz, !kFirst, c1,
-                                                     i1, j1, k1);
         unsigned flags = 0;
-        continuity_eos_values<Policy>(A.F, s0, i0, j0, k0, c0, A.rho0, A.eos0, rho_out, M.p, nullptr, A.mfx, A.mfy,
-                                      A.mfz, flags, kFirst, kFirst ? A.rho_begin : nullptr);
-        if (two)
-            continuity_eos_values<Policy>(A.F, s1, i1, j1, k1, c1, A.rho0, A.eos0, rho_out, M.p, nullptr, A.mfx,
-                                          A.mfy, A.mfz, flags, kFirst, kFirst ? A.rho_begin : nullptr);
+        if ((F.d.nz & 1) == 0)
+            continuity_eos_kpair<Policy>(F, rho, A.u, A.v, A.w, A.theta, A.rho0, A.eos0, rho_out, M.p, A.mfx, A.mfy,
+                                         A.mfz, c0, flags, kFirst, kFirst ? A.rho_begin : nullptr);
+        else
+        {
+            continuity_eos_cell<Policy>(F, rho, A.u, A.v, A.w, A.theta, A.rho0, A.eos0, rho_out, M.p, nullptr, A.mfx,
+                                        A.mfy, A.mfz, c0, flags, kFirst, kFirst ? A.rho_begin : nullptr);
+            if (c0 + 1 < n)
+                continuity_eos_cell<Policy>(F, rho, A.u, A.v, A.w, A.theta, A.rho0, A.eos0, rho_out, M.p, nullptr,
+                                            A.mfx, A.mfy, A.mfz, c0 + 1, flags, kFirst,
+                                            kFirst ? A.rho_begin : nullptr);
+        }
         if (flags) atomicOr(A.status, flags);
     }
 }
@@ -661,25 +665,25 @@ static __global__ void __launch_bounds__(128, NIMBUS_PAIR_MINB_MOM) engine_momen
     const bool even = (s & 1) == 0;
     const int half = (int)blockDim.x;
     int m = 0;
-    for (long long t = blockIdx.x; t < tiles; t += gridDim.x)
+    const int ntiles = (int)tiles;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x)
     {
-        while (t >= L.prefix[m + 1]) ++m;
+        while (t >= L.prefix32[m + 1]) ++m;
         const AcousticConst& A = L.m[m];
         const Dims d = A.F.d;
         const int n = d.cells();
-        const int c0 = (int)((t - L.prefix[m]) * (2 * half)) + (int)threadIdx.x;
+        const int c0 = (t - L.prefix32[m]) * (2 * half) + 2 * (int)threadIdx.x;
         if (c0 >= n) continue;
-        const bool two = c0 + half < n;
-        const int c1 = two ? c0 + half : c0;
         const EngineMember& M = table[m];
         const float* rho = even ? M.rho_alt : M.rho;
-        int i0, j0, k0, i1, j1, k1;
-        decompose(d, c0, i0, j0, k0);
-        decompose(d, c1, i1, j1, k1);
-        const MomentumStencil s0 = momentum_load(d, rho, M.p, A.u, A.v, A.w, c0, i0, j0, k0);
-        const MomentumStencil s1 = momentum_load(d, rho, M.p, A.u, A.v, A.w, c1, i1, j1, k1);
-        momentum_values<Policy>(A.F, s0, i0, j0, k0, c0, A.p0, A.dp0, A.u, A.v, A.w, A.vertical);
-        if (two) momentum_values<Policy>(A.F, s1, i1, j1, k1, c1, A.p0, A.dp0, A.u, A.v, A.w, A.vertical);
+        if ((d.nz & 1) == 0)
+            momentum_kpair<Policy>(A.F, rho, M.p, A.p0, A.dp0, A.u, A.v, A.w, c0, A.vertical);
+        else
+        {
+            momentum_cell<Policy>(A.F, rho, M.p, A.p0, A.dp0, A.u, A.v, A.w, A.u, A.v, A.w, c0, A.vertical);
+            if (c0 + 1 < n)
+                momentum_cell<Policy>(A.F, rho, M.p, A.p0, A.dp0, A.u, A.v, A.w, A.u, A.v, A.w, c0 + 1, A.vertical);
+        }
     }
 }
 
