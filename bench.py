@@ -68,6 +68,9 @@ def parse():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-single", action="store_true", help="skip the 250 m and 100 m single-run legs")
     ap.add_argument("--no-autotune", action="store_true", help="keep --lanes and the default kernel form")
+    ap.add_argument("--pass-forms", default=None, metavar="CONTINUITY,MOMENTUM",
+                    help="with --no-autotune: the acoustic passes' kernel forms, each one of "
+                         "table, const, march, pair, bulk, cmarch")
     ap.add_argument("--scaling", choices=("weak", "strong"), default="weak",
                     help="weak: each rank its own ensemble; strong: one ensemble split over the ranks")
     ap.add_argument("--no-error", action="store_true")
@@ -628,11 +631,17 @@ def run_ours(args):
     if not args.no_autotune:
         ctx.set_precision(precision)
         tuned = run.engine.autotune(steps=2)
+    elif args.pass_forms:
+        names = {"table": cuda.ACOUSTIC_TABLE, "const": cuda.ACOUSTIC_CONST, "march": cuda.ACOUSTIC_MARCH,
+                 "pair": cuda.ACOUSTIC_PAIR, "bulk": cuda.ACOUSTIC_BULK, "cmarch": cuda.ACOUSTIC_CMARCH}
+        cont, mom = (names[f.strip()] for f in args.pass_forms.split(","))
+        run.engine.set_pass_forms(cont, mom)
     stream = torch.cuda.ExternalStream(run.engine.stream, device=f"cuda:{device}")
     for _ in range(max(args.warmup, 3)):
         run.step(1)
     ctx.synchronize()
     lanes_used = run.engine.lanes  # the lanes the built table uses
+    forms_used = [cuda.ACOUSTIC_FORM_NAMES[f] for f in run.engine.pass_forms]
     barrier()
     torch.cuda.synchronize()
     launches0 = ctx.kernel_launches
@@ -776,6 +785,7 @@ def run_ours(args):
                 "form": f"batched member engine: the runs in {lanes_used} size-balanced lanes (parallel branches of "
                         "one CUDA graph), one launch per phase per lane",
                 "lanes": lanes_used,
+                "pass_forms": {"continuity": forms_used[0], "momentum": forms_used[1]},
                 "autotune": tuned,
                 "precision": args.precision,
                 "precision_modes": {
