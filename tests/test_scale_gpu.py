@@ -248,6 +248,8 @@ def test_device_sound_speed_scan_matches_oracle(ctx, o32):
 
 T, C, M, P2, B, CM = (cuda.ACOUSTIC_TABLE, cuda.ACOUSTIC_CONST, cuda.ACOUSTIC_MARCH, cuda.ACOUSTIC_PAIR,
                       cuda.ACOUSTIC_BULK, cuda.ACOUSTIC_CMARCH)
+# Members of the multi-tile set with odd (41, 45) and even (50, 42) nz.
+FORM_MEMBERS = (0, 1, 5, 6)
 
 
 @pytest.mark.parametrize("forms,march", [((T, T), 16), ((M, M), 5), ((M, M), 1000), ((P2, P2), 16),
@@ -270,12 +272,45 @@ def test_engine_acoustic_kernel_form_does_not_change_results(ctx, multi_tile, fo
     run.engine.set_march(march)
     assert run.engine.pass_forms == forms and run.engine.march == march
     assert run.engine.acoustic_form == forms[0]
-    ids = [run.admit(case, st, base, coriolis_f=1e-4) for case, st, base in members[:4]]
+    ids = [run.admit(*members[i][:3], coriolis_f=1e-4) for i in FORM_MEMBERS]
     run.step(2)
-    for mid, (case, _, _), (ref, _) in zip(ids, members, want):
+    for mid, i in zip(ids, FORM_MEMBERS):
+        case, ref = members[i][0], want[i][0]
         got = run.read(mid)
         for k in PROGNOSTIC:
             assert_bitwise(got[k], ref[k], f"forms {forms} march {march} member {mid} {case.shape} {k}")
+    run.close()
+
+
+@pytest.fixture(scope="module")
+def fp32_const(ctx, multi_tile):
+    """The FORM_MEMBERS after two FP32 steps in the default forms."""
+    members, _ = multi_tile
+    run = EngineRun(ctx, precision=cuda.PRECISION_FP32)
+    run.engine.set_acoustic_form(C)
+    ids = [run.admit(*members[i][:3], coriolis_f=1e-4) for i in FORM_MEMBERS]
+    run.step(2)
+    out = [run.read(mid) for mid in ids]
+    run.close()
+    return out
+
+
+@pytest.mark.parametrize("forms", [(T, T), (P2, P2), (P2, M), (C, P2), (M, M), (CM, CM), (B, B)],
+                         ids=["table", "pair", "pair-march", "const-pair", "march", "cmarch", "bulk"])
+def test_fp32_kernel_forms_give_the_same_bits(ctx, multi_tile, fp32_const, forms):
+    """In the FP32 form too, every acoustic kernel form gives the bits of the
+    constant-bank default (the arithmetic is one sequence; the FP32 unit's FMA
+    contraction must not differ between the forms), for members with odd and
+    even nz (the two-cell form's paired loads)."""
+    members, _ = multi_tile
+    run = EngineRun(ctx, precision=cuda.PRECISION_FP32)
+    run.engine.set_pass_forms(*forms)
+    ids = [run.admit(*members[i][:3], coriolis_f=1e-4) for i in FORM_MEMBERS]
+    run.step(2)
+    for mid, i, ref in zip(ids, FORM_MEMBERS, fp32_const):
+        got = run.read(mid)
+        for k in PROGNOSTIC:
+            assert_bitwise(got[k], ref[k], f"fp32 forms {forms} member {i} {members[i][0].shape} {k}")
     run.close()
 
 
