@@ -451,8 +451,9 @@ __device__ __forceinline__ void momentum_march(const FusedParams& P, const float
 // column (k even, k + 1 <= nz - 1), share i and j, and every field's values at
 // the pair and at the pair shifted by +-sx or +-sy are one aligned 8-byte load
 // (member fields start on 256-byte boundaries; sx and sy are even).  Each
-// cell's stencil holds the values the one-cell loads give, clamped
-// neighbours included, and its arithmetic is the one-cell form's.
+// cell's stencil holds the values the one-cell loads give wherever its
+// arithmetic reads them (a neighbour outside the grid or the interior may
+// hold another in-range value), and its arithmetic is the one-cell form's.
 __device__ __forceinline__ float2 load_pair(const float* __restrict__ f, int c)
 {
     return *reinterpret_cast<const float2*>(f + c);
