@@ -288,7 +288,90 @@ void destroy_graphs(nimbus_engine* e)
         if (e->graph[part]) cudaGraphDestroy(e->graph[part]);
         e->exec[part] = nullptr;
         e->graph[part] = nullptr;
+        for (auto& c : e->exec_cache[part]) cudaGraphExecDestroy(c.exec);
+        e->exec_cache[part].clear();
     }
+}
+
+constexpr size_t kExecCache = 8;  // instantiated topologies kept per part
+
+// Topology key of a captured graph: its node and edge counts and, in node
+// order, each node's type and, for kernel nodes, the kernel.  Graphs with
+// equal keys are captured by the same launch sequence; an update that the
+// runtime refuses all the same only costs the instantiation it would have
+// taken anyway.
+uint64_t graph_topology_key(cudaGraph_t g)
+{
+    uint64_t h = 1469598103934665603ull;  // FNV-1a
+    auto mix = [&](uint64_t v) {
+        for (int b = 0; b < 8; ++b)
+        {
+            h ^= (v >> (8 * b)) & 0xffu;
+            h *= 1099511628211ull;
+        }
+    };
+    size_t n = 0, edges = 0;
+    if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess) return 0;
+    if (cudaGraphGetEdges(g, nullptr, nullptr, &edges) != cudaSuccess) return 0;
+    mix(n);
+    mix(edges);
+    std::vector<cudaGraphNode_t> nodes(n);
+    if (n && cudaGraphGetNodes(g, nodes.data(), &n) != cudaSuccess) return 0;
+    for (cudaGraphNode_t node : nodes)
+    {
+        cudaGraphNodeType type;
+        if (cudaGraphNodeGetType(node, &type) != cudaSuccess) return 0;
+        mix(static_cast<uint64_t>(type));
+        if (type == cudaGraphNodeTypeKernel)
+        {
+            cudaKernelNodeParams kp{};
+            if (cudaGraphKernelNodeGetParams(node, &kp) != cudaSuccess) return 0;
+            mix(reinterpret_cast<uint64_t>(kp.func));
+        }
+    }
+    return h == 0 ? 1 : h;
+}
+
+// Makes exec (instantiated from a graph of the same key) run g; false when the
+// runtime refuses the update.
+bool update_exec(cudaGraphExec_t exec, cudaGraph_t g)
+{
+    cudaGraphExecUpdateResultInfo info{};
+    if (cudaGraphExecUpdate(exec, g, &info) == cudaSuccess) return true;
+    (void)cudaGetLastError();  // a refused update is not an error of the engine
+    return false;
+}
+
+void park_exec(nimbus_engine* e, int part, uint64_t key, cudaGraphExec_t exec)
+{
+    auto& cache = e->exec_cache[part];
+    if (key == 0)
+    {
+        cudaGraphExecDestroy(exec);
+        return;
+    }
+    if (cache.size() >= kExecCache)
+    {
+        size_t oldest = 0;
+        for (size_t i = 1; i < cache.size(); ++i)
+            if (cache[i].used < cache[oldest].used) oldest = i;
+        cudaGraphExecDestroy(cache[oldest].exec);
+        cache.erase(cache.begin() + static_cast<std::ptrdiff_t>(oldest));
+    }
+    cache.push_back({key, exec, ++e->exec_clock});
+}
+
+cudaGraphExec_t take_exec(nimbus_engine* e, int part, uint64_t key)
+{
+    auto& cache = e->exec_cache[part];
+    for (size_t i = 0; i < cache.size(); ++i)
+        if (cache[i].key == key)
+        {
+            cudaGraphExec_t x = cache[i].exec;
+            cache.erase(cache.begin() + static_cast<std::ptrdiff_t>(i));
+            return x;
+        }
+    return nullptr;
 }
 
 nimbus_status rebuild_table(nimbus_engine* e)
@@ -533,16 +616,25 @@ nimbus_status build_graphs(nimbus_engine* e)
         cudaGraph_t g = nullptr;
         const cudaError_t end = cudaStreamEndCapture(st, &g);
         if (end != cudaSuccess) return cuda_fail(ctx, end, "engine graph capture");
+        const uint64_t key = graph_topology_key(g);
         bool updated = false;
-        if (e->exec[part])
+        if (e->exec[part] && key != 0 && e->exec_key[part] == key) updated = update_exec(e->exec[part], g);
+        if (!updated && e->exec[part])
         {
-            cudaGraphExecUpdateResultInfo info{};
-            updated = cudaGraphExecUpdate(e->exec[part], g, &info) == cudaSuccess;
-            if (!updated)
+            park_exec(e, part, e->exec_key[part], e->exec[part]);  // its topology may come back
+            e->exec[part] = nullptr;
+        }
+        if (!updated && key != 0)
+        {
+            if (cudaGraphExec_t x = take_exec(e, part, key))
             {
-                (void)cudaGetLastError();  // a refused update is not an error of the engine
-                cudaGraphExecDestroy(e->exec[part]);
-                e->exec[part] = nullptr;
+                if (update_exec(x, g))
+                {
+                    e->exec[part] = x;
+                    updated = true;
+                }
+                else
+                    cudaGraphExecDestroy(x);
             }
         }
         if (!updated)
@@ -559,6 +651,7 @@ nimbus_status build_graphs(nimbus_engine* e)
         }
         else
             ++e->graph_updates;
+        e->exec_key[part] = key;
         if (e->graph[part]) cudaGraphDestroy(e->graph[part]);
         e->graph[part] = g;
         e->launches_part[part] = launches;

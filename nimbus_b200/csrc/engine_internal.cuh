@@ -76,6 +76,19 @@ struct nimbus_engine
     // host reads the next step's counts while that step's part 0 runs.
     cudaGraph_t graph[2] = {nullptr, nullptr};
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    uint64_t exec_key[2] = {0, 0};  // topology key of exec (graph_topology_key)
+    // Instantiated graphs of topologies used before (lane count and substep
+    // counts come and go as runs are admitted and retire): a rebuild whose
+    // topology matches one of them updates it in place instead of
+    // instantiating anew.  Least recently used first out.
+    struct CachedExec
+    {
+        uint64_t key;
+        cudaGraphExec_t exec;
+        uint64_t used;
+    };
+    std::vector<CachedExec> exec_cache[2];
+    uint64_t exec_clock = 0;
     int launches_per_step = 0;
     int launches_part[2] = {0, 0};
     bool graphs_stale = true;       // the table changed since the graphs were captured
