@@ -163,6 +163,44 @@ def test_continuity_kernel_with_and_without_launch_shared_values(ctx, precision)
         assert_bitwise(got[k], want[k], k)
 
 
+def test_recurring_graph_topology_is_updated_not_instantiated(ctx):
+    """A batch that returns to a lane and substep layout it had before reuses
+    that layout's instantiated step graphs (updated in place), and the
+    members' results do not depend on which instantiation ran them."""
+    cases = [_case((24, 20, 16), BCS["radiative"], seed=70 + i, dt=3.0) for i in range(2)]
+    states = [_state(c, 70 + i) for i, c in enumerate(cases)]
+    mate = _case((36, 30, 22), BCS["periodic_open"], seed=80, dt=2.0)
+    mate_st, mate_base = _state(mate, 80)
+
+    def run_cycle(cycles):
+        run = EngineRun(ctx, precision=cuda.PRECISION_FP32, lanes=2)
+        ids = [run.admit(c, s, b, n_substeps=4) for c, (s, b) in zip(cases, states)]
+        run.step(1)
+        builds = []
+        for _ in range(cycles):
+            m = run.admit(mate, mate_st, mate_base, n_substeps=6)
+            run.step(1)
+            run.engine.retire(m)
+            run.step(1)
+            builds.append(run.engine.graph_builds())
+        out = [run.read(i) for i in ids]
+        run.close()
+        return out, builds
+
+    got, builds = run_cycle(3)
+    # every later cycle finds both layouts among the kept instantiations
+    assert builds[2][0] == builds[0][0], builds
+    assert builds[2][1] > builds[0][1], builds
+    alone = EngineRun(ctx, precision=cuda.PRECISION_FP32, lanes=2)
+    ids = [alone.admit(c, s, b, n_substeps=4) for c, (s, b) in zip(cases, states)]
+    alone.step(7)
+    want = [alone.read(i) for i in ids]
+    alone.close()
+    for g, w in zip(got, want):
+        for k in PROGNOSTIC:
+            assert_bitwise(g[k], w[k], k)
+
+
 def test_engine_matches_plain_fp32_path(ctx):
     case = _case((23, 19, 16), BCS["radiative"], seed=70, dt=3.0)
     st, base = _state(case, 70)
