@@ -246,6 +246,33 @@ def test_device_sound_speed_scan_matches_oracle(ctx, o32):
         ctx.max_sound_speed(bad, st["rho"], case.shape, base)
 
 
+def test_sound_speed_scan_on_ties_and_extreme_magnitudes(ctx):
+    """Fields full of equal ratios p / rho from different values (p and rho
+    scaled by the same factor, whose quotients (gamma p) / rho round apart),
+    and magnitudes far outside the physical range, give the per-cell maximum
+    of (gamma p) / rho in FP64 bit for bit."""
+    gamma = 1004.0 / (1004.0 - 287.0)
+    rng = np.random.default_rng(21)
+    shape = (23, 19, 17)
+    n = int(np.prod(shape))
+    base_p = rng.uniform(5e4, 1e5, n).astype(np.float32)
+    base_r = rng.uniform(0.5, 1.2, n).astype(np.float32)
+    k = rng.integers(1, 40, n).astype(np.float32)  # exact scalings: the ratios tie, the quotients may not
+    # 50000 and 0.75 have few significant bits, so k * each is exact and every ratio is 50000 / 0.75
+    ties_p, ties_r = (np.float32(50000.0) * k).astype(np.float32), (np.float32(0.75) * k).astype(np.float32)
+    cases = {
+        "ties": (ties_p, ties_r),
+        "mixed": (np.where(rng.random(n) < 0.5, ties_p, base_p), np.where(rng.random(n) < 0.5, ties_r, base_r)),
+        "huge": ((rng.uniform(1, 3, n) * 1e37).astype(np.float32), rng.uniform(10, 3e5, n).astype(np.float32)),
+        "tiny": ((rng.uniform(1, 3, n) * 1e-20).astype(np.float32), (rng.uniform(1, 3, n) * 1e-18).astype(np.float32)),
+    }
+    for name, (p, r) in cases.items():
+        p = np.ascontiguousarray(p.reshape(shape), np.float32)
+        r = np.ascontiguousarray(r.reshape(shape), np.float32)
+        want = float(np.sqrt(np.max((gamma * p.astype(np.float64)) / r.astype(np.float64))))
+        assert ctx.max_sound_speed(p, r, shape) == want, name
+
+
 T, C, M, P2, B, CM = (cuda.ACOUSTIC_TABLE, cuda.ACOUSTIC_CONST, cuda.ACOUSTIC_MARCH, cuda.ACOUSTIC_PAIR,
                       cuda.ACOUSTIC_BULK, cuda.ACOUSTIC_CMARCH)
 # Members of the multi-tile set with odd (41, 45) and even (50, 42) nz.
