@@ -5,9 +5,8 @@
 // copies it is about to issue (mbarrier.arrive.expect_tx: the barrier's single
 // arrival), then each copy signals its bytes on the barrier
 // (mbarrier::complete_tx); consumers wait on the stage's phase parity.  Every
-// copy moves whole 16-byte units between 16-byte-aligned addresses.  No
-// multicast: each CTA copies from this GPU's own memory into its own shared
-// memory.
+// copy moves whole 16-byte units between 16-byte-aligned addresses.  Each CTA
+// copies from this GPU's own memory into its own shared memory only.
 //
 // Waits are bounded: a wait that has not seen its phase complete after about
 // two seconds of clock cycles gives up and reports it, so a protocol fault
